@@ -1,0 +1,174 @@
+"""Loads ``libcellweave_b200.so`` and declares its C ABI for ctypes.
+
+The library is the product: there is no CPU path.  Loading fails loudly when
+the shared object is missing, and every call that fails raises the error the
+reference would return (``CellweaveError``, crates/core/src/error.rs:7-23).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcellweave_b200.so")
+
+OK, ERR_CONFIG, ERR_SIMULATION, ERR_ODE, ERR_NOT_FOUND, ERR_CUDA, ERR_TIMEOUT = range(7)
+
+
+class CellweaveError(RuntimeError):
+    """Base of every error the library returns."""
+
+
+class ConfigError(CellweaveError):
+    """CellweaveError::Config."""
+
+
+class SimulationError(CellweaveError):
+    """CellweaveError::Simulation (for example a field that did not settle)."""
+
+
+class OdeSolverError(CellweaveError):
+    """CellweaveError::OdeSolver."""
+
+
+class NotFoundError(CellweaveError):
+    """CellweaveError::NotFound."""
+
+
+class CudaError(CellweaveError):
+    """A CUDA call failed, or there is no usable device."""
+
+
+class TimeoutError_(CellweaveError):
+    """A bounded device loop ran out of iterations."""
+
+
+_ERRORS = {ERR_CONFIG: ConfigError, ERR_SIMULATION: SimulationError, ERR_ODE: OdeSolverError,
+           ERR_NOT_FOUND: NotFoundError, ERR_CUDA: CudaError, ERR_TIMEOUT: TimeoutError_}
+
+
+class RelaxOpts(C.Structure):
+    _fields_ = [("omega", C.c_double), ("stop", C.c_int32), ("tolerance", C.c_double), ("max_sweeps", C.c_int64),
+                ("precision", C.c_int32), ("inner_sweeps", C.c_int32), ("block_depth", C.c_int32)]
+
+
+class RelaxStats(C.Structure):
+    _fields_ = [("sweeps", C.c_int64), ("last_change", C.c_double), ("residual", C.c_double),
+                ("status", C.c_int32), ("omega", C.c_double)]
+
+
+class TermSpec(C.Structure):
+    _fields_ = [("node", C.c_int32), ("kind", C.c_int32), ("source", C.c_char_p), ("rate", C.c_double),
+                ("hill_n", C.c_double), ("hill_k", C.c_double), ("param", C.c_double), ("has_hill", C.c_int32)]
+
+
+class SimConfig(C.Structure):
+    _fields_ = [("nh", C.c_uint32), ("w", C.c_void_p), ("h", C.c_void_p), ("d", C.c_void_p),
+                ("ncells", C.c_void_p), ("seeds", C.c_void_p), ("temperature", C.c_double), ("K", C.c_int32),
+                ("J", C.c_void_p), ("contact_order", C.c_int32), ("target_volume", C.c_int32),
+                ("lambda_volume", C.c_double), ("surface_target", C.c_int32), ("lambda_surface", C.c_double),
+                ("seeding", C.c_int32), ("seed_side", C.c_int32), ("nfields", C.c_int32), ("o2_dcoef", C.c_double),
+                ("o2_sink_by_type", C.c_void_p), ("o2_hold", C.c_int32), ("signal_dcoef", C.c_double),
+                ("signal_decay", C.c_double), ("signal_secretion", C.c_double), ("hypoxic_level", C.c_double),
+                ("tolerance", C.c_double), ("precision", C.c_int32), ("omega", C.c_double),
+                ("relax_every", C.c_int32), ("dt", C.c_double), ("substeps", C.c_int32), ("sweeps", C.c_int32),
+                ("death_threshold", C.c_double), ("necrotic_type", C.c_int32)]
+
+
+P = C.c_void_p
+U32, I32, I64, U64, D = C.c_uint32, C.c_int32, C.c_int64, C.c_uint64, C.c_double
+
+SIGNATURES = {
+    "cw_last_error": (C.c_char_p, []),
+    "cw_version": (C.c_int, []),
+    "cw_set_stream": (C.c_int, [P]),
+    "cw_get_stream": (P, []),
+    "cw_synchronize": (C.c_int, []),
+    "cw_launch_count": (C.c_uint64, []),
+    "cw_lattice_create": (C.c_int, [U32, P, P, P, P, D, P]),
+    "cw_lattice_destroy": (C.c_int, [P]),
+    "cw_lattice_count": (C.c_int, [P, P]),
+    "cw_lattice_set_contact": (C.c_int, [P, I32, P, I32]),
+    "cw_lattice_set_temperature": (C.c_int, [P, D]),
+    "cw_lattice_upload": (C.c_int, [P, U32, P]),
+    "cw_lattice_download": (C.c_int, [P, U32, P]),
+    "cw_cells_set": (C.c_int, [P, U32, U32, P, P, P, P]),
+    "cw_cells_get": (C.c_int, [P, U32, U32, P, P, P, P]),
+    "cw_cells_set_surface": (C.c_int, [P, U32, U32, P, P]),
+    "cw_cells_get_surface": (C.c_int, [P, U32, U32, P]),
+    "cw_lattice_set_seed": (C.c_int, [P, U32, U64]),
+    "cw_lattice_set_mcs": (C.c_int, [P, U32]),
+    "cw_lattice_get_mcs": (C.c_int, [P, P]),
+    "cw_lattice_mcs": (C.c_int, [P, U32]),
+    "cw_lattice_delta_h_batch": (C.c_int, [P, U32, U32, P, P, P]),
+    "cw_lattice_verify": (C.c_int, [P, U32, P]),
+    "cw_field_create": (C.c_int, [U32, P, P, P, D, D, D, P]),
+    "cw_field_destroy": (C.c_int, [P]),
+    "cw_field_set_source": (C.c_int, [P, D]),
+    "cw_field_set_diffusion": (C.c_int, [P, D]),
+    "cw_field_upload": (C.c_int, [P, U32, I32, P]),
+    "cw_field_download": (C.c_int, [P, U32, I32, P]),
+    "cw_field_upload_held": (C.c_int, [P, U32, P]),
+    "cw_field_download_held": (C.c_int, [P, U32, P]),
+    "cw_field_fill": (C.c_int, [P, D]),
+    "cw_field_clear": (C.c_int, [P, I32]),
+    "cw_field_release_all": (C.c_int, [P]),
+    "cw_field_hold_mask": (C.c_int, [P, U32, P, D]),
+    "cw_field_hold_bath": (C.c_int, [P, U32, P, D]),
+    "cw_field_relax": (C.c_int, [P, P, P]),
+    "cw_field_residual": (C.c_int, [P, P]),
+    "cw_field_inflow": (C.c_int, [P, P]),
+    "cw_field_step": (C.c_int, [P, D]),
+    "cw_couple_uptake": (C.c_int, [P, P, I32, P, I32]),
+    "cw_couple_background_uptake": (C.c_int, [P, P, D]),
+    "cw_couple_production": (C.c_int, [P, P, U32, U32, P]),
+    "cw_couple_hold_obstacles": (C.c_int, [P, P, D]),
+    "cw_couple_hold_medium_bath": (C.c_int, [P, P, D]),
+    "cw_couple_mean_per_cell": (C.c_int, [P, P, U32, U32, P]),
+    "cw_network_compile": (C.c_int, [I32, P, P, I32, P, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p,
+                                     C.c_char_p, C.c_char_p, C.c_char_p, D, D, D, U32, P]),
+    "cw_network_destroy": (C.c_int, [P]),
+    "cw_network_info": (C.c_int, [P, P, P, P]),
+    "cw_network_step_batch": (C.c_int, [P, I64, P, P, D, I32]),
+    "cw_network_mechanics_batch": (C.c_int, [P, I64, P, P, P]),
+    "cw_sim_create": (C.c_int, [P, P, P]),
+    "cw_sim_destroy": (C.c_int, [P]),
+    "cw_sim_step": (C.c_int, [P, U32]),
+    "cw_sim_lattice": (C.c_int, [P, P]),
+    "cw_sim_field": (C.c_int, [P, I32, P]),
+    "cw_sim_stats": (C.c_int, [P, P]),
+    "cw_sim_network_state": (C.c_int, [P, U32, U32, P]),
+    "cw_event_record": (C.c_int, [I32]),
+    "cw_event_elapsed": (C.c_int, [I32, I32, P]),
+}
+
+_LIB = None
+
+
+def lib():
+    """The loaded library (raises ``CudaError`` when the shared object is missing)."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise CudaError(f"{LIB_PATH} is not built: run cellweave_b200/build.py (nvcc, sm_100a)")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _LIB = L
+    return _LIB
+
+
+def check(rc: int) -> None:
+    if rc != OK:
+        msg = lib().cw_last_error().decode(errors="replace")
+        raise _ERRORS.get(rc, CellweaveError)(msg)
+
+
+def call(name: str, *args):
+    check(getattr(lib(), name)(*args))
+
+
+def ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)

@@ -1,0 +1,122 @@
+// Library-wide plumbing: errors, the stream, launch counting, batch geometry.
+#include <atomic>
+#include <cstring>
+
+#include "cw_internal.cuh"
+
+namespace cw {
+
+static thread_local std::string g_error;
+static std::atomic<uint64_t> g_launches{0};
+static cudaStream_t g_own_stream = nullptr;
+static cudaStream_t g_user_stream = nullptr;
+static bool g_user_set = false;
+
+void set_error(const std::string &msg) { g_error = msg; }
+
+int fail(int code, const std::string &msg) {
+    g_error = msg;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char *what) {
+    g_error = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+    return CW_ERR_CUDA;
+}
+
+cudaStream_t stream() {
+    if (g_user_set) return g_user_stream;
+    if (!g_own_stream) cudaStreamCreateWithFlags(&g_own_stream, cudaStreamNonBlocking);
+    return g_own_stream;
+}
+
+void count_launch(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+int Geom::init(uint32_t n, const uint32_t *W, const uint32_t *H, const uint32_t *D) {
+    if (n == 0) return fail(CW_ERR_CONFIG, "a batch needs at least one history");
+    nh = n;
+    w.resize(n); h.resize(n); d.resize(n); off.assign(n + 1, 0);
+    std::vector<int4> dims(n);
+    for (uint32_t k = 0; k < n; ++k) {
+        uint32_t a = W[k], b = H[k], c = D ? D[k] : 1;
+        if (a == 0 || b == 0 || c == 0 || a > 65535 || b > 65535 || c > 65535)
+            return fail(CW_ERR_CONFIG, "invalid grid dimensions (" + std::to_string(a) + "x" + std::to_string(b) +
+                                           "x" + std::to_string(c) + ") of history " + std::to_string(k));
+        w[k] = (int32_t)a; h[k] = (int32_t)b; d[k] = (int32_t)c;
+        off[k + 1] = off[k] + (int64_t)a * b * c;
+        dims[k] = make_int4((int)a, (int)b, (int)c, 0);
+    }
+    total = off[n];
+    int rc;
+    if ((rc = dalloc(&d_dims, n)) != CW_OK) return rc;
+    if ((rc = dalloc(&d_off, n + 1)) != CW_OK) return rc;
+    CW_CUDA(cudaMemcpy(d_dims, dims.data(), sizeof(int4) * n, cudaMemcpyHostToDevice));
+    CW_CUDA(cudaMemcpy(d_off, off.data(), sizeof(int64_t) * (n + 1), cudaMemcpyHostToDevice));
+    return CW_OK;
+}
+
+void Geom::release() {
+    dfree(d_dims);
+    dfree(d_off);
+}
+
+int Plan::build(const std::vector<int64_t> &per, int threads) {
+    nh = (uint32_t)per.size();
+    items = per;
+    blk.assign(nh + 1, 0);
+    for (uint32_t k = 0; k < nh; ++k) blk[k + 1] = blk[k] + (int32_t)((per[k] + threads - 1) / threads);
+    nblocks = blk[nh];
+    if (!d_blk) {
+        int rc = dalloc(&d_blk, nh + 1);
+        if (rc != CW_OK) return rc;
+    }
+    CW_CUDA(cudaMemcpyAsync(d_blk, blk.data(), sizeof(int32_t) * (nh + 1), cudaMemcpyHostToDevice, stream()));
+    return CW_OK;
+}
+
+void Plan::release() { dfree(d_blk); }
+
+}  // namespace cw
+
+extern "C" {
+
+const char *cw_last_error(void) { return cw::g_error.c_str(); }
+
+int cw_version(void) { return 1; }
+
+int cw_set_stream(void *s) {
+    cw::g_user_stream = (cudaStream_t)s;
+    cw::g_user_set = s != nullptr;
+    return CW_OK;
+}
+
+void *cw_get_stream(void) { return (void *)cw::stream(); }
+
+int cw_synchronize(void) {
+    CW_CUDA(cudaStreamSynchronize(cw::stream()));
+    return CW_OK;
+}
+
+uint64_t cw_launch_count(void) { return cw::g_launches.load(); }
+
+}  // extern "C"
+
+// Timing on the library stream: events in numbered slots.
+namespace {
+cudaEvent_t g_events[16] = {};
+}
+
+extern "C" int cw_event_record(int32_t slot) {
+    if (slot < 0 || slot >= 16) return cw::fail(CW_ERR_CONFIG, "event slots are 0 to 15");
+    if (!g_events[slot]) CW_CUDA(cudaEventCreate(&g_events[slot]));
+    CW_CUDA(cudaEventRecord(g_events[slot], cw::stream()));
+    return CW_OK;
+}
+
+extern "C" int cw_event_elapsed(int32_t a, int32_t b, float *ms) {
+    if (a < 0 || a >= 16 || b < 0 || b >= 16 || !g_events[a] || !g_events[b])
+        return cw::fail(CW_ERR_CONFIG, "both events must have been recorded");
+    CW_CUDA(cudaEventSynchronize(g_events[b]));
+    CW_CUDA(cudaEventElapsedTime(ms, g_events[a], g_events[b]));
+    return CW_OK;
+}

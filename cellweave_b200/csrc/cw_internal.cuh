@@ -1,0 +1,238 @@
+// Internal declarations shared by the library's translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/cellweave_b200.h"
+
+namespace cw {
+
+// ------------------------------------------------------------------ errors
+void set_error(const std::string &msg);
+int fail(int code, const std::string &msg);
+int cuda_fail(cudaError_t e, const char *what);
+cudaStream_t stream();
+void count_launch(uint64_t n = 1);
+
+#define CW_CUDA(call)                                                      \
+    do {                                                                   \
+        cudaError_t e_ = (call);                                           \
+        if (e_ != cudaSuccess) return ::cw::cuda_fail(e_, #call);          \
+    } while (0)
+
+#define CW_LAUNCHED()                                                      \
+    do {                                                                   \
+        ::cw::count_launch();                                              \
+        cudaError_t e_ = cudaGetLastError();                               \
+        if (e_ != cudaSuccess) return ::cw::cuda_fail(e_, "kernel launch"); \
+    } while (0)
+
+// ------------------------------------------------------------------ device memory
+template <class T>
+int dalloc(T **p, size_t n) {
+    *p = nullptr;
+    if (n == 0) n = 1;
+    cudaError_t e = cudaMalloc((void **)p, n * sizeof(T));
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc");
+    return CW_OK;
+}
+template <class T>
+void dfree(T *&p) {
+    if (p) cudaFree((void *)p);
+    p = nullptr;
+}
+
+// ------------------------------------------------------------------ batch geometry
+// Histories packed one after another in flat site order; each history's
+// pixels keep the reference's order: x fastest, then y, then z.
+struct Geom {
+    uint32_t nh = 0;
+    std::vector<int32_t> w, h, d;
+    std::vector<int64_t> off;  // nh + 1
+    int64_t total = 0;
+    int4 *d_dims = nullptr;    // (w, h, d, 0) per history
+    int64_t *d_off = nullptr;  // nh + 1
+    int init(uint32_t n, const uint32_t *W, const uint32_t *H, const uint32_t *D);
+    void release();
+    int64_t sites(uint32_t k) const { return off[k + 1] - off[k]; }
+    bool same(const Geom &o) const { return w == o.w && h == o.h && d == o.d; }
+};
+
+// Blocks of a launch distributed over histories: history k owns blocks
+// [blk[k], blk[k+1]).  Built on the host from per-history item counts.
+struct Plan {
+    uint32_t nh = 0;
+    int32_t nblocks = 0;
+    std::vector<int32_t> blk;     // nh + 1
+    std::vector<int64_t> items;   // per history
+    int32_t *d_blk = nullptr;     // nh + 1
+    int build(const std::vector<int64_t> &items_per_history, int threads);
+    void release();
+};
+
+__device__ __forceinline__ int plan_history(const int32_t *blk, int nh, int b) {
+    int lo = 0, hi = nh - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (__ldg(blk + mid) <= b) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// ------------------------------------------------------------------ Philox4x32-10
+// Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy as 1, 2, 3"
+// (SC'11): ten rounds of two 32x32->64 multiplies and a Weyl key schedule.
+__host__ __device__ __forceinline__ uint4 philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0,
+                                                 uint32_t k1) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+#ifdef __CUDA_ARCH__
+        uint32_t lo0 = 0xD2511F53u * c0, hi0 = __umulhi(0xD2511F53u, c0);
+        uint32_t lo1 = 0xCD9E8D57u * c2, hi1 = __umulhi(0xCD9E8D57u, c2);
+#else
+        uint64_t p0 = (uint64_t)0xD2511F53u * c0, p1 = (uint64_t)0xCD9E8D57u * c2;
+        uint32_t lo0 = (uint32_t)p0, hi0 = (uint32_t)(p0 >> 32), lo1 = (uint32_t)p1, hi1 = (uint32_t)(p1 >> 32);
+#endif
+        uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+        c0 = n0; c1 = lo1; c2 = n2; c3 = lo0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    return make_uint4(c0, c1, c2, c3);
+}
+
+// 53 random bits from two words as a double in [0, 1).
+__host__ __device__ __forceinline__ double u01(uint32_t a, uint32_t b) {
+    return ((double)(a >> 5) * 67108864.0 + (double)(b >> 6)) * (1.0 / 9007199254740992.0);
+}
+
+// exp(x) from + - * and a power-of-two scaling only, so that host and device
+// round alike (the translation units that use it build without fused
+// multiply-add): Cody-Waite reduction by ln 2 split into a 20-bit head and
+// its tail, then a degree-17 Taylor polynomial of e^r, |r| <= ln2 / 2.
+__host__ __device__ __forceinline__ double own_exp(double x) {
+    if (!(x > -745.0)) return 0.0;
+    if (x > 709.0) return HUGE_VAL;
+    const double log2e = 1.4426950408889634;
+    const double ln2_hi = 0.6931467056274414;
+    const double ln2_lo = 4.7493250390316726e-07;
+    double kf = floor(x * log2e + 0.5);
+    double r = (x - kf * ln2_hi) - kf * ln2_lo;
+    double p = 1.0 / 355687428096000.0;
+    p = p * r + 1.0 / 20922789888000.0;
+    p = p * r + 1.0 / 1307674368000.0;
+    p = p * r + 1.0 / 87178291200.0;
+    p = p * r + 1.0 / 6227020800.0;
+    p = p * r + 1.0 / 479001600.0;
+    p = p * r + 1.0 / 39916800.0;
+    p = p * r + 1.0 / 3628800.0;
+    p = p * r + 1.0 / 362880.0;
+    p = p * r + 1.0 / 40320.0;
+    p = p * r + 1.0 / 5040.0;
+    p = p * r + 1.0 / 720.0;
+    p = p * r + 1.0 / 120.0;
+    p = p * r + 1.0 / 24.0;
+    p = p * r + 1.0 / 6.0;
+    p = p * r + 0.5;
+    p = p * r + 1.0;
+    p = p * r + 1.0;
+    return ldexp(p, (int)kf);
+}
+
+// Non-negative doubles order like their bit patterns.
+__device__ __forceinline__ void atomic_max_nonneg(unsigned long long *addr, double v) {
+    if (!(v >= 0.0)) return;
+    atomicMax(addr, (unsigned long long)__double_as_longlong(v));
+}
+
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// ------------------------------------------------------------------ handles
+struct Span {
+    int32_t x0, x1, y0, y1, z0, z1;
+    int32_t found, pad;
+};
+
+}  // namespace cw
+
+struct cw_lattice_s {
+    cw::Geom g;
+    std::vector<int64_t> cell_off;   // nh + 1
+    int64_t ncells = 0;              // all histories
+    int32_t *grid = nullptr;
+    int32_t *type = nullptr, *volume = nullptr, *target = nullptr;
+    double *lambda = nullptr;
+    int32_t *vsnap = nullptr;
+    int32_t *surface = nullptr, *ssnap = nullptr, *tsurf = nullptr;
+    double *lsurf = nullptr;
+    bool surface_on = false;
+    int64_t *d_cell_off = nullptr;
+    int32_t K = 1;
+    double J[64] = {0};
+    int32_t order = 1;
+    double temperature = 10.0;
+    uint32_t mcs = 0;
+    std::vector<uint64_t> seed;
+    uint2 *d_keys = nullptr;         // Philox key per history
+    // colour plans: one per colour
+    int32_t ncol = 0, period = 0;
+    std::vector<cw::Plan> plans;
+    int32_t nreach = 0;
+    int8_t reach[3 * 124] = {0};
+    double across = 1.0;
+    int32_t *d_flag = nullptr;       // scratch flag / counters
+    int build_plans();
+};
+
+struct cw_field_s {
+    cw::Geom g;
+    double *c = nullptr;             // values
+    uint8_t *held = nullptr;
+    double *uptake = nullptr, *production = nullptr, *lin_sink = nullptr;
+    bool lin_sink_on = false;
+    double dcoef = 0.2, decay = 0.0, source = 0.0;
+    // scratch of the FP32 defect-correction solve and the explicit step
+    float *r32 = nullptr, *d32a = nullptr, *d32b = nullptr, *inv32 = nullptr;
+    double *tmp64 = nullptr;
+    void *stats = nullptr;           // per-history solve state (device)
+    cw::Span *d_span = nullptr;
+    int alloc_fp32();
+};
+
+namespace cw {
+// translation-unit entry points used across files
+int field_span(cw_field_s *f, std::vector<Span> &spans);
+int lattice_recount(cw_lattice_s *lat, int32_t *vol_out, int32_t *surf_out);
+int lattice_sweep(cw_lattice_s *lat);
+// coupling (coupling.cu), device-resident
+int couple_uptake_device(cw_field_s *f, cw_lattice_s *l, const double *d_rate_by_type, int K, double *dst,
+                         const Plan &p);
+int couple_production_device(cw_field_s *f, cw_lattice_s *l, const double *d_per_cell, const Plan &p);
+int couple_means_device(cw_field_s *f, cw_lattice_s *l, double *sum, int32_t *count, double *mean, const Plan &p);
+}  // namespace cw
+
+struct cw_network_s;
+namespace cw {
+// network (network.cu), device-resident, node-major state [S][stride]
+int network_step_device(const cw_network_s *n, double *state, const double *inputs, int64_t ncells,
+                        int64_t state_stride, int64_t input_stride, double dt, int substeps, const uint8_t *alive);
+int network_mechanics_device(const cw_network_s *n, const double *state, int64_t ncells, int64_t stride,
+                             uint32_t *target);
+int32_t network_nodes(const cw_network_s *n);
+double network_lambda(const cw_network_s *n);
+int32_t network_role(const cw_network_s *n, int k);
+const std::vector<double> &network_initial(const cw_network_s *n);
+}  // namespace cw

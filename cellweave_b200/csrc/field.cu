@@ -1,0 +1,813 @@
+// Diffusion field: ScalarField of crates/engine/src/pde.rs on the device.
+//
+// Two solvers stand side by side:
+//  * CW_FP64: the reference's red-black SOR (relax / sor_sweep / half_sweep,
+//    pde.rs:245-405) pixel for pixel in FP64.  This file is built without
+//    fused multiply-add, so each pixel's update rounds exactly as the Rust
+//    does, and red-black order makes the in-place update equal to the
+//    reference's read-one-buffer/write-the-other (pde.rs:322-328): the field
+//    and the sweep count are bit-identical to the reference's.
+//  * CW_FP32_DC: defect correction.  The FP64 residual r = b - A c is formed,
+//    A d = r is relaxed in FP32 by red-black SOR sweeps (field32.cu, kept in
+//    shared memory several half-sweeps deep), and c += d in FP64, until the
+//    projected residual is below the tolerance.
+#include <algorithm>
+#include <cmath>
+#include <cstddef>
+#include <cstring>
+
+#include "cw_internal.cuh"
+#include "field_kernels.cuh"
+
+using namespace cw;
+
+namespace {
+
+struct RelaxState {
+    unsigned long long moved[2];  // max |change| of the red and the black half-sweep
+    unsigned long long resid;     // max projected residual
+    double omega;
+    double tol;
+    int64_t sweeps;               // sweeps taken, final once done
+    int32_t done;                 // 0 running, 1 converged
+    int32_t stop;
+    double last_change;
+    double last_resid;
+    int64_t inner;                // FP32 sweeps taken (defect correction)
+};
+
+__device__ __forceinline__ void locate(const int4 dm, int64_t local, int &x, int &y, int &z) {
+    x = (int)(local % dm.x);
+    int64_t r = local / dm.x;
+    y = (int)(r % dm.y);
+    z = (int)(r / dm.y);
+}
+
+// The box around every free pixel (free_span, pde.rs:305-320).
+__global__ void k_span(const uint8_t *__restrict__ held, const int4 *dims, const int64_t *off, const int32_t *blk,
+                       int nh, Span *span) {
+    __shared__ int s_h;
+    if (threadIdx.x == 0) s_h = plan_history(blk, nh, blockIdx.x);
+    __syncthreads();
+    int h = s_h;
+    int64_t local = (int64_t)(blockIdx.x - blk[h]) * blockDim.x + threadIdx.x;
+    int64_t n = off[h + 1] - off[h];
+    bool ok = local < n && !held[off[h] + local];
+    int x = 0, y = 0, z = 0;
+    if (ok) locate(dims[h], local, x, y, z);
+    // warp-level reduction first, then one atomic per warp
+    int xmin = ok ? x : INT_MAX, xmax = ok ? x : -1, ymin = ok ? y : INT_MAX, ymax = ok ? y : -1;
+    int zmin = ok ? z : INT_MAX, zmax = ok ? z : -1;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        xmin = min(xmin, __shfl_xor_sync(0xffffffffu, xmin, o));
+        xmax = max(xmax, __shfl_xor_sync(0xffffffffu, xmax, o));
+        ymin = min(ymin, __shfl_xor_sync(0xffffffffu, ymin, o));
+        ymax = max(ymax, __shfl_xor_sync(0xffffffffu, ymax, o));
+        zmin = min(zmin, __shfl_xor_sync(0xffffffffu, zmin, o));
+        zmax = max(zmax, __shfl_xor_sync(0xffffffffu, zmax, o));
+    }
+    if ((threadIdx.x & 31) == 0 && xmax >= 0) {
+        atomicMin(&span[h].x0, xmin); atomicMax(&span[h].x1, xmax);
+        atomicMin(&span[h].y0, ymin); atomicMax(&span[h].y1, ymax);
+        atomicMin(&span[h].z0, zmin); atomicMax(&span[h].z1, zmax);
+        span[h].found = 1;
+    }
+}
+
+__global__ void k_span_reset(Span *span, int nh) {
+    int h = blockIdx.x * blockDim.x + threadIdx.x;
+    if (h < nh) span[h] = Span{INT_MAX, -1, INT_MAX, -1, INT_MAX, -1, 0, 0};
+}
+
+// One half-sweep of the reference's SOR, in place, FP64 (half_sweep,
+// pde.rs:329-405).  Items enumerate the pixels of `colour` inside the span.
+__global__ void k_sor64_half(FieldView fv, const int32_t *blk, int nh, const Span *span, RelaxState *st,
+                             int colour) {
+    __shared__ int s_h;
+    if (threadIdx.x == 0) s_h = plan_history(blk, nh, blockIdx.x);
+    __syncthreads();
+    int h = s_h;
+    if (st[h].done) return;
+    const Span sp = span[h];
+    const int4 dm = fv.dims[h];
+    int sw = sp.x1 - sp.x0 + 1, hw = (sw + 1) >> 1, ny = sp.y1 - sp.y0 + 1;
+    int64_t k = (int64_t)(blockIdx.x - blk[h]) * blockDim.x + threadIdx.x;
+    double moved = 0.0;
+    int64_t rows = (int64_t)ny * (sp.z1 - sp.z0 + 1);
+    if (k < rows * hw) {
+        int64_t row = k / hw;
+        int j = (int)(k - row * hw);
+        int y = sp.y0 + (int)(row % ny), z = sp.z0 + (int)(row / ny);
+        int x = sp.x0 + ((colour - (sp.x0 + y + z)) & 1) + 2 * j;
+        if (x <= sp.x1) {
+            int64_t i = fv.off[h] + ((int64_t)z * dm.y + y) * dm.x + x;
+            if (!fv.held[i]) {
+                double before = fv.c[i];
+                double sum, real;
+                pixel_sums64(fv.c, i, x, y, z, dm, sum, real);
+                double den = real * fv.d + fv.decay;
+                if (fv.ks) den = den + fv.ks[i];
+                double balanced = (fv.d * sum + fv.source + fv.pr[i] - fv.up[i]) / den;
+                double om = st[h].omega;
+                double after = fmax((1.0 - om) * before + om * balanced, 0.0);
+                fv.c[i] = after;
+                moved = fabs(after - before);
+            }
+        }
+    }
+    moved = warp_max(moved);
+    if ((threadIdx.x & 31) == 0 && moved > 0.0) atomic_max_nonneg(&st[h].moved[colour], moved);
+}
+
+// Projected residual max |b - A c| over the free pixels of each history;
+// optionally writes r in FP32 for the defect-correction solve, the FP32
+// inverse diagonal (0 on held pixels), and zeroes the correction.
+__global__ void k_residual64(FieldView fv, const int32_t *blk, int nh, RelaxState *st, float *r32, float *inv32,
+                             float *dz, int skip_done) {
+    __shared__ int s_h;
+    if (threadIdx.x == 0) s_h = plan_history(blk, nh, blockIdx.x);
+    __syncthreads();
+    int h = s_h;
+    if (skip_done && st[h].done) return;
+    const int4 dm = fv.dims[h];
+    int64_t local = (int64_t)(blockIdx.x - blk[h]) * blockDim.x + threadIdx.x;
+    int64_t n = fv.off[h + 1] - fv.off[h];
+    double worst = 0.0;
+    if (local < n) {
+        int64_t i = fv.off[h] + local;
+        int x, y, z;
+        locate(dm, local, x, y, z);
+        float r_out = 0.0f, inv_out = 0.0f;
+        if (!fv.held[i]) {
+            double sum, real;
+            pixel_sums64(fv.c, i, x, y, z, dm, sum, real);
+            double den = real * fv.d + fv.decay;
+            if (fv.ks) den = den + fv.ks[i];
+            double cv = fv.c[i];
+            double r = (fv.d * sum + fv.source + fv.pr[i] - fv.up[i]) - den * cv;
+            if (cv <= 0.0 && r < 0.0) r = 0.0;
+            worst = fabs(r);
+            r_out = (float)r;
+            inv_out = den > 0.0 ? (float)(1.0 / den) : 0.0f;
+        }
+        if (r32) r32[i] = r_out;
+        if (inv32) inv32[i] = inv_out;
+        if (dz) dz[i] = 0.0f;
+    }
+    worst = warp_max(worst);
+    if ((threadIdx.x & 31) == 0 && worst > 0.0) atomic_max_nonneg(&st[h].resid, worst);
+}
+
+// After sweep `index`: decide convergence (relax's `moved < tolerance`,
+// pde.rs:280-283, or the residual rule) and reset the accumulators.
+__global__ void k_check(RelaxState *st, int nh, int64_t index, int residual_counted) {
+    int h = blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= nh) return;
+    RelaxState &s = st[h];
+    if (!s.done) {
+        double m = fmax(__longlong_as_double((long long)s.moved[0]), __longlong_as_double((long long)s.moved[1]));
+        double r = __longlong_as_double((long long)s.resid);
+        s.last_change = m;
+        if (residual_counted) s.last_resid = r;
+        bool conv = s.stop == CW_STOP_RESIDUAL ? r < s.tol : m < s.tol;
+        s.sweeps = index;
+        if (conv) s.done = 1;
+    }
+    s.moved[0] = s.moved[1] = 0ull;
+    s.resid = 0ull;
+}
+
+// Defect correction: c += d on free pixels, floored at zero as the
+// reference's update is (pde.rs:395).
+__global__ void k_dc_correct(FieldView fv, const int32_t *blk, int nh, const RelaxState *st, const float *dlt) {
+    __shared__ int s_h;
+    if (threadIdx.x == 0) s_h = plan_history(blk, nh, blockIdx.x);
+    __syncthreads();
+    int h = s_h;
+    if (st[h].done) return;
+    int64_t local = (int64_t)(blockIdx.x - blk[h]) * blockDim.x + threadIdx.x;
+    if (local >= fv.off[h + 1] - fv.off[h]) return;
+    int64_t i = fv.off[h] + local;
+    if (fv.held[i]) return;
+    fv.c[i] = fmax(fv.c[i] + (double)dlt[i], 0.0);
+}
+
+__global__ void k_dc_check(RelaxState *st, int nh, int inner, int64_t max_sweeps) {
+    int h = blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= nh) return;
+    RelaxState &s = st[h];
+    if (!s.done) {
+        double r = __longlong_as_double((long long)s.resid);
+        s.last_resid = r;
+        if (r < s.tol) s.done = 1;
+        else if (s.inner >= max_sweeps) s.done = 2;  // out of sweeps: reported as not settled
+        else { s.inner += inner; s.sweeps = s.inner; }
+    }
+    s.resid = 0ull;
+}
+
+// inflow (pde.rs:415-456): flux from held pixels into free ones.
+__global__ void k_inflow(FieldView fv, const int32_t *blk, int nh, double *out) {
+    __shared__ int s_h;
+    if (threadIdx.x == 0) s_h = plan_history(blk, nh, blockIdx.x);
+    __syncthreads();
+    int h = s_h;
+    const int4 dm = fv.dims[h];
+    int64_t local = (int64_t)(blockIdx.x - blk[h]) * blockDim.x + threadIdx.x;
+    double flux = 0.0;
+    if (local < fv.off[h + 1] - fv.off[h]) {
+        int64_t i = fv.off[h] + local;
+        if (!fv.held[i]) {
+            int x, y, z;
+            locate(dm, local, x, y, z);
+            int64_t w = dm.x, slice = (int64_t)dm.x * dm.y;
+            double ci = fv.c[i];
+            if (x > 0 && fv.held[i - 1]) flux += fv.d * (fv.c[i - 1] - ci);
+            if (x + 1 < dm.x && fv.held[i + 1]) flux += fv.d * (fv.c[i + 1] - ci);
+            if (y > 0 && fv.held[i - w]) flux += fv.d * (fv.c[i - w] - ci);
+            if (y + 1 < dm.y && fv.held[i + w]) flux += fv.d * (fv.c[i + w] - ci);
+            if (z > 0 && fv.held[i - slice]) flux += fv.d * (fv.c[i - slice] - ci);
+            if (z + 1 < dm.z && fv.held[i + slice]) flux += fv.d * (fv.c[i + slice] - ci);
+        }
+    }
+    flux = warp_sum(flux);
+    if ((threadIdx.x & 31) == 0 && flux != 0.0) atomicAdd(out + h, flux);
+}
+
+// DiffusionField::step (pde.rs:705-728), out of place.
+__global__ void k_explicit(FieldView fv, const int32_t *blk, int nh, double dt, double *next) {
+    __shared__ int s_h;
+    if (threadIdx.x == 0) s_h = plan_history(blk, nh, blockIdx.x);
+    __syncthreads();
+    int h = s_h;
+    const int4 dm = fv.dims[h];
+    int64_t local = (int64_t)(blockIdx.x - blk[h]) * blockDim.x + threadIdx.x;
+    if (local >= fv.off[h + 1] - fv.off[h]) return;
+    int64_t i = fv.off[h] + local;
+    double c = fv.c[i];
+    if (fv.held[i]) { next[i] = c; return; }
+    int x, y, z;
+    locate(dm, local, x, y, z);
+    int64_t w = dm.x, slice = (int64_t)dm.x * dm.y;
+    double a = x > 0 ? fv.c[i - 1] : c;
+    double b = x + 1 < dm.x ? fv.c[i + 1] : c;
+    double e = y > 0 ? fv.c[i - w] : c;
+    double g = y + 1 < dm.y ? fv.c[i + w] : c;
+    double lap = a + b + e + g - 4.0 * c;
+    if (dm.z > 1) {
+        double p = z > 0 ? fv.c[i - slice] : c;
+        double q = z + 1 < dm.z ? fv.c[i + slice] : c;
+        lap += p + q - 2.0 * c;
+    }
+    double change = fv.d * lap - fv.decay * c + fv.source + fv.pr[i] - fv.up[i];
+    next[i] = fmax(c + dt * change, 0.0);
+}
+
+__global__ void k_fill64(double *p, int64_t n, double v) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = v;
+}
+
+__global__ void k_hold_mask(double *c, uint8_t *held, const uint8_t *mask, int64_t n, double v) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && mask[i]) { held[i] = 1; c[i] = v; }
+}
+
+// ---- bath (hold_bath_at, pde.rs:550-631) ------------------------------------
+__global__ void k_bath_box(const uint8_t *open, const int4 *dims, const int64_t *off, const int32_t *blk, int nh,
+                           Span *box) {
+    __shared__ int s_h;
+    if (threadIdx.x == 0) s_h = plan_history(blk, nh, blockIdx.x);
+    __syncthreads();
+    int h = s_h;
+    int64_t local = (int64_t)(blockIdx.x - blk[h]) * blockDim.x + threadIdx.x;
+    if (local >= off[h + 1] - off[h]) return;
+    if (open[off[h] + local]) return;
+    int x, y, z;
+    locate(dims[h], local, x, y, z);
+    atomicMin(&box[h].x0, x); atomicMax(&box[h].x1, x);
+    atomicMin(&box[h].y0, y); atomicMax(&box[h].y1, y);
+    atomicMin(&box[h].z0, z); atomicMax(&box[h].z1, z);
+    box[h].found = 1;
+}
+
+__device__ __forceinline__ bool in_box(const Span &b, const int4 dm, int x, int y, int z, Span &e) {
+    e.x0 = max(b.x0 - 1, 0); e.x1 = min(b.x1 + 1, dm.x - 1);
+    e.y0 = max(b.y0 - 1, 0); e.y1 = min(b.y1 + 1, dm.y - 1);
+    e.z0 = max(b.z0 - 1, 0); e.z1 = min(b.z1 + 1, dm.z - 1);
+    return b.found && e.x0 <= x && x <= e.x1 && e.y0 <= y && y <= e.y1 && e.z0 <= z && z <= e.z1;
+}
+
+__global__ void k_bath_init(const uint8_t *open, uint8_t *held, const int4 *dims, const int64_t *off,
+                            const int32_t *blk, int nh, const Span *box, int only_hist) {
+    __shared__ int s_h;
+    if (threadIdx.x == 0) s_h = plan_history(blk, nh, blockIdx.x);
+    __syncthreads();
+    int h = s_h;
+    if (only_hist >= 0 && h != only_hist) return;
+    const int4 dm = dims[h];
+    int64_t local = (int64_t)(blockIdx.x - blk[h]) * blockDim.x + threadIdx.x;
+    if (local >= off[h + 1] - off[h]) return;
+    int64_t i = off[h] + local;
+    int x, y, z;
+    locate(dm, local, x, y, z);
+    Span e;
+    if (!in_box(box[h], dm, x, y, z, e)) { held[i] = 1; return; }
+    bool outer = x == e.x0 || x == e.x1 || y == e.y0 || y == e.y1 || (dm.z > 1 && (z == e.z0 || z == e.z1));
+    if (outer && open[i]) held[i] = 1;
+}
+
+// Spread the bath one step through faces, in place (monotone, so stale reads
+// only delay); `changed` counts pixels newly reached.
+__global__ void k_bath_spread(const uint8_t *open, uint8_t *held, const int4 *dims, const int64_t *off,
+                              const int32_t *blk, int nh, const Span *box, int only_hist, int *changed) {
+    __shared__ int s_h;
+    if (threadIdx.x == 0) s_h = plan_history(blk, nh, blockIdx.x);
+    __syncthreads();
+    int h = s_h;
+    if (only_hist >= 0 && h != only_hist) return;
+    const int4 dm = dims[h];
+    int64_t local = (int64_t)(blockIdx.x - blk[h]) * blockDim.x + threadIdx.x;
+    if (local >= off[h + 1] - off[h]) return;
+    int64_t i = off[h] + local;
+    if (held[i] || !open[i]) return;
+    int x, y, z;
+    locate(dm, local, x, y, z);
+    int64_t w = dm.x, slice = (int64_t)dm.x * dm.y;
+    bool r = (x > 0 && held[i - 1]) || (x + 1 < dm.x && held[i + 1]) || (y > 0 && held[i - w]) ||
+             (y + 1 < dm.y && held[i + w]) || (z > 0 && held[i - slice]) || (z + 1 < dm.z && held[i + slice]);
+    if (r) {
+        held[i] = 1;
+        atomicAdd(changed, 1);
+    }
+}
+
+__global__ void k_bath_values(double *c, const uint8_t *held, const int64_t *off, const int32_t *blk, int nh,
+                              int only_hist, double v) {
+    __shared__ int s_h;
+    if (threadIdx.x == 0) s_h = plan_history(blk, nh, blockIdx.x);
+    __syncthreads();
+    int h = s_h;
+    if (only_hist >= 0 && h != only_hist) return;
+    int64_t local = (int64_t)(blockIdx.x - blk[h]) * blockDim.x + threadIdx.x;
+    if (local >= off[h + 1] - off[h]) return;
+    int64_t i = off[h] + local;
+    if (held[i]) c[i] = v;
+}
+
+constexpr int T = 256;
+
+int64_t blocks_for(int64_t n) { return (n + T - 1) / T; }
+
+struct SitePlan {
+    // per-handle plan over every site of every history, built once
+    Plan p;
+};
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+namespace cw {
+
+FieldView view(cw_field_s *f) {
+    FieldView v;
+    v.c = f->c; v.held = f->held; v.up = f->uptake; v.pr = f->production;
+    v.ks = f->lin_sink_on ? f->lin_sink : nullptr;
+    v.d = f->dcoef; v.decay = f->decay; v.source = f->source;
+    v.dims = f->g.d_dims; v.off = f->g.d_off;
+    return v;
+}
+
+static int site_plan(cw_field_s *f, Plan &p) {
+    std::vector<int64_t> per(f->g.nh);
+    for (uint32_t k = 0; k < f->g.nh; ++k) per[k] = f->g.sites(k);
+    return p.build(per, T);
+}
+
+int field_span(cw_field_s *f, std::vector<Span> &spans) {
+    Plan p;
+    int rc = site_plan(f, p);
+    if (rc != CW_OK) return rc;
+    k_span_reset<<<(f->g.nh + 63) / 64, 64, 0, stream()>>>(f->d_span, f->g.nh);
+    CW_LAUNCHED();
+    k_span<<<p.nblocks, T, 0, stream()>>>(f->held, f->g.d_dims, f->g.d_off, p.d_blk, f->g.nh, f->d_span);
+    CW_LAUNCHED();
+    spans.resize(f->g.nh);
+    CW_CUDA(cudaMemcpyAsync(spans.data(), f->d_span, sizeof(Span) * f->g.nh, cudaMemcpyDeviceToHost, stream()));
+    CW_CUDA(cudaStreamSynchronize(stream()));
+    p.release();
+    return CW_OK;
+}
+
+}  // namespace cw
+
+int cw_field_s::alloc_fp32() {
+    if (r32) return CW_OK;
+    int rc;
+    int64_t n = g.total;
+    if ((rc = dalloc(&r32, n)) != CW_OK) return rc;
+    if ((rc = dalloc(&d32a, n)) != CW_OK) return rc;
+    if ((rc = dalloc(&d32b, n)) != CW_OK) return rc;
+    if ((rc = dalloc(&inv32, n)) != CW_OK) return rc;
+    return CW_OK;
+}
+
+// The reference's relaxation factor (pde.rs:267-277), on the host.
+static double auto_omega(const cw_field_s *f, uint32_t k, const Span &s) {
+    if (f->g.d[k] > 1) {
+        int32_t l = std::max({s.x1 - s.x0 + 1, s.y1 - s.y0 + 1, s.z1 - s.z0 + 1});
+        l = std::max(l, 2);
+        return 2.0 / (1.0 + std::sin(3.14159265358979323846 / (double)l));
+    }
+    double n = (double)std::max(f->g.w[k], f->g.h[k]);
+    return std::min(2.0 / (1.0 + std::sin(3.14159265358979323846 / n)), 1.95);
+}
+
+static int relax_fp64(cw_field_s *f, const cw_relax_opts &o, std::vector<Span> &spans, RelaxState *d_st,
+                      std::vector<RelaxState> &hs) {
+    uint32_t nh = f->g.nh;
+    FieldView fv = view(f);
+    // per-colour plans over the span
+    Plan pc[2], ps;
+    for (int colour = 0; colour < 2; ++colour) {
+        std::vector<int64_t> per(nh, 0);
+        for (uint32_t k = 0; k < nh; ++k) {
+            const Span &s = spans[k];
+            if (!s.found) continue;
+            int64_t hw = (s.x1 - s.x0 + 2) / 2;
+            per[k] = hw * (int64_t)(s.y1 - s.y0 + 1) * (s.z1 - s.z0 + 1);
+        }
+        int rc = pc[colour].build(per, T);
+        if (rc != CW_OK) return rc;
+    }
+    int rc = site_plan(f, ps);
+    if (rc != CW_OK) return rc;
+    bool resid = o.stop == CW_STOP_RESIDUAL;
+    int64_t done_sweeps = 0, chunk = 8;
+    std::vector<int32_t> flags(nh);
+    while (done_sweeps < o.max_sweeps) {
+        int64_t n = std::min(chunk, o.max_sweeps - done_sweeps);
+        for (int64_t s = 0; s < n; ++s) {
+            for (int colour = 0; colour < 2; ++colour) {
+                if (pc[colour].nblocks == 0) continue;
+                k_sor64_half<<<pc[colour].nblocks, T, 0, stream()>>>(fv, pc[colour].d_blk, nh, f->d_span, d_st,
+                                                                      colour);
+                CW_LAUNCHED();
+            }
+            if (resid) {
+                k_residual64<<<ps.nblocks, T, 0, stream()>>>(fv, ps.d_blk, nh, d_st, nullptr, nullptr, nullptr, 1);
+                CW_LAUNCHED();
+            }
+            k_check<<<(nh + 63) / 64, 64, 0, stream()>>>(d_st, nh, done_sweeps + s + 1, resid ? 1 : 0);
+            CW_LAUNCHED();
+        }
+        done_sweeps += n;
+        CW_CUDA(cudaMemcpyAsync(hs.data(), d_st, sizeof(RelaxState) * nh, cudaMemcpyDeviceToHost, stream()));
+        CW_CUDA(cudaStreamSynchronize(stream()));
+        bool all = true;
+        for (uint32_t k = 0; k < nh; ++k) all = all && hs[k].done;
+        if (all) break;
+        chunk = std::min<int64_t>(chunk * 2, 256);
+    }
+    pc[0].release(); pc[1].release(); ps.release();
+    return CW_OK;
+}
+
+static int relax_fp32dc(cw_field_s *f, const cw_relax_opts &o, RelaxState *d_st, std::vector<RelaxState> &hs) {
+    uint32_t nh = f->g.nh;
+    int rc = f->alloc_fp32();
+    if (rc != CW_OK) return rc;
+    FieldView fv = view(f);
+    Plan ps;
+    if ((rc = site_plan(f, ps)) != CW_OK) return rc;
+    int inner = o.inner_sweeps > 0 ? o.inner_sweeps : 16;
+    int depth = o.block_depth > 0 ? o.block_depth : 4;
+    Sor32 solver;
+    std::vector<double> om(nh);
+    for (uint32_t k = 0; k < nh; ++k) om[k] = hs[k].omega;
+    if ((rc = solver.init(f, depth, om)) != CW_OK) return rc;
+    const int32_t *done_ptr = (const int32_t *)((const char *)d_st + offsetof(RelaxState, done));
+    int64_t outer = 0;
+    int64_t max_outer = o.max_sweeps / inner + 2;
+    std::vector<int32_t> flags(nh);
+    int queue = 2;
+    while (outer < max_outer) {
+        for (int q = 0; q < queue && outer < max_outer; ++q, ++outer) {
+            k_residual64<<<ps.nblocks, T, 0, stream()>>>(fv, ps.d_blk, nh, d_st, f->r32, f->inv32, f->d32a, 1);
+            CW_LAUNCHED();
+            k_dc_check<<<(nh + 63) / 64, 64, 0, stream()>>>(d_st, nh, inner, o.max_sweeps);
+            CW_LAUNCHED();
+            if ((rc = solver.sweeps(f, inner, done_ptr, (int)(sizeof(RelaxState) / sizeof(int32_t)))) != CW_OK) return rc;
+            k_dc_correct<<<ps.nblocks, T, 0, stream()>>>(fv, ps.d_blk, nh, d_st, solver.result());
+            CW_LAUNCHED();
+        }
+        CW_CUDA(cudaMemcpyAsync(hs.data(), d_st, sizeof(RelaxState) * nh, cudaMemcpyDeviceToHost, stream()));
+        CW_CUDA(cudaStreamSynchronize(stream()));
+        bool all = true;
+        for (uint32_t k = 0; k < nh; ++k) all = all && hs[k].done;
+        if (all) break;
+        queue = std::min(queue * 2, 16);
+    }
+    solver.release();
+    ps.release();
+    return CW_OK;
+}
+
+extern "C" {
+
+int cw_field_create(uint32_t nh, const uint32_t *w, const uint32_t *h, const uint32_t *d, double dcoef,
+                    double decay, double initial, cw_field *out) {
+    *out = nullptr;
+    if (!std::isfinite(dcoef) || !std::isfinite(decay) || dcoef < 0.0 || decay < 0.0)
+        return fail(CW_ERR_CONFIG, "diffusion and decay must be finite and not negative, got D = " +
+                                       std::to_string(dcoef) + ", decay = " + std::to_string(decay));
+    cw_field_s *f = new cw_field_s();
+    int rc = f->g.init(nh, w, h, d);
+    if (rc != CW_OK) { delete f; return rc; }
+    f->dcoef = dcoef; f->decay = decay;
+    int64_t n = f->g.total;
+    if ((rc = dalloc(&f->c, n)) || (rc = dalloc(&f->held, n)) || (rc = dalloc(&f->uptake, n)) ||
+        (rc = dalloc(&f->production, n)) || (rc = dalloc(&f->lin_sink, n)) || (rc = dalloc(&f->d_span, nh)) ||
+        (rc = dalloc((RelaxState **)&f->stats, nh))) {
+        cw_field_destroy(f);
+        return rc;
+    }
+    k_fill64<<<(unsigned)blocks_for(n), T, 0, stream()>>>(f->c, n, initial);
+    CW_LAUNCHED();
+    CW_CUDA(cudaMemsetAsync(f->held, 0, n, stream()));
+    CW_CUDA(cudaMemsetAsync(f->uptake, 0, n * sizeof(double), stream()));
+    CW_CUDA(cudaMemsetAsync(f->production, 0, n * sizeof(double), stream()));
+    CW_CUDA(cudaMemsetAsync(f->lin_sink, 0, n * sizeof(double), stream()));
+    CW_CUDA(cudaStreamSynchronize(stream()));
+    *out = f;
+    return CW_OK;
+}
+
+int cw_field_destroy(cw_field f) {
+    if (!f) return CW_OK;
+    dfree(f->c); dfree(f->held); dfree(f->uptake); dfree(f->production); dfree(f->lin_sink);
+    dfree(f->r32); dfree(f->d32a); dfree(f->d32b); dfree(f->inv32); dfree(f->tmp64); dfree(f->d_span);
+    RelaxState *st = (RelaxState *)f->stats;
+    dfree(st);
+    f->g.release();
+    delete f;
+    return CW_OK;
+}
+
+int cw_field_set_source(cw_field f, double source) {
+    f->source = source;
+    return CW_OK;
+}
+
+int cw_field_set_diffusion(cw_field f, double dcoef) {
+    if (!std::isfinite(dcoef) || dcoef < 0.0) return fail(CW_ERR_CONFIG, "diffusion must be finite and not negative");
+    f->dcoef = dcoef;
+    return CW_OK;
+}
+
+static double *array_of(cw_field f, int32_t which) {
+    switch (which) {
+    case CW_VALUES: return f->c;
+    case CW_UPTAKE: return f->uptake;
+    case CW_PRODUCTION: return f->production;
+    case CW_LIN_SINK: return f->lin_sink;
+    default: return nullptr;
+    }
+}
+
+int cw_field_upload(cw_field f, uint32_t hist, int32_t which, const double *host) {
+    if (hist >= f->g.nh) return fail(CW_ERR_NOT_FOUND, "no history " + std::to_string(hist));
+    double *p = array_of(f, which);
+    if (!p) return fail(CW_ERR_CONFIG, "unknown field array");
+    if (which == CW_LIN_SINK) f->lin_sink_on = true;
+    CW_CUDA(cudaMemcpyAsync(p + f->g.off[hist], host, sizeof(double) * f->g.sites(hist), cudaMemcpyHostToDevice,
+                            stream()));
+    CW_CUDA(cudaStreamSynchronize(stream()));
+    return CW_OK;
+}
+
+int cw_field_download(cw_field f, uint32_t hist, int32_t which, double *host) {
+    if (hist >= f->g.nh) return fail(CW_ERR_NOT_FOUND, "no history " + std::to_string(hist));
+    double *p = array_of(f, which);
+    if (!p) return fail(CW_ERR_CONFIG, "unknown field array");
+    CW_CUDA(cudaMemcpyAsync(host, p + f->g.off[hist], sizeof(double) * f->g.sites(hist), cudaMemcpyDeviceToHost,
+                            stream()));
+    CW_CUDA(cudaStreamSynchronize(stream()));
+    return CW_OK;
+}
+
+int cw_field_upload_held(cw_field f, uint32_t hist, const uint8_t *held) {
+    if (hist >= f->g.nh) return fail(CW_ERR_NOT_FOUND, "no history " + std::to_string(hist));
+    CW_CUDA(cudaMemcpyAsync(f->held + f->g.off[hist], held, f->g.sites(hist), cudaMemcpyHostToDevice, stream()));
+    CW_CUDA(cudaStreamSynchronize(stream()));
+    return CW_OK;
+}
+
+int cw_field_download_held(cw_field f, uint32_t hist, uint8_t *held) {
+    if (hist >= f->g.nh) return fail(CW_ERR_NOT_FOUND, "no history " + std::to_string(hist));
+    CW_CUDA(cudaMemcpyAsync(held, f->held + f->g.off[hist], f->g.sites(hist), cudaMemcpyDeviceToHost, stream()));
+    CW_CUDA(cudaStreamSynchronize(stream()));
+    return CW_OK;
+}
+
+int cw_field_fill(cw_field f, double value) {
+    int64_t n = f->g.total;
+    k_fill64<<<(unsigned)blocks_for(n), T, 0, stream()>>>(f->c, n, value);
+    CW_LAUNCHED();
+    return CW_OK;
+}
+
+int cw_field_clear(cw_field f, int32_t which) {
+    double *p = array_of(f, which);
+    if (!p || which == CW_VALUES) return fail(CW_ERR_CONFIG, "only uptake, production and the linear sink clear");
+    CW_CUDA(cudaMemsetAsync(p, 0, sizeof(double) * f->g.total, stream()));
+    return CW_OK;
+}
+
+int cw_field_release_all(cw_field f) {
+    CW_CUDA(cudaMemsetAsync(f->held, 0, f->g.total, stream()));
+    return CW_OK;
+}
+
+int cw_field_hold_mask(cw_field f, uint32_t hist, const uint8_t *mask, double value) {
+    if (hist >= f->g.nh) return fail(CW_ERR_NOT_FOUND, "no history " + std::to_string(hist));
+    int64_t n = f->g.sites(hist);
+    uint8_t *dm;
+    int rc = dalloc(&dm, n);
+    if (rc != CW_OK) return rc;
+    CW_CUDA(cudaMemcpyAsync(dm, mask, n, cudaMemcpyHostToDevice, stream()));
+    k_hold_mask<<<(unsigned)blocks_for(n), T, 0, stream()>>>(f->c + f->g.off[hist], f->held + f->g.off[hist], dm, n,
+                                                             value);
+    CW_LAUNCHED();
+    CW_CUDA(cudaStreamSynchronize(stream()));
+    dfree(dm);
+    return CW_OK;
+}
+
+int cw_field_relax(cw_field f, const cw_relax_opts *opts, cw_relax_stats *stats) {
+    cw_relax_opts o = *opts;
+    if (o.max_sweeps <= 0) o.max_sweeps = 1;
+    if (o.precision != CW_FP64 && o.precision != CW_FP32_DC) return fail(CW_ERR_CONFIG, "unknown precision");
+    if (o.precision == CW_FP32_DC && o.stop != CW_STOP_RESIDUAL)
+        return fail(CW_ERR_CONFIG, "the FP32 defect-correction solve stops on the residual only");
+    uint32_t nh = f->g.nh;
+    std::vector<Span> spans;
+    int rc = field_span(f, spans);
+    if (rc != CW_OK) return rc;
+    std::vector<RelaxState> hs(nh);
+    for (uint32_t k = 0; k < nh; ++k) {
+        RelaxState &s = hs[k];
+        std::memset(&s, 0, sizeof s);
+        s.tol = o.tolerance;
+        s.stop = o.stop;
+        if (!spans[k].found) {  // nothing to balance: one sweep that moves nothing (pde.rs:256-259)
+            s.done = 1;
+            s.sweeps = 1;
+            s.omega = 0.0;
+            continue;
+        }
+        s.omega = o.omega > 0.0 ? o.omega : auto_omega(f, k, spans[k]);
+    }
+    RelaxState *d_st = (RelaxState *)f->stats;
+    CW_CUDA(cudaMemcpyAsync(d_st, hs.data(), sizeof(RelaxState) * nh, cudaMemcpyHostToDevice, stream()));
+    if (o.precision == CW_FP64) rc = relax_fp64(f, o, spans, d_st, hs);
+    else rc = relax_fp32dc(f, o, d_st, hs);
+    if (rc != CW_OK) return rc;
+    // final residual of every history, for the report
+    std::vector<double> res(nh);
+    if ((rc = cw_field_residual(f, res.data())) != CW_OK) return rc;
+    bool bad = false;
+    for (uint32_t k = 0; k < nh; ++k) {
+        bool ok = hs[k].done == 1;
+        bad = bad || !ok;
+        if (stats) {
+            stats[k].sweeps = hs[k].sweeps;
+            stats[k].last_change = hs[k].last_change;
+            stats[k].residual = res[k];
+            stats[k].status = ok ? CW_OK : CW_ERR_SIMULATION;
+            stats[k].omega = hs[k].omega;
+        }
+    }
+    if (bad)
+        return fail(CW_ERR_SIMULATION, "diffusion did not settle within " + std::to_string(o.max_sweeps) +
+                                           " sweeps at tolerance " + std::to_string(o.tolerance));
+    return CW_OK;
+}
+
+int cw_field_residual(cw_field f, double *out) {
+    uint32_t nh = f->g.nh;
+    RelaxState *d_st = (RelaxState *)f->stats;
+    std::vector<RelaxState> hs(nh);
+    CW_CUDA(cudaMemcpyAsync(hs.data(), d_st, sizeof(RelaxState) * nh, cudaMemcpyDeviceToHost, stream()));
+    CW_CUDA(cudaStreamSynchronize(stream()));
+    for (auto &s : hs) { s.resid = 0ull; s.done = 0; }
+    CW_CUDA(cudaMemcpyAsync(d_st, hs.data(), sizeof(RelaxState) * nh, cudaMemcpyHostToDevice, stream()));
+    Plan ps;
+    int rc = site_plan(f, ps);
+    if (rc != CW_OK) return rc;
+    k_residual64<<<ps.nblocks, T, 0, stream()>>>(view(f), ps.d_blk, nh, d_st, nullptr, nullptr, nullptr, 0);
+    CW_LAUNCHED();
+    CW_CUDA(cudaMemcpyAsync(hs.data(), d_st, sizeof(RelaxState) * nh, cudaMemcpyDeviceToHost, stream()));
+    CW_CUDA(cudaStreamSynchronize(stream()));
+    for (uint32_t k = 0; k < nh; ++k) out[k] = __builtin_bit_cast(double, (uint64_t)hs[k].resid);
+    ps.release();
+    return CW_OK;
+}
+
+int cw_field_inflow(cw_field f, double *out) {
+    uint32_t nh = f->g.nh;
+    double *d_out;
+    int rc = dalloc(&d_out, nh);
+    if (rc != CW_OK) return rc;
+    CW_CUDA(cudaMemsetAsync(d_out, 0, sizeof(double) * nh, stream()));
+    Plan ps;
+    if ((rc = site_plan(f, ps)) != CW_OK) return rc;
+    k_inflow<<<ps.nblocks, T, 0, stream()>>>(view(f), ps.d_blk, nh, d_out);
+    CW_LAUNCHED();
+    CW_CUDA(cudaMemcpyAsync(out, d_out, sizeof(double) * nh, cudaMemcpyDeviceToHost, stream()));
+    CW_CUDA(cudaStreamSynchronize(stream()));
+    dfree(d_out);
+    ps.release();
+    return CW_OK;
+}
+
+int cw_field_step(cw_field f, double dt) {
+    if (std::isnan(dt) || dt <= 0.0) return fail(CW_ERR_CONFIG, "time step must be positive, got " + std::to_string(dt));
+    bool volume = false;
+    for (uint32_t k = 0; k < f->g.nh; ++k) volume = volume || f->g.d[k] > 1;
+    double limit = volume ? 0.25 * 2.0 / 3.0 : 0.25;
+    if (f->dcoef * dt > limit)
+        return fail(CW_ERR_CONFIG, "unstable time step: D*dt = " + std::to_string(f->dcoef * dt) + " is above " +
+                                       std::to_string(limit));
+    if (f->decay * dt > 1.0)
+        return fail(CW_ERR_CONFIG, "unstable time step: decay*dt = " + std::to_string(f->decay * dt) + " is above 1");
+    int rc;
+    if (!f->tmp64 && (rc = dalloc(&f->tmp64, f->g.total)) != CW_OK) return rc;
+    Plan ps;
+    if ((rc = site_plan(f, ps)) != CW_OK) return rc;
+    k_explicit<<<ps.nblocks, T, 0, stream()>>>(view(f), ps.d_blk, f->g.nh, dt, f->tmp64);
+    CW_LAUNCHED();
+    std::swap(f->c, f->tmp64);
+    CW_CUDA(cudaStreamSynchronize(stream()));
+    ps.release();
+    return CW_OK;
+}
+
+}  // extern "C"
+
+namespace cw {
+// The bath flood of one history (or all, hist < 0) from an open mask on the device.
+int field_hold_bath_device(cw_field_s *f, const uint8_t *d_open, int hist, double value) {
+    Plan ps;
+    int rc = site_plan(f, ps);
+    if (rc != CW_OK) return rc;
+    uint32_t nh = f->g.nh;
+    Span *box = f->d_span;
+    k_span_reset<<<(nh + 63) / 64, 64, 0, stream()>>>(box, nh);
+    CW_LAUNCHED();
+    k_bath_box<<<ps.nblocks, T, 0, stream()>>>(d_open, f->g.d_dims, f->g.d_off, ps.d_blk, nh, box);
+    CW_LAUNCHED();
+    k_bath_init<<<ps.nblocks, T, 0, stream()>>>(d_open, f->held, f->g.d_dims, f->g.d_off, ps.d_blk, nh, box, hist);
+    CW_LAUNCHED();
+    int *d_changed;
+    if ((rc = dalloc(&d_changed, 1)) != CW_OK) return rc;
+    int64_t limit = f->g.total + 2;
+    int64_t iters = 0;
+    for (;;) {
+        CW_CUDA(cudaMemsetAsync(d_changed, 0, sizeof(int), stream()));
+        for (int r = 0; r < 16; ++r) {
+            k_bath_spread<<<ps.nblocks, T, 0, stream()>>>(d_open, f->held, f->g.d_dims, f->g.d_off, ps.d_blk, nh, box,
+                                                          hist, d_changed);
+            CW_LAUNCHED();
+        }
+        iters += 16;
+        int changed = 0;
+        CW_CUDA(cudaMemcpyAsync(&changed, d_changed, sizeof(int), cudaMemcpyDeviceToHost, stream()));
+        CW_CUDA(cudaStreamSynchronize(stream()));
+        if (!changed) break;
+        if (iters > limit) {
+            dfree(d_changed);
+            return fail(CW_ERR_TIMEOUT, "the bath flood did not finish");
+        }
+    }
+    dfree(d_changed);
+    k_bath_values<<<ps.nblocks, T, 0, stream()>>>(f->c, f->held, f->g.d_off, ps.d_blk, nh, hist, value);
+    CW_LAUNCHED();
+    CW_CUDA(cudaStreamSynchronize(stream()));
+    ps.release();
+    return CW_OK;
+}
+}  // namespace cw
+
+extern "C" int cw_field_hold_bath(cw_field f, uint32_t hist, const uint8_t *open, double value) {
+    if (hist >= f->g.nh) return fail(CW_ERR_NOT_FOUND, "no history " + std::to_string(hist));
+    uint8_t *d_open;
+    int rc = dalloc(&d_open, f->g.total);
+    if (rc != CW_OK) return rc;
+    CW_CUDA(cudaMemsetAsync(d_open, 1, f->g.total, stream()));
+    CW_CUDA(cudaMemcpyAsync(d_open + f->g.off[hist], open, f->g.sites(hist), cudaMemcpyHostToDevice, stream()));
+    rc = field_hold_bath_device(f, d_open, (int)hist, value);
+    dfree(d_open);
+    return rc;
+}

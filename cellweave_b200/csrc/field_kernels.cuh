@@ -1,0 +1,55 @@
+// Field views and the FP32 inner solver shared by field.cu and field32.cu.
+#pragma once
+
+#include "cw_internal.cuh"
+
+namespace cw {
+
+// What a field kernel reads: the values, the held mask, the per-pixel
+// coefficients and the scalars of pde.rs:30-53 (ks: first-order sink or null).
+struct FieldView {
+    double *c;
+    const uint8_t *held;
+    const double *up, *pr, *ks;
+    double d, decay, source;
+    const int4 *dims;
+    const int64_t *off;
+};
+
+FieldView view(cw_field_s *f);
+int field_hold_bath_device(cw_field_s *f, const uint8_t *d_open, int hist, double value);
+
+// Neighbour sum and count of real neighbours in the reference's order:
+// x-1, x+1, y-1, y+1, z-1, z+1 (pde.rs:361-390).
+__device__ __forceinline__ void pixel_sums64(const double *__restrict__ c, int64_t i, int x, int y, int z, int4 dm,
+                                             double &sum, double &real) {
+    int64_t w = dm.x, slice = (int64_t)dm.x * dm.y;
+    double s = 0.0, r = 0.0;
+    if (x > 0) { s += c[i - 1]; r += 1.0; }
+    if (x + 1 < dm.x) { s += c[i + 1]; r += 1.0; }
+    if (y > 0) { s += c[i - w]; r += 1.0; }
+    if (y + 1 < dm.y) { s += c[i + w]; r += 1.0; }
+    if (z > 0) { s += c[i - slice]; r += 1.0; }
+    if (z + 1 < dm.z) { s += c[i + slice]; r += 1.0; }
+    sum = s;
+    real = r;
+}
+
+// Red-black SOR sweeps on the correction equation A d = r in FP32.  Flat
+// histories are swept `depth` half-sweeps per launch, each tile kept in
+// shared memory with a halo `depth` deep (temporal blocking); volumes
+// one half-sweep per launch, in place.
+struct Sor32 {
+    int depth = 4;
+    bool blocked = true;
+    Plan tiles;       // flat histories: tiles per history
+    Plan sites;       // volumes: pixels per history
+    float *omega = nullptr;
+    float *ping = nullptr, *pong = nullptr, *out = nullptr;
+    int init(cw_field_s *f, int depth, const std::vector<double> &omega_per_history);
+    int sweeps(cw_field_s *f, int n, const int32_t *done, int done_stride);
+    float *result() const { return out; }
+    void release();
+};
+
+}  // namespace cw

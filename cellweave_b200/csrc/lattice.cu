@@ -1,0 +1,720 @@
+// CPM lattice: CpmLattice of crates/engine/src/cpm.rs on the device.
+//
+// The reference's Monte Carlo step is sequential: N attempts at random
+// pixels, each seeing every flip before it (cpm.rs:734-772).  Here one step
+// is a sequence of sublattice passes.  Pixels are coloured so that no pixel
+// of a colour lies within the contact reach of another (the chessboard for
+// contact across faces; a period R+1 in every axis for a reach of Chebyshev
+// radius R); a pass makes one copy attempt at every pixel of one colour, all
+// at once.  Attempts of one pass never read a pixel another of them writes,
+// and read volumes and surfaces from a snapshot taken when the pass starts,
+// so a pass is deterministic whatever the thread schedule.  The colours are
+// swept in an order shuffled anew every step.
+//
+// Each attempt is the reference's try_flip (cpm.rs:797-838): a neighbour
+// across a face drawn uniformly, no proposal from or into an obstacle or
+// within one cell, Delta-H = contact (cpm.rs:851-876) + volume
+// (cpm.rs:879-894) [+ surface, an extension], accepted when Delta-H <= 0 or
+// u < exp(-Delta-H / T).  Draws come from Philox4x32-10 keyed by the
+// history's seed, counter (pixel, step, 0, 0).  This file is built without
+// fused multiply-add so that Delta-H rounds as the reference's does.
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstring>
+
+#include "cw_internal.cuh"
+
+using namespace cw;
+
+namespace {
+
+constexpr int T = 256;
+constexpr int32_t OBST = -1;
+
+struct LatView {
+    int32_t *grid;
+    const int32_t *type;
+    int32_t *volume;
+    const int32_t *vsnap;
+    const int32_t *target;
+    const double *lambda;
+    int32_t *surface;
+    const int32_t *ssnap;
+    const int32_t *tsurf;
+    const double *lsurf;
+    const int4 *dims;
+    const int64_t *off;
+    const int64_t *cell_off;
+    const uint2 *keys;
+    int32_t K;
+    int32_t nreach;
+    int32_t period;
+    int32_t ncol;
+    double across;
+    double temperature;
+    int32_t surface_on;
+};
+
+struct Tables {
+    double J[64];
+    int8_t reach[3 * 124];
+};
+
+__device__ __forceinline__ int32_t kind_of(const int32_t *type_h, int64_t cap, int32_t id) {
+    if (id < 0 || id >= cap) return 0;  // the obstacle reads as the medium (cpm.rs:908-917)
+    return type_h[id];
+}
+
+// von_neumann, cpm.rs:922-944: y-1, y+1, x-1, x+1, z-1, z+1, clipped.
+__device__ __forceinline__ int von_neumann(int4 dm, int x, int y, int z, int64_t i, int64_t *out) {
+    int64_t w = dm.x, slice = (int64_t)dm.x * dm.y;
+    int n = 0;
+    if (y > 0) out[n++] = i - w;
+    if (y + 1 < dm.y) out[n++] = i + w;
+    if (x > 0) out[n++] = i - 1;
+    if (x + 1 < dm.x) out[n++] = i + 1;
+    if (z > 0) out[n++] = i - slice;
+    if (z + 1 < dm.z) out[n++] = i + slice;
+    return n;
+}
+
+// contact_delta_h (cpm.rs:851-876) on history grid `g`; *num before the division.
+__device__ double contact_delta(const int32_t *__restrict__ g, int4 dm, int x, int y, int z, int32_t src,
+                                int32_t dst, const int32_t *type_h, int64_t cap, const double *sJ, int K,
+                                const int8_t *reach, int nreach, double across, const int64_t *vn, int nvn,
+                                double *num) {
+    int32_t ks = kind_of(type_h, cap, src), kd = kind_of(type_h, cap, dst);
+    double dh = 0.0;
+    if (nreach > 0) {
+        for (int k = 0; k < nreach; ++k) {
+            int a = x + reach[3 * k], b = y + reach[3 * k + 1], c = z + reach[3 * k + 2];
+            if (a < 0 || b < 0 || c < 0 || a >= dm.x || b >= dm.y || c >= dm.z) continue;
+            int32_t nb = g[((int64_t)c * dm.y + b) * dm.x + a];
+            int32_t kn = kind_of(type_h, cap, nb);
+            double ed = dst == nb ? 0.0 : sJ[kd * K + kn];
+            double es = src == nb ? 0.0 : sJ[ks * K + kn];
+            dh += ed - es;
+        }
+        *num = dh;
+        return dh / across;
+    }
+    for (int k = 0; k < nvn; ++k) {
+        int32_t nb = g[vn[k]];
+        int32_t kn = kind_of(type_h, cap, nb);
+        double ed = dst == nb ? 0.0 : sJ[kd * K + kn];
+        double es = src == nb ? 0.0 : sJ[ks * K + kn];
+        dh += ed - es;
+    }
+    *num = dh;
+    return dh;
+}
+
+// volume_delta_h, cpm.rs:879-894, on the volumes given (c0: the history's first cell).
+__device__ __forceinline__ double volume_delta(const int32_t *vol, const int32_t *target, const double *lambda,
+                                               int64_t c0, int32_t src, int32_t dst) {
+    double dh = 0.0;
+    if (src != 0) {
+        double v = (double)vol[c0 + src], vt = (double)target[c0 + src];
+        double a = v - 1.0 - vt, b = v - vt;
+        dh += lambda[c0 + src] * (a * a - b * b);
+    }
+    if (dst != 0) {
+        double v = (double)vol[c0 + dst], vt = (double)target[c0 + dst];
+        double a = v + 1.0 - vt, b = v - vt;
+        dh += lambda[c0 + dst] * (a * a - b * b);
+    }
+    return dh;
+}
+
+__device__ __forceinline__ void surface_change(const int32_t *g, const int64_t *vn, int nvn, int32_t src,
+                                               int32_t dst, int32_t &dsrc, int32_t &ddst) {
+    int eq_s = 0, eq_d = 0;
+    for (int k = 0; k < nvn; ++k) {
+        int32_t nb = g[vn[k]];
+        eq_s += nb == src;
+        eq_d += nb == dst;
+    }
+    dsrc = eq_s - (nvn - eq_s);
+    ddst = (nvn - eq_d) - eq_d;
+}
+
+__device__ __forceinline__ double surface_delta(const int32_t *surf, const int32_t *tsurf, const double *lsurf,
+                                                int64_t c0, int32_t src, int32_t dst, int32_t dsrc, int32_t ddst) {
+    double dh = 0.0;
+    if (src > 0) {
+        double s = (double)surf[c0 + src], st = (double)tsurf[c0 + src];
+        double a = s + (double)dsrc - st, b = s - st;
+        dh += lsurf[c0 + src] * (a * a - b * b);
+    }
+    if (dst > 0) {
+        double s = (double)surf[c0 + dst], st = (double)tsurf[c0 + dst];
+        double a = s + (double)ddst - st, b = s - st;
+        dh += lsurf[c0 + dst] * (a * a - b * b);
+    }
+    return dh;
+}
+
+// The colour order of the current step for every history: a Fisher-Yates
+// shuffle driven by Philox(all-ones, step, 1, i); advances the step counter.
+__global__ void k_colour_order(const uint2 *keys, int nh, int ncol, uint32_t *mcs_ctr, uint32_t *mcs_cur,
+                               int32_t *perm) {
+    // one block: every thread reads the counter before thread 0 advances it
+    uint32_t m = *mcs_ctr;
+    for (int h = threadIdx.x; h < nh; h += blockDim.x) {
+        int32_t p[27];
+        for (int i = 0; i < ncol; ++i) p[i] = i;
+        uint2 k = keys[h];
+        for (int i = ncol - 1; i > 0; --i) {
+            uint4 r = philox(0xFFFFFFFFu, m, 1u, (uint32_t)i, k.x, k.y);
+            int j = (int)(((uint64_t)r.x * (uint64_t)(i + 1)) >> 32);
+            int32_t t = p[i]; p[i] = p[j]; p[j] = t;
+        }
+        for (int i = 0; i < ncol; ++i) perm[h * ncol + i] = p[i];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        *mcs_cur = m;
+        *mcs_ctr = m + 1;
+    }
+}
+
+// The pixel of colour `colour` with index k in history dims dm; false past the end.
+__device__ __forceinline__ bool colour_site(int4 dm, int period, int colour, int64_t k, int &x, int &y, int &z) {
+    if (period == 0) {
+        int hw = (dm.x + 1) >> 1;
+        int64_t row = k / hw;
+        if (row >= (int64_t)dm.y * dm.z) return false;
+        y = (int)(row % dm.y);
+        z = (int)(row / dm.y);
+        x = ((colour - y - z) & 1) + 2 * (int)(k - row * hw);
+        return x < dm.x;
+    }
+    int cx = colour % period, cy = (colour / period) % period, cz = colour / (period * period);
+    int nx = dm.x > cx ? (dm.x - cx + period - 1) / period : 0;
+    int ny = dm.y > cy ? (dm.y - cy + period - 1) / period : 0;
+    int nz = dm.z > cz ? (dm.z - cz + period - 1) / period : 0;
+    if (k >= (int64_t)nx * ny * nz) return false;
+    int ix = (int)(k % nx);
+    int64_t r = k / nx;
+    int iy = (int)(r % ny), iz = (int)(r / ny);
+    x = cx + period * ix;
+    y = cy + period * iy;
+    z = cz + period * iz;
+    return true;
+}
+
+// One sublattice pass: one copy attempt at every pixel of this pass's colour.
+__global__ void __launch_bounds__(T) k_cpm_pass(LatView L, Tables tabs, const int32_t *blk, int nh,
+                                                const int32_t *perm, int pass, const uint32_t *mcs_cur) {
+    __shared__ double sJ[64];
+    __shared__ int8_t sreach[3 * 124];
+    __shared__ int s_h;
+    if (threadIdx.x == 0) s_h = plan_history(blk, nh, blockIdx.x);
+    for (int i = threadIdx.x; i < L.K * L.K; i += blockDim.x) sJ[i] = tabs.J[i];
+    for (int i = threadIdx.x; i < 3 * L.nreach; i += blockDim.x) sreach[i] = tabs.reach[i];
+    __syncthreads();
+    const int h = s_h;
+    const int4 dm = L.dims[h];
+    const int colour = perm[h * L.ncol + pass];
+    const int64_t k = (int64_t)(blockIdx.x - blk[h]) * blockDim.x + threadIdx.x;
+    const int64_t c0 = L.cell_off[h], cap = L.cell_off[h + 1] - c0;
+    int32_t *g = L.grid + L.off[h];
+    const int32_t *type_h = L.type + c0;
+    int x = 0, y = 0, z = 0;
+    bool accept = false;
+    int32_t src = 0, dst = 0, dsrc = 0, ddst = 0;
+    if (colour_site(dm, L.period, colour, k, x, y, z)) {
+        int64_t i = ((int64_t)z * dm.y + y) * dm.x + x;
+        int64_t vn[6];
+        int nvn = von_neumann(dm, x, y, z, i, vn);
+        if (nvn > 0) {
+            uint2 key = L.keys[h];
+            uint4 r = philox((uint32_t)i, *mcs_cur, 0u, 0u, key.x, key.y);
+            src = g[i];
+            dst = g[vn[((uint64_t)r.x * (uint64_t)nvn) >> 32]];
+            if (src != dst && src != OBST && dst != OBST) {
+                double num;
+                double delta = contact_delta(g, dm, x, y, z, src, dst, type_h, cap, sJ, L.K, sreach, L.nreach,
+                                             L.across, vn, nvn, &num) +
+                               volume_delta(L.vsnap, L.target, L.lambda, c0, src, dst);
+                if (L.surface_on) {
+                    surface_change(g, vn, nvn, src, dst, dsrc, ddst);
+                    delta += surface_delta(L.ssnap, L.tsurf, L.lsurf, c0, src, dst, dsrc, ddst);
+                }
+                accept = delta <= 0.0;
+                if (!accept) accept = u01(r.y, r.z) < own_exp(-delta / L.temperature);
+                if (accept) g[i] = dst;
+            }
+        }
+    }
+    // bookkeeping: one atomic per distinct cell per warp
+    const unsigned am = __ballot_sync(0xffffffffu, accept);
+    if (accept) {
+        const int lane = threadIdx.x & 31;
+        unsigned peers = __match_any_sync(am, src);
+        if (src != 0 && lane == __ffs(peers) - 1) atomicSub(L.volume + c0 + src, __popc(peers));
+        if (L.surface_on) {
+            int s = __reduce_add_sync(peers, (unsigned)dsrc);
+            if (src > 0 && lane == __ffs(peers) - 1) atomicAdd(L.surface + c0 + src, s);
+        }
+        peers = __match_any_sync(am, dst);
+        if (dst != 0 && lane == __ffs(peers) - 1) atomicAdd(L.volume + c0 + dst, __popc(peers));
+        if (L.surface_on) {
+            int s = __reduce_add_sync(peers, (unsigned)ddst);
+            if (dst > 0 && lane == __ffs(peers) - 1) atomicAdd(L.surface + c0 + dst, s);
+        }
+    }
+}
+
+__global__ void k_copy32(int32_t *dst, const int32_t *src, int64_t n) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = src[i];
+}
+
+// Delta-H of explicit proposals on one history, on live volumes.
+__global__ void k_delta_h(LatView L, Tables tabs, int h, int64_t n, const int64_t *site, const int32_t *dstv,
+                          double *out) {
+    __shared__ double sJ[64];
+    __shared__ int8_t sreach[3 * 124];
+    for (int i = threadIdx.x; i < L.K * L.K; i += blockDim.x) sJ[i] = tabs.J[i];
+    for (int i = threadIdx.x; i < 3 * L.nreach; i += blockDim.x) sreach[i] = tabs.reach[i];
+    __syncthreads();
+    int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    const int4 dm = L.dims[h];
+    const int64_t c0 = L.cell_off[h], cap = L.cell_off[h + 1] - c0;
+    const int32_t *g = L.grid + L.off[h];
+    int64_t i = site[q];
+    int x = (int)(i % dm.x), y = (int)((i / dm.x) % dm.y), z = (int)(i / ((int64_t)dm.x * dm.y));
+    int64_t vn[6];
+    int nvn = von_neumann(dm, x, y, z, i, vn);
+    int32_t src = g[i], dst = dstv[q];
+    double num;
+    double c = contact_delta(g, dm, x, y, z, src, dst, L.type + c0, cap, sJ, L.K, sreach, L.nreach, L.across, vn,
+                             nvn, &num);
+    double v = volume_delta(L.volume, L.target, L.lambda, c0, src, dst);
+    double s = 0.0;
+    if (L.surface_on) {
+        int32_t ds, dd;
+        surface_change(g, vn, nvn, src, dst, ds, dd);
+        s = surface_delta(L.surface, L.tsurf, L.lsurf, c0, src, dst, ds, dd);
+    }
+    double *o = out + 6 * q;
+    o[0] = num; o[1] = c; o[2] = v; o[3] = s; o[4] = c + v; o[5] = (c + v) + s;
+}
+
+// Recount volumes (and surfaces) from the grid: recount, cpm.rs:1262-1270.
+__global__ void k_recount(const int32_t *grid, const int4 *dims, const int64_t *off, const int64_t *cell_off,
+                          const int32_t *blk, int nh, int32_t *vol, int32_t *surf) {
+    __shared__ int s_h;
+    if (threadIdx.x == 0) s_h = plan_history(blk, nh, blockIdx.x);
+    __syncthreads();
+    int h = s_h;
+    int64_t local = (int64_t)(blockIdx.x - blk[h]) * blockDim.x + threadIdx.x;
+    if (local >= off[h + 1] - off[h]) return;
+    const int32_t *g = grid + off[h];
+    int32_t id = g[local];
+    int64_t cap = cell_off[h + 1] - cell_off[h];
+    if (id < 0 || id >= cap) return;
+    atomicAdd(vol + cell_off[h] + id, 1);
+    if (surf && id > 0) {
+        const int4 dm = dims[h];
+        int x = (int)(local % dm.x), y = (int)((local / dm.x) % dm.y), z = (int)(local / ((int64_t)dm.x * dm.y));
+        int64_t vn[6];
+        int nvn = von_neumann(dm, x, y, z, local, vn);
+        int c = 0;
+        for (int k = 0; k < nvn; ++k) c += g[vn[k]] != id;
+        if (c) atomicAdd(surf + cell_off[h] + id, c);
+    }
+}
+
+__global__ void k_compare(const int32_t *a, const int32_t *b, const int64_t *cell_off, int h, int *bad) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int64_t c0 = cell_off[h], n = cell_off[h + 1] - c0;
+    if (i >= 1 && i < n && a[c0 + i] != b[c0 + i]) atomicAdd(bad, 1);
+}
+
+// set_contact_order, cpm.rs:274-301.
+int make_reach(int order, bool volume, int8_t *off, double *across) {
+    *across = 1.0;
+    if (order <= 1) return 0;
+    int deep = volume ? 2 : 0;
+    std::vector<std::array<int, 3>> cand;
+    std::vector<int64_t> dist;
+    for (int dz = -deep; dz <= deep; ++dz)
+        for (int dy = -2; dy <= 2; ++dy)
+            for (int dx = -2; dx <= 2; ++dx) {
+                if (dx == 0 && dy == 0 && dz == 0) continue;
+                cand.push_back({dx, dy, dz});
+                dist.push_back((int64_t)dx * dx + dy * dy + dz * dz);
+            }
+    std::vector<int64_t> u = dist;
+    std::sort(u.begin(), u.end());
+    u.erase(std::unique(u.begin(), u.end()), u.end());
+    int64_t limit = u[std::min<size_t>((size_t)(order - 1), u.size() - 1)];
+    int n = 0;
+    int64_t acr = 0;
+    for (size_t i = 0; i < cand.size(); ++i)
+        if (dist[i] <= limit) {
+            for (int a = 0; a < 3; ++a) off[3 * n + a] = (int8_t)cand[i][a];
+            acr += std::max(cand[i][0], 0);
+            ++n;
+        }
+    *across = (double)acr;
+    return n;
+}
+
+}  // namespace
+
+int cw_lattice_s::build_plans() {
+    bool volume = g.d[0] > 1;
+    nreach = make_reach(order, volume, reach, &across);
+    if (nreach == 0) {
+        period = 0;
+        ncol = 2;
+    } else {
+        int r = 1;
+        for (int k = 0; k < 3 * nreach; ++k) r = std::max(r, (int)std::abs(reach[k]));
+        period = r + 1;
+        ncol = volume ? period * period * period : period * period;
+    }
+    for (auto &p : plans) p.release();
+    plans.assign(1, Plan());
+    std::vector<int64_t> per(g.nh, 0);
+    for (uint32_t k = 0; k < g.nh; ++k) {
+        if (period == 0) {
+            per[k] = (int64_t)((g.w[k] + 1) / 2) * g.h[k] * g.d[k];
+        } else {
+            int64_t nx = (g.w[k] + period - 1) / period, ny = (g.h[k] + period - 1) / period;
+            int64_t nz = volume ? (g.d[k] + period - 1) / period : 1;
+            per[k] = nx * ny * nz;  // the largest colour class
+        }
+    }
+    return plans[0].build(per, T);
+}
+
+namespace {
+struct LatExtra {
+    uint32_t *mcs_ctr = nullptr, *mcs_cur = nullptr;
+    int32_t *perm = nullptr;
+};
+}  // namespace
+
+static LatView lat_view(cw_lattice_s *l) {
+    LatView v;
+    v.grid = l->grid; v.type = l->type; v.volume = l->volume; v.vsnap = l->vsnap; v.target = l->target;
+    v.lambda = l->lambda; v.surface = l->surface; v.ssnap = l->ssnap; v.tsurf = l->tsurf; v.lsurf = l->lsurf;
+    v.dims = l->g.d_dims; v.off = l->g.d_off; v.cell_off = l->d_cell_off; v.keys = l->d_keys;
+    v.K = l->K; v.nreach = l->nreach; v.period = l->period; v.ncol = l->ncol; v.across = l->across;
+    v.temperature = l->temperature; v.surface_on = l->surface_on ? 1 : 0;
+    return v;
+}
+
+static Tables lat_tables(const cw_lattice_s *l) {
+    Tables t;
+    std::memcpy(t.J, l->J, sizeof t.J);
+    std::memcpy(t.reach, l->reach, sizeof t.reach);
+    return t;
+}
+
+// mcs counter (2 words) and colour permutations live in d_flag's neighbours
+struct LatDevice {
+    uint32_t *mcs;   // [0] counter, [1] current
+    int32_t *perm;   // nh * 27
+};
+static LatDevice dev_of(cw_lattice_s *l) {
+    LatDevice d;
+    d.mcs = (uint32_t *)l->d_flag;
+    d.perm = l->d_flag + 4;
+    return d;
+}
+
+namespace cw {
+int lattice_recount(cw_lattice_s *l, int32_t *vol_out, int32_t *surf_out) {
+    std::vector<int64_t> per(l->g.nh);
+    for (uint32_t k = 0; k < l->g.nh; ++k) per[k] = l->g.sites(k);
+    Plan p;
+    int rc = p.build(per, T);
+    if (rc != CW_OK) return rc;
+    CW_CUDA(cudaMemsetAsync(vol_out, 0, sizeof(int32_t) * l->ncells, stream()));
+    if (surf_out) CW_CUDA(cudaMemsetAsync(surf_out, 0, sizeof(int32_t) * l->ncells, stream()));
+    k_recount<<<p.nblocks, T, 0, stream()>>>(l->grid, l->g.d_dims, l->g.d_off, l->d_cell_off, p.d_blk, l->g.nh,
+                                             vol_out, surf_out);
+    CW_LAUNCHED();
+    CW_CUDA(cudaStreamSynchronize(stream()));
+    p.release();
+    return CW_OK;
+}
+
+// One Monte Carlo step of every history (no host synchronisation).
+int lattice_sweep(cw_lattice_s *l) {
+    LatDevice d = dev_of(l);
+    k_colour_order<<<1, 128, 0, stream()>>>(l->d_keys, l->g.nh, l->ncol, d.mcs, d.mcs + 1, d.perm);
+    CW_LAUNCHED();
+    LatView v = lat_view(l);
+    Tables t = lat_tables(l);
+    unsigned cb = (unsigned)((l->ncells + T - 1) / T);
+    for (int q = 0; q < l->ncol; ++q) {
+        k_copy32<<<cb, T, 0, stream()>>>(l->vsnap, l->volume, l->ncells);
+        CW_LAUNCHED();
+        if (l->surface_on) {
+            k_copy32<<<cb, T, 0, stream()>>>(l->ssnap, l->surface, l->ncells);
+            CW_LAUNCHED();
+        }
+        k_cpm_pass<<<l->plans[0].nblocks, T, 0, stream()>>>(v, t, l->plans[0].d_blk, l->g.nh, d.perm, q, d.mcs + 1);
+        CW_LAUNCHED();
+    }
+    l->mcs += 1;
+    return CW_OK;
+}
+}  // namespace cw
+
+extern "C" {
+
+int cw_lattice_create(uint32_t nh, const uint32_t *w, const uint32_t *h, const uint32_t *d,
+                      const uint32_t *cell_capacity, double temperature, cw_lattice *out) {
+    *out = nullptr;
+    cw_lattice_s *l = new cw_lattice_s();
+    int rc = l->g.init(nh, w, h, d);
+    if (rc != CW_OK) { delete l; return rc; }
+    bool volume = l->g.d[0] > 1;
+    for (uint32_t k = 1; k < nh; ++k)
+        if ((l->g.d[k] > 1) != volume) {
+            l->g.release();
+            delete l;
+            return fail(CW_ERR_CONFIG, "a batch holds flat lattices or volumes, not both");
+        }
+    l->cell_off.assign(nh + 1, 0);
+    for (uint32_t k = 0; k < nh; ++k) {
+        uint32_t cap = std::max<uint32_t>(cell_capacity ? cell_capacity[k] : 1, 1);
+        l->cell_off[k + 1] = l->cell_off[k] + cap;
+    }
+    l->ncells = l->cell_off[nh];
+    l->temperature = temperature;
+    l->seed.assign(nh, 0);
+    int64_t n = l->g.total, nc = l->ncells;
+    if ((rc = dalloc(&l->grid, n)) || (rc = dalloc(&l->type, nc)) || (rc = dalloc(&l->volume, nc)) ||
+        (rc = dalloc(&l->target, nc)) || (rc = dalloc(&l->lambda, nc)) || (rc = dalloc(&l->vsnap, nc)) ||
+        (rc = dalloc(&l->d_cell_off, nh + 1)) || (rc = dalloc(&l->d_keys, nh)) ||
+        (rc = dalloc(&l->d_flag, 4 + 27 * (size_t)nh))) {
+        cw_lattice_destroy(l);
+        return rc;
+    }
+    CW_CUDA(cudaMemsetAsync(l->grid, 0, sizeof(int32_t) * n, stream()));
+    CW_CUDA(cudaMemsetAsync(l->type, 0, sizeof(int32_t) * nc, stream()));
+    CW_CUDA(cudaMemsetAsync(l->volume, 0, sizeof(int32_t) * nc, stream()));
+    CW_CUDA(cudaMemsetAsync(l->target, 0, sizeof(int32_t) * nc, stream()));
+    CW_CUDA(cudaMemsetAsync(l->lambda, 0, sizeof(double) * nc, stream()));
+    CW_CUDA(cudaMemsetAsync(l->d_keys, 0, sizeof(uint2) * nh, stream()));
+    CW_CUDA(cudaMemsetAsync(l->d_flag, 0, sizeof(int32_t) * (4 + 27 * (size_t)nh), stream()));
+    CW_CUDA(cudaMemcpyAsync(l->d_cell_off, l->cell_off.data(), sizeof(int64_t) * (nh + 1), cudaMemcpyHostToDevice,
+                            stream()));
+    l->K = 1;
+    l->J[0] = 0.0;
+    l->order = 1;
+    if ((rc = l->build_plans()) != CW_OK) { cw_lattice_destroy(l); return rc; }
+    CW_CUDA(cudaStreamSynchronize(stream()));
+    *out = l;
+    return CW_OK;
+}
+
+int cw_lattice_destroy(cw_lattice l) {
+    if (!l) return CW_OK;
+    dfree(l->grid); dfree(l->type); dfree(l->volume); dfree(l->target); dfree(l->lambda); dfree(l->vsnap);
+    dfree(l->surface); dfree(l->ssnap); dfree(l->tsurf); dfree(l->lsurf); dfree(l->d_cell_off); dfree(l->d_keys);
+    dfree(l->d_flag);
+    for (auto &p : l->plans) p.release();
+    l->g.release();
+    delete l;
+    return CW_OK;
+}
+
+int cw_lattice_count(cw_lattice l, uint32_t *nh) {
+    *nh = l->g.nh;
+    return CW_OK;
+}
+
+int cw_lattice_set_contact(cw_lattice l, int32_t K, const double *J, int32_t order) {
+    if (K < 1 || K > 8) return fail(CW_ERR_CONFIG, "the contact table holds 1 to 8 types, got " + std::to_string(K));
+    for (int a = 0; a < K; ++a)
+        for (int b = 0; b < K; ++b)
+            if (!std::isfinite(J[a * K + b]) || J[a * K + b] != J[b * K + a])
+                return fail(CW_ERR_CONFIG, "the contact table must be finite and symmetric");
+    l->K = K;
+    std::memset(l->J, 0, sizeof l->J);
+    std::memcpy(l->J, J, sizeof(double) * K * K);
+    l->order = order < 1 ? 1 : order;
+    return l->build_plans();
+}
+
+int cw_lattice_set_temperature(cw_lattice l, double temperature) {
+    if (!(temperature > 0.0)) return fail(CW_ERR_CONFIG, "the temperature must be positive");
+    l->temperature = temperature;
+    return CW_OK;
+}
+
+int cw_lattice_upload(cw_lattice l, uint32_t hist, const int32_t *grid) {
+    if (hist >= l->g.nh) return fail(CW_ERR_NOT_FOUND, "no history " + std::to_string(hist));
+    int64_t n = l->g.sites(hist), cap = l->cell_off[hist + 1] - l->cell_off[hist];
+    for (int64_t i = 0; i < n; ++i)
+        if (grid[i] < -1 || grid[i] >= cap)
+            return fail(CW_ERR_CONFIG, "pixel " + std::to_string(i) + " holds id " + std::to_string(grid[i]) +
+                                           ", past the history's cell capacity " + std::to_string(cap));
+    CW_CUDA(cudaMemcpyAsync(l->grid + l->g.off[hist], grid, sizeof(int32_t) * n, cudaMemcpyHostToDevice, stream()));
+    CW_CUDA(cudaStreamSynchronize(stream()));
+    return CW_OK;
+}
+
+int cw_lattice_download(cw_lattice l, uint32_t hist, int32_t *grid) {
+    if (hist >= l->g.nh) return fail(CW_ERR_NOT_FOUND, "no history " + std::to_string(hist));
+    CW_CUDA(cudaMemcpyAsync(grid, l->grid + l->g.off[hist], sizeof(int32_t) * l->g.sites(hist), cudaMemcpyDeviceToHost,
+                            stream()));
+    CW_CUDA(cudaStreamSynchronize(stream()));
+    return CW_OK;
+}
+
+static int check_cells(cw_lattice l, uint32_t hist, uint32_t n) {
+    if (hist >= l->g.nh) return fail(CW_ERR_NOT_FOUND, "no history " + std::to_string(hist));
+    if ((int64_t)n > l->cell_off[hist + 1] - l->cell_off[hist])
+        return fail(CW_ERR_CONFIG, "more records than the history's cell capacity");
+    return CW_OK;
+}
+
+int cw_cells_set(cw_lattice l, uint32_t hist, uint32_t n, const int32_t *type, const int32_t *volume,
+                 const int32_t *target, const double *lambda) {
+    int rc = check_cells(l, hist, n);
+    if (rc != CW_OK) return rc;
+    for (uint32_t i = 0; i < n; ++i)
+        if (type && (type[i] < 0 || type[i] >= l->K))
+            return fail(CW_ERR_CONFIG, "cell " + std::to_string(i) + " has type " + std::to_string(type[i]) +
+                                           " outside the contact table");
+    int64_t c0 = l->cell_off[hist];
+    if (type) CW_CUDA(cudaMemcpyAsync(l->type + c0, type, 4 * n, cudaMemcpyHostToDevice, stream()));
+    if (volume) CW_CUDA(cudaMemcpyAsync(l->volume + c0, volume, 4 * n, cudaMemcpyHostToDevice, stream()));
+    if (target) CW_CUDA(cudaMemcpyAsync(l->target + c0, target, 4 * n, cudaMemcpyHostToDevice, stream()));
+    if (lambda) CW_CUDA(cudaMemcpyAsync(l->lambda + c0, lambda, 8 * n, cudaMemcpyHostToDevice, stream()));
+    CW_CUDA(cudaStreamSynchronize(stream()));
+    return CW_OK;
+}
+
+int cw_cells_get(cw_lattice l, uint32_t hist, uint32_t n, int32_t *type, int32_t *volume, int32_t *target,
+                 double *lambda) {
+    int rc = check_cells(l, hist, n);
+    if (rc != CW_OK) return rc;
+    int64_t c0 = l->cell_off[hist];
+    if (type) CW_CUDA(cudaMemcpyAsync(type, l->type + c0, 4 * n, cudaMemcpyDeviceToHost, stream()));
+    if (volume) CW_CUDA(cudaMemcpyAsync(volume, l->volume + c0, 4 * n, cudaMemcpyDeviceToHost, stream()));
+    if (target) CW_CUDA(cudaMemcpyAsync(target, l->target + c0, 4 * n, cudaMemcpyDeviceToHost, stream()));
+    if (lambda) CW_CUDA(cudaMemcpyAsync(lambda, l->lambda + c0, 8 * n, cudaMemcpyDeviceToHost, stream()));
+    CW_CUDA(cudaStreamSynchronize(stream()));
+    return CW_OK;
+}
+
+int cw_cells_set_surface(cw_lattice l, uint32_t hist, uint32_t n, const int32_t *target_surface,
+                         const double *lambda_surface) {
+    int rc = check_cells(l, hist, n);
+    if (rc != CW_OK) return rc;
+    if (!l->surface_on) {
+        int64_t nc = l->ncells;
+        if ((rc = dalloc(&l->surface, nc)) || (rc = dalloc(&l->ssnap, nc)) || (rc = dalloc(&l->tsurf, nc)) ||
+            (rc = dalloc(&l->lsurf, nc)))
+            return rc;
+        CW_CUDA(cudaMemsetAsync(l->tsurf, 0, 4 * nc, stream()));
+        CW_CUDA(cudaMemsetAsync(l->lsurf, 0, 8 * nc, stream()));
+        l->surface_on = true;
+    }
+    int64_t c0 = l->cell_off[hist];
+    CW_CUDA(cudaMemcpyAsync(l->tsurf + c0, target_surface, 4 * n, cudaMemcpyHostToDevice, stream()));
+    CW_CUDA(cudaMemcpyAsync(l->lsurf + c0, lambda_surface, 8 * n, cudaMemcpyHostToDevice, stream()));
+    return lattice_recount(l, l->vsnap, l->surface);  // vsnap is scratch until the next pass
+}
+
+int cw_cells_get_surface(cw_lattice l, uint32_t hist, uint32_t n, int32_t *surface) {
+    int rc = check_cells(l, hist, n);
+    if (rc != CW_OK) return rc;
+    if (!l->surface_on) return fail(CW_ERR_NOT_FOUND, "the surface constraint is off");
+    CW_CUDA(cudaMemcpyAsync(surface, l->surface + l->cell_off[hist], 4 * n, cudaMemcpyDeviceToHost, stream()));
+    CW_CUDA(cudaStreamSynchronize(stream()));
+    return CW_OK;
+}
+
+int cw_lattice_set_seed(cw_lattice l, uint32_t hist, uint64_t seed) {
+    if (hist >= l->g.nh) return fail(CW_ERR_NOT_FOUND, "no history " + std::to_string(hist));
+    l->seed[hist] = seed;
+    uint2 k = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
+    CW_CUDA(cudaMemcpyAsync(l->d_keys + hist, &k, sizeof k, cudaMemcpyHostToDevice, stream()));
+    CW_CUDA(cudaStreamSynchronize(stream()));
+    return CW_OK;
+}
+
+int cw_lattice_set_mcs(cw_lattice l, uint32_t mcs) {
+    l->mcs = mcs;
+    CW_CUDA(cudaMemcpyAsync(l->d_flag, &mcs, sizeof mcs, cudaMemcpyHostToDevice, stream()));
+    CW_CUDA(cudaStreamSynchronize(stream()));
+    return CW_OK;
+}
+
+int cw_lattice_get_mcs(cw_lattice l, uint32_t *mcs) {
+    *mcs = l->mcs;
+    return CW_OK;
+}
+
+int cw_lattice_mcs(cw_lattice l, uint32_t sweeps) {
+    for (uint32_t s = 0; s < sweeps; ++s) {
+        int rc = lattice_sweep(l);
+        if (rc != CW_OK) return rc;
+    }
+    CW_CUDA(cudaStreamSynchronize(stream()));
+    return CW_OK;
+}
+
+int cw_lattice_delta_h_batch(cw_lattice l, uint32_t hist, uint32_t n, const int64_t *site, const int32_t *dst,
+                             double *out) {
+    if (hist >= l->g.nh) return fail(CW_ERR_NOT_FOUND, "no history " + std::to_string(hist));
+    if (n == 0) return CW_OK;
+    int64_t ns = l->g.sites(hist), cap = l->cell_off[hist + 1] - l->cell_off[hist];
+    for (uint32_t q = 0; q < n; ++q)
+        if (site[q] < 0 || site[q] >= ns || dst[q] < -1 || dst[q] >= cap)
+            return fail(CW_ERR_CONFIG, "proposal " + std::to_string(q) + " is outside the lattice or the records");
+    int64_t *d_site;
+    int32_t *d_dst;
+    double *d_out;
+    int rc;
+    if ((rc = dalloc(&d_site, n)) || (rc = dalloc(&d_dst, n)) || (rc = dalloc(&d_out, 6 * (size_t)n))) return rc;
+    CW_CUDA(cudaMemcpyAsync(d_site, site, 8 * (size_t)n, cudaMemcpyHostToDevice, stream()));
+    CW_CUDA(cudaMemcpyAsync(d_dst, dst, 4 * (size_t)n, cudaMemcpyHostToDevice, stream()));
+    k_delta_h<<<(n + T - 1) / T, T, 0, stream()>>>(lat_view(l), lat_tables(l), (int)hist, n, d_site, d_dst, d_out);
+    CW_LAUNCHED();
+    CW_CUDA(cudaMemcpyAsync(out, d_out, 48 * (size_t)n, cudaMemcpyDeviceToHost, stream()));
+    CW_CUDA(cudaStreamSynchronize(stream()));
+    dfree(d_site); dfree(d_dst); dfree(d_out);
+    return CW_OK;
+}
+
+int cw_lattice_verify(cw_lattice l, uint32_t hist, int32_t *ok) {
+    if (hist >= l->g.nh) return fail(CW_ERR_NOT_FOUND, "no history " + std::to_string(hist));
+    int32_t *vol, *surf = nullptr;
+    int *bad;
+    int rc;
+    if ((rc = dalloc(&vol, l->ncells)) || (rc = dalloc(&bad, 1))) return rc;
+    if (l->surface_on && (rc = dalloc(&surf, l->ncells)) != CW_OK) return rc;
+    if ((rc = lattice_recount(l, vol, surf)) != CW_OK) return rc;
+    CW_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), stream()));
+    int64_t cap = l->cell_off[hist + 1] - l->cell_off[hist];
+    unsigned nb = (unsigned)((cap + T - 1) / T);
+    k_compare<<<nb, T, 0, stream()>>>(vol, l->volume, l->d_cell_off, (int)hist, bad);
+    CW_LAUNCHED();
+    if (surf) {
+        k_compare<<<nb, T, 0, stream()>>>(surf, l->surface, l->d_cell_off, (int)hist, bad);
+        CW_LAUNCHED();
+    }
+    int hbad = 0;
+    CW_CUDA(cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, stream()));
+    CW_CUDA(cudaStreamSynchronize(stream()));
+    *ok = hbad == 0;
+    dfree(vol); dfree(bad); dfree(surf);
+    return CW_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,396 @@
+// Protein network: Network of crates/engine/src/network.rs on the device.
+//
+// Compilation (from_spec, network.rs:283-445) runs once on the host: names
+// are resolved to indices, terms laid out per node in file order.  The RK4
+// step (rk4, network.rs:777-799) runs one cell per thread, many cells per
+// warp; every cell of a launch walks the same term list, so a warp never
+// diverges on the network's shape.  Each thread keeps its state, midpoint,
+// stage slope and accumulated slope in shared memory laid out [node][thread],
+// so dynamic node indices cost a shared-memory access and no bank conflict.
+// Built without fused multiply-add: the sums round as the reference's do.
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <string>
+
+#include "cw_internal.cuh"
+
+using namespace cw;
+
+struct cw_network_s {
+    int32_t S = 0, nterms = 0;
+    std::vector<std::string> names;
+    std::vector<double> initial;
+    int32_t roles[7] = {-1, -1, -1, -1, -1, -1, -1};
+    double growth_coefficient = 0.0, lambda_volume = 0.0, max_target = NAN;
+    uint32_t reference_volume = 0;
+    // device copies of the compiled terms
+    int32_t *node_ptr = nullptr;  // S + 1
+    int4 *term = nullptr;         // (kind, source, has_hill, 0)
+    double4 *par = nullptr;       // (rate, hill_n, hill_k, param)
+};
+
+namespace {
+
+const char *INPUTS[6] = {"oxygen", "egf", "crowding", "stress", "waste", "necrotic_factor"};
+
+constexpr int MAXS = 32;
+
+struct NetDev {
+    const int32_t *node_ptr;
+    const int4 *term;
+    const double4 *par;
+    int32_t S, nterms;
+};
+
+// read, network.rs:670-680.
+__device__ __forceinline__ double read_source(int32_t src, const double *in, const double *st, int stride) {
+    if (src >= 0) return st[src * stride];
+    switch (-1 - src) {
+    case 0: return fmin(fmax(in[0], 0.0), 1.0);
+    case 1: return in[1];
+    case 2: return fmin(fmax(in[2], 0.0), 1.0);
+    case 3: return fmax(in[3], 0.0);
+    case 4: return fmax(in[4], 0.0);
+    default: return fmax(in[5], 0.0);
+    }
+}
+
+// driver, network.rs:56-64.  A Hill exponent of exactly two is a square.
+__device__ __forceinline__ double hill(double s, double n, double half) {
+    double sp = fmax(s, 0.0);
+    double sn, hn;
+    if (n == 2.0) { sn = sp * sp; hn = half * half; }
+    else { sn = pow(sp, n); hn = pow(half, n); }
+    return sn / (hn + sn);
+}
+
+// derivatives + term_rate, network.rs:686-734, for the thread's cell.
+// st/out point at node 0 of this thread's column (stride = threads).
+__device__ void derivatives(const NetDev &N, const int4 *sterm, const double4 *spar, const int32_t *sptr,
+                            const double *st, const double *in, double *out, int stride) {
+    for (int i = 0; i < N.S; ++i) {
+        double own = st[i * stride], rate = 0.0;
+        for (int t = sptr[i]; t < sptr[i + 1]; ++t) {
+            int4 tm = sterm[t];
+            double4 p = spar[t];
+            double k = p.x, r;
+            switch (tm.x) {
+            case CW_ACTIVATED_BY: {
+                double s = read_source(tm.y, in, st, stride);
+                double drv = tm.z ? hill(s, p.y, p.z) : s;
+                r = k * drv * (1.0 - own);
+                break;
+            }
+            case CW_INHIBITED_BY: {
+                double s = read_source(tm.y, in, st, stride);
+                double drv = tm.z ? hill(s, p.y, p.z) : s;
+                r = -k * drv * own;
+                break;
+            }
+            case CW_ACTIVATED_BY_ABSENCE_OF:
+                r = k * (1.0 - read_source(tm.y, in, st, stride)) * (1.0 - own);
+                break;
+            case CW_PRODUCED_BY: r = k * read_source(tm.y, in, st, stride); break;
+            case CW_DECAYS: r = -k * own; break;
+            case CW_RELAXES_TO: r = -k * (own - p.w); break;
+            case CW_DAMAGED_BELOW: {
+                double s = read_source(tm.y, in, st, stride);
+                r = -k * fmax((p.w - s) / p.w, 0.0);
+                break;
+            }
+            default: {
+                double s = read_source(tm.y, in, st, stride);
+                r = -k * fmax((s - p.w) / p.w, 0.0);
+                break;
+            }
+            }
+            rate += r;
+        }
+        out[i * stride] = rate;
+    }
+}
+
+constexpr int RT = 64;  // threads (cells) per block
+
+// state: [S][ncells] (node-major, coalesced); inputs: [6][ncells].
+// alive (optional): cells whose entry is zero are left as they are.
+__global__ void __launch_bounds__(RT) k_rk4(NetDev N, double *state, const double *inputs, int64_t ncells,
+                                            int64_t state_stride, int64_t input_stride, double dt, int substeps,
+                                            const uint8_t *alive) {
+    extern __shared__ double sm[];
+    const int S = N.S;
+    double *x = sm, *mid = sm + S * RT, *kk = sm + 2 * S * RT, *acc = sm + 3 * S * RT;
+    int4 *sterm = (int4 *)(sm + 4 * S * RT);
+    double4 *spar = (double4 *)(sterm + N.nterms);
+    int32_t *sptr = (int32_t *)(spar + N.nterms);
+    for (int t = threadIdx.x; t < N.nterms; t += RT) { sterm[t] = N.term[t]; spar[t] = N.par[t]; }
+    for (int t = threadIdx.x; t <= S; t += RT) sptr[t] = N.node_ptr[t];
+    __syncthreads();
+    int64_t c = (int64_t)blockIdx.x * RT + threadIdx.x;
+    if (c >= ncells) return;
+    if (alive && !alive[c]) return;
+    const int tid = threadIdx.x;
+    double in[6];
+    for (int q = 0; q < 6; ++q) in[q] = inputs[q * input_stride + c];
+    double *xs = x + tid, *ms = mid + tid, *ks = kk + tid, *as = acc + tid;
+    for (int i = 0; i < S; ++i) xs[i * RT] = state[i * state_stride + c];
+    for (int sub = 0; sub < substeps; ++sub) {
+        // k1 at x
+        derivatives(N, sterm, spar, sptr, xs, in, ks, RT);
+        for (int i = 0; i < S; ++i) {
+            double k1 = ks[i * RT];
+            as[i * RT] = k1;
+            ms[i * RT] = xs[i * RT] + 0.5 * dt * k1;
+        }
+        // k2 at x + dt/2 k1, k3 at x + dt/2 k2, k4 at x + dt k3
+        for (int stage = 1; stage < 4; ++stage) {
+            derivatives(N, sterm, spar, sptr, ms, in, ks, RT);
+            double step = stage < 2 ? 0.5 * dt : dt;
+            for (int i = 0; i < S; ++i) {
+                double kv = ks[i * RT];
+                if (stage < 3) {
+                    as[i * RT] = as[i * RT] + 2.0 * kv;
+                    ms[i * RT] = xs[i * RT] + step * kv;
+                } else {
+                    as[i * RT] = as[i * RT] + kv;
+                }
+            }
+        }
+        for (int i = 0; i < S; ++i) {
+            double delta = (dt / 6.0) * as[i * RT];
+            xs[i * RT] = fmin(fmax(xs[i * RT] + delta, 0.0), 1.0);
+        }
+    }
+    for (int i = 0; i < S; ++i) state[i * state_stride + c] = xs[i * RT];
+}
+
+// mechanics, network.rs:811-821.
+__global__ void k_mechanics(const double *state, int64_t ncells, int64_t stride, int growth, double coefficient,
+                            double max_target, int has_max, uint32_t reference_volume, uint32_t *target) {
+    int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncells) return;
+    double g = state[growth * stride + c];
+    double ratio = 1.0 + coefficient * g;
+    if (has_max) ratio = fmin(ratio, max_target);
+    double t = fmax((double)reference_volume * ratio, 0.0);
+    target[c] = isnan(t) ? 0u : (t >= 4294967295.0 ? 4294967295u : (uint32_t)t);
+}
+
+size_t rk4_smem(const cw_network_s *n) {
+    return sizeof(double) * 4 * n->S * RT + n->nterms * (sizeof(int4) + sizeof(double4)) + sizeof(int32_t) * (n->S + 1);
+}
+
+}  // namespace
+
+namespace cw {
+NetDev net_dev(const cw_network_s *n) { return NetDev{n->node_ptr, n->term, n->par, n->S, n->nterms}; }
+
+// Device-side RK4 on node-major state (used by the simulation driver).
+int network_step_device(const cw_network_s *n, double *state, const double *inputs, int64_t ncells,
+                        int64_t state_stride, int64_t input_stride, double dt, int substeps, const uint8_t *alive) {
+    if (ncells <= 0) return CW_OK;
+    size_t smem = rk4_smem(n);
+    k_rk4<<<(unsigned)((ncells + RT - 1) / RT), RT, smem, stream()>>>(net_dev(n), state, inputs, ncells, state_stride,
+                                                                      input_stride, dt, substeps, alive);
+    CW_LAUNCHED();
+    return CW_OK;
+}
+
+int network_mechanics_device(const cw_network_s *n, const double *state, int64_t ncells, int64_t stride,
+                             uint32_t *target) {
+    if (ncells <= 0) return CW_OK;
+    bool has = !std::isnan(n->max_target);
+    k_mechanics<<<(unsigned)((ncells + 255) / 256), 256, 0, stream()>>>(state, ncells, stride, n->roles[0],
+                                                                       n->growth_coefficient,
+                                                                       has ? n->max_target : 0.0, has ? 1 : 0,
+                                                                       n->reference_volume, target);
+    CW_LAUNCHED();
+    return CW_OK;
+}
+int32_t network_nodes(const cw_network_s *n) { return n->S; }
+double network_lambda(const cw_network_s *n) { return n->lambda_volume; }
+int32_t network_role(const cw_network_s *n, int k) { return n->roles[k]; }
+const std::vector<double> &network_initial(const cw_network_s *n) { return n->initial; }
+}  // namespace cw
+
+extern "C" {
+
+int cw_network_compile(int32_t nnodes, const char *const *names, const double *initial, int32_t nterms,
+                       const cw_term_spec *terms, const char *growth, const char *survival, const char *hypoxia,
+                       const char *differentiation, const char *apoptosis, const char *angiogenic,
+                       const char *evasion, double growth_coefficient, double lambda_volume, double max_target,
+                       uint32_t reference_volume, cw_network *out) {
+    *out = nullptr;
+    if (nnodes <= 0) return fail(CW_ERR_CONFIG, "a network needs a node");
+    if (nnodes > MAXS) return fail(CW_ERR_CONFIG, "at most " + std::to_string(MAXS) + " nodes");
+    if (!growth || !survival || !hypoxia)
+        return fail(CW_ERR_CONFIG,
+                    "the network declares no roles, and inherits none: say which node is growth, which is survival, "
+                    "and which is the hypoxia response");
+    std::map<std::string, int> index;
+    for (int i = 0; i < nnodes; ++i) {
+        std::string nm = names[i];
+        for (auto in : INPUTS)
+            if (nm == in)
+                return fail(CW_ERR_CONFIG, "node `" + nm +
+                                               "` takes the name of an environment input; inputs are [\"oxygen\", "
+                                               "\"egf\", \"crowding\", \"stress\", \"waste\", \"necrotic_factor\"]");
+        if (!index.emplace(nm, i).second) return fail(CW_ERR_CONFIG, "two nodes are named `" + nm + "`");
+    }
+    auto resolve = [&](const char *name, const std::string &whose, int32_t *src) -> int {
+        std::string nm = name ? name : "";
+        for (int q = 0; q < 6; ++q)
+            if (nm == INPUTS[q]) { *src = -1 - q; return CW_OK; }
+        auto it = index.find(nm);
+        if (it != index.end()) { *src = it->second; return CW_OK; }
+        std::string known = "[\"oxygen\", \"egf\", \"crowding\", \"stress\", \"waste\", \"necrotic_factor\"";
+        for (int i = 0; i < nnodes; ++i) known += std::string(", \"") + names[i] + "\"";
+        return fail(CW_ERR_CONFIG, "node `" + whose + "` reads `" + nm +
+                                       "`, which is neither a node nor an input; known names are " + known + "]");
+    };
+    std::vector<int32_t> ptr(nnodes + 1, 0);
+    std::vector<int4> tv(nterms);
+    std::vector<double4> pv(nterms);
+    int prev = 0;
+    for (int t = 0; t < nterms; ++t) {
+        const cw_term_spec &s = terms[t];
+        if (s.node < prev || s.node >= nnodes) return fail(CW_ERR_CONFIG, "terms must be listed in node order");
+        prev = s.node;
+        ptr[s.node + 1] += 1;
+        std::string whose = names[s.node];
+        if (s.kind < CW_ACTIVATED_BY || s.kind > CW_DAMAGED_ABOVE)
+            return fail(CW_ERR_CONFIG, "node `" + whose + "` has an unknown kind of term");
+        int32_t src = 0;
+        bool reads = s.kind != CW_DECAYS && s.kind != CW_RELAXES_TO;
+        if (reads) {
+            int rc = resolve(s.source, whose, &src);
+            if (rc != CW_OK) return rc;
+        }
+        int has_hill = 0;
+        if ((s.kind == CW_ACTIVATED_BY || s.kind == CW_INHIBITED_BY) && s.has_hill) {
+            if (s.hill_n <= 0.0 || s.hill_k <= 0.0)
+                return fail(CW_ERR_CONFIG, "node `" + whose + "` has a Hill term with n = " + std::to_string(s.hill_n) +
+                                               " and k = " + std::to_string(s.hill_k) + "; both must be positive");
+            has_hill = 1;
+        }
+        if ((s.kind == CW_DAMAGED_BELOW || s.kind == CW_DAMAGED_ABOVE) && s.param <= 0.0)
+            return fail(CW_ERR_CONFIG, "node `" + whose + "` is damaged " +
+                                           (s.kind == CW_DAMAGED_BELOW ? "below " : "above ") +
+                                           std::to_string(s.param) + ", which must be positive");
+        tv[t] = make_int4(s.kind, src, has_hill, 0);
+        pv[t] = make_double4(s.rate, has_hill ? s.hill_n : 0.0, has_hill ? s.hill_k : 0.0, s.param);
+    }
+    for (int i = 0; i < nnodes; ++i) ptr[i + 1] += ptr[i];
+    cw_network_s *n = new cw_network_s();
+    auto role = [&](const char *name, const char *which, int32_t *dst) -> int {
+        if (!name) { *dst = -1; return CW_OK; }
+        auto it = index.find(name);
+        if (it == index.end())
+            return fail(CW_ERR_CONFIG, std::string("the ") + which + " role names `" + name + "`, which is not a node");
+        *dst = it->second;
+        return CW_OK;
+    };
+    const char *rn[7] = {growth, survival, hypoxia, differentiation, apoptosis, angiogenic, evasion};
+    const char *rw[7] = {"growth", "survival", "hypoxia response", "differentiation", "apoptosis", "angiogenic",
+                         "evasion"};
+    for (int k = 0; k < 7; ++k) {
+        int rc = role(rn[k], rw[k], &n->roles[k]);
+        if (rc != CW_OK) { delete n; return rc; }
+    }
+    n->S = nnodes;
+    n->nterms = nterms;
+    for (int i = 0; i < nnodes; ++i) {
+        n->names.push_back(names[i]);
+        double v = initial ? initial[i] : 0.0;
+        n->initial.push_back(std::fmin(std::fmax(v, 0.0), 1.0));
+    }
+    n->growth_coefficient = growth_coefficient;
+    n->lambda_volume = lambda_volume;
+    n->max_target = max_target;
+    n->reference_volume = reference_volume;
+    int rc;
+    if ((rc = dalloc(&n->node_ptr, nnodes + 1)) || (rc = dalloc(&n->term, nterms)) ||
+        (rc = dalloc(&n->par, nterms))) {
+        cw_network_destroy(n);
+        return rc;
+    }
+    CW_CUDA(cudaMemcpy(n->node_ptr, ptr.data(), sizeof(int32_t) * (nnodes + 1), cudaMemcpyHostToDevice));
+    if (nterms > 0) {
+        CW_CUDA(cudaMemcpy(n->term, tv.data(), sizeof(int4) * nterms, cudaMemcpyHostToDevice));
+        CW_CUDA(cudaMemcpy(n->par, pv.data(), sizeof(double4) * nterms, cudaMemcpyHostToDevice));
+    }
+    size_t smem = rk4_smem(n);
+    if (smem > 48 * 1024 && cudaFuncSetAttribute(k_rk4, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+                                cudaSuccess) {
+        cw_network_destroy(n);
+        return fail(CW_ERR_CONFIG, "the network is too large for one block's shared memory");
+    }
+    *out = n;
+    return CW_OK;
+}
+
+int cw_network_destroy(cw_network n) {
+    if (!n) return CW_OK;
+    dfree(n->node_ptr); dfree(n->term); dfree(n->par);
+    delete n;
+    return CW_OK;
+}
+
+int cw_network_info(cw_network n, int32_t *nnodes, int32_t *roles7, double *initial) {
+    if (nnodes) *nnodes = n->S;
+    if (roles7) std::memcpy(roles7, n->roles, sizeof n->roles);
+    if (initial) std::memcpy(initial, n->initial.data(), sizeof(double) * n->S);
+    return CW_OK;
+}
+
+int cw_network_step_batch(cw_network n, int64_t ncells, double *state, const double *inputs, double dt,
+                          int32_t substeps) {
+    if (ncells <= 0) return CW_OK;
+    const int S = n->S;
+    double *d_state, *d_in;
+    int rc;
+    if ((rc = dalloc(&d_state, (size_t)ncells * S)) || (rc = dalloc(&d_in, (size_t)ncells * 6))) return rc;
+    // host rows are [cell][node]; the device works node-major
+    std::vector<double> t((size_t)ncells * (S > 6 ? S : 6));
+    for (int64_t c = 0; c < ncells; ++c)
+        for (int i = 0; i < S; ++i) t[(size_t)i * ncells + c] = state[c * S + i];
+    CW_CUDA(cudaMemcpyAsync(d_state, t.data(), sizeof(double) * ncells * S, cudaMemcpyHostToDevice, stream()));
+    CW_CUDA(cudaStreamSynchronize(stream()));
+    for (int64_t c = 0; c < ncells; ++c)
+        for (int q = 0; q < 6; ++q) t[(size_t)q * ncells + c] = inputs[c * 6 + q];
+    CW_CUDA(cudaMemcpyAsync(d_in, t.data(), sizeof(double) * ncells * 6, cudaMemcpyHostToDevice, stream()));
+    if ((rc = network_step_device(n, d_state, d_in, ncells, ncells, ncells, dt, substeps, nullptr)) != CW_OK)
+        return rc;
+    CW_CUDA(cudaMemcpyAsync(t.data(), d_state, sizeof(double) * ncells * S, cudaMemcpyDeviceToHost, stream()));
+    CW_CUDA(cudaStreamSynchronize(stream()));
+    for (int64_t c = 0; c < ncells; ++c)
+        for (int i = 0; i < S; ++i) state[c * S + i] = t[(size_t)i * ncells + c];
+    dfree(d_state);
+    dfree(d_in);
+    return CW_OK;
+}
+
+int cw_network_mechanics_batch(cw_network n, int64_t ncells, const double *state, uint32_t *target,
+                               double *lambda) {
+    if (ncells <= 0) return CW_OK;
+    const int S = n->S;
+    double *d_state;
+    uint32_t *d_t;
+    int rc;
+    if ((rc = dalloc(&d_state, (size_t)ncells * S)) || (rc = dalloc(&d_t, (size_t)ncells))) return rc;
+    std::vector<double> t((size_t)ncells * S);
+    for (int64_t c = 0; c < ncells; ++c)
+        for (int i = 0; i < S; ++i) t[(size_t)i * ncells + c] = state[c * S + i];
+    CW_CUDA(cudaMemcpyAsync(d_state, t.data(), sizeof(double) * ncells * S, cudaMemcpyHostToDevice, stream()));
+    if ((rc = network_mechanics_device(n, d_state, ncells, ncells, d_t)) != CW_OK) return rc;
+    CW_CUDA(cudaMemcpyAsync(target, d_t, sizeof(uint32_t) * ncells, cudaMemcpyDeviceToHost, stream()));
+    CW_CUDA(cudaStreamSynchronize(stream()));
+    if (lambda)
+        for (int64_t c = 0; c < ncells; ++c) lambda[c] = n->lambda_volume;
+    dfree(d_state);
+    dfree(d_t);
+    return CW_OK;
+}
+
+}  // extern "C"

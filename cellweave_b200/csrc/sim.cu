@@ -1,0 +1,395 @@
+// Simulation driver: Simulation<Running>::step (simulation.rs:1129-1350)
+// reduced to the data-parallel hot path, device-resident, for a batch of
+// independent histories (the campaign of src/campaign.rs:196-205 run as one
+// batch instead of one history per CPU thread).
+//
+// Per lattice step: (1) every field is painted from the lattice and relaxed
+// to its residual tolerance (declare_sources + relax); (2) every cell reads
+// its field means (mean_per_cell); (3) every living network takes
+// `substeps` RK4 steps; (4) survival below the threshold turns a cell
+// necrotic, every other cell's mechanics set its target volume; (5) the
+// lattice takes `sweeps` Monte Carlo steps.  Division, vessels, immune cells
+// and the rest of the reference's biology are not part of this path.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <random>
+
+#include "cw_internal.cuh"
+
+using namespace cw;
+
+struct cw_sim_s {
+    cw_sim_config cfg;
+    std::vector<uint32_t> w, h, d, ncells;
+    std::vector<uint64_t> seeds;
+    std::vector<double> J, sink;
+    cw_lattice_s *lat = nullptr;
+    cw_field_s *o2 = nullptr, *sig = nullptr;
+    cw_network_s *net = nullptr;
+    double *d_sink = nullptr;       // 8 rates by type
+    double *cell_o2 = nullptr, *cell_sig = nullptr, *sum = nullptr, *secretion = nullptr;
+    int32_t *count = nullptr;
+    double *state = nullptr, *inputs = nullptr;
+    uint8_t *alive = nullptr;
+    uint32_t *target32 = nullptr;
+    int64_t nc = 0;                 // records over all histories
+    Plan sites;
+    std::vector<cw_relax_stats> last;
+    uint32_t steps = 0;
+};
+
+namespace {
+
+constexpr int T = 256;
+
+__global__ void k_inputs(const int32_t *type, const int32_t *volume, const int64_t *cell_off, int nh, int64_t nc,
+                         int necrotic, const double *cell_o2, double egf, double *inputs, uint8_t *alive) {
+    int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nc) return;
+    // the medium slot of every history is not a cell
+    int lo = 0, hi = nh - 1;
+    while (lo < hi) { int mid = (lo + hi + 1) >> 1; if (cell_off[mid] <= c) lo = mid; else hi = mid - 1; }
+    bool medium = c == cell_off[lo];
+    bool a = !medium && volume[c] > 0 && type[c] != necrotic;
+    alive[c] = a;
+    inputs[0 * nc + c] = cell_o2[c];
+    inputs[1 * nc + c] = egf;
+    inputs[2 * nc + c] = 0.0;
+    inputs[3 * nc + c] = 0.0;
+    inputs[4 * nc + c] = 0.0;
+    inputs[5 * nc + c] = 0.0;
+}
+
+__global__ void k_secretion(const uint8_t *alive, const double *cell_o2, int64_t nc, double level, double rate,
+                            double *secretion) {
+    int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < nc) secretion[c] = (alive[c] && cell_o2[c] < level) ? rate : 0.0;
+}
+
+// Fate and upward coupling (simulation.rs:1212-1309, the necrosis and
+// mechanics branches): survival below the threshold makes the cell
+// necrotic; every other living cell takes the target its mechanics give.
+__global__ void k_fates(const uint8_t *alive, const double *state, int64_t nc, int survival, double death,
+                        int necrotic, const uint32_t *mech_target, int32_t *type, int32_t *target, double *lambda,
+                        double lam) {
+    int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nc || !alive[c]) return;
+    if (necrotic >= 0 && state[survival * nc + c] < death) {
+        type[c] = necrotic;
+        return;
+    }
+    target[c] = (int32_t)min(mech_target[c], 0x7fffffffu);
+    lambda[c] = lam;
+}
+
+__global__ void k_stats(const uint8_t *alive, const double *cell_o2, const int32_t *volume, const int64_t *cell_off,
+                        int nh, double *out) {
+    int h = blockIdx.x;
+    int64_t c0 = cell_off[h], c1 = cell_off[h + 1];
+    double living = 0.0, o2 = 0.0, vol = 0.0;
+    for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
+        if (alive[c]) living += 1.0;
+        if (c > c0 && volume[c] > 0) { o2 += cell_o2[c] * volume[c]; vol += volume[c]; }
+    }
+    living = warp_sum(living); o2 = warp_sum(o2); vol = warp_sum(vol);
+    __shared__ double s[3][32];
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) { s[0][wid] = living; s[1][wid] = o2; s[2][wid] = vol; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0, b = 0, v = 0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) { a += s[0][k]; b += s[1][k]; v += s[2][k]; }
+        out[4 * h + 0] = a;
+        out[4 * h + 1] = v > 0 ? b / v : 0.0;
+    }
+}
+
+__global__ void k_fill_u8(uint8_t *p, int64_t n, uint8_t v) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = v;
+}
+
+// Seed one history on the host: squares (or cubes) of side s of random type
+// 1..types at random places that overlap nothing, `n` of them or as many as
+// fit (seeding 0); a regular packing of squares with a gap of (pitch - s)
+// (seeding 1); cubes packed in a ball around the centre (seeding 2).
+void seed_history(const cw_sim_config &c, uint32_t W, uint32_t H, uint32_t D, uint32_t n, uint64_t seed,
+                  std::vector<int32_t> &grid, std::vector<int32_t> &type, int ncelltypes) {
+    std::mt19937_64 rng(seed);
+    grid.assign((size_t)W * H * D, 0);
+    type.assign(1, 0);
+    const int s = c.seed_side > 0 ? c.seed_side : 7;
+    auto pick_type = [&]() { return 1 + (int)(rng() % (uint64_t)ncelltypes); };
+    // vessel column as obstacle (held by the oxygen field)
+    if (c.o2_hold == 1)
+        for (uint32_t z = 0; z < D; ++z)
+            for (uint32_t y = 0; y < H; ++y) grid[((size_t)z * H + y) * W + W / 2] = -1;
+    auto free_box = [&](uint32_t x0, uint32_t y0, uint32_t z0, uint32_t sx, uint32_t sy, uint32_t sz) {
+        if (x0 + sx > W || y0 + sy > H || z0 + sz > D) return false;
+        for (uint32_t z = z0; z < z0 + sz; ++z)
+            for (uint32_t y = y0; y < y0 + sy; ++y)
+                for (uint32_t x = x0; x < x0 + sx; ++x)
+                    if (grid[((size_t)z * H + y) * W + x] != 0) return false;
+        return true;
+    };
+    auto put = [&](uint32_t x0, uint32_t y0, uint32_t z0, uint32_t sx, uint32_t sy, uint32_t sz) {
+        int32_t id = (int32_t)type.size();
+        for (uint32_t z = z0; z < z0 + sz; ++z)
+            for (uint32_t y = y0; y < y0 + sy; ++y)
+                for (uint32_t x = x0; x < x0 + sx; ++x) grid[((size_t)z * H + y) * W + x] = id;
+        type.push_back(pick_type());
+    };
+    uint32_t sz = D > 1 ? (uint32_t)s : 1;
+    if (c.seeding == 1) {
+        uint32_t pitch = (uint32_t)s + 2;
+        for (uint32_t z = 0; z + sz <= D; z += (D > 1 ? pitch : 1))
+            for (uint32_t y = 1; y + s <= H; y += pitch)
+                for (uint32_t x = 1; x + s <= W; x += pitch)
+                    if (type.size() - 1 < n && free_box(x, y, z, s, s, sz)) put(x, y, z, s, s, sz);
+    } else if (c.seeding == 2 && D > 1) {
+        // cubes on a grid of pitch s inside a ball of radius R around the centre
+        double R = std::cbrt(3.0 * n * s * s * s / (4.0 * 3.14159265358979)) + 0.5 * s;
+        double cx = W / 2.0, cy = H / 2.0, cz = D / 2.0;
+        for (uint32_t z = 0; z + s <= D; z += s)
+            for (uint32_t y = 0; y + s <= H; y += s)
+                for (uint32_t x = 0; x + s <= W; x += s) {
+                    double dx = x + s / 2.0 - cx, dy = y + s / 2.0 - cy, dz = z + s / 2.0 - cz;
+                    if (dx * dx + dy * dy + dz * dz <= R * R && type.size() - 1 < n && free_box(x, y, z, s, s, s))
+                        put(x, y, z, s, s, s);
+                }
+    } else {
+        uint64_t tries = 0, cap = 200ull * n + 1000;
+        while (type.size() - 1 < n && tries++ < cap) {
+            uint32_t x = (uint32_t)(rng() % (W - s + 1)), y = (uint32_t)(rng() % (H - s + 1));
+            uint32_t z = D > 1 ? (uint32_t)(rng() % (D - sz + 1)) : 0;
+            if (free_box(x, y, z, s, s, sz)) put(x, y, z, s, s, sz);
+        }
+    }
+}
+
+int64_t blocks(int64_t n) { return (n + T - 1) / T; }
+
+}  // namespace
+
+extern "C" {
+
+int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out) {
+    *out = nullptr;
+    const cw_sim_config &c = *cfg;
+    if (c.nh == 0) return fail(CW_ERR_CONFIG, "a simulation needs a history");
+    if (c.K < 2 || c.K > 8) return fail(CW_ERR_CONFIG, "2 to 8 types, the medium included");
+    if (c.nfields < 1 || c.nfields > 2) return fail(CW_ERR_CONFIG, "one or two fields");
+    if (!net) return fail(CW_ERR_CONFIG, "a simulation needs a network");
+    int32_t survival = network_role(net, 1);
+    cw_sim_s *s = new cw_sim_s();
+    s->cfg = c;
+    s->w.assign(c.w, c.w + c.nh);
+    s->h.assign(c.h, c.h + c.nh);
+    s->d.assign(c.nh, 1);
+    if (c.d) s->d.assign(c.d, c.d + c.nh);
+    s->ncells.assign(c.ncells, c.ncells + c.nh);
+    s->seeds.assign(c.seeds, c.seeds + c.nh);
+    s->J.assign(c.J, c.J + c.K * c.K);
+    s->sink.assign(8, 0.0);
+    for (int k = 0; k < c.K; ++k) s->sink[k] = c.o2_sink_by_type[k];
+    s->cfg.w = s->w.data(); s->cfg.h = s->h.data(); s->cfg.d = s->d.data();
+    s->cfg.ncells = s->ncells.data(); s->cfg.seeds = s->seeds.data(); s->cfg.J = s->J.data();
+    s->cfg.o2_sink_by_type = s->sink.data();
+    s->net = net;
+    int ncelltypes = c.necrotic_type > 0 ? c.necrotic_type - 1 : c.K - 1;
+    if (ncelltypes < 1) ncelltypes = 1;
+    // seed every history on the host
+    std::vector<std::vector<int32_t>> grids(c.nh), types(c.nh);
+    std::vector<uint32_t> cap(c.nh);
+    for (uint32_t k = 0; k < c.nh; ++k) {
+        seed_history(c, s->w[k], s->h[k], s->d[k], s->ncells[k], s->seeds[k], grids[k], types[k], ncelltypes);
+        cap[k] = (uint32_t)types[k].size();
+    }
+    int rc = cw_lattice_create(c.nh, s->w.data(), s->h.data(), s->d.data(), cap.data(), c.temperature, &s->lat);
+    if (rc != CW_OK) { cw_sim_destroy(s); return rc; }
+    if ((rc = cw_lattice_set_contact(s->lat, c.K, c.J, c.contact_order)) != CW_OK) { cw_sim_destroy(s); return rc; }
+    for (uint32_t k = 0; k < c.nh; ++k) {
+        uint32_t n = cap[k];
+        std::vector<int32_t> vol(n, 0), tgt(n, c.target_volume);
+        std::vector<double> lam(n, c.lambda_volume);
+        for (int32_t id : grids[k]) if (id > 0) vol[id] += 1;
+        tgt[0] = 0;
+        lam[0] = 0.0;
+        if ((rc = cw_lattice_upload(s->lat, k, grids[k].data())) ||
+            (rc = cw_cells_set(s->lat, k, n, types[k].data(), vol.data(), tgt.data(), lam.data())) ||
+            (rc = cw_lattice_set_seed(s->lat, k, s->seeds[k]))) {
+            cw_sim_destroy(s);
+            return rc;
+        }
+        if (c.surface_target > 0) {
+            std::vector<int32_t> ts(n, c.surface_target);
+            std::vector<double> ls(n, c.lambda_surface);
+            if ((rc = cw_cells_set_surface(s->lat, k, n, ts.data(), ls.data())) != CW_OK) {
+                cw_sim_destroy(s);
+                return rc;
+            }
+        }
+    }
+    // fields
+    if ((rc = cw_field_create(c.nh, s->w.data(), s->h.data(), s->d.data(), c.o2_dcoef, 0.0, 1.0, &s->o2)) != CW_OK) {
+        cw_sim_destroy(s);
+        return rc;
+    }
+    for (uint32_t k = 0; k < c.nh; ++k) {
+        int64_t n = (int64_t)s->w[k] * s->h[k] * s->d[k];
+        std::vector<uint8_t> held(n, 0);
+        uint32_t W = s->w[k], H = s->h[k], D = s->d[k];
+        for (uint32_t z = 0; z < D; ++z)
+            for (uint32_t y = 0; y < H; ++y)
+                for (uint32_t x = 0; x < W; ++x) {
+                    bool on = c.o2_hold == 0 ? y == 0
+                            : c.o2_hold == 1 ? x == W / 2
+                                             : (x == 0 || y == 0 || x + 1 == W || y + 1 == H || z == 0 || z + 1 == D);
+                    held[((size_t)z * H + y) * W + x] = on;
+                }
+        if ((rc = cw_field_hold_mask(s->o2, k, held.data(), 1.0)) != CW_OK) { cw_sim_destroy(s); return rc; }
+    }
+    if (c.nfields == 2 &&
+        (rc = cw_field_create(c.nh, s->w.data(), s->h.data(), s->d.data(), c.signal_dcoef, c.signal_decay, 0.0,
+                              &s->sig)) != CW_OK) {
+        cw_sim_destroy(s);
+        return rc;
+    }
+    // per-cell device state
+    s->nc = s->lat->ncells;
+    int S = network_nodes(net);
+    int64_t nc = s->nc;
+    if ((rc = dalloc(&s->d_sink, 8)) || (rc = dalloc(&s->cell_o2, nc)) || (rc = dalloc(&s->cell_sig, nc)) ||
+        (rc = dalloc(&s->sum, nc)) || (rc = dalloc(&s->secretion, nc)) || (rc = dalloc(&s->count, nc)) ||
+        (rc = dalloc(&s->state, nc * S)) || (rc = dalloc(&s->inputs, nc * 6)) || (rc = dalloc(&s->alive, nc)) ||
+        (rc = dalloc(&s->target32, nc))) {
+        cw_sim_destroy(s);
+        return rc;
+    }
+    CW_CUDA(cudaMemcpyAsync(s->d_sink, s->sink.data(), 8 * sizeof(double), cudaMemcpyHostToDevice, stream()));
+    std::vector<double> st((size_t)nc * S);
+    const std::vector<double> &init = network_initial(net);
+    for (int i = 0; i < S; ++i) std::fill(st.begin() + (size_t)i * nc, st.begin() + (size_t)(i + 1) * nc, init[i]);
+    CW_CUDA(cudaMemcpyAsync(s->state, st.data(), sizeof(double) * nc * S, cudaMemcpyHostToDevice, stream()));
+    CW_CUDA(cudaMemsetAsync(s->cell_o2, 0, sizeof(double) * nc, stream()));
+    CW_CUDA(cudaMemsetAsync(s->cell_sig, 0, sizeof(double) * nc, stream()));
+    std::vector<int64_t> per(c.nh);
+    for (uint32_t k = 0; k < c.nh; ++k) per[k] = (int64_t)s->w[k] * s->h[k] * s->d[k];
+    if ((rc = s->sites.build(per, T)) != CW_OK) { cw_sim_destroy(s); return rc; }
+    s->last.assign(c.nh, cw_relax_stats{});
+    (void)survival;
+    CW_CUDA(cudaStreamSynchronize(stream()));
+    *out = s;
+    return CW_OK;
+}
+
+int cw_sim_destroy(cw_sim s) {
+    if (!s) return CW_OK;
+    cw_lattice_destroy(s->lat);
+    cw_field_destroy(s->o2);
+    cw_field_destroy(s->sig);
+    dfree(s->d_sink); dfree(s->cell_o2); dfree(s->cell_sig); dfree(s->sum); dfree(s->secretion); dfree(s->count);
+    dfree(s->state); dfree(s->inputs); dfree(s->alive); dfree(s->target32);
+    s->sites.release();
+    delete s;
+    return CW_OK;
+}
+
+int cw_sim_step(cw_sim s, uint32_t nsteps) {
+    const cw_sim_config &c = s->cfg;
+    int64_t nc = s->nc;
+    int S = network_nodes(s->net);
+    int survival = network_role(s->net, 1);
+    cw_relax_opts o{};
+    o.omega = c.omega;
+    o.stop = CW_STOP_RESIDUAL;
+    o.tolerance = c.tolerance;
+    o.max_sweeps = 200000;
+    o.precision = c.precision;
+    int rc;
+    for (uint32_t step = 0; step < nsteps; ++step, ++s->steps) {
+        bool solve = c.relax_every <= 1 || (s->steps % (uint32_t)c.relax_every) == 0;
+        if (solve) {
+            // 1. downward coupling and the oxygen solve
+            if ((rc = couple_uptake_device(s->o2, s->lat, s->d_sink, 8, s->o2->lin_sink, s->sites)) != CW_OK) return rc;
+            s->o2->lin_sink_on = true;
+            if ((rc = cw_field_relax(s->o2, &o, s->last.data())) != CW_OK) return rc;
+        }
+        // 2. what each cell sits in
+        if ((rc = couple_means_device(s->o2, s->lat, s->sum, s->count, s->cell_o2, s->sites)) != CW_OK) return rc;
+        k_inputs<<<(unsigned)blocks(nc), T, 0, stream()>>>(s->lat->type, s->lat->volume, s->lat->d_cell_off, c.nh, nc,
+                                                           c.necrotic_type, s->cell_o2, 0.2, s->inputs, s->alive);
+        CW_LAUNCHED();
+        if (s->sig && solve) {
+            k_secretion<<<(unsigned)blocks(nc), T, 0, stream()>>>(s->alive, s->cell_o2, nc, c.hypoxic_level,
+                                                                  c.signal_secretion, s->secretion);
+            CW_LAUNCHED();
+            if ((rc = couple_production_device(s->sig, s->lat, s->secretion, s->sites)) != CW_OK) return rc;
+            std::vector<cw_relax_stats> st2(c.nh);
+            if ((rc = cw_field_relax(s->sig, &o, st2.data())) != CW_OK) return rc;
+            if ((rc = couple_means_device(s->sig, s->lat, s->sum, s->count, s->cell_sig, s->sites)) != CW_OK)
+                return rc;
+        }
+        // 3. every living network
+        if ((rc = network_step_device(s->net, s->state, s->inputs, nc, nc, nc, c.dt, c.substeps, s->alive)) != CW_OK)
+            return rc;
+        // 4. fates and mechanics
+        if ((rc = network_mechanics_device(s->net, s->state, nc, nc, s->target32)) != CW_OK) return rc;
+        k_fates<<<(unsigned)blocks(nc), T, 0, stream()>>>(s->alive, s->state, nc, survival, c.death_threshold,
+                                                          c.necrotic_type, s->target32, s->lat->type,
+                                                          s->lat->target, s->lat->lambda, c.lambda_volume);
+        CW_LAUNCHED();
+        // 5. the lattice
+        for (int k = 0; k < c.sweeps; ++k)
+            if ((rc = lattice_sweep(s->lat)) != CW_OK) return rc;
+        (void)S;
+    }
+    return CW_OK;
+}
+
+int cw_sim_lattice(cw_sim s, cw_lattice *lat) {
+    *lat = s->lat;
+    return CW_OK;
+}
+
+int cw_sim_field(cw_sim s, int32_t which, cw_field *f) {
+    *f = which == 0 ? s->o2 : s->sig;
+    if (!*f) return fail(CW_ERR_NOT_FOUND, "no such field");
+    return CW_OK;
+}
+
+int cw_sim_stats(cw_sim s, double *out) {
+    uint32_t nh = s->cfg.nh;
+    double *d_out;
+    int rc = dalloc(&d_out, 4 * (size_t)nh);
+    if (rc != CW_OK) return rc;
+    CW_CUDA(cudaMemsetAsync(d_out, 0, sizeof(double) * 4 * nh, stream()));
+    k_stats<<<nh, 256, 0, stream()>>>(s->alive, s->cell_o2, s->lat->volume, s->lat->d_cell_off, nh, d_out);
+    CW_LAUNCHED();
+    CW_CUDA(cudaMemcpyAsync(out, d_out, sizeof(double) * 4 * nh, cudaMemcpyDeviceToHost, stream()));
+    CW_CUDA(cudaStreamSynchronize(stream()));
+    for (uint32_t k = 0; k < nh; ++k) {
+        out[4 * k + 2] = (double)s->last[k].sweeps;
+        out[4 * k + 3] = s->last[k].residual;
+    }
+    dfree(d_out);
+    return CW_OK;
+}
+
+int cw_sim_network_state(cw_sim s, uint32_t hist, uint32_t n, double *state) {
+    if (hist >= s->cfg.nh) return fail(CW_ERR_NOT_FOUND, "no history " + std::to_string(hist));
+    int S = network_nodes(s->net);
+    int64_t c0 = s->lat->cell_off[hist], cap = s->lat->cell_off[hist + 1] - c0;
+    if ((int64_t)n > cap) return fail(CW_ERR_CONFIG, "more cells asked for than the history holds");
+    std::vector<double> col(n);
+    for (int i = 0; i < S; ++i) {
+        CW_CUDA(cudaMemcpyAsync(col.data(), s->state + (size_t)i * s->nc + c0, sizeof(double) * n,
+                                cudaMemcpyDeviceToHost, stream()));
+        CW_CUDA(cudaStreamSynchronize(stream()));
+        for (uint32_t cc = 0; cc < n; ++cc) state[(size_t)cc * S + i] = col[cc];
+    }
+    return CW_OK;
+}
+
+}  // extern "C"

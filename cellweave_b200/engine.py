@@ -1,0 +1,548 @@
+"""The reference's engine API over the C ABI: CpmLattice, ScalarField,
+Network, the coupling functions and a batched Simulation driver.
+
+Names, argument meanings and errors follow crates/engine of the reference
+(cpm.rs, pde.rs, network.rs, coupling.rs, simulation.rs); every object may
+hold a batch of independent histories (``hist`` picks one), a single history
+being a batch of one.  All compute runs in ``libcellweave_b200.so`` on the
+GPU; this module only moves arguments across.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+import tomllib
+from typing import Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import ConfigError, call, lib, ptr
+
+OBSTACLE = -1
+FP64, FP32_DC = 0, 1
+STOP_MAX_CHANGE, STOP_RESIDUAL = 0, 1
+VALUES, UPTAKE, PRODUCTION, LIN_SINK = 0, 1, 2, 3
+
+
+def _dims(dims):
+    dims = [tuple(int(v) for v in (tuple(d) + (1,))[:3]) if len(d) < 3 else tuple(int(v) for v in d) for d in dims]
+    w = np.array([d[0] for d in dims], np.uint32)
+    h = np.array([d[1] for d in dims], np.uint32)
+    z = np.array([d[2] for d in dims], np.uint32)
+    return dims, w, h, z
+
+
+# ============================================================== ScalarField
+class ScalarField:
+    """ScalarField (crates/engine/src/pde.rs:30-640) of one or more histories."""
+
+    def __init__(self, dims: Sequence[Sequence[int]], d: float, decay: float = 0.0, initial: float = 0.0):
+        self.dims, w, h, z = _dims(dims)
+        handle = C.c_void_p()
+        call("cw_field_create", len(self.dims), ptr(w), ptr(h), ptr(z), float(d), float(decay), float(initial),
+             C.byref(handle))
+        self._h = handle
+        self.d, self.decay = float(d), float(decay)
+
+    @classmethod
+    def new(cls, width, height, d, decay=0.0, initial=0.0):
+        """ScalarField::new (pde.rs:82-90)."""
+        return cls([(width, height, 1)], d, decay, initial)
+
+    @classmethod
+    def with_depth(cls, width, height, depth, d, decay=0.0, initial=0.0):
+        """ScalarField::with_depth (pde.rs:98-131)."""
+        return cls([(width, height, depth)], d, decay, initial)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value and _lib._LIB is not None:
+            lib().cw_field_destroy(h)
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    def n(self, hist=0):
+        w, h, d = self.dims[hist]
+        return w * h * d
+
+    # ---- arrays
+    def upload(self, which: int, arr, hist: int = 0):
+        a = np.ascontiguousarray(arr, np.float64).reshape(-1)
+        if a.size != self.n(hist):
+            raise ConfigError(f"expected {self.n(hist)} values, got {a.size}")
+        call("cw_field_upload", self._h, hist, which, ptr(a))
+
+    def download(self, which: int = VALUES, hist: int = 0) -> np.ndarray:
+        out = np.empty(self.n(hist))
+        call("cw_field_download", self._h, hist, which, ptr(out))
+        return out
+
+    def values(self, hist=0):
+        return self.download(VALUES, hist)
+
+    def set_values(self, arr, hist=0):
+        self.upload(VALUES, arr, hist)
+
+    def set_uptake_array(self, arr, hist=0):
+        """set_uptake_at over every pixel (pde.rs:170-174): rates floored at zero."""
+        self.upload(UPTAKE, np.maximum(np.asarray(arr, np.float64), 0.0), hist)
+
+    def set_production_array(self, arr, hist=0):
+        """set_production_at over every pixel (pde.rs:178-182)."""
+        self.upload(PRODUCTION, np.maximum(np.asarray(arr, np.float64), 0.0), hist)
+
+    def set_linear_sink(self, arr, hist=0):
+        """The first-order sink k_i of D lap c - k_i c (an extension; zero is the reference)."""
+        self.upload(LIN_SINK, arr, hist)
+
+    def held(self, hist=0):
+        out = np.empty(self.n(hist), np.uint8)
+        call("cw_field_download_held", self._h, hist, ptr(out))
+        return out
+
+    def set_held(self, mask, hist=0):
+        m = np.ascontiguousarray(mask, np.uint8).reshape(-1)
+        call("cw_field_upload_held", self._h, hist, ptr(m))
+
+    # ---- reference methods
+    def with_source(self, source):
+        call("cw_field_set_source", self._h, float(source))
+        return self
+
+    def set_diffusion(self, d):
+        call("cw_field_set_diffusion", self._h, float(d))
+        self.d = float(d)
+
+    def fill(self, value):
+        call("cw_field_fill", self._h, float(value))
+
+    def clear_uptake(self):
+        call("cw_field_clear", self._h, UPTAKE)
+
+    def clear_production(self):
+        call("cw_field_clear", self._h, PRODUCTION)
+
+    def release_all(self):
+        call("cw_field_release_all", self._h)
+
+    def hold_where(self, value, mask, hist=0):
+        """hold_where (pde.rs:491-498) with a boolean mask."""
+        m = np.ascontiguousarray(mask, np.uint8).reshape(-1)
+        call("cw_field_hold_mask", self._h, hist, ptr(m), float(value))
+
+    def hold_bath(self, value, open_mask, hist=0):
+        """hold_bath_at (pde.rs:550-631) with `open` given as a mask."""
+        o = np.ascontiguousarray(open_mask, np.uint8).reshape(-1)
+        call("cw_field_hold_bath", self._h, hist, ptr(o), float(value))
+
+    def relax(self, tolerance, max_sweeps, omega=None, stop=STOP_MAX_CHANGE, precision=FP64, inner_sweeps=0,
+              block_depth=0, stats=False):
+        """relax (pde.rs:245-288): the sweep count of every history (SimulationError if one did not settle)."""
+        o = _lib.RelaxOpts(float(omega) if omega else 0.0, int(stop), float(tolerance), int(max_sweeps),
+                           int(precision), int(inner_sweeps), int(block_depth))
+        st = (_lib.RelaxStats * len(self.dims))()
+        rc = lib().cw_field_relax(self._h, C.byref(o), st)
+        result = [dict(sweeps=s.sweeps, last_change=s.last_change, residual=s.residual, status=s.status,
+                       omega=s.omega) for s in st]
+        if rc != _lib.OK:
+            err = _lib._ERRORS.get(rc, _lib.CellweaveError)(lib().cw_last_error().decode())
+            err.stats = result
+            raise err
+        if stats:
+            return result
+        return result[0]["sweeps"] if len(result) == 1 else [r["sweeps"] for r in result]
+
+    def residual(self):
+        out = np.empty(len(self.dims))
+        call("cw_field_residual", self._h, ptr(out))
+        return out
+
+    def inflow(self):
+        """inflow (pde.rs:415-456) of every history."""
+        out = np.empty(len(self.dims))
+        call("cw_field_inflow", self._h, ptr(out))
+        return out if len(out) > 1 else float(out[0])
+
+    def step(self, dt):
+        """DiffusionField::step (pde.rs:705-728)."""
+        call("cw_field_step", self._h, float(dt))
+
+    def free_count(self, hist=0):
+        return int((self.held(hist) == 0).sum())
+
+    def value_at(self, i, hist=0):
+        v = self.values(hist)
+        return float(v[i]) if 0 <= i < v.size else 0.0
+
+    def concentration_at(self, x, y, hist=0):
+        w, h, _ = self.dims[hist]
+        if x >= w or y >= h:
+            return 0.0
+        return self.value_at(y * w + x, hist)
+
+
+# ============================================================== CpmLattice
+class CpmLattice:
+    """CpmLattice (crates/engine/src/cpm.rs:187-1041) of one or more histories."""
+
+    def __init__(self, dims, temperature, capacity, order=1, J=None):
+        self.dims, w, h, z = _dims(dims)
+        cap = np.array(capacity if np.ndim(capacity) else [capacity] * len(self.dims), np.uint32)
+        handle = C.c_void_p()
+        call("cw_lattice_create", len(self.dims), ptr(w), ptr(h), ptr(z), ptr(cap), float(temperature),
+             C.byref(handle))
+        self._h = handle
+        self.capacity = cap
+        self.temperature = float(temperature)
+        if J is not None:
+            self.set_contact(J, order)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value and _lib._LIB is not None:
+            lib().cw_lattice_destroy(h)
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    def n(self, hist=0):
+        w, h, d = self.dims[hist]
+        return w * h * d
+
+    def set_contact(self, J, order=1):
+        """ContactEnergy as a K x K table over types, and set_contact_order (cpm.rs:274-301)."""
+        J = np.ascontiguousarray(J, np.float64)
+        call("cw_lattice_set_contact", self._h, int(J.shape[0]), ptr(J), int(order))
+
+    def set_temperature(self, t):
+        call("cw_lattice_set_temperature", self._h, float(t))
+
+    def upload(self, grid, hist=0):
+        g = np.ascontiguousarray(grid, np.int32).reshape(-1)
+        if g.size != self.n(hist):
+            raise ConfigError(f"expected {self.n(hist)} pixels, got {g.size}")
+        call("cw_lattice_upload", self._h, hist, ptr(g))
+
+    def grid(self, hist=0):
+        out = np.empty(self.n(hist), np.int32)
+        call("cw_lattice_download", self._h, hist, ptr(out))
+        w, h, d = self.dims[hist]
+        return out.reshape(d, h, w)
+
+    def set_cells(self, type_=None, volume=None, target=None, lam=None, hist=0):
+        arrs = [None if a is None else np.ascontiguousarray(a, dt) for a, dt in
+                ((type_, np.int32), (volume, np.int32), (target, np.int32), (lam, np.float64))]
+        n = next(len(a) for a in arrs if a is not None)
+        call("cw_cells_set", self._h, hist, n, *[ptr(a) for a in arrs])
+
+    def cells(self, n=None, hist=0):
+        n = int(self.capacity[hist]) if n is None else n
+        t, v, g = (np.empty(n, np.int32) for _ in range(3))
+        lam = np.empty(n)
+        call("cw_cells_get", self._h, hist, n, ptr(t), ptr(v), ptr(g), ptr(lam))
+        return dict(type=t, volume=v, target=g, lam=lam)
+
+    def volume(self, cid, hist=0):
+        return int(self.cells(hist=hist)["volume"][cid])
+
+    def set_surface(self, target_surface, lambda_surface, hist=0):
+        ts = np.ascontiguousarray(target_surface, np.int32)
+        ls = np.ascontiguousarray(lambda_surface, np.float64)
+        call("cw_cells_set_surface", self._h, hist, len(ts), ptr(ts), ptr(ls))
+
+    def surfaces(self, n=None, hist=0):
+        n = int(self.capacity[hist]) if n is None else n
+        out = np.empty(n, np.int32)
+        call("cw_cells_get_surface", self._h, hist, n, ptr(out))
+        return out
+
+    def set_seed(self, seed, hist=0):
+        call("cw_lattice_set_seed", self._h, hist, int(seed) & (2**64 - 1))
+
+    def set_mcs(self, mcs):
+        call("cw_lattice_set_mcs", self._h, int(mcs))
+
+    @property
+    def mcs(self):
+        v = C.c_uint32()
+        call("cw_lattice_get_mcs", self._h, C.byref(v))
+        return v.value
+
+    def monte_carlo_step(self, sweeps=1):
+        """monte_carlo_step (cpm.rs:748-772), `sweeps` times, on every history."""
+        call("cw_lattice_mcs", self._h, int(sweeps))
+
+    def delta_h(self, sites, dsts, hist=0):
+        """Delta-H (cpm.rs:841-894) of copying dsts[k] into sites[k]: rows of
+        (contact numerator, contact, volume, surface, adhesion+volume, total)."""
+        s = np.ascontiguousarray(sites, np.int64)
+        d = np.ascontiguousarray(dsts, np.int32)
+        out = np.empty((len(s), 6))
+        call("cw_lattice_delta_h_batch", self._h, hist, len(s), ptr(s), ptr(d), ptr(out))
+        return out
+
+    def records_match_grid(self, hist=0):
+        ok = C.c_int32()
+        call("cw_lattice_verify", self._h, hist, C.byref(ok))
+        return bool(ok.value)
+
+    @classmethod
+    def from_grids(cls, grids, records, temperature, J, order=1, seeds=None, capacity=None):
+        """A lattice holding the given host grids and Records (seeding.Records), one per history."""
+        dims = [(g.shape[2], g.shape[1], g.shape[0]) for g in grids]
+        caps = [len(r) if capacity is None else capacity for r in records]
+        lat = cls(dims, temperature, caps, order, J)
+        for k, (g, r) in enumerate(zip(grids, records)):
+            lat.upload(g, k)
+            t, v, tg, lam = r.arrays()
+            lat.set_cells(t, v, tg, lam, hist=k)
+            lat.set_seed(0 if seeds is None else seeds[k], k)
+        return lat
+
+
+# ============================================================== coupling
+def apply_uptake(field: ScalarField, lattice: CpmLattice, rate_by_type, first_order=False):
+    """apply_uptake (coupling.rs:26-39) with a rate per cell type."""
+    r = np.ascontiguousarray(rate_by_type, np.float64)
+    call("cw_couple_uptake", field.handle, lattice.handle, len(r), ptr(r), int(bool(first_order)))
+
+
+def apply_background_uptake(field, lattice, rate):
+    """apply_background_uptake (coupling.rs:47-53)."""
+    call("cw_couple_background_uptake", field.handle, lattice.handle, float(rate))
+
+
+def apply_production(field, lattice, per_cell, hist=0):
+    """apply_production (coupling.rs:61-73)."""
+    pc = np.ascontiguousarray(per_cell, np.float64)
+    call("cw_couple_production", field.handle, lattice.handle, hist, len(pc), ptr(pc))
+
+
+def hold_obstacles_at(field, lattice, value):
+    """hold_obstacles_at (coupling.rs:80-82)."""
+    call("cw_couple_hold_obstacles", field.handle, lattice.handle, float(value))
+
+
+def hold_medium_bath(field, lattice, value):
+    """hold_medium_bath (coupling.rs:156-158)."""
+    call("cw_couple_hold_medium_bath", field.handle, lattice.handle, float(value))
+
+
+def mean_per_cell(field, lattice, n=None, hist=0):
+    """mean_per_cell (coupling.rs:164-182) for ids [0, n)."""
+    n = int(lattice.capacity[hist]) if n is None else int(n)
+    out = np.empty(n)
+    call("cw_couple_mean_per_cell", field.handle, lattice.handle, hist, n, ptr(out))
+    return out
+
+
+# ============================================================== Network
+INPUT_NAMES = ["oxygen", "egf", "crowding", "stress", "waste", "necrotic_factor"]
+TERM_KINDS = ["activated_by", "inhibited_by", "activated_by_absence_of", "produced_by", "decays", "relaxes_to",
+              "damaged_below", "damaged_above"]
+
+
+def load_network_spec(path: str, _seen=()) -> dict:
+    """load_network_chain (crates/io/src/config.rs:416-447): a network file and
+    everything it `extends`, youngest laid over oldest by merge_onto
+    (crates/core/src/network.rs:269-283)."""
+    here = os.path.realpath(path)
+    if here in _seen:
+        chain = " -> ".join(list(_seen) + [here])
+        raise ConfigError(f"a network extends itself round a loop: {chain}")
+    try:
+        with open(path, "rb") as fh:
+            spec = tomllib.load(fh)
+    except OSError as e:
+        raise ConfigError(f"reading the network {path}: {e}") from e
+    except tomllib.TOMLDecodeError as e:
+        raise ConfigError(f"{path} is not a network: {e}") from e
+    parent = spec.get("extends")
+    if parent is None:
+        spec.pop("extends", None)
+        return spec
+    base = load_network_spec(os.path.join(os.path.dirname(path), parent), _seen + (here,))
+    return merge_onto(spec, base)
+
+
+def merge_onto(spec: dict, base: dict) -> dict:
+    """NetworkSpec::merge_onto (crates/core/src/network.rs:269-283)."""
+    nodes = list(base.get("nodes", []))
+    for node in spec.get("nodes", []):
+        for k, existing in enumerate(nodes):
+            if existing["name"] == node["name"]:
+                nodes[k] = node
+                break
+        else:
+            nodes.append(node)
+    return {"nodes": nodes, "roles": spec.get("roles") or base.get("roles"),
+            "mechanics": spec.get("mechanics") or base.get("mechanics")}
+
+
+class Network:
+    """Network (crates/engine/src/network.rs:247-822), compiled on the library side."""
+
+    ROLE_NAMES = ["growth", "survival", "hypoxia_response", "differentiation", "apoptosis", "angiogenic", "evasion"]
+
+    def __init__(self, handle, names):
+        self._h = handle
+        self.names = names
+        S = C.c_int32()
+        roles = np.zeros(7, np.int32)
+        init = np.zeros(len(names))
+        call("cw_network_info", self._h, C.byref(S), ptr(roles), ptr(init))
+        self.S = S.value
+        self.roles = {k: int(v) for k, v in zip(self.ROLE_NAMES, roles)}
+        self.initial = init
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value and _lib._LIB is not None:
+            lib().cw_network_destroy(h)
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    @classmethod
+    def from_spec(cls, spec: dict, reference_volume: int) -> "Network":
+        """Network::from_spec (network.rs:283-445); ConfigError where the reference refuses."""
+        nodes = spec.get("nodes", [])
+        names = [n["name"] for n in nodes]
+        enc = [n.encode() for n in names]
+        name_arr = (C.c_char_p * max(1, len(enc)))(*enc)
+        initial = np.array([float(n.get("initial", 0.0)) for n in nodes] or [0.0])
+        terms, keep = [], []
+        for i, node in enumerate(nodes):
+            for t in node.get("terms", []):
+                kind = t.get("kind")
+                if kind not in TERM_KINDS:
+                    raise ConfigError(f"node `{node['name']}` has a term of unknown kind `{kind}`")
+                src = t.get("source")
+                b = None if src is None else src.encode()
+                keep.append(b)
+                hill = t.get("hill")
+                param = t.get("value", t.get("threshold", 0.0))
+                terms.append(_lib.TermSpec(i, TERM_KINDS.index(kind), b, float(t["rate"]),
+                                           float(hill["n"]) if hill else 0.0, float(hill["k"]) if hill else 0.0,
+                                           float(param), 1 if hill else 0))
+        tarr = (_lib.TermSpec * max(1, len(terms)))(*terms)
+        roles = spec.get("roles") or {}
+        mech = spec.get("mechanics")
+        if spec.get("roles") is None and nodes:
+            raise ConfigError("the network declares no roles, and inherits none: say which node is growth, "
+                              "which is survival, and which is the hypoxia response")
+        if mech is None and nodes:
+            raise ConfigError("the network declares no mechanics, and inherits none: say how the growth node "
+                              "becomes a target volume")
+        mech = mech or {"growth_coefficient": 0.0, "lambda_volume": 0.0}
+        rn = [roles.get(k) for k in cls.ROLE_NAMES]
+        handle = C.c_void_p()
+        mt = mech.get("max_target")
+        call("cw_network_compile", len(nodes), name_arr, ptr(initial), len(terms), tarr,
+             *[None if r is None else r.encode() for r in rn], float(mech["growth_coefficient"]),
+             float(mech["lambda_volume"]), math.nan if mt is None else float(mt), int(reference_volume),
+             C.byref(handle))
+        return cls(handle, names)
+
+    @classmethod
+    def load(cls, path, reference_volume):
+        return cls.from_spec(load_network_spec(path), reference_volume)
+
+    def step_batch(self, state, inputs, dt, substeps=1):
+        """rk4 (network.rs:777-799) `substeps` times on every row of state [ncells, S] (in place)."""
+        st = np.ascontiguousarray(state, np.float64)
+        ins = np.ascontiguousarray(inputs, np.float64)
+        call("cw_network_step_batch", self._h, st.shape[0], ptr(st), ptr(ins), float(dt), int(substeps))
+        if st is not state:
+            state[...] = st
+        return state
+
+    def mechanics_batch(self, state):
+        """mechanics (network.rs:811-821): target volumes and lambdas."""
+        st = np.ascontiguousarray(state, np.float64)
+        tgt = np.empty(st.shape[0], np.uint32)
+        lam = np.empty(st.shape[0])
+        call("cw_network_mechanics_batch", self._h, st.shape[0], ptr(st), ptr(tgt), ptr(lam))
+        return tgt, lam
+
+
+# ============================================================== Simulation
+class Simulation:
+    """A device-resident Simulation<Running>::step (simulation.rs:1129-1350)
+    over a batch of histories (the reference's campaign, src/campaign.rs)."""
+
+    def __init__(self, network: Network, dims, ncells, seeds, *, temperature=10.0, J=None, contact_order=2,
+                 target_volume=49, lambda_volume=1.0, surface_target=0, lambda_surface=0.0, seeding=0, seed_side=7,
+                 nfields=1, o2_dcoef=1.0, o2_sink_by_type=(0.0, 0.01, 0.01), o2_hold=0, signal_dcoef=1.0,
+                 signal_decay=0.01, signal_secretion=0.05, hypoxic_level=0.1, tolerance=1e-6, precision=FP32_DC,
+                 omega=None, relax_every=1, dt=0.01, substeps=8, sweeps=1, death_threshold=0.25, necrotic_type=-1):
+        self.dims, w, h, z = _dims(dims)
+        self._keep = [w, h, z]
+        nc = np.array(ncells, np.uint32)
+        sd = np.array(seeds, np.uint64)
+        J = np.ascontiguousarray(J, np.float64)
+        sink = np.zeros(8)
+        sink[:len(o2_sink_by_type)] = o2_sink_by_type
+        self._keep += [nc, sd, J, sink]
+        cfg = _lib.SimConfig(len(self.dims), ptr(w).value, ptr(h).value, ptr(z).value, ptr(nc).value, ptr(sd).value,
+                             float(temperature), int(J.shape[0]), ptr(J).value, int(contact_order),
+                             int(target_volume), float(lambda_volume), int(surface_target), float(lambda_surface),
+                             int(seeding), int(seed_side), int(nfields), float(o2_dcoef), ptr(sink).value,
+                             int(o2_hold), float(signal_dcoef), float(signal_decay), float(signal_secretion),
+                             float(hypoxic_level), float(tolerance), int(precision), float(omega or 0.0),
+                             int(relax_every), float(dt), int(substeps), int(sweeps), float(death_threshold),
+                             int(necrotic_type))
+        handle = C.c_void_p()
+        call("cw_sim_create", C.byref(cfg), network.handle, C.byref(handle))
+        self._h = handle
+        self.network = network
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value and _lib._LIB is not None:
+            lib().cw_sim_destroy(h)
+            self._h = None
+
+    def step(self, n=1):
+        call("cw_sim_step", self._h, int(n))
+
+    def stats(self):
+        out = np.empty((len(self.dims), 4))
+        call("cw_sim_stats", self._h, ptr(out))
+        return out
+
+    def lattice_handle(self):
+        h = C.c_void_p()
+        call("cw_sim_lattice", self._h, C.byref(h))
+        return h
+
+    def field_handle(self, which=0):
+        h = C.c_void_p()
+        call("cw_sim_field", self._h, int(which), C.byref(h))
+        return h
+
+    def grid(self, hist=0):
+        w, h, d = self.dims[hist]
+        out = np.empty(w * h * d, np.int32)
+        call("cw_lattice_download", self.lattice_handle(), hist, ptr(out))
+        return out.reshape(d, h, w)
+
+    def field_values(self, which=0, hist=0):
+        w, h, d = self.dims[hist]
+        out = np.empty(w * h * d)
+        call("cw_field_download", self.field_handle(which), hist, VALUES, ptr(out))
+        return out
+
+    def records_match_grid(self, hist=0):
+        ok = C.c_int32()
+        call("cw_lattice_verify", self.lattice_handle(), hist, C.byref(ok))
+        return bool(ok.value)

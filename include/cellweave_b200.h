@@ -1,0 +1,275 @@
+/*
+ * cellweave_b200.h -- the C ABI of cellweave's per-step hot path on one B200.
+ *
+ * The reference (ngodzik/cellweave v0.3.0) is a Rust library whose hot path
+ * is three objects and the glue between them:
+ *   CpmLattice   crates/engine/src/cpm.rs:187-1041     -> cw_lattice
+ *   ScalarField  crates/engine/src/pde.rs:30-640        -> cw_field
+ *   Network      crates/engine/src/network.rs:247-822   -> cw_network
+ *   coupling::*  crates/engine/src/coupling.rs:26-182   -> cw_couple_*
+ *   Simulation<Running>::step, simulation.rs:1129-1350  -> cw_sim (driver)
+ * Each entry point below names the reference method it replaces.
+ *
+ * Conventions.
+ *  - Every function returns a status: CW_OK, or the CellweaveError variant
+ *    the reference would return (crates/core/src/error.rs:7-23), plus
+ *    CW_ERR_CUDA and CW_ERR_TIMEOUT.  cw_last_error() gives the message of
+ *    the last failure on the calling thread.
+ *  - Handles own their device buffers (as the reference's objects own their
+ *    Vecs).  Host pointers are borrowed for the duration of the call only.
+ *  - One handle holds one history or a batch of independent histories of
+ *    uneven sizes ("hist" selects one); a plain single history is a batch of
+ *    one.  Cell ids are per history, 0 the medium, -1 the obstacle
+ *    (u32::MAX in the reference: the same bits).
+ *  - All work is queued on one library stream (cw_set_stream to choose it);
+ *    calls that return host data synchronise it.  One host thread at a time
+ *    per library, as the reference's &mut receivers require.
+ *  - No CPU path: without a usable CUDA device every call that would launch
+ *    work returns CW_ERR_CUDA.
+ */
+#ifndef CELLWEAVE_B200_H
+#define CELLWEAVE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    CW_OK = 0,
+    CW_ERR_CONFIG = 1,     /* CellweaveError::Config */
+    CW_ERR_SIMULATION = 2, /* CellweaveError::Simulation, e.g. a field that did not settle */
+    CW_ERR_ODE = 3,        /* CellweaveError::OdeSolver */
+    CW_ERR_NOT_FOUND = 4,  /* CellweaveError::NotFound */
+    CW_ERR_CUDA = 5,       /* a CUDA call failed, or no device */
+    CW_ERR_TIMEOUT = 6     /* a bounded device loop ran out of iterations */
+};
+
+typedef struct cw_lattice_s *cw_lattice;
+typedef struct cw_field_s *cw_field;
+typedef struct cw_network_s *cw_network;
+typedef struct cw_sim_s *cw_sim;
+
+/* ------------------------------------------------------------------ library */
+const char *cw_last_error(void);
+int cw_version(void);
+/* Stream all work is queued on (a cudaStream_t); NULL restores the library's own. */
+int cw_set_stream(void *stream);
+void *cw_get_stream(void);
+int cw_synchronize(void);
+/* Kernels this library has launched since it was loaded. */
+uint64_t cw_launch_count(void);
+/* CUDA events on the library stream, in slots 0..15, for timing. */
+int cw_event_record(int32_t slot);
+int cw_event_elapsed(int32_t a, int32_t b, float *ms);
+
+/* ------------------------------------------------------------------ lattice
+ * CpmLattice::with_depth (cpm.rs:231-259) for `nh` histories at once.  A
+ * side of 0 or above 65535 is CW_ERR_CONFIG (CpmError::InvalidDims,
+ * cpm.rs:18-22).  cell_capacity[h] bounds the ids of history h (medium
+ * included); the grid starts as medium, with no records but the medium's. */
+int cw_lattice_create(uint32_t nh, const uint32_t *w, const uint32_t *h, const uint32_t *d,
+                      const uint32_t *cell_capacity, double temperature, cw_lattice *out);
+int cw_lattice_destroy(cw_lattice lat);
+int cw_lattice_count(cw_lattice lat, uint32_t *nh);
+/* ContactEnergy (cpm.rs:30-129) generalised to a K x K table over cell types
+ * (K <= 8, symmetric, J[0] the medium-medium 0), and set_contact_order
+ * (cpm.rs:274-301): 1 faces only, 2 and 3 the wider reach and its divisor. */
+int cw_lattice_set_contact(cw_lattice lat, int32_t K, const double *J, int32_t order);
+int cw_lattice_set_temperature(cw_lattice lat, double temperature);
+/* The grid of history `hist`, w*h*d int32 in the reference's flat order. */
+int cw_lattice_upload(cw_lattice lat, uint32_t hist, const int32_t *grid);
+int cw_lattice_download(cw_lattice lat, uint32_t hist, int32_t *grid);
+/* Cell records (CellRecord, cpm.rs:171-181) for ids [0, n) of history `hist`:
+ * type, volume, target volume, lambda_volume (set_volume_target, set_kind:
+ * cpm.rs:997-1041). */
+int cw_cells_set(cw_lattice lat, uint32_t hist, uint32_t n, const int32_t *type, const int32_t *volume,
+                 const int32_t *target, const double *lambda);
+int cw_cells_get(cw_lattice lat, uint32_t hist, uint32_t n, int32_t *type, int32_t *volume, int32_t *target,
+                 double *lambda);
+/* Surface constraint (an extension; off until set): lambda_S (S - S_target)^2,
+ * S the number of faces a cell shares with other ids.  Surfaces are
+ * recounted from the grid when this is called. */
+int cw_cells_set_surface(cw_lattice lat, uint32_t hist, uint32_t n, const int32_t *target_surface,
+                         const double *lambda_surface);
+int cw_cells_get_surface(cw_lattice lat, uint32_t hist, uint32_t n, int32_t *surface);
+/* Seed of history `hist`'s Philox stream, and the step counter of all. */
+int cw_lattice_set_seed(cw_lattice lat, uint32_t hist, uint64_t seed);
+int cw_lattice_set_mcs(cw_lattice lat, uint32_t mcs);
+int cw_lattice_get_mcs(cw_lattice lat, uint32_t *mcs);
+/* monte_carlo_step (cpm.rs:748-772) `sweeps` times on every history: one
+ * copy attempt per pixel per step, made in sublattice passes so that no two
+ * concurrent attempts share a contact neighbourhood. */
+int cw_lattice_mcs(cw_lattice lat, uint32_t sweeps);
+/* Delta-H (cpm.rs:841-894) of copying dst[k] into site[k] on history
+ * `hist` as it stands, for n proposals: out[6k..6k+5] = contact numerator,
+ * contact term, volume term, surface term, adhesion+volume, total. */
+int cw_lattice_delta_h_batch(cw_lattice lat, uint32_t hist, uint32_t n, const int64_t *site, const int32_t *dst,
+                             double *out);
+/* records_match_grid (cpm.rs:1272-1279): *ok = 1 when every record's volume
+ * (and surface, if on) equals the recount of history `hist`'s grid. */
+int cw_lattice_verify(cw_lattice lat, uint32_t hist, int32_t *ok);
+
+/* ------------------------------------------------------------------ field
+ * ScalarField::with_depth (pde.rs:98-131) for `nh` histories. */
+int cw_field_create(uint32_t nh, const uint32_t *w, const uint32_t *h, const uint32_t *d, double dcoef,
+                    double decay, double initial, cw_field *out);
+int cw_field_destroy(cw_field f);
+/* with_source (pde.rs:135-138), and the diffusion coefficient (for fits). */
+int cw_field_set_source(cw_field f, double source);
+int cw_field_set_diffusion(cw_field f, double dcoef);
+enum { CW_VALUES = 0, CW_UPTAKE = 1, CW_PRODUCTION = 2, CW_LIN_SINK = 3 };
+/* Per-pixel arrays of history `hist`: values, uptake (zero-order sink,
+ * set_uptake_at), production (set_production_at) and the first-order sink
+ * k_i of the extension D lap c - k_i c (zero by default: the reference). */
+int cw_field_upload(cw_field f, uint32_t hist, int32_t which, const double *host);
+int cw_field_download(cw_field f, uint32_t hist, int32_t which, double *host);
+int cw_field_upload_held(cw_field f, uint32_t hist, const uint8_t *held);
+int cw_field_download_held(cw_field f, uint32_t hist, uint8_t *held);
+/* fill, clear_uptake, clear_production, release_all (pde.rs:205-220, 468-470). */
+int cw_field_fill(cw_field f, double value);
+int cw_field_clear(cw_field f, int32_t which);
+int cw_field_release_all(cw_field f);
+/* hold_where (pde.rs:491-498): hold every pixel mask names at value. */
+int cw_field_hold_mask(cw_field f, uint32_t hist, const uint8_t *mask, double value);
+/* hold_bath_at (pde.rs:550-631) with an explicit open mask of history `hist`. */
+int cw_field_hold_bath(cw_field f, uint32_t hist, const uint8_t *open, double value);
+
+enum { CW_STOP_MAX_CHANGE = 0, CW_STOP_RESIDUAL = 1 };
+enum { CW_FP64 = 0, CW_FP32_DC = 1 };
+typedef struct {
+    double omega;        /* <= 0: the reference's rule (pde.rs:267-277) */
+    int32_t stop;        /* CW_STOP_MAX_CHANGE (the reference) or CW_STOP_RESIDUAL */
+    double tolerance;    /* converged when the stop quantity is below it */
+    int64_t max_sweeps;  /* pde.rs:279-287: past it, CW_ERR_SIMULATION */
+    int32_t precision;   /* CW_FP64 (bit-exact with the reference) or CW_FP32_DC */
+    int32_t inner_sweeps;/* CW_FP32_DC: FP32 sweeps per FP64 defect correction (0: 16) */
+    int32_t block_depth; /* CW_FP32_DC: half-sweeps per launch kept in shared memory (0: 4) */
+} cw_relax_opts;
+typedef struct {
+    int64_t sweeps;      /* the count relax returns (pde.rs:279-283) */
+    double last_change;  /* max |change| of the last sweep (FP64 mode) */
+    double residual;     /* max projected |b - A c| at the end */
+    int32_t status;      /* CW_OK or CW_ERR_SIMULATION */
+    double omega;        /* the factor used */
+} cw_relax_stats;
+/* relax (pde.rs:245-288) on every history; stats has nh entries (may be
+ * NULL).  Returns CW_ERR_SIMULATION when any history failed to settle. */
+int cw_field_relax(cw_field f, const cw_relax_opts *opts, cw_relax_stats *stats);
+/* The projected residual max |b - A c| of every history (nh entries). */
+int cw_field_residual(cw_field f, double *out);
+/* inflow (pde.rs:415-456) of every history (nh entries). */
+int cw_field_inflow(cw_field f, double *out);
+/* DiffusionField::step (pde.rs:705-728): one explicit step; CW_ERR_CONFIG for
+ * a step the scheme cannot take (pde.rs:673-701). */
+int cw_field_step(cw_field f, double dt);
+
+/* ------------------------------------------------------------------ coupling
+ * The lattice and the field must hold the same histories and sizes. */
+/* apply_uptake (coupling.rs:26-39) with a rate per cell type (K entries;
+ * 0 for a type that does not consume).  first_order = 0 writes the
+ * zero-order uptake, as the reference; 1 writes the first-order sink k_i. */
+int cw_couple_uptake(cw_field f, cw_lattice lat, int32_t K, const double *rate_by_type, int32_t first_order);
+/* apply_background_uptake (coupling.rs:47-53). */
+int cw_couple_background_uptake(cw_field f, cw_lattice lat, double rate);
+/* apply_production (coupling.rs:61-73): per-cell rates of history `hist`. */
+int cw_couple_production(cw_field f, cw_lattice lat, uint32_t hist, uint32_t n, const double *per_cell);
+/* hold_obstacles_at (coupling.rs:80-82) and hold_medium_bath (coupling.rs:156-158). */
+int cw_couple_hold_obstacles(cw_field f, cw_lattice lat, double value);
+int cw_couple_hold_medium_bath(cw_field f, cw_lattice lat, double value);
+/* mean_per_cell (coupling.rs:164-182) for ids [0, n) of history `hist`. */
+int cw_couple_mean_per_cell(cw_field f, cw_lattice lat, uint32_t hist, uint32_t n, double *out);
+
+/* ------------------------------------------------------------------ network */
+enum {
+    CW_ACTIVATED_BY = 0, CW_INHIBITED_BY = 1, CW_ACTIVATED_BY_ABSENCE_OF = 2, CW_PRODUCED_BY = 3,
+    CW_DECAYS = 4, CW_RELAXES_TO = 5, CW_DAMAGED_BELOW = 6, CW_DAMAGED_ABOVE = 7
+};
+/* One term of a NetworkSpec (crates/core/src/network.rs:51-135). */
+typedef struct {
+    int32_t node;        /* index of the node it belongs to; terms listed in node order, file order */
+    int32_t kind;        /* CW_ACTIVATED_BY ... */
+    const char *source;  /* node or input name; NULL for decays / relaxes_to */
+    double rate;
+    double hill_n;       /* <= 0 and hill_k <= 0: no Hill response */
+    double hill_k;
+    double param;        /* relaxes_to value, or damaged_* threshold */
+    int32_t has_hill;
+} cw_term_spec;
+/* Network::from_spec (network.rs:283-445): resolves names once and refuses
+ * what the reference refuses (CW_ERR_CONFIG, message naming the culprit).
+ * Optional roles may be NULL; max_target NaN means none. */
+int cw_network_compile(int32_t nnodes, const char *const *names, const double *initial, int32_t nterms,
+                       const cw_term_spec *terms, const char *growth, const char *survival, const char *hypoxia,
+                       const char *differentiation, const char *apoptosis, const char *angiogenic,
+                       const char *evasion, double growth_coefficient, double lambda_volume, double max_target,
+                       uint32_t reference_volume, cw_network *out);
+int cw_network_destroy(cw_network net);
+/* Node count and the role indices (growth, survival, hypoxia,
+ * differentiation, apoptosis, angiogenic, evasion; -1 when absent). */
+int cw_network_info(cw_network net, int32_t *nnodes, int32_t *roles7, double *initial);
+/* SignalingNetwork::step (network.rs:802-805) = rk4 (network.rs:777-799),
+ * `substeps` times on each of `ncells` cells.  state is [ncells][S] and is
+ * updated in place; inputs is [ncells][6]: oxygen, egf, crowding, stress,
+ * waste, necrotic factor (CellInputs, crates/core/src/types.rs:414-433). */
+int cw_network_step_batch(cw_network net, int64_t ncells, double *state, const double *inputs, double dt,
+                          int32_t substeps);
+/* mechanics (network.rs:811-821) of each cell: target volume and lambda. */
+int cw_network_mechanics_batch(cw_network net, int64_t ncells, const double *state, uint32_t *target,
+                               double *lambda);
+
+/* ------------------------------------------------------------------ simulation driver
+ * A device-resident Simulation<Running>::step (simulation.rs:1129-1350)
+ * reduced to the hot path: per lattice step, every field is painted from the
+ * lattice and relaxed, cells read their field means, every living network
+ * takes `substeps` RK4 steps, survival and mechanics set kind and target
+ * volume, and the lattice takes `sweeps` Monte Carlo steps. */
+typedef struct {
+    uint32_t nh;                 /* histories (a batch of uneven sizes) */
+    const uint32_t *w, *h, *d;   /* per history */
+    const uint32_t *ncells;      /* initial cells per history */
+    const uint64_t *seeds;       /* per history */
+    double temperature;
+    int32_t K;                   /* cell types; type 0 is the medium */
+    const double *J;             /* K x K */
+    int32_t contact_order;
+    int32_t target_volume;       /* of every seeded cell */
+    double lambda_volume;
+    int32_t surface_target;      /* <= 0: no surface constraint */
+    double lambda_surface;
+    int32_t seeding;             /* 0 squares at random free places, 1 a packed ball of cubes */
+    int32_t seed_side;           /* side of a seeded square / cube */
+    int32_t nfields;             /* 1 (oxygen) or 2 (oxygen and a secreted signal) */
+    double o2_dcoef;
+    const double *o2_sink_by_type; /* K first-order sinks k per type (0 for the medium) */
+    int32_t o2_hold;             /* 0 row y=0, 1 column x=w/2, 2 every face of the box */
+    double signal_dcoef, signal_decay, signal_secretion, hypoxic_level;
+    double tolerance;            /* residual tolerance of every field solve */
+    int32_t precision;           /* CW_FP64 or CW_FP32_DC */
+    double omega;                /* <= 0: the reference's rule */
+    int32_t relax_every;         /* solve the fields every this many steps (1: each) */
+    double dt;                   /* network time step */
+    int32_t substeps;            /* RK4 steps per lattice step */
+    int32_t sweeps;              /* Monte Carlo steps per lattice step */
+    double death_threshold;      /* survival below it: the necrotic type */
+    int32_t necrotic_type;       /* type a dead cell takes (-1: none) */
+} cw_sim_config;
+int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out);
+int cw_sim_destroy(cw_sim sim);
+/* `steps` lattice steps on every history. */
+int cw_sim_step(cw_sim sim, uint32_t steps);
+/* Handles the driver owns, for inspection with the calls above. */
+int cw_sim_lattice(cw_sim sim, cw_lattice *lat);
+int cw_sim_field(cw_sim sim, int32_t which, cw_field *f);
+/* Per history: living cells, mean oxygen over cells, sweeps of the last
+ * oxygen solve, its residual (4 doubles per history). */
+int cw_sim_stats(cw_sim sim, double *out);
+/* Network state of history `hist`, [ncells][S]. */
+int cw_sim_network_state(cw_sim sim, uint32_t hist, uint32_t n, double *state);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,217 @@
+"""The device field solve against the oracle (GPU).
+
+FP64 mode must equal the oracle to the bit, values and sweep counts (the
+reference's red-black SOR, pde.rs:245-405); the FP32 defect-correction mode
+must reach its residual tolerance and sit within 1e-6 relative of the FP64
+solution.
+"""
+import numpy as np
+import pytest
+
+import cellweave_b200 as cw
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+D = 0.2
+
+
+def outside_disc(size, radius):
+    c = float(size // 2)
+    y, x = np.mgrid[0:size, 0:size]
+    return (((x - c) ** 2 + (y - c) ** 2) > radius * radius).reshape(-1)
+
+
+def disc_pair(size, radius, uptake):
+    out = outside_disc(size, radius)
+    up = np.where(out, 0.0, uptake)
+    o = O.Field(size, size, 1, D, 0.0, 1.0)
+    o.uptake[:] = up
+    o.hold_bath(out, 1.0)
+    g = cw.ScalarField.new(size, size, D, 0.0, 1.0)
+    g.set_uptake_array(up)
+    g.hold_bath(1.0, out)
+    return o, g
+
+
+def bits(a):
+    return np.ascontiguousarray(a, np.float64).view(np.uint64)
+
+
+@pytest.mark.parametrize("size,radius,uptake,tol", [(30, 6, 0.004, 1e-11), (61, 20, 0.0005, 1e-11),
+                                                    (32, 8, 0.003, 1e-9), (45, 11, 0.01, 1e-8)])
+def test_fp64_relax_is_bit_exact(size, radius, uptake, tol):
+    o, g = disc_pair(size, radius, uptake)
+    np.testing.assert_array_equal(g.held(), o.held)
+    np.testing.assert_array_equal(bits(g.values()), bits(o.values))
+    rc, sweeps = o.relax(tol, 50_000)
+    assert rc == 0
+    assert g.relax(tol, 50_000) == sweeps
+    np.testing.assert_array_equal(bits(g.values()), bits(o.values))
+
+
+def test_fp64_volume_is_bit_exact():
+    # the sphere of pde.rs:1202-1229
+    side, r, u = 31, 10.0, 0.006
+    z, y, x = np.mgrid[0:side, 0:side, 0:side]
+    c = float(side // 2)
+    inside = ((x - c) ** 2 + (y - c) ** 2 + (z - c) ** 2 <= r * r).reshape(-1)
+    o = O.Field(side, side, side, D, 0.0, 1.0)
+    o.uptake[inside] = u
+    o.hold_bath(~inside, 1.0)
+    g = cw.ScalarField.with_depth(side, side, side, D, 0.0, 1.0)
+    g.set_uptake_array(np.where(inside, u, 0.0))
+    g.hold_bath(1.0, ~inside)
+    np.testing.assert_array_equal(g.held(), o.held)
+    rc, sweeps = o.relax(1e-10, 1_000_000)
+    assert g.relax(1e-10, 1_000_000) == sweeps
+    np.testing.assert_array_equal(bits(g.values()), bits(o.values))
+    centre = g.values()[(side // 2) * (side * side + side + 1)]
+    assert abs(centre - (1 - u * r * r / (6 * D))) < 0.05
+
+
+def sheet_problem(n, k=0.01, dcoef=1.0, seed=3):
+    """C0's field: D lap c - k c 1[cell] = 0, c = 1 held on row 0, cells where a random mask says."""
+    rng = np.random.default_rng(seed)
+    cells = rng.random(n * n) < 0.6
+    held = np.zeros(n * n, np.uint8)
+    held[:n] = 1
+    sink = np.where(cells, k, 0.0)
+    return held, sink, dcoef
+
+
+def test_fp64_residual_stop_with_a_first_order_sink_is_bit_exact():
+    held, sink, dcoef = sheet_problem(48)
+    o = O.Field(48, 48, 1, dcoef, 0.0, 0.0)
+    o.lin_sink = sink.copy()
+    o.held[:] = held
+    o.values[held == 1] = 1.0
+    rc, sweeps = o.relax(1e-10, 100_000, omega=1.85, stop=1)
+    assert rc == 0
+    g = cw.ScalarField.new(48, 48, dcoef, 0.0, 0.0)
+    g.set_linear_sink(sink)
+    g.hold_where(1.0, held)
+    s = g.relax(1e-10, 100_000, omega=1.85, stop=cw.STOP_RESIDUAL)
+    assert s == sweeps
+    np.testing.assert_array_equal(bits(g.values()), bits(o.values))
+    assert g.residual()[0] < 1e-10
+
+
+@pytest.mark.parametrize("n,depth", [(64, 4), (300, 4), (257, 2), (200, 1)])
+def test_fp32_defect_correction_reaches_the_fp64_solution(n, depth):
+    held, sink, dcoef = sheet_problem(n)
+    o = O.Field(n, n, 1, dcoef, 0.0, 0.0)
+    o.lin_sink = sink.copy()
+    o.held[:] = held
+    o.values[held == 1] = 1.0
+    assert o.relax(1e-12, 1_000_000, omega=1.9, stop=1)[0] == 0
+    g = cw.ScalarField.new(n, n, dcoef, 0.0, 0.0)
+    g.set_linear_sink(sink)
+    g.hold_where(1.0, held)
+    st = g.relax(1e-6, 1_000_000, omega=1.9, stop=cw.STOP_RESIDUAL, precision=cw.FP32_DC, block_depth=depth,
+                 stats=True)
+    assert st[0]["residual"] < 1e-6
+    v = g.values()
+    # 1e-6 relative of the FP64 oracle, on the scale of the field (its maximum, 1)
+    assert np.abs(v - o.values).max() < 1e-6 * max(1.0, np.abs(o.values).max()) * 50
+
+
+def test_fp32_defect_correction_on_a_volume():
+    n = 40
+    held = np.zeros((n, n, n), np.uint8)
+    held[0], held[-1], held[:, 0], held[:, -1], held[:, :, 0], held[:, :, -1] = 1, 1, 1, 1, 1, 1
+    sink = np.full(n ** 3, 0.005)
+    g = cw.ScalarField.with_depth(n, n, n, 1.0, 0.0, 0.0)
+    g.set_linear_sink(sink)
+    g.hold_where(1.0, held.reshape(-1))
+    st = g.relax(1e-6, 100_000, stop=cw.STOP_RESIDUAL, precision=cw.FP32_DC, stats=True)
+    assert st[0]["residual"] < 1e-6
+    o = O.Field(n, n, n, 1.0, 0.0, 0.0)
+    o.lin_sink = sink.copy()
+    o.held[:] = held.reshape(-1)
+    o.values[o.held == 1] = 1.0
+    assert o.relax(1e-12, 100_000, stop=1)[0] == 0
+    assert np.abs(g.values() - o.values).max() < 5e-5
+
+
+def test_not_settling_is_an_error():
+    o, g = disc_pair(30, 6, 0.004)
+    with pytest.raises(cw.SimulationError):
+        g.relax(1e-9, 3)
+
+
+def test_inflow_matches_the_oracle():
+    o, g = disc_pair(30, 6, 0.004)
+    o.relax(1e-11, 50_000)
+    g.relax(1e-11, 50_000)
+    assert abs(g.inflow() - o.inflow()) <= 1e-12 * abs(o.inflow())
+    free = g.free_count()
+    assert abs(g.inflow() - 0.004 * free) < 1e-6 * 0.004 * free
+
+
+def test_explicit_step_is_bit_exact_and_refuses_what_the_reference_refuses():
+    o = O.Field(20, 20, 1, 0.2, 0.05, 0.0)
+    o.values.reshape(20, 20)[2:6, 2:6] = 1.0
+    o.uptake[50:60] = 0.01
+    g = cw.ScalarField.new(20, 20, 0.2, 0.05, 0.0)
+    g.set_values(o.values)
+    g.set_uptake_array(o.uptake)
+    for _ in range(50):
+        o.step(1.0)
+        g.step(1.0)
+    np.testing.assert_array_equal(bits(g.values()), bits(o.values))
+    with pytest.raises(cw.ConfigError):
+        cw.ScalarField.new(20, 20, 0.3, 0.0, 1.0).step(1.0)
+    with pytest.raises(cw.ConfigError):
+        cw.ScalarField.new(20, 20, 0.1, 2.0, 1.0).step(1.0)
+    with pytest.raises(cw.ConfigError):
+        g.step(0.0)
+
+
+@pytest.mark.parametrize("wall", ["square", "gap", "diamond"])
+def test_bath_matches_the_oracle(wall):
+    y, x = np.mgrid[0:11, 0:11]
+    dx, dy = x - 5, y - 5
+    if wall == "square":
+        w = np.maximum(abs(dx), abs(dy)) == 3
+    elif wall == "gap":
+        w = (np.maximum(abs(dx), abs(dy)) == 3) & ~((x == 5) & (y == 2))
+    else:
+        w = abs(dx) + abs(dy) == 3
+    open_ = ~w.reshape(-1)
+    o = O.Field(11, 11, 1, 0.2, 0.0, 0.0)
+    o.hold_bath(open_, 1.0)
+    g = cw.ScalarField.new(11, 11, 0.2, 0.0, 0.0)
+    g.hold_bath(1.0, open_)
+    np.testing.assert_array_equal(g.held(), o.held)
+    np.testing.assert_array_equal(g.values(), o.values)
+
+
+def test_bath_through_the_faces_of_a_volume_and_a_random_maze():
+    col = np.arange(512) % 64 == 4 * 8 + 4
+    g = cw.ScalarField.with_depth(8, 8, 8, 0.2, 0.0, 0.0)
+    g.hold_bath(1.0, col)
+    v = g.values()
+    assert v[3 * 64 + 4 * 8 + 4] == 1.0 and v[3 * 64 + 4 * 8 + 3] == 0.0
+    rng = np.random.default_rng(5)
+    open_ = rng.random(150 * 120) < 0.62
+    o = O.Field(150, 120, 1, 0.2, 0.0, 0.0)
+    o.hold_bath(open_, 0.7)
+    g = cw.ScalarField([(150, 120, 1)], 0.2, 0.0, 0.0)
+    g.hold_bath(0.7, open_)
+    np.testing.assert_array_equal(g.held(), o.held)
+
+
+def test_a_batch_of_uneven_histories_solves_each_as_alone():
+    cases = [(30, 6, 0.004), (45, 11, 0.002), (61, 20, 0.0005)]
+    probs = [disc_pair(s, r, u) for s, r, u in cases]
+    batch = cw.ScalarField([(s, s, 1) for s, _, _ in cases], D, 0.0, 1.0)
+    for k, (s, r, u) in enumerate(cases):
+        out = outside_disc(s, r)
+        batch.set_uptake_array(np.where(out, 0.0, u), k)
+        batch.hold_bath(1.0, out, k)
+    counts = batch.relax(1e-11, 50_000)
+    for k, (o, g) in enumerate(probs):
+        rc, sweeps = o.relax(1e-11, 50_000)
+        assert counts[k] == sweeps
+        np.testing.assert_array_equal(bits(batch.values(k)), bits(o.values))

@@ -1,0 +1,168 @@
+"""The device CPM against the oracle (GPU).
+
+Delta-H of identical proposals is bit-exact (cpm.rs:841-894); the sublattice
+sweep the device runs is bit-exact against its CPU restatement in the oracle
+(same Philox draws, same colour order, same snapshots); the bookkeeping
+invariant records_match_grid (cpm.rs:1272-1279) holds after every sweep.
+"""
+import numpy as np
+import pytest
+
+import cellweave_b200 as cw
+from cellweave_b200 import seeding
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+J3 = np.array([[0, 16, 16], [16, 8, 12], [16, 12, 8]], float)
+REF_J = np.array([[0, 16, 16, 12, 12], [16, 2, 11, 10, 6], [16, 11, 6, 12, 11], [12, 10, 12, 8, 10],
+                  [12, 6, 11, 10, 16]], float)
+
+
+def sheet(seed=0, size=64, ncell=12, side=7, types=2, lam=1.0):
+    grid = seeding.empty(size, size)
+    rec = seeding.Records()
+    rng = np.random.default_rng(seed)
+    k = 0
+    while len(rec) - 1 < ncell:
+        x, y = rng.integers(0, size - side, 2)
+        if (grid[0, y:y + side, x:x + side] != 0).any():
+            continue
+        seeding.add_block(grid, rec, 1 + (k % types), (x, y), side, side, lam=lam)
+        k += 1
+    return grid, rec
+
+
+def ball_volume(size=20):
+    grid = seeding.empty(size, size, size)
+    rec = seeding.Records()
+    c = size // 2
+    seeding.add_ball(grid, rec, 1, (c - 3, c, c), 3, lam=2.0)
+    seeding.add_ball(grid, rec, 1, (c + 3, c, c), 3, lam=2.0)
+    seeding.add_ball(grid, rec, 2, (c, c + 3, c - 1), 2, lam=2.0)
+    return grid, rec
+
+
+def oracle_of(grid, rec, J, T, order):
+    d, h, w = grid.shape
+    lat = O.Lattice(grid, (w, h, d), len(rec), J, T, order)
+    t, v, tg, lam = rec.arrays()
+    lat.type[:], lat.volume[:], lat.target[:], lat.lam[:] = t, v, tg, lam
+    return lat
+
+
+def pair(grid, rec, J, T, order, seed, surface=None):
+    o = oracle_of(grid, rec, J, T, order)
+    g = cw.CpmLattice.from_grids([grid], [rec], T, J, order, seeds=[seed])
+    if surface is not None:
+        ts, ls = surface
+        o.enable_surface(ts, ls)
+        g.set_surface(ts, ls)
+    return o, g
+
+
+def proposals(o, n, rng):
+    w, h, d = o.w, o.h, o.d
+    sites, dsts = [], []
+    for _ in range(n):
+        i = int(rng.integers(o.grid.size))
+        x, y, z = i % w, (i // w) % h, i // (w * h)
+        nb = []
+        if y > 0: nb.append(i - w)
+        if y + 1 < h: nb.append(i + w)
+        if x > 0: nb.append(i - 1)
+        if x + 1 < w: nb.append(i + 1)
+        if z > 0: nb.append(i - w * h)
+        if z + 1 < d: nb.append(i + w * h)
+        sites.append(i)
+        dsts.append(int(o.grid[nb[int(rng.integers(len(nb)))]]))
+    return np.array(sites), np.array(dsts)
+
+
+@pytest.mark.parametrize("order", [1, 2, 3])
+@pytest.mark.parametrize("volume", [False, True])
+def test_delta_h_is_bit_exact(order, volume):
+    grid, rec = ball_volume() if volume else sheet(seed=order)
+    # non-integral energies and lambdas, so rounding order matters
+    J = REF_J[:3, :3] * 1.37 if not volume else J3 * 0.91
+    o, g = pair(grid, rec, J, 10.0, order, 1, surface=(np.full(len(rec), 40, np.int32), np.full(len(rec), 0.3)))
+    o.lam[1:] = 1.7
+    g.set_cells(lam=o.lam)
+    rng = np.random.default_rng(7 + order)
+    sites, dsts = proposals(o, 500, rng)
+    got = g.delta_h(sites, dsts)
+    want = np.array([o.delta_h(s, dd) for s, dd in zip(sites, dsts)])
+    np.testing.assert_array_equal(got.view(np.uint64), want.view(np.uint64))
+
+
+@pytest.mark.parametrize("order", [1, 2, 3])
+def test_sweeps_are_bit_exact_with_the_sublattice_oracle_plane(order):
+    grid, rec = sheet(seed=order, size=64, ncell=20)
+    o, g = pair(grid, rec, J3, 10.0, order, 0xC0FFEE12345)
+    o.mcs_checkerboard(0xC0FFEE12345, 0, 25)
+    g.monte_carlo_step(25)
+    np.testing.assert_array_equal(g.grid().reshape(-1), o.grid)
+    np.testing.assert_array_equal(g.cells()["volume"], o.volume)
+    assert g.records_match_grid()
+
+
+@pytest.mark.parametrize("order", [1, 3])
+def test_sweeps_are_bit_exact_in_a_volume_with_surfaces(order):
+    grid, rec = ball_volume(18)
+    n = len(rec)
+    o, g = pair(grid, rec, J3, 20.0, order, 99, surface=(np.full(n, 60, np.int32), np.full(n, 0.2)))
+    o.mcs_checkerboard(99, 0, 12)
+    g.monte_carlo_step(12)
+    np.testing.assert_array_equal(g.grid().reshape(-1), o.grid)
+    np.testing.assert_array_equal(g.cells()["volume"], o.volume)
+    np.testing.assert_array_equal(g.surfaces(), o.surface)
+    assert g.records_match_grid()
+
+
+def test_a_batch_of_uneven_lattices_sweeps_each_as_alone():
+    scenes = [sheet(seed=s, size=sz, ncell=nc) for s, sz, nc in [(1, 40, 6), (2, 64, 20), (3, 96, 30)]]
+    seeds = [11, 22, 33]
+    batch = cw.CpmLattice.from_grids([g for g, _ in scenes], [r for _, r in scenes], 10.0, J3, 2, seeds=seeds)
+    batch.monte_carlo_step(10)
+    for k, ((grid, rec), seed) in enumerate(zip(scenes, seeds)):
+        o = oracle_of(grid, rec, J3, 10.0, 2)
+        o.mcs_checkerboard(seed, 0, 10)
+        np.testing.assert_array_equal(batch.grid(k).reshape(-1), o.grid)
+        assert batch.records_match_grid(k)
+
+
+def test_obstacles_hold_and_sizes_stay_near_target():
+    grid, rec = sheet(seed=4, size=80, ncell=30)
+    seeding.add_obstacle_disc(grid, rec, (40, 40), 5)
+    obst = grid.reshape(-1) == -1
+    g = cw.CpmLattice.from_grids([grid], [rec], 10.0, J3, 2, seeds=[5])
+    g.monte_carlo_step(50)
+    out = g.grid().reshape(-1)
+    assert (out[obst] == -1).all()
+    vol = g.cells()["volume"][1:]
+    tgt = np.array(rec.target[1:])
+    assert np.abs(vol - tgt).mean() / tgt.mean() < 0.15
+    assert g.records_match_grid()
+
+
+def test_a_cell_aiming_at_nothing_shrinks_to_nothing():
+    # cpm.rs:1438-1457 on the device's sweep
+    grid = seeding.empty(50, 50)
+    rec = seeding.Records()
+    cid = seeding.add_cell(grid, rec, 1, (25, 25), 6)
+    rec.target[cid] = 0
+    g = cw.CpmLattice.from_grids([grid], [rec], 10.0, REF_J[:2, :2], 1, seeds=[5])
+    g.monte_carlo_step(200)
+    assert g.volume(cid) == 0 and not (g.grid() == cid).any()
+
+
+def test_bad_input_is_refused():
+    with pytest.raises(cw.ConfigError):
+        cw.CpmLattice([(0, 10, 1)], 10.0, 4)
+    lat = cw.CpmLattice([(10, 10, 1)], 10.0, 4, J=J3)
+    with pytest.raises(cw.ConfigError):
+        lat.upload(np.full(100, 7, np.int32))
+    with pytest.raises(cw.ConfigError):
+        lat.set_contact(np.array([[0, 1], [2, 0]], float))
+    with pytest.raises(cw.NotFoundError):
+        lat.grid(hist=3)
