@@ -1,0 +1,364 @@
+#!/usr/bin/env python
+"""Throughput of cellweave's per-step hot path on B200s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload campaign|cord]
+
+Workload (default ``campaign``): the batched campaign of 64 independent
+histories of uneven sizes (16 each at 128^2, 256^2, 512^2, 1024^2; cells at
+30% fill, target 49; oxygen and a secreted signal solved to residual 1e-6 by
+FP32 SOR with FP64 defect correction; 8-species RK4 network; Moore-contact
+CPM).  A step is one lattice step (MCS) of every history: field solves,
+means, RK4, fates, Monte Carlo sweep.  Data are synthetic (seeded).
+
+The JSON line reports histories*MCS/s of the batch (``value``), of the same
+histories stepped one at a time (``plain``), end to end through the C ABI
+with host buffers (``e2e``), the roofline of the dominant kernel (the FP32
+SOR sweep), and the reference's algorithm timed on the host cores
+(``cpu_baseline``, the CPU oracle on a bounded sample).
+
+Under torchrun every rank runs its own campaign (seeds offset by rank): weak
+scaling, no collective on the data path; ranks meet only for the barriers
+and the max-over-ranks timing.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "histories·MCS/s batched vs plain on 1 B200 at SOR resid≤1e-6; SOR HBM GB/s"
+UNIT = "histories·MCS/s"
+SOR_BYTES_PER_SITE_SWEEP = 16  # FP32 inner sweep: correction read 4 + write 4, rhs 4, coefficient 4
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--workload", choices=["campaign", "cord"], default="campaign")
+    p.add_argument("--no-plain", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--profile-step", action="store_true",
+                   help="bracket one extra step with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
+    return p.parse_args()
+
+
+def workload(name, rank=0):
+    from cellweave_b200 import synthetic
+    cfg = synthetic.campaign() if name == "campaign" else synthetic.tumour_cord()
+    cfg["seeds"] = [s + 100_000 * rank for s in cfg["seeds"]]
+    return cfg
+
+
+def config_key(name, cfg):
+    if name == "campaign":
+        return {"workload": "batched campaign: 64 histories, 16 each at 128^2/256^2/512^2/1024^2, 30% fill at "
+                            "target 49, Moore contact, 2 fields to residual 1e-6 (FP32 SOR + FP64 defect "
+                            "correction), 8-species RK4 x8 per MCS", "histories": len(cfg["dims"]),
+                "sites": int(sum(w * h * d for w, h, d in cfg["dims"])), "cells": int(sum(cfg["ncells"])),
+                "l2": "inputs larger than L2 (the lattices and fields of one step exceed 126 MB)",
+                "parallelism": "histories batched in one launch per kernel; ranks own disjoint campaigns"}
+    return {"workload": "tumour cord 2048^2, ~40k cells of target 64, 3 types, vessel column, 2 fields to "
+                        "residual 1e-6, 16-species RK4", "histories": 1,
+            "l2": "inputs larger than L2", "parallelism": "one history"}
+
+
+# ------------------------------------------------------------------ GPU clocks
+class Clocks:
+    """nvidia-smi sampled every 200 ms while the timed region runs."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait()
+        rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+        os.unlink(self.path)
+        sm = [float(r[1]) for r in rows if len(r) > 8 and r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) > 8 and r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows if len(r) > 8 for n, v in zip(names, r[5:9]) if "Active" in v})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ------------------------------------------------------------------ the CPU reference path
+def _cpu_worker(args):
+    """One worker: a few histories of the workload on the CPU oracle, stepped
+    `steps` times after `warm` untimed steps; returns (history*MCS, seconds)."""
+    items, cfg, steps, warm, barrier = args
+    os.environ["OMP_NUM_THREADS"] = "1"
+    from oracle import cpu_sim
+    hs = [cpu_sim.CpuHistory(cfg, k) for k in items]
+    for h in hs:
+        for _ in range(warm):
+            h.step()
+    if barrier is not None:
+        barrier.wait()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        for h in hs:
+            h.step()
+    return len(hs) * steps, time.perf_counter() - t0
+
+
+def cpu_sample(cfg, steps, warm, per_size, procs):
+    """The oracle (the reference's algorithms, restated in C) on a bounded
+    sample: `per_size` histories of each lattice size, one history per host
+    process as the reference's campaign runs one per thread."""
+    sizes = sorted({d[0] for d in cfg["dims"]})
+    picked = []
+    for s in sizes:
+        ks = [k for k, d in enumerate(cfg["dims"]) if d[0] == s][:per_size]
+        picked += ks
+    procs = max(1, min(procs, len(picked)))
+    chunks = [picked[i::procs] for i in range(procs)]
+    ctx = mp.get_context("spawn")
+    with ctx.Manager() as mgr:
+        barrier = mgr.Barrier(procs)
+        with ctx.Pool(procs) as pool:
+            t0 = time.perf_counter()
+            res = pool.map(_cpu_worker, [(c, cfg, steps, warm, barrier) for c in chunks])
+            wall = time.perf_counter() - t0
+    units = sum(r[0] for r in res)
+    seconds = max(r[1] for r in res)
+    return units / seconds, {"histories": len(picked), "per_size": per_size, "steps": steps, "warm": warm,
+                             "processes": procs, "wall_s": round(wall, 2)}
+
+
+# ------------------------------------------------------------------ our path
+def network_for(S, seed, refvol):
+    import cellweave_b200 as cw
+    from cellweave_b200 import synthetic
+    d = tempfile.mkdtemp()
+    path = os.path.join(d, f"synthetic-{S}.toml")
+    with open(path, "w") as fh:
+        fh.write(synthetic.network_toml(S, seed))
+    return cw.Network.load(path, refvol)
+
+
+def event_ms(L, a, b):
+    ms = C.c_float()
+    L.cw_event_elapsed(a, b, C.byref(ms))
+    return ms.value
+
+
+def run_ours(args, rank, world, dist):
+    import numpy as np
+
+    import cellweave_b200 as cw
+    from cellweave_b200 import _lib
+    L = _lib.lib()
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    _lib.check(L.cw_set_device(local))
+    cfg = workload(args.workload, rank)
+    S = cfg.pop("S")
+    net = network_for(S, S, cfg["target_volume"])
+    nh = len(cfg["dims"])
+    sim = cw.Simulation(net, **cfg)
+    sim.step(max(args.warmup, 3) if args.warmup >= 3 else args.warmup)
+
+    def barrier():
+        L.cw_synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    # ---- timed region: K batched steps, device time by events
+    barrier()
+    clocks = Clocks(local)
+    clocks.start()
+    l0 = L.cw_launch_count()
+    L.cw_event_record(0)
+    sim.step(args.steps)
+    L.cw_event_record(1)
+    L.cw_synchronize()
+    ms = event_ms(L, 0, 1)
+    launches = int(L.cw_launch_count() - l0)
+    clk = clocks.stop()
+    barrier()
+    if dist is not None:
+        import torch
+        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * nh * args.steps / (ms / 1e3)
+    stats = sim.stats()
+    if args.profile_step:
+        _lib.check(L.cw_profiler_start())
+        sim.step(1)
+        _lib.check(L.cw_profiler_stop())
+
+    # ---- end to end through the C ABI: host grids in, step, grids and stats out
+    lat = sim.lattice_handle()
+    grids = []
+    try:
+        import torch
+        for k, (w, h, d) in enumerate(cfg["dims"]):
+            t = torch.empty(w * h * d, dtype=torch.int32, pin_memory=True)
+            grids.append(t.numpy())
+    except Exception:
+        grids = [np.empty(w * h * d, np.int32) for (w, h, d) in cfg["dims"]]
+    for k, g in enumerate(grids):
+        _lib.check(L.cw_lattice_download(lat, k, _lib.ptr(g)))
+    st_host = np.empty((nh, 4))
+    e2e_steps = max(2, min(args.steps, 5))
+    barrier()
+    L.cw_event_record(2)
+    for _ in range(e2e_steps):
+        for k, g in enumerate(grids):
+            _lib.check(L.cw_lattice_upload(lat, k, _lib.ptr(g)))
+        sim.step(1)
+        for k, g in enumerate(grids):
+            _lib.check(L.cw_lattice_download(lat, k, _lib.ptr(g)))
+        _lib.check(L.cw_sim_stats(sim._h, _lib.ptr(st_host)))
+    L.cw_event_record(3)
+    e2e_ms = event_ms(L, 2, 3) / e2e_steps
+    bytes_grid = int(sum(g.nbytes for g in grids))
+    if dist is not None:
+        import torch
+        t = torch.tensor([e2e_ms], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = {"value": world * nh / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": bytes_grid,
+           "d2h_bytes_per_step": bytes_grid + st_host.nbytes, "steps": e2e_steps,
+           "path": "cw_lattice_upload (pinned host grids) + cw_sim_step + cw_lattice_download + cw_sim_stats"}
+
+    # ---- roofline of the dominant kernel: the FP32 SOR sweep on this batch's oxygen field
+    f = sim.field_handle(0)
+    depth, sweeps = 4, 32
+    kms, kl = C.c_float(), C.c_int64()
+    _lib.check(L.cw_field_time_inner(f, sweeps, depth, 1.9, C.byref(kms), C.byref(kl)))  # warm
+    _lib.check(L.cw_field_time_inner(f, sweeps, depth, 1.9, C.byref(kms), C.byref(kl)))
+    sites = int(sum(w * h * d for w, h, d in cfg["dims"]))
+    per_launch_ms = kms.value / kl.value
+    alg_bytes_per_launch = sites * (depth / 2) * SOR_BYTES_PER_SITE_SWEEP
+    achieved = alg_bytes_per_launch / (per_launch_ms / 1e3) / 1e9
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    roofline = {"kernel": "k_sor32_tb (FP32 red-black SOR, 4 half-sweeps per launch in shared memory)",
+                "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 3),
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if "hbm_gbs" in peaks else "fallback 6650",
+                "traffic": None, "alg_bytes_per_launch": int(alg_bytes_per_launch),
+                "launch_ms": round(per_launch_ms, 4),
+                "note": "algorithmic bytes count 16 B/site/sweep with no credit for the shared-memory reuse, "
+                        "so a temporally blocked kernel can exceed the HBM copy peak"}
+
+    # ---- the plain path: each history stepped alone (rank 0 at N=1)
+    plain = None
+    if not args.no_plain and world == 1:
+        total_ms, units = 0.0, 0
+        del sim
+        for k in range(nh):
+            one = {kk: (vv[k:k + 1] if kk in ("dims", "ncells", "seeds") else vv) for kk, vv in cfg.items()}
+            s1 = cw.Simulation(net, **one)
+            s1.step(max(1, min(args.warmup, 3)))
+            L.cw_synchronize()
+            L.cw_event_record(4)
+            s1.step(args.steps if k < 4 or args.steps <= 5 else 5)
+            L.cw_event_record(5)
+            L.cw_synchronize()
+            total_ms += event_ms(L, 4, 5)
+            units += args.steps if k < 4 or args.steps <= 5 else 5
+            del s1
+        plain = {"value": units / (total_ms / 1e3), "unit": UNIT,
+                 "how": "the same 64 histories, each its own Simulation stepped alone (one history per launch)"}
+    return dict(value=value, ms=ms / args.steps, launches=launches, clocks=clk, e2e=e2e, roofline=roofline,
+                plain=plain, stats=stats, nh=nh, cfg=cfg)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    base = {"metric": METRIC, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "data": "synthetic (seeded)"}
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        cfg = workload(args.workload)
+        steps = max(1, min(args.steps, 3))
+        procs = os.cpu_count() or 1
+        v, sample = cpu_sample(cfg, steps, 1, 4 if args.workload == "campaign" else 1, procs)
+        line = dict(base, impl="reference", value=v, ms_per_step=None, dtype="f64",
+                    config=config_key(args.workload, cfg),
+                    cpu_baseline={"value": v, "unit": UNIT, "cores": procs, "kind": "port",
+                                  "sample": f"{sample['histories']} of the {len(cfg['dims'])} histories "
+                                            f"({sample['per_size']} per size), {sample['steps']} timed MCS each "
+                                            f"after {sample['warm']} untimed, one process per history group",
+                                  "detail": sample},
+                    e2e={"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
+        print(json.dumps(line), flush=True)
+        return 0
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = tdist
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        # the CPU leg first, before any GPU context exists in this process
+        cfg = workload(args.workload)
+        v, sample = cpu_sample(cfg, 1, 1, 2 if args.workload == "campaign" else 1, os.cpu_count() or 1)
+        cpu = {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+               "sample": f"{sample['histories']} histories ({sample['per_size']} per size), one timed MCS each "
+                         f"after one untimed, CPU oracle (sequential Metropolis, FP64 SOR, RK4)",
+               "detail": sample}
+    r = run_ours(args, rank, world, dist)
+    if rank == 0:
+        line = dict(base, value=r["value"], ms_per_step=r["ms"], dtype="f32+f64",
+                    config=config_key(args.workload, r["cfg"]), clocks=r["clocks"], e2e=r["e2e"],
+                    gpu_launches=r["launches"], roofline=r["roofline"], cpu_baseline=cpu,
+                    plain=r["plain"],
+                    batched_over_plain=(r["value"] / r["plain"]["value"]) if r["plain"] else None,
+                    sor_gbs=r["roofline"]["achieved"],
+                    living_cells=float(r["stats"][:, 0].sum()), last_residual_max=float(r["stats"][:, 3].max()))
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

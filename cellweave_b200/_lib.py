@@ -68,7 +68,7 @@ class SimConfig(C.Structure):
                 ("J", C.c_void_p), ("contact_order", C.c_int32), ("target_volume", C.c_int32),
                 ("lambda_volume", C.c_double), ("surface_target", C.c_int32), ("lambda_surface", C.c_double),
                 ("seeding", C.c_int32), ("seed_side", C.c_int32), ("nfields", C.c_int32), ("o2_dcoef", C.c_double),
-                ("o2_sink_by_type", C.c_void_p), ("o2_hold", C.c_int32), ("signal_dcoef", C.c_double),
+                ("o2_sink_by_type", C.c_void_p), ("o2_background_sink", C.c_double), ("o2_hold", C.c_int32), ("signal_dcoef", C.c_double),
                 ("signal_decay", C.c_double), ("signal_secretion", C.c_double), ("hypoxic_level", C.c_double),
                 ("tolerance", C.c_double), ("precision", C.c_int32), ("omega", C.c_double),
                 ("relax_every", C.c_int32), ("dt", C.c_double), ("substeps", C.c_int32), ("sweeps", C.c_int32),
@@ -82,6 +82,7 @@ SIGNATURES = {
     "cw_last_error": (C.c_char_p, []),
     "cw_version": (C.c_int, []),
     "cw_set_stream": (C.c_int, [P]),
+    "cw_set_device": (C.c_int, [I32]),
     "cw_get_stream": (P, []),
     "cw_synchronize": (C.c_int, []),
     "cw_launch_count": (C.c_uint64, []),
@@ -119,6 +120,7 @@ SIGNATURES = {
     "cw_field_residual": (C.c_int, [P, P]),
     "cw_field_inflow": (C.c_int, [P, P]),
     "cw_field_step": (C.c_int, [P, D]),
+    "cw_field_time_inner": (C.c_int, [P, I32, I32, D, P, P]),
     "cw_couple_uptake": (C.c_int, [P, P, I32, P, I32]),
     "cw_couple_background_uptake": (C.c_int, [P, P, D]),
     "cw_couple_production": (C.c_int, [P, P, U32, U32, P]),
@@ -139,6 +141,8 @@ SIGNATURES = {
     "cw_sim_stats": (C.c_int, [P, P]),
     "cw_sim_network_state": (C.c_int, [P, U32, U32, P]),
     "cw_event_record": (C.c_int, [I32]),
+    "cw_profiler_start": (C.c_int, []),
+    "cw_profiler_stop": (C.c_int, []),
     "cw_event_elapsed": (C.c_int, [I32, I32, P]),
 }
 

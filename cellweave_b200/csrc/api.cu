@@ -120,3 +120,22 @@ extern "C" int cw_event_elapsed(int32_t a, int32_t b, float *ms) {
     CW_CUDA(cudaEventElapsedTime(ms, g_events[a], g_events[b]));
     return CW_OK;
 }
+
+extern "C" int cw_set_device(int32_t device) {
+    CW_CUDA(cudaSetDevice(device));
+    return CW_OK;
+}
+
+#include <cuda_profiler_api.h>
+
+// Bracket a region for a profiler started with profiling off.
+extern "C" int cw_profiler_start(void) {
+    CW_CUDA(cudaProfilerStart());
+    return CW_OK;
+}
+
+extern "C" int cw_profiler_stop(void) {
+    CW_CUDA(cudaStreamSynchronize(cw::stream()));
+    CW_CUDA(cudaProfilerStop());
+    return CW_OK;
+}

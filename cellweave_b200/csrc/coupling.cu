@@ -143,6 +143,13 @@ int couple_production_device(cw_field_s *f, cw_lattice_s *l, const double *d_per
     return CW_OK;
 }
 
+int couple_background_device(cw_field_s *f, cw_lattice_s *l, double rate, double *dst) {
+    int64_t n = f->g.total;
+    k_paint_background<<<(unsigned)((n + T - 1) / T), T, 0, stream()>>>(pair_of(l), n, rate, dst);
+    CW_LAUNCHED();
+    return CW_OK;
+}
+
 // Per-cell means over all histories into `mean` (global cell index);
 // `sum` and `count` are scratch of the lattice's record count.
 int couple_means_device(cw_field_s *f, cw_lattice_s *l, double *sum, int32_t *count, double *mean, const Plan &p) {

@@ -221,6 +221,7 @@ int lattice_sweep(cw_lattice_s *lat);
 int couple_uptake_device(cw_field_s *f, cw_lattice_s *l, const double *d_rate_by_type, int K, double *dst,
                          const Plan &p);
 int couple_production_device(cw_field_s *f, cw_lattice_s *l, const double *d_per_cell, const Plan &p);
+int couple_background_device(cw_field_s *f, cw_lattice_s *l, double rate, double *dst);
 int couple_means_device(cw_field_s *f, cw_lattice_s *l, double *sum, int32_t *count, double *mean, const Plan &p);
 }  // namespace cw
 

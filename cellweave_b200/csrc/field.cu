@@ -811,3 +811,40 @@ extern "C" int cw_field_hold_bath(cw_field f, uint32_t hist, const uint8_t *open
     dfree(d_open);
     return rc;
 }
+
+// Measurement hook: `sweeps` FP32 red-black sweeps of the correction
+// equation on the field's current residual, every history active, timed
+// with events around the sweep launches alone.  The field is not changed.
+extern "C" int cw_field_time_inner(cw_field f, int32_t sweeps, int32_t depth, double omega, float *ms,
+                                   int64_t *launches) {
+    uint32_t nh = f->g.nh;
+    int rc = f->alloc_fp32();
+    if (rc != CW_OK) return rc;
+    std::vector<RelaxState> hs(nh);
+    for (auto &s : hs) { std::memset(&s, 0, sizeof s); s.omega = omega; s.stop = CW_STOP_RESIDUAL; }
+    RelaxState *d_st = (RelaxState *)f->stats;
+    CW_CUDA(cudaMemcpyAsync(d_st, hs.data(), sizeof(RelaxState) * nh, cudaMemcpyHostToDevice, stream()));
+    Plan ps;
+    if ((rc = site_plan(f, ps)) != CW_OK) return rc;
+    k_residual64<<<ps.nblocks, T, 0, stream()>>>(view(f), ps.d_blk, nh, d_st, f->r32, f->inv32, f->d32a, 0);
+    CW_LAUNCHED();
+    Sor32 solver;
+    std::vector<double> om(nh, omega);
+    if ((rc = solver.init(f, depth, om)) != CW_OK) return rc;
+    const int32_t *done_ptr = (const int32_t *)((const char *)d_st + offsetof(RelaxState, done));
+    cudaEvent_t a, b;
+    CW_CUDA(cudaEventCreate(&a));
+    CW_CUDA(cudaEventCreate(&b));
+    uint64_t before = cw_launch_count();
+    CW_CUDA(cudaEventRecord(a, stream()));
+    if ((rc = solver.sweeps(f, sweeps, done_ptr, (int)(sizeof(RelaxState) / sizeof(int32_t)))) != CW_OK) return rc;
+    CW_CUDA(cudaEventRecord(b, stream()));
+    CW_CUDA(cudaEventSynchronize(b));
+    CW_CUDA(cudaEventElapsedTime(ms, a, b));
+    *launches = (int64_t)(cw_launch_count() - before);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    solver.release();
+    ps.release();
+    return CW_OK;
+}

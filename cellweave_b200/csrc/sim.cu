@@ -313,6 +313,9 @@ int cw_sim_step(cw_sim s, uint32_t nsteps) {
         if (solve) {
             // 1. downward coupling and the oxygen solve
             if ((rc = couple_uptake_device(s->o2, s->lat, s->d_sink, 8, s->o2->lin_sink, s->sites)) != CW_OK) return rc;
+            if (c.o2_background_sink > 0.0 &&
+                (rc = couple_background_device(s->o2, s->lat, c.o2_background_sink, s->o2->lin_sink)) != CW_OK)
+                return rc;
             s->o2->lin_sink_on = true;
             if ((rc = cw_field_relax(s->o2, &o, s->last.data())) != CW_OK) return rc;
         }

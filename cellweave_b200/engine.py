@@ -482,7 +482,7 @@ class Simulation:
 
     def __init__(self, network: Network, dims, ncells, seeds, *, temperature=10.0, J=None, contact_order=2,
                  target_volume=49, lambda_volume=1.0, surface_target=0, lambda_surface=0.0, seeding=0, seed_side=7,
-                 nfields=1, o2_dcoef=1.0, o2_sink_by_type=(0.0, 0.01, 0.01), o2_hold=0, signal_dcoef=1.0,
+                 nfields=1, o2_dcoef=1.0, o2_sink_by_type=(0.0, 0.01, 0.01), o2_background_sink=0.0, o2_hold=0, signal_dcoef=1.0,
                  signal_decay=0.01, signal_secretion=0.05, hypoxic_level=0.1, tolerance=1e-6, precision=FP32_DC,
                  omega=None, relax_every=1, dt=0.01, substeps=8, sweeps=1, death_threshold=0.25, necrotic_type=-1):
         self.dims, w, h, z = _dims(dims)
@@ -496,7 +496,7 @@ class Simulation:
         cfg = _lib.SimConfig(len(self.dims), ptr(w).value, ptr(h).value, ptr(z).value, ptr(nc).value, ptr(sd).value,
                              float(temperature), int(J.shape[0]), ptr(J).value, int(contact_order),
                              int(target_volume), float(lambda_volume), int(surface_target), float(lambda_surface),
-                             int(seeding), int(seed_side), int(nfields), float(o2_dcoef), ptr(sink).value,
+                             int(seeding), int(seed_side), int(nfields), float(o2_dcoef), ptr(sink).value, float(o2_background_sink),
                              int(o2_hold), float(signal_dcoef), float(signal_decay), float(signal_secretion),
                              float(hypoxic_level), float(tolerance), int(precision), float(omega or 0.0),
                              int(relax_every), float(dt), int(substeps), int(sweeps), float(death_threshold),

@@ -16,7 +16,7 @@ def network_toml(S: int, seed: int = 1, density: float = 0.3) -> str:
     Hill exponent 2, random +1 (activated_by) / -1 (inhibited_by) wiring between
     nodes at `density`, one `decays` per node.  Node 0 reads oxygen, node 1
     rises in its absence (the hypoxia response), node 2 reads EGF (growth),
-    node 3 is survival and is damaged below an oxygen threshold."""
+    node 3 is survival: held near 0.9 and damaged below an oxygen threshold."""
     if S < 4:
         raise ValueError("a synthetic network needs at least four nodes")
     rng = np.random.default_rng(seed)
@@ -39,7 +39,8 @@ def network_toml(S: int, seed: int = 1, density: float = 0.3) -> str:
             terms.append(f'{{ kind = "{kind}", source = "n{j}", rate = {U():.6f}, '
                          f'hill = {{ n = 2.0, k = {U():.6f} }} }}')
         if i == 3:
-            terms.append('{ kind = "damaged_below", source = "oxygen", threshold = 0.05, rate = 0.5 }')
+            terms.append('{ kind = "relaxes_to", value = 0.9, rate = 2.0 }')
+            terms.append('{ kind = "damaged_below", source = "oxygen", threshold = 0.05, rate = 4.0 }')
         terms.append(f'{{ kind = "decays", rate = {U():.6f} }}')
         lines += ["[[nodes]]", f'name = "n{i}"', "initial = 0.5" if i == 3 else "initial = 0.1", "terms = ["]
         lines += [f"  {t}," for t in terms]
@@ -82,12 +83,14 @@ def plain_2d(seed=0):
 def tumour_cord(n=2048):
     """The large cord: n x n, ~40,000 cells of target 64 (8 x 8 packed squares),
     three types (proliferating, arrested, necrotic) with J drawn U[4, 20], a
-    vessel held at 1 down the column x = n/2, oxygen and a signal secreted at
+    vessel held at 1 down the column x = n/2 with the medium around it
+    consuming as stroma (apply_background_uptake, coupling.rs:47-53), oxygen and a signal secreted at
     0.05 by hypoxic cells (c < 0.1), FP32 SOR with FP64 defect correction to
     residual 1e-6; 16-species network."""
     return dict(dims=[(n, n, 1)], ncells=[40000 * (n * n) // (2048 * 2048)], seeds=[2], temperature=10.0,
                 J=contact_table(4, seed=2), contact_order=2, target_volume=64, lambda_volume=1.0, seeding=1,
-                seed_side=8, nfields=2, o2_dcoef=1.0, o2_sink_by_type=(0.0, 0.01, 0.005, 0.0), o2_hold=1,
+                seed_side=8, nfields=2, o2_dcoef=1.0, o2_sink_by_type=(0.0, 0.01, 0.005, 0.0), o2_background_sink=0.001,
+                o2_hold=1,
                 signal_dcoef=1.0, signal_decay=0.01, signal_secretion=0.05, hypoxic_level=0.1, tolerance=1e-6,
                 precision=1, omega=None, relax_every=1, dt=0.01, substeps=8, sweeps=1, death_threshold=0.25,
                 necrotic_type=3, S=16)

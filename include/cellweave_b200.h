@@ -57,6 +57,8 @@ const char *cw_last_error(void);
 int cw_version(void);
 /* Stream all work is queued on (a cudaStream_t); NULL restores the library's own. */
 int cw_set_stream(void *stream);
+/* The CUDA device the library works on (one per process). */
+int cw_set_device(int32_t device);
 void *cw_get_stream(void);
 int cw_synchronize(void);
 /* Kernels this library has launched since it was loaded. */
@@ -64,6 +66,9 @@ uint64_t cw_launch_count(void);
 /* CUDA events on the library stream, in slots 0..15, for timing. */
 int cw_event_record(int32_t slot);
 int cw_event_elapsed(int32_t a, int32_t b, float *ms);
+/* cudaProfilerStart / cudaProfilerStop around a region (for ncu --profile-from-start off). */
+int cw_profiler_start(void);
+int cw_profiler_stop(void);
 
 /* ------------------------------------------------------------------ lattice
  * CpmLattice::with_depth (cpm.rs:231-259) for `nh` histories at once.  A
@@ -162,6 +167,10 @@ int cw_field_relax(cw_field f, const cw_relax_opts *opts, cw_relax_stats *stats)
 int cw_field_residual(cw_field f, double *out);
 /* inflow (pde.rs:415-456) of every history (nh entries). */
 int cw_field_inflow(cw_field f, double *out);
+/* Measurement: time `sweeps` FP32 sweeps of the defect-correction kernel
+ * (`depth` half-sweeps per launch) on the current residual of every history,
+ * without changing the field.  *ms is the kernels' time, *launches their count. */
+int cw_field_time_inner(cw_field f, int32_t sweeps, int32_t depth, double omega, float *ms, int64_t *launches);
 /* DiffusionField::step (pde.rs:705-728): one explicit step; CW_ERR_CONFIG for
  * a step the scheme cannot take (pde.rs:673-701). */
 int cw_field_step(cw_field f, double dt);
@@ -244,6 +253,7 @@ typedef struct {
     int32_t nfields;             /* 1 (oxygen) or 2 (oxygen and a secreted signal) */
     double o2_dcoef;
     const double *o2_sink_by_type; /* K first-order sinks k per type (0 for the medium) */
+    double o2_background_sink;   /* first-order sink of medium pixels (stroma around a vessel) */
     int32_t o2_hold;             /* 0 row y=0, 1 column x=w/2, 2 every face of the box */
     double signal_dcoef, signal_decay, signal_secretion, hypoxic_level;
     double tolerance;            /* residual tolerance of every field solve */

@@ -1,0 +1,145 @@
+"""One history of the benchmark workload stepped on the CPU oracle.
+
+TEST INFRASTRUCTURE / CPU BASELINE ONLY: ``bench.py``'s CPU leg and its
+reference arm time this; no product path imports it.  Every step runs the
+reference's own algorithms as restated in ``cw_oracle.c``: the red-black FP64
+SOR of pde.rs:245-405 (residual stopping rule, first-order sink), the
+mean_per_cell of coupling.rs:164-182, the RK4 of network.rs:777-799 with the
+mechanics of network.rs:811-821, and the sequential random-site Metropolis
+sweep of cpm.rs:748-838, in the order of simulation.rs:1129-1350.
+"""
+from __future__ import annotations
+
+import tomllib
+
+import numpy as np
+
+from . import oracle as O
+
+
+def seed_history(cfg, w, h, d, n, seed):
+    """Squares (cubes) of the workload's side at random free places (seeding 0),
+    packed with a gap of two (1), or cubes in a ball (2); types 1..K-1 (the
+    necrotic type excluded) drawn at random."""
+    rng = np.random.default_rng(seed)
+    s = int(cfg.get("seed_side", 7))
+    grid = np.zeros((d, h, w), np.int32)
+    K = cfg["J"].shape[0]
+    nec = cfg.get("necrotic_type", -1)
+    ntypes = max(1, (nec - 1) if nec and nec > 0 else K - 1)
+    if cfg.get("o2_hold", 0) == 1:
+        grid[:, :, w // 2] = -1
+    types = [0]
+    sz = s if d > 1 else 1
+
+    def free(x, y, z):
+        return (x + s <= w and y + s <= h and z + sz <= d and not grid[z:z + sz, y:y + s, x:x + s].any())
+
+    def put(x, y, z):
+        grid[z:z + sz, y:y + s, x:x + s] = len(types)
+        types.append(1 + int(rng.integers(ntypes)))
+
+    mode = cfg.get("seeding", 0)
+    if mode == 1:
+        pitch = s + 2
+        for z in range(0, d - sz + 1, pitch if d > 1 else 1):
+            for y in range(1, h - s + 1, pitch):
+                for x in range(1, w - s + 1, pitch):
+                    if len(types) - 1 < n and free(x, y, z):
+                        put(x, y, z)
+    elif mode == 2 and d > 1:
+        R = (3.0 * n * s ** 3 / (4.0 * np.pi)) ** (1 / 3) + 0.5 * s
+        for z in range(0, d - s + 1, s):
+            for y in range(0, h - s + 1, s):
+                for x in range(0, w - s + 1, s):
+                    if ((x + s / 2 - w / 2) ** 2 + (y + s / 2 - h / 2) ** 2 + (z + s / 2 - d / 2) ** 2 <= R * R
+                            and len(types) - 1 < n and free(x, y, z)):
+                        put(x, y, z)
+    else:
+        tries = 0
+        while len(types) - 1 < n and tries < 200 * n + 1000:
+            tries += 1
+            x, y = int(rng.integers(w - s + 1)), int(rng.integers(h - s + 1))
+            z = int(rng.integers(d - sz + 1)) if d > 1 else 0
+            if free(x, y, z):
+                put(x, y, z)
+    return grid, np.array(types, np.int32)
+
+
+class CpuHistory:
+    def __init__(self, cfg, k):
+        from cellweave_b200 import synthetic  # the same synthetic network text the device runs
+        self.cfg = cfg
+        w, h, d = cfg["dims"][k]
+        self.dims = (w, h, d)
+        self.seed = int(cfg["seeds"][k])
+        grid, types = seed_history(cfg, w, h, d, int(cfg["ncells"][k]), self.seed)
+        self.ncap = len(types)
+        J = np.asarray(cfg["J"], float)
+        self.lat = O.Lattice(grid, (w, h, d), self.ncap, J, cfg["temperature"], cfg.get("contact_order", 1))
+        self.lat.type[:] = types
+        self.lat.recount()
+        self.lat.volume[0] = 0
+        self.lat.target[:] = cfg["target_volume"]
+        self.lat.target[0] = 0
+        self.lat.lam[:] = cfg["lambda_volume"]
+        self.lat.lam[0] = 0.0
+        if cfg.get("surface_target", 0) > 0:
+            self.lat.enable_surface(np.full(self.ncap, cfg["surface_target"], np.int32),
+                                    np.full(self.ncap, cfg.get("lambda_surface", 0.0)))
+        n = w * h * d
+        self.o2 = O.Field(w, h, d, cfg["o2_dcoef"], 0.0, 1.0)
+        z, y, x = np.mgrid[0:d, 0:h, 0:w]
+        hold = cfg.get("o2_hold", 0)
+        held = (y == 0) if hold == 0 else (x == w // 2) if hold == 1 else (
+            (x == 0) | (y == 0) | (z == 0) | (x == w - 1) | (y == h - 1) | (z == d - 1))
+        self.o2.held[:] = held.reshape(-1)
+        self.o2.values[self.o2.held == 1] = 1.0
+        self.o2.lin_sink = np.zeros(n)
+        self.sig = None
+        if cfg.get("nfields", 1) == 2:
+            self.sig = O.Field(w, h, d, cfg["signal_dcoef"], cfg["signal_decay"], 0.0)
+        spec = tomllib.loads(synthetic.network_toml(cfg["S"], cfg["S"]))
+        self.net = O.compile_network(spec, cfg["target_volume"])
+        self.state = np.tile(self.net.initial, (self.ncap, 1))
+        sink = np.zeros(8)
+        sink[:len(cfg["o2_sink_by_type"])] = cfg["o2_sink_by_type"]
+        self.sink = sink
+        self.steps = 0
+
+    def step(self):
+        c = self.cfg
+        g = self.lat.grid
+        t = self.lat.type
+        cells = g > 0
+        sink = np.zeros(g.size)
+        sink[cells] = self.sink[t[g[cells]]]
+        sink[g == 0] = c.get("o2_background_sink", 0.0)
+        self.o2.lin_sink = sink
+        omega = c.get("omega") or 0.0
+        rc, _ = self.o2.relax(c["tolerance"], 200_000, omega=omega, stop=1, threads=1)
+        o2m = O.mean_per_cell(g, self.o2.values, self.ncap)
+        nec = c.get("necrotic_type", -1)
+        alive = (self.lat.volume > 0) & (t != nec)
+        alive[0] = False
+        if self.sig is not None:
+            sec = np.where(alive & (o2m < c["hypoxic_level"]), c["signal_secretion"], 0.0)
+            self.sig.production = O.apply_production(g, sec)
+            self.sig.relax(c["tolerance"], 200_000, omega=omega, stop=1, threads=1)
+        idx = np.nonzero(alive)[0]
+        if len(idx):
+            ins = np.zeros((len(idx), 6))
+            ins[:, 0] = o2m[idx]
+            ins[:, 1] = 0.2
+            st = np.ascontiguousarray(self.state[idx])
+            O.network_step(self.net, st, ins, c["dt"], c["substeps"])
+            self.state[idx] = st
+            tg = O.network_mechanics(self.net, st)
+            dead = (st[:, self.net.survival] < c.get("death_threshold", 0.25)) if nec >= 0 else np.zeros(len(idx), bool)
+            t[idx[dead]] = nec
+            live = idx[~dead]
+            self.lat.target[live] = np.minimum(tg[~dead], 2**31 - 1).astype(np.int32)
+            self.lat.lam[live] = c["lambda_volume"]
+        self.lat.mcs_sequential(self.seed * 1_000_003 + self.steps, c.get("sweeps", 1))
+        self.steps += 1
+        return rc

@@ -40,6 +40,10 @@ def ball_volume(size=20):
     seeding.add_ball(grid, rec, 1, (c - 3, c, c), 3, lam=2.0)
     seeding.add_ball(grid, rec, 1, (c + 3, c, c), 3, lam=2.0)
     seeding.add_ball(grid, rec, 2, (c, c + 3, c - 1), 2, lam=2.0)
+    # add_ball takes voxels from earlier cells without updating their records
+    # (cpm.rs:323-354); recount so that the books start true
+    rec.volume = list(seeding.recount(grid, len(rec)))
+    rec.volume[0] = 0
     return grid, rec
 
 
