@@ -137,6 +137,7 @@ SIGNATURES = {
     "cw_sim_destroy": (C.c_int, [P]),
     "cw_sim_step": (C.c_int, [P, U32]),
     "cw_sim_lattice": (C.c_int, [P, P]),
+    "cw_sim_tuning": (C.c_int, [P, P, P, P, P]),
     "cw_sim_field": (C.c_int, [P, I32, P]),
     "cw_sim_stats": (C.c_int, [P, P]),
     "cw_sim_network_state": (C.c_int, [P, U32, U32, P]),

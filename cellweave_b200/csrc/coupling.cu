@@ -138,6 +138,7 @@ int couple_uptake_device(cw_field_s *f, cw_lattice_s *l, const double *d_rate_by
 }
 
 int couple_production_device(cw_field_s *f, cw_lattice_s *l, const double *d_per_cell, const Plan &p) {
+    f->production_on = true;
     k_paint_production<<<p.nblocks, T, 0, stream()>>>(pair_of(l), p.d_blk, l->g.nh, d_per_cell, f->production);
     CW_LAUNCHED();
     return CW_OK;
@@ -178,6 +179,7 @@ int cw_couple_uptake(cw_field f, cw_lattice l, int32_t K, const double *rate_by_
     if ((rc = site_plan(f->g, p)) != CW_OK) return rc;
     double *dst = first_order ? f->lin_sink : f->uptake;
     if (first_order) f->lin_sink_on = true;
+    else f->uptake_on = true;
     rc = couple_uptake_device(f, l, d_rate, l->K > K ? K : l->K, dst, p);
     CW_CUDA(cudaStreamSynchronize(stream()));
     dfree(d_rate);
@@ -189,6 +191,7 @@ int cw_couple_background_uptake(cw_field f, cw_lattice l, double rate) {
     int rc = check_pair(f, l);
     if (rc != CW_OK) return rc;
     int64_t n = f->g.total;
+    f->uptake_on = true;
     k_paint_background<<<(unsigned)((n + T - 1) / T), T, 0, stream()>>>(pair_of(l), n, rate, f->uptake);
     CW_LAUNCHED();
     CW_CUDA(cudaStreamSynchronize(stream()));
@@ -212,6 +215,7 @@ int cw_couple_production(cw_field f, cw_lattice l, uint32_t hist, uint32_t n, co
     if ((rc = site_plan(f->g, p)) != CW_OK) return rc;
     k_paint_production<<<p.nblocks, T, 0, stream()>>>(pair_of(l), p.d_blk, l->g.nh, d_pc, d_out);
     CW_LAUNCHED();
+    f->production_on = true;
     CW_CUDA(cudaMemcpyAsync(f->production + f->g.off[hist], d_out + f->g.off[hist], sizeof(double) * f->g.sites(hist),
                             cudaMemcpyDeviceToDevice, stream()));
     CW_CUDA(cudaStreamSynchronize(stream()));
@@ -225,6 +229,7 @@ int cw_couple_hold_obstacles(cw_field f, cw_lattice l, double value) {
     int rc = check_pair(f, l);
     if (rc != CW_OK) return rc;
     int64_t n = f->g.total;
+    f->held_dirty = true;
     k_hold_obstacles<<<(unsigned)((n + T - 1) / T), T, 0, stream()>>>(l->grid, n, value, f->held, f->c);
     CW_LAUNCHED();
     CW_CUDA(cudaStreamSynchronize(stream()));

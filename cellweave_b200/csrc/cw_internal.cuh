@@ -202,7 +202,9 @@ struct cw_field_s {
     double *c = nullptr;             // values
     uint8_t *held = nullptr;
     double *uptake = nullptr, *production = nullptr, *lin_sink = nullptr;
-    bool lin_sink_on = false;
+    bool lin_sink_on = false, uptake_on = false, production_on = false;
+    bool held_dirty = true;          // the span cache is stale
+    std::vector<cw::Span> spans;     // free_span of every history, cached
     double dcoef = 0.2, decay = 0.0, source = 0.0;
     // scratch of the FP32 defect-correction solve and the explicit step
     float *r32 = nullptr, *d32a = nullptr, *d32b = nullptr, *inv32 = nullptr;
@@ -215,6 +217,7 @@ struct cw_field_s {
 namespace cw {
 // translation-unit entry points used across files
 int field_span(cw_field_s *f, std::vector<Span> &spans);
+int field_relax(cw_field_s *f, const cw_relax_opts *opts, const double *omega_h, cw_relax_stats *stats);
 int lattice_recount(cw_lattice_s *lat, int32_t *vol_out, int32_t *surf_out);
 int lattice_sweep(cw_lattice_s *lat);
 // coupling (coupling.cu), device-resident

@@ -108,7 +108,7 @@ __global__ void k_sor64_half(FieldView fv, const int32_t *blk, int nh, const Spa
                 pixel_sums64(fv.c, i, x, y, z, dm, sum, real);
                 double den = real * fv.d + fv.decay;
                 if (fv.ks) den = den + fv.ks[i];
-                double balanced = (fv.d * sum + fv.source + fv.pr[i] - fv.up[i]) / den;
+                double balanced = add_sources(fv, i, fv.d * sum) / den;
                 double om = st[h].omega;
                 double after = fmax((1.0 - om) * before + om * balanced, 0.0);
                 fv.c[i] = after;
@@ -145,7 +145,7 @@ __global__ void k_residual64(FieldView fv, const int32_t *blk, int nh, RelaxStat
             double den = real * fv.d + fv.decay;
             if (fv.ks) den = den + fv.ks[i];
             double cv = fv.c[i];
-            double r = (fv.d * sum + fv.source + fv.pr[i] - fv.up[i]) - den * cv;
+            double r = add_sources(fv, i, fv.d * sum) - den * cv;
             if (cv <= 0.0 && r < 0.0) r = 0.0;
             worst = fabs(r);
             r_out = (float)r;
@@ -260,7 +260,7 @@ __global__ void k_explicit(FieldView fv, const int32_t *blk, int nh, double dt, 
         double q = z + 1 < dm.z ? fv.c[i + slice] : c;
         lap += p + q - 2.0 * c;
     }
-    double change = fv.d * lap - fv.decay * c + fv.source + fv.pr[i] - fv.up[i];
+    double change = add_sources(fv, i, fv.d * lap - fv.decay * c);
     next[i] = fmax(c + dt * change, 0.0);
 }
 
@@ -372,7 +372,8 @@ namespace cw {
 
 FieldView view(cw_field_s *f) {
     FieldView v;
-    v.c = f->c; v.held = f->held; v.up = f->uptake; v.pr = f->production;
+    v.c = f->c; v.held = f->held; v.up = f->uptake_on ? f->uptake : nullptr;
+    v.pr = f->production_on ? f->production : nullptr;
     v.ks = f->lin_sink_on ? f->lin_sink : nullptr;
     v.d = f->dcoef; v.decay = f->decay; v.source = f->source;
     v.dims = f->g.d_dims; v.off = f->g.d_off;
@@ -494,7 +495,8 @@ static int relax_fp32dc(cw_field_s *f, const cw_relax_opts &o, RelaxState *d_st,
     int queue = 2;
     while (outer < max_outer) {
         for (int q = 0; q < queue && outer < max_outer; ++q, ++outer) {
-            k_residual64<<<ps.nblocks, T, 0, stream()>>>(fv, ps.d_blk, nh, d_st, f->r32, f->inv32, f->d32a, 1);
+            k_residual64<<<ps.nblocks, T, 0, stream()>>>(fv, ps.d_blk, nh, d_st, f->r32, outer == 0 ? f->inv32 : nullptr,
+                                                         f->d32a, 1);
             CW_LAUNCHED();
             k_dc_check<<<(nh + 63) / 64, 64, 0, stream()>>>(d_st, nh, inner, o.max_sweeps);
             CW_LAUNCHED();
@@ -581,6 +583,8 @@ int cw_field_upload(cw_field f, uint32_t hist, int32_t which, const double *host
     double *p = array_of(f, which);
     if (!p) return fail(CW_ERR_CONFIG, "unknown field array");
     if (which == CW_LIN_SINK) f->lin_sink_on = true;
+    if (which == CW_UPTAKE) f->uptake_on = true;
+    if (which == CW_PRODUCTION) f->production_on = true;
     CW_CUDA(cudaMemcpyAsync(p + f->g.off[hist], host, sizeof(double) * f->g.sites(hist), cudaMemcpyHostToDevice,
                             stream()));
     CW_CUDA(cudaStreamSynchronize(stream()));
@@ -599,6 +603,7 @@ int cw_field_download(cw_field f, uint32_t hist, int32_t which, double *host) {
 
 int cw_field_upload_held(cw_field f, uint32_t hist, const uint8_t *held) {
     if (hist >= f->g.nh) return fail(CW_ERR_NOT_FOUND, "no history " + std::to_string(hist));
+    f->held_dirty = true;
     CW_CUDA(cudaMemcpyAsync(f->held + f->g.off[hist], held, f->g.sites(hist), cudaMemcpyHostToDevice, stream()));
     CW_CUDA(cudaStreamSynchronize(stream()));
     return CW_OK;
@@ -622,10 +627,14 @@ int cw_field_clear(cw_field f, int32_t which) {
     double *p = array_of(f, which);
     if (!p || which == CW_VALUES) return fail(CW_ERR_CONFIG, "only uptake, production and the linear sink clear");
     CW_CUDA(cudaMemsetAsync(p, 0, sizeof(double) * f->g.total, stream()));
+    if (which == CW_UPTAKE) f->uptake_on = false;
+    if (which == CW_PRODUCTION) f->production_on = false;
+    if (which == CW_LIN_SINK) f->lin_sink_on = false;
     return CW_OK;
 }
 
 int cw_field_release_all(cw_field f) {
+    f->held_dirty = true;
     CW_CUDA(cudaMemsetAsync(f->held, 0, f->g.total, stream()));
     return CW_OK;
 }
@@ -637,6 +646,7 @@ int cw_field_hold_mask(cw_field f, uint32_t hist, const uint8_t *mask, double va
     int rc = dalloc(&dm, n);
     if (rc != CW_OK) return rc;
     CW_CUDA(cudaMemcpyAsync(dm, mask, n, cudaMemcpyHostToDevice, stream()));
+    f->held_dirty = true;
     k_hold_mask<<<(unsigned)blocks_for(n), T, 0, stream()>>>(f->c + f->g.off[hist], f->held + f->g.off[hist], dm, n,
                                                              value);
     CW_LAUNCHED();
@@ -646,15 +656,26 @@ int cw_field_hold_mask(cw_field f, uint32_t hist, const uint8_t *mask, double va
 }
 
 int cw_field_relax(cw_field f, const cw_relax_opts *opts, cw_relax_stats *stats) {
+    return cw::field_relax(f, opts, nullptr, stats);
+}
+
+}  // extern "C"
+
+// relax on every history; omega_h (nh entries, may be null) overrides the
+// options' factor history by history.
+int cw::field_relax(cw_field_s *f, const cw_relax_opts *opts, const double *omega_h, cw_relax_stats *stats) {
     cw_relax_opts o = *opts;
     if (o.max_sweeps <= 0) o.max_sweeps = 1;
     if (o.precision != CW_FP64 && o.precision != CW_FP32_DC) return fail(CW_ERR_CONFIG, "unknown precision");
     if (o.precision == CW_FP32_DC && o.stop != CW_STOP_RESIDUAL)
         return fail(CW_ERR_CONFIG, "the FP32 defect-correction solve stops on the residual only");
     uint32_t nh = f->g.nh;
-    std::vector<Span> spans;
-    int rc = field_span(f, spans);
-    if (rc != CW_OK) return rc;
+    int rc;
+    if (f->held_dirty || f->spans.size() != nh) {
+        if ((rc = field_span(f, f->spans)) != CW_OK) return rc;
+        f->held_dirty = false;
+    }
+    std::vector<Span> &spans = f->spans;
     std::vector<RelaxState> hs(nh);
     for (uint32_t k = 0; k < nh; ++k) {
         RelaxState &s = hs[k];
@@ -667,16 +688,21 @@ int cw_field_relax(cw_field f, const cw_relax_opts *opts, cw_relax_stats *stats)
             s.omega = 0.0;
             continue;
         }
-        s.omega = o.omega > 0.0 ? o.omega : auto_omega(f, k, spans[k]);
+        s.omega = (omega_h && omega_h[k] > 0.0) ? omega_h[k] : o.omega > 0.0 ? o.omega : auto_omega(f, k, spans[k]);
     }
     RelaxState *d_st = (RelaxState *)f->stats;
     CW_CUDA(cudaMemcpyAsync(d_st, hs.data(), sizeof(RelaxState) * nh, cudaMemcpyHostToDevice, stream()));
     if (o.precision == CW_FP64) rc = relax_fp64(f, o, spans, d_st, hs);
     else rc = relax_fp32dc(f, o, d_st, hs);
     if (rc != CW_OK) return rc;
-    // final residual of every history, for the report
+    // final residual of every history, for the report (the defect-correction
+    // loop ends on one it has just computed)
     std::vector<double> res(nh);
-    if ((rc = cw_field_residual(f, res.data())) != CW_OK) return rc;
+    if (o.precision == CW_FP32_DC) {
+        for (uint32_t k = 0; k < nh; ++k) res[k] = hs[k].last_resid;
+    } else if ((rc = cw_field_residual(f, res.data())) != CW_OK) {
+        return rc;
+    }
     bool bad = false;
     for (uint32_t k = 0; k < nh; ++k) {
         bool ok = hs[k].done == 1;
@@ -694,6 +720,8 @@ int cw_field_relax(cw_field f, const cw_relax_opts *opts, cw_relax_stats *stats)
                                            " sweeps at tolerance " + std::to_string(o.tolerance));
     return CW_OK;
 }
+
+extern "C" {
 
 int cw_field_residual(cw_field f, double *out) {
     uint32_t nh = f->g.nh;
@@ -763,6 +791,7 @@ int field_hold_bath_device(cw_field_s *f, const uint8_t *d_open, int hist, doubl
     int rc = site_plan(f, ps);
     if (rc != CW_OK) return rc;
     uint32_t nh = f->g.nh;
+    f->held_dirty = true;  // the span buffer is the box's scratch, and holds change
     Span *box = f->d_span;
     k_span_reset<<<(nh + 63) / 64, 64, 0, stream()>>>(box, nh);
     CW_LAUNCHED();

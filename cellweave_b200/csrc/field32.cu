@@ -2,85 +2,116 @@
 // solve (see field.cu).  Built with fused multiply-add: this is the fast
 // path, and its error is removed by the FP64 residual and correction steps.
 //
-// A flat history is cut into TX x TY tiles.  Each launch loads a tile with a
-// halo `depth` pixels deep into shared memory (correction, right-hand side
-// and inverse diagonal), runs `depth` half-sweeps there, the valid region
-// shrinking by one ring per half-sweep, and writes the tile's interior to
-// the other buffer.  The interior is exactly what `depth` global half-sweeps
-// would give, and the correction makes one round trip through HBM per
-// `depth` half-sweeps instead of one per half-sweep.
+// Temporal blocking.  A flat history is cut into tiles whose interior is
+// (64 - 2 DEPTH) pixels square; a block loads the tile with a halo DEPTH
+// pixels deep (a 64 x 64 window) and runs DEPTH half-sweeps on it before
+// writing the interior back to the other buffer.  Every window pixel is
+// updated at every half-sweep, its missing neighbours read as zero; the
+// error this makes at the window's edge moves in by one ring per half-sweep,
+// so after DEPTH of them the interior is exactly what DEPTH global
+// half-sweeps give.  The correction crosses HBM once per DEPTH half-sweeps.
+//
+// Layout.  Warp w owns window rows 8w .. 8w+7, lane l the column pair
+// (2l, 2l+1): one pixel of each colour per row, so every half-sweep gives
+// every thread the same work.  The correction, the right-hand side and the
+// inverse diagonal of a thread's sixteen pixels stay in registers for the
+// whole launch.  Neighbours come from the thread's own registers (the other
+// pixel of the pair, the rows above and below), from the next lane by a warp
+// shuffle, and across a warp boundary from the one row each neighbouring
+// warp publishes in shared memory after every half-sweep.
 #include "cw_internal.cuh"
 #include "field_kernels.cuh"
 
 namespace cw {
 namespace {
 
-constexpr int TX = 128;
-constexpr int TY = 32;
-constexpr int THREADS = 512;
+constexpr int WIN = 64;            // window side
+constexpr int WARPS = 8;           // warps per block
+constexpr int ROWS = WIN / WARPS;  // window rows per warp
 
-__global__ void __launch_bounds__(THREADS) k_sor32_tb(const float *__restrict__ src, float *__restrict__ dst,
-                                                      const float *__restrict__ rhs, const float *__restrict__ inv,
-                                                      const int4 *__restrict__ dims, const int64_t *__restrict__ off,
-                                                      const int32_t *__restrict__ blk, int nh,
-                                                      const float *__restrict__ omega, const int32_t *done,
-                                                      int done_stride, int depth, int start_colour, float dcoef) {
-    extern __shared__ float sm[];
+template <int DEPTH>
+__global__ void __launch_bounds__(32 * WARPS) k_sor32_tb(const float *__restrict__ src, float *__restrict__ dst,
+                                                         const float *__restrict__ rhs, const float *__restrict__ inv,
+                                                         const int4 *__restrict__ dims,
+                                                         const int64_t *__restrict__ off,
+                                                         const int32_t *__restrict__ blk, int nh,
+                                                         const float *__restrict__ omega, const int32_t *done,
+                                                         int done_stride, int nhalf, int start_colour, float dcoef) {
+    constexpr int IN = WIN - 2 * DEPTH;  // interior side
+    // edge rows each warp publishes: [warp][0 top, 1 bottom][column]
+    __shared__ float edge[WARPS][2][WIN];
     __shared__ int s_h;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (threadIdx.x == 0) s_h = plan_history(blk, nh, blockIdx.x);
     __syncthreads();
     const int h = s_h;
     if (done[(int64_t)h * done_stride]) return;
     const int4 dm = dims[h];
-    const int ntx = (dm.x + TX - 1) / TX;
+    const int ntx = (dm.x + IN - 1) / IN;
     const int t = blockIdx.x - blk[h];
-    const int tx0 = (t % ntx) * TX, ty0 = (t / ntx) * TY;
-    const int EW = TX + 2 * depth, EH = TY + 2 * depth, E = EW * EH;
-    float *sd = sm, *sr = sm + E, *si = sm + 2 * E;
+    const int gx0 = (t % ntx) * IN - DEPTH, gy0 = (t / ntx) * IN - DEPTH;
     const int64_t base = off[h];
     const float om = omega[h];
-    // load the tile and its halo; outside the grid everything is zero, which
-    // drops the missing neighbours from the sum (their count is in `inv`)
-    for (int e = threadIdx.x; e < E; e += THREADS) {
-        int ex = e % EW, ey = e / EW;
-        int gx = tx0 - depth + ex, gy = ty0 - depth + ey;
-        float a = 0.f, b = 0.f, c = 0.f;
-        if (gx >= 0 && gx < dm.x && gy >= 0 && gy < dm.y) {
-            int64_t i = base + (int64_t)gy * dm.x + gx;
-            a = src[i];
-            b = rhs[i];
-            c = inv[i];
+    const int gx = gx0 + 2 * lane;
+    const bool in0 = gx >= 0 && gx < dm.x, in1 = gx + 1 >= 0 && gx + 1 < dm.x;
+    float d0[ROWS], d1[ROWS], r0[ROWS], r1[ROWS], i0[ROWS], i1[ROWS];
+#pragma unroll
+    for (int j = 0; j < ROWS; ++j) {
+        const int gy = gy0 + ROWS * warp + j;
+        d0[j] = d1[j] = r0[j] = r1[j] = i0[j] = i1[j] = 0.f;
+        if (gy >= 0 && gy < dm.y) {
+            const int64_t row = base + (int64_t)gy * dm.x + gx;
+            if (in0) { d0[j] = src[row]; r0[j] = rhs[row]; i0[j] = inv[row]; }
+            if (in1) { d1[j] = src[row + 1]; r1[j] = rhs[row + 1]; i1[j] = inv[row + 1]; }
         }
-        sd[e] = a; sr[e] = b; si[e] = c;
     }
+    edge[warp][0][2 * lane] = d0[0];
+    edge[warp][0][2 * lane + 1] = d1[0];
+    edge[warp][1][2 * lane] = d0[ROWS - 1];
+    edge[warp][1][2 * lane + 1] = d1[ROWS - 1];
     __syncthreads();
-    // half-sweeps: pixels of one colour, at least s rings in from the edge.
-    // Threads take the pixels of the colour directly: row ey holds the
-    // colour at ex = p, p + 2, ... with p fixed by the row's parity.
-    const int HW = EW / 2 + 1;
-    for (int s = 1; s <= depth; ++s) {
-        const int colour = (start_colour + s - 1) & 1;
-        const int rows = EH - 2 * s;
-        for (int e = threadIdx.x; e < rows * HW; e += THREADS) {
-            int ey = s + e / HW;
-            int gy = ty0 - depth + ey;
-            int par = (colour - (tx0 - depth) - gy) & 1;  // ex parity giving (gx + gy) % 2 == colour
-            int ex = par + 2 * (e % HW);
-            if (ex < s || ex >= EW - s) continue;
-            int k = ey * EW + ex;
-            float iv = si[k];
-            if (iv == 0.f) continue;
-            float sum = (sd[k - 1] + sd[k + 1]) + (sd[k - EW] + sd[k + EW]);
-            float old = sd[k];
-            sd[k] = old + om * ((sr[k] + dcoef * sum) * iv - old);
+    // window pixel (ex, ey) has colour (gx0 + gy0 + ex + ey) mod 2 and
+    // gx0 + gy0 and 8 warp are even: in row j the pixel of colour c is the
+    // pair's (c + j) mod 2
+    for (int s = 0; s < nhalf; ++s) {
+        const int c = (start_colour + s) & 1;
+        // the rows just outside this warp's, as the neighbouring warps left them
+        const float ab0 = warp > 0 ? edge[warp - 1][1][2 * lane] : 0.f;
+        const float ab1 = warp > 0 ? edge[warp - 1][1][2 * lane + 1] : 0.f;
+        const float be0 = warp < WARPS - 1 ? edge[warp + 1][0][2 * lane] : 0.f;
+        const float be1 = warp < WARPS - 1 ? edge[warp + 1][0][2 * lane + 1] : 0.f;
+#pragma unroll
+        for (int j = 0; j < ROWS; ++j) {
+            if (((c + j) & 1) == 0) {  // the even column of the pair
+                float left = __shfl_up_sync(0xffffffffu, d1[j], 1);
+                if (lane == 0) left = 0.f;
+                const float up = j > 0 ? d0[j - 1] : ab0, down = j < ROWS - 1 ? d0[j + 1] : be0;
+                const float old = d0[j];
+                d0[j] = old + om * ((r0[j] + dcoef * ((left + d1[j]) + (up + down))) * i0[j] - old);
+            } else {  // the odd column
+                float right = __shfl_down_sync(0xffffffffu, d0[j], 1);
+                if (lane == 31) right = 0.f;
+                const float up = j > 0 ? d1[j - 1] : ab1, down = j < ROWS - 1 ? d1[j + 1] : be1;
+                const float old = d1[j];
+                d1[j] = old + om * ((r1[j] + dcoef * ((d0[j] + right) + (up + down))) * i1[j] - old);
+            }
         }
+        __syncthreads();  // every warp has read the edges of this half-sweep
+        edge[warp][0][2 * lane] = d0[0];
+        edge[warp][0][2 * lane + 1] = d1[0];
+        edge[warp][1][2 * lane] = d0[ROWS - 1];
+        edge[warp][1][2 * lane + 1] = d1[ROWS - 1];
         __syncthreads();
     }
-    // store the interior
-    for (int e = threadIdx.x; e < TX * TY; e += THREADS) {
-        int ix = e % TX, iy = e / TX;
-        int gx = tx0 + ix, gy = ty0 + iy;
-        if (gx < dm.x && gy < dm.y) dst[base + (int64_t)gy * dm.x + gx] = sd[(iy + depth) * EW + ix + depth];
+    // the interior back to global memory
+#pragma unroll
+    for (int j = 0; j < ROWS; ++j) {
+        const int ey = ROWS * warp + j, gy = gy0 + ey;
+        if (ey < DEPTH || ey >= DEPTH + IN || gy >= dm.y) continue;
+        const int64_t row = base + (int64_t)gy * dm.x + gx;
+        const int ex = 2 * lane;
+        if (ex >= DEPTH && ex < DEPTH + IN && gx < dm.x) dst[row] = d0[j];
+        if (ex + 1 >= DEPTH && ex + 1 < DEPTH + IN && gx + 1 < dm.x) dst[row + 1] = d1[j];
     }
 }
 
@@ -118,10 +149,23 @@ __global__ void k_sor32_half(float *__restrict__ dlt, const float *__restrict__ 
     dlt[i] = old + omega[h] * ((rhs[i] + dcoef * sum) * iv - old);
 }
 
+typedef void (*TbKernel)(const float *, float *, const float *, const float *, const int4 *, const int64_t *,
+                         const int32_t *, int, const float *, const int32_t *, int, int, int, float);
+
+TbKernel tb_kernel(int depth) {
+    switch (depth) {
+    case 2: return k_sor32_tb<2>;
+    case 4: return k_sor32_tb<4>;
+    case 6: return k_sor32_tb<6>;
+    default: return k_sor32_tb<8>;
+    }
+}
+
 }  // namespace
 
 int Sor32::init(cw_field_s *f, int d, const std::vector<double> &om) {
-    depth = d < 1 ? 1 : (d > 16 ? 16 : d);
+    depth = d < 1 ? 1 : d;
+    if (depth > 1) depth = depth >= 8 ? 8 : (depth >= 6 ? 6 : (depth >= 4 ? 4 : 2));
     blocked = depth > 1;
     for (uint32_t k = 0; k < f->g.nh; ++k) blocked = blocked && f->g.d[k] == 1;
     std::vector<float> omf(om.begin(), om.end());
@@ -130,18 +174,12 @@ int Sor32::init(cw_field_s *f, int d, const std::vector<double> &om) {
     CW_CUDA(cudaMemcpyAsync(omega, omf.data(), sizeof(float) * omf.size(), cudaMemcpyHostToDevice, stream()));
     std::vector<int64_t> per(f->g.nh);
     if (blocked) {
+        const int in = WIN - 2 * depth;
         for (uint32_t k = 0; k < f->g.nh; ++k)
-            per[k] = (int64_t)((f->g.w[k] + TX - 1) / TX) * ((f->g.h[k] + TY - 1) / TY);
+            per[k] = (int64_t)((f->g.w[k] + in - 1) / in) * ((f->g.h[k] + in - 1) / in);
         rc = tiles.build(per, 1);
-        if (rc == CW_OK) {
-            size_t smem = 3 * sizeof(float) * (TX + 2 * depth) * (TY + 2 * depth);
-            if (cudaFuncSetAttribute(k_sor32_tb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-                cudaSuccess)
-                return fail(CW_ERR_CUDA, "shared memory for the blocked sweep");
-        }
     } else {
-        for (uint32_t k = 0; k < f->g.nh; ++k)
-            per[k] = (int64_t)((f->g.w[k] + 1) / 2) * f->g.h[k] * f->g.d[k];
+        for (uint32_t k = 0; k < f->g.nh; ++k) per[k] = (int64_t)((f->g.w[k] + 1) / 2) * f->g.h[k] * f->g.d[k];
         rc = sites.build(per, 256);
     }
     ping = f->d32a;
@@ -163,15 +201,16 @@ int Sor32::sweeps(cw_field_s *f, int n, const int32_t *done, int done_stride) {
         out = ping;
         return CW_OK;
     }
-    // 2n half-sweeps, `depth` per launch, starting from the zeroed buffer
+    // 2n half-sweeps, `depth` per launch (fewer in the last), starting from
+    // the zeroed buffer; the tiles are those of `depth`, whose window halo is
+    // deep enough for a shorter last launch too
+    TbKernel kern = tb_kernel(depth);
     float *a = ping, *b = pong;
     int remaining = 2 * n, done_half = 0;
     while (remaining > 0) {
         int dd = remaining < depth ? remaining : depth;
-        size_t smem = 3 * sizeof(float) * (TX + 2 * dd) * (TY + 2 * dd);
-        k_sor32_tb<<<tiles.nblocks, THREADS, smem, stream()>>>(a, b, f->r32, f->inv32, f->g.d_dims, f->g.d_off,
-                                                                tiles.d_blk, f->g.nh, omega, done, done_stride, dd,
-                                                                done_half & 1, dcoef);
+        kern<<<tiles.nblocks, 32 * WARPS, 0, stream()>>>(a, b, f->r32, f->inv32, f->g.d_dims, f->g.d_off, tiles.d_blk,
+                                                         f->g.nh, omega, done, done_stride, dd, done_half & 1, dcoef);
         CW_LAUNCHED();
         remaining -= dd;
         done_half += dd;

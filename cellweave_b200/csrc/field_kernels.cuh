@@ -19,6 +19,16 @@ struct FieldView {
 FieldView view(cw_field_s *f);
 int field_hold_bath_device(cw_field_s *f, const uint8_t *d_open, int hist, double value);
 
+// The source side of a pixel's balance after `t` (d*sum or d*lap - decay*c):
+// t + source + production - uptake, added in the reference's order
+// (pde.rs:393-394, 717-718); an absent array is an exact zero.
+__device__ __forceinline__ double add_sources(const FieldView &fv, int64_t i, double t) {
+    t = t + fv.source;
+    if (fv.pr) t = t + fv.pr[i];
+    if (fv.up) t = t - fv.up[i];
+    return t;
+}
+
 // Neighbour sum and count of real neighbours in the reference's order:
 // x-1, x+1, y-1, y+1, z-1, z+1 (pde.rs:361-390).
 __device__ __forceinline__ void pixel_sums64(const double *__restrict__ c, int64_t i, int x, int y, int z, int4 dm,

@@ -11,6 +11,7 @@
 // lattice takes `sweeps` Monte Carlo steps.  Division, vessels, immune cells
 // and the rest of the reference's biology are not part of this path.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstring>
 #include <random>
@@ -37,7 +38,23 @@ struct cw_sim_s {
     Plan sites;
     std::vector<cw_relax_stats> last;
     uint32_t steps = 0;
+    // autotuner: relaxation factor per history and field, blocking depth
+    struct Tune {
+        bool active = false;
+        int steps = 0, done = 0;
+        std::vector<double> cand;
+        std::vector<int> cls, rank;             // class of each history, its index within the class
+        int nclass = 0;
+        std::vector<double> sum[2], cnt[2];     // [field][class * ncand + candidate]
+    } tune;
+    std::vector<double> omega[2];               // per history, per field
+    int32_t depth = 8;
+    bool depth_tuned = false;
 };
+
+extern "C" {
+static void tune_begin(cw_sim_s *s);
+}
 
 namespace {
 
@@ -278,6 +295,11 @@ int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out) {
     for (uint32_t k = 0; k < c.nh; ++k) per[k] = (int64_t)s->w[k] * s->h[k] * s->d[k];
     if ((rc = s->sites.build(per, T)) != CW_OK) { cw_sim_destroy(s); return rc; }
     s->last.assign(c.nh, cw_relax_stats{});
+    // relaxation factors: the configuration's, or the reference's rule
+    // until the autotuner has chosen one per lattice size
+    for (int f = 0; f < 2; ++f) s->omega[f].assign(c.nh, 0.0);
+    if (c.omega <= 0.0 && c.precision == CW_FP32_DC) tune_begin(s);
+    else s->depth_tuned = true;
     (void)survival;
     CW_CUDA(cudaStreamSynchronize(stream()));
     *out = s;
@@ -296,6 +318,87 @@ int cw_sim_destroy(cw_sim s) {
     return CW_OK;
 }
 
+// The autotuner: while it runs, the histories of one lattice size share the
+// candidate factors among them (history q of a size class takes candidate
+// (q + step) mod n), and each solve's sweep count is booked against its
+// candidate; afterwards every history takes its class's best factor.
+static void tune_begin(cw_sim_s *s) {
+    auto &t = s->tune;
+    t.cand = {1.80, 1.85, 1.88, 1.90, 1.92, 1.94, 1.96};
+    uint32_t nh = s->cfg.nh;
+    t.cls.assign(nh, 0);
+    t.rank.assign(nh, 0);
+    std::vector<std::array<uint32_t, 3>> keys;
+    std::vector<int> members;
+    for (uint32_t k = 0; k < nh; ++k) {
+        std::array<uint32_t, 3> key{s->w[k], s->h[k], s->d[k]};
+        size_t c = std::find(keys.begin(), keys.end(), key) - keys.begin();
+        if (c == keys.size()) { keys.push_back(key); members.push_back(0); }
+        t.cls[k] = (int)c;
+        t.rank[k] = members[c]++;
+    }
+    t.nclass = (int)keys.size();
+    int smallest = *std::min_element(members.begin(), members.end());
+    int n = (int)t.cand.size();
+    t.steps = std::max(2, (n + smallest - 1) / smallest);
+    for (int f = 0; f < 2; ++f) { t.sum[f].assign(t.nclass * n, 0.0); t.cnt[f].assign(t.nclass * n, 0.0); }
+    t.active = true;
+    t.done = 0;
+}
+
+static void tune_assign(cw_sim_s *s) {
+    auto &t = s->tune;
+    int n = (int)t.cand.size();
+    for (int f = 0; f < 2; ++f)
+        for (uint32_t k = 0; k < s->cfg.nh; ++k) s->omega[f][k] = t.cand[(t.rank[k] + t.done) % n];
+}
+
+static void tune_book(cw_sim_s *s, int f, const std::vector<cw_relax_stats> &st) {
+    auto &t = s->tune;
+    int n = (int)t.cand.size();
+    for (uint32_t k = 0; k < s->cfg.nh; ++k) {
+        int c = (t.rank[k] + t.done) % n;
+        t.sum[f][t.cls[k] * n + c] += (double)st[k].sweeps;
+        t.cnt[f][t.cls[k] * n + c] += 1.0;
+    }
+}
+
+static void tune_finish(cw_sim_s *s) {
+    auto &t = s->tune;
+    int n = (int)t.cand.size();
+    for (int f = 0; f < 2; ++f)
+        for (uint32_t k = 0; k < s->cfg.nh; ++k) {
+            int best = -1;
+            double bv = 0.0;
+            for (int c = 0; c < n; ++c) {
+                double cnt = t.cnt[f][t.cls[k] * n + c];
+                if (cnt <= 0) continue;
+                double v = t.sum[f][t.cls[k] * n + c] / cnt;
+                if (best < 0 || v < bv) { best = c; bv = v; }
+            }
+            if (best >= 0) s->omega[f][k] = t.cand[best];
+        }
+    t.active = false;
+}
+
+// Blocking depth: the fastest of the candidates on the oxygen field's
+// current residual.
+static int tune_depth(cw_sim_s *s) {
+    if (s->cfg.precision != CW_FP32_DC) return CW_OK;
+    float best = 0.f;
+    int bd = 8;
+    for (int d : {4, 6, 8}) {
+        float ms = 0.f;
+        int64_t launches = 0;
+        int rc = cw_field_time_inner(s->o2, 8, d, 1.9, &ms, &launches);
+        if (rc != CW_OK) return rc;
+        if (best == 0.f || ms < best) { best = ms; bd = d; }
+    }
+    s->depth = bd;
+    s->depth_tuned = true;
+    return CW_OK;
+}
+
 int cw_sim_step(cw_sim s, uint32_t nsteps) {
     const cw_sim_config &c = s->cfg;
     int64_t nc = s->nc;
@@ -310,6 +413,9 @@ int cw_sim_step(cw_sim s, uint32_t nsteps) {
     int rc;
     for (uint32_t step = 0; step < nsteps; ++step, ++s->steps) {
         bool solve = c.relax_every <= 1 || (s->steps % (uint32_t)c.relax_every) == 0;
+        o.block_depth = s->depth;
+        bool tuning = solve && s->tune.active && s->steps > 0;  // the first solve starts from scratch: not booked
+        if (tuning) tune_assign(s);
         if (solve) {
             // 1. downward coupling and the oxygen solve
             if ((rc = couple_uptake_device(s->o2, s->lat, s->d_sink, 8, s->o2->lin_sink, s->sites)) != CW_OK) return rc;
@@ -317,7 +423,10 @@ int cw_sim_step(cw_sim s, uint32_t nsteps) {
                 (rc = couple_background_device(s->o2, s->lat, c.o2_background_sink, s->o2->lin_sink)) != CW_OK)
                 return rc;
             s->o2->lin_sink_on = true;
-            if ((rc = cw_field_relax(s->o2, &o, s->last.data())) != CW_OK) return rc;
+            const double *om = c.omega > 0.0 ? nullptr : s->omega[0].data();
+            if ((rc = field_relax(s->o2, &o, om, s->last.data())) != CW_OK) return rc;
+            if (tuning) tune_book(s, 0, s->last);
+            if (!s->depth_tuned && (rc = tune_depth(s)) != CW_OK) return rc;
         }
         // 2. what each cell sits in
         if ((rc = couple_means_device(s->o2, s->lat, s->sum, s->count, s->cell_o2, s->sites)) != CW_OK) return rc;
@@ -330,7 +439,9 @@ int cw_sim_step(cw_sim s, uint32_t nsteps) {
             CW_LAUNCHED();
             if ((rc = couple_production_device(s->sig, s->lat, s->secretion, s->sites)) != CW_OK) return rc;
             std::vector<cw_relax_stats> st2(c.nh);
-            if ((rc = cw_field_relax(s->sig, &o, st2.data())) != CW_OK) return rc;
+            const double *om = c.omega > 0.0 ? nullptr : s->omega[1].data();
+            if ((rc = field_relax(s->sig, &o, om, st2.data())) != CW_OK) return rc;
+            if (tuning) tune_book(s, 1, st2);
             if ((rc = couple_means_device(s->sig, s->lat, s->sum, s->count, s->cell_sig, s->sites)) != CW_OK)
                 return rc;
         }
@@ -346,8 +457,19 @@ int cw_sim_step(cw_sim s, uint32_t nsteps) {
         // 5. the lattice
         for (int k = 0; k < c.sweeps; ++k)
             if ((rc = lattice_sweep(s->lat)) != CW_OK) return rc;
+        if (tuning && ++s->tune.done >= s->tune.steps) tune_finish(s);
         (void)S;
     }
+    return CW_OK;
+}
+
+int cw_sim_tuning(cw_sim s, double *omega_o2, double *omega_signal, int32_t *depth, int32_t *tuning) {
+    for (uint32_t k = 0; k < s->cfg.nh; ++k) {
+        if (omega_o2) omega_o2[k] = s->omega[0][k];
+        if (omega_signal) omega_signal[k] = s->omega[1][k];
+    }
+    if (depth) *depth = s->depth;
+    if (tuning) *tuning = s->tune.active ? 1 : 0;
     return CW_OK;
 }
 

@@ -26,6 +26,11 @@ STOP_MAX_CHANGE, STOP_RESIDUAL = 0, 1
 VALUES, UPTAKE, PRODUCTION, LIN_SINK = 0, 1, 2, 3
 
 
+def _check_hist(obj, hist):
+    if not 0 <= hist < len(obj.dims):
+        raise _lib.NotFoundError(f"no history {hist}")
+
+
 def _dims(dims):
     dims = [tuple(int(v) for v in (tuple(d) + (1,))[:3]) if len(d) < 3 else tuple(int(v) for v in d) for d in dims]
     w = np.array([d[0] for d in dims], np.uint32)
@@ -67,6 +72,7 @@ class ScalarField:
         return self._h
 
     def n(self, hist=0):
+        _check_hist(self, hist)
         w, h, d = self.dims[hist]
         return w * h * d
 
@@ -213,6 +219,7 @@ class CpmLattice:
         return self._h
 
     def n(self, hist=0):
+        _check_hist(self, hist)
         w, h, d = self.dims[hist]
         return w * h * d
 
@@ -514,6 +521,14 @@ class Simulation:
 
     def step(self, n=1):
         call("cw_sim_step", self._h, int(n))
+
+    def tuning(self):
+        """What the autotuner chose: factors per history (oxygen, signal), blocking depth, still tuning."""
+        n = len(self.dims)
+        a, b = np.zeros(n), np.zeros(n)
+        depth, active = C.c_int32(), C.c_int32()
+        call("cw_sim_tuning", self._h, ptr(a), ptr(b), C.byref(depth), C.byref(active))
+        return dict(omega_o2=a, omega_signal=b, depth=depth.value, tuning=bool(active.value))
 
     def stats(self):
         out = np.empty((len(self.dims), 4))

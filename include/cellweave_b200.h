@@ -270,6 +270,11 @@ int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out);
 int cw_sim_destroy(cw_sim sim);
 /* `steps` lattice steps on every history. */
 int cw_sim_step(cw_sim sim, uint32_t steps);
+/* What the autotuner chose: the SOR relaxation factor of every history for
+ * the oxygen and the signal field (0 until chosen: the reference's rule),
+ * the FP32 blocking depth, and whether it is still trying candidates.  It
+ * runs when cfg.omega <= 0 with CW_FP32_DC, over the first few steps. */
+int cw_sim_tuning(cw_sim sim, double *omega_o2, double *omega_signal, int32_t *depth, int32_t *tuning);
 /* Handles the driver owns, for inspection with the calls above. */
 int cw_sim_lattice(cw_sim sim, cw_lattice *lat);
 int cw_sim_field(cw_sim sim, int32_t which, cw_field *f);

@@ -118,7 +118,8 @@ def test_sweeps_are_bit_exact_in_a_volume_with_surfaces(order):
     o.mcs_checkerboard(99, 0, 12)
     g.monte_carlo_step(12)
     np.testing.assert_array_equal(g.grid().reshape(-1), o.grid)
-    np.testing.assert_array_equal(g.cells()["volume"], o.volume)
+    # the medium's count (index 0) is untracked by the device, as by the reference
+    np.testing.assert_array_equal(g.cells()["volume"][1:], o.volume[1:])
     np.testing.assert_array_equal(g.surfaces(), o.surface)
     assert g.records_match_grid()
 
