@@ -120,6 +120,7 @@ SIGNATURES = {
     "cw_field_residual": (C.c_int, [P, P]),
     "cw_field_inflow": (C.c_int, [P, P]),
     "cw_field_step": (C.c_int, [P, D]),
+    "cw_field_relax_noalloc": (C.c_int, [P, P, P, P, P, U32, U32, D, D, D, D, D, I64, I32, P, P]),
     "cw_field_time_inner": (C.c_int, [P, I32, I32, D, P, P]),
     "cw_couple_uptake": (C.c_int, [P, P, I32, P, I32]),
     "cw_couple_background_uptake": (C.c_int, [P, P, D]),

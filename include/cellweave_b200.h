@@ -163,6 +163,24 @@ typedef struct {
 /* relax (pde.rs:245-288) on every history; stats has nh entries (may be
  * NULL).  Returns CW_ERR_SIMULATION when any history failed to settle. */
 int cw_field_relax(cw_field f, const cw_relax_opts *opts, cw_relax_stats *stats);
+/* No counterpart in the reference: the FP32 defect-correction relax of one
+ * flat field (width x height <= 1,048,576 pixels) that allocates no device
+ * memory, for callers whose device memory belongs to another allocator (a
+ * framework's caching pool, an arena sized at start-up) or whose loop cannot
+ * afford the device-wide stall of cudaMalloc/cudaFree.  The caller passes
+ * device pointers it owns: values (w*h doubles, relaxed in place), the held
+ * mask (w*h bytes), and the first-order sink, uptake and production (w*h
+ * doubles each, or NULL for zero).  The solve's scratch is a fixed array of
+ * about 16 MiB inside the library, which every GPU that loads it keeps until
+ * exit; its device address is looked up on the first call made on each
+ * device.  All calls share that array, so calls whose work overlaps on the
+ * GPU (two streams, two threads) race: serialise them.  Larger fields return
+ * CW_ERR_CONFIG; a field that does not settle within max_sweeps returns
+ * CW_ERR_SIMULATION.  omega <= 0 takes the reference's rule. */
+int cw_field_relax_noalloc(double *values, const uint8_t *held, const double *lin_sink, const double *uptake,
+                           const double *production, uint32_t width, uint32_t height, double dcoef, double decay,
+                           double source, double omega, double tolerance, int64_t max_sweeps, int32_t inner_sweeps,
+                           int64_t *sweeps_out, double *residual_out);
 /* The projected residual max |b - A c| of every history (nh entries). */
 int cw_field_residual(cw_field f, double *out);
 /* inflow (pde.rs:415-456) of every history (nh entries). */
