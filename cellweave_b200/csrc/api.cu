@@ -42,6 +42,8 @@ int Geom::init(uint32_t n, const uint32_t *W, const uint32_t *H, const uint32_t 
         if (a == 0 || b == 0 || c == 0 || a > 65535 || b > 65535 || c > 65535)
             return fail(CW_ERR_CONFIG, "invalid grid dimensions (" + std::to_string(a) + "x" + std::to_string(b) +
                                            "x" + std::to_string(c) + ") of history " + std::to_string(k));
+        if ((uint64_t)a * b * c >= (1ull << 31))
+            return fail(CW_ERR_CONFIG, "history " + std::to_string(k) + " has 2^31 pixels or more");
         w[k] = (int32_t)a; h[k] = (int32_t)b; d[k] = (int32_t)c;
         off[k + 1] = off[k] + (int64_t)a * b * c;
         dims[k] = make_int4((int)a, (int)b, (int)c, 0);

@@ -36,11 +36,13 @@ struct RelaxState {
     int64_t inner;                // FP32 sweeps taken (defect correction)
 };
 
+// (a history holds fewer than 2^31 pixels: 32-bit division is enough)
 __device__ __forceinline__ void locate(const int4 dm, int64_t local, int &x, int &y, int &z) {
-    x = (int)(local % dm.x);
-    int64_t r = local / dm.x;
-    y = (int)(r % dm.y);
-    z = (int)(r / dm.y);
+    const uint32_t l = (uint32_t)local, w = (uint32_t)dm.x, h = (uint32_t)dm.y;
+    const uint32_t r = l / w;
+    x = (int)(l - r * w);
+    y = (int)(r % h);
+    z = (int)(r / h);
 }
 
 // The box around every free pixel (free_span, pde.rs:305-320).
@@ -178,19 +180,59 @@ __global__ void k_check(RelaxState *st, int nh, int64_t index, int residual_coun
     s.resid = 0ull;
 }
 
-// Defect correction: c += d on free pixels, floored at zero as the
-// reference's update is (pde.rs:395).
-__global__ void k_dc_correct(FieldView fv, const int32_t *blk, int nh, const RelaxState *st, const float *dlt) {
+// Defect correction fused with the next residual, in two launches, one per
+// colour: c += d (floored at zero as the reference's update is, pde.rs:395),
+// then r = b - A c at the corrected field, written in FP32 for the next FP32
+// solve, with the correction zeroed behind it.  The first launch corrects the
+// red pixels and reads its black neighbours as c + d; the second corrects the
+// black ones and reads its red neighbours as they now stand, so no thread
+// reads a value another thread of the same launch writes.  One block takes
+// 512 consecutive pixels of one row, a thread the pair (2t, 2t+1): one
+// pixel of each colour.
+__global__ void __launch_bounds__(256) k_dc_update(FieldView fv, const int32_t *blk, int nh, RelaxState *st,
+                                                   float *dlt, float *r32, int colour) {
     __shared__ int s_h;
     if (threadIdx.x == 0) s_h = plan_history(blk, nh, blockIdx.x);
     __syncthreads();
-    int h = s_h;
+    const int h = s_h;
     if (st[h].done) return;
-    int64_t local = (int64_t)(blockIdx.x - blk[h]) * blockDim.x + threadIdx.x;
-    if (local >= fv.off[h + 1] - fv.off[h]) return;
-    int64_t i = fv.off[h] + local;
-    if (fv.held[i]) return;
-    fv.c[i] = fmax(fv.c[i] + (double)dlt[i], 0.0);
+    const int4 dm = fv.dims[h];
+    const uint32_t segs = ((uint32_t)dm.x + 511u) / 512u;
+    const uint32_t lb = blockIdx.x - blk[h];
+    const uint32_t row = lb / segs, seg = lb - row * segs;
+    const int y = (int)(row % (uint32_t)dm.y), z = (int)(row / (uint32_t)dm.y);
+    const int x = (int)seg * 512 + 2 * (int)threadIdx.x + ((colour + y + z) & 1);
+    double worst = 0.0;
+    if (x < dm.x) {
+        const int64_t w = dm.x, slice = (int64_t)dm.x * dm.y;
+        const int64_t i = fv.off[h] + (int64_t)row * w + x;
+        if (!fv.held[i]) {
+            const bool red = colour == 0;
+            auto nb = [&](int64_t j) -> double {
+                double cj = fv.c[j];
+                if (red && !fv.held[j]) cj = fmax(cj + (double)dlt[j], 0.0);
+                return cj;
+            };
+            const double ci = fmax(fv.c[i] + (double)dlt[i], 0.0);
+            double sum = 0.0, real = 0.0;
+            if (x > 0) { sum += nb(i - 1); real += 1.0; }
+            if (x + 1 < dm.x) { sum += nb(i + 1); real += 1.0; }
+            if (y > 0) { sum += nb(i - w); real += 1.0; }
+            if (y + 1 < dm.y) { sum += nb(i + w); real += 1.0; }
+            if (z > 0) { sum += nb(i - slice); real += 1.0; }
+            if (z + 1 < dm.z) { sum += nb(i + slice); real += 1.0; }
+            double den = real * fv.d + fv.decay;
+            if (fv.ks) den = den + fv.ks[i];
+            double r = add_sources(fv, i, fv.d * sum) - den * ci;
+            if (ci <= 0.0 && r < 0.0) r = 0.0;
+            worst = fabs(r);
+            fv.c[i] = ci;
+            r32[i] = (float)r;
+            dlt[i] = 0.f;
+        }
+    }
+    worst = warp_max(worst);
+    if ((threadIdx.x & 31) == 0 && worst > 0.0) atomic_max_nonneg(&st[h].resid, worst);
 }
 
 __global__ void k_dc_check(RelaxState *st, int nh, int inner, int64_t max_sweeps) {
@@ -480,8 +522,13 @@ static int relax_fp32dc(cw_field_s *f, const cw_relax_opts &o, RelaxState *d_st,
     int rc = f->alloc_fp32();
     if (rc != CW_OK) return rc;
     FieldView fv = view(f);
-    Plan ps;
+    Plan ps, pr;
     if ((rc = site_plan(f, ps)) != CW_OK) return rc;
+    {
+        std::vector<int64_t> per(nh);
+        for (uint32_t k = 0; k < nh; ++k) per[k] = (int64_t)f->g.h[k] * f->g.d[k] * ((f->g.w[k] + 511) / 512);
+        if ((rc = pr.build(per, 1)) != CW_OK) return rc;
+    }
     int inner = o.inner_sweeps > 0 ? o.inner_sweeps : 16;
     int depth = o.block_depth > 0 ? o.block_depth : 4;
     Sor32 solver;
@@ -493,16 +540,22 @@ static int relax_fp32dc(cw_field_s *f, const cw_relax_opts &o, RelaxState *d_st,
     int64_t max_outer = o.max_sweeps / inner + 2;
     std::vector<int32_t> flags(nh);
     int queue = 2;
+    // the first residual also sets the inverse diagonal and zeroes d32a
+    k_residual64<<<ps.nblocks, T, 0, stream()>>>(fv, ps.d_blk, nh, d_st, f->r32, f->inv32, f->d32a, 1);
+    CW_LAUNCHED();
+    float *start = f->d32a;
+    const int stride = (int)(sizeof(RelaxState) / sizeof(int32_t));
     while (outer < max_outer) {
         for (int q = 0; q < queue && outer < max_outer; ++q, ++outer) {
-            k_residual64<<<ps.nblocks, T, 0, stream()>>>(fv, ps.d_blk, nh, d_st, f->r32, outer == 0 ? f->inv32 : nullptr,
-                                                         f->d32a, 1);
-            CW_LAUNCHED();
             k_dc_check<<<(nh + 63) / 64, 64, 0, stream()>>>(d_st, nh, inner, o.max_sweeps);
             CW_LAUNCHED();
-            if ((rc = solver.sweeps(f, inner, done_ptr, (int)(sizeof(RelaxState) / sizeof(int32_t)))) != CW_OK) return rc;
-            k_dc_correct<<<ps.nblocks, T, 0, stream()>>>(fv, ps.d_blk, nh, d_st, solver.result());
-            CW_LAUNCHED();
+            if ((rc = solver.sweeps(f, inner, done_ptr, stride, start)) != CW_OK) return rc;
+            float *d = solver.result();
+            for (int colour = 0; colour < 2; ++colour) {
+                k_dc_update<<<pr.nblocks, 256, 0, stream()>>>(fv, pr.d_blk, nh, d_st, d, f->r32, colour);
+                CW_LAUNCHED();
+            }
+            start = d;  // zeroed behind the update
         }
         CW_CUDA(cudaMemcpyAsync(hs.data(), d_st, sizeof(RelaxState) * nh, cudaMemcpyDeviceToHost, stream()));
         CW_CUDA(cudaStreamSynchronize(stream()));
@@ -513,6 +566,7 @@ static int relax_fp32dc(cw_field_s *f, const cw_relax_opts &o, RelaxState *d_st,
     }
     solver.release();
     ps.release();
+    pr.release();
     return CW_OK;
 }
 

@@ -188,8 +188,12 @@ int Sor32::init(cw_field_s *f, int d, const std::vector<double> &om) {
     return rc;
 }
 
-int Sor32::sweeps(cw_field_s *f, int n, const int32_t *done, int done_stride) {
+int Sor32::sweeps(cw_field_s *f, int n, const int32_t *done, int done_stride, float *start) {
     float dcoef = (float)f->dcoef;
+    if (start) {  // begin from this (zeroed) buffer; the other is scratch
+        ping = start;
+        pong = start == f->d32a ? f->d32b : f->d32a;
+    }
     if (!blocked) {
         for (int s = 0; s < n; ++s)
             for (int colour = 0; colour < 2; ++colour) {

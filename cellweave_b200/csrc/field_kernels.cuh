@@ -57,7 +57,7 @@ struct Sor32 {
     float *omega = nullptr;
     float *ping = nullptr, *pong = nullptr, *out = nullptr;
     int init(cw_field_s *f, int depth, const std::vector<double> &omega_per_history);
-    int sweeps(cw_field_s *f, int n, const int32_t *done, int done_stride);
+    int sweeps(cw_field_s *f, int n, const int32_t *done, int done_stride, float *start = nullptr);
     float *result() const { return out; }
     void release();
 };

@@ -180,23 +180,24 @@ __global__ void k_colour_order(const uint2 *keys, int nh, int ncol, uint32_t *mc
 }
 
 // The pixel of colour `colour` with index k in history dims dm; false past the end.
-__device__ __forceinline__ bool colour_site(int4 dm, int period, int colour, int64_t k, int &x, int &y, int &z) {
+// (32-bit index arithmetic: a history holds fewer than 2^32 pixels.)
+__device__ __forceinline__ bool colour_site(int4 dm, int period, int colour, uint32_t k, int &x, int &y, int &z) {
     if (period == 0) {
-        int hw = (dm.x + 1) >> 1;
-        int64_t row = k / hw;
-        if (row >= (int64_t)dm.y * dm.z) return false;
-        y = (int)(row % dm.y);
-        z = (int)(row / dm.y);
+        const uint32_t hw = ((uint32_t)dm.x + 1u) >> 1;
+        const uint32_t row = k / hw;
+        if (row >= (uint32_t)dm.y * (uint32_t)dm.z) return false;
+        y = (int)(row % (uint32_t)dm.y);
+        z = (int)(row / (uint32_t)dm.y);
         x = ((colour - y - z) & 1) + 2 * (int)(k - row * hw);
         return x < dm.x;
     }
     int cx = colour % period, cy = (colour / period) % period, cz = colour / (period * period);
-    int nx = dm.x > cx ? (dm.x - cx + period - 1) / period : 0;
-    int ny = dm.y > cy ? (dm.y - cy + period - 1) / period : 0;
-    int nz = dm.z > cz ? (dm.z - cz + period - 1) / period : 0;
-    if (k >= (int64_t)nx * ny * nz) return false;
+    uint32_t nx = dm.x > cx ? (dm.x - cx + period - 1) / period : 0;
+    uint32_t ny = dm.y > cy ? (dm.y - cy + period - 1) / period : 0;
+    uint32_t nz = dm.z > cz ? (dm.z - cz + period - 1) / period : 0;
+    if (nx == 0 || ny == 0 || k >= nx * ny * nz) return false;
     int ix = (int)(k % nx);
-    int64_t r = k / nx;
+    uint32_t r = k / nx;
     int iy = (int)(r % ny), iz = (int)(r / ny);
     x = cx + period * ix;
     y = cy + period * iy;
@@ -217,7 +218,7 @@ __global__ void __launch_bounds__(T) k_cpm_pass(LatView L, Tables tabs, const in
     const int h = s_h;
     const int4 dm = L.dims[h];
     const int colour = perm[h * L.ncol + pass];
-    const int64_t k = (int64_t)(blockIdx.x - blk[h]) * blockDim.x + threadIdx.x;
+    const uint32_t k = (uint32_t)(blockIdx.x - blk[h]) * blockDim.x + threadIdx.x;
     const int64_t c0 = L.cell_off[h], cap = L.cell_off[h + 1] - c0;
     int32_t *g = L.grid + L.off[h];
     const int32_t *type_h = L.type + c0;
