@@ -71,7 +71,7 @@ class SimConfig(C.Structure):
                 ("o2_sink_by_type", C.c_void_p), ("o2_background_sink", C.c_double), ("o2_hold", C.c_int32), ("signal_dcoef", C.c_double),
                 ("signal_decay", C.c_double), ("signal_secretion", C.c_double), ("hypoxic_level", C.c_double),
                 ("tolerance", C.c_double), ("precision", C.c_int32), ("omega", C.c_double),
-                ("relax_every", C.c_int32), ("dt", C.c_double), ("substeps", C.c_int32), ("sweeps", C.c_int32),
+                ("inner_sweeps", C.c_int32), ("relax_every", C.c_int32), ("dt", C.c_double), ("substeps", C.c_int32), ("sweeps", C.c_int32),
                 ("death_threshold", C.c_double), ("necrotic_type", C.c_int32)]
 
 

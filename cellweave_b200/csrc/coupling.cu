@@ -97,15 +97,30 @@ __global__ void k_cell_sums(Pair p, const int32_t *blk, int nh, const double *c,
         int32_t id = p.grid[i];
         if (id > 0 && id < cap) { key = c0 + id; v = c[i]; }
     }
-    unsigned peers = __match_any_sync(0xffffffffu, key);
-    int lane = threadIdx.x & 31;
-    int leader = __ffs(peers) - 1;
-    // sum over the peers, in lane order
-    double s = 0.0;
-    for (unsigned m = peers; m; m &= m - 1) s += __shfl_sync(peers, v, __ffs(m) - 1);
-    if (key >= 0 && lane == leader) {
+    // Cells are compact, so a warp's 32 consecutive pixels hold a few runs of
+    // one id: a segmented inclusive scan along the warp gives each run's sum
+    // and length at its last lane, which alone touches global memory.
+    const int lane = threadIdx.x & 31;
+    if (!__any_sync(0xffffffffu, key >= 0)) return;
+    const long long prev = __shfl_up_sync(0xffffffffu, key, 1);
+    const bool head = lane == 0 || prev != key;
+    unsigned heads = __ballot_sync(0xffffffffu, head);
+    // distance back to this lane's run head
+    const unsigned below = heads & ((2u << lane) - 1u);
+    const int start = 31 - __clz(below);
+    double s = v;
+    int n = 1;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        double sv = __shfl_up_sync(0xffffffffu, s, o);
+        int nv = __shfl_up_sync(0xffffffffu, n, o);
+        if (lane - o >= start) { s += sv; n += nv; }
+    }
+    const long long next = __shfl_down_sync(0xffffffffu, key, 1);
+    const bool tail = lane == 31 || next != key;
+    if (key >= 0 && tail) {
         atomicAdd(sum + key, s);
-        atomicAdd(count + key, __popc(peers));
+        atomicAdd(count + key, n);
     }
 }
 

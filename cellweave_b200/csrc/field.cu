@@ -133,13 +133,15 @@ __global__ void k_residual64(FieldView fv, const int32_t *blk, int nh, RelaxStat
     int h = s_h;
     if (skip_done && st[h].done) return;
     const int4 dm = fv.dims[h];
-    int64_t local = (int64_t)(blockIdx.x - blk[h]) * blockDim.x + threadIdx.x;
-    int64_t n = fv.off[h + 1] - fv.off[h];
+    // one block: 256 consecutive pixels of one row
+    const uint32_t segs = ((uint32_t)dm.x + 255u) / 256u;
+    const uint32_t lb = blockIdx.x - blk[h];
+    const uint32_t row = lb / segs;
+    const int x = (int)((lb - row * segs) * 256u + threadIdx.x);
+    const int y = (int)(row % (uint32_t)dm.y), z = (int)(row / (uint32_t)dm.y);
     double worst = 0.0;
-    if (local < n) {
-        int64_t i = fv.off[h] + local;
-        int x, y, z;
-        locate(dm, local, x, y, z);
+    if (x < dm.x) {
+        int64_t i = fv.off[h] + (int64_t)row * dm.x + x;
         float r_out = 0.0f, inv_out = 0.0f;
         if (!fv.held[i]) {
             double sum, real;
@@ -422,6 +424,13 @@ FieldView view(cw_field_s *f) {
     return v;
 }
 
+// One block per 256 consecutive pixels of a row (k_residual64's mapping).
+static int row_plan(cw_field_s *f, Plan &p) {
+    std::vector<int64_t> per(f->g.nh);
+    for (uint32_t k = 0; k < f->g.nh; ++k) per[k] = (int64_t)f->g.h[k] * f->g.d[k] * ((f->g.w[k] + 255) / 256);
+    return p.build(per, 1);
+}
+
 static int site_plan(cw_field_s *f, Plan &p) {
     std::vector<int64_t> per(f->g.nh);
     for (uint32_t k = 0; k < f->g.nh; ++k) per[k] = f->g.sites(k);
@@ -486,6 +495,8 @@ static int relax_fp64(cw_field_s *f, const cw_relax_opts &o, std::vector<Span> &
     }
     int rc = site_plan(f, ps);
     if (rc != CW_OK) return rc;
+    Plan prow;
+    if ((rc = row_plan(f, prow)) != CW_OK) return rc;
     bool resid = o.stop == CW_STOP_RESIDUAL;
     int64_t done_sweeps = 0, chunk = 8;
     std::vector<int32_t> flags(nh);
@@ -499,7 +510,7 @@ static int relax_fp64(cw_field_s *f, const cw_relax_opts &o, std::vector<Span> &
                 CW_LAUNCHED();
             }
             if (resid) {
-                k_residual64<<<ps.nblocks, T, 0, stream()>>>(fv, ps.d_blk, nh, d_st, nullptr, nullptr, nullptr, 1);
+                k_residual64<<<prow.nblocks, T, 0, stream()>>>(fv, prow.d_blk, nh, d_st, nullptr, nullptr, nullptr, 1);
                 CW_LAUNCHED();
             }
             k_check<<<(nh + 63) / 64, 64, 0, stream()>>>(d_st, nh, done_sweeps + s + 1, resid ? 1 : 0);
@@ -513,7 +524,7 @@ static int relax_fp64(cw_field_s *f, const cw_relax_opts &o, std::vector<Span> &
         if (all) break;
         chunk = std::min<int64_t>(chunk * 2, 256);
     }
-    pc[0].release(); pc[1].release(); ps.release();
+    pc[0].release(); pc[1].release(); ps.release(); prow.release();
     return CW_OK;
 }
 
@@ -522,8 +533,9 @@ static int relax_fp32dc(cw_field_s *f, const cw_relax_opts &o, RelaxState *d_st,
     int rc = f->alloc_fp32();
     if (rc != CW_OK) return rc;
     FieldView fv = view(f);
-    Plan ps, pr;
+    Plan ps, pr, prow;
     if ((rc = site_plan(f, ps)) != CW_OK) return rc;
+    if ((rc = row_plan(f, prow)) != CW_OK) return rc;
     {
         std::vector<int64_t> per(nh);
         for (uint32_t k = 0; k < nh; ++k) per[k] = (int64_t)f->g.h[k] * f->g.d[k] * ((f->g.w[k] + 511) / 512);
@@ -541,7 +553,7 @@ static int relax_fp32dc(cw_field_s *f, const cw_relax_opts &o, RelaxState *d_st,
     std::vector<int32_t> flags(nh);
     int queue = 2;
     // the first residual also sets the inverse diagonal and zeroes d32a
-    k_residual64<<<ps.nblocks, T, 0, stream()>>>(fv, ps.d_blk, nh, d_st, f->r32, f->inv32, f->d32a, 1);
+    k_residual64<<<prow.nblocks, T, 0, stream()>>>(fv, prow.d_blk, nh, d_st, f->r32, f->inv32, f->d32a, 1);
     CW_LAUNCHED();
     float *start = f->d32a;
     const int stride = (int)(sizeof(RelaxState) / sizeof(int32_t));
@@ -567,6 +579,7 @@ static int relax_fp32dc(cw_field_s *f, const cw_relax_opts &o, RelaxState *d_st,
     solver.release();
     ps.release();
     pr.release();
+    prow.release();
     return CW_OK;
 }
 
@@ -785,15 +798,15 @@ int cw_field_residual(cw_field f, double *out) {
     CW_CUDA(cudaStreamSynchronize(stream()));
     for (auto &s : hs) { s.resid = 0ull; s.done = 0; }
     CW_CUDA(cudaMemcpyAsync(d_st, hs.data(), sizeof(RelaxState) * nh, cudaMemcpyHostToDevice, stream()));
-    Plan ps;
-    int rc = site_plan(f, ps);
+    Plan prow;
+    int rc = row_plan(f, prow);
     if (rc != CW_OK) return rc;
-    k_residual64<<<ps.nblocks, T, 0, stream()>>>(view(f), ps.d_blk, nh, d_st, nullptr, nullptr, nullptr, 0);
+    k_residual64<<<prow.nblocks, T, 0, stream()>>>(view(f), prow.d_blk, nh, d_st, nullptr, nullptr, nullptr, 0);
     CW_LAUNCHED();
     CW_CUDA(cudaMemcpyAsync(hs.data(), d_st, sizeof(RelaxState) * nh, cudaMemcpyDeviceToHost, stream()));
     CW_CUDA(cudaStreamSynchronize(stream()));
     for (uint32_t k = 0; k < nh; ++k) out[k] = __builtin_bit_cast(double, (uint64_t)hs[k].resid);
-    ps.release();
+    prow.release();
     return CW_OK;
 }
 
@@ -907,9 +920,9 @@ extern "C" int cw_field_time_inner(cw_field f, int32_t sweeps, int32_t depth, do
     for (auto &s : hs) { std::memset(&s, 0, sizeof s); s.omega = omega; s.stop = CW_STOP_RESIDUAL; }
     RelaxState *d_st = (RelaxState *)f->stats;
     CW_CUDA(cudaMemcpyAsync(d_st, hs.data(), sizeof(RelaxState) * nh, cudaMemcpyHostToDevice, stream()));
-    Plan ps;
-    if ((rc = site_plan(f, ps)) != CW_OK) return rc;
-    k_residual64<<<ps.nblocks, T, 0, stream()>>>(view(f), ps.d_blk, nh, d_st, f->r32, f->inv32, f->d32a, 0);
+    Plan prow;
+    if ((rc = row_plan(f, prow)) != CW_OK) return rc;
+    k_residual64<<<prow.nblocks, T, 0, stream()>>>(view(f), prow.d_blk, nh, d_st, f->r32, f->inv32, f->d32a, 0);
     CW_LAUNCHED();
     Sor32 solver;
     std::vector<double> om(nh, omega);
@@ -928,6 +941,6 @@ extern "C" int cw_field_time_inner(cw_field f, int32_t sweeps, int32_t depth, do
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     solver.release();
-    ps.release();
+    prow.release();
     return CW_OK;
 }

@@ -18,7 +18,8 @@
 // whole launch.  Neighbours come from the thread's own registers (the other
 // pixel of the pair, the rows above and below), from the next lane by a warp
 // shuffle, and across a warp boundary from the one row each neighbouring
-// warp publishes in shared memory after every half-sweep.
+// warp publishes in shared memory after every half-sweep (double-buffered,
+// so one barrier per half-sweep suffices).
 #include "cw_internal.cuh"
 #include "field_kernels.cuh"
 
@@ -29,6 +30,32 @@ constexpr int WIN = 64;            // window side
 constexpr int WARPS = 8;           // warps per block
 constexpr int ROWS = WIN / WARPS;  // window rows per warp
 
+// One half-sweep of colour C over the thread's rows (C known at compile
+// time: the colour of each row's pixels is then fixed and no branch is left).
+// ab/be: the rows just above and below this warp's, from the neighbours.
+template <int C>
+__device__ __forceinline__ void half_sweep(float (&d0)[ROWS], float (&d1)[ROWS], const float (&r0)[ROWS],
+                                           const float (&r1)[ROWS], const float (&i0)[ROWS],
+                                           const float (&i1)[ROWS], float ab0, float ab1, float be0, float be1,
+                                           int lane, float om, float dcoef) {
+#pragma unroll
+    for (int j = 0; j < ROWS; ++j) {
+        if (((C + j) & 1) == 0) {  // the even column of the pair
+            float left = __shfl_up_sync(0xffffffffu, d1[j], 1);
+            left = lane == 0 ? 0.f : left;
+            const float up = j > 0 ? d0[j - 1] : ab0, down = j < ROWS - 1 ? d0[j + 1] : be0;
+            const float old = d0[j];
+            d0[j] = fmaf(om, fmaf(fmaf(dcoef, (left + d1[j]) + (up + down), r0[j]), i0[j], -old), old);
+        } else {  // the odd column
+            float right = __shfl_down_sync(0xffffffffu, d0[j], 1);
+            right = lane == 31 ? 0.f : right;
+            const float up = j > 0 ? d1[j - 1] : ab1, down = j < ROWS - 1 ? d1[j + 1] : be1;
+            const float old = d1[j];
+            d1[j] = fmaf(om, fmaf(fmaf(dcoef, (d0[j] + right) + (up + down), r1[j]), i1[j], -old), old);
+        }
+    }
+}
+
 template <int DEPTH>
 __global__ void __launch_bounds__(32 * WARPS) k_sor32_tb(const float *__restrict__ src, float *__restrict__ dst,
                                                          const float *__restrict__ rhs, const float *__restrict__ inv,
@@ -38,8 +65,9 @@ __global__ void __launch_bounds__(32 * WARPS) k_sor32_tb(const float *__restrict
                                                          const float *__restrict__ omega, const int32_t *done,
                                                          int done_stride, int nhalf, int start_colour, float dcoef) {
     constexpr int IN = WIN - 2 * DEPTH;  // interior side
-    // edge rows each warp publishes: [warp][0 top, 1 bottom][column]
-    __shared__ float edge[WARPS][2][WIN];
+    // edge rows each warp publishes, double-buffered by half-sweep parity:
+    // [buffer][warp][0 top, 1 bottom][column]
+    __shared__ float edge[2][WARPS][2][WIN];
     __shared__ int s_h;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (threadIdx.x == 0) s_h = plan_history(blk, nh, blockIdx.x);
@@ -65,42 +93,28 @@ __global__ void __launch_bounds__(32 * WARPS) k_sor32_tb(const float *__restrict
             if (in1) { d1[j] = src[row + 1]; r1[j] = rhs[row + 1]; i1[j] = inv[row + 1]; }
         }
     }
-    edge[warp][0][2 * lane] = d0[0];
-    edge[warp][0][2 * lane + 1] = d1[0];
-    edge[warp][1][2 * lane] = d0[ROWS - 1];
-    edge[warp][1][2 * lane + 1] = d1[ROWS - 1];
+    auto publish = [&](int buf) {
+        edge[buf][warp][0][2 * lane] = d0[0];
+        edge[buf][warp][0][2 * lane + 1] = d1[0];
+        edge[buf][warp][1][2 * lane] = d0[ROWS - 1];
+        edge[buf][warp][1][2 * lane + 1] = d1[ROWS - 1];
+    };
+    publish(0);
     __syncthreads();
-    // window pixel (ex, ey) has colour (gx0 + gy0 + ex + ey) mod 2 and
-    // gx0 + gy0 and 8 warp are even: in row j the pixel of colour c is the
-    // pair's (c + j) mod 2
+    // window pixel (ex, ey) has colour (gx0 + gy0 + ex + ey) mod 2, and gx0 + gy0
+    // and 8 warp are even: in row j the pixel of colour c is the pair's (c + j) mod 2
     for (int s = 0; s < nhalf; ++s) {
-        const int c = (start_colour + s) & 1;
-        // the rows just outside this warp's, as the neighbouring warps left them
-        const float ab0 = warp > 0 ? edge[warp - 1][1][2 * lane] : 0.f;
-        const float ab1 = warp > 0 ? edge[warp - 1][1][2 * lane + 1] : 0.f;
-        const float be0 = warp < WARPS - 1 ? edge[warp + 1][0][2 * lane] : 0.f;
-        const float be1 = warp < WARPS - 1 ? edge[warp + 1][0][2 * lane + 1] : 0.f;
-#pragma unroll
-        for (int j = 0; j < ROWS; ++j) {
-            if (((c + j) & 1) == 0) {  // the even column of the pair
-                float left = __shfl_up_sync(0xffffffffu, d1[j], 1);
-                if (lane == 0) left = 0.f;
-                const float up = j > 0 ? d0[j - 1] : ab0, down = j < ROWS - 1 ? d0[j + 1] : be0;
-                const float old = d0[j];
-                d0[j] = old + om * ((r0[j] + dcoef * ((left + d1[j]) + (up + down))) * i0[j] - old);
-            } else {  // the odd column
-                float right = __shfl_down_sync(0xffffffffu, d0[j], 1);
-                if (lane == 31) right = 0.f;
-                const float up = j > 0 ? d1[j - 1] : ab1, down = j < ROWS - 1 ? d1[j + 1] : be1;
-                const float old = d1[j];
-                d1[j] = old + om * ((r1[j] + dcoef * ((d0[j] + right) + (up + down))) * i1[j] - old);
-            }
-        }
-        __syncthreads();  // every warp has read the edges of this half-sweep
-        edge[warp][0][2 * lane] = d0[0];
-        edge[warp][0][2 * lane + 1] = d1[0];
-        edge[warp][1][2 * lane] = d0[ROWS - 1];
-        edge[warp][1][2 * lane + 1] = d1[ROWS - 1];
+        const int buf = s & 1;
+        const float ab0 = warp > 0 ? edge[buf][warp - 1][1][2 * lane] : 0.f;
+        const float ab1 = warp > 0 ? edge[buf][warp - 1][1][2 * lane + 1] : 0.f;
+        const float be0 = warp < WARPS - 1 ? edge[buf][warp + 1][0][2 * lane] : 0.f;
+        const float be1 = warp < WARPS - 1 ? edge[buf][warp + 1][0][2 * lane + 1] : 0.f;
+        if (((start_colour + s) & 1) == 0)
+            half_sweep<0>(d0, d1, r0, r1, i0, i1, ab0, ab1, be0, be1, lane, om, dcoef);
+        else
+            half_sweep<1>(d0, d1, r0, r1, i0, i1, ab0, ab1, be0, be1, lane, om, dcoef);
+        // the other buffer was last read before the previous barrier
+        publish(buf ^ 1);
         __syncthreads();
     }
     // the interior back to global memory

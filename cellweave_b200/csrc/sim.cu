@@ -410,6 +410,7 @@ int cw_sim_step(cw_sim s, uint32_t nsteps) {
     o.tolerance = c.tolerance;
     o.max_sweeps = 200000;
     o.precision = c.precision;
+    o.inner_sweeps = c.inner_sweeps > 0 ? c.inner_sweeps : 32;
     int rc;
     for (uint32_t step = 0; step < nsteps; ++step, ++s->steps) {
         bool solve = c.relax_every <= 1 || (s->steps % (uint32_t)c.relax_every) == 0;

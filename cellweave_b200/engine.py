@@ -491,7 +491,8 @@ class Simulation:
                  target_volume=49, lambda_volume=1.0, surface_target=0, lambda_surface=0.0, seeding=0, seed_side=7,
                  nfields=1, o2_dcoef=1.0, o2_sink_by_type=(0.0, 0.01, 0.01), o2_background_sink=0.0, o2_hold=0, signal_dcoef=1.0,
                  signal_decay=0.01, signal_secretion=0.05, hypoxic_level=0.1, tolerance=1e-6, precision=FP32_DC,
-                 omega=None, relax_every=1, dt=0.01, substeps=8, sweeps=1, death_threshold=0.25, necrotic_type=-1):
+                 omega=None, inner_sweeps=0, relax_every=1, dt=0.01, substeps=8, sweeps=1, death_threshold=0.25,
+                 necrotic_type=-1):
         self.dims, w, h, z = _dims(dims)
         self._keep = [w, h, z]
         nc = np.array(ncells, np.uint32)
@@ -505,7 +506,7 @@ class Simulation:
                              int(target_volume), float(lambda_volume), int(surface_target), float(lambda_surface),
                              int(seeding), int(seed_side), int(nfields), float(o2_dcoef), ptr(sink).value, float(o2_background_sink),
                              int(o2_hold), float(signal_dcoef), float(signal_decay), float(signal_secretion),
-                             float(hypoxic_level), float(tolerance), int(precision), float(omega or 0.0),
+                             float(hypoxic_level), float(tolerance), int(precision), float(omega or 0.0), int(inner_sweeps),
                              int(relax_every), float(dt), int(substeps), int(sweeps), float(death_threshold),
                              int(necrotic_type))
         handle = C.c_void_p()
