@@ -62,6 +62,16 @@ class TermSpec(C.Structure):
                 ("hill_n", C.c_double), ("hill_k", C.c_double), ("param", C.c_double), ("has_hill", C.c_int32)]
 
 
+class FitConfig(C.Structure):
+    _fields_ = [("dcoef", C.c_double), ("uptake", C.c_double * 3), ("vessel_value", C.c_double),
+                ("vessel_x", C.c_int32), ("egf", C.c_double), ("signal_dcoef", C.c_double),
+                ("signal_decay", C.c_double), ("secretion", C.c_double), ("steps", C.c_int32),
+                ("checkpoint_every", C.c_int32), ("dt", C.c_double), ("nbins", C.c_int32), ("bin_width", C.c_double),
+                ("hypoxic_level", C.c_double), ("tau", C.c_double), ("signal_weight", C.c_double),
+                ("tolerance", C.c_double), ("adjoint_tolerance", C.c_double), ("precision", C.c_int32),
+                ("omega", C.c_double), ("network_params", C.c_int32)]
+
+
 class SimConfig(C.Structure):
     _fields_ = [("nh", C.c_uint32), ("w", C.c_void_p), ("h", C.c_void_p), ("d", C.c_void_p),
                 ("ncells", C.c_void_p), ("seeds", C.c_void_p), ("temperature", C.c_double), ("K", C.c_int32),
@@ -107,6 +117,7 @@ SIGNATURES = {
     "cw_field_destroy": (C.c_int, [P]),
     "cw_field_set_source": (C.c_int, [P, D]),
     "cw_field_set_diffusion": (C.c_int, [P, D]),
+    "cw_field_set_floor": (C.c_int, [P, I32]),
     "cw_field_upload": (C.c_int, [P, U32, I32, P]),
     "cw_field_download": (C.c_int, [P, U32, I32, P]),
     "cw_field_upload_held": (C.c_int, [P, U32, P]),
@@ -142,6 +153,14 @@ SIGNATURES = {
     "cw_sim_field": (C.c_int, [P, I32, P]),
     "cw_sim_stats": (C.c_int, [P, P]),
     "cw_sim_network_state": (C.c_int, [P, U32, U32, P]),
+    "cw_fit_create": (C.c_int, [P, P, P, P]),
+    "cw_fit_destroy": (C.c_int, [P]),
+    "cw_fit_nparams": (C.c_int, [P, P]),
+    "cw_fit_get_params": (C.c_int, [P, P]),
+    "cw_fit_set_params": (C.c_int, [P, P]),
+    "cw_fit_set_target": (C.c_int, [P, P, P]),
+    "cw_fit_forward": (C.c_int, [P, P, P, P]),
+    "cw_fit_gradient": (C.c_int, [P, P, P]),
     "cw_event_record": (C.c_int, [I32]),
     "cw_profiler_start": (C.c_int, []),
     "cw_profiler_stop": (C.c_int, []),

@@ -204,6 +204,7 @@ struct cw_field_s {
     double *uptake = nullptr, *production = nullptr, *lin_sink = nullptr;
     bool lin_sink_on = false, uptake_on = false, production_on = false;
     bool held_dirty = true;          // the span cache is stale
+    bool floor = true;               // updates floored at zero (pde.rs:395); off for adjoint solves
     std::vector<cw::Span> spans;     // free_span of every history, cached
     double dcoef = 0.2, decay = 0.0, source = 0.0;
     // scratch of the FP32 defect-correction solve and the explicit step

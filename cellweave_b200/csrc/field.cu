@@ -112,7 +112,8 @@ __global__ void k_sor64_half(FieldView fv, const int32_t *blk, int nh, const Spa
                 if (fv.ks) den = den + fv.ks[i];
                 double balanced = add_sources(fv, i, fv.d * sum) / den;
                 double om = st[h].omega;
-                double after = fmax((1.0 - om) * before + om * balanced, 0.0);
+                double after = (1.0 - om) * before + om * balanced;
+                if (fv.floor) after = fmax(after, 0.0);
                 fv.c[i] = after;
                 moved = fabs(after - before);
             }
@@ -150,7 +151,7 @@ __global__ void k_residual64(FieldView fv, const int32_t *blk, int nh, RelaxStat
             if (fv.ks) den = den + fv.ks[i];
             double cv = fv.c[i];
             double r = add_sources(fv, i, fv.d * sum) - den * cv;
-            if (cv <= 0.0 && r < 0.0) r = 0.0;
+            if (fv.floor && cv <= 0.0 && r < 0.0) r = 0.0;
             worst = fabs(r);
             r_out = (float)r;
             inv_out = den > 0.0 ? (float)(1.0 / den) : 0.0f;
@@ -210,12 +211,17 @@ __global__ void __launch_bounds__(256) k_dc_update(FieldView fv, const int32_t *
         const int64_t i = fv.off[h] + (int64_t)row * w + x;
         if (!fv.held[i]) {
             const bool red = colour == 0;
+            const bool fl = fv.floor;
             auto nb = [&](int64_t j) -> double {
                 double cj = fv.c[j];
-                if (red && !fv.held[j]) cj = fmax(cj + (double)dlt[j], 0.0);
+                if (red && !fv.held[j]) {
+                    cj = cj + (double)dlt[j];
+                    if (fl) cj = fmax(cj, 0.0);
+                }
                 return cj;
             };
-            const double ci = fmax(fv.c[i] + (double)dlt[i], 0.0);
+            double ci = fv.c[i] + (double)dlt[i];
+            if (fl) ci = fmax(ci, 0.0);
             double sum = 0.0, real = 0.0;
             if (x > 0) { sum += nb(i - 1); real += 1.0; }
             if (x + 1 < dm.x) { sum += nb(i + 1); real += 1.0; }
@@ -226,7 +232,7 @@ __global__ void __launch_bounds__(256) k_dc_update(FieldView fv, const int32_t *
             double den = real * fv.d + fv.decay;
             if (fv.ks) den = den + fv.ks[i];
             double r = add_sources(fv, i, fv.d * sum) - den * ci;
-            if (ci <= 0.0 && r < 0.0) r = 0.0;
+            if (fl && ci <= 0.0 && r < 0.0) r = 0.0;
             worst = fabs(r);
             fv.c[i] = ci;
             r32[i] = (float)r;
@@ -420,6 +426,7 @@ FieldView view(cw_field_s *f) {
     v.pr = f->production_on ? f->production : nullptr;
     v.ks = f->lin_sink_on ? f->lin_sink : nullptr;
     v.d = f->dcoef; v.decay = f->decay; v.source = f->source;
+    v.floor = f->floor ? 1 : 0;
     v.dims = f->g.d_dims; v.off = f->g.d_off;
     return v;
 }
@@ -626,6 +633,11 @@ int cw_field_destroy(cw_field f) {
 
 int cw_field_set_source(cw_field f, double source) {
     f->source = source;
+    return CW_OK;
+}
+
+int cw_field_set_floor(cw_field f, int32_t on) {
+    f->floor = on != 0;
     return CW_OK;
 }
 

@@ -14,6 +14,7 @@ struct FieldView {
     double d, decay, source;
     const int4 *dims;
     const int64_t *off;
+    int floor;  // 1: updates floored at zero, residual projected (the reference); 0: a linear solve
 };
 
 FieldView view(cw_field_s *f);

@@ -562,3 +562,63 @@ class Simulation:
         ok = C.c_int32()
         call("cw_lattice_verify", self.lattice_handle(), hist, C.byref(ok))
         return bool(ok.value)
+
+
+# ============================================================== Fit (adjoint)
+class Fit:
+    """Loss and gradient of a frozen lattice's step (cw_fit_*): parameters are
+    D, the uptake k of types 1..3 and the first `network_params` network rates.
+    The reference has no counterpart; see include/cellweave_b200.h."""
+
+    def __init__(self, lattice: CpmLattice, network: Network, *, dcoef=1.0, uptake=(0.01, 0.005, 0.0),
+                 vessel_value=1.0, vessel_x=0, egf=0.2, signal_dcoef=1.0, signal_decay=0.01, secretion=0.05,
+                 steps=2000, checkpoint_every=100, dt=0.01, nbins=64, bin_width=16.0, hypoxic_level=0.1, tau=0.02,
+                 signal_weight=1.0, tolerance=1e-8, adjoint_tolerance=1e-10, precision=FP32_DC, omega=None,
+                 network_params=32):
+        cfg = _lib.FitConfig(float(dcoef), (C.c_double * 3)(*uptake), float(vessel_value), int(vessel_x),
+                             float(egf), float(signal_dcoef), float(signal_decay), float(secretion), int(steps),
+                             int(checkpoint_every), float(dt), int(nbins), float(bin_width), float(hypoxic_level),
+                             float(tau), float(signal_weight), float(tolerance), float(adjoint_tolerance),
+                             int(precision), float(omega or 0.0), int(network_params))
+        handle = C.c_void_p()
+        call("cw_fit_create", lattice.handle, network.handle, C.byref(cfg), C.byref(handle))
+        self._h = handle
+        self._keep = (lattice, network)
+        self.nbins = int(nbins)
+        n = C.c_int32()
+        call("cw_fit_nparams", self._h, C.byref(n))
+        self.nparams = n.value
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value and _lib._LIB is not None:
+            lib().cw_fit_destroy(h)
+            self._h = None
+
+    @property
+    def params(self):
+        p = np.empty(self.nparams)
+        call("cw_fit_get_params", self._h, ptr(p))
+        return p
+
+    @params.setter
+    def params(self, p):
+        p = np.ascontiguousarray(p, np.float64)
+        call("cw_fit_set_params", self._h, ptr(p))
+
+    def set_target(self, hypoxic, signal):
+        h = np.ascontiguousarray(hypoxic, np.float64)
+        g = np.ascontiguousarray(signal, np.float64)
+        call("cw_fit_set_target", self._h, ptr(h), ptr(g))
+
+    def forward(self):
+        loss = C.c_double()
+        h, g = np.empty(self.nbins), np.empty(self.nbins)
+        call("cw_fit_forward", self._h, C.byref(loss), ptr(h), ptr(g))
+        return loss.value, h, g
+
+    def gradient(self):
+        loss = C.c_double()
+        g = np.empty(self.nparams)
+        call("cw_fit_gradient", self._h, C.byref(loss), ptr(g))
+        return loss.value, g

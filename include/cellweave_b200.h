@@ -51,6 +51,7 @@ typedef struct cw_lattice_s *cw_lattice;
 typedef struct cw_field_s *cw_field;
 typedef struct cw_network_s *cw_network;
 typedef struct cw_sim_s *cw_sim;
+typedef struct cw_fit_s *cw_fit;
 
 /* ------------------------------------------------------------------ library */
 const char *cw_last_error(void);
@@ -125,6 +126,9 @@ int cw_field_destroy(cw_field f);
 /* with_source (pde.rs:135-138), and the diffusion coefficient (for fits). */
 int cw_field_set_source(cw_field f, double source);
 int cw_field_set_diffusion(cw_field f, double dcoef);
+/* The floor at zero of every update (pde.rs:395), on by default; off makes
+ * relax a plain linear solve (values may go negative), as an adjoint needs. */
+int cw_field_set_floor(cw_field f, int32_t on);
 enum { CW_VALUES = 0, CW_UPTAKE = 1, CW_PRODUCTION = 2, CW_LIN_SINK = 3 };
 /* Per-pixel arrays of history `hist`: values, uptake (zero-order sink,
  * set_uptake_at), production (set_production_at) and the first-order sink
@@ -302,6 +306,50 @@ int cw_sim_field(cw_sim sim, int32_t which, cw_field *f);
 int cw_sim_stats(cw_sim sim, double *out);
 /* Network state of history `hist`, [ncells][S]. */
 int cw_sim_network_state(cw_sim sim, uint32_t hist, uint32_t n, double *state);
+
+/* ------------------------------------------------------------------ differentiation
+ * No counterpart in the reference (it has no adjoint, loss or autodiff): a
+ * hand-written adjoint of one frozen lattice's step, for fitting.  Oxygen
+ * solves D lap c - k_type c = 0 with the lattice's obstacles held at
+ * vessel_value; each cell's network runs `steps` RK4 steps of dt on its mean
+ * oxygen, checkpointed every `checkpoint_every`; the cells secrete
+ * secretion * (angiogenic node) into a signal field (signal_dcoef,
+ * signal_decay).  The loss is sum_b (h_b - h*_b)^2 + signal_weight *
+ * sum_b (g_b - g*_b)^2 over `nbins` bins of |x - vessel_x| / bin_width, h_b
+ * the bin's hypoxic fraction of cell pixels, smoothed as
+ * sigmoid((hypoxic_level - c) / tau), g_b their mean signal.  Parameters:
+ * D, k for types 1..3, and the rates of the network's first
+ * `network_params` terms (file order). */
+typedef struct {
+    double dcoef;               /* D (the first parameter's initial value) */
+    double uptake[3];           /* k of types 1, 2, 3 */
+    double vessel_value;        /* oxygen held on the lattice's obstacles */
+    int32_t vessel_x;           /* bins measure the distance from this column */
+    double egf;
+    double signal_dcoef, signal_decay, secretion;
+    int32_t steps, checkpoint_every;
+    double dt;
+    int32_t nbins;
+    double bin_width, hypoxic_level, tau, signal_weight;
+    double tolerance;           /* forward solves: residual */
+    double adjoint_tolerance;   /* adjoint solves: residual */
+    int32_t precision;          /* CW_FP64 or CW_FP32_DC for every solve */
+    double omega;               /* <= 0: the reference's rule */
+    int32_t network_params;     /* rates fitted, at most 32 */
+} cw_fit_config;
+/* The lattice (one history) and the network are borrowed, not copied: keep
+ * them alive, and the lattice unchanged, while the fit lives. */
+int cw_fit_create(cw_lattice lat, cw_network net, const cw_fit_config *cfg, cw_fit *out);
+int cw_fit_destroy(cw_fit fit);
+int cw_fit_nparams(cw_fit fit, int32_t *n);
+int cw_fit_get_params(cw_fit fit, double *params);
+int cw_fit_set_params(cw_fit fit, const double *params);
+/* Target profiles h* and g*, nbins each. */
+int cw_fit_set_target(cw_fit fit, const double *hypoxic, const double *signal);
+/* Forward: the loss and the profiles h, g (nbins each; either may be NULL). */
+int cw_fit_forward(cw_fit fit, double *loss, double *hypoxic, double *signal);
+/* Forward and adjoint: the loss and dL/dparams (cw_fit_nparams entries). */
+int cw_fit_gradient(cw_fit fit, double *loss, double *grad);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,116 @@
+"""The hand-written adjoint against central finite differences and an FP64 gradient (GPU).
+
+The fit (cw_fit_*): oxygen D lap c - k_type c = 0 held at a vessel column,
+cells' RK4 networks on their mean oxygen with checkpoints, a signal secreted
+by the angiogenic node, and a loss on the radial hypoxic-fraction and signal
+profiles.  Gradients with respect to D, k (three types) and network rates
+must match central differences (h = 1e-4 relative) to 1e-4 relative, with the
+FP32 defect-correction solves as with the FP64 ones.
+"""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+import cellweave_b200 as cw
+from cellweave_b200 import seeding, synthetic
+
+pytestmark = pytest.mark.gpu
+
+J4 = synthetic.contact_table(4, seed=2)
+
+
+def geometry(size=96, side=6, seed=4):
+    grid = seeding.empty(size, size)
+    rec = seeding.Records()
+    grid[0, :, size // 2] = -1  # the vessel, an obstacle column
+    rng = np.random.default_rng(seed)
+    for y in range(1, size - side, side + 1):
+        for x in range(1, size - side, side + 1):
+            if (grid[0, y:y + side, x:x + side] != 0).any() or rng.random() < 0.15:
+                continue
+            seeding.add_block(grid, rec, 1 + int(rng.integers(3)), (x, y), side, side, lam=1.0)
+    return cw.CpmLattice.from_grids([grid], [rec], 10.0, J4, 2, seeds=[1])
+
+
+def network(S=8):
+    d = tempfile.mkdtemp()
+    p = os.path.join(d, "n.toml")
+    open(p, "w").write(synthetic.network_toml(S, seed=S))
+    return cw.Network.load(p, 36)
+
+
+def make_fit(lat, net, precision, tol=1e-12):
+    return cw.Fit(lat, net, dcoef=1.0, uptake=(0.01, 0.005, 0.002), vessel_x=48, steps=200, checkpoint_every=20,
+                  dt=0.05, nbins=16, bin_width=3.0, hypoxic_level=0.3, tau=0.05, signal_weight=1.0, tolerance=tol,
+                  adjoint_tolerance=tol * 1e-2, precision=precision, network_params=8)
+
+
+@pytest.fixture(scope="module")
+def problem():
+    lat, net = geometry(), network()
+    fit = make_fit(lat, net, cw.FP32_DC)
+    start = fit.params.copy()
+    # the target: the same model at D = 1.3 and k = 0.008 for every type
+    p = start.copy()
+    p[0], p[1:4] = 1.3, 0.008
+    fit.params = p
+    _, h, g = fit.forward()
+    fit.set_target(h, g)
+    fit.params = start
+    return lat, net, fit, start, h, g
+
+
+def test_gradient_matches_central_differences(problem):
+    lat, net, fit, start, h, g = problem
+    loss, grad = fit.gradient()
+    assert loss > 0
+    scale = np.abs(grad).max()
+    for k in range(fit.nparams):
+        step = 1e-4 * abs(start[k]) if start[k] != 0 else 1e-7
+        p = start.copy()
+        p[k] += step
+        fit.params = p
+        up = fit.forward()[0]
+        p[k] -= 2 * step
+        fit.params = p
+        down = fit.forward()[0]
+        fd = (up - down) / (2 * step)
+        assert abs(grad[k] - fd) <= 1e-4 * max(abs(fd), 1e-3 * scale), (k, grad[k], fd)
+    fit.params = start
+
+
+def test_fp32_adjoint_matches_the_fp64_gradient(problem):
+    lat, net, fit, start, h, g = problem
+    ref = make_fit(lat, net, cw.FP64)
+    ref.set_target(h, g)
+    ref.params = start
+    l64, g64 = ref.gradient()
+    l32, g32 = fit.gradient()
+    assert abs(l32 - l64) <= 1e-9 * abs(l64)
+    np.testing.assert_allclose(g32, g64, rtol=1e-6, atol=1e-9 * np.abs(g64).max())
+
+
+def test_gradient_descent_lowers_the_loss(problem):
+    lat, net, fit, start, h, g = problem
+    # steepest descent in the log of the parameters, with backtracking
+    p = start.copy()
+    fit.params = p
+    loss0, grad = fit.gradient()
+    loss = loss0
+    for _ in range(4):
+        d = -grad * p * p  # the gradient in log p, back in p
+        alpha = 0.1 / (np.abs(d / np.where(p != 0, p, 1)).max() + 1e-300)
+        for _ in range(20):
+            q = np.maximum(p + alpha * d, 1e-6)
+            fit.params = q
+            lq = fit.forward()[0]
+            if lq < loss:
+                break
+            alpha *= 0.5
+        p, loss = q, lq
+        fit.params = p
+        loss, grad = fit.gradient()
+    assert loss < loss0
+    fit.params = start
