@@ -52,6 +52,8 @@ def parse():
     p.add_argument("--workload", choices=["campaign", "cord"], default="campaign")
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-fit", action="store_true")
+    p.add_argument("--fit-iters", type=int, default=4)
     p.add_argument("--profile-step", action="store_true",
                    help="bracket one extra step with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     return p.parse_args()
@@ -306,8 +308,61 @@ def run_ours(args, rank, world, dist):
             del s1
         plain = {"value": units / (total_ms / 1e3), "unit": UNIT,
                  "how": "the same 64 histories, each its own Simulation stepped alone (one history per launch)"}
-    return dict(value=value, ms=ms / args.steps, launches=launches, clocks=clk, e2e=e2e, roofline=roofline,
+    fit = None
+    if not args.no_fit and world == 1:
+        fit = run_fit(args, L)
+    return dict(value=value, ms=ms / args.steps, launches=launches, clocks=clk, e2e=e2e, roofline=roofline, fit=fit,
                 plain=plain, stats=stats, nh=nh, cfg=cfg, tuned=tuned)
+
+
+def run_fit(args, L):
+    """The differentiated fit at the cord's scale: the 2048^2 cord stepped to
+    MCS 500 and frozen; 2000 RK4 steps checkpointed every 100; parameters D,
+    k (three types) and 32 network rates; the target from D = 1.3, k = 0.008.
+    Gradient-descent iterations (forward + adjoint + a line-search forward)
+    are timed one by one with CUDA events."""
+    import numpy as np
+
+    import cellweave_b200 as cw
+    cfg = workload("cord")
+    S = cfg.pop("S")
+    net = network_for(S, S, cfg["target_volume"])
+    sim = cw.Simulation(net, **cfg)
+    sim.step(500)
+    lat = sim.lattice()
+    w = cfg["dims"][0][0]
+    fit = cw.Fit(lat, net, dcoef=1.0, uptake=(0.01, 0.005, 0.0), vessel_x=w // 2, steps=2000, checkpoint_every=100,
+                 dt=0.01, nbins=64, bin_width=w / 128.0, tolerance=1e-6, adjoint_tolerance=1e-8,
+                 precision=cw.FP32_DC, network_params=32)
+    start = fit.params.copy()
+    p = start.copy()
+    p[0], p[1:4] = 1.3, 0.008
+    fit.params = p
+    _, h, g = fit.forward()
+    fit.set_target(h, g)
+    p = start.copy()
+    fit.params = p
+    times, losses = [], []
+    for _ in range(args.fit_iters):
+        L.cw_synchronize()
+        L.cw_event_record(6)
+        loss, grad = fit.gradient()
+        d = -grad * p * p
+        q = np.maximum(p + 0.05 / (np.abs(d / p).max() + 1e-300) * d, 1e-6)
+        fit.params = q
+        lq = fit.forward()[0]
+        L.cw_event_record(7)
+        times.append(event_ms(L, 6, 7) / 1e3)
+        losses.append(loss)
+        if lq < loss:
+            p = q
+        fit.params = p
+    del fit, lat, sim
+    return {"seconds_per_iteration": float(np.median(times)), "iterations": len(times),
+            "loss_first": losses[0], "loss_last": losses[-1], "parameters": int(len(start)),
+            "workload": "2048^2 cord frozen at MCS 500, 2000 RK4 steps (checkpoints every 100), "
+                        "FP32 defect-correction forward and adjoint solves, 1 + 3 + 32 parameters; "
+                        "an iteration = forward + adjoint + one line-search forward"}
 
 
 def main():
@@ -359,6 +414,7 @@ def main():
                     gpu_launches=r["launches"], roofline=r["roofline"], cpu_baseline=cpu,
                     plain=r["plain"],
                     batched_over_plain=(r["value"] / r["plain"]["value"]) if r["plain"] else None,
+                    fit=r["fit"],
                     sor_gbs=r["roofline"]["achieved"], sor_site_sweeps_per_s=r["roofline"]["site_sweeps_per_s"],
                     living_cells=float(r["stats"][:, 0].sum()), last_residual_max=float(r["stats"][:, 3].max()),
                     autotuned={"omega_o2": sorted(set(float(v) for v in r["tuned"]["omega_o2"])),

@@ -82,7 +82,7 @@ class SimConfig(C.Structure):
                 ("signal_decay", C.c_double), ("signal_secretion", C.c_double), ("hypoxic_level", C.c_double),
                 ("tolerance", C.c_double), ("precision", C.c_int32), ("omega", C.c_double),
                 ("inner_sweeps", C.c_int32), ("relax_every", C.c_int32), ("dt", C.c_double), ("substeps", C.c_int32), ("sweeps", C.c_int32),
-                ("death_threshold", C.c_double), ("necrotic_type", C.c_int32)]
+                ("death_threshold", C.c_double), ("necrotic_type", C.c_int32), ("use_graphs", C.c_int32)]
 
 
 P = C.c_void_p
@@ -150,6 +150,7 @@ SIGNATURES = {
     "cw_sim_step": (C.c_int, [P, U32]),
     "cw_sim_lattice": (C.c_int, [P, P]),
     "cw_sim_tuning": (C.c_int, [P, P, P, P, P]),
+    "cw_sim_graph_info": (C.c_int, [P, P, P, P]),
     "cw_sim_field": (C.c_int, [P, I32, P]),
     "cw_sim_stats": (C.c_int, [P, P]),
     "cw_sim_network_state": (C.c_int, [P, U32, U32, P]),

@@ -257,6 +257,19 @@ __global__ void k_dc_check(RelaxState *st, int nh, int inner, int64_t max_sweeps
     s.resid = 0ull;
 }
 
+// The test of k_dc_check without its bookkeeping: marks what settled and
+// records the residual, leaving the accumulator for the next k_dc_check.
+__global__ void k_dc_peek(RelaxState *st, int nh) {
+    int h = blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= nh) return;
+    RelaxState &s = st[h];
+    if (!s.done) {
+        double r = __longlong_as_double((long long)s.resid);
+        s.last_resid = r;
+        if (r < s.tol) s.done = 1;
+    }
+}
+
 // inflow (pde.rs:415-456): flux from held pixels into free ones.
 __global__ void k_inflow(FieldView fv, const int32_t *blk, int nh, double *out) {
     __shared__ int s_h;
@@ -535,47 +548,101 @@ static int relax_fp64(cw_field_s *f, const cw_relax_opts &o, std::vector<Span> &
     return CW_OK;
 }
 
-static int relax_fp32dc(cw_field_s *f, const cw_relax_opts &o, RelaxState *d_st, std::vector<RelaxState> &hs) {
+// Launch plans and the FP32 solver of the defect-correction solve, built on a
+// field's first FP32 solve and kept: no allocation in later solves, so that
+// a whole step can be captured in a CUDA graph.
+struct DcCache {
+    Plan pr, prow;
+    Sor32 solver;
+    int depth = -1;
+    std::vector<double> omega;
+    double *d_omega = nullptr;  // per history, for the state initialisation on the device
+};
+
+__global__ void k_dc_state_init(RelaxState *st, int nh, const double *omega, double tol) {
+    int h = blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= nh) return;
+    RelaxState s{};
+    s.omega = omega[h];
+    s.tol = tol;
+    s.stop = CW_STOP_RESIDUAL;
+    st[h] = s;
+}
+
+static int dc_prepare(cw_field_s *f, int depth, const std::vector<double> &om, DcCache **out) {
     uint32_t nh = f->g.nh;
     int rc = f->alloc_fp32();
     if (rc != CW_OK) return rc;
-    FieldView fv = view(f);
-    Plan ps, pr, prow;
-    if ((rc = site_plan(f, ps)) != CW_OK) return rc;
-    if ((rc = row_plan(f, prow)) != CW_OK) return rc;
-    {
+    DcCache *c = (DcCache *)f->dc_cache;
+    if (c && c->depth != depth) {
+        c->solver.release();
+        c->depth = -1;
+    }
+    if (!c) {
+        c = new DcCache();
+        f->dc_cache = c;
+        if ((rc = row_plan(f, c->prow)) != CW_OK) return rc;
         std::vector<int64_t> per(nh);
         for (uint32_t k = 0; k < nh; ++k) per[k] = (int64_t)f->g.h[k] * f->g.d[k] * ((f->g.w[k] + 511) / 512);
-        if ((rc = pr.build(per, 1)) != CW_OK) return rc;
+        if ((rc = c->pr.build(per, 1)) != CW_OK) return rc;
+        if ((rc = dalloc(&c->d_omega, nh)) != CW_OK) return rc;
     }
+    if (c->depth < 0) {
+        if ((rc = c->solver.init(f, depth, om)) != CW_OK) return rc;
+        c->depth = depth;
+        c->omega.clear();
+    }
+    if (c->omega != om) {
+        std::vector<float> omf(om.begin(), om.end());
+        CW_CUDA(cudaMemcpyAsync(c->solver.omega, omf.data(), sizeof(float) * nh, cudaMemcpyHostToDevice, stream()));
+        CW_CUDA(cudaMemcpyAsync(c->d_omega, om.data(), sizeof(double) * nh, cudaMemcpyHostToDevice, stream()));
+        CW_CUDA(cudaStreamSynchronize(stream()));
+        c->omega = om;
+    }
+    *out = c;
+    return CW_OK;
+}
+
+// One outer iteration: the convergence test, `inner` FP32 sweeps, the fused
+// correction and residual.  No host synchronisation.
+static int dc_outer(cw_field_s *f, DcCache *c, RelaxState *d_st, int inner, int64_t max_sweeps, float *&start) {
+    uint32_t nh = f->g.nh;
+    FieldView fv = view(f);
+    const int32_t *done_ptr = (const int32_t *)((const char *)d_st + offsetof(RelaxState, done));
+    const int stride = (int)(sizeof(RelaxState) / sizeof(int32_t));
+    k_dc_check<<<(nh + 63) / 64, 64, 0, stream()>>>(d_st, nh, inner, max_sweeps);
+    CW_LAUNCHED();
+    int rc = c->solver.sweeps(f, inner, done_ptr, stride, start);
+    if (rc != CW_OK) return rc;
+    float *d = c->solver.result();
+    for (int colour = 0; colour < 2; ++colour) {
+        k_dc_update<<<c->pr.nblocks, 256, 0, stream()>>>(fv, c->pr.d_blk, nh, d_st, d, f->r32, colour);
+        CW_LAUNCHED();
+    }
+    start = d;  // zeroed behind the update
+    return CW_OK;
+}
+
+static int relax_fp32dc(cw_field_s *f, const cw_relax_opts &o, RelaxState *d_st, std::vector<RelaxState> &hs) {
+    uint32_t nh = f->g.nh;
     int inner = o.inner_sweeps > 0 ? o.inner_sweeps : 16;
     int depth = o.block_depth > 0 ? o.block_depth : 4;
-    Sor32 solver;
     std::vector<double> om(nh);
     for (uint32_t k = 0; k < nh; ++k) om[k] = hs[k].omega;
-    if ((rc = solver.init(f, depth, om)) != CW_OK) return rc;
-    const int32_t *done_ptr = (const int32_t *)((const char *)d_st + offsetof(RelaxState, done));
+    DcCache *c = nullptr;
+    int rc = dc_prepare(f, depth, om, &c);
+    if (rc != CW_OK) return rc;
+    FieldView fv = view(f);
     int64_t outer = 0;
     int64_t max_outer = o.max_sweeps / inner + 2;
-    std::vector<int32_t> flags(nh);
     int queue = 2;
     // the first residual also sets the inverse diagonal and zeroes d32a
-    k_residual64<<<prow.nblocks, T, 0, stream()>>>(fv, prow.d_blk, nh, d_st, f->r32, f->inv32, f->d32a, 1);
+    k_residual64<<<c->prow.nblocks, T, 0, stream()>>>(fv, c->prow.d_blk, nh, d_st, f->r32, f->inv32, f->d32a, 1);
     CW_LAUNCHED();
     float *start = f->d32a;
-    const int stride = (int)(sizeof(RelaxState) / sizeof(int32_t));
     while (outer < max_outer) {
-        for (int q = 0; q < queue && outer < max_outer; ++q, ++outer) {
-            k_dc_check<<<(nh + 63) / 64, 64, 0, stream()>>>(d_st, nh, inner, o.max_sweeps);
-            CW_LAUNCHED();
-            if ((rc = solver.sweeps(f, inner, done_ptr, stride, start)) != CW_OK) return rc;
-            float *d = solver.result();
-            for (int colour = 0; colour < 2; ++colour) {
-                k_dc_update<<<pr.nblocks, 256, 0, stream()>>>(fv, pr.d_blk, nh, d_st, d, f->r32, colour);
-                CW_LAUNCHED();
-            }
-            start = d;  // zeroed behind the update
-        }
+        for (int q = 0; q < queue && outer < max_outer; ++q, ++outer)
+            if ((rc = dc_outer(f, c, d_st, inner, o.max_sweeps, start)) != CW_OK) return rc;
         CW_CUDA(cudaMemcpyAsync(hs.data(), d_st, sizeof(RelaxState) * nh, cudaMemcpyDeviceToHost, stream()));
         CW_CUDA(cudaStreamSynchronize(stream()));
         bool all = true;
@@ -583,12 +650,86 @@ static int relax_fp32dc(cw_field_s *f, const cw_relax_opts &o, RelaxState *d_st,
         if (all) break;
         queue = std::min(queue * 2, 16);
     }
-    solver.release();
-    ps.release();
-    pr.release();
-    prow.release();
     return CW_OK;
 }
+
+namespace cw {
+// Build (or update) a field's FP32 plans for `depth` and its factors per history.
+int field_dc_prepare(cw_field_s *f, int depth, const std::vector<double> &omega) {
+    DcCache *c = nullptr;
+    return dc_prepare(f, depth, omega, &c);
+}
+
+// The defect-correction solve enqueued with a fixed number of outer
+// iterations and no host synchronisation (every kernel skips a history once
+// it has settled), for capture in a CUDA graph.  A previous field_relax with
+// the same options must have built the field's plans; omega is unchanged.
+int field_relax_enqueue(cw_field_s *f, const cw_relax_opts *opts, int outer, float **start_out) {
+    DcCache *c = (DcCache *)f->dc_cache;
+    if (!c || c->depth < 0) return fail(CW_ERR_CONFIG, "the field has not been solved in FP32 yet");
+    uint32_t nh = f->g.nh;
+    RelaxState *d_st = (RelaxState *)f->stats;
+    int inner = opts->inner_sweeps > 0 ? opts->inner_sweeps : 16;
+    k_dc_state_init<<<(nh + 63) / 64, 64, 0, stream()>>>(d_st, nh, c->d_omega, opts->tolerance);
+    CW_LAUNCHED();
+    FieldView fv = view(f);
+    k_residual64<<<c->prow.nblocks, T, 0, stream()>>>(fv, c->prow.d_blk, nh, d_st, f->r32, f->inv32, f->d32a, 1);
+    CW_LAUNCHED();
+    float *start = f->d32a;
+    for (int q = 0; q < outer; ++q) {
+        int rc = dc_outer(f, c, d_st, inner, opts->max_sweeps, start);
+        if (rc != CW_OK) return rc;
+    }
+    // a last test marks what settled
+    k_dc_peek<<<(nh + 63) / 64, 64, 0, stream()>>>(d_st, nh);
+    CW_LAUNCHED();
+    if (start_out) *start_out = start;
+    return CW_OK;
+}
+
+// Carry an enqueued solve on, host-driven, until every history has settled
+// (or max_sweeps is spent): for the rare step that needs more outer
+// iterations than a captured graph holds.  `start` is the zeroed correction
+// buffer the enqueued solve ended on.
+int field_relax_finish(cw_field_s *f, const cw_relax_opts *opts, float *start) {
+    DcCache *c = (DcCache *)f->dc_cache;
+    uint32_t nh = f->g.nh;
+    RelaxState *d_st = (RelaxState *)f->stats;
+    int inner = opts->inner_sweeps > 0 ? opts->inner_sweeps : 16;
+    std::vector<RelaxState> hs(nh);
+    for (int64_t outer = 0; outer < opts->max_sweeps / inner + 2; ++outer) {
+        CW_CUDA(cudaMemcpyAsync(hs.data(), d_st, sizeof(RelaxState) * nh, cudaMemcpyDeviceToHost, stream()));
+        CW_CUDA(cudaStreamSynchronize(stream()));
+        bool all = true;
+        for (uint32_t k = 0; k < nh; ++k) all = all && hs[k].done;
+        if (all) return CW_OK;
+        int rc = dc_outer(f, c, d_st, inner, opts->max_sweeps, start);
+        if (rc != CW_OK) return rc;
+        k_dc_peek<<<(nh + 63) / 64, 64, 0, stream()>>>(d_st, nh);
+        CW_LAUNCHED();
+    }
+    return CW_OK;
+}
+
+// The state an enqueued solve left: per history sweeps, residual, settled.
+int field_relax_collect(cw_field_s *f, std::vector<cw_relax_stats> &out, bool &all_settled) {
+    uint32_t nh = f->g.nh;
+    std::vector<RelaxState> hs(nh);
+    CW_CUDA(cudaMemcpyAsync(hs.data(), f->stats, sizeof(RelaxState) * nh, cudaMemcpyDeviceToHost, stream()));
+    CW_CUDA(cudaStreamSynchronize(stream()));
+    out.resize(nh);
+    all_settled = true;
+    for (uint32_t k = 0; k < nh; ++k) {
+        out[k].sweeps = hs[k].sweeps;
+        out[k].last_change = 0.0;
+        out[k].residual = hs[k].last_resid;
+        out[k].status = hs[k].done == 1 ? CW_OK : CW_ERR_SIMULATION;
+        out[k].omega = hs[k].omega;
+        all_settled = all_settled && hs[k].done == 1;
+    }
+    return CW_OK;
+}
+}  // namespace cw
 
 extern "C" {
 
@@ -624,6 +765,14 @@ int cw_field_destroy(cw_field f) {
     if (!f) return CW_OK;
     dfree(f->c); dfree(f->held); dfree(f->uptake); dfree(f->production); dfree(f->lin_sink);
     dfree(f->r32); dfree(f->d32a); dfree(f->d32b); dfree(f->inv32); dfree(f->tmp64); dfree(f->d_span);
+    if (f->dc_cache) {
+        DcCache *c = (DcCache *)f->dc_cache;
+        c->solver.release();
+        c->pr.release();
+        c->prow.release();
+        dfree(c->d_omega);
+        delete c;
+    }
     RelaxState *st = (RelaxState *)f->stats;
     dfree(st);
     f->g.release();

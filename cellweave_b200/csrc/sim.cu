@@ -50,10 +50,21 @@ struct cw_sim_s {
     std::vector<double> omega[2];               // per history, per field
     int32_t depth = 8;
     bool depth_tuned = false;
+    // a step as three captured CUDA graphs (oxygen solve; means and signal
+    // solve; network, fates and lattice), each solve with a fixed budget of
+    // outer iterations checked, and finished host-side if ever short
+    cudaGraphExec_t gexec[3] = {nullptr, nullptr, nullptr};
+    uint64_t gkernels[3] = {0, 0, 0};
+    bool graphs = false;
+    int budget[2] = {0, 0};
+    float *gstart[2] = {nullptr, nullptr};
+    std::vector<cw_relax_stats> last_sig;
+    uint64_t graph_steps = 0, budget_misses = 0;
 };
 
 extern "C" {
 static void tune_begin(cw_sim_s *s);
+static void drop_graphs(cw_sim_s *s);
 }
 
 namespace {
@@ -308,6 +319,7 @@ int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out) {
 
 int cw_sim_destroy(cw_sim s) {
     if (!s) return CW_OK;
+    drop_graphs(s);
     cw_lattice_destroy(s->lat);
     cw_field_destroy(s->o2);
     cw_field_destroy(s->sig);
@@ -399,6 +411,127 @@ static int tune_depth(cw_sim_s *s) {
     return CW_OK;
 }
 
+static void drop_graphs(cw_sim_s *s) {
+    for (auto &g : s->gexec)
+        if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    s->graphs = false;
+}
+
+// One of the three phases of a step, enqueued without host synchronisation.
+static int enqueue_phase(cw_sim_s *s, int p, const cw_relax_opts &o) {
+    const cw_sim_config &c = s->cfg;
+    const int64_t nc = s->nc;
+    int rc;
+    if (p == 0) {
+        if ((rc = couple_uptake_device(s->o2, s->lat, s->d_sink, 8, s->o2->lin_sink, s->sites)) != CW_OK) return rc;
+        if (c.o2_background_sink > 0.0 &&
+            (rc = couple_background_device(s->o2, s->lat, c.o2_background_sink, s->o2->lin_sink)) != CW_OK)
+            return rc;
+        return field_relax_enqueue(s->o2, &o, s->budget[0], &s->gstart[0]);
+    }
+    if (p == 1) {
+        if ((rc = couple_means_device(s->o2, s->lat, s->sum, s->count, s->cell_o2, s->sites)) != CW_OK) return rc;
+        k_inputs<<<(unsigned)blocks(nc), T, 0, stream()>>>(s->lat->type, s->lat->volume, s->lat->d_cell_off, c.nh, nc,
+                                                           c.necrotic_type, s->cell_o2, 0.2, s->inputs, s->alive);
+        CW_LAUNCHED();
+        if (!s->sig) return CW_OK;
+        k_secretion<<<(unsigned)blocks(nc), T, 0, stream()>>>(s->alive, s->cell_o2, nc, c.hypoxic_level,
+                                                              c.signal_secretion, s->secretion);
+        CW_LAUNCHED();
+        if ((rc = couple_production_device(s->sig, s->lat, s->secretion, s->sites)) != CW_OK) return rc;
+        return field_relax_enqueue(s->sig, &o, s->budget[1], &s->gstart[1]);
+    }
+    if (s->sig && (rc = couple_means_device(s->sig, s->lat, s->sum, s->count, s->cell_sig, s->sites)) != CW_OK)
+        return rc;
+    if ((rc = network_step_device(s->net, s->state, s->inputs, nc, nc, nc, c.dt, c.substeps, s->alive)) != CW_OK)
+        return rc;
+    if ((rc = network_mechanics_device(s->net, s->state, nc, nc, s->target32)) != CW_OK) return rc;
+    k_fates<<<(unsigned)blocks(nc), T, 0, stream()>>>(s->alive, s->state, nc, network_role(s->net, 1),
+                                                      c.death_threshold, c.necrotic_type, s->target32, s->lat->type,
+                                                      s->lat->target, s->lat->lambda, c.lambda_volume);
+    CW_LAUNCHED();
+    for (int k = 0; k < c.sweeps; ++k)
+        if ((rc = lattice_sweep(s->lat)) != CW_OK) return rc;
+    return CW_OK;
+}
+
+static int outer_budget(const std::vector<cw_relax_stats> &st, int inner) {
+    int64_t most = 0;
+    for (auto &x : st) most = std::max<int64_t>(most, x.sweeps);
+    return (int)((most + inner - 1) / inner) + 1;
+}
+
+static int build_graphs(cw_sim_s *s, const cw_relax_opts &o) {
+    drop_graphs(s);
+    s->budget[0] = outer_budget(s->last, o.inner_sweeps);
+    s->budget[1] = outer_budget(s->last_sig, o.inner_sweeps);
+    // the factors the graphs will use: the configuration's or the tuned ones
+    int rc0;
+    for (int fi = 0; fi < 2; ++fi) {
+        cw_field_s *f = fi == 0 ? s->o2 : s->sig;
+        if (!f) continue;
+        std::vector<double> om(s->cfg.nh, s->cfg.omega);
+        if (s->cfg.omega <= 0.0) om = s->omega[fi];
+        if ((rc0 = field_dc_prepare(f, s->depth, om)) != CW_OK) return rc0;
+    }
+    const uint32_t mcs = s->lat->mcs;
+    for (int p = 0; p < 3; ++p) {
+        cudaGraph_t g = nullptr;
+        CW_CUDA(cudaStreamBeginCapture(stream(), cudaStreamCaptureModeThreadLocal));
+        const uint64_t before = cw_launch_count();
+        int rc = enqueue_phase(s, p, o);
+        cudaError_t e = cudaStreamEndCapture(stream(), &g);
+        if (rc != CW_OK) { if (g) cudaGraphDestroy(g); return rc; }
+        if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+        s->gkernels[p] = cw_launch_count() - before;
+        e = cudaGraphInstantiate(&s->gexec[p], g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
+    }
+    s->lat->mcs = mcs;  // the capture ran no sweep
+    s->graphs = true;
+    return CW_OK;
+}
+
+// Collect a graph's solve; finish it host-side if its budget fell short.
+static int settle(cw_sim_s *s, int which, const cw_relax_opts &o, std::vector<cw_relax_stats> &st) {
+    cw_field_s *f = which == 0 ? s->o2 : s->sig;
+    bool ok = false;
+    int rc = field_relax_collect(f, st, ok);
+    if (rc != CW_OK) return rc;
+    if (ok) return CW_OK;
+    s->budget_misses += 1;
+    if ((rc = field_relax_finish(f, &o, s->gstart[which])) != CW_OK) return rc;
+    if ((rc = field_relax_collect(f, st, ok)) != CW_OK) return rc;
+    if (!ok) return fail(CW_ERR_SIMULATION, "diffusion did not settle within the sweep limit");
+    s->budget[which] += 1;  // rebuilt with room for one more next step
+    drop_graphs(s);
+    return CW_OK;
+}
+
+static int step_graph(cw_sim_s *s, const cw_relax_opts &o) {
+    int rc;
+    CW_CUDA(cudaGraphLaunch(s->gexec[0], stream()));
+    count_launch(s->gkernels[0]);
+    if ((rc = settle(s, 0, o, s->last)) != CW_OK) return rc;
+    if (!s->graphs) {  // rebuilt below; finish this step on the plain path
+        for (int p = 1; p < 3; ++p) {
+            if ((rc = enqueue_phase(s, p, o)) != CW_OK) return rc;
+            if (p == 1 && s->sig && (rc = settle(s, 1, o, s->last_sig)) != CW_OK) return rc;
+        }
+        return CW_OK;
+    }
+    CW_CUDA(cudaGraphLaunch(s->gexec[1], stream()));
+    count_launch(s->gkernels[1]);
+    if (s->sig && (rc = settle(s, 1, o, s->last_sig)) != CW_OK) return rc;
+    if (!s->graphs) return enqueue_phase(s, 2, o);
+    CW_CUDA(cudaGraphLaunch(s->gexec[2], stream()));
+    count_launch(s->gkernels[2]);
+    s->lat->mcs += (uint32_t)s->cfg.sweeps;
+    s->graph_steps += 1;
+    return CW_OK;
+}
+
 int cw_sim_step(cw_sim s, uint32_t nsteps) {
     const cw_sim_config &c = s->cfg;
     int64_t nc = s->nc;
@@ -415,6 +548,14 @@ int cw_sim_step(cw_sim s, uint32_t nsteps) {
     for (uint32_t step = 0; step < nsteps; ++step, ++s->steps) {
         bool solve = c.relax_every <= 1 || (s->steps % (uint32_t)c.relax_every) == 0;
         o.block_depth = s->depth;
+        const bool graph_ok = c.use_graphs && c.precision == CW_FP32_DC && c.relax_every <= 1 && !s->tune.active &&
+                              s->depth_tuned && s->steps >= 2 && !s->last.empty() &&
+                              (!s->sig || !s->last_sig.empty());
+        if (graph_ok) {
+            if (!s->graphs && (rc = build_graphs(s, o)) != CW_OK) return rc;
+            if ((rc = step_graph(s, o)) != CW_OK) return rc;
+            continue;
+        }
         bool tuning = solve && s->tune.active && s->steps > 0;  // the first solve starts from scratch: not booked
         if (tuning) tune_assign(s);
         if (solve) {
@@ -439,7 +580,8 @@ int cw_sim_step(cw_sim s, uint32_t nsteps) {
                                                                   c.signal_secretion, s->secretion);
             CW_LAUNCHED();
             if ((rc = couple_production_device(s->sig, s->lat, s->secretion, s->sites)) != CW_OK) return rc;
-            std::vector<cw_relax_stats> st2(c.nh);
+            std::vector<cw_relax_stats> &st2 = s->last_sig;
+            st2.resize(c.nh);
             const double *om = c.omega > 0.0 ? nullptr : s->omega[1].data();
             if ((rc = field_relax(s->sig, &o, om, st2.data())) != CW_OK) return rc;
             if (tuning) tune_book(s, 1, st2);
@@ -461,6 +603,13 @@ int cw_sim_step(cw_sim s, uint32_t nsteps) {
         if (tuning && ++s->tune.done >= s->tune.steps) tune_finish(s);
         (void)S;
     }
+    return CW_OK;
+}
+
+int cw_sim_graph_info(cw_sim s, uint64_t *graph_steps, uint64_t *budget_misses, int32_t *budgets) {
+    if (graph_steps) *graph_steps = s->graph_steps;
+    if (budget_misses) *budget_misses = s->budget_misses;
+    if (budgets) { budgets[0] = s->budget[0]; budgets[1] = s->budget[1]; }
     return CW_OK;
 }
 

@@ -210,9 +210,21 @@ class CpmLattice:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value and _lib._LIB is not None:
+        if h is not None and h.value and _lib._LIB is not None and getattr(self, "_owned", True):
             lib().cw_lattice_destroy(h)
             self._h = None
+
+    @classmethod
+    def borrowed(cls, handle, dims, owner):
+        """A view of a lattice another object owns (a Simulation's)."""
+        lat = cls.__new__(cls)
+        lat._h, lat._owned, lat._owner = handle, False, owner
+        lat.dims, w, h, z = _dims(dims)
+        nh = C.c_uint32()
+        call("cw_lattice_count", handle, C.byref(nh))
+        lat.capacity = None
+        lat.temperature = None
+        return lat
 
     @property
     def handle(self):
@@ -492,7 +504,7 @@ class Simulation:
                  nfields=1, o2_dcoef=1.0, o2_sink_by_type=(0.0, 0.01, 0.01), o2_background_sink=0.0, o2_hold=0, signal_dcoef=1.0,
                  signal_decay=0.01, signal_secretion=0.05, hypoxic_level=0.1, tolerance=1e-6, precision=FP32_DC,
                  omega=None, inner_sweeps=0, relax_every=1, dt=0.01, substeps=8, sweeps=1, death_threshold=0.25,
-                 necrotic_type=-1):
+                 necrotic_type=-1, use_graphs=True):
         self.dims, w, h, z = _dims(dims)
         self._keep = [w, h, z]
         nc = np.array(ncells, np.uint32)
@@ -508,7 +520,7 @@ class Simulation:
                              int(o2_hold), float(signal_dcoef), float(signal_decay), float(signal_secretion),
                              float(hypoxic_level), float(tolerance), int(precision), float(omega or 0.0), int(inner_sweeps),
                              int(relax_every), float(dt), int(substeps), int(sweeps), float(death_threshold),
-                             int(necrotic_type))
+                             int(necrotic_type), int(bool(use_graphs)))
         handle = C.c_void_p()
         call("cw_sim_create", C.byref(cfg), network.handle, C.byref(handle))
         self._h = handle
@@ -531,6 +543,13 @@ class Simulation:
         call("cw_sim_tuning", self._h, ptr(a), ptr(b), C.byref(depth), C.byref(active))
         return dict(omega_o2=a, omega_signal=b, depth=depth.value, tuning=bool(active.value))
 
+    def graph_info(self):
+        """(steps replayed from CUDA graphs, budget misses, outer-iteration budgets)."""
+        steps, misses = C.c_uint64(), C.c_uint64()
+        budgets = np.zeros(2, np.int32)
+        call("cw_sim_graph_info", self._h, C.byref(steps), C.byref(misses), ptr(budgets))
+        return steps.value, misses.value, budgets
+
     def stats(self):
         out = np.empty((len(self.dims), 4))
         call("cw_sim_stats", self._h, ptr(out))
@@ -551,6 +570,10 @@ class Simulation:
         out = np.empty(w * h * d, np.int32)
         call("cw_lattice_download", self.lattice_handle(), hist, ptr(out))
         return out.reshape(d, h, w)
+
+    def lattice(self):
+        """The driver's lattice, as a CpmLattice view (owned by this Simulation)."""
+        return CpmLattice.borrowed(self.lattice_handle(), self.dims, self)
 
     def field_values(self, which=0, hist=0):
         w, h, d = self.dims[hist]

@@ -288,6 +288,7 @@ typedef struct {
     int32_t sweeps;              /* Monte Carlo steps per lattice step */
     double death_threshold;      /* survival below it: the necrotic type */
     int32_t necrotic_type;       /* type a dead cell takes (-1: none) */
+    int32_t use_graphs;          /* once tuned, replay each step as captured CUDA graphs */
 } cw_sim_config;
 int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out);
 int cw_sim_destroy(cw_sim sim);
@@ -298,6 +299,9 @@ int cw_sim_step(cw_sim sim, uint32_t steps);
  * the FP32 blocking depth, and whether it is still trying candidates.  It
  * runs when cfg.omega <= 0 with CW_FP32_DC, over the first few steps. */
 int cw_sim_tuning(cw_sim sim, double *omega_o2, double *omega_signal, int32_t *depth, int32_t *tuning);
+/* Steps replayed from CUDA graphs, solves whose graph budget of outer
+ * iterations fell short (finished host-side), and the budgets (2 entries). */
+int cw_sim_graph_info(cw_sim sim, uint64_t *graph_steps, uint64_t *budget_misses, int32_t *budgets);
 /* Handles the driver owns, for inspection with the calls above. */
 int cw_sim_lattice(cw_sim sim, cw_lattice *lat);
 int cw_sim_field(cw_sim sim, int32_t which, cw_field *f);

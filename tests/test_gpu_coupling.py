@@ -103,3 +103,26 @@ def test_a_history_in_a_batch_runs_as_it_runs_alone():
     both.step(3)
     alone.step(3)
     np.testing.assert_array_equal(both.grid(1), alone.grid(0))
+
+
+def test_graph_replay_gives_the_same_histories():
+    net_text = synthetic.network_toml(8, seed=8)
+    import tempfile, os
+    with tempfile.TemporaryDirectory() as d:
+        p = os.path.join(d, "n.toml")
+        open(p, "w").write(net_text)
+        net = cw.Network.load(p, 49)
+    cfg = synthetic.campaign(per_size=1, sizes=(64, 96, 128))
+    cfg.pop("S")
+    cfg["omega"] = 1.9
+    plain = cw.Simulation(net, **dict(cfg, use_graphs=False))
+    graph = cw.Simulation(net, **dict(cfg, use_graphs=True))
+    plain.step(8)
+    graph.step(8)
+    steps, misses, budgets = graph.graph_info()
+    assert steps >= 5 and (budgets > 0).all()
+    assert plain.graph_info()[0] == 0
+    for k in range(3):
+        np.testing.assert_array_equal(plain.grid(k), graph.grid(k))
+        np.testing.assert_array_equal(plain.field_values(0, k), graph.field_values(0, k))
+        assert graph.records_match_grid(k)
