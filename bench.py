@@ -217,6 +217,8 @@ def run_ours(args, rank, world, dist):
         ms = float(t.item())
     value = world * nh * args.steps / (ms / 1e3)
     stats = sim.stats()
+    gsteps, gmiss, gbudget = sim.graph_info()
+    graphs = {"steps_replayed": int(gsteps), "budget_misses": int(gmiss), "outer_budgets": [int(b) for b in gbudget]}
     if args.profile_step:
         _lib.check(L.cw_profiler_start())
         sim.step(1)
@@ -312,6 +314,7 @@ def run_ours(args, rank, world, dist):
     if not args.no_fit and world == 1:
         fit = run_fit(args, L)
     return dict(value=value, ms=ms / args.steps, launches=launches, clocks=clk, e2e=e2e, roofline=roofline, fit=fit,
+                graphs=graphs,
                 plain=plain, stats=stats, nh=nh, cfg=cfg, tuned=tuned)
 
 
@@ -414,7 +417,7 @@ def main():
                     gpu_launches=r["launches"], roofline=r["roofline"], cpu_baseline=cpu,
                     plain=r["plain"],
                     batched_over_plain=(r["value"] / r["plain"]["value"]) if r["plain"] else None,
-                    fit=r["fit"],
+                    fit=r["fit"], cuda_graphs=r["graphs"],
                     sor_gbs=r["roofline"]["achieved"], sor_site_sweeps_per_s=r["roofline"]["site_sweeps_per_s"],
                     living_cells=float(r["stats"][:, 0].sum()), last_residual_max=float(r["stats"][:, 3].max()),
                     autotuned={"omega_o2": sorted(set(float(v) for v in r["tuned"]["omega_o2"])),
