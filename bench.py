@@ -350,8 +350,10 @@ def run_fit(args, L):
         L.cw_synchronize()
         L.cw_event_record(6)
         loss, grad = fit.gradient()
-        d = -grad * p * p
-        q = np.maximum(p + 0.05 / (np.abs(d / p).max() + 1e-300) * d, 1e-6)
+        d = -grad * p * p  # steepest descent in log p (a parameter at zero stays there)
+        rel = np.abs(d / np.where(p != 0, p, 1.0)).max()
+        q = np.maximum(p + 0.05 / (rel + 1e-300) * d, 0.0)
+        q[0] = max(q[0], 1e-3)
         fit.params = q
         lq = fit.forward()[0]
         L.cw_event_record(7)
