@@ -289,32 +289,40 @@ def run_ours(args, rank, world, dist):
                              "read once and the correction written once; the launch's half-sweeps stay on chip"}
 
     # ---- the plain path: each history stepped alone (rank 0 at N=1)
-    plain = None
+    plain = plain_graphs = None
     if not args.no_plain and world == 1:
-        total_ms, units = 0.0, 0
         del sim
-        for k in range(nh):
-            one = {kk: (vv[k:k + 1] if kk in ("dims", "ncells", "seeds") else vv) for kk, vv in cfg.items()}
-            s1 = cw.Simulation(net, **one)
-            # warm up through the autotuner's trials (seven candidates, one history)
-            while s1.tuning()["tuning"]:
-                s1.step(1)
-            s1.step(1)
-            L.cw_synchronize()
-            L.cw_event_record(4)
-            s1.step(args.steps if k < 4 or args.steps <= 5 else 5)
-            L.cw_event_record(5)
-            L.cw_synchronize()
-            total_ms += event_ms(L, 4, 5)
-            units += args.steps if k < 4 or args.steps <= 5 else 5
-            del s1
-        plain = {"value": units / (total_ms / 1e3), "unit": UNIT,
-                 "how": "the same 64 histories, each its own Simulation stepped alone (one history per launch)"}
+
+        def one_at_a_time(graphs):
+            total_ms, units = 0.0, 0
+            for k in range(nh):
+                one = {kk: (vv[k:k + 1] if kk in ("dims", "ncells", "seeds") else vv) for kk, vv in cfg.items()}
+                s1 = cw.Simulation(net, **one, use_graphs=graphs)
+                # warm up through the autotuner's trials (seven candidates, one history)
+                while s1.tuning()["tuning"]:
+                    s1.step(1)
+                s1.step(2)
+                n = args.steps if args.steps <= 5 else 5
+                L.cw_synchronize()
+                L.cw_event_record(4)
+                s1.step(n)
+                L.cw_event_record(5)
+                L.cw_synchronize()
+                total_ms += event_ms(L, 4, 5)
+                units += n
+                del s1
+            return units / (total_ms / 1e3)
+
+        plain = {"value": one_at_a_time(False), "unit": UNIT,
+                 "how": "the same 64 histories, each its own Simulation stepped alone: one history per launch, "
+                        "launched kernel by kernel (the path without the batching form)"}
+        plain_graphs = {"value": one_at_a_time(True), "unit": UNIT,
+                        "how": "as plain, each history's tuned step replayed from CUDA graphs"}
     fit = None
     if not args.no_fit and world == 1:
         fit = run_fit(args, L)
     return dict(value=value, ms=ms / args.steps, launches=launches, clocks=clk, e2e=e2e, roofline=roofline, fit=fit,
-                graphs=graphs,
+                graphs=graphs, plain_graphs=plain_graphs,
                 plain=plain, stats=stats, nh=nh, cfg=cfg, tuned=tuned)
 
 
@@ -417,7 +425,7 @@ def main():
         line = dict(base, value=r["value"], ms_per_step=r["ms"], dtype="f32+f64",
                     config=config_key(args.workload, r["cfg"]), clocks=r["clocks"], e2e=r["e2e"],
                     gpu_launches=r["launches"], roofline=r["roofline"], cpu_baseline=cpu,
-                    plain=r["plain"],
+                    plain=r["plain"], plain_with_graphs=r["plain_graphs"],
                     batched_over_plain=(r["value"] / r["plain"]["value"]) if r["plain"] else None,
                     fit=r["fit"], cuda_graphs=r["graphs"],
                     sor_gbs=r["roofline"]["achieved"], sor_site_sweeps_per_s=r["roofline"]["site_sweeps_per_s"],

@@ -60,6 +60,8 @@ struct cw_sim_s {
     float *gstart[2] = {nullptr, nullptr};
     std::vector<cw_relax_stats> last_sig;
     uint64_t graph_steps = 0, budget_misses = 0;
+    int need[2] = {0, 0};        // most outer iterations a solve needed over the current window
+    int window = 0;              // graph steps in the window
 };
 
 extern "C" {
@@ -463,8 +465,8 @@ static int outer_budget(const std::vector<cw_relax_stats> &st, int inner) {
 
 static int build_graphs(cw_sim_s *s, const cw_relax_opts &o) {
     drop_graphs(s);
-    s->budget[0] = outer_budget(s->last, o.inner_sweeps);
-    s->budget[1] = outer_budget(s->last_sig, o.inner_sweeps);
+    if (s->budget[0] <= 0) s->budget[0] = outer_budget(s->last, o.inner_sweeps);
+    if (s->budget[1] <= 0) s->budget[1] = outer_budget(s->last_sig, o.inner_sweeps);
     // the factors the graphs will use: the configuration's or the tuned ones
     int rc0;
     for (int fi = 0; fi < 2; ++fi) {
@@ -499,6 +501,7 @@ static int settle(cw_sim_s *s, int which, const cw_relax_opts &o, std::vector<cw
     bool ok = false;
     int rc = field_relax_collect(f, st, ok);
     if (rc != CW_OK) return rc;
+    s->need[which] = std::max(s->need[which], outer_budget(st, o.inner_sweeps) - 1);
     if (ok) return CW_OK;
     s->budget_misses += 1;
     if ((rc = field_relax_finish(f, &o, s->gstart[which])) != CW_OK) return rc;
@@ -529,6 +532,16 @@ static int step_graph(cw_sim_s *s, const cw_relax_opts &o) {
     count_launch(s->gkernels[2]);
     s->lat->mcs += (uint32_t)s->cfg.sweeps;
     s->graph_steps += 1;
+    // every 8 steps, trim a budget well above what the solves needed: kernels
+    // of a settled history exit at once, but their launches still cost
+    if (++s->window >= 8) {
+        bool rebuild = false;
+        for (int w = 0; w < 2; ++w)
+            if (s->need[w] > 0 && s->budget[w] > s->need[w] + 2) { s->budget[w] = s->need[w] + 1; rebuild = true; }
+        s->need[0] = s->need[1] = 0;
+        s->window = 0;
+        if (rebuild) drop_graphs(s);
+    }
     return CW_OK;
 }
 
