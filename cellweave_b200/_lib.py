@@ -133,6 +133,7 @@ SIGNATURES = {
     "cw_field_step": (C.c_int, [P, D]),
     "cw_field_relax_noalloc": (C.c_int, [P, P, P, P, P, U32, U32, D, D, D, D, D, I64, I32, P, P]),
     "cw_field_time_inner": (C.c_int, [P, I32, I32, D, P, P]),
+    "cw_field_inner_correction": (C.c_int, [P, U32, P]),
     "cw_couple_uptake": (C.c_int, [P, P, I32, P, I32]),
     "cw_couple_background_uptake": (C.c_int, [P, P, D]),
     "cw_couple_production": (C.c_int, [P, P, U32, U32, P]),

@@ -207,8 +207,11 @@ struct cw_field_s {
     bool floor = true;               // updates floored at zero (pde.rs:395); off for adjoint solves
     std::vector<cw::Span> spans;     // free_span of every history, cached
     double dcoef = 0.2, decay = 0.0, source = 0.0;
-    // scratch of the FP32 defect-correction solve and the explicit step
+    // scratch of the FP32 defect-correction solve and the explicit step:
+    // r32 = omega r / den, inv32 = omega D / den (the SOR's coefficients, 0 on
+    // held pixels), d32a / d32b the correction, ping-ponged
     float *r32 = nullptr, *d32a = nullptr, *d32b = nullptr, *inv32 = nullptr;
+    float *last_inner = nullptr;     // d32a or d32b: where cw_field_time_inner's correction is
     double *tmp64 = nullptr;
     void *stats = nullptr;           // per-history solve state (device)
     cw::Span *d_span = nullptr;

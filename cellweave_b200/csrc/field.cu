@@ -124,8 +124,9 @@ __global__ void k_sor64_half(FieldView fv, const int32_t *blk, int nh, const Spa
 }
 
 // Projected residual max |b - A c| over the free pixels of each history;
-// optionally writes r in FP32 for the defect-correction solve, the FP32
-// inverse diagonal (0 on held pixels), and zeroes the correction.
+// optionally writes the FP32 coefficients of the defect-correction solve's
+// SOR on A d = r, the relaxation factor folded in: omega r / den and
+// omega D / den (both 0 on held pixels), and zeroes the correction.
 __global__ void k_residual64(FieldView fv, const int32_t *blk, int nh, RelaxState *st, float *r32, float *inv32,
                              float *dz, int skip_done) {
     __shared__ int s_h;
@@ -153,8 +154,11 @@ __global__ void k_residual64(FieldView fv, const int32_t *blk, int nh, RelaxStat
             double r = add_sources(fv, i, fv.d * sum) - den * cv;
             if (fv.floor && cv <= 0.0 && r < 0.0) r = 0.0;
             worst = fabs(r);
-            r_out = (float)r;
-            inv_out = den > 0.0 ? (float)(1.0 / den) : 0.0f;
+            if (den > 0.0) {
+                const double q = st[h].omega / den;
+                r_out = (float)(q * r);
+                inv_out = (float)(q * fv.d);
+            }
         }
         if (r32) r32[i] = r_out;
         if (inv32) inv32[i] = inv_out;
@@ -185,8 +189,8 @@ __global__ void k_check(RelaxState *st, int nh, int64_t index, int residual_coun
 
 // Defect correction fused with the next residual, in two launches, one per
 // colour: c += d (floored at zero as the reference's update is, pde.rs:395),
-// then r = b - A c at the corrected field, written in FP32 for the next FP32
-// solve, with the correction zeroed behind it.  The first launch corrects the
+// then r = b - A c at the corrected field, written in FP32 as omega r / den
+// for the next FP32 solve, with the correction zeroed behind it.  The first launch corrects the
 // red pixels and reads its black neighbours as c + d; the second corrects the
 // black ones and reads its red neighbours as they now stand, so no thread
 // reads a value another thread of the same launch writes.  One block takes
@@ -235,7 +239,7 @@ __global__ void __launch_bounds__(256) k_dc_update(FieldView fv, const int32_t *
             if (fl && ci <= 0.0 && r < 0.0) r = 0.0;
             worst = fabs(r);
             fv.c[i] = ci;
-            r32[i] = (float)r;
+            r32[i] = den > 0.0 ? (float)(st[h].omega / den * r) : 0.f;
             dlt[i] = 0.f;
         }
     }
@@ -645,6 +649,7 @@ static int relax_fp32dc(cw_field_s *f, const cw_relax_opts &o, RelaxState *d_st,
             if ((rc = dc_outer(f, c, d_st, inner, o.max_sweeps, start)) != CW_OK) return rc;
         CW_CUDA(cudaMemcpyAsync(hs.data(), d_st, sizeof(RelaxState) * nh, cudaMemcpyDeviceToHost, stream()));
         CW_CUDA(cudaStreamSynchronize(stream()));
+        if ((rc = sor32_wait_failed()) != CW_OK) return rc;
         bool all = true;
         for (uint32_t k = 0; k < nh; ++k) all = all && hs[k].done;
         if (all) break;
@@ -717,6 +722,8 @@ int field_relax_collect(cw_field_s *f, std::vector<cw_relax_stats> &out, bool &a
     std::vector<RelaxState> hs(nh);
     CW_CUDA(cudaMemcpyAsync(hs.data(), f->stats, sizeof(RelaxState) * nh, cudaMemcpyDeviceToHost, stream()));
     CW_CUDA(cudaStreamSynchronize(stream()));
+    int rc = sor32_wait_failed();
+    if (rc != CW_OK) return rc;
     out.resize(nh);
     all_settled = true;
     for (uint32_t k = 0; k < nh; ++k) {
@@ -1101,7 +1108,15 @@ extern "C" int cw_field_time_inner(cw_field f, int32_t sweeps, int32_t depth, do
     *launches = (int64_t)(cw_launch_count() - before);
     cudaEventDestroy(a);
     cudaEventDestroy(b);
+    f->last_inner = solver.result();
     solver.release();
     prow.release();
+    return sor32_wait_failed();
+}
+
+extern "C" int cw_field_inner_correction(cw_field f, uint32_t hist, float *out) {
+    if (hist >= f->g.nh) return fail(CW_ERR_NOT_FOUND, "no history " + std::to_string(hist));
+    if (!f->last_inner) return fail(CW_ERR_CONFIG, "no inner solve has run on this field");
+    CW_CUDA(cudaMemcpy(out, f->last_inner + f->g.off[hist], sizeof(float) * f->g.sites(hist), cudaMemcpyDeviceToHost));
     return CW_OK;
 }

@@ -1,30 +1,47 @@
-// FP32 red-black SOR on the correction equation of the defect-correction
-// solve (see field.cu).  Built with fused multiply-add: this is the fast
-// path, and its error is removed by the FP64 residual and correction steps.
+// FP32 red-black SOR on the correction equation A d = r of the
+// defect-correction solve (see field.cu).  Built with fused multiply-add:
+// this is the fast path, and its error is removed by the FP64 residual and
+// correction steps.  The coefficients come with the relaxation factor folded
+// in (field.cu writes them): b = omega r / den and a = omega D / den, so one
+// update is d' = (1 - omega) d + a (sum of the four neighbours) + b, two
+// fused multiply-adds after the neighbour sum.
 //
-// Temporal blocking.  A flat history is cut into tiles whose interior is
-// (64 - 2 DEPTH) pixels square; a block loads the tile with a halo DEPTH
-// pixels deep (a 64 x 64 window) and runs DEPTH half-sweeps on it before
-// writing the interior back to the other buffer.  Every window pixel is
-// updated at every half-sweep, its missing neighbours read as zero; the
-// error this makes at the window's edge moves in by one ring per half-sweep,
-// so after DEPTH of them the interior is exactly what DEPTH global
-// half-sweeps give.  The correction crosses HBM once per DEPTH half-sweeps.
+// Temporal blocking.  A flat history is cut into windows; a block takes a
+// window and runs DEPTH half-sweeps on it before writing its interior back to
+// the other buffer.  Every window pixel is updated at every half-sweep, its
+// missing neighbours read as zero; the error this makes at a window edge that
+// lies inside the history moves in by one ring per half-sweep, so after DEPTH
+// of them every pixel at least DEPTH from such an edge is exactly what DEPTH
+// global half-sweeps give.  A window edge on or beyond the history's border
+// makes no error (outside pixels are zero there too), so the interior reaches
+// that border.  The correction crosses HBM once per DEPTH half-sweeps.
 //
-// Layout.  Warp w owns window rows 8w .. 8w+7, lane l the column pair
-// (2l, 2l+1): one pixel of each colour per row, so every half-sweep gives
-// every thread the same work.  The correction, the right-hand side and the
-// inverse diagonal of a thread's sixteen pixels stay in registers for the
-// whole launch.  Neighbours come from the thread's own registers (the other
-// pixel of the pair, the rows above and below), from the next lane by a warp
-// shuffle, and across a warp boundary from the one row each neighbouring
-// warp publishes in shared memory after every half-sweep (double-buffered,
-// so one barrier per half-sweep suffices).
+// The wide kernel (rows 16-byte aligned in every history, the campaign's
+// case): 128 x 64 windows, a warp per 8 rows, a lane per 4 consecutive
+// columns held as float4 registers (two pixels of each colour per row, one
+// warp shuffle per two updates).  Blocks are persistent, two per SM; while a
+// block sweeps one window in registers, the TMA engine brings the next
+// window's correction and coefficients into shared memory (one mbarrier,
+// 96 KB), so the HBM reads overlap the sweeps.  Windows start at x = k (128 -
+// 2 DEPTH), a multiple of 4 floats as TMA needs, and at y = k (64 - 2 DEPTH).
+//
+// The narrow kernel (any width): 64 x 64 windows, a lane per column pair,
+// plain loads, one window per block.
+//
+// Between warps, each warp publishes its top and bottom rows in shared memory
+// after every half-sweep (double-buffered, so one barrier per half-sweep).
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <mutex>
+
 #include "cw_internal.cuh"
 #include "field_kernels.cuh"
 
 namespace cw {
 namespace {
+
+// ------------------------------------------------------------------ narrow windows
 
 constexpr int WIN = 64;            // window side
 constexpr int WARPS = 8;           // warps per block
@@ -37,21 +54,17 @@ template <int C>
 __device__ __forceinline__ void half_sweep(float (&d0)[ROWS], float (&d1)[ROWS], const float (&r0)[ROWS],
                                            const float (&r1)[ROWS], const float (&i0)[ROWS],
                                            const float (&i1)[ROWS], float ab0, float ab1, float be0, float be1,
-                                           int lane, float om, float dcoef) {
+                                           float lm, float rm, float omc) {
 #pragma unroll
     for (int j = 0; j < ROWS; ++j) {
         if (((C + j) & 1) == 0) {  // the even column of the pair
-            float left = __shfl_up_sync(0xffffffffu, d1[j], 1);
-            left = lane == 0 ? 0.f : left;
+            const float left = __shfl_up_sync(0xffffffffu, d1[j], 1);
             const float up = j > 0 ? d0[j - 1] : ab0, down = j < ROWS - 1 ? d0[j + 1] : be0;
-            const float old = d0[j];
-            d0[j] = fmaf(om, fmaf(fmaf(dcoef, (left + d1[j]) + (up + down), r0[j]), i0[j], -old), old);
+            d0[j] = fmaf(i0[j], fmaf(lm, left, d1[j]) + (up + down), fmaf(omc, d0[j], r0[j]));
         } else {  // the odd column
-            float right = __shfl_down_sync(0xffffffffu, d0[j], 1);
-            right = lane == 31 ? 0.f : right;
+            const float right = __shfl_down_sync(0xffffffffu, d0[j], 1);
             const float up = j > 0 ? d1[j - 1] : ab1, down = j < ROWS - 1 ? d1[j + 1] : be1;
-            const float old = d1[j];
-            d1[j] = fmaf(om, fmaf(fmaf(dcoef, (d0[j] + right) + (up + down), r1[j]), i1[j], -old), old);
+            d1[j] = fmaf(i1[j], fmaf(rm, right, d0[j]) + (up + down), fmaf(omc, d1[j], r1[j]));
         }
     }
 }
@@ -63,7 +76,7 @@ __global__ void __launch_bounds__(32 * WARPS) k_sor32_tb(const float *__restrict
                                                          const int64_t *__restrict__ off,
                                                          const int32_t *__restrict__ blk, int nh,
                                                          const float *__restrict__ omega, const int32_t *done,
-                                                         int done_stride, int nhalf, int start_colour, float dcoef) {
+                                                         int done_stride, int nhalf, int start_colour) {
     constexpr int IN = WIN - 2 * DEPTH;  // interior side
     // edge rows each warp publishes, double-buffered by half-sweep parity:
     // [buffer][warp][0 top, 1 bottom][column]
@@ -79,7 +92,10 @@ __global__ void __launch_bounds__(32 * WARPS) k_sor32_tb(const float *__restrict
     const int t = blockIdx.x - blk[h];
     const int gx0 = (t % ntx) * IN - DEPTH, gy0 = (t / ntx) * IN - DEPTH;
     const int64_t base = off[h];
-    const float om = omega[h];
+    const float omc = 1.f - omega[h];
+    // the lanes at the window's sides have no neighbour across it (a zero);
+    // the shuffle's own value, finite, is multiplied by zero instead
+    const float lm = lane == 0 ? 0.f : 1.f, rm = lane == 31 ? 0.f : 1.f;
     const int gx = gx0 + 2 * lane;
     const bool in0 = gx >= 0 && gx < dm.x, in1 = gx + 1 >= 0 && gx + 1 < dm.x;
     float d0[ROWS], d1[ROWS], r0[ROWS], r1[ROWS], i0[ROWS], i1[ROWS];
@@ -110,9 +126,9 @@ __global__ void __launch_bounds__(32 * WARPS) k_sor32_tb(const float *__restrict
         const float be0 = warp < WARPS - 1 ? edge[buf][warp + 1][0][2 * lane] : 0.f;
         const float be1 = warp < WARPS - 1 ? edge[buf][warp + 1][0][2 * lane + 1] : 0.f;
         if (((start_colour + s) & 1) == 0)
-            half_sweep<0>(d0, d1, r0, r1, i0, i1, ab0, ab1, be0, be1, lane, om, dcoef);
+            half_sweep<0>(d0, d1, r0, r1, i0, i1, ab0, ab1, be0, be1, lm, rm, omc);
         else
-            half_sweep<1>(d0, d1, r0, r1, i0, i1, ab0, ab1, be0, be1, lane, om, dcoef);
+            half_sweep<1>(d0, d1, r0, r1, i0, i1, ab0, ab1, be0, be1, lm, rm, omc);
         // the other buffer was last read before the previous barrier
         publish(buf ^ 1);
         __syncthreads();
@@ -129,11 +145,211 @@ __global__ void __launch_bounds__(32 * WARPS) k_sor32_tb(const float *__restrict
     }
 }
 
+// ------------------------------------------------------------------ wide windows (TMA)
+
+constexpr int WX = 128, WY = 64;     // window columns, rows
+constexpr int WWARPS = 8;            // warps per block
+constexpr int WROWS = WY / WWARPS;   // rows per warp
+constexpr int STAGE = WX * WY;       // floats per array of the staged window
+constexpr int EDGE_F4 = 2 * WWARPS * 2 * (WX / 4);
+constexpr size_t WIDE_SMEM = (size_t)3 * STAGE * sizeof(float) + (size_t)EDGE_F4 * sizeof(float4);
+constexpr unsigned long long WAIT_NS = 2000000000ull;  // a stage that has not landed in 2 s is an error
+
+__device__ int g_wide_wait_failed;
+
+__device__ __forceinline__ uint32_t sh_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// The phase `parity` of the stage's barrier, waited for WAIT_NS at most.
+__device__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = global_ns();
+    for (;;) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (global_ns() - t0 > WAIT_NS) return false;
+    }
+}
+
+// One 128 x 64 box of a history's array into shared memory, completing on `bar`.
+__device__ __forceinline__ void tma_box(float *dst, const CUtensorMap *map, uint32_t bar, int x, int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+        :
+        : "r"(sh_addr(dst)), "l"((uint64_t)map), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+
+// The first window at or after `t`, in steps of `step`, whose history is not settled.
+__device__ __forceinline__ int next_live(int t, int ntiles, int step, const int4 *tiles, const int32_t *done,
+                                         int stride) {
+    while (t < ntiles && done[(int64_t)tiles[t].x * stride]) t += step;
+    return t;
+}
+
+// One half-sweep of colour C over a lane's 8 rows x 4 columns.  Column c of
+// row j has colour (c + j) mod 2 (windows start at even x and y): colour C
+// takes columns 0 and 2 of the rows with C + j even, 1 and 3 of the others.
+template <int C>
+__device__ __forceinline__ void half4(float4 (&d)[WROWS], const float4 (&a)[WROWS], const float4 (&b)[WROWS],
+                                      const float4 ab, const float4 be, float lm, float rm, float omc) {
+#pragma unroll
+    for (int j = 0; j < WROWS; ++j) {
+        const float4 up = j > 0 ? d[j - 1] : ab, dn = j < WROWS - 1 ? d[j + 1] : be;
+        if (((C + j) & 1) == 0) {
+            const float left = __shfl_up_sync(0xffffffffu, d[j].w, 1);
+            const float s0 = fmaf(lm, left, d[j].y) + (up.x + dn.x);
+            const float s2 = (d[j].y + d[j].w) + (up.z + dn.z);
+            d[j].x = fmaf(a[j].x, s0, fmaf(omc, d[j].x, b[j].x));
+            d[j].z = fmaf(a[j].z, s2, fmaf(omc, d[j].z, b[j].z));
+        } else {
+            const float right = __shfl_down_sync(0xffffffffu, d[j].x, 1);
+            const float s1 = (d[j].x + d[j].z) + (up.y + dn.y);
+            const float s3 = fmaf(rm, right, d[j].z) + (up.w + dn.w);
+            d[j].y = fmaf(a[j].y, s1, fmaf(omc, d[j].y, b[j].y));
+            d[j].w = fmaf(a[j].w, s3, fmaf(omc, d[j].w, b[j].w));
+        }
+    }
+}
+
+// maps: 4 per history (d32a, d32b, r32, inv32); src_map picks the buffer
+// read (0 or 1), dst is the other.  tiles: (history, x0, y0, 0) per window.
+template <int DEPTH>
+__global__ void __launch_bounds__(32 * WWARPS, 2)
+    k_sor32_wide(const CUtensorMap *__restrict__ maps, int src_map, float *__restrict__ dst,
+                 const int4 *__restrict__ tiles, int ntiles, const int4 *__restrict__ dims,
+                 const int64_t *__restrict__ off, const float *__restrict__ omega, const int32_t *done,
+                 int done_stride, int nhalf, int start_colour) {
+    extern __shared__ __align__(128) float smem[];
+    const float4 *sd = (const float4 *)smem, *sb = (const float4 *)(smem + STAGE),
+                 *sa = (const float4 *)(smem + 2 * STAGE);
+    float4 *edge = (float4 *)(smem + 3 * STAGE);  // [buffer][warp][0 top, 1 bottom][lane]
+    __shared__ __align__(8) uint64_t bar_word;
+    __shared__ int s_next, s_fail;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t bar = sh_addr(&bar_word);
+    auto issue = [&](int t) {
+        const int4 tl = tiles[t];
+        const CUtensorMap *m = maps + 4 * tl.x;
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+                     "r"((uint32_t)(3 * STAGE * sizeof(float)))
+                     : "memory");
+        tma_box(smem, m + src_map, bar, tl.y, tl.z);
+        tma_box(smem + STAGE, m + 2, bar, tl.y, tl.z);
+        tma_box(smem + 2 * STAGE, m + 3, bar, tl.y, tl.z);
+    };
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        s_fail = 0;
+        const int t = next_live(blockIdx.x, ntiles, gridDim.x, tiles, done, done_stride);
+        s_next = t;
+        if (t < ntiles) issue(t);
+    }
+    __syncthreads();
+    int t = s_next;
+    uint32_t parity = 0;
+    const float lm = lane == 0 ? 0.f : 1.f, rm = lane == 31 ? 0.f : 1.f;
+    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    auto ed = [&](int buf, int w, int side) -> float4 & { return edge[((buf * WWARPS + w) * 2 + side) * 32 + lane]; };
+    while (t < ntiles) {
+        const int4 tl = tiles[t];
+        const int h = tl.x, x0 = tl.y, y0 = tl.z;
+        if (!mbar_wait_bounded(bar, parity)) s_fail = 1;
+        float4 d[WROWS], a[WROWS], b[WROWS];
+#pragma unroll
+        for (int j = 0; j < WROWS; ++j) {
+            const int k = (warp * WROWS + j) * 32 + lane;
+            d[j] = sd[k];
+            b[j] = sb[k];
+            a[j] = sa[k];
+        }
+        __syncthreads();  // the stage is read: free for the next window
+        if (s_fail) {
+            // leave no copy in flight into this block's shared memory
+            if (threadIdx.x == 0) {
+                mbar_wait_bounded(bar, parity);
+                atomicExch(&g_wide_wait_failed, 1);
+            }
+            return;
+        }
+        parity ^= 1u;
+        if (threadIdx.x == 0) {
+            const int n = next_live(t + gridDim.x, ntiles, gridDim.x, tiles, done, done_stride);
+            s_next = n;
+            if (n < ntiles) {
+                // the generic-proxy reads of the stage before the async-proxy writes
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                issue(n);
+            }
+        }
+        const float omc = 1.f - omega[h];
+        ed(0, warp, 0) = d[0];
+        ed(0, warp, 1) = d[WROWS - 1];
+        __syncthreads();
+        const int tn = s_next;
+        for (int s = 0; s < nhalf; ++s) {
+            const int buf = s & 1;
+            const float4 ab = warp > 0 ? ed(buf, warp - 1, 1) : z4;
+            const float4 be = warp < WWARPS - 1 ? ed(buf, warp + 1, 0) : z4;
+            if (((start_colour + s) & 1) == 0)
+                half4<0>(d, a, b, ab, be, lm, rm, omc);
+            else
+                half4<1>(d, a, b, ab, be, lm, rm, omc);
+            if (s + 1 < nhalf) {
+                // the other buffer was last read before the previous barrier
+                ed(buf ^ 1, warp, 0) = d[0];
+                ed(buf ^ 1, warp, 1) = d[WROWS - 1];
+                __syncthreads();
+            }
+        }
+        // the interior back to global memory
+        const int4 dm = dims[h];
+        const int ix0 = x0 == 0 ? 0 : x0 + DEPTH, ix1 = x0 + WX >= dm.x ? dm.x : x0 + WX - DEPTH;
+        const int iy0 = y0 == 0 ? 0 : y0 + DEPTH, iy1 = y0 + WY >= dm.y ? dm.y : y0 + WY - DEPTH;
+        const int gx = x0 + 4 * lane;
+        float *base = dst + off[h];
+#pragma unroll
+        for (int j = 0; j < WROWS; ++j) {
+            const int gy = y0 + warp * WROWS + j;
+            if (gy < iy0 || gy >= iy1) continue;
+            float *row = base + (int64_t)gy * dm.x + gx;
+            if (gx >= ix0 && gx + 4 <= ix1) {
+                *(float4 *)row = d[j];
+            } else {
+                if (gx >= ix0 && gx < ix1) row[0] = d[j].x;
+                if (gx + 1 >= ix0 && gx + 1 < ix1) row[1] = d[j].y;
+                if (gx + 2 >= ix0 && gx + 2 < ix1) row[2] = d[j].z;
+                if (gx + 3 >= ix0 && gx + 3 < ix1) row[3] = d[j].w;
+            }
+        }
+        t = tn;
+    }
+}
+
+// ------------------------------------------------------------------ volumes
+
 // One half-sweep in place, any depth of lattice (volumes).
 __global__ void k_sor32_half(float *__restrict__ dlt, const float *__restrict__ rhs, const float *__restrict__ inv,
                              const int4 *__restrict__ dims, const int64_t *__restrict__ off,
                              const int32_t *__restrict__ blk, int nh, const float *__restrict__ omega,
-                             const int32_t *done, int done_stride, int colour, float dcoef) {
+                             const int32_t *done, int done_stride, int colour) {
     __shared__ int s_h;
     if (threadIdx.x == 0) s_h = plan_history(blk, nh, blockIdx.x);
     __syncthreads();
@@ -150,21 +366,18 @@ __global__ void k_sor32_half(float *__restrict__ dlt, const float *__restrict__ 
     if (x >= dm.x) return;
     int64_t w = dm.x, slice = (int64_t)dm.x * dm.y;
     int64_t i = off[h] + row * w + x;
-    float iv = inv[i];
-    if (iv == 0.f) return;
-    float sum = 0.f;
-    if (x > 0) sum += dlt[i - 1];
-    if (x + 1 < dm.x) sum += dlt[i + 1];
-    if (y > 0) sum += dlt[i - w];
-    if (y + 1 < dm.y) sum += dlt[i + w];
-    if (z > 0) sum += dlt[i - slice];
-    if (z + 1 < dm.z) sum += dlt[i + slice];
-    float old = dlt[i];
-    dlt[i] = old + omega[h] * ((rhs[i] + dcoef * sum) * iv - old);
+    // (x pair) + (y pair) [+ (z pair)]: in 2D the windowed kernels' order
+    const float xm = x > 0 ? dlt[i - 1] : 0.f, xp = x + 1 < dm.x ? dlt[i + 1] : 0.f;
+    const float ym = y > 0 ? dlt[i - w] : 0.f, yp = y + 1 < dm.y ? dlt[i + w] : 0.f;
+    float sum = (xm + xp) + (ym + yp);
+    if (dm.z > 1) sum += (z > 0 ? dlt[i - slice] : 0.f) + (z + 1 < dm.z ? dlt[i + slice] : 0.f);
+    dlt[i] = fmaf(inv[i], sum, fmaf(1.f - omega[h], dlt[i], rhs[i]));
 }
 
 typedef void (*TbKernel)(const float *, float *, const float *, const float *, const int4 *, const int64_t *,
-                         const int32_t *, int, const float *, const int32_t *, int, int, int, float);
+                         const int32_t *, int, const float *, const int32_t *, int, int, int);
+typedef void (*WideKernel)(const CUtensorMap *, int, float *, const int4 *, int, const int4 *, const int64_t *,
+                           const float *, const int32_t *, int, int, int);
 
 TbKernel tb_kernel(int depth) {
     switch (depth) {
@@ -173,6 +386,91 @@ TbKernel tb_kernel(int depth) {
     case 6: return k_sor32_tb<6>;
     default: return k_sor32_tb<8>;
     }
+}
+
+WideKernel wide_kernel(int depth) {
+    switch (depth) {
+    case 2: return k_sor32_wide<2>;
+    case 4: return k_sor32_wide<4>;
+    case 6: return k_sor32_wide<6>;
+    default: return k_sor32_wide<8>;
+    }
+}
+
+// Window starts along one axis of n pixels for windows of `win` with a halo
+// of `depth`: the first at 0, then every win - 2 depth until one reaches n.
+void axis_starts(int n, int win, int depth, std::vector<int> &out) {
+    out.clear();
+    out.push_back(0);
+    if (n <= win) return;
+    const int step = win - 2 * depth;
+    const int last = (n - win + step - 1) / step;
+    for (int k = 1; k <= last; ++k) out.push_back(k * step);
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+    });
+    return fn;
+}
+
+// The wide kernel's tensor maps, windows and grid, if every history allows it.
+int wide_init(Sor32 &s, cw_field_s *f) {
+    s.wide = false;
+    const Geom &g = f->g;
+    for (uint32_t k = 0; k < g.nh; ++k)
+        if (g.d[k] != 1 || g.w[k] % 4 != 0 || g.off[k] % 4 != 0) return CW_OK;
+    if (s.depth % 2 != 0 || s.depth > 8) return CW_OK;
+    PFN_cuTensorMapEncodeTiled_v12000 enc = encode_fn();
+    if (!enc) return CW_OK;
+    std::vector<CUtensorMap> maps(4 * (size_t)g.nh);
+    float *arrays[4] = {f->d32a, f->d32b, f->r32, f->inv32};
+    for (uint32_t k = 0; k < g.nh; ++k)
+        for (int m = 0; m < 4; ++m) {
+            cuuint64_t dim[2] = {(cuuint64_t)g.w[k], (cuuint64_t)g.h[k]};
+            cuuint64_t stride[1] = {(cuuint64_t)g.w[k] * sizeof(float)};
+            cuuint32_t box[2] = {WX, WY};
+            cuuint32_t estride[2] = {1, 1};
+            CUresult r = enc(&maps[4 * k + m], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, arrays[m] + g.off[k], dim, stride,
+                             box, estride, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+            if (r != CUDA_SUCCESS) return CW_OK;  // the narrow kernel serves
+        }
+    WideKernel kern = wide_kernel(s.depth);
+    CW_CUDA(cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)WIDE_SMEM));
+    int per_sm = 0, dev = 0, nsm = 0;
+    CW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)kern, 32 * WWARPS, WIDE_SMEM));
+    if (per_sm < 1) return CW_OK;
+    CW_CUDA(cudaGetDevice(&dev));
+    CW_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    std::vector<int4> tiles;
+    std::vector<int> xs, ys;
+    for (uint32_t k = 0; k < g.nh; ++k) {
+        axis_starts(g.w[k], WX, s.depth, xs);
+        axis_starts(g.h[k], WY, s.depth, ys);
+        for (int y : ys)
+            for (int x : xs) tiles.push_back(make_int4((int)k, x, y, 0));
+    }
+    int rc;
+    CUtensorMap *dm = nullptr;
+    if ((rc = dalloc(&dm, maps.size())) != CW_OK) return rc;
+    s.maps = dm;
+    if ((rc = dalloc(&s.wtiles, tiles.size())) != CW_OK) return rc;
+    CW_CUDA(cudaMemcpyAsync(s.maps, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice,
+                            stream()));
+    CW_CUDA(cudaMemcpyAsync(s.wtiles, tiles.data(), tiles.size() * sizeof(int4), cudaMemcpyHostToDevice, stream()));
+    CW_CUDA(cudaStreamSynchronize(stream()));
+    s.nwtiles = (int)tiles.size();
+    s.wgrid = std::min<int>(s.nwtiles, per_sm * nsm);
+    s.wide = true;
+    return CW_OK;
 }
 
 }  // namespace
@@ -188,10 +486,13 @@ int Sor32::init(cw_field_s *f, int d, const std::vector<double> &om) {
     CW_CUDA(cudaMemcpyAsync(omega, omf.data(), sizeof(float) * omf.size(), cudaMemcpyHostToDevice, stream()));
     std::vector<int64_t> per(f->g.nh);
     if (blocked) {
-        const int in = WIN - 2 * depth;
-        for (uint32_t k = 0; k < f->g.nh; ++k)
-            per[k] = (int64_t)((f->g.w[k] + in - 1) / in) * ((f->g.h[k] + in - 1) / in);
-        rc = tiles.build(per, 1);
+        if ((rc = wide_init(*this, f)) != CW_OK) return rc;
+        if (!wide) {
+            const int in = WIN - 2 * depth;
+            for (uint32_t k = 0; k < f->g.nh; ++k)
+                per[k] = (int64_t)((f->g.w[k] + in - 1) / in) * ((f->g.h[k] + in - 1) / in);
+            rc = tiles.build(per, 1);
+        }
     } else {
         for (uint32_t k = 0; k < f->g.nh; ++k) per[k] = (int64_t)((f->g.w[k] + 1) / 2) * f->g.h[k] * f->g.d[k];
         rc = sites.build(per, 256);
@@ -203,7 +504,6 @@ int Sor32::init(cw_field_s *f, int d, const std::vector<double> &om) {
 }
 
 int Sor32::sweeps(cw_field_s *f, int n, const int32_t *done, int done_stride, float *start) {
-    float dcoef = (float)f->dcoef;
     if (start) {  // begin from this (zeroed) buffer; the other is scratch
         ping = start;
         pong = start == f->d32a ? f->d32b : f->d32a;
@@ -213,22 +513,28 @@ int Sor32::sweeps(cw_field_s *f, int n, const int32_t *done, int done_stride, fl
             for (int colour = 0; colour < 2; ++colour) {
                 k_sor32_half<<<sites.nblocks, 256, 0, stream()>>>(ping, f->r32, f->inv32, f->g.d_dims, f->g.d_off,
                                                                   sites.d_blk, f->g.nh, omega, done, done_stride,
-                                                                  colour, dcoef);
+                                                                  colour);
                 CW_LAUNCHED();
             }
         out = ping;
         return CW_OK;
     }
     // 2n half-sweeps, `depth` per launch (fewer in the last), starting from
-    // the zeroed buffer; the tiles are those of `depth`, whose window halo is
-    // deep enough for a shorter last launch too
-    TbKernel kern = tb_kernel(depth);
+    // the zeroed buffer; the windows are those of `depth`, whose halo is deep
+    // enough for a shorter last launch too
     float *a = ping, *b = pong;
     int remaining = 2 * n, done_half = 0;
     while (remaining > 0) {
         int dd = remaining < depth ? remaining : depth;
-        kern<<<tiles.nblocks, 32 * WARPS, 0, stream()>>>(a, b, f->r32, f->inv32, f->g.d_dims, f->g.d_off, tiles.d_blk,
-                                                         f->g.nh, omega, done, done_stride, dd, done_half & 1, dcoef);
+        if (wide) {
+            wide_kernel(depth)<<<wgrid, 32 * WWARPS, WIDE_SMEM, stream()>>>(
+                (const CUtensorMap *)maps, a == f->d32a ? 0 : 1, b, wtiles, nwtiles, f->g.d_dims, f->g.d_off, omega,
+                done, done_stride, dd, done_half & 1);
+        } else {
+            tb_kernel(depth)<<<tiles.nblocks, 32 * WARPS, 0, stream()>>>(a, b, f->r32, f->inv32, f->g.d_dims,
+                                                                         f->g.d_off, tiles.d_blk, f->g.nh, omega,
+                                                                         done, done_stride, dd, done_half & 1);
+        }
         CW_LAUNCHED();
         remaining -= dd;
         done_half += dd;
@@ -242,6 +548,22 @@ void Sor32::release() {
     dfree(omega);
     tiles.release();
     sites.release();
+    CUtensorMap *m = (CUtensorMap *)maps;
+    dfree(m);
+    maps = nullptr;
+    dfree(wtiles);
+    wide = false;
+}
+
+// Whether a wide-kernel block gave up waiting for its window (and clears the record).
+int sor32_wait_failed() {
+    int v = 0, zero = 0;
+    CW_CUDA(cudaMemcpyFromSymbol(&v, g_wide_wait_failed, sizeof v));
+    if (v) {
+        CW_CUDA(cudaMemcpyToSymbol(g_wide_wait_failed, &zero, sizeof zero));
+        return fail(CW_ERR_TIMEOUT, "an FP32 SOR block waited more than 2 s for its window's TMA copies");
+    }
+    return CW_OK;
 }
 
 }  // namespace cw

@@ -47,14 +47,20 @@ __device__ __forceinline__ void pixel_sums64(const double *__restrict__ c, int64
 }
 
 // Red-black SOR sweeps on the correction equation A d = r in FP32.  Flat
-// histories are swept `depth` half-sweeps per launch, each tile kept in
-// shared memory with a halo `depth` deep (temporal blocking); volumes
-// one half-sweep per launch, in place.
+// histories are swept `depth` half-sweeps per launch, each tile held on chip
+// with a halo `depth` deep (temporal blocking): 128 x 64 windows fed by TMA
+// to persistent blocks where every history's rows are 16-byte aligned,
+// 64 x 64 windows read by plain loads otherwise; volumes one half-sweep per
+// launch, in place.
 struct Sor32 {
     int depth = 4;
     bool blocked = true;
-    Plan tiles;       // flat histories: tiles per history
-    Plan sites;       // volumes: pixels per history
+    bool wide = false;          // the TMA-fed kernel
+    Plan tiles;                 // 64 x 64 windows: tiles per history
+    Plan sites;                 // volumes: pixels per history
+    void *maps = nullptr;       // wide: 4 tensor maps per history (d32a, d32b, r32, inv32), device
+    int4 *wtiles = nullptr;     // wide: (history, x0, y0, 0) per window, device
+    int nwtiles = 0, wgrid = 0;
     float *omega = nullptr;
     float *ping = nullptr, *pong = nullptr, *out = nullptr;
     int init(cw_field_s *f, int depth, const std::vector<double> &omega_per_history);
@@ -62,5 +68,9 @@ struct Sor32 {
     float *result() const { return out; }
     void release();
 };
+
+// CW_ERR_TIMEOUT if a wide-kernel block gave up waiting for its window since
+// the last call (synchronous; clears the record).
+int sor32_wait_failed();
 
 }  // namespace cw

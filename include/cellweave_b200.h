@@ -193,6 +193,10 @@ int cw_field_inflow(cw_field f, double *out);
  * (`depth` half-sweeps per launch) on the current residual of every history,
  * without changing the field.  *ms is the kernels' time, *launches their count. */
 int cw_field_time_inner(cw_field f, int32_t sweeps, int32_t depth, double omega, float *ms, int64_t *launches);
+/* The FP32 correction the last cw_field_time_inner left, history `hist`
+ * (w*h*d floats).  A check of the sweep kernels: every depth gives the same
+ * correction as one half-sweep per launch.  No counterpart in the reference. */
+int cw_field_inner_correction(cw_field f, uint32_t hist, float *out);
 /* DiffusionField::step (pde.rs:705-728): one explicit step; CW_ERR_CONFIG for
  * a step the scheme cannot take (pde.rs:673-701). */
 int cw_field_step(cw_field f, double dt);

@@ -215,3 +215,41 @@ def test_a_batch_of_uneven_histories_solves_each_as_alone():
         rc, sweeps = o.relax(1e-11, 50_000)
         assert counts[k] == sweeps
         np.testing.assert_array_equal(bits(batch.values(k)), bits(o.values))
+
+
+def inner_corrections(dims, depth, sweeps=5, seed=3):
+    """cw_field_time_inner's FP32 correction for each history of a random batch."""
+    import ctypes as C
+    from cellweave_b200 import _lib
+    rng = np.random.default_rng(seed)
+    f = cw.ScalarField([(w, h, 1) for w, h in dims], D, 0.001, 0.0)
+    for k, (w, h) in enumerate(dims):
+        f.set_values(rng.random(w * h), k)
+        f.set_uptake_array(rng.random(w * h) * 0.01, k)
+        f.hold_where(1.0, (rng.random(w * h) < 0.05).astype(np.uint8), k)
+    ms, launches = C.c_float(), C.c_int64()
+    L = _lib.lib()
+    _lib.check(L.cw_field_time_inner(f.handle, sweeps, depth, 1.9, C.byref(ms), C.byref(launches)))
+    out = []
+    for k, (w, h) in enumerate(dims):
+        a = np.empty(w * h, np.float32)
+        _lib.check(L.cw_field_inner_correction(f.handle, k, a.ctypes.data))
+        out.append(a)
+    return out, launches.value
+
+
+@pytest.mark.parametrize("dims", [
+    [(128, 128), (200, 96), (260, 130), (1024, 70), (64, 300)],   # rows 16-byte aligned: 128 x 64 TMA windows
+    [(127, 90), (61, 61), (300, 33)],                               # any width: 64 x 64 windows
+])
+def test_blocked_fp32_sweeps_equal_one_half_sweep_per_launch(dims):
+    # temporal blocking is exact: every depth gives, to the bit, the in-place
+    # red-black sweeps of one half-sweep per launch (5 sweeps: 10 half-sweeps,
+    # so a depth-8 run ends on a launch of 2)
+    ref, n1 = inner_corrections(dims, 1)
+    assert n1 == 10
+    assert all(np.abs(r).max() > 0 for r in ref)
+    for depth in (2, 4, 6, 8):
+        got, _ = inner_corrections(dims, depth)
+        for k in range(len(dims)):
+            np.testing.assert_array_equal(got[k], ref[k], err_msg=f"depth {depth}, history {k} {dims[k]}")
