@@ -41,6 +41,9 @@ METRIC = "histories·MCS/s batched vs plain on 1 B200 at SOR resid≤1e-6; SOR H
 UNIT = "histories·MCS/s"
 # FP32 inner sweep, one pass through HBM: correction read 4 + write 4, right-hand side 4, inverse diagonal 4
 SOR_BYTES_PER_SITE_PASS = 16
+# DRAM bytes per site of one k_sor32_wide<8> launch on the campaign's oxygen
+# field, from ncu (dram__bytes_read.sum + dram__bytes_write.sum)
+SOR_TRAFFIC_PER_SITE = None
 
 
 def parse():
@@ -262,12 +265,19 @@ def run_ours(args, rank, world, dist):
     # ---- roofline of the dominant kernel: the FP32 SOR sweep on this batch's oxygen field
     f = sim.field_handle(0)
     tuned = sim.tuning()
-    depth, sweeps = tuned["depth"], 32
-    kms, kl = C.c_float(), C.c_int64()
-    _lib.check(L.cw_field_time_inner(f, sweeps, depth, 1.9, C.byref(kms), C.byref(kl)))  # warm
-    _lib.check(L.cw_field_time_inner(f, sweeps, depth, 1.9, C.byref(kms), C.byref(kl)))
+    depth, window, sweeps = tuned["depth"], tuned["window"], 32
     sites = int(sum(w * h * d for w, h, d in cfg["dims"]))
-    per_launch_ms = kms.value / kl.value
+
+    def launch_ms(d):
+        kms, kl = C.c_float(), C.c_int64()
+        _lib.check(L.cw_field_time_inner(f, sweeps, d, window, 1.9, C.byref(kms), C.byref(kl)))  # warm
+        _lib.check(L.cw_field_time_inner(f, sweeps, d, window, 1.9, C.byref(kms), C.byref(kl)))
+        return kms.value / kl.value
+
+    per_launch_ms = launch_ms(depth)
+    # depth 2: one sweep per launch, so a launch moves exactly one sweep's
+    # 16 B/site: the unblocked kernel's fraction of the HBM roofline
+    one_sweep_ms = launch_ms(2)
     # one launch is one round trip of correction, right-hand side and inverse
     # diagonal through HBM (16 B/site) for `depth` half-sweeps kept on chip
     alg_bytes_per_launch = sites * SOR_BYTES_PER_SITE_PASS
@@ -279,14 +289,26 @@ def run_ours(args, rank, world, dist):
     except Exception:
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
-    roofline = {"kernel": f"k_sor32_tb<{depth}> (FP32 red-black SOR, {depth} half-sweeps per launch on chip)",
+    kname = (f"k_sor32_wide<{depth}> (FP32 red-black SOR, 128x64 TMA-fed windows, {depth} half-sweeps per launch "
+             f"on chip)" if window == cw.WINDOW_AUTO else
+             f"k_sor32_tb<{depth}> (FP32 red-black SOR, 64x64 windows, {depth} half-sweeps per launch on chip)")
+    one_sweep_gbs = alg_bytes_per_launch / (one_sweep_ms / 1e3) / 1e9
+    roofline = {"kernel": kname,
                 "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 3),
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if "hbm_gbs" in peaks else "fallback 6650",
-                "traffic": None, "alg_bytes_per_launch": int(alg_bytes_per_launch),
+                "traffic": (int(SOR_TRAFFIC_PER_SITE * sites) if SOR_TRAFFIC_PER_SITE and window == cw.WINDOW_AUTO
+                            and depth == 8 else None),
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_sor32_wide<8> launch "
+                                  "on this workload, per site, times the sites",
+                "alg_bytes_per_launch": int(alg_bytes_per_launch),
                 "launch_ms": round(per_launch_ms, 4), "site_sweeps_per_s": sweep_rate,
-                "alg_bytes": "16 B per site per launch: the correction, right-hand side and inverse diagonal "
-                             "read once and the correction written once; the launch's half-sweeps stay on chip"}
+                "alg_bytes": "16 B per site per launch: the correction and both coefficients read once and the "
+                             "correction written once; the launch's half-sweeps stay on chip",
+                "per_sweep_equivalent_gbs": round(alg_bytes_per_launch * depth / 2 / (per_launch_ms / 1e3) / 1e9, 1),
+                "one_sweep_per_launch": {"launch_ms": round(one_sweep_ms, 4), "achieved": round(one_sweep_gbs, 1),
+                                         "frac": round(one_sweep_gbs / peak, 3),
+                                         "what": "depth 2: one sweep per launch, 16 B/site moved per sweep"}}
 
     # ---- the plain path: each history stepped alone (rank 0 at N=1)
     plain = plain_graphs = None

@@ -49,7 +49,8 @@ _ERRORS = {ERR_CONFIG: ConfigError, ERR_SIMULATION: SimulationError, ERR_ODE: Od
 
 class RelaxOpts(C.Structure):
     _fields_ = [("omega", C.c_double), ("stop", C.c_int32), ("tolerance", C.c_double), ("max_sweeps", C.c_int64),
-                ("precision", C.c_int32), ("inner_sweeps", C.c_int32), ("block_depth", C.c_int32)]
+                ("precision", C.c_int32), ("inner_sweeps", C.c_int32), ("block_depth", C.c_int32),
+                ("window", C.c_int32)]
 
 
 class RelaxStats(C.Structure):
@@ -132,7 +133,7 @@ SIGNATURES = {
     "cw_field_inflow": (C.c_int, [P, P]),
     "cw_field_step": (C.c_int, [P, D]),
     "cw_field_relax_noalloc": (C.c_int, [P, P, P, P, P, U32, U32, D, D, D, D, D, I64, I32, P, P]),
-    "cw_field_time_inner": (C.c_int, [P, I32, I32, D, P, P]),
+    "cw_field_time_inner": (C.c_int, [P, I32, I32, I32, D, P, P]),
     "cw_field_inner_correction": (C.c_int, [P, U32, P]),
     "cw_couple_uptake": (C.c_int, [P, P, I32, P, I32]),
     "cw_couple_background_uptake": (C.c_int, [P, P, D]),
@@ -150,7 +151,7 @@ SIGNATURES = {
     "cw_sim_destroy": (C.c_int, [P]),
     "cw_sim_step": (C.c_int, [P, U32]),
     "cw_sim_lattice": (C.c_int, [P, P]),
-    "cw_sim_tuning": (C.c_int, [P, P, P, P, P]),
+    "cw_sim_tuning": (C.c_int, [P, P, P, P, P, P]),
     "cw_sim_graph_info": (C.c_int, [P, P, P, P]),
     "cw_sim_field": (C.c_int, [P, I32, P]),
     "cw_sim_stats": (C.c_int, [P, P]),

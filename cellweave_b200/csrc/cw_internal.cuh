@@ -225,7 +225,7 @@ int field_span(cw_field_s *f, std::vector<Span> &spans);
 int field_relax(cw_field_s *f, const cw_relax_opts *opts, const double *omega_h, cw_relax_stats *stats);
 int field_relax_enqueue(cw_field_s *f, const cw_relax_opts *opts, int outer, float **start_out);
 int field_relax_finish(cw_field_s *f, const cw_relax_opts *opts, float *start);
-int field_dc_prepare(cw_field_s *f, int depth, const std::vector<double> &omega);
+int field_dc_prepare(cw_field_s *f, int depth, int window, const std::vector<double> &omega);
 int field_relax_collect(cw_field_s *f, std::vector<cw_relax_stats> &out, bool &all_settled);
 int lattice_recount(cw_lattice_s *lat, int32_t *vol_out, int32_t *surf_out);
 int lattice_sweep(cw_lattice_s *lat);

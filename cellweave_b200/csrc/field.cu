@@ -123,26 +123,33 @@ __global__ void k_sor64_half(FieldView fv, const int32_t *blk, int nh, const Spa
     if ((threadIdx.x & 31) == 0 && moved > 0.0) atomic_max_nonneg(&st[h].moved[colour], moved);
 }
 
+// Rows per block of the residual kernel (and of its launch plan, row_plan).
+constexpr int RES_ROWS = 4;
+
 // Projected residual max |b - A c| over the free pixels of each history;
 // optionally writes the FP32 coefficients of the defect-correction solve's
 // SOR on A d = r, the relaxation factor folded in: omega r / den and
 // omega D / den (both 0 on held pixels), and zeroes the correction.
-__global__ void k_residual64(FieldView fv, const int32_t *blk, int nh, RelaxState *st, float *r32, float *inv32,
-                             float *dz, int skip_done) {
+__global__ void __launch_bounds__(256) k_residual64(FieldView fv, const int32_t *blk, int nh, RelaxState *st,
+                                                    float *r32, float *inv32, float *dz, int skip_done) {
     __shared__ int s_h;
+    __shared__ double s_worst[8];
     if (threadIdx.x == 0) s_h = plan_history(blk, nh, blockIdx.x);
     __syncthreads();
     int h = s_h;
     if (skip_done && st[h].done) return;
     const int4 dm = fv.dims[h];
-    // one block: 256 consecutive pixels of one row
+    const double om = st[h].omega;
+    // one block: 256 consecutive pixels of each of RES_ROWS consecutive rows
     const uint32_t segs = ((uint32_t)dm.x + 255u) / 256u;
     const uint32_t lb = blockIdx.x - blk[h];
-    const uint32_t row = lb / segs;
-    const int x = (int)((lb - row * segs) * 256u + threadIdx.x);
-    const int y = (int)(row % (uint32_t)dm.y), z = (int)(row / (uint32_t)dm.y);
+    const uint32_t row0 = (lb / segs) * RES_ROWS;
+    const uint32_t nrows = (uint32_t)dm.y * (uint32_t)dm.z;
+    const int x = (int)((lb % segs) * 256u + threadIdx.x);
     double worst = 0.0;
-    if (x < dm.x) {
+    for (uint32_t row = row0; row < row0 + RES_ROWS && row < nrows; ++row) {
+        if (x >= dm.x) break;
+        const int y = (int)(row % (uint32_t)dm.y), z = (int)(row / (uint32_t)dm.y);
         int64_t i = fv.off[h] + (int64_t)row * dm.x + x;
         float r_out = 0.0f, inv_out = 0.0f;
         if (!fv.held[i]) {
@@ -153,9 +160,9 @@ __global__ void k_residual64(FieldView fv, const int32_t *blk, int nh, RelaxStat
             double cv = fv.c[i];
             double r = add_sources(fv, i, fv.d * sum) - den * cv;
             if (fv.floor && cv <= 0.0 && r < 0.0) r = 0.0;
-            worst = fabs(r);
+            worst = fmax(worst, fabs(r));
             if (den > 0.0) {
-                const double q = st[h].omega / den;
+                const double q = om / den;
                 r_out = (float)(q * r);
                 inv_out = (float)(q * fv.d);
             }
@@ -164,8 +171,15 @@ __global__ void k_residual64(FieldView fv, const int32_t *blk, int nh, RelaxStat
         if (inv32) inv32[i] = inv_out;
         if (dz) dz[i] = 0.0f;
     }
+    // one atomic per block: many per history would queue on its one word
     worst = warp_max(worst);
-    if ((threadIdx.x & 31) == 0 && worst > 0.0) atomic_max_nonneg(&st[h].resid, worst);
+    if ((threadIdx.x & 31) == 0) s_worst[threadIdx.x >> 5] = worst;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        worst = threadIdx.x < (blockDim.x >> 5) ? s_worst[threadIdx.x] : 0.0;
+        worst = warp_max(worst);
+        if (threadIdx.x == 0 && worst > 0.0) atomic_max_nonneg(&st[h].resid, worst);
+    }
 }
 
 // After sweep `index`: decide convergence (relax's `moved < tolerance`,
@@ -451,7 +465,8 @@ FieldView view(cw_field_s *f) {
 // One block per 256 consecutive pixels of a row (k_residual64's mapping).
 static int row_plan(cw_field_s *f, Plan &p) {
     std::vector<int64_t> per(f->g.nh);
-    for (uint32_t k = 0; k < f->g.nh; ++k) per[k] = (int64_t)f->g.h[k] * f->g.d[k] * ((f->g.w[k] + 255) / 256);
+    for (uint32_t k = 0; k < f->g.nh; ++k)
+        per[k] = ((int64_t)f->g.h[k] * f->g.d[k] + RES_ROWS - 1) / RES_ROWS * ((f->g.w[k] + 255) / 256);
     return p.build(per, 1);
 }
 
@@ -558,7 +573,7 @@ static int relax_fp64(cw_field_s *f, const cw_relax_opts &o, std::vector<Span> &
 struct DcCache {
     Plan pr, prow;
     Sor32 solver;
-    int depth = -1;
+    int depth = -1, window = 0;
     std::vector<double> omega;
     double *d_omega = nullptr;  // per history, for the state initialisation on the device
 };
@@ -573,12 +588,12 @@ __global__ void k_dc_state_init(RelaxState *st, int nh, const double *omega, dou
     st[h] = s;
 }
 
-static int dc_prepare(cw_field_s *f, int depth, const std::vector<double> &om, DcCache **out) {
+static int dc_prepare(cw_field_s *f, int depth, int window, const std::vector<double> &om, DcCache **out) {
     uint32_t nh = f->g.nh;
     int rc = f->alloc_fp32();
     if (rc != CW_OK) return rc;
     DcCache *c = (DcCache *)f->dc_cache;
-    if (c && c->depth != depth) {
+    if (c && (c->depth != depth || c->window != window)) {
         c->solver.release();
         c->depth = -1;
     }
@@ -592,8 +607,9 @@ static int dc_prepare(cw_field_s *f, int depth, const std::vector<double> &om, D
         if ((rc = dalloc(&c->d_omega, nh)) != CW_OK) return rc;
     }
     if (c->depth < 0) {
-        if ((rc = c->solver.init(f, depth, om)) != CW_OK) return rc;
+        if ((rc = c->solver.init(f, depth, om, window)) != CW_OK) return rc;
         c->depth = depth;
+        c->window = window;
         c->omega.clear();
     }
     if (c->omega != om) {
@@ -616,6 +632,16 @@ static int dc_outer(cw_field_s *f, DcCache *c, RelaxState *d_st, int inner, int6
     const int stride = (int)(sizeof(RelaxState) / sizeof(int32_t));
     k_dc_check<<<(nh + 63) / 64, 64, 0, stream()>>>(d_st, nh, inner, max_sweeps);
     CW_LAUNCHED();
+    if (c->solver.wide) {
+        // the last sweep launch adds the correction to c; then the residual
+        // at the corrected field, in one pass (the correction buffer needs no
+        // zeroing: the next solve's first launch does not read it)
+        int rc = c->solver.sweeps(f, inner, done_ptr, stride, start, true);
+        if (rc != CW_OK) return rc;
+        k_residual64<<<c->prow.nblocks, T, 0, stream()>>>(fv, c->prow.d_blk, nh, d_st, f->r32, nullptr, nullptr, 1);
+        CW_LAUNCHED();
+        return CW_OK;
+    }
     int rc = c->solver.sweeps(f, inner, done_ptr, stride, start);
     if (rc != CW_OK) return rc;
     float *d = c->solver.result();
@@ -634,7 +660,7 @@ static int relax_fp32dc(cw_field_s *f, const cw_relax_opts &o, RelaxState *d_st,
     std::vector<double> om(nh);
     for (uint32_t k = 0; k < nh; ++k) om[k] = hs[k].omega;
     DcCache *c = nullptr;
-    int rc = dc_prepare(f, depth, om, &c);
+    int rc = dc_prepare(f, depth, o.window, om, &c);
     if (rc != CW_OK) return rc;
     FieldView fv = view(f);
     int64_t outer = 0;
@@ -660,9 +686,9 @@ static int relax_fp32dc(cw_field_s *f, const cw_relax_opts &o, RelaxState *d_st,
 
 namespace cw {
 // Build (or update) a field's FP32 plans for `depth` and its factors per history.
-int field_dc_prepare(cw_field_s *f, int depth, const std::vector<double> &omega) {
+int field_dc_prepare(cw_field_s *f, int depth, int window, const std::vector<double> &omega) {
     DcCache *c = nullptr;
-    return dc_prepare(f, depth, omega, &c);
+    return dc_prepare(f, depth, window, omega, &c);
 }
 
 // The defect-correction solve enqueued with a fixed number of outer
@@ -1079,7 +1105,7 @@ extern "C" int cw_field_hold_bath(cw_field f, uint32_t hist, const uint8_t *open
 // Measurement hook: `sweeps` FP32 red-black sweeps of the correction
 // equation on the field's current residual, every history active, timed
 // with events around the sweep launches alone.  The field is not changed.
-extern "C" int cw_field_time_inner(cw_field f, int32_t sweeps, int32_t depth, double omega, float *ms,
+extern "C" int cw_field_time_inner(cw_field f, int32_t sweeps, int32_t depth, int32_t window, double omega, float *ms,
                                    int64_t *launches) {
     uint32_t nh = f->g.nh;
     int rc = f->alloc_fp32();
@@ -1094,7 +1120,7 @@ extern "C" int cw_field_time_inner(cw_field f, int32_t sweeps, int32_t depth, do
     CW_LAUNCHED();
     Sor32 solver;
     std::vector<double> om(nh, omega);
-    if ((rc = solver.init(f, depth, om)) != CW_OK) return rc;
+    if ((rc = solver.init(f, depth, om, window)) != CW_OK) return rc;
     const int32_t *done_ptr = (const int32_t *)((const char *)d_st + offsetof(RelaxState, done));
     cudaEvent_t a, b;
     CW_CUDA(cudaEventCreate(&a));

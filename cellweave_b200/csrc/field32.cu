@@ -209,17 +209,23 @@ __device__ __forceinline__ int next_live(int t, int ntiles, int step, const int4
 template <int C>
 __device__ __forceinline__ void half4(float4 (&d)[WROWS], const float4 (&a)[WROWS], const float4 (&b)[WROWS],
                                       const float4 ab, const float4 be, float lm, float rm, float omc) {
+    // the across-lane neighbours first: they are of the other colour, which
+    // this half-sweep does not change, and their latency then overlaps
+    float nb[WROWS];
+#pragma unroll
+    for (int j = 0; j < WROWS; ++j)
+        nb[j] = ((C + j) & 1) == 0 ? __shfl_up_sync(0xffffffffu, d[j].w, 1) : __shfl_down_sync(0xffffffffu, d[j].x, 1);
 #pragma unroll
     for (int j = 0; j < WROWS; ++j) {
         const float4 up = j > 0 ? d[j - 1] : ab, dn = j < WROWS - 1 ? d[j + 1] : be;
         if (((C + j) & 1) == 0) {
-            const float left = __shfl_up_sync(0xffffffffu, d[j].w, 1);
+            const float left = nb[j];
             const float s0 = fmaf(lm, left, d[j].y) + (up.x + dn.x);
             const float s2 = (d[j].y + d[j].w) + (up.z + dn.z);
             d[j].x = fmaf(a[j].x, s0, fmaf(omc, d[j].x, b[j].x));
             d[j].z = fmaf(a[j].z, s2, fmaf(omc, d[j].z, b[j].z));
         } else {
-            const float right = __shfl_down_sync(0xffffffffu, d[j].x, 1);
+            const float right = nb[j];
             const float s1 = (d[j].x + d[j].z) + (up.y + dn.y);
             const float s3 = fmaf(rm, right, d[j].z) + (up.w + dn.w);
             d[j].y = fmaf(a[j].y, s1, fmaf(omc, d[j].y, b[j].y));
@@ -228,55 +234,79 @@ __device__ __forceinline__ void half4(float4 (&d)[WROWS], const float4 (&a)[WROW
     }
 }
 
+// What a block needs of a window, staged in shared memory by thread 0 one
+// window ahead, so that no thread waits on a global load at a window's start.
+struct WideTile {
+    int4 tl;      // (history, x0, y0, 0); history < 0: no window left
+    int4 dm;      // the history's dimensions
+    int64_t off;  // its first pixel
+    float omc;    // 1 - omega
+};
+
 // maps: 4 per history (d32a, d32b, r32, inv32); src_map picks the buffer
 // read (0 or 1), dst is the other.  tiles: (history, x0, y0, 0) per window.
+// zero_start: the correction starts at zero (the first launch of a solve):
+// it is not read.  apply_c: the last launch of a solve adds its correction to
+// the FP64 field (floored at zero when `floor`) instead of writing it to dst.
 template <int DEPTH>
 __global__ void __launch_bounds__(32 * WWARPS, 2)
     k_sor32_wide(const CUtensorMap *__restrict__ maps, int src_map, float *__restrict__ dst,
                  const int4 *__restrict__ tiles, int ntiles, const int4 *__restrict__ dims,
                  const int64_t *__restrict__ off, const float *__restrict__ omega, const int32_t *done,
-                 int done_stride, int nhalf, int start_colour) {
+                 int done_stride, int nhalf, int start_colour, int zero_start, double *__restrict__ apply_c,
+                 int floor) {
     extern __shared__ __align__(128) float smem[];
     const float4 *sd = (const float4 *)smem, *sb = (const float4 *)(smem + STAGE),
                  *sa = (const float4 *)(smem + 2 * STAGE);
     float4 *edge = (float4 *)(smem + 3 * STAGE);  // [buffer][warp][0 top, 1 bottom][lane]
     __shared__ __align__(8) uint64_t bar_word;
-    __shared__ int s_next, s_fail;
+    __shared__ WideTile s_info[2];
+    __shared__ int s_fail;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t bar = sh_addr(&bar_word);
-    auto issue = [&](int t) {
-        const int4 tl = tiles[t];
-        const CUtensorMap *m = maps + 4 * tl.x;
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
-                     "r"((uint32_t)(3 * STAGE * sizeof(float)))
-                     : "memory");
-        tma_box(smem, m + src_map, bar, tl.y, tl.z);
-        tma_box(smem + STAGE, m + 2, bar, tl.y, tl.z);
-        tma_box(smem + 2 * STAGE, m + 3, bar, tl.y, tl.z);
+    const uint32_t boxes = zero_start ? 2u : 3u;
+    // thread 0: find the next live window at or after t, stage its scalars
+    // in s_info[slot] and start its copies
+    auto stage_next = [&](int t, int slot) {
+        t = next_live(t, ntiles, gridDim.x, tiles, done, done_stride);
+        WideTile w;
+        w.tl = make_int4(-1, 0, 0, 0);
+        if (t < ntiles) {
+            w.tl = tiles[t];
+            w.tl.w = t;
+            w.dm = dims[w.tl.x];
+            w.off = off[w.tl.x];
+            w.omc = 1.f - omega[w.tl.x];
+            const CUtensorMap *m = maps + 4 * w.tl.x;
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+                         "r"((uint32_t)(boxes * STAGE * sizeof(float)))
+                         : "memory");
+            if (!zero_start) tma_box(smem, m + src_map, bar, w.tl.y, w.tl.z);
+            tma_box(smem + STAGE, m + 2, bar, w.tl.y, w.tl.z);
+            tma_box(smem + 2 * STAGE, m + 3, bar, w.tl.y, w.tl.z);
+        }
+        s_info[slot] = w;
     };
     if (threadIdx.x == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         s_fail = 0;
-        const int t = next_live(blockIdx.x, ntiles, gridDim.x, tiles, done, done_stride);
-        s_next = t;
-        if (t < ntiles) issue(t);
+        stage_next(blockIdx.x, 0);
     }
     __syncthreads();
-    int t = s_next;
     uint32_t parity = 0;
     const float lm = lane == 0 ? 0.f : 1.f, rm = lane == 31 ? 0.f : 1.f;
     const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
     auto ed = [&](int buf, int w, int side) -> float4 & { return edge[((buf * WWARPS + w) * 2 + side) * 32 + lane]; };
-    while (t < ntiles) {
-        const int4 tl = tiles[t];
-        const int h = tl.x, x0 = tl.y, y0 = tl.z;
+    for (int slot = 0;; slot ^= 1) {
+        const WideTile info = s_info[slot];
+        if (info.tl.x < 0) break;
         if (!mbar_wait_bounded(bar, parity)) s_fail = 1;
         float4 d[WROWS], a[WROWS], b[WROWS];
 #pragma unroll
         for (int j = 0; j < WROWS; ++j) {
             const int k = (warp * WROWS + j) * 32 + lane;
-            d[j] = sd[k];
+            d[j] = zero_start ? z4 : sd[k];
             b[j] = sb[k];
             a[j] = sa[k];
         }
@@ -291,19 +321,14 @@ __global__ void __launch_bounds__(32 * WWARPS, 2)
         }
         parity ^= 1u;
         if (threadIdx.x == 0) {
-            const int n = next_live(t + gridDim.x, ntiles, gridDim.x, tiles, done, done_stride);
-            s_next = n;
-            if (n < ntiles) {
-                // the generic-proxy reads of the stage before the async-proxy writes
-                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                issue(n);
-            }
+            // the generic-proxy reads of the stage before the async-proxy writes
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            stage_next(info.tl.w + gridDim.x, slot ^ 1);
         }
-        const float omc = 1.f - omega[h];
+        const float omc = info.omc;
         ed(0, warp, 0) = d[0];
         ed(0, warp, 1) = d[WROWS - 1];
         __syncthreads();
-        const int tn = s_next;
         for (int s = 0; s < nhalf; ++s) {
             const int buf = s & 1;
             const float4 ab = warp > 0 ? ed(buf, warp - 1, 1) : z4;
@@ -319,27 +344,62 @@ __global__ void __launch_bounds__(32 * WWARPS, 2)
                 __syncthreads();
             }
         }
-        // the interior back to global memory
-        const int4 dm = dims[h];
+        // the interior back to global memory: the warp's rows inside it (a
+        // range uniform over the warp), the lane's columns inside it (all four,
+        // none, or a few at a history border that cuts a float4)
+        const int x0 = info.tl.y, y0 = info.tl.z;
+        const int4 dm = info.dm;
         const int ix0 = x0 == 0 ? 0 : x0 + DEPTH, ix1 = x0 + WX >= dm.x ? dm.x : x0 + WX - DEPTH;
         const int iy0 = y0 == 0 ? 0 : y0 + DEPTH, iy1 = y0 + WY >= dm.y ? dm.y : y0 + WY - DEPTH;
+        const int wy = y0 + warp * WROWS;
+        const int j0 = max(iy0 - wy, 0), j1 = min(iy1 - wy, WROWS);
         const int gx = x0 + 4 * lane;
-        float *base = dst + off[h];
+        const bool full = gx >= ix0 && gx + 4 <= ix1;
+        const bool part = !full && gx + 4 > ix0 && gx < ix1;
+        const int64_t first = info.off + (int64_t)wy * dm.x + gx;
+        if (apply_c) {
+            // c += d on the free pixels (held ones have a = 0 and d = 0 throughout)
+            double *row = apply_c + first;
 #pragma unroll
-        for (int j = 0; j < WROWS; ++j) {
-            const int gy = y0 + warp * WROWS + j;
-            if (gy < iy0 || gy >= iy1) continue;
-            float *row = base + (int64_t)gy * dm.x + gx;
-            if (gx >= ix0 && gx + 4 <= ix1) {
-                *(float4 *)row = d[j];
-            } else {
-                if (gx >= ix0 && gx < ix1) row[0] = d[j].x;
-                if (gx + 1 >= ix0 && gx + 1 < ix1) row[1] = d[j].y;
-                if (gx + 2 >= ix0 && gx + 2 < ix1) row[2] = d[j].z;
-                if (gx + 3 >= ix0 && gx + 3 < ix1) row[3] = d[j].w;
+            for (int j = 0; j < WROWS; ++j, row += dm.x) {
+                if (j < j0 || j >= j1 || !(full || part)) continue;
+                const float dv[4] = {d[j].x, d[j].y, d[j].z, d[j].w};
+                const float av[4] = {a[j].x, a[j].y, a[j].z, a[j].w};
+                if (full) {
+                    double2 c01 = *(double2 *)row, c23 = *(double2 *)(row + 2);
+                    double cv[4] = {c01.x, c01.y, c23.x, c23.y};
+#pragma unroll
+                    for (int e = 0; e < 4; ++e)
+                        if (dv[e] != 0.f || av[e] != 0.f) {
+                            cv[e] = cv[e] + (double)dv[e];
+                            if (floor) cv[e] = fmax(cv[e], 0.0);
+                        }
+                    *(double2 *)row = make_double2(cv[0], cv[1]);
+                    *(double2 *)(row + 2) = make_double2(cv[2], cv[3]);
+                } else {
+#pragma unroll
+                    for (int e = 0; e < 4; ++e)
+                        if (gx + e >= ix0 && gx + e < ix1 && (dv[e] != 0.f || av[e] != 0.f)) {
+                            double v = row[e] + (double)dv[e];
+                            row[e] = floor ? fmax(v, 0.0) : v;
+                        }
+                }
+            }
+        } else {
+            float *row = dst + first;
+#pragma unroll
+            for (int j = 0; j < WROWS; ++j, row += dm.x) {
+                if (j < j0 || j >= j1) continue;
+                if (full) {
+                    *(float4 *)row = d[j];
+                } else if (part) {
+                    if (gx >= ix0 && gx < ix1) row[0] = d[j].x;
+                    if (gx + 1 >= ix0 && gx + 1 < ix1) row[1] = d[j].y;
+                    if (gx + 2 >= ix0 && gx + 2 < ix1) row[2] = d[j].z;
+                    if (gx + 3 >= ix0 && gx + 3 < ix1) row[3] = d[j].w;
+                }
             }
         }
-        t = tn;
     }
 }
 
@@ -377,7 +437,7 @@ __global__ void k_sor32_half(float *__restrict__ dlt, const float *__restrict__ 
 typedef void (*TbKernel)(const float *, float *, const float *, const float *, const int4 *, const int64_t *,
                          const int32_t *, int, const float *, const int32_t *, int, int, int);
 typedef void (*WideKernel)(const CUtensorMap *, int, float *, const int4 *, int, const int4 *, const int64_t *,
-                           const float *, const int32_t *, int, int, int);
+                           const float *, const int32_t *, int, int, int, int, double *, int);
 
 TbKernel tb_kernel(int depth) {
     switch (depth) {
@@ -475,7 +535,7 @@ int wide_init(Sor32 &s, cw_field_s *f) {
 
 }  // namespace
 
-int Sor32::init(cw_field_s *f, int d, const std::vector<double> &om) {
+int Sor32::init(cw_field_s *f, int d, const std::vector<double> &om, int window) {
     depth = d < 1 ? 1 : d;
     if (depth > 1) depth = depth >= 8 ? 8 : (depth >= 6 ? 6 : (depth >= 4 ? 4 : 2));
     blocked = depth > 1;
@@ -486,7 +546,8 @@ int Sor32::init(cw_field_s *f, int d, const std::vector<double> &om) {
     CW_CUDA(cudaMemcpyAsync(omega, omf.data(), sizeof(float) * omf.size(), cudaMemcpyHostToDevice, stream()));
     std::vector<int64_t> per(f->g.nh);
     if (blocked) {
-        if ((rc = wide_init(*this, f)) != CW_OK) return rc;
+        wide = false;
+        if (window == CW_WINDOW_AUTO && (rc = wide_init(*this, f)) != CW_OK) return rc;
         if (!wide) {
             const int in = WIN - 2 * depth;
             for (uint32_t k = 0; k < f->g.nh; ++k)
@@ -503,7 +564,8 @@ int Sor32::init(cw_field_s *f, int d, const std::vector<double> &om) {
     return rc;
 }
 
-int Sor32::sweeps(cw_field_s *f, int n, const int32_t *done, int done_stride, float *start) {
+int Sor32::sweeps(cw_field_s *f, int n, const int32_t *done, int done_stride, float *start, bool apply) {
+    if (apply && !wide) return fail(CW_ERR_CONFIG, "only the wide FP32 kernel applies its correction");
     if (start) {  // begin from this (zeroed) buffer; the other is scratch
         ping = start;
         pong = start == f->d32a ? f->d32b : f->d32a;
@@ -527,9 +589,13 @@ int Sor32::sweeps(cw_field_s *f, int n, const int32_t *done, int done_stride, fl
     while (remaining > 0) {
         int dd = remaining < depth ? remaining : depth;
         if (wide) {
+            // the first launch starts from zero without reading it; with
+            // `apply` the last adds its correction to the field
+            const bool last = remaining == dd;
             wide_kernel(depth)<<<wgrid, 32 * WWARPS, WIDE_SMEM, stream()>>>(
                 (const CUtensorMap *)maps, a == f->d32a ? 0 : 1, b, wtiles, nwtiles, f->g.d_dims, f->g.d_off, omega,
-                done, done_stride, dd, done_half & 1);
+                done, done_stride, dd, done_half & 1, done_half == 0 ? 1 : 0, apply && last ? f->c : nullptr,
+                f->floor ? 1 : 0);
         } else {
             tb_kernel(depth)<<<tiles.nblocks, 32 * WARPS, 0, stream()>>>(a, b, f->r32, f->inv32, f->g.d_dims,
                                                                          f->g.d_off, tiles.d_blk, f->g.nh, omega,
@@ -540,7 +606,7 @@ int Sor32::sweeps(cw_field_s *f, int n, const int32_t *done, int done_stride, fl
         done_half += dd;
         float *t = a; a = b; b = t;
     }
-    out = a;
+    out = apply ? nullptr : a;
     return CW_OK;
 }
 

@@ -63,8 +63,12 @@ struct Sor32 {
     int nwtiles = 0, wgrid = 0;
     float *omega = nullptr;
     float *ping = nullptr, *pong = nullptr, *out = nullptr;
-    int init(cw_field_s *f, int depth, const std::vector<double> &omega_per_history);
-    int sweeps(cw_field_s *f, int n, const int32_t *done, int done_stride, float *start = nullptr);
+    int init(cw_field_s *f, int depth, const std::vector<double> &omega_per_history, int window = CW_WINDOW_AUTO);
+    // n sweeps from the zeroed correction buffer `start` (or the last result);
+    // `apply` (wide only): the last launch adds the correction to the field's
+    // values instead of writing it, and result() is null
+    int sweeps(cw_field_s *f, int n, const int32_t *done, int done_stride, float *start = nullptr,
+               bool apply = false);
     float *result() const { return out; }
     void release();
 };

@@ -50,6 +50,7 @@ struct cw_sim_s {
     std::vector<double> omega[2];               // per history, per field
     int32_t depth = 8;
     bool depth_tuned = false;
+    int sor_window = CW_WINDOW_AUTO;  // FP32 sweep windows, tuned with the depth
     // a step as three captured CUDA graphs (oxygen solve; means and signal
     // solve; network, fates and lattice), each solve with a fixed budget of
     // outer iterations checked, and finished host-side if ever short
@@ -400,15 +401,17 @@ static void tune_finish(cw_sim_s *s) {
 static int tune_depth(cw_sim_s *s) {
     if (s->cfg.precision != CW_FP32_DC) return CW_OK;
     float best = 0.f;
-    int bd = 8;
-    for (int d : {4, 6, 8}) {
-        float ms = 0.f;
-        int64_t launches = 0;
-        int rc = cw_field_time_inner(s->o2, 8, d, 1.9, &ms, &launches);
-        if (rc != CW_OK) return rc;
-        if (best == 0.f || ms < best) { best = ms; bd = d; }
-    }
+    int bd = 8, bw = CW_WINDOW_AUTO;
+    for (int w : {CW_WINDOW_AUTO, CW_WINDOW_64})
+        for (int d : {4, 6, 8}) {
+            float ms = 0.f;
+            int64_t launches = 0;
+            int rc = cw_field_time_inner(s->o2, 8, d, w, 1.9, &ms, &launches);
+            if (rc != CW_OK) return rc;
+            if (best == 0.f || ms < best) { best = ms; bd = d; bw = w; }
+        }
     s->depth = bd;
+    s->sor_window = bw;
     s->depth_tuned = true;
     return CW_OK;
 }
@@ -474,7 +477,7 @@ static int build_graphs(cw_sim_s *s, const cw_relax_opts &o) {
         if (!f) continue;
         std::vector<double> om(s->cfg.nh, s->cfg.omega);
         if (s->cfg.omega <= 0.0) om = s->omega[fi];
-        if ((rc0 = field_dc_prepare(f, s->depth, om)) != CW_OK) return rc0;
+        if ((rc0 = field_dc_prepare(f, s->depth, s->sor_window, om)) != CW_OK) return rc0;
     }
     const uint32_t mcs = s->lat->mcs;
     for (int p = 0; p < 3; ++p) {
@@ -561,6 +564,7 @@ int cw_sim_step(cw_sim s, uint32_t nsteps) {
     for (uint32_t step = 0; step < nsteps; ++step, ++s->steps) {
         bool solve = c.relax_every <= 1 || (s->steps % (uint32_t)c.relax_every) == 0;
         o.block_depth = s->depth;
+        o.window = s->sor_window;
         const bool graph_ok = c.use_graphs && c.precision == CW_FP32_DC && c.relax_every <= 1 && !s->tune.active &&
                               s->depth_tuned && s->steps >= 2 && !s->last.empty() &&
                               (!s->sig || !s->last_sig.empty());
@@ -626,12 +630,14 @@ int cw_sim_graph_info(cw_sim s, uint64_t *graph_steps, uint64_t *budget_misses, 
     return CW_OK;
 }
 
-int cw_sim_tuning(cw_sim s, double *omega_o2, double *omega_signal, int32_t *depth, int32_t *tuning) {
+int cw_sim_tuning(cw_sim s, double *omega_o2, double *omega_signal, int32_t *depth, int32_t *window,
+                  int32_t *tuning) {
     for (uint32_t k = 0; k < s->cfg.nh; ++k) {
         if (omega_o2) omega_o2[k] = s->omega[0][k];
         if (omega_signal) omega_signal[k] = s->omega[1][k];
     }
     if (depth) *depth = s->depth;
+    if (window) *window = s->sor_window;
     if (tuning) *tuning = s->tune.active ? 1 : 0;
     return CW_OK;
 }

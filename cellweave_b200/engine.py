@@ -22,6 +22,7 @@ from ._lib import ConfigError, call, lib, ptr
 
 OBSTACLE = -1
 FP64, FP32_DC = 0, 1
+WINDOW_AUTO, WINDOW_64 = 0, 1
 STOP_MAX_CHANGE, STOP_RESIDUAL = 0, 1
 VALUES, UPTAKE, PRODUCTION, LIN_SINK = 0, 1, 2, 3
 
@@ -147,10 +148,10 @@ class ScalarField:
         call("cw_field_hold_bath", self._h, hist, ptr(o), float(value))
 
     def relax(self, tolerance, max_sweeps, omega=None, stop=STOP_MAX_CHANGE, precision=FP64, inner_sweeps=0,
-              block_depth=0, stats=False):
+              block_depth=0, window=WINDOW_AUTO, stats=False):
         """relax (pde.rs:245-288): the sweep count of every history (SimulationError if one did not settle)."""
         o = _lib.RelaxOpts(float(omega) if omega else 0.0, int(stop), float(tolerance), int(max_sweeps),
-                           int(precision), int(inner_sweeps), int(block_depth))
+                           int(precision), int(inner_sweeps), int(block_depth), int(window))
         st = (_lib.RelaxStats * len(self.dims))()
         rc = lib().cw_field_relax(self._h, C.byref(o), st)
         result = [dict(sweeps=s.sweeps, last_change=s.last_change, residual=s.residual, status=s.status,
@@ -536,12 +537,12 @@ class Simulation:
         call("cw_sim_step", self._h, int(n))
 
     def tuning(self):
-        """What the autotuner chose: factors per history (oxygen, signal), blocking depth, still tuning."""
+        """What the autotuner chose: factors per history (oxygen, signal), blocking depth and window, still tuning."""
         n = len(self.dims)
         a, b = np.zeros(n), np.zeros(n)
-        depth, active = C.c_int32(), C.c_int32()
-        call("cw_sim_tuning", self._h, ptr(a), ptr(b), C.byref(depth), C.byref(active))
-        return dict(omega_o2=a, omega_signal=b, depth=depth.value, tuning=bool(active.value))
+        depth, window, active = C.c_int32(), C.c_int32(), C.c_int32()
+        call("cw_sim_tuning", self._h, ptr(a), ptr(b), C.byref(depth), C.byref(window), C.byref(active))
+        return dict(omega_o2=a, omega_signal=b, depth=depth.value, window=window.value, tuning=bool(active.value))
 
     def graph_info(self):
         """(steps replayed from CUDA graphs, budget misses, outer-iteration budgets)."""

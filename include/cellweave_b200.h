@@ -148,6 +148,10 @@ int cw_field_hold_bath(cw_field f, uint32_t hist, const uint8_t *open, double va
 
 enum { CW_STOP_MAX_CHANGE = 0, CW_STOP_RESIDUAL = 1 };
 enum { CW_FP64 = 0, CW_FP32_DC = 1 };
+/* CW_FP32_DC sweep windows: the widest the batch allows (128 x 64, fed by
+ * TMA, where every history's rows are 16-byte aligned; else 64 x 64), or
+ * 64 x 64 always. */
+enum { CW_WINDOW_AUTO = 0, CW_WINDOW_64 = 1 };
 typedef struct {
     double omega;        /* <= 0: the reference's rule (pde.rs:267-277) */
     int32_t stop;        /* CW_STOP_MAX_CHANGE (the reference) or CW_STOP_RESIDUAL */
@@ -156,6 +160,7 @@ typedef struct {
     int32_t precision;   /* CW_FP64 (bit-exact with the reference) or CW_FP32_DC */
     int32_t inner_sweeps;/* CW_FP32_DC: FP32 sweeps per FP64 defect correction (0: 16) */
     int32_t block_depth; /* CW_FP32_DC: half-sweeps per launch kept in shared memory (0: 4) */
+    int32_t window;      /* CW_FP32_DC: CW_WINDOW_AUTO or CW_WINDOW_64 */
 } cw_relax_opts;
 typedef struct {
     int64_t sweeps;      /* the count relax returns (pde.rs:279-283) */
@@ -190,9 +195,11 @@ int cw_field_residual(cw_field f, double *out);
 /* inflow (pde.rs:415-456) of every history (nh entries). */
 int cw_field_inflow(cw_field f, double *out);
 /* Measurement: time `sweeps` FP32 sweeps of the defect-correction kernel
- * (`depth` half-sweeps per launch) on the current residual of every history,
- * without changing the field.  *ms is the kernels' time, *launches their count. */
-int cw_field_time_inner(cw_field f, int32_t sweeps, int32_t depth, double omega, float *ms, int64_t *launches);
+ * (`depth` half-sweeps per launch, `window` a CW_WINDOW_*) on the current
+ * residual of every history, without changing the field.  *ms is the kernels'
+ * time, *launches their count. */
+int cw_field_time_inner(cw_field f, int32_t sweeps, int32_t depth, int32_t window, double omega, float *ms,
+                        int64_t *launches);
 /* The FP32 correction the last cw_field_time_inner left, history `hist`
  * (w*h*d floats).  A check of the sweep kernels: every depth gives the same
  * correction as one half-sweep per launch.  No counterpart in the reference. */
@@ -300,9 +307,11 @@ int cw_sim_destroy(cw_sim sim);
 int cw_sim_step(cw_sim sim, uint32_t steps);
 /* What the autotuner chose: the SOR relaxation factor of every history for
  * the oxygen and the signal field (0 until chosen: the reference's rule),
- * the FP32 blocking depth, and whether it is still trying candidates.  It
- * runs when cfg.omega <= 0 with CW_FP32_DC, over the first few steps. */
-int cw_sim_tuning(cw_sim sim, double *omega_o2, double *omega_signal, int32_t *depth, int32_t *tuning);
+ * the FP32 blocking depth and window (CW_WINDOW_*), and whether it is still
+ * trying candidates.  It runs when cfg.omega <= 0 with CW_FP32_DC, over the
+ * first few steps. */
+int cw_sim_tuning(cw_sim sim, double *omega_o2, double *omega_signal, int32_t *depth, int32_t *window,
+                  int32_t *tuning);
 /* Steps replayed from CUDA graphs, solves whose graph budget of outer
  * iterations fell short (finished host-side), and the budgets (2 entries). */
 int cw_sim_graph_info(cw_sim sim, uint64_t *graph_steps, uint64_t *budget_misses, int32_t *budgets);

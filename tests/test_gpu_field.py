@@ -217,7 +217,7 @@ def test_a_batch_of_uneven_histories_solves_each_as_alone():
         np.testing.assert_array_equal(bits(batch.values(k)), bits(o.values))
 
 
-def inner_corrections(dims, depth, sweeps=5, seed=3):
+def inner_corrections(dims, depth, window=cw.WINDOW_AUTO, sweeps=5, seed=3):
     """cw_field_time_inner's FP32 correction for each history of a random batch."""
     import ctypes as C
     from cellweave_b200 import _lib
@@ -229,7 +229,7 @@ def inner_corrections(dims, depth, sweeps=5, seed=3):
         f.hold_where(1.0, (rng.random(w * h) < 0.05).astype(np.uint8), k)
     ms, launches = C.c_float(), C.c_int64()
     L = _lib.lib()
-    _lib.check(L.cw_field_time_inner(f.handle, sweeps, depth, 1.9, C.byref(ms), C.byref(launches)))
+    _lib.check(L.cw_field_time_inner(f.handle, sweeps, depth, window, 1.9, C.byref(ms), C.byref(launches)))
     out = []
     for k, (w, h) in enumerate(dims):
         a = np.empty(w * h, np.float32)
@@ -249,7 +249,30 @@ def test_blocked_fp32_sweeps_equal_one_half_sweep_per_launch(dims):
     ref, n1 = inner_corrections(dims, 1)
     assert n1 == 10
     assert all(np.abs(r).max() > 0 for r in ref)
-    for depth in (2, 4, 6, 8):
-        got, _ = inner_corrections(dims, depth)
-        for k in range(len(dims)):
-            np.testing.assert_array_equal(got[k], ref[k], err_msg=f"depth {depth}, history {k} {dims[k]}")
+    for window in (cw.WINDOW_AUTO, cw.WINDOW_64):
+        for depth in (2, 4, 6, 8):
+            got, _ = inner_corrections(dims, depth, window)
+            for k in range(len(dims)):
+                np.testing.assert_array_equal(got[k], ref[k], err_msg=f"window {window}, depth {depth}, {dims[k]}")
+
+
+@pytest.mark.parametrize("sizes,depth", [([256], 8), ([128, 200, 512], 4), ([64, 1024], 6)])
+def test_wide_windows_with_the_fused_correction_equal_the_64_windows(sizes, depth):
+    # the 128 x 64 TMA windows add the correction in their last launch and take
+    # the residual in one pass; the 64 x 64 windows write the correction and
+    # update in two colour passes: the same arithmetic, so the same bits
+    fields = []
+    for window in (cw.WINDOW_AUTO, cw.WINDOW_64):
+        g = cw.ScalarField([(n, n, 1) for n in sizes], 1.0, 0.0, 0.0)
+        for k, n in enumerate(sizes):
+            held, sink, _ = sheet_problem(n, seed=k)
+            g.set_linear_sink(sink, k)
+            g.hold_where(1.0, held, k)
+        st = g.relax(1e-6, 1_000_000, omega=1.9, stop=cw.STOP_RESIDUAL, precision=cw.FP32_DC, block_depth=depth,
+                     window=window, stats=True)
+        fields.append((g, st))
+    (ga, sa), (gb, sb) = fields
+    for k in range(len(sizes)):
+        assert sa[k]["sweeps"] == sb[k]["sweeps"]
+        assert sa[k]["residual"] == sb[k]["residual"] < 1e-6
+        np.testing.assert_array_equal(bits(ga.values(k)), bits(gb.values(k)))
