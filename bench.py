@@ -42,8 +42,10 @@ UNIT = "histories·MCS/s"
 # FP32 inner sweep, one pass through HBM: correction read 4 + write 4, right-hand side 4, inverse diagonal 4
 SOR_BYTES_PER_SITE_PASS = 16
 # DRAM bytes per site of one k_sor32_wide<8> launch on the campaign's oxygen
-# field, from ncu (dram__bytes_read.sum + dram__bytes_write.sum)
-SOR_TRAFFIC_PER_SITE = None
+# field, from ncu (dram__bytes_read.sum + dram__bytes_write.sum: 267.5 MB +
+# 65.5 MB over 22,282,240 sites), a launch that reads and writes the
+# correction (neither the first nor the last of a solve)
+SOR_TRAFFIC_PER_SITE = 14.95
 
 
 def parse():
@@ -63,10 +65,27 @@ def parse():
 
 
 def workload(name, rank=0):
+    """The workload's configuration for one rank: every rank its own
+    campaign, the same shapes, seeds offset by the rank (disjoint histories)."""
     from cellweave_b200 import synthetic
     cfg = synthetic.campaign() if name == "campaign" else synthetic.tumour_cord()
     cfg["seeds"] = [s + 100_000 * rank for s in cfg["seeds"]]
     return cfg
+
+
+def max_over_ranks(x, dist, device):
+    """The largest x over the ranks (every rank calls it, in the same order)."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(world, histories, steps, ms):
+    """Whole-job histories*MCS/s: every rank's histories over the slowest rank's time."""
+    return world * histories * steps / (ms / 1e3)
 
 
 def config_key(name, cfg):
@@ -213,12 +232,8 @@ def run_ours(args, rank, world, dist):
     launches = int(L.cw_launch_count() - l0)
     clk = clocks.stop()
     barrier()
-    if dist is not None:
-        import torch
-        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * nh * args.steps / (ms / 1e3)
+    ms = max_over_ranks(ms, dist, f"cuda:{local}")
+    value = job_rate(world, nh, args.steps, ms)
     stats = sim.stats()
     gsteps, gmiss, gbudget = sim.graph_info()
     graphs = {"steps_replayed": int(gsteps), "budget_misses": int(gmiss), "outer_budgets": [int(b) for b in gbudget]}
@@ -253,12 +268,8 @@ def run_ours(args, rank, world, dist):
     L.cw_event_record(3)
     e2e_ms = event_ms(L, 2, 3) / e2e_steps
     bytes_grid = int(sum(g.nbytes for g in grids))
-    if dist is not None:
-        import torch
-        t = torch.tensor([e2e_ms], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e = {"value": world * nh / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": bytes_grid,
+    e2e_ms = max_over_ranks(e2e_ms, dist, f"cuda:{local}")
+    e2e = {"value": job_rate(world, nh, 1, e2e_ms), "unit": UNIT, "h2d_bytes_per_step": bytes_grid,
            "d2h_bytes_per_step": bytes_grid + st_host.nbytes, "steps": e2e_steps,
            "path": "cw_lattice_upload (pinned host grids) + cw_sim_step + cw_lattice_download + cw_sim_stats"}
 

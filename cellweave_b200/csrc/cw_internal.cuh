@@ -154,6 +154,20 @@ __device__ __forceinline__ double warp_max(double v) {
     for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
     return v;
 }
+// The block's maximum of a non-negative v into *addr with one atomic (every
+// thread of the block calls it; at most 1024 threads).  Many atomics per
+// history on its one word would queue in L2.
+__device__ __forceinline__ void block_max_to(unsigned long long *addr, double v) {
+    __shared__ double s_part[32];
+    v = warp_max(v);
+    if ((threadIdx.x & 31) == 0) s_part[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        v = threadIdx.x < ((blockDim.x + 31) >> 5) ? s_part[threadIdx.x] : 0.0;
+        v = warp_max(v);
+        if (threadIdx.x == 0 && v > 0.0) atomic_max_nonneg(addr, v);
+    }
+}
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);

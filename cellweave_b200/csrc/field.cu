@@ -119,8 +119,7 @@ __global__ void k_sor64_half(FieldView fv, const int32_t *blk, int nh, const Spa
             }
         }
     }
-    moved = warp_max(moved);
-    if ((threadIdx.x & 31) == 0 && moved > 0.0) atomic_max_nonneg(&st[h].moved[colour], moved);
+    block_max_to(&st[h].moved[colour], moved);
 }
 
 // Rows per block of the residual kernel (and of its launch plan, row_plan).
@@ -133,7 +132,6 @@ constexpr int RES_ROWS = 4;
 __global__ void __launch_bounds__(256) k_residual64(FieldView fv, const int32_t *blk, int nh, RelaxState *st,
                                                     float *r32, float *inv32, float *dz, int skip_done) {
     __shared__ int s_h;
-    __shared__ double s_worst[8];
     if (threadIdx.x == 0) s_h = plan_history(blk, nh, blockIdx.x);
     __syncthreads();
     int h = s_h;
@@ -171,15 +169,7 @@ __global__ void __launch_bounds__(256) k_residual64(FieldView fv, const int32_t 
         if (inv32) inv32[i] = inv_out;
         if (dz) dz[i] = 0.0f;
     }
-    // one atomic per block: many per history would queue on its one word
-    worst = warp_max(worst);
-    if ((threadIdx.x & 31) == 0) s_worst[threadIdx.x >> 5] = worst;
-    __syncthreads();
-    if (threadIdx.x < 32) {
-        worst = threadIdx.x < (blockDim.x >> 5) ? s_worst[threadIdx.x] : 0.0;
-        worst = warp_max(worst);
-        if (threadIdx.x == 0 && worst > 0.0) atomic_max_nonneg(&st[h].resid, worst);
-    }
+    block_max_to(&st[h].resid, worst);
 }
 
 // After sweep `index`: decide convergence (relax's `moved < tolerance`,
@@ -257,8 +247,7 @@ __global__ void __launch_bounds__(256) k_dc_update(FieldView fv, const int32_t *
             dlt[i] = 0.f;
         }
     }
-    worst = warp_max(worst);
-    if ((threadIdx.x & 31) == 0 && worst > 0.0) atomic_max_nonneg(&st[h].resid, worst);
+    block_max_to(&st[h].resid, worst);
 }
 
 __global__ void k_dc_check(RelaxState *st, int nh, int inner, int64_t max_sweeps) {
