@@ -208,6 +208,12 @@ struct cw_lattice_s {
     int8_t reach[3 * 124] = {0};
     double across = 1.0;
     int32_t *d_flag = nullptr;       // scratch flag / counters
+    // scratch of the sublattice passes (lattice.cu): claims, pending lists, control words
+    unsigned long long *claim = nullptr;  // 2 * ncells
+    uint4 *plist = nullptr;               // 2 * plist_cap
+    int64_t plist_cap = 0;
+    uint32_t *pctl = nullptr;             // 8 + nh
+    int pass_grid = 0;                    // blocks of the cooperative pass launch
     int build_plans();
 };
 
@@ -243,6 +249,7 @@ int field_dc_prepare(cw_field_s *f, int depth, int window, const std::vector<dou
 int field_relax_collect(cw_field_s *f, std::vector<cw_relax_stats> &out, bool &all_settled);
 int lattice_recount(cw_lattice_s *lat, int32_t *vol_out, int32_t *surf_out);
 int lattice_sweep(cw_lattice_s *lat);
+int lattice_pass_error(cw_lattice_s *l);
 // coupling (coupling.cu), device-resident
 int couple_uptake_device(cw_field_s *f, cw_lattice_s *l, const double *d_rate_by_type, int K, double *dst,
                          const Plan &p);

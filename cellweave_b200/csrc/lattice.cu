@@ -5,11 +5,15 @@
 // is a sequence of sublattice passes.  Pixels are coloured so that no pixel
 // of a colour lies within the contact reach of another (the chessboard for
 // contact across faces; a period R+1 in every axis for a reach of Chebyshev
-// radius R); a pass makes one copy attempt at every pixel of one colour, all
-// at once.  Attempts of one pass never read a pixel another of them writes,
-// and read volumes and surfaces from a snapshot taken when the pass starts,
-// so a pass is deterministic whatever the thread schedule.  The colours are
-// swept in an order shuffled anew every step.
+// radius R); a pass makes one copy attempt at every pixel of one colour.
+// Attempts of one pass never read a pixel another of them writes; they meet
+// only through the volume and surface records of cells they share.  A pass
+// runs its attempts as the sequence in a per-pass priority order would (each
+// seeing the records every earlier one left): attempts that share no cell run
+// at once, the others in rounds, in priority order (k_cpm_pass).  So a pass is
+// deterministic whatever the thread schedule, and keeps the sequential
+// sweep's volume statistics.  The colours are swept in an order shuffled anew
+// every step.
 //
 // Each attempt is the reference's try_flip (cpm.rs:797-838): a neighbour
 // across a face drawn uniformly, no proposal from or into an obstacle or
@@ -205,75 +209,215 @@ __device__ __forceinline__ bool colour_site(int4 dm, int period, int colour, uin
     return true;
 }
 
-// One sublattice pass: one copy attempt at every pixel of this pass's colour.
-__global__ void __launch_bounds__(T) k_cpm_pass(LatView L, Tables tabs, const int32_t *blk, int nh,
-                                                const int32_t *perm, int pass, const uint32_t *mcs_cur) {
-    __shared__ double sJ[64];
-    __shared__ int8_t sreach[3 * 124];
-    __shared__ int s_h;
-    if (threadIdx.x == 0) s_h = plan_history(blk, nh, blockIdx.x);
-    for (int i = threadIdx.x; i < L.K * L.K; i += blockDim.x) sJ[i] = tabs.J[i];
-    for (int i = threadIdx.x; i < 3 * L.nreach; i += blockDim.x) sreach[i] = tabs.reach[i];
+// MurmurHash3's 32-bit finaliser (Appleby): a bijection of 32-bit words, so
+// the pixels of one history get distinct priorities in a pass.
+__device__ __forceinline__ uint32_t fmix32(uint32_t h) {
+    h ^= h >> 16;
+    h *= 0x85ebca6bu;
+    h ^= h >> 13;
+    h *= 0xc2b2ae35u;
+    h ^= h >> 16;
+    return h;
+}
+
+// Scratch of the passes: two claim words per cell (by round parity), two
+// lists of pending attempts, and control words.
+struct PassScratch {
+    unsigned long long *claim[2];  // ncells each
+    uint4 *list[2];                // (history, pixel, source id, copied id)
+    uint32_t *ctl;                 // CTL_* below, then a pass key per history
+};
+enum { CTL_COUNT = 0, CTL_BAR = 3, CTL_GEN = 4, CTL_ERR = 5, CTL_ROUNDS = 6, CTL_KEYS = 8 };
+constexpr int MAX_ROUNDS = 256;
+constexpr unsigned long long BARRIER_NS = 2000000000ull;
+
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// A barrier over the whole (co-resident, cooperatively launched) grid whose
+// wait gives up after BARRIER_NS; false then, on every thread of the block.
+__device__ bool grid_barrier(uint32_t *ctl, int *s_ok) {
     __syncthreads();
-    const int h = s_h;
-    const int4 dm = L.dims[h];
-    const int colour = perm[h * L.ncol + pass];
-    const uint32_t k = (uint32_t)(blockIdx.x - blk[h]) * blockDim.x + threadIdx.x;
-    const int64_t c0 = L.cell_off[h], cap = L.cell_off[h + 1] - c0;
-    int32_t *g = L.grid + L.off[h];
-    const int32_t *type_h = L.type + c0;
-    int x = 0, y = 0, z = 0;
-    bool accept = false;
-    int32_t src = 0, dst = 0, dsrc = 0, ddst = 0;
-    if (colour_site(dm, L.period, colour, k, x, y, z)) {
-        int64_t i = ((int64_t)z * dm.y + y) * dm.x + x;
-        int64_t vn[6];
-        int nvn = von_neumann(dm, x, y, z, i, vn);
-        if (nvn > 0) {
-            uint2 key = L.keys[h];
-            uint4 r = philox((uint32_t)i, *mcs_cur, 0u, 0u, key.x, key.y);
-            src = g[i];
-            dst = g[vn[((uint64_t)r.x * (uint64_t)nvn) >> 32]];
-            if (src != dst && src != OBST && dst != OBST) {
-                double num;
-                double delta = contact_delta(g, dm, x, y, z, src, dst, type_h, cap, sJ, L.K, sreach, L.nreach,
-                                             L.across, vn, nvn, &num) +
-                               volume_delta(L.vsnap, L.target, L.lambda, c0, src, dst);
-                if (L.surface_on) {
-                    surface_change(g, vn, nvn, src, dst, dsrc, ddst);
-                    delta += surface_delta(L.ssnap, L.tsurf, L.lsurf, c0, src, dst, dsrc, ddst);
-                }
-                accept = delta <= 0.0;
-                if (!accept) accept = u01(r.y, r.z) < own_exp(-delta / L.temperature);
-                if (accept) g[i] = dst;
+    if (threadIdx.x == 0) {
+        volatile uint32_t *gen = ctl + CTL_GEN;
+        const uint32_t g0 = *gen;
+        int ok = 1;
+        __threadfence();
+        if (atomicAdd(ctl + CTL_BAR, 1u) == gridDim.x - 1) {
+            ctl[CTL_BAR] = 0u;
+            __threadfence();
+            atomicAdd(ctl + CTL_GEN, 1u);
+        } else {
+            const uint64_t t0 = global_ns();
+            while (*gen == g0) {
+                if (global_ns() - t0 > BARRIER_NS) { ok = 0; break; }
+                __nanosleep(64);
             }
         }
+        __threadfence();
+        *s_ok = ok;
     }
-    // bookkeeping: one atomic per distinct cell per warp
-    const unsigned am = __ballot_sync(0xffffffffu, accept);
-    if (accept) {
-        const int lane = threadIdx.x & 31;
-        unsigned peers = __match_any_sync(am, src);
-        if (src != 0 && lane == __ffs(peers) - 1) atomicSub(L.volume + c0 + src, __popc(peers));
-        if (L.surface_on) {
-            int s = __reduce_add_sync(peers, (unsigned)dsrc);
-            if (src > 0 && lane == __ffs(peers) - 1) atomicAdd(L.surface + c0 + src, s);
+    __syncthreads();
+    return *s_ok != 0;
+}
+
+// One sublattice pass: one copy attempt at every pixel of this pass's colour
+// (the reference's try_flip, cpm.rs:797-838), the attempts ordered by a
+// per-pass priority and run as that sequence would run them.  The pixels of
+// a colour lie outside one another's reach, so two attempts meet only
+// through the records of a cell they both involve (volume, surface).  First
+// every attempt that copies (source and copied ids differ, neither the
+// obstacle) claims its cells other than the medium with its priority; in
+// each round an attempt holding the claim on all its cells runs against the
+// live records, the others claim again for the next round.  An attempt runs
+// only after every higher-priority attempt sharing a cell with it, which is
+// the sequence in decreasing priority, whatever the thread schedule.
+__global__ void __launch_bounds__(T) k_cpm_pass(LatView L, Tables tabs, const int32_t *blk, int nh, int nvb,
+                                                const int32_t *perm, int pass, const uint32_t *mcs_cur,
+                                                PassScratch S) {
+    __shared__ double sJ[64];
+    __shared__ int8_t sreach[3 * 124];
+    __shared__ int s_h, s_ok;
+    __shared__ uint32_t s_key;
+    for (int i = threadIdx.x; i < L.K * L.K; i += blockDim.x) sJ[i] = tabs.J[i];
+    for (int i = threadIdx.x; i < 3 * L.nreach; i += blockDim.x) sreach[i] = tabs.reach[i];
+    const uint32_t mcs = *mcs_cur;
+    const int lane = threadIdx.x & 31;
+    // ---- propose and claim (round 1's claims)
+    for (int vb = blockIdx.x; vb < nvb; vb += gridDim.x) {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const int h = plan_history(blk, nh, vb);
+            const uint2 key = L.keys[h];
+            s_h = h;
+            s_key = philox(0xFFFFFFFEu, mcs, 2u, (uint32_t)perm[h * L.ncol + pass], key.x, key.y).x;
+            if (vb == blk[h]) S.ctl[CTL_KEYS + h] = s_key;
         }
-        peers = __match_any_sync(am, dst);
-        if (dst != 0 && lane == __ffs(peers) - 1) atomicAdd(L.volume + c0 + dst, __popc(peers));
-        if (L.surface_on) {
-            int s = __reduce_add_sync(peers, (unsigned)ddst);
-            if (dst > 0 && lane == __ffs(peers) - 1) atomicAdd(L.surface + c0 + dst, s);
+        __syncthreads();
+        const int h = s_h;
+        const int4 dm = L.dims[h];
+        const int colour = perm[h * L.ncol + pass];
+        const uint32_t k = (uint32_t)(vb - blk[h]) * blockDim.x + threadIdx.x;
+        const int64_t c0 = L.cell_off[h];
+        const int32_t *g = L.grid + L.off[h];
+        int x = 0, y = 0, z = 0;
+        bool copies = false;
+        uint4 entry = make_uint4(0, 0, 0, 0);
+        if (colour_site(dm, L.period, colour, k, x, y, z)) {
+            const int64_t i = ((int64_t)z * dm.y + y) * dm.x + x;
+            int64_t vn[6];
+            const int nvn = von_neumann(dm, x, y, z, i, vn);
+            if (nvn > 0) {
+                const uint2 key = L.keys[h];
+                const uint4 r = philox((uint32_t)i, mcs, 0u, 0u, key.x, key.y);
+                const int32_t src = g[i];
+                const int32_t dst = g[vn[((uint64_t)r.x * (uint64_t)nvn) >> 32]];
+                if (src != dst && src != OBST && dst != OBST) {
+                    copies = true;
+                    const unsigned long long claim = (1ull << 32) | fmix32((uint32_t)i ^ s_key);
+                    if (src > 0) atomicMax(S.claim[1] + c0 + src, claim);
+                    if (dst > 0) atomicMax(S.claim[1] + c0 + dst, claim);
+                    entry = make_uint4((uint32_t)h, (uint32_t)i, (uint32_t)src, (uint32_t)dst);
+                }
+            }
+        }
+        // append, one atomic per warp
+        const unsigned m = __ballot_sync(0xffffffffu, copies);
+        uint32_t base = 0;
+        if (lane == 0 && m) base = atomicAdd(S.ctl + CTL_COUNT + 0, (uint32_t)__popc(m));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (copies) S.list[0][base + __popc(m & ((1u << lane) - 1u))] = entry;
+    }
+    if (!grid_barrier(S.ctl, &s_ok)) {
+        if (threadIdx.x == 0) atomicExch(S.ctl + CTL_ERR, 1u);
+        return;
+    }
+    // ---- rounds
+    for (int r = 1;; ++r) {
+        const uint32_t n_in = *(volatile uint32_t *)(S.ctl + CTL_COUNT + (r - 1) % 3);
+        if (n_in == 0) break;
+        if (r > MAX_ROUNDS) {
+            if (blockIdx.x == 0 && threadIdx.x == 0) atomicExch(S.ctl + CTL_ERR, 2u);
+            break;
+        }
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            S.ctl[CTL_COUNT + (r + 1) % 3] = 0u;  // the output of round r + 1; last read as round r - 1's input
+            atomicMax(S.ctl + CTL_ROUNDS, (uint32_t)r);
+        }
+        const uint4 *in = S.list[(r - 1) & 1];
+        uint4 *out = S.list[r & 1];
+        const unsigned long long *mine = S.claim[r & 1];
+        unsigned long long *next = S.claim[(r + 1) & 1];
+        const uint32_t stride = gridDim.x * blockDim.x;
+        for (uint32_t e0 = blockIdx.x * blockDim.x; e0 < n_in; e0 += stride) {
+            const uint32_t e = e0 + threadIdx.x;
+            bool again = false, accept = false;
+            uint4 en = make_uint4(0, 0, 0, 0);
+            int32_t src = 0, dst = 0, dsrc = 0, ddst = 0;
+            int64_t c0 = 0;
+            if (e < n_in) {
+                en = in[e];
+                const int h = (int)en.x;
+                src = (int32_t)en.z;
+                dst = (int32_t)en.w;
+                c0 = L.cell_off[h];
+                const uint32_t prio = fmix32(en.y ^ S.ctl[CTL_KEYS + h]);
+                const unsigned long long key = ((unsigned long long)r << 32) | prio;
+                const bool win = (src <= 0 || mine[c0 + src] == key) && (dst <= 0 || mine[c0 + dst] == key);
+                if (win) {
+                    const int4 dm = L.dims[h];
+                    const int64_t i = en.y;
+                    const int x = (int)(i % dm.x), y = (int)((i / dm.x) % dm.y);
+                    const int z = (int)(i / ((int64_t)dm.x * dm.y));
+                    int32_t *g = L.grid + L.off[h];
+                    const int64_t cap = L.cell_off[h + 1] - c0;
+                    int64_t vn[6];
+                    const int nvn = von_neumann(dm, x, y, z, i, vn);
+                    const uint2 kk = L.keys[h];
+                    const uint4 rr = philox((uint32_t)i, mcs, 0u, 0u, kk.x, kk.y);
+                    double num;
+                    double delta = contact_delta(g, dm, x, y, z, src, dst, L.type + c0, cap, sJ, L.K, sreach,
+                                                 L.nreach, L.across, vn, nvn, &num) +
+                                   volume_delta(L.volume, L.target, L.lambda, c0, src, dst);
+                    if (L.surface_on) {
+                        surface_change(g, vn, nvn, src, dst, dsrc, ddst);
+                        delta += surface_delta(L.surface, L.tsurf, L.lsurf, c0, src, dst, dsrc, ddst);
+                    }
+                    accept = delta <= 0.0;
+                    if (!accept) accept = u01(rr.y, rr.z) < own_exp(-delta / L.temperature);
+                    if (accept) g[i] = dst;
+                } else {
+                    const unsigned long long claim = ((unsigned long long)(r + 1) << 32) | prio;
+                    if (src > 0) atomicMax(next + c0 + src, claim);
+                    if (dst > 0) atomicMax(next + c0 + dst, claim);
+                    again = true;
+                }
+            }
+            // the records of an accepted copy: its cells are its own this round
+            if (accept) {
+                if (src != 0) L.volume[c0 + src] -= 1;
+                if (dst != 0) L.volume[c0 + dst] += 1;
+                if (L.surface_on) {
+                    if (src > 0) L.surface[c0 + src] += dsrc;
+                    if (dst > 0) L.surface[c0 + dst] += ddst;
+                }
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, again);
+            uint32_t base = 0;
+            if (lane == 0 && m) base = atomicAdd(S.ctl + CTL_COUNT + r % 3, (uint32_t)__popc(m));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (again) out[base + __popc(m & ((1u << lane) - 1u))] = en;
+        }
+        if (!grid_barrier(S.ctl, &s_ok)) {
+            if (threadIdx.x == 0) atomicExch(S.ctl + CTL_ERR, 1u);
+            return;
         }
     }
 }
 
-__global__ void k_copy32(int32_t *dst, const int32_t *src, int64_t n) {
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) dst[i] = src[i];
-}
-
-// Delta-H of explicit proposals on one history, on live volumes.
 __global__ void k_delta_h(LatView L, Tables tabs, int h, int64_t n, const int64_t *site, const int32_t *dstv,
                           double *out) {
     __shared__ double sJ[64];
@@ -383,6 +527,7 @@ int cw_lattice_s::build_plans() {
     for (auto &p : plans) p.release();
     plans.assign(1, Plan());
     std::vector<int64_t> per(g.nh, 0);
+    int64_t cap = 0;
     for (uint32_t k = 0; k < g.nh; ++k) {
         if (period == 0) {
             per[k] = (int64_t)((g.w[k] + 1) / 2) * g.h[k] * g.d[k];
@@ -391,8 +536,29 @@ int cw_lattice_s::build_plans() {
             int64_t nz = volume ? (g.d[k] + period - 1) / period : 1;
             per[k] = nx * ny * nz;  // the largest colour class
         }
+        cap += per[k];
     }
-    return plans[0].build(per, T);
+    int rc = plans[0].build(per, T);
+    if (rc != CW_OK) return rc;
+    // the pass scratch: a pending list holds at most every pixel of a colour
+    if (cap > plist_cap) {
+        dfree(plist);
+        if ((rc = dalloc(&plist, 2 * (size_t)cap)) != CW_OK) return rc;
+        plist_cap = cap;
+    }
+    if (!claim && (rc = dalloc(&claim, 2 * (size_t)ncells)) != CW_OK) return rc;
+    if (!pctl) {
+        if ((rc = dalloc(&pctl, 8 + (size_t)g.nh)) != CW_OK) return rc;
+        CW_CUDA(cudaMemsetAsync(pctl, 0, sizeof(uint32_t) * (8 + (size_t)g.nh), stream()));
+    }
+    if (pass_grid == 0) {
+        int per_sm = 0, dev = 0, nsm = 0;
+        CW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)k_cpm_pass, T, 0));
+        CW_CUDA(cudaGetDevice(&dev));
+        CW_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        pass_grid = std::max(1, per_sm * nsm);
+    }
+    return CW_OK;
 }
 
 namespace {
@@ -448,26 +614,57 @@ int lattice_recount(cw_lattice_s *l, int32_t *vol_out, int32_t *surf_out) {
     return CW_OK;
 }
 
-// One Monte Carlo step of every history (no host synchronisation).
+// One Monte Carlo step of every history (no host synchronisation): the
+// colour order, then one cooperative launch per colour (its rounds meet at a
+// grid barrier), the claims and control words cleared before each.
 int lattice_sweep(cw_lattice_s *l) {
     LatDevice d = dev_of(l);
     k_colour_order<<<1, 128, 0, stream()>>>(l->d_keys, l->g.nh, l->ncol, d.mcs, d.mcs + 1, d.perm);
     CW_LAUNCHED();
     LatView v = lat_view(l);
     Tables t = lat_tables(l);
-    unsigned cb = (unsigned)((l->ncells + T - 1) / T);
+    PassScratch S;
+    S.claim[0] = l->claim;
+    S.claim[1] = l->claim + l->ncells;
+    S.list[0] = l->plist;
+    S.list[1] = l->plist + l->plist_cap;
+    S.ctl = l->pctl;
+    int nvb = l->plans[0].nblocks;
+    const int grid = std::min(nvb, l->pass_grid);
+    const int32_t *blk = l->plans[0].d_blk;
+    int nh = (int)l->g.nh;
+    const uint32_t *cur = d.mcs + 1;
     for (int q = 0; q < l->ncol; ++q) {
-        k_copy32<<<cb, T, 0, stream()>>>(l->vsnap, l->volume, l->ncells);
-        CW_LAUNCHED();
-        if (l->surface_on) {
-            k_copy32<<<cb, T, 0, stream()>>>(l->ssnap, l->surface, l->ncells);
-            CW_LAUNCHED();
-        }
-        k_cpm_pass<<<l->plans[0].nblocks, T, 0, stream()>>>(v, t, l->plans[0].d_blk, l->g.nh, d.perm, q, d.mcs + 1);
-        CW_LAUNCHED();
+        CW_CUDA(cudaMemsetAsync(l->claim, 0, sizeof(unsigned long long) * 2 * (size_t)l->ncells, stream()));
+        // the three list counters and the barrier's count and generation
+        CW_CUDA(cudaMemsetAsync(l->pctl + CTL_COUNT, 0, sizeof(uint32_t) * 5, stream()));
+        void *args[] = {&v, &t, (void *)&blk, &nh, &nvb, &d.perm, &q, (void *)&cur, &S};
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+        cfg.gridDim = dim3((unsigned)grid);
+        cfg.blockDim = dim3(T);
+        cfg.dynamicSmemBytes = 0;
+        cfg.stream = stream();
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        CW_CUDA(cudaLaunchKernelExC(&cfg, (const void *)k_cpm_pass, args));
+        count_launch(1);
     }
     l->mcs += 1;
     return CW_OK;
+}
+
+// CW_ERR_TIMEOUT (or CW_ERR_SIMULATION) if a pass gave up since the last
+// call: a grid barrier that waited too long, or more rounds than allowed.
+int lattice_pass_error(cw_lattice_s *l) {
+    uint32_t e = 0, zero = 0;
+    CW_CUDA(cudaMemcpy(&e, l->pctl + CTL_ERR, sizeof e, cudaMemcpyDeviceToHost));
+    if (!e) return CW_OK;
+    CW_CUDA(cudaMemcpy(l->pctl + CTL_ERR, &zero, sizeof zero, cudaMemcpyHostToDevice));
+    return e == 1 ? fail(CW_ERR_TIMEOUT, "a sublattice pass waited more than 2 s at a grid barrier")
+                  : fail(CW_ERR_SIMULATION, "a sublattice pass needed more than 256 rounds");
 }
 }  // namespace cw
 
@@ -524,10 +721,16 @@ int cw_lattice_destroy(cw_lattice l) {
     if (!l) return CW_OK;
     dfree(l->grid); dfree(l->type); dfree(l->volume); dfree(l->target); dfree(l->lambda); dfree(l->vsnap);
     dfree(l->surface); dfree(l->ssnap); dfree(l->tsurf); dfree(l->lsurf); dfree(l->d_cell_off); dfree(l->d_keys);
-    dfree(l->d_flag);
+    dfree(l->d_flag); dfree(l->claim); dfree(l->plist); dfree(l->pctl);
     for (auto &p : l->plans) p.release();
     l->g.release();
     delete l;
+    return CW_OK;
+}
+
+int cw_lattice_capacity(cw_lattice l, uint32_t hist, uint32_t *cap) {
+    if (hist >= l->g.nh) return fail(CW_ERR_NOT_FOUND, "no history " + std::to_string(hist));
+    *cap = (uint32_t)(l->cell_off[hist + 1] - l->cell_off[hist]);
     return CW_OK;
 }
 
@@ -667,7 +870,7 @@ int cw_lattice_mcs(cw_lattice l, uint32_t sweeps) {
         if (rc != CW_OK) return rc;
     }
     CW_CUDA(cudaStreamSynchronize(stream()));
-    return CW_OK;
+    return lattice_pass_error(l);
 }
 
 int cw_lattice_delta_h_batch(cw_lattice l, uint32_t hist, uint32_t n, const int64_t *site, const int32_t *dst,

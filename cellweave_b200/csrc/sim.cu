@@ -663,11 +663,12 @@ int cw_sim_stats(cw_sim s, double *out) {
     CW_LAUNCHED();
     CW_CUDA(cudaMemcpyAsync(out, d_out, sizeof(double) * 4 * nh, cudaMemcpyDeviceToHost, stream()));
     CW_CUDA(cudaStreamSynchronize(stream()));
+    dfree(d_out);
+    if ((rc = lattice_pass_error(s->lat)) != CW_OK) return rc;
     for (uint32_t k = 0; k < nh; ++k) {
         out[4 * k + 2] = (double)s->last[k].sweeps;
         out[4 * k + 3] = s->last[k].residual;
     }
-    dfree(d_out);
     return CW_OK;
 }
 

@@ -223,7 +223,12 @@ class CpmLattice:
         lat.dims, w, h, z = _dims(dims)
         nh = C.c_uint32()
         call("cw_lattice_count", handle, C.byref(nh))
-        lat.capacity = None
+        caps = []
+        for k in range(nh.value):
+            c = C.c_uint32()
+            call("cw_lattice_capacity", handle, k, C.byref(c))
+            caps.append(c.value)
+        lat.capacity = np.array(caps, np.uint32)
         lat.temperature = None
         return lat
 

@@ -80,6 +80,8 @@ int cw_lattice_create(uint32_t nh, const uint32_t *w, const uint32_t *h, const u
                       const uint32_t *cell_capacity, double temperature, cw_lattice *out);
 int cw_lattice_destroy(cw_lattice lat);
 int cw_lattice_count(cw_lattice lat, uint32_t *nh);
+/* The cell records history `hist` holds (its capacity, the medium's included). */
+int cw_lattice_capacity(cw_lattice lat, uint32_t hist, uint32_t *cap);
 /* ContactEnergy (cpm.rs:30-129) generalised to a K x K table over cell types
  * (K <= 8, symmetric, J[0] the medium-medium 0), and set_contact_order
  * (cpm.rs:274-301): 1 faces only, 2 and 3 the wider reach and its divisor. */

@@ -727,62 +727,111 @@ void or_colour_order(int32_t ncol, uint32_t mcs, uint32_t k0, uint32_t k1, int32
     }
 }
 
+/* MurmurHash3's 32-bit finaliser (Appleby): a bijection of 32-bit words, so
+ * distinct pixels of one pass get distinct priorities. */
+static inline uint32_t or_fmix32(uint32_t h) {
+    h ^= h >> 16;
+    h *= 0x85ebca6bu;
+    h ^= h >> 13;
+    h *= 0xc2b2ae35u;
+    h ^= h >> 16;
+    return h;
+}
+
+/* A pass's priority of pixel `site`: the pass's key is word 0 of
+ * Philox(0xFFFFFFFE, step, 2, colour) under the history's key. */
+uint32_t or_pass_priority(uint32_t site, uint32_t mcs, int32_t colour, uint32_t k0, uint32_t k1) {
+    or_u32x4 r = or_philox(0xFFFFFFFEu, mcs, 2u, (uint32_t)colour, k0, k1);
+    return or_fmix32(site ^ r.v[0]);
+}
+
+typedef struct {
+    uint32_t prio;
+    int64_t site;
+} or_ranked;
+
+static int or_by_priority_desc(const void *a, const void *b) {
+    uint32_t pa = ((const or_ranked *)a)->prio, pb = ((const or_ranked *)b)->prio;
+    return pa < pb ? 1 : (pa > pb ? -1 : 0);
+}
+
 /* `sweeps` lattice steps of the sublattice scheme, starting at step counter
  * `mcs0`.  Per colour pass every pixel of the colour makes one attempt from
- * draws Philox(site, mcs, 0, 0) under key (k0, k1); volumes and surfaces in
- * Delta-H are read from a snapshot taken at the start of the pass, and the
- * accepted changes are added to the live records. */
-void or_lattice_mcs_checkerboard(or_lattice *l, uint32_t k0, uint32_t k1, uint32_t mcs0, int32_t sweeps) {
+ * draws Philox(site, mcs, 0, 0) under key (k0, k1), the pixels taken one at a
+ * time in decreasing pass priority (or_pass_priority), each seeing the
+ * volumes and surfaces every earlier one left.  The pixels of a colour lie
+ * outside one another's reach, so two attempts of a pass meet only through
+ * the records of a cell they share; the device runs the attempts that share
+ * no cell at once and settles the others in priority order, which is this
+ * sequence.
+ *
+ * `snapshot` != 0 is a planted mistake for the statistical tests: every
+ * attempt of a pass reads the volumes and surfaces the pass started with. */
+void or_lattice_mcs_checkerboard(or_lattice *l, uint32_t k0, uint32_t k1, uint32_t mcs0, int32_t sweeps,
+                                 int32_t snapshot) {
     int32_t reach[3 * OR_MAX_REACH];
     double across;
     int nreach = or_reach(l->order, l->d > 1, reach, &across);
     int32_t period;
     int32_t ncol = or_colouring(l, &period);
     int32_t perm[27];
-    int32_t *vsnap = (int32_t *)malloc(sizeof(int32_t) * (size_t)l->ncells);
-    int32_t *ssnap = l->surface ? (int32_t *)malloc(sizeof(int32_t) * (size_t)l->ncells) : NULL;
-    int64_t w = l->w, slice = (int64_t)l->w * l->h;
+    int64_t w = l->w, slice = (int64_t)l->w * l->h, n = slice * l->d;
+    or_ranked *order = (or_ranked *)malloc(sizeof(or_ranked) * (size_t)(n > 0 ? n : 1));
+    int32_t *vsnap = snapshot ? (int32_t *)malloc(sizeof(int32_t) * (size_t)l->ncells) : NULL;
+    int32_t *ssnap = snapshot && l->surface ? (int32_t *)malloc(sizeof(int32_t) * (size_t)l->ncells) : NULL;
     for (int32_t s = 0; s < sweeps; ++s) {
         uint32_t mcs = mcs0 + (uint32_t)s;
         or_colour_order(ncol, mcs, k0, k1, perm);
         for (int32_t q = 0; q < ncol; ++q) {
             int32_t colour = perm[q];
-            memcpy(vsnap, l->volume, sizeof(int32_t) * (size_t)l->ncells);
+            if (vsnap) memcpy(vsnap, l->volume, sizeof(int32_t) * (size_t)l->ncells);
             if (ssnap) memcpy(ssnap, l->surface, sizeof(int32_t) * (size_t)l->ncells);
+            const int32_t *vol = vsnap ? vsnap : l->volume;
+            const int32_t *surf = ssnap ? ssnap : l->surface;
+            int64_t m = 0;
             for (int32_t z = 0; z < l->d; ++z)
                 for (int32_t y = 0; y < l->h; ++y)
                     for (int32_t x = 0; x < l->w; ++x) {
                         if (or_colour_of(period, x, y, z) != colour) continue;
                         int64_t site = (int64_t)z * slice + (int64_t)y * w + x;
-                        int64_t nbr[6];
-                        int nn = or_von_neumann(l, x, y, z, nbr);
-                        if (nn == 0) continue;
-                        or_u32x4 r = or_philox((uint32_t)site, mcs, 0u, 0u, k0, k1);
-                        int32_t src = l->grid[site];
-                        int32_t dst = l->grid[nbr[((uint64_t)r.v[0] * (uint64_t)nn) >> 32]];
-                        if (src == dst || src == OR_OBSTACLE || dst == OR_OBSTACLE) continue;
-                        double num;
-                        double delta = or_contact_delta(l, reach, nreach, across, x, y, z, src, dst, &num) +
-                                       or_volume_delta(l, vsnap, src, dst);
-                        int32_t ds = 0, dd = 0;
-                        if (ssnap) {
-                            or_surface_change(l, x, y, z, src, dst, &ds, &dd);
-                            delta += or_surface_delta(l, ssnap, src, dst, ds, dd);
-                        }
-                        int accept = delta <= 0.0;
-                        if (!accept) accept = or_u01(r.v[1], r.v[2]) < or_cw_exp(-delta / l->temperature);
-                        if (accept) {
-                            l->grid[site] = dst;
-                            if (src != 0) l->volume[src] -= 1;
-                            if (dst != 0) l->volume[dst] += 1;
-                            if (ssnap) {
-                                if (src > 0) l->surface[src] += ds;
-                                if (dst > 0) l->surface[dst] += dd;
-                            }
-                        }
+                        order[m].site = site;
+                        order[m].prio = or_pass_priority((uint32_t)site, mcs, colour, k0, k1);
+                        ++m;
                     }
+            qsort(order, (size_t)m, sizeof(or_ranked), or_by_priority_desc);
+            for (int64_t e = 0; e < m; ++e) {
+                int64_t site = order[e].site;
+                int32_t x = (int32_t)(site % w), y = (int32_t)((site / w) % l->h), z = (int32_t)(site / slice);
+                int64_t nbr[6];
+                int nn = or_von_neumann(l, x, y, z, nbr);
+                if (nn == 0) continue;
+                or_u32x4 r = or_philox((uint32_t)site, mcs, 0u, 0u, k0, k1);
+                int32_t src = l->grid[site];
+                int32_t dst = l->grid[nbr[((uint64_t)r.v[0] * (uint64_t)nn) >> 32]];
+                if (src == dst || src == OR_OBSTACLE || dst == OR_OBSTACLE) continue;
+                double num;
+                double delta = or_contact_delta(l, reach, nreach, across, x, y, z, src, dst, &num) +
+                               or_volume_delta(l, vol, src, dst);
+                int32_t ds = 0, dd = 0;
+                if (l->surface) {
+                    or_surface_change(l, x, y, z, src, dst, &ds, &dd);
+                    delta += or_surface_delta(l, surf, src, dst, ds, dd);
+                }
+                int accept = delta <= 0.0;
+                if (!accept) accept = or_u01(r.v[1], r.v[2]) < or_cw_exp(-delta / l->temperature);
+                if (accept) {
+                    l->grid[site] = dst;
+                    if (src != 0) l->volume[src] -= 1;
+                    if (dst != 0) l->volume[dst] += 1;
+                    if (l->surface) {
+                        if (src > 0) l->surface[src] += ds;
+                        if (dst > 0) l->surface[dst] += dd;
+                    }
+                }
+            }
         }
     }
+    free(order);
     free(vsnap);
     free(ssnap);
 }

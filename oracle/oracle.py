@@ -50,7 +50,7 @@ def lib():
         L.or_lattice_delta_h.restype = None
         L.or_lattice_mcs_sequential.argtypes = [P, C.c_uint64, C.c_int32]
         L.or_lattice_mcs_sequential.restype = None
-        L.or_lattice_mcs_checkerboard.argtypes = [P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int32]
+        L.or_lattice_mcs_checkerboard.argtypes = [P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int32, C.c_int32]
         L.or_lattice_mcs_checkerboard.restype = None
         L.or_lattice_recount.argtypes = [P, P, P]
         L.or_lattice_recount.restype = None
@@ -243,10 +243,12 @@ class Lattice:
         s = self._struct()
         lib().or_lattice_mcs_sequential(C.byref(s), int(seed) & (2**64 - 1), int(sweeps))
 
-    def mcs_checkerboard(self, seed: int, mcs0: int, sweeps: int = 1):
+    def mcs_checkerboard(self, seed: int, mcs0: int, sweeps: int = 1, snapshot: bool = False):
+        """The device's sublattice sweeps; `snapshot`: the planted mistake of
+        reading one snapshot of the records per pass (statistical tests only)."""
         s = self._struct()
         lib().or_lattice_mcs_checkerboard(C.byref(s), int(seed) & 0xFFFFFFFF, (int(seed) >> 32) & 0xFFFFFFFF,
-                                          int(mcs0) & 0xFFFFFFFF, int(sweeps))
+                                          int(mcs0) & 0xFFFFFFFF, int(sweeps), int(bool(snapshot)))
 
     def occupied_span(self):
         s = self._struct()

@@ -1,0 +1,89 @@
+"""The device's dynamics as distributions over 32 seeds (GPU).
+
+The CPM: 32 histories swept in one batch on the device against the oracle's
+restatement of the reference's sequential random-pixel sweep (cpm.rs:748-838)
+from the same starting lattices: pooled cell volumes alike (KS test, spread,
+mean), the boundary length inside the sequential ensemble's band.
+
+The whole step: 32 histories of a small cord-like campaign stepped by the
+device against the CPU oracle stepping the reference's algorithms one
+history at a time (sequential sweep, FP64 SOR, RK4; oracle/cpu_sim.py):
+population, mean oxygen over the cells and the hypoxic fraction of the
+living cells inside the oracle's band at several steps.
+"""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+import cellweave_b200 as cw
+from cellweave_b200 import synthetic
+from cpm_ensembles import J, ORDER, SEEDS, SIZE, T, observables, oracle_ensemble, same_volume_law, sheet, within_band
+from oracle import oracle as O
+from oracle.cpu_sim import CpuHistory
+
+pytestmark = pytest.mark.gpu
+
+
+def test_device_sweeps_match_the_sequential_ensemble():
+    mcs = 60
+    sheets = [sheet(k) for k in range(SEEDS)]
+    lat = cw.CpmLattice.from_grids([g for g, _ in sheets], [r for _, r in sheets], T, J, ORDER,
+                                   seeds=[1_000_003 * k + 17 for k in range(SEEDS)])
+    lat.monte_carlo_step(mcs)
+    vols, bnd = [], []
+    for k in range(SEEDS):
+        assert lat.records_match_grid(k)
+        g = lat.grid(k).reshape(SIZE, SIZE)
+        v, b = observables(g, np.bincount(g[g >= 0].ravel(), minlength=len(sheets[k][1])))
+        vols.append(v)
+        bnd.append(b)
+    dev_v, dev_b = np.concatenate(vols), np.array(bnd, float)
+    seq_v, seq_b = oracle_ensemble("sequential", mcs)
+    assert same_volume_law(seq_v, dev_v), (seq_v.std(), dev_v.std())
+    assert within_band(dev_b, seq_b), (seq_b.mean(), seq_b.std(), dev_b.mean())
+
+
+def small_cord(n=SEEDS):
+    cfg = synthetic.campaign(per_size=n, sizes=(64,), fill=0.45)
+    cfg.update(necrotic_type=3, death_threshold=0.25, J=synthetic.contact_table(4, seed=2), dt=0.03,
+               o2_sink_by_type=(0.0, 0.03, 0.03, 0.0))
+    return cfg
+
+
+def per_history(grid, o2, volume, types, necrotic, level):
+    living = (volume > 0) & (types != necrotic)
+    living[0] = False
+    means = O.mean_per_cell(grid, o2, len(volume))
+    cells = np.flatnonzero(living)
+    return len(cells), float(means[cells].mean()), float((means[cells] < level).mean())
+
+
+def test_the_step_stays_inside_the_oracle_band():
+    cfg = small_cord()
+    S = cfg.pop("S")
+    d = tempfile.mkdtemp()
+    p = os.path.join(d, "n.toml")
+    open(p, "w").write(synthetic.network_toml(S, S))
+    net = cw.Network.load(p, cfg["target_volume"])
+    sim = cw.Simulation(net, **dict(cfg, seeds=[s + 50_000 for s in cfg["seeds"]]))
+    ora = [CpuHistory(dict(cfg, S=S), k) for k in range(SEEDS)]
+    for step in range(1, 31):
+        sim.step(1)
+        for h in ora:
+            h.step()
+        if step not in (5, 15, 30):
+            continue
+        dev, ref = [], []
+        lat = sim.lattice()
+        for k in range(SEEDS):
+            cells = lat.cells(hist=k)
+            dev.append(per_history(sim.grid(k), sim.field_values(0, k), cells["volume"], cells["type"], 3,
+                                   cfg["hypoxic_level"]))
+            h = ora[k]
+            ref.append(per_history(h.lat.grid, h.o2.values, h.lat.volume, h.lat.type, 3, cfg["hypoxic_level"]))
+        dev, ref = np.array(dev), np.array(ref)
+        for j, name in enumerate(("living", "mean oxygen", "hypoxic fraction")):
+            assert within_band(dev[:, j], ref[:, j]), (step, name, dev[:, j].mean(), ref[:, j].mean(),
+                                                        ref[:, j].std())
