@@ -212,7 +212,7 @@ struct cw_lattice_s {
     unsigned long long *claim = nullptr;  // 2 * ncells
     uint4 *plist = nullptr;               // 2 * plist_cap
     int64_t plist_cap = 0;
-    uint32_t *pctl = nullptr;             // 8 + nh
+    uint32_t *pctl = nullptr;             // 8 + 27 nh
     int pass_grid = 0;                    // blocks of the cooperative pass launch
     int build_plans();
 };

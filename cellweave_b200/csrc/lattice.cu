@@ -70,24 +70,33 @@ __device__ __forceinline__ int32_t kind_of(const int32_t *type_h, int64_t cap, i
     return type_h[id];
 }
 
-// von_neumann, cpm.rs:922-944: y-1, y+1, x-1, x+1, z-1, z+1, clipped.
-__device__ __forceinline__ int von_neumann(int4 dm, int x, int y, int z, int64_t i, int64_t *out) {
-    int64_t w = dm.x, slice = (int64_t)dm.x * dm.y;
-    int n = 0;
-    if (y > 0) out[n++] = i - w;
-    if (y + 1 < dm.y) out[n++] = i + w;
-    if (x > 0) out[n++] = i - 1;
-    if (x + 1 < dm.x) out[n++] = i + 1;
-    if (z > 0) out[n++] = i - slice;
-    if (z + 1 < dm.z) out[n++] = i + slice;
-    return n;
+// von_neumann, cpm.rs:922-944: y-1, y+1, x-1, x+1, z-1, z+1, clipped; as a
+// mask of the six directions in that order (bit k: direction k exists), so
+// that the neighbours live in registers.
+struct Vn {
+    unsigned mask;
+    int64_t w, slice;
+    __device__ __forceinline__ int count() const { return __popc(mask); }
+    __device__ __forceinline__ bool has(int k) const { return (mask >> k) & 1u; }
+    __device__ __forceinline__ int64_t step(int k) const {
+        return k == 0 ? -w : k == 1 ? w : k == 2 ? -1 : k == 3 ? 1 : k == 4 ? -slice : slice;
+    }
+    // the offset of the j-th existing neighbour (j < count)
+    __device__ __forceinline__ int64_t nth(int j) const { return step(__fns(mask, 0, j + 1)); }
+};
+__device__ __forceinline__ Vn vn_of(int4 dm, int x, int y, int z) {
+    Vn v;
+    v.w = dm.x;
+    v.slice = (int64_t)dm.x * dm.y;
+    v.mask = (y > 0 ? 1u : 0u) | (y + 1 < dm.y ? 2u : 0u) | (x > 0 ? 4u : 0u) | (x + 1 < dm.x ? 8u : 0u) |
+             (z > 0 ? 16u : 0u) | (z + 1 < dm.z ? 32u : 0u);
+    return v;
 }
 
 // contact_delta_h (cpm.rs:851-876) on history grid `g`; *num before the division.
-__device__ double contact_delta(const int32_t *__restrict__ g, int4 dm, int x, int y, int z, int32_t src,
+__device__ __forceinline__ double contact_delta(const int32_t *__restrict__ g, int4 dm, int x, int y, int z, int32_t src,
                                 int32_t dst, const int32_t *type_h, int64_t cap, const double *sJ, int K,
-                                const int8_t *reach, int nreach, double across, const int64_t *vn, int nvn,
-                                double *num) {
+                                const int8_t *reach, int nreach, double across, int64_t i, Vn vn, double *num) {
     int32_t ks = kind_of(type_h, cap, src), kd = kind_of(type_h, cap, dst);
     double dh = 0.0;
     if (nreach > 0) {
@@ -103,8 +112,10 @@ __device__ double contact_delta(const int32_t *__restrict__ g, int4 dm, int x, i
         *num = dh;
         return dh / across;
     }
-    for (int k = 0; k < nvn; ++k) {
-        int32_t nb = g[vn[k]];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        if (!vn.has(k)) continue;
+        int32_t nb = g[i + vn.step(k)];
         int32_t kn = kind_of(type_h, cap, nb);
         double ed = dst == nb ? 0.0 : sJ[kd * K + kn];
         double es = src == nb ? 0.0 : sJ[ks * K + kn];
@@ -131,14 +142,17 @@ __device__ __forceinline__ double volume_delta(const int32_t *vol, const int32_t
     return dh;
 }
 
-__device__ __forceinline__ void surface_change(const int32_t *g, const int64_t *vn, int nvn, int32_t src,
-                                               int32_t dst, int32_t &dsrc, int32_t &ddst) {
+__device__ __forceinline__ void surface_change(const int32_t *g, int64_t i, Vn vn, int32_t src, int32_t dst,
+                                               int32_t &dsrc, int32_t &ddst) {
     int eq_s = 0, eq_d = 0;
-    for (int k = 0; k < nvn; ++k) {
-        int32_t nb = g[vn[k]];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        if (!vn.has(k)) continue;
+        int32_t nb = g[i + vn.step(k)];
         eq_s += nb == src;
         eq_d += nb == dst;
     }
+    const int nvn = vn.count();
     dsrc = eq_s - (nvn - eq_s);
     ddst = (nvn - eq_d) - eq_d;
 }
@@ -160,9 +174,11 @@ __device__ __forceinline__ double surface_delta(const int32_t *surf, const int32
 }
 
 // The colour order of the current step for every history: a Fisher-Yates
-// shuffle driven by Philox(all-ones, step, 1, i); advances the step counter.
+// shuffle driven by Philox(all-ones, step, 1, i); with `pass_keys`, each
+// pass's priority key, word 0 of Philox(all-ones - 1, step, 2, colour);
+// advances the step counter.
 __global__ void k_colour_order(const uint2 *keys, int nh, int ncol, uint32_t *mcs_ctr, uint32_t *mcs_cur,
-                               int32_t *perm) {
+                               int32_t *perm, uint32_t *pass_keys) {
     // one block: every thread reads the counter before thread 0 advances it
     uint32_t m = *mcs_ctr;
     for (int h = threadIdx.x; h < nh; h += blockDim.x) {
@@ -175,6 +191,9 @@ __global__ void k_colour_order(const uint2 *keys, int nh, int ncol, uint32_t *mc
             int32_t t = p[i]; p[i] = p[j]; p[j] = t;
         }
         for (int i = 0; i < ncol; ++i) perm[h * ncol + i] = p[i];
+        if (pass_keys)
+            for (int i = 0; i < ncol; ++i)
+                pass_keys[h * ncol + i] = philox(0xFFFFFFFEu, m, 2u, (uint32_t)p[i], k.x, k.y).x;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -221,14 +240,17 @@ __device__ __forceinline__ uint32_t fmix32(uint32_t h) {
 }
 
 // Scratch of the passes: two claim words per cell (by round parity), two
-// lists of pending attempts, and control words.
+// lists of pending attempts (a segment of `seg` entries per block), and
+// control words.
 struct PassScratch {
     unsigned long long *claim[2];  // ncells each
     uint4 *list[2];                // (history, pixel, source id, copied id)
-    uint32_t *ctl;                 // CTL_* below, then a pass key per history
+    uint32_t seg;                  // entries per block segment
+    uint32_t *ctl;                 // CTL_* below, then the pass keys (history x pass)
 };
 enum { CTL_COUNT = 0, CTL_BAR = 3, CTL_GEN = 4, CTL_ERR = 5, CTL_ROUNDS = 6, CTL_KEYS = 8 };
 constexpr int MAX_ROUNDS = 256;
+constexpr int PLAN_SMEM = 1024;  // block plans of up to 1023 histories sit in shared memory
 constexpr unsigned long long BARRIER_NS = 2000000000ull;
 
 __device__ __forceinline__ uint64_t global_ns() {
@@ -239,7 +261,7 @@ __device__ __forceinline__ uint64_t global_ns() {
 
 // A barrier over the whole (co-resident, cooperatively launched) grid whose
 // wait gives up after BARRIER_NS; false then, on every thread of the block.
-__device__ bool grid_barrier(uint32_t *ctl, int *s_ok) {
+__device__ __forceinline__ bool grid_barrier(uint32_t *ctl, int *s_ok) {
     __syncthreads();
     if (threadIdx.x == 0) {
         volatile uint32_t *gen = ctl + CTL_GEN;
@@ -264,6 +286,17 @@ __device__ bool grid_barrier(uint32_t *ctl, int *s_ok) {
     return *s_ok != 0;
 }
 
+// Append `entry` (where `take`) to this block's segment of `list`, one
+// shared-memory atomic per warp; *s_n counts the segment's entries.
+__device__ __forceinline__ void seg_append(uint4 *list, uint32_t seg, uint32_t *s_n, bool take, uint4 entry) {
+    const int lane = threadIdx.x & 31;
+    const unsigned m = __ballot_sync(0xffffffffu, take);
+    uint32_t base = 0;
+    if (lane == 0 && m) base = atomicAdd(s_n, (uint32_t)__popc(m));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (take) list[(size_t)blockIdx.x * seg + base + __popc(m & ((1u << lane) - 1u))] = entry;
+}
+
 // One sublattice pass: one copy attempt at every pixel of this pass's colour
 // (the reference's try_flip, cpm.rs:797-838), the attempts ordered by a
 // per-pass priority and run as that sequence would run them.  The pixels of
@@ -274,33 +307,36 @@ __device__ bool grid_barrier(uint32_t *ctl, int *s_ok) {
 // each round an attempt holding the claim on all its cells runs against the
 // live records, the others claim again for the next round.  An attempt runs
 // only after every higher-priority attempt sharing a cell with it, which is
-// the sequence in decreasing priority, whatever the thread schedule.
+// the sequence in decreasing priority, whatever the thread schedule.  Each
+// block keeps the attempts it found in its own list segment; the blocks meet
+// at a grid barrier between rounds and count what is left in one word.
 __global__ void __launch_bounds__(T) k_cpm_pass(LatView L, Tables tabs, const int32_t *blk, int nh, int nvb,
                                                 const int32_t *perm, int pass, const uint32_t *mcs_cur,
                                                 PassScratch S) {
     __shared__ double sJ[64];
     __shared__ int8_t sreach[3 * 124];
-    __shared__ int s_h, s_ok;
-    __shared__ uint32_t s_key;
+    __shared__ int s_ok;
+    __shared__ uint32_t s_n[2];
+    __shared__ int32_t s_blk[PLAN_SMEM];
     for (int i = threadIdx.x; i < L.K * L.K; i += blockDim.x) sJ[i] = tabs.J[i];
     for (int i = threadIdx.x; i < 3 * L.nreach; i += blockDim.x) sreach[i] = tabs.reach[i];
+    // the block plan in shared memory when it fits (every thread walks it)
+    const bool plan_shared = nh + 1 <= PLAN_SMEM;
+    if (plan_shared)
+        for (int i = threadIdx.x; i <= nh; i += blockDim.x) s_blk[i] = blk[i];
+    if (threadIdx.x == 0) s_n[0] = s_n[1] = 0u;
+    __syncthreads();
+    const int32_t *plan = plan_shared ? s_blk : blk;
     const uint32_t mcs = *mcs_cur;
-    const int lane = threadIdx.x & 31;
-    // ---- propose and claim (round 1's claims)
+    const uint32_t *pass_key = S.ctl + CTL_KEYS;
+    // ---- propose and claim (round 1's claims); a block's chunks come in
+    // increasing order, so its history only moves forward
+    int h = blockIdx.x < nvb ? plan_history(blk, nh, blockIdx.x) : 0;  // (global: it reads through __ldg)
     for (int vb = blockIdx.x; vb < nvb; vb += gridDim.x) {
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            const int h = plan_history(blk, nh, vb);
-            const uint2 key = L.keys[h];
-            s_h = h;
-            s_key = philox(0xFFFFFFFEu, mcs, 2u, (uint32_t)perm[h * L.ncol + pass], key.x, key.y).x;
-            if (vb == blk[h]) S.ctl[CTL_KEYS + h] = s_key;
-        }
-        __syncthreads();
-        const int h = s_h;
+        while (h + 1 < nh && plan[h + 1] <= vb) ++h;
         const int4 dm = L.dims[h];
         const int colour = perm[h * L.ncol + pass];
-        const uint32_t k = (uint32_t)(vb - blk[h]) * blockDim.x + threadIdx.x;
+        const uint32_t k = (uint32_t)(vb - plan[h]) * blockDim.x + threadIdx.x;
         const int64_t c0 = L.cell_off[h];
         const int32_t *g = L.grid + L.off[h];
         int x = 0, y = 0, z = 0;
@@ -308,63 +344,63 @@ __global__ void __launch_bounds__(T) k_cpm_pass(LatView L, Tables tabs, const in
         uint4 entry = make_uint4(0, 0, 0, 0);
         if (colour_site(dm, L.period, colour, k, x, y, z)) {
             const int64_t i = ((int64_t)z * dm.y + y) * dm.x + x;
-            int64_t vn[6];
-            const int nvn = von_neumann(dm, x, y, z, i, vn);
+            const Vn vn = vn_of(dm, x, y, z);
+            const int nvn = vn.count();
             if (nvn > 0) {
                 const uint2 key = L.keys[h];
                 const uint4 r = philox((uint32_t)i, mcs, 0u, 0u, key.x, key.y);
                 const int32_t src = g[i];
-                const int32_t dst = g[vn[((uint64_t)r.x * (uint64_t)nvn) >> 32]];
+                const int32_t dst = g[i + vn.nth((int)(((uint64_t)r.x * (uint64_t)nvn) >> 32))];
                 if (src != dst && src != OBST && dst != OBST) {
                     copies = true;
-                    const unsigned long long claim = (1ull << 32) | fmix32((uint32_t)i ^ s_key);
+                    const uint32_t prio = fmix32((uint32_t)i ^ pass_key[h * L.ncol + pass]);
+                    const unsigned long long claim = (1ull << 32) | prio;
                     if (src > 0) atomicMax(S.claim[1] + c0 + src, claim);
                     if (dst > 0) atomicMax(S.claim[1] + c0 + dst, claim);
                     entry = make_uint4((uint32_t)h, (uint32_t)i, (uint32_t)src, (uint32_t)dst);
                 }
             }
         }
-        // append, one atomic per warp
-        const unsigned m = __ballot_sync(0xffffffffu, copies);
-        uint32_t base = 0;
-        if (lane == 0 && m) base = atomicAdd(S.ctl + CTL_COUNT + 0, (uint32_t)__popc(m));
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (copies) S.list[0][base + __popc(m & ((1u << lane) - 1u))] = entry;
+        seg_append(S.list[0], S.seg, &s_n[0], copies, entry);
     }
+    __syncthreads();
+    if (threadIdx.x == 0 && s_n[0]) atomicAdd(S.ctl + CTL_COUNT + 0, s_n[0]);
     if (!grid_barrier(S.ctl, &s_ok)) {
         if (threadIdx.x == 0) atomicExch(S.ctl + CTL_ERR, 1u);
         return;
     }
     // ---- rounds
     for (int r = 1;; ++r) {
-        const uint32_t n_in = *(volatile uint32_t *)(S.ctl + CTL_COUNT + (r - 1) % 3);
-        if (n_in == 0) break;
+        const uint32_t left = *(volatile uint32_t *)(S.ctl + CTL_COUNT + (r - 1) % 3);
+        if (left == 0) break;
         if (r > MAX_ROUNDS) {
             if (blockIdx.x == 0 && threadIdx.x == 0) atomicExch(S.ctl + CTL_ERR, 2u);
             break;
         }
         if (blockIdx.x == 0 && threadIdx.x == 0) {
-            S.ctl[CTL_COUNT + (r + 1) % 3] = 0u;  // the output of round r + 1; last read as round r - 1's input
+            S.ctl[CTL_COUNT + (r + 1) % 3] = 0u;  // round r + 1's count; last read as round r - 1's
             atomicMax(S.ctl + CTL_ROUNDS, (uint32_t)r);
         }
-        const uint4 *in = S.list[(r - 1) & 1];
-        uint4 *out = S.list[r & 1];
+        const uint32_t mine_n = s_n[(r - 1) & 1];
+        __syncthreads();  // every thread has read its count before it is reset
+        if (threadIdx.x == 0) s_n[r & 1] = 0u;
+        __syncthreads();
+        const uint4 *in = S.list[(r - 1) & 1] + (size_t)blockIdx.x * S.seg;
         const unsigned long long *mine = S.claim[r & 1];
         unsigned long long *next = S.claim[(r + 1) & 1];
-        const uint32_t stride = gridDim.x * blockDim.x;
-        for (uint32_t e0 = blockIdx.x * blockDim.x; e0 < n_in; e0 += stride) {
+        for (uint32_t e0 = 0; e0 < mine_n; e0 += blockDim.x) {
             const uint32_t e = e0 + threadIdx.x;
             bool again = false, accept = false;
             uint4 en = make_uint4(0, 0, 0, 0);
             int32_t src = 0, dst = 0, dsrc = 0, ddst = 0;
             int64_t c0 = 0;
-            if (e < n_in) {
+            if (e < mine_n) {
                 en = in[e];
                 const int h = (int)en.x;
                 src = (int32_t)en.z;
                 dst = (int32_t)en.w;
                 c0 = L.cell_off[h];
-                const uint32_t prio = fmix32(en.y ^ S.ctl[CTL_KEYS + h]);
+                const uint32_t prio = fmix32(en.y ^ pass_key[h * L.ncol + pass]);
                 const unsigned long long key = ((unsigned long long)r << 32) | prio;
                 const bool win = (src <= 0 || mine[c0 + src] == key) && (dst <= 0 || mine[c0 + dst] == key);
                 if (win) {
@@ -374,16 +410,15 @@ __global__ void __launch_bounds__(T) k_cpm_pass(LatView L, Tables tabs, const in
                     const int z = (int)(i / ((int64_t)dm.x * dm.y));
                     int32_t *g = L.grid + L.off[h];
                     const int64_t cap = L.cell_off[h + 1] - c0;
-                    int64_t vn[6];
-                    const int nvn = von_neumann(dm, x, y, z, i, vn);
+                    const Vn vn = vn_of(dm, x, y, z);
                     const uint2 kk = L.keys[h];
                     const uint4 rr = philox((uint32_t)i, mcs, 0u, 0u, kk.x, kk.y);
                     double num;
                     double delta = contact_delta(g, dm, x, y, z, src, dst, L.type + c0, cap, sJ, L.K, sreach,
-                                                 L.nreach, L.across, vn, nvn, &num) +
+                                                 L.nreach, L.across, i, vn, &num) +
                                    volume_delta(L.volume, L.target, L.lambda, c0, src, dst);
                     if (L.surface_on) {
-                        surface_change(g, vn, nvn, src, dst, dsrc, ddst);
+                        surface_change(g, i, vn, src, dst, dsrc, ddst);
                         delta += surface_delta(L.surface, L.tsurf, L.lsurf, c0, src, dst, dsrc, ddst);
                     }
                     accept = delta <= 0.0;
@@ -405,12 +440,10 @@ __global__ void __launch_bounds__(T) k_cpm_pass(LatView L, Tables tabs, const in
                     if (dst > 0) L.surface[c0 + dst] += ddst;
                 }
             }
-            const unsigned m = __ballot_sync(0xffffffffu, again);
-            uint32_t base = 0;
-            if (lane == 0 && m) base = atomicAdd(S.ctl + CTL_COUNT + r % 3, (uint32_t)__popc(m));
-            base = __shfl_sync(0xffffffffu, base, 0);
-            if (again) out[base + __popc(m & ((1u << lane) - 1u))] = en;
+            seg_append(S.list[r & 1], S.seg, &s_n[r & 1], again, en);
         }
+        __syncthreads();
+        if (threadIdx.x == 0 && s_n[r & 1]) atomicAdd(S.ctl + CTL_COUNT + r % 3, s_n[r & 1]);
         if (!grid_barrier(S.ctl, &s_ok)) {
             if (threadIdx.x == 0) atomicExch(S.ctl + CTL_ERR, 1u);
             return;
@@ -432,17 +465,16 @@ __global__ void k_delta_h(LatView L, Tables tabs, int h, int64_t n, const int64_
     const int32_t *g = L.grid + L.off[h];
     int64_t i = site[q];
     int x = (int)(i % dm.x), y = (int)((i / dm.x) % dm.y), z = (int)(i / ((int64_t)dm.x * dm.y));
-    int64_t vn[6];
-    int nvn = von_neumann(dm, x, y, z, i, vn);
+    const Vn vn = vn_of(dm, x, y, z);
     int32_t src = g[i], dst = dstv[q];
     double num;
-    double c = contact_delta(g, dm, x, y, z, src, dst, L.type + c0, cap, sJ, L.K, sreach, L.nreach, L.across, vn,
-                             nvn, &num);
+    double c = contact_delta(g, dm, x, y, z, src, dst, L.type + c0, cap, sJ, L.K, sreach, L.nreach, L.across, i, vn,
+                             &num);
     double v = volume_delta(L.volume, L.target, L.lambda, c0, src, dst);
     double s = 0.0;
     if (L.surface_on) {
         int32_t ds, dd;
-        surface_change(g, vn, nvn, src, dst, ds, dd);
+        surface_change(g, i, vn, src, dst, ds, dd);
         s = surface_delta(L.surface, L.tsurf, L.lsurf, c0, src, dst, ds, dd);
     }
     double *o = out + 6 * q;
@@ -466,10 +498,11 @@ __global__ void k_recount(const int32_t *grid, const int4 *dims, const int64_t *
     if (surf && id > 0) {
         const int4 dm = dims[h];
         int x = (int)(local % dm.x), y = (int)((local / dm.x) % dm.y), z = (int)(local / ((int64_t)dm.x * dm.y));
-        int64_t vn[6];
-        int nvn = von_neumann(dm, x, y, z, local, vn);
+        const Vn vn = vn_of(dm, x, y, z);
         int c = 0;
-        for (int k = 0; k < nvn; ++k) c += g[vn[k]] != id;
+#pragma unroll
+        for (int k = 0; k < 6; ++k)
+            if (vn.has(k)) c += g[local + vn.step(k)] != id;
         if (c) atomicAdd(surf + cell_off[h] + id, c);
     }
 }
@@ -527,7 +560,6 @@ int cw_lattice_s::build_plans() {
     for (auto &p : plans) p.release();
     plans.assign(1, Plan());
     std::vector<int64_t> per(g.nh, 0);
-    int64_t cap = 0;
     for (uint32_t k = 0; k < g.nh; ++k) {
         if (period == 0) {
             per[k] = (int64_t)((g.w[k] + 1) / 2) * g.h[k] * g.d[k];
@@ -536,27 +568,29 @@ int cw_lattice_s::build_plans() {
             int64_t nz = volume ? (g.d[k] + period - 1) / period : 1;
             per[k] = nx * ny * nz;  // the largest colour class
         }
-        cap += per[k];
     }
     int rc = plans[0].build(per, T);
     if (rc != CW_OK) return rc;
-    // the pass scratch: a pending list holds at most every pixel of a colour
-    if (cap > plist_cap) {
-        dfree(plist);
-        if ((rc = dalloc(&plist, 2 * (size_t)cap)) != CW_OK) return rc;
-        plist_cap = cap;
-    }
-    if (!claim && (rc = dalloc(&claim, 2 * (size_t)ncells)) != CW_OK) return rc;
-    if (!pctl) {
-        if ((rc = dalloc(&pctl, 8 + (size_t)g.nh)) != CW_OK) return rc;
-        CW_CUDA(cudaMemsetAsync(pctl, 0, sizeof(uint32_t) * (8 + (size_t)g.nh), stream()));
-    }
     if (pass_grid == 0) {
         int per_sm = 0, dev = 0, nsm = 0;
         CW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)k_cpm_pass, T, 0));
         CW_CUDA(cudaGetDevice(&dev));
         CW_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
         pass_grid = std::max(1, per_sm * nsm);
+    }
+    // the pass scratch: a block's list segment holds every pixel of the
+    // colour it visits, (blocks of the plan / blocks launched, rounded up) x T
+    const int grid = std::min(plans[0].nblocks, pass_grid);
+    const int64_t need = (int64_t)grid * ((plans[0].nblocks + grid - 1) / grid) * T;
+    if (need > plist_cap) {
+        dfree(plist);
+        if ((rc = dalloc(&plist, 2 * (size_t)need)) != CW_OK) return rc;
+        plist_cap = need;
+    }
+    if (!claim && (rc = dalloc(&claim, 2 * (size_t)ncells)) != CW_OK) return rc;
+    if (!pctl) {
+        if ((rc = dalloc(&pctl, 8 + 27 * (size_t)g.nh)) != CW_OK) return rc;
+        CW_CUDA(cudaMemsetAsync(pctl, 0, sizeof(uint32_t) * (8 + 27 * (size_t)g.nh), stream()));
     }
     return CW_OK;
 }
@@ -619,7 +653,8 @@ int lattice_recount(cw_lattice_s *l, int32_t *vol_out, int32_t *surf_out) {
 // grid barrier), the claims and control words cleared before each.
 int lattice_sweep(cw_lattice_s *l) {
     LatDevice d = dev_of(l);
-    k_colour_order<<<1, 128, 0, stream()>>>(l->d_keys, l->g.nh, l->ncol, d.mcs, d.mcs + 1, d.perm);
+    k_colour_order<<<1, 128, 0, stream()>>>(l->d_keys, l->g.nh, l->ncol, d.mcs, d.mcs + 1, d.perm,
+                                            l->pctl + CTL_KEYS);
     CW_LAUNCHED();
     LatView v = lat_view(l);
     Tables t = lat_tables(l);
@@ -631,6 +666,7 @@ int lattice_sweep(cw_lattice_s *l) {
     S.ctl = l->pctl;
     int nvb = l->plans[0].nblocks;
     const int grid = std::min(nvb, l->pass_grid);
+    S.seg = (uint32_t)((nvb + grid - 1) / grid) * T;
     const int32_t *blk = l->plans[0].d_blk;
     int nh = (int)l->g.nh;
     const uint32_t *cur = d.mcs + 1;
