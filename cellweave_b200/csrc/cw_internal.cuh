@@ -210,9 +210,9 @@ struct cw_lattice_s {
     int32_t *d_flag = nullptr;       // scratch flag / counters
     // scratch of the sublattice passes (lattice.cu): claims, pending lists, control words
     unsigned long long *claim = nullptr;  // 2 * ncells
-    uint4 *plist = nullptr;               // 2 * plist_cap
+    uint4 *plist = nullptr;               // 2 * plist_cap attempts of 3 uint4 (lattice.cu)
     int64_t plist_cap = 0;
-    uint32_t *pctl = nullptr;             // 8 + 27 nh
+    uint32_t *pctl = nullptr;             // control words, then 27 pass keys per history (lattice.cu)
     int pass_grid = 0;                    // blocks of the cooperative pass launch
     int build_plans();
 };

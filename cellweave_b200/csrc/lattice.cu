@@ -239,16 +239,34 @@ __device__ __forceinline__ uint32_t fmix32(uint32_t h) {
     return h;
 }
 
+// One copy attempt of a pass, with everything about it that the pass cannot
+// change: the pixels of a colour lie outside one another's reach, so the
+// contact term, the surface counts' changes and the draws are fixed when the
+// pass starts; only the volume and surface records move.
+struct __align__(16) Attempt {
+    uint32_t hz, xy;   // history | z << 16, x | y << 16
+    int32_t src, dst;  // source and copied ids
+    uint32_t prio;     // the pass priority
+    int32_t dsurf;     // surface changes of source and copied cell (int16 each)
+    uint32_t u0, u1;   // the acceptance draw's words
+    double contact;    // contact Delta-H (cpm.rs:851-876)
+    double pad;
+};
+static_assert(sizeof(Attempt) == 48, "an attempt is three 16-byte words");
+
 // Scratch of the passes: two claim words per cell (by round parity), two
 // lists of pending attempts (a segment of `seg` entries per block), and
 // control words.
 struct PassScratch {
     unsigned long long *claim[2];  // ncells each
-    uint4 *list[2];                // (history, pixel, source id, copied id)
+    Attempt *list[2];
     uint32_t seg;                  // entries per block segment
     uint32_t *ctl;                 // CTL_* below, then the pass keys (history x pass)
 };
-enum { CTL_COUNT = 0, CTL_BAR = 3, CTL_GEN = 4, CTL_ERR = 5, CTL_ROUNDS = 6, CTL_KEYS = 8 };
+// control words: list counts and the barrier's arrivals (cleared before each
+// pass) share a line; the barrier's generation (only ever compared with
+// itself) another; the error and round records a third; then the pass keys
+enum { CTL_COUNT = 0, CTL_BAR = 3, CTL_GEN = 32, CTL_ERR = 48, CTL_ROUNDS = 49, CTL_KEYS = 64 };
 constexpr int MAX_ROUNDS = 256;
 constexpr int PLAN_SMEM = 1024;  // block plans of up to 1023 histories sit in shared memory
 constexpr unsigned long long BARRIER_NS = 2000000000ull;
@@ -259,13 +277,18 @@ __device__ __forceinline__ uint64_t global_ns() {
     return t;
 }
 
+__device__ __forceinline__ uint32_t ld_acquire_gpu(const uint32_t *p) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
 // A barrier over the whole (co-resident, cooperatively launched) grid whose
 // wait gives up after BARRIER_NS; false then, on every thread of the block.
 __device__ __forceinline__ bool grid_barrier(uint32_t *ctl, int *s_ok) {
     __syncthreads();
     if (threadIdx.x == 0) {
-        volatile uint32_t *gen = ctl + CTL_GEN;
-        const uint32_t g0 = *gen;
+        const uint32_t g0 = ld_acquire_gpu(ctl + CTL_GEN);
         int ok = 1;
         __threadfence();
         if (atomicAdd(ctl + CTL_BAR, 1u) == gridDim.x - 1) {
@@ -273,10 +296,14 @@ __device__ __forceinline__ bool grid_barrier(uint32_t *ctl, int *s_ok) {
             __threadfence();
             atomicAdd(ctl + CTL_GEN, 1u);
         } else {
-            const uint64_t t0 = global_ns();
-            while (*gen == g0) {
-                if (global_ns() - t0 > BARRIER_NS) { ok = 0; break; }
-                __nanosleep(64);
+            uint32_t spins = 0;
+            uint64_t t0 = 0;
+            while (ld_acquire_gpu(ctl + CTL_GEN) == g0) {
+                if ((++spins & 1023u) == 0) {  // the clock only now and then
+                    const uint64_t t = global_ns();
+                    if (t0 == 0) t0 = t;
+                    else if (t - t0 > BARRIER_NS) { ok = 0; break; }
+                }
             }
         }
         __threadfence();
@@ -286,15 +313,16 @@ __device__ __forceinline__ bool grid_barrier(uint32_t *ctl, int *s_ok) {
     return *s_ok != 0;
 }
 
-// Append `entry` (where `take`) to this block's segment of `list`, one
+// Append `a` (where `take`) to this block's segment of `list`, one
 // shared-memory atomic per warp; *s_n counts the segment's entries.
-__device__ __forceinline__ void seg_append(uint4 *list, uint32_t seg, uint32_t *s_n, bool take, uint4 entry) {
+__device__ __forceinline__ void seg_append(Attempt *list, uint32_t seg, uint32_t *s_n, bool take,
+                                           const Attempt &a) {
     const int lane = threadIdx.x & 31;
     const unsigned m = __ballot_sync(0xffffffffu, take);
     uint32_t base = 0;
     if (lane == 0 && m) base = atomicAdd(s_n, (uint32_t)__popc(m));
     base = __shfl_sync(0xffffffffu, base, 0);
-    if (take) list[(size_t)blockIdx.x * seg + base + __popc(m & ((1u << lane) - 1u))] = entry;
+    if (take) list[(size_t)blockIdx.x * seg + base + __popc(m & ((1u << lane) - 1u))] = a;
 }
 
 // One sublattice pass: one copy attempt at every pixel of this pass's colour
@@ -303,13 +331,14 @@ __device__ __forceinline__ void seg_append(uint4 *list, uint32_t seg, uint32_t *
 // a colour lie outside one another's reach, so two attempts meet only
 // through the records of a cell they both involve (volume, surface).  First
 // every attempt that copies (source and copied ids differ, neither the
-// obstacle) claims its cells other than the medium with its priority; in
-// each round an attempt holding the claim on all its cells runs against the
-// live records, the others claim again for the next round.  An attempt runs
-// only after every higher-priority attempt sharing a cell with it, which is
-// the sequence in decreasing priority, whatever the thread schedule.  Each
-// block keeps the attempts it found in its own list segment; the blocks meet
-// at a grid barrier between rounds and count what is left in one word.
+// obstacle) claims its cells other than the medium with its priority and
+// takes down what the pass cannot change; in each round an attempt holding
+// the claim on all its cells runs against the live records, the others claim
+// again for the next round.  An attempt runs only after every
+// higher-priority attempt sharing a cell with it, which is the sequence in
+// decreasing priority, whatever the thread schedule.  Each block keeps the
+// attempts it found in its own list segment; the blocks meet at a grid
+// barrier between rounds and count what is left in one word.
 __global__ void __launch_bounds__(T) k_cpm_pass(LatView L, Tables tabs, const int32_t *blk, int nh, int nvb,
                                                 const int32_t *perm, int pass, const uint32_t *mcs_cur,
                                                 PassScratch S) {
@@ -341,29 +370,63 @@ __global__ void __launch_bounds__(T) k_cpm_pass(LatView L, Tables tabs, const in
         const int32_t *g = L.grid + L.off[h];
         int x = 0, y = 0, z = 0;
         bool copies = false;
-        uint4 entry = make_uint4(0, 0, 0, 0);
+        Attempt a;
         if (colour_site(dm, L.period, colour, k, x, y, z)) {
             const int64_t i = ((int64_t)z * dm.y + y) * dm.x + x;
             const Vn vn = vn_of(dm, x, y, z);
             const int nvn = vn.count();
-            if (nvn > 0) {
+            const int32_t src = nvn > 0 ? g[i] : 0;
+            // a pixel whose neighbours all hold its own id cannot copy: no draw needed
+            bool edge = false;
+#pragma unroll
+            for (int q = 0; q < 6; ++q)
+                if (vn.has(q)) edge = edge || g[i + vn.step(q)] != src;
+            if (edge && src != OBST) {
                 const uint2 key = L.keys[h];
                 const uint4 r = philox((uint32_t)i, mcs, 0u, 0u, key.x, key.y);
-                const int32_t src = g[i];
                 const int32_t dst = g[i + vn.nth((int)(((uint64_t)r.x * (uint64_t)nvn) >> 32))];
-                if (src != dst && src != OBST && dst != OBST) {
+                if (src != dst && dst != OBST) {
                     copies = true;
                     const uint32_t prio = fmix32((uint32_t)i ^ pass_key[h * L.ncol + pass]);
                     const unsigned long long claim = (1ull << 32) | prio;
                     if (src > 0) atomicMax(S.claim[1] + c0 + src, claim);
                     if (dst > 0) atomicMax(S.claim[1] + c0 + dst, claim);
-                    entry = make_uint4((uint32_t)h, (uint32_t)i, (uint32_t)src, (uint32_t)dst);
+                    a.hz = (uint32_t)h | ((uint32_t)z << 16);
+                    a.xy = (uint32_t)x | ((uint32_t)y << 16);
+                    a.src = src;
+                    a.dst = dst;
+                    a.prio = prio;
+                    a.u0 = r.y;
+                    a.u1 = r.z;
                 }
             }
         }
-        seg_append(S.list[0], S.seg, &s_n[0], copies, entry);
+        seg_append(S.list[0], S.seg, &s_n[0], copies, a);
     }
     __syncthreads();
+    // ---- what the pass cannot change, over the block's attempts packed
+    // together (a contact term reads no pixel of the colour, which only the
+    // rounds write)
+    {
+        Attempt *mine = S.list[0] + (size_t)blockIdx.x * S.seg;
+        const uint32_t n = s_n[0];
+        for (uint32_t e = threadIdx.x; e < n; e += blockDim.x) {
+            Attempt &a = mine[e];
+            const int h = (int)(a.hz & 0xFFFFu);
+            const int x = (int)(a.xy & 0xFFFFu), y = (int)(a.xy >> 16), z = (int)(a.hz >> 16);
+            const int4 dm = L.dims[h];
+            const int64_t c0 = L.cell_off[h], cap = L.cell_off[h + 1] - c0;
+            const int64_t i = ((int64_t)z * dm.y + y) * dm.x + x;
+            const int32_t *g = L.grid + L.off[h];
+            const Vn vn = vn_of(dm, x, y, z);
+            double num;
+            a.contact = contact_delta(g, dm, x, y, z, a.src, a.dst, L.type + c0, cap, sJ, L.K, sreach, L.nreach,
+                                      L.across, i, vn, &num);
+            int32_t ds = 0, dd = 0;
+            if (L.surface_on) surface_change(g, i, vn, a.src, a.dst, ds, dd);
+            a.dsurf = (int32_t)((uint32_t)(uint16_t)(int16_t)ds | ((uint32_t)(uint16_t)(int16_t)dd << 16));
+        }
+    }
     if (threadIdx.x == 0 && s_n[0]) atomicAdd(S.ctl + CTL_COUNT + 0, s_n[0]);
     if (!grid_barrier(S.ctl, &s_ok)) {
         if (threadIdx.x == 0) atomicExch(S.ctl + CTL_ERR, 1u);
@@ -385,62 +448,45 @@ __global__ void __launch_bounds__(T) k_cpm_pass(LatView L, Tables tabs, const in
         __syncthreads();  // every thread has read its count before it is reset
         if (threadIdx.x == 0) s_n[r & 1] = 0u;
         __syncthreads();
-        const uint4 *in = S.list[(r - 1) & 1] + (size_t)blockIdx.x * S.seg;
+        const Attempt *in = S.list[(r - 1) & 1] + (size_t)blockIdx.x * S.seg;
         const unsigned long long *mine = S.claim[r & 1];
         unsigned long long *next = S.claim[(r + 1) & 1];
         for (uint32_t e0 = 0; e0 < mine_n; e0 += blockDim.x) {
             const uint32_t e = e0 + threadIdx.x;
-            bool again = false, accept = false;
-            uint4 en = make_uint4(0, 0, 0, 0);
-            int32_t src = 0, dst = 0, dsrc = 0, ddst = 0;
-            int64_t c0 = 0;
+            bool again = false;
+            Attempt a;
             if (e < mine_n) {
-                en = in[e];
-                const int h = (int)en.x;
-                src = (int32_t)en.z;
-                dst = (int32_t)en.w;
-                c0 = L.cell_off[h];
-                const uint32_t prio = fmix32(en.y ^ pass_key[h * L.ncol + pass]);
-                const unsigned long long key = ((unsigned long long)r << 32) | prio;
-                const bool win = (src <= 0 || mine[c0 + src] == key) && (dst <= 0 || mine[c0 + dst] == key);
+                a = in[e];
+                const int h = (int)(a.hz & 0xFFFFu);
+                const int64_t c0 = L.cell_off[h];
+                const unsigned long long key = ((unsigned long long)r << 32) | a.prio;
+                const bool win = (a.src <= 0 || mine[c0 + a.src] == key) && (a.dst <= 0 || mine[c0 + a.dst] == key);
                 if (win) {
-                    const int4 dm = L.dims[h];
-                    const int64_t i = en.y;
-                    const int x = (int)(i % dm.x), y = (int)((i / dm.x) % dm.y);
-                    const int z = (int)(i / ((int64_t)dm.x * dm.y));
-                    int32_t *g = L.grid + L.off[h];
-                    const int64_t cap = L.cell_off[h + 1] - c0;
-                    const Vn vn = vn_of(dm, x, y, z);
-                    const uint2 kk = L.keys[h];
-                    const uint4 rr = philox((uint32_t)i, mcs, 0u, 0u, kk.x, kk.y);
-                    double num;
-                    double delta = contact_delta(g, dm, x, y, z, src, dst, L.type + c0, cap, sJ, L.K, sreach,
-                                                 L.nreach, L.across, i, vn, &num) +
-                                   volume_delta(L.volume, L.target, L.lambda, c0, src, dst);
-                    if (L.surface_on) {
-                        surface_change(g, i, vn, src, dst, dsrc, ddst);
-                        delta += surface_delta(L.surface, L.tsurf, L.lsurf, c0, src, dst, dsrc, ddst);
+                    const int32_t ds = (int32_t)(int16_t)(a.dsurf & 0xFFFF), dd = (int32_t)(int16_t)(a.dsurf >> 16);
+                    double delta = a.contact + volume_delta(L.volume, L.target, L.lambda, c0, a.src, a.dst);
+                    if (L.surface_on) delta += surface_delta(L.surface, L.tsurf, L.lsurf, c0, a.src, a.dst, ds, dd);
+                    bool accept = delta <= 0.0;
+                    if (!accept) accept = u01(a.u0, a.u1) < own_exp(-delta / L.temperature);
+                    if (accept) {
+                        const int4 dm = L.dims[h];
+                        const int x = (int)(a.xy & 0xFFFFu), y = (int)(a.xy >> 16), z = (int)(a.hz >> 16);
+                        L.grid[L.off[h] + ((int64_t)z * dm.y + y) * dm.x + x] = a.dst;
+                        // the records: its cells are its own this round
+                        if (a.src != 0) L.volume[c0 + a.src] -= 1;
+                        if (a.dst != 0) L.volume[c0 + a.dst] += 1;
+                        if (L.surface_on) {
+                            if (a.src > 0) L.surface[c0 + a.src] += ds;
+                            if (a.dst > 0) L.surface[c0 + a.dst] += dd;
+                        }
                     }
-                    accept = delta <= 0.0;
-                    if (!accept) accept = u01(rr.y, rr.z) < own_exp(-delta / L.temperature);
-                    if (accept) g[i] = dst;
                 } else {
-                    const unsigned long long claim = ((unsigned long long)(r + 1) << 32) | prio;
-                    if (src > 0) atomicMax(next + c0 + src, claim);
-                    if (dst > 0) atomicMax(next + c0 + dst, claim);
+                    const unsigned long long claim = ((unsigned long long)(r + 1) << 32) | a.prio;
+                    if (a.src > 0) atomicMax(next + c0 + a.src, claim);
+                    if (a.dst > 0) atomicMax(next + c0 + a.dst, claim);
                     again = true;
                 }
             }
-            // the records of an accepted copy: its cells are its own this round
-            if (accept) {
-                if (src != 0) L.volume[c0 + src] -= 1;
-                if (dst != 0) L.volume[c0 + dst] += 1;
-                if (L.surface_on) {
-                    if (src > 0) L.surface[c0 + src] += dsrc;
-                    if (dst > 0) L.surface[c0 + dst] += ddst;
-                }
-            }
-            seg_append(S.list[r & 1], S.seg, &s_n[r & 1], again, en);
+            seg_append(S.list[r & 1], S.seg, &s_n[r & 1], again, a);
         }
         __syncthreads();
         if (threadIdx.x == 0 && s_n[r & 1]) atomicAdd(S.ctl + CTL_COUNT + r % 3, s_n[r & 1]);
@@ -584,13 +630,13 @@ int cw_lattice_s::build_plans() {
     const int64_t need = (int64_t)grid * ((plans[0].nblocks + grid - 1) / grid) * T;
     if (need > plist_cap) {
         dfree(plist);
-        if ((rc = dalloc(&plist, 2 * (size_t)need)) != CW_OK) return rc;
+        if ((rc = dalloc(&plist, 2 * 3 * (size_t)need)) != CW_OK) return rc;  // an attempt is 3 uint4
         plist_cap = need;
     }
     if (!claim && (rc = dalloc(&claim, 2 * (size_t)ncells)) != CW_OK) return rc;
     if (!pctl) {
-        if ((rc = dalloc(&pctl, 8 + 27 * (size_t)g.nh)) != CW_OK) return rc;
-        CW_CUDA(cudaMemsetAsync(pctl, 0, sizeof(uint32_t) * (8 + 27 * (size_t)g.nh), stream()));
+        if ((rc = dalloc(&pctl, CTL_KEYS + 27 * (size_t)g.nh)) != CW_OK) return rc;
+        CW_CUDA(cudaMemsetAsync(pctl, 0, sizeof(uint32_t) * (CTL_KEYS + 27 * (size_t)g.nh), stream()));
     }
     return CW_OK;
 }
@@ -661,8 +707,8 @@ int lattice_sweep(cw_lattice_s *l) {
     PassScratch S;
     S.claim[0] = l->claim;
     S.claim[1] = l->claim + l->ncells;
-    S.list[0] = l->plist;
-    S.list[1] = l->plist + l->plist_cap;
+    S.list[0] = (Attempt *)l->plist;
+    S.list[1] = (Attempt *)l->plist + l->plist_cap;
     S.ctl = l->pctl;
     int nvb = l->plans[0].nblocks;
     const int grid = std::min(nvb, l->pass_grid);
@@ -672,8 +718,8 @@ int lattice_sweep(cw_lattice_s *l) {
     const uint32_t *cur = d.mcs + 1;
     for (int q = 0; q < l->ncol; ++q) {
         CW_CUDA(cudaMemsetAsync(l->claim, 0, sizeof(unsigned long long) * 2 * (size_t)l->ncells, stream()));
-        // the three list counters and the barrier's count and generation
-        CW_CUDA(cudaMemsetAsync(l->pctl + CTL_COUNT, 0, sizeof(uint32_t) * 5, stream()));
+        // the three list counts and the barrier's arrivals
+        CW_CUDA(cudaMemsetAsync(l->pctl + CTL_COUNT, 0, sizeof(uint32_t) * 4, stream()));
         void *args[] = {&v, &t, (void *)&blk, &nh, &nvb, &d.perm, &q, (void *)&cur, &S};
         cudaLaunchConfig_t cfg = {};
         cudaLaunchAttribute attr[1];
@@ -709,6 +755,7 @@ extern "C" {
 int cw_lattice_create(uint32_t nh, const uint32_t *w, const uint32_t *h, const uint32_t *d,
                       const uint32_t *cell_capacity, double temperature, cw_lattice *out) {
     *out = nullptr;
+    if (nh > 65535) return fail(CW_ERR_CONFIG, "a lattice batch holds at most 65535 histories");
     cw_lattice_s *l = new cw_lattice_s();
     int rc = l->g.init(nh, w, h, d);
     if (rc != CW_OK) { delete l; return rc; }
@@ -767,6 +814,14 @@ int cw_lattice_destroy(cw_lattice l) {
 int cw_lattice_capacity(cw_lattice l, uint32_t hist, uint32_t *cap) {
     if (hist >= l->g.nh) return fail(CW_ERR_NOT_FOUND, "no history " + std::to_string(hist));
     *cap = (uint32_t)(l->cell_off[hist + 1] - l->cell_off[hist]);
+    return CW_OK;
+}
+
+int cw_lattice_pass_rounds(cw_lattice l, uint32_t *rounds) {
+    uint32_t zero = 0;
+    CW_CUDA(cudaStreamSynchronize(stream()));
+    CW_CUDA(cudaMemcpy(rounds, l->pctl + CTL_ROUNDS, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    CW_CUDA(cudaMemcpy(l->pctl + CTL_ROUNDS, &zero, sizeof zero, cudaMemcpyHostToDevice));
     return CW_OK;
 }
 

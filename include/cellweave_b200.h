@@ -82,6 +82,10 @@ int cw_lattice_destroy(cw_lattice lat);
 int cw_lattice_count(cw_lattice lat, uint32_t *nh);
 /* The cell records history `hist` holds (its capacity, the medium's included). */
 int cw_lattice_capacity(cw_lattice lat, uint32_t hist, uint32_t *cap);
+/* The most rounds a sublattice pass needed since the last call (a pass runs
+ * its attempts that share no cell at once, the others in later rounds);
+ * resets the count.  A diagnostic; no counterpart in the reference. */
+int cw_lattice_pass_rounds(cw_lattice lat, uint32_t *rounds);
 /* ContactEnergy (cpm.rs:30-129) generalised to a K x K table over cell types
  * (K <= 8, symmetric, J[0] the medium-medium 0), and set_contact_order
  * (cpm.rs:274-301): 1 faces only, 2 and 3 the wider reach and its divisor. */
