@@ -129,6 +129,18 @@ constexpr int RES_ROWS = 4;
 // optionally writes the FP32 coefficients of the defect-correction solve's
 // SOR on A d = r, the relaxation factor folded in: omega r / den and
 // omega D / den (both 0 on held pixels), and zeroes the correction.
+// The FP32 coefficients of the defect-correction sweep at a free pixel:
+// b = omega r / den and a = omega D / den, scaled by q = omega / den formed
+// in FP32 (they feed FP32 sweeps; r itself is FP64).
+__device__ __forceinline__ void dc_coefficients(double om, double den, double r, double d, float &b, float &a) {
+    b = a = 0.0f;
+    if (den > 0.0) {
+        const float q = (float)om / (float)den;
+        b = q * (float)r;
+        a = q * (float)d;
+    }
+}
+
 __global__ void __launch_bounds__(256) k_residual64(FieldView fv, const int32_t *blk, int nh, RelaxState *st,
                                                     float *r32, float *inv32, float *dz, int skip_done) {
     __shared__ int s_h;
@@ -159,11 +171,7 @@ __global__ void __launch_bounds__(256) k_residual64(FieldView fv, const int32_t 
             double r = add_sources(fv, i, fv.d * sum) - den * cv;
             if (fv.floor && cv <= 0.0 && r < 0.0) r = 0.0;
             worst = fmax(worst, fabs(r));
-            if (den > 0.0) {
-                const double q = om / den;
-                r_out = (float)(q * r);
-                inv_out = (float)(q * fv.d);
-            }
+            dc_coefficients(om, den, r, fv.d, r_out, inv_out);
         }
         if (r32) r32[i] = r_out;
         if (inv32) inv32[i] = inv_out;
@@ -243,7 +251,9 @@ __global__ void __launch_bounds__(256) k_dc_update(FieldView fv, const int32_t *
             if (fl && ci <= 0.0 && r < 0.0) r = 0.0;
             worst = fabs(r);
             fv.c[i] = ci;
-            r32[i] = den > 0.0 ? (float)(st[h].omega / den * r) : 0.f;
+            float b32, a32;
+            dc_coefficients(st[h].omega, den, r, fv.d, b32, a32);
+            r32[i] = b32;
             dlt[i] = 0.f;
         }
     }
