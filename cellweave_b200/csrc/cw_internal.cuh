@@ -198,6 +198,7 @@ struct cw_lattice_s {
     double J[64] = {0};
     int32_t order = 1;
     double temperature = 10.0;
+    bool copy_moore = false;         // copies from any Chebyshev neighbour, not only across faces
     uint32_t mcs = 0;
     std::vector<uint64_t> seed;
     uint2 *d_keys = nullptr;         // Philox key per history

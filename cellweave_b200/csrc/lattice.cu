@@ -58,6 +58,7 @@ struct LatView {
     double across;
     double temperature;
     int32_t surface_on;
+    int32_t copy_moore;
 };
 
 struct Tables {
@@ -84,6 +85,35 @@ struct Vn {
     // the offset of the j-th existing neighbour (j < count)
     __device__ __forceinline__ int64_t nth(int j) const { return step(__fns(mask, 0, j + 1)); }
 };
+// The copy neighbourhood with Moore copies: every in-box pixel at Chebyshev
+// distance 1, bit k = (dz + 1) 9 + (dy + 1) 3 + (dx + 1) (the centre, 13, never
+// set), taken in that order (the oracle's or_copy_neighbours).
+struct Moore {
+    unsigned mask;
+    int64_t w, slice;
+    __device__ __forceinline__ int count() const { return __popc(mask); }
+    __device__ __forceinline__ int64_t step(int k) const {
+        return (int64_t)(k / 9 - 1) * slice + (int64_t)((k / 3) % 3 - 1) * w + (k % 3 - 1);
+    }
+    __device__ __forceinline__ int64_t nth(int j) const { return step(__fns(mask, 0, j + 1)); }
+};
+__device__ __forceinline__ Moore moore_of(int4 dm, int x, int y, int z) {
+    Moore m;
+    m.w = dm.x;
+    m.slice = (int64_t)dm.x * dm.y;
+    m.mask = 0u;
+    const int deep = dm.z > 1 ? 1 : 0;
+    for (int dz = -deep; dz <= deep; ++dz)
+        for (int dy = -1; dy <= 1; ++dy)
+            for (int dx = -1; dx <= 1; ++dx) {
+                if ((dx | dy | dz) == 0) continue;
+                if (x + dx < 0 || x + dx >= dm.x || y + dy < 0 || y + dy >= dm.y || z + dz < 0 || z + dz >= dm.z)
+                    continue;
+                m.mask |= 1u << ((dz + 1) * 9 + (dy + 1) * 3 + (dx + 1));
+            }
+    return m;
+}
+
 __device__ __forceinline__ Vn vn_of(int4 dm, int x, int y, int z) {
     Vn v;
     v.w = dm.x;
@@ -373,18 +403,28 @@ __global__ void __launch_bounds__(T) k_cpm_pass(LatView L, Tables tabs, const in
         Attempt a;
         if (colour_site(dm, L.period, colour, k, x, y, z)) {
             const int64_t i = ((int64_t)z * dm.y + y) * dm.x + x;
-            const Vn vn = vn_of(dm, x, y, z);
-            const int nvn = vn.count();
-            const int32_t src = nvn > 0 ? g[i] : 0;
-            // a pixel whose neighbours all hold its own id cannot copy: no draw needed
+            const int32_t src = g[i];
+            // a pixel whose copy neighbours all hold its own id cannot copy: no draw needed
             bool edge = false;
+            int nvn = 0;
+            Vn vn;
+            Moore mo;
+            if (!L.copy_moore) {
+                vn = vn_of(dm, x, y, z);
+                nvn = vn.count();
 #pragma unroll
-            for (int q = 0; q < 6; ++q)
-                if (vn.has(q)) edge = edge || g[i + vn.step(q)] != src;
+                for (int q = 0; q < 6; ++q)
+                    if (vn.has(q)) edge = edge || g[i + vn.step(q)] != src;
+            } else {
+                mo = moore_of(dm, x, y, z);
+                nvn = mo.count();
+                for (unsigned m = mo.mask; m; m &= m - 1u) edge = edge || g[i + mo.step(__ffs(m) - 1)] != src;
+            }
             if (edge && src != OBST) {
                 const uint2 key = L.keys[h];
                 const uint4 r = philox((uint32_t)i, mcs, 0u, 0u, key.x, key.y);
-                const int32_t dst = g[i + vn.nth((int)(((uint64_t)r.x * (uint64_t)nvn) >> 32))];
+                const int j = (int)(((uint64_t)r.x * (uint64_t)nvn) >> 32);
+                const int32_t dst = g[i + (L.copy_moore ? mo.nth(j) : vn.nth(j))];
                 if (src != dst && dst != OBST) {
                     copies = true;
                     const uint32_t prio = fmix32((uint32_t)i ^ pass_key[h * L.ncol + pass]);
@@ -594,9 +634,14 @@ int make_reach(int order, bool volume, int8_t *off, double *across) {
 int cw_lattice_s::build_plans() {
     bool volume = g.d[0] > 1;
     nreach = make_reach(order, volume, reach, &across);
-    if (nreach == 0) {
+    if (nreach == 0 && !copy_moore) {
         period = 0;
         ncol = 2;
+    } else if (nreach == 0) {
+        // face contact with diagonal copies: a copy's source must not be a
+        // pixel of the same colour, so the chessboard gives way to period 2
+        period = 2;
+        ncol = volume ? 8 : 4;
     } else {
         int r = 1;
         for (int k = 0; k < 3 * nreach; ++k) r = std::max(r, (int)std::abs(reach[k]));
@@ -654,7 +699,7 @@ static LatView lat_view(cw_lattice_s *l) {
     v.lambda = l->lambda; v.surface = l->surface; v.ssnap = l->ssnap; v.tsurf = l->tsurf; v.lsurf = l->lsurf;
     v.dims = l->g.d_dims; v.off = l->g.d_off; v.cell_off = l->d_cell_off; v.keys = l->d_keys;
     v.K = l->K; v.nreach = l->nreach; v.period = l->period; v.ncol = l->ncol; v.across = l->across;
-    v.temperature = l->temperature; v.surface_on = l->surface_on ? 1 : 0;
+    v.temperature = l->temperature; v.surface_on = l->surface_on ? 1 : 0; v.copy_moore = l->copy_moore ? 1 : 0;
     return v;
 }
 
@@ -840,6 +885,13 @@ int cw_lattice_set_contact(cw_lattice l, int32_t K, const double *J, int32_t ord
     std::memset(l->J, 0, sizeof l->J);
     std::memcpy(l->J, J, sizeof(double) * K * K);
     l->order = order < 1 ? 1 : order;
+    return l->build_plans();
+}
+
+int cw_lattice_set_copy_nbhd(cw_lattice l, int32_t nbhd) {
+    if (nbhd != CW_COPY_VON_NEUMANN && nbhd != CW_COPY_MOORE)
+        return fail(CW_ERR_CONFIG, "copy neighbourhood " + std::to_string(nbhd) + " is neither von Neumann nor Moore");
+    l->copy_moore = nbhd == CW_COPY_MOORE;
     return l->build_plans();
 }
 

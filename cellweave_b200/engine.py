@@ -24,6 +24,7 @@ OBSTACLE = -1
 FP64, FP32_DC = 0, 1
 WINDOW_AUTO, WINDOW_64 = 0, 1
 STOP_MAX_CHANGE, STOP_RESIDUAL = 0, 1
+COPY_VON_NEUMANN, COPY_MOORE = 0, 1
 VALUES, UPTAKE, PRODUCTION, LIN_SINK = 0, 1, 2, 3
 
 
@@ -248,6 +249,11 @@ class CpmLattice:
 
     def set_temperature(self, t):
         call("cw_lattice_set_temperature", self._h, float(t))
+
+    def set_copy_neighbourhood(self, moore: bool):
+        """Copies from a face neighbour (try_flip, cpm.rs:797-838; the default) or, with
+        moore=True, from any pixel at Chebyshev distance 1 (an extension)."""
+        call("cw_lattice_set_copy_nbhd", self._h, COPY_MOORE if moore else COPY_VON_NEUMANN)
 
     def upload(self, grid, hist=0):
         g = np.ascontiguousarray(grid, np.int32).reshape(-1)

@@ -91,6 +91,11 @@ int cw_lattice_pass_rounds(cw_lattice lat, uint32_t *rounds);
  * (cpm.rs:274-301): 1 faces only, 2 and 3 the wider reach and its divisor. */
 int cw_lattice_set_contact(cw_lattice lat, int32_t K, const double *J, int32_t order);
 int cw_lattice_set_temperature(cw_lattice lat, double temperature);
+/* Where a copy attempt takes its id from: CW_COPY_VON_NEUMANN, a face
+ * neighbour as try_flip does (cpm.rs:797-838, 922-944; the default), or
+ * CW_COPY_MOORE, any in-box pixel at Chebyshev distance 1 (an extension). */
+enum { CW_COPY_VON_NEUMANN = 0, CW_COPY_MOORE = 1 };
+int cw_lattice_set_copy_nbhd(cw_lattice lat, int32_t nbhd);
 /* The grid of history `hist`, w*h*d int32 in the reference's flat order. */
 int cw_lattice_upload(cw_lattice lat, uint32_t hist, const int32_t *grid);
 int cw_lattice_download(cw_lattice lat, uint32_t hist, int32_t *grid);

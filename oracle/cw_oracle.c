@@ -428,6 +428,8 @@ typedef struct {
     double *J;        /* K*K, row-major, symmetric, J[0] = 0 */
     int32_t order;    /* contact order, cpm.rs:274 */
     double temperature;
+    int32_t copy_moore; /* 0: copy from a face neighbour (cpm.rs:922-944); 1: from any of the
+                           8 (26) Chebyshev neighbours, an extension */
 } or_lattice;
 
 /* set_contact_order, cpm.rs:274-301.  Returns the offsets (x, y, z) and the
@@ -494,6 +496,25 @@ static inline int or_von_neumann(const or_lattice *l, int32_t x, int32_t y, int3
     if (x + 1 < l->w) out[n++] = i + 1;
     if (z > 0) out[n++] = i - slice;
     if (z + 1 < l->d) out[n++] = i + slice;
+    return n;
+}
+
+/* The pixels a copy may come from: the face neighbours of von_neumann, or
+ * with copy_moore every in-box pixel at Chebyshev distance 1, in the order
+ * dz, dy, dx = -1, 0, 1 (an extension; the reference copies across faces). */
+static inline int or_copy_neighbours(const or_lattice *l, int32_t x, int32_t y, int32_t z, int64_t *out) {
+    if (!l->copy_moore) return or_von_neumann(l, x, y, z, out);
+    int64_t w = l->w, slice = (int64_t)l->w * l->h, i = (int64_t)z * slice + (int64_t)y * w + x;
+    int n = 0;
+    int deep = l->d > 1 ? 1 : 0;
+    for (int dz = -deep; dz <= deep; ++dz)
+        for (int dy = -1; dy <= 1; ++dy)
+            for (int dx = -1; dx <= 1; ++dx) {
+                if (dx == 0 && dy == 0 && dz == 0) continue;
+                if (x + dx < 0 || x + dx >= l->w || y + dy < 0 || y + dy >= l->h || z + dz < 0 || z + dz >= l->d)
+                    continue;
+                out[n++] = i + dz * slice + dy * w + dx;
+            }
     return n;
 }
 
@@ -637,8 +658,8 @@ static void or_try_flip(or_lattice *l, const int32_t *reach, int nreach, double 
                         int32_t z, uint64_t *rng) {
     int64_t w = l->w, slice = (int64_t)l->w * l->h, site = (int64_t)z * slice + (int64_t)y * w + x;
     int32_t src = l->grid[site];
-    int64_t nbr[6];
-    int nn = or_von_neumann(l, x, y, z, nbr);
+    int64_t nbr[26];
+    int nn = or_copy_neighbours(l, x, y, z, nbr);
     if (nn == 0) return;
     int32_t dst = l->grid[nbr[or_range(rng, (uint64_t)nn)]];
     if (src == dst || src == OR_OBSTACLE || dst == OR_OBSTACLE) return;
@@ -693,14 +714,15 @@ void or_lattice_mcs_sequential(or_lattice *l, uint64_t seed, int32_t sweeps) {
 
 /* ---- the sublattice scheme the GPU runs, restated on the CPU ----------- */
 
-/* Colouring: with faces only, the chessboard (x+y+z) mod 2; otherwise a
- * period p = R+1 in every axis, R the Chebyshev radius of the contact reach,
- * so that no pixel of a colour lies within the reach of another. */
+/* Colouring: with faces only (contact and copy), the chessboard (x+y+z) mod
+ * 2; otherwise a period p = R+1 in every axis, R the Chebyshev radius of the
+ * contact reach (1 for face contact with Moore copy), so that no pixel of a
+ * colour lies within the reach, or the copy neighbourhood, of another. */
 int or_colouring(const or_lattice *l, int32_t *period) {
     int32_t reach[3 * OR_MAX_REACH];
     double across;
     int n = or_reach(l->order, l->d > 1, reach, &across);
-    if (n == 0) { *period = 0; return 2; }
+    if (n == 0 && !l->copy_moore) { *period = 0; return 2; }
     int32_t r = 1;
     for (int k = 0; k < 3 * n; ++k) {
         int32_t a = reach[k] < 0 ? -reach[k] : reach[k];
@@ -802,8 +824,8 @@ void or_lattice_mcs_checkerboard(or_lattice *l, uint32_t k0, uint32_t k1, uint32
             for (int64_t e = 0; e < m; ++e) {
                 int64_t site = order[e].site;
                 int32_t x = (int32_t)(site % w), y = (int32_t)((site / w) % l->h), z = (int32_t)(site / slice);
-                int64_t nbr[6];
-                int nn = or_von_neumann(l, x, y, z, nbr);
+                int64_t nbr[26];
+                int nn = or_copy_neighbours(l, x, y, z, nbr);
                 if (nn == 0) continue;
                 or_u32x4 r = or_philox((uint32_t)site, mcs, 0u, 0u, k0, k1);
                 int32_t src = l->grid[site];

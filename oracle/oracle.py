@@ -167,7 +167,7 @@ class _LatticeStruct(C.Structure):
                 ("ncells", C.c_int32), ("type", C.c_void_p), ("volume", C.c_void_p), ("target", C.c_void_p),
                 ("lambda_", C.c_void_p), ("surface", C.c_void_p), ("target_surface", C.c_void_p),
                 ("lambda_surface", C.c_void_p), ("K", C.c_int32), ("J", C.c_void_p), ("order", C.c_int32),
-                ("temperature", C.c_double)]
+                ("temperature", C.c_double), ("copy_moore", C.c_int32)]
 
 
 def reach(order: int, volume: bool):
@@ -200,6 +200,7 @@ class Lattice:
         self.J = self.J.reshape(-1).copy()
         self.order = int(order)
         self.temperature = float(temperature)
+        self.copy_moore = False  # copy across faces (cpm.rs:922-944); True: from any Chebyshev neighbour
 
     def enable_surface(self, target_surface, lambda_surface):
         self.target_surface = np.ascontiguousarray(target_surface, dtype=np.int32).copy()
@@ -213,7 +214,7 @@ class Lattice:
                               None if self.surface is None else _p(self.surface).value,
                               None if self.target_surface is None else _p(self.target_surface).value,
                               None if self.lambda_surface is None else _p(self.lambda_surface).value,
-                              self.K, _p(self.J).value, self.order, self.temperature)
+                              self.K, _p(self.J).value, self.order, self.temperature, int(self.copy_moore))
 
     def recount(self):
         s = self._struct()

@@ -46,16 +46,18 @@ def observables(grid2d, volumes):
     return np.asarray(volumes[1:]), boundary
 
 
-def oracle_ensemble(scheme, mcs):
+def oracle_ensemble(scheme, mcs, moore=False):
     """(pooled volumes, boundary per history) of SEEDS oracle histories after `mcs` steps.
 
     scheme: "sequential" (the reference's sweep), "sublattice" (the device's,
     restated) or "snapshot" (the sublattice sweep with the planted mistake of
-    one records snapshot per pass)."""
+    one records snapshot per pass); `moore`: copies from any Chebyshev
+    neighbour."""
     vols, bnd = [], []
     for k in range(SEEDS):
         grid, rec = sheet(k)
         lat = oracle_lattice(grid, rec)
+        lat.copy_moore = moore
         if scheme == "sequential":
             lat.mcs_sequential(7919 * k + 1, mcs)
         else:

@@ -23,3 +23,9 @@ def test_the_check_sees_a_records_snapshot_per_pass():
     seq_v, _ = oracle_ensemble("sequential", 60)
     snap_v, _ = oracle_ensemble("snapshot", 60)
     assert not same_volume_law(seq_v, snap_v), (seq_v.std(), snap_v.std())
+
+
+def test_moore_copies_keep_the_sequential_volume_distribution_too():
+    seq_v, _ = oracle_ensemble("sequential", 40, moore=True)
+    sub_v, _ = oracle_ensemble("sublattice", 40, moore=True)
+    assert same_volume_law(seq_v, sub_v), (seq_v.std(), sub_v.std())

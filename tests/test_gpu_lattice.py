@@ -124,6 +124,30 @@ def test_sweeps_are_bit_exact_in_a_volume_with_surfaces(order):
     assert g.records_match_grid()
 
 
+@pytest.mark.parametrize("order,volume", [(1, False), (2, False), (3, True)])
+def test_moore_copies_are_bit_exact_with_the_oracle(order, volume):
+    # copies from any Chebyshev neighbour (an extension; the reference copies
+    # across faces): face contact then needs period 2, not the chessboard
+    if volume:
+        grid, rec = ball_volume(18)
+        n = len(rec)
+        o, g = pair(grid, rec, J3, 20.0, order, 5, surface=(np.full(n, 60, np.int32), np.full(n, 0.2)))
+    else:
+        grid, rec = sheet(seed=order + 10, size=64, ncell=20)
+        o, g = pair(grid, rec, J3, 10.0, order, 0xBEEF)
+    o.copy_moore = True
+    g.set_copy_neighbourhood(True)
+    assert o.colouring() == ((8 if volume else 4), 2) or order > 1
+    seed = 5 if volume else 0xBEEF
+    o.mcs_checkerboard(seed, 0, 12)
+    g.monte_carlo_step(12)
+    np.testing.assert_array_equal(g.grid().reshape(-1), o.grid)
+    np.testing.assert_array_equal(g.cells()["volume"][1:], o.volume[1:])
+    if volume:
+        np.testing.assert_array_equal(g.surfaces(), o.surface)
+    assert g.records_match_grid()
+
+
 def test_a_batch_of_uneven_lattices_sweeps_each_as_alone():
     scenes = [sheet(seed=s, size=sz, ncell=nc) for s, sz, nc in [(1, 40, 6), (2, 64, 20), (3, 96, 30)]]
     seeds = [11, 22, 33]

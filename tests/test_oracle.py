@@ -492,3 +492,18 @@ def test_a_cell_in_the_middle_reads_less_oxygen_than_one_on_the_rim():
     inner, outer = o2[c], max(o2[r] for r in ring)
     assert inner < outer and inner < 0.9 and outer > inner + 0.05
     assert o2[0] == 0.0 and (o2[1:] > 0).all()
+
+
+def test_moore_copies_need_period_two_with_face_contact():
+    # with copies from diagonal neighbours a chessboard colour would hold a
+    # copy's source: face contact then takes period 2 (4 colours, 8 in a volume)
+    grid = np.zeros((1, 12, 12), np.int32)
+    lat = O.Lattice(grid, (12, 12, 1), 1, np.zeros((1, 1)), 10.0, 1)
+    assert lat.colouring() == (2, 0)
+    lat.copy_moore = True
+    assert lat.colouring() == (4, 2)
+    vol = O.Lattice(np.zeros((6, 6, 6), np.int32), (6, 6, 6), 1, np.zeros((1, 1)), 10.0, 1)
+    vol.copy_moore = True
+    assert vol.colouring() == (8, 2)
+    vol.order = 3  # the 26-neighbourhood: Chebyshev radius 1, period 2 either way
+    assert vol.colouring() == (8, 2)
