@@ -136,6 +136,7 @@ SIGNATURES = {
     "cw_field_inflow": (C.c_int, [P, P]),
     "cw_field_step": (C.c_int, [P, D]),
     "cw_field_relax_noalloc": (C.c_int, [P, P, P, P, P, U32, U32, D, D, D, D, D, I64, I32, P, P]),
+    "cw_field_relax_adjoint": (C.c_int, [P, P, P, P, P]),
     "cw_field_time_inner": (C.c_int, [P, I32, I32, I32, D, P, P]),
     "cw_field_inner_correction": (C.c_int, [P, U32, P]),
     "cw_couple_uptake": (C.c_int, [P, P, I32, P, I32]),
@@ -149,6 +150,7 @@ SIGNATURES = {
     "cw_network_destroy": (C.c_int, [P]),
     "cw_network_info": (C.c_int, [P, P, P, P]),
     "cw_network_step_batch": (C.c_int, [P, I64, P, P, D, I32]),
+    "cw_network_backward_batch": (C.c_int, [P, I64, P, P, D, I32, P, P, I32, P]),
     "cw_network_mechanics_batch": (C.c_int, [P, I64, P, P, P]),
     "cw_sim_create": (C.c_int, [P, P, P]),
     "cw_sim_destroy": (C.c_int, [P]),

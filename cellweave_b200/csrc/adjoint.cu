@@ -594,3 +594,64 @@ int cw_fit_gradient(cw_fit f, double *loss, double *grad) {
 }
 
 }  // extern "C"
+
+extern "C" int cw_network_backward_batch(cw_network net, int64_t ncells, const double *state, const double *inputs,
+                                         double dt, int32_t substeps, double *adjoint, double *d_oxygen,
+                                         int32_t nrates, double *d_rates) {
+    if (ncells < 0 || substeps < 1 || !(dt > 0.0))
+        return fail(CW_ERR_CONFIG, "a backward step needs cells >= 0, substeps >= 1 and dt > 0");
+    if (nrates < 0 || nrates > std::min(MAXTH, net->nterms))
+        return fail(CW_ERR_CONFIG, "rates to differentiate: 0 to " + std::to_string(std::min(MAXTH, net->nterms)));
+    if (ncells == 0) {
+        for (int32_t t = 0; t < nrates; ++t) d_rates[t] = 0.0;
+        return CW_OK;
+    }
+    const int64_t nc = ncells, S = net->S;
+    // cell-major host arrays to node-major device columns
+    std::vector<double> xs(S * nc), in(6 * nc), lam(S * nc);
+    for (int64_t c = 0; c < nc; ++c) {
+        for (int64_t i = 0; i < S; ++i) {
+            xs[i * nc + c] = state[c * S + i];
+            lam[i * nc + c] = adjoint[c * S + i];
+        }
+        for (int q = 0; q < 6; ++q) in[q * nc + c] = inputs[c * 6 + q];
+    }
+    double *d_x = nullptr, *d_in = nullptr, *d_seg = nullptr, *d_lam = nullptr, *d_gin = nullptr, *d_gth = nullptr;
+    auto release = [&]() { dfree(d_x); dfree(d_in); dfree(d_seg); dfree(d_lam); dfree(d_gin); dfree(d_gth); };
+    int rc;
+    if ((rc = dalloc(&d_x, S * nc)) || (rc = dalloc(&d_in, 6 * nc)) || (rc = dalloc(&d_seg, (substeps + 1) * S * nc)) ||
+        (rc = dalloc(&d_lam, S * nc)) || (rc = dalloc(&d_gin, nc)) || (rc = dalloc(&d_gth, MAXTH))) {
+        release();
+        return rc;
+    }
+    CW_CUDA(cudaMemcpyAsync(d_x, xs.data(), sizeof(double) * S * nc, cudaMemcpyHostToDevice, stream()));
+    CW_CUDA(cudaMemcpyAsync(d_in, in.data(), sizeof(double) * 6 * nc, cudaMemcpyHostToDevice, stream()));
+    CW_CUDA(cudaMemcpyAsync(d_lam, lam.data(), sizeof(double) * S * nc, cudaMemcpyHostToDevice, stream()));
+    CW_CUDA(cudaMemsetAsync(d_gin, 0, sizeof(double) * nc, stream()));
+    CW_CUDA(cudaMemsetAsync(d_gth, 0, sizeof(double) * MAXTH, stream()));
+    const size_t smem = sizeof(double) * (10 * S + MAXTH) * RB + net->nterms * (sizeof(int4) + sizeof(double4)) +
+                        sizeof(int32_t) * (S + 1);
+    if (smem > 48 * 1024 &&
+        cudaFuncSetAttribute(k_fit_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+        release();
+        return fail(CW_ERR_CONFIG, "the network is too large for the backward step's shared memory");
+    }
+    NetDev N{net->node_ptr, net->term, net->par, net->S, net->nterms};
+    k_fit_backward<<<(unsigned)((nc + RB - 1) / RB), RB, smem, stream()>>>(N, d_x, d_in, nc, substeps, dt, d_seg,
+                                                                          d_lam, d_gin, d_gth, nrates);
+    count_launch();
+    const cudaError_t le = cudaGetLastError();
+    if (le != cudaSuccess) { release(); return cuda_fail(le, "kernel launch"); }
+    std::vector<double> gin(nc), gth(MAXTH);
+    CW_CUDA(cudaMemcpyAsync(lam.data(), d_lam, sizeof(double) * S * nc, cudaMemcpyDeviceToHost, stream()));
+    CW_CUDA(cudaMemcpyAsync(gin.data(), d_gin, sizeof(double) * nc, cudaMemcpyDeviceToHost, stream()));
+    CW_CUDA(cudaMemcpyAsync(gth.data(), d_gth, sizeof(double) * MAXTH, cudaMemcpyDeviceToHost, stream()));
+    CW_CUDA(cudaStreamSynchronize(stream()));
+    release();
+    for (int64_t c = 0; c < nc; ++c)
+        for (int64_t i = 0; i < S; ++i) adjoint[c * S + i] = lam[i * nc + c];
+    if (d_oxygen)
+        for (int64_t c = 0; c < nc; ++c) d_oxygen[c] = gin[c];
+    for (int32_t t = 0; t < nrates; ++t) d_rates[t] = gth[t];
+    return CW_OK;
+}

@@ -237,6 +237,7 @@ struct cw_field_s {
     void *stats = nullptr;           // per-history solve state (device)
     cw::Span *d_span = nullptr;
     void *dc_cache = nullptr;        // plans and solver of the FP32 solve (field.cu)
+    cw_field_s *adjoint = nullptr;   // twin of cw_field_relax_adjoint, made on its first call
     int alloc_fp32();
 };
 

@@ -807,6 +807,7 @@ int cw_field_destroy(cw_field f) {
     }
     RelaxState *st = (RelaxState *)f->stats;
     dfree(st);
+    if (f->adjoint) cw_field_destroy(f->adjoint);
     f->g.release();
     delete f;
     return CW_OK;
@@ -917,6 +918,41 @@ int cw_field_hold_mask(cw_field f, uint32_t hist, const uint8_t *mask, double va
 
 int cw_field_relax(cw_field f, const cw_relax_opts *opts, cw_relax_stats *stats) {
     return cw::field_relax(f, opts, nullptr, stats);
+}
+
+// The operator restricted to the free pixels is symmetric (den_i on the
+// diagonal, -D between neighbours), so its adjoint solve is the same solver
+// on a twin with dl_dc as the source, zero on the held pixels and no floor.
+int cw_field_relax_adjoint(cw_field f, const double *dl_dc, double *lambda, const cw_relax_opts *opts,
+                           cw_relax_stats *stats) {
+    int rc;
+    cw_field_s *a = f->adjoint;
+    const int64_t n = f->g.total;
+    if (!a) {
+        std::vector<uint32_t> W(f->g.w.begin(), f->g.w.end()), H(f->g.h.begin(), f->g.h.end()),
+            D(f->g.d.begin(), f->g.d.end());
+        if ((rc = cw_field_create(f->g.nh, W.data(), H.data(), D.data(), f->dcoef, f->decay, 0.0, &a)) != CW_OK)
+            return rc;
+        f->adjoint = a;
+    }
+    a->dcoef = f->dcoef;
+    a->decay = f->decay;
+    a->source = 0.0;
+    a->floor = false;
+    CW_CUDA(cudaMemcpyAsync(a->held, f->held, (size_t)n, cudaMemcpyDeviceToDevice, stream()));
+    a->held_dirty = true;
+    CW_CUDA(cudaMemsetAsync(a->c, 0, sizeof(double) * n, stream()));
+    a->lin_sink_on = f->lin_sink_on;
+    if (f->lin_sink_on)
+        CW_CUDA(cudaMemcpyAsync(a->lin_sink, f->lin_sink, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream()));
+    a->uptake_on = false;
+    a->production_on = true;
+    CW_CUDA(cudaMemcpyAsync(a->production, dl_dc, sizeof(double) * n, cudaMemcpyHostToDevice, stream()));
+    rc = cw::field_relax(a, opts, nullptr, stats);
+    if (rc != CW_OK && rc != CW_ERR_SIMULATION) return rc;
+    CW_CUDA(cudaMemcpyAsync(lambda, a->c, sizeof(double) * n, cudaMemcpyDeviceToHost, stream()));
+    CW_CUDA(cudaStreamSynchronize(stream()));
+    return rc;
 }
 
 }  // extern "C"

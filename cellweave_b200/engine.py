@@ -165,6 +165,21 @@ class ScalarField:
             return result
         return result[0]["sweeps"] if len(result) == 1 else [r["sweeps"] for r in result]
 
+    def relax_adjoint(self, dl_dc, tolerance, max_sweeps, omega=None, stop=STOP_RESIDUAL, precision=FP64,
+                      inner_sweeps=0, block_depth=0, window=WINDOW_AUTO):
+        """lambda with A^T lambda = dl_dc for the field's operator as it stands (zero on held
+        pixels); dl_dc and the result hold every history's pixels, one after another."""
+        g = np.ascontiguousarray(dl_dc, np.float64).reshape(-1)
+        total = sum(w * h * d for w, h, d in self.dims)
+        if g.size != total:
+            raise ConfigError(f"expected {total} values, got {g.size}")
+        o = _lib.RelaxOpts(float(omega) if omega else 0.0, int(stop), float(tolerance), int(max_sweeps),
+                           int(precision), int(inner_sweeps), int(block_depth), int(window))
+        st = (_lib.RelaxStats * len(self.dims))()
+        lam = np.empty(total)
+        call("cw_field_relax_adjoint", self._h, ptr(g), ptr(lam), C.byref(o), st)
+        return lam
+
     def residual(self):
         out = np.empty(len(self.dims))
         call("cw_field_residual", self._h, ptr(out))
@@ -496,6 +511,19 @@ class Network:
         if st is not state:
             state[...] = st
         return state
+
+    def backward_batch(self, state, inputs, dt, substeps, adjoint, nrates=0):
+        """The adjoint of step_batch from `state` (the state before the steps): returns
+        (dL/d state before, dL/d oxygen input per cell, dL/d rate of the first nrates terms)
+        given `adjoint` = dL/d state after."""
+        st = np.ascontiguousarray(state, np.float64)
+        ins = np.ascontiguousarray(inputs, np.float64)
+        adj = np.array(adjoint, np.float64, order="C", copy=True)
+        d_o2 = np.zeros(st.shape[0])
+        d_rates = np.zeros(max(int(nrates), 1))
+        call("cw_network_backward_batch", self._h, st.shape[0], ptr(st), ptr(ins), float(dt), int(substeps), ptr(adj),
+             ptr(d_o2), int(nrates), ptr(d_rates))
+        return adj, d_o2, d_rates[:int(nrates)]
 
     def mechanics_batch(self, state):
         """mechanics (network.rs:811-821): target volumes and lambdas."""

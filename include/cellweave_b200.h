@@ -183,6 +183,16 @@ typedef struct {
 /* relax (pde.rs:245-288) on every history; stats has nh entries (may be
  * NULL).  Returns CW_ERR_SIMULATION when any history failed to settle. */
 int cw_field_relax(cw_field f, const cw_relax_opts *opts, cw_relax_stats *stats);
+/* The adjoint of the steady solve (no counterpart in the reference, which has
+ * no derivatives): lambda solves A^T lambda = dl_dc for the field's operator
+ * as it stands (diffusion, decay, first-order sink, held pixels), with
+ * lambda = 0 on held pixels; then dL/dtheta = -lambda . (dA/dtheta c -
+ * db/dtheta) for any coefficient theta.  dl_dc and lambda hold every
+ * history's pixels in the batch's flat order.  Exact where the forward
+ * solve's floor at zero does not bind.  Options and errors as cw_field_relax
+ * (lambda is written also when CW_ERR_SIMULATION reports it unsettled). */
+int cw_field_relax_adjoint(cw_field f, const double *dl_dc, double *lambda, const cw_relax_opts *opts,
+                           cw_relax_stats *stats);
 /* No counterpart in the reference: the FP32 defect-correction relax of one
  * flat field (width x height <= 1,048,576 pixels) that allocates no device
  * memory, for callers whose device memory belongs to another allocator (a
@@ -272,6 +282,16 @@ int cw_network_step_batch(cw_network net, int64_t ncells, double *state, const d
 /* mechanics (network.rs:811-821) of each cell: target volume and lambda. */
 int cw_network_mechanics_batch(cw_network net, int64_t ncells, const double *state, uint32_t *target,
                                double *lambda);
+/* The adjoint of cw_network_step_batch (no counterpart in the reference,
+ * which has no derivatives): for `substeps` RK4 steps from `state` ([ncells][S],
+ * the state before them) under `inputs` ([ncells][6]), `adjoint` ([ncells][S])
+ * holds dL/d(state after) on entry and dL/d(state before) on return; d_oxygen
+ * (ncells, or NULL) receives dL/d(oxygen input); d_rates the first `nrates`
+ * terms' dL/d(rate) summed over the cells (terms in compile order: node by
+ * node, each node's in file order; nrates <= 32).  The forward steps are
+ * recomputed; the clamp to [0, 1] passes no gradient where it binds. */
+int cw_network_backward_batch(cw_network net, int64_t ncells, const double *state, const double *inputs, double dt,
+                              int32_t substeps, double *adjoint, double *d_oxygen, int32_t nrates, double *d_rates);
 
 /* ------------------------------------------------------------------ simulation driver
  * A device-resident Simulation<Running>::step (simulation.rs:1129-1350)

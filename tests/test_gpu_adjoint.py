@@ -114,3 +114,91 @@ def test_gradient_descent_lowers_the_loss(problem):
         loss, grad = fit.gradient()
     assert loss < loss0
     fit.params = start
+
+
+def adjoint_field(dims, seed=3):
+    rng = np.random.default_rng(seed)
+    f = cw.ScalarField(dims, 0.7, 0.001, 0.0)
+    for k, (w, h, _) in enumerate(dims):
+        f.set_linear_sink(np.where(rng.random(w * h) < 0.6, 0.02, 0.0), k)
+        held = np.zeros(w * h, np.uint8)
+        held[:w] = 1
+        f.hold_where(1.0, held, k)
+    return f
+
+
+def test_field_adjoint_gives_the_derivative_of_a_linear_functional():
+    # J(s) = g . c(s), A c = b(s) with a source s m: dJ/ds = lambda . m
+    dims = [(48, 40, 1), (30, 30, 1)]
+    rng = np.random.default_rng(11)
+    m = [rng.random(w * h) for w, h, _ in dims]
+    g = np.concatenate([rng.random(w * h) for w, h, _ in dims])
+
+    def J(s):
+        f = adjoint_field(dims)
+        for k in range(len(dims)):
+            f.set_production_array(s * m[k], k)
+        f.relax(1e-13, 1_000_000, omega=1.8, stop=cw.STOP_RESIDUAL)
+        return float(np.concatenate([f.values(k) for k in range(len(dims))]) @ g)
+
+    f = adjoint_field(dims)
+    lam = f.relax_adjoint(g, 1e-13, 1_000_000, omega=1.8)
+    held = np.concatenate([f.held(k) for k in range(len(dims))]) == 1
+    assert np.all(lam[held] == 0.0)
+    s, h = 0.3, 1e-3  # J is linear in s: central differences are exact up to the solves' residual
+    fd = (J(s + h) - J(s - h)) / (2 * h)
+    assert abs(lam @ np.concatenate(m) - fd) <= 1e-8 * abs(fd)
+    # A is symmetric: g2 . lambda(g1) = g1 . lambda(g2), in either precision
+    g2 = np.concatenate([rng.random(w * h) for w, h, _ in dims])
+    for precision in (cw.FP64, cw.FP32_DC):
+        l1 = f.relax_adjoint(g, 1e-12, 1_000_000, omega=1.8, precision=precision)
+        l2 = f.relax_adjoint(g2, 1e-12, 1_000_000, omega=1.8, precision=precision)
+        assert abs(g2 @ l1 - g @ l2) <= 1e-9 * abs(g @ l2)
+
+
+def test_network_backward_matches_finite_differences():
+    S = 8
+    import tomllib
+    spec = tomllib.loads(synthetic.network_toml(S, seed=S))
+    net = cw.Network.from_spec(spec, 36)
+    rng = np.random.default_rng(5)
+    n, dt, sub = 40, 0.01, 8
+    st = rng.uniform(0.2, 0.8, (n, S))
+    ins = np.zeros((n, 6))
+    ins[:, 0] = rng.uniform(0.05, 0.95, n)
+    ins[:, 1] = 0.2
+    w = rng.normal(size=(n, S))
+
+    def L(state, inputs, network=net):
+        x = state.copy()
+        network.step_batch(x, inputs, dt, sub)
+        return float((w * x).sum())
+
+    nterms = sum(len(nd.get("terms", [])) for nd in spec["nodes"])
+    nr = min(nterms, 12)
+    adj, d_o2, d_rates = net.backward_batch(st, ins, dt, sub, w, nrates=nr)
+    h = 1e-6
+    for c, i in [(0, 0), (3, 5), (17, 2), (39, 7)]:
+        up, dn = st.copy(), st.copy()
+        up[c, i] += h
+        dn[c, i] -= h
+        fd = (L(up, ins) - L(dn, ins)) / (2 * h)
+        assert abs(adj[c, i] - fd) <= 1e-6 * max(abs(fd), 1e-3), (c, i, adj[c, i], fd)
+    for c in (1, 20):
+        up, dn = ins.copy(), ins.copy()
+        up[c, 0] += h
+        dn[c, 0] -= h
+        fd = (L(st, up) - L(st, dn)) / (2 * h)
+        assert abs(d_o2[c] - fd) <= 1e-6 * max(abs(fd), 1e-3), (c, d_o2[c], fd)
+    # rates: terms in compile order, node by node
+    where = [(a, b) for a, nd in enumerate(spec["nodes"]) for b in range(len(nd.get("terms", [])))]
+    for t in (0, 3, nr - 1):
+        a, b = where[t]
+        vals = []
+        for sgn in (1, -1):
+            sp = tomllib.loads(synthetic.network_toml(S, seed=S))
+            rate = sp["nodes"][a]["terms"][b]["rate"]
+            sp["nodes"][a]["terms"][b]["rate"] = rate + sgn * h * rate
+            vals.append(L(st, ins, cw.Network.from_spec(sp, 36)))
+        fd = (vals[0] - vals[1]) / (2 * h * spec["nodes"][a]["terms"][b]["rate"])
+        assert abs(d_rates[t] - fd) <= 1e-5 * max(abs(fd), 1e-3), (t, d_rates[t], fd)
