@@ -101,6 +101,8 @@ SIGNATURES = {
     "cw_lattice_destroy": (C.c_int, [P]),
     "cw_lattice_count": (C.c_int, [P, P]),
     "cw_lattice_set_copy_nbhd": (C.c_int, [P, I32]),
+    "cw_lattice_divide": (C.c_int, [P, U32, U32, P, P, P]),
+    "cw_lattice_cell_count": (C.c_int, [P, U32, P]),
     "cw_lattice_capacity": (C.c_int, [P, U32, P]),
     "cw_lattice_pass_rounds": (C.c_int, [P, P]),
     "cw_lattice_set_contact": (C.c_int, [P, I32, P, I32]),

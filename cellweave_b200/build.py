@@ -23,7 +23,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
                  "--expt-relaxed-constexpr", "-I", CSRC, "-I", INCLUDE, "-Xptxas", "-warn-spills"]
 # bit-exact translation units: no contraction of a*b+c into one rounding
-NO_FMA = {"field.cu", "lattice.cu", "network.cu", "coupling.cu", "sim.cu", "api.cu", "noalloc.cu"}
+NO_FMA = {"field.cu", "lattice.cu", "network.cu", "coupling.cu", "sim.cu", "api.cu", "noalloc.cu", "division.cu"}
 
 
 def nvcc() -> str:

@@ -182,6 +182,19 @@ struct Span {
 
 }  // namespace cw
 
+namespace cw {
+// Per-cell scratch of a division round (division.cu).
+struct DivScratch {
+    uint8_t *flag = nullptr;               // cells to divide
+    double *normal = nullptr;              // 3 per cell: the plane's normal
+    unsigned long long *sums = nullptr;    // 3 per cell: coordinate sums
+    int32_t *npix = nullptr, *moved = nullptr, *daughter = nullptr;
+    int64_t cap = 0;
+    int ensure(int64_t ncells);
+    void release();
+};
+}  // namespace cw
+
 struct cw_lattice_s {
     cw::Geom g;
     std::vector<int64_t> cell_off;   // nh + 1
@@ -215,6 +228,12 @@ struct cw_lattice_s {
     int64_t plist_cap = 0;
     uint32_t *pctl = nullptr;             // control words, then 27 pass keys per history (lattice.cu)
     int pass_grid = 0;                    // blocks of the cooperative pass launch
+    // records in use per history (the medium's included): cw_cells_set raises
+    // it, divisions advance it on the device
+    std::vector<int32_t> used;
+    int32_t *d_used = nullptr;
+    cw::DivScratch div;
+    cw::Plan site_plan;                   // every pixel of every history, T per block
     int build_plans();
 };
 
@@ -252,6 +271,8 @@ int field_relax_collect(cw_field_s *f, std::vector<cw_relax_stats> &out, bool &a
 int lattice_recount(cw_lattice_s *lat, int32_t *vol_out, int32_t *surf_out);
 int lattice_sweep(cw_lattice_s *lat);
 int lattice_pass_error(cw_lattice_s *l);
+int lattice_recount_surfaces(cw_lattice_s *l);  // surfaces from the grid into the records, no sync
+int lattice_divide_enqueue(cw_lattice_s *l, const uint8_t *alive, int max_living, double *state, int S);
 // coupling (coupling.cu), device-resident
 int couple_uptake_device(cw_field_s *f, cw_lattice_s *l, const double *d_rate_by_type, int K, double *dst,
                          const Plan &p);

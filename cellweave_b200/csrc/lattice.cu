@@ -723,6 +723,22 @@ static LatDevice dev_of(cw_lattice_s *l) {
 }
 
 namespace cw {
+int lattice_recount_surfaces(cw_lattice_s *l) {
+    Plan &p = l->site_plan;
+    if (p.nblocks == 0) {
+        std::vector<int64_t> per(l->g.nh);
+        for (uint32_t k = 0; k < l->g.nh; ++k) per[k] = l->g.sites(k);
+        int rc = p.build(per, T);
+        if (rc != CW_OK) return rc;
+    }
+    CW_CUDA(cudaMemsetAsync(l->vsnap, 0, sizeof(int32_t) * l->ncells, stream()));
+    CW_CUDA(cudaMemsetAsync(l->surface, 0, sizeof(int32_t) * l->ncells, stream()));
+    k_recount<<<p.nblocks, T, 0, stream()>>>(l->grid, l->g.d_dims, l->g.d_off, l->d_cell_off, p.d_blk, l->g.nh,
+                                             l->vsnap, l->surface);
+    CW_LAUNCHED();
+    return CW_OK;
+}
+
 int lattice_recount(cw_lattice_s *l, int32_t *vol_out, int32_t *surf_out) {
     std::vector<int64_t> per(l->g.nh);
     for (uint32_t k = 0; k < l->g.nh; ++k) per[k] = l->g.sites(k);
@@ -823,7 +839,7 @@ int cw_lattice_create(uint32_t nh, const uint32_t *w, const uint32_t *h, const u
     if ((rc = dalloc(&l->grid, n)) || (rc = dalloc(&l->type, nc)) || (rc = dalloc(&l->volume, nc)) ||
         (rc = dalloc(&l->target, nc)) || (rc = dalloc(&l->lambda, nc)) || (rc = dalloc(&l->vsnap, nc)) ||
         (rc = dalloc(&l->d_cell_off, nh + 1)) || (rc = dalloc(&l->d_keys, nh)) ||
-        (rc = dalloc(&l->d_flag, 4 + 27 * (size_t)nh))) {
+        (rc = dalloc(&l->d_flag, 4 + 27 * (size_t)nh)) || (rc = dalloc(&l->d_used, nh))) {
         cw_lattice_destroy(l);
         return rc;
     }
@@ -834,6 +850,8 @@ int cw_lattice_create(uint32_t nh, const uint32_t *w, const uint32_t *h, const u
     CW_CUDA(cudaMemsetAsync(l->lambda, 0, sizeof(double) * nc, stream()));
     CW_CUDA(cudaMemsetAsync(l->d_keys, 0, sizeof(uint2) * nh, stream()));
     CW_CUDA(cudaMemsetAsync(l->d_flag, 0, sizeof(int32_t) * (4 + 27 * (size_t)nh), stream()));
+    l->used.assign(nh, 1);  // the medium's record
+    CW_CUDA(cudaMemcpyAsync(l->d_used, l->used.data(), sizeof(int32_t) * nh, cudaMemcpyHostToDevice, stream()));
     CW_CUDA(cudaMemcpyAsync(l->d_cell_off, l->cell_off.data(), sizeof(int64_t) * (nh + 1), cudaMemcpyHostToDevice,
                             stream()));
     l->K = 1;
@@ -849,7 +867,9 @@ int cw_lattice_destroy(cw_lattice l) {
     if (!l) return CW_OK;
     dfree(l->grid); dfree(l->type); dfree(l->volume); dfree(l->target); dfree(l->lambda); dfree(l->vsnap);
     dfree(l->surface); dfree(l->ssnap); dfree(l->tsurf); dfree(l->lsurf); dfree(l->d_cell_off); dfree(l->d_keys);
-    dfree(l->d_flag); dfree(l->claim); dfree(l->plist); dfree(l->pctl);
+    dfree(l->d_flag); dfree(l->claim); dfree(l->plist); dfree(l->pctl); dfree(l->d_used);
+    l->div.release();
+    l->site_plan.release();
     for (auto &p : l->plans) p.release();
     l->g.release();
     delete l;
@@ -937,6 +957,10 @@ int cw_cells_set(cw_lattice l, uint32_t hist, uint32_t n, const int32_t *type, c
             return fail(CW_ERR_CONFIG, "cell " + std::to_string(i) + " has type " + std::to_string(type[i]) +
                                            " outside the contact table");
     int64_t c0 = l->cell_off[hist];
+    if ((int32_t)n > l->used[hist]) {
+        l->used[hist] = (int32_t)n;
+        CW_CUDA(cudaMemcpyAsync(l->d_used + hist, &l->used[hist], sizeof(int32_t), cudaMemcpyHostToDevice, stream()));
+    }
     if (type) CW_CUDA(cudaMemcpyAsync(l->type + c0, type, 4 * n, cudaMemcpyHostToDevice, stream()));
     if (volume) CW_CUDA(cudaMemcpyAsync(l->volume + c0, volume, 4 * n, cudaMemcpyHostToDevice, stream()));
     if (target) CW_CUDA(cudaMemcpyAsync(l->target + c0, target, 4 * n, cudaMemcpyHostToDevice, stream()));

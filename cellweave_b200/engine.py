@@ -265,6 +265,23 @@ class CpmLattice:
     def set_temperature(self, t):
         call("cw_lattice_set_temperature", self._h, float(t))
 
+    def divide(self, ids, normals, hist=0):
+        """divide_across (cpm.rs:1094-1160) for each of `ids` with its plane's normal
+        (rows of 2 or 3 components): the daughters' ids, -1 where nothing changed."""
+        ids = np.ascontiguousarray(ids, np.int32).reshape(-1)
+        nrm = np.zeros((ids.size, 3))
+        given = np.asarray(normals, np.float64).reshape(ids.size, -1)
+        nrm[:, :given.shape[1]] = given
+        out = np.empty(ids.size, np.int32)
+        call("cw_lattice_divide", self._h, hist, ids.size, ptr(ids), ptr(np.ascontiguousarray(nrm)), ptr(out))
+        return out
+
+    def cell_count(self, hist=0):
+        """Records in use (the medium's included): cell_count + 1 of the reference."""
+        n = C.c_uint32()
+        call("cw_lattice_cell_count", self._h, hist, C.byref(n))
+        return int(n.value)
+
     def set_copy_neighbourhood(self, moore: bool):
         """Copies from a face neighbour (try_flip, cpm.rs:797-838; the default) or, with
         moore=True, from any pixel at Chebyshev distance 1 (an extension)."""

@@ -91,6 +91,18 @@ int cw_lattice_pass_rounds(cw_lattice lat, uint32_t *rounds);
  * (cpm.rs:274-301): 1 faces only, 2 and 3 the wider reach and its divisor. */
 int cw_lattice_set_contact(cw_lattice lat, int32_t K, const double *J, int32_t order);
 int cw_lattice_set_temperature(cw_lattice lat, double temperature);
+/* divide_across (cpm.rs:1087-1160) for cells `ids` of history `hist`, each
+ * across the plane through its centre of mass with normal normals[3k..3k+2]
+ * (the third component counts in a volume only): the pixels on the side the
+ * normal points to go to a new cell of the same kind and volume parameters,
+ * whose id (the next free record, in the order of `ids` sorted by id) is
+ * written to daughters[k]; -1 where nothing changed (the medium, fewer than
+ * 8 pixels, a plane that leaves one side empty, no free record). */
+int cw_lattice_divide(cw_lattice lat, uint32_t hist, uint32_t n, const int32_t *ids, const double *normals,
+                      int32_t *daughters);
+/* The records history `hist` uses (the medium's included): cells set, plus
+ * the daughters of divisions. */
+int cw_lattice_cell_count(cw_lattice lat, uint32_t hist, uint32_t *n);
 /* Where a copy attempt takes its id from: CW_COPY_VON_NEUMANN, a face
  * neighbour as try_flip does (cpm.rs:797-838, 922-944; the default), or
  * CW_COPY_MOORE, any in-box pixel at Chebyshev distance 1 (an extension). */

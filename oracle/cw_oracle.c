@@ -858,6 +858,54 @@ void or_lattice_mcs_checkerboard(or_lattice *l, uint32_t k0, uint32_t k1, uint32
     free(ssnap);
 }
 
+/* divide_across, cpm.rs:1094-1160: split cell `id` across the plane through
+ * its centre of mass with normal (nx, ny, nz) (nz counts in a volume only);
+ * the pixels with (x - cx) nx + (y - cy) ny [+ (z - cz) nz] > 0 go to a new
+ * record *used (which then advances), of the parent's kind and volume
+ * parameters.  -1, nothing changed: the medium, an unknown id, fewer than 8
+ * pixels (cpm.rs:132), a plane leaving one side empty, or no free record. */
+int32_t or_lattice_divide_across(or_lattice *l, int32_t id, double nx, double ny, double nz, int32_t *used) {
+    if (id <= 0 || id >= *used) return -1;
+    int64_t w = l->w, slice = (int64_t)l->w * l->h, n = slice * l->d;
+    int64_t total = 0;
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+    for (int64_t i = 0; i < n; ++i)
+        if (l->grid[i] == id) {
+            sx += (double)(i % w);
+            sy += (double)((i / w) % l->h);
+            sz += (double)(i / slice);
+            ++total;
+        }
+    if (total < 8) return -1;
+    if (*used >= l->ncells) return -1;
+    double fn = (double)total, cx = sx / fn, cy = sy / fn, cz = l->d > 1 ? sz / fn : 0.0;
+    int32_t daughter = *used;
+    int64_t moved = 0;
+    for (int64_t i = 0; i < n; ++i) {
+        if (l->grid[i] != id) continue;
+        double x = (double)(i % w), y = (double)((i / w) % l->h), z = (double)(i / slice);
+        double side = (x - cx) * nx + (y - cy) * ny;
+        if (l->d > 1) side += (z - cz) * nz;
+        if (side > 0.0) { l->grid[i] = daughter; ++moved; }
+    }
+    if (moved == 0 || moved == total) {
+        for (int64_t i = 0; i < n; ++i)
+            if (l->grid[i] == daughter) l->grid[i] = id;
+        return -1;
+    }
+    l->volume[id] = (int32_t)(total - moved);
+    l->type[daughter] = l->type[id];
+    l->volume[daughter] = (int32_t)moved;
+    l->target[daughter] = l->target[id];
+    l->lambda[daughter] = l->lambda[id];
+    if (l->surface) {
+        l->target_surface[daughter] = l->target_surface[id];
+        l->lambda_surface[daughter] = l->lambda_surface[id];
+    }
+    *used += 1;
+    return daughter;
+}
+
 /* Recount volumes (and surfaces) from the grid: records_match_grid,
  * cpm.rs:1262-1279.  Obstacles are skipped; ids past ncells are ignored. */
 void or_lattice_recount(const or_lattice *l, int32_t *volume, int32_t *surface) {

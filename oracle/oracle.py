@@ -50,6 +50,8 @@ def lib():
         L.or_lattice_delta_h.restype = None
         L.or_lattice_mcs_sequential.argtypes = [P, C.c_uint64, C.c_int32]
         L.or_lattice_mcs_sequential.restype = None
+        L.or_lattice_divide_across.argtypes = [P, C.c_int32, C.c_double, C.c_double, C.c_double, P]
+        L.or_lattice_divide_across.restype = C.c_int32
         L.or_lattice_mcs_checkerboard.argtypes = [P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int32, C.c_int32]
         L.or_lattice_mcs_checkerboard.restype = None
         L.or_lattice_recount.argtypes = [P, P, P]
@@ -250,6 +252,15 @@ class Lattice:
         s = self._struct()
         lib().or_lattice_mcs_checkerboard(C.byref(s), int(seed) & 0xFFFFFFFF, (int(seed) >> 32) & 0xFFFFFFFF,
                                           int(mcs0) & 0xFFFFFFFF, int(sweeps), int(bool(snapshot)))
+
+    def divide_across(self, cid: int, normal, used: int):
+        """divide_across (cpm.rs:1094-1160) with the daughter at record `used`:
+        (daughter id or -1, records in use after)."""
+        s = self._struct()
+        u = np.array([used], np.int32)
+        nx, ny, nz = (float(v) for v in (tuple(normal) + (0.0, 0.0, 0.0))[:3])
+        d = lib().or_lattice_divide_across(C.byref(s), int(cid), nx, ny, nz, _p(u))
+        return int(d), int(u[0])
 
     def occupied_span(self):
         s = self._struct()

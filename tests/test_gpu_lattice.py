@@ -195,3 +195,40 @@ def test_bad_input_is_refused():
         lat.set_contact(np.array([[0, 1], [2, 0]], float))
     with pytest.raises(cw.NotFoundError):
         lat.grid(hist=3)
+
+
+@pytest.mark.parametrize("volume", [False, True])
+def test_divisions_are_bit_exact_with_the_oracle(volume):
+    # divide_across (cpm.rs:1094-1160) of many cells at once against the
+    # oracle's one at a time, in id order; plus what must not divide
+    if volume:
+        grid, rec = ball_volume(18)
+    else:
+        grid, rec = sheet(seed=21, size=80, ncell=24)
+    n = len(rec)
+    cap = 2 * n + 2
+    o = oracle_of(grid, rec, J3, 10.0, 1)
+    lat = O.Lattice(o.grid, (o.w, o.h, o.d), cap, J3, 10.0, 1)
+    lat.type[:n], lat.volume[:n], lat.target[:n], lat.lam[:n] = o.type, o.volume, o.target, o.lam
+    g = cw.CpmLattice.from_grids([grid], [rec], 10.0, J3, 1, seeds=[1], capacity=cap)
+    rng = np.random.default_rng(4 + volume)
+    ids = np.array([0] + list(range(1, n)), np.int32)  # existing cells only, as divide_ready_cells takes them
+    v = rng.normal(size=(ids.size, 3))
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    if not volume:
+        v[:, 2] = 0.0
+    got = g.divide(ids, v)
+    used = n
+    want = []
+    for cid, nrm in zip(ids, v):
+        d, used = lat.divide_across(int(cid), nrm, used)
+        want.append(d)
+    np.testing.assert_array_equal(got, want)
+    assert (np.array(want) > 0).sum() >= n // 2
+    np.testing.assert_array_equal(g.grid().reshape(-1), lat.grid)
+    cells = g.cells()
+    np.testing.assert_array_equal(cells["volume"][1:used], lat.volume[1:used])
+    np.testing.assert_array_equal(cells["type"][:used], lat.type[:used])
+    np.testing.assert_array_equal(cells["target"][:used], lat.target[:used])
+    assert g.cell_count() == used
+    assert g.records_match_grid()

@@ -507,3 +507,46 @@ def test_moore_copies_need_period_two_with_face_contact():
     assert vol.colouring() == (8, 2)
     vol.order = 3  # the 26-neighbourhood: Chebyshev radius 1, period 2 either way
     assert vol.colouring() == (8, 2)
+
+
+def _disc_lattice(size, centre, radius, lam=1.0, capacity=8):
+    from cellweave_b200 import seeding
+    grid = seeding.empty(size, size)
+    rec = seeding.Records()
+    seeding.add_cell(grid, rec, 1, centre, radius, lam=lam)
+    lat = O.Lattice(grid, (size, size, 1), capacity, np.zeros((2, 2)), 10.0, 1)
+    t, v, tg, lm = rec.arrays()
+    lat.type[:len(rec)], lat.volume[:len(rec)], lat.target[:len(rec)], lat.lam[:len(rec)] = t, v, tg, lm
+    return lat, len(rec)
+
+
+def test_division_hands_every_pixel_to_exactly_one_of_the_two():
+    # cpm.rs:1302-1316 and 1319-1332
+    lat, used = _disc_lattice(60, (30, 30), 10)
+    before = int(lat.volume[1])
+    lat.target[1], lat.lam[1] = 500, 33.0
+    d, used = lat.divide_across(1, (math.cos(0.3), math.sin(0.3)), used)
+    assert d == 2 and used == 3
+    p, q = int(lat.volume[1]), int(lat.volume[2])
+    assert p + q == before and p > 0 and q > 0
+    assert abs(p - q) < before / 5
+    assert lat.type[2] == lat.type[1] and lat.target[2] == 500 and lat.lam[2] == 33.0
+    vol, _ = lat.counts()
+    np.testing.assert_array_equal(vol[1:3], lat.volume[1:3])
+
+
+def test_what_cannot_be_divided_is_left_alone():
+    # cpm.rs:1335-1379: a cell under 8 pixels, the medium, an unknown id, and a
+    # cut that leaves one side empty change nothing
+    lat, used = _disc_lattice(30, (15, 15), 1)
+    grid = lat.grid.copy()
+    assert lat.divide_across(1, (math.cos(0.5), math.sin(0.5)), used) == (-1, used)
+    assert lat.divide_across(0, (1.0, 0.0), used) == (-1, used)
+    assert lat.divide_across(42, (1.0, 0.0), used) == (-1, used)
+    np.testing.assert_array_equal(lat.grid, grid)
+    bar = np.zeros((1, 20, 20), np.int32)
+    bar[0, 5:15, 10] = 1
+    lat = O.Lattice(bar, (20, 20, 1), 4, np.zeros((2, 2)), 10.0, 1)
+    lat.type[1], lat.volume[1], lat.target[1], lat.lam[1] = 1, 10, 10, 1.0
+    assert lat.divide_across(1, (1.0, 0.0), 2) == (-1, 2)
+    np.testing.assert_array_equal(lat.grid, bar.reshape(-1))
