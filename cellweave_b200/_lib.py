@@ -83,7 +83,8 @@ class SimConfig(C.Structure):
                 ("signal_decay", C.c_double), ("signal_secretion", C.c_double), ("hypoxic_level", C.c_double),
                 ("tolerance", C.c_double), ("precision", C.c_int32), ("omega", C.c_double),
                 ("inner_sweeps", C.c_int32), ("relax_every", C.c_int32), ("dt", C.c_double), ("substeps", C.c_int32), ("sweeps", C.c_int32),
-                ("death_threshold", C.c_double), ("necrotic_type", C.c_int32), ("use_graphs", C.c_int32)]
+                ("death_threshold", C.c_double), ("necrotic_type", C.c_int32), ("use_graphs", C.c_int32),
+                ("divide", C.c_int32), ("max_cells", C.c_int32), ("spare_cells", C.c_int32)]
 
 
 P = C.c_void_p

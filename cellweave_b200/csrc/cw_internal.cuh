@@ -189,6 +189,7 @@ struct DivScratch {
     double *normal = nullptr;              // 3 per cell: the plane's normal
     unsigned long long *sums = nullptr;    // 3 per cell: coordinate sums
     int32_t *npix = nullptr, *moved = nullptr, *daughter = nullptr;
+    int32_t *count = nullptr;              // cells flagged: the passes skip all work at 0
     int64_t cap = 0;
     int ensure(int64_t ncells);
     void release();
@@ -291,5 +292,6 @@ int network_mechanics_device(const cw_network_s *n, const double *state, int64_t
 int32_t network_nodes(const cw_network_s *n);
 double network_lambda(const cw_network_s *n);
 int32_t network_role(const cw_network_s *n, int k);
+uint32_t network_reference_volume(const cw_network_s *n);
 const std::vector<double> &network_initial(const cw_network_s *n);
 }  // namespace cw

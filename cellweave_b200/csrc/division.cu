@@ -41,7 +41,9 @@ __device__ __forceinline__ void pixel_xyz(int64_t i, int4 dm, int &x, int &y, in
 
 // The coordinate sums and pixel counts of the flagged cells.
 __global__ void k_div_sums(const int32_t *grid, const int4 *dims, const int64_t *off, const int64_t *cell_off,
-                           const int32_t *blk, int nh, const uint8_t *flag, unsigned long long *sums, int32_t *npix) {
+                           const int32_t *blk, int nh, const uint8_t *flag, unsigned long long *sums, int32_t *npix,
+                           const int32_t *count) {
+    if (*count == 0) return;
     __shared__ int s_h;
     if (threadIdx.x == 0) s_h = plan_history(blk, nh, blockIdx.x);
     __syncthreads();
@@ -76,7 +78,8 @@ __device__ __forceinline__ double side_of(const unsigned long long *sums, const 
 // How many pixels each flagged cell's plane moves.
 __global__ void k_div_moved(const int32_t *grid, const int4 *dims, const int64_t *off, const int64_t *cell_off,
                             const int32_t *blk, int nh, const uint8_t *flag, const unsigned long long *sums,
-                            const int32_t *npix, const double *normal, int32_t *moved) {
+                            const int32_t *npix, const double *normal, int32_t *moved, const int32_t *count) {
+    if (*count == 0) return;
     __shared__ int s_h;
     if (threadIdx.x == 0) s_h = plan_history(blk, nh, blockIdx.x);
     __syncthreads();
@@ -98,7 +101,8 @@ __global__ void k_div_moved(const int32_t *grid, const int4 *dims, const int64_t
 // allow; daughter[c] = the new id or -1.  used[h] advances.
 __global__ void k_div_select(const int64_t *cell_off, int nh, const uint8_t *flag, const int32_t *npix,
                              const int32_t *moved, const uint8_t *alive, int max_living, int32_t *used,
-                             int32_t *daughter) {
+                             int32_t *daughter, const int32_t *count) {
+    if (*count == 0) return;
     __shared__ int s_scan[T];
     __shared__ int s_base, s_living, s_room;
     const int h = blockIdx.x;
@@ -153,7 +157,8 @@ __global__ void k_div_select(const int64_t *cell_off, int nh, const uint8_t *fla
 // The dividing cells' pixels on the far side of their planes to the daughters.
 __global__ void k_div_relabel(int32_t *grid, const int4 *dims, const int64_t *off, const int64_t *cell_off,
                               const int32_t *blk, int nh, const int32_t *daughter, const unsigned long long *sums,
-                              const int32_t *npix, const double *normal) {
+                              const int32_t *npix, const double *normal, const int32_t *count) {
+    if (*count == 0) return;
     __shared__ int s_h;
     if (threadIdx.x == 0) s_h = plan_history(blk, nh, blockIdx.x);
     __syncthreads();
@@ -178,7 +183,8 @@ __global__ void k_div_relabel(int32_t *grid, const int4 *dims, const int64_t *of
 __global__ void k_div_records(const int64_t *cell_off, int nh, int64_t nc, const int32_t *daughter,
                               const int32_t *npix, const int32_t *moved, int32_t *type, int32_t *volume,
                               int32_t *target, double *lambda, int32_t *tsurf, double *lsurf, double *state, int S,
-                              uint8_t *alive) {
+                              uint8_t *alive, const int32_t *count) {
+    if (*count == 0) return;
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nc) return;
     const int32_t dg = daughter[c];
@@ -197,9 +203,39 @@ __global__ void k_div_records(const int64_t *cell_off, int nh, int64_t nc, const
     if (alive) alive[d] = 1;
 }
 
-__global__ void k_zero_surface(int32_t *surface, int64_t nc) {
+// Surfaces counted again after divisions (two cells' surfaces change with
+// each): zeroed, then every pixel adds its faces against other ids.
+__global__ void k_div_surface_zero(int32_t *surface, int64_t nc, const int32_t *count) {
+    if (*count == 0) return;
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (c < nc) surface[c] = 0;
+}
+
+__global__ void k_div_surface_count(const int32_t *grid, const int4 *dims, const int64_t *off, const int64_t *cell_off,
+                                    const int32_t *blk, int nh, int32_t *surface, const int32_t *count) {
+    if (*count == 0) return;
+    __shared__ int s_h;
+    if (threadIdx.x == 0) s_h = plan_history(blk, nh, blockIdx.x);
+    __syncthreads();
+    const int h = s_h;
+    const int64_t i = (int64_t)(blockIdx.x - blk[h]) * blockDim.x + threadIdx.x;
+    if (i >= off[h + 1] - off[h]) return;
+    const int32_t *g = grid + off[h];
+    const int32_t id = g[i];
+    const int64_t c0 = cell_off[h], cap = cell_off[h + 1] - c0;
+    if (id <= 0 || id >= cap) return;
+    const int4 dm = dims[h];
+    int x, y, z;
+    pixel_xyz(i, dm, x, y, z);
+    const int64_t w = dm.x, slice = (int64_t)dm.x * dm.y;
+    int faces = 0;
+    if (y > 0) faces += g[i - w] != id;
+    if (y + 1 < dm.y) faces += g[i + w] != id;
+    if (x > 0) faces += g[i - 1] != id;
+    if (x + 1 < dm.x) faces += g[i + 1] != id;
+    if (z > 0) faces += g[i - slice] != id;
+    if (z + 1 < dm.z) faces += g[i + slice] != id;
+    if (faces) atomicAdd(surface + c0 + id, faces);
 }
 
 }  // namespace
@@ -211,19 +247,22 @@ int DivScratch::ensure(int64_t nc) {
     release();
     int rc;
     if ((rc = dalloc(&flag, nc)) || (rc = dalloc(&normal, 3 * nc)) || (rc = dalloc(&sums, 3 * nc)) ||
-        (rc = dalloc(&npix, nc)) || (rc = dalloc(&moved, nc)) || (rc = dalloc(&daughter, nc)))
+        (rc = dalloc(&npix, nc)) || (rc = dalloc(&moved, nc)) || (rc = dalloc(&daughter, nc)) ||
+        (rc = dalloc(&count, 1)))
         return rc;
+    CW_CUDA(cudaMemsetAsync(count, 0, sizeof(int32_t), stream()));
     cap = nc;
     return CW_OK;
 }
 
 void DivScratch::release() {
-    dfree(flag); dfree(normal); dfree(sums); dfree(npix); dfree(moved); dfree(daughter);
+    dfree(flag); dfree(normal); dfree(sums); dfree(npix); dfree(moved); dfree(daughter); dfree(count);
     cap = 0;
 }
 
-// Divide the cells flagged in l->div.flag across the planes in l->div.normal
-// (no host synchronisation).  alive / max_living: the living-cell limit
+// Divide the cells flagged in l->div.flag (l->div.count of them) across the
+// planes in l->div.normal (no host synchronisation); with none flagged every
+// pass returns at once.  alive / max_living: the living-cell limit
 // (null: none); state ([S][nc]) is copied to daughters when given.
 int lattice_divide_enqueue(cw_lattice_s *l, const uint8_t *alive, int max_living, double *state, int S) {
     DivScratch &D = l->div;
@@ -236,32 +275,35 @@ int lattice_divide_enqueue(cw_lattice_s *l, const uint8_t *alive, int max_living
         if (rc != CW_OK) return rc;
     }
     const int nh = (int)l->g.nh;
+    const int32_t *cnt = D.count;
     CW_CUDA(cudaMemsetAsync(D.sums, 0, sizeof(unsigned long long) * 3 * nc, stream()));
     CW_CUDA(cudaMemsetAsync(D.npix, 0, sizeof(int32_t) * nc, stream()));
     CW_CUDA(cudaMemsetAsync(D.moved, 0, sizeof(int32_t) * nc, stream()));
+    CW_CUDA(cudaMemsetAsync(D.daughter, 0xFF, sizeof(int32_t) * nc, stream()));
     k_div_sums<<<p.nblocks, T, 0, stream()>>>(l->grid, l->g.d_dims, l->g.d_off, l->d_cell_off, p.d_blk, nh, D.flag,
-                                              D.sums, D.npix);
+                                              D.sums, D.npix, cnt);
     CW_LAUNCHED();
     k_div_moved<<<p.nblocks, T, 0, stream()>>>(l->grid, l->g.d_dims, l->g.d_off, l->d_cell_off, p.d_blk, nh, D.flag,
-                                               D.sums, D.npix, D.normal, D.moved);
+                                               D.sums, D.npix, D.normal, D.moved, cnt);
     CW_LAUNCHED();
     k_div_select<<<nh, T, 0, stream()>>>(l->d_cell_off, nh, D.flag, D.npix, D.moved, alive, max_living, l->d_used,
-                                         D.daughter);
+                                         D.daughter, cnt);
     CW_LAUNCHED();
     k_div_relabel<<<p.nblocks, T, 0, stream()>>>(l->grid, l->g.d_dims, l->g.d_off, l->d_cell_off, p.d_blk, nh,
-                                                 D.daughter, D.sums, D.npix, D.normal);
+                                                 D.daughter, D.sums, D.npix, D.normal, cnt);
     CW_LAUNCHED();
     const unsigned cb = (unsigned)((nc + T - 1) / T);
     k_div_records<<<cb, T, 0, stream()>>>(l->d_cell_off, nh, nc, D.daughter, D.npix, D.moved, l->type, l->volume,
                                           l->target, l->lambda, l->surface_on ? l->tsurf : nullptr,
                                           l->surface_on ? l->lsurf : nullptr, state, S,
-                                          const_cast<uint8_t *>(alive));
+                                          const_cast<uint8_t *>(alive), cnt);
     CW_LAUNCHED();
-    if (l->surface_on) {  // two cells' surfaces changed for every division: count them all again
-        k_zero_surface<<<cb, T, 0, stream()>>>(l->surface, nc);
+    if (l->surface_on) {
+        k_div_surface_zero<<<cb, T, 0, stream()>>>(l->surface, nc, cnt);
         CW_LAUNCHED();
-        int rc = lattice_recount_surfaces(l);
-        if (rc != CW_OK) return rc;
+        k_div_surface_count<<<p.nblocks, T, 0, stream()>>>(l->grid, l->g.d_dims, l->g.d_off, l->d_cell_off, p.d_blk,
+                                                           nh, l->surface, cnt);
+        CW_LAUNCHED();
     }
     return CW_OK;
 }
@@ -287,6 +329,9 @@ int cw_lattice_divide(cw_lattice l, uint32_t hist, uint32_t n, const int32_t *id
     CW_CUDA(cudaMemcpyAsync(l->div.flag, flag.data(), nc, cudaMemcpyHostToDevice, stream()));
     CW_CUDA(cudaMemcpyAsync(l->div.normal, normal.data(), sizeof(double) * 3 * nc, cudaMemcpyHostToDevice,
                             stream()));
+    int32_t flagged = 0;
+    for (uint8_t f : flag) flagged += f;
+    CW_CUDA(cudaMemcpyAsync(l->div.count, &flagged, sizeof flagged, cudaMemcpyHostToDevice, stream()));
     if ((rc = lattice_divide_enqueue(l, nullptr, 0, nullptr, 0)) != CW_OK) return rc;
     std::vector<int32_t> dg(nc);
     CW_CUDA(cudaMemcpyAsync(dg.data(), l->div.daughter, sizeof(int32_t) * nc, cudaMemcpyDeviceToHost, stream()));

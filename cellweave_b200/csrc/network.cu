@@ -124,6 +124,7 @@ int network_mechanics_device(const cw_network_s *n, const double *state, int64_t
 int32_t network_nodes(const cw_network_s *n) { return n->S; }
 double network_lambda(const cw_network_s *n) { return n->lambda_volume; }
 int32_t network_role(const cw_network_s *n, int k) { return n->roles[k]; }
+uint32_t network_reference_volume(const cw_network_s *n) { return n->reference_volume; }
 const std::vector<double> &network_initial(const cw_network_s *n) { return n->initial; }
 }  // namespace cw
 

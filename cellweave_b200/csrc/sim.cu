@@ -98,20 +98,73 @@ __global__ void k_secretion(const uint8_t *alive, const double *cell_o2, int64_t
     if (c < nc) secretion[c] = (alive[c] && cell_o2[c] < level) ? rate : 0.0;
 }
 
+constexpr int32_t RESORPTION_RATE = 2;    // pixels a necrotic cell gives up a step (simulation.rs:127)
+constexpr double DIVISION_RATIO = 1.4;    // of the reference volume (simulation.rs:45)
+constexpr double QUIESCENCE_THRESHOLD = 0.45;  // hypoxia response that stops cycling (simulation.rs:117)
+constexpr int DEFAULT_MAX_CELLS = 2000;   // simulation.rs:61
+
 // Fate and upward coupling (simulation.rs:1212-1309, the necrosis and
-// mechanics branches): survival below the threshold makes the cell
+// mechanics branches): a necrotic cell gives up RESORPTION_RATE pixels a step
+// until it is gone; survival below the threshold makes a living cell
 // necrotic; every other living cell takes the target its mechanics give.
 __global__ void k_fates(const uint8_t *alive, const double *state, int64_t nc, int survival, double death,
-                        int necrotic, const uint32_t *mech_target, int32_t *type, int32_t *target, double *lambda,
-                        double lam) {
+                        int necrotic, const uint32_t *mech_target, int32_t *type, const int32_t *volume,
+                        int32_t *target, double *lambda, double lam) {
     int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= nc || !alive[c]) return;
+    if (c >= nc) return;
+    if (necrotic >= 0 && type[c] == necrotic) {
+        const int32_t v = volume[c];
+        if (v > 0) {
+            target[c] = v > RESORPTION_RATE ? v - RESORPTION_RATE : 0;
+            lambda[c] = lam;
+        }
+        return;
+    }
+    if (!alive[c]) return;
     if (necrotic >= 0 && state[survival * nc + c] < death) {
         type[c] = necrotic;
         return;
     }
     target[c] = (int32_t)min(mech_target[c], 0x7fffffffu);
     lambda[c] = lam;
+}
+
+// Which cells divide this step (divide_ready_cells, simulation.rs:1603-1626):
+// living, of at least DIVISION_RATIO times the reference volume, cycling
+// (hypoxia response under QUIESCENCE_THRESHOLD); the plane's normal from
+// Philox(cell, step, 3, 0) under the history's key: a uniform angle in the
+// plane, a uniform direction in a volume (simulation.rs:1631-1642).  Also
+// refreshes `alive` for the living-cell limit.
+__global__ void k_div_ready(const int32_t *type, const int32_t *volume, const int64_t *cell_off, const uint2 *keys,
+                            const int4 *dims, int nh, int64_t nc, int necrotic, const double *state, int hyp,
+                            double threshold, const uint32_t *mcs_ctr, uint8_t *alive, uint8_t *flag,
+                            double *normal, int32_t *count) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nc) return;
+    int lo = 0, hi = nh - 1;
+    while (lo < hi) { int mid = (lo + hi + 1) >> 1; if (cell_off[mid] <= c) lo = mid; else hi = mid - 1; }
+    const int64_t local = c - cell_off[lo];
+    const bool a = local > 0 && volume[c] > 0 && type[c] != necrotic;
+    alive[c] = a;
+    const bool ready = a && (double)volume[c] >= threshold && (hyp < 0 || state[(int64_t)hyp * nc + c] < QUIESCENCE_THRESHOLD);
+    flag[c] = ready;
+    if (!ready) return;
+    atomicAdd(count, 1);  // few cells are ready at once
+    const uint2 k = keys[lo];
+    const uint4 r = philox((uint32_t)local, *mcs_ctr, 3u, 0u, k.x, k.y);
+    const double u0 = u01(r.x, r.y), u1 = u01(r.z, r.w);
+    if (dims[lo].z > 1) {
+        const double z = 2.0 * u0 - 1.0, around = u1 * 6.283185307179586;
+        const double rr = sqrt(fmax(1.0 - z * z, 0.0));
+        normal[3 * c + 0] = rr * cos(around);
+        normal[3 * c + 1] = rr * sin(around);
+        normal[3 * c + 2] = z;
+    } else {
+        const double angle = u0 * 3.141592653589793;
+        normal[3 * c + 0] = cos(angle);
+        normal[3 * c + 1] = sin(angle);
+        normal[3 * c + 2] = 0.0;
+    }
 }
 
 __global__ void k_stats(const uint8_t *alive, const double *cell_o2, const int32_t *volume, const int64_t *cell_off,
@@ -235,13 +288,17 @@ int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out) {
     std::vector<uint32_t> cap(c.nh);
     for (uint32_t k = 0; k < c.nh; ++k) {
         seed_history(c, s->w[k], s->h[k], s->d[k], s->ncells[k], s->seeds[k], grids[k], types[k], ncelltypes);
-        cap[k] = (uint32_t)types[k].size();
+        // records for the daughters of divisions too
+        const int32_t spare = !c.divide ? 0 : c.spare_cells > 0 ? c.spare_cells : c.max_cells > 0 ? c.max_cells
+                                                                                              : DEFAULT_MAX_CELLS;
+        cap[k] = (uint32_t)(types[k].size() + spare);
     }
     int rc = cw_lattice_create(c.nh, s->w.data(), s->h.data(), s->d.data(), cap.data(), c.temperature, &s->lat);
     if (rc != CW_OK) { cw_sim_destroy(s); return rc; }
     if ((rc = cw_lattice_set_contact(s->lat, c.K, c.J, c.contact_order)) != CW_OK) { cw_sim_destroy(s); return rc; }
+    if (c.divide && (rc = s->lat->div.ensure(s->lat->ncells)) != CW_OK) { cw_sim_destroy(s); return rc; }
     for (uint32_t k = 0; k < c.nh; ++k) {
-        uint32_t n = cap[k];
+        uint32_t n = (uint32_t)types[k].size();  // the seeded records; the spares stay free
         std::vector<int32_t> vol(n, 0), tgt(n, c.target_volume);
         std::vector<double> lam(n, c.lambda_volume);
         for (int32_t id : grids[k]) if (id > 0) vol[id] += 1;
@@ -422,6 +479,24 @@ static void drop_graphs(cw_sim_s *s) {
     s->graphs = false;
 }
 
+// The division step (simulation.rs:1338-1347): every step, the ready cells
+// of each history in id order as far as the living-cell limit allows, each
+// daughter taking a copy of its parent's network state.
+static int division_step(cw_sim_s *s) {
+    const cw_sim_config &c = s->cfg;
+    if (!c.divide) return CW_OK;
+    const int64_t nc = s->nc;
+    cw_lattice_s *l = s->lat;
+    CW_CUDA(cudaMemsetAsync(l->div.count, 0, sizeof(int32_t), stream()));
+    k_div_ready<<<(unsigned)blocks(nc), T, 0, stream()>>>(
+        l->type, l->volume, l->d_cell_off, l->d_keys, l->g.d_dims, (int)c.nh, nc, c.necrotic_type, s->state,
+        network_role(s->net, 2), DIVISION_RATIO * (double)network_reference_volume(s->net),
+        (const uint32_t *)l->d_flag, s->alive, l->div.flag, l->div.normal, l->div.count);
+    CW_LAUNCHED();
+    return lattice_divide_enqueue(l, s->alive, c.max_cells > 0 ? c.max_cells : DEFAULT_MAX_CELLS, s->state,
+                                  network_nodes(s->net));
+}
+
 // One of the three phases of a step, enqueued without host synchronisation.
 static int enqueue_phase(cw_sim_s *s, int p, const cw_relax_opts &o) {
     const cw_sim_config &c = s->cfg;
@@ -453,10 +528,11 @@ static int enqueue_phase(cw_sim_s *s, int p, const cw_relax_opts &o) {
     if ((rc = network_mechanics_device(s->net, s->state, nc, nc, s->target32)) != CW_OK) return rc;
     k_fates<<<(unsigned)blocks(nc), T, 0, stream()>>>(s->alive, s->state, nc, network_role(s->net, 1),
                                                       c.death_threshold, c.necrotic_type, s->target32, s->lat->type,
-                                                      s->lat->target, s->lat->lambda, c.lambda_volume);
+                                                      s->lat->volume, s->lat->target, s->lat->lambda, c.lambda_volume);
     CW_LAUNCHED();
     for (int k = 0; k < c.sweeps; ++k)
         if ((rc = lattice_sweep(s->lat)) != CW_OK) return rc;
+    if ((rc = division_step(s)) != CW_OK) return rc;
     return CW_OK;
 }
 
@@ -612,11 +688,13 @@ int cw_sim_step(cw_sim s, uint32_t nsteps) {
         if ((rc = network_mechanics_device(s->net, s->state, nc, nc, s->target32)) != CW_OK) return rc;
         k_fates<<<(unsigned)blocks(nc), T, 0, stream()>>>(s->alive, s->state, nc, survival, c.death_threshold,
                                                           c.necrotic_type, s->target32, s->lat->type,
-                                                          s->lat->target, s->lat->lambda, c.lambda_volume);
+                                                          s->lat->volume, s->lat->target, s->lat->lambda,
+                                                          c.lambda_volume);
         CW_LAUNCHED();
-        // 5. the lattice
+        // 5. the lattice, then 6. division
         for (int k = 0; k < c.sweeps; ++k)
             if ((rc = lattice_sweep(s->lat)) != CW_OK) return rc;
+        if ((rc = division_step(s)) != CW_OK) return rc;
         if (tuning && ++s->tune.done >= s->tune.steps) tune_finish(s);
         (void)S;
     }

@@ -561,7 +561,7 @@ class Simulation:
                  nfields=1, o2_dcoef=1.0, o2_sink_by_type=(0.0, 0.01, 0.01), o2_background_sink=0.0, o2_hold=0, signal_dcoef=1.0,
                  signal_decay=0.01, signal_secretion=0.05, hypoxic_level=0.1, tolerance=1e-6, precision=FP32_DC,
                  omega=None, inner_sweeps=0, relax_every=1, dt=0.01, substeps=8, sweeps=1, death_threshold=0.25,
-                 necrotic_type=-1, use_graphs=True):
+                 necrotic_type=-1, use_graphs=True, divide=True, max_cells=2000, spare_cells=0):
         self.dims, w, h, z = _dims(dims)
         self._keep = [w, h, z]
         nc = np.array(ncells, np.uint32)
@@ -577,7 +577,8 @@ class Simulation:
                              int(o2_hold), float(signal_dcoef), float(signal_decay), float(signal_secretion),
                              float(hypoxic_level), float(tolerance), int(precision), float(omega or 0.0), int(inner_sweeps),
                              int(relax_every), float(dt), int(substeps), int(sweeps), float(death_threshold),
-                             int(necrotic_type), int(bool(use_graphs)))
+                             int(necrotic_type), int(bool(use_graphs)), int(bool(divide)), int(max_cells),
+                             int(spare_cells))
         handle = C.c_void_p()
         call("cw_sim_create", C.byref(cfg), network.handle, C.byref(handle))
         self._h = handle

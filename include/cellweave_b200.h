@@ -310,7 +310,10 @@ int cw_network_backward_batch(cw_network net, int64_t ncells, const double *stat
  * reduced to the hot path: per lattice step, every field is painted from the
  * lattice and relaxed, cells read their field means, every living network
  * takes `substeps` RK4 steps, survival and mechanics set kind and target
- * volume, and the lattice takes `sweeps` Monte Carlo steps. */
+ * volume (a necrotic cell's shrinking by 2 pixels a step until it is gone),
+ * the lattice takes `sweeps` Monte Carlo steps, and cells grown past 1.4
+ * times the network's reference volume, not too hypoxic to cycle, divide
+ * (simulation.rs:1338-1347, 1603-1716). */
 typedef struct {
     uint32_t nh;                 /* histories (a batch of uneven sizes) */
     const uint32_t *w, *h, *d;   /* per history */
@@ -343,6 +346,9 @@ typedef struct {
     double death_threshold;      /* survival below it: the necrotic type */
     int32_t necrotic_type;       /* type a dead cell takes (-1: none) */
     int32_t use_graphs;          /* once tuned, replay each step as captured CUDA graphs */
+    int32_t divide;              /* 1: the division step; 0: none */
+    int32_t max_cells;           /* living cells a history divides up to (<= 0: 2000, the reference's default) */
+    int32_t spare_cells;         /* records per history for daughters (<= 0: max_cells) */
 } cw_sim_config;
 int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out);
 int cw_sim_destroy(cw_sim sim);

@@ -74,15 +74,19 @@ class CpuHistory:
         self.dims = (w, h, d)
         self.seed = int(cfg["seeds"][k])
         grid, types = seed_history(cfg, w, h, d, int(cfg["ncells"][k]), self.seed)
-        self.ncap = len(types)
+        self.divide = bool(cfg.get("divide", True))
+        self.max_cells = int(cfg.get("max_cells", 2000) or 2000)
+        spare = int(cfg.get("spare_cells", 0) or self.max_cells) if self.divide else 0
+        self.used = len(types)
+        self.ncap = len(types) + spare
         J = np.asarray(cfg["J"], float)
         self.lat = O.Lattice(grid, (w, h, d), self.ncap, J, cfg["temperature"], cfg.get("contact_order", 1))
-        self.lat.type[:] = types
+        self.lat.type[:len(types)] = types
         self.lat.recount()
         self.lat.volume[0] = 0
-        self.lat.target[:] = cfg["target_volume"]
+        self.lat.target[:self.used] = cfg["target_volume"]
         self.lat.target[0] = 0
-        self.lat.lam[:] = cfg["lambda_volume"]
+        self.lat.lam[:self.used] = cfg["lambda_volume"]
         self.lat.lam[0] = 0.0
         if cfg.get("surface_target", 0) > 0:
             self.lat.enable_surface(np.full(self.ncap, cfg["surface_target"], np.int32),
@@ -99,9 +103,10 @@ class CpuHistory:
         self.sig = None
         if cfg.get("nfields", 1) == 2:
             self.sig = O.Field(w, h, d, cfg["signal_dcoef"], cfg["signal_decay"], 0.0)
-        spec = tomllib.loads(synthetic.network_toml(cfg["S"], cfg["S"]))
+        spec = tomllib.loads(cfg.get("network_toml") or synthetic.network_toml(cfg["S"], cfg["S"]))
         self.net = O.compile_network(spec, cfg["target_volume"])
         self.state = np.tile(self.net.initial, (self.ncap, 1))
+        self.div_rng = np.random.default_rng(self.seed * 7 + 13)
         sink = np.zeros(8)
         sink[:len(cfg["o2_sink_by_type"])] = cfg["o2_sink_by_type"]
         self.sink = sink
@@ -126,6 +131,12 @@ class CpuHistory:
             sec = np.where(alive & (o2m < c["hypoxic_level"]), c["signal_secretion"], 0.0)
             self.sig.production = O.apply_production(g, sec)
             self.sig.relax(c["tolerance"], 200_000, omega=omega, stop=1, threads=1)
+        # a necrotic cell gives up 2 pixels a step until it is gone (simulation.rs:1230-1262)
+        if nec >= 0:
+            dying = np.nonzero((t == nec) & (self.lat.volume > 0))[0]
+            dying = dying[dying > 0]
+            self.lat.target[dying] = np.maximum(self.lat.volume[dying] - 2, 0)
+            self.lat.lam[dying] = c["lambda_volume"]
         idx = np.nonzero(alive)[0]
         if len(idx):
             ins = np.zeros((len(idx), 6))
@@ -141,5 +152,39 @@ class CpuHistory:
             self.lat.target[live] = np.minimum(tg[~dead], 2**31 - 1).astype(np.int32)
             self.lat.lam[live] = c["lambda_volume"]
         self.lat.mcs_sequential(self.seed * 1_000_003 + self.steps, c.get("sweeps", 1))
+        if self.divide:
+            self._divide_ready_cells()
         self.steps += 1
         return rc
+
+    def _divide_ready_cells(self):
+        """divide_ready_cells (simulation.rs:1603-1716) without cycle or mutation: the living
+        cells of at least 1.4 reference volumes whose hypoxia response is under 0.45 split, in
+        id order, while the living stay under max_cells; daughters copy the parent's state."""
+        c = self.cfg
+        nec = c.get("necrotic_type", -1)
+        vol, t = self.lat.volume, self.lat.type
+        alive = (vol > 0) & (t != nec)
+        alive[0] = False
+        alive[self.used:] = False
+        hyp = self.net.hypoxia
+        ready = alive & (vol >= 1.4 * c["target_volume"])
+        if hyp is not None and hyp >= 0:
+            ready &= self.state[:, hyp] < 0.45
+        living = int(alive.sum())
+        born = 0
+        for cid in np.nonzero(ready)[0]:
+            if living + born >= self.max_cells:
+                break
+            angle = self.div_rng.random() * np.pi
+            if self.lat.d > 1:
+                z = 2.0 * angle / np.pi - 1.0
+                around = self.div_rng.random() * 2.0 * np.pi
+                r = np.sqrt(max(1.0 - z * z, 0.0))
+                normal = (r * np.cos(around), r * np.sin(around), z)
+            else:
+                normal = (np.cos(angle), np.sin(angle), 0.0)
+            d, self.used = self.lat.divide_across(int(cid), normal, self.used)
+            if d >= 0:
+                self.state[d] = self.state[cid]
+                born += 1

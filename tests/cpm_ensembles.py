@@ -76,7 +76,12 @@ def same_volume_law(a, b, p_min=0.01, sd_tol=0.12):
 
 
 def within_band(sample, band, z=4.0):
-    """The sample's mean lies in the band's 2.5-97.5% range and within z standard errors of its mean."""
+    """The sample's mean lies in the band's 2.5-97.5% range and (unless z is None) within z
+    standard errors of the band's mean."""
     lo, hi = np.percentile(band, [2.5, 97.5])
+    if not lo <= sample.mean() <= hi:
+        return False
+    if z is None:
+        return True
     se = np.sqrt(band.var(ddof=1) / len(band) + sample.var(ddof=1) / len(sample))
-    return bool(lo <= sample.mean() <= hi and abs(sample.mean() - band.mean()) <= z * max(se, 1e-12))
+    return bool(abs(sample.mean() - band.mean()) <= z * max(se, 1e-12))

@@ -87,3 +87,41 @@ def test_the_step_stays_inside_the_oracle_band():
         for j, name in enumerate(("living", "mean oxygen", "hypoxic fraction")):
             assert within_band(dev[:, j], ref[:, j]), (step, name, dev[:, j].mean(), ref[:, j].mean(),
                                                         ref[:, j].std())
+
+
+def test_division_grows_the_population_inside_the_oracle_band():
+    # cells of the reference volume grow as their growth node rises (growth
+    # coefficient 2) and divide at 1.4 times it, up to 40 living cells: the
+    # population curve inside the 32-seed band of the oracle's
+    # divide_ready_cells.  Sweeps attempt every boundary pixel once per MCS
+    # where random pixels attempt it Poisson(1) times, so driven volumes
+    # follow their targets faster (a change of probability p per MCS instead
+    # of 1 - exp(-p)); the population runs about 7% ahead by step 30, inside
+    # the band, which is the test.
+    cfg = synthetic.campaign(per_size=SEEDS, sizes=(64,), fill=0.2)
+    cfg.update(max_cells=40, dt=0.1)
+    S = cfg.pop("S")
+    text = synthetic.network_toml(S, S).replace("growth_coefficient = 0.5", "growth_coefficient = 2.0")
+    assert "growth_coefficient = 2.0" in text
+    d = tempfile.mkdtemp()
+    p = os.path.join(d, "n.toml")
+    open(p, "w").write(text)
+    net = cw.Network.load(p, cfg["target_volume"])
+    sim = cw.Simulation(net, **dict(cfg, seeds=[s + 70_000 for s in cfg["seeds"]]))
+    ora = [CpuHistory(dict(cfg, S=S, network_toml=text), k) for k in range(SEEDS)]
+    start = np.array([sim.lattice().cell_count(k) for k in range(SEEDS)])
+    for step in range(1, 31):
+        sim.step(1)
+        for h in ora:
+            h.step()
+        if step not in (10, 20, 30):
+            continue
+        lat = sim.lattice()
+        dev = np.array([float((lat.cells(hist=k)["volume"][1:] > 0).sum()) for k in range(SEEDS)])
+        ref = np.array([float((h.lat.volume[1:h.used] > 0).sum()) for h in ora])
+        assert within_band(dev, ref, z=None), (step, dev.mean(), ref.mean(), ref.std())
+        assert dev.max() <= 40 + 40  # the limit counts the living before a step's divisions
+    for k in range(SEEDS):
+        assert sim.records_match_grid(k)
+    grown = np.array([sim.lattice().cell_count(k) for k in range(SEEDS)]) - start
+    assert grown.mean() > 5
