@@ -18,6 +18,7 @@
 
 #include "cw_internal.cuh"
 #include "field_kernels.cuh"
+#include "tma.cuh"
 
 using namespace cw;
 
@@ -131,11 +132,13 @@ constexpr int RES_ROWS = 4;
 // omega D / den (both 0 on held pixels), and zeroes the correction.
 // The FP32 coefficients of the defect-correction sweep at a free pixel:
 // b = omega r / den and a = omega D / den, scaled by q = omega / den formed
-// in FP32 (they feed FP32 sweeps; r itself is FP64).
+// in FP32 by the fast reciprocal division (within 2 ulp; the same q for a and
+// b of a pixel, so the FP32 equation is only rescaled, and its error is the
+// FP32 solve's, removed by the FP64 residual; r itself is FP64).
 __device__ __forceinline__ void dc_coefficients(double om, double den, double r, double d, float &b, float &a) {
     b = a = 0.0f;
     if (den > 0.0) {
-        const float q = (float)om / (float)den;
+        const float q = __fdividef((float)om, (float)den);
         b = q * (float)r;
         a = q * (float)d;
     }
@@ -566,12 +569,344 @@ static int relax_fp64(cw_field_s *f, const cw_relax_opts &o, std::vector<Span> &
     return CW_OK;
 }
 
+// ------------------------------------------------------------------ residual by TMA tiles
+//
+// k_residual64 with its reads staged by the TMA engine.  A persistent block
+// per SM walks 128 x 16 tiles with a producer warp and 16 consumer warps:
+// the producer looks up the block's next tiles 32 at a time (a lane per
+// candidate: its record, then whether its history has settled), and for each
+// live one waits for a free stage and has the TMA engine bring in the tile's
+// values (with a ring of neighbours: x from x0 - 2, so that the box starts on
+// 16 bytes), held mask and per-pixel coefficients, with the tile's scalars
+// beside them.  A consumer warp takes one row of the tile, four pixels a
+// lane, folds its maximum into the history's with one atomic and frees the
+// stage.  No block-wide barrier after the start, and no global load on a
+// consumer's path but its outputs.  Per pixel the arithmetic is
+// k_residual64's, in the same order: the same bits.  Used for flat histories
+// whose width is a multiple of 16 (the held mask's rows must start on 16
+// bytes), the campaign's case.
+
+constexpr int RT_X = 128, RT_Y = 16;               // pixels of a tile
+constexpr int RT_CX = RT_X + 4, RT_CY = RT_Y + 2;  // its values' box: x0 - 2 .. x0 + 129, y0 - 1 .. y0 + 16
+constexpr int RT_CONSUMERS = RT_Y;                 // a warp per row of a tile
+constexpr int RT_THREADS = 32 * (RT_CONSUMERS + 1);
+constexpr int RT_MAX_STAGES = 6;
+constexpr int RT_MAPS = 5;                         // per history: values, held, sink, production, uptake
+constexpr int RT_SMEM = 200 * 1024;                // stages of every field fit in this
+
+__device__ int g_rt_wait_failed;
+
+// A tile as the host lays it out: its history, corner and the history's
+// shape and first pixel.
+struct RtTile {
+    int h, x0, y0, w, ht, pad;
+    long long off;
+};
+
+// What a stage holds besides the boxes: the tile, or h < 0 for no more tiles.
+struct RtStaged {
+    RtTile t;
+    double omega;
+};
+
+struct RtArgs {
+    const CUtensorMap *maps;  // RT_MAPS per history
+    const RtTile *tiles;
+    int ntiles;
+    int stages;               // tiles in flight per block
+    int stage;                // bytes of one stage
+    int o_held, o_ks, o_pr, o_up;  // offsets in a stage, -1 for an absent array
+    uint32_t tx;              // bytes one stage receives
+};
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+__global__ void __launch_bounds__(RT_THREADS, 1)
+    k_residual64_tiles(RtArgs a, FieldView fv, RelaxState *st, float *r32, float *inv32, float *dz, int skip_done) {
+    extern __shared__ __align__(128) unsigned char rsm[];
+    __shared__ __align__(8) uint64_t full[RT_MAX_STAGES], empty[RT_MAX_STAGES];
+    __shared__ RtStaged s_tile[RT_MAX_STAGES];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < a.stages; ++k) {
+            mbar_init(sh_addr(&full[k]), 1);
+            mbar_init(sh_addr(&empty[k]), RT_CONSUMERS);
+        }
+        mbar_init_fence();
+    }
+    __syncthreads();
+    if (warp == RT_CONSUMERS) {
+        // ---- producer
+        int it = 0;
+        bool stop = false;
+        for (int base = blockIdx.x; !stop; base += 32 * gridDim.x) {
+            const int t = base + lane * gridDim.x;
+            RtStaged c;
+            c.t = RtTile{-1, 0, 0, 0, 0, 0, 0};
+            c.omega = 0.0;
+            if (t < a.ntiles) {
+                c.t = a.tiles[t];
+                if (skip_done && st[c.t.h].done) c.t.h = -1;
+                else c.omega = st[c.t.h].omega;
+            }
+            unsigned live = __ballot_sync(0xffffffffu, c.t.h >= 0);
+            const bool last = __shfl_sync(0xffffffffu, t, 31) >= a.ntiles;
+            while (live && !stop) {
+                const int src = __ffs(live) - 1;
+                live &= live - 1;
+                RtStaged v;
+                v.t.h = __shfl_sync(0xffffffffu, c.t.h, src);
+                v.t.x0 = __shfl_sync(0xffffffffu, c.t.x0, src);
+                v.t.y0 = __shfl_sync(0xffffffffu, c.t.y0, src);
+                v.t.w = __shfl_sync(0xffffffffu, c.t.w, src);
+                v.t.ht = __shfl_sync(0xffffffffu, c.t.ht, src);
+                v.t.off = __shfl_sync(0xffffffffu, c.t.off, src);
+                v.omega = __shfl_sync(0xffffffffu, c.omega, src);
+                int ok = 1;
+                if (lane == 0) {
+                    const int slot = it % a.stages;
+                    if (it >= a.stages && !mbar_wait_bounded(sh_addr(&empty[slot]), (uint32_t)((it / a.stages) - 1) & 1u))
+                        ok = 0;
+                    if (ok) {
+                        s_tile[slot] = v;
+                        const uint32_t bar = sh_addr(&full[slot]);
+                        unsigned char *stage = rsm + (size_t)slot * a.stage;
+                        const CUtensorMap *m = a.maps + RT_MAPS * v.t.h;
+                        // the consumers' reads of this stage before the copies' writes
+                        fence_proxy_async_shared();
+                        mbar_expect_tx(bar, a.tx);
+                        tma_load_2d(stage, m, bar, v.t.x0 - 2, v.t.y0 - 1);
+                        tma_load_2d(stage + a.o_held, m + 1, bar, v.t.x0, v.t.y0);
+                        if (a.o_ks >= 0) tma_load_2d(stage + a.o_ks, m + 2, bar, v.t.x0, v.t.y0);
+                        if (a.o_pr >= 0) tma_load_2d(stage + a.o_pr, m + 3, bar, v.t.x0, v.t.y0);
+                        if (a.o_up >= 0) tma_load_2d(stage + a.o_up, m + 4, bar, v.t.x0, v.t.y0);
+                    } else {
+                        atomicExch(&g_rt_wait_failed, 1);
+                    }
+                }
+                ok = __shfl_sync(0xffffffffu, ok, 0);
+                if (!ok) stop = true;
+                ++it;
+            }
+            if (last && !stop) {
+                // no more tiles: the next stage says so
+                if (lane == 0) {
+                    const int slot = it % a.stages;
+                    if (it < a.stages || mbar_wait_bounded(sh_addr(&empty[slot]), (uint32_t)((it / a.stages) - 1) & 1u)) {
+                        s_tile[slot].t.h = -1;
+                        mbar_arrive(sh_addr(&full[slot]));
+                    } else {
+                        atomicExch(&g_rt_wait_failed, 1);
+                    }
+                }
+                stop = true;
+            }
+        }
+        return;
+    }
+    // ---- consumers: warp `warp` takes row `warp` of each tile
+    for (int it = 0;; ++it) {
+        const int slot = it % a.stages;
+        if (!mbar_wait_bounded(sh_addr(&full[slot]), (uint32_t)(it / a.stages) & 1u)) {
+            atomicExch(&g_rt_wait_failed, 1);
+            break;
+        }
+        const RtStaged v = s_tile[slot];
+        if (v.t.h < 0) break;
+        const unsigned char *stage = rsm + (size_t)slot * a.stage;
+        const double *sc = (const double *)stage;
+        const uint8_t *sheld = stage + a.o_held;
+        const double *sks = (const double *)(stage + a.o_ks), *spr = (const double *)(stage + a.o_pr),
+                     *sup = (const double *)(stage + a.o_up);
+        const double den4 = 4.0 * fv.d + fv.decay;
+        const int row = warp, y = v.t.y0 + row;
+        double worst = 0.0;
+        if (y < v.t.ht) {
+            const int64_t rowbase = v.t.off + (int64_t)y * v.t.w;
+#pragma unroll
+            for (int j = 0; j < RT_X / 32; ++j) {
+                const int col = lane + 32 * j, x = v.t.x0 + col, k = row * RT_X + col;
+                if (x >= v.t.w) continue;
+                const int64_t i = rowbase + x;
+                float r_out = 0.0f, inv_out = 0.0f;
+                if (!sheld[k]) {
+                    // pixel_sums64's order onto zero: x-1, x+1, y-1, y+1; a
+                    // pixel with all four neighbours real has real = 4, and
+                    // real d + decay is then one number
+                    const double *p = sc + (row + 1) * RT_CX + (col + 2);
+                    double sum, den;
+                    if (x > 0 && x + 1 < v.t.w && y > 0 && y + 1 < v.t.ht) {
+                        sum = 0.0 + p[-1];
+                        sum = sum + p[1];
+                        sum = sum + p[-RT_CX];
+                        sum = sum + p[RT_CX];
+                        den = den4;
+                    } else {
+                        double real = 0.0;
+                        sum = 0.0;
+                        if (x > 0) { sum += p[-1]; real += 1.0; }
+                        if (x + 1 < v.t.w) { sum += p[1]; real += 1.0; }
+                        if (y > 0) { sum += p[-RT_CX]; real += 1.0; }
+                        if (y + 1 < v.t.ht) { sum += p[RT_CX]; real += 1.0; }
+                        den = real * fv.d + fv.decay;
+                    }
+                    if (a.o_ks >= 0) den = den + sks[k];
+                    const double cv = p[0];
+                    // add_sources' order
+                    double t = fv.d * sum + fv.source;
+                    if (a.o_pr >= 0) t = t + spr[k];
+                    if (a.o_up >= 0) t = t - sup[k];
+                    double r = t - den * cv;
+                    if (fv.floor && cv <= 0.0 && r < 0.0) r = 0.0;
+                    worst = fmax(worst, fabs(r));
+                    dc_coefficients(v.omega, den, r, fv.d, r_out, inv_out);
+                }
+                if (r32) r32[i] = r_out;
+                if (inv32) inv32[i] = inv_out;
+                if (dz) dz[i] = 0.0f;
+            }
+        }
+        worst = warp_max(worst);
+        __syncwarp();
+        if (lane == 0) {
+            if (worst > 0.0) atomic_max_nonneg(&st[v.t.h].resid, worst);
+            mbar_arrive(sh_addr(&empty[slot]));
+        }
+    }
+}
+
+// The tensor maps and tiles of k_residual64_tiles for a field, built where
+// every history allows it, with the arrays they were built on.
+struct ResTiles {
+    bool ok = false;
+    CUtensorMap *maps = nullptr;
+    RtTile *tiles = nullptr;
+    RtArgs args{};
+    int grid = 0, smem = 0;
+    const void *built_on[RT_MAPS] = {};
+
+    void release() {
+        dfree(maps);
+        dfree(tiles);
+        ok = false;
+    }
+};
+
+static bool rt_matches(const ResTiles &rt, const FieldView &fv) {
+    const void *now[RT_MAPS] = {fv.c, fv.held, fv.ks, fv.pr, fv.up};
+    for (int m = 0; m < RT_MAPS; ++m)
+        if (now[m] != rt.built_on[m]) return false;
+    return rt.ok;
+}
+
+static int rt_prepare(cw_field_s *f, ResTiles &rt) {
+    const FieldView fv = view(f);
+    if (rt.ok && rt_matches(rt, fv)) return CW_OK;
+    rt.release();
+    const Geom &g = f->g;
+    for (uint32_t k = 0; k < g.nh; ++k)
+        if (g.d[k] != 1 || g.w[k] % 16 != 0 || g.off[k] % 16 != 0) return CW_OK;
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc) return CW_OK;
+    // the stage: values, held mask, then each present coefficient array
+    RtArgs &a = rt.args;
+    int at = ((RT_CX * RT_CY * 8) + 127) / 128 * 128;
+    a.o_held = at;
+    at += RT_X * RT_Y;
+    a.tx = RT_CX * RT_CY * 8 + RT_X * RT_Y;
+    const void *arrays[3] = {fv.ks, fv.pr, fv.up};
+    int *slots[3] = {&a.o_ks, &a.o_pr, &a.o_up};
+    for (int m = 0; m < 3; ++m) {
+        *slots[m] = -1;
+        if (!arrays[m]) continue;
+        *slots[m] = at;
+        at += RT_X * RT_Y * 8;
+        a.tx += RT_X * RT_Y * 8;
+    }
+    a.stage = at;
+    a.stages = std::min(RT_MAX_STAGES, RT_SMEM / a.stage);
+    if (a.stages < 2) return CW_OK;
+    rt.smem = a.stages * a.stage;
+    std::vector<CUtensorMap> maps((size_t)RT_MAPS * g.nh);
+    std::memset(maps.data(), 0, maps.size() * sizeof(CUtensorMap));
+    for (uint32_t k = 0; k < g.nh; ++k) {
+        for (int m = 0; m < RT_MAPS; ++m) {
+            const void *base = m == 0 ? (const void *)fv.c : m == 1 ? (const void *)fv.held : arrays[m - 2];
+            if (!base) continue;
+            const bool u8 = m == 1;
+            const size_t es = u8 ? 1 : 8;
+            cuuint64_t dim[2] = {(cuuint64_t)g.w[k], (cuuint64_t)g.h[k]};
+            cuuint64_t stride[1] = {(cuuint64_t)g.w[k] * es};
+            cuuint32_t box[2] = {m == 0 ? (cuuint32_t)RT_CX : (cuuint32_t)RT_X,
+                                 m == 0 ? (cuuint32_t)RT_CY : (cuuint32_t)RT_Y};
+            cuuint32_t estride[2] = {1, 1};
+            CUresult r = enc(&maps[(size_t)RT_MAPS * k + m],
+                             u8 ? CU_TENSOR_MAP_DATA_TYPE_UINT8 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2,
+                             (void *)((const char *)base + (size_t)g.off[k] * es), dim, stride, box, estride,
+                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+            if (r != CUDA_SUCCESS) return CW_OK;  // k_residual64 serves
+        }
+    }
+    std::vector<RtTile> tiles;
+    for (uint32_t k = 0; k < g.nh; ++k)
+        for (int y = 0; y < (int)g.h[k]; y += RT_Y)
+            for (int x = 0; x < (int)g.w[k]; x += RT_X)
+                tiles.push_back(RtTile{(int)k, x, y, (int)g.w[k], (int)g.h[k], 0, (long long)g.off[k]});
+    CW_CUDA(cudaFuncSetAttribute((const void *)k_residual64_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 RT_SMEM));
+    int per_sm = 0, dev = 0, nsm = 0;
+    CW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)k_residual64_tiles, RT_THREADS,
+                                                          rt.smem));
+    if (per_sm < 1) return CW_OK;
+    CW_CUDA(cudaGetDevice(&dev));
+    CW_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    int rc;
+    if ((rc = dalloc(&rt.maps, maps.size())) != CW_OK) return rc;
+    if ((rc = dalloc(&rt.tiles, tiles.size())) != CW_OK) return rc;
+    CW_CUDA(cudaMemcpyAsync(rt.maps, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice,
+                            stream()));
+    CW_CUDA(cudaMemcpyAsync(rt.tiles, tiles.data(), tiles.size() * sizeof(RtTile), cudaMemcpyHostToDevice,
+                            stream()));
+    CW_CUDA(cudaStreamSynchronize(stream()));
+    a.maps = rt.maps;
+    a.tiles = rt.tiles;
+    a.ntiles = (int)tiles.size();
+    rt.grid = std::min<int>(a.ntiles, per_sm * nsm);
+    const void *on[RT_MAPS] = {fv.c, fv.held, fv.ks, fv.pr, fv.up};
+    for (int m = 0; m < RT_MAPS; ++m) rt.built_on[m] = on[m];
+    rt.ok = true;
+    return CW_OK;
+}
+
+static int rt_wait_failed();
+
+// Whether a staged copy of the FP32 sweeps or of the residual timed out.
+static int dc_waits_failed() {
+    int rc = sor32_wait_failed();
+    return rc != CW_OK ? rc : rt_wait_failed();
+}
+
+static int rt_wait_failed() {
+    int v = 0;
+    CW_CUDA(cudaMemcpyFromSymbol(&v, g_rt_wait_failed, sizeof v));
+    if (v) {
+        const int zero = 0;
+        CW_CUDA(cudaMemcpyToSymbol(g_rt_wait_failed, &zero, sizeof zero));
+        return fail(CW_ERR_TIMEOUT, "a residual tile's copy did not land in time");
+    }
+    return CW_OK;
+}
+
 // Launch plans and the FP32 solver of the defect-correction solve, built on a
 // field's first FP32 solve and kept: no allocation in later solves, so that
 // a whole step can be captured in a CUDA graph.
 struct DcCache {
     Plan pr, prow;
     Sor32 solver;
+    ResTiles rt;
     int depth = -1, window = 0;
     std::vector<double> omega;
     double *d_omega = nullptr;  // per history, for the state initialisation on the device
@@ -611,6 +946,7 @@ static int dc_prepare(cw_field_s *f, int depth, int window, const std::vector<do
         c->window = window;
         c->omega.clear();
     }
+    if ((rc = rt_prepare(f, c->rt)) != CW_OK) return rc;
     if (c->omega != om) {
         std::vector<float> omf(om.begin(), om.end());
         CW_CUDA(cudaMemcpyAsync(c->solver.omega, omf.data(), sizeof(float) * nh, cudaMemcpyHostToDevice, stream()));
@@ -620,6 +956,16 @@ static int dc_prepare(cw_field_s *f, int depth, int window, const std::vector<do
     }
     *out = c;
     return CW_OK;
+}
+
+// The defect-correction solve's residual: by TMA tiles where they were built
+// on the field's current arrays, else k_residual64.
+static void dc_residual(DcCache *c, const FieldView &fv, uint32_t nh, RelaxState *d_st, float *r32, float *inv32,
+                        float *dz) {
+    if (rt_matches(c->rt, fv))
+        k_residual64_tiles<<<c->rt.grid, RT_THREADS, c->rt.smem, stream()>>>(c->rt.args, fv, d_st, r32, inv32, dz, 1);
+    else
+        k_residual64<<<c->prow.nblocks, T, 0, stream()>>>(fv, c->prow.d_blk, (int)nh, d_st, r32, inv32, dz, 1);
 }
 
 // One outer iteration: the convergence test, `inner` FP32 sweeps, the fused
@@ -637,7 +983,7 @@ static int dc_outer(cw_field_s *f, DcCache *c, RelaxState *d_st, int inner, int6
         // zeroing: the next solve's first launch does not read it)
         int rc = c->solver.sweeps(f, inner, done_ptr, stride, start, true);
         if (rc != CW_OK) return rc;
-        k_residual64<<<c->prow.nblocks, T, 0, stream()>>>(fv, c->prow.d_blk, nh, d_st, f->r32, nullptr, nullptr, 1);
+        dc_residual(c, fv, nh, d_st, f->r32, nullptr, nullptr);
         CW_LAUNCHED();
         return CW_OK;
     }
@@ -666,7 +1012,7 @@ static int relax_fp32dc(cw_field_s *f, const cw_relax_opts &o, RelaxState *d_st,
     int64_t max_outer = o.max_sweeps / inner + 2;
     int queue = 2;
     // the first residual also sets the inverse diagonal and zeroes d32a
-    k_residual64<<<c->prow.nblocks, T, 0, stream()>>>(fv, c->prow.d_blk, nh, d_st, f->r32, f->inv32, f->d32a, 1);
+    dc_residual(c, fv, nh, d_st, f->r32, f->inv32, f->d32a);
     CW_LAUNCHED();
     float *start = f->d32a;
     while (outer < max_outer) {
@@ -674,7 +1020,7 @@ static int relax_fp32dc(cw_field_s *f, const cw_relax_opts &o, RelaxState *d_st,
             if ((rc = dc_outer(f, c, d_st, inner, o.max_sweeps, start)) != CW_OK) return rc;
         CW_CUDA(cudaMemcpyAsync(hs.data(), d_st, sizeof(RelaxState) * nh, cudaMemcpyDeviceToHost, stream()));
         CW_CUDA(cudaStreamSynchronize(stream()));
-        if ((rc = sor32_wait_failed()) != CW_OK) return rc;
+        if ((rc = dc_waits_failed()) != CW_OK) return rc;
         bool all = true;
         for (uint32_t k = 0; k < nh; ++k) all = all && hs[k].done;
         if (all) break;
@@ -703,7 +1049,7 @@ int field_relax_enqueue(cw_field_s *f, const cw_relax_opts *opts, int outer, flo
     k_dc_state_init<<<(nh + 63) / 64, 64, 0, stream()>>>(d_st, nh, c->d_omega, opts->tolerance);
     CW_LAUNCHED();
     FieldView fv = view(f);
-    k_residual64<<<c->prow.nblocks, T, 0, stream()>>>(fv, c->prow.d_blk, nh, d_st, f->r32, f->inv32, f->d32a, 1);
+    dc_residual(c, fv, nh, d_st, f->r32, f->inv32, f->d32a);
     CW_LAUNCHED();
     float *start = f->d32a;
     for (int q = 0; q < outer; ++q) {
@@ -747,7 +1093,7 @@ int field_relax_collect(cw_field_s *f, std::vector<cw_relax_stats> &out, bool &a
     std::vector<RelaxState> hs(nh);
     CW_CUDA(cudaMemcpyAsync(hs.data(), f->stats, sizeof(RelaxState) * nh, cudaMemcpyDeviceToHost, stream()));
     CW_CUDA(cudaStreamSynchronize(stream()));
-    int rc = sor32_wait_failed();
+    int rc = dc_waits_failed();
     if (rc != CW_OK) return rc;
     out.resize(nh);
     all_settled = true;
@@ -802,6 +1148,7 @@ int cw_field_destroy(cw_field f) {
         c->solver.release();
         c->pr.release();
         c->prow.release();
+        c->rt.release();
         dfree(c->d_omega);
         delete c;
     }
@@ -1172,7 +1519,7 @@ extern "C" int cw_field_time_inner(cw_field f, int32_t sweeps, int32_t depth, in
     f->last_inner = solver.result();
     solver.release();
     prow.release();
-    return sor32_wait_failed();
+    return dc_waits_failed();
 }
 
 extern "C" int cw_field_inner_correction(cw_field f, uint32_t hist, float *out) {

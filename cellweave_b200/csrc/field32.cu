@@ -30,13 +30,12 @@
 //
 // Between warps, each warp publishes its top and bottom rows in shared memory
 // after every half-sweep (double-buffered, so one barrier per half-sweep).
-#include <cuda.h>
-#include <cudaTypedefs.h>
 
 #include <mutex>
 
 #include "cw_internal.cuh"
 #include "field_kernels.cuh"
+#include "tma.cuh"
 
 namespace cw {
 namespace {
@@ -153,48 +152,7 @@ constexpr int WROWS = WY / WWARPS;   // rows per warp
 constexpr int STAGE = WX * WY;       // floats per array of the staged window
 constexpr int EDGE_F4 = 2 * WWARPS * 2 * (WX / 4);
 constexpr size_t WIDE_SMEM = (size_t)3 * STAGE * sizeof(float) + (size_t)EDGE_F4 * sizeof(float4);
-constexpr unsigned long long WAIT_NS = 2000000000ull;  // a stage that has not landed in 2 s is an error
-
 __device__ int g_wide_wait_failed;
-
-__device__ __forceinline__ uint32_t sh_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ uint64_t global_ns() {
-    uint64_t t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-// The phase `parity` of the stage's barrier, waited for WAIT_NS at most.
-__device__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity) {
-    if (mbar_try_wait(bar, parity)) return true;
-    const uint64_t t0 = global_ns();
-    for (;;) {
-        if (mbar_try_wait(bar, parity)) return true;
-        if (global_ns() - t0 > WAIT_NS) return false;
-    }
-}
-
-// One 128 x 64 box of a history's array into shared memory, completing on `bar`.
-__device__ __forceinline__ void tma_box(float *dst, const CUtensorMap *map, uint32_t bar, int x, int y) {
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
-        :
-        : "r"(sh_addr(dst)), "l"((uint64_t)map), "r"(x), "r"(y), "r"(bar)
-        : "memory");
-}
 
 // The first window at or after `t`, in steps of `step`, whose history is not settled.
 __device__ __forceinline__ int next_live(int t, int ntiles, int step, const int4 *tiles, const int32_t *done,
@@ -278,18 +236,16 @@ __global__ void __launch_bounds__(32 * WWARPS, 2)
             w.off = off[w.tl.x];
             w.omc = 1.f - omega[w.tl.x];
             const CUtensorMap *m = maps + 4 * w.tl.x;
-            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
-                         "r"((uint32_t)(boxes * STAGE * sizeof(float)))
-                         : "memory");
-            if (!zero_start) tma_box(smem, m + src_map, bar, w.tl.y, w.tl.z);
-            tma_box(smem + STAGE, m + 2, bar, w.tl.y, w.tl.z);
-            tma_box(smem + 2 * STAGE, m + 3, bar, w.tl.y, w.tl.z);
+            mbar_expect_tx(bar, (uint32_t)(boxes * STAGE * sizeof(float)));
+            if (!zero_start) tma_load_2d(smem, m + src_map, bar, w.tl.y, w.tl.z);
+            tma_load_2d(smem + STAGE, m + 2, bar, w.tl.y, w.tl.z);
+            tma_load_2d(smem + 2 * STAGE, m + 3, bar, w.tl.y, w.tl.z);
         }
         s_info[slot] = w;
     };
     if (threadIdx.x == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        mbar_init(bar, 1);
+        mbar_init_fence();
         s_fail = 0;
         stage_next(blockIdx.x, 0);
     }
@@ -322,7 +278,7 @@ __global__ void __launch_bounds__(32 * WWARPS, 2)
         parity ^= 1u;
         if (threadIdx.x == 0) {
             // the generic-proxy reads of the stage before the async-proxy writes
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            fence_proxy_async_shared();
             stage_next(info.tl.w + gridDim.x, slot ^ 1);
         }
         const float omc = info.omc;
@@ -468,19 +424,6 @@ void axis_starts(int n, int win, int depth, std::vector<int> &out) {
     for (int k = 1; k <= last; ++k) out.push_back(k * step);
 }
 
-PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    static std::once_flag once;
-    std::call_once(once, [] {
-        void *p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
-    });
-    return fn;
-}
-
 // The wide kernel's tensor maps, windows and grid, if every history allows it.
 int wide_init(Sor32 &s, cw_field_s *f) {
     s.wide = false;
@@ -488,7 +431,7 @@ int wide_init(Sor32 &s, cw_field_s *f) {
     for (uint32_t k = 0; k < g.nh; ++k)
         if (g.d[k] != 1 || g.w[k] % 4 != 0 || g.off[k] % 4 != 0) return CW_OK;
     if (s.depth % 2 != 0 || s.depth > 8) return CW_OK;
-    PFN_cuTensorMapEncodeTiled_v12000 enc = encode_fn();
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
     if (!enc) return CW_OK;
     std::vector<CUtensorMap> maps(4 * (size_t)g.nh);
     float *arrays[4] = {f->d32a, f->d32b, f->r32, f->inv32};
