@@ -68,15 +68,26 @@ int Plan::build(const std::vector<int64_t> &per, int threads) {
     blk.assign(nh + 1, 0);
     for (uint32_t k = 0; k < nh; ++k) blk[k + 1] = blk[k] + (int32_t)((per[k] + threads - 1) / threads);
     nblocks = blk[nh];
-    if (!d_blk) {
-        int rc = dalloc(&d_blk, nh + 1);
+    // on the device: the prefix, then each block's history (one load for a
+    // kernel to find its history)
+    table = blk;
+    table.resize((size_t)nh + 1 + (size_t)nblocks);
+    for (uint32_t k = 0; k < nh; ++k)
+        for (int32_t b = blk[k]; b < blk[k + 1]; ++b) table[nh + 1 + (size_t)b] = (int32_t)k;
+    if (!d_blk || cap < table.size()) {
+        dfree(d_blk);
+        int rc = dalloc(&d_blk, table.size());
         if (rc != CW_OK) return rc;
+        cap = table.size();
     }
-    CW_CUDA(cudaMemcpyAsync(d_blk, blk.data(), sizeof(int32_t) * (nh + 1), cudaMemcpyHostToDevice, stream()));
+    CW_CUDA(cudaMemcpyAsync(d_blk, table.data(), sizeof(int32_t) * table.size(), cudaMemcpyHostToDevice, stream()));
     return CW_OK;
 }
 
-void Plan::release() { dfree(d_blk); }
+void Plan::release() {
+    dfree(d_blk);
+    cap = 0;
+}
 
 }  // namespace cw
 

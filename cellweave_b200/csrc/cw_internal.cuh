@@ -68,20 +68,16 @@ struct Plan {
     uint32_t nh = 0;
     int32_t nblocks = 0;
     std::vector<int32_t> blk;     // nh + 1
+    std::vector<int32_t> table;   // what d_blk holds (kept for the asynchronous copy)
     std::vector<int64_t> items;   // per history
-    int32_t *d_blk = nullptr;     // nh + 1
+    int32_t *d_blk = nullptr;     // nh + 1 prefix entries, then the history of each of the nblocks blocks
+    size_t cap = 0;               // entries allocated at d_blk
     int build(const std::vector<int64_t> &items_per_history, int threads);
     void release();
 };
 
-__device__ __forceinline__ int plan_history(const int32_t *blk, int nh, int b) {
-    int lo = 0, hi = nh - 1;
-    while (lo < hi) {
-        int mid = (lo + hi + 1) >> 1;
-        if (__ldg(blk + mid) <= b) lo = mid; else hi = mid - 1;
-    }
-    return lo;
-}
+// The history of block b of a plan (Plan::build lays the table after the prefix).
+__device__ __forceinline__ int plan_history(const int32_t *blk, int nh, int b) { return __ldg(blk + nh + 1 + b); }
 
 // ------------------------------------------------------------------ Philox4x32-10
 // Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy as 1, 2, 3"

@@ -409,16 +409,23 @@ __global__ void __launch_bounds__(T) k_cpm_pass(LatView L, Tables tabs, const in
             int nvn = 0;
             Vn vn;
             Moore mo;
+            // every neighbour read at once (no read waits on another's test)
             if (!L.copy_moore) {
                 vn = vn_of(dm, x, y, z);
                 nvn = vn.count();
+                int32_t nb[6];
 #pragma unroll
-                for (int q = 0; q < 6; ++q)
-                    if (vn.has(q)) edge = edge || g[i + vn.step(q)] != src;
+                for (int q = 0; q < 6; ++q) nb[q] = vn.has(q) ? g[i + vn.step(q)] : src;
+#pragma unroll
+                for (int q = 0; q < 6; ++q) edge |= nb[q] != src;
             } else {
                 mo = moore_of(dm, x, y, z);
                 nvn = mo.count();
-                for (unsigned m = mo.mask; m; m &= m - 1u) edge = edge || g[i + mo.step(__ffs(m) - 1)] != src;
+                int32_t nb[27];
+#pragma unroll
+                for (int q = 0; q < 27; ++q) nb[q] = q != 13 && ((mo.mask >> q) & 1u) ? g[i + mo.step(q)] : src;
+#pragma unroll
+                for (int q = 0; q < 27; ++q) edge |= nb[q] != src;
             }
             if (edge && src != OBST) {
                 const uint2 key = L.keys[h];
