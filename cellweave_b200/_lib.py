@@ -63,6 +63,11 @@ class TermSpec(C.Structure):
                 ("hill_n", C.c_double), ("hill_k", C.c_double), ("param", C.c_double), ("has_hill", C.c_int32)]
 
 
+class Mutation(C.Structure):
+    _fields_ = [("node", C.c_int32), ("term", C.c_int32), ("kind", C.c_int32), ("change", C.c_int32),
+                ("value", C.c_double), ("source", C.c_int32), ("pad", C.c_int32)]
+
+
 class FitConfig(C.Structure):
     _fields_ = [("dcoef", C.c_double), ("uptake", C.c_double * 3), ("vessel_value", C.c_double),
                 ("vessel_x", C.c_int32), ("egf", C.c_double), ("signal_dcoef", C.c_double),
@@ -155,6 +160,9 @@ SIGNATURES = {
     "cw_network_step_batch": (C.c_int, [P, I64, P, P, D, I32]),
     "cw_network_backward_batch": (C.c_int, [P, I64, P, P, D, I32, P, P, I32, P]),
     "cw_network_mechanics_batch": (C.c_int, [P, I64, P, P, P]),
+    "cw_network_mutate": (C.c_int, [P, D, D, P, P]),
+    "cw_network_rewire": (C.c_int, [P, P, P, P]),
+    "cw_network_step_clones": (C.c_int, [I32, P, I64, P, P, P, D, I32]),
     "cw_sim_create": (C.c_int, [P, P, P]),
     "cw_sim_destroy": (C.c_int, [P]),
     "cw_sim_step": (C.c_int, [P, U32]),

@@ -8,6 +8,7 @@
 // stage slope and accumulated slope in shared memory laid out [node][thread],
 // so dynamic node indices cost a shared-memory access and no bank conflict.
 // Built without fused multiply-add: the sums round as the reference's do.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -26,28 +27,13 @@ constexpr int MAXS = 32;
 
 constexpr int RT = 64;  // threads (cells) per block
 
-// state: [S][ncells] (node-major, coalesced); inputs: [6][ncells].
-// alive (optional): cells whose entry is zero are left as they are.
-__global__ void __launch_bounds__(RT) k_rk4(NetDev N, double *state, const double *inputs, int64_t ncells,
-                                            int64_t state_stride, int64_t input_stride, double dt, int substeps,
-                                            const uint8_t *alive) {
-    extern __shared__ double sm[];
+// One cell's `substeps` RK4 steps (rk4, network.rs:777-799) on its column of
+// the block's shared arrays (xs: state, ms: midpoint, ks: stage slope, as:
+// accumulated slope, each [node][RT]), under the terms at sterm/spar/sptr.
+__device__ __forceinline__ void rk4_cell(const NetDev &N, const int4 *sterm, const double4 *spar, const int32_t *sptr,
+                                         double *xs, double *ms, double *ks, double *as, const double *in, double dt,
+                                         int substeps) {
     const int S = N.S;
-    double *x = sm, *mid = sm + S * RT, *kk = sm + 2 * S * RT, *acc = sm + 3 * S * RT;
-    int4 *sterm = (int4 *)(sm + 4 * S * RT);
-    double4 *spar = (double4 *)(sterm + N.nterms);
-    int32_t *sptr = (int32_t *)(spar + N.nterms);
-    for (int t = threadIdx.x; t < N.nterms; t += RT) { sterm[t] = N.term[t]; spar[t] = N.par[t]; }
-    for (int t = threadIdx.x; t <= S; t += RT) sptr[t] = N.node_ptr[t];
-    __syncthreads();
-    int64_t c = (int64_t)blockIdx.x * RT + threadIdx.x;
-    if (c >= ncells) return;
-    if (alive && !alive[c]) return;
-    const int tid = threadIdx.x;
-    double in[6];
-    for (int q = 0; q < 6; ++q) in[q] = inputs[q * input_stride + c];
-    double *xs = x + tid, *ms = mid + tid, *ks = kk + tid, *as = acc + tid;
-    for (int i = 0; i < S; ++i) xs[i * RT] = state[i * state_stride + c];
     for (int sub = 0; sub < substeps; ++sub) {
         // k1 at x
         derivatives(N, sterm, spar, sptr, xs, in, ks, RT);
@@ -75,7 +61,51 @@ __global__ void __launch_bounds__(RT) k_rk4(NetDev N, double *state, const doubl
             xs[i * RT] = fmin(fmax(xs[i * RT] + delta, 0.0), 1.0);
         }
     }
+}
+
+// state: [S][ncells] (node-major, coalesced); inputs: [6][ncells].
+// alive (optional): cells whose entry is zero are left as they are.
+__global__ void __launch_bounds__(RT) k_rk4(NetDev N, double *state, const double *inputs, int64_t ncells,
+                                            int64_t state_stride, int64_t input_stride, double dt, int substeps,
+                                            const uint8_t *alive) {
+    extern __shared__ double sm[];
+    const int S = N.S;
+    double *x = sm, *mid = sm + S * RT, *kk = sm + 2 * S * RT, *acc = sm + 3 * S * RT;
+    int4 *sterm = (int4 *)(sm + 4 * S * RT);
+    double4 *spar = (double4 *)(sterm + N.nterms);
+    int32_t *sptr = (int32_t *)(spar + N.nterms);
+    for (int t = threadIdx.x; t < N.nterms; t += RT) { sterm[t] = N.term[t]; spar[t] = N.par[t]; }
+    for (int t = threadIdx.x; t <= S; t += RT) sptr[t] = N.node_ptr[t];
+    __syncthreads();
+    int64_t c = (int64_t)blockIdx.x * RT + threadIdx.x;
+    if (c >= ncells) return;
+    if (alive && !alive[c]) return;
+    const int tid = threadIdx.x;
+    double in[6];
+    for (int q = 0; q < 6; ++q) in[q] = inputs[q * input_stride + c];
+    double *xs = x + tid, *ms = mid + tid, *ks = kk + tid, *as = acc + tid;
+    for (int i = 0; i < S; ++i) xs[i * RT] = state[i * state_stride + c];
+    rk4_cell(N, sterm, spar, sptr, xs, ms, ks, as, in, dt, substeps);
     for (int i = 0; i < S; ++i) state[i * state_stride + c] = xs[i * RT];
+}
+
+// The same for cells of many networks: cell c under nets[clone[c]], its
+// terms read from global memory (a network's tables are a few KB: they stay
+// in L1 across the block's cells of that network).
+__global__ void __launch_bounds__(RT) k_rk4_clones(const NetDev *nets, const int32_t *clone, int S, double *state,
+                                                   const double *inputs, int64_t ncells, double dt, int substeps) {
+    extern __shared__ double sm[];
+    double *x = sm, *mid = sm + S * RT, *kk = sm + 2 * S * RT, *acc = sm + 3 * S * RT;
+    int64_t c = (int64_t)blockIdx.x * RT + threadIdx.x;
+    if (c >= ncells) return;
+    const NetDev N = nets[clone[c]];
+    const int tid = threadIdx.x;
+    double in[6];
+    for (int q = 0; q < 6; ++q) in[q] = inputs[q * ncells + c];
+    double *xs = x + tid, *ms = mid + tid, *ks = kk + tid, *as = acc + tid;
+    for (int i = 0; i < S; ++i) xs[i * RT] = state[i * ncells + c];
+    rk4_cell(N, N.term, N.par, N.node_ptr, xs, ms, ks, as, in, dt, substeps);
+    for (int i = 0; i < S; ++i) state[i * ncells + c] = xs[i * RT];
 }
 
 // mechanics, network.rs:811-821.
@@ -93,6 +123,64 @@ __global__ void k_mechanics(const double *state, int64_t ncells, int64_t stride,
 size_t rk4_smem(const cw_network_s *n) {
     return sizeof(double) * 4 * n->S * RT + n->nterms * (sizeof(int4) + sizeof(double4)) + sizeof(int32_t) * (n->S + 1);
 }
+
+// The device copies of a network's host tables (h_ptr, h_term, h_par).
+int network_upload(cw_network_s *n) {
+    n->nterms = (int32_t)n->h_term.size();
+    int rc;
+    if ((rc = dalloc(&n->node_ptr, n->S + 1)) || (rc = dalloc(&n->term, n->nterms)) ||
+        (rc = dalloc(&n->par, n->nterms)))
+        return rc;
+    CW_CUDA(cudaMemcpy(n->node_ptr, n->h_ptr.data(), sizeof(int32_t) * (n->S + 1), cudaMemcpyHostToDevice));
+    if (n->nterms > 0) {
+        CW_CUDA(cudaMemcpy(n->term, n->h_term.data(), sizeof(int4) * n->nterms, cudaMemcpyHostToDevice));
+        CW_CUDA(cudaMemcpy(n->par, n->h_par.data(), sizeof(double4) * n->nterms, cudaMemcpyHostToDevice));
+    }
+    size_t smem = rk4_smem(n);
+    if (smem > 48 * 1024 &&
+        cudaFuncSetAttribute(k_rk4, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return fail(CW_ERR_CONFIG, "the network is too large for one block's shared memory");
+    return CW_OK;
+}
+
+// A network like `n` with host tables to be changed and uploaded: every
+// field but the device copies.
+cw_network_s *network_derive(const cw_network_s *n) {
+    cw_network_s *m = new cw_network_s();
+    m->S = n->S;
+    m->names = n->names;
+    m->initial = n->initial;
+    std::memcpy(m->roles, n->roles, sizeof m->roles);
+    m->growth_coefficient = n->growth_coefficient;
+    m->lambda_volume = n->lambda_volume;
+    m->max_target = n->max_target;
+    m->reference_volume = n->reference_volume;
+    m->h_ptr = n->h_ptr;
+    m->h_term = n->h_term;
+    m->h_par = n->h_par;
+    return m;
+}
+
+// `(u * n as f64) as usize`, at most n - 1 (network.rs:488, 521): Rust's
+// cast truncates and saturates (below zero and NaN give 0).
+size_t pick_of(size_t n, double u) {
+    if (n == 0) return 0;
+    const double v = u * (double)n;
+    if (!(v > 0.0)) return 0;
+    if (v >= (double)n) return n - 1;
+    return std::min<size_t>((size_t)v, n - 1);
+}
+
+// The node holding the term at global index t (terms in node order).
+int node_of_term(const cw_network_s *n, int32_t t) {
+    int i = 0;
+    while (i + 1 < n->S && n->h_ptr[i + 1] <= t) ++i;
+    return i;
+}
+
+constexpr double MUTATION_SPREAD = 2.0;  // network.rs:158
+constexpr double GAINED_RATE = 0.1;      // network.rs:163
+constexpr int REWIRED_INPUTS = 4;        // network.rs:169: oxygen, egf, crowding, stress
 
 }  // namespace
 
@@ -223,22 +311,13 @@ int cw_network_compile(int32_t nnodes, const char *const *names, const double *i
     n->lambda_volume = lambda_volume;
     n->max_target = max_target;
     n->reference_volume = reference_volume;
-    int rc;
-    if ((rc = dalloc(&n->node_ptr, nnodes + 1)) || (rc = dalloc(&n->term, nterms)) ||
-        (rc = dalloc(&n->par, nterms))) {
+    n->h_ptr = ptr;
+    n->h_term = tv;
+    n->h_par = pv;
+    int rc = network_upload(n);
+    if (rc != CW_OK) {
         cw_network_destroy(n);
         return rc;
-    }
-    CW_CUDA(cudaMemcpy(n->node_ptr, ptr.data(), sizeof(int32_t) * (nnodes + 1), cudaMemcpyHostToDevice));
-    if (nterms > 0) {
-        CW_CUDA(cudaMemcpy(n->term, tv.data(), sizeof(int4) * nterms, cudaMemcpyHostToDevice));
-        CW_CUDA(cudaMemcpy(n->par, pv.data(), sizeof(double4) * nterms, cudaMemcpyHostToDevice));
-    }
-    size_t smem = rk4_smem(n);
-    if (smem > 48 * 1024 && cudaFuncSetAttribute(k_rk4, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-                                cudaSuccess) {
-        cw_network_destroy(n);
-        return fail(CW_ERR_CONFIG, "the network is too large for one block's shared memory");
     }
     *out = n;
     return CW_OK;
@@ -304,6 +383,115 @@ int cw_network_mechanics_batch(cw_network n, int64_t ncells, const double *state
         for (int64_t c = 0; c < ncells; ++c) lambda[c] = n->lambda_volume;
     dfree(d_state);
     dfree(d_t);
+    return CW_OK;
+}
+
+int cw_network_mutate(cw_network n, double which, double how, cw_network *out, cw_mutation *rec) {
+    if (!out) return fail(CW_ERR_CONFIG, "no place for the mutated network");
+    *out = nullptr;
+    const size_t count = n->h_term.size();
+    if (count == 0) return fail(CW_ERR_NOT_FOUND, "a network without a single term has nothing a mutation could change");
+    const int32_t pick = (int32_t)pick_of(count, which);
+    const double factor = std::pow(MUTATION_SPREAD, 2.0 * how - 1.0);
+    cw_network_s *m = network_derive(n);
+    m->h_par[pick].x = m->h_par[pick].x * factor;
+    const int node = node_of_term(n, pick);
+    int rc = network_upload(m);
+    if (rc != CW_OK) {
+        cw_network_destroy(m);
+        return rc;
+    }
+    if (rec) *rec = cw_mutation{node, pick - n->h_ptr[node], n->h_term[pick].x, CW_CHANGE_SCALED, factor, 0, 0};
+    *out = m;
+    return CW_OK;
+}
+
+int cw_network_rewire(cw_network n, const double draws[5], cw_network *out, cw_mutation *rec) {
+    if (!out || !draws) return fail(CW_ERR_CONFIG, "rewiring takes five draws and a place for the network");
+    *out = nullptr;
+    const double mode = draws[0], which = draws[1], source = draws[2], sign = draws[3], how = draws[4];
+    cw_network_s *m = network_derive(n);
+    cw_mutation r{};
+    if (mode < 0.5) {
+        // a gained link, the node's last term
+        const int node = (int)pick_of((size_t)n->S, which);
+        const int s = (int)pick_of((size_t)(REWIRED_INPUTS + n->S), source);
+        const int32_t src = s < REWIRED_INPUTS ? -1 - s : s - REWIRED_INPUTS;
+        const double rate = GAINED_RATE * std::pow(MUTATION_SPREAD, 2.0 * how - 1.0);
+        const int32_t kind = sign < 0.5 ? CW_ACTIVATED_BY : CW_ACTIVATED_BY_ABSENCE_OF;
+        const int32_t at = m->h_ptr[node + 1];
+        m->h_term.insert(m->h_term.begin() + at, make_int4(kind, src, 0, 0));
+        m->h_par.insert(m->h_par.begin() + at, make_double4(rate, 0.0, 0.0, 0.0));
+        for (int i = node + 1; i <= n->S; ++i) m->h_ptr[i] += 1;
+        r = cw_mutation{node, at - n->h_ptr[node], kind, CW_CHANGE_GAINED, rate, src, 0};
+    } else {
+        const size_t count = n->h_term.size();
+        if (count == 0) {
+            delete m;
+            return fail(CW_ERR_NOT_FOUND, "a network without a single term has no term to lose");
+        }
+        const int32_t at = (int32_t)pick_of(count, which);
+        const int node = node_of_term(n, at);
+        r = cw_mutation{node, at - n->h_ptr[node], n->h_term[at].x, CW_CHANGE_LOST, 0.0, 0, 0};
+        m->h_term.erase(m->h_term.begin() + at);
+        m->h_par.erase(m->h_par.begin() + at);
+        for (int i = node + 1; i <= n->S; ++i) m->h_ptr[i] -= 1;
+    }
+    int rc = network_upload(m);
+    if (rc != CW_OK) {
+        cw_network_destroy(m);
+        return rc;
+    }
+    if (rec) *rec = r;
+    *out = m;
+    return CW_OK;
+}
+
+int cw_network_step_clones(int32_t nnets, const cw_network *nets, int64_t ncells, const int32_t *clone,
+                           double *state, const double *inputs, double dt, int32_t substeps) {
+    if (ncells <= 0) return CW_OK;
+    if (nnets <= 0 || !nets) return fail(CW_ERR_CONFIG, "no networks to step the cells under");
+    const int S = nets[0]->S;
+    std::vector<NetDev> dev(nnets);
+    for (int k = 0; k < nnets; ++k) {
+        if (!nets[k] || nets[k]->S != S) return fail(CW_ERR_CONFIG, "every network of a batch has the same nodes");
+        dev[k] = net_dev(nets[k]);
+    }
+    for (int64_t c = 0; c < ncells; ++c)
+        if (clone[c] < 0 || clone[c] >= nnets)
+            return fail(CW_ERR_CONFIG, "cell " + std::to_string(c) + " names network " + std::to_string(clone[c]) +
+                                           " of " + std::to_string(nnets));
+    const size_t smem = sizeof(double) * 4 * S * RT;
+    if (smem > 48 * 1024)
+        CW_CUDA(cudaFuncSetAttribute(k_rk4_clones, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    NetDev *d_nets;
+    int32_t *d_clone;
+    double *d_state, *d_in;
+    int rc;
+    if ((rc = dalloc(&d_nets, (size_t)nnets)) || (rc = dalloc(&d_clone, (size_t)ncells)) ||
+        (rc = dalloc(&d_state, (size_t)ncells * S)) || (rc = dalloc(&d_in, (size_t)ncells * 6)))
+        return rc;
+    std::vector<double> t((size_t)ncells * (S > 6 ? S : 6));
+    for (int64_t c = 0; c < ncells; ++c)
+        for (int i = 0; i < S; ++i) t[(size_t)i * ncells + c] = state[c * S + i];
+    CW_CUDA(cudaMemcpy(d_state, t.data(), sizeof(double) * ncells * S, cudaMemcpyHostToDevice));
+    for (int64_t c = 0; c < ncells; ++c)
+        for (int q = 0; q < 6; ++q) t[(size_t)q * ncells + c] = inputs[c * 6 + q];
+    CW_CUDA(cudaMemcpy(d_in, t.data(), sizeof(double) * ncells * 6, cudaMemcpyHostToDevice));
+    CW_CUDA(cudaMemcpy(d_nets, dev.data(), sizeof(NetDev) * nnets, cudaMemcpyHostToDevice));
+    CW_CUDA(cudaMemcpy(d_clone, clone, sizeof(int32_t) * ncells, cudaMemcpyHostToDevice));
+    k_rk4_clones<<<(unsigned)((ncells + RT - 1) / RT), RT, smem, stream()>>>(d_nets, d_clone, S, d_state, d_in, ncells,
+                                                                          dt, substeps);
+    CW_LAUNCHED();
+    CW_CUDA(cudaGetLastError());
+    CW_CUDA(cudaMemcpyAsync(t.data(), d_state, sizeof(double) * ncells * S, cudaMemcpyDeviceToHost, stream()));
+    CW_CUDA(cudaStreamSynchronize(stream()));
+    for (int64_t c = 0; c < ncells; ++c)
+        for (int i = 0; i < S; ++i) state[c * S + i] = t[(size_t)i * ncells + c];
+    dfree(d_nets);
+    dfree(d_clone);
+    dfree(d_state);
+    dfree(d_in);
     return CW_OK;
 }
 

@@ -15,6 +15,11 @@ struct cw_network_s {
     int32_t roles[7] = {-1, -1, -1, -1, -1, -1, -1};
     double growth_coefficient = 0.0, lambda_volume = 0.0, max_target = NAN;
     uint32_t reference_volume = 0;
+    // the compiled terms on the host (node_ptr, term, par below), for the
+    // mutations that derive a network from this one
+    std::vector<int32_t> h_ptr;
+    std::vector<int4> h_term;
+    std::vector<double4> h_par;
     // device copies of the compiled terms
     int32_t *node_ptr = nullptr;  // S + 1
     int4 *term = nullptr;         // (kind, source, has_hill, 0)

@@ -542,6 +542,55 @@ class Network:
              ptr(d_o2), int(nrates), ptr(d_rates))
         return adj, d_o2, d_rates[:int(nrates)]
 
+    INPUT_NAMES = ["oxygen", "egf", "crowding", "stress", "waste", "necrotic_factor"]
+    CHANGES = ["scaled", "gained", "lost"]
+
+    def _record(self, r):
+        """A Mutation (network.rs:171-199) as a dict, with its Display text."""
+        kind = TERM_KINDS[r.kind]
+        node = self.names[r.node]
+        change = self.CHANGES[r.change]
+        rec = dict(node=node, term=int(r.term), kind=kind, change=change)
+        if change == "scaled":
+            rec["factor"] = r.value
+            rec["text"] = f"{node} {kind} #{r.term} x{r.value:.2f}"
+        elif change == "gained":
+            src = self.INPUT_NAMES[-1 - r.source] if r.source < 0 else self.names[r.source]
+            rec.update(source=src, rate=r.value, text=f"{node} gains {kind} {src} @{r.value:.2f}")
+        else:
+            rec["text"] = f"{node} loses {kind} #{r.term}"
+        return rec
+
+    def mutate(self, which, how):
+        """Network::mutate (network.rs:479-501) on a copy: (daughter network, mutation record);
+        NotFoundError for a network without a single term."""
+        h, r = C.c_void_p(), _lib.Mutation()
+        call("cw_network_mutate", self._h, float(which), float(how), C.byref(h), C.byref(r))
+        return Network(h, self.names), self._record(r)
+
+    def rewire(self, draws):
+        """Network::rewire (network.rs:503-575) on a copy, draws = (mode, which, source, sign, how)."""
+        d = np.ascontiguousarray(draws, np.float64)
+        if d.shape != (5,):
+            raise ConfigError("rewiring takes five draws")
+        h, r = C.c_void_p(), _lib.Mutation()
+        call("cw_network_rewire", self._h, ptr(d), C.byref(h), C.byref(r))
+        return Network(h, self.names), self._record(r)
+
+    @staticmethod
+    def step_clones(nets, clone, state, inputs, dt, substeps=1):
+        """RK4 for cells of many networks at once: row c of state [ncells, S] steps under
+        nets[clone[c]] (the per-cell networks of an evolving run), in place."""
+        st = np.ascontiguousarray(state, np.float64)
+        ins = np.ascontiguousarray(inputs, np.float64)
+        cl = np.ascontiguousarray(clone, np.int32)
+        handles = (C.c_void_p * len(nets))(*[n.handle.value for n in nets])
+        call("cw_network_step_clones", len(nets), handles, st.shape[0], ptr(cl), ptr(st), ptr(ins), float(dt),
+             int(substeps))
+        if st is not state:
+            state[...] = st
+        return state
+
     def mechanics_batch(self, state):
         """mechanics (network.rs:811-821): target volumes and lambdas."""
         st = np.ascontiguousarray(state, np.float64)

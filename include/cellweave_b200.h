@@ -305,6 +305,37 @@ int cw_network_mechanics_batch(cw_network net, int64_t ncells, const double *sta
 int cw_network_backward_batch(cw_network net, int64_t ncells, const double *state, const double *inputs, double dt,
                               int32_t substeps, double *adjoint, double *d_oxygen, int32_t nrates, double *d_rates);
 
+/* ------------------------------------------------------------------ mutated networks
+ * A heritable change to a network (Mutation, network.rs:171-199). */
+enum { CW_CHANGE_SCALED = 0, CW_CHANGE_GAINED = 1, CW_CHANGE_LOST = 2 };
+typedef struct {
+    int32_t node;    /* the node whose terms changed */
+    int32_t term;    /* which of its terms, from zero in file order; a gained link is the last */
+    int32_t kind;    /* CW_ACTIVATED_BY ... */
+    int32_t change;  /* CW_CHANGE_* */
+    double value;    /* the factor of a scaled rate, or the rate of a gained link */
+    int32_t source;  /* a gained link's source: a node index, or -1 - input (oxygen, egf, crowding, stress) */
+    int32_t pad;
+} cw_mutation;
+/* Network::mutate (network.rs:479-501): one rate, picked by `which` among
+ * every node's terms in file order, scaled by 2^(2 how - 1); `which` and `how`
+ * are uniform draws in [0, 1) taken by the caller.  *out is a new network;
+ * `net` is unchanged.  CW_ERR_NOT_FOUND (and *out NULL) for a network
+ * without a single term. */
+int cw_network_mutate(cw_network net, double which, double how, cw_network *out, cw_mutation *rec);
+/* Network::rewire (network.rs:503-575), draws = (mode, which, source, sign,
+ * how): below one half a node gains an activated_by (sign < 1/2) or
+ * activated_by_absence_of link from one of the first four inputs or any
+ * node, at 0.1 x 2^(2 how - 1); otherwise one term is lost.  *out is a new
+ * network; CW_ERR_NOT_FOUND for a loss from a network without a term. */
+int cw_network_rewire(cw_network net, const double draws[5], cw_network *out, cw_mutation *rec);
+/* RK4 for cells of many networks at once (the per-cell mutated networks of
+ * an evolving run, network.rs:487-616): cell c steps under nets[clone[c]].
+ * Every network has the same node count; state [ncells][S], inputs
+ * [ncells][6], as cw_network_step_batch. */
+int cw_network_step_clones(int32_t nnets, const cw_network *nets, int64_t ncells, const int32_t *clone,
+                           double *state, const double *inputs, double dt, int32_t substeps);
+
 /* ------------------------------------------------------------------ simulation driver
  * A device-resident Simulation<Running>::step (simulation.rs:1129-1350)
  * reduced to the hot path: per lattice step, every field is painted from the

@@ -8,7 +8,9 @@ citations in that file); ``compile_network`` restates ``Network::from_spec``
 """
 from __future__ import annotations
 
+import copy
 import ctypes as C
+import math
 import os
 
 import numpy as np
@@ -389,6 +391,74 @@ def network_step(net: CompiledNetwork, state: np.ndarray, inputs: np.ndarray, dt
                    _p(net.hill_n).value, _p(net.hill_k).value, _p(net.param).value)
     lib().or_network_step(C.byref(s), state.shape[0], _p(state), _p(inputs), float(dt), int(substeps))
     return state
+
+
+# ---------------------------------------------------------------- mutations
+MUTATION_SPREAD = 2.0  # network.rs:158
+GAINED_RATE = 0.1      # network.rs:163
+REWIRED_INPUTS = 4     # network.rs:165-169: oxygen, egf, crowding, stress
+NETWORK_INPUTS = ["oxygen", "egf", "crowding", "stress", "waste", "necrotic_factor"]  # core network.rs INPUT_NAMES
+
+
+def _pick(n: int, u: float) -> int:
+    """``((u * n as f64) as usize).min(n.saturating_sub(1))`` (network.rs:488-489, 521)."""
+    v = u * n
+    k = int(v) if v > 0.0 else 0
+    return min(k, max(n - 1, 0))
+
+
+def mutate_spec(spec: dict, which: float, how: float):
+    """Network::mutate (network.rs:479-501) on a network table: one rate of
+    every node's terms in file order, picked by ``which``, times
+    MUTATION_SPREAD^(2 how - 1).  Returns (new table, record) or (table, None)."""
+    spec = copy.deepcopy(spec)
+    count = sum(len(n.get("terms", [])) for n in spec["nodes"])
+    pick = _pick(count, which)
+    factor = math.pow(MUTATION_SPREAD, 2.0 * how - 1.0)
+    for node in spec["nodes"]:
+        terms = node.get("terms", [])
+        if pick < len(terms):
+            terms[pick]["rate"] = float(terms[pick]["rate"]) * factor
+            return spec, dict(node=node["name"], term=pick, kind=terms[pick]["kind"], change="scaled",
+                              factor=factor)
+        pick -= len(terms)
+    return spec, None
+
+
+def rewire_spec(spec: dict, draws):
+    """Network::rewire (network.rs:503-575) on a network table, draws =
+    (mode, which, source, sign, how): a gained activated_by /
+    activated_by_absence_of link below one half, a lost term otherwise."""
+    mode, which, source, sign, how = draws
+    spec = copy.deepcopy(spec)
+    nodes = spec["nodes"]
+    if mode < 0.5:
+        node = nodes[_pick(len(nodes), which)]
+        s = _pick(REWIRED_INPUTS + len(nodes), source)
+        name = NETWORK_INPUTS[s] if s < REWIRED_INPUTS else nodes[s - REWIRED_INPUTS]["name"]
+        rate = GAINED_RATE * math.pow(MUTATION_SPREAD, 2.0 * how - 1.0)
+        kind = "activated_by" if sign < 0.5 else "activated_by_absence_of"
+        terms = node.setdefault("terms", [])
+        terms.append({"kind": kind, "rate": rate, "source": name})
+        return spec, dict(node=node["name"], term=len(terms) - 1, kind=kind, change="gained", source=name, rate=rate)
+    count = sum(len(n.get("terms", [])) for n in nodes)
+    at = _pick(count, which)
+    for node in nodes:
+        terms = node.get("terms", [])
+        if at < len(terms):
+            lost = terms.pop(at)
+            return spec, dict(node=node["name"], term=at, kind=lost["kind"], change="lost")
+        at -= len(terms)
+    return spec, None
+
+
+def mutation_text(rec: dict) -> str:
+    """Mutation's Display (network.rs:201-226)."""
+    if rec["change"] == "scaled":
+        return f"{rec['node']} {rec['kind']} #{rec['term']} x{rec['factor']:.2f}"
+    if rec["change"] == "gained":
+        return f"{rec['node']} gains {rec['kind']} {rec['source']} @{rec['rate']:.2f}"
+    return f"{rec['node']} loses {rec['kind']} #{rec['term']}"
 
 
 def network_mechanics(net: CompiledNetwork, state: np.ndarray) -> np.ndarray:

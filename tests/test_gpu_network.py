@@ -88,3 +88,93 @@ def test_refusals_name_the_culprit():
                                    "hill": {"n": 2.0, "k": 0.0}}]), 1)
     with pytest.raises(cw.ConfigError):
         cw.Network.from_spec({**one([]), "nodes": []}, 1)
+
+
+# ---------------------------------------------------------------- mutated networks
+DRAWS = [(0.0, 0.5), (0.99, 0.999_999), (0.37, 0.1), (0.62, 0.93)]
+REWIRES = [[0.0, 0.0, 0.0, 0.0, 0.5], [0.9, 0.0, 0.0, 0.0, 0.0], [0.2, 0.7, 0.95, 0.6, 0.3],
+           [0.4, 0.99, 0.5, 0.1, 0.8], [0.75, 0.55, 0.0, 0.0, 0.0]]
+
+
+def same_record(dev, ref):
+    keys = ("node", "term", "kind", "change")
+    assert tuple(dev[k] for k in keys) == tuple(ref[k] for k in keys)
+    assert dev["text"] == O.mutation_text(ref)
+    if ref["change"] == "scaled":
+        assert dev["factor"] == ref["factor"]
+    if ref["change"] == "gained":
+        assert dev["source"] == ref["source"] and dev["rate"] == ref["rate"]
+
+
+def test_mutations_on_the_device_match_the_oracle(golden):
+    # Network::mutate / rewire (network.rs:479-575): the same pick, factor,
+    # gained source and rate as the oracle's restatement
+    spec = golden["networks"]["ras-erk"]
+    net = cw.Network.from_spec(spec, 200)
+    for which, how in DRAWS:
+        _, rec = net.mutate(which, how)
+        same_record(rec, O.mutate_spec(spec, which, how)[1])
+    for d in REWIRES:
+        _, rec = net.rewire(d)
+        same_record(rec, O.rewire_spec(spec, d)[1])
+
+
+def test_a_batch_of_clones_steps_each_cell_under_its_own_network(golden, tmp_path):
+    # the per-cell networks of an evolving run: every cell of one launch under
+    # the network its clone has, against the oracle stepping each clone's
+    # table alone; bit for bit without Hill terms, 1e-12 with them
+    for name, spec, dt, exact in [("ras-erk", golden["networks"]["ras-erk"], 1.0, True),
+                                  ("synthetic", None, 0.01, False)]:
+        if spec is None:
+            p = tmp_path / "net.toml"
+            p.write_text(synthetic.network_toml(8, seed=8))
+            spec = cw.load_network_spec(str(p))
+        founder = cw.Network.from_spec(spec, 64)
+        nets, specs = [founder], [spec]
+        for which, how in DRAWS[1:]:
+            n, _ = founder.mutate(which, how)
+            nets.append(n)
+            specs.append(O.mutate_spec(spec, which, how)[0])
+        for d in REWIRES:
+            n, _ = nets[-1].rewire(d)
+            nets.append(n)
+            specs.append(O.rewire_spec(specs[-1], d)[0])
+        rng = np.random.default_rng(3)
+        ncell = 700
+        clone = rng.integers(0, len(nets), ncell).astype(np.int32)
+        st = rng.uniform(0, 1, (ncell, founder.S))
+        ins = rng.uniform(0, 1, (ncell, 6))
+        got = st.copy()
+        cw.Network.step_clones(nets, clone, got, ins, dt, 8)
+        want = st.copy()
+        for k, s in enumerate(specs):
+            rows = np.flatnonzero(clone == k)
+            sub = want[rows].copy()
+            O.network_step(O.compile_network(s, 64), sub, ins[rows], dt, 8)
+            want[rows] = sub
+        if exact:
+            np.testing.assert_array_equal(got.view(np.uint64), want.view(np.uint64), err_msg=name)
+        else:
+            np.testing.assert_allclose(got, want, rtol=1e-12, atol=1e-15, err_msg=name)
+        # and one network's cells alone are what step_batch gives
+        one = st[clone == 0].copy()
+        founder.step_batch(one, ins[clone == 0], dt, 8)
+        np.testing.assert_array_equal(one.view(np.uint64), got[clone == 0].view(np.uint64))
+
+
+def test_mutations_refuse_what_the_reference_cannot_do(golden):
+    bare = {"nodes": [{"name": "a", "initial": 0.1}], "roles": {"growth": "a", "survival": "a",
+            "hypoxia_response": "a"}, "mechanics": {"growth_coefficient": 0.5, "lambda_volume": 10.0}}
+    net = cw.Network.from_spec(bare, 50)
+    with pytest.raises(cw.NotFoundError):
+        net.mutate(0.5, 0.5)
+    with pytest.raises(cw.NotFoundError):
+        net.rewire([0.9, 0.0, 0.0, 0.0, 0.0])
+    gained, rec = net.rewire([0.1, 0.0, 0.99, 0.0, 0.5])  # a gain needs no term: reads itself
+    assert rec["text"] == "a gains activated_by a @0.10"
+    ras = cw.Network.from_spec(golden["networks"]["ras-erk"], 200)
+    st = np.full((3, ras.S), 0.5)
+    with pytest.raises(cw.ConfigError):
+        cw.Network.step_clones([ras, gained], np.zeros(3, np.int32), st, np.zeros((3, 6)), 1.0)
+    with pytest.raises(cw.ConfigError):
+        cw.Network.step_clones([ras], np.array([0, 1, 0], np.int32), st, np.zeros((3, 6)), 1.0)

@@ -8,8 +8,10 @@ mean), the boundary length inside the sequential ensemble's band.
 The whole step: 32 histories of a small cord-like campaign stepped by the
 device against the CPU oracle stepping the reference's algorithms one
 history at a time (sequential sweep, FP64 SOR, RK4; oracle/cpu_sim.py):
-population, mean oxygen over the cells and the hypoxic fraction of the
-living cells inside the oracle's band at several steps.
+population, mean oxygen over the cells, the hypoxic fraction of the living
+cells and the hypoxic radius (how many rows from the held source row the
+oxygen stays above the hypoxic level) inside the oracle's band at several
+steps.
 """
 import os
 import tempfile
@@ -52,12 +54,27 @@ def small_cord(n=SEEDS):
     return cfg
 
 
-def per_history(grid, o2, volume, types, necrotic, level):
+def hypoxic_radius(o2, size, level):
+    """How deep the tissue is fed: the distance from the held source row (row
+    0) at which the row-mean oxygen first falls under the hypoxic level,
+    interpolated between rows (the box's height if it never does)."""
+    rows = np.asarray(o2, float).reshape(-1, size).mean(axis=1)
+    below = np.flatnonzero(rows < level)
+    if not below.size:
+        return float(len(rows))
+    j = int(below[0])
+    if j == 0:
+        return 0.0
+    return (j - 1) + float((rows[j - 1] - level) / (rows[j - 1] - rows[j]))
+
+
+def per_history(grid, o2, volume, types, necrotic, level, size=64):
     living = (volume > 0) & (types != necrotic)
     living[0] = False
     means = O.mean_per_cell(grid, o2, len(volume))
     cells = np.flatnonzero(living)
-    return len(cells), float(means[cells].mean()), float((means[cells] < level).mean())
+    return (len(cells), float(means[cells].mean()), float((means[cells] < level).mean()),
+            hypoxic_radius(o2, size, level))
 
 
 def test_the_step_stays_inside_the_oracle_band():
@@ -84,7 +101,7 @@ def test_the_step_stays_inside_the_oracle_band():
             h = ora[k]
             ref.append(per_history(h.lat.grid, h.o2.values, h.lat.volume, h.lat.type, 3, cfg["hypoxic_level"]))
         dev, ref = np.array(dev), np.array(ref)
-        for j, name in enumerate(("living", "mean oxygen", "hypoxic fraction")):
+        for j, name in enumerate(("living", "mean oxygen", "hypoxic fraction", "hypoxic radius")):
             assert within_band(dev[:, j], ref[:, j]), (step, name, dev[:, j].mean(), ref[:, j].mean(),
                                                         ref[:, j].std())
 

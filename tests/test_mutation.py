@@ -1,0 +1,78 @@
+"""Per-cell mutated networks: the oracle's restatement of Network::mutate and
+Network::rewire (crates/engine/src/network.rs:479-575) pinned on the
+reference's own tests of them (network.rs:1398-1530), on CPU."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+
+def ras_erk(golden):
+    return golden["networks"]["ras-erk"]
+
+
+def at(o2, egf):
+    # CellInputs of network.rs:839-849: oxygen and EGF, every other input zero
+    return np.array([[o2, egf, 0.0, 0.0, 0.0, 0.0]])
+
+
+def run(spec, steps, o2, egf):
+    net = O.compile_network(spec, 200)
+    st = net.initial.reshape(1, -1).copy()
+    O.network_step(net, st, at(o2, egf), 1.0, steps)
+    return net, st[0]
+
+
+def test_a_mutation_scales_one_rate_and_the_parent_keeps_its_own(golden):
+    # network.rs:1398-1425: the last of the eleven terms is BCL2's damage
+    # below the anoxia threshold; a draw near one doubles it
+    parent = ras_erk(golden)
+    daughter, m = O.mutate_spec(parent, 0.99, 0.999_999)
+    assert (m["node"], m["term"], m["kind"]) == ("bcl2", 3, "damaged_below")
+    assert abs(m["factor"] - O.MUTATION_SPREAD) < 1e-5
+    net_p, sp = run(parent, 40, 0.05, 0.2)
+    net_d, sd = run(daughter, 40, 0.05, 0.2)
+    assert sd[net_d.survival] < sp[net_p.survival], "doubled damage kills faster in the dark"
+    assert parent["nodes"][4]["terms"][3]["rate"] == 0.25  # the parent keeps its own
+
+
+def test_a_draw_in_the_middle_changes_nothing(golden):
+    # network.rs:1427-1443
+    spec, m = O.mutate_spec(ras_erk(golden), 0.0, 0.5)
+    assert (m["node"], m["term"], m["kind"]) == ("ras", 0, "activated_by")
+    assert m["factor"] == 1.0
+    _, a = run(spec, 5, 0.8, 0.2)
+    _, b = run(ras_erk(golden), 5, 0.8, 0.2)
+    np.testing.assert_array_equal(a.view(np.uint64), b.view(np.uint64))
+
+
+def test_a_gained_link_makes_a_node_answer_what_it_ignored(golden):
+    # network.rs:1484-1502
+    spec, m = O.rewire_spec(ras_erk(golden), [0.0, 0.0, 0.0, 0.0, 0.5])
+    assert O.mutation_text(m) == "ras gains activated_by oxygen @0.10"
+    assert m["term"] == 2, "added after RAS's two terms"
+    assert run(ras_erk(golden), 40, 1.0, 0.0)[1][0] < 0.01
+    assert run(spec, 40, 1.0, 0.0)[1][0] > 0.1
+
+
+def test_a_lost_term_takes_its_answer_away(golden):
+    # network.rs:1504-1520
+    spec, m = O.rewire_spec(ras_erk(golden), [0.9, 0.0, 0.0, 0.0, 0.0])
+    assert O.mutation_text(m) == "ras loses activated_by #0"
+    assert m["change"] == "lost"
+    assert run(ras_erk(golden), 40, 0.8, 0.2)[1][0] > 0.2, "EGF switches the healthy RAS on"
+    assert run(spec, 40, 0.8, 0.2)[1][0] < 0.01, "and nothing switches this one on"
+
+
+@pytest.mark.parametrize("which", [0.0, 0.3, 0.5, 0.999999])
+def test_picks_cover_every_term_and_stay_in_range(golden, which):
+    spec = ras_erk(golden)
+    count = sum(len(n["terms"]) for n in spec["nodes"])
+    _, m = O.mutate_spec(spec, which, 0.25)
+    flat = [(n["name"], j) for n in spec["nodes"] for j in range(len(n["terms"]))]
+    assert flat[min(int(which * count), count - 1)] == (m["node"], m["term"])
+    assert abs(m["factor"] - 2.0 ** -0.5) < 1e-15
+    # a network without a single term: nothing to change, nothing to lose
+    bare = {"nodes": [{"name": "a", "initial": 0.1}], "roles": spec["roles"], "mechanics": spec["mechanics"]}
+    assert O.mutate_spec(bare, which, 0.5)[1] is None
+    assert O.rewire_spec(bare, [0.9, which, 0.0, 0.0, 0.0])[1] is None
