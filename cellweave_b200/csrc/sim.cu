@@ -74,8 +74,12 @@ namespace {
 
 constexpr int T = 256;
 
+// A cell's inputs (cell_inputs, simulation.rs:2511-2527): its mean oxygen,
+// EGF everywhere the same, crowding 1 - volume / reference volume clamped to
+// [0, 1]; no stress, waste or necrotic factor on this path.
 __global__ void k_inputs(const int32_t *type, const int32_t *volume, const int64_t *cell_off, int nh, int64_t nc,
-                         int necrotic, const double *cell_o2, double egf, double *inputs, uint8_t *alive) {
+                         int necrotic, const double *cell_o2, double egf, double reference, double *inputs,
+                         uint8_t *alive) {
     int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nc) return;
     // the medium slot of every history is not a cell
@@ -86,7 +90,7 @@ __global__ void k_inputs(const int32_t *type, const int32_t *volume, const int64
     alive[c] = a;
     inputs[0 * nc + c] = cell_o2[c];
     inputs[1 * nc + c] = egf;
-    inputs[2 * nc + c] = 0.0;
+    inputs[2 * nc + c] = a ? fmin(fmax(1.0 - (double)volume[c] / reference, 0.0), 1.0) : 0.0;
     inputs[3 * nc + c] = 0.0;
     inputs[4 * nc + c] = 0.0;
     inputs[5 * nc + c] = 0.0;
@@ -512,7 +516,9 @@ static int enqueue_phase(cw_sim_s *s, int p, const cw_relax_opts &o) {
     if (p == 1) {
         if ((rc = couple_means_device(s->o2, s->lat, s->sum, s->count, s->cell_o2, s->sites)) != CW_OK) return rc;
         k_inputs<<<(unsigned)blocks(nc), T, 0, stream()>>>(s->lat->type, s->lat->volume, s->lat->d_cell_off, c.nh, nc,
-                                                           c.necrotic_type, s->cell_o2, 0.2, s->inputs, s->alive);
+                                                           c.necrotic_type, s->cell_o2, 0.2,
+                                                           (double)std::max(network_reference_volume(s->net), 1u),
+                                                           s->inputs, s->alive);
         CW_LAUNCHED();
         if (!s->sig) return CW_OK;
         k_secretion<<<(unsigned)blocks(nc), T, 0, stream()>>>(s->alive, s->cell_o2, nc, c.hypoxic_level,
@@ -666,7 +672,9 @@ int cw_sim_step(cw_sim s, uint32_t nsteps) {
         // 2. what each cell sits in
         if ((rc = couple_means_device(s->o2, s->lat, s->sum, s->count, s->cell_o2, s->sites)) != CW_OK) return rc;
         k_inputs<<<(unsigned)blocks(nc), T, 0, stream()>>>(s->lat->type, s->lat->volume, s->lat->d_cell_off, c.nh, nc,
-                                                           c.necrotic_type, s->cell_o2, 0.2, s->inputs, s->alive);
+                                                           c.necrotic_type, s->cell_o2, 0.2,
+                                                           (double)std::max(network_reference_volume(s->net), 1u),
+                                                           s->inputs, s->alive);
         CW_LAUNCHED();
         if (s->sig && solve) {
             k_secretion<<<(unsigned)blocks(nc), T, 0, stream()>>>(s->alive, s->cell_o2, nc, c.hypoxic_level,

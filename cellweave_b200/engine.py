@@ -693,6 +693,12 @@ class Simulation:
         call("cw_lattice_verify", self.lattice_handle(), hist, C.byref(ok))
         return bool(ok.value)
 
+    def network_state(self, n, hist=0):
+        """The protein levels of records 0..n-1 of a history, [n, S]."""
+        out = np.empty((int(n), self.network.S))
+        call("cw_sim_network_state", self._h, int(hist), int(n), ptr(out))
+        return out
+
 
 # ============================================================== Fit (adjoint)
 class Fit:

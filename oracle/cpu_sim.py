@@ -142,6 +142,8 @@ class CpuHistory:
             ins = np.zeros((len(idx), 6))
             ins[:, 0] = o2m[idx]
             ins[:, 1] = 0.2
+            # crowding (simulation.rs:2523-2527): 1 - volume / reference volume, clamped
+            ins[:, 2] = np.clip(1.0 - self.lat.volume[idx] / float(max(c["target_volume"], 1)), 0.0, 1.0)
             st = np.ascontiguousarray(self.state[idx])
             O.network_step(self.net, st, ins, c["dt"], c["substeps"])
             self.state[idx] = st

@@ -178,3 +178,32 @@ def test_mutations_refuse_what_the_reference_cannot_do(golden):
         cw.Network.step_clones([ras, gained], np.zeros(3, np.int32), st, np.zeros((3, 6)), 1.0)
     with pytest.raises(cw.ConfigError):
         cw.Network.step_clones([ras], np.array([0, 1, 0], np.int32), st, np.zeros((3, 6)), 1.0)
+
+
+def test_the_step_feeds_each_cell_its_crowding():
+    # cell_inputs / crowding (simulation.rs:2511-2527): a network that reads
+    # crowding, 1 - volume / reference volume clamped to [0, 1], steps every
+    # living cell from its volume before the step's Monte Carlo sweep
+    spec = {"nodes": [{"name": "a", "initial": 0.1, "terms": [
+        {"kind": "activated_by", "source": "crowding", "rate": 1.0}, {"kind": "decays", "rate": 0.5}]}],
+        "roles": {"growth": "a", "survival": "a", "hypoxia_response": "a"},
+        "mechanics": {"growth_coefficient": 0.0, "lambda_volume": 1.0}}
+    ref_volume = 60
+    net = cw.Network.from_spec(spec, ref_volume)
+    J = np.array([[0, 16, 16], [16, 8, 12], [16, 12, 8]], float)
+    sim = cw.Simulation(net, [(64, 64, 1)], [20], [7], J=J, target_volume=49, nfields=1, dt=0.25, substeps=4,
+                        death_threshold=0.0, divide=False)
+    cells = sim.lattice().cells(hist=0)
+    n = len(cells["volume"])
+    sim.step(1)
+    got = sim.network_state(n)
+    vol = cells["volume"].astype(float)
+    live = np.flatnonzero((vol > 0) & (np.arange(n) > 0))
+    assert len(live) > 5
+    ins = np.zeros((len(live), 6))
+    ins[:, 1] = 0.2
+    ins[:, 2] = np.clip(1.0 - vol[live] / ref_volume, 0.0, 1.0)
+    want = np.full((len(live), 1), 0.1)
+    O.network_step(O.compile_network(spec, ref_volume), want, ins, 0.25, 4)
+    np.testing.assert_array_equal(got[live].view(np.uint64), want.view(np.uint64))
+    assert (ins[:, 2] > 0.1).all()
