@@ -300,8 +300,9 @@ def run_ours(args, rank, world, dist):
     except Exception:
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
-    kname = (f"k_sor32_wide<{depth}> (FP32 red-black SOR, 128x64 TMA-fed windows, {depth} half-sweeps per launch "
-             f"on chip)" if window == cw.WINDOW_AUTO else
+    shape = {cw.WINDOW_AUTO: "128x64", cw.WINDOW_TALL: "128x128"}.get(window)
+    kname = (f"k_sor32_wide<{depth}> (FP32 red-black SOR, {shape} TMA-fed windows, {depth} half-sweeps per launch "
+             f"on chip)" if shape else
              f"k_sor32_tb<{depth}> (FP32 red-black SOR, 64x64 windows, {depth} half-sweeps per launch on chip)")
     one_sweep_gbs = alg_bytes_per_launch / (one_sweep_ms / 1e3) / 1e9
     roofline = {"kernel": kname,

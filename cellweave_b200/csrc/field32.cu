@@ -146,12 +146,14 @@ __global__ void __launch_bounds__(32 * WARPS) k_sor32_tb(const float *__restrict
 
 // ------------------------------------------------------------------ wide windows (TMA)
 
-constexpr int WX = 128, WY = 64;     // window columns, rows
-constexpr int WWARPS = 8;            // warps per block
-constexpr int WROWS = WY / WWARPS;   // rows per warp
-constexpr int STAGE = WX * WY;       // floats per array of the staged window
-constexpr int EDGE_F4 = 2 * WWARPS * 2 * (WX / 4);
-constexpr size_t WIDE_SMEM = (size_t)3 * STAGE * sizeof(float) + (size_t)EDGE_F4 * sizeof(float4);
+constexpr int WX = 128;              // window columns
+constexpr int WROWS = 8;             // rows per warp; a window has 8 rows per warp of its block
+// Two shapes: 8 warps (128 x 64 windows, two blocks per SM) or 16 warps
+// (128 x 128 windows, one block per SM: a smaller share of the window is
+// halo, 1.31 pixels swept per interior pixel at depth 8 against 1.52).
+constexpr size_t wide_smem(int warps) {
+    return (size_t)3 * WX * WROWS * warps * sizeof(float) + (size_t)2 * warps * 2 * (WX / 4) * sizeof(float4);
+}
 __device__ int g_wide_wait_failed;
 
 // The first window at or after `t`, in steps of `step`, whose history is not settled.
@@ -206,13 +208,15 @@ struct WideTile {
 // zero_start: the correction starts at zero (the first launch of a solve):
 // it is not read.  apply_c: the last launch of a solve adds its correction to
 // the FP64 field (floored at zero when `floor`) instead of writing it to dst.
-template <int DEPTH>
-__global__ void __launch_bounds__(32 * WWARPS, 2)
+template <int DEPTH, int WWARPS>
+__global__ void __launch_bounds__(32 * WWARPS, WWARPS == 8 ? 2 : 1)
     k_sor32_wide(const CUtensorMap *__restrict__ maps, int src_map, float *__restrict__ dst,
                  const int4 *__restrict__ tiles, int ntiles, const int4 *__restrict__ dims,
                  const int64_t *__restrict__ off, const float *__restrict__ omega, const int32_t *done,
                  int done_stride, int nhalf, int start_colour, int zero_start, double *__restrict__ apply_c,
                  int floor) {
+    constexpr int WY = WROWS * WWARPS;  // window rows
+    constexpr int STAGE = WX * WY;      // floats per array of the staged window
     extern __shared__ __align__(128) float smem[];
     const float4 *sd = (const float4 *)smem, *sb = (const float4 *)(smem + STAGE),
                  *sa = (const float4 *)(smem + 2 * STAGE);
@@ -404,14 +408,17 @@ TbKernel tb_kernel(int depth) {
     }
 }
 
-WideKernel wide_kernel(int depth) {
+template <int W>
+WideKernel wide_kernel_of(int depth) {
     switch (depth) {
-    case 2: return k_sor32_wide<2>;
-    case 4: return k_sor32_wide<4>;
-    case 6: return k_sor32_wide<6>;
-    default: return k_sor32_wide<8>;
+    case 2: return k_sor32_wide<2, W>;
+    case 4: return k_sor32_wide<4, W>;
+    case 6: return k_sor32_wide<6, W>;
+    default: return k_sor32_wide<8, W>;
     }
 }
+
+WideKernel wide_kernel(int depth, int warps) { return warps == 16 ? wide_kernel_of<16>(depth) : wide_kernel_of<8>(depth); }
 
 // Window starts along one axis of n pixels for windows of `win` with a halo
 // of `depth`: the first at 0, then every win - 2 depth until one reaches n.
@@ -425,8 +432,11 @@ void axis_starts(int n, int win, int depth, std::vector<int> &out) {
 }
 
 // The wide kernel's tensor maps, windows and grid, if every history allows it.
-int wide_init(Sor32 &s, cw_field_s *f) {
+int wide_init(Sor32 &s, cw_field_s *f, int warps) {
     s.wide = false;
+    s.wwarps = warps;
+    const int WY = WROWS * warps;
+    const size_t smem = wide_smem(warps);
     const Geom &g = f->g;
     for (uint32_t k = 0; k < g.nh; ++k)
         if (g.d[k] != 1 || g.w[k] % 4 != 0 || g.off[k] % 4 != 0) return CW_OK;
@@ -439,17 +449,21 @@ int wide_init(Sor32 &s, cw_field_s *f) {
         for (int m = 0; m < 4; ++m) {
             cuuint64_t dim[2] = {(cuuint64_t)g.w[k], (cuuint64_t)g.h[k]};
             cuuint64_t stride[1] = {(cuuint64_t)g.w[k] * sizeof(float)};
-            cuuint32_t box[2] = {WX, WY};
+            cuuint32_t box[2] = {(cuuint32_t)WX, (cuuint32_t)WY};
             cuuint32_t estride[2] = {1, 1};
             CUresult r = enc(&maps[4 * k + m], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, arrays[m] + g.off[k], dim, stride,
                              box, estride, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
             if (r != CUDA_SUCCESS) return CW_OK;  // the narrow kernel serves
         }
-    WideKernel kern = wide_kernel(s.depth);
-    CW_CUDA(cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)WIDE_SMEM));
+    WideKernel kern = wide_kernel(s.depth, warps);
+    if (cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess) {
+        (void)cudaGetLastError();
+        return CW_OK;  // the narrow kernel serves
+    }
     int per_sm = 0, dev = 0, nsm = 0;
-    CW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)kern, 32 * WWARPS, WIDE_SMEM));
+    CW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)kern, 32 * warps, smem));
     if (per_sm < 1) return CW_OK;
     CW_CUDA(cudaGetDevice(&dev));
     CW_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
@@ -490,7 +504,9 @@ int Sor32::init(cw_field_s *f, int d, const std::vector<double> &om, int window)
     std::vector<int64_t> per(f->g.nh);
     if (blocked) {
         wide = false;
-        if (window == CW_WINDOW_AUTO && (rc = wide_init(*this, f)) != CW_OK) return rc;
+        if ((window == CW_WINDOW_AUTO || window == CW_WINDOW_TALL) &&
+            (rc = wide_init(*this, f, window == CW_WINDOW_TALL ? 16 : 8)) != CW_OK)
+            return rc;
         if (!wide) {
             const int in = WIN - 2 * depth;
             for (uint32_t k = 0; k < f->g.nh; ++k)
@@ -535,7 +551,7 @@ int Sor32::sweeps(cw_field_s *f, int n, const int32_t *done, int done_stride, fl
             // the first launch starts from zero without reading it; with
             // `apply` the last adds its correction to the field
             const bool last = remaining == dd;
-            wide_kernel(depth)<<<wgrid, 32 * WWARPS, WIDE_SMEM, stream()>>>(
+            wide_kernel(depth, wwarps)<<<wgrid, 32 * wwarps, wide_smem(wwarps), stream()>>>(
                 (const CUtensorMap *)maps, a == f->d32a ? 0 : 1, b, wtiles, nwtiles, f->g.d_dims, f->g.d_off, omega,
                 done, done_stride, dd, done_half & 1, done_half == 0 ? 1 : 0, apply && last ? f->c : nullptr,
                 f->floor ? 1 : 0);

@@ -61,6 +61,7 @@ struct Sor32 {
     void *maps = nullptr;       // wide: 4 tensor maps per history (d32a, d32b, r32, inv32), device
     int4 *wtiles = nullptr;     // wide: (history, x0, y0, 0) per window, device
     int nwtiles = 0, wgrid = 0;
+    int wwarps = 8;             // wide: warps per block (8: 128 x 64 windows, 16: 128 x 128)
     float *omega = nullptr;
     float *ping = nullptr, *pong = nullptr, *out = nullptr;
     int init(cw_field_s *f, int depth, const std::vector<double> &omega_per_history, int window = CW_WINDOW_AUTO);

@@ -22,7 +22,7 @@ from ._lib import ConfigError, call, lib, ptr
 
 OBSTACLE = -1
 FP64, FP32_DC = 0, 1
-WINDOW_AUTO, WINDOW_64 = 0, 1
+WINDOW_AUTO, WINDOW_64, WINDOW_TALL = 0, 1, 2
 STOP_MAX_CHANGE, STOP_RESIDUAL = 0, 1
 COPY_VON_NEUMANN, COPY_MOORE = 0, 1
 VALUES, UPTAKE, PRODUCTION, LIN_SINK = 0, 1, 2, 3

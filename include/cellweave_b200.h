@@ -172,9 +172,10 @@ int cw_field_hold_bath(cw_field f, uint32_t hist, const uint8_t *open, double va
 enum { CW_STOP_MAX_CHANGE = 0, CW_STOP_RESIDUAL = 1 };
 enum { CW_FP64 = 0, CW_FP32_DC = 1 };
 /* CW_FP32_DC sweep windows: the widest the batch allows (128 x 64, fed by
- * TMA, where every history's rows are 16-byte aligned; else 64 x 64), or
- * 64 x 64 always. */
-enum { CW_WINDOW_AUTO = 0, CW_WINDOW_64 = 1 };
+ * TMA, where every history's rows are 16-byte aligned; else 64 x 64),
+ * 64 x 64 always, or 128 x 128 TMA-fed windows, one block per SM, where the
+ * rows allow (else 64 x 64). */
+enum { CW_WINDOW_AUTO = 0, CW_WINDOW_64 = 1, CW_WINDOW_TALL = 2 };
 typedef struct {
     double omega;        /* <= 0: the reference's rule (pde.rs:267-277) */
     int32_t stop;        /* CW_STOP_MAX_CHANGE (the reference) or CW_STOP_RESIDUAL */
@@ -183,7 +184,7 @@ typedef struct {
     int32_t precision;   /* CW_FP64 (bit-exact with the reference) or CW_FP32_DC */
     int32_t inner_sweeps;/* CW_FP32_DC: FP32 sweeps per FP64 defect correction (0: 16) */
     int32_t block_depth; /* CW_FP32_DC: half-sweeps per launch kept in shared memory (0: 4) */
-    int32_t window;      /* CW_FP32_DC: CW_WINDOW_AUTO or CW_WINDOW_64 */
+    int32_t window;      /* CW_FP32_DC: a CW_WINDOW_* */
 } cw_relax_opts;
 typedef struct {
     int64_t sweeps;      /* the count relax returns (pde.rs:279-283) */

@@ -239,7 +239,7 @@ def inner_corrections(dims, depth, window=cw.WINDOW_AUTO, sweeps=5, seed=3):
 
 
 @pytest.mark.parametrize("dims", [
-    [(128, 128), (200, 96), (260, 130), (1024, 70), (64, 300)],   # rows 16-byte aligned: 128 x 64 TMA windows
+    [(128, 128), (200, 96), (260, 130), (1024, 70), (64, 300)],   # rows 16-byte aligned: TMA windows
     [(127, 90), (61, 61), (300, 33)],                               # any width: 64 x 64 windows
 ])
 def test_blocked_fp32_sweeps_equal_one_half_sweep_per_launch(dims):
@@ -249,7 +249,7 @@ def test_blocked_fp32_sweeps_equal_one_half_sweep_per_launch(dims):
     ref, n1 = inner_corrections(dims, 1)
     assert n1 == 10
     assert all(np.abs(r).max() > 0 for r in ref)
-    for window in (cw.WINDOW_AUTO, cw.WINDOW_64):
+    for window in (cw.WINDOW_AUTO, cw.WINDOW_TALL, cw.WINDOW_64):
         for depth in (2, 4, 6, 8):
             got, _ = inner_corrections(dims, depth, window)
             for k in range(len(dims)):
@@ -262,7 +262,7 @@ def test_wide_windows_with_the_fused_correction_equal_the_64_windows(sizes, dept
     # the residual in one pass; the 64 x 64 windows write the correction and
     # update in two colour passes: the same arithmetic, so the same bits
     fields = []
-    for window in (cw.WINDOW_AUTO, cw.WINDOW_64):
+    for window in (cw.WINDOW_AUTO, cw.WINDOW_64, cw.WINDOW_TALL):
         g = cw.ScalarField([(n, n, 1) for n in sizes], 1.0, 0.0, 0.0)
         for k, n in enumerate(sizes):
             held, sink, _ = sheet_problem(n, seed=k)
@@ -271,8 +271,9 @@ def test_wide_windows_with_the_fused_correction_equal_the_64_windows(sizes, dept
         st = g.relax(1e-6, 1_000_000, omega=1.9, stop=cw.STOP_RESIDUAL, precision=cw.FP32_DC, block_depth=depth,
                      window=window, stats=True)
         fields.append((g, st))
-    (ga, sa), (gb, sb) = fields
-    for k in range(len(sizes)):
-        assert sa[k]["sweeps"] == sb[k]["sweeps"]
-        assert sa[k]["residual"] == sb[k]["residual"] < 1e-6
-        np.testing.assert_array_equal(bits(ga.values(k)), bits(gb.values(k)))
+    (ga, sa), *rest = fields
+    for gb, sb in rest:
+        for k in range(len(sizes)):
+            assert sa[k]["sweeps"] == sb[k]["sweeps"]
+            assert sa[k]["residual"] == sb[k]["residual"] < 1e-6
+            np.testing.assert_array_equal(bits(ga.values(k)), bits(gb.values(k)))
