@@ -89,7 +89,9 @@ class SimConfig(C.Structure):
                 ("tolerance", C.c_double), ("precision", C.c_int32), ("omega", C.c_double),
                 ("inner_sweeps", C.c_int32), ("relax_every", C.c_int32), ("dt", C.c_double), ("substeps", C.c_int32), ("sweeps", C.c_int32),
                 ("death_threshold", C.c_double), ("necrotic_type", C.c_int32), ("use_graphs", C.c_int32),
-                ("divide", C.c_int32), ("max_cells", C.c_int32), ("spare_cells", C.c_int32)]
+                ("divide", C.c_int32), ("max_cells", C.c_int32), ("spare_cells", C.c_int32),
+                ("waste_production", C.c_double), ("necrotic_production", C.c_double),
+                ("necrotic_release_for", C.c_int32)]
 
 
 P = C.c_void_p
@@ -161,6 +163,7 @@ SIGNATURES = {
     "cw_network_backward_batch": (C.c_int, [P, I64, P, P, D, I32, P, P, I32, P]),
     "cw_network_mechanics_batch": (C.c_int, [P, I64, P, P, P]),
     "cw_network_mutate": (C.c_int, [P, D, D, P, P]),
+    "cw_lattice_bath": (C.c_int, [P, U32, P]),
     "cw_network_rewire": (C.c_int, [P, P, P, P]),
     "cw_network_step_clones": (C.c_int, [I32, P, I64, P, P, P, D, I32]),
     "cw_sim_create": (C.c_int, [P, P, P]),

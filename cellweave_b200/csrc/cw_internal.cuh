@@ -231,6 +231,8 @@ struct cw_lattice_s {
     int32_t *d_used = nullptr;
     cw::DivScratch div;
     cw::Plan site_plan;                   // every pixel of every history, T per block
+    int32_t *bath_label = nullptr;        // the bath's union-find labels, one per site (bath.cu)
+    uint8_t *bath_mark = nullptr;         // roots that reach the outer layer (bath.cu)
     int build_plans();
 };
 
@@ -270,6 +272,8 @@ int lattice_sweep(cw_lattice_s *lat);
 int lattice_pass_error(cw_lattice_s *l);
 int lattice_recount_surfaces(cw_lattice_s *l);  // surfaces from the grid into the records, no sync
 int lattice_divide_enqueue(cw_lattice_s *l, const uint8_t *alive, int max_living, double *state, int S);
+int lattice_bath_enqueue(cw_lattice_s *l, uint8_t *bath);  // bath.cu: medium joined to the box's outer layer
+int lattice_bath_error();
 // coupling (coupling.cu), device-resident
 int couple_uptake_device(cw_field_s *f, cw_lattice_s *l, const double *d_rate_by_type, int K, double *dst,
                          const Plan &p);

@@ -875,6 +875,7 @@ int cw_lattice_destroy(cw_lattice l) {
     dfree(l->grid); dfree(l->type); dfree(l->volume); dfree(l->target); dfree(l->lambda); dfree(l->vsnap);
     dfree(l->surface); dfree(l->ssnap); dfree(l->tsurf); dfree(l->lsurf); dfree(l->d_cell_off); dfree(l->d_keys);
     dfree(l->d_flag); dfree(l->claim); dfree(l->plist); dfree(l->pctl); dfree(l->d_used);
+    dfree(l->bath_label); dfree(l->bath_mark);
     l->div.release();
     l->site_plan.release();
     for (auto &p : l->plans) p.release();

@@ -27,6 +27,12 @@ struct cw_sim_s {
     std::vector<double> J, sink;
     cw_lattice_s *lat = nullptr;
     cw_field_s *o2 = nullptr, *sig = nullptr;
+    cw_field_s *wst = nullptr, *nfc = nullptr;  // the released fields: waste, necrotic factor
+    double *cell_wst = nullptr, *cell_nfc = nullptr, *wst_rate = nullptr, *nfc_rate = nullptr;
+    int32_t *died_at = nullptr;     // the step a cell turned necrotic (-1: not yet)
+    uint32_t *d_step = nullptr;     // the step being taken, on the device
+    uint8_t *bath = nullptr;        // the bath of the current lattice, one byte per site
+    std::vector<cw_relax_stats> last_wst, last_nfc;
     cw_network_s *net = nullptr;
     double *d_sink = nullptr;       // 8 rates by type
     double *cell_o2 = nullptr, *cell_sig = nullptr, *sum = nullptr, *secretion = nullptr;
@@ -96,6 +102,42 @@ __global__ void k_inputs(const int32_t *type, const int32_t *volume, const int64
     inputs[5 * nc + c] = 0.0;
 }
 
+// What each cell releases into the released fields this step
+// (settle_released, simulation.rs:2546-2570): a living cell's pixels the
+// waste's production; a necrotic cell's the factor's, for `release_for`
+// steps after the one it died at (for as long as it is there when < 0).
+__global__ void k_release_rates(const uint8_t *alive, const int32_t *type, const int32_t *volume,
+                                const int32_t *died_at, const uint32_t *step, int64_t nc, int necrotic,
+                                double waste, double factor, int release_for, double *wst_rate, double *nfc_rate) {
+    int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nc) return;
+    if (wst_rate) wst_rate[c] = alive[c] ? waste : 0.0;
+    if (nfc_rate) {
+        const bool dead = necrotic >= 0 && type[c] == necrotic && volume[c] > 0;
+        const bool releasing = release_for < 0 || died_at[c] < 0 || (int64_t)*step <= (int64_t)died_at[c] + release_for;
+        nfc_rate[c] = dead && releasing ? factor : 0.0;
+    }
+}
+
+// The cells' waste and necrotic-factor inputs (cell_inputs, simulation.rs:2511-2521).
+__global__ void k_inputs_released(const double *cell_wst, const double *cell_nfc, int64_t nc, double *inputs) {
+    int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nc) return;
+    if (cell_wst) inputs[4 * nc + c] = cell_wst[c];
+    if (cell_nfc) inputs[5 * nc + c] = cell_nfc[c];
+}
+
+// A field held exactly on `mask` at `value` (release_all, then hold_bath_at).
+__global__ void k_hold_from_mask(const uint8_t *mask, int64_t n, double value, uint8_t *held, double *c) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint8_t m = mask[i];
+    held[i] = m;
+    if (m) c[i] = value;
+}
+
+__global__ void k_step_advance(uint32_t *step) { *step += 1u; }
+
 __global__ void k_secretion(const uint8_t *alive, const double *cell_o2, int64_t nc, double level, double rate,
                             double *secretion) {
     int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -113,7 +155,7 @@ constexpr int DEFAULT_MAX_CELLS = 2000;   // simulation.rs:61
 // necrotic; every other living cell takes the target its mechanics give.
 __global__ void k_fates(const uint8_t *alive, const double *state, int64_t nc, int survival, double death,
                         int necrotic, const uint32_t *mech_target, int32_t *type, const int32_t *volume,
-                        int32_t *target, double *lambda, double lam) {
+                        int32_t *target, double *lambda, double lam, int32_t *died_at, const uint32_t *step) {
     int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nc) return;
     if (necrotic >= 0 && type[c] == necrotic) {
@@ -127,6 +169,7 @@ __global__ void k_fates(const uint8_t *alive, const double *state, int64_t nc, i
     if (!alive[c]) return;
     if (necrotic >= 0 && state[survival * nc + c] < death) {
         type[c] = necrotic;
+        if (died_at) died_at[c] = (int32_t)*step;
         return;
     }
     target[c] = (int32_t)min(mech_target[c], 0x7fffffffu);
@@ -268,6 +311,7 @@ int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out) {
     if (c.nh == 0) return fail(CW_ERR_CONFIG, "a simulation needs a history");
     if (c.K < 2 || c.K > 8) return fail(CW_ERR_CONFIG, "2 to 8 types, the medium included");
     if (c.nfields < 1 || c.nfields > 2) return fail(CW_ERR_CONFIG, "one or two fields");
+    if (c.o2_hold < 0 || c.o2_hold > 3) return fail(CW_ERR_CONFIG, "the oxygen is held on a row, a column, the faces or the bath");
     if (!net) return fail(CW_ERR_CONFIG, "a simulation needs a network");
     int32_t survival = network_role(net, 1);
     cw_sim_s *s = new cw_sim_s();
@@ -337,7 +381,8 @@ int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out) {
                 for (uint32_t x = 0; x < W; ++x) {
                     bool on = c.o2_hold == 0 ? y == 0
                             : c.o2_hold == 1 ? x == W / 2
-                                             : (x == 0 || y == 0 || x + 1 == W || y + 1 == H || z == 0 || z + 1 == D);
+                            : c.o2_hold == 2 ? (x == 0 || y == 0 || x + 1 == W || y + 1 == H || z == 0 || z + 1 == D)
+                                             : false;  // 3: the bath, taken every step
                     held[((size_t)z * H + y) * W + x] = on;
                 }
         if ((rc = cw_field_hold_mask(s->o2, k, held.data(), 1.0)) != CW_OK) { cw_sim_destroy(s); return rc; }
@@ -347,6 +392,22 @@ int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out) {
                               &s->sig)) != CW_OK) {
         cw_sim_destroy(s);
         return rc;
+    }
+    if (c.waste_production > 0.0 &&
+        (rc = cw_field_create(c.nh, s->w.data(), s->h.data(), s->d.data(), c.o2_dcoef, 0.0, 0.0, &s->wst)) != CW_OK) {
+        cw_sim_destroy(s);
+        return rc;
+    }
+    if (c.necrotic_production > 0.0) {
+        if (c.necrotic_type < 0) {
+            cw_sim_destroy(s);
+            return fail(CW_ERR_CONFIG, "a necrotic factor is released by necrotic cells, and this simulation has none");
+        }
+        if ((rc = cw_field_create(c.nh, s->w.data(), s->h.data(), s->d.data(), c.o2_dcoef, 0.0, 0.0, &s->nfc)) !=
+            CW_OK) {
+            cw_sim_destroy(s);
+            return rc;
+        }
     }
     // per-cell device state
     s->nc = s->lat->ncells;
@@ -359,6 +420,19 @@ int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out) {
         cw_sim_destroy(s);
         return rc;
     }
+    if ((rc = dalloc(&s->d_step, 1)) || (rc = dalloc(&s->died_at, nc)) || (rc = dalloc(&s->cell_wst, nc)) ||
+        (rc = dalloc(&s->cell_nfc, nc)) || (rc = dalloc(&s->wst_rate, nc)) || (rc = dalloc(&s->nfc_rate, nc))) {
+        cw_sim_destroy(s);
+        return rc;
+    }
+    if ((c.o2_hold == 3 || s->wst || s->nfc) && (rc = dalloc(&s->bath, (size_t)s->lat->g.total)) != CW_OK) {
+        cw_sim_destroy(s);
+        return rc;
+    }
+    CW_CUDA(cudaMemsetAsync(s->d_step, 0, sizeof(uint32_t), stream()));
+    CW_CUDA(cudaMemsetAsync(s->died_at, 0xFF, sizeof(int32_t) * nc, stream()));
+    CW_CUDA(cudaMemsetAsync(s->cell_wst, 0, sizeof(double) * nc, stream()));
+    CW_CUDA(cudaMemsetAsync(s->cell_nfc, 0, sizeof(double) * nc, stream()));
     CW_CUDA(cudaMemcpyAsync(s->d_sink, s->sink.data(), 8 * sizeof(double), cudaMemcpyHostToDevice, stream()));
     std::vector<double> st((size_t)nc * S);
     const std::vector<double> &init = network_initial(net);
@@ -387,6 +461,10 @@ int cw_sim_destroy(cw_sim s) {
     cw_lattice_destroy(s->lat);
     cw_field_destroy(s->o2);
     cw_field_destroy(s->sig);
+    cw_field_destroy(s->wst);
+    cw_field_destroy(s->nfc);
+    dfree(s->cell_wst); dfree(s->cell_nfc); dfree(s->wst_rate); dfree(s->nfc_rate); dfree(s->died_at);
+    dfree(s->d_step); dfree(s->bath);
     dfree(s->d_sink); dfree(s->cell_o2); dfree(s->cell_sig); dfree(s->sum); dfree(s->secretion); dfree(s->count);
     dfree(s->state); dfree(s->inputs); dfree(s->alive); dfree(s->target32);
     s->sites.release();
@@ -534,11 +612,14 @@ static int enqueue_phase(cw_sim_s *s, int p, const cw_relax_opts &o) {
     if ((rc = network_mechanics_device(s->net, s->state, nc, nc, s->target32)) != CW_OK) return rc;
     k_fates<<<(unsigned)blocks(nc), T, 0, stream()>>>(s->alive, s->state, nc, network_role(s->net, 1),
                                                       c.death_threshold, c.necrotic_type, s->target32, s->lat->type,
-                                                      s->lat->volume, s->lat->target, s->lat->lambda, c.lambda_volume);
+                                                      s->lat->volume, s->lat->target, s->lat->lambda, c.lambda_volume,
+                                                      s->died_at, s->d_step);
     CW_LAUNCHED();
     for (int k = 0; k < c.sweeps; ++k)
         if ((rc = lattice_sweep(s->lat)) != CW_OK) return rc;
     if ((rc = division_step(s)) != CW_OK) return rc;
+    k_step_advance<<<1, 1, 0, stream()>>>(s->d_step);
+    CW_LAUNCHED();
     return CW_OK;
 }
 
@@ -649,7 +730,7 @@ int cw_sim_step(cw_sim s, uint32_t nsteps) {
         o.window = s->sor_window;
         const bool graph_ok = c.use_graphs && c.precision == CW_FP32_DC && c.relax_every <= 1 && !s->tune.active &&
                               s->depth_tuned && s->steps >= 2 && !s->last.empty() &&
-                              (!s->sig || !s->last_sig.empty());
+                              (!s->sig || !s->last_sig.empty()) && !s->wst && !s->nfc && c.o2_hold != 3;
         if (graph_ok) {
             if (!s->graphs && (rc = build_graphs(s, o)) != CW_OK) return rc;
             if ((rc = step_graph(s, o)) != CW_OK) return rc;
@@ -657,6 +738,16 @@ int cw_sim_step(cw_sim s, uint32_t nsteps) {
         }
         bool tuning = solve && s->tune.active && s->steps > 0;  // the first solve starts from scratch: not booked
         if (tuning) tune_assign(s);
+        if (solve && s->bath) {
+            // the bath of the lattice as it stands (hold_medium_bath, coupling.rs:156-158)
+            if ((rc = lattice_bath_enqueue(s->lat, s->bath)) != CW_OK) return rc;
+            if (c.o2_hold == 3) {
+                k_hold_from_mask<<<(unsigned)blocks(s->o2->g.total), T, 0, stream()>>>(s->bath, s->o2->g.total, 1.0,
+                                                                                      s->o2->held, s->o2->c);
+                CW_LAUNCHED();
+                s->o2->held_dirty = true;
+            }
+        }
         if (solve) {
             // 1. downward coupling and the oxygen solve
             if ((rc = couple_uptake_device(s->o2, s->lat, s->d_sink, 8, s->o2->lin_sink, s->sites)) != CW_OK) return rc;
@@ -689,6 +780,41 @@ int cw_sim_step(cw_sim s, uint32_t nsteps) {
             if ((rc = couple_means_device(s->sig, s->lat, s->sum, s->count, s->cell_sig, s->sites)) != CW_OK)
                 return rc;
         }
+        // 2b. the released fields: the waste from the living, the necrotic
+        // factor from the dead, held at zero on the bath (settle_waste,
+        // settle_necrotic_factor; simulation.rs:2057-2113)
+        if ((s->wst || s->nfc) && solve) {
+            k_release_rates<<<(unsigned)blocks(nc), T, 0, stream()>>>(
+                s->alive, s->lat->type, s->lat->volume, s->died_at, s->d_step, nc, c.necrotic_type,
+                c.waste_production, c.necrotic_production, c.necrotic_release_for, s->wst ? s->wst_rate : nullptr,
+                s->nfc ? s->nfc_rate : nullptr);
+            CW_LAUNCHED();
+            cw_field_s *fs[2] = {s->wst, s->nfc};
+            double *rates[2] = {s->wst_rate, s->nfc_rate};
+            double *means[2] = {s->cell_wst, s->cell_nfc};
+            std::vector<cw_relax_stats> *sts[2] = {&s->last_wst, &s->last_nfc};
+            for (int q = 0; q < 2; ++q) {
+                cw_field_s *f = fs[q];
+                if (!f) continue;
+                if ((rc = couple_production_device(f, s->lat, rates[q], s->sites)) != CW_OK) return rc;
+                k_hold_from_mask<<<(unsigned)blocks(f->g.total), T, 0, stream()>>>(s->bath, f->g.total, 0.0, f->held,
+                                                                                  f->c);
+                CW_LAUNCHED();
+                f->held_dirty = true;
+                sts[q]->resize(c.nh);
+                const double *om = c.omega > 0.0 ? nullptr : s->omega[0].data();
+                if ((rc = field_relax(f, &o, om, sts[q]->data())) != CW_OK) return rc;
+                if ((rc = couple_means_device(f, s->lat, s->sum, s->count, means[q], s->sites)) != CW_OK) return rc;
+            }
+            k_inputs_released<<<(unsigned)blocks(nc), T, 0, stream()>>>(s->wst ? s->cell_wst : nullptr,
+                                                                        s->nfc ? s->cell_nfc : nullptr, nc, s->inputs);
+            CW_LAUNCHED();
+        } else if (s->wst || s->nfc) {
+            // a step between solves: the cells read the last means
+            k_inputs_released<<<(unsigned)blocks(nc), T, 0, stream()>>>(s->wst ? s->cell_wst : nullptr,
+                                                                        s->nfc ? s->cell_nfc : nullptr, nc, s->inputs);
+            CW_LAUNCHED();
+        }
         // 3. every living network
         if ((rc = network_step_device(s->net, s->state, s->inputs, nc, nc, nc, c.dt, c.substeps, s->alive)) != CW_OK)
             return rc;
@@ -697,12 +823,14 @@ int cw_sim_step(cw_sim s, uint32_t nsteps) {
         k_fates<<<(unsigned)blocks(nc), T, 0, stream()>>>(s->alive, s->state, nc, survival, c.death_threshold,
                                                           c.necrotic_type, s->target32, s->lat->type,
                                                           s->lat->volume, s->lat->target, s->lat->lambda,
-                                                          c.lambda_volume);
+                                                          c.lambda_volume, s->died_at, s->d_step);
         CW_LAUNCHED();
         // 5. the lattice, then 6. division
         for (int k = 0; k < c.sweeps; ++k)
             if ((rc = lattice_sweep(s->lat)) != CW_OK) return rc;
         if ((rc = division_step(s)) != CW_OK) return rc;
+        k_step_advance<<<1, 1, 0, stream()>>>(s->d_step);
+        CW_LAUNCHED();
         if (tuning && ++s->tune.done >= s->tune.steps) tune_finish(s);
         (void)S;
     }
@@ -734,7 +862,7 @@ int cw_sim_lattice(cw_sim s, cw_lattice *lat) {
 }
 
 int cw_sim_field(cw_sim s, int32_t which, cw_field *f) {
-    *f = which == 0 ? s->o2 : s->sig;
+    *f = which == 0 ? s->o2 : which == 1 ? s->sig : which == 2 ? s->wst : which == 3 ? s->nfc : nullptr;
     if (!*f) return fail(CW_ERR_NOT_FOUND, "no such field");
     return CW_OK;
 }
@@ -751,6 +879,7 @@ int cw_sim_stats(cw_sim s, double *out) {
     CW_CUDA(cudaStreamSynchronize(stream()));
     dfree(d_out);
     if ((rc = lattice_pass_error(s->lat)) != CW_OK) return rc;
+    if (s->bath && (rc = lattice_bath_error()) != CW_OK) return rc;
     for (uint32_t k = 0; k < nh; ++k) {
         out[4 * k + 2] = (double)s->last[k].sweeps;
         out[4 * k + 3] = s->last[k].residual;

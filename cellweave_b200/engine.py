@@ -282,6 +282,14 @@ class CpmLattice:
         call("cw_lattice_cell_count", self._h, hist, C.byref(n))
         return int(n.value)
 
+    def bath(self, hist=0):
+        """The pixels hold_medium_bath holds (coupling.rs:156-158): medium joined to the
+        box's outer layer through medium; uint8 per pixel, [d, h, w]."""
+        w, h, d = self.dims[hist]
+        out = np.empty(w * h * d, np.uint8)
+        call("cw_lattice_bath", self._h, int(hist), ptr(out))
+        return out.reshape(d, h, w)
+
     def set_copy_neighbourhood(self, moore: bool):
         """Copies from a face neighbour (try_flip, cpm.rs:797-838; the default) or, with
         moore=True, from any pixel at Chebyshev distance 1 (an extension)."""
@@ -610,7 +618,8 @@ class Simulation:
                  nfields=1, o2_dcoef=1.0, o2_sink_by_type=(0.0, 0.01, 0.01), o2_background_sink=0.0, o2_hold=0, signal_dcoef=1.0,
                  signal_decay=0.01, signal_secretion=0.05, hypoxic_level=0.1, tolerance=1e-6, precision=FP32_DC,
                  omega=None, inner_sweeps=0, relax_every=1, dt=0.01, substeps=8, sweeps=1, death_threshold=0.25,
-                 necrotic_type=-1, use_graphs=True, divide=True, max_cells=2000, spare_cells=0):
+                 necrotic_type=-1, use_graphs=True, divide=True, max_cells=2000, spare_cells=0,
+                 waste_production=0.0, necrotic_production=0.0, necrotic_release_for=-1):
         self.dims, w, h, z = _dims(dims)
         self._keep = [w, h, z]
         nc = np.array(ncells, np.uint32)
@@ -627,7 +636,8 @@ class Simulation:
                              float(hypoxic_level), float(tolerance), int(precision), float(omega or 0.0), int(inner_sweeps),
                              int(relax_every), float(dt), int(substeps), int(sweeps), float(death_threshold),
                              int(necrotic_type), int(bool(use_graphs)), int(bool(divide)), int(max_cells),
-                             int(spare_cells))
+                             int(spare_cells), float(waste_production), float(necrotic_production),
+                             int(necrotic_release_for))
         handle = C.c_void_p()
         call("cw_sim_create", C.byref(cfg), network.handle, C.byref(handle))
         self._h = handle

@@ -91,6 +91,11 @@ int cw_lattice_pass_rounds(cw_lattice lat, uint32_t *rounds);
  * (cpm.rs:274-301): 1 faces only, 2 and 3 the wider reach and its divisor. */
 int cw_lattice_set_contact(cw_lattice lat, int32_t K, const double *J, int32_t order);
 int cw_lattice_set_temperature(cw_lattice lat, double temperature);
+/* The medium the bath reaches in history `hist`: out[i] = 1 for the pixels
+ * hold_medium_bath would hold (coupling.rs:156-158, pde.rs:550-631: medium
+ * joined to the box's outer layer through medium, 4-connected in the plane,
+ * 6-connected in a volume), 0 elsewhere.  out holds one byte per pixel. */
+int cw_lattice_bath(cw_lattice lat, uint32_t hist, uint8_t *out);
 /* divide_across (cpm.rs:1087-1160) for cells `ids` of history `hist`, each
  * across the plane through its centre of mass with normal normals[3k..3k+2]
  * (the third component counts in a volume only): the pixels on the side the
@@ -365,7 +370,9 @@ typedef struct {
     double o2_dcoef;
     const double *o2_sink_by_type; /* K first-order sinks k per type (0 for the medium) */
     double o2_background_sink;   /* first-order sink of medium pixels (stroma around a vessel) */
-    int32_t o2_hold;             /* 0 row y=0, 1 column x=w/2, 2 every face of the box */
+    int32_t o2_hold;             /* 0 row y=0, 1 column x=w/2, 2 every face of the box, 3 the bath: the
+                                    medium joined to the box's outer layer, taken every step
+                                    (declare_sources with OxygenSource::Bath, simulation.rs:2138-2146) */
     double signal_dcoef, signal_decay, signal_secretion, hypoxic_level;
     double tolerance;            /* residual tolerance of every field solve */
     int32_t precision;           /* CW_FP64 or CW_FP32_DC */
@@ -381,6 +388,14 @@ typedef struct {
     int32_t divide;              /* 1: the division step; 0: none */
     int32_t max_cells;           /* living cells a history divides up to (<= 0: 2000, the reference's default) */
     int32_t spare_cells;         /* records per history for daughters (<= 0: max_cells) */
+    /* The released fields (settle_waste / settle_necrotic_factor and
+     * settle_released, simulation.rs:2057-2113, 2546-2570), each diffusing as
+     * oxygen does, held at zero on the bath, solved like the other fields, its
+     * mean over a cell the cell's `waste` / `necrotic_factor` input.  They run
+     * on the step's un-captured path (no CUDA graphs). */
+    double waste_production;     /* > 0: what a living cell's pixel releases a step (Waste, types.rs:240-244) */
+    double necrotic_production;  /* > 0: what a necrotic cell's pixel releases (NecroticFactor, types.rs:256-266) */
+    int32_t necrotic_release_for;/* steps after the one it died at a necrotic cell releases; < 0: while it is there */
 } cw_sim_config;
 int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out);
 int cw_sim_destroy(cw_sim sim);

@@ -96,13 +96,18 @@ class CpuHistory:
         z, y, x = np.mgrid[0:d, 0:h, 0:w]
         hold = cfg.get("o2_hold", 0)
         held = (y == 0) if hold == 0 else (x == w // 2) if hold == 1 else (
-            (x == 0) | (y == 0) | (z == 0) | (x == w - 1) | (y == h - 1) | (z == d - 1))
+            (x == 0) | (y == 0) | (z == 0) | (x == w - 1) | (y == h - 1) | (z == d - 1)) if hold == 2 else (
+            np.zeros_like(y, bool))  # 3: the bath, taken every step
         self.o2.held[:] = held.reshape(-1)
         self.o2.values[self.o2.held == 1] = 1.0
         self.o2.lin_sink = np.zeros(n)
         self.sig = None
         if cfg.get("nfields", 1) == 2:
             self.sig = O.Field(w, h, d, cfg["signal_dcoef"], cfg["signal_decay"], 0.0)
+        # the released fields (simulation.rs:2057-2113): they diffuse as oxygen does
+        self.wst = O.Field(w, h, d, cfg["o2_dcoef"], 0.0, 0.0) if cfg.get("waste_production", 0.0) > 0 else None
+        self.nfc = O.Field(w, h, d, cfg["o2_dcoef"], 0.0, 0.0) if cfg.get("necrotic_production", 0.0) > 0 else None
+        self.cell_wst = self.cell_nfc = None
         spec = tomllib.loads(cfg.get("network_toml") or synthetic.network_toml(cfg["S"], cfg["S"]))
         self.net = O.compile_network(spec, cfg["target_volume"])
         self.state = np.tile(self.net.initial, (self.ncap, 1))
@@ -111,6 +116,18 @@ class CpuHistory:
         sink[:len(cfg["o2_sink_by_type"])] = cfg["o2_sink_by_type"]
         self.sink = sink
         self.steps = 0
+        self.died_at = np.full(self.ncap, -1, np.int64)
+
+    def _settle_released(self, field, per_cell):
+        """settle_released (simulation.rs:2546-2570): production from the cells
+        that release, the bath held at zero, relaxed; the per-cell means."""
+        c = self.cfg
+        g = self.lat.grid
+        field.production = O.apply_production(g, per_cell)
+        field.held[:] = 0
+        field.hold_bath(g == 0, 0.0)
+        field.relax(c["tolerance"], 200_000, omega=c.get("omega") or 0.0, stop=1, threads=1)
+        return O.mean_per_cell(g, field.values, self.ncap)
 
     def step(self):
         c = self.cfg
@@ -121,6 +138,10 @@ class CpuHistory:
         sink[cells] = self.sink[t[g[cells]]]
         sink[g == 0] = c.get("o2_background_sink", 0.0)
         self.o2.lin_sink = sink
+        if c.get("o2_hold", 0) == 3:
+            # the bath as the lattice stands (declare_sources, simulation.rs:2138-2146)
+            self.o2.held[:] = 0
+            self.o2.hold_bath(g == 0, 1.0)
         omega = c.get("omega") or 0.0
         rc, _ = self.o2.relax(c["tolerance"], 200_000, omega=omega, stop=1, threads=1)
         o2m = O.mean_per_cell(g, self.o2.values, self.ncap)
@@ -131,6 +152,14 @@ class CpuHistory:
             sec = np.where(alive & (o2m < c["hypoxic_level"]), c["signal_secretion"], 0.0)
             self.sig.production = O.apply_production(g, sec)
             self.sig.relax(c["tolerance"], 200_000, omega=omega, stop=1, threads=1)
+        if self.wst is not None:
+            self.cell_wst = self._settle_released(self.wst, np.where(alive, c["waste_production"], 0.0))
+        if self.nfc is not None:
+            rel = c.get("necrotic_release_for", -1)
+            releasing = (rel < 0) | (self.died_at < 0) | (self.steps <= self.died_at + rel)
+            dead = (t == nec) & (self.lat.volume > 0) & releasing
+            dead[0] = False
+            self.cell_nfc = self._settle_released(self.nfc, np.where(dead, c["necrotic_production"], 0.0))
         # a necrotic cell gives up 2 pixels a step until it is gone (simulation.rs:1230-1262)
         if nec >= 0:
             dying = np.nonzero((t == nec) & (self.lat.volume > 0))[0]
@@ -144,12 +173,17 @@ class CpuHistory:
             ins[:, 1] = 0.2
             # crowding (simulation.rs:2523-2527): 1 - volume / reference volume, clamped
             ins[:, 2] = np.clip(1.0 - self.lat.volume[idx] / float(max(c["target_volume"], 1)), 0.0, 1.0)
+            if self.cell_wst is not None:
+                ins[:, 4] = self.cell_wst[idx]
+            if self.cell_nfc is not None:
+                ins[:, 5] = self.cell_nfc[idx]
             st = np.ascontiguousarray(self.state[idx])
             O.network_step(self.net, st, ins, c["dt"], c["substeps"])
             self.state[idx] = st
             tg = O.network_mechanics(self.net, st)
             dead = (st[:, self.net.survival] < c.get("death_threshold", 0.25)) if nec >= 0 else np.zeros(len(idx), bool)
             t[idx[dead]] = nec
+            self.died_at[idx[dead]] = self.steps
             live = idx[~dead]
             self.lat.target[live] = np.minimum(tg[~dead], 2**31 - 1).astype(np.int32)
             self.lat.lam[live] = c["lambda_volume"]

@@ -232,3 +232,46 @@ def test_divisions_are_bit_exact_with_the_oracle(volume):
     np.testing.assert_array_equal(cells["target"][:used], lat.target[:used])
     assert g.cell_count() == used
     assert g.records_match_grid()
+
+
+def oracle_bath(grid):
+    d, h, w = grid.shape
+    o = O.Field(w, h, d, 0.2, 0.0, 0.0)
+    o.hold_bath((grid.reshape(-1) == 0), 1.0)
+    return o.held.reshape(d, h, w).astype(np.uint8)
+
+
+def test_the_device_bath_is_the_reference_flood():
+    # hold_medium_bath (coupling.rs:156-158 over pde.rs:550-631): the medium
+    # joined to the box's outer layer; the device's union-find against the
+    # oracle's flood, in a batch of uneven lattices: sheets of cells, a ring
+    # that shuts medium in, a random maze, a volume
+    rng = np.random.default_rng(9)
+    grids = []
+    g, _ = sheet(seed=3, size=96, ncell=60)
+    grids.append(g)
+    ring = seeding.empty(40, 30)
+    y, x = np.mgrid[0:30, 0:40]
+    ring[0][(np.maximum(abs(x - 20), abs(y - 15)) == 6)] = 1
+    ring[0][0, 5:9] = -1
+    grids.append(ring)
+    maze = np.where(rng.random((1, 70, 130)) < 0.45, 1, 0).astype(np.int32)
+    grids.append(maze)
+    vol = np.where(rng.random((12, 14, 16)) < 0.4, 2, 0).astype(np.int32)
+    grids.append(vol)
+    recs = []
+    for gr in grids:
+        r = seeding.Records()
+        n = int(gr.max()) + 1
+        r.type = [0] + [1] * (n - 1)
+        r.volume = list(seeding.recount(gr, n))
+        r.target = [0] + [49] * (n - 1)
+        r.lam = [0.0] + [1.0] * (n - 1)
+        recs.append(r)
+    flat = cw.CpmLattice.from_grids(grids[:3], recs[:3], 10.0, J3, 1, seeds=[1, 2, 3])
+    box = cw.CpmLattice.from_grids(grids[3:], recs[3:], 10.0, J3, 1, seeds=[4])  # a batch is flat or a volume
+    for k, gr in enumerate(grids):
+        lat, hist = (flat, k) if k < 3 else (box, 0)
+        np.testing.assert_array_equal(lat.bath(hist), oracle_bath(gr), err_msg=f"lattice {k}")
+    # the shut-in medium inside the ring is not bath; the rest of the medium is
+    assert flat.bath(1)[0, 15, 20] == 0 and flat.bath(1)[0, 1, 1] == 1

@@ -142,3 +142,97 @@ def test_division_grows_the_population_inside_the_oracle_band():
         assert sim.records_match_grid(k)
     grown = np.array([sim.lattice().cell_count(k) for k in range(SEEDS)]) - start
     assert grown.mean() > 5
+
+
+def released_network(S):
+    # the synthetic network, its survival node also damaged by the necrotic
+    # factor and its growth node inhibited by the waste
+    text = synthetic.network_toml(S, S)
+    old = '{ kind = "relaxes_to", value = 0.9, rate = 2.0 },'
+    assert text.count(old) == 1
+    text = text.replace(old, old + '\n  { kind = "damaged_above", source = "necrotic_factor", threshold = 0.02, rate = 1.0 },')
+    grow = 'name = "n2"\ninitial = 0.1\nterms = [\n'
+    assert text.count(grow) == 1
+    text = text.replace(grow, grow + '  { kind = "inhibited_by", source = "waste", rate = 0.5 },\n')
+    return text
+
+
+def test_the_released_fields_stay_inside_the_oracle_band():
+    # settle_waste / settle_necrotic_factor (simulation.rs:2057-2113): the
+    # waste from every living pixel, the necrotic factor from the dead for 20
+    # steps after they died, both held at zero on the bath and read by the
+    # network; living cells, their mean oxygen, waste and factor inside the
+    # oracle's 32-seed band
+    cfg = small_cord()
+    cfg.update(waste_production=0.01, necrotic_production=0.05, necrotic_release_for=20)
+    S = cfg.pop("S")
+    text = released_network(S)
+    d = tempfile.mkdtemp()
+    p = os.path.join(d, "n.toml")
+    open(p, "w").write(text)
+    net = cw.Network.load(p, cfg["target_volume"])
+    sim = cw.Simulation(net, **dict(cfg, seeds=[s + 90_000 for s in cfg["seeds"]]))
+    ora = [CpuHistory(dict(cfg, S=S, network_toml=text), k) for k in range(SEEDS)]
+    names = ("living", "mean oxygen", "mean waste", "mean necrotic factor")
+    for step in range(1, 31):
+        sim.step(1)
+        for h in ora:
+            h.step()
+        if step not in (5, 15, 30):
+            continue
+        dev, ref = [], []
+        lat = sim.lattice()
+        for k in range(SEEDS):
+            cells = lat.cells(hist=k)
+            g = sim.grid(k)
+            vol, types = cells["volume"], cells["type"]
+            living = np.flatnonzero((vol > 0) & (types != 3) & (np.arange(len(vol)) > 0))
+            row = [len(living)]
+            for f in (0, 2, 3):
+                m = O.mean_per_cell(g, sim.field_values(f, k), len(vol))
+                row.append(float(m[living].mean()))
+            dev.append(row)
+            h = ora[k]
+            hl = np.flatnonzero((h.lat.volume > 0) & (h.lat.type != 3) & (np.arange(len(h.lat.volume)) > 0))
+            rrow = [len(hl)]
+            for fld in (h.o2, h.wst, h.nfc):
+                m = O.mean_per_cell(h.lat.grid, fld.values, len(h.lat.volume))
+                rrow.append(float(m[hl].mean()))
+            ref.append(rrow)
+        dev, ref = np.array(dev), np.array(ref)
+        assert ref[:, 2].mean() > 1e-3
+        # the factor once the first dead have stopped releasing is what the
+        # solves' tolerance leaves of a sourceless field: compared while they release
+        checked = names if step <= 15 else names[:3]
+        if step <= 15:
+            assert ref[:, 3].mean() > 1e-3
+        for j, name in enumerate(checked):
+            assert within_band(dev[:, j], ref[:, j]), (step, name, dev[:, j].mean(), ref[:, j].mean(),
+                                                        ref[:, j].std())
+    for k in range(SEEDS):
+        assert sim.records_match_grid(k)
+
+
+def test_the_bath_holds_the_oxygen_where_the_medium_reaches_the_edge():
+    # declare_sources with a bath (simulation.rs:2138-2146): the medium the
+    # bath reaches held at the source's level, the cells taking it up
+    cfg = small_cord(4)
+    cfg.update(o2_hold=3)
+    S = cfg.pop("S")
+    d = tempfile.mkdtemp()
+    p = os.path.join(d, "n.toml")
+    open(p, "w").write(synthetic.network_toml(S, S))
+    net = cw.Network.load(p, cfg["target_volume"])
+    sim = cw.Simulation(net, **cfg)
+    baths = [sim.lattice().bath(k).reshape(-1) for k in range(4)]
+    grids = [sim.grid(k).reshape(-1).copy() for k in range(4)]
+    sim.step(1)
+    for k in range(4):
+        v = sim.field_values(0, k)
+        bath = baths[k].astype(bool)
+        assert bath.sum() > 0
+        np.testing.assert_array_equal(v[bath], 1.0)
+        assert v[grids[k] > 0].min() < 1.0
+        o = O.Field(64, 64, 1, 1.0, 0.0, 0.0)
+        o.hold_bath(grids[k] == 0, 1.0)
+        np.testing.assert_array_equal(baths[k], o.held.astype(np.uint8))
