@@ -68,6 +68,12 @@ class Mutation(C.Structure):
                 ("value", C.c_double), ("source", C.c_int32), ("pad", C.c_int32)]
 
 
+class Measurements(C.Structure):
+    _fields_ = [("mcs", C.c_uint64), ("cycling", C.c_uint64), ("quiescent", C.c_uint64), ("necrotic", C.c_uint64),
+                ("born", C.c_uint64), ("gone", C.c_uint64), ("vessel", C.c_uint64), ("tissue_radius", C.c_double),
+                ("necrotic_radius", C.c_double), ("viable_depth", C.c_double)]
+
+
 class FitConfig(C.Structure):
     _fields_ = [("dcoef", C.c_double), ("uptake", C.c_double * 3), ("vessel_value", C.c_double),
                 ("vessel_x", C.c_int32), ("egf", C.c_double), ("signal_dcoef", C.c_double),
@@ -91,7 +97,7 @@ class SimConfig(C.Structure):
                 ("death_threshold", C.c_double), ("necrotic_type", C.c_int32), ("use_graphs", C.c_int32),
                 ("divide", C.c_int32), ("max_cells", C.c_int32), ("spare_cells", C.c_int32),
                 ("waste_production", C.c_double), ("necrotic_production", C.c_double),
-                ("necrotic_release_for", C.c_int32)]
+                ("necrotic_release_for", C.c_int32), ("subsweeps", C.c_int32)]
 
 
 P = C.c_void_p
@@ -164,6 +170,8 @@ SIGNATURES = {
     "cw_network_mechanics_batch": (C.c_int, [P, I64, P, P, P]),
     "cw_network_mutate": (C.c_int, [P, D, D, P, P]),
     "cw_lattice_bath": (C.c_int, [P, U32, P]),
+    "cw_lattice_set_subsweeps": (C.c_int, [P, I32]),
+    "cw_sim_measure": (C.c_int, [P, P]),
     "cw_network_rewire": (C.c_int, [P, P, P, P]),
     "cw_network_step_clones": (C.c_int, [I32, P, I64, P, P, P, D, I32]),
     "cw_sim_create": (C.c_int, [P, P, P]),

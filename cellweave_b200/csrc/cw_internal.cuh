@@ -209,6 +209,7 @@ struct cw_lattice_s {
     int32_t order = 1;
     double temperature = 10.0;
     bool copy_moore = false;         // copies from any Chebyshev neighbour, not only across faces
+    int32_t subsweeps = 1;           // sweeps of every colour a Monte Carlo step, each pixel in each with 1 / this
     uint32_t mcs = 0;
     std::vector<uint64_t> seed;
     uint2 *d_keys = nullptr;         // Philox key per history
@@ -269,6 +270,7 @@ int field_dc_prepare(cw_field_s *f, int depth, int window, const std::vector<dou
 int field_relax_collect(cw_field_s *f, std::vector<cw_relax_stats> &out, bool &all_settled);
 int lattice_recount(cw_lattice_s *lat, int32_t *vol_out, int32_t *surf_out);
 int lattice_sweep(cw_lattice_s *lat);
+int lattice_subsweep(cw_lattice_s *lat);
 int lattice_pass_error(cw_lattice_s *l);
 int lattice_recount_surfaces(cw_lattice_s *l);  // surfaces from the grid into the records, no sync
 int lattice_divide_enqueue(cw_lattice_s *l, const uint8_t *alive, int max_living, double *state, int S);

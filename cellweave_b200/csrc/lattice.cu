@@ -59,6 +59,7 @@ struct LatView {
     double temperature;
     int32_t surface_on;
     int32_t copy_moore;
+    uint32_t take_below;   // sub-sweeps: a pixel attempts when its draw is below this (0: every pixel)
 };
 
 struct Tables {
@@ -427,6 +428,13 @@ __global__ void __launch_bounds__(T) k_cpm_pass(LatView L, Tables tabs, const in
 #pragma unroll
                 for (int q = 0; q < 27; ++q) edge |= nb[q] != src;
             }
+            // with sub-sweeps, a pixel attempts in this one with probability
+            // 1 / subsweeps (its own draw), so that over the Monte Carlo step
+            // its attempts are Binomial(subsweeps, 1 / subsweeps), near the
+            // Poisson(1) of random pixels
+            if (edge && src != OBST && L.take_below &&
+                philox((uint32_t)i, mcs, 4u, 0u, L.keys[h].x, L.keys[h].y).x >= L.take_below)
+                edge = false;
             if (edge && src != OBST) {
                 const uint2 key = L.keys[h];
                 const uint4 r = philox((uint32_t)i, mcs, 0u, 0u, key.x, key.y);
@@ -707,6 +715,7 @@ static LatView lat_view(cw_lattice_s *l) {
     v.dims = l->g.d_dims; v.off = l->g.d_off; v.cell_off = l->d_cell_off; v.keys = l->d_keys;
     v.K = l->K; v.nreach = l->nreach; v.period = l->period; v.ncol = l->ncol; v.across = l->across;
     v.temperature = l->temperature; v.surface_on = l->surface_on ? 1 : 0; v.copy_moore = l->copy_moore ? 1 : 0;
+    v.take_below = l->subsweeps > 1 ? (uint32_t)(4294967296.0 / (double)l->subsweeps) : 0u;
     return v;
 }
 
@@ -766,6 +775,17 @@ int lattice_recount(cw_lattice_s *l, int32_t *vol_out, int32_t *surf_out) {
 // colour order, then one cooperative launch per colour (its rounds meet at a
 // grid barrier), the claims and control words cleared before each.
 int lattice_sweep(cw_lattice_s *l) {
+    for (int s = 0; s < std::max(l->subsweeps, 1); ++s) {
+        int rc = lattice_subsweep(l);
+        if (rc != CW_OK) return rc;
+    }
+    l->mcs += 1;
+    return CW_OK;
+}
+
+// One sweep of every colour (a whole Monte Carlo step with one sub-sweep);
+// the device's step counter advances by one per sub-sweep.
+int lattice_subsweep(cw_lattice_s *l) {
     LatDevice d = dev_of(l);
     k_colour_order<<<1, 128, 0, stream()>>>(l->d_keys, l->g.nh, l->ncol, d.mcs, d.mcs + 1, d.perm,
                                             l->pctl + CTL_KEYS);
@@ -802,7 +822,6 @@ int lattice_sweep(cw_lattice_s *l) {
         CW_CUDA(cudaLaunchKernelExC(&cfg, (const void *)k_cpm_pass, args));
         count_launch(1);
     }
-    l->mcs += 1;
     return CW_OK;
 }
 
@@ -923,6 +942,12 @@ int cw_lattice_set_copy_nbhd(cw_lattice l, int32_t nbhd) {
     return l->build_plans();
 }
 
+int cw_lattice_set_subsweeps(cw_lattice l, int32_t subsweeps) {
+    if (subsweeps < 1 || subsweeps > 64) return fail(CW_ERR_CONFIG, "1 to 64 sub-sweeps a Monte Carlo step");
+    l->subsweeps = subsweeps;
+    return CW_OK;
+}
+
 int cw_lattice_set_temperature(cw_lattice l, double temperature) {
     if (!(temperature > 0.0)) return fail(CW_ERR_CONFIG, "the temperature must be positive");
     l->temperature = temperature;
@@ -1029,7 +1054,9 @@ int cw_lattice_set_seed(cw_lattice l, uint32_t hist, uint64_t seed) {
 
 int cw_lattice_set_mcs(cw_lattice l, uint32_t mcs) {
     l->mcs = mcs;
-    CW_CUDA(cudaMemcpyAsync(l->d_flag, &mcs, sizeof mcs, cudaMemcpyHostToDevice, stream()));
+    // the draws count sub-sweeps
+    const uint32_t eff = mcs * (uint32_t)std::max(l->subsweeps, 1);
+    CW_CUDA(cudaMemcpyAsync(l->d_flag, &eff, sizeof eff, cudaMemcpyHostToDevice, stream()));
     CW_CUDA(cudaStreamSynchronize(stream()));
     return CW_OK;
 }

@@ -149,6 +149,61 @@ constexpr double DIVISION_RATIO = 1.4;    // of the reference volume (simulation
 constexpr double QUIESCENCE_THRESHOLD = 0.45;  // hypoxia response that stops cycling (simulation.rs:117)
 constexpr int DEFAULT_MAX_CELLS = 2000;   // simulation.rs:61
 
+// Measure::measure's counts per history (measure.rs:133-170): one block a
+// history over its records; out[8 h ..] = cycling, quiescent, necrotic,
+// living area, necrotic area, born, gone, lines holding living pixels.
+__global__ void k_measure(const int32_t *type, const int32_t *volume, const int64_t *cell_off, const int32_t *used,
+                          int necrotic, const double *state, int hyp, int64_t nc, const uint8_t *lines,
+                          const int64_t *line_off, unsigned long long *out) {
+    const int h = blockIdx.x;
+    __shared__ unsigned long long acc[8];
+    if (threadIdx.x < 8) acc[threadIdx.x] = 0ull;
+    __syncthreads();
+    const int64_t c0 = cell_off[h];
+    const int32_t n = used[h];
+    unsigned long long v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int64_t k = 1 + threadIdx.x; k < n; k += blockDim.x) {
+        const int64_t c = c0 + k;
+        const int32_t vol = volume[c];
+        const bool dead = necrotic >= 0 && type[c] == necrotic;
+        if (vol == 0) {
+            if (dead) v[6] += 1;
+            continue;
+        }
+        if (dead) {
+            v[2] += 1;
+            v[4] += (unsigned long long)vol;
+        } else {
+            if (hyp < 0 || state[(int64_t)hyp * nc + c] < QUIESCENCE_THRESHOLD) v[0] += 1;
+            else v[1] += 1;
+            v[3] += (unsigned long long)vol;
+        }
+    }
+    if (lines)
+        for (int64_t q = line_off[h] + threadIdx.x; q < line_off[h + 1]; q += blockDim.x) v[7] += lines[q];
+    for (int j = 0; j < 8; ++j)
+        if (v[j]) atomicAdd(&acc[j], v[j]);
+    __syncthreads();
+    if (threadIdx.x < 8) out[8 * h + threadIdx.x] = acc[threadIdx.x];
+    if (threadIdx.x == 0) out[8 * h + 5] = (unsigned long long)(n - 1);
+}
+
+// The columns (by_row 0) or rows (1) of each history that hold a living pixel.
+__global__ void k_measure_lines(const int32_t *grid, const int32_t *type, const int32_t *volume,
+                                const int64_t *cell_off, const int4 *dims, const int64_t *off, const int32_t *blk,
+                                int nh, int necrotic, int by_row, const int64_t *line_off, uint8_t *lines) {
+    const int h = plan_history(blk, nh, blockIdx.x);
+    const int4 dm = dims[h];
+    const int64_t local = (int64_t)(blockIdx.x - blk[h]) * blockDim.x + threadIdx.x;
+    if (local >= off[h + 1] - off[h]) return;
+    const int32_t id = grid[off[h] + local];
+    if (id <= 0) return;
+    const int64_t c = cell_off[h] + id;
+    if (volume[c] <= 0 || (necrotic >= 0 && type[c] == necrotic)) return;
+    const int x = (int)(local % dm.x), y = (int)((local / dm.x) % dm.y);
+    lines[line_off[h] + (by_row ? y : x)] = 1;
+}
+
 // Fate and upward coupling (simulation.rs:1212-1309, the necrosis and
 // mechanics branches): a necrotic cell gives up RESORPTION_RATE pixels a step
 // until it is gone; survival below the threshold makes a living cell
@@ -344,6 +399,7 @@ int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out) {
     int rc = cw_lattice_create(c.nh, s->w.data(), s->h.data(), s->d.data(), cap.data(), c.temperature, &s->lat);
     if (rc != CW_OK) { cw_sim_destroy(s); return rc; }
     if ((rc = cw_lattice_set_contact(s->lat, c.K, c.J, c.contact_order)) != CW_OK) { cw_sim_destroy(s); return rc; }
+    if (c.subsweeps > 1 && (rc = cw_lattice_set_subsweeps(s->lat, c.subsweeps)) != CW_OK) { cw_sim_destroy(s); return rc; }
     if (c.divide && (rc = s->lat->div.ensure(s->lat->ncells)) != CW_OK) { cw_sim_destroy(s); return rc; }
     for (uint32_t k = 0; k < c.nh; ++k) {
         uint32_t n = (uint32_t)types[k].size();  // the seeded records; the spares stay free
@@ -883,6 +939,64 @@ int cw_sim_stats(cw_sim s, double *out) {
     for (uint32_t k = 0; k < nh; ++k) {
         out[4 * k + 2] = (double)s->last[k].sweeps;
         out[4 * k + 3] = s->last[k].residual;
+    }
+    return CW_OK;
+}
+
+int cw_sim_measure(cw_sim s, cw_measurements *out) {
+    const cw_sim_config &c = s->cfg;
+    const uint32_t nh = c.nh;
+    cw_lattice_s *l = s->lat;
+    const bool lined = c.o2_hold == 0 || c.o2_hold == 1;
+    std::vector<int64_t> loff(nh + 1, 0);
+    for (uint32_t k = 0; k < nh; ++k) loff[k + 1] = loff[k] + (c.o2_hold == 1 ? s->h[k] : s->w[k]);
+    unsigned long long *d_out;
+    uint8_t *d_lines = nullptr;
+    int64_t *d_loff = nullptr;
+    int rc;
+    if ((rc = dalloc(&d_out, 8 * (size_t)nh)) != CW_OK) return rc;
+    if (lined && ((rc = dalloc(&d_lines, (size_t)loff[nh])) || (rc = dalloc(&d_loff, nh + 1)))) return rc;
+    if (lined) {
+        CW_CUDA(cudaMemsetAsync(d_lines, 0, (size_t)loff[nh], stream()));
+        CW_CUDA(cudaMemcpyAsync(d_loff, loff.data(), sizeof(int64_t) * (nh + 1), cudaMemcpyHostToDevice, stream()));
+        k_measure_lines<<<s->sites.nblocks, T, 0, stream()>>>(l->grid, l->type, l->volume, l->d_cell_off, l->g.d_dims,
+                                                              l->g.d_off, s->sites.d_blk, (int)nh, c.necrotic_type,
+                                                              c.o2_hold == 1 ? 1 : 0, d_loff, d_lines);
+        CW_LAUNCHED();
+    }
+    k_measure<<<nh, 256, 0, stream()>>>(l->type, l->volume, l->d_cell_off, l->d_used, c.necrotic_type, s->state,
+                                        network_role(s->net, 2), s->nc, d_lines, d_loff, d_out);
+    CW_LAUNCHED();
+    std::vector<unsigned long long> h(8 * (size_t)nh);
+    CW_CUDA(cudaMemcpyAsync(h.data(), d_out, sizeof(unsigned long long) * 8 * nh, cudaMemcpyDeviceToHost, stream()));
+    CW_CUDA(cudaStreamSynchronize(stream()));
+    dfree(d_out);
+    dfree(d_lines);
+    dfree(d_loff);
+    const double pi = 3.14159265358979323846;
+    for (uint32_t k = 0; k < nh; ++k) {
+        const unsigned long long *v = &h[8 * (size_t)k];
+        cw_measurements &m = out[k];
+        m.mcs = s->steps > 0 ? s->steps - 1 : 0;
+        m.cycling = v[0];
+        m.quiescent = v[1];
+        m.necrotic = v[2];
+        m.born = v[5];
+        m.gone = v[6];
+        // the held column of o2_hold 1 is the lattice's only obstacle
+        m.vessel = c.o2_hold == 1 ? (uint64_t)s->h[k] * s->d[k] : 0;
+        const uint32_t D = s->d[k];
+        // radius_of (measure.rs:103-113): a disc in the plane, a ball in a volume
+        auto radius = [&](uint64_t size) {
+            if (D <= 1) return std::sqrt((double)size / pi);
+            return std::cbrt(3.0 * (double)size / (4.0 * pi));
+        };
+        const uint64_t living = v[3], dead = v[4];
+        m.tissue_radius = radius(m.vessel + living + dead);
+        m.necrotic_radius = radius(dead);
+        if (c.o2_hold == 0) m.viable_depth = v[7] == 0 ? 0.0 : (double)living / (double)v[7];
+        else if (c.o2_hold == 1) m.viable_depth = v[7] == 0 ? 0.0 : (double)living / (2.0 * (double)v[7]);
+        else m.viable_depth = m.tissue_radius - m.necrotic_radius;
     }
     return CW_OK;
 }

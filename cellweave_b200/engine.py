@@ -290,6 +290,11 @@ class CpmLattice:
         call("cw_lattice_bath", self._h, int(hist), ptr(out))
         return out.reshape(d, h, w)
 
+    def set_subsweeps(self, n: int):
+        """n sweeps of every colour a Monte Carlo step, each pixel attempting in
+        each with probability 1/n: attempts nearer the Poisson(1) of random pixels."""
+        call("cw_lattice_set_subsweeps", self._h, int(n))
+
     def set_copy_neighbourhood(self, moore: bool):
         """Copies from a face neighbour (try_flip, cpm.rs:797-838; the default) or, with
         moore=True, from any pixel at Chebyshev distance 1 (an extension)."""
@@ -619,7 +624,7 @@ class Simulation:
                  signal_decay=0.01, signal_secretion=0.05, hypoxic_level=0.1, tolerance=1e-6, precision=FP32_DC,
                  omega=None, inner_sweeps=0, relax_every=1, dt=0.01, substeps=8, sweeps=1, death_threshold=0.25,
                  necrotic_type=-1, use_graphs=True, divide=True, max_cells=2000, spare_cells=0,
-                 waste_production=0.0, necrotic_production=0.0, necrotic_release_for=-1):
+                 waste_production=0.0, necrotic_production=0.0, necrotic_release_for=-1, subsweeps=1):
         self.dims, w, h, z = _dims(dims)
         self._keep = [w, h, z]
         nc = np.array(ncells, np.uint32)
@@ -637,7 +642,7 @@ class Simulation:
                              int(relax_every), float(dt), int(substeps), int(sweeps), float(death_threshold),
                              int(necrotic_type), int(bool(use_graphs)), int(bool(divide)), int(max_cells),
                              int(spare_cells), float(waste_production), float(necrotic_production),
-                             int(necrotic_release_for))
+                             int(necrotic_release_for), int(subsweeps))
         handle = C.c_void_p()
         call("cw_sim_create", C.byref(cfg), network.handle, C.byref(handle))
         self._h = handle
@@ -702,6 +707,13 @@ class Simulation:
         ok = C.c_int32()
         call("cw_lattice_verify", self.lattice_handle(), hist, C.byref(ok))
         return bool(ok.value)
+
+    def measure(self):
+        """Simulation::measure (measure.rs:133-236) of every history: a dict each."""
+        arr = (_lib.Measurements * len(self.dims))()
+        call("cw_sim_measure", self._h, arr)
+        keys = [f for f, _ in _lib.Measurements._fields_]
+        return [{k: getattr(m, k) for k in keys} for m in arr]
 
     def network_state(self, n, hist=0):
         """The protein levels of records 0..n-1 of a history, [n, S]."""

@@ -113,6 +113,15 @@ int cw_lattice_cell_count(cw_lattice lat, uint32_t hist, uint32_t *n);
  * CW_COPY_MOORE, any in-box pixel at Chebyshev distance 1 (an extension). */
 enum { CW_COPY_VON_NEUMANN = 0, CW_COPY_MOORE = 1 };
 int cw_lattice_set_copy_nbhd(cw_lattice lat, int32_t nbhd);
+/* The update order's kinetics (no counterpart in the reference, whose
+ * random pixels attempt each pixel Poisson(1) times a Monte Carlo step).
+ * 1, the default: a Monte Carlo step sweeps every colour once and attempts
+ * every pixel once, so a favoured copy happens at once where random pixels
+ * take it with probability 1 - 1/e; driven shrinking and growth run faster.
+ * n > 1: n sweeps of every colour, a pixel attempting in each with
+ * probability 1/n (its own Philox draw), Binomial(n, 1/n) attempts a step,
+ * which nears Poisson(1) as n grows; n times the passes. */
+int cw_lattice_set_subsweeps(cw_lattice lat, int32_t subsweeps);
 /* The grid of history `hist`, w*h*d int32 in the reference's flat order. */
 int cw_lattice_upload(cw_lattice lat, uint32_t hist, const int32_t *grid);
 int cw_lattice_download(cw_lattice lat, uint32_t hist, int32_t *grid);
@@ -396,6 +405,7 @@ typedef struct {
     double waste_production;     /* > 0: what a living cell's pixel releases a step (Waste, types.rs:240-244) */
     double necrotic_production;  /* > 0: what a necrotic cell's pixel releases (NecroticFactor, types.rs:256-266) */
     int32_t necrotic_release_for;/* steps after the one it died at a necrotic cell releases; < 0: while it is there */
+    int32_t subsweeps;           /* <= 1: one sweep of every colour a Monte Carlo step; n: cw_lattice_set_subsweeps */
 } cw_sim_config;
 int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out);
 int cw_sim_destroy(cw_sim sim);
@@ -417,6 +427,25 @@ int cw_sim_field(cw_sim sim, int32_t which, cw_field *f);
 /* Per history: living cells, mean oxygen over cells, sweeps of the last
  * oxygen solve, its residual (4 doubles per history). */
 int cw_sim_stats(cw_sim sim, double *out);
+/* Measurements (crates/engine/src/measure.rs:21-90, Simulation::measure
+ * 133-236) of every history as it stands after the last step: the counts of
+ * cycling (hypoxia response under 0.45), quiescent and necrotic cells with
+ * pixels, cells ever born and gone (resorbed to nothing), the obstacle
+ * pixels, and the equivalent radii of the tissue and of the necrotic area
+ * (a disc in the plane, a ball in a volume).  viable_depth is the
+ * reference's for the source the oxygen hold stands for: the tissue radius
+ * less the necrotic one around the faces or the bath (o2_hold 2, 3), the
+ * living area over the columns living cells hold along a held row (0, the
+ * reference's capillary), and over twice the rows they hold beside the held
+ * column (1, tissue on either side). */
+typedef struct {
+    uint64_t mcs;        /* index of the step last taken (0 before the first) */
+    uint64_t cycling, quiescent, necrotic;
+    uint64_t born, gone;
+    uint64_t vessel;
+    double tissue_radius, necrotic_radius, viable_depth;
+} cw_measurements;
+int cw_sim_measure(cw_sim sim, cw_measurements *out);
 /* Network state of history `hist`, [ncells][S]. */
 int cw_sim_network_state(cw_sim sim, uint32_t hist, uint32_t n, double *state);
 

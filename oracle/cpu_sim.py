@@ -66,6 +66,45 @@ def seed_history(cfg, w, h, d, n, seed):
     return grid, np.array(types, np.int32)
 
 
+def measure_records(grid, types, volume, used, hypoxia, necrotic, o2_hold, mcs):
+    """measure.rs:133-236 on a lattice's records: counts of cycling (hypoxia
+    response under 0.45), quiescent and necrotic cells with pixels, born (every
+    record assigned), gone (dead and resorbed to nothing), equivalent radii (a
+    disc in the plane, a ball in a volume); viable_depth as measure.rs:171-199
+    reads it for the source the hold stands for (bath-like faces and bath: the
+    tissue radius less the necrotic one; a held row: the living area over the
+    columns living cells hold; a held column: over twice the rows)."""
+    d, h, w = grid.shape
+    ids = np.arange(1, used)
+    vol = volume[1:used].astype(np.int64)
+    dead = (types[1:used] == necrotic) if necrotic >= 0 else np.zeros(used - 1, bool)
+    has = vol > 0
+    live = has & ~dead
+    cyc = live & (hypoxia[1:used] < 0.45)
+    m = dict(mcs=mcs, cycling=int(cyc.sum()), quiescent=int((live & ~cyc).sum()), necrotic=int((has & dead).sum()),
+             born=int(used - 1), gone=int((~has & dead).sum()))
+    m["vessel"] = h * d if o2_hold == 1 else 0
+    living_area, dead_area = int(vol[live].sum()), int(vol[has & dead].sum())
+
+    def radius(size):
+        if d <= 1:
+            return float(np.sqrt(size / np.pi))
+        return float(np.cbrt(3.0 * size / (4.0 * np.pi)))
+
+    m["tissue_radius"] = radius(m["vessel"] + living_area + dead_area)
+    m["necrotic_radius"] = radius(dead_area)
+    if o2_hold in (0, 1):
+        alive_id = np.zeros(int(types.size), bool)
+        alive_id[ids[live]] = True
+        g = grid.reshape(d, h, w)
+        lv = (g > 0) & alive_id[np.clip(g, 0, None)]
+        lines = lv.any(axis=(0, 1)).sum() if o2_hold == 0 else lv.any(axis=(0, 2)).sum()
+        m["viable_depth"] = 0.0 if lines == 0 else living_area / (float(lines) * (1.0 if o2_hold == 0 else 2.0))
+    else:
+        m["viable_depth"] = m["tissue_radius"] - m["necrotic_radius"]
+    return m
+
+
 class CpuHistory:
     def __init__(self, cfg, k):
         from cellweave_b200 import synthetic  # the same synthetic network text the device runs
@@ -117,6 +156,13 @@ class CpuHistory:
         self.sink = sink
         self.steps = 0
         self.died_at = np.full(self.ncap, -1, np.int64)
+
+    def measure(self):
+        """Simulation::measure (measure.rs:103-236) of this history, with the
+        device step's reading of viable_depth for each oxygen hold."""
+        return measure_records(self.lat.grid.reshape(self.dims[2], self.dims[1], self.dims[0]), self.lat.type,
+                               self.lat.volume, self.used, self.state[:, self.net.hypoxia],
+                               self.cfg.get("necrotic_type", -1), self.cfg.get("o2_hold", 0), max(self.steps - 1, 0))
 
     def _settle_released(self, field, per_cell):
         """settle_released (simulation.rs:2546-2570): production from the cells

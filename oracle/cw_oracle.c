@@ -790,7 +790,7 @@ static int or_by_priority_desc(const void *a, const void *b) {
  * `snapshot` != 0 is a planted mistake for the statistical tests: every
  * attempt of a pass reads the volumes and surfaces the pass started with. */
 void or_lattice_mcs_checkerboard(or_lattice *l, uint32_t k0, uint32_t k1, uint32_t mcs0, int32_t sweeps,
-                                 int32_t snapshot) {
+                                 int32_t snapshot, int32_t subsweeps) {
     int32_t reach[3 * OR_MAX_REACH];
     double across;
     int nreach = or_reach(l->order, l->d > 1, reach, &across);
@@ -801,8 +801,13 @@ void or_lattice_mcs_checkerboard(or_lattice *l, uint32_t k0, uint32_t k1, uint32
     or_ranked *order = (or_ranked *)malloc(sizeof(or_ranked) * (size_t)(n > 0 ? n : 1));
     int32_t *vsnap = snapshot ? (int32_t *)malloc(sizeof(int32_t) * (size_t)l->ncells) : NULL;
     int32_t *ssnap = snapshot && l->surface ? (int32_t *)malloc(sizeof(int32_t) * (size_t)l->ncells) : NULL;
-    for (int32_t s = 0; s < sweeps; ++s) {
-        uint32_t mcs = mcs0 + (uint32_t)s;
+    /* subsweeps > 1: every colour swept that many times a Monte Carlo step, a
+     * pixel attempting in each sweep when its draw (counter word 2 = 4) is
+     * below 2^32 / subsweeps; the draws count sub-sweeps */
+    if (subsweeps < 1) subsweeps = 1;
+    const uint32_t take_below = subsweeps > 1 ? (uint32_t)(4294967296.0 / (double)subsweeps) : 0u;
+    for (int32_t s = 0; s < sweeps * subsweeps; ++s) {
+        uint32_t mcs = mcs0 * (uint32_t)subsweeps + (uint32_t)s;
         or_colour_order(ncol, mcs, k0, k1, perm);
         for (int32_t q = 0; q < ncol; ++q) {
             int32_t colour = perm[q];
@@ -827,6 +832,7 @@ void or_lattice_mcs_checkerboard(or_lattice *l, uint32_t k0, uint32_t k1, uint32
                 int64_t nbr[26];
                 int nn = or_copy_neighbours(l, x, y, z, nbr);
                 if (nn == 0) continue;
+                if (take_below && or_philox((uint32_t)site, mcs, 4u, 0u, k0, k1).v[0] >= take_below) continue;
                 or_u32x4 r = or_philox((uint32_t)site, mcs, 0u, 0u, k0, k1);
                 int32_t src = l->grid[site];
                 int32_t dst = l->grid[nbr[((uint64_t)r.v[0] * (uint64_t)nn) >> 32]];

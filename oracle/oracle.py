@@ -54,7 +54,8 @@ def lib():
         L.or_lattice_mcs_sequential.restype = None
         L.or_lattice_divide_across.argtypes = [P, C.c_int32, C.c_double, C.c_double, C.c_double, P]
         L.or_lattice_divide_across.restype = C.c_int32
-        L.or_lattice_mcs_checkerboard.argtypes = [P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int32, C.c_int32]
+        L.or_lattice_mcs_checkerboard.argtypes = [P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int32, C.c_int32,
+                                                  C.c_int32]
         L.or_lattice_mcs_checkerboard.restype = None
         L.or_lattice_recount.argtypes = [P, P, P]
         L.or_lattice_recount.restype = None
@@ -248,12 +249,13 @@ class Lattice:
         s = self._struct()
         lib().or_lattice_mcs_sequential(C.byref(s), int(seed) & (2**64 - 1), int(sweeps))
 
-    def mcs_checkerboard(self, seed: int, mcs0: int, sweeps: int = 1, snapshot: bool = False):
+    def mcs_checkerboard(self, seed: int, mcs0: int, sweeps: int = 1, snapshot: bool = False, subsweeps: int = 1):
         """The device's sublattice sweeps; `snapshot`: the planted mistake of
-        reading one snapshot of the records per pass (statistical tests only)."""
+        reading one snapshot of the records per pass (statistical tests only);
+        `subsweeps`: the device's sub-sweep kinetics."""
         s = self._struct()
         lib().or_lattice_mcs_checkerboard(C.byref(s), int(seed) & 0xFFFFFFFF, (int(seed) >> 32) & 0xFFFFFFFF,
-                                          int(mcs0) & 0xFFFFFFFF, int(sweeps), int(bool(snapshot)))
+                                          int(mcs0) & 0xFFFFFFFF, int(sweeps), int(bool(snapshot)), int(subsweeps))
 
     def divide_across(self, cid: int, normal, used: int):
         """divide_across (cpm.rs:1094-1160) with the daughter at record `used`:

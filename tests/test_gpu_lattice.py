@@ -99,23 +99,25 @@ def test_delta_h_is_bit_exact(order, volume):
     np.testing.assert_array_equal(got.view(np.uint64), want.view(np.uint64))
 
 
-@pytest.mark.parametrize("order", [1, 2, 3])
-def test_sweeps_are_bit_exact_with_the_sublattice_oracle_plane(order):
+@pytest.mark.parametrize("order,subsweeps", [(1, 1), (2, 1), (3, 1), (2, 4), (1, 3)])
+def test_sweeps_are_bit_exact_with_the_sublattice_oracle_plane(order, subsweeps):
     grid, rec = sheet(seed=order, size=64, ncell=20)
     o, g = pair(grid, rec, J3, 10.0, order, 0xC0FFEE12345)
-    o.mcs_checkerboard(0xC0FFEE12345, 0, 25)
+    g.set_subsweeps(subsweeps)
+    o.mcs_checkerboard(0xC0FFEE12345, 0, 25, subsweeps=subsweeps)
     g.monte_carlo_step(25)
     np.testing.assert_array_equal(g.grid().reshape(-1), o.grid)
     np.testing.assert_array_equal(g.cells()["volume"], o.volume)
     assert g.records_match_grid()
 
 
-@pytest.mark.parametrize("order", [1, 3])
-def test_sweeps_are_bit_exact_in_a_volume_with_surfaces(order):
+@pytest.mark.parametrize("order,subsweeps", [(1, 1), (3, 1), (3, 2)])
+def test_sweeps_are_bit_exact_in_a_volume_with_surfaces(order, subsweeps):
     grid, rec = ball_volume(18)
     n = len(rec)
     o, g = pair(grid, rec, J3, 20.0, order, 99, surface=(np.full(n, 60, np.int32), np.full(n, 0.2)))
-    o.mcs_checkerboard(99, 0, 12)
+    g.set_subsweeps(subsweeps)
+    o.mcs_checkerboard(99, 0, 12, subsweeps=subsweeps)
     g.monte_carlo_step(12)
     np.testing.assert_array_equal(g.grid().reshape(-1), o.grid)
     # the medium's count (index 0) is untracked by the device, as by the reference

@@ -23,7 +23,7 @@ import cellweave_b200 as cw
 from cellweave_b200 import synthetic
 from cpm_ensembles import J, ORDER, SEEDS, SIZE, T, observables, oracle_ensemble, same_volume_law, sheet, within_band
 from oracle import oracle as O
-from oracle.cpu_sim import CpuHistory
+from oracle.cpu_sim import CpuHistory, measure_records
 
 pytestmark = pytest.mark.gpu
 
@@ -77,14 +77,22 @@ def per_history(grid, o2, volume, types, necrotic, level, size=64):
             hypoxic_radius(o2, size, level))
 
 
-def test_the_step_stays_inside_the_oracle_band():
+@pytest.mark.parametrize("subsweeps", [1, 4])
+def test_the_step_stays_inside_the_oracle_band(subsweeps):
+    # one sweep of every colour a step attempts each pixel once where random
+    # pixels attempt it Poisson(1) times: a favoured copy happens at once, not
+    # with probability 1 - 1/e, so the necrotic cells' resorption (a target
+    # two pixels under their volume each step) runs ahead, and the dead are
+    # gone sooner; with four sub-sweeps a step (each pixel attempting in each
+    # with probability 1/4) the tissue and necrotic radii and the cells gone
+    # come inside the band as well
     cfg = small_cord()
     S = cfg.pop("S")
     d = tempfile.mkdtemp()
     p = os.path.join(d, "n.toml")
     open(p, "w").write(synthetic.network_toml(S, S))
     net = cw.Network.load(p, cfg["target_volume"])
-    sim = cw.Simulation(net, **dict(cfg, seeds=[s + 50_000 for s in cfg["seeds"]]))
+    sim = cw.Simulation(net, **dict(cfg, seeds=[s + 50_000 for s in cfg["seeds"]], subsweeps=subsweeps))
     ora = [CpuHistory(dict(cfg, S=S), k) for k in range(SEEDS)]
     for step in range(1, 31):
         sim.step(1)
@@ -100,8 +108,14 @@ def test_the_step_stays_inside_the_oracle_band():
                                    cfg["hypoxic_level"]))
             h = ora[k]
             ref.append(per_history(h.lat.grid, h.o2.values, h.lat.volume, h.lat.type, 3, cfg["hypoxic_level"]))
+        # the reference's own geometry (measure.rs): tissue and necrotic radii,
+        # and how deep living tissue reaches from the held row
+        radii = ("tissue_radius", "necrotic_radius", "gone", "viable_depth") if subsweeps > 1 else ("viable_depth",)
+        dm = sim.measure()
+        dev = [list(r) + [dm[k][q] for q in radii] for k, r in enumerate(dev)]
+        ref = [list(r) + [ora[k].measure()[q] for q in radii] for k, r in enumerate(ref)]
         dev, ref = np.array(dev), np.array(ref)
-        for j, name in enumerate(("living", "mean oxygen", "hypoxic fraction", "hypoxic radius")):
+        for j, name in enumerate(("living", "mean oxygen", "hypoxic fraction", "hypoxic radius") + radii):
             assert within_band(dev[:, j], ref[:, j]), (step, name, dev[:, j].mean(), ref[:, j].mean(),
                                                         ref[:, j].std())
 
@@ -236,3 +250,32 @@ def test_the_bath_holds_the_oxygen_where_the_medium_reaches_the_edge():
         o = O.Field(64, 64, 1, 1.0, 0.0, 0.0)
         o.hold_bath(grids[k] == 0, 1.0)
         np.testing.assert_array_equal(baths[k], o.held.astype(np.uint8))
+
+
+def test_the_device_measures_as_the_reference_does():
+    # Simulation::measure (measure.rs:133-236) on the device against the
+    # oracle's restatement applied to the device's own lattice and network
+    # state, for each oxygen hold
+    for hold in (0, 1, 2, 3):
+        cfg = small_cord(4)
+        cfg.update(o2_hold=hold)
+        S = cfg.pop("S")
+        d = tempfile.mkdtemp()
+        p = os.path.join(d, "n.toml")
+        open(p, "w").write(synthetic.network_toml(S, S))
+        net = cw.Network.load(p, cfg["target_volume"])
+        sim = cw.Simulation(net, **cfg)
+        sim.step(12)
+        got = sim.measure()
+        lat = sim.lattice()
+        hyp = net.roles["hypoxia_response"]
+        for k in range(4):
+            used = lat.cell_count(k)
+            cells = lat.cells(hist=k)
+            state = sim.network_state(len(cells["volume"]), k)
+            want = measure_records(sim.grid(k), cells["type"], cells["volume"], used, state[:, hyp], 3, hold, 11)
+            for key in ("mcs", "cycling", "quiescent", "necrotic", "born", "gone", "vessel"):
+                assert got[k][key] == want[key], (hold, k, key, got[k][key], want[key])
+            for key in ("tissue_radius", "necrotic_radius", "viable_depth"):
+                assert abs(got[k][key] - want[key]) <= 1e-12 * max(1.0, abs(want[key])), (hold, k, key)
+            assert got[k]["cycling"] + got[k]["quiescent"] > 0
