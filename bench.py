@@ -95,7 +95,8 @@ def config_key(name, cfg):
                             "correction), 8-species RK4 x8 per MCS", "histories": len(cfg["dims"]),
                 "sites": int(sum(w * h * d for w, h, d in cfg["dims"])), "cells": int(sum(cfg["ncells"])),
                 "l2": "inputs larger than L2 (the lattices and fields of one step exceed 126 MB)",
-                "parallelism": "histories batched in one launch per kernel; ranks own disjoint campaigns"}
+                "parallelism": "histories batched in one launch per kernel; ranks own disjoint campaigns",
+                "subsweeps": 1}
     return {"workload": "tumour cord 2048^2, ~40k cells of target 64, 3 types, vessel column, 2 fields to "
                         "residual 1e-6, 16-species RK4", "histories": 1,
             "l2": "inputs larger than L2", "parallelism": "one history"}
@@ -324,8 +325,24 @@ def run_ours(args, rank, world, dist):
 
     # ---- the plain path: each history stepped alone (rank 0 at N=1)
     plain = plain_graphs = None
+    kinetics4 = None
     if not args.no_plain and world == 1:
         del sim
+        # the same batch with four sub-sweeps a step: the update-order kinetics
+        # that put driven cells (resorption, growth) inside the reference's band
+        s4 = cw.Simulation(net, **dict(cfg, subsweeps=4))
+        s4.step(max(args.warmup, 3))
+        L.cw_synchronize()
+        L.cw_event_record(4)
+        n4 = min(args.steps, 10)
+        s4.step(n4)
+        L.cw_event_record(5)
+        L.cw_synchronize()
+        kinetics4 = {"value": job_rate(1, nh, n4, event_ms(L, 4, 5)), "unit": UNIT, "subsweeps": 4,
+                     "how": "the same batch, every colour swept four times a step with each pixel attempting in "
+                            "each with probability 1/4 (Binomial(4, 1/4) attempts a step, near the Poisson(1) of "
+                            "random pixels)"}
+        del s4
 
         def one_at_a_time(graphs):
             total_ms, units = 0.0, 0
@@ -356,7 +373,7 @@ def run_ours(args, rank, world, dist):
     if not args.no_fit and world == 1:
         fit = run_fit(args, L)
     return dict(value=value, ms=ms / args.steps, launches=launches, clocks=clk, e2e=e2e, roofline=roofline, fit=fit,
-                graphs=graphs, plain_graphs=plain_graphs,
+                graphs=graphs, plain_graphs=plain_graphs, kinetics4=kinetics4,
                 plain=plain, stats=stats, nh=nh, cfg=cfg, tuned=tuned)
 
 
@@ -461,7 +478,7 @@ def main():
                     gpu_launches=r["launches"], roofline=r["roofline"], cpu_baseline=cpu,
                     plain=r["plain"], plain_with_graphs=r["plain_graphs"],
                     batched_over_plain=(r["value"] / r["plain"]["value"]) if r["plain"] else None,
-                    fit=r["fit"], cuda_graphs=r["graphs"],
+                    fit=r["fit"], cuda_graphs=r["graphs"], subsweeps4=r["kinetics4"],
                     sor_gbs=r["roofline"]["achieved"], sor_site_sweeps_per_s=r["roofline"]["site_sweeps_per_s"],
                     living_cells=float(r["stats"][:, 0].sum()), last_residual_max=float(r["stats"][:, 3].max()),
                     autotuned={"omega_o2": sorted(set(float(v) for v in r["tuned"]["omega_o2"])),
