@@ -97,7 +97,8 @@ class SimConfig(C.Structure):
                 ("death_threshold", C.c_double), ("necrotic_type", C.c_int32), ("use_graphs", C.c_int32),
                 ("divide", C.c_int32), ("max_cells", C.c_int32), ("spare_cells", C.c_int32),
                 ("waste_production", C.c_double), ("necrotic_production", C.c_double),
-                ("necrotic_release_for", C.c_int32), ("subsweeps", C.c_int32)]
+                ("necrotic_release_for", C.c_int32), ("subsweeps", C.c_int32), ("o2_uptake", C.c_double),
+                ("divide_every", C.c_int32), ("vessel_radius", C.c_int32), ("stop_rule", C.c_int32)]
 
 
 P = C.c_void_p

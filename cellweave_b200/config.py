@@ -1,0 +1,201 @@
+"""A cellweave configuration file (crates/io/src/config.rs) run on the device.
+
+``load_sim_config`` reads a configuration as SimConfig does: its fields with
+their defaults (config.rs:12-140 and the serde defaults beside them), the
+network named relative to the file with its ``extends`` chain followed
+(load_network_chain, config.rs:410-447).  ``simulation_from_config`` sets up
+the reference's scenario (Simulation::new, simulation.rs:510-1066) where the
+device step can run it: one cell seeded in a bath or against a vessel, the
+reference's contact energies between medium, tumour, normal and necrotic
+cells (ContactEnergy::default, cpm.rs:63-86), oxygen diffusing at 0.2 and
+taken up at ``oxygen_uptake`` by every living pixel (and by the stroma around
+a vessel), networks stepped eight units of their time a step, division
+checked every 20 steps, waste and necrotic factor when configured.  Every
+other feature of the file (capillaries, sheets, mutation and rewiring,
+exposure, lesions, angiogenesis, immunity, tracing, debris loss, cell cycles,
+still media) is refused by name.  ``run`` steps it for ``mcs`` steps or until
+the tissue touches the box's edge, writing measurements.csv as the reference
+does.
+
+The oxygen is the reference's relax pixel for pixel: FP64 red-black SOR until
+no pixel moves by more than 0.01 x uptake a sweep (simulation.rs:79-99; a
+zero-order uptake empties the core, where the reference's update floors the
+field at zero, which the FP32 defect correction's linear inner solve does not
+follow).  Two differences stand: no warm-up solve to 1e-8 before the first
+step (the field starts at the source's level everywhere), and the Monte Carlo
+step is the device's sub-sweeps (four by default, the kinetics nearest
+random pixels).
+"""
+from __future__ import annotations
+
+import math
+import os
+import tomllib
+
+import numpy as np
+
+from ._lib import ConfigError
+from .engine import FP64, STOP_MAX_CHANGE, Network, Simulation, load_network_spec
+from .output import MeasurementLog
+
+# SimConfig's fields without a default (config.rs:12-40) and their defaults
+REQUIRED = ("width", "height", "mcs", "temperature", "snapshot_interval", "output_dir")
+DEFAULTS = dict(depth=1, max_cells=2000, oxygen_source={"kind": "bath"}, oxygen_uptake=0.00002, network=None,
+                mutation_rate=0.0, seed=42, seeding={"kind": "single"}, exposure=None, suppress=[],
+                suppress_before=None, rewiring=0.0, hours_per_step=None, lesion=None, angiogenesis=None,
+                immunity=None, tracing=None, debris_loss=None, sweeps_per_step=1, cycle=None, contact_order=1,
+                waste=None, necrotic_factor=None, still_medium=None)
+
+OXYGEN_DIFFUSION = 0.2       # simulation.rs:77
+OXYGEN_TOLERANCE = 0.01      # simulation.rs:85
+NETWORK_TIME_PER_MCS = 8     # simulation.rs:115
+DEATH_THRESHOLD = 0.25       # simulation.rs:118
+DIVISION_CHECK_EVERY = 20    # simulation.rs:55
+FIRST_CELL_RADIUS = 8        # simulation.rs:65
+FIRST_CELL_RADIUS_3D = 3     # simulation.rs:74
+MEDIUM, TUMOR, NORMAL, NECROTIC = 0, 1, 2, 3
+
+# ContactEnergy::default (cpm.rs:63-86) between the kinds the device step has
+CONTACT = np.array([[0.0, 16.0, 16.0, 12.0],
+                    [16.0, 2.0, 11.0, 10.0],
+                    [16.0, 11.0, 6.0, 12.0],
+                    [12.0, 10.0, 12.0, 8.0]])
+
+
+def load_sim_config(path: str) -> dict:
+    """SimConfig::from_file (config.rs:300-311) with its defaults; the
+    network's path resolved next to the file (config.rs:396-403)."""
+    try:
+        with open(path, "rb") as fh:
+            raw = tomllib.load(fh)
+    except OSError as e:
+        raise ConfigError(f"{path}: {e}") from None
+    except tomllib.TOMLDecodeError as e:
+        raise ConfigError(f"{path}: {e}") from None
+    missing = [k for k in REQUIRED if k not in raw]
+    if missing:
+        raise ConfigError(f"{path}: missing field `{missing[0]}`")
+    cfg = dict(DEFAULTS)
+    cfg.update(raw)
+    cfg["path"] = os.path.abspath(path)
+    if cfg["network"] is not None:
+        cfg["network_path"] = os.path.join(os.path.dirname(cfg["path"]), cfg["network"])
+    return cfg
+
+
+def _refuse(cfg):
+    name = os.path.basename(cfg.get("path", "the configuration"))
+    src = cfg["oxygen_source"].get("kind", "bath")
+    if src not in ("bath", "vessel"):
+        raise ConfigError(f"{name}: the device step runs a bath or a vessel, not a {src}")
+    if cfg["seeding"].get("kind", "single") != "single":
+        raise ConfigError(f"{name}: the device step seeds one cell, not a {cfg['seeding'].get('kind')}")
+    for key in ("exposure", "lesion", "angiogenesis", "immunity", "tracing", "debris_loss", "cycle",
+                "still_medium", "suppress_before"):
+        if cfg.get(key) is not None:
+            raise ConfigError(f"{name}: `{key}` is not part of the device step")
+    if cfg["mutation_rate"] or cfg["rewiring"] or cfg["suppress"]:
+        raise ConfigError(f"{name}: mutation and rewiring are not part of the device step "
+                          "(cw_network_mutate / rewire derive the networks; the step does not draw them)")
+    if cfg["contact_order"] not in (1, 2, 3):
+        raise ConfigError(f"{name}: contact_order is {cfg['contact_order']}; it is 1, 2 or 3")
+    if cfg["network"] is None:
+        raise ConfigError(f"{name}: name the network file; the built-in RAS/ERK network is not carried here")
+    if cfg["oxygen_uptake"] <= 0:
+        raise ConfigError(f"{name}: the device step solves the oxygen; oxygen_uptake must be above zero")
+
+
+def first_cell_volume(cfg) -> int:
+    """The pixels of the seeded ball (add_ball, cpm.rs:323-354): the network's
+    reference volume (simulation.rs:726-733)."""
+    w, h, d = cfg["width"], cfg["height"], cfg["depth"]
+    r = FIRST_CELL_RADIUS_3D if d > 1 else FIRST_CELL_RADIUS
+    src = cfg["oxygen_source"]
+    cx = w // 2 + (int(src.get("radius", 0)) + r if src.get("kind") == "vessel" else 0)
+    cy, cz = h // 2, d // 2
+    z, y, x = np.mgrid[0:d, 0:h, 0:w]
+    ball = (x - cx) ** 2 + (y - cy) ** 2 + (z - cz) ** 2 <= r * r
+    if src.get("kind") == "vessel":
+        rv = int(src.get("radius", 0))
+        ball &= (x - w // 2) ** 2 + (y - h // 2) ** 2 > rv * rv
+    return int(ball.sum())
+
+
+def simulation_kwargs(cfg, histories=1, seeds=None, subsweeps=4):
+    """Simulation's options for the scenario, and the network's reference volume."""
+    _refuse(cfg)
+    src = cfg["oxygen_source"]
+    vessel = src.get("kind") == "vessel"
+    refvol = first_cell_volume(cfg)
+    uptake = float(cfg["oxygen_uptake"])
+    kw = dict(dims=[(cfg["width"], cfg["height"], cfg["depth"])] * histories, ncells=[1] * histories,
+              seeds=list(seeds) if seeds is not None else [int(cfg["seed"]) + k for k in range(histories)],
+              temperature=float(cfg["temperature"]), J=CONTACT, contact_order=int(cfg["contact_order"]),
+              target_volume=0, seeding=3,
+              seed_side=FIRST_CELL_RADIUS_3D if cfg["depth"] > 1 else FIRST_CELL_RADIUS, nfields=1,
+              o2_dcoef=OXYGEN_DIFFUSION, o2_sink_by_type=(0.0, 0.0, 0.0, 0.0), o2_hold=4 if vessel else 3,
+              vessel_radius=int(src.get("radius", 0)) if vessel else 0, o2_uptake=uptake,
+              tolerance=OXYGEN_TOLERANCE * uptake, precision=FP64, stop_rule=STOP_MAX_CHANGE,
+              dt=1.0, substeps=NETWORK_TIME_PER_MCS, sweeps=int(cfg["sweeps_per_step"]),
+              death_threshold=DEATH_THRESHOLD, necrotic_type=NECROTIC, divide=True,
+              max_cells=int(cfg["max_cells"]), divide_every=DIVISION_CHECK_EVERY, subsweeps=int(subsweeps))
+    if cfg.get("waste"):
+        kw["waste_production"] = float(cfg["waste"]["production"])
+    if cfg.get("necrotic_factor"):
+        nf = cfg["necrotic_factor"]
+        kw["necrotic_production"] = float(nf["production"])
+        kw["necrotic_release_for"] = int(nf["release_for"]) if nf.get("release_for") is not None else -1
+    return kw, refvol
+
+
+def simulation_from_config(cfg, histories=1, seeds=None, subsweeps=4):
+    """(Simulation, Network) for a configuration read by load_sim_config."""
+    kw, refvol = simulation_kwargs(cfg, histories, seeds, subsweeps)
+    net = Network.from_spec(load_network_spec(cfg["network_path"]), refvol)
+    kw["lambda_volume"] = _network_lambda(cfg)
+    return Simulation(net, **kw), net
+
+
+def _network_lambda(cfg):
+    spec = load_network_spec(cfg["network_path"])
+    return float((spec.get("mechanics") or {}).get("lambda_volume", 50.0))
+
+
+def touches_the_edge(grid, vessel=False) -> bool:
+    """touches_the_edge (simulation.rs:2165-2198) for a bath or a vessel: a
+    cell on the box's sides, or in a volume around no vessel its faces."""
+    g = np.asarray(grid)
+    d = g.shape[0]
+    cell = g > 0
+    sides = cell[:, 0, :].any() or cell[:, -1, :].any() or cell[:, :, 0].any() or cell[:, :, -1].any()
+    return bool(sides or (d > 1 and not vessel and (cell[0].any() or cell[-1].any())))
+
+
+def run(path, out_dir=None, histories=1, seeds=None, subsweeps=4, steps=None):
+    """The reference's run loop (src/main.rs:162-190) on the device: every
+    step measured into measurements.csv (one directory per history when there
+    are several), stopping after the step the tissue touches the edge."""
+    cfg = load_sim_config(path)
+    sim, _ = simulation_from_config(cfg, histories, seeds, subsweeps)
+    out_dir = out_dir or os.path.join(os.path.dirname(cfg["path"]), cfg["output_dir"])
+    dirs = [out_dir] if histories == 1 else [os.path.join(out_dir, f"history-{k}") for k in range(histories)]
+    logs = [MeasurementLog(d) for d in dirs]
+    vessel = cfg["oxygen_source"].get("kind") == "vessel"
+    done = [False] * histories
+    n = int(cfg["mcs"] if steps is None else steps)
+    taken = 0
+    for _ in range(n):
+        sim.step(1)
+        taken += 1
+        ms = sim.measure()
+        for k in range(histories):
+            if done[k]:
+                continue
+            logs[k].record(ms[k])
+            if touches_the_edge(sim.grid(k), vessel):
+                done[k] = True
+        if all(done):
+            break
+    for lg in logs:
+        lg.close()
+    return dict(steps=taken, reached_edge=done, directories=dirs)

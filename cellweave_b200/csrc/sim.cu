@@ -23,6 +23,7 @@ using namespace cw;
 struct cw_sim_s {
     cw_sim_config cfg;
     std::vector<uint32_t> w, h, d, ncells;
+    std::vector<uint64_t> obstacles;  // obstacle pixels seeded per history (a vessel's)
     std::vector<uint64_t> seeds;
     std::vector<double> J, sink;
     cw_lattice_s *lat = nullptr;
@@ -35,6 +36,7 @@ struct cw_sim_s {
     std::vector<cw_relax_stats> last_wst, last_nfc;
     cw_network_s *net = nullptr;
     double *d_sink = nullptr;       // 8 rates by type
+    double *d_uptake = nullptr;     // 8 zero-order uptakes by type (the living types at o2_uptake)
     double *cell_o2 = nullptr, *cell_sig = nullptr, *sum = nullptr, *secretion = nullptr;
     int32_t *count = nullptr;
     double *state = nullptr, *inputs = nullptr;
@@ -240,7 +242,7 @@ __global__ void k_fates(const uint8_t *alive, const double *state, int64_t nc, i
 __global__ void k_div_ready(const int32_t *type, const int32_t *volume, const int64_t *cell_off, const uint2 *keys,
                             const int4 *dims, int nh, int64_t nc, int necrotic, const double *state, int hyp,
                             double threshold, const uint32_t *mcs_ctr, uint8_t *alive, uint8_t *flag,
-                            double *normal, int32_t *count) {
+                            double *normal, int32_t *count, const uint32_t *step, int every) {
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nc) return;
     int lo = 0, hi = nh - 1;
@@ -248,7 +250,10 @@ __global__ void k_div_ready(const int32_t *type, const int32_t *volume, const in
     const int64_t local = c - cell_off[lo];
     const bool a = local > 0 && volume[c] > 0 && type[c] != necrotic;
     alive[c] = a;
-    const bool ready = a && (double)volume[c] >= threshold && (hyp < 0 || state[(int64_t)hyp * nc + c] < QUIESCENCE_THRESHOLD);
+    // the check on the steps it is taken on (every > 1: step % every == 0)
+    const bool due = every <= 1 || (*step % (uint32_t)every) == 0u;
+    const bool ready = due && a && (double)volume[c] >= threshold &&
+                       (hyp < 0 || state[(int64_t)hyp * nc + c] < QUIESCENCE_THRESHOLD);
     flag[c] = ready;
     if (!ready) return;
     atomicAdd(count, 1);  // few cells are ready at once
@@ -311,6 +316,31 @@ void seed_history(const cw_sim_config &c, uint32_t W, uint32_t H, uint32_t D, ui
     if (c.o2_hold == 1)
         for (uint32_t z = 0; z < D; ++z)
             for (uint32_t y = 0; y < H; ++y) grid[((size_t)z * H + y) * W + W / 2] = -1;
+    // a vessel: an obstacle disc at the centre through every slice (add_obstacle_disc, cpm.rs:389-415)
+    if (c.o2_hold == 4) {
+        const int64_t cx = W / 2, cy = H / 2, r2 = (int64_t)c.vessel_radius * c.vessel_radius;
+        for (uint32_t z = 0; z < D; ++z)
+            for (uint32_t y = 0; y < H; ++y)
+                for (uint32_t x = 0; x < W; ++x) {
+                    const int64_t dx = (int64_t)x - cx, dy = (int64_t)y - cy;
+                    if (dx * dx + dy * dy <= r2) grid[((size_t)z * H + y) * W + x] = -1;
+                }
+    }
+    // one cell (Seeding::Single, simulation.rs:666-694): a ball of radius s at
+    // the centre, or against the vessel's wall (add_ball, cpm.rs:323-354)
+    if (c.seeding == 3) {
+        const int64_t cx = (int64_t)(W / 2) + (c.o2_hold == 4 ? c.vessel_radius + s : 0), cy = H / 2, cz = D / 2;
+        const int64_t r2 = (int64_t)s * s;
+        for (uint32_t z = 0; z < D; ++z)
+            for (uint32_t y = 0; y < H; ++y)
+                for (uint32_t x = 0; x < W; ++x) {
+                    const int64_t dx = (int64_t)x - cx, dy = (int64_t)y - cy, dz = (int64_t)z - cz;
+                    int32_t &g = grid[((size_t)z * H + y) * W + x];
+                    if (dx * dx + dy * dy + dz * dz <= r2 && g != -1) g = 1;
+                }
+        type.push_back(1);
+        return;
+    }
     auto free_box = [&](uint32_t x0, uint32_t y0, uint32_t z0, uint32_t sx, uint32_t sy, uint32_t sz) {
         if (x0 + sx > W || y0 + sy > H || z0 + sz > D) return false;
         for (uint32_t z = z0; z < z0 + sz; ++z)
@@ -366,7 +396,11 @@ int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out) {
     if (c.nh == 0) return fail(CW_ERR_CONFIG, "a simulation needs a history");
     if (c.K < 2 || c.K > 8) return fail(CW_ERR_CONFIG, "2 to 8 types, the medium included");
     if (c.nfields < 1 || c.nfields > 2) return fail(CW_ERR_CONFIG, "one or two fields");
-    if (c.o2_hold < 0 || c.o2_hold > 3) return fail(CW_ERR_CONFIG, "the oxygen is held on a row, a column, the faces or the bath");
+    if (c.o2_hold < 0 || c.o2_hold > 4)
+        return fail(CW_ERR_CONFIG, "the oxygen is held on a row, a column, the faces, the bath or a vessel");
+    if (c.o2_hold == 4 && c.vessel_radius < 1) return fail(CW_ERR_CONFIG, "a vessel needs a radius of a pixel or more");
+    if (c.stop_rule == CW_STOP_MAX_CHANGE && c.precision != CW_FP64)
+        return fail(CW_ERR_CONFIG, "the largest change a sweep is the FP64 solve's stopping rule");
     if (!net) return fail(CW_ERR_CONFIG, "a simulation needs a network");
     int32_t survival = network_role(net, 1);
     cw_sim_s *s = new cw_sim_s();
@@ -395,6 +429,7 @@ int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out) {
         const int32_t spare = !c.divide ? 0 : c.spare_cells > 0 ? c.spare_cells : c.max_cells > 0 ? c.max_cells
                                                                                               : DEFAULT_MAX_CELLS;
         cap[k] = (uint32_t)(types[k].size() + spare);
+        s->obstacles.push_back((uint64_t)std::count(grids[k].begin(), grids[k].end(), -1));
     }
     int rc = cw_lattice_create(c.nh, s->w.data(), s->h.data(), s->d.data(), cap.data(), c.temperature, &s->lat);
     if (rc != CW_OK) { cw_sim_destroy(s); return rc; }
@@ -406,6 +441,7 @@ int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out) {
         std::vector<int32_t> vol(n, 0), tgt(n, c.target_volume);
         std::vector<double> lam(n, c.lambda_volume);
         for (int32_t id : grids[k]) if (id > 0) vol[id] += 1;
+        if (c.seeding == 3 || c.target_volume <= 0) tgt = vol;  // a seeded cell aims at what it holds
         tgt[0] = 0;
         lam[0] = 0.0;
         if ((rc = cw_lattice_upload(s->lat, k, grids[k].data())) ||
@@ -438,6 +474,7 @@ int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out) {
                     bool on = c.o2_hold == 0 ? y == 0
                             : c.o2_hold == 1 ? x == W / 2
                             : c.o2_hold == 2 ? (x == 0 || y == 0 || x + 1 == W || y + 1 == H || z == 0 || z + 1 == D)
+                            : c.o2_hold == 4 ? grids[k][((size_t)z * H + y) * W + x] == -1  // the vessel's pixels
                                              : false;  // 3: the bath, taken every step
                     held[((size_t)z * H + y) * W + x] = on;
                 }
@@ -490,6 +527,17 @@ int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out) {
     CW_CUDA(cudaMemsetAsync(s->cell_wst, 0, sizeof(double) * nc, stream()));
     CW_CUDA(cudaMemsetAsync(s->cell_nfc, 0, sizeof(double) * nc, stream()));
     CW_CUDA(cudaMemcpyAsync(s->d_sink, s->sink.data(), 8 * sizeof(double), cudaMemcpyHostToDevice, stream()));
+    {
+        // the zero-order uptake of the living types (not the medium, not the dead)
+        std::vector<double> up(8, 0.0);
+        for (int k = 1; k < c.K; ++k) up[k] = k == c.necrotic_type ? 0.0 : std::max(c.o2_uptake, 0.0);
+        if ((rc = dalloc(&s->d_uptake, 8)) != CW_OK) { cw_sim_destroy(s); return rc; }
+        CW_CUDA(cudaMemcpyAsync(s->d_uptake, up.data(), 8 * sizeof(double), cudaMemcpyHostToDevice, stream()));
+        if (c.o2_uptake > 0.0) {
+            s->o2->uptake_on = true;
+            CW_CUDA(cudaMemsetAsync(s->o2->uptake, 0, sizeof(double) * (size_t)s->o2->g.total, stream()));
+        }
+    }
     std::vector<double> st((size_t)nc * S);
     const std::vector<double> &init = network_initial(net);
     for (int i = 0; i < S; ++i) std::fill(st.begin() + (size_t)i * nc, st.begin() + (size_t)(i + 1) * nc, init[i]);
@@ -520,7 +568,7 @@ int cw_sim_destroy(cw_sim s) {
     cw_field_destroy(s->wst);
     cw_field_destroy(s->nfc);
     dfree(s->cell_wst); dfree(s->cell_nfc); dfree(s->wst_rate); dfree(s->nfc_rate); dfree(s->died_at);
-    dfree(s->d_step); dfree(s->bath);
+    dfree(s->d_step); dfree(s->bath); dfree(s->d_uptake);
     dfree(s->d_sink); dfree(s->cell_o2); dfree(s->cell_sig); dfree(s->sum); dfree(s->secretion); dfree(s->count);
     dfree(s->state); dfree(s->inputs); dfree(s->alive); dfree(s->target32);
     s->sites.release();
@@ -629,10 +677,30 @@ static int division_step(cw_sim_s *s) {
     k_div_ready<<<(unsigned)blocks(nc), T, 0, stream()>>>(
         l->type, l->volume, l->d_cell_off, l->d_keys, l->g.d_dims, (int)c.nh, nc, c.necrotic_type, s->state,
         network_role(s->net, 2), DIVISION_RATIO * (double)network_reference_volume(s->net),
-        (const uint32_t *)l->d_flag, s->alive, l->div.flag, l->div.normal, l->div.count);
+        (const uint32_t *)l->d_flag, s->alive, l->div.flag, l->div.normal, l->div.count, s->d_step, c.divide_every);
     CW_LAUNCHED();
     return lattice_divide_enqueue(l, s->alive, c.max_cells > 0 ? c.max_cells : DEFAULT_MAX_CELLS, s->state,
                                   network_nodes(s->net));
+}
+
+// Who takes up oxygen (declare_sources, simulation.rs:2138-2163): the
+// first-order sinks by type (and of the medium), and with o2_uptake the
+// zero-order uptake of every living cell's pixel (apply_uptake) and, around a
+// vessel, of the medium too (apply_background_uptake).
+static int paint_oxygen(cw_sim_s *s) {
+    const cw_sim_config &c = s->cfg;
+    int rc;
+    if ((rc = couple_uptake_device(s->o2, s->lat, s->d_sink, 8, s->o2->lin_sink, s->sites)) != CW_OK) return rc;
+    if (c.o2_background_sink > 0.0 &&
+        (rc = couple_background_device(s->o2, s->lat, c.o2_background_sink, s->o2->lin_sink)) != CW_OK)
+        return rc;
+    s->o2->lin_sink_on = true;
+    if (c.o2_uptake > 0.0) {
+        if ((rc = couple_uptake_device(s->o2, s->lat, s->d_uptake, 8, s->o2->uptake, s->sites)) != CW_OK) return rc;
+        if (c.o2_hold == 4 && (rc = couple_background_device(s->o2, s->lat, c.o2_uptake, s->o2->uptake)) != CW_OK)
+            return rc;
+    }
+    return CW_OK;
 }
 
 // One of the three phases of a step, enqueued without host synchronisation.
@@ -641,10 +709,7 @@ static int enqueue_phase(cw_sim_s *s, int p, const cw_relax_opts &o) {
     const int64_t nc = s->nc;
     int rc;
     if (p == 0) {
-        if ((rc = couple_uptake_device(s->o2, s->lat, s->d_sink, 8, s->o2->lin_sink, s->sites)) != CW_OK) return rc;
-        if (c.o2_background_sink > 0.0 &&
-            (rc = couple_background_device(s->o2, s->lat, c.o2_background_sink, s->o2->lin_sink)) != CW_OK)
-            return rc;
+        if ((rc = paint_oxygen(s)) != CW_OK) return rc;
         return field_relax_enqueue(s->o2, &o, s->budget[0], &s->gstart[0]);
     }
     if (p == 1) {
@@ -774,7 +839,7 @@ int cw_sim_step(cw_sim s, uint32_t nsteps) {
     int survival = network_role(s->net, 1);
     cw_relax_opts o{};
     o.omega = c.omega;
-    o.stop = CW_STOP_RESIDUAL;
+    o.stop = c.stop_rule == CW_STOP_MAX_CHANGE ? CW_STOP_MAX_CHANGE : CW_STOP_RESIDUAL;
     o.tolerance = c.tolerance;
     o.max_sweeps = 200000;
     o.precision = c.precision;
@@ -806,11 +871,7 @@ int cw_sim_step(cw_sim s, uint32_t nsteps) {
         }
         if (solve) {
             // 1. downward coupling and the oxygen solve
-            if ((rc = couple_uptake_device(s->o2, s->lat, s->d_sink, 8, s->o2->lin_sink, s->sites)) != CW_OK) return rc;
-            if (c.o2_background_sink > 0.0 &&
-                (rc = couple_background_device(s->o2, s->lat, c.o2_background_sink, s->o2->lin_sink)) != CW_OK)
-                return rc;
-            s->o2->lin_sink_on = true;
+            if ((rc = paint_oxygen(s)) != CW_OK) return rc;
             const double *om = c.omega > 0.0 ? nullptr : s->omega[0].data();
             if ((rc = field_relax(s->o2, &o, om, s->last.data())) != CW_OK) return rc;
             if (tuning) tune_book(s, 0, s->last);
@@ -983,12 +1044,13 @@ int cw_sim_measure(cw_sim s, cw_measurements *out) {
         m.necrotic = v[2];
         m.born = v[5];
         m.gone = v[6];
-        // the held column of o2_hold 1 is the lattice's only obstacle
-        m.vessel = c.o2_hold == 1 ? (uint64_t)s->h[k] * s->d[k] : 0;
+        // the held column of o2_hold 1, the vessel of 4: the lattice's only obstacles
+        m.vessel = (c.o2_hold == 1 || c.o2_hold == 4) ? s->obstacles[k] : 0;
         const uint32_t D = s->d[k];
         // radius_of (measure.rs:103-113): a disc in the plane, a ball in a volume
         auto radius = [&](uint64_t size) {
             if (D <= 1) return std::sqrt((double)size / pi);
+            if (c.o2_hold == 4) return std::sqrt((double)size / (pi * (double)D));  // a cylinder as long as the box
             return std::cbrt(3.0 * (double)size / (4.0 * pi));
         };
         const uint64_t living = v[3], dead = v[4];
@@ -996,6 +1058,7 @@ int cw_sim_measure(cw_sim s, cw_measurements *out) {
         m.necrotic_radius = radius(dead);
         if (c.o2_hold == 0) m.viable_depth = v[7] == 0 ? 0.0 : (double)living / (double)v[7];
         else if (c.o2_hold == 1) m.viable_depth = v[7] == 0 ? 0.0 : (double)living / (2.0 * (double)v[7]);
+        else if (c.o2_hold == 4) m.viable_depth = radius(m.vessel + living) - radius(m.vessel);
         else m.viable_depth = m.tissue_radius - m.necrotic_radius;
     }
     return CW_OK;

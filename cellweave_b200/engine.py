@@ -624,7 +624,8 @@ class Simulation:
                  signal_decay=0.01, signal_secretion=0.05, hypoxic_level=0.1, tolerance=1e-6, precision=FP32_DC,
                  omega=None, inner_sweeps=0, relax_every=1, dt=0.01, substeps=8, sweeps=1, death_threshold=0.25,
                  necrotic_type=-1, use_graphs=True, divide=True, max_cells=2000, spare_cells=0,
-                 waste_production=0.0, necrotic_production=0.0, necrotic_release_for=-1, subsweeps=1):
+                 waste_production=0.0, necrotic_production=0.0, necrotic_release_for=-1, subsweeps=1,
+                 o2_uptake=0.0, divide_every=1, vessel_radius=0, stop_rule=STOP_RESIDUAL):
         self.dims, w, h, z = _dims(dims)
         self._keep = [w, h, z]
         nc = np.array(ncells, np.uint32)
@@ -642,7 +643,8 @@ class Simulation:
                              int(relax_every), float(dt), int(substeps), int(sweeps), float(death_threshold),
                              int(necrotic_type), int(bool(use_graphs)), int(bool(divide)), int(max_cells),
                              int(spare_cells), float(waste_production), float(necrotic_production),
-                             int(necrotic_release_for), int(subsweeps))
+                             int(necrotic_release_for), int(subsweeps), float(o2_uptake), int(divide_every),
+                             int(vessel_radius), int(stop_rule))
         handle = C.c_void_p()
         call("cw_sim_create", C.byref(cfg), network.handle, C.byref(handle))
         self._h = handle

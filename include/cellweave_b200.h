@@ -379,7 +379,7 @@ typedef struct {
     double o2_dcoef;
     const double *o2_sink_by_type; /* K first-order sinks k per type (0 for the medium) */
     double o2_background_sink;   /* first-order sink of medium pixels (stroma around a vessel) */
-    int32_t o2_hold;             /* 0 row y=0, 1 column x=w/2, 2 every face of the box, 3 the bath: the
+    int32_t o2_hold;             /* 0 row y=0, 1 column x=w/2, 2 every face of the box, 4 a vessel (below), 3 the bath: the
                                     medium joined to the box's outer layer, taken every step
                                     (declare_sources with OxygenSource::Bath, simulation.rs:2138-2146) */
     double signal_dcoef, signal_decay, signal_secretion, hypoxic_level;
@@ -406,6 +406,19 @@ typedef struct {
     double necrotic_production;  /* > 0: what a necrotic cell's pixel releases (NecroticFactor, types.rs:256-266) */
     int32_t necrotic_release_for;/* steps after the one it died at a necrotic cell releases; < 0: while it is there */
     int32_t subsweeps;           /* <= 1: one sweep of every colour a Monte Carlo step; n: cw_lattice_set_subsweeps */
+    /* The reference's scenarios (Simulation::new, simulation.rs:510-1066):
+     * seeding 3 is one cell (a disc in the plane, a ball in a volume, of
+     * radius seed_side) at the centre, or against the vessel's wall with
+     * o2_hold 4, its target its own volume; o2_hold 4 is a vessel, an
+     * obstacle disc of vessel_radius at the centre through every slice, held
+     * at the source's level (add_obstacle_disc, cpm.rs:389-415). */
+    double o2_uptake;            /* > 0: zero-order uptake of every living cell's pixel (apply_uptake,
+                                    coupling.rs:22-40), and of the medium around a vessel (apply_background_uptake) */
+    int32_t divide_every;        /* the division check every this many steps (<= 1: every step; the reference
+                                    checks a single seeded tissue every 20, simulation.rs:1338-1345) */
+    int32_t vessel_radius;       /* o2_hold 4 */
+    int32_t stop_rule;           /* CW_STOP_RESIDUAL, or CW_STOP_MAX_CHANGE with CW_FP64: the reference's
+                                    relax, pixel for pixel (no pixel moves by more than `tolerance` a sweep) */
 } cw_sim_config;
 int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out);
 int cw_sim_destroy(cw_sim sim);
@@ -435,7 +448,9 @@ int cw_sim_stats(cw_sim sim, double *out);
  * (a disc in the plane, a ball in a volume).  viable_depth is the
  * reference's for the source the oxygen hold stands for: the tissue radius
  * less the necrotic one around the faces or the bath (o2_hold 2, 3), the
- * living area over the columns living cells hold along a held row (0, the
+ * radius of vessel and living together less the vessel's around a vessel
+ * (4; in a volume the radii are of cylinders as long as the box), the living
+ * area over the columns living cells hold along a held row (0, the
  * reference's capillary), and over twice the rows they hold beside the held
  * column (1, tissue on either side). */
 typedef struct {

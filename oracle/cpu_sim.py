@@ -29,6 +29,17 @@ def seed_history(cfg, w, h, d, n, seed):
     ntypes = max(1, (nec - 1) if nec and nec > 0 else K - 1)
     if cfg.get("o2_hold", 0) == 1:
         grid[:, :, w // 2] = -1
+    z_, y_, x_ = np.mgrid[0:d, 0:h, 0:w]
+    if cfg.get("o2_hold", 0) == 4:
+        # a vessel: an obstacle disc at the centre through every slice (add_obstacle_disc, cpm.rs:389-415)
+        rv = int(cfg["vessel_radius"])
+        grid[(x_ - w // 2) ** 2 + (y_ - h // 2) ** 2 <= rv * rv] = -1
+    if cfg.get("seeding", 0) == 3:
+        # one cell (Seeding::Single, simulation.rs:666-694; add_ball, cpm.rs:323-354)
+        cx = w // 2 + (int(cfg["vessel_radius"]) + s if cfg.get("o2_hold", 0) == 4 else 0)
+        ball = ((x_ - cx) ** 2 + (y_ - h // 2) ** 2 + (z_ - d // 2) ** 2 <= s * s) & (grid != -1)
+        grid[ball] = 1
+        return grid, np.array([0, 1], np.int32)
     types = [0]
     sz = s if d > 1 else 1
 
@@ -83,12 +94,14 @@ def measure_records(grid, types, volume, used, hypoxia, necrotic, o2_hold, mcs):
     cyc = live & (hypoxia[1:used] < 0.45)
     m = dict(mcs=mcs, cycling=int(cyc.sum()), quiescent=int((live & ~cyc).sum()), necrotic=int((has & dead).sum()),
              born=int(used - 1), gone=int((~has & dead).sum()))
-    m["vessel"] = h * d if o2_hold == 1 else 0
+    m["vessel"] = int((grid == -1).sum()) if o2_hold in (1, 4) else 0
     living_area, dead_area = int(vol[live].sum()), int(vol[has & dead].sum())
 
     def radius(size):
         if d <= 1:
             return float(np.sqrt(size / np.pi))
+        if o2_hold == 4:
+            return float(np.sqrt(size / (np.pi * d)))
         return float(np.cbrt(3.0 * size / (4.0 * np.pi)))
 
     m["tissue_radius"] = radius(m["vessel"] + living_area + dead_area)
@@ -100,6 +113,8 @@ def measure_records(grid, types, volume, used, hypoxia, necrotic, o2_hold, mcs):
         lv = (g > 0) & alive_id[np.clip(g, 0, None)]
         lines = lv.any(axis=(0, 1)).sum() if o2_hold == 0 else lv.any(axis=(0, 2)).sum()
         m["viable_depth"] = 0.0 if lines == 0 else living_area / (float(lines) * (1.0 if o2_hold == 0 else 2.0))
+    elif o2_hold == 4:
+        m["viable_depth"] = radius(m["vessel"] + living_area) - radius(m["vessel"])
     else:
         m["viable_depth"] = m["tissue_radius"] - m["necrotic_radius"]
     return m
@@ -124,6 +139,8 @@ class CpuHistory:
         self.lat.recount()
         self.lat.volume[0] = 0
         self.lat.target[:self.used] = cfg["target_volume"]
+        if cfg.get("seeding", 0) == 3 or cfg["target_volume"] <= 0:
+            self.lat.target[:self.used] = self.lat.volume[:self.used]  # a seeded cell aims at what it holds
         self.lat.target[0] = 0
         self.lat.lam[:self.used] = cfg["lambda_volume"]
         self.lat.lam[0] = 0.0
@@ -136,7 +153,7 @@ class CpuHistory:
         hold = cfg.get("o2_hold", 0)
         held = (y == 0) if hold == 0 else (x == w // 2) if hold == 1 else (
             (x == 0) | (y == 0) | (z == 0) | (x == w - 1) | (y == h - 1) | (z == d - 1)) if hold == 2 else (
-            np.zeros_like(y, bool))  # 3: the bath, taken every step
+            grid == -1) if hold == 4 else np.zeros_like(y, bool)  # 4: the vessel; 3: the bath, taken every step
         self.o2.held[:] = held.reshape(-1)
         self.o2.values[self.o2.held == 1] = 1.0
         self.o2.lin_sink = np.zeros(n)
@@ -147,8 +164,11 @@ class CpuHistory:
         self.wst = O.Field(w, h, d, cfg["o2_dcoef"], 0.0, 0.0) if cfg.get("waste_production", 0.0) > 0 else None
         self.nfc = O.Field(w, h, d, cfg["o2_dcoef"], 0.0, 0.0) if cfg.get("necrotic_production", 0.0) > 0 else None
         self.cell_wst = self.cell_nfc = None
-        spec = tomllib.loads(cfg.get("network_toml") or synthetic.network_toml(cfg["S"], cfg["S"]))
-        self.net = O.compile_network(spec, cfg["target_volume"])
+        spec = cfg.get("network_spec") or tomllib.loads(cfg.get("network_toml") or
+                                                          synthetic.network_toml(cfg["S"], cfg["S"]))
+        # the network's reference volume: the seeded cell's (simulation.rs:726-733) or the target
+        self.refvol = int(self.lat.volume[1]) if cfg.get("seeding", 0) == 3 else int(cfg["target_volume"])
+        self.net = O.compile_network(spec, self.refvol)
         self.state = np.tile(self.net.initial, (self.ncap, 1))
         self.div_rng = np.random.default_rng(self.seed * 7 + 13)
         sink = np.zeros(8)
@@ -172,7 +192,7 @@ class CpuHistory:
         field.production = O.apply_production(g, per_cell)
         field.held[:] = 0
         field.hold_bath(g == 0, 0.0)
-        field.relax(c["tolerance"], 200_000, omega=c.get("omega") or 0.0, stop=1, threads=1)
+        field.relax(c["tolerance"], 200_000, omega=c.get("omega") or 0.0, stop=c.get("stop_rule", 1), threads=1)
         return O.mean_per_cell(g, field.values, self.ncap)
 
     def step(self):
@@ -184,12 +204,21 @@ class CpuHistory:
         sink[cells] = self.sink[t[g[cells]]]
         sink[g == 0] = c.get("o2_background_sink", 0.0)
         self.o2.lin_sink = sink
+        if c.get("o2_uptake", 0.0) > 0:
+            # apply_uptake (coupling.rs:22-40): every living pixel; around a vessel the medium too
+            nec0 = c.get("necrotic_type", -1)
+            up = np.zeros(g.size)
+            live = cells & (t[np.clip(g, 0, None)] != nec0)
+            up[live] = c["o2_uptake"]
+            if c.get("o2_hold", 0) == 4:
+                up[g == 0] = c["o2_uptake"]
+            self.o2.uptake = up
         if c.get("o2_hold", 0) == 3:
             # the bath as the lattice stands (declare_sources, simulation.rs:2138-2146)
             self.o2.held[:] = 0
             self.o2.hold_bath(g == 0, 1.0)
         omega = c.get("omega") or 0.0
-        rc, _ = self.o2.relax(c["tolerance"], 200_000, omega=omega, stop=1, threads=1)
+        rc, _ = self.o2.relax(c["tolerance"], 200_000, omega=omega, stop=c.get("stop_rule", 1), threads=1)
         o2m = O.mean_per_cell(g, self.o2.values, self.ncap)
         nec = c.get("necrotic_type", -1)
         alive = (self.lat.volume > 0) & (t != nec)
@@ -197,7 +226,7 @@ class CpuHistory:
         if self.sig is not None:
             sec = np.where(alive & (o2m < c["hypoxic_level"]), c["signal_secretion"], 0.0)
             self.sig.production = O.apply_production(g, sec)
-            self.sig.relax(c["tolerance"], 200_000, omega=omega, stop=1, threads=1)
+            self.sig.relax(c["tolerance"], 200_000, omega=omega, stop=c.get("stop_rule", 1), threads=1)
         if self.wst is not None:
             self.cell_wst = self._settle_released(self.wst, np.where(alive, c["waste_production"], 0.0))
         if self.nfc is not None:
@@ -218,7 +247,7 @@ class CpuHistory:
             ins[:, 0] = o2m[idx]
             ins[:, 1] = 0.2
             # crowding (simulation.rs:2523-2527): 1 - volume / reference volume, clamped
-            ins[:, 2] = np.clip(1.0 - self.lat.volume[idx] / float(max(c["target_volume"], 1)), 0.0, 1.0)
+            ins[:, 2] = np.clip(1.0 - self.lat.volume[idx] / float(max(self.refvol, 1)), 0.0, 1.0)
             if self.cell_wst is not None:
                 ins[:, 4] = self.cell_wst[idx]
             if self.cell_nfc is not None:
@@ -234,7 +263,8 @@ class CpuHistory:
             self.lat.target[live] = np.minimum(tg[~dead], 2**31 - 1).astype(np.int32)
             self.lat.lam[live] = c["lambda_volume"]
         self.lat.mcs_sequential(self.seed * 1_000_003 + self.steps, c.get("sweeps", 1))
-        if self.divide:
+        every = int(c.get("divide_every", 1) or 1)
+        if self.divide and (every <= 1 or self.steps % every == 0):
             self._divide_ready_cells()
         self.steps += 1
         return rc
@@ -250,7 +280,7 @@ class CpuHistory:
         alive[0] = False
         alive[self.used:] = False
         hyp = self.net.hypoxia
-        ready = alive & (vol >= 1.4 * c["target_volume"])
+        ready = alive & (vol >= 1.4 * self.refvol)
         if hyp is not None and hyp >= 0:
             ready &= self.state[:, hyp] < 0.45
         living = int(alive.sum())

@@ -1,0 +1,98 @@
+"""A cellweave configuration file read as SimConfig does (crates/io/src/config.rs), on CPU."""
+import os
+
+import numpy as np
+import pytest
+
+import cellweave_b200 as cw
+from cellweave_b200 import config as C
+
+NET = """
+[[nodes]]
+name = "a"
+initial = 0.5
+terms = [ { kind = "activated_by", source = "oxygen", rate = 0.5 }, { kind = "decays", rate = 0.3 } ]
+[roles]
+growth = "a"
+survival = "a"
+hypoxia_response = "a"
+[mechanics]
+growth_coefficient = 0.5
+lambda_volume = 40.0
+"""
+
+
+def write(tmp_path, text, net=True):
+    if net:
+        (tmp_path / "net.toml").write_text(NET)
+    p = tmp_path / "run.toml"
+    p.write_text(text)
+    return str(p)
+
+
+BASE = """width = 60
+height = 50
+mcs = 30
+temperature = 10.0
+snapshot_interval = 10
+output_dir = "out"
+network = "net.toml"
+"""
+
+
+def test_defaults_are_the_reference_configurations(tmp_path):
+    cfg = C.load_sim_config(write(tmp_path, BASE))
+    # config.rs:12-140 with its serde defaults
+    assert cfg["depth"] == 1 and cfg["max_cells"] == 2000 and cfg["seed"] == 42
+    assert cfg["oxygen_source"] == {"kind": "bath"} and cfg["seeding"] == {"kind": "single"}
+    assert cfg["oxygen_uptake"] == 0.00002 and cfg["sweeps_per_step"] == 1 and cfg["contact_order"] == 1
+    assert cfg["network_path"] == os.path.join(str(tmp_path), "net.toml")
+    kw, refvol = C.simulation_kwargs(cfg)
+    # one disc of radius 8 at the centre: 197 pixels, the network's reference volume
+    assert refvol == 197
+    assert kw["o2_hold"] == 3 and kw["seeding"] == 3 and kw["seed_side"] == 8 and kw["divide_every"] == 20
+    assert kw["o2_dcoef"] == 0.2 and kw["dt"] == 1.0 and kw["substeps"] == 8 and kw["necrotic_type"] == 3
+    np.testing.assert_array_equal(C.CONTACT, C.CONTACT.T)
+
+
+def test_a_vessel_seeds_its_cell_against_the_wall(tmp_path):
+    cfg = C.load_sim_config(write(tmp_path, BASE + "\n[oxygen_source]\nkind = \"vessel\"\nradius = 6\n"))
+    kw, refvol = C.simulation_kwargs(cfg)
+    assert kw["o2_hold"] == 4 and kw["vessel_radius"] == 6
+    # the ball's centre is radius + 8 from the vessel's: their edges meet on one
+    # pixel, which stays vessel (add_ball skips obstacles, cpm.rs:338-339)
+    assert refvol == 196
+
+
+def test_what_the_device_step_does_not_run_is_refused_by_name(tmp_path):
+    for extra, word in [("\n[oxygen_source]\nkind = \"capillary\"\nradius = 3\n", "capillary"),
+                        ("\n[seeding]\nkind = \"sheet\"\nside = 10\n", "sheet"),
+                        ("mutation_rate = 0.1\n", "mutation"),
+                        ("\n[angiogenesis]\nthreshold = 0.5\n", "angiogenesis"),
+                        ("debris_loss = 0.1\n", "debris_loss"),
+                        ("contact_order = 4\n", "contact_order")]:
+        cfg = C.load_sim_config(write(tmp_path, (extra + BASE) if extra.startswith("\n") is False else BASE + extra))
+        with pytest.raises(cw.ConfigError, match=word):
+            C.simulation_kwargs(cfg)
+    with pytest.raises(cw.ConfigError, match="mcs"):
+        C.load_sim_config(write(tmp_path, BASE.replace("mcs = 30\n", "")))
+    with pytest.raises(cw.ConfigError, match="network"):
+        C.simulation_kwargs(C.load_sim_config(write(tmp_path, BASE.replace('network = "net.toml"\n', ""))))
+
+
+def test_released_fields_map_onto_the_step(tmp_path):
+    cfg = C.load_sim_config(write(tmp_path, BASE + "\n[waste]\nproduction = 0.01\n[necrotic_factor]\n"
+                                                   "production = 0.05\nrelease_for = 12\n"))
+    kw, _ = C.simulation_kwargs(cfg)
+    assert kw["waste_production"] == 0.01 and kw["necrotic_production"] == 0.05 and kw["necrotic_release_for"] == 12
+
+
+def test_the_edge_is_the_boxs_sides_and_a_baths_faces():
+    g = np.zeros((1, 10, 10), np.int32)
+    g[0, 4:6, 4:6] = 1
+    assert not C.touches_the_edge(g)
+    g[0, 0, 5] = 1
+    assert C.touches_the_edge(g)
+    v = np.zeros((5, 10, 10), np.int32)
+    v[0, 5, 5] = 1
+    assert C.touches_the_edge(v) and not C.touches_the_edge(v, vessel=True)

@@ -1,0 +1,88 @@
+"""A configuration file's scenario on the device against the oracle (GPU).
+
+A spheroid and a cord written as the reference's configuration files are
+(crates/io/src/config.rs), with the RAS/ERK network of the reference's
+examples: one cell in a bath (or against a vessel) grows, divides every 20
+steps, starves inside; the device's 32 histories against the oracle stepping
+the same scenario with the reference's algorithms (sequential random-pixel
+sweep, FP64 SOR, RK4), living and necrotic cells and the tissue's radius and
+viable depth inside the oracle's 32-seed band; and the run loop's
+measurements.csv.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import cellweave_b200 as cw
+from cellweave_b200 import config as C
+from cpm_ensembles import SEEDS, within_band
+from oracle.cpu_sim import CpuHistory
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def ras_erk_toml(tmp_path):
+    spec = json.load(open(os.path.join(HERE, "golden", "golden.json")))["networks"]["ras-erk"]
+    lines = []
+    for node in spec["nodes"]:
+        lines += ["[[nodes]]", f'name = "{node["name"]}"', f'initial = {node["initial"]}', "terms = ["]
+        for t in node["terms"]:
+            kv = ", ".join(f'{k} = "{v}"' if isinstance(v, str) else f"{k} = {v}" for k, v in t.items())
+            lines.append(f"  {{ {kv} }},")
+        lines.append("]")
+    lines.append("[roles]")
+    lines += [f'{k} = "{v}"' for k, v in spec["roles"].items()]
+    lines.append("[mechanics]")
+    lines += [f"{k} = {v}" for k, v in spec["mechanics"].items()]
+    (tmp_path / "ras-erk.toml").write_text("\n".join(lines) + "\n")
+    return spec
+
+
+def scenario(tmp_path, source, uptake=0.001):
+    spec = ras_erk_toml(tmp_path)
+    text = ("width = 120\nheight = 120\nmcs = 140\ntemperature = 10.0\nsnapshot_interval = 20\n"
+            f"output_dir = \"out\"\noxygen_uptake = {uptake}\nnetwork = \"ras-erk.toml\"\n" + source)
+    p = tmp_path / "run.toml"
+    p.write_text(text)
+    return str(p), spec
+
+
+@pytest.mark.parametrize("source,uptake", [("", 0.001), ("\n[oxygen_source]\nkind = \"vessel\"\nradius = 5\n", 0.0001)])
+def test_a_configured_tissue_grows_inside_the_oracle_band(tmp_path, source, uptake):
+    path, spec = scenario(tmp_path, source, uptake)
+    cfg = C.load_sim_config(path)
+    seeds = [7_000 + k for k in range(SEEDS)]
+    sim, _ = C.simulation_from_config(cfg, histories=SEEDS, seeds=seeds)
+    kw, _ = C.simulation_kwargs(cfg, SEEDS, seeds)
+    ocfg = dict(kw, network_spec=spec, lambda_volume=float(spec["mechanics"]["lambda_volume"]), hypoxic_level=0.1)
+    ora = [CpuHistory(ocfg, k) for k in range(SEEDS)]
+    keys = ("cycling", "quiescent", "necrotic", "tissue_radius", "viable_depth")
+    for step in range(1, 141):
+        sim.step(1)
+        for h in ora:
+            h.step()
+        if step not in (60, 100, 140):
+            continue
+        dm = sim.measure()
+        om = [h.measure() for h in ora]
+        for q in keys:
+            dv = np.array([float(m[q]) for m in dm])
+            rv = np.array([float(m[q]) for m in om])
+            assert within_band(dv, rv), (step, q, dv.mean(), rv.mean(), rv.std())
+    final = np.array([m["cycling"] + m["quiescent"] for m in sim.measure()])
+    assert final.mean() > 8  # it grew
+    for k in range(SEEDS):
+        assert sim.records_match_grid(k)
+
+
+def test_the_run_writes_the_measurements_of_every_step(tmp_path):
+    path, _ = scenario(tmp_path, "")
+    out = C.run(path, str(tmp_path / "out"), steps=25)
+    rows = (tmp_path / "out" / "measurements.csv").read_text().splitlines()
+    assert rows[0] == cw.output.MEASUREMENT_COLUMNS
+    assert len(rows) == 1 + out["steps"] == 26
+    assert rows[1].startswith("0,") and rows[-1].startswith("24,")
