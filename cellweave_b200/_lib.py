@@ -98,7 +98,8 @@ class SimConfig(C.Structure):
                 ("divide", C.c_int32), ("max_cells", C.c_int32), ("spare_cells", C.c_int32),
                 ("waste_production", C.c_double), ("necrotic_production", C.c_double),
                 ("necrotic_release_for", C.c_int32), ("subsweeps", C.c_int32), ("o2_uptake", C.c_double),
-                ("divide_every", C.c_int32), ("vessel_radius", C.c_int32), ("stop_rule", C.c_int32)]
+                ("divide_every", C.c_int32), ("vessel_radius", C.c_int32), ("stop_rule", C.c_int32),
+                ("first_tolerance", C.c_double), ("cycle_median", C.c_double), ("cycle_spread", C.c_double)]
 
 
 P = C.c_void_p
@@ -184,6 +185,7 @@ SIGNATURES = {
     "cw_sim_field": (C.c_int, [P, I32, P]),
     "cw_sim_stats": (C.c_int, [P, P]),
     "cw_sim_network_state": (C.c_int, [P, U32, U32, P]),
+    "cw_sim_cycle": (C.c_int, [P, U32, U32, P, P]),
     "cw_fit_create": (C.c_int, [P, P, P, P]),
     "cw_fit_destroy": (C.c_int, [P]),
     "cw_fit_nparams": (C.c_int, [P, P]),

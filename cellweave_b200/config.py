@@ -10,21 +10,21 @@ reference's contact energies between medium, tumour, normal and necrotic
 cells (ContactEnergy::default, cpm.rs:63-86), oxygen diffusing at 0.2 and
 taken up at ``oxygen_uptake`` by every living pixel (and by the stroma around
 a vessel), networks stepped eight units of their time a step, division
-checked every 20 steps, waste and necrotic factor when configured.  Every
-other feature of the file (capillaries, sheets, mutation and rewiring,
-exposure, lesions, angiogenesis, immunity, tracing, debris loss, cell cycles,
-still media) is refused by name.  ``run`` steps it for ``mcs`` steps or until
-the tissue touches the box's edge, writing measurements.csv as the reference
+checked every 20 steps (every step with a cell cycle of its own), waste and
+necrotic factor when configured.  Every other feature of the file
+(capillaries, sheets, mutation and rewiring, exposure, lesions,
+angiogenesis, immunity, tracing, debris loss, still media) is refused by
+name.  ``run`` steps it for ``mcs`` steps or until the tissue touches the
+box's edge, writing measurements.csv and the snapshots as the reference
 does.
 
 The oxygen is the reference's relax pixel for pixel: FP64 red-black SOR until
 no pixel moves by more than 0.01 x uptake a sweep (simulation.rs:79-99; a
 zero-order uptake empties the core, where the reference's update floors the
 field at zero, which the FP32 defect correction's linear inner solve does not
-follow).  Two differences stand: no warm-up solve to 1e-8 before the first
-step (the field starts at the source's level everywhere), and the Monte Carlo
-step is the device's sub-sweeps (four by default, the kinetics nearest
-random pixels).
+follow); the first step's solve goes to 1e-8 from the source's level, as
+start() does.  One difference stands: the Monte Carlo step is the device's
+sub-sweeps (four by default, the kinetics nearest random pixels).
 """
 from __future__ import annotations
 
@@ -36,7 +36,7 @@ import numpy as np
 
 from ._lib import ConfigError
 from .engine import FP64, STOP_MAX_CHANGE, Network, Simulation, load_network_spec
-from .output import MeasurementLog
+from .output import MeasurementLog, snapshot, write_snapshot
 
 # SimConfig's fields without a default (config.rs:12-40) and their defaults
 REQUIRED = ("width", "height", "mcs", "temperature", "snapshot_interval", "output_dir")
@@ -51,6 +51,7 @@ OXYGEN_TOLERANCE = 0.01      # simulation.rs:85
 NETWORK_TIME_PER_MCS = 8     # simulation.rs:115
 DEATH_THRESHOLD = 0.25       # simulation.rs:118
 DIVISION_CHECK_EVERY = 20    # simulation.rs:55
+OXYGEN_WARMUP_TOLERANCE = 1e-8  # simulation.rs:95
 FIRST_CELL_RADIUS = 8        # simulation.rs:65
 FIRST_CELL_RADIUS_3D = 3     # simulation.rs:74
 MEDIUM, TUMOR, NORMAL, NECROTIC = 0, 1, 2, 3
@@ -90,8 +91,8 @@ def _refuse(cfg):
         raise ConfigError(f"{name}: the device step runs a bath or a vessel, not a {src}")
     if cfg["seeding"].get("kind", "single") != "single":
         raise ConfigError(f"{name}: the device step seeds one cell, not a {cfg['seeding'].get('kind')}")
-    for key in ("exposure", "lesion", "angiogenesis", "immunity", "tracing", "debris_loss", "cycle",
-                "still_medium", "suppress_before"):
+    for key in ("exposure", "lesion", "angiogenesis", "immunity", "tracing", "debris_loss", "still_medium",
+                "suppress_before"):
         if cfg.get(key) is not None:
             raise ConfigError(f"{name}: `{key}` is not part of the device step")
     if cfg["mutation_rate"] or cfg["rewiring"] or cfg["suppress"]:
@@ -138,7 +139,13 @@ def simulation_kwargs(cfg, histories=1, seeds=None, subsweeps=4):
               tolerance=OXYGEN_TOLERANCE * uptake, precision=FP64, stop_rule=STOP_MAX_CHANGE,
               dt=1.0, substeps=NETWORK_TIME_PER_MCS, sweeps=int(cfg["sweeps_per_step"]),
               death_threshold=DEATH_THRESHOLD, necrotic_type=NECROTIC, divide=True,
-              max_cells=int(cfg["max_cells"]), divide_every=DIVISION_CHECK_EVERY, subsweeps=int(subsweeps))
+              max_cells=int(cfg["max_cells"]), divide_every=DIVISION_CHECK_EVERY, subsweeps=int(subsweeps),
+              first_tolerance=OXYGEN_WARMUP_TOLERANCE)
+    if cfg.get("cycle"):
+        cy = cfg["cycle"]
+        if "median" not in cy or "spread" not in cy:
+            raise ConfigError(f"{os.path.basename(cfg['path'])}: a cycle names its median and its spread")
+        kw.update(cycle_median=float(cy["median"]), cycle_spread=float(cy["spread"]), divide_every=1)
     if cfg.get("waste"):
         kw["waste_production"] = float(cfg["waste"]["production"])
     if cfg.get("necrotic_factor"):
@@ -171,10 +178,21 @@ def touches_the_edge(grid, vessel=False) -> bool:
     return bool(sides or (d > 1 and not vessel and (cell[0].any() or cell[-1].any())))
 
 
+def snapshot_of(sim, hist, mcs):
+    """Simulation::snapshot (simulation.rs:1980-2003) of one history."""
+    lat = sim.lattice()
+    n = lat.cell_count(hist)
+    rec = lat.cells(n, hist)
+    return snapshot(mcs, sim.grid(hist), rec["type"], rec["volume"], sim.network_state(n, hist),
+                    sim.field_values(0, hist))
+
+
 def run(path, out_dir=None, histories=1, seeds=None, subsweeps=4, steps=None):
-    """The reference's run loop (src/main.rs:162-190) on the device: every
-    step measured into measurements.csv (one directory per history when there
-    are several), stopping after the step the tissue touches the edge."""
+    """The reference's run loop (src/main.rs:162-206) on the device: every
+    step measured into measurements.csv, a snapshot every
+    `snapshot_interval` steps and at the step the tissue touches the edge,
+    after which that history stops (one directory per history when there
+    are several)."""
     cfg = load_sim_config(path)
     sim, _ = simulation_from_config(cfg, histories, seeds, subsweeps)
     out_dir = out_dir or os.path.join(os.path.dirname(cfg["path"]), cfg["output_dir"])
@@ -192,8 +210,12 @@ def run(path, out_dir=None, histories=1, seeds=None, subsweeps=4, steps=None):
             if done[k]:
                 continue
             logs[k].record(ms[k])
+            mcs = int(ms[k]["mcs"])
             if touches_the_edge(sim.grid(k), vessel):
                 done[k] = True
+                write_snapshot(dirs[k], snapshot_of(sim, k, mcs))
+            elif mcs % int(cfg["snapshot_interval"]) == 0:
+                write_snapshot(dirs[k], snapshot_of(sim, k, mcs))
         if all(done):
             break
     for lg in logs:

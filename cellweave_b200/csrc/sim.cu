@@ -31,6 +31,7 @@ struct cw_sim_s {
     cw_field_s *wst = nullptr, *nfc = nullptr;  // the released fields: waste, necrotic factor
     double *cell_wst = nullptr, *cell_nfc = nullptr, *wst_rate = nullptr, *nfc_rate = nullptr;
     int32_t *died_at = nullptr;     // the step a cell turned necrotic (-1: not yet)
+    int32_t *began = nullptr, *due = nullptr;  // a cell's cycle: the step it began and the step it is over
     uint32_t *d_step = nullptr;     // the step being taken, on the device
     uint8_t *bath = nullptr;        // the bath of the current lattice, one byte per site
     std::vector<cw_relax_stats> last_wst, last_nfc;
@@ -210,9 +211,12 @@ __global__ void k_measure_lines(const int32_t *grid, const int32_t *type, const 
 // mechanics branches): a necrotic cell gives up RESORPTION_RATE pixels a step
 // until it is gone; survival below the threshold makes a living cell
 // necrotic; every other living cell takes the target its mechanics give.
+// With a cycle (simulation.rs:1301-1304) the target is grown(): half the
+// network's target when the cycle begins, all of it when it is over.
 __global__ void k_fates(const uint8_t *alive, const double *state, int64_t nc, int survival, double death,
                         int necrotic, const uint32_t *mech_target, int32_t *type, const int32_t *volume,
-                        int32_t *target, double *lambda, double lam, int32_t *died_at, const uint32_t *step) {
+                        int32_t *target, double *lambda, double lam, int32_t *died_at, const uint32_t *step,
+                        const int32_t *began, const int32_t *due) {
     int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nc) return;
     if (necrotic >= 0 && type[c] == necrotic) {
@@ -229,8 +233,41 @@ __global__ void k_fates(const uint8_t *alive, const double *state, int64_t nc, i
         if (died_at) died_at[c] = (int32_t)*step;
         return;
     }
-    target[c] = (int32_t)min(mech_target[c], 0x7fffffffu);
+    uint32_t full = min(mech_target[c], 0x7fffffffu);
+    if (began && due[c] > began[c]) {
+        // grown (simulation.rs:2534-2540)
+        const double passed = fmin((double)((int64_t)*step - began[c]) / (double)(due[c] - began[c]), 1.0);
+        full = (uint32_t)round((double)full * (0.5 + 0.5 * passed));
+    }
+    target[c] = (int32_t)full;
     lambda[c] = lam;
+}
+
+// The cycle lengths of each division (simulation.rs:1701-1713, 1739-1745):
+// the parent's and the daughter's begin at this step and last median x
+// exp(spread z), z a standard normal by Box and Muller from two uniform draws
+// (Philox(parent, step, 5, 0) under the history's key), rounded, a step at
+// least.
+__device__ __forceinline__ int32_t cycle_length(double u, double v, double median, double spread) {
+    const double z = sqrt(-2.0 * log(1.0 - u)) * cos(6.283185307179586 * v);
+    return (int32_t)fmax(round(median * exp(spread * z)), 1.0);
+}
+__global__ void k_cycle_births(const int64_t *cell_off, int nh, int64_t nc, const int32_t *daughter, const uint2 *keys,
+                               const uint32_t *step, double median, double spread, int32_t *began, int32_t *due,
+                               const int32_t *count) {
+    if (*count == 0) return;
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nc || daughter[c] < 0) return;
+    int lo = 0, hi = nh - 1;
+    while (lo < hi) { const int mid = (lo + hi + 1) >> 1; if (cell_off[mid] <= c) lo = mid; else hi = mid - 1; }
+    const int64_t d = cell_off[lo] + daughter[c];
+    const uint2 k = keys[lo];
+    const uint32_t now = *step;
+    const uint4 r = philox((uint32_t)(c - cell_off[lo]), now, 5u, 0u, k.x, k.y);
+    const uint4 q = philox((uint32_t)(c - cell_off[lo]), now, 5u, 1u, k.x, k.y);
+    began[c] = began[d] = (int32_t)now;
+    due[c] = (int32_t)now + cycle_length(u01(r.x, r.y), u01(r.z, r.w), median, spread);
+    due[d] = (int32_t)now + cycle_length(u01(q.x, q.y), u01(q.z, q.w), median, spread);
 }
 
 // Which cells divide this step (divide_ready_cells, simulation.rs:1603-1626):
@@ -242,7 +279,7 @@ __global__ void k_fates(const uint8_t *alive, const double *state, int64_t nc, i
 __global__ void k_div_ready(const int32_t *type, const int32_t *volume, const int64_t *cell_off, const uint2 *keys,
                             const int4 *dims, int nh, int64_t nc, int necrotic, const double *state, int hyp,
                             double threshold, const uint32_t *mcs_ctr, uint8_t *alive, uint8_t *flag,
-                            double *normal, int32_t *count, const uint32_t *step, int every) {
+                            double *normal, int32_t *count, const uint32_t *step, int every, const int32_t *due_at) {
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nc) return;
     int lo = 0, hi = nh - 1;
@@ -252,7 +289,7 @@ __global__ void k_div_ready(const int32_t *type, const int32_t *volume, const in
     alive[c] = a;
     // the check on the steps it is taken on (every > 1: step % every == 0)
     const bool due = every <= 1 || (*step % (uint32_t)every) == 0u;
-    const bool ready = due && a && (double)volume[c] >= threshold &&
+    const bool ready = due && a && (double)volume[c] >= threshold && (!due_at || due_at[c] <= (int32_t)*step) &&
                        (hyp < 0 || state[(int64_t)hyp * nc + c] < QUIESCENCE_THRESHOLD);
     flag[c] = ready;
     if (!ready) return;
@@ -401,6 +438,9 @@ int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out) {
     if (c.o2_hold == 4 && c.vessel_radius < 1) return fail(CW_ERR_CONFIG, "a vessel needs a radius of a pixel or more");
     if (c.stop_rule == CW_STOP_MAX_CHANGE && c.precision != CW_FP64)
         return fail(CW_ERR_CONFIG, "the largest change a sweep is the FP64 solve's stopping rule");
+    if (c.cycle_median != 0.0 && !(c.cycle_median >= 1.0 && c.cycle_median < 1e9 && c.cycle_spread >= 0.0 &&
+                                   c.cycle_spread < 1e3))
+        return fail(CW_ERR_CONFIG, "a cycle lasts a step at least, and its spread is not below zero");
     if (!net) return fail(CW_ERR_CONFIG, "a simulation needs a network");
     int32_t survival = network_role(net, 1);
     cw_sim_s *s = new cw_sim_s();
@@ -522,6 +562,15 @@ int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out) {
         cw_sim_destroy(s);
         return rc;
     }
+    if (c.cycle_median > 0.0) {
+        if ((rc = dalloc(&s->began, nc)) || (rc = dalloc(&s->due, nc))) {
+            cw_sim_destroy(s);
+            return rc;
+        }
+        // the cells the tissue starts with: no cycle behind them (simulation.rs:1055-1056)
+        CW_CUDA(cudaMemsetAsync(s->began, 0, sizeof(int32_t) * nc, stream()));
+        CW_CUDA(cudaMemsetAsync(s->due, 0, sizeof(int32_t) * nc, stream()));
+    }
     CW_CUDA(cudaMemsetAsync(s->d_step, 0, sizeof(uint32_t), stream()));
     CW_CUDA(cudaMemsetAsync(s->died_at, 0xFF, sizeof(int32_t) * nc, stream()));
     CW_CUDA(cudaMemsetAsync(s->cell_wst, 0, sizeof(double) * nc, stream()));
@@ -567,7 +616,7 @@ int cw_sim_destroy(cw_sim s) {
     cw_field_destroy(s->sig);
     cw_field_destroy(s->wst);
     cw_field_destroy(s->nfc);
-    dfree(s->cell_wst); dfree(s->cell_nfc); dfree(s->wst_rate); dfree(s->nfc_rate); dfree(s->died_at);
+    dfree(s->cell_wst); dfree(s->cell_nfc); dfree(s->wst_rate); dfree(s->nfc_rate); dfree(s->died_at); dfree(s->began); dfree(s->due);
     dfree(s->d_step); dfree(s->bath); dfree(s->d_uptake);
     dfree(s->d_sink); dfree(s->cell_o2); dfree(s->cell_sig); dfree(s->sum); dfree(s->secretion); dfree(s->count);
     dfree(s->state); dfree(s->inputs); dfree(s->alive); dfree(s->target32);
@@ -677,10 +726,17 @@ static int division_step(cw_sim_s *s) {
     k_div_ready<<<(unsigned)blocks(nc), T, 0, stream()>>>(
         l->type, l->volume, l->d_cell_off, l->d_keys, l->g.d_dims, (int)c.nh, nc, c.necrotic_type, s->state,
         network_role(s->net, 2), DIVISION_RATIO * (double)network_reference_volume(s->net),
-        (const uint32_t *)l->d_flag, s->alive, l->div.flag, l->div.normal, l->div.count, s->d_step, c.divide_every);
+        (const uint32_t *)l->d_flag, s->alive, l->div.flag, l->div.normal, l->div.count, s->d_step, c.divide_every,
+        s->due);
     CW_LAUNCHED();
-    return lattice_divide_enqueue(l, s->alive, c.max_cells > 0 ? c.max_cells : DEFAULT_MAX_CELLS, s->state,
-                                  network_nodes(s->net));
+    int rc = lattice_divide_enqueue(l, s->alive, c.max_cells > 0 ? c.max_cells : DEFAULT_MAX_CELLS, s->state,
+                                    network_nodes(s->net));
+    if (rc != CW_OK || !s->due) return rc;
+    k_cycle_births<<<(unsigned)blocks(nc), T, 0, stream()>>>(l->d_cell_off, (int)c.nh, nc, l->div.daughter, l->d_keys,
+                                                             s->d_step, c.cycle_median, c.cycle_spread, s->began,
+                                                             s->due, l->div.count);
+    CW_LAUNCHED();
+    return CW_OK;
 }
 
 // Who takes up oxygen (declare_sources, simulation.rs:2138-2163): the
@@ -734,7 +790,7 @@ static int enqueue_phase(cw_sim_s *s, int p, const cw_relax_opts &o) {
     k_fates<<<(unsigned)blocks(nc), T, 0, stream()>>>(s->alive, s->state, nc, network_role(s->net, 1),
                                                       c.death_threshold, c.necrotic_type, s->target32, s->lat->type,
                                                       s->lat->volume, s->lat->target, s->lat->lambda, c.lambda_volume,
-                                                      s->died_at, s->d_step);
+                                                      s->died_at, s->d_step, s->began, s->due);
     CW_LAUNCHED();
     for (int k = 0; k < c.sweeps; ++k)
         if ((rc = lattice_sweep(s->lat)) != CW_OK) return rc;
@@ -873,7 +929,13 @@ int cw_sim_step(cw_sim s, uint32_t nsteps) {
             // 1. downward coupling and the oxygen solve
             if ((rc = paint_oxygen(s)) != CW_OK) return rc;
             const double *om = c.omega > 0.0 ? nullptr : s->omega[0].data();
-            if ((rc = field_relax(s->o2, &o, om, s->last.data())) != CW_OK) return rc;
+            cw_relax_opts o1 = o;
+            if (s->steps == 0 && c.first_tolerance > 0.0) {
+                // settled tightly once, from scratch (OXYGEN_WARMUP_*, simulation.rs:91-98)
+                o1.tolerance = std::min(c.first_tolerance, c.tolerance);
+                o1.max_sweeps = 2000000;
+            }
+            if ((rc = field_relax(s->o2, &o1, om, s->last.data())) != CW_OK) return rc;
             if (tuning) tune_book(s, 0, s->last);
             if (!s->depth_tuned && (rc = tune_depth(s)) != CW_OK) return rc;
         }
@@ -940,7 +1002,7 @@ int cw_sim_step(cw_sim s, uint32_t nsteps) {
         k_fates<<<(unsigned)blocks(nc), T, 0, stream()>>>(s->alive, s->state, nc, survival, c.death_threshold,
                                                           c.necrotic_type, s->target32, s->lat->type,
                                                           s->lat->volume, s->lat->target, s->lat->lambda,
-                                                          c.lambda_volume, s->died_at, s->d_step);
+                                                          c.lambda_volume, s->died_at, s->d_step, s->began, s->due);
         CW_LAUNCHED();
         // 5. the lattice, then 6. division
         for (int k = 0; k < c.sweeps; ++k)
@@ -1076,6 +1138,17 @@ int cw_sim_network_state(cw_sim s, uint32_t hist, uint32_t n, double *state) {
         CW_CUDA(cudaStreamSynchronize(stream()));
         for (uint32_t cc = 0; cc < n; ++cc) state[(size_t)cc * S + i] = col[cc];
     }
+    return CW_OK;
+}
+
+int cw_sim_cycle(cw_sim s, uint32_t hist, uint32_t n, int32_t *began, int32_t *due) {
+    if (hist >= s->cfg.nh) return fail(CW_ERR_NOT_FOUND, "no history " + std::to_string(hist));
+    if (!s->due) return fail(CW_ERR_CONFIG, "this simulation has no cell cycle");
+    int64_t c0 = s->lat->cell_off[hist], cap = s->lat->cell_off[hist + 1] - c0;
+    if ((int64_t)n > cap) return fail(CW_ERR_CONFIG, "more cells asked for than the history holds");
+    CW_CUDA(cudaMemcpyAsync(began, s->began + c0, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, stream()));
+    CW_CUDA(cudaMemcpyAsync(due, s->due + c0, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, stream()));
+    CW_CUDA(cudaStreamSynchronize(stream()));
     return CW_OK;
 }
 

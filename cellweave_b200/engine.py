@@ -625,7 +625,8 @@ class Simulation:
                  omega=None, inner_sweeps=0, relax_every=1, dt=0.01, substeps=8, sweeps=1, death_threshold=0.25,
                  necrotic_type=-1, use_graphs=True, divide=True, max_cells=2000, spare_cells=0,
                  waste_production=0.0, necrotic_production=0.0, necrotic_release_for=-1, subsweeps=1,
-                 o2_uptake=0.0, divide_every=1, vessel_radius=0, stop_rule=STOP_RESIDUAL):
+                 o2_uptake=0.0, divide_every=1, vessel_radius=0, stop_rule=STOP_RESIDUAL, first_tolerance=0.0,
+                 cycle_median=0.0, cycle_spread=0.0):
         self.dims, w, h, z = _dims(dims)
         self._keep = [w, h, z]
         nc = np.array(ncells, np.uint32)
@@ -644,7 +645,8 @@ class Simulation:
                              int(necrotic_type), int(bool(use_graphs)), int(bool(divide)), int(max_cells),
                              int(spare_cells), float(waste_production), float(necrotic_production),
                              int(necrotic_release_for), int(subsweeps), float(o2_uptake), int(divide_every),
-                             int(vessel_radius), int(stop_rule))
+                             int(vessel_radius), int(stop_rule), float(first_tolerance), float(cycle_median),
+                             float(cycle_spread))
         handle = C.c_void_p()
         call("cw_sim_create", C.byref(cfg), network.handle, C.byref(handle))
         self._h = handle
@@ -722,6 +724,12 @@ class Simulation:
         out = np.empty((int(n), self.network.S))
         call("cw_sim_network_state", self._h, int(hist), int(n), ptr(out))
         return out
+
+    def cycle(self, n, hist=0):
+        """(began, due) of records 0..n-1 of a history: each cell's cycle."""
+        began, due = np.empty(int(n), np.int32), np.empty(int(n), np.int32)
+        call("cw_sim_cycle", self._h, int(hist), int(n), ptr(began), ptr(due))
+        return began, due
 
 
 # ============================================================== Fit (adjoint)

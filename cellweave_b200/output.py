@@ -1,4 +1,5 @@
-"""measurements.csv, as the reference writes it (crates/io/src/output.rs:30-97).
+"""measurements.csv and the JSON snapshots, as the reference writes them
+(crates/io/src/output.rs:10-97).
 
 One row per step, the columns of MEASUREMENT_COLUMNS in that order, counts as
 integers and the exposure and the three radii to four decimals, so that two
@@ -11,7 +12,10 @@ vessel, all of it perfused.
 """
 from __future__ import annotations
 
+import json
 import os
+
+import numpy as np
 
 MEASUREMENT_COLUMNS = ("mcs,cycling,quiescent,necrotic,differentiating,apoptotic,exposure,born,gone,clones,lesion,"
                        "vessel,perfused,sprouts,regressed,immune,killed,tissue_radius,necrotic_radius,viable_depth")
@@ -55,3 +59,41 @@ class MeasurementLog:
 
     def __exit__(self, *exc):
         self.close()
+
+
+# CellKind (crates/core/src/types.rs:61-76) by the device's type index
+KIND_NAMES = ("Medium", "Tumor", "Normal", "Necrotic", "Differentiated", "Apoptotic")
+
+
+def snapshot(mcs: int, grid, types, volumes, proteins, oxygen) -> dict:
+    """Simulation::snapshot (simulation.rs:1980-2003): every cell with pixels,
+    in id order, its kind, volume, protein levels, the mean oxygen over its
+    pixels now (mean_per_cell, coupling.rs:165-182) and its clone (the
+    founder's, 0: the device step does not mutate).  `grid` the lattice,
+    `types`/`volumes` the records, `proteins` [records, S], `oxygen` the
+    field, both flat or shaped as the lattice."""
+    g = np.asarray(grid).reshape(-1)
+    n = len(volumes)
+    inside = g > 0
+    sums = np.bincount(g[inside], weights=np.asarray(oxygen, np.float64).reshape(-1)[inside], minlength=n)[:n]
+    count = np.bincount(g[inside], minlength=n)[:n]
+    cells = []
+    for cid in range(1, n):
+        if volumes[cid] <= 0:
+            continue
+        cells.append(dict(id=cid, kind=KIND_NAMES[int(types[cid])], volume=int(volumes[cid]),
+                          proteins=dict(values=[float(v) for v in proteins[cid]]),
+                          oxygen=float(sums[cid] / count[cid]) if count[cid] else 0.0, clone=0))
+    return dict(mcs=int(mcs), cells=cells)
+
+
+def write_snapshot(directory: str, snap: dict) -> str:
+    """JsonOutput::write_snapshot (output.rs:24-35): snapshot_NNNNNN.json in
+    `directory`, pretty-printed with two-space indents.  Numbers are written
+    shortest-round-trip, as the reference's are; a float in exponent form
+    may be spelled differently (1e-07 for 1e-7) and reads back the same."""
+    os.makedirs(directory, exist_ok=True)
+    path = os.path.join(directory, "snapshot_{:06d}.json".format(int(snap["mcs"])))
+    with open(path, "w") as fh:
+        fh.write(json.dumps(snap, indent=2))
+    return path

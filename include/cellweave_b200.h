@@ -419,6 +419,12 @@ typedef struct {
     int32_t vessel_radius;       /* o2_hold 4 */
     int32_t stop_rule;           /* CW_STOP_RESIDUAL, or CW_STOP_MAX_CHANGE with CW_FP64: the reference's
                                     relax, pixel for pixel (no pixel moves by more than `tolerance` a sweep) */
+    double first_tolerance;      /* > 0: the first step's oxygen solved to this, up to 2,000,000 sweeps, from the
+                                    field's initial level (start(), simulation.rs:1068-1083) */
+    double cycle_median;         /* > 0: a cell cycle (Cycle, simulation.rs:1701-1745, 2529-2540): each division
+                                    draws the two cells' lengths, median x exp(spread z), a cell divides once its
+                                    cycle is over and asks meanwhile for half to all of its target */
+    double cycle_spread;
 } cw_sim_config;
 int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out);
 int cw_sim_destroy(cw_sim sim);
@@ -463,6 +469,9 @@ typedef struct {
 int cw_sim_measure(cw_sim sim, cw_measurements *out);
 /* Network state of history `hist`, [ncells][S]. */
 int cw_sim_network_state(cw_sim sim, uint32_t hist, uint32_t n, double *state);
+/* The cycle of records 0..n-1 of history `hist`: the step each began and the step it is over (the
+   reference's began / due, simulation.rs:486-491); CW_ERR_CONFIG without a cycle. */
+int cw_sim_cycle(cw_sim sim, uint32_t hist, uint32_t n, int32_t *began, int32_t *due);
 
 /* ------------------------------------------------------------------ differentiation
  * No counterpart in the reference (it has no adjoint, loss or autodiff): a

@@ -171,6 +171,9 @@ class CpuHistory:
         self.net = O.compile_network(spec, self.refvol)
         self.state = np.tile(self.net.initial, (self.ncap, 1))
         self.div_rng = np.random.default_rng(self.seed * 7 + 13)
+        # a cell's cycle (simulation.rs:1055-1056): none behind the cells the tissue starts with
+        self.began = np.zeros(self.ncap, np.int64)
+        self.due = np.zeros(self.ncap, np.int64)
         sink = np.zeros(8)
         sink[:len(cfg["o2_sink_by_type"])] = cfg["o2_sink_by_type"]
         self.sink = sink
@@ -218,7 +221,10 @@ class CpuHistory:
             self.o2.held[:] = 0
             self.o2.hold_bath(g == 0, 1.0)
         omega = c.get("omega") or 0.0
-        rc, _ = self.o2.relax(c["tolerance"], 200_000, omega=omega, stop=c.get("stop_rule", 1), threads=1)
+        tol, most = c["tolerance"], 200_000
+        if self.steps == 0 and c.get("first_tolerance", 0.0) > 0:
+            tol, most = min(c["first_tolerance"], tol), 2_000_000  # start() (simulation.rs:1068-1083)
+        rc, _ = self.o2.relax(tol, most, omega=omega, stop=c.get("stop_rule", 1), threads=1)
         o2m = O.mean_per_cell(g, self.o2.values, self.ncap)
         nec = c.get("necrotic_type", -1)
         alive = (self.lat.volume > 0) & (t != nec)
@@ -260,7 +266,14 @@ class CpuHistory:
             t[idx[dead]] = nec
             self.died_at[idx[dead]] = self.steps
             live = idx[~dead]
-            self.lat.target[live] = np.minimum(tg[~dead], 2**31 - 1).astype(np.int32)
+            full = np.minimum(tg[~dead], 2**31 - 1).astype(np.int64)
+            if c.get("cycle_median", 0.0) > 0:
+                # grown (simulation.rs:2534-2540)
+                b, e = self.began[live], self.due[live]
+                span = np.maximum(e - b, 1)
+                passed = np.minimum((self.steps - b) / span, 1.0)
+                full = np.where(e > b, np.floor(full * (0.5 + 0.5 * passed) + 0.5), full).astype(np.int64)
+            self.lat.target[live] = full.astype(np.int32)
             self.lat.lam[live] = c["lambda_volume"]
         self.lat.mcs_sequential(self.seed * 1_000_003 + self.steps, c.get("sweeps", 1))
         every = int(c.get("divide_every", 1) or 1)
@@ -268,6 +281,13 @@ class CpuHistory:
             self._divide_ready_cells()
         self.steps += 1
         return rc
+
+    def _cycle_length(self):
+        """cycle_length (simulation.rs:1739-1745): median x exp(spread z), z by Box and Muller."""
+        c = self.cfg
+        u, v = 1.0 - self.div_rng.random(), self.div_rng.random()
+        z = np.sqrt(-2.0 * np.log(u)) * np.cos(2.0 * np.pi * v)
+        return int(max(np.floor(c["cycle_median"] * np.exp(c.get("cycle_spread", 0.0) * z) + 0.5), 1.0))
 
     def _divide_ready_cells(self):
         """divide_ready_cells (simulation.rs:1603-1716) without cycle or mutation: the living
@@ -283,6 +303,8 @@ class CpuHistory:
         ready = alive & (vol >= 1.4 * self.refvol)
         if hyp is not None and hyp >= 0:
             ready &= self.state[:, hyp] < 0.45
+        if c.get("cycle_median", 0.0) > 0:
+            ready[:len(self.due)] &= self.due <= self.steps
         living = int(alive.sum())
         born = 0
         for cid in np.nonzero(ready)[0]:
@@ -299,4 +321,8 @@ class CpuHistory:
             d, self.used = self.lat.divide_across(int(cid), normal, self.used)
             if d >= 0:
                 self.state[d] = self.state[cid]
+                if c.get("cycle_median", 0.0) > 0:
+                    self.began[cid] = self.began[d] = self.steps
+                    self.due[cid] = self.steps + self._cycle_length()
+                    self.due[d] = self.steps + self._cycle_length()
                 born += 1

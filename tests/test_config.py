@@ -96,3 +96,16 @@ def test_the_edge_is_the_boxs_sides_and_a_baths_faces():
     v = np.zeros((5, 10, 10), np.int32)
     v[0, 5, 5] = 1
     assert C.touches_the_edge(v) and not C.touches_the_edge(v, vessel=True)
+
+
+def test_a_cycle_of_its_own_divides_every_step_and_is_checked(tmp_path):
+    cfg = C.load_sim_config(write(tmp_path, BASE + "\n[cycle]\nmedian = 20.0\nspread = 0.3\n"))
+    kw, _ = C.simulation_kwargs(cfg)
+    # divide_ready_cells every step with a cycle (simulation.rs:1341-1344)
+    assert kw["cycle_median"] == 20.0 and kw["cycle_spread"] == 0.3 and kw["divide_every"] == 1
+    # the first solve is start()'s (simulation.rs:91-98)
+    assert kw["first_tolerance"] == 1e-8
+    with pytest.raises(cw.ConfigError, match="median and its spread"):
+        C.simulation_kwargs(C.load_sim_config(write(tmp_path, BASE + "\n[cycle]\nmedian = 20.0\n")))
+    plain, _ = C.simulation_kwargs(C.load_sim_config(write(tmp_path, BASE)))
+    assert "cycle_median" not in plain and plain["divide_every"] == 20

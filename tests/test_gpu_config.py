@@ -51,7 +51,11 @@ def scenario(tmp_path, source, uptake=0.001):
     return str(p), spec
 
 
-@pytest.mark.parametrize("source,uptake", [("", 0.001), ("\n[oxygen_source]\nkind = \"vessel\"\nradius = 5\n", 0.0001)])
+CYCLE = "\n[cycle]\nmedian = 20.0\nspread = 0.3\n"
+
+
+@pytest.mark.parametrize("source,uptake", [("", 0.001), ("\n[oxygen_source]\nkind = \"vessel\"\nradius = 5\n", 0.0001),
+                                           (CYCLE, 0.001)])
 def test_a_configured_tissue_grows_inside_the_oracle_band(tmp_path, source, uptake):
     path, spec = scenario(tmp_path, source, uptake)
     cfg = C.load_sim_config(path)
@@ -79,10 +83,45 @@ def test_a_configured_tissue_grows_inside_the_oracle_band(tmp_path, source, upta
         assert sim.records_match_grid(k)
 
 
-def test_the_run_writes_the_measurements_of_every_step(tmp_path):
-    path, _ = scenario(tmp_path, "")
+def test_the_run_writes_the_measurements_of_every_step_and_the_snapshots(tmp_path):
+    path, spec = scenario(tmp_path, "")
     out = C.run(path, str(tmp_path / "out"), steps=25)
     rows = (tmp_path / "out" / "measurements.csv").read_text().splitlines()
     assert rows[0] == cw.output.MEASUREMENT_COLUMNS
     assert len(rows) == 1 + out["steps"] == 26
     assert rows[1].startswith("0,") and rows[-1].startswith("24,")
+    # snapshot_interval 20: steps 0 and 20 (src/main.rs:193-194)
+    names = sorted(p.name for p in (tmp_path / "out").iterdir() if p.name.startswith("snapshot_"))
+    assert names == ["snapshot_000000.json", "snapshot_000020.json"]
+    snap = json.loads((tmp_path / "out" / "snapshot_000020.json").read_text())
+    assert snap["mcs"] == 20 and len(snap["cells"]) >= 1
+    cell = snap["cells"][0]
+    assert cell["id"] == 1 and cell["kind"] == "Tumor" and cell["clone"] == 0
+    assert len(cell["proteins"]["values"]) == len(spec["nodes"]) and 0.0 < cell["oxygen"] <= 1.0
+
+
+def test_cells_with_a_cycle_draw_its_lengths_and_divide_on_their_own_clocks(tmp_path):
+    """cycle_lengths_have_the_median_and_spread_asked_for and
+    with_a_cycle_of_their_own_cells_stop_dividing_together
+    (simulation.rs:2868-2925): the lengths each division draws have the
+    median and the spread of their logarithm asked for, and births fall on
+    many steps of the 20-step check's period, not on one."""
+    path, _ = scenario(tmp_path, CYCLE.replace("20.0", "16.0"), uptake=0.0001)
+    cfg = C.load_sim_config(path)
+    hists = 32
+    sim, _ = C.simulation_from_config(cfg, histories=hists, seeds=[500 + k for k in range(hists)])
+    lat = sim.lattice()
+    drawn, residues = [], set()
+    for step in range(120):
+        sim.step(1)
+        for k in range(hists):
+            began, due = sim.cycle(lat.cell_count(k), k)
+            fresh = np.nonzero((began == step) & (due > began))[0]
+            if len(fresh):
+                drawn += list(due[fresh] - began[fresh])
+                residues.add(step % 20)
+    logs = np.log(np.array(drawn, float))
+    assert len(logs) >= 300, len(logs)
+    assert abs(np.exp(np.median(logs)) - 16.0) < 1.5, np.exp(np.median(logs))
+    assert abs(logs.std() - 0.3) < 0.05, logs.std()
+    assert len(residues) >= 10, residues

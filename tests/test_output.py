@@ -1,4 +1,10 @@
-"""measurements.csv as the reference writes it (crates/io/src/output.rs), on CPU."""
+"""measurements.csv and the snapshots as the reference writes them (crates/io/src/output.rs), on CPU."""
+import os
+
+import numpy as np
+import pytest
+
+from cellweave_b200 import output
 from cellweave_b200.output import MEASUREMENT_COLUMNS, MeasurementLog, measurement_row
 
 
@@ -18,3 +24,27 @@ def test_a_device_measurement_fills_the_columns_it_has():
     m = dict(mcs=3, cycling=10, quiescent=2, necrotic=4, born=20, gone=1, vessel=0, tissue_radius=5.5,
              necrotic_radius=2.0, viable_depth=3.5)
     assert measurement_row(m) == "3,10,2,4,0,0,0.0000,20,1,1,0,0,0,0,0,0,0,5.5000,2.0000,3.5000"
+
+
+def test_a_snapshot_lists_the_cells_with_pixels_as_the_reference_serialises_them(tmp_path):
+    import json
+    grid = np.zeros((1, 4, 5), np.int32)
+    grid[0, 0, :2] = 1
+    grid[0, 1:3, 3:] = 3
+    types = np.array([0, 1, 2, 3], np.int32)
+    volumes = np.array([0, 2, 0, 4], np.int32)   # record 2 is gone
+    proteins = np.arange(8, dtype=float).reshape(4, 2) / 8
+    o2 = np.linspace(0.0, 1.0, 20).reshape(1, 4, 5)
+    snap = output.snapshot(40, grid, types, volumes, proteins, o2)
+    assert snap["mcs"] == 40 and [c["id"] for c in snap["cells"]] == [1, 3]
+    first, dead = snap["cells"]
+    assert first["kind"] == "Tumor" and dead["kind"] == "Necrotic" and dead["volume"] == 4
+    assert first["proteins"] == {"values": [0.25, 0.375]} and first["clone"] == 0
+    assert first["oxygen"] == pytest.approx(o2.reshape(-1)[[0, 1]].mean())
+    assert dead["oxygen"] == pytest.approx(o2.reshape(-1)[[8, 9, 13, 14]].mean())
+    path = output.write_snapshot(str(tmp_path), snap)
+    assert os.path.basename(path) == "snapshot_000040.json"
+    text = open(path).read()
+    assert json.loads(text) == snap
+    # serde_json's pretty form: two-space indents, the fields in declaration order
+    assert text.startswith('{\n  "mcs": 40,\n  "cells": [\n    {\n      "id": 1,\n      "kind": "Tumor",')
