@@ -99,7 +99,8 @@ class SimConfig(C.Structure):
                 ("waste_production", C.c_double), ("necrotic_production", C.c_double),
                 ("necrotic_release_for", C.c_int32), ("subsweeps", C.c_int32), ("o2_uptake", C.c_double),
                 ("divide_every", C.c_int32), ("vessel_radius", C.c_int32), ("stop_rule", C.c_int32),
-                ("first_tolerance", C.c_double), ("cycle_median", C.c_double), ("cycle_spread", C.c_double)]
+                ("first_tolerance", C.c_double), ("cycle_median", C.c_double), ("cycle_spread", C.c_double),
+                ("debris_loss", C.c_double), ("still_medium", C.c_double)]
 
 
 P = C.c_void_p

@@ -10,11 +10,10 @@ reference's contact energies between medium, tumour, normal and necrotic
 cells (ContactEnergy::default, cpm.rs:63-86), oxygen diffusing at 0.2 and
 taken up at ``oxygen_uptake`` by every living pixel (and by the stroma around
 a vessel), networks stepped eight units of their time a step, division
-checked every 20 steps (every step with a cell cycle of its own), waste and
-necrotic factor when configured.  Every other feature of the file
-(capillaries, sheets, mutation and rewiring, exposure, lesions,
-angiogenesis, immunity, tracing, debris loss, still media) is refused by
-name.  ``run`` steps it for ``mcs`` steps or until the tissue touches the
+checked every 20 steps (every step with a cell cycle of its own); waste,
+necrotic factor, debris loss and a still medium when configured.  Every
+other feature of the file (capillaries, sheets, mutation and rewiring,
+exposure, lesions, angiogenesis, immunity, tracing) is refused by name.  ``run`` steps it for ``mcs`` steps or until the tissue touches the
 box's edge, writing measurements.csv and the snapshots as the reference
 does.
 
@@ -91,8 +90,7 @@ def _refuse(cfg):
         raise ConfigError(f"{name}: the device step runs a bath or a vessel, not a {src}")
     if cfg["seeding"].get("kind", "single") != "single":
         raise ConfigError(f"{name}: the device step seeds one cell, not a {cfg['seeding'].get('kind')}")
-    for key in ("exposure", "lesion", "angiogenesis", "immunity", "tracing", "debris_loss", "still_medium",
-                "suppress_before"):
+    for key in ("exposure", "lesion", "angiogenesis", "immunity", "tracing", "suppress_before"):
         if cfg.get(key) is not None:
             raise ConfigError(f"{name}: `{key}` is not part of the device step")
     if cfg["mutation_rate"] or cfg["rewiring"] or cfg["suppress"]:
@@ -146,6 +144,12 @@ def simulation_kwargs(cfg, histories=1, seeds=None, subsweeps=4):
         if "median" not in cy or "spread" not in cy:
             raise ConfigError(f"{os.path.basename(cfg['path'])}: a cycle names its median and its spread")
         kw.update(cycle_median=float(cy["median"]), cycle_spread=float(cy["spread"]), divide_every=1)
+    if cfg.get("debris_loss") is not None:
+        kw["debris_loss"] = float(cfg["debris_loss"])
+    if cfg.get("still_medium"):
+        if "diffusion" not in cfg["still_medium"]:
+            raise ConfigError(f"{os.path.basename(cfg['path'])}: a still medium names its diffusion")
+        kw["still_medium"] = float(cfg["still_medium"]["diffusion"])
     if cfg.get("waste"):
         kw["waste_production"] = float(cfg["waste"]["production"])
     if cfg.get("necrotic_factor"):

@@ -257,6 +257,7 @@ struct cw_field_s {
     cw::Span *d_span = nullptr;
     void *dc_cache = nullptr;        // plans and solver of the FP32 solve (field.cu)
     cw_field_s *adjoint = nullptr;   // twin of cw_field_relax_adjoint, made on its first call
+    cw::Plan inflow_plan;            // every site, for the inflow enqueued inside a step
     int alloc_fp32();
 };
 
@@ -276,6 +277,21 @@ int lattice_recount_surfaces(cw_lattice_s *l);  // surfaces from the grid into t
 int lattice_divide_enqueue(cw_lattice_s *l, const uint8_t *alive, int max_living, double *state, int S);
 int lattice_bath_enqueue(cw_lattice_s *l, uint8_t *bath);  // bath.cu: medium joined to the box's outer layer
 int lattice_bath_error();
+// debris.cu: the dead tissue's debris lost at its edge, the fluid shut in drained
+struct DebrisState {
+    uint8_t *kept = nullptr;   // per cell: dead, keeping the volume it died with
+    int32_t *given = nullptr;  // per cell: pixels given up this step
+    double *owed = nullptr;    // per history: pixels owed to the fluid, carried
+    int64_t *held = nullptr;   // per history: what the kept dead hold
+    int32_t *paid = nullptr, *edges = nullptr;  // per history, this step / this pass
+    int32_t *claim = nullptr;  // per site: the cell taking it this pass (-1: none)
+    int ensure(int64_t ncells, int nh, int64_t sites);
+    void release();
+};
+int debris_break_down_enqueue(cw_lattice_s *l, DebrisState &D, double loss, int necrotic, const uint32_t *step);
+int debris_drain_enqueue(cw_lattice_s *l, DebrisState &D, const uint8_t *bath, int necrotic, const uint32_t *step);
+// field.cu: inflow (pde.rs:415-456) and free_count per history, added into inflow / free_count
+int field_inflow_enqueue(cw_field_s *f, double *inflow, unsigned long long *free_count);
 // coupling (coupling.cu), device-resident
 int couple_uptake_device(cw_field_s *f, cw_lattice_s *l, const double *d_rate_by_type, int K, double *dst,
                          const Plan &p);

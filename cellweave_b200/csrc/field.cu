@@ -290,8 +290,10 @@ __global__ void k_dc_peek(RelaxState *st, int nh) {
     }
 }
 
-// inflow (pde.rs:415-456): flux from held pixels into free ones.
-__global__ void k_inflow(FieldView fv, const int32_t *blk, int nh, double *out) {
+// inflow (pde.rs:415-456): flux from held pixels into free ones; with
+// `free_count`, the free pixels counted too (free_count, pde.rs:459-462).
+__global__ void k_inflow(FieldView fv, const int32_t *blk, int nh, double *out,
+                         unsigned long long *free_count = nullptr) {
     __shared__ int s_h;
     if (threadIdx.x == 0) s_h = plan_history(blk, nh, blockIdx.x);
     __syncthreads();
@@ -316,6 +318,11 @@ __global__ void k_inflow(FieldView fv, const int32_t *blk, int nh, double *out) 
     }
     flux = warp_sum(flux);
     if ((threadIdx.x & 31) == 0 && flux != 0.0) atomicAdd(out + h, flux);
+    if (free_count) {
+        const bool free = local < fv.off[h + 1] - fv.off[h] && !fv.held[fv.off[h] + local];
+        const unsigned n = __popc(__ballot_sync(0xffffffffu, free));
+        if ((threadIdx.x & 31) == 0 && n) atomicAdd(free_count + h, (unsigned long long)n);
+    }
 }
 
 // DiffusionField::step (pde.rs:705-728), out of place.
@@ -1155,6 +1162,7 @@ int cw_field_destroy(cw_field f) {
     RelaxState *st = (RelaxState *)f->stats;
     dfree(st);
     if (f->adjoint) cw_field_destroy(f->adjoint);
+    f->inflow_plan.release();
     f->g.release();
     delete f;
     return CW_OK;
@@ -1363,6 +1371,17 @@ int cw::field_relax(cw_field_s *f, const cw_relax_opts *opts, const double *omeg
                                            " sweeps at tolerance " + std::to_string(o.tolerance));
     return CW_OK;
 }
+
+namespace cw {
+int field_inflow_enqueue(cw_field_s *f, double *inflow, unsigned long long *free_count) {
+    Plan &ps = f->inflow_plan;
+    int rc;
+    if (ps.nblocks == 0 && (rc = site_plan(f, ps)) != CW_OK) return rc;
+    k_inflow<<<ps.nblocks, T, 0, stream()>>>(view(f), ps.d_blk, (int)f->g.nh, inflow, free_count);
+    CW_LAUNCHED();
+    return CW_OK;
+}
+}  // namespace cw
 
 extern "C" {
 

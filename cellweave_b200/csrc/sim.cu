@@ -32,6 +32,11 @@ struct cw_sim_s {
     double *cell_wst = nullptr, *cell_nfc = nullptr, *wst_rate = nullptr, *nfc_rate = nullptr;
     int32_t *died_at = nullptr;     // the step a cell turned necrotic (-1: not yet)
     int32_t *began = nullptr, *due = nullptr;  // a cell's cycle: the step it began and the step it is over
+    cw::DebrisState debris;         // with a debris loss
+    bool debris_on = false;
+    double *level = nullptr;        // per history: the level the bath holds (1, or a still medium's)
+    double *d_inflow = nullptr;     // per history: what the tissue takes up from the held pixels
+    unsigned long long *d_free = nullptr;  // per history: the oxygen's free pixels
     uint32_t *d_step = nullptr;     // the step being taken, on the device
     uint8_t *bath = nullptr;        // the bath of the current lattice, one byte per site
     std::vector<cw_relax_stats> last_wst, last_nfc;
@@ -130,13 +135,33 @@ __global__ void k_inputs_released(const double *cell_wst, const double *cell_nfc
     if (cell_nfc) inputs[5 * nc + c] = cell_nfc[c];
 }
 
-// A field held exactly on `mask` at `value` (release_all, then hold_bath_at).
-__global__ void k_hold_from_mask(const uint8_t *mask, int64_t n, double value, uint8_t *held, double *c) {
+// A field held exactly on `mask` at `value` (release_all, then hold_bath_at),
+// or, given `level`, at its history's level (off: the histories' sites).
+__global__ void k_hold_from_mask(const uint8_t *mask, int64_t n, double value, uint8_t *held, double *c,
+                                 const double *level = nullptr, const int64_t *off = nullptr, int nh = 0) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint8_t m = mask[i];
     held[i] = m;
-    if (m) c[i] = value;
+    if (!m) return;
+    if (level) {
+        int lo = 0, hi = nh - 1;
+        while (lo < hi) { const int mid = (lo + hi + 1) >> 1; if (off[mid] <= i) lo = mid; else hi = mid - 1; }
+        value = level[lo];
+    }
+    c[i] = value;
+}
+
+// settle_bath_level (simulation.rs:2114-2125): a still medium of diffusion
+// `dm` around the tissue holds 1 - inflow / (4 pi dm r), r the radius of a
+// ball of the free pixels, at zero at least.
+__global__ void k_bath_level(int nh, const double *inflow, const unsigned long long *free_count, double dm,
+                             double *level) {
+    const int h = blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= nh) return;
+    const double four_pi = 4.0 * 3.141592653589793;
+    const double r = cbrt(3.0 * (double)free_count[h] / four_pi);
+    level[h] = r > 0.0 ? fmax(1.0 - inflow[h] / (four_pi * dm * r), 0.0) : 1.0;
 }
 
 __global__ void k_step_advance(uint32_t *step) { *step += 1u; }
@@ -216,12 +241,15 @@ __global__ void k_measure_lines(const int32_t *grid, const int32_t *type, const 
 __global__ void k_fates(const uint8_t *alive, const double *state, int64_t nc, int survival, double death,
                         int necrotic, const uint32_t *mech_target, int32_t *type, const int32_t *volume,
                         int32_t *target, double *lambda, double lam, int32_t *died_at, const uint32_t *step,
-                        const int32_t *began, const int32_t *due) {
+                        const int32_t *began, const int32_t *due, uint8_t *kept) {
     int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nc) return;
     if (necrotic >= 0 && type[c] == necrotic) {
         const int32_t v = volume[c];
-        if (v > 0) {
+        if (v > 0 && kept) {
+            // with a debris loss the dead keep what they held (simulation.rs:1226-1244)
+            if (!kept[c]) { kept[c] = 1; target[c] = v; lambda[c] = lam; }
+        } else if (v > 0) {
             target[c] = v > RESORPTION_RATE ? v - RESORPTION_RATE : 0;
             lambda[c] = lam;
         }
@@ -231,6 +259,7 @@ __global__ void k_fates(const uint8_t *alive, const double *state, int64_t nc, i
     if (necrotic >= 0 && state[survival * nc + c] < death) {
         type[c] = necrotic;
         if (died_at) died_at[c] = (int32_t)*step;
+        if (kept) { kept[c] = 1; target[c] = volume[c]; lambda[c] = lam; }  // simulation.rs:1264-1275
         return;
     }
     uint32_t full = min(mech_target[c], 0x7fffffffu);
@@ -441,6 +470,17 @@ int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out) {
     if (c.cycle_median != 0.0 && !(c.cycle_median >= 1.0 && c.cycle_median < 1e9 && c.cycle_spread >= 0.0 &&
                                    c.cycle_spread < 1e3))
         return fail(CW_ERR_CONFIG, "a cycle lasts a step at least, and its spread is not below zero");
+    if (c.debris_loss != 0.0 && !(c.debris_loss > 0.0 && c.debris_loss <= 1.0))
+        return fail(CW_ERR_CONFIG, "debris loss is the share of a dead cell lost per step, above zero and at most one");
+    if (c.debris_loss > 0.0 && c.necrotic_type < 0) return fail(CW_ERR_CONFIG, "debris loss needs a necrotic type");
+    if (c.still_medium != 0.0) {
+        if (!(c.still_medium > 0.0 && c.still_medium < 1e300))
+            return fail(CW_ERR_CONFIG, "the still medium's diffusion is above zero");
+        if (c.o2_hold != 3) return fail(CW_ERR_CONFIG, "a still medium is the bath's, and this scenario has none");
+        for (uint32_t k = 0; k < c.nh; ++k)
+            if (!c.d || c.d[k] <= 1)
+                return fail(CW_ERR_CONFIG, "a still medium is solved around a ball, and a plane has none");
+    }
     if (!net) return fail(CW_ERR_CONFIG, "a simulation needs a network");
     int32_t survival = network_role(net, 1);
     cw_sim_s *s = new cw_sim_s();
@@ -558,9 +598,23 @@ int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out) {
         cw_sim_destroy(s);
         return rc;
     }
-    if ((c.o2_hold == 3 || s->wst || s->nfc) && (rc = dalloc(&s->bath, (size_t)s->lat->g.total)) != CW_OK) {
+    s->debris_on = c.debris_loss > 0.0;
+    if ((c.o2_hold == 3 || s->wst || s->nfc || s->debris_on) &&
+        (rc = dalloc(&s->bath, (size_t)s->lat->g.total)) != CW_OK) {
         cw_sim_destroy(s);
         return rc;
+    }
+    if (s->debris_on && (rc = s->debris.ensure(nc, (int)c.nh, s->lat->g.total)) != CW_OK) {
+        cw_sim_destroy(s);
+        return rc;
+    }
+    if ((rc = dalloc(&s->level, c.nh)) || (rc = dalloc(&s->d_inflow, c.nh)) || (rc = dalloc(&s->d_free, c.nh))) {
+        cw_sim_destroy(s);
+        return rc;
+    }
+    {
+        std::vector<double> ones(c.nh, 1.0);
+        CW_CUDA(cudaMemcpy(s->level, ones.data(), sizeof(double) * c.nh, cudaMemcpyHostToDevice));
     }
     if (c.cycle_median > 0.0) {
         if ((rc = dalloc(&s->began, nc)) || (rc = dalloc(&s->due, nc))) {
@@ -617,6 +671,7 @@ int cw_sim_destroy(cw_sim s) {
     cw_field_destroy(s->wst);
     cw_field_destroy(s->nfc);
     dfree(s->cell_wst); dfree(s->cell_nfc); dfree(s->wst_rate); dfree(s->nfc_rate); dfree(s->died_at); dfree(s->began); dfree(s->due);
+    s->debris.release(); dfree(s->level); dfree(s->d_inflow); dfree(s->d_free);
     dfree(s->d_step); dfree(s->bath); dfree(s->d_uptake);
     dfree(s->d_sink); dfree(s->cell_o2); dfree(s->cell_sig); dfree(s->sum); dfree(s->secretion); dfree(s->count);
     dfree(s->state); dfree(s->inputs); dfree(s->alive); dfree(s->target32);
@@ -739,6 +794,18 @@ static int division_step(cw_sim_s *s) {
     return CW_OK;
 }
 
+// settle_bath_level (simulation.rs:2114-2125) from the field as solved.
+static int settle_bath_level(cw_sim_s *s) {
+    const int nh = (int)s->cfg.nh;
+    CW_CUDA(cudaMemsetAsync(s->d_inflow, 0, sizeof(double) * nh, stream()));
+    CW_CUDA(cudaMemsetAsync(s->d_free, 0, sizeof(unsigned long long) * nh, stream()));
+    int rc = field_inflow_enqueue(s->o2, s->d_inflow, s->d_free);
+    if (rc != CW_OK) return rc;
+    k_bath_level<<<(unsigned)blocks(nh), T, 0, stream()>>>(nh, s->d_inflow, s->d_free, s->cfg.still_medium, s->level);
+    CW_LAUNCHED();
+    return CW_OK;
+}
+
 // Who takes up oxygen (declare_sources, simulation.rs:2138-2163): the
 // first-order sinks by type (and of the medium), and with o2_uptake the
 // zero-order uptake of every living cell's pixel (apply_uptake) and, around a
@@ -790,7 +857,8 @@ static int enqueue_phase(cw_sim_s *s, int p, const cw_relax_opts &o) {
     k_fates<<<(unsigned)blocks(nc), T, 0, stream()>>>(s->alive, s->state, nc, network_role(s->net, 1),
                                                       c.death_threshold, c.necrotic_type, s->target32, s->lat->type,
                                                       s->lat->volume, s->lat->target, s->lat->lambda, c.lambda_volume,
-                                                      s->died_at, s->d_step, s->began, s->due);
+                                                      s->died_at, s->d_step, s->began, s->due,
+                                                          s->debris_on ? s->debris.kept : nullptr);
     CW_LAUNCHED();
     for (int k = 0; k < c.sweeps; ++k)
         if ((rc = lattice_sweep(s->lat)) != CW_OK) return rc;
@@ -907,7 +975,8 @@ int cw_sim_step(cw_sim s, uint32_t nsteps) {
         o.window = s->sor_window;
         const bool graph_ok = c.use_graphs && c.precision == CW_FP32_DC && c.relax_every <= 1 && !s->tune.active &&
                               s->depth_tuned && s->steps >= 2 && !s->last.empty() &&
-                              (!s->sig || !s->last_sig.empty()) && !s->wst && !s->nfc && c.o2_hold != 3;
+                              (!s->sig || !s->last_sig.empty()) && !s->wst && !s->nfc && c.o2_hold != 3 &&
+                              !s->debris_on;
         if (graph_ok) {
             if (!s->graphs && (rc = build_graphs(s, o)) != CW_OK) return rc;
             if ((rc = step_graph(s, o)) != CW_OK) return rc;
@@ -919,8 +988,8 @@ int cw_sim_step(cw_sim s, uint32_t nsteps) {
             // the bath of the lattice as it stands (hold_medium_bath, coupling.rs:156-158)
             if ((rc = lattice_bath_enqueue(s->lat, s->bath)) != CW_OK) return rc;
             if (c.o2_hold == 3) {
-                k_hold_from_mask<<<(unsigned)blocks(s->o2->g.total), T, 0, stream()>>>(s->bath, s->o2->g.total, 1.0,
-                                                                                      s->o2->held, s->o2->c);
+                k_hold_from_mask<<<(unsigned)blocks(s->o2->g.total), T, 0, stream()>>>(
+                    s->bath, s->o2->g.total, 1.0, s->o2->held, s->o2->c, s->level, s->lat->g.d_off, (int)c.nh);
                 CW_LAUNCHED();
                 s->o2->held_dirty = true;
             }
@@ -930,12 +999,24 @@ int cw_sim_step(cw_sim s, uint32_t nsteps) {
             if ((rc = paint_oxygen(s)) != CW_OK) return rc;
             const double *om = c.omega > 0.0 ? nullptr : s->omega[0].data();
             cw_relax_opts o1 = o;
-            if (s->steps == 0 && c.first_tolerance > 0.0) {
+            const bool warm = s->steps == 0 && c.first_tolerance > 0.0;
+            if (warm) {
                 // settled tightly once, from scratch (OXYGEN_WARMUP_*, simulation.rs:91-98)
                 o1.tolerance = std::min(c.first_tolerance, c.tolerance);
                 o1.max_sweeps = 2000000;
             }
             if ((rc = field_relax(s->o2, &o1, om, s->last.data())) != CW_OK) return rc;
+            if (c.still_medium > 0.0) {
+                // the level a step behind the field (settle_bath_level after start() and each solve)
+                if ((rc = settle_bath_level(s)) != CW_OK) return rc;
+                if (warm) {
+                    k_hold_from_mask<<<(unsigned)blocks(s->o2->g.total), T, 0, stream()>>>(
+                        s->bath, s->o2->g.total, 1.0, s->o2->held, s->o2->c, s->level, s->lat->g.d_off, (int)c.nh);
+                    CW_LAUNCHED();
+                    if ((rc = field_relax(s->o2, &o, om, s->last.data())) != CW_OK) return rc;
+                    if ((rc = settle_bath_level(s)) != CW_OK) return rc;
+                }
+            }
             if (tuning) tune_book(s, 0, s->last);
             if (!s->depth_tuned && (rc = tune_depth(s)) != CW_OK) return rc;
         }
@@ -1002,8 +1083,20 @@ int cw_sim_step(cw_sim s, uint32_t nsteps) {
         k_fates<<<(unsigned)blocks(nc), T, 0, stream()>>>(s->alive, s->state, nc, survival, c.death_threshold,
                                                           c.necrotic_type, s->target32, s->lat->type,
                                                           s->lat->volume, s->lat->target, s->lat->lambda,
-                                                          c.lambda_volume, s->died_at, s->d_step, s->began, s->due);
+                                                          c.lambda_volume, s->died_at, s->d_step, s->began, s->due,
+                                                          s->debris_on ? s->debris.kept : nullptr);
         CW_LAUNCHED();
+        // 4b. with a debris loss, the dead tissue's debris lost at its edge and
+        // the fluid shut in drained (simulation.rs:1311-1315)
+        if (s->debris_on) {
+            if ((rc = debris_break_down_enqueue(s->lat, s->debris, c.debris_loss, c.necrotic_type, s->d_step)) !=
+                CW_OK)
+                return rc;
+            if ((rc = lattice_bath_enqueue(s->lat, s->bath)) != CW_OK) return rc;
+            if ((rc = debris_drain_enqueue(s->lat, s->debris, s->bath, c.necrotic_type, s->d_step)) != CW_OK)
+                return rc;
+            if (s->lat->surface_on && (rc = lattice_recount_surfaces(s->lat)) != CW_OK) return rc;
+        }
         // 5. the lattice, then 6. division
         for (int k = 0; k < c.sweeps; ++k)
             if ((rc = lattice_sweep(s->lat)) != CW_OK) return rc;

@@ -425,6 +425,13 @@ typedef struct {
                                     draws the two cells' lengths, median x exp(spread z), a cell divides once its
                                     cycle is over and asks meanwhile for half to all of its target */
     double cycle_spread;
+    double debris_loss;          /* (0, 1]: the share of a dead cell's volume its debris loses a step, taken at the
+                                    tissue's edge, and the fluid the tissue shuts in drained (break_down_debris,
+                                    drain_shut_in, simulation.rs:1746-1826); 0: dead cells resorb RESORPTION_RATE
+                                    pixels a step.  Needs necrotic_type */
+    double still_medium;         /* > 0: the bath is still medium of this diffusion, and the level it holds falls
+                                    with what the tissue takes up (settle_bath_level, simulation.rs:2104-2125);
+                                    o2_hold 3 in volumes only */
 } cw_sim_config;
 int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out);
 int cw_sim_destroy(cw_sim sim);

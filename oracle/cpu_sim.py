@@ -174,6 +174,10 @@ class CpuHistory:
         # a cell's cycle (simulation.rs:1055-1056): none behind the cells the tissue starts with
         self.began = np.zeros(self.ncap, np.int64)
         self.due = np.zeros(self.ncap, np.int64)
+        # debris loss (simulation.rs:1226-1275): the dead kept, the debt to the fluid
+        self.kept = np.zeros(self.ncap, bool)
+        self.debris_owed = 0.0
+        self.bath_level = 1.0  # a still medium's level (simulation.rs:1054)
         sink = np.zeros(8)
         sink[:len(cfg["o2_sink_by_type"])] = cfg["o2_sink_by_type"]
         self.sink = sink
@@ -219,12 +223,20 @@ class CpuHistory:
         if c.get("o2_hold", 0) == 3:
             # the bath as the lattice stands (declare_sources, simulation.rs:2138-2146)
             self.o2.held[:] = 0
-            self.o2.hold_bath(g == 0, 1.0)
+            self.o2.hold_bath(g == 0, self.bath_level)
         omega = c.get("omega") or 0.0
         tol, most = c["tolerance"], 200_000
         if self.steps == 0 and c.get("first_tolerance", 0.0) > 0:
             tol, most = min(c["first_tolerance"], tol), 2_000_000  # start() (simulation.rs:1068-1083)
         rc, _ = self.o2.relax(tol, most, omega=omega, stop=c.get("stop_rule", 1), threads=1)
+        if c.get("still_medium", 0.0) > 0:
+            self._settle_bath_level()
+            if most == 2_000_000:
+                # start() settled the level after its solve; the first step solves against it
+                self.o2.held[:] = 0
+                self.o2.hold_bath(g == 0, self.bath_level)
+                rc, _ = self.o2.relax(c["tolerance"], 200_000, omega=omega, stop=c.get("stop_rule", 1), threads=1)
+                self._settle_bath_level()
         o2m = O.mean_per_cell(g, self.o2.values, self.ncap)
         nec = c.get("necrotic_type", -1)
         alive = (self.lat.volume > 0) & (t != nec)
@@ -242,11 +254,19 @@ class CpuHistory:
             dead[0] = False
             self.cell_nfc = self._settle_released(self.nfc, np.where(dead, c["necrotic_production"], 0.0))
         # a necrotic cell gives up 2 pixels a step until it is gone (simulation.rs:1230-1262)
+        loss = c.get("debris_loss", 0.0)
         if nec >= 0:
             dying = np.nonzero((t == nec) & (self.lat.volume > 0))[0]
             dying = dying[dying > 0]
-            self.lat.target[dying] = np.maximum(self.lat.volume[dying] - 2, 0)
-            self.lat.lam[dying] = c["lambda_volume"]
+            if loss > 0:
+                # the dead keep what they held when kept (simulation.rs:1226-1244)
+                new = dying[~self.kept[dying]]
+                self.kept[new] = True
+                self.lat.target[new] = self.lat.volume[new]
+                self.lat.lam[new] = c["lambda_volume"]
+            else:
+                self.lat.target[dying] = np.maximum(self.lat.volume[dying] - 2, 0)
+                self.lat.lam[dying] = c["lambda_volume"]
         idx = np.nonzero(alive)[0]
         if len(idx):
             ins = np.zeros((len(idx), 6))
@@ -265,6 +285,12 @@ class CpuHistory:
             dead = (st[:, self.net.survival] < c.get("death_threshold", 0.25)) if nec >= 0 else np.zeros(len(idx), bool)
             t[idx[dead]] = nec
             self.died_at[idx[dead]] = self.steps
+            if loss > 0:
+                # kept from the step it dies (simulation.rs:1264-1275)
+                nd = idx[dead]
+                self.kept[nd] = True
+                self.lat.target[nd] = self.lat.volume[nd]
+                self.lat.lam[nd] = c["lambda_volume"]
             live = idx[~dead]
             full = np.minimum(tg[~dead], 2**31 - 1).astype(np.int64)
             if c.get("cycle_median", 0.0) > 0:
@@ -275,12 +301,114 @@ class CpuHistory:
                 full = np.where(e > b, np.floor(full * (0.5 + 0.5 * passed) + 0.5), full).astype(np.int64)
             self.lat.target[live] = full.astype(np.int32)
             self.lat.lam[live] = c["lambda_volume"]
+        if loss > 0:
+            self._break_down_debris(loss)
+            self._drain_shut_in()
         self.lat.mcs_sequential(self.seed * 1_000_003 + self.steps, c.get("sweeps", 1))
         every = int(c.get("divide_every", 1) or 1)
         if self.divide and (every <= 1 or self.steps % every == 0):
             self._divide_ready_cells()
         self.steps += 1
         return rc
+
+    def _settle_bath_level(self):
+        """settle_bath_level (simulation.rs:2114-2125): 1 - inflow / (4 pi D r), r
+        the radius of a ball of the free pixels, at zero at least."""
+        taken = self.o2.inflow()
+        radius = np.cbrt(3.0 * float((self.o2.held == 0).sum()) / (4.0 * np.pi))
+        d = self.cfg["still_medium"]
+        self.bath_level = max(1.0 - taken / (4.0 * np.pi * d * radius), 0.0) if radius > 0 else 1.0
+
+    def _faces(self):
+        """Per direction: (pixels with a neighbour that way, the neighbour's flat index)."""
+        w, h, d = self.lat.w, self.lat.h, self.lat.d
+        i = np.arange(w * h * d)
+        x, y, z = i % w, (i // w) % h, i // (w * h)
+        dirs = [(x > 0, i - 1), (x + 1 < w, i + 1), (y > 0, i - w), (y + 1 < h, i + w)]
+        if d > 1:
+            dirs += [(z > 0, i - w * h), (z + 1 < d, i + w * h)]
+        return [(ok, np.where(ok, j, 0)) for ok, j in dirs]
+
+    def _living_around(self, pix, faces):
+        """living_around (cpm.rs:709-722) of each pixel in `pix`: [n, 6] neighbour
+        ids that are living tissue of another cell (0 where none), and their count."""
+        g, t = self.lat.grid, self.lat.type
+        nec = self.cfg.get("necrotic_type", -1)
+        own = g[pix]
+        ids = np.zeros((len(pix), len(faces)), np.int64)
+        for k, (ok, j) in enumerate(faces):
+            o = np.where(ok[pix], g[j[pix]], 0)
+            good = (o > 0) & (o != own)
+            good &= t[np.clip(o, 0, None)] != nec
+            ids[:, k] = np.where(good, o, 0)
+        return ids, (ids > 0).sum(axis=1)
+
+    def _give(self, pix, ids, n, rng):
+        """Each pixel to one of its living neighbours, drawn uniformly."""
+        pick = np.minimum((rng.random(len(pix)) * n).astype(np.int64), n - 1)
+        order = np.cumsum(ids > 0, axis=1) - 1
+        taker = ids[np.arange(len(pix)), np.argmax((order == pick[:, None]) & (ids > 0), axis=1)]
+        return taker
+
+    def _break_down_debris(self, loss):
+        """break_down_debris (simulation.rs:1746-1808): every whole pixel owed
+        taken at the dead tissue's edge, up to EDGE_PASSES passes; within a pass
+        a uniform draw of the edge without replacement, each taker drawn against
+        the lattice at the pass's start."""
+        vol = self.lat.volume
+        kept = np.nonzero(self.kept & (vol > 0))[0]
+        self.debris_owed += loss * float(vol[kept].sum())
+        owed = int(np.floor(self.debris_owed))
+        if owed <= 0:
+            return
+        g = self.lat.grid
+        keptmask = np.zeros(len(vol), bool)
+        keptmask[kept] = True
+        pool = np.nonzero((g > 0) & keptmask[np.clip(g, 0, None)])[0]
+        held, paid = len(pool), 0
+        given = np.zeros(len(vol), np.int64)
+        faces = self._faces()
+        for _ in range(8):
+            ids, n = self._living_around(pool, faces)
+            edge, rest = pool[n > 0], pool[n == 0]
+            if len(edge) == 0:
+                break
+            take = min(owed - paid, len(edge))
+            chosen = self.div_rng.permutation(len(edge))[:take]
+            pix, pids, pn = edge[chosen], ids[n > 0][chosen], n[n > 0][chosen]
+            taker = self._give(pix, pids, pn, self.div_rng)
+            dead = g[pix]
+            g[pix] = taker
+            np.subtract.at(vol, dead, 1)
+            np.add.at(vol, taker, 1)
+            np.add.at(given, dead, 1)
+            paid += take
+            if paid == owed:
+                break
+            left = np.ones(len(edge), bool)
+            left[chosen] = False
+            pool = np.concatenate([rest, edge[left]])
+        self.debris_owed = min(self.debris_owed - paid, float(held - paid))
+        lost = np.nonzero(given > 0)[0]
+        self.lat.target[lost] = np.maximum(self.lat.target[lost] - given[lost], 0)
+
+    def _drain_shut_in(self):
+        """drain_shut_in (simulation.rs:1810-1826): medium the bath does not
+        reach, with living tissue across a face, to one of those neighbours,
+        each drawn against the lattice as it stood."""
+        g = self.lat.grid
+        scratch = O.Field(self.lat.w, self.lat.h, self.lat.d)
+        scratch.hold_bath(g == 0, 1.0)
+        shut = np.nonzero((g == 0) & (scratch.held == 0))[0]
+        if len(shut) == 0:
+            return
+        ids, n = self._living_around(shut, self._faces())
+        pix, ids, n = shut[n > 0], ids[n > 0], n[n > 0]
+        if len(pix) == 0:
+            return
+        taker = self._give(pix, ids, n, self.div_rng)
+        g[pix] = taker
+        np.add.at(self.lat.volume, taker, 1)
 
     def _cycle_length(self):
         """cycle_length (simulation.rs:1739-1745): median x exp(spread z), z by Box and Muller."""

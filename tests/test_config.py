@@ -69,7 +69,7 @@ def test_what_the_device_step_does_not_run_is_refused_by_name(tmp_path):
                         ("\n[seeding]\nkind = \"sheet\"\nside = 10\n", "sheet"),
                         ("mutation_rate = 0.1\n", "mutation"),
                         ("\n[angiogenesis]\nthreshold = 0.5\n", "angiogenesis"),
-                        ("debris_loss = 0.1\n", "debris_loss"),
+                        ("\n[lesion]\nat = 10\nradius = 4\n", "lesion"),
                         ("contact_order = 4\n", "contact_order")]:
         cfg = C.load_sim_config(write(tmp_path, (extra + BASE) if extra.startswith("\n") is False else BASE + extra))
         with pytest.raises(cw.ConfigError, match=word):
@@ -109,3 +109,12 @@ def test_a_cycle_of_its_own_divides_every_step_and_is_checked(tmp_path):
         C.simulation_kwargs(C.load_sim_config(write(tmp_path, BASE + "\n[cycle]\nmedian = 20.0\n")))
     plain, _ = C.simulation_kwargs(C.load_sim_config(write(tmp_path, BASE)))
     assert "cycle_median" not in plain and plain["divide_every"] == 20
+
+
+def test_debris_loss_and_a_still_medium_are_carried(tmp_path):
+    cfg = C.load_sim_config(write(tmp_path, "depth = 40\ndebris_loss = 0.024\n" + BASE.replace("width = 60", "width = 40")
+                                  .replace("height = 50", "height = 40") + "\n[still_medium]\ndiffusion = 0.606\n"))
+    kw, refvol = C.simulation_kwargs(cfg)
+    assert kw["debris_loss"] == 0.024 and kw["still_medium"] == 0.606
+    # a ball of radius 3 in a volume (simulation.rs:74)
+    assert kw["seed_side"] == 3 and refvol == 123

@@ -55,7 +55,7 @@ CYCLE = "\n[cycle]\nmedian = 20.0\nspread = 0.3\n"
 
 
 @pytest.mark.parametrize("source,uptake", [("", 0.001), ("\n[oxygen_source]\nkind = \"vessel\"\nradius = 5\n", 0.0001),
-                                           (CYCLE, 0.001)])
+                                           (CYCLE, 0.001), ("debris_loss = 0.05\n", 0.001)])
 def test_a_configured_tissue_grows_inside_the_oracle_band(tmp_path, source, uptake):
     path, spec = scenario(tmp_path, source, uptake)
     cfg = C.load_sim_config(path)
@@ -125,3 +125,38 @@ def test_cells_with_a_cycle_draw_its_lengths_and_divide_on_their_own_clocks(tmp_
     assert abs(np.exp(np.median(logs)) - 16.0) < 1.5, np.exp(np.median(logs))
     assert abs(logs.std() - 0.3) < 0.05, logs.std()
     assert len(residues) >= 10, residues
+
+
+def test_a_still_spheroid_in_a_volume_loses_its_debris_inside_the_oracle_band(tmp_path):
+    """A small spheroid-3d: a ball of radius 3 in a 40^3 box, 26-neighbour
+    contact, four sweeps a step, a cell cycle, a still medium whose level
+    falls as the tissue grows, and a debris loss that takes the dead core's
+    pixels at its edge; living, quiescent and necrotic cells, the tissue's
+    and the necrotic radius inside the oracle's 32-seed band."""
+    spec = ras_erk_toml(tmp_path)
+    text = ("width = 40\nheight = 40\ndepth = 40\nmcs = 180\ntemperature = 10.0\nsnapshot_interval = 20\n"
+            "output_dir = \"out\"\noxygen_uptake = 0.005\ndebris_loss = 0.024\nsweeps_per_step = 4\n"
+            "contact_order = 3\nnetwork = \"ras-erk.toml\"\n" + CYCLE + "[still_medium]\ndiffusion = 0.606\n")
+    (tmp_path / "run.toml").write_text(text)
+    cfg = C.load_sim_config(str(tmp_path / "run.toml"))
+    seeds = [9_000 + k for k in range(SEEDS)]
+    sim, _ = C.simulation_from_config(cfg, histories=SEEDS, seeds=seeds)
+    kw, _ = C.simulation_kwargs(cfg, SEEDS, seeds)
+    ocfg = dict(kw, network_spec=spec, lambda_volume=float(spec["mechanics"]["lambda_volume"]), hypoxic_level=0.1)
+    ora = [CpuHistory(ocfg, k) for k in range(SEEDS)]
+    keys = ("cycling", "quiescent", "necrotic", "tissue_radius", "necrotic_radius")
+    for step in range(1, 181):
+        sim.step(1)
+        for h in ora:
+            h.step()
+        if step not in (100, 140, 180):
+            continue
+        dm = sim.measure()
+        om = [h.measure() for h in ora]
+        for q in keys:
+            dv = np.array([float(m[q]) for m in dm])
+            rv = np.array([float(m[q]) for m in om])
+            assert within_band(dv, rv), (step, q, dv.mean(), rv.mean(), rv.std())
+    assert np.mean([m["necrotic"] for m in sim.measure()]) > 2  # a core died and is breaking down
+    for k in range(SEEDS):
+        assert sim.records_match_grid(k)
