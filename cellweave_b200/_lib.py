@@ -71,7 +71,7 @@ class Mutation(C.Structure):
 class Measurements(C.Structure):
     _fields_ = [("mcs", C.c_uint64), ("cycling", C.c_uint64), ("quiescent", C.c_uint64), ("necrotic", C.c_uint64),
                 ("born", C.c_uint64), ("gone", C.c_uint64), ("vessel", C.c_uint64), ("tissue_radius", C.c_double),
-                ("necrotic_radius", C.c_double), ("viable_depth", C.c_double)]
+                ("necrotic_radius", C.c_double), ("viable_depth", C.c_double), ("exposure", C.c_double)]
 
 
 class FitConfig(C.Structure):
@@ -100,7 +100,9 @@ class SimConfig(C.Structure):
                 ("necrotic_release_for", C.c_int32), ("subsweeps", C.c_int32), ("o2_uptake", C.c_double),
                 ("divide_every", C.c_int32), ("vessel_radius", C.c_int32), ("stop_rule", C.c_int32),
                 ("first_tolerance", C.c_double), ("cycle_median", C.c_double), ("cycle_spread", C.c_double),
-                ("debris_loss", C.c_double), ("still_medium", C.c_double)]
+                ("debris_loss", C.c_double), ("still_medium", C.c_double),
+                ("exposure_intensity", C.c_double), ("exposure_uptake", C.c_double), ("exposure_start", C.c_int32),
+                ("exposure_on", C.c_int32), ("exposure_off", C.c_int32)]
 
 
 P = C.c_void_p

@@ -10,10 +10,11 @@ reference's contact energies between medium, tumour, normal and necrotic
 cells (ContactEnergy::default, cpm.rs:63-86), oxygen diffusing at 0.2 and
 taken up at ``oxygen_uptake`` by every living pixel (and by the stroma around
 a vessel), networks stepped eight units of their time a step, division
-checked every 20 steps (every step with a cell cycle of its own); waste,
-necrotic factor, debris loss and a still medium when configured.  Every
-other feature of the file (capillaries, sheets, mutation and rewiring,
-exposure, lesions, angiogenesis, immunity, tracing) is refused by name.  ``run`` steps it for ``mcs`` steps or until the tissue touches the
+checked every 20 steps (every step with a cell cycle of its own); an
+exposure's stress, waste, necrotic factor, debris loss and a still medium
+when configured.  Every other feature of the file (capillaries, sheets,
+mutation and rewiring, lesions, angiogenesis, immunity, tracing) is refused
+by name.  ``run`` steps it for ``mcs`` steps or until the tissue touches the
 box's edge, writing measurements.csv and the snapshots as the reference
 does.
 
@@ -90,7 +91,7 @@ def _refuse(cfg):
         raise ConfigError(f"{name}: the device step runs a bath or a vessel, not a {src}")
     if cfg["seeding"].get("kind", "single") != "single":
         raise ConfigError(f"{name}: the device step seeds one cell, not a {cfg['seeding'].get('kind')}")
-    for key in ("exposure", "lesion", "angiogenesis", "immunity", "tracing", "suppress_before"):
+    for key in ("lesion", "angiogenesis", "immunity", "tracing", "suppress_before"):
         if cfg.get(key) is not None:
             raise ConfigError(f"{name}: `{key}` is not part of the device step")
     if cfg["mutation_rate"] or cfg["rewiring"] or cfg["suppress"]:
@@ -144,6 +145,8 @@ def simulation_kwargs(cfg, histories=1, seeds=None, subsweeps=4):
         if "median" not in cy or "spread" not in cy:
             raise ConfigError(f"{os.path.basename(cfg['path'])}: a cycle names its median and its spread")
         kw.update(cycle_median=float(cy["median"]), cycle_spread=float(cy["spread"]), divide_every=1)
+    if cfg.get("exposure"):
+        kw.update(_exposure(cfg))
     if cfg.get("debris_loss") is not None:
         kw["debris_loss"] = float(cfg["debris_loss"])
     if cfg.get("still_medium"):
@@ -157,6 +160,28 @@ def simulation_kwargs(cfg, histories=1, seeds=None, subsweeps=4):
         kw["necrotic_production"] = float(nf["production"])
         kw["necrotic_release_for"] = int(nf["release_for"]) if nf.get("release_for") is not None else -1
     return kw, refvol
+
+
+def _exposure(cfg):
+    """Exposure (types.rs:92-104): intensity, uptake, start and a continuous or
+    periodic schedule, as Simulation's exposure_* options."""
+    name = os.path.basename(cfg["path"])
+    e = cfg["exposure"]
+    missing = [k for k in ("intensity", "uptake", "start", "schedule") if k not in e]
+    if missing:
+        raise ConfigError(f"{name}: the exposure names its {missing[0]}")
+    sched = e["schedule"]
+    kind = sched.get("kind")
+    if kind == "continuous":
+        on, off = 0, 0
+    elif kind == "periodic":
+        on, off = int(sched["on"]), int(sched["off"])
+        if on == 0:
+            raise ConfigError(f"{name}: a periodic exposure that is on for zero steps is never on")
+    else:
+        raise ConfigError(f"{name}: an exposure's schedule is continuous or periodic, not {kind}")
+    return dict(exposure_intensity=float(e["intensity"]), exposure_uptake=float(e["uptake"]),
+                exposure_start=int(e["start"]), exposure_on=on, exposure_off=off)
 
 
 def simulation_from_config(cfg, histories=1, seeds=None, subsweeps=4):

@@ -32,6 +32,10 @@ struct cw_sim_s {
     double *cell_wst = nullptr, *cell_nfc = nullptr, *wst_rate = nullptr, *nfc_rate = nullptr;
     int32_t *died_at = nullptr;     // the step a cell turned necrotic (-1: not yet)
     int32_t *began = nullptr, *due = nullptr;  // a cell's cycle: the step it began and the step it is over
+    cw_field_s *str = nullptr;      // the stress field of an exposure
+    double *cell_str = nullptr, *d_str_uptake = nullptr;
+    double str_level = 0.0;         // the level the stress field was last solved at
+    std::vector<cw_relax_stats> last_str;
     cw::DebrisState debris;         // with a debris loss
     bool debris_on = false;
     double *level = nullptr;        // per history: the level the bath holds (1, or a still medium's)
@@ -128,6 +132,22 @@ __global__ void k_release_rates(const uint8_t *alive, const int32_t *type, const
 }
 
 // The cells' waste and necrotic-factor inputs (cell_inputs, simulation.rs:2511-2521).
+__global__ void k_inputs_stress(const double *cell_str, int64_t nc, double *inputs) {
+    int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nc) return;
+    inputs[3 * nc + c] = cell_str ? cell_str[c] : 0.0;
+}
+
+// A field held where `src` is held, at `level` (the stress where the oxygen
+// comes in: hold_medium_bath or hold_vessels_at at the exposure's level).
+__global__ void k_hold_like(const uint8_t *src, int64_t n, double level, uint8_t *held, double *c) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint8_t m = src[i];
+    held[i] = m;
+    if (m) c[i] = level;
+}
+
 __global__ void k_inputs_released(const double *cell_wst, const double *cell_nfc, int64_t nc, double *inputs) {
     int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nc) return;
@@ -473,6 +493,16 @@ int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out) {
     if (c.debris_loss != 0.0 && !(c.debris_loss > 0.0 && c.debris_loss <= 1.0))
         return fail(CW_ERR_CONFIG, "debris loss is the share of a dead cell lost per step, above zero and at most one");
     if (c.debris_loss > 0.0 && c.necrotic_type < 0) return fail(CW_ERR_CONFIG, "debris loss needs a necrotic type");
+    if (c.exposure_intensity != 0.0) {
+        if (!(c.exposure_intensity > 0.0 && c.exposure_intensity < 1e300))
+            return fail(CW_ERR_CONFIG, "the exposure's intensity must be zero or more");
+        if (!(c.exposure_uptake > 0.0 && c.exposure_uptake < 1e300))
+            return fail(CW_ERR_CONFIG, "the exposure's uptake must be above zero, or it fills the box");
+        if (c.exposure_start < 0 || c.exposure_on < 0 || c.exposure_off < 0)
+            return fail(CW_ERR_CONFIG, "an exposure's start and schedule are counts of steps");
+        if (c.exposure_on == 0 && c.exposure_off > 0)
+            return fail(CW_ERR_CONFIG, "a periodic exposure that is on for zero steps is never on");
+    }
     if (c.still_medium != 0.0) {
         if (!(c.still_medium > 0.0 && c.still_medium < 1e300))
             return fail(CW_ERR_CONFIG, "the still medium's diffusion is above zero");
@@ -539,8 +569,9 @@ int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out) {
             }
         }
     }
-    // fields
-    if ((rc = cw_field_create(c.nh, s->w.data(), s->h.data(), s->d.data(), c.o2_dcoef, 0.0, 1.0, &s->o2)) != CW_OK) {
+    // fields: the oxygen starts at the source's level, or at zero around a vessel (simulation.rs:786-793)
+    if ((rc = cw_field_create(c.nh, s->w.data(), s->h.data(), s->d.data(), c.o2_dcoef, 0.0, c.o2_hold == 4 ? 0.0 : 1.0,
+                              &s->o2)) != CW_OK) {
         cw_sim_destroy(s);
         return rc;
     }
@@ -570,6 +601,20 @@ int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out) {
         (rc = cw_field_create(c.nh, s->w.data(), s->h.data(), s->d.data(), c.o2_dcoef, 0.0, 0.0, &s->wst)) != CW_OK) {
         cw_sim_destroy(s);
         return rc;
+    }
+    if (c.exposure_intensity > 0.0) {
+        // STRESS_DIFFUSION = OXYGEN_DIFFUSION (simulation.rs:157), from zero
+        if ((rc = cw_field_create(c.nh, s->w.data(), s->h.data(), s->d.data(), c.o2_dcoef, 0.0, 0.0, &s->str)) !=
+            CW_OK) {
+            cw_sim_destroy(s);
+            return rc;
+        }
+        std::vector<double> up(8, 0.0);
+        for (int k = 1; k < c.K; ++k) up[k] = k == c.necrotic_type ? 0.0 : c.exposure_uptake;
+        if ((rc = dalloc(&s->d_str_uptake, 8)) != CW_OK) { cw_sim_destroy(s); return rc; }
+        CW_CUDA(cudaMemcpy(s->d_str_uptake, up.data(), 8 * sizeof(double), cudaMemcpyHostToDevice));
+        s->str->uptake_on = true;
+        CW_CUDA(cudaMemset(s->str->uptake, 0, sizeof(double) * (size_t)s->str->g.total));
     }
     if (c.necrotic_production > 0.0) {
         if (c.necrotic_type < 0) {
@@ -608,7 +653,8 @@ int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out) {
         cw_sim_destroy(s);
         return rc;
     }
-    if ((rc = dalloc(&s->level, c.nh)) || (rc = dalloc(&s->d_inflow, c.nh)) || (rc = dalloc(&s->d_free, c.nh))) {
+    if ((rc = dalloc(&s->level, c.nh)) || (rc = dalloc(&s->d_inflow, c.nh)) || (rc = dalloc(&s->d_free, c.nh)) ||
+        (rc = dalloc(&s->cell_str, nc))) {
         cw_sim_destroy(s);
         return rc;
     }
@@ -672,6 +718,7 @@ int cw_sim_destroy(cw_sim s) {
     cw_field_destroy(s->nfc);
     dfree(s->cell_wst); dfree(s->cell_nfc); dfree(s->wst_rate); dfree(s->nfc_rate); dfree(s->died_at); dfree(s->began); dfree(s->due);
     s->debris.release(); dfree(s->level); dfree(s->d_inflow); dfree(s->d_free);
+    cw_field_destroy(s->str); dfree(s->cell_str); dfree(s->d_str_uptake);
     dfree(s->d_step); dfree(s->bath); dfree(s->d_uptake);
     dfree(s->d_sink); dfree(s->cell_o2); dfree(s->cell_sig); dfree(s->sum); dfree(s->secretion); dfree(s->count);
     dfree(s->state); dfree(s->inputs); dfree(s->alive); dfree(s->target32);
@@ -790,6 +837,48 @@ static int division_step(cw_sim_s *s) {
     k_cycle_births<<<(unsigned)blocks(nc), T, 0, stream()>>>(l->d_cell_off, (int)c.nh, nc, l->div.daughter, l->d_keys,
                                                              s->d_step, c.cycle_median, c.cycle_spread, s->began,
                                                              s->due, l->div.count);
+    CW_LAUNCHED();
+    return CW_OK;
+}
+
+// Exposure::level_at (types.rs:319-332): the intensity while on, else 0.
+static double exposure_level(const cw_sim_config &c, uint64_t mcs) {
+    if (c.exposure_intensity <= 0.0 || mcs < (uint64_t)c.exposure_start) return 0.0;
+    if (c.exposure_on <= 0) return c.exposure_intensity;  // continuous
+    const uint64_t period = std::max<uint64_t>((uint64_t)c.exposure_on + (uint64_t)c.exposure_off, 1);
+    return (mcs - (uint64_t)c.exposure_start) % period < (uint64_t)c.exposure_on ? c.exposure_intensity : 0.0;
+}
+
+// settle_stress (simulation.rs:2015-2055) for the step `mcs`: zero while the
+// exposure is off; otherwise the living (and, around a vessel, the medium)
+// take it up, it is held at the level where the oxygen is held, and solved,
+// from scratch and tightly when the level changed.
+static int settle_stress(cw_sim_s *s, const cw_relax_opts &o, uint64_t mcs) {
+    const cw_sim_config &c = s->cfg;
+    cw_field_s *f = s->str;
+    const double level = exposure_level(c, mcs);
+    int rc;
+    if (level == 0.0) {
+        CW_CUDA(cudaMemsetAsync(f->c, 0, sizeof(double) * (size_t)f->g.total, stream()));
+        s->str_level = 0.0;
+    } else {
+        if ((rc = couple_uptake_device(f, s->lat, s->d_str_uptake, 8, f->uptake, s->sites)) != CW_OK) return rc;
+        if (c.o2_hold == 4 &&
+            (rc = couple_background_device(f, s->lat, c.exposure_uptake, f->uptake)) != CW_OK)
+            return rc;
+        k_hold_like<<<(unsigned)blocks(f->g.total), T, 0, stream()>>>(s->o2->held, f->g.total, level, f->held, f->c);
+        CW_LAUNCHED();
+        f->held_dirty = true;
+        cw_relax_opts os = o;
+        os.tolerance = 0.01 * c.exposure_uptake;  // OXYGEN_TOLERANCE x the exposure's uptake
+        if (level != s->str_level) { os.tolerance = 1e-8; os.max_sweeps = 2000000; }
+        s->last_str.resize(c.nh);
+        const double *om = c.omega > 0.0 ? nullptr : s->omega[0].data();
+        if ((rc = field_relax(f, &os, om, s->last_str.data())) != CW_OK) return rc;
+        s->str_level = level;
+    }
+    if ((rc = couple_means_device(f, s->lat, s->sum, s->count, s->cell_str, s->sites)) != CW_OK) return rc;
+    k_inputs_stress<<<(unsigned)blocks(s->nc), T, 0, stream()>>>(s->cell_str, s->nc, s->inputs);
     CW_LAUNCHED();
     return CW_OK;
 }
@@ -976,7 +1065,7 @@ int cw_sim_step(cw_sim s, uint32_t nsteps) {
         const bool graph_ok = c.use_graphs && c.precision == CW_FP32_DC && c.relax_every <= 1 && !s->tune.active &&
                               s->depth_tuned && s->steps >= 2 && !s->last.empty() &&
                               (!s->sig || !s->last_sig.empty()) && !s->wst && !s->nfc && c.o2_hold != 3 &&
-                              !s->debris_on;
+                              !s->debris_on && !s->str;
         if (graph_ok) {
             if (!s->graphs && (rc = build_graphs(s, o)) != CW_OK) return rc;
             if ((rc = step_graph(s, o)) != CW_OK) return rc;
@@ -1039,6 +1128,13 @@ int cw_sim_step(cw_sim s, uint32_t nsteps) {
             if (tuning) tune_book(s, 1, st2);
             if ((rc = couple_means_device(s->sig, s->lat, s->sum, s->count, s->cell_sig, s->sites)) != CW_OK)
                 return rc;
+        }
+        // 2a. an exposure's stress (settle_stress, simulation.rs:1158-1162)
+        if (s->str && solve) {
+            if ((rc = settle_stress(s, o, s->steps)) != CW_OK) return rc;
+        } else if (s->str) {
+            k_inputs_stress<<<(unsigned)blocks(nc), T, 0, stream()>>>(s->cell_str, nc, s->inputs);
+            CW_LAUNCHED();
         }
         // 2b. the released fields: the waste from the living, the necrotic
         // factor from the dead, held at zero on the bath (settle_waste,
@@ -1134,7 +1230,8 @@ int cw_sim_lattice(cw_sim s, cw_lattice *lat) {
 }
 
 int cw_sim_field(cw_sim s, int32_t which, cw_field *f) {
-    *f = which == 0 ? s->o2 : which == 1 ? s->sig : which == 2 ? s->wst : which == 3 ? s->nfc : nullptr;
+    *f = which == 0 ? s->o2 : which == 1 ? s->sig : which == 2 ? s->wst : which == 3 ? s->nfc
+       : which == 4 ? s->str : nullptr;
     if (!*f) return fail(CW_ERR_NOT_FOUND, "no such field");
     return CW_OK;
 }
@@ -1194,6 +1291,7 @@ int cw_sim_measure(cw_sim s, cw_measurements *out) {
         const unsigned long long *v = &h[8 * (size_t)k];
         cw_measurements &m = out[k];
         m.mcs = s->steps > 0 ? s->steps - 1 : 0;
+        m.exposure = exposure_level(c, m.mcs);
         m.cycling = v[0];
         m.quiescent = v[1];
         m.necrotic = v[2];

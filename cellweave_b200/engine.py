@@ -626,7 +626,8 @@ class Simulation:
                  necrotic_type=-1, use_graphs=True, divide=True, max_cells=2000, spare_cells=0,
                  waste_production=0.0, necrotic_production=0.0, necrotic_release_for=-1, subsweeps=1,
                  o2_uptake=0.0, divide_every=1, vessel_radius=0, stop_rule=STOP_RESIDUAL, first_tolerance=0.0,
-                 cycle_median=0.0, cycle_spread=0.0, debris_loss=0.0, still_medium=0.0):
+                 cycle_median=0.0, cycle_spread=0.0, debris_loss=0.0, still_medium=0.0, exposure_intensity=0.0,
+                 exposure_uptake=0.0, exposure_start=0, exposure_on=0, exposure_off=0):
         self.dims, w, h, z = _dims(dims)
         self._keep = [w, h, z]
         nc = np.array(ncells, np.uint32)
@@ -646,7 +647,8 @@ class Simulation:
                              int(spare_cells), float(waste_production), float(necrotic_production),
                              int(necrotic_release_for), int(subsweeps), float(o2_uptake), int(divide_every),
                              int(vessel_radius), int(stop_rule), float(first_tolerance), float(cycle_median),
-                             float(cycle_spread), float(debris_loss), float(still_medium))
+                             float(cycle_spread), float(debris_loss), float(still_medium), float(exposure_intensity),
+                             float(exposure_uptake), int(exposure_start), int(exposure_on), int(exposure_off))
         handle = C.c_void_p()
         call("cw_sim_create", C.byref(cfg), network.handle, C.byref(handle))
         self._h = handle

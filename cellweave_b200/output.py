@@ -3,7 +3,7 @@
 
 One row per step, the columns of MEASUREMENT_COLUMNS in that order, counts as
 integers and the exposure and the three radii to four decimals, so that two
-runs of one seed write the same bytes.  The device step has no exposure,
+runs of one seed write the same bytes.  The device step has no
 differentiation, apoptosis, lesion, angiogenesis or immune cells: those
 columns are written as the reference writes them without those features (0),
 the clones column counts the founder's clone while anything lives (no

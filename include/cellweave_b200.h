@@ -432,6 +432,14 @@ typedef struct {
     double still_medium;         /* > 0: the bath is still medium of this diffusion, and the level it holds falls
                                     with what the tissue takes up (settle_bath_level, simulation.rs:2104-2125);
                                     o2_hold 3 in volumes only */
+    double exposure_intensity;   /* > 0: an exposure (Exposure, types.rs:92-104, 319-332; settle_stress,
+                                    simulation.rs:2006-2056): a stress field, diffusing as oxygen does, held at
+                                    this level where the oxygen is held from step exposure_start on (with
+                                    exposure_on > 0, for exposure_on steps of every exposure_on + exposure_off),
+                                    zero while off, taken up at exposure_uptake by every living pixel (and the
+                                    medium around a vessel); a cell's mean is its network's stress input */
+    double exposure_uptake;
+    int32_t exposure_start, exposure_on, exposure_off;
 } cw_sim_config;
 int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out);
 int cw_sim_destroy(cw_sim sim);
@@ -447,7 +455,8 @@ int cw_sim_tuning(cw_sim sim, double *omega_o2, double *omega_signal, int32_t *d
 /* Steps replayed from CUDA graphs, solves whose graph budget of outer
  * iterations fell short (finished host-side), and the budgets (2 entries). */
 int cw_sim_graph_info(cw_sim sim, uint64_t *graph_steps, uint64_t *budget_misses, int32_t *budgets);
-/* Handles the driver owns, for inspection with the calls above. */
+/* Handles the driver owns, for inspection with the calls above; fields 0 oxygen, 1 signal, 2 waste,
+   3 necrotic factor, 4 stress (CW_ERR_NOT_FOUND for one the simulation does not have). */
 int cw_sim_lattice(cw_sim sim, cw_lattice *lat);
 int cw_sim_field(cw_sim sim, int32_t which, cw_field *f);
 /* Per history: living cells, mean oxygen over cells, sweeps of the last
@@ -472,6 +481,7 @@ typedef struct {
     uint64_t born, gone;
     uint64_t vessel;
     double tissue_radius, necrotic_radius, viable_depth;
+    double exposure;     /* the exposure's level at the step last taken (0 without one or while off) */
 } cw_measurements;
 int cw_sim_measure(cw_sim sim, cw_measurements *out);
 /* Network state of history `hist`, [ncells][S]. */

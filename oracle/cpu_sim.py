@@ -148,7 +148,7 @@ class CpuHistory:
             self.lat.enable_surface(np.full(self.ncap, cfg["surface_target"], np.int32),
                                     np.full(self.ncap, cfg.get("lambda_surface", 0.0)))
         n = w * h * d
-        self.o2 = O.Field(w, h, d, cfg["o2_dcoef"], 0.0, 1.0)
+        self.o2 = O.Field(w, h, d, cfg["o2_dcoef"], 0.0, 0.0 if cfg.get("o2_hold", 0) == 4 else 1.0)
         z, y, x = np.mgrid[0:d, 0:h, 0:w]
         hold = cfg.get("o2_hold", 0)
         held = (y == 0) if hold == 0 else (x == w // 2) if hold == 1 else (
@@ -164,6 +164,10 @@ class CpuHistory:
         self.wst = O.Field(w, h, d, cfg["o2_dcoef"], 0.0, 0.0) if cfg.get("waste_production", 0.0) > 0 else None
         self.nfc = O.Field(w, h, d, cfg["o2_dcoef"], 0.0, 0.0) if cfg.get("necrotic_production", 0.0) > 0 else None
         self.cell_wst = self.cell_nfc = None
+        # an exposure's stress (simulation.rs:802-840): diffusing as oxygen does, from zero
+        self.str = O.Field(w, h, d, cfg["o2_dcoef"], 0.0, 0.0) if cfg.get("exposure_intensity", 0.0) > 0 else None
+        self.str_level = 0.0
+        self.cell_str = None
         spec = cfg.get("network_spec") or tomllib.loads(cfg.get("network_toml") or
                                                           synthetic.network_toml(cfg["S"], cfg["S"]))
         # the network's reference volume: the seeded cell's (simulation.rs:726-733) or the target
@@ -241,6 +245,8 @@ class CpuHistory:
         nec = c.get("necrotic_type", -1)
         alive = (self.lat.volume > 0) & (t != nec)
         alive[0] = False
+        if self.str is not None:
+            self.cell_str = self._settle_stress()
         if self.sig is not None:
             sec = np.where(alive & (o2m < c["hypoxic_level"]), c["signal_secretion"], 0.0)
             self.sig.production = O.apply_production(g, sec)
@@ -274,6 +280,8 @@ class CpuHistory:
             ins[:, 1] = 0.2
             # crowding (simulation.rs:2523-2527): 1 - volume / reference volume, clamped
             ins[:, 2] = np.clip(1.0 - self.lat.volume[idx] / float(max(self.refvol, 1)), 0.0, 1.0)
+            if self.cell_str is not None:
+                ins[:, 3] = self.cell_str[idx]
             if self.cell_wst is not None:
                 ins[:, 4] = self.cell_wst[idx]
             if self.cell_nfc is not None:
@@ -310,6 +318,43 @@ class CpuHistory:
             self._divide_ready_cells()
         self.steps += 1
         return rc
+
+    def _level_at(self, mcs):
+        """Exposure::level_at (types.rs:319-332)."""
+        c = self.cfg
+        if mcs < c.get("exposure_start", 0):
+            return 0.0
+        on, off = c.get("exposure_on", 0), c.get("exposure_off", 0)
+        if on > 0 and (mcs - c.get("exposure_start", 0)) % max(on + off, 1) >= on:
+            return 0.0
+        return c["exposure_intensity"]
+
+    def _settle_stress(self):
+        """settle_stress (simulation.rs:2015-2055): zero while off; else taken up
+        by the living (and the medium around a vessel), held at the level where
+        the oxygen is held, solved from scratch and tightly when the level
+        changed; the per-cell means."""
+        c = self.cfg
+        f = self.str
+        level = self._level_at(self.steps)
+        if level == 0.0:
+            f.values[:] = 0.0
+            self.str_level = 0.0
+        else:
+            g, t = self.lat.grid, self.lat.type
+            up = np.zeros(f.values.size)
+            up[(g > 0) & (t[np.clip(g, 0, None)] != c.get("necrotic_type", -1))] = c["exposure_uptake"]
+            if c.get("o2_hold", 0) == 4:
+                up[self.lat.grid == 0] = c["exposure_uptake"]
+            f.uptake = up
+            f.held[:] = self.o2.held
+            f.values[f.held == 1] = level
+            tol, most = 0.01 * c["exposure_uptake"], 200_000
+            if level != self.str_level:
+                tol, most = 1e-8, 2_000_000
+            f.relax(tol, most, omega=c.get("omega") or 0.0, stop=c.get("stop_rule", 1), threads=1)
+            self.str_level = level
+        return O.mean_per_cell(self.lat.grid, f.values, self.ncap)
 
     def _settle_bath_level(self):
         """settle_bath_level (simulation.rs:2114-2125): 1 - inflow / (4 pi D r), r

@@ -118,3 +118,18 @@ def test_debris_loss_and_a_still_medium_are_carried(tmp_path):
     assert kw["debris_loss"] == 0.024 and kw["still_medium"] == 0.606
     # a ball of radius 3 in a volume (simulation.rs:74)
     assert kw["seed_side"] == 3 and refvol == 123
+
+
+def test_an_exposure_is_read_with_its_schedule(tmp_path):
+    per = "\n[exposure]\nintensity = 0.8\nuptake = 0.001\nstart = 100\nschedule = { kind = \"periodic\", on = 5, off = 7 }\n"
+    kw, _ = C.simulation_kwargs(C.load_sim_config(write(tmp_path, BASE + per)))
+    assert (kw["exposure_intensity"], kw["exposure_uptake"], kw["exposure_start"]) == (0.8, 0.001, 100)
+    assert (kw["exposure_on"], kw["exposure_off"]) == (5, 7)
+    cont = per.replace('{ kind = "periodic", on = 5, off = 7 }', '{ kind = "continuous" }')
+    kw, _ = C.simulation_kwargs(C.load_sim_config(write(tmp_path, BASE + cont)))
+    assert (kw["exposure_on"], kw["exposure_off"]) == (0, 0)
+    never = per.replace("on = 5", "on = 0")
+    with pytest.raises(cw.ConfigError, match="never on"):
+        C.simulation_kwargs(C.load_sim_config(write(tmp_path, BASE + never)))
+    with pytest.raises(cw.ConfigError, match="uptake"):
+        C.simulation_kwargs(C.load_sim_config(write(tmp_path, BASE + per.replace("uptake = 0.001\n", ""))))

@@ -25,8 +25,11 @@ pytestmark = pytest.mark.gpu
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 
-def ras_erk_toml(tmp_path):
+def ras_erk_toml(tmp_path, stressed=False):
     spec = json.load(open(os.path.join(HERE, "golden", "golden.json")))["networks"]["ras-erk"]
+    if stressed:
+        # survival damaged by stress above a threshold (DamagedAbove, crates/core/src/network.rs:127-135)
+        spec["nodes"][4]["terms"].append({"kind": "damaged_above", "rate": 0.2, "source": "stress", "threshold": 0.3})
     lines = []
     for node in spec["nodes"]:
         lines += ["[[nodes]]", f'name = "{node["name"]}"', f'initial = {node["initial"]}', "terms = ["]
@@ -42,8 +45,8 @@ def ras_erk_toml(tmp_path):
     return spec
 
 
-def scenario(tmp_path, source, uptake=0.001):
-    spec = ras_erk_toml(tmp_path)
+def scenario(tmp_path, source, uptake=0.001, stressed=False):
+    spec = ras_erk_toml(tmp_path, stressed)
     text = ("width = 120\nheight = 120\nmcs = 140\ntemperature = 10.0\nsnapshot_interval = 20\n"
             f"output_dir = \"out\"\noxygen_uptake = {uptake}\nnetwork = \"ras-erk.toml\"\n" + source)
     p = tmp_path / "run.toml"
@@ -160,3 +163,39 @@ def test_a_still_spheroid_in_a_volume_loses_its_debris_inside_the_oracle_band(tm
     assert np.mean([m["necrotic"] for m in sim.measure()]) > 2  # a core died and is breaking down
     for k in range(SEEDS):
         assert sim.records_match_grid(k)
+
+
+def test_an_exposure_stresses_the_tissue_inside_the_oracle_band(tmp_path):
+    """settle_stress (simulation.rs:2015-2055): a periodic exposure from step
+    70, on 20 steps in 40, held where the oxygen comes in and taken up by the
+    living, read by a network whose survival is damaged above a stress of
+    0.3 (the tissue's rim dies each time it is on); the population inside the
+    oracle's band while on and off, the measurements' exposure column the
+    schedule's level."""
+    src = ("\n[exposure]\nintensity = 1.0\nuptake = 0.004\nstart = 70\n"
+           "schedule = { kind = \"periodic\", on = 20, off = 20 }\n")
+    path, spec = scenario(tmp_path, src, 0.0005, stressed=True)
+    cfg = C.load_sim_config(path)
+    seeds = [11_000 + k for k in range(SEEDS)]
+    sim, _ = C.simulation_from_config(cfg, histories=SEEDS, seeds=seeds)
+    kw, _ = C.simulation_kwargs(cfg, SEEDS, seeds)
+    ocfg = dict(kw, network_spec=spec, lambda_volume=float(spec["mechanics"]["lambda_volume"]), hypoxic_level=0.1)
+    ora = [CpuHistory(ocfg, k) for k in range(SEEDS)]
+    keys = ("cycling", "quiescent", "necrotic", "tissue_radius")
+    for step in range(1, 141):
+        sim.step(1)
+        for h in ora:
+            h.step()
+        dm = sim.measure()
+        mcs = step - 1
+        level = 1.0 if mcs >= 70 and (mcs - 70) % 40 < 20 else 0.0
+        assert all(m["exposure"] == level for m in dm), (mcs, dm[0]["exposure"])
+        if step not in (80, 100, 120, 140):
+            continue
+        om = [h.measure() for h in ora]
+        for q in keys:
+            dv = np.array([float(m[q]) for m in dm])
+            rv = np.array([float(m[q]) for m in om])
+            assert within_band(dv, rv), (step, q, dv.mean(), rv.mean(), rv.std())
+    stress = sim.field_values(4, 0)
+    assert stress.max() <= 1.0 + 1e-9
