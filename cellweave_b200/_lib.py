@@ -128,6 +128,8 @@ SIGNATURES = {
     "cw_lattice_set_temperature": (C.c_int, [P, D]),
     "cw_lattice_upload": (C.c_int, [P, U32, P]),
     "cw_lattice_download": (C.c_int, [P, U32, P]),
+    "cw_lattice_upload_all": (C.c_int, [P, P]),
+    "cw_lattice_download_all": (C.c_int, [P, P]),
     "cw_cells_set": (C.c_int, [P, U32, U32, P, P, P, P]),
     "cw_cells_get": (C.c_int, [P, U32, U32, P, P, P, P]),
     "cw_cells_set_surface": (C.c_int, [P, U32, U32, P, P]),

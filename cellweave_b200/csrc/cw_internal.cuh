@@ -232,6 +232,8 @@ struct cw_lattice_s {
     int32_t *d_used = nullptr;
     cw::DivScratch div;
     cw::Plan site_plan;                   // every pixel of every history, T per block
+    int32_t *stage = nullptr;             // uploads land here and are checked before they become the grid
+    unsigned long long *d_bad = nullptr;  // the first pixel of an upload past its history's capacity
     int32_t *bath_label = nullptr;        // the bath's union-find labels, one per site (bath.cu)
     uint8_t *bath_mark = nullptr;         // roots that reach the outer layer (bath.cu)
     int build_plans();

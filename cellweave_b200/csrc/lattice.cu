@@ -552,6 +552,19 @@ __global__ void __launch_bounds__(T) k_cpm_pass(LatView L, Tables tabs, const in
     }
 }
 
+// The first staged pixel of histories h0..h1 (n sites from `a`) whose id is
+// below -1 or at least its history's cell capacity, as an offset from `a`.
+__global__ void k_check_ids(const int32_t *stage, int64_t a, int64_t n, const int64_t *off, const int64_t *cell_off,
+                            int h0, int h1, unsigned long long *first_bad) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int64_t i = a + k;
+    int lo = h0, hi = h1;
+    while (lo < hi) { const int mid = (lo + hi + 1) >> 1; if (off[mid] <= i) lo = mid; else hi = mid - 1; }
+    const int32_t v = stage[i];
+    if (v < -1 || (int64_t)v >= cell_off[lo + 1] - cell_off[lo]) atomicMin(first_bad, (unsigned long long)k);
+}
+
 __global__ void k_delta_h(LatView L, Tables tabs, int h, int64_t n, const int64_t *site, const int32_t *dstv,
                           double *out) {
     __shared__ double sJ[64];
@@ -894,7 +907,7 @@ int cw_lattice_destroy(cw_lattice l) {
     dfree(l->grid); dfree(l->type); dfree(l->volume); dfree(l->target); dfree(l->lambda); dfree(l->vsnap);
     dfree(l->surface); dfree(l->ssnap); dfree(l->tsurf); dfree(l->lsurf); dfree(l->d_cell_off); dfree(l->d_keys);
     dfree(l->d_flag); dfree(l->claim); dfree(l->plist); dfree(l->pctl); dfree(l->d_used);
-    dfree(l->bath_label); dfree(l->bath_mark);
+    dfree(l->bath_label); dfree(l->bath_mark); dfree(l->stage); dfree(l->d_bad);
     l->div.release();
     l->site_plan.release();
     for (auto &p : l->plans) p.release();
@@ -954,22 +967,55 @@ int cw_lattice_set_temperature(cw_lattice l, double temperature) {
     return CW_OK;
 }
 
+// Histories h0..h1's sites, staged at `off[h0]`, copied into the grid when
+// every id lies in [-1, capacity): the host data lands in the staging buffer,
+// a kernel records the first pixel that does not, and only a clean upload
+// becomes the grid.
+static int upload_range(cw_lattice l, uint32_t h0, uint32_t h1, const int32_t *grid) {
+    int rc;
+    if (!l->stage && ((rc = dalloc(&l->stage, (size_t)l->g.total)) || (rc = dalloc(&l->d_bad, 1)))) return rc;
+    const int64_t a = l->g.off[h0], n = l->g.off[h1 + 1] - a;
+    const unsigned long long none = ~0ull;
+    CW_CUDA(cudaMemcpyAsync(l->stage + a, grid, sizeof(int32_t) * n, cudaMemcpyHostToDevice, stream()));
+    CW_CUDA(cudaMemcpyAsync(l->d_bad, &none, sizeof none, cudaMemcpyHostToDevice, stream()));
+    k_check_ids<<<(unsigned)((n + T - 1) / T), T, 0, stream()>>>(l->stage, a, n, l->g.d_off, l->d_cell_off, (int)h0,
+                                                                 (int)h1, l->d_bad);
+    CW_LAUNCHED();
+    unsigned long long bad = none;
+    CW_CUDA(cudaMemcpyAsync(&bad, l->d_bad, sizeof bad, cudaMemcpyDeviceToHost, stream()));
+    CW_CUDA(cudaStreamSynchronize(stream()));
+    if (bad != none) {
+        uint32_t h = h0;
+        while (h < h1 && l->g.off[h + 1] <= a + (int64_t)bad) ++h;
+        const int64_t i = a + (int64_t)bad - l->g.off[h];
+        return fail(CW_ERR_CONFIG, "pixel " + std::to_string(i) + " holds id " + std::to_string(grid[bad]) +
+                                       ", past the history's cell capacity " +
+                                       std::to_string(l->cell_off[h + 1] - l->cell_off[h]));
+    }
+    CW_CUDA(cudaMemcpyAsync(l->grid + a, l->stage + a, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, stream()));
+    return CW_OK;
+}
+
 int cw_lattice_upload(cw_lattice l, uint32_t hist, const int32_t *grid) {
     if (hist >= l->g.nh) return fail(CW_ERR_NOT_FOUND, "no history " + std::to_string(hist));
-    int64_t n = l->g.sites(hist), cap = l->cell_off[hist + 1] - l->cell_off[hist];
-    for (int64_t i = 0; i < n; ++i)
-        if (grid[i] < -1 || grid[i] >= cap)
-            return fail(CW_ERR_CONFIG, "pixel " + std::to_string(i) + " holds id " + std::to_string(grid[i]) +
-                                           ", past the history's cell capacity " + std::to_string(cap));
-    CW_CUDA(cudaMemcpyAsync(l->grid + l->g.off[hist], grid, sizeof(int32_t) * n, cudaMemcpyHostToDevice, stream()));
-    CW_CUDA(cudaStreamSynchronize(stream()));
-    return CW_OK;
+    return upload_range(l, hist, hist, grid);
+}
+
+int cw_lattice_upload_all(cw_lattice l, const int32_t *grids) {
+    if (l->g.nh == 0) return CW_OK;
+    return upload_range(l, 0, l->g.nh - 1, grids);
 }
 
 int cw_lattice_download(cw_lattice l, uint32_t hist, int32_t *grid) {
     if (hist >= l->g.nh) return fail(CW_ERR_NOT_FOUND, "no history " + std::to_string(hist));
     CW_CUDA(cudaMemcpyAsync(grid, l->grid + l->g.off[hist], sizeof(int32_t) * l->g.sites(hist), cudaMemcpyDeviceToHost,
                             stream()));
+    CW_CUDA(cudaStreamSynchronize(stream()));
+    return CW_OK;
+}
+
+int cw_lattice_download_all(cw_lattice l, int32_t *grids) {
+    CW_CUDA(cudaMemcpyAsync(grids, l->grid, sizeof(int32_t) * l->g.total, cudaMemcpyDeviceToHost, stream()));
     CW_CUDA(cudaStreamSynchronize(stream()));
     return CW_OK;
 }

@@ -122,9 +122,15 @@ int cw_lattice_set_copy_nbhd(cw_lattice lat, int32_t nbhd);
  * probability 1/n (its own Philox draw), Binomial(n, 1/n) attempts a step,
  * which nears Poisson(1) as n grows; n times the passes. */
 int cw_lattice_set_subsweeps(cw_lattice lat, int32_t subsweeps);
-/* The grid of history `hist`, w*h*d int32 in the reference's flat order. */
+/* The grid of history `hist`, w*h*d int32 in the reference's flat order.  An upload holding an id
+ * past the history's cell capacity (or below -1, the obstacle) is refused with CW_ERR_CONFIG naming
+ * the first such pixel, and the lattice keeps its grid; the check runs on the device. */
 int cw_lattice_upload(cw_lattice lat, uint32_t hist, const int32_t *grid);
 int cw_lattice_download(cw_lattice lat, uint32_t hist, int32_t *grid);
+/* Every history's grid at once, one after another in history order (the sum of w*h*d int32): one
+ * copy, one check and one synchronisation for the whole batch (a campaign's grids in one buffer). */
+int cw_lattice_upload_all(cw_lattice lat, const int32_t *grids);
+int cw_lattice_download_all(cw_lattice lat, int32_t *grids);
 /* Cell records (CellRecord, cpm.rs:171-181) for ids [0, n) of history `hist`:
  * type, volume, target volume, lambda_volume (set_volume_target, set_kind:
  * cpm.rs:997-1041). */

@@ -277,3 +277,38 @@ def test_the_device_bath_is_the_reference_flood():
         np.testing.assert_array_equal(lat.bath(hist), oracle_bath(gr), err_msg=f"lattice {k}")
     # the shut-in medium inside the ring is not bath; the rest of the medium is
     assert flat.bath(1)[0, 15, 20] == 0 and flat.bath(1)[0, 1, 1] == 1
+
+
+def test_an_upload_past_the_capacity_is_refused_and_the_grid_kept():
+    """The upload check runs on the device: a clean upload becomes the grid,
+    one holding an id past its history's capacity (or below the obstacle's
+    -1) is refused naming its first such pixel, and the grid stays as it was;
+    the all-history calls move every history in one buffer."""
+    from cellweave_b200 import _lib
+    lat = cw.CpmLattice([(16, 8, 1), (8, 16, 1)], 10.0, [5, 9], order=1, J=np.zeros((2, 2)))
+    rng = np.random.default_rng(4)
+    a = rng.integers(-1, 5, 16 * 8).astype(np.int32)
+    b = rng.integers(-1, 9, 8 * 8 * 2).astype(np.int32)
+    lat.upload(a, 0)
+    lat.upload(b, 1)
+    np.testing.assert_array_equal(lat.grid(0).reshape(-1), a)
+    bad = b.copy()
+    bad[37], bad[90] = 9, 12
+    with pytest.raises(cw.ConfigError, match="pixel 37 holds id 9, past the history's cell capacity 9"):
+        lat.upload(bad, 1)
+    np.testing.assert_array_equal(lat.grid(1).reshape(-1), b)
+    low = a.copy()
+    low[3] = -2
+    with pytest.raises(cw.ConfigError, match="pixel 3 holds id -2"):
+        lat.upload(low, 0)
+    both = np.empty(16 * 8 + 8 * 8 * 2, np.int32)
+    _lib.check(_lib.lib().cw_lattice_download_all(lat.handle, _lib.ptr(both)))
+    np.testing.assert_array_equal(both, np.concatenate([a, b]))
+    swapped = np.concatenate([np.clip(a[::-1], -1, 4), b[::-1]]).astype(np.int32)
+    _lib.check(_lib.lib().cw_lattice_upload_all(lat.handle, _lib.ptr(swapped)))
+    np.testing.assert_array_equal(lat.grid(1).reshape(-1), b[::-1])
+    wrong = swapped.copy()
+    wrong[16 * 8 + 5] = 9  # history 1's pixel 5
+    with pytest.raises(cw.ConfigError, match="pixel 5 holds id 9"):
+        _lib.check(_lib.lib().cw_lattice_upload_all(lat.handle, _lib.ptr(wrong)))
+    np.testing.assert_array_equal(lat.grid(0).reshape(-1), swapped[:16 * 8])
