@@ -250,3 +250,27 @@ def run(path, out_dir=None, histories=1, seeds=None, subsweeps=4, steps=None):
     for lg in logs:
         lg.close()
     return dict(steps=taken, reached_edge=done, directories=dirs)
+
+
+def main(argv=None):
+    """``python -m cellweave_b200 run.toml [--steps N] [--histories H]
+    [--out DIR]``: the run loop on the device, then one JSON line: steps taken,
+    wall seconds and milliseconds a step (measurements, snapshots and the
+    edge test included)."""
+    import argparse
+    import json
+    import time
+    p = argparse.ArgumentParser(prog="python -m cellweave_b200")
+    p.add_argument("config")
+    p.add_argument("--steps", type=int, default=None)
+    p.add_argument("--histories", type=int, default=1)
+    p.add_argument("--subsweeps", type=int, default=4)
+    p.add_argument("--out", default=None)
+    a = p.parse_args(argv)
+    t0 = time.perf_counter()
+    out = run(a.config, a.out, histories=a.histories, subsweeps=a.subsweeps, steps=a.steps)
+    wall = time.perf_counter() - t0
+    print(json.dumps(dict(config=os.path.abspath(a.config), histories=a.histories, steps=out["steps"],
+                          wall_s=round(wall, 3), ms_per_step=round(1000.0 * wall / max(out["steps"], 1), 3),
+                          reached_edge=out["reached_edge"], directories=out["directories"])))
+

@@ -133,3 +133,9 @@ def test_an_exposure_is_read_with_its_schedule(tmp_path):
         C.simulation_kwargs(C.load_sim_config(write(tmp_path, BASE + never)))
     with pytest.raises(cw.ConfigError, match="uptake"):
         C.simulation_kwargs(C.load_sim_config(write(tmp_path, BASE + per.replace("uptake = 0.001\n", ""))))
+
+
+def test_the_runner_refuses_a_configuration_it_cannot_run(tmp_path, capsys):
+    path = write(tmp_path, BASE + "\n[lesion]\nat = 3\nradius = 2\n")
+    with pytest.raises(cw.ConfigError, match="lesion"):
+        C.main([path, "--steps", "2"])
