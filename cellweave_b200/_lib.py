@@ -191,6 +191,7 @@ SIGNATURES = {
     "cw_sim_stats": (C.c_int, [P, P]),
     "cw_sim_network_state": (C.c_int, [P, U32, U32, P]),
     "cw_sim_cycle": (C.c_int, [P, U32, U32, P, P]),
+    "cw_sim_touches_edge": (C.c_int, [P, P]),
     "cw_fit_create": (C.c_int, [P, P, P, P]),
     "cw_fit_destroy": (C.c_int, [P]),
     "cw_fit_nparams": (C.c_int, [P, P]),

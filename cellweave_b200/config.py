@@ -227,7 +227,6 @@ def run(path, out_dir=None, histories=1, seeds=None, subsweeps=4, steps=None):
     out_dir = out_dir or os.path.join(os.path.dirname(cfg["path"]), cfg["output_dir"])
     dirs = [out_dir] if histories == 1 else [os.path.join(out_dir, f"history-{k}") for k in range(histories)]
     logs = [MeasurementLog(d) for d in dirs]
-    vessel = cfg["oxygen_source"].get("kind") == "vessel"
     done = [False] * histories
     n = int(cfg["mcs"] if steps is None else steps)
     taken = 0
@@ -235,12 +234,13 @@ def run(path, out_dir=None, histories=1, seeds=None, subsweeps=4, steps=None):
         sim.step(1)
         taken += 1
         ms = sim.measure()
+        edge = sim.touches_edge()
         for k in range(histories):
             if done[k]:
                 continue
             logs[k].record(ms[k])
             mcs = int(ms[k]["mcs"])
-            if touches_the_edge(sim.grid(k), vessel):
+            if edge[k]:
                 done[k] = True
                 write_snapshot(dirs[k], snapshot_of(sim, k, mcs))
             elif mcs % int(cfg["snapshot_interval"]) == 0:

@@ -186,6 +186,23 @@ __global__ void k_bath_level(int nh, const double *inflow, const unsigned long l
 
 __global__ void k_step_advance(uint32_t *step) { *step += 1u; }
 
+// A cell on the box's sides (and faces, with `faces`) of each history.
+__global__ void k_touches_edge(const int32_t *grid, const int4 *dims, const int64_t *off, int nh, int faces,
+                               int32_t *out) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= off[nh] || grid[i] <= 0) return;
+    int lo = 0, hi = nh - 1;
+    while (lo < hi) { const int mid = (lo + hi + 1) >> 1; if (off[mid] <= i) lo = mid; else hi = mid - 1; }
+    const int4 dm = dims[lo];
+    const int64_t local = i - off[lo], slice = (int64_t)dm.x * dm.y;
+    const int z = (int)(local / slice);
+    const int64_t r = local - (int64_t)z * slice;
+    const int y = (int)(r / dm.x), x = (int)(r - (int64_t)y * dm.x);
+    const bool side = x == 0 || x == dm.x - 1 || y == 0 || y == dm.y - 1;
+    const bool face = faces && dm.z > 1 && (z == 0 || z == dm.z - 1);
+    if (side || face) out[lo] = 1;
+}
+
 __global__ void k_secretion(const uint8_t *alive, const double *cell_o2, int64_t nc, double level, double rate,
                             double *secretion) {
     int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1253,6 +1270,23 @@ int cw_sim_stats(cw_sim s, double *out) {
         out[4 * k + 2] = (double)s->last[k].sweeps;
         out[4 * k + 3] = s->last[k].residual;
     }
+    return CW_OK;
+}
+
+int cw_sim_touches_edge(cw_sim s, int32_t *out) {
+    const cw_sim_config &c = s->cfg;
+    int32_t *d_out = nullptr;
+    int rc = dalloc(&d_out, c.nh);
+    if (rc != CW_OK) return rc;
+    CW_CUDA(cudaMemsetAsync(d_out, 0, sizeof(int32_t) * c.nh, stream()));
+    const int64_t n = s->lat->g.total;
+    // in a volume the vessel runs through the front and back faces
+    k_touches_edge<<<(unsigned)((n + T - 1) / T), T, 0, stream()>>>(s->lat->grid, s->lat->g.d_dims, s->lat->g.d_off,
+                                                                   (int)c.nh, c.o2_hold == 4 ? 0 : 1, d_out);
+    CW_LAUNCHED();
+    CW_CUDA(cudaMemcpyAsync(out, d_out, sizeof(int32_t) * c.nh, cudaMemcpyDeviceToHost, stream()));
+    CW_CUDA(cudaStreamSynchronize(stream()));
+    dfree(d_out);
     return CW_OK;
 }
 

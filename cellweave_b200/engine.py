@@ -727,6 +727,12 @@ class Simulation:
         call("cw_sim_network_state", self._h, int(hist), int(n), ptr(out))
         return out
 
+    def touches_edge(self):
+        """touches_the_edge (simulation.rs:2165-2198) of every history, on the device."""
+        out = np.zeros(len(self.dims), np.int32)
+        call("cw_sim_touches_edge", self._h, ptr(out))
+        return out.astype(bool)
+
     def cycle(self, n, hist=0):
         """(began, due) of records 0..n-1 of a history: each cell's cycle."""
         began, due = np.empty(int(n), np.int32), np.empty(int(n), np.int32)

@@ -490,6 +490,9 @@ typedef struct {
     double exposure;     /* the exposure's level at the step last taken (0 without one or while off) */
 } cw_measurements;
 int cw_sim_measure(cw_sim sim, cw_measurements *out);
+/* touches_the_edge (simulation.rs:2165-2198) of every history, one int32 each: a cell on a pixel of
+ * the box's sides, or, in a volume around no vessel, of its faces; one pass over the sites. */
+int cw_sim_touches_edge(cw_sim sim, int32_t *out);
 /* Network state of history `hist`, [ncells][S]. */
 int cw_sim_network_state(cw_sim sim, uint32_t hist, uint32_t n, double *state);
 /* The cycle of records 0..n-1 of history `hist`: the step each began and the step it is over (the

@@ -199,3 +199,24 @@ def test_an_exposure_stresses_the_tissue_inside_the_oracle_band(tmp_path):
             assert within_band(dv, rv), (step, q, dv.mean(), rv.mean(), rv.std())
     stress = sim.field_values(4, 0)
     assert stress.max() <= 1.0 + 1e-9
+
+
+@pytest.mark.parametrize("width,source", [(22, ""), (40, "\n[oxygen_source]\nkind = \"vessel\"\nradius = 2\n")])
+def test_the_device_edge_test_is_the_reference_s(tmp_path, width, source):
+    """touches_the_edge (simulation.rs:2165-2198) on the device against the
+    host restatement, every step of small boxes the tissue soon reaches."""
+    ras_erk_toml(tmp_path)
+    (tmp_path / "run.toml").write_text(f"width = {width}\nheight = 20\nmcs = 40\ntemperature = 10.0\n"
+                                       "snapshot_interval = 20\noutput_dir = \"out\"\noxygen_uptake = 0.0001\n"
+                                       "network = \"ras-erk.toml\"\n" + source)
+    cfg = C.load_sim_config(str(tmp_path / "run.toml"))
+    sim, _ = C.simulation_from_config(cfg, histories=8, seeds=list(range(8)))
+    vessel = bool(source)
+    seen = set()
+    for _ in range(40):
+        sim.step(1)
+        dev = sim.touches_edge()
+        host = [C.touches_the_edge(sim.grid(k), vessel) for k in range(8)]
+        assert list(dev) == host
+        seen |= set(host)
+    assert seen == {False, True}
