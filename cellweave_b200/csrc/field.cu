@@ -185,7 +185,9 @@ __global__ void __launch_bounds__(256) k_residual64(FieldView fv, const int32_t 
 
 // After sweep `index`: decide convergence (relax's `moved < tolerance`,
 // pde.rs:280-283, or the residual rule) and reset the accumulators.
-__global__ void k_check(RelaxState *st, int nh, int64_t index, int residual_counted) {
+// The stop test after each FP64 sweep; a running history counts the sweep
+// (so that a chunk of sweeps launches with the same arguments every time).
+__global__ void k_check(RelaxState *st, int nh, int residual_counted) {
     int h = blockIdx.x * blockDim.x + threadIdx.x;
     if (h >= nh) return;
     RelaxState &s = st[h];
@@ -195,7 +197,7 @@ __global__ void k_check(RelaxState *st, int nh, int64_t index, int residual_coun
         s.last_change = m;
         if (residual_counted) s.last_resid = r;
         bool conv = s.stop == CW_STOP_RESIDUAL ? r < s.tol : m < s.tol;
-        s.sweeps = index;
+        s.sweeps += 1;
         if (conv) s.done = 1;
     }
     s.moved[0] = s.moved[1] = 0ull;
@@ -546,32 +548,67 @@ static int relax_fp64(cw_field_s *f, const cw_relax_opts &o, std::vector<Span> &
     Plan prow;
     if ((rc = row_plan(f, prow)) != CW_OK) return rc;
     bool resid = o.stop == CW_STOP_RESIDUAL;
-    int64_t done_sweeps = 0, chunk = 8;
-    std::vector<int32_t> flags(nh);
-    while (done_sweeps < o.max_sweeps) {
-        int64_t n = std::min(chunk, o.max_sweeps - done_sweeps);
-        for (int64_t s = 0; s < n; ++s) {
-            for (int colour = 0; colour < 2; ++colour) {
-                if (pc[colour].nblocks == 0) continue;
-                k_sor64_half<<<pc[colour].nblocks, T, 0, stream()>>>(fv, pc[colour].d_blk, nh, f->d_span, d_st,
-                                                                      colour);
-                CW_LAUNCHED();
-            }
-            if (resid) {
-                k_residual64<<<prow.nblocks, T, 0, stream()>>>(fv, prow.d_blk, nh, d_st, nullptr, nullptr, nullptr, 1);
-                CW_LAUNCHED();
-            }
-            k_check<<<(nh + 63) / 64, 64, 0, stream()>>>(d_st, nh, done_sweeps + s + 1, resid ? 1 : 0);
+    auto sweep = [&]() -> int {
+        for (int colour = 0; colour < 2; ++colour) {
+            if (pc[colour].nblocks == 0) continue;
+            k_sor64_half<<<pc[colour].nblocks, T, 0, stream()>>>(fv, pc[colour].d_blk, nh, f->d_span, d_st, colour);
             CW_LAUNCHED();
         }
-        done_sweeps += n;
-        CW_CUDA(cudaMemcpyAsync(hs.data(), d_st, sizeof(RelaxState) * nh, cudaMemcpyDeviceToHost, stream()));
-        CW_CUDA(cudaStreamSynchronize(stream()));
+        if (resid) {
+            k_residual64<<<prow.nblocks, T, 0, stream()>>>(fv, prow.d_blk, nh, d_st, nullptr, nullptr, nullptr, 1);
+            CW_LAUNCHED();
+        }
+        k_check<<<(nh + 63) / 64, 64, 0, stream()>>>(d_st, nh, resid ? 1 : 0);
+        CW_LAUNCHED();
+        return CW_OK;
+    };
+    // The first GRAPH_SWEEPS sweeps launched one by one; a solve that goes on
+    // replays them captured as one graph (the same launches with the same
+    // arguments), 1, 2, 4, ... up to 32 replays between checks, the last few
+    // sweeps below a whole chunk launched one by one again.
+    constexpr int64_t GRAPH_SWEEPS = 8;
+    cudaGraphExec_t chunk_graph = nullptr;
+    int64_t done_sweeps = 0, reps = 1;
+    bool first = true;
+    while (done_sweeps < o.max_sweeps) {
+        const int64_t left = o.max_sweeps - done_sweeps;
+        if (first || left < GRAPH_SWEEPS) {
+            const int64_t n = std::min(GRAPH_SWEEPS, left);
+            for (int64_t s = 0; s < n; ++s)
+                if ((rc = sweep()) != CW_OK) return rc;
+            done_sweeps += n;
+            first = false;
+        } else {
+            if (!chunk_graph) {
+                cudaGraph_t g = nullptr;
+                CW_CUDA(cudaStreamBeginCapture(stream(), cudaStreamCaptureModeThreadLocal));
+                for (int64_t s = 0; s < GRAPH_SWEEPS && rc == CW_OK; ++s) rc = sweep();
+                cudaError_t e = cudaStreamEndCapture(stream(), &g);
+                if (rc != CW_OK) { if (g) cudaGraphDestroy(g); return rc; }
+                if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+                e = cudaGraphInstantiate(&chunk_graph, g, 0);
+                cudaGraphDestroy(g);
+                if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
+            }
+            const int64_t n = std::min(reps, left / GRAPH_SWEEPS);
+            for (int64_t r = 0; r < n; ++r) {
+                cudaError_t e = cudaGraphLaunch(chunk_graph, stream());
+                if (e != cudaSuccess) { cudaGraphExecDestroy(chunk_graph); return cuda_fail(e, "cudaGraphLaunch"); }
+            }
+            done_sweeps += n * GRAPH_SWEEPS;
+            reps = std::min<int64_t>(reps * 2, 32);
+        }
+        cudaError_t e = cudaMemcpyAsync(hs.data(), d_st, sizeof(RelaxState) * nh, cudaMemcpyDeviceToHost, stream());
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream());
+        if (e != cudaSuccess) {
+            if (chunk_graph) cudaGraphExecDestroy(chunk_graph);
+            return cuda_fail(e, "relax state");
+        }
         bool all = true;
         for (uint32_t k = 0; k < nh; ++k) all = all && hs[k].done;
         if (all) break;
-        chunk = std::min<int64_t>(chunk * 2, 256);
     }
+    if (chunk_graph) cudaGraphExecDestroy(chunk_graph);
     pc[0].release(); pc[1].release(); ps.release(); prow.release();
     return CW_OK;
 }
