@@ -51,7 +51,7 @@ SOR_TRAFFIC_PER_SITE = 14.95
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--steps", type=int, default=100)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--workload", choices=["campaign", "cord"], default="campaign")
@@ -104,7 +104,9 @@ def config_key(name, cfg):
 
 # ------------------------------------------------------------------ GPU clocks
 class Clocks:
-    """nvidia-smi sampled every 200 ms while the timed region runs."""
+    """nvidia-smi sampled every 100 ms while the timed region runs; start()
+    returns once the sampler has written its first row (up to 3 s), so that
+    the samples cover the timed region rather than nvidia-smi's start."""
 
     def __init__(self, index):
         self.index = index
@@ -119,10 +121,16 @@ class Clocks:
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
+            return
+        t0 = time.perf_counter()
+        while time.perf_counter() - t0 < 3.0 and self.proc.poll() is None:
+            if os.path.getsize(self.path) > 0:
+                break
+            time.sleep(0.02)
 
     def stop(self):
         if self.proc is None:
