@@ -233,6 +233,7 @@ struct cw_lattice_s {
     cw::DivScratch div;
     cw::Plan site_plan;                   // every pixel of every history, T per block
     int32_t *stage = nullptr;             // uploads land here and are checked before they become the grid
+    int32_t *d_span = nullptr;            // volumes: the occupied span of each history (x0 y0 z0 x1 y1 z1)
     unsigned long long *d_bad = nullptr;  // the first pixel of an upload past its history's capacity
     int32_t *bath_label = nullptr;        // the bath's union-find labels, one per site (bath.cu)
     uint8_t *bath_mark = nullptr;         // roots that reach the outer layer (bath.cu)

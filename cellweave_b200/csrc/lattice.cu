@@ -60,6 +60,7 @@ struct LatView {
     int32_t surface_on;
     int32_t copy_moore;
     uint32_t take_below;   // sub-sweeps: a pixel attempts when its draw is below this (0: every pixel)
+    const int32_t *span;   // volumes: the pixels a Monte Carlo step visits (x0 y0 z0 x1 y1 z1 a history)
 };
 
 struct Tables {
@@ -356,6 +357,70 @@ __device__ __forceinline__ void seg_append(Attempt *list, uint32_t seg, uint32_t
     if (take) list[(size_t)blockIdx.x * seg + base + __popc(m & ((1u << lane) - 1u))] = a;
 }
 
+// occupied_span (cpm.rs:774-793) of every volume history, at the start of a
+// Monte Carlo step: min and max of x, y, z over the pixels that are not
+// medium (the obstacle counts), reduced per warp, one atomic a warp; then one
+// pixel wider on every side, clipped, or empty (x0 > x1) when all is medium.
+__global__ void k_span_reset(int32_t *span, int nh) {
+    const int h = blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= nh) return;
+    for (int a = 0; a < 3; ++a) {
+        span[6 * h + a] = 0x7fffffff;
+        span[6 * h + 3 + a] = -1;
+    }
+}
+__global__ void k_span_occupied(const int32_t *grid, const int4 *dims, const int64_t *off, const int32_t *blk, int nh,
+                                int32_t *span) {
+    __shared__ int s_h;
+    if (threadIdx.x == 0) s_h = plan_history(blk, nh, blockIdx.x);
+    __syncthreads();
+    const int h = s_h;
+    const int4 dm = dims[h];
+    if (dm.z <= 1) return;  // the whole block: a plane visits its whole box
+    const int64_t local = (int64_t)(blockIdx.x - blk[h]) * blockDim.x + threadIdx.x;
+    int mn[3] = {0x7fffffff, 0x7fffffff, 0x7fffffff}, mx[3] = {-1, -1, -1};
+    if (local < off[h + 1] - off[h] && grid[off[h] + local] != 0) {
+        const int64_t slice = (int64_t)dm.x * dm.y;
+        const int z = (int)(local / slice);
+        const int64_t r = local - (int64_t)z * slice;
+        const int y = (int)(r / dm.x), x = (int)(r - (int64_t)y * dm.x);
+        mn[0] = mx[0] = x;
+        mn[1] = mx[1] = y;
+        mn[2] = mx[2] = z;
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        mn[a] = __reduce_min_sync(0xffffffffu, mn[a]);
+        mx[a] = __reduce_max_sync(0xffffffffu, mx[a]);
+    }
+    if ((threadIdx.x & 31) == 0 && mx[0] >= 0)
+        for (int a = 0; a < 3; ++a) {
+            atomicMin(span + 6 * h + a, mn[a]);
+            atomicMax(span + 6 * h + 3 + a, mx[a]);
+        }
+}
+__global__ void k_span_finish(int32_t *span, const int4 *dims, int nh) {
+    const int h = blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= nh) return;
+    int32_t *s = span + 6 * h;
+    if (s[3] < 0) {  // all medium: nothing to visit
+        s[0] = 1;
+        s[3] = 0;
+        return;
+    }
+    const int lim[3] = {dims[h].x, dims[h].y, dims[h].z};
+    for (int a = 0; a < 3; ++a) {
+        s[a] = s[a] > 0 ? s[a] - 1 : 0;
+        s[3 + a] = s[3 + a] + 1 < lim[a] - 1 ? s[3 + a] + 1 : lim[a] - 1;
+    }
+}
+
+__device__ __forceinline__ bool in_span(const int32_t *span, int h, int4 dm, int x, int y, int z) {
+    if (!span || dm.z <= 1) return true;
+    const int32_t *s = span + 6 * h;
+    return x >= s[0] && x <= s[3] && y >= s[1] && y <= s[4] && z >= s[2] && z <= s[5];
+}
+
 // One sublattice pass: one copy attempt at every pixel of this pass's colour
 // (the reference's try_flip, cpm.rs:797-838), the attempts ordered by a
 // per-pass priority and run as that sequence would run them.  The pixels of
@@ -402,7 +467,8 @@ __global__ void __launch_bounds__(T) k_cpm_pass(LatView L, Tables tabs, const in
         int x = 0, y = 0, z = 0;
         bool copies = false;
         Attempt a;
-        if (colour_site(dm, L.period, colour, k, x, y, z)) {
+        // in a volume, the pixels of the occupied span only (cpm.rs:748-763)
+        if (colour_site(dm, L.period, colour, k, x, y, z) && in_span(L.span, h, dm, x, y, z)) {
             const int64_t i = ((int64_t)z * dm.y + y) * dm.x + x;
             const int32_t src = g[i];
             // a pixel whose copy neighbours all hold its own id cannot copy: no draw needed
@@ -729,6 +795,7 @@ static LatView lat_view(cw_lattice_s *l) {
     v.K = l->K; v.nreach = l->nreach; v.period = l->period; v.ncol = l->ncol; v.across = l->across;
     v.temperature = l->temperature; v.surface_on = l->surface_on ? 1 : 0; v.copy_moore = l->copy_moore ? 1 : 0;
     v.take_below = l->subsweeps > 1 ? (uint32_t)(4294967296.0 / (double)l->subsweeps) : 0u;
+    v.span = l->d_span;
     return v;
 }
 
@@ -788,6 +855,22 @@ int lattice_recount(cw_lattice_s *l, int32_t *vol_out, int32_t *surf_out) {
 // colour order, then one cooperative launch per colour (its rounds meet at a
 // grid barrier), the claims and control words cleared before each.
 int lattice_sweep(cw_lattice_s *l) {
+    if (l->d_span) {
+        Plan &p = l->site_plan;
+        if (p.nblocks == 0) {
+            std::vector<int64_t> per(l->g.nh);
+            for (uint32_t k = 0; k < l->g.nh; ++k) per[k] = l->g.sites(k);
+            int rc = p.build(per, T);
+            if (rc != CW_OK) return rc;
+        }
+        const int nh = (int)l->g.nh;
+        k_span_reset<<<(nh + 127) / 128, 128, 0, stream()>>>(l->d_span, nh);
+        CW_LAUNCHED();
+        k_span_occupied<<<p.nblocks, T, 0, stream()>>>(l->grid, l->g.d_dims, l->g.d_off, p.d_blk, nh, l->d_span);
+        CW_LAUNCHED();
+        k_span_finish<<<(nh + 127) / 128, 128, 0, stream()>>>(l->d_span, l->g.d_dims, nh);
+        CW_LAUNCHED();
+    }
     for (int s = 0; s < std::max(l->subsweeps, 1); ++s) {
         int rc = lattice_subsweep(l);
         if (rc != CW_OK) return rc;
@@ -878,7 +961,8 @@ int cw_lattice_create(uint32_t nh, const uint32_t *w, const uint32_t *h, const u
     if ((rc = dalloc(&l->grid, n)) || (rc = dalloc(&l->type, nc)) || (rc = dalloc(&l->volume, nc)) ||
         (rc = dalloc(&l->target, nc)) || (rc = dalloc(&l->lambda, nc)) || (rc = dalloc(&l->vsnap, nc)) ||
         (rc = dalloc(&l->d_cell_off, nh + 1)) || (rc = dalloc(&l->d_keys, nh)) ||
-        (rc = dalloc(&l->d_flag, 4 + 27 * (size_t)nh)) || (rc = dalloc(&l->d_used, nh))) {
+        (rc = dalloc(&l->d_flag, 4 + 27 * (size_t)nh)) || (rc = dalloc(&l->d_used, nh)) ||
+        (volume && (rc = dalloc(&l->d_span, 6 * (size_t)nh)))) {
         cw_lattice_destroy(l);
         return rc;
     }
@@ -907,7 +991,7 @@ int cw_lattice_destroy(cw_lattice l) {
     dfree(l->grid); dfree(l->type); dfree(l->volume); dfree(l->target); dfree(l->lambda); dfree(l->vsnap);
     dfree(l->surface); dfree(l->ssnap); dfree(l->tsurf); dfree(l->lsurf); dfree(l->d_cell_off); dfree(l->d_keys);
     dfree(l->d_flag); dfree(l->claim); dfree(l->plist); dfree(l->pctl); dfree(l->d_used);
-    dfree(l->bath_label); dfree(l->bath_mark); dfree(l->stage); dfree(l->d_bad);
+    dfree(l->bath_label); dfree(l->bath_mark); dfree(l->stage); dfree(l->d_bad); dfree(l->d_span);
     l->div.release();
     l->site_plan.release();
     for (auto &p : l->plans) p.release();

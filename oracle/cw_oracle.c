@@ -806,8 +806,15 @@ void or_lattice_mcs_checkerboard(or_lattice *l, uint32_t k0, uint32_t k1, uint32
      * below 2^32 / subsweeps; the draws count sub-sweeps */
     if (subsweeps < 1) subsweeps = 1;
     const uint32_t take_below = subsweeps > 1 ? (uint32_t)(4294967296.0 / (double)subsweeps) : 0u;
+    /* in a volume a Monte Carlo step visits the occupied span at its start
+     * (monte_carlo_step, cpm.rs:748-763): the box around every pixel that is
+     * not medium, one wider on every side; nothing when all is medium.  A
+     * plane visits the whole box. */
+    int32_t sp[6] = {0, l->w - 1, 0, l->h - 1, 0, l->d - 1};
+    int occupied = 1;
     for (int32_t s = 0; s < sweeps * subsweeps; ++s) {
         uint32_t mcs = mcs0 * (uint32_t)subsweeps + (uint32_t)s;
+        if (l->d > 1 && s % subsweeps == 0) occupied = or_occupied_span(l, sp);
         or_colour_order(ncol, mcs, k0, k1, perm);
         for (int32_t q = 0; q < ncol; ++q) {
             int32_t colour = perm[q];
@@ -816,9 +823,9 @@ void or_lattice_mcs_checkerboard(or_lattice *l, uint32_t k0, uint32_t k1, uint32
             const int32_t *vol = vsnap ? vsnap : l->volume;
             const int32_t *surf = ssnap ? ssnap : l->surface;
             int64_t m = 0;
-            for (int32_t z = 0; z < l->d; ++z)
-                for (int32_t y = 0; y < l->h; ++y)
-                    for (int32_t x = 0; x < l->w; ++x) {
+            for (int32_t z = sp[4]; occupied && z <= sp[5]; ++z)
+                for (int32_t y = sp[2]; y <= sp[3]; ++y)
+                    for (int32_t x = sp[0]; x <= sp[1]; ++x) {
                         if (or_colour_of(period, x, y, z) != colour) continue;
                         int64_t site = (int64_t)z * slice + (int64_t)y * w + x;
                         order[m].site = site;
