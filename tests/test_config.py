@@ -139,3 +139,18 @@ def test_the_runner_refuses_a_configuration_it_cannot_run(tmp_path, capsys):
     path = write(tmp_path, BASE + "\n[lesion]\nat = 3\nradius = 2\n")
     with pytest.raises(cw.ConfigError, match="lesion"):
         C.main([path, "--steps", "2"])
+
+
+def test_the_example_shaped_scenarios_load(tmp_path):
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "make_scenarios", os.path.join(os.path.dirname(__file__), "golden", "make_scenarios.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    mod.main(str(tmp_path))
+    for name in mod.SCENARIOS:
+        kw, refvol = C.simulation_kwargs(C.load_sim_config(str(tmp_path / f"{name}.toml")))
+        assert refvol > 0 and kw["first_tolerance"] == 1e-8
+    kw, _ = C.simulation_kwargs(C.load_sim_config(str(tmp_path / "spheroid3d.toml")))
+    assert kw["debris_loss"] == 0.024 and kw["still_medium"] == 0.606 and kw["cycle_median"] == 20.0
+    assert kw["dims"] == [(320, 320, 320)] and kw["max_cells"] == 200000 and kw["sweeps"] == 4
