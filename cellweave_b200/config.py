@@ -216,7 +216,7 @@ def snapshot_of(sim, hist, mcs):
                     sim.field_values(0, hist))
 
 
-def run(path, out_dir=None, histories=1, seeds=None, subsweeps=4, steps=None):
+def run(path, out_dir=None, histories=1, seeds=None, subsweeps=4, steps=None, profile_last=False):
     """The reference's run loop (src/main.rs:162-206) on the device: every
     step measured into measurements.csv, a snapshot every
     `snapshot_interval` steps and at the step the tissue touches the edge,
@@ -230,8 +230,14 @@ def run(path, out_dir=None, histories=1, seeds=None, subsweeps=4, steps=None):
     done = [False] * histories
     n = int(cfg["mcs"] if steps is None else steps)
     taken = 0
-    for _ in range(n):
-        sim.step(1)
+    for i in range(n):
+        if profile_last and i == n - 1:
+            from . import _lib
+            _lib.check(_lib.lib().cw_profiler_start())
+            sim.step(1)
+            _lib.check(_lib.lib().cw_profiler_stop())
+        else:
+            sim.step(1)
         taken += 1
         ms = sim.measure()
         edge = sim.touches_edge()
@@ -266,9 +272,12 @@ def main(argv=None):
     p.add_argument("--histories", type=int, default=1)
     p.add_argument("--subsweeps", type=int, default=4)
     p.add_argument("--out", default=None)
+    p.add_argument("--profile-last", action="store_true",
+                   help="bracket the last step with the CUDA profiler's start and stop")
     a = p.parse_args(argv)
     t0 = time.perf_counter()
-    out = run(a.config, a.out, histories=a.histories, subsweeps=a.subsweeps, steps=a.steps)
+    out = run(a.config, a.out, histories=a.histories, subsweeps=a.subsweeps, steps=a.steps,
+              profile_last=a.profile_last)
     wall = time.perf_counter() - t0
     print(json.dumps(dict(config=os.path.abspath(a.config), histories=a.histories, steps=out["steps"],
                           wall_s=round(wall, 3), ms_per_step=round(1000.0 * wall / max(out["steps"], 1), 3),
