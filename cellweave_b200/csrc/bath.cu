@@ -13,6 +13,14 @@
 // convergence loop on the host, so the bath can be taken inside a captured
 // step.  The same pixels as the reference's flood: a component is held
 // exactly when it reaches the outer layer.
+//
+// In a volume the union-find covers the occupied span (the box around every
+// pixel that is not medium, one wider on every side) only: the medium outside
+// it is bath (from any pixel outside the span a straight line away from it
+// stays outside and ends on the outer layer), and a medium component inside
+// is bath exactly when it reaches the span's border layer (next to the
+// outside) or the outer layer.  The same mask for a fraction of the work
+// when a small tissue sits in a large box.
 #include "cw_internal.cuh"
 
 using namespace cw;
@@ -52,6 +60,15 @@ __device__ __forceinline__ void unite(int32_t *L, int32_t a, int32_t b) {
     atomicExch(&g_bath_error, 1);
 }
 
+constexpr int32_t OUTSIDE = -2;  // a label: medium outside the span, bath
+
+// Inside the span of history h (always, without one or in a plane).
+__device__ __forceinline__ bool inside(const int32_t *span, int h, int4 dm, int x, int y, int z) {
+    if (!span || dm.z <= 1) return true;
+    const int32_t *s = span + 6 * h;
+    return x >= s[0] && x <= s[3] && y >= s[1] && y <= s[4] && z >= s[2] && z <= s[5];
+}
+
 __device__ __forceinline__ bool site_of(const int32_t *blk, int nh, const int4 *dims, const int64_t *off,
                                         int &h, int64_t &i, int &x, int &y, int &z) {
     h = plan_history(blk, nh, blockIdx.x);
@@ -65,10 +82,12 @@ __device__ __forceinline__ bool site_of(const int32_t *blk, int nh, const int4 *
     return true;
 }
 
-__global__ void k_cc_init(const int32_t *grid, int64_t n, int32_t *L, uint8_t *mark) {
-    const int64_t i = (int64_t)blockIdx.x * T + threadIdx.x;
-    if (i >= n) return;
-    L[i] = grid[i] == 0 ? (int32_t)i : -1;
+__global__ void k_cc_init(const int32_t *blk, int nh, const int4 *dims, const int64_t *off, const int32_t *span,
+                          const int32_t *grid, int32_t *L, uint8_t *mark) {
+    int h, x, y, z;
+    int64_t i;
+    if (!site_of(blk, nh, dims, off, h, i, x, y, z)) return;
+    L[i] = grid[i] != 0 ? -1 : inside(span, h, dims[h], x, y, z) ? (int32_t)i : OUTSIDE;
     mark[i] = 0;
 }
 
@@ -92,15 +111,20 @@ __global__ void k_cc_flatten(int64_t n, int32_t *L) {
 
 // the roots of the medium on the box's outer layer (a flat box's one slice
 // is its whole area: its first and last slice are not a layer)
-__global__ void k_cc_mark(const int32_t *blk, int nh, const int4 *dims, const int64_t *off, const int32_t *L,
-                          uint8_t *mark) {
+// (and, in a volume with a span, the roots of the medium on its border layer)
+__global__ void k_cc_mark(const int32_t *blk, int nh, const int4 *dims, const int64_t *off, const int32_t *span,
+                          const int32_t *L, uint8_t *mark) {
     int h, x, y, z;
     int64_t i;
     if (!site_of(blk, nh, dims, off, h, i, x, y, z)) return;
     const int32_t r = L[i];
     if (r < 0) return;
     const int4 dm = dims[h];
-    const bool outer = x == 0 || y == 0 || x + 1 == dm.x || y + 1 == dm.y || (dm.z > 1 && (z == 0 || z + 1 == dm.z));
+    bool outer = x == 0 || y == 0 || x + 1 == dm.x || y + 1 == dm.y || (dm.z > 1 && (z == 0 || z + 1 == dm.z));
+    if (span && dm.z > 1) {
+        const int32_t *s = span + 6 * h;
+        outer = outer || x == s[0] || x == s[3] || y == s[1] || y == s[4] || z == s[2] || z == s[5];
+    }
     if (outer) mark[r] = 1;
 }
 
@@ -108,7 +132,7 @@ __global__ void k_cc_bath(int64_t n, const int32_t *L, const uint8_t *mark, uint
     const int64_t i = (int64_t)blockIdx.x * T + threadIdx.x;
     if (i >= n) return;
     const int32_t r = L[i];
-    bath[i] = r >= 0 && mark[r] ? 1 : 0;
+    bath[i] = r == OUTSIDE || (r >= 0 && mark[r]) ? 1 : 0;
 }
 
 }  // namespace
@@ -133,13 +157,17 @@ int lattice_bath_enqueue(cw_lattice_s *l, uint8_t *bath) {
     }
     const unsigned flat = (unsigned)((n + T - 1) / T);
     const int nh = (int)l->g.nh;
-    k_cc_init<<<flat, T, 0, stream()>>>(l->grid, n, l->bath_label, l->bath_mark);
+    // the span of the lattice as it stands (a step's may be out of date)
+    if ((rc = lattice_span_enqueue(l)) != CW_OK) return rc;
+    k_cc_init<<<p.nblocks, T, 0, stream()>>>(p.d_blk, nh, l->g.d_dims, l->g.d_off, l->d_span, l->grid, l->bath_label,
+                                            l->bath_mark);
     CW_LAUNCHED();
     k_cc_merge<<<p.nblocks, T, 0, stream()>>>(p.d_blk, nh, l->g.d_dims, l->g.d_off, l->bath_label);
     CW_LAUNCHED();
     k_cc_flatten<<<flat, T, 0, stream()>>>(n, l->bath_label);
     CW_LAUNCHED();
-    k_cc_mark<<<p.nblocks, T, 0, stream()>>>(p.d_blk, nh, l->g.d_dims, l->g.d_off, l->bath_label, l->bath_mark);
+    k_cc_mark<<<p.nblocks, T, 0, stream()>>>(p.d_blk, nh, l->g.d_dims, l->g.d_off, l->d_span, l->bath_label,
+                                             l->bath_mark);
     CW_LAUNCHED();
     k_cc_bath<<<flat, T, 0, stream()>>>(n, l->bath_label, l->bath_mark, bath);
     CW_LAUNCHED();

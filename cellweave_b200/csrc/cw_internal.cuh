@@ -278,6 +278,7 @@ int lattice_subsweep(cw_lattice_s *lat);
 int lattice_pass_error(cw_lattice_s *l);
 int lattice_recount_surfaces(cw_lattice_s *l);  // surfaces from the grid into the records, no sync
 int lattice_divide_enqueue(cw_lattice_s *l, const uint8_t *alive, int max_living, double *state, int S);
+int lattice_span_enqueue(cw_lattice_s *l);  // volumes: the occupied span of the lattice as it stands, into d_span
 int lattice_bath_enqueue(cw_lattice_s *l, uint8_t *bath);  // bath.cu: medium joined to the box's outer layer
 int lattice_bath_error();
 // debris.cu: the dead tissue's debris lost at its edge, the fluid shut in drained

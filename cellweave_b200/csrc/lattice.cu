@@ -854,23 +854,28 @@ int lattice_recount(cw_lattice_s *l, int32_t *vol_out, int32_t *surf_out) {
 // One Monte Carlo step of every history (no host synchronisation): the
 // colour order, then one cooperative launch per colour (its rounds meet at a
 // grid barrier), the claims and control words cleared before each.
-int lattice_sweep(cw_lattice_s *l) {
-    if (l->d_span) {
-        Plan &p = l->site_plan;
-        if (p.nblocks == 0) {
-            std::vector<int64_t> per(l->g.nh);
-            for (uint32_t k = 0; k < l->g.nh; ++k) per[k] = l->g.sites(k);
-            int rc = p.build(per, T);
-            if (rc != CW_OK) return rc;
-        }
-        const int nh = (int)l->g.nh;
-        k_span_reset<<<(nh + 127) / 128, 128, 0, stream()>>>(l->d_span, nh);
-        CW_LAUNCHED();
-        k_span_occupied<<<p.nblocks, T, 0, stream()>>>(l->grid, l->g.d_dims, l->g.d_off, p.d_blk, nh, l->d_span);
-        CW_LAUNCHED();
-        k_span_finish<<<(nh + 127) / 128, 128, 0, stream()>>>(l->d_span, l->g.d_dims, nh);
-        CW_LAUNCHED();
+int lattice_span_enqueue(cw_lattice_s *l) {
+    if (!l->d_span) return CW_OK;
+    Plan &p = l->site_plan;
+    if (p.nblocks == 0) {
+        std::vector<int64_t> per(l->g.nh);
+        for (uint32_t k = 0; k < l->g.nh; ++k) per[k] = l->g.sites(k);
+        int rc = p.build(per, T);
+        if (rc != CW_OK) return rc;
     }
+    const int nh = (int)l->g.nh;
+    k_span_reset<<<(nh + 127) / 128, 128, 0, stream()>>>(l->d_span, nh);
+    CW_LAUNCHED();
+    k_span_occupied<<<p.nblocks, T, 0, stream()>>>(l->grid, l->g.d_dims, l->g.d_off, p.d_blk, nh, l->d_span);
+    CW_LAUNCHED();
+    k_span_finish<<<(nh + 127) / 128, 128, 0, stream()>>>(l->d_span, l->g.d_dims, nh);
+    CW_LAUNCHED();
+    return CW_OK;
+}
+
+int lattice_sweep(cw_lattice_s *l) {
+    int rc0 = lattice_span_enqueue(l);
+    if (rc0 != CW_OK) return rc0;
     for (int s = 0; s < std::max(l->subsweeps, 1); ++s) {
         int rc = lattice_subsweep(l);
         if (rc != CW_OK) return rc;
