@@ -288,6 +288,7 @@ struct DebrisState {
     double *owed = nullptr;    // per history: pixels owed to the fluid, carried
     int64_t *held = nullptr;   // per history: what the kept dead hold
     int32_t *paid = nullptr, *edges = nullptr;  // per history, this step / this pass
+    int32_t *active = nullptr; // per history: still owes this step (the passes skip the others whole)
     int32_t *claim = nullptr;  // per site: the cell taking it this pass (-1: none)
     int ensure(int64_t ncells, int nh, int64_t sites);
     void release();

@@ -78,7 +78,7 @@ __device__ __forceinline__ int history_of(const int32_t *blk, int nh) {
 // What the kept dead of each history hold, and the share of it owed this
 // step (simulation.rs:1243, 1272): one block per history.
 __global__ void k_debris_owe(const int64_t *cell_off, const uint8_t *kept, const int32_t *volume, double loss,
-                             double *owed, int64_t *held) {
+                             double *owed, int64_t *held, int32_t *active) {
     const int h = blockIdx.x;
     const int64_t c0 = cell_off[h], c1 = cell_off[h + 1];
     unsigned long long v = 0;
@@ -93,7 +93,14 @@ __global__ void k_debris_owe(const int64_t *cell_off, const uint8_t *kept, const
         for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += s[k];
         held[h] = (int64_t)t;
         owed[h] += loss * (double)t;
+        active[h] = floor(owed[h]) >= 1.0;
     }
+}
+
+// After a pass: a history that has paid what it owes sits out the rest.
+__global__ void k_debris_still(int nh, const double *owed, const int32_t *paid, int32_t *active) {
+    const int h = blockIdx.x * blockDim.x + threadIdx.x;
+    if (h < nh && active[h] && (int64_t)floor(owed[h]) - (int64_t)paid[h] <= 0) active[h] = 0;
 }
 
 __device__ __forceinline__ int64_t still_owed(const double *owed, const int32_t *paid, int h) {
@@ -103,8 +110,10 @@ __device__ __forceinline__ int64_t still_owed(const double *owed, const int32_t 
 // Mark the edge: kept dead pixels with living tissue across a face.
 __global__ void k_debris_edges(const int32_t *grid, const int4 *dims, const int64_t *off, const int64_t *cell_off,
                                const int32_t *blk, int nh, const int32_t *type, const uint8_t *kept, int necrotic,
-                               const double *owed, const int32_t *paid, int32_t *claim, int32_t *edges) {
+                               const double *owed, const int32_t *paid, const int32_t *active, int32_t *claim,
+                               int32_t *edges) {
     const int h = history_of(blk, nh);
+    if (!active[h]) return;  // the whole block: its claims are not read this step
     const int64_t i = (int64_t)(blockIdx.x - blk[h]) * blockDim.x + threadIdx.x;
     if (i >= off[h + 1] - off[h]) return;
     const int64_t gi = off[h] + i;
@@ -124,8 +133,9 @@ __global__ void k_debris_edges(const int32_t *grid, const int4 *dims, const int6
 __global__ void k_debris_draw(const int32_t *grid, const int4 *dims, const int64_t *off, const int64_t *cell_off,
                               const int32_t *blk, int nh, const int32_t *type, int necrotic, const double *owed,
                               const int32_t *paid, const int32_t *edges, const uint2 *keys, const uint32_t *step,
-                              int pass, int32_t *claim) {
+                              int pass, const int32_t *active, int32_t *claim) {
     const int h = history_of(blk, nh);
+    if (!active[h]) return;
     const int64_t i = (int64_t)(blockIdx.x - blk[h]) * blockDim.x + threadIdx.x;
     if (i >= off[h + 1] - off[h]) return;
     const int64_t gi = off[h] + i;
@@ -168,8 +178,10 @@ __global__ void k_drain_draw(const int32_t *grid, const int4 *dims, const int64_
 // Hand each claimed pixel to its taker; a cell's loss counted in `given`
 // and the history's in `paid` (the medium's is not counted).
 __global__ void k_claims_apply(int32_t *grid, const int64_t *off, const int64_t *cell_off, const int32_t *blk, int nh,
-                               const int32_t *claim, int32_t *volume, int32_t *given, int32_t *paid) {
+                               const int32_t *claim, int32_t *volume, int32_t *given, int32_t *paid,
+                               const int32_t *active) {
     const int h = history_of(blk, nh);
+    if (active && !active[h]) return;
     const int64_t i = (int64_t)(blockIdx.x - blk[h]) * blockDim.x + threadIdx.x;
     if (i >= off[h + 1] - off[h]) return;
     const int64_t gi = off[h] + i;
@@ -212,7 +224,7 @@ int DebrisState::ensure(int64_t ncells, int nh, int64_t sites) {
     int rc;
     if ((rc = dalloc(&kept, ncells)) || (rc = dalloc(&given, ncells)) || (rc = dalloc(&owed, nh)) ||
         (rc = dalloc(&held, nh)) || (rc = dalloc(&paid, nh)) || (rc = dalloc(&edges, nh)) ||
-        (rc = dalloc(&claim, sites)))
+        (rc = dalloc(&active, nh)) || (rc = dalloc(&claim, sites)))
         return rc;
     CW_CUDA(cudaMemsetAsync(kept, 0, sizeof(uint8_t) * ncells, stream()));
     CW_CUDA(cudaMemsetAsync(given, 0, sizeof(int32_t) * ncells, stream()));
@@ -223,9 +235,9 @@ int DebrisState::ensure(int64_t ncells, int nh, int64_t sites) {
 }
 
 void DebrisState::release() {
-    dfree(kept); dfree(given); dfree(owed); dfree(held); dfree(paid); dfree(edges); dfree(claim);
+    dfree(kept); dfree(given); dfree(owed); dfree(held); dfree(paid); dfree(edges); dfree(active); dfree(claim);
     kept = nullptr; given = nullptr; owed = nullptr; held = nullptr; paid = nullptr; edges = nullptr;
-    claim = nullptr;
+    active = nullptr; claim = nullptr;
 }
 
 static int site_plan_of(cw_lattice_s *l) {
@@ -244,19 +256,22 @@ int debris_break_down_enqueue(cw_lattice_s *l, DebrisState &D, double loss, int 
     if ((rc = site_plan_of(l)) != CW_OK) return rc;
     const Plan &p = l->site_plan;
     const int nh = (int)l->g.nh;
-    k_debris_owe<<<nh, T, 0, stream()>>>(l->d_cell_off, D.kept, l->volume, loss, D.owed, D.held);
+    k_debris_owe<<<nh, T, 0, stream()>>>(l->d_cell_off, D.kept, l->volume, loss, D.owed, D.held, D.active);
     CW_LAUNCHED();
     for (int pass = 0; pass < EDGE_PASSES; ++pass) {
         CW_CUDA(cudaMemsetAsync(D.edges, 0, sizeof(int32_t) * nh, stream()));
         k_debris_edges<<<p.nblocks, T, 0, stream()>>>(l->grid, l->g.d_dims, l->g.d_off, l->d_cell_off, p.d_blk, nh,
-                                                      l->type, D.kept, necrotic, D.owed, D.paid, D.claim, D.edges);
+                                                      l->type, D.kept, necrotic, D.owed, D.paid, D.active, D.claim,
+                                                      D.edges);
         CW_LAUNCHED();
         k_debris_draw<<<p.nblocks, T, 0, stream()>>>(l->grid, l->g.d_dims, l->g.d_off, l->d_cell_off, p.d_blk, nh,
                                                      l->type, necrotic, D.owed, D.paid, D.edges, l->d_keys, step,
-                                                     pass, D.claim);
+                                                     pass, D.active, D.claim);
         CW_LAUNCHED();
         k_claims_apply<<<p.nblocks, T, 0, stream()>>>(l->grid, l->g.d_off, l->d_cell_off, p.d_blk, nh, D.claim,
-                                                      l->volume, D.given, D.paid);
+                                                      l->volume, D.given, D.paid, D.active);
+        CW_LAUNCHED();
+        k_debris_still<<<(unsigned)((nh + T - 1) / T), T, 0, stream()>>>(nh, D.owed, D.paid, D.active);
         CW_LAUNCHED();
     }
     const int64_t nc = l->ncells;
@@ -278,7 +293,7 @@ int debris_drain_enqueue(cw_lattice_s *l, DebrisState &D, const uint8_t *bath, i
                                                 necrotic, bath, l->d_keys, step, D.claim);
     CW_LAUNCHED();
     k_claims_apply<<<p.nblocks, T, 0, stream()>>>(l->grid, l->g.d_off, l->d_cell_off, p.d_blk, nh, D.claim,
-                                                  l->volume, D.given, D.paid);
+                                                  l->volume, D.given, D.paid, nullptr);
     CW_LAUNCHED();
     return CW_OK;
 }
