@@ -149,46 +149,73 @@ class Clocks:
 
 # ------------------------------------------------------------------ the CPU reference path
 def _cpu_worker(args):
-    """One worker: a few histories of the workload on the CPU oracle, stepped
-    `steps` times after `warm` untimed steps; returns (history*MCS, seconds)."""
-    items, cfg, steps, warm, barrier = args
+    """One history of the workload on the CPU oracle: `warm` untimed steps,
+    then `steps` timed ones; returns (history index, seconds per MCS)."""
+    k, cfg, steps, warm = args
     os.environ["OMP_NUM_THREADS"] = "1"
     from oracle import cpu_sim
-    hs = [cpu_sim.CpuHistory(cfg, k) for k in items]
-    for h in hs:
-        for _ in range(warm):
-            h.step()
-    if barrier is not None:
-        barrier.wait()
+    h = cpu_sim.CpuHistory(cfg, k)
+    for _ in range(warm):
+        h.step()
     t0 = time.perf_counter()
     for _ in range(steps):
-        for h in hs:
-            h.step()
-    return len(hs) * steps, time.perf_counter() - t0
+        h.step()
+    return k, (time.perf_counter() - t0) / steps
 
 
-def cpu_sample(cfg, steps, warm, per_size, procs):
-    """The oracle (the reference's algorithms, restated in C) on a bounded
-    sample: `per_size` histories of each lattice size, one history per host
-    process as the reference's campaign runs one per thread."""
-    sizes = sorted({d[0] for d in cfg["dims"]})
+def lpt_makespan(costs, workers):
+    """Makespan of the longest-first list schedule of `costs` over `workers`
+    (the order a work-stealing pool fed the longest histories first reaches)."""
+    import heapq
+    loads = [0.0] * max(1, workers)
+    heapq.heapify(loads)
+    for c in sorted(costs, reverse=True):
+        heapq.heappush(loads, heapq.heappop(loads) + c)
+    return max(loads)
+
+
+CPU_SAMPLE = {"per_size": 4, "warm": 1, "steps": 2}
+
+
+def cpu_sample(cfg, cores):
+    """The reference's campaign on the host cores (src/campaign.rs:196-205:
+    every history its own run, rayon spreading the runs over the cores),
+    measured on a bounded sample and scheduled over the whole campaign.
+
+    Sample: CPU_SAMPLE["per_size"] histories of every lattice size, each run
+    by the oracle (sequential Metropolis, FP64 SOR, RK4: the reference's
+    algorithms) in its own process, all of them at once on `cores` processes
+    fed largest first, `warm` untimed MCS then `steps` timed ones.  Every
+    history of the campaign costs its size's mean seconds per MCS; the
+    campaign's MCS takes the makespan of those costs scheduled longest first
+    over `cores` workers, so the rate is histories / makespan.  Both CPU arms
+    use this one method and sample."""
+    sizes = sorted({tuple(d) for d in cfg["dims"]}, key=lambda d: -d[0] * d[1] * d[2])
     picked = []
     for s in sizes:
-        ks = [k for k, d in enumerate(cfg["dims"]) if d[0] == s][:per_size]
-        picked += ks
-    procs = max(1, min(procs, len(picked)))
-    chunks = [picked[i::procs] for i in range(procs)]
+        picked += [k for k, d in enumerate(cfg["dims"]) if tuple(d) == s][:CPU_SAMPLE["per_size"]]
+    procs = max(1, min(cores, len(picked)))
     ctx = mp.get_context("spawn")
-    with ctx.Manager() as mgr:
-        barrier = mgr.Barrier(procs)
-        with ctx.Pool(procs) as pool:
-            t0 = time.perf_counter()
-            res = pool.map(_cpu_worker, [(c, cfg, steps, warm, barrier) for c in chunks])
-            wall = time.perf_counter() - t0
-    units = sum(r[0] for r in res)
-    seconds = max(r[1] for r in res)
-    return units / seconds, {"histories": len(picked), "per_size": per_size, "steps": steps, "warm": warm,
-                             "processes": procs, "wall_s": round(wall, 2)}
+    t0 = time.perf_counter()
+    with ctx.Pool(procs) as pool:
+        res = pool.map(_cpu_worker, [(k, cfg, CPU_SAMPLE["steps"], CPU_SAMPLE["warm"]) for k in picked], chunksize=1)
+    wall = time.perf_counter() - t0
+    per = {}
+    for k, sec in res:
+        per.setdefault(tuple(cfg["dims"][k]), []).append(sec)
+    mean = {d: sum(v) / len(v) for d, v in per.items()}
+    costs = [mean[tuple(d)] for d in cfg["dims"]]
+    span = lpt_makespan(costs, cores)
+    detail = {"method": "per-size seconds per MCS from the sample; the campaign's histories scheduled longest "
+                        "first over the cores; rate = histories / makespan",
+              "sampled_histories": len(picked), "per_size": CPU_SAMPLE["per_size"], "warm": CPU_SAMPLE["warm"],
+              "timed_mcs": CPU_SAMPLE["steps"], "processes": procs, "wall_s": round(wall, 2),
+              "seconds_per_mcs": {f"{d[0]}x{d[1]}x{d[2]}": round(v, 4) for d, v in mean.items()},
+              "makespan_s": round(span, 4), "serial_s": round(sum(costs), 3)}
+    sample = (f"{len(picked)} of the {len(cfg['dims'])} histories ({CPU_SAMPLE['per_size']} per size) on the oracle, "
+              f"{CPU_SAMPLE['steps']} timed MCS each after {CPU_SAMPLE['warm']} untimed; all {len(cfg['dims'])} "
+              f"histories' MCS scheduled longest first over {cores} cores")
+    return len(cfg["dims"]) / span, detail, sample
 
 
 # ------------------------------------------------------------------ our path
@@ -443,16 +470,12 @@ def main():
         if rank != 0:
             return 0
         cfg = workload(args.workload)
-        steps = max(1, min(args.steps, 3))
-        procs = os.cpu_count() or 1
-        v, sample = cpu_sample(cfg, steps, 1, 4 if args.workload == "campaign" else 1, procs)
-        line = dict(base, impl="reference", value=v, ms_per_step=None, dtype="f64",
-                    config=config_key(args.workload, cfg),
-                    cpu_baseline={"value": v, "unit": UNIT, "cores": procs, "kind": "port",
-                                  "sample": f"{sample['histories']} of the {len(cfg['dims'])} histories "
-                                            f"({sample['per_size']} per size), {sample['steps']} timed MCS each "
-                                            f"after {sample['warm']} untimed, one process per history group",
-                                  "detail": sample},
+        cores = os.cpu_count() or 1
+        v, detail, sample = cpu_sample(cfg, cores)
+        line = dict(base, impl="reference", value=v, ms_per_step=1e3 * len(cfg["dims"]) / v,
+                    dtype="f64", config=config_key(args.workload, cfg),
+                    cpu_baseline={"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample,
+                                  "detail": detail},
                     e2e={"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
         print(json.dumps(line), flush=True)
         return 0
@@ -470,11 +493,9 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu:
         # the CPU leg first, before any GPU context exists in this process
         cfg = workload(args.workload)
-        v, sample = cpu_sample(cfg, 1, 1, 2 if args.workload == "campaign" else 1, os.cpu_count() or 1)
-        cpu = {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
-               "sample": f"{sample['histories']} histories ({sample['per_size']} per size), one timed MCS each "
-                         f"after one untimed, CPU oracle (sequential Metropolis, FP64 SOR, RK4)",
-               "detail": sample}
+        cores = os.cpu_count() or 1
+        v, detail, sample = cpu_sample(cfg, cores)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample, "detail": detail}
     r = run_ours(args, rank, world, dist)
     if rank == 0:
         line = dict(base, value=r["value"], ms_per_step=r["ms"], dtype="f32+f64",

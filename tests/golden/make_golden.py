@@ -1,8 +1,9 @@
 """Regenerate ``tests/golden/golden.json`` from the reference's own files.
 
-Run in a checkout that has the reference at ``/root/reference`` (read only):
+Give it the reference's checkout (read only), as an argument or in the
+environment variable CELLWEAVE_REFERENCE:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py PATH_TO_CELLWEAVE_CHECKOUT
 
 It reads, and records with their source locations:
   * the network files under examples/networks/ (parsed with tomllib, with
@@ -16,9 +17,10 @@ The JSON is committed so the tests never read the reference at run time.
 import json
 import os
 import re
+import sys
 import tomllib
 
-REF = "/root/reference"
+REF = None  # the reference checkout, set by main()
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden.json")
 
 
@@ -59,7 +61,12 @@ def rk4_table():
     return rows
 
 
-def main():
+def main(argv=None):
+    global REF
+    argv = sys.argv[1:] if argv is None else argv
+    REF = argv[0] if argv else os.environ.get("CELLWEAVE_REFERENCE")
+    if not REF or not os.path.isdir(os.path.join(REF, "crates", "engine")):
+        sys.exit("usage: make_golden.py PATH_TO_CELLWEAVE_CHECKOUT (or set CELLWEAVE_REFERENCE)")
     nets = {}
     ndir = os.path.join(REF, "examples/networks")
     for name in sorted(os.listdir(ndir)):

@@ -64,3 +64,20 @@ def test_the_reference_arm_runs_on_rank_0_only():
     r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus", "2"],
                        env=env, capture_output=True, text=True, timeout=120)
     assert r.returncode == 0 and r.stdout.strip() == ""
+
+
+def test_the_cpu_arms_schedule_the_whole_campaign_longest_first():
+    sys.path.insert(0, ROOT)
+    import bench
+    # longest-first list scheduling: 3, 3 | 2 -> 5, 3 | 2 -> 5, 5 | 2 -> 7, 5
+    assert bench.lpt_makespan([2, 3, 2, 3, 2], 2) == 7
+    assert bench.lpt_makespan([1.0] * 8, 16) == 1.0
+    assert bench.lpt_makespan([4.0, 1.0, 1.0, 1.0, 1.0], 2) == 4.0
+    from cellweave_b200 import synthetic
+    cfg = synthetic.campaign(per_size=3, sizes=(32, 48))
+    v, detail, sample = bench.cpu_sample(cfg, 2)
+    per = detail["seconds_per_mcs"]
+    assert set(per) == {"32x32x1", "48x48x1"} and detail["sampled_histories"] == 6
+    costs = [per["32x32x1"]] * 3 + [per["48x48x1"]] * 3
+    assert v == pytest.approx(6 / bench.lpt_makespan(costs, 2), rel=0.02)  # the detail is rounded
+    assert detail["makespan_s"] >= detail["serial_s"] / 2 - 1e-3
