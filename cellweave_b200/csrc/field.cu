@@ -1357,7 +1357,17 @@ int cw::field_relax(cw_field_s *f, const cw_relax_opts *opts, const double *omeg
     if (o.precision != CW_FP64 && o.precision != CW_FP32_DC) return fail(CW_ERR_CONFIG, "unknown precision");
     if (o.precision == CW_FP32_DC && o.stop != CW_STOP_RESIDUAL)
         return fail(CW_ERR_CONFIG, "the FP32 defect-correction solve stops on the residual only");
+    if (!(o.tolerance > 0.0 && o.tolerance < INFINITY))
+        return fail(CW_ERR_CONFIG, "the tolerance must be finite and above zero, got " + std::to_string(o.tolerance));
+    if (!(o.omega < 2.0))
+        return fail(CW_ERR_CONFIG, "the relaxation factor must lie in (0, 2) (or be <= 0 for the rule), got " +
+                                       std::to_string(o.omega));
     uint32_t nh = f->g.nh;
+    if (omega_h)
+        for (uint32_t k = 0; k < nh; ++k)
+            if (!(omega_h[k] < 2.0))
+                return fail(CW_ERR_CONFIG, "a history's relaxation factor must lie below 2, got " +
+                                               std::to_string(omega_h[k]));
     int rc;
     if (f->held_dirty || f->spans.size() != nh) {
         if ((rc = field_span(f, f->spans)) != CW_OK) return rc;

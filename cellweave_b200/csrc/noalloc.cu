@@ -224,10 +224,26 @@ extern "C" int cw_field_relax_noalloc(double *values, const uint8_t *held, const
         double m = (double)(width > height ? width : height);
         omega = std::fmin(2.0 / (1.0 + std::sin(3.14159265358979323846 / m)), 1.95);
     }
+    if (!(omega > 0.0 && omega < 2.0))
+        return cw::fail(CW_ERR_CONFIG, "the relaxation factor must lie in (0, 2) (or be <= 0 for the rule), got " +
+                                           std::to_string(omega));
+    if (!(tolerance > 0.0 && tolerance < INFINITY))
+        return cw::fail(CW_ERR_CONFIG, "the tolerance must be finite and above zero, got " + std::to_string(tolerance));
     const int inner = inner_sweeps > 0 ? inner_sweeps : 16;
     if (max_sweeps <= 0) max_sweeps = 1;
     NaField f{values, held, uptake, production, lin_sink, dcoef, decay, source, (int)width, (int)height};
     cudaStream_t s = cw::stream();
+    if (s) {
+        // the library stream is created on the device current at its first
+        // use (or handed in by cw_set_stream): it must be this device's
+        int dev = -1, sdev = -1;
+        CW_CUDA(cudaGetDevice(&dev));
+        CW_CUDA(cudaStreamGetDevice(s, &sdev));
+        if (sdev != dev)
+            return cw::fail(CW_ERR_CONFIG, "the library stream belongs to device " + std::to_string(sdev) +
+                                               ", the current device is " + std::to_string(dev) +
+                                               ": give this device's stream to cw_set_stream first");
+    }
     NaState init{};
     CW_CUDA(cudaMemcpyAsync(st, &init, sizeof init, cudaMemcpyHostToDevice, s));
     const int T = 256, nb = (n + T - 1) / T;

@@ -237,9 +237,14 @@ int cw_field_relax_adjoint(cw_field f, const double *dl_dc, double *lambda, cons
  * about 16 MiB inside the library, which every GPU that loads it keeps until
  * exit; its device address is looked up on the first call made on each
  * device.  All calls share that array, so calls whose work overlaps on the
- * GPU (two streams, two threads) race: serialise them.  Larger fields return
- * CW_ERR_CONFIG; a field that does not settle within max_sweeps returns
- * CW_ERR_SIMULATION.  omega <= 0 takes the reference's rule. */
+ * GPU (two streams, two threads) race: serialise them.  The work runs on the
+ * library stream (cw_set_stream chooses it), which must belong to the current
+ * device (else CW_ERR_CONFIG), and the caller's buffers must be ready for
+ * that stream: synchronise whatever stream wrote them first.  Larger fields
+ * return CW_ERR_CONFIG; a field that does not settle within max_sweeps
+ * returns CW_ERR_SIMULATION.  omega <= 0 takes the reference's rule; an
+ * omega of 2 or more, or a tolerance that is not finite and above zero,
+ * returns CW_ERR_CONFIG. */
 int cw_field_relax_noalloc(double *values, const uint8_t *held, const double *lin_sink, const double *uptake,
                            const double *production, uint32_t width, uint32_t height, double dcoef, double decay,
                            double source, double omega, double tolerance, int64_t max_sweeps, int32_t inner_sweeps,

@@ -279,6 +279,47 @@ def test_the_device_bath_is_the_reference_flood():
     assert flat.bath(1)[0, 15, 20] == 0 and flat.bath(1)[0, 1, 1] == 1
 
 
+def _volume_records(gr):
+    r = seeding.Records()
+    n = int(gr.max()) + 1
+    r.type = [0] + [1] * (n - 1)
+    r.volume = list(seeding.recount(gr, n))
+    r.target = [0] + [49] * (n - 1)
+    r.lam = [0.0] + [1.0] * (n - 1)
+    return r
+
+
+def test_the_volume_bath_over_the_occupied_span_is_the_reference_flood():
+    # In a volume the union-find covers the occupied span only: medium outside
+    # it is bath, a component inside is bath when it reaches the span's border
+    # or the box's outer layer.  Four boxes where that rule could go wrong,
+    # each against the oracle's flood over the whole box.
+    n = 40
+    z, y, x = np.mgrid[0:n, 0:n, 0:n]
+    r = np.sqrt((x - 20) ** 2 + (y - 20) ** 2 + (z - 20) ** 2)
+    # (a) a hollow shell: the sealed pocket inside is not bath, all outside is
+    shell = np.where((r >= 6) & (r < 8), 1, 0).astype(np.int32)
+    # (b) a bowl (the shell's lower half) whose pocket opens upward onto the
+    # span's border layer: the pocket is bath through the layer above the span
+    cup = np.where(((r >= 6) & (r < 8)) & (z <= 20), 1, 0).astype(np.int32)
+    # (c) tissue touching one box face, so the span is clipped by the box, with
+    # a pocket sealed two pixels in from that face
+    face = np.where((x <= 8) & (y >= 10) & (y < 30) & (z >= 10) & (z < 30), 1, 0).astype(np.int32)
+    face[14:26, 14:26, 2:6] = 0
+    # (d) all medium: the span is empty, and every pixel is bath
+    empty = np.zeros((n, n, n), np.int32)
+    for k, gr in enumerate([shell, cup, face, empty]):
+        if gr.max() > 0:
+            rec = _volume_records(gr)
+        else:
+            rec = seeding.Records()
+            rec.type, rec.volume, rec.target, rec.lam = [0], [0], [0], [0.0]
+        box = cw.CpmLattice.from_grids([gr], [rec], 10.0, J3, 1, seeds=[k + 1])
+        np.testing.assert_array_equal(box.bath(0), oracle_bath(gr), err_msg=f"box {k}")
+    assert oracle_bath(shell)[20, 20, 20] == 0 and oracle_bath(shell)[0, 0, 0] == 1
+    assert oracle_bath(cup)[18, 20, 20] == 1 and oracle_bath(face)[20, 20, 3] == 0 and oracle_bath(empty).all()
+
+
 def test_an_upload_past_the_capacity_is_refused_and_the_grid_kept():
     """The upload check runs on the device: a clean upload becomes the grid,
     one holding an id past its history's capacity (or below the obstacle's

@@ -72,3 +72,37 @@ def test_a_field_past_the_fixed_scratch_is_refused():
         _lib.check(_lib.lib().cw_field_relax_noalloc(
             C.c_void_p(v.data_ptr()), C.c_void_p(h.data_ptr()), None, None, None, 1025, 1024, 1.0, 0.0, 0.0, 1.9,
             1e-6, 10, 16, None, None))
+
+
+def test_a_call_takes_no_device_memory():
+    # what the entry point is for: after a first call (which loads the
+    # library's module with its fixed array), a call of another size leaves
+    # the device's free memory exactly as it was
+    torch = pytest.importorskip("torch")
+    noalloc(200, *problem(200, 3))
+    n = 150
+    values, held, sink = problem(n, 4)
+    dev = torch.device("cuda:0")
+    v = torch.tensor(values, dtype=torch.float64, device=dev)
+    h = torch.tensor(held, dtype=torch.uint8, device=dev)
+    k = torch.tensor(sink, dtype=torch.float64, device=dev)
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info()[0]
+    sweeps, resid = C.c_int64(), C.c_double()
+    _lib.check(_lib.lib().cw_field_relax_noalloc(
+        C.c_void_p(v.data_ptr()), C.c_void_p(h.data_ptr()), C.c_void_p(k.data_ptr()), None, None, n, n, 1.0, 0.0,
+        0.0, 1.9, 1e-6, 1_000_000, 16, C.byref(sweeps), C.byref(resid)))
+    _lib.check(_lib.lib().cw_synchronize())
+    assert torch.cuda.mem_get_info()[0] == free_before
+    assert resid.value < 1e-6
+
+
+def test_a_relaxation_factor_or_tolerance_out_of_range_is_refused():
+    torch = pytest.importorskip("torch")
+    v = torch.zeros(64, dtype=torch.float64, device="cuda:0")
+    h = torch.zeros(64, dtype=torch.uint8, device="cuda:0")
+    for omega, tol in [(2.0, 1e-6), (float("nan"), 1e-6), (1.9, float("nan")), (1.9, -1.0), (1.9, 0.0)]:
+        with pytest.raises(cw.ConfigError):
+            _lib.check(_lib.lib().cw_field_relax_noalloc(
+                C.c_void_p(v.data_ptr()), C.c_void_p(h.data_ptr()), None, None, None, 8, 8, 1.0, 0.0, 0.0, omega,
+                tol, 10, 16, None, None))
