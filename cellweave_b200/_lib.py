@@ -116,6 +116,7 @@ SIGNATURES = {
     "cw_get_stream": (P, []),
     "cw_synchronize": (C.c_int, []),
     "cw_launch_count": (C.c_uint64, []),
+    "cw_test_faults": (C.c_int, [U64, I32, I32, I32]),
     "cw_lattice_create": (C.c_int, [U32, P, P, P, P, D, P]),
     "cw_lattice_destroy": (C.c_int, [P]),
     "cw_lattice_count": (C.c_int, [P, P]),

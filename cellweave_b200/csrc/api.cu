@@ -12,6 +12,9 @@ static cudaStream_t g_own_stream = nullptr;
 static cudaStream_t g_user_stream = nullptr;
 static bool g_user_set = false;
 
+static TestFaults g_faults;
+const TestFaults &test_faults() { return g_faults; }
+
 void set_error(const std::string &msg) { g_error = msg; }
 
 int fail(int code, const std::string &msg) {
@@ -111,6 +114,17 @@ int cw_synchronize(void) {
 }
 
 uint64_t cw_launch_count(void) { return cw::g_launches.load(); }
+
+int cw_test_faults(uint64_t wait_ns, int32_t withhold_block, int32_t max_rounds, int32_t skip_tma) {
+    if (wait_ns != 0 && (wait_ns < 1000000ull || wait_ns > 2000000000ull))
+        return cw::fail(CW_ERR_CONFIG, "a test's wait limit lies between 1 ms and 2 s (0: the default)");
+    if (max_rounds < 0) return cw::fail(CW_ERR_CONFIG, "a round limit is not below zero (0: the default)");
+    cw::g_faults.wait_ns = wait_ns;
+    cw::g_faults.withhold_block = withhold_block < 0 ? -1 : withhold_block;
+    cw::g_faults.max_rounds = max_rounds;
+    cw::g_faults.skip_tma = skip_tma ? 1 : 0;
+    return CW_OK;
+}
 
 }  // extern "C"
 

@@ -18,6 +18,19 @@ int cuda_fail(cudaError_t e, const char *what);
 cudaStream_t stream();
 void count_launch(uint64_t n = 1);
 
+// Failure-test settings (cw_test_faults): all off by default.  wait_ns
+// shortens every bounded device wait (grid barriers, TMA copies) from its
+// 2 s; withhold_block keeps one block of a pass from arriving at its grid
+// barriers; max_rounds caps a pass's priority rounds; skip_tma makes the
+// FP32 sweep kernels issue no copy, so that their waits run out.
+struct TestFaults {
+    unsigned long long wait_ns = 0;
+    int32_t withhold_block = -1;
+    int32_t max_rounds = 0;
+    int32_t skip_tma = 0;
+};
+const TestFaults &test_faults();
+
 #define CW_CUDA(call)                                                      \
     do {                                                                   \
         cudaError_t e_ = (call);                                           \
@@ -213,19 +226,22 @@ struct cw_lattice_s {
     uint32_t mcs = 0;
     std::vector<uint64_t> seed;
     uint2 *d_keys = nullptr;         // Philox key per history
-    // colour plans: one per colour
+    // the colouring: ncol colours of period `period` (0: the chessboard)
     int32_t ncol = 0, period = 0;
-    std::vector<cw::Plan> plans;
     int32_t nreach = 0;
     int8_t reach[3 * 124] = {0};
     double across = 1.0;
     int32_t *d_flag = nullptr;       // scratch flag / counters
     // scratch of the sublattice passes (lattice.cu): claims, pending lists, control words
     unsigned long long *claim = nullptr;  // 2 * ncells
-    uint4 *plist = nullptr;               // 2 * plist_cap attempts of 3 uint4 (lattice.cu)
+    uint4 *plist = nullptr;               // plist_cap attempts of 3 uint4 (lattice.cu)
+    uint32_t *pidx = nullptr;             // 2 * plist_cap pending-attempt indices
     int64_t plist_cap = 0;
+    int32_t *d_vplan = nullptr;           // nh + 1: the pass plan (first chunk of each history)
     uint32_t *pctl = nullptr;             // control words, then 27 pass keys per history (lattice.cu)
-    int pass_grid = 0;                    // blocks of the cooperative pass launch
+    int pass_grid = 0;                    // blocks the device holds at once in a cooperative pass launch
+    int pass_blocks = 0;                  // blocks of the pass launch
+    int64_t pass_seg = 0;                 // attempts a block's segment holds
     // records in use per history (the medium's included): cw_cells_set raises
     // it, divisions advance it on the device
     std::vector<int32_t> used;

@@ -214,7 +214,7 @@ __global__ void __launch_bounds__(32 * WWARPS, WWARPS == 8 ? 2 : 1)
                  const int4 *__restrict__ tiles, int ntiles, const int4 *__restrict__ dims,
                  const int64_t *__restrict__ off, const float *__restrict__ omega, const int32_t *done,
                  int done_stride, int nhalf, int start_colour, int zero_start, double *__restrict__ apply_c,
-                 int floor) {
+                 int floor, unsigned long long wait_ns, int skip_copies) {
     constexpr int WY = WROWS * WWARPS;  // window rows
     constexpr int STAGE = WX * WY;      // floats per array of the staged window
     extern __shared__ __align__(128) float smem[];
@@ -241,9 +241,13 @@ __global__ void __launch_bounds__(32 * WWARPS, WWARPS == 8 ? 2 : 1)
             w.omc = 1.f - omega[w.tl.x];
             const CUtensorMap *m = maps + 4 * w.tl.x;
             mbar_expect_tx(bar, (uint32_t)(boxes * STAGE * sizeof(float)));
-            if (!zero_start) tma_load_2d(smem, m + src_map, bar, w.tl.y, w.tl.z);
-            tma_load_2d(smem + STAGE, m + 2, bar, w.tl.y, w.tl.z);
-            tma_load_2d(smem + 2 * STAGE, m + 3, bar, w.tl.y, w.tl.z);
+            // skip_copies (a failure test): the bytes announced never come,
+            // and the wait below runs out
+            if (!skip_copies) {
+                if (!zero_start) tma_load_2d(smem, m + src_map, bar, w.tl.y, w.tl.z);
+                tma_load_2d(smem + STAGE, m + 2, bar, w.tl.y, w.tl.z);
+                tma_load_2d(smem + 2 * STAGE, m + 3, bar, w.tl.y, w.tl.z);
+            }
         }
         s_info[slot] = w;
     };
@@ -261,7 +265,7 @@ __global__ void __launch_bounds__(32 * WWARPS, WWARPS == 8 ? 2 : 1)
     for (int slot = 0;; slot ^= 1) {
         const WideTile info = s_info[slot];
         if (info.tl.x < 0) break;
-        if (!mbar_wait_bounded(bar, parity)) s_fail = 1;
+        if (!mbar_wait_bounded(bar, parity, wait_ns)) s_fail = 1;
         float4 d[WROWS], a[WROWS], b[WROWS];
 #pragma unroll
         for (int j = 0; j < WROWS; ++j) {
@@ -274,7 +278,7 @@ __global__ void __launch_bounds__(32 * WWARPS, WWARPS == 8 ? 2 : 1)
         if (s_fail) {
             // leave no copy in flight into this block's shared memory
             if (threadIdx.x == 0) {
-                mbar_wait_bounded(bar, parity);
+                mbar_wait_bounded(bar, parity, wait_ns);
                 atomicExch(&g_wide_wait_failed, 1);
             }
             return;
@@ -397,7 +401,8 @@ __global__ void k_sor32_half(float *__restrict__ dlt, const float *__restrict__ 
 typedef void (*TbKernel)(const float *, float *, const float *, const float *, const int4 *, const int64_t *,
                          const int32_t *, int, const float *, const int32_t *, int, int, int);
 typedef void (*WideKernel)(const CUtensorMap *, int, float *, const int4 *, int, const int4 *, const int64_t *,
-                           const float *, const int32_t *, int, int, int, int, double *, int);
+                           const float *, const int32_t *, int, int, int, int, double *, int, unsigned long long,
+                           int);
 
 TbKernel tb_kernel(int depth) {
     switch (depth) {
@@ -554,7 +559,7 @@ int Sor32::sweeps(cw_field_s *f, int n, const int32_t *done, int done_stride, fl
             wide_kernel(depth, wwarps)<<<wgrid, 32 * wwarps, wide_smem(wwarps), stream()>>>(
                 (const CUtensorMap *)maps, a == f->d32a ? 0 : 1, b, wtiles, nwtiles, f->g.d_dims, f->g.d_off, omega,
                 done, done_stride, dd, done_half & 1, done_half == 0 ? 1 : 0, apply && last ? f->c : nullptr,
-                f->floor ? 1 : 0);
+                f->floor ? 1 : 0, test_faults().wait_ns ? test_faults().wait_ns : TMA_WAIT_NS, test_faults().skip_tma);
         } else {
             tb_kernel(depth)<<<tiles.nblocks, 32 * WARPS, 0, stream()>>>(a, b, f->r32, f->inv32, f->g.d_dims,
                                                                          f->g.d_off, tiles.d_blk, f->g.nh, omega,
@@ -586,7 +591,7 @@ int sor32_wait_failed() {
     CW_CUDA(cudaMemcpyFromSymbol(&v, g_wide_wait_failed, sizeof v));
     if (v) {
         CW_CUDA(cudaMemcpyToSymbol(g_wide_wait_failed, &zero, sizeof zero));
-        return fail(CW_ERR_TIMEOUT, "an FP32 SOR block waited more than 2 s for its window's TMA copies");
+        return fail(CW_ERR_TIMEOUT, "an FP32 SOR block waited too long for its window's TMA copies");
     }
     return CW_OK;
 }

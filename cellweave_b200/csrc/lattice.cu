@@ -234,30 +234,46 @@ __global__ void k_colour_order(const uint2 *keys, int nh, int ncol, uint32_t *mc
     }
 }
 
-// The pixel of colour `colour` with index k in history dims dm; false past the end.
-// (32-bit index arithmetic: a history holds fewer than 2^32 pixels.)
-__device__ __forceinline__ bool colour_site(int4 dm, int period, int colour, uint32_t k, int &x, int &y, int &z) {
+// The pixel with index k among the pixels of colour `colour` inside the box
+// b = (x0, y0, z0, x1, y1, z1) (inclusive) of a history; false past the end.
+// Colour classes: the chessboard (x + y + z) mod 2 for period 0, else the
+// residues of x, y, z modulo the period.  (32-bit index arithmetic: a
+// history holds fewer than 2^31 pixels.)
+__device__ __forceinline__ bool colour_site_box(const int (&b)[6], int period, int colour, uint32_t k, int &x, int &y,
+                                                int &z) {
+    if (b[3] < b[0] || b[4] < b[1] || b[5] < b[2]) return false;
     if (period == 0) {
-        const uint32_t hw = ((uint32_t)dm.x + 1u) >> 1;
+        const uint32_t hw = ((uint32_t)(b[3] - b[0]) + 2u) >> 1;
+        const uint32_t wy = (uint32_t)(b[4] - b[1] + 1);
         const uint32_t row = k / hw;
-        if (row >= (uint32_t)dm.y * (uint32_t)dm.z) return false;
-        y = (int)(row % (uint32_t)dm.y);
-        z = (int)(row / (uint32_t)dm.y);
-        x = ((colour - y - z) & 1) + 2 * (int)(k - row * hw);
-        return x < dm.x;
+        if (row >= wy * (uint32_t)(b[5] - b[2] + 1)) return false;
+        y = b[1] + (int)(row % wy);
+        z = b[2] + (int)(row / wy);
+        x = b[0] + ((colour - b[0] - y - z) & 1) + 2 * (int)(k - row * hw);
+        return x <= b[3];
     }
-    int cx = colour % period, cy = (colour / period) % period, cz = colour / (period * period);
-    uint32_t nx = dm.x > cx ? (dm.x - cx + period - 1) / period : 0;
-    uint32_t ny = dm.y > cy ? (dm.y - cy + period - 1) / period : 0;
-    uint32_t nz = dm.z > cz ? (dm.z - cz + period - 1) / period : 0;
-    if (nx == 0 || ny == 0 || k >= nx * ny * nz) return false;
-    int ix = (int)(k % nx);
-    uint32_t r = k / nx;
-    int iy = (int)(r % ny), iz = (int)(r / ny);
-    x = cx + period * ix;
-    y = cy + period * iy;
-    z = cz + period * iz;
+    const int c[3] = {colour % period, (colour / period) % period, colour / (period * period)};
+    int f[3];
+    uint32_t n[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        f[a] = b[a] + ((c[a] - b[a] % period + period) % period);
+        n[a] = f[a] <= b[3 + a] ? (uint32_t)((b[3 + a] - f[a]) / period + 1) : 0u;
+    }
+    if (n[0] == 0 || n[1] == 0 || n[2] == 0 || k >= n[0] * n[1] * n[2]) return false;
+    const uint32_t r = k / n[0];
+    x = f[0] + period * (int)(k - r * n[0]);
+    y = f[1] + period * (int)(r % n[1]);
+    z = f[2] + period * (int)(r / n[1]);
     return true;
+}
+
+// The most pixels one colour holds in a box of sides (wx, wy, wz): the plan
+// of a pass gives each history that many sites.
+__host__ __device__ __forceinline__ int64_t colour_sites_max(int64_t wx, int64_t wy, int64_t wz, int period) {
+    if (wx <= 0 || wy <= 0 || wz <= 0) return 0;
+    if (period == 0) return ((wx + 1) / 2) * wy * wz;
+    return ((wx + period - 1) / period) * ((wy + period - 1) / period) * ((wz + period - 1) / period);
 }
 
 // MurmurHash3's 32-bit finaliser (Appleby): a bijection of 32-bit words, so
@@ -276,32 +292,53 @@ __device__ __forceinline__ uint32_t fmix32(uint32_t h) {
 // contact term, the surface counts' changes and the draws are fixed when the
 // pass starts; only the volume and surface records move.
 struct __align__(16) Attempt {
-    uint32_t hz, xy;   // history | z << 16, x | y << 16
+    int64_t c0;        // the history's first cell record
     int32_t src, dst;  // source and copied ids
     uint32_t prio;     // the pass priority
     int32_t dsurf;     // surface changes of source and copied cell (int16 each)
     uint32_t u0, u1;   // the acceptance draw's words
-    double contact;    // contact Delta-H (cpm.rs:851-876)
-    double pad;
+    int64_t gi;        // the pixel in the batch's flat order
+    union {
+        double contact;  // contact Delta-H (cpm.rs:851-876)
+        uint2 where;     // until the contact is taken: history | z << 16, x | y << 16
+    };
 };
 static_assert(sizeof(Attempt) == 48, "an attempt is three 16-byte words");
 
-// Scratch of the passes: two claim words per cell (by round parity), two
-// lists of pending attempts (a segment of `seg` entries per block), and
-// control words.
+constexpr int PT = 1024;           // threads of a pass block; one block per SM
+constexpr int PEND_SMEM = 4096;    // pending attempts a block lists in shared memory (else in its global segment)
+constexpr int PLAN_SMEM = 1024;    // pass plans of up to 1023 histories sit in shared memory
+constexpr int ILP = 2;             // attempts a thread carries at once through a round
+constexpr int MAX_ROUNDS = 256;
+constexpr uint32_t ROUND_SPAN = MAX_ROUNDS + 2;  // claim tags one pass may use
+// passes before the claim tags would overflow 32 bits: the pass that reaches
+// it clears the claims and starts the count again
+constexpr uint32_t SEQ_LIMIT = 0xFFFFFFFFu / ROUND_SPAN - 1u;
+constexpr unsigned long long BARRIER_NS = 2000000000ull;
+
+// Scratch of the passes.  Claims: two words per cell (by round parity), each
+// (tag << 32 | priority) with the tag (pass sequence x ROUND_SPAN + round)
+// rising from pass to pass, so that old claims lose to new ones and nothing
+// needs clearing.  Attempts: a segment of `seg` per block.  Pending lists:
+// indices into the block's segment, in shared memory or, for a block with
+// more than PEND_SMEM attempts, in two segments of `seg` in `idx`.
 struct PassScratch {
     unsigned long long *claim[2];  // ncells each
-    Attempt *list[2];
-    uint32_t seg;                  // entries per block segment
-    uint32_t *ctl;                 // CTL_* below, then the pass keys (history x pass)
+    Attempt *list;
+    uint32_t *idx;
+    uint32_t seg;
+    int64_t ncells;
+    uint32_t *ctl;                 // CTL_* below, then the pass keys (history x colour)
+    const int32_t *vplan;          // nh + 1: each history's first chunk of PT sites; vplan[nh]: all chunks
+    unsigned long long barrier_ns; // a grid barrier's wait limit
+    int32_t withhold;              // a block that never arrives at a barrier (failure tests; -1: none)
+    int32_t max_rounds;            // rounds before a pass gives up (CW_ERR_SIMULATION)
 };
-// control words: list counts and the barrier's arrivals (cleared before each
-// pass) share a line; the barrier's generation (only ever compared with
-// itself) another; the error and round records a third; then the pass keys
-enum { CTL_COUNT = 0, CTL_BAR = 3, CTL_GEN = 32, CTL_ERR = 48, CTL_ROUNDS = 49, CTL_KEYS = 64 };
-constexpr int MAX_ROUNDS = 256;
-constexpr int PLAN_SMEM = 1024;  // block plans of up to 1023 histories sit in shared memory
-constexpr unsigned long long BARRIER_NS = 2000000000ull;
+// control words: list counts and the barrier's arrivals share a line (both
+// left at zero when a pass ends); the barrier's generation (only ever
+// compared with itself) another; the error, round and sequence records a
+// third; then the pass keys
+enum { CTL_COUNT = 0, CTL_BAR = 3, CTL_GEN = 32, CTL_ERR = 48, CTL_ROUNDS = 49, CTL_SEQ = 50, CTL_KEYS = 64 };
 
 __device__ __forceinline__ uint64_t global_ns() {
     uint64_t t;
@@ -316,25 +353,31 @@ __device__ __forceinline__ uint32_t ld_acquire_gpu(const uint32_t *p) {
 }
 
 // A barrier over the whole (co-resident, cooperatively launched) grid whose
-// wait gives up after BARRIER_NS; false then, on every thread of the block.
-__device__ __forceinline__ bool grid_barrier(uint32_t *ctl, int *s_ok) {
+// wait gives up after S.barrier_ns; false then, on every thread of the block.
+// The block S.withhold (a failure test) never arrives and returns false.
+__device__ __forceinline__ bool grid_barrier(const PassScratch &S, int *s_ok) {
     __syncthreads();
     if (threadIdx.x == 0) {
-        const uint32_t g0 = ld_acquire_gpu(ctl + CTL_GEN);
         int ok = 1;
-        __threadfence();
-        if (atomicAdd(ctl + CTL_BAR, 1u) == gridDim.x - 1) {
-            ctl[CTL_BAR] = 0u;
-            __threadfence();
-            atomicAdd(ctl + CTL_GEN, 1u);
+        if ((int)blockIdx.x == S.withhold) {
+            ok = 0;
         } else {
-            uint32_t spins = 0;
-            uint64_t t0 = 0;
-            while (ld_acquire_gpu(ctl + CTL_GEN) == g0) {
-                if ((++spins & 1023u) == 0) {  // the clock only now and then
-                    const uint64_t t = global_ns();
-                    if (t0 == 0) t0 = t;
-                    else if (t - t0 > BARRIER_NS) { ok = 0; break; }
+            uint32_t *ctl = S.ctl;
+            const uint32_t g0 = ld_acquire_gpu(ctl + CTL_GEN);
+            __threadfence();
+            if (atomicAdd(ctl + CTL_BAR, 1u) == gridDim.x - 1) {
+                ctl[CTL_BAR] = 0u;
+                __threadfence();
+                atomicAdd(ctl + CTL_GEN, 1u);
+            } else {
+                uint32_t spins = 0;
+                uint64_t t0 = 0;
+                while (ld_acquire_gpu(ctl + CTL_GEN) == g0) {
+                    if ((++spins & 255u) == 0) {  // the clock only now and then
+                        const uint64_t t = global_ns();
+                        if (t0 == 0) t0 = t;
+                        else if (t - t0 > S.barrier_ns) { ok = 0; break; }
+                    }
                 }
             }
         }
@@ -345,16 +388,27 @@ __device__ __forceinline__ bool grid_barrier(uint32_t *ctl, int *s_ok) {
     return *s_ok != 0;
 }
 
-// Append `a` (where `take`) to this block's segment of `list`, one
-// shared-memory atomic per warp; *s_n counts the segment's entries.
-__device__ __forceinline__ void seg_append(Attempt *list, uint32_t seg, uint32_t *s_n, bool take,
-                                           const Attempt &a) {
+// Append `v` (where `take`) to `list` at a slot counted by *s_n, one
+// shared-memory atomic per warp.
+template <typename V>
+__device__ __forceinline__ void warp_append(V *list, uint32_t *s_n, bool take, const V &v) {
     const int lane = threadIdx.x & 31;
     const unsigned m = __ballot_sync(0xffffffffu, take);
     uint32_t base = 0;
     if (lane == 0 && m) base = atomicAdd(s_n, (uint32_t)__popc(m));
     base = __shfl_sync(0xffffffffu, base, 0);
-    if (take) list[(size_t)blockIdx.x * seg + base + __popc(m & ((1u << lane) - 1u))] = a;
+    if (take) list[base + __popc(m & ((1u << lane) - 1u))] = v;
+}
+
+// The history whose chunks hold chunk vb (plan: nh + 1 prefix of chunks).
+__device__ __forceinline__ int plan_find(const int32_t *plan, int nh, int vb) {
+    int lo = 0, hi = nh - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (plan[mid] <= vb) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
 }
 
 // occupied_span (cpm.rs:774-793) of every volume history, at the start of a
@@ -415,62 +469,99 @@ __global__ void k_span_finish(int32_t *span, const int4 *dims, int nh) {
     }
 }
 
-__device__ __forceinline__ bool in_span(const int32_t *span, int h, int4 dm, int x, int y, int z) {
-    if (!span || dm.z <= 1) return true;
-    const int32_t *s = span + 6 * h;
-    return x >= s[0] && x <= s[3] && y >= s[1] && y <= s[4] && z >= s[2] && z <= s[5];
+// The pass plan of every volume history from its span: the chunks of PT sites
+// the largest colour of the span holds, as a prefix over the histories
+// (vplan[nh] = all of them).  One block: each thread sums a run of
+// histories, the runs' totals are scanned, then each run is written.
+__global__ void __launch_bounds__(1024) k_pass_plan(const int32_t *span, int nh, int period, int32_t *vplan) {
+    __shared__ int32_t s_run[1024];
+    const int per = (nh + blockDim.x - 1) / blockDim.x;
+    const int h0 = threadIdx.x * per, h1 = min(h0 + per, nh);
+    auto chunks = [&](int h) -> int32_t {
+        const int32_t *s = span + 6 * h;
+        const int64_t n = colour_sites_max(s[3] - s[0] + 1, s[4] - s[1] + 1, s[5] - s[2] + 1, period);
+        return (int32_t)((n + PT - 1) / PT);
+    };
+    int32_t tot = 0;
+    for (int h = h0; h < h1; ++h) tot += chunks(h);
+    s_run[threadIdx.x] = tot;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int32_t acc = 0;
+        for (int t = 0; t < (int)blockDim.x; ++t) {
+            const int32_t v = s_run[t];
+            s_run[t] = acc;
+            acc += v;
+        }
+        vplan[nh] = acc;
+    }
+    __syncthreads();
+    int32_t acc = s_run[threadIdx.x];
+    for (int h = h0; h < h1; ++h) {
+        vplan[h] = acc;
+        acc += chunks(h);
+    }
 }
 
 // One sublattice pass: one copy attempt at every pixel of this pass's colour
-// (the reference's try_flip, cpm.rs:797-838), the attempts ordered by a
+// (the reference's try_flip, cpm.rs:797-838) inside each history's box (a
+// volume's occupied span, a plane's whole box), the attempts ordered by a
 // per-pass priority and run as that sequence would run them.  The pixels of
 // a colour lie outside one another's reach, so two attempts meet only
-// through the records of a cell they both involve (volume, surface).  First
-// every attempt that copies (source and copied ids differ, neither the
-// obstacle) claims its cells other than the medium with its priority and
-// takes down what the pass cannot change; in each round an attempt holding
-// the claim on all its cells runs against the live records, the others claim
-// again for the next round.  An attempt runs only after every
-// higher-priority attempt sharing a cell with it, which is the sequence in
-// decreasing priority, whatever the thread schedule.  Each block keeps the
-// attempts it found in its own list segment; the blocks meet at a grid
-// barrier between rounds and count what is left in one word.
-__global__ void __launch_bounds__(T) k_cpm_pass(LatView L, Tables tabs, const int32_t *blk, int nh, int nvb,
-                                                const int32_t *perm, int pass, const uint32_t *mcs_cur,
-                                                PassScratch S) {
+// through the records of a cell they both involve (volume, surface).
+//
+// Propose: every attempt that copies (source and copied ids differ, neither
+// the obstacle) claims its cells other than the medium with its priority and
+// is packed into its block's segment; then the terms the pass cannot change
+// (contact, surface counts) are taken over the packed attempts.  Rounds: an
+// attempt holding the claim on all its cells runs against the live records;
+// the others claim again for the next round.  An attempt runs only after
+// every higher-priority attempt sharing a cell with it, which is the
+// sequence in decreasing priority, whatever the thread schedule.  The blocks
+// meet at a grid barrier between rounds and count what is left in one word;
+// each block lists its pending attempts by index, in shared memory when they
+// fit.
+__global__ void __launch_bounds__(PT, 1) k_cpm_pass(LatView L, Tables tabs, int nh, const int32_t *perm, int pass,
+                                                    const uint32_t *mcs_cur, PassScratch S) {
     __shared__ double sJ[64];
     __shared__ int8_t sreach[3 * 124];
     __shared__ int s_ok;
     __shared__ uint32_t s_n[2];
-    __shared__ int32_t s_blk[PLAN_SMEM];
+    __shared__ int32_t s_plan[PLAN_SMEM];
+    __shared__ uint32_t s_pend[2][PEND_SMEM];
     for (int i = threadIdx.x; i < L.K * L.K; i += blockDim.x) sJ[i] = tabs.J[i];
     for (int i = threadIdx.x; i < 3 * L.nreach; i += blockDim.x) sreach[i] = tabs.reach[i];
-    // the block plan in shared memory when it fits (every thread walks it)
     const bool plan_shared = nh + 1 <= PLAN_SMEM;
     if (plan_shared)
-        for (int i = threadIdx.x; i <= nh; i += blockDim.x) s_blk[i] = blk[i];
+        for (int i = threadIdx.x; i <= nh; i += blockDim.x) s_plan[i] = S.vplan[i];
     if (threadIdx.x == 0) s_n[0] = s_n[1] = 0u;
     __syncthreads();
-    const int32_t *plan = plan_shared ? s_blk : blk;
+    const int32_t *plan = plan_shared ? s_plan : S.vplan;
+    const int nvb = plan[nh];
     const uint32_t mcs = *mcs_cur;
+    const uint32_t seq = S.ctl[CTL_SEQ];
+    const uint32_t tag0 = seq * ROUND_SPAN;  // round r claims with tag tag0 + r
     const uint32_t *pass_key = S.ctl + CTL_KEYS;
+    Attempt *mine = S.list + (size_t)blockIdx.x * S.seg;
     // ---- propose and claim (round 1's claims); a block's chunks come in
     // increasing order, so its history only moves forward
-    int h = blockIdx.x < nvb ? plan_history(blk, nh, blockIdx.x) : 0;  // (global: it reads through __ldg)
+    int h = blockIdx.x < nvb ? plan_find(plan, nh, blockIdx.x) : 0;
     for (int vb = blockIdx.x; vb < nvb; vb += gridDim.x) {
         while (h + 1 < nh && plan[h + 1] <= vb) ++h;
         const int4 dm = L.dims[h];
+        int box[6] = {0, 0, 0, dm.x - 1, dm.y - 1, dm.z - 1};
+        if (L.span && dm.z > 1)
+#pragma unroll
+            for (int a = 0; a < 6; ++a) box[a] = L.span[6 * h + a];
         const int colour = perm[h * L.ncol + pass];
-        const uint32_t k = (uint32_t)(vb - plan[h]) * blockDim.x + threadIdx.x;
-        const int64_t c0 = L.cell_off[h];
+        const uint32_t k = (uint32_t)(vb - plan[h]) * PT + threadIdx.x;
         const int32_t *g = L.grid + L.off[h];
         int x = 0, y = 0, z = 0;
         bool copies = false;
         Attempt a;
-        // in a volume, the pixels of the occupied span only (cpm.rs:748-763)
-        if (colour_site(dm, L.period, colour, k, x, y, z) && in_span(L.span, h, dm, x, y, z)) {
+        if (colour_site_box(box, L.period, colour, k, x, y, z)) {
             const int64_t i = ((int64_t)z * dm.y + y) * dm.x + x;
-            const int32_t src = g[i];
+            const int32_t src = __ldg(g + i);
             // a pixel whose copy neighbours all hold its own id cannot copy: no draw needed
             bool edge = false;
             int nvn = 0;
@@ -482,7 +573,7 @@ __global__ void __launch_bounds__(T) k_cpm_pass(LatView L, Tables tabs, const in
                 nvn = vn.count();
                 int32_t nb[6];
 #pragma unroll
-                for (int q = 0; q < 6; ++q) nb[q] = vn.has(q) ? g[i + vn.step(q)] : src;
+                for (int q = 0; q < 6; ++q) nb[q] = vn.has(q) ? __ldg(g + i + vn.step(q)) : src;
 #pragma unroll
                 for (int q = 0; q < 6; ++q) edge |= nb[q] != src;
             } else {
@@ -490,7 +581,8 @@ __global__ void __launch_bounds__(T) k_cpm_pass(LatView L, Tables tabs, const in
                 nvn = mo.count();
                 int32_t nb[27];
 #pragma unroll
-                for (int q = 0; q < 27; ++q) nb[q] = q != 13 && ((mo.mask >> q) & 1u) ? g[i + mo.step(q)] : src;
+                for (int q = 0; q < 27; ++q)
+                    nb[q] = q != 13 && ((mo.mask >> q) & 1u) ? __ldg(g + i + mo.step(q)) : src;
 #pragma unroll
                 for (int q = 0; q < 27; ++q) edge |= nb[q] != src;
             }
@@ -505,59 +597,67 @@ __global__ void __launch_bounds__(T) k_cpm_pass(LatView L, Tables tabs, const in
                 const uint2 key = L.keys[h];
                 const uint4 r = philox((uint32_t)i, mcs, 0u, 0u, key.x, key.y);
                 const int j = (int)(((uint64_t)r.x * (uint64_t)nvn) >> 32);
-                const int32_t dst = g[i + (L.copy_moore ? mo.nth(j) : vn.nth(j))];
+                const int32_t dst = __ldg(g + i + (L.copy_moore ? mo.nth(j) : vn.nth(j)));
                 if (src != dst && dst != OBST) {
                     copies = true;
                     const uint32_t prio = fmix32((uint32_t)i ^ pass_key[h * L.ncol + pass]);
-                    const unsigned long long claim = (1ull << 32) | prio;
+                    const int64_t c0 = L.cell_off[h];
+                    const unsigned long long claim = ((unsigned long long)(tag0 + 1u) << 32) | prio;
                     if (src > 0) atomicMax(S.claim[1] + c0 + src, claim);
                     if (dst > 0) atomicMax(S.claim[1] + c0 + dst, claim);
-                    a.hz = (uint32_t)h | ((uint32_t)z << 16);
-                    a.xy = (uint32_t)x | ((uint32_t)y << 16);
+                    a.c0 = c0;
                     a.src = src;
                     a.dst = dst;
                     a.prio = prio;
+                    a.dsurf = 0;
                     a.u0 = r.y;
                     a.u1 = r.z;
+                    a.gi = L.off[h] + i;
+                    a.where = make_uint2((uint32_t)h | ((uint32_t)z << 16), (uint32_t)x | ((uint32_t)y << 16));
                 }
             }
         }
-        seg_append(S.list[0], S.seg, &s_n[0], copies, a);
+        warp_append(mine, &s_n[0], copies, a);
     }
     __syncthreads();
+    const uint32_t n = s_n[0];
     // ---- what the pass cannot change, over the block's attempts packed
     // together (a contact term reads no pixel of the colour, which only the
     // rounds write)
-    {
-        Attempt *mine = S.list[0] + (size_t)blockIdx.x * S.seg;
-        const uint32_t n = s_n[0];
-        for (uint32_t e = threadIdx.x; e < n; e += blockDim.x) {
-            Attempt &a = mine[e];
-            const int h = (int)(a.hz & 0xFFFFu);
-            const int x = (int)(a.xy & 0xFFFFu), y = (int)(a.xy >> 16), z = (int)(a.hz >> 16);
-            const int4 dm = L.dims[h];
-            const int64_t c0 = L.cell_off[h], cap = L.cell_off[h + 1] - c0;
-            const int64_t i = ((int64_t)z * dm.y + y) * dm.x + x;
-            const int32_t *g = L.grid + L.off[h];
-            const Vn vn = vn_of(dm, x, y, z);
-            double num;
-            a.contact = contact_delta(g, dm, x, y, z, a.src, a.dst, L.type + c0, cap, sJ, L.K, sreach, L.nreach,
-                                      L.across, i, vn, &num);
-            int32_t ds = 0, dd = 0;
-            if (L.surface_on) surface_change(g, i, vn, a.src, a.dst, ds, dd);
-            a.dsurf = (int32_t)((uint32_t)(uint16_t)(int16_t)ds | ((uint32_t)(uint16_t)(int16_t)dd << 16));
-        }
+    for (uint32_t e = threadIdx.x; e < n; e += blockDim.x) {
+        Attempt &a = mine[e];
+        const uint2 wh = a.where;
+        const int hh = (int)(wh.x & 0xFFFFu);
+        const int x = (int)(wh.y & 0xFFFFu), y = (int)(wh.y >> 16), z = (int)(wh.x >> 16);
+        const int4 dm = L.dims[hh];
+        const int64_t cap = L.cell_off[hh + 1] - a.c0;
+        const int64_t i = ((int64_t)z * dm.y + y) * dm.x + x;
+        const int32_t *g = L.grid + L.off[hh];
+        const Vn vn = vn_of(dm, x, y, z);
+        double num;
+        const double contact = contact_delta(g, dm, x, y, z, a.src, a.dst, L.type + a.c0, cap, sJ, L.K, sreach,
+                                             L.nreach, L.across, i, vn, &num);
+        int32_t ds = 0, dd = 0;
+        if (L.surface_on) surface_change(g, i, vn, a.src, a.dst, ds, dd);
+        a.contact = contact;
+        a.dsurf = (int32_t)((uint32_t)(uint16_t)(int16_t)ds | ((uint32_t)(uint16_t)(int16_t)dd << 16));
     }
-    if (threadIdx.x == 0 && s_n[0]) atomicAdd(S.ctl + CTL_COUNT + 0, s_n[0]);
-    if (!grid_barrier(S.ctl, &s_ok)) {
+    if (threadIdx.x == 0 && n) atomicAdd(S.ctl + CTL_COUNT + 0, n);
+    uint32_t *pend[2] = {s_pend[0], s_pend[1]};
+    if (n > PEND_SMEM) {
+        pend[0] = S.idx + (size_t)blockIdx.x * 2 * S.seg;
+        pend[1] = pend[0] + S.seg;
+    }
+    if (!grid_barrier(S, &s_ok)) {
         if (threadIdx.x == 0) atomicExch(S.ctl + CTL_ERR, 1u);
         return;
     }
     // ---- rounds
+    uint32_t npend = n;  // this block's attempts entering the round
     for (int r = 1;; ++r) {
-        const uint32_t left = *(volatile uint32_t *)(S.ctl + CTL_COUNT + (r - 1) % 3);
+        const uint32_t left = __ldcg(S.ctl + CTL_COUNT + (r - 1) % 3);
         if (left == 0) break;
-        if (r > MAX_ROUNDS) {
+        if (r > S.max_rounds) {
             if (blockIdx.x == 0 && threadIdx.x == 0) atomicExch(S.ctl + CTL_ERR, 2u);
             break;
         }
@@ -565,58 +665,95 @@ __global__ void __launch_bounds__(T) k_cpm_pass(LatView L, Tables tabs, const in
             S.ctl[CTL_COUNT + (r + 1) % 3] = 0u;  // round r + 1's count; last read as round r - 1's
             atomicMax(S.ctl + CTL_ROUNDS, (uint32_t)r);
         }
-        const uint32_t mine_n = s_n[(r - 1) & 1];
-        __syncthreads();  // every thread has read its count before it is reset
         if (threadIdx.x == 0) s_n[r & 1] = 0u;
         __syncthreads();
-        const Attempt *in = S.list[(r - 1) & 1] + (size_t)blockIdx.x * S.seg;
-        const unsigned long long *mine = S.claim[r & 1];
+        const unsigned long long *cl = S.claim[r & 1];
         unsigned long long *next = S.claim[(r + 1) & 1];
-        for (uint32_t e0 = 0; e0 < mine_n; e0 += blockDim.x) {
-            const uint32_t e = e0 + threadIdx.x;
-            bool again = false;
-            Attempt a;
-            if (e < mine_n) {
-                a = in[e];
-                const int h = (int)(a.hz & 0xFFFFu);
-                const int64_t c0 = L.cell_off[h];
-                const unsigned long long key = ((unsigned long long)r << 32) | a.prio;
-                const bool win = (a.src <= 0 || mine[c0 + a.src] == key) && (a.dst <= 0 || mine[c0 + a.dst] == key);
-                if (win) {
-                    const int32_t ds = (int32_t)(int16_t)(a.dsurf & 0xFFFF), dd = (int32_t)(int16_t)(a.dsurf >> 16);
-                    double delta = a.contact + volume_delta(L.volume, L.target, L.lambda, c0, a.src, a.dst);
-                    if (L.surface_on) delta += surface_delta(L.surface, L.tsurf, L.lsurf, c0, a.src, a.dst, ds, dd);
-                    bool accept = delta <= 0.0;
-                    if (!accept) accept = u01(a.u0, a.u1) < own_exp(-delta / L.temperature);
-                    if (accept) {
-                        const int4 dm = L.dims[h];
-                        const int x = (int)(a.xy & 0xFFFFu), y = (int)(a.xy >> 16), z = (int)(a.hz >> 16);
-                        L.grid[L.off[h] + ((int64_t)z * dm.y + y) * dm.x + x] = a.dst;
-                        // the records: its cells are its own this round
-                        if (a.src != 0) L.volume[c0 + a.src] -= 1;
-                        if (a.dst != 0) L.volume[c0 + a.dst] += 1;
-                        if (L.surface_on) {
-                            if (a.src > 0) L.surface[c0 + a.src] += ds;
-                            if (a.dst > 0) L.surface[c0 + a.dst] += dd;
-                        }
-                    }
-                } else {
-                    const unsigned long long claim = ((unsigned long long)(r + 1) << 32) | a.prio;
-                    if (a.src > 0) atomicMax(next + c0 + a.src, claim);
-                    if (a.dst > 0) atomicMax(next + c0 + a.dst, claim);
-                    again = true;
+        const uint32_t *pin = pend[(r - 1) & 1];
+        uint32_t *pout = pend[r & 1];
+        const unsigned long long key_tag = (unsigned long long)(tag0 + (uint32_t)r) << 32;
+        const unsigned long long next_tag = (unsigned long long)(tag0 + (uint32_t)r + 1u) << 32;
+        for (uint32_t e0 = 0; e0 < npend; e0 += ILP * PT) {
+            uint32_t id[ILP];
+            bool has[ILP], win[ILP];
+            Attempt a[ILP];
+            unsigned long long cs[ILP], cd[ILP];
+#pragma unroll
+            for (int j = 0; j < ILP; ++j) {
+                const uint32_t e = e0 + (uint32_t)j * PT + threadIdx.x;
+                has[j] = e < npend;
+                id[j] = has[j] ? (r == 1 ? e : pin[e]) : 0u;
+            }
+#pragma unroll
+            for (int j = 0; j < ILP; ++j)
+                if (has[j]) a[j] = mine[id[j]];
+#pragma unroll
+            for (int j = 0; j < ILP; ++j) {
+                cs[j] = cd[j] = 0ull;
+                if (has[j]) {
+                    if (a[j].src > 0) cs[j] = __ldcg(cl + a[j].c0 + a[j].src);
+                    if (a[j].dst > 0) cd[j] = __ldcg(cl + a[j].c0 + a[j].dst);
                 }
             }
-            seg_append(S.list[r & 1], S.seg, &s_n[r & 1], again, a);
+#pragma unroll
+            for (int j = 0; j < ILP; ++j) {
+                win[j] = false;
+                if (has[j]) {
+                    const unsigned long long key = key_tag | a[j].prio;
+                    win[j] = (a[j].src <= 0 || cs[j] == key) && (a[j].dst <= 0 || cd[j] == key);
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < ILP; ++j) {
+                bool again = false;
+                if (win[j]) {
+                    const Attempt &t = a[j];
+                    const int32_t ds = (int32_t)(int16_t)(t.dsurf & 0xFFFF), dd = (int32_t)(int16_t)(t.dsurf >> 16);
+                    double delta = t.contact + volume_delta(L.volume, L.target, L.lambda, t.c0, t.src, t.dst);
+                    if (L.surface_on) delta += surface_delta(L.surface, L.tsurf, L.lsurf, t.c0, t.src, t.dst, ds, dd);
+                    bool accept = delta <= 0.0;
+                    if (!accept) accept = u01(t.u0, t.u1) < own_exp(-delta / L.temperature);
+                    if (accept) {
+                        L.grid[t.gi] = t.dst;
+                        // the records: its cells are its own this round
+                        if (t.src != 0) L.volume[t.c0 + t.src] -= 1;
+                        if (t.dst != 0) L.volume[t.c0 + t.dst] += 1;
+                        if (L.surface_on) {
+                            if (t.src > 0) L.surface[t.c0 + t.src] += ds;
+                            if (t.dst > 0) L.surface[t.c0 + t.dst] += dd;
+                        }
+                    }
+                } else if (has[j]) {
+                    const unsigned long long claim = next_tag | a[j].prio;
+                    if (a[j].src > 0) atomicMax(next + a[j].c0 + a[j].src, claim);
+                    if (a[j].dst > 0) atomicMax(next + a[j].c0 + a[j].dst, claim);
+                    again = true;
+                }
+                warp_append(pout, &s_n[r & 1], again, id[j]);
+            }
         }
         __syncthreads();
-        if (threadIdx.x == 0 && s_n[r & 1]) atomicAdd(S.ctl + CTL_COUNT + r % 3, s_n[r & 1]);
-        if (!grid_barrier(S.ctl, &s_ok)) {
+        npend = s_n[r & 1];
+        if (threadIdx.x == 0 && npend) atomicAdd(S.ctl + CTL_COUNT + r % 3, npend);
+        if (!grid_barrier(S, &s_ok)) {
             if (threadIdx.x == 0) atomicExch(S.ctl + CTL_ERR, 1u);
             return;
         }
     }
+    // ---- the pass is over on every block: the counts go back to zero for the
+    // next pass (no block reads them again), the sequence advances; at the
+    // sequence's limit the claims are cleared and it starts again
+    if (seq + 1u >= SEQ_LIMIT) {
+        for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < S.ncells;
+             c += (int64_t)gridDim.x * blockDim.x)
+            S.claim[0][c] = S.claim[1][c] = 0ull;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        S.ctl[CTL_COUNT + 0] = S.ctl[CTL_COUNT + 1] = S.ctl[CTL_COUNT + 2] = 0u;
+        S.ctl[CTL_SEQ] = seq + 1u >= SEQ_LIMIT ? 0u : seq + 1u;
+    }
 }
+
 
 // The first staged pixel of histories h0..h1 (n sites from `a`) whose id is
 // below -1 or at least its history's cell capacity, as an offset from `a`.
@@ -742,41 +879,47 @@ int cw_lattice_s::build_plans() {
         period = r + 1;
         ncol = volume ? period * period * period : period * period;
     }
-    for (auto &p : plans) p.release();
-    plans.assign(1, Plan());
-    std::vector<int64_t> per(g.nh, 0);
+    // the pass plan: chunks of PT sites, as many as the largest colour of each
+    // history's box holds (a plane's plan; in a volume a bound of the plan the
+    // device takes from the occupied span every Monte Carlo step)
+    std::vector<int32_t> vp(g.nh + 1, 0);
     for (uint32_t k = 0; k < g.nh; ++k) {
-        if (period == 0) {
-            per[k] = (int64_t)((g.w[k] + 1) / 2) * g.h[k] * g.d[k];
-        } else {
-            int64_t nx = (g.w[k] + period - 1) / period, ny = (g.h[k] + period - 1) / period;
-            int64_t nz = volume ? (g.d[k] + period - 1) / period : 1;
-            per[k] = nx * ny * nz;  // the largest colour class
-        }
+        const int64_t sites = colour_sites_max(g.w[k], g.h[k], g.d[k], period);
+        vp[k + 1] = vp[k] + (int32_t)((sites + PT - 1) / PT);
     }
-    int rc = plans[0].build(per, T);
-    if (rc != CW_OK) return rc;
+    int rc;
     if (pass_grid == 0) {
         int per_sm = 0, dev = 0, nsm = 0;
-        CW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)k_cpm_pass, T, 0));
+        CW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)k_cpm_pass, PT, 0));
         CW_CUDA(cudaGetDevice(&dev));
         CW_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
         pass_grid = std::max(1, per_sm * nsm);
     }
-    // the pass scratch: a block's list segment holds every pixel of the
-    // colour it visits, (blocks of the plan / blocks launched, rounded up) x T
-    const int grid = std::min(plans[0].nblocks, pass_grid);
-    const int64_t need = (int64_t)grid * ((plans[0].nblocks + grid - 1) / grid) * T;
+    // the pass scratch: a block's segment holds every site of the chunks it
+    // visits, (chunks / blocks launched, rounded up) x PT
+    const int32_t nvb = vp[g.nh];
+    pass_blocks = std::max(1, std::min(nvb, pass_grid));
+    pass_seg = (int64_t)((nvb + pass_blocks - 1) / pass_blocks) * PT;
+    const int64_t need = (int64_t)pass_blocks * pass_seg;
     if (need > plist_cap) {
         dfree(plist);
-        if ((rc = dalloc(&plist, 2 * 3 * (size_t)need)) != CW_OK) return rc;  // an attempt is 3 uint4
+        dfree(pidx);
+        plist_cap = 0;
+        if ((rc = dalloc(&plist, 3 * (size_t)need)) != CW_OK) return rc;  // an attempt is 3 uint4
+        if ((rc = dalloc(&pidx, 2 * (size_t)need)) != CW_OK) return rc;   // two pending lists
         plist_cap = need;
     }
-    if (!claim && (rc = dalloc(&claim, 2 * (size_t)ncells)) != CW_OK) return rc;
+    if (!d_vplan && (rc = dalloc(&d_vplan, (size_t)g.nh + 1)) != CW_OK) return rc;
+    CW_CUDA(cudaMemcpyAsync(d_vplan, vp.data(), sizeof(int32_t) * (g.nh + 1), cudaMemcpyHostToDevice, stream()));
+    if (!claim) {
+        if ((rc = dalloc(&claim, 2 * (size_t)ncells)) != CW_OK) return rc;
+        CW_CUDA(cudaMemsetAsync(claim, 0, sizeof(unsigned long long) * 2 * (size_t)ncells, stream()));
+    }
     if (!pctl) {
         if ((rc = dalloc(&pctl, CTL_KEYS + 27 * (size_t)g.nh)) != CW_OK) return rc;
         CW_CUDA(cudaMemsetAsync(pctl, 0, sizeof(uint32_t) * (CTL_KEYS + 27 * (size_t)g.nh), stream()));
     }
+    CW_CUDA(cudaStreamSynchronize(stream()));
     return CW_OK;
 }
 
@@ -870,6 +1013,8 @@ int lattice_span_enqueue(cw_lattice_s *l) {
     CW_LAUNCHED();
     k_span_finish<<<(nh + 127) / 128, 128, 0, stream()>>>(l->d_span, l->g.d_dims, nh);
     CW_LAUNCHED();
+    k_pass_plan<<<1, 1024, 0, stream()>>>(l->d_span, nh, l->period, l->d_vplan);
+    CW_LAUNCHED();
     return CW_OK;
 }
 
@@ -896,26 +1041,26 @@ int lattice_subsweep(cw_lattice_s *l) {
     PassScratch S;
     S.claim[0] = l->claim;
     S.claim[1] = l->claim + l->ncells;
-    S.list[0] = (Attempt *)l->plist;
-    S.list[1] = (Attempt *)l->plist + l->plist_cap;
+    S.list = (Attempt *)l->plist;
+    S.idx = l->pidx;
+    S.seg = (uint32_t)l->pass_seg;
+    S.ncells = l->ncells;
     S.ctl = l->pctl;
-    int nvb = l->plans[0].nblocks;
-    const int grid = std::min(nvb, l->pass_grid);
-    S.seg = (uint32_t)((nvb + grid - 1) / grid) * T;
-    const int32_t *blk = l->plans[0].d_blk;
+    S.vplan = l->d_vplan;
+    const TestFaults &tf = test_faults();
+    S.barrier_ns = tf.wait_ns ? tf.wait_ns : BARRIER_NS;
+    S.withhold = tf.withhold_block;
+    S.max_rounds = tf.max_rounds > 0 ? tf.max_rounds : MAX_ROUNDS;
     int nh = (int)l->g.nh;
     const uint32_t *cur = d.mcs + 1;
     for (int q = 0; q < l->ncol; ++q) {
-        CW_CUDA(cudaMemsetAsync(l->claim, 0, sizeof(unsigned long long) * 2 * (size_t)l->ncells, stream()));
-        // the three list counts and the barrier's arrivals
-        CW_CUDA(cudaMemsetAsync(l->pctl + CTL_COUNT, 0, sizeof(uint32_t) * 4, stream()));
-        void *args[] = {&v, &t, (void *)&blk, &nh, &nvb, &d.perm, &q, (void *)&cur, &S};
+        void *args[] = {&v, &t, &nh, &d.perm, &q, (void *)&cur, &S};
         cudaLaunchConfig_t cfg = {};
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeCooperative;
         attr[0].val.cooperative = 1;
-        cfg.gridDim = dim3((unsigned)grid);
-        cfg.blockDim = dim3(T);
+        cfg.gridDim = dim3((unsigned)l->pass_blocks);
+        cfg.blockDim = dim3(PT);
         cfg.dynamicSmemBytes = 0;
         cfg.stream = stream();
         cfg.attrs = attr;
@@ -929,12 +1074,15 @@ int lattice_subsweep(cw_lattice_s *l) {
 // CW_ERR_TIMEOUT (or CW_ERR_SIMULATION) if a pass gave up since the last
 // call: a grid barrier that waited too long, or more rounds than allowed.
 int lattice_pass_error(cw_lattice_s *l) {
-    uint32_t e = 0, zero = 0;
+    uint32_t e = 0;
     CW_CUDA(cudaMemcpy(&e, l->pctl + CTL_ERR, sizeof e, cudaMemcpyDeviceToHost));
     if (!e) return CW_OK;
-    CW_CUDA(cudaMemcpy(l->pctl + CTL_ERR, &zero, sizeof zero, cudaMemcpyHostToDevice));
-    return e == 1 ? fail(CW_ERR_TIMEOUT, "a sublattice pass waited more than 2 s at a grid barrier")
-                  : fail(CW_ERR_SIMULATION, "a sublattice pass needed more than 256 rounds");
+    // a pass that gave up left its counts, the barrier's arrivals and its
+    // claims behind: all start again from zero
+    CW_CUDA(cudaMemset(l->pctl, 0, sizeof(uint32_t) * CTL_KEYS));
+    CW_CUDA(cudaMemset(l->claim, 0, sizeof(unsigned long long) * 2 * (size_t)l->ncells));
+    return e == 1 ? fail(CW_ERR_TIMEOUT, "a sublattice pass waited too long at a grid barrier")
+                  : fail(CW_ERR_SIMULATION, "a sublattice pass needed more rounds than allowed");
 }
 }  // namespace cw
 
@@ -995,11 +1143,10 @@ int cw_lattice_destroy(cw_lattice l) {
     if (!l) return CW_OK;
     dfree(l->grid); dfree(l->type); dfree(l->volume); dfree(l->target); dfree(l->lambda); dfree(l->vsnap);
     dfree(l->surface); dfree(l->ssnap); dfree(l->tsurf); dfree(l->lsurf); dfree(l->d_cell_off); dfree(l->d_keys);
-    dfree(l->d_flag); dfree(l->claim); dfree(l->plist); dfree(l->pctl); dfree(l->d_used);
+    dfree(l->d_flag); dfree(l->claim); dfree(l->plist); dfree(l->pidx); dfree(l->d_vplan); dfree(l->pctl); dfree(l->d_used);
     dfree(l->bath_label); dfree(l->bath_mark); dfree(l->stage); dfree(l->d_bad); dfree(l->d_span);
     l->div.release();
     l->site_plan.release();
-    for (auto &p : l->plans) p.release();
     l->g.release();
     delete l;
     return CW_OK;

@@ -51,13 +51,14 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
     return ok != 0;
 }
 
-// The phase `parity` of a barrier, waited for TMA_WAIT_NS at most.
-__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity) {
+// The phase `parity` of a barrier, waited for `limit_ns` (TMA_WAIT_NS) at most.
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity,
+                                                  unsigned long long limit_ns = TMA_WAIT_NS) {
     if (mbar_try_wait(bar, parity)) return true;
     const uint64_t t0 = tma_clock_ns();
     for (;;) {
         if (mbar_try_wait(bar, parity)) return true;
-        if (tma_clock_ns() - t0 > TMA_WAIT_NS) return false;
+        if (tma_clock_ns() - t0 > limit_ns) return false;
     }
 }
 

@@ -64,6 +64,16 @@ void *cw_get_stream(void);
 int cw_synchronize(void);
 /* Kernels this library has launched since it was loaded. */
 uint64_t cw_launch_count(void);
+/* Failure tests, no counterpart in the reference (its loops cannot hang):
+ * make the library's bounded device waits run out without faulting the GPU.
+ * wait_ns (1 ms to 2 s; 0: the default 2 s) limits every grid-barrier and
+ * TMA-copy wait; withhold_block >= 0 keeps that block of each sublattice pass
+ * from arriving at its grid barriers (the others give up: CW_ERR_TIMEOUT);
+ * max_rounds > 0 caps a pass's priority rounds (past it: CW_ERR_SIMULATION);
+ * skip_tma != 0 makes the FP32 sweeps issue no TMA copy, so their waits run
+ * out (CW_ERR_TIMEOUT).  Every call replaces all four; (0, -1, 0, 0) is the
+ * default.  Work captured in a CUDA graph keeps the settings of its capture. */
+int cw_test_faults(uint64_t wait_ns, int32_t withhold_block, int32_t max_rounds, int32_t skip_tma);
 /* CUDA events on the library stream, in slots 0..15, for timing. */
 int cw_event_record(int32_t slot);
 int cw_event_elapsed(int32_t a, int32_t b, float *ms);
