@@ -58,7 +58,8 @@ def parse():
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-fit", action="store_true")
-    p.add_argument("--fit-iters", type=int, default=4)
+    p.add_argument("--fit-iters", type=int, default=10)
+    p.add_argument("--no-shapes", action="store_true")
     p.add_argument("--profile-step", action="store_true",
                    help="bracket one extra step with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     return p.parse_args()
@@ -305,6 +306,11 @@ def run_ours(args, rank, world, dist):
            "path": "cw_lattice_upload_all (pinned host grids, checked on the device) + cw_sim_step + "
                    "cw_lattice_download_all + cw_sim_stats"}
 
+    # ---- each field against its FP64 solution (the north star's 1e-6 relative)
+    ferr = {"oxygen": field_error(L, sim, 0, cfg["o2_dcoef"], 0.0)}
+    if cfg.get("nfields", 1) > 1:
+        ferr["signal"] = field_error(L, sim, 1, cfg["signal_dcoef"], cfg["signal_decay"])
+
     # ---- roofline of the dominant kernel: the FP32 SOR sweep on this batch's oxygen field
     f = sim.field_handle(0)
     tuned = sim.tuning()
@@ -400,12 +406,113 @@ def run_ours(args, rank, world, dist):
                         "launched kernel by kernel (the path without the batching form)"}
         plain_graphs = {"value": one_at_a_time(True), "unit": UNIT,
                         "how": "as plain, each history's tuned step replayed from CUDA graphs"}
+    shapes = None
+    if not args.no_shapes and world == 1:
+        from cellweave_b200 import synthetic
+        shapes = {"cord2048": shape_record(L, synthetic.tumour_cord(), 10, 4, peak),
+                  "spheroid256": shape_record(L, synthetic.spheroid_3d(), 6, 3, peak)}
     fit = None
     if not args.no_fit and world == 1:
         fit = run_fit(args, L)
     return dict(value=value, ms=ms / args.steps, launches=launches, clocks=clk, e2e=e2e, roofline=roofline, fit=fit,
+                shapes=shapes, field_error=ferr,
                 graphs=graphs, plain_graphs=plain_graphs, kinetics4=kinetics4,
                 plain=plain, stats=stats, nh=nh, cfg=cfg, tuned=tuned)
+
+
+def field_error(L, sim, which, dcoef, decay):
+    """Largest |field - FP64 solution| / largest |FP64 solution| over the
+    histories of a simulation's field: the FP64 solution is the library's
+    FP64 relax (the reference's SOR, bit-exact with it) of the problem the
+    field last solved, from the field's values to residual 1e-12."""
+    import numpy as np
+
+    import cellweave_b200 as cw
+    from cellweave_b200 import _lib
+    fh = sim.field_handle(which)
+    twin = cw.ScalarField(sim.dims, dcoef, decay, 0.0)
+    vals = []
+    for k, (w, h, d) in enumerate(sim.dims):
+        n = w * h * d
+        for arr in (cw.VALUES, cw.UPTAKE, cw.PRODUCTION, cw.LIN_SINK):
+            out = np.empty(n)
+            _lib.check(L.cw_field_download(fh, k, arr, _lib.ptr(out)))
+            if arr == cw.VALUES:
+                vals.append(out)
+            twin.upload(arr, out, k)
+        held = np.empty(n, np.uint8)
+        _lib.check(L.cw_field_download_held(fh, k, _lib.ptr(held)))
+        twin.set_held(held, k)
+    twin.relax(1e-12, 20_000_000, stop=cw.STOP_RESIDUAL, precision=cw.FP64)
+    worst = 0.0
+    for k in range(len(sim.dims)):
+        ref = twin.values(k)
+        worst = max(worst, float(np.abs(vals[k] - ref).max() / max(np.abs(ref).max(), 1e-300)))
+    return worst
+
+
+def sor_launch_ms(L, f, depth, window, sweeps=32):
+    """Device time of one FP32 sweep launch (depth half-sweeps) on a field's
+    current residual, the kernel the solves run, after one warm pass."""
+    from cellweave_b200 import _lib
+    kms, kl = C.c_float(), C.c_int64()
+    _lib.check(L.cw_field_time_inner(f, sweeps, depth, window, 1.9, C.byref(kms), C.byref(kl)))
+    _lib.check(L.cw_field_time_inner(f, sweeps, depth, window, 1.9, C.byref(kms), C.byref(kl)))
+    return kms.value / kl.value
+
+
+def shape_record(L, cfg, steps, warm, peak):
+    """One of the other benchmark shapes (the 2048^2 cord, the 256^3
+    spheroid), stepped alone: ms per step and histories*MCS/s by CUDA events,
+    the FP32 sweep's roofline on its oxygen field, one Monte Carlo step of
+    its lattice alone, the solves' residual and each field's error."""
+    import cellweave_b200 as cw
+    from cellweave_b200 import _lib
+    cfg = dict(cfg)
+    S = cfg.pop("S")
+    net = network_for(S, S, cfg["target_volume"])
+    t0 = time.perf_counter()
+    sim = cw.Simulation(net, **cfg)
+    setup_s = time.perf_counter() - t0
+    sim.step(warm)
+    L.cw_synchronize()
+    L.cw_event_record(8)
+    sim.step(steps)
+    L.cw_event_record(9)
+    L.cw_synchronize()
+    ms = event_ms(L, 8, 9) / steps
+    stats = sim.stats()
+    rec = {"ms_per_step": round(ms, 3), "value": round(len(cfg["dims"]) * 1e3 / ms, 2), "unit": UNIT,
+           "steps": steps, "warmup": warm, "setup_s": round(setup_s, 1), "living_cells": float(stats[:, 0].sum()),
+           "residual_max": float(stats[:, 3].max()), "tolerance": cfg["tolerance"]}
+    errs = {"oxygen": field_error(L, sim, 0, cfg["o2_dcoef"], 0.0)}
+    if cfg.get("nfields", 1) > 1:
+        errs["signal"] = field_error(L, sim, 1, cfg["signal_dcoef"], cfg["signal_decay"])
+    rec["field_error"] = errs
+    # the FP32 sweep on the oxygen field: 16 B per site per launch
+    tuned = sim.tuning()
+    sites = int(sum(w * h * d for w, h, d in cfg["dims"]))
+    volume = any(d > 1 for _, _, d in cfg["dims"])
+    depth = 2 if volume else tuned["depth"]
+    lm = sor_launch_ms(L, sim.field_handle(0), depth, tuned["window"])
+    # a volume's sweep is one half-sweep per launch (k_sor32_half): two
+    # launches move one sweep's 16 B per site
+    alg = sites * SOR_BYTES_PER_SITE_PASS / (2 if volume else 1)
+    gbs = alg / (lm / 1e3) / 1e9
+    rec["sor"] = {"kernel": "k_sor32_half (one half-sweep per launch)" if volume else
+                  f"k_sor32_wide<{depth}> ({depth} half-sweeps per launch on chip)",
+                  "launch_ms": round(lm, 4), "alg_bytes_per_launch": int(alg), "achieved_gbs": round(gbs, 1),
+                  "frac": round(gbs / peak, 3)}
+    # one Monte Carlo step of the lattice alone (the passes of every colour)
+    lat = sim.lattice_handle()
+    L.cw_synchronize()
+    L.cw_event_record(8)
+    _lib.check(L.cw_lattice_mcs(lat, 1))
+    L.cw_event_record(9)
+    L.cw_synchronize()
+    rec["cpm_mcs_ms"] = round(event_ms(L, 8, 9), 3)
+    del sim
+    return rec
 
 
 def run_fit(args, L):
@@ -503,7 +610,8 @@ def main():
                     gpu_launches=r["launches"], roofline=r["roofline"], cpu_baseline=cpu,
                     plain=r["plain"], plain_with_graphs=r["plain_graphs"],
                     batched_over_plain=(r["value"] / r["plain"]["value"]) if r["plain"] else None,
-                    fit=r["fit"], cuda_graphs=r["graphs"], subsweeps4=r["kinetics4"],
+                    fit=r["fit"], shapes=r["shapes"], field_error=r["field_error"], cuda_graphs=r["graphs"],
+                    subsweeps4=r["kinetics4"],
                     sor_gbs=r["roofline"]["achieved"], sor_site_sweeps_per_s=r["roofline"]["site_sweeps_per_s"],
                     living_cells=float(r["stats"][:, 0].sum()), last_residual_max=float(r["stats"][:, 3].max()),
                     autotuned={"omega_o2": sorted(set(float(v) for v in r["tuned"]["omega_o2"])),
