@@ -261,9 +261,9 @@ def run_ours(args, rank, world, dist):
     clocks = Clocks(local)
     clocks.start()
     l0 = L.cw_launch_count()
-    L.cw_event_record(0)
+    L.cw_event_record_on(L.cw_sim_get_stream(sim._h), 0)
     sim.step(args.steps)
-    L.cw_event_record(1)
+    L.cw_event_record_on(L.cw_sim_get_stream(sim._h), 1)
     L.cw_synchronize()
     ms = event_ms(L, 0, 1)
     launches = int(L.cw_launch_count() - l0)
@@ -291,13 +291,13 @@ def run_ours(args, rank, world, dist):
     st_host = np.empty((nh, 4))
     e2e_steps = max(2, min(args.steps, 5))
     barrier()
-    L.cw_event_record(2)
+    L.cw_event_record_on(L.cw_sim_get_stream(sim._h), 2)
     for _ in range(e2e_steps):
         _lib.check(L.cw_lattice_upload_all(lat, _lib.ptr(grids)))
         sim.step(1)
         _lib.check(L.cw_lattice_download_all(lat, _lib.ptr(grids)))
         _lib.check(L.cw_sim_stats(sim._h, _lib.ptr(st_host)))
-    L.cw_event_record(3)
+    L.cw_event_record_on(L.cw_sim_get_stream(sim._h), 3)
     e2e_ms = event_ms(L, 2, 3) / e2e_steps
     bytes_grid = int(grids.nbytes)
     e2e_ms = max_over_ranks(e2e_ms, dist, f"cuda:{local}")
@@ -370,10 +370,10 @@ def run_ours(args, rank, world, dist):
         s4 = cw.Simulation(net, **dict(cfg, subsweeps=4))
         s4.step(max(args.warmup, 3))
         L.cw_synchronize()
-        L.cw_event_record(4)
+        L.cw_event_record_on(L.cw_sim_get_stream(s4._h), 4)
         n4 = min(args.steps, 10)
         s4.step(n4)
-        L.cw_event_record(5)
+        L.cw_event_record_on(L.cw_sim_get_stream(s4._h), 5)
         L.cw_synchronize()
         kinetics4 = {"value": job_rate(1, nh, n4, event_ms(L, 4, 5)), "unit": UNIT, "subsweeps": 4,
                      "how": "the same batch, every colour swept four times a step with each pixel attempting in "
@@ -392,9 +392,9 @@ def run_ours(args, rank, world, dist):
                 s1.step(2)
                 n = args.steps if args.steps <= 5 else 5
                 L.cw_synchronize()
-                L.cw_event_record(4)
+                L.cw_event_record_on(L.cw_sim_get_stream(s1._h), 4)
                 s1.step(n)
-                L.cw_event_record(5)
+                L.cw_event_record_on(L.cw_sim_get_stream(s1._h), 5)
                 L.cw_synchronize()
                 total_ms += event_ms(L, 4, 5)
                 units += n
@@ -476,9 +476,9 @@ def shape_record(L, cfg, steps, warm, peak):
     setup_s = time.perf_counter() - t0
     sim.step(warm)
     L.cw_synchronize()
-    L.cw_event_record(8)
+    L.cw_event_record_on(L.cw_sim_get_stream(sim._h), 8)
     sim.step(steps)
-    L.cw_event_record(9)
+    L.cw_event_record_on(L.cw_sim_get_stream(sim._h), 9)
     L.cw_synchronize()
     ms = event_ms(L, 8, 9) / steps
     stats = sim.stats()
@@ -506,9 +506,9 @@ def shape_record(L, cfg, steps, warm, peak):
     # one Monte Carlo step of the lattice alone (the passes of every colour)
     lat = sim.lattice_handle()
     L.cw_synchronize()
-    L.cw_event_record(8)
+    L.cw_event_record_on(L.cw_sim_get_stream(sim._h), 8)
     _lib.check(L.cw_lattice_mcs(lat, 1))
-    L.cw_event_record(9)
+    L.cw_event_record_on(L.cw_sim_get_stream(sim._h), 9)
     L.cw_synchronize()
     rec["cpm_mcs_ms"] = round(event_ms(L, 8, 9), 3)
     del sim
@@ -545,7 +545,7 @@ def run_fit(args, L):
     times, losses = [], []
     for _ in range(args.fit_iters):
         L.cw_synchronize()
-        L.cw_event_record(6)
+        L.cw_event_record_on(L.cw_sim_get_stream(sim._h), 6)
         loss, grad = fit.gradient()
         d = -grad * p * p  # steepest descent in log p (a parameter at zero stays there)
         rel = np.abs(d / np.where(p != 0, p, 1.0)).max()
@@ -553,7 +553,7 @@ def run_fit(args, L):
         q[0] = max(q[0], 1e-3)
         fit.params = q
         lq = fit.forward()[0]
-        L.cw_event_record(7)
+        L.cw_event_record_on(L.cw_sim_get_stream(sim._h), 7)
         times.append(event_ms(L, 6, 7) / 1e3)
         losses.append(loss)
         if lq < loss:

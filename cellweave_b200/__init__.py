@@ -8,7 +8,7 @@ compute call raises.
 """
 from ._lib import (CellweaveError, ConfigError, CudaError, NotFoundError, OdeSolverError,  # noqa: F401
                    SimulationError)
-from .engine import (FP32_DC, FP64, OBSTACLE, WINDOW_64, WINDOW_AUTO, WINDOW_TALL, STOP_MAX_CHANGE, STOP_RESIDUAL, CpmLattice, Fit, Network,  # noqa: F401
+from .engine import (FP32_DC, FP64, LIN_SINK, OBSTACLE, PRODUCTION, UPTAKE, VALUES, WINDOW_64, WINDOW_AUTO, WINDOW_TALL, STOP_MAX_CHANGE, STOP_RESIDUAL, CpmLattice, Fit, Network,  # noqa: F401
                      ScalarField, Simulation, apply_background_uptake, apply_production, apply_uptake,
                      hold_medium_bath, hold_obstacles_at, load_network_spec, mean_per_cell)
 from . import config, output  # noqa: F401,E402

@@ -117,6 +117,20 @@ SIGNATURES = {
     "cw_synchronize": (C.c_int, []),
     "cw_launch_count": (C.c_uint64, []),
     "cw_test_faults": (C.c_int, [U64, I32, I32, I32]),
+    "cw_event_record_on": (C.c_int, [P, I32]),
+    "cw_lattice_set_stream": (C.c_int, [P, P]),
+    "cw_field_set_stream": (C.c_int, [P, P]),
+    "cw_network_set_stream": (C.c_int, [P, P]),
+    "cw_sim_set_stream": (C.c_int, [P, P]),
+    "cw_lattice_get_stream": (P, [P]),
+    "cw_field_get_stream": (P, [P]),
+    "cw_network_get_stream": (P, [P]),
+    "cw_sim_get_stream": (P, [P]),
+    "cw_lattice_last_error": (C.c_char_p, [P]),
+    "cw_field_last_error": (C.c_char_p, [P]),
+    "cw_network_last_error": (C.c_char_p, [P]),
+    "cw_sim_last_error": (C.c_char_p, [P]),
+    "cw_fit_last_error": (C.c_char_p, [P]),
     "cw_lattice_create": (C.c_int, [U32, P, P, P, P, D, P]),
     "cw_lattice_destroy": (C.c_int, [P]),
     "cw_lattice_count": (C.c_int, [P, P]),

@@ -30,6 +30,7 @@
 using namespace cw;
 
 struct cw_fit_s {
+    cw::HandleStream hs;  // its lattice's stream and its last error
     cw_lattice_s *lat = nullptr;
     cw_network_s *net = nullptr;
     cw_fit_config cfg;
@@ -376,12 +377,14 @@ int blocks(int64_t n) { return (int)((n + T - 1) / T); }
 extern "C" {
 
 int cw_fit_create(cw_lattice lat, cw_network net, const cw_fit_config *cfg, cw_fit *out) {
+    CW_SCOPE(lat);  // the fit and its fields work on the lattice's stream
     *out = nullptr;
     if (lat->g.nh != 1) return fail(CW_ERR_CONFIG, "a fit takes a lattice of one history");
     if (cfg->steps <= 0 || cfg->checkpoint_every <= 0 || cfg->steps % cfg->checkpoint_every)
         return fail(CW_ERR_CONFIG, "the RK4 steps must be a positive multiple of the checkpoint interval");
     if (cfg->nbins <= 0 || cfg->nbins > 4096) return fail(CW_ERR_CONFIG, "1 to 4096 bins");
     cw_fit_s *f = new cw_fit_s();
+    f->hs.init();
     f->lat = lat;
     f->net = net;
     f->cfg = *cfg;
@@ -448,21 +451,27 @@ int cw_fit_create(cw_lattice lat, cw_network net, const cw_fit_config *cfg, cw_f
 
 int cw_fit_destroy(cw_fit f) {
     if (!f) return CW_OK;
+    CW_SCOPE(f);
     cw_field_destroy(f->o2); cw_field_destroy(f->sig); cw_field_destroy(f->ao2); cw_field_destroy(f->asig);
     dfree(f->term); dfree(f->par); dfree(f->d_rate); dfree(f->sum); dfree(f->mean); dfree(f->sum2); dfree(f->mean2);
     dfree(f->count); dfree(f->count2); dfree(f->inputs); dfree(f->x0); dfree(f->xT); dfree(f->lam); dfree(f->gin);
     dfree(f->ck); dfree(f->seg); dfree(f->bins); dfree(f->coef); dfree(f->grad);
     f->sites.release();
+    f->hs.release();
     delete f;
     return CW_OK;
 }
 
+const char *cw_fit_last_error(cw_fit f) { return f->hs.err.c_str(); }
+
 int cw_fit_nparams(cw_fit f, int32_t *n) {
+    CW_SCOPE(f);
     *n = 4 + f->ntheta;
     return CW_OK;
 }
 
 int cw_fit_get_params(cw_fit f, double *p) {
+    CW_SCOPE(f);
     p[0] = f->Dc;
     for (int q = 0; q < 3; ++q) p[1 + q] = f->k[q];
     for (int t = 0; t < f->ntheta; ++t) p[4 + t] = f->theta[t];
@@ -470,6 +479,7 @@ int cw_fit_get_params(cw_fit f, double *p) {
 }
 
 int cw_fit_set_params(cw_fit f, const double *p) {
+    CW_SCOPE(f);
     if (!(p[0] > 0.0)) return fail(CW_ERR_CONFIG, "the diffusion coefficient must be positive");
     f->Dc = p[0];
     for (int q = 0; q < 3; ++q) f->k[q] = p[1 + q];
@@ -479,12 +489,14 @@ int cw_fit_set_params(cw_fit f, const double *p) {
 }
 
 int cw_fit_set_target(cw_fit f, const double *h, const double *g) {
+    CW_SCOPE(f);
     f->target_h.assign(h, h + f->cfg.nbins);
     f->target_g.assign(g, g + f->cfg.nbins);
     return CW_OK;
 }
 
 int cw_fit_forward(cw_fit f, double *loss, double *h_out, double *g_out) {
+    CW_SCOPE(f);
     const cw_fit_config &c = f->cfg;
     const int nb = c.nbins;
     int rc;
@@ -541,6 +553,7 @@ int cw_fit_forward(cw_fit f, double *loss, double *h_out, double *g_out) {
 }
 
 int cw_fit_gradient(cw_fit f, double *loss, double *grad) {
+    CW_SCOPE(f);
     int rc;
     if ((rc = cw_fit_forward(f, loss, nullptr, nullptr)) != CW_OK) return rc;
     const cw_fit_config &c = f->cfg;
@@ -598,6 +611,7 @@ int cw_fit_gradient(cw_fit f, double *loss, double *grad) {
 extern "C" int cw_network_backward_batch(cw_network net, int64_t ncells, const double *state, const double *inputs,
                                          double dt, int32_t substeps, double *adjoint, double *d_oxygen,
                                          int32_t nrates, double *d_rates) {
+    CW_SCOPE(net);
     if (ncells < 0 || substeps < 1 || !(dt > 0.0))
         return fail(CW_ERR_CONFIG, "a backward step needs cells >= 0, substeps >= 1 and dt > 0");
     if (nrates < 0 || nrates > std::min(MAXTH, net->nterms))

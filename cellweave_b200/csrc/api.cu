@@ -1,6 +1,7 @@
 // Library-wide plumbing: errors, the stream, launch counting, batch geometry.
 #include <atomic>
 #include <cstring>
+#include <mutex>
 
 #include "cw_internal.cuh"
 
@@ -9,28 +10,109 @@ namespace cw {
 static thread_local std::string g_error;
 static std::atomic<uint64_t> g_launches{0};
 static cudaStream_t g_own_stream = nullptr;
+static std::once_flag g_own_once;
 static cudaStream_t g_user_stream = nullptr;
 static bool g_user_set = false;
+// the scope of the entry point running on this thread (Scope)
+static thread_local cudaStream_t t_stream = nullptr;
+static thread_local bool t_scoped = false;
+static thread_local std::string *t_err = nullptr;
 
 static TestFaults g_faults;
 const TestFaults &test_faults() { return g_faults; }
 
-void set_error(const std::string &msg) { g_error = msg; }
+void set_error(const std::string &msg) {
+    g_error = msg;
+    if (t_err) *t_err = msg;
+}
 
 int fail(int code, const std::string &msg) {
-    g_error = msg;
+    set_error(msg);
     return code;
 }
 
 int cuda_fail(cudaError_t e, const char *what) {
-    g_error = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+    set_error(std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")");
     return CW_ERR_CUDA;
 }
 
-cudaStream_t stream() {
+// The library stream: the caller's (cw_set_stream), else one of its own.
+static cudaStream_t library_stream() {
     if (g_user_set) return g_user_stream;
-    if (!g_own_stream) cudaStreamCreateWithFlags(&g_own_stream, cudaStreamNonBlocking);
+    std::call_once(g_own_once, [] { cudaStreamCreateWithFlags(&g_own_stream, cudaStreamNonBlocking); });
     return g_own_stream;
+}
+
+cudaStream_t stream() {
+    if (t_scoped && t_stream) return t_stream;
+    return library_stream();
+}
+
+int HandleStream::init(bool adopt) {
+    if (adopt && t_scoped && t_stream) {
+        stream = t_stream;  // a handle made inside another's call shares its stream
+        own = false;
+        return CW_OK;
+    }
+    CW_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    own = true;
+    return CW_OK;
+}
+
+int HandleStream::set(cudaStream_t s) {
+    if (s && s == stream) return CW_OK;
+    if (stream) CW_CUDA(cudaStreamSynchronize(stream));  // work queued so far finishes first
+    if (own && stream) cudaStreamDestroy(stream);
+    stream = nullptr;
+    own = false;
+    if (s) {
+        stream = s;
+        return CW_OK;
+    }
+    CW_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    own = true;
+    return CW_OK;
+}
+
+void HandleStream::release() {
+    if (own && stream) {
+        cudaStreamSynchronize(stream);
+        cudaStreamDestroy(stream);
+    }
+    stream = nullptr;
+    own = false;
+}
+
+Scope::Scope(HandleStream *hs) : prev_stream_(t_stream), prev_err_(t_err), prev_set_(t_scoped) {
+    t_stream = hs->stream;
+    t_err = &hs->err;
+    t_scoped = true;
+}
+
+Scope::~Scope() {
+    t_stream = prev_stream_;
+    t_err = prev_err_;
+    t_scoped = prev_set_;
+}
+
+// The other handle's queued work before this call's, and this call's before
+// the other handle's next (one event each way; nothing when they share a stream).
+Join::Join(const HandleStream *other) : mine_(stream()), other_(other->stream ? other->stream : library_stream()) {
+    if (mine_ == other_) return;
+    cudaEvent_t e;
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return;
+    cudaEventRecord(e, other_);
+    cudaStreamWaitEvent(mine_, e, 0);
+    cudaEventDestroy(e);
+}
+
+Join::~Join() {
+    if (mine_ == other_) return;
+    cudaEvent_t e;
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return;
+    cudaEventRecord(e, mine_);
+    cudaStreamWaitEvent(other_, e, 0);
+    cudaEventDestroy(e);
 }
 
 void count_launch(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
@@ -109,7 +191,8 @@ int cw_set_stream(void *s) {
 void *cw_get_stream(void) { return (void *)cw::stream(); }
 
 int cw_synchronize(void) {
-    CW_CUDA(cudaStreamSynchronize(cw::stream()));
+    // every handle's stream and the library's
+    CW_CUDA(cudaDeviceSynchronize());
     return CW_OK;
 }
 
@@ -137,6 +220,13 @@ extern "C" int cw_event_record(int32_t slot) {
     if (slot < 0 || slot >= 16) return cw::fail(CW_ERR_CONFIG, "event slots are 0 to 15");
     if (!g_events[slot]) CW_CUDA(cudaEventCreate(&g_events[slot]));
     CW_CUDA(cudaEventRecord(g_events[slot], cw::stream()));
+    return CW_OK;
+}
+
+extern "C" int cw_event_record_on(void *stream, int32_t slot) {
+    if (slot < 0 || slot >= 16) return cw::fail(CW_ERR_CONFIG, "event slots are 0 to 15");
+    if (!g_events[slot]) CW_CUDA(cudaEventCreate(&g_events[slot]));
+    CW_CUDA(cudaEventRecord(g_events[slot], stream ? (cudaStream_t)stream : cw::stream()));
     return CW_OK;
 }
 

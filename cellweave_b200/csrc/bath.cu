@@ -190,6 +190,7 @@ int lattice_bath_error() {
 }  // namespace cw
 
 extern "C" int cw_lattice_bath(cw_lattice l, uint32_t hist, uint8_t *out) {
+    CW_SCOPE(l);
     if (hist >= l->g.nh) return fail(CW_ERR_NOT_FOUND, "no history " + std::to_string(hist));
     uint8_t *d;
     int rc;

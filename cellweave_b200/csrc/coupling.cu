@@ -183,6 +183,8 @@ int couple_means_device(cw_field_s *f, cw_lattice_s *l, double *sum, int32_t *co
 extern "C" {
 
 int cw_couple_uptake(cw_field f, cw_lattice l, int32_t K, const double *rate_by_type, int32_t first_order) {
+    CW_SCOPE(f);
+    CW_JOIN(l);
     int rc = check_pair(f, l);
     if (rc != CW_OK) return rc;
     if (K < 1 || K > 8) return fail(CW_ERR_CONFIG, "rates for 1 to 8 types");
@@ -203,6 +205,8 @@ int cw_couple_uptake(cw_field f, cw_lattice l, int32_t K, const double *rate_by_
 }
 
 int cw_couple_background_uptake(cw_field f, cw_lattice l, double rate) {
+    CW_SCOPE(f);
+    CW_JOIN(l);
     int rc = check_pair(f, l);
     if (rc != CW_OK) return rc;
     int64_t n = f->g.total;
@@ -214,6 +218,8 @@ int cw_couple_background_uptake(cw_field f, cw_lattice l, double rate) {
 }
 
 int cw_couple_production(cw_field f, cw_lattice l, uint32_t hist, uint32_t n, const double *per_cell) {
+    CW_SCOPE(f);
+    CW_JOIN(l);
     int rc = check_pair(f, l);
     if (rc != CW_OK) return rc;
     if (hist >= l->g.nh) return fail(CW_ERR_NOT_FOUND, "no history " + std::to_string(hist));
@@ -241,6 +247,8 @@ int cw_couple_production(cw_field f, cw_lattice l, uint32_t hist, uint32_t n, co
 }
 
 int cw_couple_hold_obstacles(cw_field f, cw_lattice l, double value) {
+    CW_SCOPE(f);
+    CW_JOIN(l);
     int rc = check_pair(f, l);
     if (rc != CW_OK) return rc;
     int64_t n = f->g.total;
@@ -252,6 +260,8 @@ int cw_couple_hold_obstacles(cw_field f, cw_lattice l, double value) {
 }
 
 int cw_couple_hold_medium_bath(cw_field f, cw_lattice l, double value) {
+    CW_SCOPE(f);
+    CW_JOIN(l);
     int rc = check_pair(f, l);
     if (rc != CW_OK) return rc;
     int64_t n = f->g.total;
@@ -265,6 +275,8 @@ int cw_couple_hold_medium_bath(cw_field f, cw_lattice l, double value) {
 }
 
 int cw_couple_mean_per_cell(cw_field f, cw_lattice l, uint32_t hist, uint32_t n, double *out) {
+    CW_SCOPE(f);
+    CW_JOIN(l);
     int rc = check_pair(f, l);
     if (rc != CW_OK) return rc;
     if (hist >= l->g.nh) return fail(CW_ERR_NOT_FOUND, "no history " + std::to_string(hist));

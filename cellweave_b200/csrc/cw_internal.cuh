@@ -18,6 +18,51 @@ int cuda_fail(cudaError_t e, const char *what);
 cudaStream_t stream();
 void count_launch(uint64_t n = 1);
 
+// ------------------------------------------------------------------ streams and errors per handle
+// Every handle queues its work on its own CUDA stream (created with it, or
+// the stream of the handle that created it: a simulation's lattice and
+// fields share the simulation's) and keeps the message of its last failure.
+// A public entry point opens a Scope on its handle: stream() is then that
+// stream, and a failure is recorded on the handle as well as on the calling
+// thread.  A call that also reads another handle's buffers joins that
+// handle's stream on entry and on exit (Join), so the two queues stay ordered.
+struct HandleStream {
+    cudaStream_t stream = nullptr;  // null: the library stream
+    bool own = false;               // created for this handle (destroyed with it)
+    std::string err;                // the last failure of a call on this handle
+    int init(bool adopt = true);    // the current scope's stream (adopt), else a new one
+    int set(cudaStream_t s);        // the caller's stream (null: a new one of its own)
+    void release();
+    HandleStream() = default;
+    HandleStream(const HandleStream &) = delete;
+    HandleStream &operator=(const HandleStream &) = delete;
+    ~HandleStream() { release(); }
+};
+class Scope {
+  public:
+    explicit Scope(HandleStream *hs);
+    ~Scope();
+    Scope(const Scope &) = delete;
+    Scope &operator=(const Scope &) = delete;
+
+  private:
+    cudaStream_t prev_stream_;
+    std::string *prev_err_;
+    bool prev_set_;
+};
+class Join {
+  public:
+    explicit Join(const HandleStream *other);
+    ~Join();
+    Join(const Join &) = delete;
+    Join &operator=(const Join &) = delete;
+
+  private:
+    cudaStream_t mine_, other_;
+};
+#define CW_SCOPE(h) ::cw::Scope cw_scope_(&(h)->hs)
+#define CW_JOIN(h) ::cw::Join cw_join_(&(h)->hs)
+
 // Failure-test settings (cw_test_faults): all off by default.  wait_ns
 // shortens every bounded device wait (grid barriers, TMA copies) from its
 // 2 s; withhold_block keeps one block of a pass from arriving at its grid
@@ -206,6 +251,7 @@ struct DivScratch {
 }  // namespace cw
 
 struct cw_lattice_s {
+    cw::HandleStream hs;             // its stream and last error
     cw::Geom g;
     std::vector<int64_t> cell_off;   // nh + 1
     int64_t ncells = 0;              // all histories
@@ -257,6 +303,7 @@ struct cw_lattice_s {
 };
 
 struct cw_field_s {
+    cw::HandleStream hs;             // its stream and last error
     cw::Geom g;
     double *c = nullptr;             // values
     uint8_t *held = nullptr;

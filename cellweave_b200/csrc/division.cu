@@ -314,6 +314,7 @@ extern "C" {
 
 int cw_lattice_divide(cw_lattice l, uint32_t hist, uint32_t n, const int32_t *ids, const double *normals,
                       int32_t *daughters) {
+    CW_SCOPE(l);
     if (hist >= l->g.nh) return fail(CW_ERR_NOT_FOUND, "no history " + std::to_string(hist));
     const int64_t c0 = l->cell_off[hist], cap = l->cell_off[hist + 1] - c0, nc = l->ncells;
     std::vector<uint8_t> flag(nc, 0);
@@ -341,6 +342,7 @@ int cw_lattice_divide(cw_lattice l, uint32_t hist, uint32_t n, const int32_t *id
 }
 
 int cw_lattice_cell_count(cw_lattice l, uint32_t hist, uint32_t *n) {
+    CW_SCOPE(l);
     if (hist >= l->g.nh) return fail(CW_ERR_NOT_FOUND, "no history " + std::to_string(hist));
     int32_t v = 0;
     CW_CUDA(cudaMemcpy(&v, l->d_used + hist, sizeof v, cudaMemcpyDeviceToHost));

@@ -1162,6 +1162,8 @@ int cw_field_create(uint32_t nh, const uint32_t *w, const uint32_t *h, const uin
         return fail(CW_ERR_CONFIG, "diffusion and decay must be finite and not negative, got D = " +
                                        std::to_string(dcoef) + ", decay = " + std::to_string(decay));
     cw_field_s *f = new cw_field_s();
+    if (f->hs.init() != CW_OK) { delete f; return CW_ERR_CUDA; }
+    CW_SCOPE(f);
     int rc = f->g.init(nh, w, h, d);
     if (rc != CW_OK) { delete f; return rc; }
     f->dcoef = dcoef; f->decay = decay;
@@ -1185,6 +1187,7 @@ int cw_field_create(uint32_t nh, const uint32_t *w, const uint32_t *h, const uin
 
 int cw_field_destroy(cw_field f) {
     if (!f) return CW_OK;
+    CW_SCOPE(f);
     dfree(f->c); dfree(f->held); dfree(f->uptake); dfree(f->production); dfree(f->lin_sink);
     dfree(f->r32); dfree(f->d32a); dfree(f->d32b); dfree(f->inv32); dfree(f->tmp64); dfree(f->d_span);
     if (f->dc_cache) {
@@ -1201,21 +1204,34 @@ int cw_field_destroy(cw_field f) {
     if (f->adjoint) cw_field_destroy(f->adjoint);
     f->inflow_plan.release();
     f->g.release();
+    f->hs.release();
     delete f;
     return CW_OK;
 }
 
+int cw_field_set_stream(cw_field f, void *stream) {
+    CW_SCOPE(f);
+    return f->hs.set((cudaStream_t)stream);
+}
+
+void *cw_field_get_stream(cw_field f) { return (void *)f->hs.stream; }
+
+const char *cw_field_last_error(cw_field f) { return f->hs.err.c_str(); }
+
 int cw_field_set_source(cw_field f, double source) {
+    CW_SCOPE(f);
     f->source = source;
     return CW_OK;
 }
 
 int cw_field_set_floor(cw_field f, int32_t on) {
+    CW_SCOPE(f);
     f->floor = on != 0;
     return CW_OK;
 }
 
 int cw_field_set_diffusion(cw_field f, double dcoef) {
+    CW_SCOPE(f);
     if (!std::isfinite(dcoef) || dcoef < 0.0) return fail(CW_ERR_CONFIG, "diffusion must be finite and not negative");
     f->dcoef = dcoef;
     return CW_OK;
@@ -1232,6 +1248,7 @@ static double *array_of(cw_field f, int32_t which) {
 }
 
 int cw_field_upload(cw_field f, uint32_t hist, int32_t which, const double *host) {
+    CW_SCOPE(f);
     if (hist >= f->g.nh) return fail(CW_ERR_NOT_FOUND, "no history " + std::to_string(hist));
     double *p = array_of(f, which);
     if (!p) return fail(CW_ERR_CONFIG, "unknown field array");
@@ -1245,6 +1262,7 @@ int cw_field_upload(cw_field f, uint32_t hist, int32_t which, const double *host
 }
 
 int cw_field_download(cw_field f, uint32_t hist, int32_t which, double *host) {
+    CW_SCOPE(f);
     if (hist >= f->g.nh) return fail(CW_ERR_NOT_FOUND, "no history " + std::to_string(hist));
     double *p = array_of(f, which);
     if (!p) return fail(CW_ERR_CONFIG, "unknown field array");
@@ -1255,6 +1273,7 @@ int cw_field_download(cw_field f, uint32_t hist, int32_t which, double *host) {
 }
 
 int cw_field_upload_held(cw_field f, uint32_t hist, const uint8_t *held) {
+    CW_SCOPE(f);
     if (hist >= f->g.nh) return fail(CW_ERR_NOT_FOUND, "no history " + std::to_string(hist));
     f->held_dirty = true;
     CW_CUDA(cudaMemcpyAsync(f->held + f->g.off[hist], held, f->g.sites(hist), cudaMemcpyHostToDevice, stream()));
@@ -1263,6 +1282,7 @@ int cw_field_upload_held(cw_field f, uint32_t hist, const uint8_t *held) {
 }
 
 int cw_field_download_held(cw_field f, uint32_t hist, uint8_t *held) {
+    CW_SCOPE(f);
     if (hist >= f->g.nh) return fail(CW_ERR_NOT_FOUND, "no history " + std::to_string(hist));
     CW_CUDA(cudaMemcpyAsync(held, f->held + f->g.off[hist], f->g.sites(hist), cudaMemcpyDeviceToHost, stream()));
     CW_CUDA(cudaStreamSynchronize(stream()));
@@ -1270,6 +1290,7 @@ int cw_field_download_held(cw_field f, uint32_t hist, uint8_t *held) {
 }
 
 int cw_field_fill(cw_field f, double value) {
+    CW_SCOPE(f);
     int64_t n = f->g.total;
     k_fill64<<<(unsigned)blocks_for(n), T, 0, stream()>>>(f->c, n, value);
     CW_LAUNCHED();
@@ -1277,6 +1298,7 @@ int cw_field_fill(cw_field f, double value) {
 }
 
 int cw_field_clear(cw_field f, int32_t which) {
+    CW_SCOPE(f);
     double *p = array_of(f, which);
     if (!p || which == CW_VALUES) return fail(CW_ERR_CONFIG, "only uptake, production and the linear sink clear");
     CW_CUDA(cudaMemsetAsync(p, 0, sizeof(double) * f->g.total, stream()));
@@ -1287,12 +1309,14 @@ int cw_field_clear(cw_field f, int32_t which) {
 }
 
 int cw_field_release_all(cw_field f) {
+    CW_SCOPE(f);
     f->held_dirty = true;
     CW_CUDA(cudaMemsetAsync(f->held, 0, f->g.total, stream()));
     return CW_OK;
 }
 
 int cw_field_hold_mask(cw_field f, uint32_t hist, const uint8_t *mask, double value) {
+    CW_SCOPE(f);
     if (hist >= f->g.nh) return fail(CW_ERR_NOT_FOUND, "no history " + std::to_string(hist));
     int64_t n = f->g.sites(hist);
     uint8_t *dm;
@@ -1309,6 +1333,7 @@ int cw_field_hold_mask(cw_field f, uint32_t hist, const uint8_t *mask, double va
 }
 
 int cw_field_relax(cw_field f, const cw_relax_opts *opts, cw_relax_stats *stats) {
+    CW_SCOPE(f);
     return cw::field_relax(f, opts, nullptr, stats);
 }
 
@@ -1317,6 +1342,7 @@ int cw_field_relax(cw_field f, const cw_relax_opts *opts, cw_relax_stats *stats)
 // on a twin with dl_dc as the source, zero on the held pixels and no floor.
 int cw_field_relax_adjoint(cw_field f, const double *dl_dc, double *lambda, const cw_relax_opts *opts,
                            cw_relax_stats *stats) {
+    CW_SCOPE(f);
     int rc;
     cw_field_s *a = f->adjoint;
     const int64_t n = f->g.total;
@@ -1433,6 +1459,7 @@ int field_inflow_enqueue(cw_field_s *f, double *inflow, unsigned long long *free
 extern "C" {
 
 int cw_field_residual(cw_field f, double *out) {
+    CW_SCOPE(f);
     uint32_t nh = f->g.nh;
     RelaxState *d_st = (RelaxState *)f->stats;
     std::vector<RelaxState> hs(nh);
@@ -1453,6 +1480,7 @@ int cw_field_residual(cw_field f, double *out) {
 }
 
 int cw_field_inflow(cw_field f, double *out) {
+    CW_SCOPE(f);
     uint32_t nh = f->g.nh;
     double *d_out;
     int rc = dalloc(&d_out, nh);
@@ -1470,6 +1498,7 @@ int cw_field_inflow(cw_field f, double *out) {
 }
 
 int cw_field_step(cw_field f, double dt) {
+    CW_SCOPE(f);
     if (std::isnan(dt) || dt <= 0.0) return fail(CW_ERR_CONFIG, "time step must be positive, got " + std::to_string(dt));
     bool volume = false;
     for (uint32_t k = 0; k < f->g.nh; ++k) volume = volume || f->g.d[k] > 1;
@@ -1539,6 +1568,7 @@ int field_hold_bath_device(cw_field_s *f, const uint8_t *d_open, int hist, doubl
 }  // namespace cw
 
 extern "C" int cw_field_hold_bath(cw_field f, uint32_t hist, const uint8_t *open, double value) {
+    CW_SCOPE(f);
     if (hist >= f->g.nh) return fail(CW_ERR_NOT_FOUND, "no history " + std::to_string(hist));
     uint8_t *d_open;
     int rc = dalloc(&d_open, f->g.total);
@@ -1555,6 +1585,7 @@ extern "C" int cw_field_hold_bath(cw_field f, uint32_t hist, const uint8_t *open
 // with events around the sweep launches alone.  The field is not changed.
 extern "C" int cw_field_time_inner(cw_field f, int32_t sweeps, int32_t depth, int32_t window, double omega, float *ms,
                                    int64_t *launches) {
+    CW_SCOPE(f);
     uint32_t nh = f->g.nh;
     int rc = f->alloc_fp32();
     if (rc != CW_OK) return rc;
@@ -1589,6 +1620,7 @@ extern "C" int cw_field_time_inner(cw_field f, int32_t sweeps, int32_t depth, in
 }
 
 extern "C" int cw_field_inner_correction(cw_field f, uint32_t hist, float *out) {
+    CW_SCOPE(f);
     if (hist >= f->g.nh) return fail(CW_ERR_NOT_FOUND, "no history " + std::to_string(hist));
     if (!f->last_inner) return fail(CW_ERR_CONFIG, "no inner solve has run on this field");
     CW_CUDA(cudaMemcpy(out, f->last_inner + f->g.off[hist], sizeof(float) * f->g.sites(hist), cudaMemcpyDeviceToHost));

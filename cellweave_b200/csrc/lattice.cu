@@ -523,6 +523,9 @@ __global__ void __launch_bounds__(1024) k_pass_plan(const int32_t *span, int nh,
 // fit.
 __global__ void __launch_bounds__(PT, 1) k_cpm_pass(LatView L, Tables tabs, int nh, const int32_t *perm, int pass,
                                                     const uint32_t *mcs_cur, PassScratch S) {
+    // a pass queued after one that gave up does nothing: the barrier's count
+    // and the claims that one left behind are cleared by the host first
+    if (__ldcg(S.ctl + CTL_ERR) != 0u) return;
     __shared__ double sJ[64];
     __shared__ int8_t sreach[3 * 124];
     __shared__ int s_ok;
@@ -1093,6 +1096,8 @@ int cw_lattice_create(uint32_t nh, const uint32_t *w, const uint32_t *h, const u
     *out = nullptr;
     if (nh > 65535) return fail(CW_ERR_CONFIG, "a lattice batch holds at most 65535 histories");
     cw_lattice_s *l = new cw_lattice_s();
+    if (l->hs.init() != CW_OK) { delete l; return CW_ERR_CUDA; }
+    CW_SCOPE(l);
     int rc = l->g.init(nh, w, h, d);
     if (rc != CW_OK) { delete l; return rc; }
     bool volume = l->g.d[0] > 1;
@@ -1141,6 +1146,7 @@ int cw_lattice_create(uint32_t nh, const uint32_t *w, const uint32_t *h, const u
 
 int cw_lattice_destroy(cw_lattice l) {
     if (!l) return CW_OK;
+    CW_SCOPE(l);
     dfree(l->grid); dfree(l->type); dfree(l->volume); dfree(l->target); dfree(l->lambda); dfree(l->vsnap);
     dfree(l->surface); dfree(l->ssnap); dfree(l->tsurf); dfree(l->lsurf); dfree(l->d_cell_off); dfree(l->d_keys);
     dfree(l->d_flag); dfree(l->claim); dfree(l->plist); dfree(l->pidx); dfree(l->d_vplan); dfree(l->pctl); dfree(l->d_used);
@@ -1148,17 +1154,20 @@ int cw_lattice_destroy(cw_lattice l) {
     l->div.release();
     l->site_plan.release();
     l->g.release();
+    l->hs.release();
     delete l;
     return CW_OK;
 }
 
 int cw_lattice_capacity(cw_lattice l, uint32_t hist, uint32_t *cap) {
+    CW_SCOPE(l);
     if (hist >= l->g.nh) return fail(CW_ERR_NOT_FOUND, "no history " + std::to_string(hist));
     *cap = (uint32_t)(l->cell_off[hist + 1] - l->cell_off[hist]);
     return CW_OK;
 }
 
 int cw_lattice_pass_rounds(cw_lattice l, uint32_t *rounds) {
+    CW_SCOPE(l);
     uint32_t zero = 0;
     CW_CUDA(cudaStreamSynchronize(stream()));
     CW_CUDA(cudaMemcpy(rounds, l->pctl + CTL_ROUNDS, sizeof(uint32_t), cudaMemcpyDeviceToHost));
@@ -1166,12 +1175,23 @@ int cw_lattice_pass_rounds(cw_lattice l, uint32_t *rounds) {
     return CW_OK;
 }
 
+int cw_lattice_set_stream(cw_lattice l, void *stream) {
+    CW_SCOPE(l);
+    return l->hs.set((cudaStream_t)stream);
+}
+
+void *cw_lattice_get_stream(cw_lattice l) { return (void *)l->hs.stream; }
+
+const char *cw_lattice_last_error(cw_lattice l) { return l->hs.err.c_str(); }
+
 int cw_lattice_count(cw_lattice l, uint32_t *nh) {
+    CW_SCOPE(l);
     *nh = l->g.nh;
     return CW_OK;
 }
 
 int cw_lattice_set_contact(cw_lattice l, int32_t K, const double *J, int32_t order) {
+    CW_SCOPE(l);
     if (K < 1 || K > 8) return fail(CW_ERR_CONFIG, "the contact table holds 1 to 8 types, got " + std::to_string(K));
     for (int a = 0; a < K; ++a)
         for (int b = 0; b < K; ++b)
@@ -1185,6 +1205,7 @@ int cw_lattice_set_contact(cw_lattice l, int32_t K, const double *J, int32_t ord
 }
 
 int cw_lattice_set_copy_nbhd(cw_lattice l, int32_t nbhd) {
+    CW_SCOPE(l);
     if (nbhd != CW_COPY_VON_NEUMANN && nbhd != CW_COPY_MOORE)
         return fail(CW_ERR_CONFIG, "copy neighbourhood " + std::to_string(nbhd) + " is neither von Neumann nor Moore");
     l->copy_moore = nbhd == CW_COPY_MOORE;
@@ -1192,12 +1213,14 @@ int cw_lattice_set_copy_nbhd(cw_lattice l, int32_t nbhd) {
 }
 
 int cw_lattice_set_subsweeps(cw_lattice l, int32_t subsweeps) {
+    CW_SCOPE(l);
     if (subsweeps < 1 || subsweeps > 64) return fail(CW_ERR_CONFIG, "1 to 64 sub-sweeps a Monte Carlo step");
     l->subsweeps = subsweeps;
     return CW_OK;
 }
 
 int cw_lattice_set_temperature(cw_lattice l, double temperature) {
+    CW_SCOPE(l);
     if (!(temperature > 0.0)) return fail(CW_ERR_CONFIG, "the temperature must be positive");
     l->temperature = temperature;
     return CW_OK;
@@ -1233,16 +1256,19 @@ static int upload_range(cw_lattice l, uint32_t h0, uint32_t h1, const int32_t *g
 }
 
 int cw_lattice_upload(cw_lattice l, uint32_t hist, const int32_t *grid) {
+    CW_SCOPE(l);
     if (hist >= l->g.nh) return fail(CW_ERR_NOT_FOUND, "no history " + std::to_string(hist));
     return upload_range(l, hist, hist, grid);
 }
 
 int cw_lattice_upload_all(cw_lattice l, const int32_t *grids) {
+    CW_SCOPE(l);
     if (l->g.nh == 0) return CW_OK;
     return upload_range(l, 0, l->g.nh - 1, grids);
 }
 
 int cw_lattice_download(cw_lattice l, uint32_t hist, int32_t *grid) {
+    CW_SCOPE(l);
     if (hist >= l->g.nh) return fail(CW_ERR_NOT_FOUND, "no history " + std::to_string(hist));
     CW_CUDA(cudaMemcpyAsync(grid, l->grid + l->g.off[hist], sizeof(int32_t) * l->g.sites(hist), cudaMemcpyDeviceToHost,
                             stream()));
@@ -1251,6 +1277,7 @@ int cw_lattice_download(cw_lattice l, uint32_t hist, int32_t *grid) {
 }
 
 int cw_lattice_download_all(cw_lattice l, int32_t *grids) {
+    CW_SCOPE(l);
     CW_CUDA(cudaMemcpyAsync(grids, l->grid, sizeof(int32_t) * l->g.total, cudaMemcpyDeviceToHost, stream()));
     CW_CUDA(cudaStreamSynchronize(stream()));
     return CW_OK;
@@ -1265,6 +1292,7 @@ static int check_cells(cw_lattice l, uint32_t hist, uint32_t n) {
 
 int cw_cells_set(cw_lattice l, uint32_t hist, uint32_t n, const int32_t *type, const int32_t *volume,
                  const int32_t *target, const double *lambda) {
+    CW_SCOPE(l);
     int rc = check_cells(l, hist, n);
     if (rc != CW_OK) return rc;
     for (uint32_t i = 0; i < n; ++i)
@@ -1286,6 +1314,7 @@ int cw_cells_set(cw_lattice l, uint32_t hist, uint32_t n, const int32_t *type, c
 
 int cw_cells_get(cw_lattice l, uint32_t hist, uint32_t n, int32_t *type, int32_t *volume, int32_t *target,
                  double *lambda) {
+    CW_SCOPE(l);
     int rc = check_cells(l, hist, n);
     if (rc != CW_OK) return rc;
     int64_t c0 = l->cell_off[hist];
@@ -1299,6 +1328,7 @@ int cw_cells_get(cw_lattice l, uint32_t hist, uint32_t n, int32_t *type, int32_t
 
 int cw_cells_set_surface(cw_lattice l, uint32_t hist, uint32_t n, const int32_t *target_surface,
                          const double *lambda_surface) {
+    CW_SCOPE(l);
     int rc = check_cells(l, hist, n);
     if (rc != CW_OK) return rc;
     if (!l->surface_on) {
@@ -1317,6 +1347,7 @@ int cw_cells_set_surface(cw_lattice l, uint32_t hist, uint32_t n, const int32_t 
 }
 
 int cw_cells_get_surface(cw_lattice l, uint32_t hist, uint32_t n, int32_t *surface) {
+    CW_SCOPE(l);
     int rc = check_cells(l, hist, n);
     if (rc != CW_OK) return rc;
     if (!l->surface_on) return fail(CW_ERR_NOT_FOUND, "the surface constraint is off");
@@ -1326,6 +1357,7 @@ int cw_cells_get_surface(cw_lattice l, uint32_t hist, uint32_t n, int32_t *surfa
 }
 
 int cw_lattice_set_seed(cw_lattice l, uint32_t hist, uint64_t seed) {
+    CW_SCOPE(l);
     if (hist >= l->g.nh) return fail(CW_ERR_NOT_FOUND, "no history " + std::to_string(hist));
     l->seed[hist] = seed;
     uint2 k = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
@@ -1335,6 +1367,7 @@ int cw_lattice_set_seed(cw_lattice l, uint32_t hist, uint64_t seed) {
 }
 
 int cw_lattice_set_mcs(cw_lattice l, uint32_t mcs) {
+    CW_SCOPE(l);
     l->mcs = mcs;
     // the draws count sub-sweeps
     const uint32_t eff = mcs * (uint32_t)std::max(l->subsweeps, 1);
@@ -1344,11 +1377,13 @@ int cw_lattice_set_mcs(cw_lattice l, uint32_t mcs) {
 }
 
 int cw_lattice_get_mcs(cw_lattice l, uint32_t *mcs) {
+    CW_SCOPE(l);
     *mcs = l->mcs;
     return CW_OK;
 }
 
 int cw_lattice_mcs(cw_lattice l, uint32_t sweeps) {
+    CW_SCOPE(l);
     for (uint32_t s = 0; s < sweeps; ++s) {
         int rc = lattice_sweep(l);
         if (rc != CW_OK) return rc;
@@ -1359,6 +1394,7 @@ int cw_lattice_mcs(cw_lattice l, uint32_t sweeps) {
 
 int cw_lattice_delta_h_batch(cw_lattice l, uint32_t hist, uint32_t n, const int64_t *site, const int32_t *dst,
                              double *out) {
+    CW_SCOPE(l);
     if (hist >= l->g.nh) return fail(CW_ERR_NOT_FOUND, "no history " + std::to_string(hist));
     if (n == 0) return CW_OK;
     int64_t ns = l->g.sites(hist), cap = l->cell_off[hist + 1] - l->cell_off[hist];
@@ -1381,6 +1417,7 @@ int cw_lattice_delta_h_batch(cw_lattice l, uint32_t hist, uint32_t n, const int6
 }
 
 int cw_lattice_verify(cw_lattice l, uint32_t hist, int32_t *ok) {
+    CW_SCOPE(l);
     if (hist >= l->g.nh) return fail(CW_ERR_NOT_FOUND, "no history " + std::to_string(hist));
     int32_t *vol, *surf = nullptr;
     int *bad;

@@ -147,6 +147,7 @@ int network_upload(cw_network_s *n) {
 // field but the device copies.
 cw_network_s *network_derive(const cw_network_s *n) {
     cw_network_s *m = new cw_network_s();
+    m->hs.init(false);
     m->S = n->S;
     m->names = n->names;
     m->initial = n->initial;
@@ -285,6 +286,7 @@ int cw_network_compile(int32_t nnodes, const char *const *names, const double *i
     }
     for (int i = 0; i < nnodes; ++i) ptr[i + 1] += ptr[i];
     cw_network_s *n = new cw_network_s();
+    if (n->hs.init(false) != CW_OK) { delete n; return CW_ERR_CUDA; }
     auto role = [&](const char *name, const char *which, int32_t *dst) -> int {
         if (!name) { *dst = -1; return CW_OK; }
         auto it = index.find(name);
@@ -325,12 +327,24 @@ int cw_network_compile(int32_t nnodes, const char *const *names, const double *i
 
 int cw_network_destroy(cw_network n) {
     if (!n) return CW_OK;
+    CW_SCOPE(n);
     dfree(n->node_ptr); dfree(n->term); dfree(n->par);
+    n->hs.release();
     delete n;
     return CW_OK;
 }
 
+int cw_network_set_stream(cw_network n, void *stream) {
+    CW_SCOPE(n);
+    return n->hs.set((cudaStream_t)stream);
+}
+
+void *cw_network_get_stream(cw_network n) { return (void *)n->hs.stream; }
+
+const char *cw_network_last_error(cw_network n) { return n->hs.err.c_str(); }
+
 int cw_network_info(cw_network n, int32_t *nnodes, int32_t *roles7, double *initial) {
+    CW_SCOPE(n);
     if (nnodes) *nnodes = n->S;
     if (roles7) std::memcpy(roles7, n->roles, sizeof n->roles);
     if (initial) std::memcpy(initial, n->initial.data(), sizeof(double) * n->S);
@@ -339,6 +353,7 @@ int cw_network_info(cw_network n, int32_t *nnodes, int32_t *roles7, double *init
 
 int cw_network_step_batch(cw_network n, int64_t ncells, double *state, const double *inputs, double dt,
                           int32_t substeps) {
+    CW_SCOPE(n);
     if (ncells <= 0) return CW_OK;
     const int S = n->S;
     double *d_state, *d_in;
@@ -366,6 +381,7 @@ int cw_network_step_batch(cw_network n, int64_t ncells, double *state, const dou
 
 int cw_network_mechanics_batch(cw_network n, int64_t ncells, const double *state, uint32_t *target,
                                double *lambda) {
+    CW_SCOPE(n);
     if (ncells <= 0) return CW_OK;
     const int S = n->S;
     double *d_state;
@@ -387,6 +403,7 @@ int cw_network_mechanics_batch(cw_network n, int64_t ncells, const double *state
 }
 
 int cw_network_mutate(cw_network n, double which, double how, cw_network *out, cw_mutation *rec) {
+    CW_SCOPE(n);
     if (!out) return fail(CW_ERR_CONFIG, "no place for the mutated network");
     *out = nullptr;
     const size_t count = n->h_term.size();
@@ -407,6 +424,7 @@ int cw_network_mutate(cw_network n, double which, double how, cw_network *out, c
 }
 
 int cw_network_rewire(cw_network n, const double draws[5], cw_network *out, cw_mutation *rec) {
+    CW_SCOPE(n);
     if (!out || !draws) return fail(CW_ERR_CONFIG, "rewiring takes five draws and a place for the network");
     *out = nullptr;
     const double mode = draws[0], which = draws[1], source = draws[2], sign = draws[3], how = draws[4];

@@ -9,6 +9,7 @@
 #include "cw_internal.cuh"
 
 struct cw_network_s {
+    cw::HandleStream hs;  // its stream and last error
     int32_t S = 0, nterms = 0;
     std::vector<std::string> names;
     std::vector<double> initial;

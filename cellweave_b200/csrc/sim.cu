@@ -21,6 +21,7 @@
 using namespace cw;
 
 struct cw_sim_s {
+    cw::HandleStream hs;  // its stream (its lattice's and fields' too) and last error
     cw_sim_config cfg;
     std::vector<uint32_t> w, h, d, ncells;
     std::vector<uint64_t> obstacles;  // obstacle pixels seeded per history (a vessel's)
@@ -531,6 +532,8 @@ int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out) {
     if (!net) return fail(CW_ERR_CONFIG, "a simulation needs a network");
     int32_t survival = network_role(net, 1);
     cw_sim_s *s = new cw_sim_s();
+    if (s->hs.init() != CW_OK) { delete s; return CW_ERR_CUDA; }
+    CW_SCOPE(s);  // its lattice and fields take its stream
     s->cfg = c;
     s->w.assign(c.w, c.w + c.nh);
     s->h.assign(c.h, c.h + c.nh);
@@ -727,6 +730,7 @@ int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out) {
 
 int cw_sim_destroy(cw_sim s) {
     if (!s) return CW_OK;
+    CW_SCOPE(s);
     drop_graphs(s);
     cw_lattice_destroy(s->lat);
     cw_field_destroy(s->o2);
@@ -740,6 +744,7 @@ int cw_sim_destroy(cw_sim s) {
     dfree(s->d_sink); dfree(s->cell_o2); dfree(s->cell_sig); dfree(s->sum); dfree(s->secretion); dfree(s->count);
     dfree(s->state); dfree(s->inputs); dfree(s->alive); dfree(s->target32);
     s->sites.release();
+    s->hs.release();
     delete s;
     return CW_OK;
 }
@@ -1063,6 +1068,7 @@ static int step_graph(cw_sim_s *s, const cw_relax_opts &o) {
 }
 
 int cw_sim_step(cw_sim s, uint32_t nsteps) {
+    CW_SCOPE(s);
     const cw_sim_config &c = s->cfg;
     int64_t nc = s->nc;
     int S = network_nodes(s->net);
@@ -1223,6 +1229,7 @@ int cw_sim_step(cw_sim s, uint32_t nsteps) {
 }
 
 int cw_sim_graph_info(cw_sim s, uint64_t *graph_steps, uint64_t *budget_misses, int32_t *budgets) {
+    CW_SCOPE(s);
     if (graph_steps) *graph_steps = s->graph_steps;
     if (budget_misses) *budget_misses = s->budget_misses;
     if (budgets) { budgets[0] = s->budget[0]; budgets[1] = s->budget[1]; }
@@ -1231,6 +1238,7 @@ int cw_sim_graph_info(cw_sim s, uint64_t *graph_steps, uint64_t *budget_misses, 
 
 int cw_sim_tuning(cw_sim s, double *omega_o2, double *omega_signal, int32_t *depth, int32_t *window,
                   int32_t *tuning) {
+    CW_SCOPE(s);
     for (uint32_t k = 0; k < s->cfg.nh; ++k) {
         if (omega_o2) omega_o2[k] = s->omega[0][k];
         if (omega_signal) omega_signal[k] = s->omega[1][k];
@@ -1241,12 +1249,32 @@ int cw_sim_tuning(cw_sim s, double *omega_o2, double *omega_signal, int32_t *dep
     return CW_OK;
 }
 
+// The simulation's stream is its lattice's and fields' too.
+int cw_sim_set_stream(cw_sim s, void *stream) {
+    CW_SCOPE(s);
+    // the old stream's work finishes first (set synchronises it)
+    int rc = s->hs.set((cudaStream_t)stream);
+    if (rc != CW_OK) return rc;
+    // the children follow the simulation's stream without owning it
+    if (s->lat) { s->lat->hs.stream = s->hs.stream; s->lat->hs.own = false; }
+    cw_field_s *fs[5] = {s->o2, s->sig, s->wst, s->nfc, s->str};
+    for (cw_field_s *f : fs)
+        if (f) { f->hs.stream = s->hs.stream; f->hs.own = false; }
+    return CW_OK;
+}
+
+void *cw_sim_get_stream(cw_sim s) { return (void *)s->hs.stream; }
+
+const char *cw_sim_last_error(cw_sim s) { return s->hs.err.c_str(); }
+
 int cw_sim_lattice(cw_sim s, cw_lattice *lat) {
+    CW_SCOPE(s);
     *lat = s->lat;
     return CW_OK;
 }
 
 int cw_sim_field(cw_sim s, int32_t which, cw_field *f) {
+    CW_SCOPE(s);
     *f = which == 0 ? s->o2 : which == 1 ? s->sig : which == 2 ? s->wst : which == 3 ? s->nfc
        : which == 4 ? s->str : nullptr;
     if (!*f) return fail(CW_ERR_NOT_FOUND, "no such field");
@@ -1254,6 +1282,7 @@ int cw_sim_field(cw_sim s, int32_t which, cw_field *f) {
 }
 
 int cw_sim_stats(cw_sim s, double *out) {
+    CW_SCOPE(s);
     uint32_t nh = s->cfg.nh;
     double *d_out;
     int rc = dalloc(&d_out, 4 * (size_t)nh);
@@ -1274,6 +1303,7 @@ int cw_sim_stats(cw_sim s, double *out) {
 }
 
 int cw_sim_touches_edge(cw_sim s, int32_t *out) {
+    CW_SCOPE(s);
     const cw_sim_config &c = s->cfg;
     int32_t *d_out = nullptr;
     int rc = dalloc(&d_out, c.nh);
@@ -1291,6 +1321,7 @@ int cw_sim_touches_edge(cw_sim s, int32_t *out) {
 }
 
 int cw_sim_measure(cw_sim s, cw_measurements *out) {
+    CW_SCOPE(s);
     const cw_sim_config &c = s->cfg;
     const uint32_t nh = c.nh;
     cw_lattice_s *l = s->lat;
@@ -1352,6 +1383,7 @@ int cw_sim_measure(cw_sim s, cw_measurements *out) {
 }
 
 int cw_sim_network_state(cw_sim s, uint32_t hist, uint32_t n, double *state) {
+    CW_SCOPE(s);
     if (hist >= s->cfg.nh) return fail(CW_ERR_NOT_FOUND, "no history " + std::to_string(hist));
     int S = network_nodes(s->net);
     int64_t c0 = s->lat->cell_off[hist], cap = s->lat->cell_off[hist + 1] - c0;
@@ -1367,6 +1399,7 @@ int cw_sim_network_state(cw_sim s, uint32_t hist, uint32_t n, double *state) {
 }
 
 int cw_sim_cycle(cw_sim s, uint32_t hist, uint32_t n, int32_t *began, int32_t *due) {
+    CW_SCOPE(s);
     if (hist >= s->cfg.nh) return fail(CW_ERR_NOT_FOUND, "no history " + std::to_string(hist));
     if (!s->due) return fail(CW_ERR_CONFIG, "this simulation has no cell cycle");
     int64_t c0 = s->lat->cell_off[hist], cap = s->lat->cell_off[hist + 1] - c0;

@@ -21,9 +21,17 @@
  *    uneven sizes ("hist" selects one); a plain single history is a batch of
  *    one.  Cell ids are per history, 0 the medium, -1 the obstacle
  *    (u32::MAX in the reference: the same bits).
- *  - All work is queued on one library stream (cw_set_stream to choose it);
- *    calls that return host data synchronise it.  One host thread at a time
- *    per library, as the reference's &mut receivers require.
+ *  - Every handle queues its work on its own CUDA stream, created with it
+ *    (a simulation's lattice and fields share the simulation's; a fit takes
+ *    its lattice's); cw_*_set_stream hands in the caller's stream instead.
+ *    A call that reads two handles (cw_couple_*) orders their streams with
+ *    events.  Calls that return host data synchronise the handle's stream.
+ *    One host thread at a time per handle, as the reference's &mut receivers
+ *    require (simulation.rs:456); different handles may be driven from
+ *    different threads at once.  cw_*_last_error(h) gives the message of the
+ *    last failure of a call on h, cw_last_error() that of the calling thread.
+ *    Calls without a handle (cw_field_relax_noalloc, cw_event_record,
+ *    cw_network_step_clones) use the library stream (cw_set_stream).
  *  - No CPU path: without a usable CUDA device every call that would launch
  *    work returns CW_ERR_CUDA.
  */
@@ -56,8 +64,28 @@ typedef struct cw_fit_s *cw_fit;
 /* ------------------------------------------------------------------ library */
 const char *cw_last_error(void);
 int cw_version(void);
-/* Stream all work is queued on (a cudaStream_t); NULL restores the library's own. */
+/* The library stream, for calls without a handle (a cudaStream_t); NULL
+ * restores the library's own. */
 int cw_set_stream(void *stream);
+/* Each handle's stream (a cudaStream_t): the caller's, or NULL for a new one
+ * of the handle's own; work queued before finishes first.  A simulation's
+ * lattice and fields follow cw_sim_set_stream (do not set theirs apart).
+ * The per-handle streams stand for the reference's exclusive &mut borrow of
+ * each object (simulation.rs:456): handles on different streams run at once. */
+int cw_lattice_set_stream(cw_lattice lat, void *stream);
+int cw_field_set_stream(cw_field f, void *stream);
+int cw_network_set_stream(cw_network net, void *stream);
+int cw_sim_set_stream(cw_sim sim, void *stream);
+void *cw_lattice_get_stream(cw_lattice lat);
+void *cw_field_get_stream(cw_field f);
+void *cw_network_get_stream(cw_network net);
+void *cw_sim_get_stream(cw_sim sim);
+/* The message of the last failure of a call on the handle ("" if none). */
+const char *cw_lattice_last_error(cw_lattice lat);
+const char *cw_field_last_error(cw_field f);
+const char *cw_network_last_error(cw_network net);
+const char *cw_sim_last_error(cw_sim sim);
+const char *cw_fit_last_error(cw_fit fit);
 /* The CUDA device the library works on (one per process). */
 int cw_set_device(int32_t device);
 void *cw_get_stream(void);
@@ -74,8 +102,11 @@ uint64_t cw_launch_count(void);
  * out (CW_ERR_TIMEOUT).  Every call replaces all four; (0, -1, 0, 0) is the
  * default.  Work captured in a CUDA graph keeps the settings of its capture. */
 int cw_test_faults(uint64_t wait_ns, int32_t withhold_block, int32_t max_rounds, int32_t skip_tma);
-/* CUDA events on the library stream, in slots 0..15, for timing. */
+/* CUDA events on the library stream, in slots 0..15, for timing.  cw_synchronize
+ * waits for every stream of the device. */
 int cw_event_record(int32_t slot);
+/* The same on a given stream (a handle's, from cw_*_get_stream); NULL: the library stream. */
+int cw_event_record_on(void *stream, int32_t slot);
 int cw_event_elapsed(int32_t a, int32_t b, float *ms);
 /* cudaProfilerStart / cudaProfilerStop around a region (for ncu --profile-from-start off). */
 int cw_profiler_start(void);
