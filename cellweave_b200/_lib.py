@@ -102,7 +102,8 @@ class SimConfig(C.Structure):
                 ("first_tolerance", C.c_double), ("cycle_median", C.c_double), ("cycle_spread", C.c_double),
                 ("debris_loss", C.c_double), ("still_medium", C.c_double),
                 ("exposure_intensity", C.c_double), ("exposure_uptake", C.c_double), ("exposure_start", C.c_int32),
-                ("exposure_on", C.c_int32), ("exposure_off", C.c_int32)]
+                ("exposure_on", C.c_int32), ("exposure_off", C.c_int32), ("mutation_rate", C.c_double),
+                ("rewiring", C.c_double)]
 
 
 P = C.c_void_p
@@ -116,6 +117,9 @@ SIGNATURES = {
     "cw_get_stream": (P, []),
     "cw_synchronize": (C.c_int, []),
     "cw_launch_count": (C.c_uint64, []),
+    "cw_sim_clones": (C.c_int, [P, U32, U32, P]),
+    "cw_sim_clone_count": (C.c_int, [P, P]),
+    "cw_sim_clone_records": (C.c_int, [P, P, P]),
     "cw_test_faults": (C.c_int, [U64, I32, I32, I32]),
     "cw_event_record_on": (C.c_int, [P, I32]),
     "cw_lattice_set_stream": (C.c_int, [P, P]),

@@ -11,10 +11,11 @@ cells (ContactEnergy::default, cpm.rs:63-86), oxygen diffusing at 0.2 and
 taken up at ``oxygen_uptake`` by every living pixel (and by the stroma around
 a vessel), networks stepped eight units of their time a step, division
 checked every 20 steps (every step with a cell cycle of its own); an
-exposure's stress, waste, necrotic factor, debris loss and a still medium
+exposure's stress, waste, necrotic factor, debris loss, a still medium and
+daughters that mutate or rewire their networks (mutation_rate, rewiring)
 when configured.  Every other feature of the file (capillaries, sheets,
-mutation and rewiring, lesions, angiogenesis, immunity, tracing) is refused
-by name.  ``run`` steps it for ``mcs`` steps or until the tissue touches the
+suppressed clones, lesions, angiogenesis, immunity, tracing) is refused by
+name.  ``run`` steps it for ``mcs`` steps or until the tissue touches the
 box's edge, writing measurements.csv and the snapshots as the reference
 does.
 
@@ -94,9 +95,10 @@ def _refuse(cfg):
     for key in ("lesion", "angiogenesis", "immunity", "tracing", "suppress_before"):
         if cfg.get(key) is not None:
             raise ConfigError(f"{name}: `{key}` is not part of the device step")
-    if cfg["mutation_rate"] or cfg["rewiring"] or cfg["suppress"]:
-        raise ConfigError(f"{name}: mutation and rewiring are not part of the device step "
-                          "(cw_network_mutate / rewire derive the networks; the step does not draw them)")
+    if cfg["suppress"]:
+        raise ConfigError(f"{name}: `suppress` is not part of the device step (its mutations are all made)")
+    if not 0.0 <= float(cfg["mutation_rate"]) <= 1.0 or not 0.0 <= float(cfg["rewiring"]) <= 1.0:
+        raise ConfigError(f"{name}: mutation_rate and rewiring are chances, in [0, 1]")
     if cfg["contact_order"] not in (1, 2, 3):
         raise ConfigError(f"{name}: contact_order is {cfg['contact_order']}; it is 1, 2 or 3")
     if cfg["network"] is None:
@@ -153,6 +155,8 @@ def simulation_kwargs(cfg, histories=1, seeds=None, subsweeps=4):
         if "diffusion" not in cfg["still_medium"]:
             raise ConfigError(f"{os.path.basename(cfg['path'])}: a still medium names its diffusion")
         kw["still_medium"] = float(cfg["still_medium"]["diffusion"])
+    if cfg["mutation_rate"]:
+        kw.update(mutation_rate=float(cfg["mutation_rate"]), rewiring=float(cfg["rewiring"]))
     if cfg.get("waste"):
         kw["waste_production"] = float(cfg["waste"]["production"])
     if cfg.get("necrotic_factor"):

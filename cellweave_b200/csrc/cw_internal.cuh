@@ -373,6 +373,11 @@ namespace cw {
 // network (network.cu), device-resident, node-major state [S][stride]
 int network_step_device(const cw_network_s *n, double *state, const double *inputs, int64_t ncells,
                         int64_t state_stride, int64_t input_stride, double dt, int substeps, const uint8_t *alive);
+struct NetDev;
+NetDev net_dev(const cw_network_s *n);
+int network_step_clones_device(const NetDev *nets, const int32_t *clone, int S, double *state, const double *inputs,
+                               int64_t ncells, int64_t state_stride, int64_t input_stride, double dt, int substeps,
+                               const uint8_t *alive);
 int network_mechanics_device(const cw_network_s *n, const double *state, int64_t ncells, int64_t stride,
                              uint32_t *target);
 int32_t network_nodes(const cw_network_s *n);

@@ -92,20 +92,25 @@ __global__ void __launch_bounds__(RT) k_rk4(NetDev N, double *state, const doubl
 // The same for cells of many networks: cell c under nets[clone[c]], its
 // terms read from global memory (a network's tables are a few KB: they stay
 // in L1 across the block's cells of that network).
+// state: [S][state_stride], inputs: [6][input_stride]; alive (optional):
+// cells whose entry is zero are left as they are.
 __global__ void __launch_bounds__(RT) k_rk4_clones(const NetDev *nets, const int32_t *clone, int S, double *state,
-                                                   const double *inputs, int64_t ncells, double dt, int substeps) {
+                                                   const double *inputs, int64_t ncells, int64_t state_stride,
+                                                   int64_t input_stride, double dt, int substeps,
+                                                   const uint8_t *alive) {
     extern __shared__ double sm[];
     double *x = sm, *mid = sm + S * RT, *kk = sm + 2 * S * RT, *acc = sm + 3 * S * RT;
     int64_t c = (int64_t)blockIdx.x * RT + threadIdx.x;
     if (c >= ncells) return;
+    if (alive && !alive[c]) return;
     const NetDev N = nets[clone[c]];
     const int tid = threadIdx.x;
     double in[6];
-    for (int q = 0; q < 6; ++q) in[q] = inputs[q * ncells + c];
+    for (int q = 0; q < 6; ++q) in[q] = inputs[q * input_stride + c];
     double *xs = x + tid, *ms = mid + tid, *ks = kk + tid, *as = acc + tid;
-    for (int i = 0; i < S; ++i) xs[i * RT] = state[i * ncells + c];
+    for (int i = 0; i < S; ++i) xs[i * RT] = state[i * state_stride + c];
     rk4_cell(N, N.term, N.par, N.node_ptr, xs, ms, ks, as, in, dt, substeps);
-    for (int i = 0; i < S; ++i) state[i * ncells + c] = xs[i * RT];
+    for (int i = 0; i < S; ++i) state[i * state_stride + c] = xs[i * RT];
 }
 
 // mechanics, network.rs:811-821.
@@ -195,6 +200,22 @@ int network_step_device(const cw_network_s *n, double *state, const double *inpu
     size_t smem = rk4_smem(n);
     k_rk4<<<(unsigned)((ncells + RT - 1) / RT), RT, smem, stream()>>>(net_dev(n), state, inputs, ncells, state_stride,
                                                                       input_stride, dt, substeps, alive);
+    CW_LAUNCHED();
+    return CW_OK;
+}
+
+// RK4 for cells of many networks on node-major state (the driver's evolving
+// histories): cell c under nets[clone[c]], living cells only.
+int network_step_clones_device(const NetDev *nets, const int32_t *clone, int S, double *state, const double *inputs,
+                               int64_t ncells, int64_t state_stride, int64_t input_stride, double dt, int substeps,
+                               const uint8_t *alive) {
+    if (ncells <= 0) return CW_OK;
+    const size_t smem = sizeof(double) * 4 * S * RT;
+    if (smem > 48 * 1024)
+        CW_CUDA(cudaFuncSetAttribute(k_rk4_clones, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_rk4_clones<<<(unsigned)((ncells + RT - 1) / RT), RT, smem, stream()>>>(nets, clone, S, state, inputs, ncells,
+                                                                          state_stride, input_stride, dt, substeps,
+                                                                          alive);
     CW_LAUNCHED();
     return CW_OK;
 }
@@ -499,7 +520,7 @@ int cw_network_step_clones(int32_t nnets, const cw_network *nets, int64_t ncells
     CW_CUDA(cudaMemcpy(d_nets, dev.data(), sizeof(NetDev) * nnets, cudaMemcpyHostToDevice));
     CW_CUDA(cudaMemcpy(d_clone, clone, sizeof(int32_t) * ncells, cudaMemcpyHostToDevice));
     k_rk4_clones<<<(unsigned)((ncells + RT - 1) / RT), RT, smem, stream()>>>(d_nets, d_clone, S, d_state, d_in, ncells,
-                                                                          dt, substeps);
+                                                                          ncells, ncells, dt, substeps, nullptr);
     CW_LAUNCHED();
     CW_CUDA(cudaGetLastError());
     CW_CUDA(cudaMemcpyAsync(t.data(), d_state, sizeof(double) * ncells * S, cudaMemcpyDeviceToHost, stream()));

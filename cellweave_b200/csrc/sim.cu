@@ -17,6 +17,7 @@
 #include <random>
 
 #include "cw_internal.cuh"
+#include "network_kernels.cuh"
 
 using namespace cw;
 
@@ -54,6 +55,16 @@ struct cw_sim_s {
     uint8_t *alive = nullptr;
     uint32_t *target32 = nullptr;
     int64_t nc = 0;                 // records over all histories
+    // an evolving batch (mutation_rate > 0): every record's clone, the clones'
+    // networks (0: the founding one, not owned) and their device tables
+    bool evolve = false;
+    std::vector<cw_network_s *> clones;
+    std::vector<int32_t> clone_parent;
+    std::vector<cw_mutation> clone_mutation;
+    std::vector<int32_t> h_clone;
+    int32_t *d_clone = nullptr;
+    cw::NetDev *d_nets = nullptr;
+    size_t nets_cap = 0;
     Plan sites;
     std::vector<cw_relax_stats> last;
     uint32_t steps = 0;
@@ -86,6 +97,7 @@ struct cw_sim_s {
 
 extern "C" {
 static void tune_begin(cw_sim_s *s);
+static int upload_clones(cw_sim_s *s, bool tables);
 static void drop_graphs(cw_sim_s *s);
 }
 
@@ -529,6 +541,10 @@ int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out) {
             if (!c.d || c.d[k] <= 1)
                 return fail(CW_ERR_CONFIG, "a still medium is solved around a ball, and a plane has none");
     }
+    if (!(c.mutation_rate >= 0.0 && c.mutation_rate <= 1.0) || !(c.rewiring >= 0.0 && c.rewiring <= 1.0))
+        return fail(CW_ERR_CONFIG, "the mutation rate and the rewiring share lie in [0, 1]");
+    if (c.mutation_rate > 0.0 && !c.divide)
+        return fail(CW_ERR_CONFIG, "mutations come at divisions, and this simulation does not divide");
     if (!net) return fail(CW_ERR_CONFIG, "a simulation needs a network");
     int32_t survival = network_role(net, 1);
     cw_sim_s *s = new cw_sim_s();
@@ -691,6 +707,16 @@ int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out) {
         CW_CUDA(cudaMemsetAsync(s->began, 0, sizeof(int32_t) * nc, stream()));
         CW_CUDA(cudaMemsetAsync(s->due, 0, sizeof(int32_t) * nc, stream()));
     }
+    if (c.mutation_rate > 0.0) {
+        // every record starts in the founding clone
+        s->evolve = true;
+        s->clones.assign(1, net);
+        s->h_clone.assign(nc, 0);
+        if ((rc = dalloc(&s->d_clone, nc)) != CW_OK || (rc = upload_clones(s, true)) != CW_OK) {
+            cw_sim_destroy(s);
+            return rc;
+        }
+    }
     CW_CUDA(cudaMemsetAsync(s->d_step, 0, sizeof(uint32_t), stream()));
     CW_CUDA(cudaMemsetAsync(s->died_at, 0xFF, sizeof(int32_t) * nc, stream()));
     CW_CUDA(cudaMemsetAsync(s->cell_wst, 0, sizeof(double) * nc, stream()));
@@ -743,6 +769,8 @@ int cw_sim_destroy(cw_sim s) {
     dfree(s->d_step); dfree(s->bath); dfree(s->d_uptake);
     dfree(s->d_sink); dfree(s->cell_o2); dfree(s->cell_sig); dfree(s->sum); dfree(s->secretion); dfree(s->count);
     dfree(s->state); dfree(s->inputs); dfree(s->alive); dfree(s->target32);
+    for (size_t k = 1; k < s->clones.size(); ++k) cw_network_destroy(s->clones[k]);
+    dfree(s->d_clone); dfree(s->d_nets);
     s->sites.release();
     s->hs.release();
     delete s;
@@ -838,6 +866,84 @@ static void drop_graphs(cw_sim_s *s) {
     s->graphs = false;
 }
 
+// The clone of every record and the clones' network tables onto the device
+// (all of the tables when `tables`).
+static int upload_clones(cw_sim_s *s, bool tables) {
+    if (tables) {
+        if (s->clones.size() > s->nets_cap) {
+            dfree(s->d_nets);
+            s->nets_cap = std::max<size_t>(2 * s->clones.size(), 16);
+            int rc = dalloc(&s->d_nets, s->nets_cap);
+            if (rc != CW_OK) { s->nets_cap = 0; return rc; }
+        }
+        std::vector<cw::NetDev> dev(s->clones.size());
+        for (size_t k = 0; k < s->clones.size(); ++k) dev[k] = cw::net_dev(s->clones[k]);
+        CW_CUDA(cudaMemcpyAsync(s->d_nets, dev.data(), sizeof(cw::NetDev) * dev.size(), cudaMemcpyHostToDevice,
+                                stream()));
+    }
+    CW_CUDA(cudaMemcpyAsync(s->d_clone, s->h_clone.data(), sizeof(int32_t) * s->h_clone.size(),
+                            cudaMemcpyHostToDevice, stream()));
+    CW_CUDA(cudaStreamSynchronize(stream()));
+    return CW_OK;
+}
+
+// Daughters that are not quite copies (simulation.rs:1655-1700): after a
+// division step, each daughter joins its parent's clone; with chance
+// mutation_rate its network changes (mutate, or with chance `rewiring`
+// rewire) and it founds a clone of its own.  The draws come from Philox
+// under the history's key, counter (parent id, step, 6 / 7 / 8, 0): the rate
+// test and `which` from the first, `how` and the rewiring test from the
+// second, the gained link's source and sign from the third.
+static int evolve_after_division(cw_sim_s *s) {
+    cw_lattice_s *l = s->lat;
+    int32_t count = 0;
+    CW_CUDA(cudaMemcpyAsync(&count, l->div.count, sizeof(int32_t), cudaMemcpyDeviceToHost, stream()));
+    CW_CUDA(cudaStreamSynchronize(stream()));
+    if (count == 0) return CW_OK;  // no cell was ready: the daughters' table is last step's
+    std::vector<int32_t> dg(s->nc);
+    CW_CUDA(cudaMemcpyAsync(dg.data(), l->div.daughter, sizeof(int32_t) * s->nc, cudaMemcpyDeviceToHost, stream()));
+    CW_CUDA(cudaStreamSynchronize(stream()));
+    const cw_sim_config &c = s->cfg;
+    const uint32_t step = (uint32_t)s->steps;
+    bool grown = false, moved = false;
+    for (uint32_t h = 0; h < c.nh; ++h) {
+        const int64_t c0 = l->cell_off[h], cap = l->cell_off[h + 1] - c0;
+        const uint64_t seed = l->seed[h];
+        const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+        for (int64_t id = 1; id < cap; ++id) {
+            const int32_t d = dg[c0 + id];
+            if (d < 0) continue;
+            const int32_t parent_clone = s->h_clone[c0 + id];
+            s->h_clone[c0 + d] = parent_clone;
+            moved = true;
+            const uint4 r0 = cw::philox((uint32_t)id, step, 6u, 0u, k0, k1);
+            if (!(cw::u01(r0.x, r0.y) < c.mutation_rate)) continue;
+            const double which = cw::u01(r0.z, r0.w);
+            const uint4 r1 = cw::philox((uint32_t)id, step, 7u, 0u, k0, k1);
+            const double how = cw::u01(r1.x, r1.y);
+            cw_network nn = nullptr;
+            cw_mutation rec{};
+            int rc;
+            double u = c.rewiring > 0.0 ? cw::u01(r1.z, r1.w) : 1.0;
+            if (c.rewiring > 0.0 && u < c.rewiring) {
+                const uint4 r2 = cw::philox((uint32_t)id, step, 8u, 0u, k0, k1);
+                const double draws[5] = {u / c.rewiring, which, cw::u01(r2.x, r2.y), cw::u01(r2.z, r2.w), how};
+                rc = cw_network_rewire(s->clones[parent_clone], draws, &nn, &rec);
+            } else {
+                rc = cw_network_mutate(s->clones[parent_clone], which, how, &nn, &rec);
+            }
+            if (rc == CW_ERR_NOT_FOUND) continue;  // nothing to change: the daughter stays in its parent's clone
+            if (rc != CW_OK) return rc;
+            s->clones.push_back(nn);
+            s->clone_parent.push_back(parent_clone);
+            s->clone_mutation.push_back(rec);
+            s->h_clone[c0 + d] = (int32_t)(s->clones.size() - 1);
+            grown = true;
+        }
+    }
+    return moved ? upload_clones(s, grown) : CW_OK;
+}
+
 // The division step (simulation.rs:1338-1347): every step, the ready cells
 // of each history in id order as far as the living-cell limit allows, each
 // daughter taking a copy of its parent's network state.
@@ -855,6 +961,7 @@ static int division_step(cw_sim_s *s) {
     CW_LAUNCHED();
     int rc = lattice_divide_enqueue(l, s->alive, c.max_cells > 0 ? c.max_cells : DEFAULT_MAX_CELLS, s->state,
                                     network_nodes(s->net));
+    if (rc == CW_OK && s->evolve) rc = evolve_after_division(s);
     if (rc != CW_OK || !s->due) return rc;
     k_cycle_births<<<(unsigned)blocks(nc), T, 0, stream()>>>(l->d_cell_off, (int)c.nh, nc, l->div.daughter, l->d_keys,
                                                              s->d_step, c.cycle_median, c.cycle_spread, s->began,
@@ -937,6 +1044,17 @@ static int paint_oxygen(cw_sim_s *s) {
     return CW_OK;
 }
 
+// Every living cell's network: the one network, or in an evolving batch each
+// cell under its clone's.
+static int step_networks(cw_sim_s *s) {
+    const cw_sim_config &c = s->cfg;
+    const int64_t nc = s->nc;
+    if (s->evolve)
+        return network_step_clones_device(s->d_nets, s->d_clone, network_nodes(s->net), s->state, s->inputs, nc, nc,
+                                          nc, c.dt, c.substeps, s->alive);
+    return network_step_device(s->net, s->state, s->inputs, nc, nc, nc, c.dt, c.substeps, s->alive);
+}
+
 // One of the three phases of a step, enqueued without host synchronisation.
 static int enqueue_phase(cw_sim_s *s, int p, const cw_relax_opts &o) {
     const cw_sim_config &c = s->cfg;
@@ -962,8 +1080,7 @@ static int enqueue_phase(cw_sim_s *s, int p, const cw_relax_opts &o) {
     }
     if (s->sig && (rc = couple_means_device(s->sig, s->lat, s->sum, s->count, s->cell_sig, s->sites)) != CW_OK)
         return rc;
-    if ((rc = network_step_device(s->net, s->state, s->inputs, nc, nc, nc, c.dt, c.substeps, s->alive)) != CW_OK)
-        return rc;
+    if ((rc = step_networks(s)) != CW_OK) return rc;
     if ((rc = network_mechanics_device(s->net, s->state, nc, nc, s->target32)) != CW_OK) return rc;
     k_fates<<<(unsigned)blocks(nc), T, 0, stream()>>>(s->alive, s->state, nc, network_role(s->net, 1),
                                                       c.death_threshold, c.necrotic_type, s->target32, s->lat->type,
@@ -1088,7 +1205,7 @@ int cw_sim_step(cw_sim s, uint32_t nsteps) {
         const bool graph_ok = c.use_graphs && c.precision == CW_FP32_DC && c.relax_every <= 1 && !s->tune.active &&
                               s->depth_tuned && s->steps >= 2 && !s->last.empty() &&
                               (!s->sig || !s->last_sig.empty()) && !s->wst && !s->nfc && c.o2_hold != 3 &&
-                              !s->debris_on && !s->str;
+                              !s->debris_on && !s->str && !s->evolve;
         if (graph_ok) {
             if (!s->graphs && (rc = build_graphs(s, o)) != CW_OK) return rc;
             if ((rc = step_graph(s, o)) != CW_OK) return rc;
@@ -1195,8 +1312,7 @@ int cw_sim_step(cw_sim s, uint32_t nsteps) {
             CW_LAUNCHED();
         }
         // 3. every living network
-        if ((rc = network_step_device(s->net, s->state, s->inputs, nc, nc, nc, c.dt, c.substeps, s->alive)) != CW_OK)
-            return rc;
+        if ((rc = step_networks(s)) != CW_OK) return rc;
         // 4. fates and mechanics
         if ((rc = network_mechanics_device(s->net, s->state, nc, nc, s->target32)) != CW_OK) return rc;
         k_fates<<<(unsigned)blocks(nc), T, 0, stream()>>>(s->alive, s->state, nc, survival, c.death_threshold,
@@ -1266,6 +1382,29 @@ int cw_sim_set_stream(cw_sim s, void *stream) {
 void *cw_sim_get_stream(cw_sim s) { return (void *)s->hs.stream; }
 
 const char *cw_sim_last_error(cw_sim s) { return s->hs.err.c_str(); }
+
+int cw_sim_clones(cw_sim s, uint32_t hist, uint32_t n, int32_t *clone) {
+    CW_SCOPE(s);
+    if (hist >= s->cfg.nh) return fail(CW_ERR_NOT_FOUND, "no history " + std::to_string(hist));
+    const int64_t c0 = s->lat->cell_off[hist], cap = s->lat->cell_off[hist + 1] - c0;
+    if ((int64_t)n > cap) return fail(CW_ERR_CONFIG, "history " + std::to_string(hist) + " holds " +
+                                                         std::to_string(cap) + " records");
+    for (uint32_t k = 0; k < n; ++k) clone[k] = s->evolve ? s->h_clone[c0 + k] : 0;
+    return CW_OK;
+}
+
+int cw_sim_clone_count(cw_sim s, uint32_t *nclones) {
+    *nclones = s->evolve ? (uint32_t)s->clones.size() : 1u;
+    return CW_OK;
+}
+
+int cw_sim_clone_records(cw_sim s, int32_t *parent, cw_mutation *mutation) {
+    for (size_t k = 0; k < s->clone_parent.size(); ++k) {
+        if (parent) parent[k] = s->clone_parent[k];
+        if (mutation) mutation[k] = s->clone_mutation[k];
+    }
+    return CW_OK;
+}
 
 int cw_sim_lattice(cw_sim s, cw_lattice *lat) {
     CW_SCOPE(s);

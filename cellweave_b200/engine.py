@@ -627,7 +627,8 @@ class Simulation:
                  waste_production=0.0, necrotic_production=0.0, necrotic_release_for=-1, subsweeps=1,
                  o2_uptake=0.0, divide_every=1, vessel_radius=0, stop_rule=STOP_RESIDUAL, first_tolerance=0.0,
                  cycle_median=0.0, cycle_spread=0.0, debris_loss=0.0, still_medium=0.0, exposure_intensity=0.0,
-                 exposure_uptake=0.0, exposure_start=0, exposure_on=0, exposure_off=0):
+                 exposure_uptake=0.0, exposure_start=0, exposure_on=0, exposure_off=0, mutation_rate=0.0,
+                 rewiring=0.0):
         self.dims, w, h, z = _dims(dims)
         self._keep = [w, h, z]
         nc = np.array(ncells, np.uint32)
@@ -648,7 +649,8 @@ class Simulation:
                              int(necrotic_release_for), int(subsweeps), float(o2_uptake), int(divide_every),
                              int(vessel_radius), int(stop_rule), float(first_tolerance), float(cycle_median),
                              float(cycle_spread), float(debris_loss), float(still_medium), float(exposure_intensity),
-                             float(exposure_uptake), int(exposure_start), int(exposure_on), int(exposure_off))
+                             float(exposure_uptake), int(exposure_start), int(exposure_on), int(exposure_off),
+                             float(mutation_rate), float(rewiring))
         handle = C.c_void_p()
         call("cw_sim_create", C.byref(cfg), network.handle, C.byref(handle))
         self._h = handle
@@ -732,6 +734,22 @@ class Simulation:
         out = np.zeros(len(self.dims), np.int32)
         call("cw_sim_touches_edge", self._h, ptr(out))
         return out.astype(bool)
+
+    def clones(self, n, hist=0):
+        """The clone of records 0..n-1 of a history (0: the founding network)."""
+        out = np.zeros(int(n), np.int32)
+        call("cw_sim_clones", self._h, int(hist), int(n), ptr(out))
+        return out
+
+    def clone_records(self):
+        """Every clone founded so far, in order: (parent clone, mutation record)."""
+        n = C.c_uint32()
+        call("cw_sim_clone_count", self._h, C.byref(n))
+        k = n.value - 1
+        parent = np.zeros(max(k, 1), np.int32)
+        recs = (_lib.Mutation * max(k, 1))()
+        call("cw_sim_clone_records", self._h, ptr(parent), recs)
+        return [(int(parent[i]), self.network._record(recs[i])) for i in range(k)]
 
     def cycle(self, n, hist=0):
         """(began, due) of records 0..n-1 of a history: each cell's cycle."""

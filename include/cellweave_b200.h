@@ -492,11 +492,28 @@ typedef struct {
                                     medium around a vessel); a cell's mean is its network's stress input */
     double exposure_uptake;
     int32_t exposure_start, exposure_on, exposure_off;
+    double mutation_rate;        /* (0, 1]: at each division the daughter's network changes with this chance and
+                                    the daughter founds a clone (simulation.rs:1655-1700): one rate scaled by up
+                                    to MUTATION_SPREAD either way (Network::mutate, network.rs:479-501), or, with
+                                    `rewiring`, that share of the changes a link gained or lost
+                                    (Network::rewire, network.rs:503-575); every clone's cells step under its
+                                    own network.  The draws: Philox under the history's key, counters (parent
+                                    id, step, 6 / 7 / 8, 0).  0: every cell under the one network */
+    double rewiring;             /* [0, 1]: the share of the changes that rewire */
 } cw_sim_config;
 int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out);
 int cw_sim_destroy(cw_sim sim);
 /* `steps` lattice steps on every history. */
 int cw_sim_step(cw_sim sim, uint32_t steps);
+/* An evolving simulation's clones (mutation_rate > 0): the clone of records
+ * 0..n-1 of history `hist` (0: the founding network), the clones founded in
+ * the whole batch (the founding network counted), and each founded clone's
+ * parent clone and mutation (cw_mutation as cw_network_mutate gives it), in
+ * the order they were founded (nclones - 1 entries; either may be NULL).
+ * No counterpart in the reference beyond its CloneRecord (simulation.rs:1686-1694). */
+int cw_sim_clones(cw_sim sim, uint32_t hist, uint32_t n, int32_t *clone);
+int cw_sim_clone_count(cw_sim sim, uint32_t *nclones);
+int cw_sim_clone_records(cw_sim sim, int32_t *parent, cw_mutation *mutation);
 /* What the autotuner chose: the SOR relaxation factor of every history for
  * the oxygen and the signal field (0 until chosen: the reference's rule),
  * the FP32 blocking depth and window (CW_WINDOW_*), and whether it is still

@@ -174,6 +174,13 @@ class CpuHistory:
         self.refvol = int(self.lat.volume[1]) if cfg.get("seeding", 0) == 3 else int(cfg["target_volume"])
         self.net = O.compile_network(spec, self.refvol)
         self.state = np.tile(self.net.initial, (self.ncap, 1))
+        # an evolving history (simulation.rs:1655-1700): every record's clone and
+        # each clone's network table, mutated or rewired at divisions
+        self.mutation_rate = float(cfg.get("mutation_rate", 0.0) or 0.0)
+        self.rewiring = float(cfg.get("rewiring", 0.0) or 0.0)
+        self.clone = np.zeros(self.ncap, np.int64)
+        self.clone_specs = [spec]
+        self.clone_nets = [self.net]
         self.div_rng = np.random.default_rng(self.seed * 7 + 13)
         # a cell's cycle (simulation.rs:1055-1056): none behind the cells the tissue starts with
         self.began = np.zeros(self.ncap, np.int64)
@@ -287,7 +294,17 @@ class CpuHistory:
             if self.cell_nfc is not None:
                 ins[:, 5] = self.cell_nfc[idx]
             st = np.ascontiguousarray(self.state[idx])
-            O.network_step(self.net, st, ins, c["dt"], c["substeps"])
+            if len(self.clone_nets) == 1:
+                O.network_step(self.net, st, ins, c["dt"], c["substeps"])
+            else:
+                # every clone's cells under its own network
+                cl = self.clone[idx]
+                for k in np.unique(cl):
+                    sel = np.nonzero(cl == k)[0]
+                    part = np.ascontiguousarray(st[sel])
+                    O.network_step(self.clone_nets[int(k)], part, np.ascontiguousarray(ins[sel]), c["dt"],
+                                   c["substeps"])
+                    st[sel] = part
             self.state[idx] = st
             tg = O.network_mechanics(self.net, st)
             dead = (st[:, self.net.survival] < c.get("death_threshold", 0.25)) if nec >= 0 else np.zeros(len(idx), bool)
@@ -318,6 +335,27 @@ class CpuHistory:
             self._divide_ready_cells()
         self.steps += 1
         return rc
+
+    def _mutate(self, d):
+        """A daughter not quite a copy (simulation.rs:1655-1700): one rate of its
+        network scaled (Network::mutate) or, with chance `rewiring`, a link
+        gained or lost (Network::rewire); a change made founds a clone."""
+        which, how = self.div_rng.random(), self.div_rng.random()
+        spec = self.clone_specs[int(self.clone[d])]
+        if self.rewiring > 0.0:
+            u = self.div_rng.random()
+            if u < self.rewiring:
+                source, sign = self.div_rng.random(), self.div_rng.random()
+                new, rec = O.rewire_spec(spec, (u / self.rewiring, which, source, sign, how))
+            else:
+                new, rec = O.mutate_spec(spec, which, how)
+        else:
+            new, rec = O.mutate_spec(spec, which, how)
+        if rec is None:
+            return
+        self.clone_specs.append(new)
+        self.clone_nets.append(O.compile_network(new, self.refvol))
+        self.clone[d] = len(self.clone_specs) - 1
 
     def _level_at(self, mcs):
         """Exposure::level_at (types.rs:319-332)."""
@@ -463,7 +501,7 @@ class CpuHistory:
         return int(max(np.floor(c["cycle_median"] * np.exp(c.get("cycle_spread", 0.0) * z) + 0.5), 1.0))
 
     def _divide_ready_cells(self):
-        """divide_ready_cells (simulation.rs:1603-1716) without cycle or mutation: the living
+        """divide_ready_cells (simulation.rs:1603-1716): the living
         cells of at least 1.4 reference volumes whose hypoxia response is under 0.45 split, in
         id order, while the living stay under max_cells; daughters copy the parent's state."""
         c = self.cfg
@@ -494,6 +532,9 @@ class CpuHistory:
             d, self.used = self.lat.divide_across(int(cid), normal, self.used)
             if d >= 0:
                 self.state[d] = self.state[cid]
+                self.clone[d] = self.clone[cid]
+                if self.mutation_rate > 0.0 and self.div_rng.random() < self.mutation_rate:
+                    self._mutate(d)
                 if c.get("cycle_median", 0.0) > 0:
                     self.began[cid] = self.began[d] = self.steps
                     self.due[cid] = self.steps + self._cycle_length()

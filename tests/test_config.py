@@ -67,7 +67,8 @@ def test_a_vessel_seeds_its_cell_against_the_wall(tmp_path):
 def test_what_the_device_step_does_not_run_is_refused_by_name(tmp_path):
     for extra, word in [("\n[oxygen_source]\nkind = \"capillary\"\nradius = 3\n", "capillary"),
                         ("\n[seeding]\nkind = \"sheet\"\nside = 10\n", "sheet"),
-                        ("mutation_rate = 0.1\n", "mutation"),
+                        ("mutation_rate = 1.5\n", "mutation_rate"),
+                        ("suppress = [1]\n", "suppress"),
                         ("\n[angiogenesis]\nthreshold = 0.5\n", "angiogenesis"),
                         ("\n[lesion]\nat = 10\nradius = 4\n", "lesion"),
                         ("contact_order = 4\n", "contact_order")]:
@@ -78,6 +79,14 @@ def test_what_the_device_step_does_not_run_is_refused_by_name(tmp_path):
         C.load_sim_config(write(tmp_path, BASE.replace("mcs = 30\n", "")))
     with pytest.raises(cw.ConfigError, match="network"):
         C.simulation_kwargs(C.load_sim_config(write(tmp_path, BASE.replace('network = "net.toml"\n', ""))))
+
+
+def test_mutation_and_rewiring_map_onto_the_step(tmp_path):
+    cfg = C.load_sim_config(write(tmp_path, "mutation_rate = 0.05\nrewiring = 0.3\n" + BASE))
+    kw, _ = C.simulation_kwargs(cfg)
+    assert kw["mutation_rate"] == 0.05 and kw["rewiring"] == 0.3
+    kw, _ = C.simulation_kwargs(C.load_sim_config(write(tmp_path, BASE)))
+    assert "mutation_rate" not in kw
 
 
 def test_released_fields_map_onto_the_step(tmp_path):

@@ -6,7 +6,8 @@ examples: one cell in a bath (or against a vessel) grows, divides every 20
 steps, starves inside; the device's 32 histories against the oracle stepping
 the same scenario with the reference's algorithms (sequential random-pixel
 sweep, FP64 SOR, RK4), living and necrotic cells and the tissue's radius and
-viable depth inside the oracle's 32-seed band; and the run loop's
+viable depth inside the oracle's 32-seed band (also with daughters that
+mutate or rewire their networks and found clones); and the run loop's
 measurements.csv.
 """
 import json
@@ -58,7 +59,8 @@ CYCLE = "\n[cycle]\nmedian = 20.0\nspread = 0.3\n"
 
 
 @pytest.mark.parametrize("source,uptake", [("", 0.001), ("\n[oxygen_source]\nkind = \"vessel\"\nradius = 5\n", 0.0001),
-                                           (CYCLE, 0.001), ("debris_loss = 0.05\n", 0.001)])
+                                           (CYCLE, 0.001), ("debris_loss = 0.05\n", 0.001),
+                                           ("mutation_rate = 0.3\nrewiring = 0.3\n", 0.001)])
 def test_a_configured_tissue_grows_inside_the_oracle_band(tmp_path, source, uptake):
     path, spec = scenario(tmp_path, source, uptake)
     cfg = C.load_sim_config(path)
@@ -82,6 +84,13 @@ def test_a_configured_tissue_grows_inside_the_oracle_band(tmp_path, source, upta
             assert within_band(dv, rv), (step, q, dv.mean(), rv.mean(), rv.std())
     final = np.array([m["cycling"] + m["quiescent"] for m in sim.measure()])
     assert final.mean() > 8  # it grew
+    if "mutation_rate" in source:
+        # daughters founded clones, each under its own network, on the device as in the oracle
+        founded = sim.clone_records()
+        assert len(founded) >= 5 and sum(len(h.clone_specs) - 1 for h in ora) >= 5
+        assert {r["change"] for _, r in founded} >= {"scaled", "gained"} or len(founded) < 10
+        clones = np.concatenate([sim.clones(200, k) for k in range(SEEDS)])
+        assert clones.max() == len(founded)
     for k in range(SEEDS):
         assert sim.records_match_grid(k)
 

@@ -108,12 +108,15 @@ def test_fp32_defect_correction_reaches_the_fp64_solution(n, depth):
     g = cw.ScalarField.new(n, n, dcoef, 0.0, 0.0)
     g.set_linear_sink(sink)
     g.hold_where(1.0, held)
-    st = g.relax(1e-6, 1_000_000, omega=1.9, stop=cw.STOP_RESIDUAL, precision=cw.FP32_DC, block_depth=depth,
+    # the residual that buys 1e-6 of the field: the error is A^-1 r, and A's
+    # smallest eigenvalue here is about the mean sink (0.006), so 1e-9 of
+    # residual leaves under 2e-7 of error
+    st = g.relax(1e-9, 1_000_000, omega=1.9, stop=cw.STOP_RESIDUAL, precision=cw.FP32_DC, block_depth=depth,
                  stats=True)
-    assert st[0]["residual"] < 1e-6
+    assert st[0]["residual"] < 1e-9
     v = g.values()
     # 1e-6 relative of the FP64 oracle, on the scale of the field (its maximum, 1)
-    assert np.abs(v - o.values).max() < 1e-6 * max(1.0, np.abs(o.values).max()) * 50
+    assert np.abs(v - o.values).max() < 1e-6 * np.abs(o.values).max()
 
 
 def test_fp32_defect_correction_on_a_volume():
@@ -124,14 +127,14 @@ def test_fp32_defect_correction_on_a_volume():
     g = cw.ScalarField.with_depth(n, n, n, 1.0, 0.0, 0.0)
     g.set_linear_sink(sink)
     g.hold_where(1.0, held.reshape(-1))
-    st = g.relax(1e-6, 100_000, stop=cw.STOP_RESIDUAL, precision=cw.FP32_DC, stats=True)
-    assert st[0]["residual"] < 1e-6
+    st = g.relax(1e-9, 100_000, stop=cw.STOP_RESIDUAL, precision=cw.FP32_DC, stats=True)
+    assert st[0]["residual"] < 1e-9
     o = O.Field(n, n, n, 1.0, 0.0, 0.0)
     o.lin_sink = sink.copy()
     o.held[:] = held.reshape(-1)
     o.values[o.held == 1] = 1.0
     assert o.relax(1e-12, 100_000, stop=1)[0] == 0
-    assert np.abs(g.values() - o.values).max() < 5e-5
+    assert np.abs(g.values() - o.values).max() < 1e-6 * np.abs(o.values).max()
 
 
 def test_not_settling_is_an_error():
