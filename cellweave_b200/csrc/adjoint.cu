@@ -50,6 +50,12 @@ struct cw_fit_s {
     double *grad = nullptr;  // [4 + ntheta]
     std::vector<double> target_h, target_g, h, g, cnt;
     Plan sites;
+    // the frozen lattice's pixels listed by cell and by bin, in pixel order:
+    // the means and the bins' sums are then taken in one fixed order, so that a
+    // forward pass gives the same loss to the bit every time (central
+    // differences of it resolve the smallest derivatives)
+    int64_t *cell_ptr = nullptr, *bin_ptr = nullptr;
+    int32_t *cell_px = nullptr, *bin_px = nullptr;
     bool forward_done = false;
 };
 
@@ -263,16 +269,52 @@ __global__ void __launch_bounds__(RB) k_fit_backward(NetDev N, const double *ckm
     }
 }
 
-// Bin statistics: hypoxic sum, signal sum and cell pixels per bin.
-__global__ void k_fit_bins(const int32_t *grid, const double *c, const double *s, int W, int64_t n, int xc,
-                           double width, int nbins, double level, double tau, double *bins) {
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    if (grid[i] <= 0) return;
-    int b = bin_of((int)(i % W), xc, width, nbins);
-    atomicAdd(bins + b, sigmoid((level - c[i]) / tau));
-    atomicAdd(bins + nbins + b, s[i]);
-    atomicAdd(bins + 2 * nbins + b, 1.0);
+// Every cell's mean of `v` over its pixels (mean_per_cell, coupling.rs:164-182),
+// summed in pixel order from the cell's pixel list; count: its pixels; sum
+// (optional): the sum itself.
+__global__ void k_fit_cell_means(const int64_t *ptr, const int32_t *px, int64_t nc, const double *v, double *mean,
+                                 int32_t *count, double *sum_out) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nc) return;
+    const int64_t a = ptr[c], b = ptr[c + 1];
+    double sum = 0.0;
+    for (int64_t k = a; k < b; ++k) sum += v[px[k]];
+    const int32_t n = (int32_t)(b - a);
+    count[c] = n;
+    mean[c] = n == 0 ? 0.0 : sum / (double)n;
+    if (sum_out) sum_out[c] = sum;
+}
+
+// Bin statistics, one block per bin over the bin's cell pixels: hypoxic sum,
+// signal sum and pixels, each a fixed-order tree sum.
+constexpr int BIN_T = 256;
+__global__ void __launch_bounds__(BIN_T) k_fit_bins_fixed(const int64_t *ptr, const int32_t *px, const double *c,
+                                                         const double *s, int nbins, double level, double tau,
+                                                         double *bins) {
+    __shared__ double sh[BIN_T], sg[BIN_T];
+    const int b = blockIdx.x;
+    const int64_t a = ptr[b], e = ptr[b + 1];
+    double h = 0.0, g = 0.0;
+    for (int64_t k = a + threadIdx.x; k < e; k += BIN_T) {
+        const int32_t i = px[k];
+        h += sigmoid((level - c[i]) / tau);
+        g += s[i];
+    }
+    sh[threadIdx.x] = h;
+    sg[threadIdx.x] = g;
+    __syncthreads();
+    for (int w = BIN_T / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) {
+            sh[threadIdx.x] += sh[threadIdx.x + w];
+            sg[threadIdx.x] += sg[threadIdx.x + w];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        bins[b] = sh[0];
+        bins[nbins + b] = sg[0];
+        bins[2 * nbins + b] = (double)(e - a);
+    }
 }
 
 // Signal production p = sigma x(T)[angio] on the cell's pixels.
@@ -440,6 +482,44 @@ int cw_fit_create(cw_lattice lat, cw_network net, const cw_fit_config *cfg, cw_f
     f->target_g.assign(cfg->nbins, 0.0);
     std::vector<int64_t> per(1, f->n);
     if ((rc = f->sites.build(per, T)) != CW_OK) { cw_fit_destroy(f); return rc; }
+    {
+        // pixel lists of the frozen lattice, by cell and by bin, in pixel order
+        std::vector<int32_t> grid(f->n);
+        CW_CUDA(cudaMemcpyAsync(grid.data(), lat->grid, sizeof(int32_t) * f->n, cudaMemcpyDeviceToHost, stream()));
+        CW_CUDA(cudaStreamSynchronize(stream()));
+        const int nb = cfg->nbins;
+        std::vector<int64_t> cp(nc + 1, 0), bp(nb + 1, 0);
+        auto bin_of_host = [&](int64_t i) {
+            int b = (int)(std::fabs((double)((int)(i % W) - cfg->vessel_x)) / cfg->bin_width);
+            return b < nb ? b : nb - 1;
+        };
+        for (int64_t i = 0; i < f->n; ++i) {
+            const int32_t id = grid[i];
+            if (id > 0 && id < nc) cp[id + 1] += 1;
+            if (id > 0) bp[bin_of_host(i) + 1] += 1;
+        }
+        for (int64_t c2 = 0; c2 < nc; ++c2) cp[c2 + 1] += cp[c2];
+        for (int b = 0; b < nb; ++b) bp[b + 1] += bp[b];
+        std::vector<int32_t> cpx(std::max<int64_t>(cp[nc], 1)), bpx(std::max<int64_t>(bp[nb], 1));
+        std::vector<int64_t> cn(cp.begin(), cp.end() - 1), bn(bp.begin(), bp.end() - 1);
+        for (int64_t i = 0; i < f->n; ++i) {
+            const int32_t id = grid[i];
+            if (id > 0 && id < nc) cpx[cn[id]++] = (int32_t)i;
+            if (id > 0) bpx[bn[bin_of_host(i)]++] = (int32_t)i;
+        }
+        if ((rc = dalloc(&f->cell_ptr, nc + 1)) || (rc = dalloc(&f->bin_ptr, nb + 1)) ||
+            (rc = dalloc(&f->cell_px, cpx.size())) || (rc = dalloc(&f->bin_px, bpx.size()))) {
+            cw_fit_destroy(f);
+            return rc;
+        }
+        CW_CUDA(cudaMemcpyAsync(f->cell_ptr, cp.data(), sizeof(int64_t) * (nc + 1), cudaMemcpyHostToDevice, stream()));
+        CW_CUDA(cudaMemcpyAsync(f->bin_ptr, bp.data(), sizeof(int64_t) * (nb + 1), cudaMemcpyHostToDevice, stream()));
+        CW_CUDA(cudaMemcpyAsync(f->cell_px, cpx.data(), sizeof(int32_t) * cpx.size(), cudaMemcpyHostToDevice,
+                                stream()));
+        CW_CUDA(cudaMemcpyAsync(f->bin_px, bpx.data(), sizeof(int32_t) * bpx.size(), cudaMemcpyHostToDevice,
+                                stream()));
+        CW_CUDA(cudaStreamSynchronize(stream()));
+    }
     size_t sb = bwd_smem(f), sf = fwd_smem(f);
     if (sb > 48 * 1024 && cudaFuncSetAttribute(k_fit_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb))
         return fail(CW_ERR_CONFIG, "the network is too large for the adjoint's shared memory");
@@ -456,6 +536,7 @@ int cw_fit_destroy(cw_fit f) {
     dfree(f->term); dfree(f->par); dfree(f->d_rate); dfree(f->sum); dfree(f->mean); dfree(f->sum2); dfree(f->mean2);
     dfree(f->count); dfree(f->count2); dfree(f->inputs); dfree(f->x0); dfree(f->xT); dfree(f->lam); dfree(f->gin);
     dfree(f->ck); dfree(f->seg); dfree(f->bins); dfree(f->coef); dfree(f->grad);
+    dfree(f->cell_ptr); dfree(f->bin_ptr); dfree(f->cell_px); dfree(f->bin_px);
     f->sites.release();
     f->hs.release();
     delete f;
@@ -511,7 +592,9 @@ int cw_fit_forward(cw_fit f, double *loss, double *h_out, double *g_out) {
     if ((rc = couple_uptake_device(f->o2, f->lat, f->d_rate, 8, f->o2->lin_sink, f->sites)) != CW_OK) return rc;
     f->o2->lin_sink_on = true;
     if ((rc = fit_relax(f, f->o2, c.tolerance)) != CW_OK) return rc;
-    if ((rc = couple_means_device(f->o2, f->lat, f->sum, f->count, f->mean, f->sites)) != CW_OK) return rc;
+    k_fit_cell_means<<<blocks(f->nc), T, 0, stream()>>>(f->cell_ptr, f->cell_px, f->nc, f->o2->c, f->mean, f->count,
+                                                        nullptr);
+    CW_LAUNCHED();
     k_fit_inputs<<<blocks(f->nc), T, 0, stream()>>>(f->mean, f->nc, c.egf, f->inputs);
     CW_LAUNCHED();
     // the network, checkpointed
@@ -526,10 +609,8 @@ int cw_fit_forward(cw_fit f, double *loss, double *h_out, double *g_out) {
     f->sig->production_on = true;
     if ((rc = fit_relax(f, f->sig, c.tolerance)) != CW_OK) return rc;
     // profiles and the loss
-    CW_CUDA(cudaMemsetAsync(f->bins, 0, sizeof(double) * 3 * nb, stream()));
-    const int W = f->lat->g.w[0];
-    k_fit_bins<<<blocks(f->n), T, 0, stream()>>>(f->lat->grid, f->o2->c, f->sig->c, W, f->n, c.vessel_x,
-                                                 c.bin_width, nb, c.hypoxic_level, c.tau, f->bins);
+    k_fit_bins_fixed<<<nb, BIN_T, 0, stream()>>>(f->bin_ptr, f->bin_px, f->o2->c, f->sig->c, nb, c.hypoxic_level,
+                                                 c.tau, f->bins);
     CW_LAUNCHED();
     std::vector<double> hb(3 * nb);
     CW_CUDA(cudaMemcpyAsync(hb.data(), f->bins, sizeof(double) * 3 * nb, cudaMemcpyDeviceToHost, stream()));
@@ -574,7 +655,9 @@ int cw_fit_gradient(cw_fit f, double *loss, double *grad) {
     CW_LAUNCHED();
     f->asig->production_on = true;
     if ((rc = fit_relax(f, f->asig, c.adjoint_tolerance)) != CW_OK) return rc;
-    if ((rc = couple_means_device(f->asig, f->lat, f->sum2, f->count2, f->mean2, f->sites)) != CW_OK) return rc;
+    k_fit_cell_means<<<blocks(f->nc), T, 0, stream()>>>(f->cell_ptr, f->cell_px, f->nc, f->asig->c, f->mean2,
+                                                        f->count2, f->sum2);
+    CW_LAUNCHED();
     k_fit_lam_init<<<blocks(f->nc), T, 0, stream()>>>(f->sum2, f->nc, f->S, f->angio, c.secretion, f->lam, f->gin);
     CW_LAUNCHED();
     // reverse RK4, segment by segment
