@@ -6,9 +6,9 @@
 
 Workload (default ``campaign``): the batched campaign of 64 independent
 histories of uneven sizes (16 each at 128^2, 256^2, 512^2, 1024^2; cells at
-30% fill, target 49; oxygen and a secreted signal solved to residual 1e-6 by
-FP32 SOR with FP64 defect correction; 8-species RK4 network; Moore-contact
-CPM).  A step is one lattice step (MCS) of every history: field solves,
+30% fill, target 49; oxygen and a secreted signal solved to residual 1e-8 by
+FP32 SOR with FP64 defect correction, which puts every field within 1e-6 of
+its FP64 solution; 8-species RK4 network; Moore-contact CPM).  A step is one lattice step (MCS) of every history: field solves,
 means, RK4, fates, Monte Carlo sweep.  Data are synthetic (seeded).
 
 The JSON line reports histories*MCS/s of the batch (``value``), of the same
@@ -92,14 +92,14 @@ def job_rate(world, histories, steps, ms):
 def config_key(name, cfg):
     if name == "campaign":
         return {"workload": "batched campaign: 64 histories, 16 each at 128^2/256^2/512^2/1024^2, 30% fill at "
-                            "target 49, Moore contact, 2 fields to residual 1e-6 (FP32 SOR + FP64 defect "
-                            "correction), 8-species RK4 x8 per MCS", "histories": len(cfg["dims"]),
+                            "target 49, Moore contact, 2 fields to residual 1e-8 (FP32 SOR + FP64 defect "
+                            "correction; each field within 1e-6 of its FP64 solution), 8-species RK4 x8 per MCS", "histories": len(cfg["dims"]),
                 "sites": int(sum(w * h * d for w, h, d in cfg["dims"])), "cells": int(sum(cfg["ncells"])),
                 "l2": "inputs larger than L2 (the lattices and fields of one step exceed 126 MB)",
                 "parallelism": "histories batched in one launch per kernel; ranks own disjoint campaigns",
                 "subsweeps": 1}
     return {"workload": "tumour cord 2048^2, ~40k cells of target 64, 3 types, vessel column, 2 fields to "
-                        "residual 1e-6, 16-species RK4", "histories": 1,
+                        "residual 1e-8, 16-species RK4", "histories": 1,
             "l2": "inputs larger than L2", "parallelism": "one history"}
 
 
@@ -532,7 +532,7 @@ def run_fit(args, L):
     lat = sim.lattice()
     w = cfg["dims"][0][0]
     fit = cw.Fit(lat, net, dcoef=1.0, uptake=(0.01, 0.005, 0.0), vessel_x=w // 2, steps=2000, checkpoint_every=100,
-                 dt=0.01, nbins=64, bin_width=w / 128.0, tolerance=1e-6, adjoint_tolerance=1e-8,
+                 dt=0.01, nbins=64, bin_width=w / 128.0, tolerance=1e-8, adjoint_tolerance=1e-10,
                  precision=cw.FP32_DC, network_params=32)
     start = fit.params.copy()
     p = start.copy()

@@ -41,6 +41,10 @@ def network_toml(S: int, seed: int = 1, density: float = 0.3) -> str:
         if i == 3:
             terms.append('{ kind = "relaxes_to", value = 0.9, rate = 2.0 }')
             terms.append('{ kind = "damaged_below", source = "oxygen", threshold = 0.05, rate = 4.0 }')
+        if i == 4:
+            # the angiogenic node answers the hypoxia response, as a VEGF-like
+            # signal does (fixed parameters: the draws of the rest stay as they were)
+            terms.append('{ kind = "activated_by", source = "n1", rate = 1.0, hill = { n = 2.0, k = 0.3 } }')
         terms.append(f'{{ kind = "decays", rate = {U():.6f} }}')
         lines += ["[[nodes]]", f'name = "n{i}"', "initial = 0.5" if i == 3 else "initial = 0.1", "terms = ["]
         lines += [f"  {t}," for t in terms]
@@ -86,12 +90,13 @@ def tumour_cord(n=2048):
     vessel held at 1 down the column x = n/2 with the medium around it
     consuming as stroma (apply_background_uptake, coupling.rs:47-53), oxygen and a signal secreted at
     0.05 by hypoxic cells (c < 0.1), FP32 SOR with FP64 defect correction to
-    residual 1e-6; 16-species network."""
+    residual 1e-8 (each field then within 1e-6 of its FP64 solution; residual
+    1e-6 left the oxygen 1e-6 to 5e-5 off); 16-species network."""
     return dict(dims=[(n, n, 1)], ncells=[40000 * (n * n) // (2048 * 2048)], seeds=[2], temperature=10.0,
                 J=contact_table(4, seed=2), contact_order=2, target_volume=64, lambda_volume=1.0, seeding=1,
                 seed_side=8, nfields=2, o2_dcoef=1.0, o2_sink_by_type=(0.0, 0.01, 0.005, 0.0), o2_background_sink=0.001,
                 o2_hold=1,
-                signal_dcoef=1.0, signal_decay=0.01, signal_secretion=0.05, hypoxic_level=0.1, tolerance=1e-6,
+                signal_dcoef=1.0, signal_decay=0.01, signal_secretion=0.05, hypoxic_level=0.1, tolerance=1e-8,
                 precision=1, omega=None, relax_every=1, dt=0.01, substeps=8, sweeps=1, death_threshold=0.25,
                 necrotic_type=3, S=16)
 
@@ -99,7 +104,8 @@ def tumour_cord(n=2048):
 def campaign(per_size=16, sizes=(128, 256, 512, 1024), fill=0.3, base_seed=1000):
     """The batched campaign: `per_size` histories at each size, seeds 1000+h,
     cells filling 30% at target 49, the plain config's physics with two fields
-    and an 8-species network."""
+    solved to residual 1e-8 (each field within 1e-6 of its FP64 solution) and
+    an 8-species network."""
     dims, ncells, seeds = [], [], []
     h = 0
     for s in sizes:
@@ -111,16 +117,18 @@ def campaign(per_size=16, sizes=(128, 256, 512, 1024), fill=0.3, base_seed=1000)
     return dict(dims=dims, ncells=ncells, seeds=seeds, temperature=10.0, J=two_type_table(), contact_order=2,
                 target_volume=49, lambda_volume=1.0, seeding=0, seed_side=7, nfields=2, o2_dcoef=1.0,
                 o2_sink_by_type=(0.0, 0.01, 0.01), o2_hold=0, signal_dcoef=1.0, signal_decay=0.01,
-                signal_secretion=0.05, hypoxic_level=0.1, tolerance=1e-6, precision=1, omega=None, relax_every=1,
+                signal_secretion=0.05, hypoxic_level=0.1, tolerance=1e-8, precision=1, omega=None, relax_every=1,
                 dt=0.01, substeps=8, sweeps=1, S=8)
 
 
 def spheroid_3d(n=256):
     """The 3D spheroid: n^3, 26-neighbour contact, cells of 5^3 packed in a ball
     of radius 40, T 20, lambda_V 1, surface lambda 0.2 target 150; oxygen held
-    at 1 on every face, k 0.005 in cells; 12-species network."""
+    at 1 on every face, k 0.005 in cells, solved to residual 1e-9 (the medium
+    around the ball consumes nothing, so the error is up to a few hundred
+    times the residual); 12-species network."""
     ncell = int(4.0 / 3.0 * np.pi * 40 ** 3 / 125)
     return dict(dims=[(n, n, n)], ncells=[ncell], seeds=[3], temperature=20.0, J=two_type_table(),
                 contact_order=3, target_volume=125, lambda_volume=1.0, surface_target=150, lambda_surface=0.2,
                 seeding=2, seed_side=5, nfields=1, o2_dcoef=1.0, o2_sink_by_type=(0.0, 0.005, 0.005), o2_hold=2,
-                tolerance=1e-6, precision=1, omega=None, relax_every=1, dt=0.01, substeps=8, sweeps=1, S=12)
+                tolerance=1e-9, precision=1, omega=None, relax_every=1, dt=0.01, substeps=8, sweeps=1, S=12)
