@@ -71,7 +71,8 @@ class Mutation(C.Structure):
 class Measurements(C.Structure):
     _fields_ = [("mcs", C.c_uint64), ("cycling", C.c_uint64), ("quiescent", C.c_uint64), ("necrotic", C.c_uint64),
                 ("born", C.c_uint64), ("gone", C.c_uint64), ("vessel", C.c_uint64), ("tissue_radius", C.c_double),
-                ("necrotic_radius", C.c_double), ("viable_depth", C.c_double), ("exposure", C.c_double)]
+                ("necrotic_radius", C.c_double), ("viable_depth", C.c_double), ("exposure", C.c_double),
+                ("differentiating", C.c_uint64), ("apoptotic", C.c_uint64), ("clones", C.c_uint64)]
 
 
 class FitConfig(C.Structure):
@@ -103,7 +104,8 @@ class SimConfig(C.Structure):
                 ("debris_loss", C.c_double), ("still_medium", C.c_double),
                 ("exposure_intensity", C.c_double), ("exposure_uptake", C.c_double), ("exposure_start", C.c_int32),
                 ("exposure_on", C.c_int32), ("exposure_off", C.c_int32), ("mutation_rate", C.c_double),
-                ("rewiring", C.c_double)]
+                ("rewiring", C.c_double), ("field_off", C.c_int32), ("differentiated_type", C.c_int32),
+                ("apoptotic_type", C.c_int32), ("lineage", C.c_int32)]
 
 
 P = C.c_void_p
@@ -119,7 +121,7 @@ SIGNATURES = {
     "cw_launch_count": (C.c_uint64, []),
     "cw_sim_clones": (C.c_int, [P, U32, U32, P]),
     "cw_sim_clone_count": (C.c_int, [P, P]),
-    "cw_sim_clone_records": (C.c_int, [P, P, P]),
+    "cw_sim_clone_records": (C.c_int, [P, P, P, P]),
     "cw_test_faults": (C.c_int, [U64, I32, I32, I32]),
     "cw_event_record_on": (C.c_int, [P, I32]),
     "cw_lattice_set_stream": (C.c_int, [P, P]),

@@ -13,9 +13,11 @@ a vessel), networks stepped eight units of their time a step, division
 checked every 20 steps (every step with a cell cycle of its own); an
 exposure's stress, waste, necrotic factor, debris loss, a still medium and
 daughters that mutate or rewire their networks (mutation_rate, rewiring)
-when configured.  Every other feature of the file (capillaries, sheets,
-suppressed clones, lesions, angiogenesis, immunity, tracing) is refused by
-name.  ``run`` steps it for ``mcs`` steps or until the tissue touches the
+when configured; a sheet of normal tissue with the field off, every cell the
+founder of its clone, cells committing to differentiate (or to apoptosis)
+at their network's node's level and leaving the layer.  Every other feature
+of the file (capillaries, suppressed clones, lesions, angiogenesis, immunity,
+tracing) is refused by name.  ``run`` steps it for ``mcs`` steps or until the tissue touches the
 box's edge, writing measurements.csv and the snapshots as the reference
 does.
 
@@ -55,13 +57,17 @@ DIVISION_CHECK_EVERY = 20    # simulation.rs:55
 OXYGEN_WARMUP_TOLERANCE = 1e-8  # simulation.rs:95
 FIRST_CELL_RADIUS = 8        # simulation.rs:65
 FIRST_CELL_RADIUS_3D = 3     # simulation.rs:74
-MEDIUM, TUMOR, NORMAL, NECROTIC = 0, 1, 2, 3
+MEDIUM, TUMOR, NORMAL, NECROTIC, DIFFERENTIATED, APOPTOTIC = 0, 1, 2, 3, 4, 5
 
-# ContactEnergy::default (cpm.rs:63-86) between the kinds the device step has
-CONTACT = np.array([[0.0, 16.0, 16.0, 12.0],
-                    [16.0, 2.0, 11.0, 10.0],
-                    [16.0, 11.0, 6.0, 12.0],
-                    [12.0, 10.0, 12.0, 8.0]])
+# ContactEnergy::default (cpm.rs:63-86) between the kinds the device step has;
+# a differentiated cell costs what a normal one does, an apoptotic one what a
+# necrotic one does (ContactEnergy::index, cpm.rs:116-128)
+_BASE = np.array([[0.0, 16.0, 16.0, 12.0],
+                  [16.0, 2.0, 11.0, 10.0],
+                  [16.0, 11.0, 6.0, 12.0],
+                  [12.0, 10.0, 12.0, 8.0]])
+_AS = [0, 1, 2, 3, 2, 3]
+CONTACT = _BASE[np.ix_(_AS, _AS)]
 
 
 def load_sim_config(path: str) -> dict:
@@ -90,8 +96,26 @@ def _refuse(cfg):
     src = cfg["oxygen_source"].get("kind", "bath")
     if src not in ("bath", "vessel"):
         raise ConfigError(f"{name}: the device step runs a bath or a vessel, not a {src}")
-    if cfg["seeding"].get("kind", "single") != "single":
-        raise ConfigError(f"{name}: the device step seeds one cell, not a {cfg['seeding'].get('kind')}")
+    kind = cfg["seeding"].get("kind", "single")
+    if kind not in ("single", "sheet"):
+        raise ConfigError(f"{name}: the device step seeds one cell or a sheet, not a {kind}")
+    if kind == "sheet":
+        # simulation.rs:696-731
+        side = int(cfg["seeding"].get("side", 0))
+        if float(cfg["oxygen_uptake"]) != 0.0:
+            raise ConfigError(f"{name}: a sheet fills the box and leaves no medium to supply oxygen; "
+                              "set oxygen_uptake = 0 to run it with the field off")
+        if side < 4:
+            raise ConfigError(f"{name}: a sheet of cells {side} pixels across is too fine for any of them to divide")
+        if cfg["width"] % side or cfg["height"] % side:
+            raise ConfigError(f"{name}: a sheet of cells {side} pixels across does not tile a "
+                              f"{cfg['width']}x{cfg['height']} box; make both sides a multiple of {side}")
+        if src == "vessel":
+            raise ConfigError(f"{name}: a sheet is a layer of normal tissue with nothing inside it; "
+                              "it cannot be laid around a vessel")
+        if cfg["depth"] > 1:
+            raise ConfigError(f"{name}: a sheet, which is a layer one cell thick, runs only in the plane; "
+                              "set depth = 1")
     for key in ("lesion", "angiogenesis", "immunity", "tracing", "suppress_before"):
         if cfg.get(key) is not None:
             raise ConfigError(f"{name}: `{key}` is not part of the device step")
@@ -103,8 +127,8 @@ def _refuse(cfg):
         raise ConfigError(f"{name}: contact_order is {cfg['contact_order']}; it is 1, 2 or 3")
     if cfg["network"] is None:
         raise ConfigError(f"{name}: name the network file; the built-in RAS/ERK network is not carried here")
-    if cfg["oxygen_uptake"] <= 0:
-        raise ConfigError(f"{name}: the device step solves the oxygen; oxygen_uptake must be above zero")
+    if cfg["oxygen_uptake"] < 0:
+        raise ConfigError(f"{name}: oxygen_uptake must not be below zero (zero leaves the field off)")
 
 
 def first_cell_volume(cfg) -> int:
@@ -128,7 +152,11 @@ def simulation_kwargs(cfg, histories=1, seeds=None, subsweeps=4):
     _refuse(cfg)
     src = cfg["oxygen_source"]
     vessel = src.get("kind") == "vessel"
-    refvol = first_cell_volume(cfg)
+    sheet = cfg["seeding"].get("kind", "single") == "sheet"
+    side = int(cfg["seeding"].get("side", 0)) if sheet else 0
+    # the network's reference volume: the seeded cell's, or a sheet cell's
+    # (newborn_volume, simulation.rs:742-749)
+    refvol = side * side if sheet else first_cell_volume(cfg)
     uptake = float(cfg["oxygen_uptake"])
     kw = dict(dims=[(cfg["width"], cfg["height"], cfg["depth"])] * histories, ncells=[1] * histories,
               seeds=list(seeds) if seeds is not None else [int(cfg["seed"]) + k for k in range(histories)],
@@ -141,7 +169,17 @@ def simulation_kwargs(cfg, histories=1, seeds=None, subsweeps=4):
               dt=1.0, substeps=NETWORK_TIME_PER_MCS, sweeps=int(cfg["sweeps_per_step"]),
               death_threshold=DEATH_THRESHOLD, necrotic_type=NECROTIC, divide=True,
               max_cells=int(cfg["max_cells"]), divide_every=DIVISION_CHECK_EVERY, subsweeps=int(subsweeps),
-              first_tolerance=OXYGEN_WARMUP_TOLERANCE)
+              first_tolerance=OXYGEN_WARMUP_TOLERANCE, differentiated_type=DIFFERENTIATED,
+              apoptotic_type=APOPTOTIC)
+    if uptake == 0.0:
+        # nothing consumes: the field stays at its source's level, unsolved
+        # (field_is_off, simulation.rs:786-793, 2127-2131)
+        kw.update(field_off=True, tolerance=1e-8, first_tolerance=0.0)
+    if sheet:
+        # the box tiled with side x side cells of normal tissue, each the
+        # founder of its own clone (simulation.rs:696-740, 780-785)
+        kw.update(seeding=4, seed_side=side, ncells=[(cfg["width"] // side) * (cfg["height"] // side)] * histories,
+                  lineage=True)
     if cfg.get("cycle"):
         cy = cfg["cycle"]
         if "median" not in cy or "spread" not in cy:

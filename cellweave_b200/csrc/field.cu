@@ -615,8 +615,10 @@ static int relax_fp64(cw_field_s *f, const cw_relax_opts &o, std::vector<Span> &
 
 // ------------------------------------------------------------------ residual by TMA tiles
 //
-// k_residual64 with its reads staged by the TMA engine.  A persistent block
-// per SM walks 128 x 16 tiles with a producer warp and 16 consumer warps:
+// k_residual64 with its reads staged by the TMA engine.  Persistent blocks,
+// two per SM (34 warps an SM: twice the consumers to hide the FP64 chains
+// behind; measured 1.7% faster a campaign step than one block of five
+// stages), walk 128 x 16 tiles with a producer warp and 16 consumer warps:
 // the producer looks up the block's next tiles 32 at a time (a lane per
 // candidate: its record, then whether its history has settled), and for each
 // live one waits for a free stage and has the TMA engine bring in the tile's
@@ -636,7 +638,7 @@ constexpr int RT_CONSUMERS = RT_Y;                 // a warp per row of a tile
 constexpr int RT_THREADS = 32 * (RT_CONSUMERS + 1);
 constexpr int RT_MAX_STAGES = 6;
 constexpr int RT_MAPS = 5;                         // per history: values, held, sink, production, uptake
-constexpr int RT_SMEM = 200 * 1024;                // stages of every field fit in this
+constexpr int RT_SMEM = 100 * 1024;                // two blocks per SM: the stages of a block fit in this
 
 __device__ int g_rt_wait_failed;
 
@@ -667,7 +669,7 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 
-__global__ void __launch_bounds__(RT_THREADS, 1)
+__global__ void __launch_bounds__(RT_THREADS, 2)
     k_residual64_tiles(RtArgs a, FieldView fv, RelaxState *st, float *r32, float *inv32, float *dz, int skip_done) {
     extern __shared__ __align__(128) unsigned char rsm[];
     __shared__ __align__(8) uint64_t full[RT_MAX_STAGES], empty[RT_MAX_STAGES];

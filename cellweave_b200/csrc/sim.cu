@@ -55,8 +55,12 @@ struct cw_sim_s {
     uint8_t *alive = nullptr;
     uint32_t *target32 = nullptr;
     int64_t nc = 0;                 // records over all histories
-    // an evolving batch (mutation_rate > 0): every record's clone, the clones'
-    // networks (0: the founding one, not owned) and their device tables
+    // types that are no longer living (necrotic, differentiated, apoptotic), as bits
+    uint32_t leaving = 0;
+    // clones: tracked with mutation or a lineage; with mutation (evolve) every
+    // clone also steps under its own network (0: the founding one, not owned;
+    // a lineage's founders all share it)
+    bool track = false;
     bool evolve = false;
     std::vector<cw_network_s *> clones;
     std::vector<int32_t> clone_parent;
@@ -109,7 +113,7 @@ constexpr int T = 256;
 // EGF everywhere the same, crowding 1 - volume / reference volume clamped to
 // [0, 1]; no stress, waste or necrotic factor on this path.
 __global__ void k_inputs(const int32_t *type, const int32_t *volume, const int64_t *cell_off, int nh, int64_t nc,
-                         int necrotic, const double *cell_o2, double egf, double reference, double *inputs,
+                         uint32_t leaving, const double *cell_o2, double egf, double reference, double *inputs,
                          uint8_t *alive) {
     int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nc) return;
@@ -117,7 +121,7 @@ __global__ void k_inputs(const int32_t *type, const int32_t *volume, const int64
     int lo = 0, hi = nh - 1;
     while (lo < hi) { int mid = (lo + hi + 1) >> 1; if (cell_off[mid] <= c) lo = mid; else hi = mid - 1; }
     bool medium = c == cell_off[lo];
-    bool a = !medium && volume[c] > 0 && type[c] != necrotic;
+    bool a = !medium && volume[c] > 0 && !((leaving >> (type[c] & 31)) & 1u);
     alive[c] = a;
     inputs[0 * nc + c] = cell_o2[c];
     inputs[1 * nc + c] = egf;
@@ -223,6 +227,8 @@ __global__ void k_secretion(const uint8_t *alive, const double *cell_o2, int64_t
 }
 
 constexpr int32_t RESORPTION_RATE = 2;    // pixels a necrotic cell gives up a step (simulation.rs:127)
+constexpr int32_t SHEDDING_RATE = 6;      // a differentiated cell leaving the layer (simulation.rs:135)
+constexpr int32_t FRAGMENTATION_RATE = 8; // an apoptotic cell breaking up (simulation.rs:142)
 constexpr double DIVISION_RATIO = 1.4;    // of the reference volume (simulation.rs:45)
 constexpr double QUIESCENCE_THRESHOLD = 0.45;  // hypoxia response that stops cycling (simulation.rs:117)
 constexpr int DEFAULT_MAX_CELLS = 2000;   // simulation.rs:61
@@ -230,25 +236,34 @@ constexpr int DEFAULT_MAX_CELLS = 2000;   // simulation.rs:61
 // Measure::measure's counts per history (measure.rs:133-170): one block a
 // history over its records; out[8 h ..] = cycling, quiescent, necrotic,
 // living area, necrotic area, born, gone, lines holding living pixels.
+// out[MEASURES h ..]: cycling, quiescent, necrotic, living area, necrotic
+// area, born, gone, lines holding living pixels, differentiating, apoptotic,
+// leaving area (measure.rs:115-170).
+constexpr int MEASURES = 12;
 __global__ void k_measure(const int32_t *type, const int32_t *volume, const int64_t *cell_off, const int32_t *used,
-                          int necrotic, const double *state, int hyp, int64_t nc, const uint8_t *lines,
-                          const int64_t *line_off, unsigned long long *out) {
+                          int necrotic, int differentiated, int apoptotic, const double *state, int hyp, int64_t nc,
+                          const uint8_t *lines, const int64_t *line_off, unsigned long long *out) {
     const int h = blockIdx.x;
-    __shared__ unsigned long long acc[8];
-    if (threadIdx.x < 8) acc[threadIdx.x] = 0ull;
+    __shared__ unsigned long long acc[MEASURES];
+    if (threadIdx.x < MEASURES) acc[threadIdx.x] = 0ull;
     __syncthreads();
     const int64_t c0 = cell_off[h];
     const int32_t n = used[h];
-    unsigned long long v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    unsigned long long v[MEASURES] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     for (int64_t k = 1 + threadIdx.x; k < n; k += blockDim.x) {
         const int64_t c = c0 + k;
         const int32_t vol = volume[c];
         const bool dead = necrotic >= 0 && type[c] == necrotic;
+        const bool diff = differentiated >= 0 && type[c] == differentiated;
+        const bool apop = apoptotic >= 0 && type[c] == apoptotic;
         if (vol == 0) {
-            if (dead) v[6] += 1;
+            if (dead || diff || apop) v[6] += 1;  // resorbed, shed or broken up: gone for good
             continue;
         }
-        if (dead) {
+        if (diff || apop) {
+            v[diff ? 8 : 9] += 1;
+            v[10] += (unsigned long long)vol;
+        } else if (dead) {
             v[2] += 1;
             v[4] += (unsigned long long)vol;
         } else {
@@ -259,11 +274,11 @@ __global__ void k_measure(const int32_t *type, const int32_t *volume, const int6
     }
     if (lines)
         for (int64_t q = line_off[h] + threadIdx.x; q < line_off[h + 1]; q += blockDim.x) v[7] += lines[q];
-    for (int j = 0; j < 8; ++j)
+    for (int j = 0; j < MEASURES; ++j)
         if (v[j]) atomicAdd(&acc[j], v[j]);
     __syncthreads();
-    if (threadIdx.x < 8) out[8 * h + threadIdx.x] = acc[threadIdx.x];
-    if (threadIdx.x == 0) out[8 * h + 5] = (unsigned long long)(n - 1);
+    if (threadIdx.x < MEASURES) out[MEASURES * h + threadIdx.x] = acc[threadIdx.x];
+    if (threadIdx.x == 0) out[MEASURES * h + 5] = (unsigned long long)(n - 1);
 }
 
 // The columns (by_row 0) or rows (1) of each history that hold a living pixel.
@@ -288,12 +303,35 @@ __global__ void k_measure_lines(const int32_t *grid, const int32_t *type, const 
 // necrotic; every other living cell takes the target its mechanics give.
 // With a cycle (simulation.rs:1301-1304) the target is grown(): half the
 // network's target when the cycle begins, all of it when it is over.
+// Cells leaving the layer or breaking up (simulation.rs:1209-1296): a cell
+// committed to differentiate sheds SHEDDING_RATE pixels a step, one in
+// apoptosis FRAGMENTATION_RATE, until gone; a living cell whose network has the
+// apoptosis (or else the differentiation) node commits with that node's level
+// as its chance this step, drawn from Philox(record, step, 9 / 10, 0) under its
+// history's key.
+struct Leaving {
+    int32_t differentiated, apoptotic;  // types, -1: none
+    int32_t role_diff, role_apop;       // network nodes, -1: none
+    const uint2 *keys;
+    const int64_t *cell_off;
+    int32_t nh;
+};
+
 __global__ void k_fates(const uint8_t *alive, const double *state, int64_t nc, int survival, double death,
                         int necrotic, const uint32_t *mech_target, int32_t *type, const int32_t *volume,
                         int32_t *target, double *lambda, double lam, int32_t *died_at, const uint32_t *step,
-                        const int32_t *began, const int32_t *due, uint8_t *kept) {
+                        const int32_t *began, const int32_t *due, uint8_t *kept, Leaving lv) {
     int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nc) return;
+    if ((lv.differentiated >= 0 && type[c] == lv.differentiated) || (lv.apoptotic >= 0 && type[c] == lv.apoptotic)) {
+        const int32_t v = volume[c];
+        const int32_t rate = type[c] == lv.apoptotic ? FRAGMENTATION_RATE : SHEDDING_RATE;
+        if (v > 0) {
+            target[c] = v > rate ? v - rate : 0;
+            lambda[c] = lam;
+        }
+        return;
+    }
     if (necrotic >= 0 && type[c] == necrotic) {
         const int32_t v = volume[c];
         if (v > 0 && kept) {
@@ -311,6 +349,20 @@ __global__ void k_fates(const uint8_t *alive, const double *state, int64_t nc, i
         if (died_at) died_at[c] = (int32_t)*step;
         if (kept) { kept[c] = 1; target[c] = volume[c]; lambda[c] = lam; }  // simulation.rs:1264-1275
         return;
+    }
+    if ((lv.apoptotic >= 0 && lv.role_apop >= 0) || (lv.differentiated >= 0 && lv.role_diff >= 0)) {
+        int lo = 0, hi = lv.nh - 1;
+        while (lo < hi) { const int mid = (lo + hi + 1) >> 1; if (lv.cell_off[mid] <= c) lo = mid; else hi = mid - 1; }
+        const uint32_t local = (uint32_t)(c - lv.cell_off[lo]);
+        const uint2 k = lv.keys[lo];
+        if (lv.apoptotic >= 0 && lv.role_apop >= 0) {
+            const uint4 r = philox(local, *step, 9u, 0u, k.x, k.y);
+            if (u01(r.x, r.y) < state[(int64_t)lv.role_apop * nc + c]) { type[c] = lv.apoptotic; return; }
+        }
+        if (lv.differentiated >= 0 && lv.role_diff >= 0) {
+            const uint4 r = philox(local, *step, 10u, 0u, k.x, k.y);
+            if (u01(r.x, r.y) < state[(int64_t)lv.role_diff * nc + c]) { type[c] = lv.differentiated; return; }
+        }
     }
     uint32_t full = min(mech_target[c], 0x7fffffffu);
     if (began && due[c] > began[c]) {
@@ -356,7 +408,7 @@ __global__ void k_cycle_births(const int64_t *cell_off, int nh, int64_t nc, cons
 // plane, a uniform direction in a volume (simulation.rs:1631-1642).  Also
 // refreshes `alive` for the living-cell limit.
 __global__ void k_div_ready(const int32_t *type, const int32_t *volume, const int64_t *cell_off, const uint2 *keys,
-                            const int4 *dims, int nh, int64_t nc, int necrotic, const double *state, int hyp,
+                            const int4 *dims, int nh, int64_t nc, uint32_t leaving, const double *state, int hyp,
                             double threshold, const uint32_t *mcs_ctr, uint8_t *alive, uint8_t *flag,
                             double *normal, int32_t *count, const uint32_t *step, int every, const int32_t *due_at) {
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -364,7 +416,7 @@ __global__ void k_div_ready(const int32_t *type, const int32_t *volume, const in
     int lo = 0, hi = nh - 1;
     while (lo < hi) { int mid = (lo + hi + 1) >> 1; if (cell_off[mid] <= c) lo = mid; else hi = mid - 1; }
     const int64_t local = c - cell_off[lo];
-    const bool a = local > 0 && volume[c] > 0 && type[c] != necrotic;
+    const bool a = local > 0 && volume[c] > 0 && !((leaving >> (type[c] & 31)) & 1u);
     alive[c] = a;
     // the check on the steps it is taken on (every > 1: step % every == 0)
     const bool due = every <= 1 || (*step % (uint32_t)every) == 0u;
@@ -457,6 +509,18 @@ void seed_history(const cw_sim_config &c, uint32_t W, uint32_t H, uint32_t D, ui
         type.push_back(1);
         return;
     }
+    // a sheet (Seeding::Sheet, simulation.rs:696-740): the box tiled with
+    // side x side blocks of normal tissue (type 2), row by row
+    if (c.seeding == 4) {
+        for (uint32_t y = 0; y < H; y += (uint32_t)s)
+            for (uint32_t x = 0; x < W; x += (uint32_t)s) {
+                const int32_t id = (int32_t)type.size();
+                for (uint32_t yy = y; yy < y + (uint32_t)s && yy < H; ++yy)
+                    for (uint32_t xx = x; xx < x + (uint32_t)s && xx < W; ++xx) grid[(size_t)yy * W + xx] = id;
+                type.push_back(2);
+            }
+        return;
+    }
     auto free_box = [&](uint32_t x0, uint32_t y0, uint32_t z0, uint32_t sx, uint32_t sy, uint32_t sz) {
         if (x0 + sx > W || y0 + sy > H || z0 + sz > D) return false;
         for (uint32_t z = z0; z < z0 + sz; ++z)
@@ -541,6 +605,30 @@ int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out) {
             if (!c.d || c.d[k] <= 1)
                 return fail(CW_ERR_CONFIG, "a still medium is solved around a ball, and a plane has none");
     }
+    if (c.seeding == 4) {
+        // simulation.rs:696-731
+        if (c.seed_side < 4)
+            return fail(CW_ERR_CONFIG, "a sheet of cells " + std::to_string(c.seed_side) +
+                                           " pixels across is too fine for any of them to divide");
+        for (uint32_t k = 0; k < c.nh; ++k) {
+            if ((c.d && c.d[k] > 1))
+                return fail(CW_ERR_CONFIG, "a sheet, which is a layer one cell thick, runs only in the plane");
+            if (c.w[k] % (uint32_t)c.seed_side || c.h[k] % (uint32_t)c.seed_side)
+                return fail(CW_ERR_CONFIG, "a sheet of cells " + std::to_string(c.seed_side) +
+                                               " pixels across does not tile a " + std::to_string(c.w[k]) + "x" +
+                                               std::to_string(c.h[k]) + " box");
+        }
+        if (!c.field_off)
+            return fail(CW_ERR_CONFIG, "a sheet fills the box and leaves no medium to supply oxygen; "
+                                       "it runs with the field off");
+    }
+    if (c.field_off && c.nfields != 1)
+        return fail(CW_ERR_CONFIG, "with the field off there is only the oxygen, at its start");
+    for (int32_t t : {c.differentiated_type, c.apoptotic_type})
+        if (t >= c.K || t == 0 || t < -1 || (t >= 0 && t == c.necrotic_type))
+            return fail(CW_ERR_CONFIG, "a leaving type is a cell type of the contact table, apart from the necrotic");
+    if (c.differentiated_type >= 0 && c.differentiated_type == c.apoptotic_type)
+        return fail(CW_ERR_CONFIG, "differentiated and apoptotic cells take different types");
     if (!(c.mutation_rate >= 0.0 && c.mutation_rate <= 1.0) || !(c.rewiring >= 0.0 && c.rewiring <= 1.0))
         return fail(CW_ERR_CONFIG, "the mutation rate and the rewiring share lie in [0, 1]");
     if (c.mutation_rate > 0.0 && !c.divide)
@@ -707,11 +795,21 @@ int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out) {
         CW_CUDA(cudaMemsetAsync(s->began, 0, sizeof(int32_t) * nc, stream()));
         CW_CUDA(cudaMemsetAsync(s->due, 0, sizeof(int32_t) * nc, stream()));
     }
-    if (c.mutation_rate > 0.0) {
-        // every record starts in the founding clone
-        s->evolve = true;
-        s->clones.assign(1, net);
+    for (int32_t t : {c.necrotic_type, c.differentiated_type, c.apoptotic_type})
+        if (t >= 0 && t < 32) s->leaving |= 1u << t;
+    if (c.mutation_rate > 0.0 || c.lineage) {
+        // every record starts in the founding clone, or (a lineage) every seeded
+        // cell founds its own: its clone is its record's index in the batch
+        s->track = true;
+        s->evolve = c.mutation_rate > 0.0;
         s->h_clone.assign(nc, 0);
+        if (c.lineage)
+            for (uint32_t k = 0; k < c.nh; ++k)
+                for (size_t id = 1; id < types[k].size(); ++id) {
+                    const int64_t g = s->lat->cell_off[k] + (int64_t)id;
+                    s->h_clone[g] = (int32_t)g;
+                }
+        s->clones.assign(c.lineage ? (size_t)nc : 1, net);
         if ((rc = dalloc(&s->d_clone, nc)) != CW_OK || (rc = upload_clones(s, true)) != CW_OK) {
             cw_sim_destroy(s);
             return rc;
@@ -916,6 +1014,7 @@ static int evolve_after_division(cw_sim_s *s) {
             const int32_t parent_clone = s->h_clone[c0 + id];
             s->h_clone[c0 + d] = parent_clone;
             moved = true;
+            if (!s->evolve) continue;
             const uint4 r0 = cw::philox((uint32_t)id, step, 6u, 0u, k0, k1);
             if (!(cw::u01(r0.x, r0.y) < c.mutation_rate)) continue;
             const double which = cw::u01(r0.z, r0.w);
@@ -954,14 +1053,14 @@ static int division_step(cw_sim_s *s) {
     cw_lattice_s *l = s->lat;
     CW_CUDA(cudaMemsetAsync(l->div.count, 0, sizeof(int32_t), stream()));
     k_div_ready<<<(unsigned)blocks(nc), T, 0, stream()>>>(
-        l->type, l->volume, l->d_cell_off, l->d_keys, l->g.d_dims, (int)c.nh, nc, c.necrotic_type, s->state,
+        l->type, l->volume, l->d_cell_off, l->d_keys, l->g.d_dims, (int)c.nh, nc, s->leaving, s->state,
         network_role(s->net, 2), DIVISION_RATIO * (double)network_reference_volume(s->net),
         (const uint32_t *)l->d_flag, s->alive, l->div.flag, l->div.normal, l->div.count, s->d_step, c.divide_every,
         s->due);
     CW_LAUNCHED();
     int rc = lattice_divide_enqueue(l, s->alive, c.max_cells > 0 ? c.max_cells : DEFAULT_MAX_CELLS, s->state,
                                     network_nodes(s->net));
-    if (rc == CW_OK && s->evolve) rc = evolve_after_division(s);
+    if (rc == CW_OK && s->track) rc = evolve_after_division(s);
     if (rc != CW_OK || !s->due) return rc;
     k_cycle_births<<<(unsigned)blocks(nc), T, 0, stream()>>>(l->d_cell_off, (int)c.nh, nc, l->div.daughter, l->d_keys,
                                                              s->d_step, c.cycle_median, c.cycle_spread, s->began,
@@ -1044,6 +1143,12 @@ static int paint_oxygen(cw_sim_s *s) {
     return CW_OK;
 }
 
+static Leaving leaving_of(const cw_sim_s *s) {
+    const cw_sim_config &c = s->cfg;
+    return Leaving{c.differentiated_type, c.apoptotic_type, network_role(s->net, 3), network_role(s->net, 4),
+                   s->lat->d_keys, s->lat->d_cell_off, (int32_t)c.nh};
+}
+
 // Every living cell's network: the one network, or in an evolving batch each
 // cell under its clone's.
 static int step_networks(cw_sim_s *s) {
@@ -1067,7 +1172,7 @@ static int enqueue_phase(cw_sim_s *s, int p, const cw_relax_opts &o) {
     if (p == 1) {
         if ((rc = couple_means_device(s->o2, s->lat, s->sum, s->count, s->cell_o2, s->sites)) != CW_OK) return rc;
         k_inputs<<<(unsigned)blocks(nc), T, 0, stream()>>>(s->lat->type, s->lat->volume, s->lat->d_cell_off, c.nh, nc,
-                                                           c.necrotic_type, s->cell_o2, 0.2,
+                                                           s->leaving, s->cell_o2, 0.2,
                                                            (double)std::max(network_reference_volume(s->net), 1u),
                                                            s->inputs, s->alive);
         CW_LAUNCHED();
@@ -1086,7 +1191,7 @@ static int enqueue_phase(cw_sim_s *s, int p, const cw_relax_opts &o) {
                                                       c.death_threshold, c.necrotic_type, s->target32, s->lat->type,
                                                       s->lat->volume, s->lat->target, s->lat->lambda, c.lambda_volume,
                                                       s->died_at, s->d_step, s->began, s->due,
-                                                          s->debris_on ? s->debris.kept : nullptr);
+                                                          s->debris_on ? s->debris.kept : nullptr, leaving_of(s));
     CW_LAUNCHED();
     for (int k = 0; k < c.sweeps; ++k)
         if ((rc = lattice_sweep(s->lat)) != CW_OK) return rc;
@@ -1205,7 +1310,7 @@ int cw_sim_step(cw_sim s, uint32_t nsteps) {
         const bool graph_ok = c.use_graphs && c.precision == CW_FP32_DC && c.relax_every <= 1 && !s->tune.active &&
                               s->depth_tuned && s->steps >= 2 && !s->last.empty() &&
                               (!s->sig || !s->last_sig.empty()) && !s->wst && !s->nfc && c.o2_hold != 3 &&
-                              !s->debris_on && !s->str && !s->evolve;
+                              !s->debris_on && !s->str && !s->track && !c.field_off;
         if (graph_ok) {
             if (!s->graphs && (rc = build_graphs(s, o)) != CW_OK) return rc;
             if ((rc = step_graph(s, o)) != CW_OK) return rc;
@@ -1213,7 +1318,10 @@ int cw_sim_step(cw_sim s, uint32_t nsteps) {
         }
         bool tuning = solve && s->tune.active && s->steps > 0;  // the first solve starts from scratch: not booked
         if (tuning) tune_assign(s);
-        if (solve && s->bath) {
+        // with the field off nothing consumes: the oxygen stays at its start
+        // and is not solved (field_is_off, simulation.rs:2127-2131)
+        const bool o2_solve = solve && !c.field_off;
+        if (o2_solve && s->bath) {
             // the bath of the lattice as it stands (hold_medium_bath, coupling.rs:156-158)
             if ((rc = lattice_bath_enqueue(s->lat, s->bath)) != CW_OK) return rc;
             if (c.o2_hold == 3) {
@@ -1223,7 +1331,7 @@ int cw_sim_step(cw_sim s, uint32_t nsteps) {
                 s->o2->held_dirty = true;
             }
         }
-        if (solve) {
+        if (o2_solve) {
             // 1. downward coupling and the oxygen solve
             if ((rc = paint_oxygen(s)) != CW_OK) return rc;
             const double *om = c.omega > 0.0 ? nullptr : s->omega[0].data();
@@ -1252,7 +1360,7 @@ int cw_sim_step(cw_sim s, uint32_t nsteps) {
         // 2. what each cell sits in
         if ((rc = couple_means_device(s->o2, s->lat, s->sum, s->count, s->cell_o2, s->sites)) != CW_OK) return rc;
         k_inputs<<<(unsigned)blocks(nc), T, 0, stream()>>>(s->lat->type, s->lat->volume, s->lat->d_cell_off, c.nh, nc,
-                                                           c.necrotic_type, s->cell_o2, 0.2,
+                                                           s->leaving, s->cell_o2, 0.2,
                                                            (double)std::max(network_reference_volume(s->net), 1u),
                                                            s->inputs, s->alive);
         CW_LAUNCHED();
@@ -1319,7 +1427,7 @@ int cw_sim_step(cw_sim s, uint32_t nsteps) {
                                                           c.necrotic_type, s->target32, s->lat->type,
                                                           s->lat->volume, s->lat->target, s->lat->lambda,
                                                           c.lambda_volume, s->died_at, s->d_step, s->began, s->due,
-                                                          s->debris_on ? s->debris.kept : nullptr);
+                                                          s->debris_on ? s->debris.kept : nullptr, leaving_of(s));
         CW_LAUNCHED();
         // 4b. with a debris loss, the dead tissue's debris lost at its edge and
         // the fluid shut in drained (simulation.rs:1311-1315)
@@ -1389,16 +1497,17 @@ int cw_sim_clones(cw_sim s, uint32_t hist, uint32_t n, int32_t *clone) {
     const int64_t c0 = s->lat->cell_off[hist], cap = s->lat->cell_off[hist + 1] - c0;
     if ((int64_t)n > cap) return fail(CW_ERR_CONFIG, "history " + std::to_string(hist) + " holds " +
                                                          std::to_string(cap) + " records");
-    for (uint32_t k = 0; k < n; ++k) clone[k] = s->evolve ? s->h_clone[c0 + k] : 0;
+    for (uint32_t k = 0; k < n; ++k) clone[k] = s->track ? s->h_clone[c0 + k] : 0;
     return CW_OK;
 }
 
 int cw_sim_clone_count(cw_sim s, uint32_t *nclones) {
-    *nclones = s->evolve ? (uint32_t)s->clones.size() : 1u;
+    *nclones = s->track ? (uint32_t)s->clones.size() : 1u;
     return CW_OK;
 }
 
-int cw_sim_clone_records(cw_sim s, int32_t *parent, cw_mutation *mutation) {
+int cw_sim_clone_records(cw_sim s, uint32_t *count, int32_t *parent, cw_mutation *mutation) {
+    if (count) *count = (uint32_t)s->clone_parent.size();
     for (size_t k = 0; k < s->clone_parent.size(); ++k) {
         if (parent) parent[k] = s->clone_parent[k];
         if (mutation) mutation[k] = s->clone_mutation[k];
@@ -1471,7 +1580,7 @@ int cw_sim_measure(cw_sim s, cw_measurements *out) {
     uint8_t *d_lines = nullptr;
     int64_t *d_loff = nullptr;
     int rc;
-    if ((rc = dalloc(&d_out, 8 * (size_t)nh)) != CW_OK) return rc;
+    if ((rc = dalloc(&d_out, MEASURES * (size_t)nh)) != CW_OK) return rc;
     if (lined && ((rc = dalloc(&d_lines, (size_t)loff[nh])) || (rc = dalloc(&d_loff, nh + 1)))) return rc;
     if (lined) {
         CW_CUDA(cudaMemsetAsync(d_lines, 0, (size_t)loff[nh], stream()));
@@ -1481,18 +1590,28 @@ int cw_sim_measure(cw_sim s, cw_measurements *out) {
                                                               c.o2_hold == 1 ? 1 : 0, d_loff, d_lines);
         CW_LAUNCHED();
     }
-    k_measure<<<nh, 256, 0, stream()>>>(l->type, l->volume, l->d_cell_off, l->d_used, c.necrotic_type, s->state,
-                                        network_role(s->net, 2), s->nc, d_lines, d_loff, d_out);
+    k_measure<<<nh, 256, 0, stream()>>>(l->type, l->volume, l->d_cell_off, l->d_used, c.necrotic_type,
+                                        c.differentiated_type, c.apoptotic_type, s->state, network_role(s->net, 2),
+                                        s->nc, d_lines, d_loff, d_out);
     CW_LAUNCHED();
-    std::vector<unsigned long long> h(8 * (size_t)nh);
-    CW_CUDA(cudaMemcpyAsync(h.data(), d_out, sizeof(unsigned long long) * 8 * nh, cudaMemcpyDeviceToHost, stream()));
+    std::vector<unsigned long long> h(MEASURES * (size_t)nh);
+    CW_CUDA(cudaMemcpyAsync(h.data(), d_out, sizeof(unsigned long long) * MEASURES * nh, cudaMemcpyDeviceToHost,
+                            stream()));
+    // clones with a living cell (measure.rs: clone_sizes), from the records on the host
+    std::vector<int32_t> ty, vo;
+    if (s->track) {
+        ty.resize(s->nc);
+        vo.resize(s->nc);
+        CW_CUDA(cudaMemcpyAsync(ty.data(), l->type, sizeof(int32_t) * s->nc, cudaMemcpyDeviceToHost, stream()));
+        CW_CUDA(cudaMemcpyAsync(vo.data(), l->volume, sizeof(int32_t) * s->nc, cudaMemcpyDeviceToHost, stream()));
+    }
     CW_CUDA(cudaStreamSynchronize(stream()));
     dfree(d_out);
     dfree(d_lines);
     dfree(d_loff);
     const double pi = 3.14159265358979323846;
     for (uint32_t k = 0; k < nh; ++k) {
-        const unsigned long long *v = &h[8 * (size_t)k];
+        const unsigned long long *v = &h[MEASURES * (size_t)k];
         cw_measurements &m = out[k];
         m.mcs = s->steps > 0 ? s->steps - 1 : 0;
         m.exposure = exposure_level(c, m.mcs);
@@ -1501,6 +1620,18 @@ int cw_sim_measure(cw_sim s, cw_measurements *out) {
         m.necrotic = v[2];
         m.born = v[5];
         m.gone = v[6];
+        m.differentiating = v[8];
+        m.apoptotic = v[9];
+        if (s->track) {
+            std::vector<int32_t> seen;
+            const int64_t c0 = l->cell_off[k], c1 = l->cell_off[k + 1];
+            for (int64_t g = c0 + 1; g < c1; ++g)
+                if (vo[g] > 0 && !((s->leaving >> (ty[g] & 31)) & 1u)) seen.push_back(s->h_clone[g]);
+            std::sort(seen.begin(), seen.end());
+            m.clones = (uint64_t)(std::unique(seen.begin(), seen.end()) - seen.begin());
+        } else {
+            m.clones = v[0] + v[1] > 0 ? 1 : 0;
+        }
         // the held column of o2_hold 1, the vessel of 4: the lattice's only obstacles
         m.vessel = (c.o2_hold == 1 || c.o2_hold == 4) ? s->obstacles[k] : 0;
         const uint32_t D = s->d[k];
@@ -1510,8 +1641,8 @@ int cw_sim_measure(cw_sim s, cw_measurements *out) {
             if (c.o2_hold == 4) return std::sqrt((double)size / (pi * (double)D));  // a cylinder as long as the box
             return std::cbrt(3.0 * (double)size / (4.0 * pi));
         };
-        const uint64_t living = v[3], dead = v[4];
-        m.tissue_radius = radius(m.vessel + living + dead);
+        const uint64_t living = v[3], dead = v[4], leaving = v[10];
+        m.tissue_radius = radius(m.vessel + living + dead + leaving);
         m.necrotic_radius = radius(dead);
         if (c.o2_hold == 0) m.viable_depth = v[7] == 0 ? 0.0 : (double)living / (double)v[7];
         else if (c.o2_hold == 1) m.viable_depth = v[7] == 0 ? 0.0 : (double)living / (2.0 * (double)v[7]);

@@ -628,7 +628,7 @@ class Simulation:
                  o2_uptake=0.0, divide_every=1, vessel_radius=0, stop_rule=STOP_RESIDUAL, first_tolerance=0.0,
                  cycle_median=0.0, cycle_spread=0.0, debris_loss=0.0, still_medium=0.0, exposure_intensity=0.0,
                  exposure_uptake=0.0, exposure_start=0, exposure_on=0, exposure_off=0, mutation_rate=0.0,
-                 rewiring=0.0):
+                 rewiring=0.0, field_off=False, differentiated_type=-1, apoptotic_type=-1, lineage=False):
         self.dims, w, h, z = _dims(dims)
         self._keep = [w, h, z]
         nc = np.array(ncells, np.uint32)
@@ -650,7 +650,8 @@ class Simulation:
                              int(vessel_radius), int(stop_rule), float(first_tolerance), float(cycle_median),
                              float(cycle_spread), float(debris_loss), float(still_medium), float(exposure_intensity),
                              float(exposure_uptake), int(exposure_start), int(exposure_on), int(exposure_off),
-                             float(mutation_rate), float(rewiring))
+                             float(mutation_rate), float(rewiring), int(bool(field_off)), int(differentiated_type),
+                             int(apoptotic_type), int(bool(lineage)))
         handle = C.c_void_p()
         call("cw_sim_create", C.byref(cfg), network.handle, C.byref(handle))
         self._h = handle
@@ -742,13 +743,13 @@ class Simulation:
         return out
 
     def clone_records(self):
-        """Every clone founded so far, in order: (parent clone, mutation record)."""
+        """Every clone a mutation founded so far, in order: (parent clone, mutation record)."""
         n = C.c_uint32()
-        call("cw_sim_clone_count", self._h, C.byref(n))
-        k = n.value - 1
+        call("cw_sim_clone_records", self._h, C.byref(n), None, None)
+        k = n.value
         parent = np.zeros(max(k, 1), np.int32)
         recs = (_lib.Mutation * max(k, 1))()
-        call("cw_sim_clone_records", self._h, ptr(parent), recs)
+        call("cw_sim_clone_records", self._h, C.byref(n), ptr(parent), recs)
         return [(int(parent[i]), self.network._record(recs[i])) for i in range(k)]
 
     def cycle(self, n, hist=0):

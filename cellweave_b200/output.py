@@ -3,12 +3,11 @@
 
 One row per step, the columns of MEASUREMENT_COLUMNS in that order, counts as
 integers and the exposure and the three radii to four decimals, so that two
-runs of one seed write the same bytes.  The device step has no
-differentiation, apoptosis, lesion, angiogenesis or immune cells: those
-columns are written as the reference writes them without those features (0),
-the clones column counts the founder's clone while anything lives (no
-mutation happens inside the device step), and a held column of oxygen is the
-vessel, all of it perfused.
+runs of one seed write the same bytes.  The device step has no lesion,
+angiogenesis or immune cells: those columns are written as the reference
+writes them without those features (0); the clones column counts the clones
+with a living cell (the founder's alone without mutation or a lineage), and
+a held column of oxygen is the vessel, all of it perfused.
 """
 from __future__ import annotations
 

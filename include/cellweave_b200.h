@@ -500,20 +500,29 @@ typedef struct {
                                     own network.  The draws: Philox under the history's key, counters (parent
                                     id, step, 6 / 7 / 8, 0).  0: every cell under the one network */
     double rewiring;             /* [0, 1]: the share of the changes that rewire */
+    int32_t field_off;           /* nothing consumes: the oxygen is not solved and stays at its start, 1 (the
+                                    field left off, simulation.rs:786-793, 2127-2131) */
+    int32_t differentiated_type; /* >= 0: the type a cell takes when it commits to differentiate (its network's
+                                    differentiation node's level its chance a step), then shedding SHEDDING_RATE
+                                    pixels a step until gone; -1: no such fate (simulation.rs:1209-1296) */
+    int32_t apoptotic_type;      /* >= 0: the same for apoptosis (the apoptosis node; FRAGMENTATION_RATE) */
+    int32_t lineage;             /* every seeded cell founds a clone of its own (a lineage-tracing sheet,
+                                    simulation.rs:780-785): cw_sim_clones and the measurements count them */
 } cw_sim_config;
 int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out);
 int cw_sim_destroy(cw_sim sim);
 /* `steps` lattice steps on every history. */
 int cw_sim_step(cw_sim sim, uint32_t steps);
-/* An evolving simulation's clones (mutation_rate > 0): the clone of records
- * 0..n-1 of history `hist` (0: the founding network), the clones founded in
- * the whole batch (the founding network counted), and each founded clone's
- * parent clone and mutation (cw_mutation as cw_network_mutate gives it), in
- * the order they were founded (nclones - 1 entries; either may be NULL).
- * No counterpart in the reference beyond its CloneRecord (simulation.rs:1686-1694). */
+/* The clones of a simulation with mutation or a lineage (CloneRecord,
+ * simulation.rs:780-785, 1686-1694): the clone of records 0..n-1 of history
+ * `hist` (0: the founding clone; with a lineage a seeded cell's clone is its
+ * record's index in the batch); the clones in the whole batch; and the clones
+ * mutations founded, in the order they were founded, which are the last
+ * *count clone indices: each one's parent clone and its mutation (cw_mutation
+ * as cw_network_mutate gives it; parent and mutation may be NULL). */
 int cw_sim_clones(cw_sim sim, uint32_t hist, uint32_t n, int32_t *clone);
 int cw_sim_clone_count(cw_sim sim, uint32_t *nclones);
-int cw_sim_clone_records(cw_sim sim, int32_t *parent, cw_mutation *mutation);
+int cw_sim_clone_records(cw_sim sim, uint32_t *count, int32_t *parent, cw_mutation *mutation);
 /* What the autotuner chose: the SOR relaxation factor of every history for
  * the oxygen and the signal field (0 until chosen: the reference's rule),
  * the FP32 blocking depth and window (CW_WINDOW_*), and whether it is still
@@ -551,6 +560,8 @@ typedef struct {
     uint64_t vessel;
     double tissue_radius, necrotic_radius, viable_depth;
     double exposure;     /* the exposure's level at the step last taken (0 without one or while off) */
+    uint64_t differentiating, apoptotic;  /* cells leaving the layer, cells breaking up */
+    uint64_t clones;     /* clones with a living cell (with lineage or mutation; else 1 while any cell lives) */
 } cw_measurements;
 int cw_sim_measure(cw_sim sim, cw_measurements *out);
 /* touches_the_edge (simulation.rs:2165-2198) of every history, one int32 each: a cell on a pixel of

@@ -27,6 +27,15 @@ def seed_history(cfg, w, h, d, n, seed):
     K = cfg["J"].shape[0]
     nec = cfg.get("necrotic_type", -1)
     ntypes = max(1, (nec - 1) if nec and nec > 0 else K - 1)
+    if cfg.get("seeding", 0) == 4:
+        # a sheet (Seeding::Sheet, simulation.rs:732-740): side x side blocks of
+        # normal tissue (type 2) tiling the box row by row
+        types = [0]
+        for y in range(0, h, s):
+            for x in range(0, w, s):
+                grid[0, y:y + s, x:x + s] = len(types)
+                types.append(2)
+        return grid, np.array(types, np.int32)
     if cfg.get("o2_hold", 0) == 1:
         grid[:, :, w // 2] = -1
     z_, y_, x_ = np.mgrid[0:d, 0:h, 0:w]
@@ -77,7 +86,7 @@ def seed_history(cfg, w, h, d, n, seed):
     return grid, np.array(types, np.int32)
 
 
-def measure_records(grid, types, volume, used, hypoxia, necrotic, o2_hold, mcs):
+def measure_records(grid, types, volume, used, hypoxia, necrotic, o2_hold, mcs, leaving=(), clone=None):
     """measure.rs:133-236 on a lattice's records: counts of cycling (hypoxia
     response under 0.45), quiescent and necrotic cells with pixels, born (every
     record assigned), gone (dead and resorbed to nothing), equivalent radii (a
@@ -89,11 +98,20 @@ def measure_records(grid, types, volume, used, hypoxia, necrotic, o2_hold, mcs):
     ids = np.arange(1, used)
     vol = volume[1:used].astype(np.int64)
     dead = (types[1:used] == necrotic) if necrotic >= 0 else np.zeros(used - 1, bool)
+    # cells leaving the layer or breaking up (differentiated, apoptotic types)
+    diff = (types[1:used] == leaving[0]) if len(leaving) > 0 and leaving[0] >= 0 else np.zeros(used - 1, bool)
+    apop = (types[1:used] == leaving[1]) if len(leaving) > 1 and leaving[1] >= 0 else np.zeros(used - 1, bool)
     has = vol > 0
-    live = has & ~dead
+    live = has & ~dead & ~diff & ~apop
     cyc = live & (hypoxia[1:used] < 0.45)
     m = dict(mcs=mcs, cycling=int(cyc.sum()), quiescent=int((live & ~cyc).sum()), necrotic=int((has & dead).sum()),
-             born=int(used - 1), gone=int((~has & dead).sum()))
+             born=int(used - 1), gone=int((~has & (dead | diff | apop)).sum()),
+             differentiating=int((has & diff).sum()), apoptotic=int((has & apop).sum()))
+    if clone is not None:
+        m["clones"] = int(np.unique(clone[1:used][live]).size)
+    else:
+        m["clones"] = 1 if live.any() else 0
+    leaving_area = int(vol[has & (diff | apop)].sum())
     m["vessel"] = int((grid == -1).sum()) if o2_hold in (1, 4) else 0
     living_area, dead_area = int(vol[live].sum()), int(vol[has & dead].sum())
 
@@ -104,7 +122,7 @@ def measure_records(grid, types, volume, used, hypoxia, necrotic, o2_hold, mcs):
             return float(np.sqrt(size / (np.pi * d)))
         return float(np.cbrt(3.0 * size / (4.0 * np.pi)))
 
-    m["tissue_radius"] = radius(m["vessel"] + living_area + dead_area)
+    m["tissue_radius"] = radius(m["vessel"] + living_area + dead_area + leaving_area)
     m["necrotic_radius"] = radius(dead_area)
     if o2_hold in (0, 1):
         alive_id = np.zeros(int(types.size), bool)
@@ -171,7 +189,8 @@ class CpuHistory:
         spec = cfg.get("network_spec") or tomllib.loads(cfg.get("network_toml") or
                                                           synthetic.network_toml(cfg["S"], cfg["S"]))
         # the network's reference volume: the seeded cell's (simulation.rs:726-733) or the target
-        self.refvol = int(self.lat.volume[1]) if cfg.get("seeding", 0) == 3 else int(cfg["target_volume"])
+        self.refvol = (int(self.lat.volume[1]) if cfg.get("seeding", 0) == 3 else
+                       int(cfg["seed_side"]) ** 2 if cfg.get("seeding", 0) == 4 else int(cfg["target_volume"]))
         self.net = O.compile_network(spec, self.refvol)
         self.state = np.tile(self.net.initial, (self.ncap, 1))
         # an evolving history (simulation.rs:1655-1700): every record's clone and
@@ -181,6 +200,12 @@ class CpuHistory:
         self.clone = np.zeros(self.ncap, np.int64)
         self.clone_specs = [spec]
         self.clone_nets = [self.net]
+        # a lineage (a sheet, simulation.rs:780-785): every seeded cell its own
+        # clone; its cells step under the one network
+        self.lineage = bool(cfg.get("lineage", False))
+        if self.lineage:
+            self.clone[:self.used] = np.arange(self.used)
+        self.leaving = (int(cfg.get("differentiated_type", -1)), int(cfg.get("apoptotic_type", -1)))
         self.div_rng = np.random.default_rng(self.seed * 7 + 13)
         # a cell's cycle (simulation.rs:1055-1056): none behind the cells the tissue starts with
         self.began = np.zeros(self.ncap, np.int64)
@@ -200,7 +225,9 @@ class CpuHistory:
         device step's reading of viable_depth for each oxygen hold."""
         return measure_records(self.lat.grid.reshape(self.dims[2], self.dims[1], self.dims[0]), self.lat.type,
                                self.lat.volume, self.used, self.state[:, self.net.hypoxia],
-                               self.cfg.get("necrotic_type", -1), self.cfg.get("o2_hold", 0), max(self.steps - 1, 0))
+                               self.cfg.get("necrotic_type", -1), self.cfg.get("o2_hold", 0), max(self.steps - 1, 0),
+                               leaving=self.leaving,
+                               clone=self.clone if (self.lineage or self.mutation_rate > 0) else None)
 
     def _settle_released(self, field, per_cell):
         """settle_released (simulation.rs:2546-2570): production from the cells
@@ -231,7 +258,8 @@ class CpuHistory:
             if c.get("o2_hold", 0) == 4:
                 up[g == 0] = c["o2_uptake"]
             self.o2.uptake = up
-        if c.get("o2_hold", 0) == 3:
+        field_off = bool(c.get("field_off", False))
+        if c.get("o2_hold", 0) == 3 and not field_off:
             # the bath as the lattice stands (declare_sources, simulation.rs:2138-2146)
             self.o2.held[:] = 0
             self.o2.hold_bath(g == 0, self.bath_level)
@@ -239,7 +267,8 @@ class CpuHistory:
         tol, most = c["tolerance"], 200_000
         if self.steps == 0 and c.get("first_tolerance", 0.0) > 0:
             tol, most = min(c["first_tolerance"], tol), 2_000_000  # start() (simulation.rs:1068-1083)
-        rc, _ = self.o2.relax(tol, most, omega=omega, stop=c.get("stop_rule", 1), threads=1)
+        # with the field off nothing consumes: the oxygen stays at its start (simulation.rs:2127-2131)
+        rc = 0 if field_off else self.o2.relax(tol, most, omega=omega, stop=c.get("stop_rule", 1), threads=1)[0]
         if c.get("still_medium", 0.0) > 0:
             self._settle_bath_level()
             if most == 2_000_000:
@@ -250,8 +279,17 @@ class CpuHistory:
                 self._settle_bath_level()
         o2m = O.mean_per_cell(g, self.o2.values, self.ncap)
         nec = c.get("necrotic_type", -1)
-        alive = (self.lat.volume > 0) & (t != nec)
+        ldiff, lapop = self.leaving
+        leaving_cell = ((t == ldiff) & (ldiff >= 0)) | ((t == lapop) & (lapop >= 0))
+        alive = (self.lat.volume > 0) & (t != nec) & ~leaving_cell
         alive[0] = False
+        # cells leaving the layer shed, those breaking up fragment (simulation.rs:1209-1262)
+        going = np.nonzero(leaving_cell & (self.lat.volume > 0))[0]
+        going = going[going > 0]
+        if len(going):
+            rate = np.where(t[going] == lapop, 8, 6)
+            self.lat.target[going] = np.maximum(self.lat.volume[going] - rate, 0)
+            self.lat.lam[going] = c["lambda_volume"]
         if self.str is not None:
             self.cell_str = self._settle_stress()
         if self.sig is not None:
@@ -316,8 +354,19 @@ class CpuHistory:
                 self.kept[nd] = True
                 self.lat.target[nd] = self.lat.volume[nd]
                 self.lat.lam[nd] = c["lambda_volume"]
-            live = idx[~dead]
-            full = np.minimum(tg[~dead], 2**31 - 1).astype(np.int64)
+            # apoptosis, then differentiation, each at its node's level as the
+            # cell's chance this step (simulation.rs:1276-1296)
+            keep = ~dead
+            ra, rd = self.net.optional.get("apoptosis", -1), self.net.optional.get("differentiation", -1)
+            for j in np.nonzero(keep)[0]:
+                if lapop >= 0 and ra is not None and ra >= 0 and self.div_rng.random() < st[j, ra]:
+                    t[idx[j]] = lapop
+                    keep[j] = False
+                elif ldiff >= 0 and rd is not None and rd >= 0 and self.div_rng.random() < st[j, rd]:
+                    t[idx[j]] = ldiff
+                    keep[j] = False
+            live = idx[keep]
+            full = np.minimum(tg[keep], 2**31 - 1).astype(np.int64)
             if c.get("cycle_median", 0.0) > 0:
                 # grown (simulation.rs:2534-2540)
                 b, e = self.began[live], self.due[live]
@@ -507,7 +556,8 @@ class CpuHistory:
         c = self.cfg
         nec = c.get("necrotic_type", -1)
         vol, t = self.lat.volume, self.lat.type
-        alive = (vol > 0) & (t != nec)
+        ldiff, lapop = self.leaving
+        alive = (vol > 0) & (t != nec) & ~((t == ldiff) & (ldiff >= 0)) & ~((t == lapop) & (lapop >= 0))
         alive[0] = False
         alive[self.used:] = False
         hyp = self.net.hypoxia

@@ -15,7 +15,8 @@ profiles.  Gradients with respect to D, k (three types) and network rates:
 * at the differentiated fit's own shape (the 2048 x 2048 cord stepped to MCS
   500 and frozen, 2000 RK4 steps with checkpoints every 100, D, three k and
   32 network rates) against central differences of the device's forward,
-  within 1e-4 relative.
+  within 1e-4 relative (a derivative too small for a step of 1e-4 of its
+  parameter to move the loss by more than FP64 resolves takes a larger step).
 
 A forward pass takes its cell means and bin sums in a fixed order, so it
 gives the same loss to the bit every time: the differences then resolve even
@@ -77,22 +78,39 @@ def problem():
 
 
 def central_differences(make, start, target, rel=1e-4):
-    """Central differences of the loss, each evaluation on a fresh fit (FP64
-    solves from the same start), so that the solves' last sweeps make the
-    same error on both sides of a step."""
+    """Central differences of the loss, each evaluation on a fresh fit (solves
+    from the same start, cell means and bin sums in a fixed order: the same
+    loss to the bit for the same parameters).  The step is `rel` of the
+    parameter; where the two losses then differ by less than 1e8 units in the
+    last place of the loss (a derivative some eight orders below the loss's
+    scale, whose difference the loss's own rounding could move by 1e-4 of
+    itself) it grows ten times, up to 1e-2 of the parameter, so that every
+    difference carries the digits the bound asks of it."""
     fd = np.zeros(len(start))
+
+    def loss_at(q):
+        f = make()
+        f.set_target(*target)
+        f.params = q
+        v = f.forward()[0]
+        del f
+        return v
+
+    base = loss_at(start)
+    ulp = np.spacing(base)
     for k in range(len(start)):
-        step = rel * abs(start[k]) if start[k] != 0 else 1e-7
-        vals = []
-        for sgn in (1, -1):
-            f = make()
-            f.set_target(*target)
+        r = rel
+        while True:
+            step = r * abs(start[k]) if start[k] != 0 else 1e-7
             q = start.copy()
-            q[k] += sgn * step
-            f.params = q
-            vals.append(f.forward()[0])
-            del f
-        fd[k] = (vals[0] - vals[1]) / (2 * step)
+            q[k] += step
+            up = loss_at(q)
+            q[k] -= 2 * step
+            down = loss_at(q)
+            if up == down or abs(up - down) >= 1e8 * ulp or r >= 1e-2 or start[k] == 0:
+                break
+            r *= 10
+        fd[k] = (up - down) / (2 * step)
     return fd
 
 

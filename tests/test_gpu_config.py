@@ -46,6 +46,27 @@ def ras_erk_toml(tmp_path, stressed=False):
     return spec
 
 
+def toml_value(v):
+    if isinstance(v, str):
+        return f'"{v}"'
+    if isinstance(v, dict):
+        return "{ " + ", ".join(f"{k} = {toml_value(x)}" for k, x in v.items()) + " }"
+    return str(v)
+
+
+def network_file(tmp_path, name, spec):
+    lines = []
+    for node in spec["nodes"]:
+        lines += ["[[nodes]]", f'name = "{node["name"]}"', f'initial = {node["initial"]}', "terms = ["]
+        lines += ["  " + toml_value(t) + "," for t in node["terms"]]
+        lines.append("]")
+    lines.append("[roles]")
+    lines += [f'{k} = "{v}"' for k, v in spec["roles"].items()]
+    lines.append("[mechanics]")
+    lines += [f"{k} = {v}" for k, v in spec["mechanics"].items()]
+    (tmp_path / name).write_text("\n".join(lines) + "\n")
+
+
 def scenario(tmp_path, source, uptake=0.001, stressed=False):
     spec = ras_erk_toml(tmp_path, stressed)
     text = ("width = 120\nheight = 120\nmcs = 140\ntemperature = 10.0\nsnapshot_interval = 20\n"
@@ -91,6 +112,49 @@ def test_a_configured_tissue_grows_inside_the_oracle_band(tmp_path, source, upta
         assert {r["change"] for _, r in founded} >= {"scaled", "gained"} or len(founded) < 10
         clones = np.concatenate([sim.clones(200, k) for k in range(SEEDS)])
         assert clones.max() == len(founded)
+    for k in range(SEEDS):
+        assert sim.records_match_grid(k)
+
+
+def test_a_sheet_of_epithelium_turns_over_inside_the_oracle_band(tmp_path):
+    # Seeding::Sheet with the field off (simulation.rs:696-749): a 60 x 60 box
+    # tiled with 10 x 10 cells of normal tissue, each the founder of a clone,
+    # under the reference's epithelium network (its NOTCH node the chance to
+    # commit to differentiate; committed cells shed until gone).  The device's
+    # 32 histories against the oracle's: living and differentiating cells, the
+    # cells gone and the clones left inside the 32-seed band
+    spec = json.load(open(os.path.join(HERE, "golden", "golden.json")))["networks"]["epithelium"]
+    network_file(tmp_path, "epithelium.toml", spec)
+    p = tmp_path / "run.toml"
+    p.write_text("width = 60\nheight = 60\nmcs = 300\ntemperature = 10.0\nsnapshot_interval = 100\n"
+                 "output_dir = \"out\"\noxygen_uptake = 0.0\nnetwork = \"epithelium.toml\"\n"
+                 "[seeding]\nkind = \"sheet\"\nside = 10\n")
+    cfg = C.load_sim_config(str(p))
+    seeds = [9_000 + k for k in range(SEEDS)]
+    sim, _ = C.simulation_from_config(cfg, histories=SEEDS, seeds=seeds)
+    kw, refvol = C.simulation_kwargs(cfg, SEEDS, seeds)
+    assert refvol == 100 and kw["field_off"] and kw["lineage"]
+    ocfg = dict(kw, network_spec=spec, lambda_volume=float(spec["mechanics"]["lambda_volume"]), hypoxic_level=0.1)
+    ora = [CpuHistory(ocfg, k) for k in range(SEEDS)]
+    first = sim.measure()
+    assert all(m["clones"] == 36 and m["cycling"] + m["quiescent"] == 36 for m in first)
+    keys = ("cycling", "differentiating", "gone", "clones")
+    for step in range(1, 301):
+        sim.step(1)
+        for h in ora:
+            h.step()
+        if step not in (100, 200, 300):
+            continue
+        dm = sim.measure()
+        om = [h.measure() for h in ora]
+        for q in keys:
+            dv = np.array([float(m[q]) for m in dm])
+            rv = np.array([float(m[q]) for m in om])
+            assert within_band(dv, rv), (step, q, dv.mean(), rv.mean(), rv.std())
+    dm = sim.measure()
+    assert np.mean([m["gone"] for m in dm]) > 10 and np.mean([m["clones"] for m in dm]) < 36
+    # the oxygen was never solved: every cell read full oxygen
+    assert np.all(sim.field_values(0, 0) == 1.0)
     for k in range(SEEDS):
         assert sim.records_match_grid(k)
 
