@@ -50,7 +50,7 @@ _ERRORS = {ERR_CONFIG: ConfigError, ERR_SIMULATION: SimulationError, ERR_ODE: Od
 class RelaxOpts(C.Structure):
     _fields_ = [("omega", C.c_double), ("stop", C.c_int32), ("tolerance", C.c_double), ("max_sweeps", C.c_int64),
                 ("precision", C.c_int32), ("inner_sweeps", C.c_int32), ("block_depth", C.c_int32),
-                ("window", C.c_int32)]
+                ("window", C.c_int32), ("error_tolerance", C.c_double)]
 
 
 class RelaxStats(C.Structure):
@@ -105,7 +105,7 @@ class SimConfig(C.Structure):
                 ("exposure_intensity", C.c_double), ("exposure_uptake", C.c_double), ("exposure_start", C.c_int32),
                 ("exposure_on", C.c_int32), ("exposure_off", C.c_int32), ("mutation_rate", C.c_double),
                 ("rewiring", C.c_double), ("field_off", C.c_int32), ("differentiated_type", C.c_int32),
-                ("apoptotic_type", C.c_int32), ("lineage", C.c_int32)]
+                ("apoptotic_type", C.c_int32), ("lineage", C.c_int32), ("error_tolerance", C.c_double)]
 
 
 P = C.c_void_p

@@ -35,6 +35,14 @@ struct RelaxState {
     double last_change;
     double last_resid;
     int64_t inner;                // FP32 sweeps taken (defect correction)
+    // the error estimate of the defect-correction solve (the wide sweeps'
+    // apply): the largest |correction| of the last outer iteration and the
+    // largest |c| it left, as the bits of non-negative doubles (atomic max),
+    // the previous iteration's largest correction, and the bound asked
+    unsigned long long corr;
+    unsigned long long cmax;
+    double prev_corr;
+    double etol;
 };
 
 // (a history holds fewer than 2^31 pixels: 32-bit division is enough)
@@ -265,30 +273,56 @@ __global__ void __launch_bounds__(256) k_dc_update(FieldView fv, const int32_t *
     block_max_to(&st[h].resid, worst);
 }
 
-__global__ void k_dc_check(RelaxState *st, int nh, int inner, int64_t max_sweeps) {
+// The error a contraction leaves after a correction of largest size c whose
+// ratio to the one before is q < 1: the corrections to come sum to at most
+// c q / (1 - q) if the ratio holds; doubled for the ratio's wobble.  A zero
+// correction leaves nothing; no ratio (the first correction, or q >= 1)
+// gives no estimate (a huge one).
+__device__ __forceinline__ double error_estimate(double c, double prev) {
+    if (c == 0.0) return 0.0;
+    if (!(prev > 0.0) || c >= prev) return 1e308;
+    double q = c / prev;
+    return 2.0 * c * q / (1.0 - q);
+}
+
+// `estimated`: the sweeps report their corrections (the wide apply), and a
+// history with etol > 0 also waits for its error estimate to fall below etol
+// times its largest |c|.
+__global__ void k_dc_check(RelaxState *st, int nh, int inner, int64_t max_sweeps, int estimated) {
     int h = blockIdx.x * blockDim.x + threadIdx.x;
     if (h >= nh) return;
     RelaxState &s = st[h];
     if (!s.done) {
         double r = __longlong_as_double((long long)s.resid);
         s.last_resid = r;
-        if (r < s.tol) s.done = 1;
+        double c = __longlong_as_double((long long)s.corr);
+        bool close = true;
+        if (estimated && s.etol > 0.0)
+            close = s.inner > 0 && error_estimate(c, s.prev_corr) < s.etol * __longlong_as_double((long long)s.cmax);
+        if (r < s.tol && close) s.done = 1;
         else if (s.inner >= max_sweeps) s.done = 2;  // out of sweeps: reported as not settled
         else { s.inner += inner; s.sweeps = s.inner; }
+        s.prev_corr = c;
     }
     s.resid = 0ull;
+    s.corr = 0ull;
+    s.cmax = 0ull;
 }
 
 // The test of k_dc_check without its bookkeeping: marks what settled and
 // records the residual, leaving the accumulator for the next k_dc_check.
-__global__ void k_dc_peek(RelaxState *st, int nh) {
+__global__ void k_dc_peek(RelaxState *st, int nh, int estimated) {
     int h = blockIdx.x * blockDim.x + threadIdx.x;
     if (h >= nh) return;
     RelaxState &s = st[h];
     if (!s.done) {
         double r = __longlong_as_double((long long)s.resid);
         s.last_resid = r;
-        if (r < s.tol) s.done = 1;
+        bool close = true;
+        if (estimated && s.etol > 0.0)
+            close = s.inner > 0 && error_estimate(__longlong_as_double((long long)s.corr), s.prev_corr) <
+                                       s.etol * __longlong_as_double((long long)s.cmax);
+        if (r < s.tol && close) s.done = 1;
     }
 }
 
@@ -958,12 +992,13 @@ struct DcCache {
     double *d_omega = nullptr;  // per history, for the state initialisation on the device
 };
 
-__global__ void k_dc_state_init(RelaxState *st, int nh, const double *omega, double tol) {
+__global__ void k_dc_state_init(RelaxState *st, int nh, const double *omega, double tol, double etol) {
     int h = blockIdx.x * blockDim.x + threadIdx.x;
     if (h >= nh) return;
     RelaxState s{};
     s.omega = omega[h];
     s.tol = tol;
+    s.etol = etol;
     s.stop = CW_STOP_RESIDUAL;
     st[h] = s;
 }
@@ -1021,13 +1056,16 @@ static int dc_outer(cw_field_s *f, DcCache *c, RelaxState *d_st, int inner, int6
     FieldView fv = view(f);
     const int32_t *done_ptr = (const int32_t *)((const char *)d_st + offsetof(RelaxState, done));
     const int stride = (int)(sizeof(RelaxState) / sizeof(int32_t));
-    k_dc_check<<<(nh + 63) / 64, 64, 0, stream()>>>(d_st, nh, inner, max_sweeps);
+    k_dc_check<<<(nh + 63) / 64, 64, 0, stream()>>>(d_st, nh, inner, max_sweeps, c->solver.wide ? 1 : 0);
     CW_LAUNCHED();
     if (c->solver.wide) {
-        // the last sweep launch adds the correction to c; then the residual
-        // at the corrected field, in one pass (the correction buffer needs no
-        // zeroing: the next solve's first launch does not read it)
-        int rc = c->solver.sweeps(f, inner, done_ptr, stride, start, true);
+        // the last sweep launch adds the correction to c, recording its
+        // largest size and the largest |c| for the error estimate; then the
+        // residual at the corrected field, in one pass (the correction buffer
+        // needs no zeroing: the next solve's first launch does not read it)
+        unsigned long long *corr = (unsigned long long *)((char *)d_st + offsetof(RelaxState, corr));
+        int rc = c->solver.sweeps(f, inner, done_ptr, stride, start, true, corr,
+                                  (int)(sizeof(RelaxState) / sizeof(unsigned long long)));
         if (rc != CW_OK) return rc;
         dc_residual(c, fv, nh, d_st, f->r32, nullptr, nullptr);
         CW_LAUNCHED();
@@ -1092,7 +1130,8 @@ int field_relax_enqueue(cw_field_s *f, const cw_relax_opts *opts, int outer, flo
     uint32_t nh = f->g.nh;
     RelaxState *d_st = (RelaxState *)f->stats;
     int inner = opts->inner_sweeps > 0 ? opts->inner_sweeps : 16;
-    k_dc_state_init<<<(nh + 63) / 64, 64, 0, stream()>>>(d_st, nh, c->d_omega, opts->tolerance);
+    k_dc_state_init<<<(nh + 63) / 64, 64, 0, stream()>>>(d_st, nh, c->d_omega, opts->tolerance,
+                                                         opts->error_tolerance);
     CW_LAUNCHED();
     FieldView fv = view(f);
     dc_residual(c, fv, nh, d_st, f->r32, f->inv32, f->d32a);
@@ -1103,7 +1142,7 @@ int field_relax_enqueue(cw_field_s *f, const cw_relax_opts *opts, int outer, flo
         if (rc != CW_OK) return rc;
     }
     // a last test marks what settled
-    k_dc_peek<<<(nh + 63) / 64, 64, 0, stream()>>>(d_st, nh);
+    k_dc_peek<<<(nh + 63) / 64, 64, 0, stream()>>>(d_st, nh, c->solver.wide ? 1 : 0);
     CW_LAUNCHED();
     if (start_out) *start_out = start;
     return CW_OK;
@@ -1127,7 +1166,7 @@ int field_relax_finish(cw_field_s *f, const cw_relax_opts *opts, float *start) {
         if (all) return CW_OK;
         int rc = dc_outer(f, c, d_st, inner, opts->max_sweeps, start);
         if (rc != CW_OK) return rc;
-        k_dc_peek<<<(nh + 63) / 64, 64, 0, stream()>>>(d_st, nh);
+        k_dc_peek<<<(nh + 63) / 64, 64, 0, stream()>>>(d_st, nh, c->solver.wide ? 1 : 0);
         CW_LAUNCHED();
     }
     return CW_OK;
@@ -1387,6 +1426,9 @@ int cw::field_relax(cw_field_s *f, const cw_relax_opts *opts, const double *omeg
         return fail(CW_ERR_CONFIG, "the FP32 defect-correction solve stops on the residual only");
     if (!(o.tolerance > 0.0 && o.tolerance < INFINITY))
         return fail(CW_ERR_CONFIG, "the tolerance must be finite and above zero, got " + std::to_string(o.tolerance));
+    if (!(o.error_tolerance >= 0.0 && o.error_tolerance < INFINITY))
+        return fail(CW_ERR_CONFIG, "the error tolerance must be finite and not negative, got " +
+                                       std::to_string(o.error_tolerance));
     if (!(o.omega < 2.0))
         return fail(CW_ERR_CONFIG, "the relaxation factor must lie in (0, 2) (or be <= 0 for the rule), got " +
                                        std::to_string(o.omega));
@@ -1407,6 +1449,7 @@ int cw::field_relax(cw_field_s *f, const cw_relax_opts *opts, const double *omeg
         RelaxState &s = hs[k];
         std::memset(&s, 0, sizeof s);
         s.tol = o.tolerance;
+        s.etol = o.error_tolerance;
         s.stop = o.stop;
         if (!spans[k].found) {  // nothing to balance: one sweep that moves nothing (pde.rs:256-259)
             s.done = 1;

@@ -214,7 +214,7 @@ __global__ void __launch_bounds__(32 * WWARPS, WWARPS == 8 ? 2 : 1)
                  const int4 *__restrict__ tiles, int ntiles, const int4 *__restrict__ dims,
                  const int64_t *__restrict__ off, const float *__restrict__ omega, const int32_t *done,
                  int done_stride, int nhalf, int start_colour, int zero_start, double *__restrict__ apply_c,
-                 int floor, unsigned long long wait_ns, int skip_copies) {
+                 int floor, unsigned long long wait_ns, int skip_copies, unsigned long long *corr, int corr_stride) {
     constexpr int WY = WROWS * WWARPS;  // window rows
     constexpr int STAGE = WX * WY;      // floats per array of the staged window
     extern __shared__ __align__(128) float smem[];
@@ -324,11 +324,18 @@ __global__ void __launch_bounds__(32 * WWARPS, WWARPS == 8 ? 2 : 1)
         if (apply_c) {
             // c += d on the free pixels (held ones have a = 0 and d = 0 throughout)
             double *row = apply_c + first;
+            float most = 0.f;   // the largest |d| the window adds
+            double top = 0.0;   // and the largest |c| it leaves
 #pragma unroll
             for (int j = 0; j < WROWS; ++j, row += dm.x) {
                 if (j < j0 || j >= j1 || !(full || part)) continue;
                 const float dv[4] = {d[j].x, d[j].y, d[j].z, d[j].w};
                 const float av[4] = {a[j].x, a[j].y, a[j].z, a[j].w};
+                if (corr) {
+#pragma unroll
+                    for (int e = 0; e < 4; ++e)
+                        if (full || (gx + e >= ix0 && gx + e < ix1)) most = fmaxf(most, fabsf(dv[e]));
+                }
                 if (full) {
                     double2 c01 = *(double2 *)row, c23 = *(double2 *)(row + 2);
                     double cv[4] = {c01.x, c01.y, c23.x, c23.y};
@@ -337,6 +344,7 @@ __global__ void __launch_bounds__(32 * WWARPS, WWARPS == 8 ? 2 : 1)
                         if (dv[e] != 0.f || av[e] != 0.f) {
                             cv[e] = cv[e] + (double)dv[e];
                             if (floor) cv[e] = fmax(cv[e], 0.0);
+                            top = fmax(top, fabs(cv[e]));
                         }
                     *(double2 *)row = make_double2(cv[0], cv[1]);
                     *(double2 *)(row + 2) = make_double2(cv[2], cv[3]);
@@ -346,7 +354,19 @@ __global__ void __launch_bounds__(32 * WWARPS, WWARPS == 8 ? 2 : 1)
                         if (gx + e >= ix0 && gx + e < ix1 && (dv[e] != 0.f || av[e] != 0.f)) {
                             double v = row[e] + (double)dv[e];
                             row[e] = floor ? fmax(v, 0.0) : v;
+                            top = fmax(top, fabs(row[e]));
                         }
+                }
+            }
+            if (corr) {
+                // one atomic per warp and window
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) most = fmaxf(most, __shfl_xor_sync(0xffffffffu, most, o));
+                for (int o = 16; o > 0; o >>= 1) top = fmax(top, __shfl_xor_sync(0xffffffffu, top, o));
+                if (lane == 0) {
+                    unsigned long long *mine = corr + (int64_t)info.tl.x * corr_stride;
+                    if (most > 0.f) atomicMax(mine, (unsigned long long)__double_as_longlong((double)most));
+                    if (top > 0.0) atomicMax(mine + 1, (unsigned long long)__double_as_longlong(top));
                 }
             }
         } else {
@@ -402,7 +422,7 @@ typedef void (*TbKernel)(const float *, float *, const float *, const float *, c
                          const int32_t *, int, const float *, const int32_t *, int, int, int);
 typedef void (*WideKernel)(const CUtensorMap *, int, float *, const int4 *, int, const int4 *, const int64_t *,
                            const float *, const int32_t *, int, int, int, int, double *, int, unsigned long long,
-                           int);
+                           int, unsigned long long *, int);
 
 TbKernel tb_kernel(int depth) {
     switch (depth) {
@@ -528,7 +548,8 @@ int Sor32::init(cw_field_s *f, int d, const std::vector<double> &om, int window)
     return rc;
 }
 
-int Sor32::sweeps(cw_field_s *f, int n, const int32_t *done, int done_stride, float *start, bool apply) {
+int Sor32::sweeps(cw_field_s *f, int n, const int32_t *done, int done_stride, float *start, bool apply,
+                  unsigned long long *corr, int corr_stride) {
     if (apply && !wide) return fail(CW_ERR_CONFIG, "only the wide FP32 kernel applies its correction");
     if (start) {  // begin from this (zeroed) buffer; the other is scratch
         ping = start;
@@ -559,7 +580,8 @@ int Sor32::sweeps(cw_field_s *f, int n, const int32_t *done, int done_stride, fl
             wide_kernel(depth, wwarps)<<<wgrid, 32 * wwarps, wide_smem(wwarps), stream()>>>(
                 (const CUtensorMap *)maps, a == f->d32a ? 0 : 1, b, wtiles, nwtiles, f->g.d_dims, f->g.d_off, omega,
                 done, done_stride, dd, done_half & 1, done_half == 0 ? 1 : 0, apply && last ? f->c : nullptr,
-                f->floor ? 1 : 0, test_faults().wait_ns ? test_faults().wait_ns : TMA_WAIT_NS, test_faults().skip_tma);
+                f->floor ? 1 : 0, test_faults().wait_ns ? test_faults().wait_ns : TMA_WAIT_NS, test_faults().skip_tma,
+                apply && last ? corr : nullptr, corr_stride);
         } else {
             tb_kernel(depth)<<<tiles.nblocks, 32 * WARPS, 0, stream()>>>(a, b, f->r32, f->inv32, f->g.d_dims,
                                                                          f->g.d_off, tiles.d_blk, f->g.nh, omega,

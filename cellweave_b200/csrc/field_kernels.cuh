@@ -68,8 +68,11 @@ struct Sor32 {
     // n sweeps from the zeroed correction buffer `start` (or the last result);
     // `apply` (wide only): the last launch adds the correction to the field's
     // values instead of writing it, and result() is null
+    // corr (optional, apply only): per history, with stride corr_stride, the
+    // largest |correction| the launch added, as the bits of a non-negative
+    // double (atomic max)
     int sweeps(cw_field_s *f, int n, const int32_t *done, int done_stride, float *start = nullptr,
-               bool apply = false);
+               bool apply = false, unsigned long long *corr = nullptr, int corr_stride = 0);
     float *result() const { return out; }
     void release();
 };

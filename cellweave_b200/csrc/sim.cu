@@ -576,6 +576,8 @@ int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out) {
     if (c.nh == 0) return fail(CW_ERR_CONFIG, "a simulation needs a history");
     if (c.K < 2 || c.K > 8) return fail(CW_ERR_CONFIG, "2 to 8 types, the medium included");
     if (c.nfields < 1 || c.nfields > 2) return fail(CW_ERR_CONFIG, "one or two fields");
+    if (!(c.error_tolerance >= 0.0 && c.error_tolerance < INFINITY))
+        return fail(CW_ERR_CONFIG, "the error tolerance must be finite and not negative");
     if (c.o2_hold < 0 || c.o2_hold > 4)
         return fail(CW_ERR_CONFIG, "the oxygen is held on a row, a column, the faces, the bath or a vessel");
     if (c.o2_hold == 4 && c.vessel_radius < 1) return fail(CW_ERR_CONFIG, "a vessel needs a radius of a pixel or more");
@@ -1299,6 +1301,7 @@ int cw_sim_step(cw_sim s, uint32_t nsteps) {
     o.omega = c.omega;
     o.stop = c.stop_rule == CW_STOP_MAX_CHANGE ? CW_STOP_MAX_CHANGE : CW_STOP_RESIDUAL;
     o.tolerance = c.tolerance;
+    o.error_tolerance = c.error_tolerance;
     o.max_sweeps = 200000;
     o.precision = c.precision;
     o.inner_sweeps = c.inner_sweeps > 0 ? c.inner_sweeps : 32;

@@ -149,10 +149,10 @@ class ScalarField:
         call("cw_field_hold_bath", self._h, hist, ptr(o), float(value))
 
     def relax(self, tolerance, max_sweeps, omega=None, stop=STOP_MAX_CHANGE, precision=FP64, inner_sweeps=0,
-              block_depth=0, window=WINDOW_AUTO, stats=False):
+              block_depth=0, window=WINDOW_AUTO, stats=False, error_tolerance=0.0):
         """relax (pde.rs:245-288): the sweep count of every history (SimulationError if one did not settle)."""
         o = _lib.RelaxOpts(float(omega) if omega else 0.0, int(stop), float(tolerance), int(max_sweeps),
-                           int(precision), int(inner_sweeps), int(block_depth), int(window))
+                           int(precision), int(inner_sweeps), int(block_depth), int(window), float(error_tolerance))
         st = (_lib.RelaxStats * len(self.dims))()
         rc = lib().cw_field_relax(self._h, C.byref(o), st)
         result = [dict(sweeps=s.sweeps, last_change=s.last_change, residual=s.residual, status=s.status,
@@ -174,7 +174,7 @@ class ScalarField:
         if g.size != total:
             raise ConfigError(f"expected {total} values, got {g.size}")
         o = _lib.RelaxOpts(float(omega) if omega else 0.0, int(stop), float(tolerance), int(max_sweeps),
-                           int(precision), int(inner_sweeps), int(block_depth), int(window))
+                           int(precision), int(inner_sweeps), int(block_depth), int(window), 0.0)
         st = (_lib.RelaxStats * len(self.dims))()
         lam = np.empty(total)
         call("cw_field_relax_adjoint", self._h, ptr(g), ptr(lam), C.byref(o), st)
@@ -628,7 +628,8 @@ class Simulation:
                  o2_uptake=0.0, divide_every=1, vessel_radius=0, stop_rule=STOP_RESIDUAL, first_tolerance=0.0,
                  cycle_median=0.0, cycle_spread=0.0, debris_loss=0.0, still_medium=0.0, exposure_intensity=0.0,
                  exposure_uptake=0.0, exposure_start=0, exposure_on=0, exposure_off=0, mutation_rate=0.0,
-                 rewiring=0.0, field_off=False, differentiated_type=-1, apoptotic_type=-1, lineage=False):
+                 rewiring=0.0, field_off=False, differentiated_type=-1, apoptotic_type=-1, lineage=False,
+                 error_tolerance=0.0):
         self.dims, w, h, z = _dims(dims)
         self._keep = [w, h, z]
         nc = np.array(ncells, np.uint32)
@@ -651,7 +652,7 @@ class Simulation:
                              float(cycle_spread), float(debris_loss), float(still_medium), float(exposure_intensity),
                              float(exposure_uptake), int(exposure_start), int(exposure_on), int(exposure_off),
                              float(mutation_rate), float(rewiring), int(bool(field_off)), int(differentiated_type),
-                             int(apoptotic_type), int(bool(lineage)))
+                             int(apoptotic_type), int(bool(lineage)), float(error_tolerance))
         handle = C.c_void_p()
         call("cw_sim_create", C.byref(cfg), network.handle, C.byref(handle))
         self._h = handle

@@ -246,6 +246,12 @@ typedef struct {
     int32_t inner_sweeps;/* CW_FP32_DC: FP32 sweeps per FP64 defect correction (0: 16) */
     int32_t block_depth; /* CW_FP32_DC: half-sweeps per launch kept in shared memory (0: 4) */
     int32_t window;      /* CW_FP32_DC: a CW_WINDOW_* */
+    double error_tolerance; /* CW_FP32_DC on flat fields (the TMA-fed sweeps): > 0 also asks that the
+                               error left, estimated from the last two corrections (the largest
+                               change c_k and their ratio q: c_k q / (1 - q), doubled), be below this,
+                               so that a solve stops once its field is that close to the converged
+                               one whatever the residual says; the residual rule still holds.
+                               0: the residual alone.  No counterpart in the reference */
 } cw_relax_opts;
 typedef struct {
     int64_t sweeps;      /* the count relax returns (pde.rs:279-283) */
@@ -508,6 +514,7 @@ typedef struct {
     int32_t apoptotic_type;      /* >= 0: the same for apoptosis (the apoptosis node; FRAGMENTATION_RATE) */
     int32_t lineage;             /* every seeded cell founds a clone of its own (a lineage-tracing sheet,
                                     simulation.rs:780-785): cw_sim_clones and the measurements count them */
+    double error_tolerance;      /* the FP32 solves' error_tolerance (cw_relax_opts); 0: the residual alone */
 } cw_sim_config;
 int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out);
 int cw_sim_destroy(cw_sim sim);

@@ -119,6 +119,52 @@ def test_fp32_defect_correction_reaches_the_fp64_solution(n, depth):
     assert np.abs(v - o.values).max() < 1e-6 * np.abs(o.values).max()
 
 
+def relaxed_from(values, held, sink, dcoef, n):
+    """The oracle's FP64 solution to residual 1e-12, started from `values`
+    (the unique fixed point: where SOR starts only shortens the CPU solve)."""
+    o = O.Field(n, n, 1, dcoef, 0.0, 0.0)
+    o.lin_sink = sink.copy()
+    o.held[:] = held
+    o.values[:] = values
+    assert o.relax(1e-12, 5_000_000, omega=1.9, stop=1)[0] == 0
+    return o.values
+
+
+@pytest.mark.parametrize("n,k", [(512, 0.01), (512, 0.002), (1024, 0.001)])
+def test_the_error_estimate_stop_leaves_the_field_within_its_bound(n, k):
+    # a loose residual (1e-6) with an error bound of 1e-7 of the field's
+    # scale: the solve runs on until the estimate from its last two
+    # corrections is under the bound, and the field is within 1e-6 of the
+    # FP64 oracle's wherever the residual alone would have stopped
+    held, sink, dcoef = sheet_problem(n, k=k)
+    g = cw.ScalarField.new(n, n, dcoef, 0.0, 0.0)
+    g.set_linear_sink(sink)
+    g.hold_where(1.0, held)
+    loose = g.relax(1e-6, 1_000_000, omega=1.9, stop=cw.STOP_RESIDUAL, precision=cw.FP32_DC, block_depth=8,
+                    stats=True)[0]
+    g2 = cw.ScalarField.new(n, n, dcoef, 0.0, 0.0)
+    g2.set_linear_sink(sink)
+    g2.hold_where(1.0, held)
+    st = g2.relax(1e-6, 1_000_000, omega=1.9, stop=cw.STOP_RESIDUAL, precision=cw.FP32_DC, block_depth=8,
+                  error_tolerance=1e-7, stats=True)[0]
+    assert st["residual"] < 1e-6 and st["sweeps"] >= loose["sweeps"]
+    v = g2.values()
+    exact = relaxed_from(v, held, sink, dcoef, n)
+    assert np.abs(v - exact).max() < 1e-6 * np.abs(exact).max()
+    # solved again from its own solution: two outer iterations give the ratio
+    again = g2.relax(1e-6, 1_000_000, omega=1.9, stop=cw.STOP_RESIDUAL, precision=cw.FP32_DC, block_depth=8,
+                     error_tolerance=1e-7, stats=True)[0]
+    assert again["sweeps"] <= st["sweeps"]
+    assert np.abs(g2.values() - exact).max() < 1e-6 * np.abs(exact).max()
+
+
+def test_the_error_tolerance_is_checked():
+    g = cw.ScalarField.new(64, 64, 1.0, 0.0, 0.0)
+    for bad in (-1e-7, float("inf"), float("nan")):
+        with pytest.raises(cw.ConfigError):
+            g.relax(1e-6, 1000, precision=cw.FP32_DC, stop=cw.STOP_RESIDUAL, error_tolerance=bad)
+
+
 def test_fp32_defect_correction_on_a_volume():
     n = 40
     held = np.zeros((n, n, n), np.uint8)
