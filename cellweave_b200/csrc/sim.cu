@@ -869,7 +869,9 @@ int cw_sim_destroy(cw_sim s) {
     dfree(s->d_step); dfree(s->bath); dfree(s->d_uptake);
     dfree(s->d_sink); dfree(s->cell_o2); dfree(s->cell_sig); dfree(s->sum); dfree(s->secretion); dfree(s->count);
     dfree(s->state); dfree(s->inputs); dfree(s->alive); dfree(s->target32);
-    for (size_t k = 1; k < s->clones.size(); ++k) cw_network_destroy(s->clones[k]);
+    // the clones mutation founded; a lineage's founders share the caller's network
+    for (size_t k = 1; k < s->clones.size(); ++k)
+        if (s->clones[k] != s->net) cw_network_destroy(s->clones[k]);
     dfree(s->d_clone); dfree(s->d_nets);
     s->sites.release();
     s->hs.release();

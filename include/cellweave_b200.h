@@ -431,7 +431,9 @@ typedef struct {
     double lambda_volume;
     int32_t surface_target;      /* <= 0: no surface constraint */
     double lambda_surface;
-    int32_t seeding;             /* 0 squares at random free places, 1 a packed ball of cubes */
+    int32_t seeding;             /* 0 squares at random free places, 1 a packed ball of cubes, 3 one cell (below),
+                                    4 a sheet: the plane tiled by seed_side-square cells of type 2 (simulation.rs:
+                                    696-731; needs field_off) */
     int32_t seed_side;           /* side of a seeded square / cube */
     int32_t nfields;             /* 1 (oxygen) or 2 (oxygen and a secreted signal) */
     double o2_dcoef;

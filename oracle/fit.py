@@ -3,15 +3,18 @@
 The reference has no loss, no adjoint and no autodiff; this restates the loss
 the library's fit (cw_fit_*) differentiates, from the oracle's restatements
 of the reference's pieces, so that a gradient can be taken independently of
-the device: central differences of this loss, every solve to a residual of
-1e-14 (a solve's last sweeps then move the loss by less than a part in 1e4 of
-its smallest non-zero derivative times the step).
+the device: central differences of this loss.  Each field is the fixed point
+the reference's SOR (pde.rs:245-405) converges to, solved directly here (a
+sparse LU of the same five-point operator: pde.rs's balance per free pixel,
+held neighbours on the right-hand side), so that the loss is a smooth
+function of the parameters to FP64's rounding and no stopping point of an
+iteration moves it between two nearby parameter sets; the floor at zero is
+checked to be idle (every free value positive).
 
     oxygen  D lap c - k_type c = 0, held at `vessel_value` on the lattice's
             obstacle pixels (hold_obstacles_at, coupling.rs:80-82; the
             first-order sink by type as apply_uptake paints it,
-            coupling.rs:26-39), relaxed by the reference's SOR
-            (pde.rs:245-405) to the residual `tolerance`;
+            coupling.rs:26-39);
     o_j     mean_per_cell (coupling.rs:164-182);
     x_j(T)  `steps` RK4 steps (network.rs:777-799) from the network's initial
             state, inputs (o_j, egf, 0, 0, 0, 0), the first `ntheta` term
@@ -30,16 +33,58 @@ from __future__ import annotations
 import copy
 
 import numpy as np
+import scipy.sparse as sp
+import scipy.sparse.linalg as spla
 
 from . import oracle as O
+
+
+def solve_direct(f):
+    """The fixed point of pde.rs's relax for field `f` (an oracle Field): per
+    free pixel i, (D n_i + decay + k_i) c_i - D sum of its free neighbours =
+    source + production_i - uptake_i + D sum of its held neighbours' values,
+    n_i its neighbours inside the box (or_pixel_sums, or_denominator).
+    Written into f.values; the floor at zero must be idle."""
+    w, h, d = f.w, f.h, f.d
+    n = w * h * d
+    held = f.held.astype(bool)
+    free = np.flatnonzero(~held)
+    idx = np.full(n, -1, np.int64)
+    idx[free] = np.arange(free.size)
+    x = np.arange(n) % w
+    y = (np.arange(n) // w) % h
+    z = np.arange(n) // (w * h)
+    real = np.zeros(n)
+    rhs = (f.source + f.production - f.uptake).astype(np.float64)
+    rows, cols, vals = [], [], []
+    for ok, step in ((x > 0, -1), (x + 1 < w, 1), (y > 0, -w), (y + 1 < h, w), (z > 0, -w * h),
+                     (z + 1 < d, w * h)):
+        real += ok
+        i = free[ok[free]]
+        j = i + step
+        hj = held[j]
+        np.add.at(rhs, i[hj], f.dcoef * f.values[j[hj]])
+        rows.append(idx[i[~hj]])
+        cols.append(idx[j[~hj]])
+        vals.append(np.full((~hj).sum(), -f.dcoef))
+    den = real * f.dcoef + f.decay
+    if f.lin_sink is not None:
+        den = den + f.lin_sink
+    rows.append(np.arange(free.size))
+    cols.append(np.arange(free.size))
+    vals.append(den[free])
+    a = sp.csc_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))),
+                      shape=(free.size, free.size))
+    c = spla.spsolve(a, rhs[free])
+    assert (c > 0).all(), "the floor at zero would act: not the linear problem"
+    f.values[free] = c
 
 
 class FitOracle:
     def __init__(self, grid, types, spec, reference_volume, *, dcoef=1.0, uptake=(0.01, 0.005, 0.0),
                  vessel_value=1.0, vessel_x=0, egf=0.2, signal_dcoef=1.0, signal_decay=0.01, secretion=0.05,
                  steps=200, dt=0.01, nbins=16, bin_width=3.0, hypoxic_level=0.1, tau=0.02, signal_weight=1.0,
-                 network_params=8, tolerance=1e-14):
-        self.tol = float(tolerance)
+                 network_params=8):
         self.grid = np.ascontiguousarray(grid, np.int32)
         self.d, self.h, self.w = self.grid.shape
         self.flat = self.grid.reshape(-1)
@@ -70,8 +115,7 @@ class FitOracle:
         rate = np.zeros(8)
         rate[1:4] = p[1:4]
         o2.lin_sink = O.apply_uptake(self.flat, self.types, rate)
-        rc, _ = o2.relax(self.tol, 20_000_000, stop=1)
-        assert rc == 0, "the oracle's oxygen did not settle"
+        solve_direct(o2)
         c = o2.values
         means = O.mean_per_cell(self.flat, c, self.nc)
         # the network on every record (the medium's too, as the device does)
@@ -89,8 +133,7 @@ class FitOracle:
             per_cell[1:] = self.secretion * state[1:, self.angio]
         sig = O.Field(self.w, self.h, self.d, self.sd, self.sdecay, 0.0)
         sig.production = O.apply_production(self.flat, per_cell)
-        rc, _ = sig.relax(self.tol, 20_000_000, stop=1)
-        assert rc == 0, "the oracle's signal did not settle"
+        solve_direct(sig)
         s = sig.values
         hyp = 1.0 / (1.0 + np.exp(-(self.level - c) / self.tau))
         hb = np.bincount(self.bin[self.cell], weights=hyp[self.cell], minlength=self.nbins)
@@ -108,15 +151,24 @@ class FitOracle:
 
     def gradient(self, p, rel=1e-4, floor=1e-6):
         """Central differences of the loss, parameter by parameter (h = rel |p|,
-        or `floor` for a parameter at zero)."""
+        or `floor` for a parameter at zero).  Where the two losses differ by
+        less than 1e8 units in the last place of the loss (a derivative some
+        eight orders below the loss's scale, which the loss's rounding could
+        move by 1e-4 of itself), the step grows ten times, up to 1e-2 |p|."""
         p = np.asarray(p, np.float64)
         g = np.zeros_like(p)
+        ulp = np.spacing(self.loss(p))
         for k in range(p.size):
-            step = rel * abs(p[k]) if p[k] != 0 else floor
-            q = p.copy()
-            q[k] += step
-            up = self.loss(q)
-            q[k] -= 2 * step
-            down = self.loss(q)
+            r = rel
+            while True:
+                step = r * abs(p[k]) if p[k] != 0 else floor
+                q = p.copy()
+                q[k] += step
+                up = self.loss(q)
+                q[k] -= 2 * step
+                down = self.loss(q)
+                if up == down or abs(up - down) >= 1e8 * ulp or r >= 1e-2 or p[k] == 0:
+                    break
+                r *= 10
             g[k] = (up - down) / (2 * step)
         return g

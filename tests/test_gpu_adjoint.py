@@ -8,10 +8,10 @@ profiles.  Gradients with respect to D, k (three types) and network rates:
 * on a 96 x 96 lattice, against central differences of the device's FP64
   forward (h = 1e-4 relative, every evaluation on a fresh fit) and against
   the CPU oracle's FP64 gradient (oracle/fit.py: the same loss from the
-  oracle's restatements of the reference's solve, coupling and RK4,
-  differenced with every solve at residual 1e-14), each within 1e-4 of the
-  reference value, relatively, component by component (a parameter with no
-  path to the loss has an exact zero on both sides);
+  oracle's restatements of the reference's coupling and RK4 with each field
+  solved directly to the fixed point of the reference's relax), each within
+  1e-4 of the reference value, relatively, component by component (a
+  parameter with no path to the loss has an exact zero on both sides);
 * at the differentiated fit's own shape (the 2048 x 2048 cord stepped to MCS
   500 and frozen, 2000 RK4 steps with checkpoints every 100, D, three k and
   32 network rates) against central differences of the device's forward,

@@ -550,3 +550,27 @@ def test_what_cannot_be_divided_is_left_alone():
     lat.type[1], lat.volume[1], lat.target[1], lat.lam[1] = 1, 10, 10, 1.0
     assert lat.divide_across(1, (1.0, 0.0), 2) == (-1, 2)
     np.testing.assert_array_equal(lat.grid, bar.reshape(-1))
+
+
+def test_the_fit_oracles_direct_solve_is_the_fixed_point_of_relax():
+    # the differentiated fit's CPU loss solves its fields directly; that is the
+    # field pde.rs's relax converges to (held pixels, first-order sink, decay,
+    # production and uptake, in the plane and in a volume)
+    from oracle.fit import solve_direct
+    rng = np.random.default_rng(11)
+    for w, h, d in ((40, 32, 1), (12, 10, 8)):
+        n = w * h * d
+        a = O.Field(w, h, d, 0.7, 0.01, 0.5)
+        held = (rng.random(n) < 0.05).astype(np.uint8)
+        held[:w] = 1
+        a.held[:] = held
+        a.values[held == 1] = rng.uniform(0.5, 1.5, int(held.sum()))
+        a.lin_sink = np.where(rng.random(n) < 0.6, 0.02, 0.0)
+        a.production[:] = np.where(rng.random(n) < 0.3, 0.01, 0.0)
+        a.uptake[:] = np.where(rng.random(n) < 0.2, 0.001, 0.0)
+        b = O.Field(w, h, d, 0.7, 0.01, 0.5)
+        b.held[:], b.values[:], b.lin_sink = a.held, a.values, a.lin_sink.copy()
+        b.production[:], b.uptake[:] = a.production, a.uptake
+        assert a.relax(1e-13, 1_000_000, stop=1)[0] == 0
+        solve_direct(b)
+        np.testing.assert_allclose(b.values, a.values, rtol=0, atol=1e-10)
