@@ -65,14 +65,15 @@ class TermSpec(C.Structure):
 
 class Mutation(C.Structure):
     _fields_ = [("node", C.c_int32), ("term", C.c_int32), ("kind", C.c_int32), ("change", C.c_int32),
-                ("value", C.c_double), ("source", C.c_int32), ("pad", C.c_int32)]
+                ("value", C.c_double), ("source", C.c_int32), ("suppressed", C.c_int32)]
 
 
 class Measurements(C.Structure):
     _fields_ = [("mcs", C.c_uint64), ("cycling", C.c_uint64), ("quiescent", C.c_uint64), ("necrotic", C.c_uint64),
                 ("born", C.c_uint64), ("gone", C.c_uint64), ("vessel", C.c_uint64), ("tissue_radius", C.c_double),
                 ("necrotic_radius", C.c_double), ("viable_depth", C.c_double), ("exposure", C.c_double),
-                ("differentiating", C.c_uint64), ("apoptotic", C.c_uint64), ("clones", C.c_uint64)]
+                ("differentiating", C.c_uint64), ("apoptotic", C.c_uint64), ("clones", C.c_uint64),
+                ("lesion", C.c_uint64)]
 
 
 class FitConfig(C.Structure):
@@ -105,7 +106,8 @@ class SimConfig(C.Structure):
                 ("exposure_intensity", C.c_double), ("exposure_uptake", C.c_double), ("exposure_start", C.c_int32),
                 ("exposure_on", C.c_int32), ("exposure_off", C.c_int32), ("mutation_rate", C.c_double),
                 ("rewiring", C.c_double), ("field_off", C.c_int32), ("differentiated_type", C.c_int32),
-                ("apoptotic_type", C.c_int32), ("lineage", C.c_int32), ("error_tolerance", C.c_double)]
+                ("apoptotic_type", C.c_int32), ("lineage", C.c_int32), ("error_tolerance", C.c_double),
+                ("suppress_before", C.c_int32)]
 
 
 P = C.c_void_p
@@ -188,6 +190,7 @@ SIGNATURES = {
     "cw_couple_production": (C.c_int, [P, P, U32, U32, P]),
     "cw_couple_hold_obstacles": (C.c_int, [P, P, D]),
     "cw_couple_hold_medium_bath": (C.c_int, [P, P, D]),
+    "cw_couple_hold_vessels_by": (C.c_int, [P, P, D, P]),
     "cw_couple_mean_per_cell": (C.c_int, [P, P, U32, U32, P]),
     "cw_network_compile": (C.c_int, [I32, P, P, I32, P, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p,
                                      C.c_char_p, C.c_char_p, C.c_char_p, D, D, D, U32, P]),
@@ -203,6 +206,7 @@ SIGNATURES = {
     "cw_network_rewire": (C.c_int, [P, P, P, P]),
     "cw_network_step_clones": (C.c_int, [I32, P, I64, P, P, P, D, I32]),
     "cw_sim_create": (C.c_int, [P, P, P]),
+    "cw_sim_set_lesion": (C.c_int, [P, P, C.c_uint32, D, D, D]),
     "cw_sim_destroy": (C.c_int, [P]),
     "cw_sim_step": (C.c_int, [P, U32]),
     "cw_sim_lattice": (C.c_int, [P, P]),

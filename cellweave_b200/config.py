@@ -15,9 +15,11 @@ exposure's stress, waste, necrotic factor, debris loss, a still medium and
 daughters that mutate or rewire their networks (mutation_rate, rewiring)
 when configured; a sheet of normal tissue with the field off, every cell the
 founder of its clone, cells committing to differentiate (or to apoptosis)
-at their network's node's level and leaving the layer.  Every other feature
-of the file (capillaries, suppressed clones, lesions, angiogenesis, immunity,
-tracing) is refused by name.  ``run`` steps it for ``mcs`` steps or until the tissue touches the
+at their network's node's level and leaving the layer; a lesion, whose
+cells carry a network of their own from the step it appears at; mutations
+suppressed before a step (drawn and recorded, not made).  Every other
+feature of the file (capillaries, a list of suppressed clones, angiogenesis,
+immunity, tracing) is refused by name.  ``run`` steps it for ``mcs`` steps or until the tissue touches the
 box's edge, writing measurements.csv and the snapshots as the reference
 does.
 
@@ -116,9 +118,25 @@ def _refuse(cfg):
         if cfg["depth"] > 1:
             raise ConfigError(f"{name}: a sheet, which is a layer one cell thick, runs only in the plane; "
                               "set depth = 1")
-    for key in ("lesion", "angiogenesis", "immunity", "tracing", "suppress_before"):
+    for key in ("angiogenesis", "immunity", "tracing"):
         if cfg.get(key) is not None:
             raise ConfigError(f"{name}: `{key}` is not part of the device step")
+    if cfg.get("lesion") is not None:
+        # LesionConfig (config.rs:142-160); Lesion checks (simulation.rs:751-770)
+        les = cfg["lesion"]
+        missing = [k for k in ("network", "at", "radius") if k not in les]
+        if missing:
+            raise ConfigError(f"{name}: missing field `{missing[0]}` in the lesion")
+        if cfg["depth"] > 1:
+            raise ConfigError(f"{name}: a lesion is placed in a plane; set depth = 1")
+        if les.get("centre") is not None:
+            cx, cy = (float(v) for v in les["centre"])
+            if not (0.0 <= cx < cfg["width"] and 0.0 <= cy < cfg["height"]):
+                raise ConfigError(f"{name}: a lesion centred at ({cx}, {cy}) lies outside the "
+                                  f"{cfg['width']}x{cfg['height']} box")
+        r = float(les["radius"])
+        if not (math.isfinite(r) and r > 0.0):
+            raise ConfigError(f"{name}: a lesion of radius {r} holds no cell")
     if cfg["suppress"]:
         raise ConfigError(f"{name}: `suppress` is not part of the device step (its mutations are all made)")
     if not 0.0 <= float(cfg["mutation_rate"]) <= 1.0 or not 0.0 <= float(cfg["rewiring"]) <= 1.0:
@@ -195,6 +213,8 @@ def simulation_kwargs(cfg, histories=1, seeds=None, subsweeps=4):
         kw["still_medium"] = float(cfg["still_medium"]["diffusion"])
     if cfg["mutation_rate"]:
         kw.update(mutation_rate=float(cfg["mutation_rate"]), rewiring=float(cfg["rewiring"]))
+    if cfg.get("suppress_before") is not None:
+        kw["suppress_before"] = int(cfg["suppress_before"])
     if cfg.get("waste"):
         kw["waste_production"] = float(cfg["waste"]["production"])
     if cfg.get("necrotic_factor"):
@@ -231,7 +251,15 @@ def simulation_from_config(cfg, histories=1, seeds=None, subsweeps=4):
     kw, refvol = simulation_kwargs(cfg, histories, seeds, subsweeps)
     net = Network.from_spec(load_network_spec(cfg["network_path"]), refvol)
     kw["lambda_volume"] = _network_lambda(cfg)
-    return Simulation(net, **kw), net
+    sim = Simulation(net, **kw)
+    if cfg.get("lesion") is not None:
+        # the lesion's network, beside the configuration like its own, compiled
+        # for a newborn cell's volume (simulation.rs:751-770)
+        les = cfg["lesion"]
+        path = os.path.join(os.path.dirname(cfg["path"]), les["network"])
+        lesion_net = Network.from_spec(load_network_spec(path), refvol)
+        sim.set_lesion(lesion_net, int(les["at"]), float(les["radius"]), les.get("centre"))
+    return sim, net
 
 
 def _network_lambda(cfg):

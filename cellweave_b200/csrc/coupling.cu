@@ -76,6 +76,44 @@ __global__ void k_hold_obstacles(const int32_t *grid, int64_t n, double v, uint8
     if (i < n && grid[i] == -1) { held[i] = 1; c[i] = v; }
 }
 
+// hold_vessels_by (coupling.rs:114-150) on planes: an obstacle pixel with a
+// delivery share above zero is held at value x min(share, 1) unless the mean
+// of the field over its in-box neighbours that are not obstacles (x-1, x+1,
+// y-1, y+1, summed in that order) already reaches that level.  Only obstacle
+// pixels are written and only the others read, so one pass decides on the
+// field as it stood, as the reference's two passes do.
+__global__ void k_hold_vessels_by(Pair p, const int32_t *blk, int nh, double value, const double *delivery,
+                                  uint8_t *held, double *c) {
+    __shared__ int s_h;
+    if (threadIdx.x == 0) s_h = plan_history(blk, nh, blockIdx.x);
+    __syncthreads();
+    const int h = s_h;
+    const int64_t local = (int64_t)(blockIdx.x - blk[h]) * blockDim.x + threadIdx.x;
+    if (local >= p.off[h + 1] - p.off[h]) return;
+    const int64_t i = p.off[h] + local;
+    if (p.grid[i] != -1) return;
+    const double share = delivery[i];
+    if (share <= 0.0) return;
+    const double level = value * fmin(share, 1.0);
+    const int4 dm = p.dims[h];
+    const int x = (int)(local % dm.x), y = (int)(local / dm.x);
+    const int nx[4] = {x - 1, x + 1, x, x};
+    const int ny[4] = {y, y, y - 1, y + 1};
+    double sum = 0.0;
+    int n = 0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        if (nx[q] < 0 || nx[q] >= dm.x || ny[q] < 0 || ny[q] >= dm.y) continue;
+        const int64_t j = p.off[h] + (int64_t)ny[q] * dm.x + nx[q];
+        if (p.grid[j] == -1) continue;
+        sum += c[j];
+        n += 1;
+    }
+    if (n > 0 && sum / (double)n >= level) return;  // richer around it: left free
+    held[i] = 1;
+    c[i] = level;
+}
+
 __global__ void k_open_medium(const int32_t *grid, int64_t n, uint8_t *open) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) open[i] = grid[i] == 0;
@@ -256,6 +294,31 @@ int cw_couple_hold_obstacles(cw_field f, cw_lattice l, double value) {
     k_hold_obstacles<<<(unsigned)((n + T - 1) / T), T, 0, stream()>>>(l->grid, n, value, f->held, f->c);
     CW_LAUNCHED();
     CW_CUDA(cudaStreamSynchronize(stream()));
+    return CW_OK;
+}
+
+int cw_couple_hold_vessels_by(cw_field f, cw_lattice l, double value, const double *delivery) {
+    CW_SCOPE(f);
+    CW_JOIN(l);
+    int rc = check_pair(f, l);
+    if (rc != CW_OK) return rc;
+    if (!delivery) return fail(CW_ERR_CONFIG, "hold_vessels_by needs a delivery share for every pixel");
+    for (uint32_t k = 0; k < f->g.nh; ++k)
+        if (f->g.d[k] > 1)
+            return fail(CW_ERR_CONFIG, "hold_vessels_by holds the vessels of a plane; history " + std::to_string(k) +
+                                           " is a volume");
+    const int64_t n = f->g.total;
+    double *d_share;
+    if ((rc = dalloc(&d_share, n)) != CW_OK) return rc;
+    CW_CUDA(cudaMemcpyAsync(d_share, delivery, sizeof(double) * n, cudaMemcpyHostToDevice, stream()));
+    Plan p;
+    if ((rc = site_plan(f->g, p)) != CW_OK) return rc;
+    f->held_dirty = true;
+    k_hold_vessels_by<<<p.nblocks, T, 0, stream()>>>(pair_of(l), p.d_blk, l->g.nh, value, d_share, f->held, f->c);
+    CW_LAUNCHED();
+    CW_CUDA(cudaStreamSynchronize(stream()));
+    dfree(d_share);
+    p.release();
     return CW_OK;
 }
 

@@ -62,9 +62,17 @@ struct cw_sim_s {
     // a lineage's founders all share it)
     bool track = false;
     bool evolve = false;
+    bool clone_nets = false;        // every cell steps under its clone's network (mutation or a lesion)
     std::vector<cw_network_s *> clones;
+    std::vector<uint8_t> clone_owned;   // the simulation made it (a mutation), and destroys it
+    std::vector<uint8_t> clone_lesion;  // a lesion's clone, or descended from one
     std::vector<int32_t> clone_parent;
     std::vector<cw_mutation> clone_mutation;
+    // a lesion (Lesion, simulation.rs:348-360): its network (the caller's), the
+    // step it appears at (-1: none), its radius and centre (NaN: the box's)
+    cw_network_s *lesion_net = nullptr;
+    int64_t lesion_at = -1;
+    double lesion_radius = 0.0, lesion_cx = 0.0, lesion_cy = 0.0;
     std::vector<int32_t> h_clone;
     int32_t *d_clone = nullptr;
     cw::NetDev *d_nets = nullptr;
@@ -812,6 +820,9 @@ int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out) {
                     s->h_clone[g] = (int32_t)g;
                 }
         s->clones.assign(c.lineage ? (size_t)nc : 1, net);
+        s->clone_owned.assign(s->clones.size(), 0);
+        s->clone_lesion.assign(s->clones.size(), 0);
+        s->clone_nets = s->evolve;
         if ((rc = dalloc(&s->d_clone, nc)) != CW_OK || (rc = upload_clones(s, true)) != CW_OK) {
             cw_sim_destroy(s);
             return rc;
@@ -854,6 +865,54 @@ int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out) {
     return CW_OK;
 }
 
+int cw_sim_set_lesion(cw_sim s, cw_network net, uint32_t at, double radius, double cx, double cy) {
+    CW_SCOPE(s);
+    const cw_sim_config &c = s->cfg;
+    if (!net) return fail(CW_ERR_CONFIG, "a lesion needs a network");
+    for (uint32_t k = 0; k < c.nh; ++k) {
+        if (s->d[k] > 1)
+            return fail(CW_ERR_CONFIG, "a lesion is placed in a plane; history " + std::to_string(k) + " is a volume");
+        // simulation.rs:751-770
+        if ((!std::isnan(cx) || !std::isnan(cy)) &&
+            !(cx >= 0.0 && cx < (double)s->w[k] && cy >= 0.0 && cy < (double)s->h[k]))
+            return fail(CW_ERR_CONFIG, "a lesion centred at (" + std::to_string(cx) + ", " + std::to_string(cy) +
+                                           ") lies outside the " + std::to_string(s->w[k]) + "x" +
+                                           std::to_string(s->h[k]) + " box");
+    }
+    if (std::isnan(cx) != std::isnan(cy)) return fail(CW_ERR_CONFIG, "a lesion's centre names both coordinates");
+    if (!(std::isfinite(radius) && radius > 0.0))
+        return fail(CW_ERR_CONFIG, "a lesion of radius " + std::to_string(radius) + " holds no cell");
+    // every cell steps under its clone's network with the tissue's roles and
+    // mechanics: the lesion's network must share them
+    const cw_network_s *a = s->net, *b = net;
+    bool same = a->S == b->S && a->growth_coefficient == b->growth_coefficient &&
+                a->lambda_volume == b->lambda_volume && a->reference_volume == b->reference_volume &&
+                (a->max_target == b->max_target || (std::isnan(a->max_target) && std::isnan(b->max_target)));
+    for (int r = 0; r < 7; ++r) same = same && a->roles[r] == b->roles[r];
+    if (!same)
+        return fail(CW_ERR_CONFIG, "the device steps a lesion whose network has the tissue's nodes, roles, "
+                                   "mechanics and reference volume");
+    if (s->steps > at) return fail(CW_ERR_CONFIG, "the lesion's step " + std::to_string(at) + " has passed");
+    if (!s->track) {
+        // from now on every record's clone is followed (all in the founding one)
+        s->track = true;
+        s->h_clone.assign(s->nc, 0);
+        s->clones.assign(1, s->net);
+        s->clone_owned.assign(1, 0);
+        s->clone_lesion.assign(1, 0);
+        int rc = dalloc(&s->d_clone, s->nc);
+        if (rc != CW_OK) return rc;
+    }
+    s->clone_nets = true;
+    s->lesion_net = net;
+    s->lesion_at = (int64_t)at;
+    s->lesion_radius = radius;
+    s->lesion_cx = cx;
+    s->lesion_cy = cy;
+    drop_graphs(s);
+    return upload_clones(s, true);
+}
+
 int cw_sim_destroy(cw_sim s) {
     if (!s) return CW_OK;
     CW_SCOPE(s);
@@ -869,9 +928,10 @@ int cw_sim_destroy(cw_sim s) {
     dfree(s->d_step); dfree(s->bath); dfree(s->d_uptake);
     dfree(s->d_sink); dfree(s->cell_o2); dfree(s->cell_sig); dfree(s->sum); dfree(s->secretion); dfree(s->count);
     dfree(s->state); dfree(s->inputs); dfree(s->alive); dfree(s->target32);
-    // the clones mutation founded; a lineage's founders share the caller's network
-    for (size_t k = 1; k < s->clones.size(); ++k)
-        if (s->clones[k] != s->net) cw_network_destroy(s->clones[k]);
+    // the networks mutations made; the founders, a lesion's clone and the
+    // clones of suppressed mutations share networks the simulation does not own
+    for (size_t k = 0; k < s->clones.size(); ++k)
+        if (k < s->clone_owned.size() && s->clone_owned[k]) cw_network_destroy(s->clones[k]);
     dfree(s->d_clone); dfree(s->d_nets);
     s->sites.release();
     s->hs.release();
@@ -1037,7 +1097,18 @@ static int evolve_after_division(cw_sim_s *s) {
             }
             if (rc == CW_ERR_NOT_FOUND) continue;  // nothing to change: the daughter stays in its parent's clone
             if (rc != CW_OK) return rc;
+            // a mutation founded before suppress_before is drawn and recorded,
+            // but made on a copy that is thrown away: the daughter founds its
+            // clone with its parent's network unchanged (simulation.rs:1671-1694)
+            const bool suppressed = c.suppress_before > 0 && (int64_t)step < (int64_t)c.suppress_before;
+            if (suppressed) {
+                cw_network_destroy(nn);
+                nn = s->clones[parent_clone];
+                rec.suppressed = 1;
+            }
             s->clones.push_back(nn);
+            s->clone_owned.push_back(suppressed ? 0 : 1);
+            s->clone_lesion.push_back(s->clone_lesion[parent_clone]);
             s->clone_parent.push_back(parent_clone);
             s->clone_mutation.push_back(rec);
             s->h_clone[c0 + d] = (int32_t)(s->clones.size() - 1);
@@ -1045,6 +1116,71 @@ static int evolve_after_division(cw_sim_s *s) {
         }
     }
     return moved ? upload_clones(s, grown) : CW_OK;
+}
+
+// place_lesion (simulation.rs:1920-1970), before anything else in the step
+// it appears at: in every history, each living cell (not necrotic, not
+// leaving the layer, holding pixels) whose centre of mass lies within the
+// lesion's radius of its centre joins one new clone carrying the lesion's
+// network, fresh (its state the network's initial one).  Centres are the
+// reference's: x + 1/2 and y + 1/2 summed in row order per cell, over the
+// count.  A history with no such cell founds no clone.  Draws nothing.
+static int place_lesion(cw_sim_s *s) {
+    cw_lattice_s *l = s->lat;
+    const cw_sim_config &c = s->cfg;
+    const int64_t nc = s->nc, total = l->g.total;
+    const int S = network_nodes(s->net);
+    std::vector<int32_t> grid(total), ty(nc), vo(nc);
+    std::vector<double> state((size_t)S * nc);
+    CW_CUDA(cudaMemcpyAsync(grid.data(), l->grid, sizeof(int32_t) * total, cudaMemcpyDeviceToHost, stream()));
+    CW_CUDA(cudaMemcpyAsync(ty.data(), l->type, sizeof(int32_t) * nc, cudaMemcpyDeviceToHost, stream()));
+    CW_CUDA(cudaMemcpyAsync(vo.data(), l->volume, sizeof(int32_t) * nc, cudaMemcpyDeviceToHost, stream()));
+    CW_CUDA(cudaMemcpyAsync(state.data(), s->state, sizeof(double) * state.size(), cudaMemcpyDeviceToHost, stream()));
+    CW_CUDA(cudaStreamSynchronize(stream()));
+    const std::vector<double> &fresh = network_initial(s->lesion_net);
+    bool joined = false;
+    for (uint32_t h = 0; h < c.nh; ++h) {
+        const int64_t c0 = l->cell_off[h], cap = l->cell_off[h + 1] - c0;
+        const int32_t W = s->w[h], H = s->h[h];
+        const double cx = std::isnan(s->lesion_cx) ? (double)W / 2.0 : s->lesion_cx;
+        const double cy = std::isnan(s->lesion_cy) ? (double)H / 2.0 : s->lesion_cy;
+        std::vector<double> sx(cap, 0.0), sy(cap, 0.0);
+        std::vector<uint32_t> n(cap, 0u);
+        const int32_t *g = grid.data() + l->g.off[h];
+        for (int32_t y = 0; y < H; ++y)
+            for (int32_t x = 0; x < W; ++x) {
+                const int32_t id = g[(int64_t)y * W + x];
+                if (id < 0 || id >= cap) continue;
+                sx[id] += (double)x + 0.5;
+                sy[id] += (double)y + 0.5;
+                n[id] += 1u;
+            }
+        std::vector<int64_t> joining;
+        for (int64_t id = 1; id < cap; ++id) {
+            const int64_t gi = c0 + id;
+            const bool alive = vo[gi] > 0 && !((s->leaving >> (ty[gi] & 31)) & 1u);
+            if (alive && n[id] > 0 &&
+                std::hypot(sx[id] / (double)n[id] - cx, sy[id] / (double)n[id] - cy) <= s->lesion_radius)
+                joining.push_back(gi);
+        }
+        if (joining.empty()) continue;
+        const int32_t founded = (int32_t)s->clones.size();
+        s->clones.push_back(s->lesion_net);
+        s->clone_owned.push_back(0);
+        s->clone_lesion.push_back(1);
+        s->clone_parent.push_back(-1);
+        cw_mutation none{};
+        none.node = none.term = none.kind = none.change = none.source = -1;
+        s->clone_mutation.push_back(none);
+        for (int64_t gi : joining) {
+            s->h_clone[gi] = founded;
+            for (int k = 0; k < S; ++k) state[(size_t)k * nc + gi] = fresh[k];
+        }
+        joined = true;
+    }
+    if (!joined) return CW_OK;
+    CW_CUDA(cudaMemcpyAsync(s->state, state.data(), sizeof(double) * state.size(), cudaMemcpyHostToDevice, stream()));
+    return upload_clones(s, true);
 }
 
 // The division step (simulation.rs:1338-1347): every step, the ready cells
@@ -1158,7 +1294,7 @@ static Leaving leaving_of(const cw_sim_s *s) {
 static int step_networks(cw_sim_s *s) {
     const cw_sim_config &c = s->cfg;
     const int64_t nc = s->nc;
-    if (s->evolve)
+    if (s->clone_nets)
         return network_step_clones_device(s->d_nets, s->d_clone, network_nodes(s->net), s->state, s->inputs, nc, nc,
                                           nc, c.dt, c.substeps, s->alive);
     return network_step_device(s->net, s->state, s->inputs, nc, nc, nc, c.dt, c.substeps, s->alive);
@@ -1309,6 +1445,7 @@ int cw_sim_step(cw_sim s, uint32_t nsteps) {
     o.inner_sweeps = c.inner_sweeps > 0 ? c.inner_sweeps : 32;
     int rc;
     for (uint32_t step = 0; step < nsteps; ++step, ++s->steps) {
+        if (s->lesion_net && (int64_t)s->steps == s->lesion_at && (rc = place_lesion(s)) != CW_OK) return rc;
         bool solve = c.relax_every <= 1 || (s->steps % (uint32_t)c.relax_every) == 0;
         o.block_depth = s->depth;
         o.window = s->sor_window;
@@ -1629,13 +1766,20 @@ int cw_sim_measure(cw_sim s, cw_measurements *out) {
         m.apoptotic = v[9];
         if (s->track) {
             std::vector<int32_t> seen;
+            uint64_t lesion = 0;
             const int64_t c0 = l->cell_off[k], c1 = l->cell_off[k + 1];
             for (int64_t g = c0 + 1; g < c1; ++g)
-                if (vo[g] > 0 && !((s->leaving >> (ty[g] & 31)) & 1u)) seen.push_back(s->h_clone[g]);
+                if (vo[g] > 0 && !((s->leaving >> (ty[g] & 31)) & 1u)) {
+                    seen.push_back(s->h_clone[g]);
+                    lesion += s->clone_lesion[s->h_clone[g]];
+                }
             std::sort(seen.begin(), seen.end());
             m.clones = (uint64_t)(std::unique(seen.begin(), seen.end()) - seen.begin());
+            // living cells descended from a lesion (lesion_cells, evolution.rs:182-197)
+            m.lesion = lesion;
         } else {
             m.clones = v[0] + v[1] > 0 ? 1 : 0;
+            m.lesion = 0;
         }
         // the held column of o2_hold 1, the vessel of 4: the lattice's only obstacles
         m.vessel = (c.o2_hold == 1 || c.o2_hold == 4) ? s->obstacles[k] : 0;

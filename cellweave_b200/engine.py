@@ -406,6 +406,16 @@ def hold_obstacles_at(field, lattice, value):
     call("cw_couple_hold_obstacles", field.handle, lattice.handle, float(value))
 
 
+def hold_vessels_by(field, lattice, value, delivery):
+    """hold_vessels_by (coupling.rs:114-150): `delivery` is each pixel's share
+    of a full vessel's supply, one value per pixel of the batch (flat, the
+    batch's order), as the reference's `delivery(x, y)` closure gives it."""
+    share = np.ascontiguousarray(delivery, np.float64).reshape(-1)
+    if share.size != int(sum(int(w) * int(h) * int(d) for w, h, d in field.dims)):
+        raise ValueError("hold_vessels_by needs one delivery share per pixel of the batch")
+    call("cw_couple_hold_vessels_by", field.handle, lattice.handle, float(value), ptr(share))
+
+
 def hold_medium_bath(field, lattice, value):
     """hold_medium_bath (coupling.rs:156-158)."""
     call("cw_couple_hold_medium_bath", field.handle, lattice.handle, float(value))
@@ -629,7 +639,7 @@ class Simulation:
                  cycle_median=0.0, cycle_spread=0.0, debris_loss=0.0, still_medium=0.0, exposure_intensity=0.0,
                  exposure_uptake=0.0, exposure_start=0, exposure_on=0, exposure_off=0, mutation_rate=0.0,
                  rewiring=0.0, field_off=False, differentiated_type=-1, apoptotic_type=-1, lineage=False,
-                 error_tolerance=0.0):
+                 error_tolerance=0.0, suppress_before=0):
         self.dims, w, h, z = _dims(dims)
         self._keep = [w, h, z]
         nc = np.array(ncells, np.uint32)
@@ -652,7 +662,7 @@ class Simulation:
                              float(cycle_spread), float(debris_loss), float(still_medium), float(exposure_intensity),
                              float(exposure_uptake), int(exposure_start), int(exposure_on), int(exposure_off),
                              float(mutation_rate), float(rewiring), int(bool(field_off)), int(differentiated_type),
-                             int(apoptotic_type), int(bool(lineage)), float(error_tolerance))
+                             int(apoptotic_type), int(bool(lineage)), float(error_tolerance), int(suppress_before))
         handle = C.c_void_p()
         call("cw_sim_create", C.byref(cfg), network.handle, C.byref(handle))
         self._h = handle
@@ -666,6 +676,14 @@ class Simulation:
 
     def step(self, n=1):
         call("cw_sim_step", self._h, int(n))
+
+    def set_lesion(self, network: "Network", at, radius, centre=None):
+        """A lesion (Lesion, simulation.rs:348-360): at the start of step `at`
+        every living cell whose centre lies within `radius` of `centre` (the
+        box's centre when None) joins one new clone carrying `network`, fresh."""
+        cx, cy = (float("nan"), float("nan")) if centre is None else (float(centre[0]), float(centre[1]))
+        call("cw_sim_set_lesion", self._h, network.handle, int(at), float(radius), cx, cy)
+        self._lesion_network = network  # the simulation reads it until it is destroyed
 
     def tuning(self):
         """What the autotuner chose: factors per history (oxygen, signal), blocking depth and window, still tuning."""
@@ -744,14 +762,25 @@ class Simulation:
         return out
 
     def clone_records(self):
-        """Every clone a mutation founded so far, in order: (parent clone, mutation record)."""
+        """Every clone founded during the run so far, in order: (parent clone,
+        mutation record); a lesion's clone is (-1, {"lesion": True}), a
+        suppressed mutation's record carries "suppressed": True."""
         n = C.c_uint32()
         call("cw_sim_clone_records", self._h, C.byref(n), None, None)
         k = n.value
         parent = np.zeros(max(k, 1), np.int32)
         recs = (_lib.Mutation * max(k, 1))()
         call("cw_sim_clone_records", self._h, C.byref(n), ptr(parent), recs)
-        return [(int(parent[i]), self.network._record(recs[i])) for i in range(k)]
+        out = []
+        for i in range(k):
+            if recs[i].change < 0:
+                out.append((int(parent[i]), {"lesion": True}))
+                continue
+            rec = self.network._record(recs[i])
+            if recs[i].suppressed:
+                rec["suppressed"] = True
+            out.append((int(parent[i]), rec))
+        return out
 
     def cycle(self, n, hist=0):
         """(began, due) of records 0..n-1 of a history: each cell's cycle."""

@@ -3,11 +3,12 @@
 
 One row per step, the columns of MEASUREMENT_COLUMNS in that order, counts as
 integers and the exposure and the three radii to four decimals, so that two
-runs of one seed write the same bytes.  The device step has no lesion,
+runs of one seed write the same bytes.  The device step has no
 angiogenesis or immune cells: those columns are written as the reference
 writes them without those features (0); the clones column counts the clones
-with a living cell (the founder's alone without mutation or a lineage), and
-a held column of oxygen is the vessel, all of it perfused.
+with a living cell (the founder's alone without mutation, a lineage or a
+lesion), the lesion column the living cells descended from a lesion, and a
+held column of oxygen is the vessel, all of it perfused.
 """
 from __future__ import annotations
 

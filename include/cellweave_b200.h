@@ -327,6 +327,12 @@ int cw_couple_production(cw_field f, cw_lattice lat, uint32_t hist, uint32_t n, 
 /* hold_obstacles_at (coupling.rs:80-82) and hold_medium_bath (coupling.rs:156-158). */
 int cw_couple_hold_obstacles(cw_field f, cw_lattice lat, double value);
 int cw_couple_hold_medium_bath(cw_field f, cw_lattice lat, double value);
+/* hold_vessels_by (coupling.rs:114-150) on planes: every obstacle pixel whose
+ * delivery share (host array, one double per pixel of the batch, flat in the
+ * batch's order) is above zero is held at value x min(share, 1), unless the
+ * field's mean over its in-box neighbours that are not obstacles is already
+ * at least that; it is left as it is otherwise.  CW_ERR_CONFIG for a volume. */
+int cw_couple_hold_vessels_by(cw_field f, cw_lattice lat, double value, const double *delivery);
 /* mean_per_cell (coupling.rs:164-182) for ids [0, n) of history `hist`. */
 int cw_couple_mean_per_cell(cw_field f, cw_lattice lat, uint32_t hist, uint32_t n, double *out);
 
@@ -388,7 +394,7 @@ typedef struct {
     int32_t change;  /* CW_CHANGE_* */
     double value;    /* the factor of a scaled rate, or the rate of a gained link */
     int32_t source;  /* a gained link's source: a node index, or -1 - input (oxygen, egf, crowding, stress) */
-    int32_t pad;
+    int32_t suppressed; /* a simulation's mutation drawn and recorded but not made (suppress_before) */
 } cw_mutation;
 /* Network::mutate (network.rs:479-501): one rate, picked by `which` among
  * every node's terms in file order, scaled by 2^(2 how - 1); `which` and `how`
@@ -517,8 +523,24 @@ typedef struct {
     int32_t lineage;             /* every seeded cell founds a clone of its own (a lineage-tracing sheet,
                                     simulation.rs:780-785): cw_sim_clones and the measurements count them */
     double error_tolerance;      /* the FP32 solves' error_tolerance (cw_relax_opts); 0: the residual alone */
+    int32_t suppress_before;     /* > 0: every mutation founded before this step is drawn and recorded (its
+                                    clone founded, cw_mutation.suppressed set) but not made: the daughter keeps
+                                    its parent's network (Scenario::suppress_before, simulation.rs:240-244,
+                                    1671-1694); <= 0: none */
 } cw_sim_config;
 int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out);
+/* A lesion (Lesion, simulation.rs:348-360; place_lesion 1920-1970): at the
+ * start of step `at`, before anything else in it, every living cell of each
+ * history whose centre of mass lies within `radius` pixels of (cx, cy) (both
+ * NaN: the centre of the box) joins one new clone carrying `net`, its state
+ * the network's initial one; the clone is recorded with parent -1 and a
+ * mutation whose change is -1, and measurements count the lesion's living
+ * descendants.  Planes only.  `net` stays the caller's and must outlive the
+ * simulation; it has the simulation network's nodes, roles, mechanics and
+ * reference volume (every cell steps under its clone's network, with the
+ * tissue's roles).  CW_ERR_CONFIG for a centre outside the box, a radius not
+ * finite and above zero, a volume, another network frame, or a step past. */
+int cw_sim_set_lesion(cw_sim sim, cw_network net, uint32_t at, double radius, double cx, double cy);
 int cw_sim_destroy(cw_sim sim);
 /* `steps` lattice steps on every history. */
 int cw_sim_step(cw_sim sim, uint32_t steps);
@@ -526,9 +548,10 @@ int cw_sim_step(cw_sim sim, uint32_t steps);
  * simulation.rs:780-785, 1686-1694): the clone of records 0..n-1 of history
  * `hist` (0: the founding clone; with a lineage a seeded cell's clone is its
  * record's index in the batch); the clones in the whole batch; and the clones
- * mutations founded, in the order they were founded, which are the last
- * *count clone indices: each one's parent clone and its mutation (cw_mutation
- * as cw_network_mutate gives it; parent and mutation may be NULL). */
+ * clones founded during the run, in the order they were founded, which are
+ * the last *count clone indices: each one's parent clone and its mutation
+ * (cw_mutation as cw_network_mutate gives it; a lesion's clone has parent -1
+ * and change -1; parent and mutation may be NULL). */
 int cw_sim_clones(cw_sim sim, uint32_t hist, uint32_t n, int32_t *clone);
 int cw_sim_clone_count(cw_sim sim, uint32_t *nclones);
 int cw_sim_clone_records(cw_sim sim, uint32_t *count, int32_t *parent, cw_mutation *mutation);
@@ -571,6 +594,7 @@ typedef struct {
     double exposure;     /* the exposure's level at the step last taken (0 without one or while off) */
     uint64_t differentiating, apoptotic;  /* cells leaving the layer, cells breaking up */
     uint64_t clones;     /* clones with a living cell (with lineage or mutation; else 1 while any cell lives) */
+    uint64_t lesion;     /* living cells descended from a lesion (lesion_cells, evolution.rs:182-197) */
 } cw_measurements;
 int cw_sim_measure(cw_sim sim, cw_measurements *out);
 /* touches_the_edge (simulation.rs:2165-2198) of every history, one int32 each: a cell on a pixel of

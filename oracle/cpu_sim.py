@@ -12,6 +12,8 @@ from __future__ import annotations
 
 import tomllib
 
+import math
+
 import numpy as np
 
 from . import oracle as O
@@ -86,7 +88,34 @@ def seed_history(cfg, w, h, d, n, seed):
     return grid, np.array(types, np.int32)
 
 
-def measure_records(grid, types, volume, used, hypoxia, necrotic, o2_hold, mcs, leaving=(), clone=None):
+def lesion_joining(grid, types, volume, leaving, centre, radius):
+    """The cells a lesion takes (place_lesion, simulation.rs:1920-1962) on a
+    plane grid [h][w]: every cell holding pixels whose type is not one of
+    `leaving` (necrotic, differentiated, apoptotic) and whose centre of mass,
+    x + 1/2 and y + 1/2 summed in row order over its pixels and divided by
+    their count, lies within `radius` of `centre` (the box's centre when
+    None).  Record ids in increasing order."""
+    g = np.asarray(grid)
+    h, w = g.shape
+    cx, cy = (w / 2.0, h / 2.0) if centre is None else (float(centre[0]), float(centre[1]))
+    ncap = len(types)
+    y, x = np.mgrid[0:h, 0:w]
+    ok = (g >= 0) & (g < ncap)
+    ids = g[ok]
+    # bincount adds the weights in array order: the reference's row order
+    sx = np.bincount(ids, weights=(x[ok] + 0.5), minlength=ncap)
+    sy = np.bincount(ids, weights=(y[ok] + 0.5), minlength=ncap)
+    n = np.bincount(ids, minlength=ncap)
+    out = []
+    for cid in range(1, ncap):
+        alive = volume[cid] > 0 and int(types[cid]) not in [t for t in leaving if t >= 0]
+        if alive and n[cid] > 0 and math.hypot(sx[cid] / n[cid] - cx, sy[cid] / n[cid] - cy) <= radius:
+            out.append(cid)
+    return out
+
+
+def measure_records(grid, types, volume, used, hypoxia, necrotic, o2_hold, mcs, leaving=(), clone=None,
+                    clone_lesion=None):
     """measure.rs:133-236 on a lattice's records: counts of cycling (hypoxia
     response under 0.45), quiescent and necrotic cells with pixels, born (every
     record assigned), gone (dead and resorbed to nothing), equivalent radii (a
@@ -111,6 +140,11 @@ def measure_records(grid, types, volume, used, hypoxia, necrotic, o2_hold, mcs, 
         m["clones"] = int(np.unique(clone[1:used][live]).size)
     else:
         m["clones"] = 1 if live.any() else 0
+    # living cells descended from a lesion (lesion_cells, evolution.rs:182-197)
+    m["lesion"] = 0
+    if clone is not None and clone_lesion is not None:
+        flags = np.asarray(clone_lesion, bool)
+        m["lesion"] = int(flags[clone[1:used][live]].sum())
     leaving_area = int(vol[has & (diff | apop)].sum())
     m["vessel"] = int((grid == -1).sum()) if o2_hold in (1, 4) else 0
     living_area, dead_area = int(vol[live].sum()), int(vol[has & dead].sum())
@@ -200,11 +234,21 @@ class CpuHistory:
         self.clone = np.zeros(self.ncap, np.int64)
         self.clone_specs = [spec]
         self.clone_nets = [self.net]
+        self.clone_lesion = [False]
+        self.suppress_before = int(cfg.get("suppress_before", 0) or 0)
+        # a lesion (simulation.rs:348-360): its network, step, radius, centre
+        self.lesion_spec = cfg.get("lesion_spec")
+        self.lesion_at = int(cfg.get("lesion_at", -1))
+        self.lesion_radius = float(cfg.get("lesion_radius", 0.0))
+        self.lesion_centre = cfg.get("lesion_centre")
         # a lineage (a sheet, simulation.rs:780-785): every seeded cell its own
         # clone; its cells step under the one network
         self.lineage = bool(cfg.get("lineage", False))
         if self.lineage:
             self.clone[:self.used] = np.arange(self.used)
+            self.clone_specs = [spec] * self.ncap
+            self.clone_nets = [self.net] * self.ncap
+            self.clone_lesion = [False] * self.ncap
         self.leaving = (int(cfg.get("differentiated_type", -1)), int(cfg.get("apoptotic_type", -1)))
         self.div_rng = np.random.default_rng(self.seed * 7 + 13)
         # a cell's cycle (simulation.rs:1055-1056): none behind the cells the tissue starts with
@@ -227,7 +271,30 @@ class CpuHistory:
                                self.lat.volume, self.used, self.state[:, self.net.hypoxia],
                                self.cfg.get("necrotic_type", -1), self.cfg.get("o2_hold", 0), max(self.steps - 1, 0),
                                leaving=self.leaving,
-                               clone=self.clone if (self.lineage or self.mutation_rate > 0) else None)
+                               clone=self.clone if self._tracked() else None, clone_lesion=self.clone_lesion)
+
+    def _tracked(self):
+        return self.lineage or self.mutation_rate > 0 or self.lesion_spec is not None
+
+    def _place_lesion(self):
+        """place_lesion (simulation.rs:1920-1970): every living cell whose
+        centre of mass (x + 1/2, y + 1/2 summed in row order over its pixels,
+        over their count) lies within the radius of the centre (the box's
+        when none is given) joins one new clone carrying the lesion's
+        network, its state that network's initial one."""
+        w, h = self.dims[0], self.dims[1]
+        leaving = (self.cfg.get("necrotic_type", -1),) + tuple(self.leaving)
+        joining = lesion_joining(self.lat.grid.reshape(h, w), self.lat.type, self.lat.volume, leaving,
+                                 self.lesion_centre, self.lesion_radius)
+        if not joining:
+            return
+        self.clone_specs.append(self.lesion_spec)
+        self.clone_nets.append(O.compile_network(self.lesion_spec, self.refvol))
+        self.clone_lesion.append(True)
+        k = len(self.clone_specs) - 1
+        for cid in joining:
+            self.clone[cid] = k
+            self.state[cid] = self.clone_nets[k].initial
 
     def _settle_released(self, field, per_cell):
         """settle_released (simulation.rs:2546-2570): production from the cells
@@ -242,6 +309,8 @@ class CpuHistory:
 
     def step(self):
         c = self.cfg
+        if self.lesion_spec is not None and self.steps == self.lesion_at:
+            self._place_lesion()  # before anything else in the step (simulation.rs:1135-1137)
         g = self.lat.grid
         t = self.lat.type
         cells = g > 0
@@ -332,16 +401,25 @@ class CpuHistory:
             if self.cell_nfc is not None:
                 ins[:, 5] = self.cell_nfc[idx]
             st = np.ascontiguousarray(self.state[idx])
-            if len(self.clone_nets) == 1:
+            if all(n is self.net for n in self.clone_nets):
                 O.network_step(self.net, st, ins, c["dt"], c["substeps"])
             else:
-                # every clone's cells under its own network
-                cl = self.clone[idx]
-                for k in np.unique(cl):
-                    sel = np.nonzero(cl == k)[0]
+                # every clone's cells under its own network, the cells of
+                # clones that share one network stepped together
+                nets, which = [], np.empty(len(idx), np.int64)
+                for j, k in enumerate(self.clone[idx]):
+                    net = self.clone_nets[int(k)]
+                    for q, n in enumerate(nets):
+                        if n is net:
+                            which[j] = q
+                            break
+                    else:
+                        nets.append(net)
+                        which[j] = len(nets) - 1
+                for q, net in enumerate(nets):
+                    sel = np.nonzero(which == q)[0]
                     part = np.ascontiguousarray(st[sel])
-                    O.network_step(self.clone_nets[int(k)], part, np.ascontiguousarray(ins[sel]), c["dt"],
-                                   c["substeps"])
+                    O.network_step(net, part, np.ascontiguousarray(ins[sel]), c["dt"], c["substeps"])
                     st[sel] = part
             self.state[idx] = st
             tg = O.network_mechanics(self.net, st)
@@ -402,8 +480,16 @@ class CpuHistory:
             new, rec = O.mutate_spec(spec, which, how)
         if rec is None:
             return
-        self.clone_specs.append(new)
-        self.clone_nets.append(O.compile_network(new, self.refvol))
+        parent = int(self.clone[d])
+        if self.steps < self.suppress_before:
+            # drawn and recorded, not made: the clone keeps its parent's network
+            # (simulation.rs:1671-1694)
+            self.clone_specs.append(spec)
+            self.clone_nets.append(self.clone_nets[parent])
+        else:
+            self.clone_specs.append(new)
+            self.clone_nets.append(O.compile_network(new, self.refvol))
+        self.clone_lesion.append(self.clone_lesion[parent])
         self.clone[d] = len(self.clone_specs) - 1
 
     def _level_at(self, mcs):

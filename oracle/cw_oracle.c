@@ -17,7 +17,8 @@
  *                                 term_rate, rk4, mechanics
  *   crates/engine/src/coupling.rs apply_uptake, apply_background_uptake,
  *                                 apply_production, hold_obstacles_at,
- *                                 hold_medium_bath, mean_per_cell
+ *                                 hold_vessels_by, hold_medium_bath,
+ *                                 mean_per_cell
  * Build with -ffp-contract=off so that no multiply-add is fused, as in Rust.
  *
  * Parity status.  RK4 is pinned by the reference's golden table
@@ -1093,6 +1094,39 @@ void or_apply_production(int64_t n, const int32_t *grid, int64_t nrates, const d
 void or_hold_obstacles(int64_t n, const int32_t *grid, double value, uint8_t *held, double *values) {
     for (int64_t i = 0; i < n; ++i)
         if (grid[i] == OR_OBSTACLE) { held[i] = 1; values[i] = value; }
+}
+
+/* hold_vessels_by, coupling.rs:114-150, on a w x h plane: every obstacle pixel
+ * whose delivery share is above zero is held at value x min(share, 1), unless
+ * the mean of the field over its in-box, non-obstacle neighbours (x-1, x+1,
+ * y-1, y+1, summed in that order) is at least that level.  Every decision
+ * reads the field as it stood before any hold (the holds are applied after,
+ * hold_pixels_by, pde.rs:504-514); only obstacle pixels are written and only
+ * other pixels are read, so deciding and holding in one loop is the same. */
+void or_hold_vessels_by(int32_t w, int32_t h, const int32_t *grid, double value, const double *delivery,
+                        uint8_t *held, double *values) {
+    for (int32_t y = 0; y < h; ++y)
+        for (int32_t x = 0; x < w; ++x) {
+            const int64_t i = (int64_t)y * w + x;
+            if (grid[i] != OR_OBSTACLE) continue;
+            const double share = delivery[i];
+            if (share <= 0.0) continue;
+            /* f64::min and fmin both give the number when one side is NaN */
+            const double level = value * fmin(share, 1.0);
+            const int32_t nx[4] = {x - 1, x + 1, x, x};
+            const int32_t ny[4] = {y, y, y - 1, y + 1};
+            double sum = 0.0;
+            int n = 0;
+            for (int q = 0; q < 4; ++q) {
+                if (nx[q] < 0 || nx[q] >= w || ny[q] < 0 || ny[q] >= h) continue;
+                const int64_t j = (int64_t)ny[q] * w + nx[q];
+                if (grid[j] == OR_OBSTACLE) continue;
+                sum += values[j];
+                n += 1;
+            }
+            const int richer = n > 0 && sum / (double)n >= level;
+            if (!richer) { held[i] = 1; values[i] = level; }
+        }
 }
 
 /* mean_per_cell, coupling.rs:164-182: sums in lattice order. */

@@ -78,6 +78,8 @@ def lib():
         L.or_apply_production.restype = None
         L.or_hold_obstacles.argtypes = [C.c_int64, P, C.c_double, P, P]
         L.or_hold_obstacles.restype = None
+        L.or_hold_vessels_by.argtypes = [C.c_int32, C.c_int32, P, C.c_double, P, P, P]
+        L.or_hold_vessels_by.restype = None
         L.or_mean_per_cell.argtypes = [C.c_int64, P, P, C.c_int32, P]
         L.or_mean_per_cell.restype = None
         _LIB = L
@@ -499,6 +501,15 @@ def apply_production(grid, per_cell):
 def hold_obstacles(grid, value, held, values):
     grid = np.ascontiguousarray(grid, np.int32).reshape(-1)
     lib().or_hold_obstacles(grid.size, _p(grid), float(value), _p(held), _p(values))
+
+
+def hold_vessels_by(grid, value, delivery, held, values):
+    """hold_vessels_by (coupling.rs:114-150) on a plane grid [h][w]; held and
+    values are updated in place (flat, the grid's order)."""
+    g = np.ascontiguousarray(grid, np.int32)
+    h, w = g.shape
+    dl = np.ascontiguousarray(delivery, np.float64).reshape(-1)
+    lib().or_hold_vessels_by(w, h, _p(g), float(value), _p(dl), _p(held), _p(values))
 
 
 def mean_per_cell(grid, values, ncells):

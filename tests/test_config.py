@@ -89,6 +89,23 @@ def test_mutation_and_rewiring_map_onto_the_step(tmp_path):
     assert "mutation_rate" not in kw
 
 
+def test_a_lesion_and_suppressed_mutations_are_read_and_checked(tmp_path):
+    # LesionConfig (config.rs:142-160) and the checks of simulation.rs:751-770
+    sheet = BASE + "oxygen_uptake = 0.0\nmutation_rate = 0.01\nsuppress_before = 40\n[seeding]\nkind = \"sheet\"\nside = 10\n"
+    cfg = C.load_sim_config(write(tmp_path, sheet + "[lesion]\nnetwork = \"net.toml\"\nat = 20\nradius = 15.0\n"))
+    kw, refvol = C.simulation_kwargs(cfg)
+    assert kw["suppress_before"] == 40 and refvol == 100 and cfg["lesion"]["at"] == 20
+    for lesion, word in [("at = 20\nradius = 15.0\n", "network"),
+                         ("network = \"net.toml\"\nat = 20\nradius = 0.0\n", "radius"),
+                         ("network = \"net.toml\"\nat = 20\nradius = 5.0\ncentre = [60.0, 10.0]\n", "outside")]:
+        cfg = C.load_sim_config(write(tmp_path, sheet + "[lesion]\n" + lesion))
+        with pytest.raises(cw.ConfigError, match=word):
+            C.simulation_kwargs(cfg)
+    vol = BASE.replace("height = 50\n", "height = 50\ndepth = 20\n") + "[lesion]\nnetwork = \"net.toml\"\nat = 2\nradius = 3.0\n"
+    with pytest.raises(cw.ConfigError, match="plane"):
+        C.simulation_kwargs(C.load_sim_config(write(tmp_path, vol)))
+
+
 def test_released_fields_map_onto_the_step(tmp_path):
     cfg = C.load_sim_config(write(tmp_path, BASE + "\n[waste]\nproduction = 0.01\n[necrotic_factor]\n"
                                                    "production = 0.05\nrelease_for = 12\n"))

@@ -19,7 +19,7 @@ import pytest
 import cellweave_b200 as cw
 from cellweave_b200 import config as C
 from cpm_ensembles import SEEDS, within_band
-from oracle.cpu_sim import CpuHistory
+from oracle.cpu_sim import CpuHistory, lesion_joining
 
 pytestmark = pytest.mark.gpu
 
@@ -155,6 +155,100 @@ def test_a_sheet_of_epithelium_turns_over_inside_the_oracle_band(tmp_path):
     assert np.mean([m["gone"] for m in dm]) > 10 and np.mean([m["clones"] for m in dm]) < 36
     # the oxygen was never solved: every cell read full oxygen
     assert np.all(sim.field_values(0, 0) == 1.0)
+    for k in range(SEEDS):
+        assert sim.records_match_grid(k)
+
+
+LESION_SHEET = ("width = 60\nheight = 60\nmcs = 240\ntemperature = 10.0\nsnapshot_interval = 100\n"
+                "output_dir = \"out\"\noxygen_uptake = 0.0\nnetwork = \"tissue.toml\"\n"
+                "mutation_rate = 0.02\nrewiring = 0.3\n{extra}"
+                "[seeding]\nkind = \"sheet\"\nside = 10\n"
+                "[lesion]\nnetwork = \"lesion.toml\"\nat = {at}\nradius = 15.0\n")
+
+
+def lesion_files(tmp_path):
+    nets = json.load(open(os.path.join(HERE, "golden", "golden.json")))["networks"]
+    network_file(tmp_path, "tissue.toml", nets["epithelium-no-pressing"])
+    network_file(tmp_path, "lesion.toml", nets["lesion"])
+    return nets["epithelium-no-pressing"], nets["lesion"]
+
+
+def test_a_lesion_takes_the_cells_whose_centres_lie_within_its_radius(tmp_path):
+    # place_lesion (simulation.rs:1920-1970) at step 12 of four sheets: the
+    # cells that join are the oracle's choice on the device's lattice just
+    # before, each history founds one clone (parent -1), and every record
+    # outside it keeps its clone
+    lesion_files(tmp_path)
+    p = tmp_path / "run.toml"
+    p.write_text(LESION_SHEET.format(extra="", at=12))
+    cfg = C.load_sim_config(str(p))
+    sim, net = C.simulation_from_config(cfg, histories=4, seeds=[31, 32, 33, 34])
+    sim.step(12)
+    lat = sim.lattice()
+    before, want, held = [], [], []
+    for k in range(4):
+        n = lat.capacity[k]
+        rec = lat.cells(n, k)
+        grid = sim.grid(k).reshape(60, 60)
+        want.append(lesion_joining(grid, rec["type"], rec["volume"], (C.NECROTIC, C.DIFFERENTIATED, C.APOPTOTIC),
+                                   None, 15.0))
+        before.append(sim.clones(n, k))
+        held.append(np.asarray(rec["volume"]) > 0)
+        assert 4 <= len(want[k]) < 36
+    nrec = len(sim.clone_records())
+    sim.step(1)
+    recs = sim.clone_records()
+    lesions = [r for r in recs[nrec:] if r[1].get("lesion")]
+    assert len(lesions) == 4 and all(parent == -1 for parent, _ in lesions)
+    founded = set()
+    for k in range(4):
+        n = lat.capacity[k]
+        after = sim.clones(n, k)
+        joined = np.zeros(n, bool)
+        joined[want[k]] = True
+        assert len(set(after[joined])) == 1 and after[joined][0] not in before[k]
+        founded.add(int(after[joined][0]))
+        # every other cell that held pixels before the step kept its clone
+        others = held[k] & ~joined
+        np.testing.assert_array_equal(after[others], before[k][others])
+    assert len(founded) == 4
+    ms = sim.measure()
+    for k in range(4):
+        assert 0 < ms[k]["lesion"] <= len(want[k]) + 4
+
+
+def test_a_lesion_in_a_mutating_sheet_grows_inside_the_oracle_band(tmp_path):
+    # epithelium-lesion.toml's scenario, scaled to a 60 x 60 sheet: mutations
+    # (suppressed before step 60), a lesion of NOTCH-slowed cells at step 40;
+    # the device's 32 histories against the oracle's: living cells, the
+    # lesion's descendants, the clones left and the cells gone
+    tissue, lesion = lesion_files(tmp_path)
+    p = tmp_path / "run.toml"
+    p.write_text(LESION_SHEET.format(extra="suppress_before = 60\n", at=40))
+    cfg = C.load_sim_config(str(p))
+    seeds = [7_000 + k for k in range(SEEDS)]
+    sim, _ = C.simulation_from_config(cfg, histories=SEEDS, seeds=seeds)
+    kw, _ = C.simulation_kwargs(cfg, SEEDS, seeds)
+    ocfg = dict(kw, network_spec=tissue, lambda_volume=float(tissue["mechanics"]["lambda_volume"]), hypoxic_level=0.1,
+                lesion_spec=lesion, lesion_at=40, lesion_radius=15.0)
+    ora = [CpuHistory(ocfg, k) for k in range(SEEDS)]
+    keys = ("cycling", "differentiating", "gone", "clones", "lesion")
+    for step in range(1, 241):
+        sim.step(1)
+        for h in ora:
+            h.step()
+        if step not in (41, 120, 240):
+            continue
+        dm = sim.measure()
+        om = [h.measure() for h in ora]
+        for q in keys:
+            dv = np.array([float(m[q]) for m in dm])
+            rv = np.array([float(m[q]) for m in om])
+            assert within_band(dv, rv), (step, q, dv.mean(), rv.mean(), rv.std())
+    dm = sim.measure()
+    assert np.mean([m["lesion"] for m in dm]) > 0
+    recs = sim.clone_records()
+    assert any(r.get("suppressed") for _, r in recs) and any(r.get("lesion") for _, r in recs)
     for k in range(SEEDS):
         assert sim.records_match_grid(k)
 

@@ -60,6 +60,61 @@ def test_uptake_production_bath_and_means_match_the_oracle():
     assert got[c] < max(got[r] for r in ring)
 
 
+def test_vessels_held_by_their_delivery_match_the_oracle():
+    """hold_vessels_by (coupling.rs:114-150) on a batch of two planes: vessel
+    discs in tissue, a field that is not uniform, shares that are zero,
+    negative, partial, above one and NaN; every hold and value equal the
+    oracle's, history by history."""
+    rng = np.random.default_rng(7)
+    grids, recs, shares, fields = [], [], [], []
+    for (w, h) in [(64, 48), (90, 90)]:
+        grid = seeding.empty(w, h)
+        rec = seeding.Records()
+        for k in range(6):
+            seeding.add_cell(grid, rec, 1 + k % 2, (int(rng.integers(8, w - 8)), int(rng.integers(8, h - 8))), 5)
+        for k in range(4):
+            seeding.add_obstacle_disc(grid, rec, (int(rng.integers(0, w)), int(rng.integers(0, h))), int(rng.integers(0, 4)))
+        share = rng.choice([0.0, -0.5, 0.25, 0.5, 0.9, 1.0, 3.0, np.nan], size=w * h)
+        grids.append(grid)
+        recs.append(rec)
+        shares.append(share)
+        fields.append(rng.uniform(0.0, 1.2, size=w * h))
+    lat = cw.CpmLattice.from_grids(grids, recs, 10.0, J5, 1)
+    f = cw.ScalarField([(64, 48, 1), (90, 90, 1)], 0.2)
+    for k in range(2):
+        f.set_values(fields[k], k)
+    cw.engine.hold_vessels_by(f, lat, 0.8, np.concatenate(shares))
+    for k in range(2):
+        held, values = np.zeros(fields[k].size, np.uint8), fields[k].copy()
+        O.hold_vessels_by(grids[k].reshape(grids[k].shape[-2:]), 0.8, shares[k], held, values)
+        assert held.any() and (held.sum() < (grids[k] == -1).sum())  # some held, some left free
+        np.testing.assert_array_equal(f.held(k), held)
+        np.testing.assert_array_equal(f.values(k).view(np.uint64), values.view(np.uint64))
+
+
+def test_vessels_held_by_their_delivery_the_reference_cases():
+    # coupling.rs:300-331 on the device
+    grid = np.zeros((1, 1, 10), np.int32)
+    grid[0, 0, :3] = -1
+    rec = seeding.Records()
+    lat = cw.CpmLattice.from_grids([grid], [rec], 10.0, J5, 1)
+    f = cw.ScalarField.new(10, 1, 0.2)
+    cw.engine.hold_vessels_by(f, lat, 2.0, [0.0, 0.5, 3.0] + [0.0] * 7)
+    assert list(f.values()[:3]) == [0.0, 1.0, 2.0] and list(f.held()[:3]) == [0, 1, 1]
+    grid = np.zeros((1, 1, 10), np.int32)
+    grid[0, 0, 5] = -1
+    lat = cw.CpmLattice.from_grids([grid], [rec], 10.0, J5, 1)
+    f = cw.ScalarField.new(10, 1, 0.2, initial=0.9)
+    cw.engine.hold_vessels_by(f, lat, 1.0, np.full(10, 0.5))
+    assert f.values()[5] == 0.9 and f.held()[5] == 0
+    cw.engine.hold_vessels_by(f, lat, 1.0, np.full(10, 1.0))
+    assert f.values()[5] == 1.0 and f.held()[5] == 1
+    v = cw.ScalarField.with_depth(10, 1, 2, 0.2)
+    lv = cw.CpmLattice.from_grids([np.zeros((2, 1, 10), np.int32)], [rec], 10.0, J5, 1)
+    with pytest.raises(cw.ConfigError):
+        cw.engine.hold_vessels_by(v, lv, 1.0, np.zeros(20))
+
+
 def small_sim(nh=3, precision=cw.FP32_DC):
     net_text = synthetic.network_toml(8, seed=8)
     import tempfile, os

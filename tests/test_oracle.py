@@ -494,6 +494,29 @@ def test_a_cell_in_the_middle_reads_less_oxygen_than_one_on_the_rim():
     assert o2[0] == 0.0 and (o2[1:] > 0).all()
 
 
+def test_a_vessel_delivers_what_its_share_says_and_a_dry_one_nothing():
+    # coupling.rs:300-315: three vessel pixels on a 10 x 1 strip, shares 0, 1/2, 3 of 2
+    grid = np.zeros((1, 10), np.int32)
+    grid[0, :3] = -1
+    held, values = np.zeros(10, np.uint8), np.zeros(10)
+    O.hold_vessels_by(grid, 2.0, [0.0, 0.5, 3.0] + [0.0] * 7, held, values)
+    assert values[0] == 0.0 and not held[0], "a dry vessel is not held"
+    assert values[1] == 1.0 and held[1], "half of 2"
+    assert values[2] == 2.0 and held[2], "never more than in full"
+    assert not held[3:].any()
+
+
+def test_a_vessel_poorer_than_the_tissue_around_it_takes_nothing_from_it():
+    # coupling.rs:317-331
+    grid = np.zeros((1, 10), np.int32)
+    grid[0, 5] = -1
+    held, values = np.zeros(10, np.uint8), np.full(10, 0.9)
+    O.hold_vessels_by(grid, 1.0, np.full(10, 0.5), held, values)
+    assert values[5] == 0.9 and not held[5], "left free, not held down to half"
+    O.hold_vessels_by(grid, 1.0, np.full(10, 1.0), held, values)
+    assert values[5] == 1.0 and held[5], "held where it is richer"
+
+
 def test_moore_copies_need_period_two_with_face_contact():
     # with copies from diagonal neighbours a chessboard colour would hold a
     # copy's source: face contact then takes period 2 (4 colours, 8 in a volume)
