@@ -248,9 +248,36 @@ def test_a_lesion_in_a_mutating_sheet_grows_inside_the_oracle_band(tmp_path):
     dm = sim.measure()
     assert np.mean([m["lesion"] for m in dm]) > 0
     recs = sim.clone_records()
-    assert any(r.get("suppressed") for _, r in recs) and any(r.get("lesion") for _, r in recs)
+    assert sum(1 for _, r in recs if r.get("lesion")) == SEEDS
     for k in range(SEEDS):
         assert sim.records_match_grid(k)
+
+
+def test_suppressed_mutations_leave_the_run_as_it_was(tmp_path):
+    # Scenario::suppress_before (simulation.rs:240-244, 1671-1694): mutations
+    # drawn and recorded but not made; the draws take nothing from the step's
+    # other draws, so a sheet whose every mutation is suppressed runs as the
+    # sheet without mutation, lattice and protein levels to the bit, while its
+    # daughters still found (suppressed) clones
+    lesion_files(tmp_path)
+    runs = {}
+    for name, extra in [("plain", "mutation_rate = 0.0\n"), ("suppressed", "suppress_before = 100000\n")]:
+        p = tmp_path / f"{name}.toml"
+        p.write_text(LESION_SHEET.format(extra="", at=0).split("[lesion]")[0]
+                     .replace("mutation_rate = 0.02\n", "mutation_rate = 0.5\n" if name == "suppressed" else extra)
+                     .replace("rewiring = 0.3\n", "rewiring = 0.3\n" + (extra if name == "suppressed" else "")))
+        cfg = C.load_sim_config(str(p))
+        sim, _ = C.simulation_from_config(cfg, histories=4, seeds=[51, 52, 53, 54])
+        sim.step(150)
+        runs[name] = sim
+    a, b = runs["plain"], runs["suppressed"]
+    recs = b.clone_records()
+    assert len(recs) >= 8 and all(r.get("suppressed") for _, r in recs)
+    assert a.clone_records() == []
+    for k in range(4):
+        np.testing.assert_array_equal(a.grid(k), b.grid(k))
+        n = a.lattice().capacity[k]
+        np.testing.assert_array_equal(a.network_state(n, k).view(np.uint64), b.network_state(n, k).view(np.uint64))
 
 
 def test_the_run_writes_the_measurements_of_every_step_and_the_snapshots(tmp_path):
