@@ -163,20 +163,24 @@ __device__ __forceinline__ int next_live(int t, int ntiles, int step, const int4
     return t;
 }
 
-// One half-sweep of colour C over a lane's 8 rows x 4 columns.  Column c of
-// row j has colour (c + j) mod 2 (windows start at even x and y): colour C
-// takes columns 0 and 2 of the rows with C + j even, 1 and 3 of the others.
-template <int C>
-__device__ __forceinline__ void half4(float4 (&d)[WROWS], const float4 (&a)[WROWS], const float4 (&b)[WROWS],
+// One half-sweep of colour C over rows J0..J1-1 of a lane's 8 rows x 4
+// columns.  Column c of row j has colour (c + j) mod 2 (windows start at even
+// x and y): colour C takes columns 0 and 2 of the rows with C + j even, 1 and
+// 3 of the others.  Every update reads only pixels of the other colour, which
+// this half-sweep does not change, so rows may be taken in any order: the
+// rows inside the warp's band first (J0 = 1, J1 = WROWS - 1), then the two
+// that read the neighbouring warps' edges once those have arrived.
+template <int C, int J0, int J1>
+__device__ __forceinline__ void rows4(float4 (&d)[WROWS], const float4 (&a)[WROWS], const float4 (&b)[WROWS],
                                       const float4 ab, const float4 be, float lm, float rm, float omc) {
     // the across-lane neighbours first: they are of the other colour, which
     // this half-sweep does not change, and their latency then overlaps
     float nb[WROWS];
 #pragma unroll
-    for (int j = 0; j < WROWS; ++j)
+    for (int j = J0; j < J1; ++j)
         nb[j] = ((C + j) & 1) == 0 ? __shfl_up_sync(0xffffffffu, d[j].w, 1) : __shfl_down_sync(0xffffffffu, d[j].x, 1);
 #pragma unroll
-    for (int j = 0; j < WROWS; ++j) {
+    for (int j = J0; j < J1; ++j) {
         const float4 up = j > 0 ? d[j - 1] : ab, dn = j < WROWS - 1 ? d[j + 1] : be;
         if (((C + j) & 1) == 0) {
             const float left = nb[j];
@@ -192,6 +196,20 @@ __device__ __forceinline__ void half4(float4 (&d)[WROWS], const float4 (&a)[WROW
             d[j].w = fmaf(a[j].w, s3, fmaf(omc, d[j].w, b[j].w));
         }
     }
+}
+
+// Named barriers 1 and 2 (0 is __syncthreads'), alternating by half-sweep:
+// a warp arrives once it has published its edge rows and waits only when it
+// needs the others' (PTX bar.arrive / bar.sync over the block's threads; both
+// order the shared-memory accesses before them for the threads that meet).
+// (immediate ids, so that the compiler reserves three barriers, not all 16).
+__device__ __forceinline__ void edge_arrive(int id, int nthreads) {
+    if (id == 1) asm volatile("bar.arrive 1, %0;" ::"r"(nthreads) : "memory");
+    else asm volatile("bar.arrive 2, %0;" ::"r"(nthreads) : "memory");
+}
+__device__ __forceinline__ void edge_wait(int id, int nthreads) {
+    if (id == 1) asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory");
+    else asm volatile("bar.sync 2, %0;" ::"r"(nthreads) : "memory");
 }
 
 // What a block needs of a window, staged in shared memory by thread 0 one
@@ -290,22 +308,36 @@ __global__ void __launch_bounds__(32 * WWARPS, WWARPS == 8 ? 2 : 1)
             stage_next(info.tl.w + gridDim.x, slot ^ 1);
         }
         const float omc = info.omc;
+        // half-sweep s reads the edges published after half-sweep s - 1 in
+        // buffer s & 1, behind named barrier 1 + (s & 1): a warp sweeps its
+        // band's inner rows while the others' edges arrive, then its two edge
+        // rows.  Buffer (s + 1) & 1 is written only after barrier 1 + (s & 1)
+        // has completed, that is after every warp read it in half-sweep s - 1.
+        constexpr int NT = 32 * WWARPS;
         ed(0, warp, 0) = d[0];
         ed(0, warp, 1) = d[WROWS - 1];
-        __syncthreads();
+        edge_arrive(1, NT);
         for (int s = 0; s < nhalf; ++s) {
             const int buf = s & 1;
+            const bool c0 = ((start_colour + s) & 1) == 0;
+            if (c0)
+                rows4<0, 1, WROWS - 1>(d, a, b, z4, z4, lm, rm, omc);
+            else
+                rows4<1, 1, WROWS - 1>(d, a, b, z4, z4, lm, rm, omc);
+            edge_wait(1 + buf, NT);
             const float4 ab = warp > 0 ? ed(buf, warp - 1, 1) : z4;
             const float4 be = warp < WWARPS - 1 ? ed(buf, warp + 1, 0) : z4;
-            if (((start_colour + s) & 1) == 0)
-                half4<0>(d, a, b, ab, be, lm, rm, omc);
-            else
-                half4<1>(d, a, b, ab, be, lm, rm, omc);
+            if (c0) {
+                rows4<0, 0, 1>(d, a, b, ab, be, lm, rm, omc);
+                rows4<0, WROWS - 1, WROWS>(d, a, b, ab, be, lm, rm, omc);
+            } else {
+                rows4<1, 0, 1>(d, a, b, ab, be, lm, rm, omc);
+                rows4<1, WROWS - 1, WROWS>(d, a, b, ab, be, lm, rm, omc);
+            }
             if (s + 1 < nhalf) {
-                // the other buffer was last read before the previous barrier
                 ed(buf ^ 1, warp, 0) = d[0];
                 ed(buf ^ 1, warp, 1) = d[WROWS - 1];
-                __syncthreads();
+                edge_arrive(1 + (buf ^ 1), NT);
             }
         }
         // the interior back to global memory: the warp's rows inside it (a
@@ -418,6 +450,122 @@ __global__ void k_sor32_half(float *__restrict__ dlt, const float *__restrict__ 
     dlt[i] = fmaf(inv[i], sum, fmaf(1.f - omega[h], dlt[i], rhs[i]));
 }
 
+// ------------------------------------------------------------------ volumes, blocked
+
+// Temporal blocking in a volume (2.5-D: tiles across x and y marched along
+// z).  A block takes a VX x VY tile of a history's columns over a chunk of
+// its slices [z0, z1) and runs S <= D half-sweeps on it in one pass along z:
+// at step t, stage s (the s-th half-sweep) updates slice t - 2 (s - 1), its
+// pixels of that half-sweep's colour, in place in a ring of slices in shared
+// memory.  Two slices between stages keep every read at the right level:
+// stage s reads slices p - 1, p, p + 1 after stage s - 1 (slice p + 1 was
+// done a step ago, slice p - 1 holds stage s's own colour, which stage s
+// does not read), and no slice a stage reads is written in the same step.
+// The tile's halo is D pixels across x and y and D slices along z beyond
+// the chunk; what lies beyond the loaded slices or the tile reads as zero,
+// exact at the history's border and an error that moves in one ring per
+// half-sweep inside it, so every pixel D or more from such an edge equals S
+// in-place half-sweeps of the whole history (as k_sor32_half gives them,
+// to the bit: the same sums in the same order).  A thread owns a pair of
+// columns (one pixel of each colour per slice); the next slice is brought
+// into registers while the stages run, then into the ring, one barrier a
+// step.  The stage's coefficients are read from global memory (L1 keeps a
+// slice's for the S steps that use it).
+constexpr int VX = 64;  // tile columns: 32 lanes x 2
+
+template <int D, int VY>
+__global__ void __launch_bounds__(32 * VY) k_sor32_vol(const float *__restrict__ src, float *__restrict__ dst,
+                                                       const float *__restrict__ rhs, const float *__restrict__ inv,
+                                                       const int4 *__restrict__ dims, const int64_t *__restrict__ off,
+                                                       const int4 *__restrict__ tiles, int vz,
+                                                       const float *__restrict__ omega, const int32_t *done,
+                                                       int done_stride, int nhalf, int start_colour, int zero_start) {
+    constexpr int R = 2 * D + 2;  // ring slots: slices t - 2 D + 1 .. t + 2 in use at step t
+    extern __shared__ __align__(16) float ring[];  // [R][VY][VX]
+    const int4 tl = tiles[blockIdx.x];
+    const int h = tl.x;
+    if (done[(int64_t)h * done_stride]) return;
+    const int4 dm = dims[h];
+    const int x0 = tl.y, y0 = tl.z, z0 = tl.w;
+    const int z1 = min(z0 + vz, dm.z);
+    const int zlo = max(z0 - D, 0), zhi = min(z1 + D, dm.z);
+    const int S = nhalf;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int lx = 2 * tx, gx = x0 + lx, gy = y0 + ty;
+    const bool in0 = gx < dm.x && gy < dm.y, in1 = gx + 1 < dm.x && gy < dm.y;
+    const int64_t plane = (int64_t)dm.x * dm.y;
+    const int64_t col = off[h] + (int64_t)gy * dm.x + gx;  // this thread's first pixel in slice 0
+    const float omc = 1.f - omega[h];
+    // the output interior of the tile (a window edge on the history's border makes no error)
+    const int ix0 = x0 == 0 ? 0 : x0 + D, ix1 = x0 + VX >= dm.x ? dm.x : x0 + VX - D;
+    const int iy0 = y0 == 0 ? 0 : y0 + D, iy1 = y0 + VY >= dm.y ? dm.y : y0 + VY - D;
+    const bool out_y = gy >= iy0 && gy < iy1;
+    const bool out0 = in0 && out_y && gx >= ix0 && gx < ix1, out1 = in1 && out_y && gx + 1 >= ix0 && gx + 1 < ix1;
+    auto slot = [&](int z) -> float * { return ring + (size_t)(z % R) * (VY * VX); };
+    auto load = [&](int z, float &v0, float &v1) {
+        v0 = v1 = 0.f;
+        if (!zero_start) {
+            const int64_t i = col + (int64_t)z * plane;
+            if (in0) v0 = __ldg(src + i);
+            if (in1) v1 = __ldg(src + i + 1);
+        }
+    };
+    // the first two slices
+    for (int z = zlo; z < min(zlo + 2, zhi); ++z) {
+        float v0, v1;
+        load(z, v0, v1);
+        ((float2 *)(slot(z) + ty * VX))[tx] = make_float2(v0, v1);
+    }
+    __syncthreads();
+    const int tend = zhi - 1 + 2 * (S - 1);
+    for (int t = zlo; t <= tend; ++t) {
+        // the slice after next into registers while the stages run
+        const int zn = t + 2;
+        float n0 = 0.f, n1 = 0.f;
+        if (zn < zhi) load(zn, n0, n1);
+        for (int s = 1; s <= S; ++s) {
+            const int p = t - 2 * (s - 1);  // the same for the whole block
+            if (p < zlo || p >= zhi) continue;
+            const int c = (start_colour + s - 1) & 1;
+            // the pixel of colour c in this thread's pair ((x + y + z) mod 2 == c,
+            // x0 even): the same e for a warp, which holds one row
+            const int e = (c + gy + p) & 1;
+            float2 *row = (float2 *)(slot(p) + ty * VX) + tx;
+            const float2 me = *row;
+            // x neighbours: the left pair's second pixel, the right pair's first
+            const float left = __shfl_up_sync(0xffffffffu, me.y, 1);
+            const float right = __shfl_down_sync(0xffffffffu, me.x, 1);
+            const float2 z2 = make_float2(0.f, 0.f);
+            const float2 ym2 = ty > 0 ? row[-VX / 2] : z2, yp2 = ty + 1 < VY ? row[VX / 2] : z2;
+            const float2 zm2 = p - 1 >= zlo ? ((const float2 *)(slot(p - 1) + ty * VX))[tx] : z2;
+            const float2 zp2 = p + 1 < zhi ? ((const float2 *)(slot(p + 1) + ty * VX))[tx] : z2;
+            if (!(e ? in1 : in0)) continue;  // outside the history: stays zero
+            float xm, xp, ym, yp, zm, zp, cur;
+            if (e == 0) {
+                xm = tx > 0 ? left : 0.f; xp = me.y; ym = ym2.x; yp = yp2.x; zm = zm2.x; zp = zp2.x; cur = me.x;
+            } else {
+                xm = me.x; xp = tx < 31 ? right : 0.f; ym = ym2.y; yp = yp2.y; zm = zm2.y; zp = zp2.y; cur = me.y;
+            }
+            // k_sor32_half's sums, in its order
+            float sum = (xm + xp) + (ym + yp);
+            sum += (zm + zp);
+            const int64_t i = col + (int64_t)p * plane + e;
+            const float v = fmaf(__ldg(inv + i), sum, fmaf(omc, cur, __ldg(rhs + i)));
+            *row = e == 0 ? make_float2(v, me.y) : make_float2(me.x, v);
+        }
+        // slice t - 2 (S - 1) has had every half-sweep: its interior out
+        const int pf = t - 2 * (S - 1);
+        if (pf >= z0 && pf < z1) {
+            const float2 q = ((const float2 *)(slot(pf) + ty * VX))[tx];
+            const int64_t i = col + (int64_t)pf * plane;
+            if (out0) dst[i] = q.x;
+            if (out1) dst[i + 1] = q.y;
+        }
+        if (zn < zhi) ((float2 *)(slot(zn) + ty * VX))[tx] = make_float2(n0, n1);
+        __syncthreads();
+    }
+}
+
 typedef void (*TbKernel)(const float *, float *, const float *, const float *, const int4 *, const int64_t *,
                          const int32_t *, int, const float *, const int32_t *, int, int, int);
 typedef void (*WideKernel)(const CUtensorMap *, int, float *, const int4 *, int, const int4 *, const int64_t *,
@@ -442,6 +590,16 @@ WideKernel wide_kernel_of(int depth) {
     default: return k_sor32_wide<8, W>;
     }
 }
+
+typedef void (*VolKernel)(const float *, float *, const float *, const float *, const int4 *, const int64_t *,
+                          const int4 *, int, const float *, const int32_t *, int, int, int, int);
+
+VolKernel vol_kernel(int depth, int vy) {
+    if (vy == 16) return depth >= 4 ? k_sor32_vol<4, 16> : k_sor32_vol<2, 16>;
+    return depth >= 4 ? k_sor32_vol<4, 32> : k_sor32_vol<2, 32>;
+}
+
+size_t vol_smem(int depth, int vy) { return (size_t)(2 * depth + 2) * vy * VX * sizeof(float); }
 
 WideKernel wide_kernel(int depth, int warps) { return warps == 16 ? wide_kernel_of<16>(depth) : wide_kernel_of<8>(depth); }
 
@@ -515,6 +673,57 @@ int wide_init(Sor32 &s, cw_field_s *f, int warps) {
     return CW_OK;
 }
 
+// The volume kernel's tiles: VX x vy columns (halo `depth`) by chunks of vz
+// slices, vz the largest of 64, 32, 16 that still gives the device three
+// tiles for every block it holds at once.
+int vol_init(Sor32 &s, cw_field_s *f, int window) {
+    s.vol = false;
+    const Geom &g = f->g;
+    for (uint32_t k = 0; k < g.nh; ++k)
+        if (g.d[k] < 2) return CW_OK;
+    s.vdepth = s.depth >= 4 ? 4 : 2;
+    s.vy = window == CW_WINDOW_64 ? 16 : 32;
+    VolKernel kern = vol_kernel(s.vdepth, s.vy);
+    const size_t smem = vol_smem(s.vdepth, s.vy);
+    CW_CUDA(cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0, dev = 0, nsm = 0;
+    CW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)kern, 32 * s.vy, smem));
+    if (per_sm < 1) return CW_OK;  // one half-sweep per launch serves
+    CW_CUDA(cudaGetDevice(&dev));
+    CW_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    std::vector<int> xs, ys;
+    std::vector<int64_t> columns(g.nh);
+    for (uint32_t k = 0; k < g.nh; ++k) {
+        axis_starts(g.w[k], VX, s.vdepth, xs);
+        axis_starts(g.h[k], s.vy, s.vdepth, ys);
+        columns[k] = (int64_t)xs.size() * ys.size();
+    }
+    s.vz = 16;
+    for (int vz : {64, 32}) {
+        int64_t n = 0;
+        for (uint32_t k = 0; k < g.nh; ++k) n += columns[k] * ((g.d[k] + vz - 1) / vz);
+        if (n >= 3LL * per_sm * nsm) {
+            s.vz = vz;
+            break;
+        }
+    }
+    std::vector<int4> tiles;
+    for (uint32_t k = 0; k < g.nh; ++k) {
+        axis_starts(g.w[k], VX, s.vdepth, xs);
+        axis_starts(g.h[k], s.vy, s.vdepth, ys);
+        for (int z = 0; z < g.d[k]; z += s.vz)
+            for (int y : ys)
+                for (int x : xs) tiles.push_back(make_int4((int)k, x, y, z));
+    }
+    int rc;
+    if ((rc = dalloc(&s.vtiles, tiles.size())) != CW_OK) return rc;
+    CW_CUDA(cudaMemcpyAsync(s.vtiles, tiles.data(), tiles.size() * sizeof(int4), cudaMemcpyHostToDevice, stream()));
+    CW_CUDA(cudaStreamSynchronize(stream()));
+    s.nvtiles = (int)tiles.size();
+    s.vol = true;
+    return CW_OK;
+}
+
 }  // namespace
 
 int Sor32::init(cw_field_s *f, int d, const std::vector<double> &om, int window) {
@@ -539,8 +748,12 @@ int Sor32::init(cw_field_s *f, int d, const std::vector<double> &om, int window)
             rc = tiles.build(per, 1);
         }
     } else {
-        for (uint32_t k = 0; k < f->g.nh; ++k) per[k] = (int64_t)((f->g.w[k] + 1) / 2) * f->g.h[k] * f->g.d[k];
-        rc = sites.build(per, 256);
+        vol = false;
+        if (depth > 1 && (rc = vol_init(*this, f, window)) != CW_OK) return rc;
+        if (!vol) {
+            for (uint32_t k = 0; k < f->g.nh; ++k) per[k] = (int64_t)((f->g.w[k] + 1) / 2) * f->g.h[k] * f->g.d[k];
+            rc = sites.build(per, 256);
+        }
     }
     ping = f->d32a;
     pong = f->d32b;
@@ -554,6 +767,26 @@ int Sor32::sweeps(cw_field_s *f, int n, const int32_t *done, int done_stride, fl
     if (start) {  // begin from this (zeroed) buffer; the other is scratch
         ping = start;
         pong = start == f->d32a ? f->d32b : f->d32a;
+    }
+    if (vol) {
+        // 2n half-sweeps, vdepth per launch (fewer in the last), ping-pong
+        // between the buffers; the first launch starts from zero
+        float *a = ping, *b = pong;
+        int remaining = 2 * n, done_half = 0;
+        VolKernel kern = vol_kernel(vdepth, vy);
+        const size_t smem = vol_smem(vdepth, vy);
+        while (remaining > 0) {
+            const int dd = remaining < vdepth ? remaining : vdepth;
+            kern<<<nvtiles, 32 * vy, smem, stream()>>>(a, b, f->r32, f->inv32, f->g.d_dims, f->g.d_off, vtiles, vz,
+                                                       omega, done, done_stride, dd, done_half & 1,
+                                                       done_half == 0 ? 1 : 0);
+            CW_LAUNCHED();
+            remaining -= dd;
+            done_half += dd;
+            float *t = a; a = b; b = t;
+        }
+        out = a;
+        return CW_OK;
     }
     if (!blocked) {
         for (int s = 0; s < n; ++s)
@@ -605,6 +838,8 @@ void Sor32::release() {
     maps = nullptr;
     dfree(wtiles);
     wide = false;
+    dfree(vtiles);
+    vol = false;
 }
 
 // Whether a wide-kernel block gave up waiting for its window (and clears the record).

@@ -50,12 +50,16 @@ __device__ __forceinline__ void pixel_sums64(const double *__restrict__ c, int64
 // histories are swept `depth` half-sweeps per launch, each tile held on chip
 // with a halo `depth` deep (temporal blocking): 128 x 64 windows fed by TMA
 // to persistent blocks where every history's rows are 16-byte aligned,
-// 64 x 64 windows read by plain loads otherwise; volumes one half-sweep per
-// launch, in place.
+// 64 x 64 windows read by plain loads otherwise; volumes by 64 x 32 (or
+// 64 x 16) tiles marched along z, two or four half-sweeps per launch, or at
+// depth 1 one half-sweep per launch, in place.
 struct Sor32 {
     int depth = 4;
     bool blocked = true;
     bool wide = false;          // the TMA-fed kernel
+    bool vol = false;           // volumes: the tiles marched along z
+    int4 *vtiles = nullptr;     // vol: (history, x0, y0, z0) per tile, device
+    int nvtiles = 0, vy = 32, vz = 32, vdepth = 2;
     Plan tiles;                 // 64 x 64 windows: tiles per history
     Plan sites;                 // volumes: pixels per history
     void *maps = nullptr;       // wide: 4 tensor maps per history (d32a, d32b, r32, inv32), device

@@ -1008,8 +1008,10 @@ static int tune_depth(cw_sim_s *s) {
     if (s->cfg.precision != CW_FP32_DC) return CW_OK;
     float best = 0.f;
     int bd = 8, bw = CW_WINDOW_AUTO;
+    // volumes march tiles along z at two or four half-sweeps a launch
+    const bool volume = s->d[0] > 1;
     for (int w : {CW_WINDOW_AUTO, CW_WINDOW_64})
-        for (int d : {4, 6, 8}) {
+        for (int d : {volume ? 2 : 6, 4, 8}) {
             float ms = 0.f;
             int64_t launches = 0;
             int rc = cw_field_time_inner(s->o2, 8, d, w, 1.9, &ms, &launches);

@@ -268,7 +268,7 @@ def test_suppressed_mutations_leave_the_run_as_it_was(tmp_path):
                      .replace("rewiring = 0.3\n", "rewiring = 0.3\n" + (extra if name == "suppressed" else "")))
         cfg = C.load_sim_config(str(p))
         sim, _ = C.simulation_from_config(cfg, histories=4, seeds=[51, 52, 53, 54])
-        sim.step(150)
+        sim.step(400)  # the sheet's first divisions come after about 200 steps
         runs[name] = sim
     a, b = runs["plain"], runs["suppressed"]
     recs = b.clone_records()

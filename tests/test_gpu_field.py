@@ -267,24 +267,46 @@ def test_a_batch_of_uneven_histories_solves_each_as_alone():
 
 
 def inner_corrections(dims, depth, window=cw.WINDOW_AUTO, sweeps=5, seed=3):
-    """cw_field_time_inner's FP32 correction for each history of a random batch."""
+    """cw_field_time_inner's FP32 correction for each history of a random
+    batch (dims (w, h) for planes, (w, h, d) for volumes)."""
     import ctypes as C
     from cellweave_b200 import _lib
     rng = np.random.default_rng(seed)
-    f = cw.ScalarField([(w, h, 1) for w, h in dims], D, 0.001, 0.0)
-    for k, (w, h) in enumerate(dims):
-        f.set_values(rng.random(w * h), k)
-        f.set_uptake_array(rng.random(w * h) * 0.01, k)
-        f.hold_where(1.0, (rng.random(w * h) < 0.05).astype(np.uint8), k)
+    dims = [tuple(x) + (1,) * (3 - len(x)) for x in dims]
+    f = cw.ScalarField(dims, D, 0.001, 0.0)
+    for k, (w, h, d) in enumerate(dims):
+        n = w * h * d
+        f.set_values(rng.random(n), k)
+        f.set_uptake_array(rng.random(n) * 0.01, k)
+        f.hold_where(1.0, (rng.random(n) < 0.05).astype(np.uint8), k)
     ms, launches = C.c_float(), C.c_int64()
     L = _lib.lib()
     _lib.check(L.cw_field_time_inner(f.handle, sweeps, depth, window, 1.9, C.byref(ms), C.byref(launches)))
     out = []
-    for k, (w, h) in enumerate(dims):
-        a = np.empty(w * h, np.float32)
+    for k, (w, h, d) in enumerate(dims):
+        a = np.empty(w * h * d, np.float32)
         _lib.check(L.cw_field_inner_correction(f.handle, k, a.ctypes.data))
         out.append(a)
     return out, launches.value
+
+
+@pytest.mark.parametrize("dims", [
+    [(70, 37, 9), (130, 40, 11), (33, 19, 6)],   # odd widths, a tile's halo across every axis
+    [(96, 96, 96), (64, 200, 40)],               # several slice chunks
+])
+def test_blocked_volume_sweeps_equal_one_half_sweep_per_launch(dims):
+    # the tiles marched along z are exact: two or four half-sweeps a launch,
+    # tiles 32 or 16 rows high, give to the bit the in-place half-sweeps of
+    # one per launch (5 sweeps: a depth-4 run ends on a launch of 2)
+    ref, n1 = inner_corrections(dims, 1)
+    assert n1 == 10
+    assert all(np.abs(r).max() > 0 for r in ref)
+    for window in (cw.WINDOW_AUTO, cw.WINDOW_64):
+        for depth in (2, 4):
+            got, launches = inner_corrections(dims, depth, window)
+            assert launches == (10 + depth - 1) // depth
+            for k in range(len(dims)):
+                np.testing.assert_array_equal(got[k], ref[k], err_msg=f"window {window}, depth {depth}, {dims[k]}")
 
 
 @pytest.mark.parametrize("dims", [
