@@ -198,18 +198,13 @@ __device__ __forceinline__ void rows4(float4 (&d)[WROWS], const float4 (&a)[WROW
     }
 }
 
-// Named barriers 1 and 2 (0 is __syncthreads'), alternating by half-sweep:
-// a warp arrives once it has published its edge rows and waits only when it
-// needs the others' (PTX bar.arrive / bar.sync over the block's threads; both
-// order the shared-memory accesses before them for the threads that meet).
-// (immediate ids, so that the compiler reserves three barriers, not all 16).
-__device__ __forceinline__ void edge_arrive(int id, int nthreads) {
-    if (id == 1) asm volatile("bar.arrive 1, %0;" ::"r"(nthreads) : "memory");
-    else asm volatile("bar.arrive 2, %0;" ::"r"(nthreads) : "memory");
-}
-__device__ __forceinline__ void edge_wait(int id, int nthreads) {
-    if (id == 1) asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory");
-    else asm volatile("bar.sync 2, %0;" ::"r"(nthreads) : "memory");
+// The edge rows' split-phase barriers: two mbarriers (one per edge buffer),
+// every thread of the block arriving once it has published (release), and
+// waiting on the phase only when it needs the others' edges (acquire).  A
+// named barrier cannot do this: a thread may take part in one of its
+// generations once, by arriving or by waiting, not both.
+__device__ __forceinline__ void edge_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 
 // What a block needs of a window, staged in shared memory by thread 0 one
@@ -240,6 +235,7 @@ __global__ void __launch_bounds__(32 * WWARPS, WWARPS == 8 ? 2 : 1)
                  *sa = (const float4 *)(smem + 2 * STAGE);
     float4 *edge = (float4 *)(smem + 3 * STAGE);  // [buffer][warp][0 top, 1 bottom][lane]
     __shared__ __align__(8) uint64_t bar_word;
+    __shared__ __align__(8) uint64_t edge_word[2];
     __shared__ WideTile s_info[2];
     __shared__ int s_fail;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -271,12 +267,16 @@ __global__ void __launch_bounds__(32 * WWARPS, WWARPS == 8 ? 2 : 1)
     };
     if (threadIdx.x == 0) {
         mbar_init(bar, 1);
+        mbar_init(sh_addr(&edge_word[0]), 32 * WWARPS);
+        mbar_init(sh_addr(&edge_word[1]), 32 * WWARPS);
         mbar_init_fence();
         s_fail = 0;
         stage_next(blockIdx.x, 0);
     }
     __syncthreads();
     uint32_t parity = 0;
+    const uint32_t ebar0 = sh_addr(&edge_word[0]), ebar1 = sh_addr(&edge_word[1]);
+    uint32_t eph0 = 0, eph1 = 0;  // the phase of each edge barrier this thread waits for next
     const float lm = lane == 0 ? 0.f : 1.f, rm = lane == 31 ? 0.f : 1.f;
     const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
     auto ed = [&](int buf, int w, int side) -> float4 & { return edge[((buf * WWARPS + w) * 2 + side) * 32 + lane]; };
@@ -309,14 +309,14 @@ __global__ void __launch_bounds__(32 * WWARPS, WWARPS == 8 ? 2 : 1)
         }
         const float omc = info.omc;
         // half-sweep s reads the edges published after half-sweep s - 1 in
-        // buffer s & 1, behind named barrier 1 + (s & 1): a warp sweeps its
-        // band's inner rows while the others' edges arrive, then its two edge
-        // rows.  Buffer (s + 1) & 1 is written only after barrier 1 + (s & 1)
-        // has completed, that is after every warp read it in half-sweep s - 1.
-        constexpr int NT = 32 * WWARPS;
+        // buffer s & 1, behind that buffer's mbarrier: a thread sweeps its
+        // band's inner rows while the others' edges arrive, then waits for
+        // the phase and sweeps its two edge rows.  Buffer (s + 1) & 1 is
+        // written only after the phase of buffer s & 1 has completed, that is
+        // after every thread read it in half-sweep s - 1.
         ed(0, warp, 0) = d[0];
         ed(0, warp, 1) = d[WROWS - 1];
-        edge_arrive(1, NT);
+        edge_arrive(ebar0);
         for (int s = 0; s < nhalf; ++s) {
             const int buf = s & 1;
             const bool c0 = ((start_colour + s) & 1) == 0;
@@ -324,7 +324,10 @@ __global__ void __launch_bounds__(32 * WWARPS, WWARPS == 8 ? 2 : 1)
                 rows4<0, 1, WROWS - 1>(d, a, b, z4, z4, lm, rm, omc);
             else
                 rows4<1, 1, WROWS - 1>(d, a, b, z4, z4, lm, rm, omc);
-            edge_wait(1 + buf, NT);
+            if (!mbar_wait_bounded(buf ? ebar1 : ebar0, buf ? eph1 : eph0, wait_ns))
+                atomicExch(&g_wide_wait_failed, 1);
+            if (buf) eph1 ^= 1u;
+            else eph0 ^= 1u;
             const float4 ab = warp > 0 ? ed(buf, warp - 1, 1) : z4;
             const float4 be = warp < WWARPS - 1 ? ed(buf, warp + 1, 0) : z4;
             if (c0) {
@@ -337,7 +340,7 @@ __global__ void __launch_bounds__(32 * WWARPS, WWARPS == 8 ? 2 : 1)
             if (s + 1 < nhalf) {
                 ed(buf ^ 1, warp, 0) = d[0];
                 ed(buf ^ 1, warp, 1) = d[WROWS - 1];
-                edge_arrive(1 + (buf ^ 1), NT);
+                edge_arrive(buf ? ebar0 : ebar1);
             }
         }
         // the interior back to global memory: the warp's rows inside it (a
