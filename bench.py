@@ -495,11 +495,12 @@ def shape_record(L, cfg, steps, warm, peak):
     volume = any(d > 1 for _, _, d in cfg["dims"])
     depth = 2 if volume else tuned["depth"]
     lm = sor_launch_ms(L, sim.field_handle(0), depth, tuned["window"])
-    # a volume's sweep is one half-sweep per launch (k_sor32_half): two
-    # launches move one sweep's 16 B per site
-    alg = sites * SOR_BYTES_PER_SITE_PASS / (2 if volume else 1)
+    # a volume's launch is one sweep (two half-sweeps) of tiles marched along
+    # z (k_sor32_vol); a plane's, `depth` half-sweeps on chip: 16 B per site a launch
+    alg = sites * SOR_BYTES_PER_SITE_PASS
     gbs = alg / (lm / 1e3) / 1e9
-    rec["sor"] = {"kernel": "k_sor32_half (one half-sweep per launch)" if volume else
+    rec["sor"] = {"kernel": ("k_sor32_vol<%d> (64x%d tiles marched along z, one sweep per launch)" %
+                             ((16, 16) if tuned["window"] == 1 else (32, 32))) if volume else
                   f"k_sor32_wide<{depth}> ({depth} half-sweeps per launch on chip)",
                   "launch_ms": round(lm, 4), "alg_bytes_per_launch": int(alg), "achieved_gbs": round(gbs, 1),
                   "frac": round(gbs / peak, 3)}

@@ -167,9 +167,7 @@ __device__ __forceinline__ int next_live(int t, int ntiles, int step, const int4
 // columns.  Column c of row j has colour (c + j) mod 2 (windows start at even
 // x and y): colour C takes columns 0 and 2 of the rows with C + j even, 1 and
 // 3 of the others.  Every update reads only pixels of the other colour, which
-// this half-sweep does not change, so rows may be taken in any order: the
-// rows inside the warp's band first (J0 = 1, J1 = WROWS - 1), then the two
-// that read the neighbouring warps' edges once those have arrived.
+// this half-sweep does not change.
 template <int C, int J0, int J1>
 __device__ __forceinline__ void rows4(float4 (&d)[WROWS], const float4 (&a)[WROWS], const float4 (&b)[WROWS],
                                       const float4 ab, const float4 be, float lm, float rm, float omc) {
@@ -196,15 +194,6 @@ __device__ __forceinline__ void rows4(float4 (&d)[WROWS], const float4 (&a)[WROW
             d[j].w = fmaf(a[j].w, s3, fmaf(omc, d[j].w, b[j].w));
         }
     }
-}
-
-// The edge rows' split-phase barriers: two mbarriers (one per edge buffer),
-// every thread of the block arriving once it has published (release), and
-// waiting on the phase only when it needs the others' edges (acquire).  A
-// named barrier cannot do this: a thread may take part in one of its
-// generations once, by arriving or by waiting, not both.
-__device__ __forceinline__ void edge_arrive(uint32_t bar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 
 // What a block needs of a window, staged in shared memory by thread 0 one
@@ -235,7 +224,6 @@ __global__ void __launch_bounds__(32 * WWARPS, WWARPS == 8 ? 2 : 1)
                  *sa = (const float4 *)(smem + 2 * STAGE);
     float4 *edge = (float4 *)(smem + 3 * STAGE);  // [buffer][warp][0 top, 1 bottom][lane]
     __shared__ __align__(8) uint64_t bar_word;
-    __shared__ __align__(8) uint64_t edge_word[2];
     __shared__ WideTile s_info[2];
     __shared__ int s_fail;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -267,16 +255,12 @@ __global__ void __launch_bounds__(32 * WWARPS, WWARPS == 8 ? 2 : 1)
     };
     if (threadIdx.x == 0) {
         mbar_init(bar, 1);
-        mbar_init(sh_addr(&edge_word[0]), 32 * WWARPS);
-        mbar_init(sh_addr(&edge_word[1]), 32 * WWARPS);
         mbar_init_fence();
         s_fail = 0;
         stage_next(blockIdx.x, 0);
     }
     __syncthreads();
     uint32_t parity = 0;
-    const uint32_t ebar0 = sh_addr(&edge_word[0]), ebar1 = sh_addr(&edge_word[1]);
-    uint32_t eph0 = 0, eph1 = 0;  // the phase of each edge barrier this thread waits for next
     const float lm = lane == 0 ? 0.f : 1.f, rm = lane == 31 ? 0.f : 1.f;
     const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
     auto ed = [&](int buf, int w, int side) -> float4 & { return edge[((buf * WWARPS + w) * 2 + side) * 32 + lane]; };
@@ -308,39 +292,22 @@ __global__ void __launch_bounds__(32 * WWARPS, WWARPS == 8 ? 2 : 1)
             stage_next(info.tl.w + gridDim.x, slot ^ 1);
         }
         const float omc = info.omc;
-        // half-sweep s reads the edges published after half-sweep s - 1 in
-        // buffer s & 1, behind that buffer's mbarrier: a thread sweeps its
-        // band's inner rows while the others' edges arrive, then waits for
-        // the phase and sweeps its two edge rows.  Buffer (s + 1) & 1 is
-        // written only after the phase of buffer s & 1 has completed, that is
-        // after every thread read it in half-sweep s - 1.
         ed(0, warp, 0) = d[0];
         ed(0, warp, 1) = d[WROWS - 1];
-        edge_arrive(ebar0);
+        __syncthreads();
         for (int s = 0; s < nhalf; ++s) {
             const int buf = s & 1;
-            const bool c0 = ((start_colour + s) & 1) == 0;
-            if (c0)
-                rows4<0, 1, WROWS - 1>(d, a, b, z4, z4, lm, rm, omc);
-            else
-                rows4<1, 1, WROWS - 1>(d, a, b, z4, z4, lm, rm, omc);
-            if (!mbar_wait_bounded(buf ? ebar1 : ebar0, buf ? eph1 : eph0, wait_ns))
-                atomicExch(&g_wide_wait_failed, 1);
-            if (buf) eph1 ^= 1u;
-            else eph0 ^= 1u;
             const float4 ab = warp > 0 ? ed(buf, warp - 1, 1) : z4;
             const float4 be = warp < WWARPS - 1 ? ed(buf, warp + 1, 0) : z4;
-            if (c0) {
-                rows4<0, 0, 1>(d, a, b, ab, be, lm, rm, omc);
-                rows4<0, WROWS - 1, WROWS>(d, a, b, ab, be, lm, rm, omc);
-            } else {
-                rows4<1, 0, 1>(d, a, b, ab, be, lm, rm, omc);
-                rows4<1, WROWS - 1, WROWS>(d, a, b, ab, be, lm, rm, omc);
-            }
+            if (((start_colour + s) & 1) == 0)
+                rows4<0, 0, WROWS>(d, a, b, ab, be, lm, rm, omc);
+            else
+                rows4<1, 0, WROWS>(d, a, b, ab, be, lm, rm, omc);
             if (s + 1 < nhalf) {
+                // the other buffer was last read before the previous barrier
                 ed(buf ^ 1, warp, 0) = d[0];
                 ed(buf ^ 1, warp, 1) = d[WROWS - 1];
-                edge_arrive(buf ? ebar0 : ebar1);
+                __syncthreads();
             }
         }
         // the interior back to global memory: the warp's rows inside it (a
@@ -457,41 +424,54 @@ __global__ void k_sor32_half(float *__restrict__ dlt, const float *__restrict__ 
 
 // Temporal blocking in a volume (2.5-D: tiles across x and y marched along
 // z).  A block takes a VX x VY tile of a history's columns over a chunk of
-// its slices [z0, z1) and runs S <= D half-sweeps on it in one pass along z:
-// at step t, stage s (the s-th half-sweep) updates slice t - 2 (s - 1), its
-// pixels of that half-sweep's colour, in place in a ring of slices in shared
-// memory.  Two slices between stages keep every read at the right level:
-// stage s reads slices p - 1, p, p + 1 after stage s - 1 (slice p + 1 was
-// done a step ago, slice p - 1 holds stage s's own colour, which stage s
+// its slices [z0, z1) and runs S <= 2 half-sweeps (one sweep) on it in one
+// pass along z: at step t, stage s updates slice t - 2 (s - 1), its pixels
+// of that half-sweep's colour, in place in a ring of slices in shared
+// memory.  Two slices between the stages keep every read at the right
+// level: stage 2 reads slices p - 1, p, p + 1 after stage 1 (slice p + 1 was
+// done a step ago; slice p - 1 holds stage 2's own colour, which stage 2
 // does not read), and no slice a stage reads is written in the same step.
-// The tile's halo is D pixels across x and y and D slices along z beyond
+// The tile's halo is VD pixels across x and y and VD slices along z beyond
 // the chunk; what lies beyond the loaded slices or the tile reads as zero,
 // exact at the history's border and an error that moves in one ring per
-// half-sweep inside it, so every pixel D or more from such an edge equals S
-// in-place half-sweeps of the whole history (as k_sor32_half gives them,
+// half-sweep inside it, so every pixel VD or more from such an edge equals
+// S in-place half-sweeps of the whole history (as k_sor32_half gives them,
 // to the bit: the same sums in the same order).  A thread owns a pair of
-// columns (one pixel of each colour per slice); the next slice is brought
-// into registers while the stages run, then into the ring, one barrier a
-// step.  The stage's coefficients are read from global memory (L1 keeps a
-// slice's for the S steps that use it).
+// columns (one pixel of each colour per slice).  The correction and both
+// coefficients of slice t + 1 + VP are copied into the ring by cp.async
+// while step t runs (VP slices ahead), one barrier a step.
 constexpr int VX = 64;  // tile columns: 32 lanes x 2
+constexpr int VD = 2;   // half-sweeps per launch at most, and the halo
+constexpr int VP = 3;   // slices copied ahead
+constexpr int VR = 2 * VD + VP + 1;  // ring slots: slices t - 2 VD + 1 .. t + 1 + VP
 
-template <int D, int VY>
+__device__ __forceinline__ void cp_async4(float *dst, const float *src, bool take) {
+    // 4 bytes, or (take false) a zero written without reading src
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(sh_addr(dst)), "l"(src), "r"(take ? 4 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+constexpr size_t vol_smem_of(int vy) { return (size_t)VR * 3 * vy * VX * sizeof(float); }
+
+template <int VY>
 __global__ void __launch_bounds__(32 * VY) k_sor32_vol(const float *__restrict__ src, float *__restrict__ dst,
                                                        const float *__restrict__ rhs, const float *__restrict__ inv,
                                                        const int4 *__restrict__ dims, const int64_t *__restrict__ off,
                                                        const int4 *__restrict__ tiles, int vz,
                                                        const float *__restrict__ omega, const int32_t *done,
                                                        int done_stride, int nhalf, int start_colour, int zero_start) {
-    constexpr int R = 2 * D + 2;  // ring slots: slices t - 2 D + 1 .. t + 2 in use at step t
-    extern __shared__ __align__(16) float ring[];  // [R][VY][VX]
+    constexpr int PL = VY * VX;               // floats of one slice of one array
+    extern __shared__ __align__(16) float ring[];  // [VR][3: correction, b, a][VY][VX]
     const int4 tl = tiles[blockIdx.x];
     const int h = tl.x;
     if (done[(int64_t)h * done_stride]) return;
     const int4 dm = dims[h];
     const int x0 = tl.y, y0 = tl.z, z0 = tl.w;
     const int z1 = min(z0 + vz, dm.z);
-    const int zlo = max(z0 - D, 0), zhi = min(z1 + D, dm.z);
+    const int zlo = max(z0 - VD, 0), zhi = min(z1 + VD, dm.z);
     const int S = nhalf;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     const int lx = 2 * tx, gx = x0 + lx, gy = y0 + ty;
@@ -500,32 +480,37 @@ __global__ void __launch_bounds__(32 * VY) k_sor32_vol(const float *__restrict__
     const int64_t col = off[h] + (int64_t)gy * dm.x + gx;  // this thread's first pixel in slice 0
     const float omc = 1.f - omega[h];
     // the output interior of the tile (a window edge on the history's border makes no error)
-    const int ix0 = x0 == 0 ? 0 : x0 + D, ix1 = x0 + VX >= dm.x ? dm.x : x0 + VX - D;
-    const int iy0 = y0 == 0 ? 0 : y0 + D, iy1 = y0 + VY >= dm.y ? dm.y : y0 + VY - D;
+    const int ix0 = x0 == 0 ? 0 : x0 + VD, ix1 = x0 + VX >= dm.x ? dm.x : x0 + VX - VD;
+    const int iy0 = y0 == 0 ? 0 : y0 + VD, iy1 = y0 + VY >= dm.y ? dm.y : y0 + VY - VD;
     const bool out_y = gy >= iy0 && gy < iy1;
     const bool out0 = in0 && out_y && gx >= ix0 && gx < ix1, out1 = in1 && out_y && gx + 1 >= ix0 && gx + 1 < ix1;
-    auto slot = [&](int z) -> float * { return ring + (size_t)(z % R) * (VY * VX); };
-    auto load = [&](int z, float &v0, float &v1) {
-        v0 = v1 = 0.f;
-        if (!zero_start) {
+    const int me_off = ty * VX + lx;
+    auto slot = [&](int z, int arr) -> float * { return ring + ((z % VR) * 3 + arr) * PL; };
+    // slice z's pair of each array into the ring (zeros outside the history;
+    // the correction zero without reading it on a launch that starts from zero);
+    // one copy group per slice, empty past the chunk's last slice
+    auto issue = [&](int z) {
+        if (z < zhi) {
             const int64_t i = col + (int64_t)z * plane;
-            if (in0) v0 = __ldg(src + i);
-            if (in1) v1 = __ldg(src + i + 1);
+            const int64_t i0 = in0 ? i : off[h], i1 = in1 ? i + 1 : off[h];  // a valid address when not read
+            float *d = slot(z, 0) + me_off, *b = slot(z, 1) + me_off, *a = slot(z, 2) + me_off;
+            cp_async4(d, src + i0, in0 && !zero_start);
+            cp_async4(d + 1, src + i1, in1 && !zero_start);
+            cp_async4(b, rhs + i0, in0);
+            cp_async4(b + 1, rhs + i1, in1);
+            cp_async4(a, inv + i0, in0);
+            cp_async4(a + 1, inv + i1, in1);
         }
+        cp_async_commit();
     };
-    // the first two slices
-    for (int z = zlo; z < min(zlo + 2, zhi); ++z) {
-        float v0, v1;
-        load(z, v0, v1);
-        ((float2 *)(slot(z) + ty * VX))[tx] = make_float2(v0, v1);
-    }
-    __syncthreads();
+    for (int z = zlo; z <= zlo + VP; ++z) issue(z);
     const int tend = zhi - 1 + 2 * (S - 1);
     for (int t = zlo; t <= tend; ++t) {
-        // the slice after next into registers while the stages run
-        const int zn = t + 2;
-        float n0 = 0.f, n1 = 0.f;
-        if (zn < zhi) load(zn, n0, n1);
+        // slice t + 1 landed (the VP - 1 copies after it may still be in
+        // flight), for every thread; every thread is done with step t - 1
+        cp_async_wait<VP - 1>();
+        __syncthreads();
+        issue(t + 1 + VP);  // its slot last held slice t + 1 + VP - VR, no longer read
         for (int s = 1; s <= S; ++s) {
             const int p = t - 2 * (s - 1);  // the same for the whole block
             if (p < zlo || p >= zhi) continue;
@@ -533,40 +518,41 @@ __global__ void __launch_bounds__(32 * VY) k_sor32_vol(const float *__restrict__
             // the pixel of colour c in this thread's pair ((x + y + z) mod 2 == c,
             // x0 even): the same e for a warp, which holds one row
             const int e = (c + gy + p) & 1;
-            float2 *row = (float2 *)(slot(p) + ty * VX) + tx;
+            float2 *row = (float2 *)(slot(p, 0) + me_off);
             const float2 me = *row;
             // x neighbours: the left pair's second pixel, the right pair's first
             const float left = __shfl_up_sync(0xffffffffu, me.y, 1);
             const float right = __shfl_down_sync(0xffffffffu, me.x, 1);
             const float2 z2 = make_float2(0.f, 0.f);
             const float2 ym2 = ty > 0 ? row[-VX / 2] : z2, yp2 = ty + 1 < VY ? row[VX / 2] : z2;
-            const float2 zm2 = p - 1 >= zlo ? ((const float2 *)(slot(p - 1) + ty * VX))[tx] : z2;
-            const float2 zp2 = p + 1 < zhi ? ((const float2 *)(slot(p + 1) + ty * VX))[tx] : z2;
+            const float2 zm2 = p - 1 >= zlo ? *(const float2 *)(slot(p - 1, 0) + me_off) : z2;
+            const float2 zp2 = p + 1 < zhi ? *(const float2 *)(slot(p + 1, 0) + me_off) : z2;
+            const float2 b2 = *(const float2 *)(slot(p, 1) + me_off), a2 = *(const float2 *)(slot(p, 2) + me_off);
             if (!(e ? in1 : in0)) continue;  // outside the history: stays zero
-            float xm, xp, ym, yp, zm, zp, cur;
+            float xm, xp, ym, yp, zm, zp, cur, bv, av;
             if (e == 0) {
                 xm = tx > 0 ? left : 0.f; xp = me.y; ym = ym2.x; yp = yp2.x; zm = zm2.x; zp = zp2.x; cur = me.x;
+                bv = b2.x; av = a2.x;
             } else {
                 xm = me.x; xp = tx < 31 ? right : 0.f; ym = ym2.y; yp = yp2.y; zm = zm2.y; zp = zp2.y; cur = me.y;
+                bv = b2.y; av = a2.y;
             }
             // k_sor32_half's sums, in its order
             float sum = (xm + xp) + (ym + yp);
             sum += (zm + zp);
-            const int64_t i = col + (int64_t)p * plane + e;
-            const float v = fmaf(__ldg(inv + i), sum, fmaf(omc, cur, __ldg(rhs + i)));
+            const float v = fmaf(av, sum, fmaf(omc, cur, bv));
             *row = e == 0 ? make_float2(v, me.y) : make_float2(me.x, v);
         }
         // slice t - 2 (S - 1) has had every half-sweep: its interior out
         const int pf = t - 2 * (S - 1);
         if (pf >= z0 && pf < z1) {
-            const float2 q = ((const float2 *)(slot(pf) + ty * VX))[tx];
+            const float2 q = *(const float2 *)(slot(pf, 0) + me_off);
             const int64_t i = col + (int64_t)pf * plane;
             if (out0) dst[i] = q.x;
             if (out1) dst[i + 1] = q.y;
         }
-        if (zn < zhi) ((float2 *)(slot(zn) + ty * VX))[tx] = make_float2(n0, n1);
-        __syncthreads();
     }
+    cp_async_wait<0>();  // no copy in flight into shared memory at exit
 }
 
 typedef void (*TbKernel)(const float *, float *, const float *, const float *, const int4 *, const int64_t *,
@@ -597,12 +583,7 @@ WideKernel wide_kernel_of(int depth) {
 typedef void (*VolKernel)(const float *, float *, const float *, const float *, const int4 *, const int64_t *,
                           const int4 *, int, const float *, const int32_t *, int, int, int, int);
 
-VolKernel vol_kernel(int depth, int vy) {
-    if (vy == 16) return depth >= 4 ? k_sor32_vol<4, 16> : k_sor32_vol<2, 16>;
-    return depth >= 4 ? k_sor32_vol<4, 32> : k_sor32_vol<2, 32>;
-}
-
-size_t vol_smem(int depth, int vy) { return (size_t)(2 * depth + 2) * vy * VX * sizeof(float); }
+VolKernel vol_kernel(int vy) { return vy == 16 ? k_sor32_vol<16> : k_sor32_vol<32>; }
 
 WideKernel wide_kernel(int depth, int warps) { return warps == 16 ? wide_kernel_of<16>(depth) : wide_kernel_of<8>(depth); }
 
@@ -684,10 +665,10 @@ int vol_init(Sor32 &s, cw_field_s *f, int window) {
     const Geom &g = f->g;
     for (uint32_t k = 0; k < g.nh; ++k)
         if (g.d[k] < 2) return CW_OK;
-    s.vdepth = s.depth >= 4 ? 4 : 2;
+    s.vdepth = VD;
     s.vy = window == CW_WINDOW_64 ? 16 : 32;
-    VolKernel kern = vol_kernel(s.vdepth, s.vy);
-    const size_t smem = vol_smem(s.vdepth, s.vy);
+    VolKernel kern = vol_kernel(s.vy);
+    const size_t smem = vol_smem_of(s.vy);
     CW_CUDA(cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0, dev = 0, nsm = 0;
     CW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)kern, 32 * s.vy, smem));
@@ -776,8 +757,8 @@ int Sor32::sweeps(cw_field_s *f, int n, const int32_t *done, int done_stride, fl
         // between the buffers; the first launch starts from zero
         float *a = ping, *b = pong;
         int remaining = 2 * n, done_half = 0;
-        VolKernel kern = vol_kernel(vdepth, vy);
-        const size_t smem = vol_smem(vdepth, vy);
+        VolKernel kern = vol_kernel(vy);
+        const size_t smem = vol_smem_of(vy);
         while (remaining > 0) {
             const int dd = remaining < vdepth ? remaining : vdepth;
             kern<<<nvtiles, 32 * vy, smem, stream()>>>(a, b, f->r32, f->inv32, f->g.d_dims, f->g.d_off, vtiles, vz,
