@@ -426,35 +426,27 @@ __global__ void k_sor32_half(float *__restrict__ dlt, const float *__restrict__ 
 // z).  A block takes a VX x VY tile of a history's columns over a chunk of
 // its slices [z0, z1) and runs S <= 2 half-sweeps (one sweep) on it in one
 // pass along z: at step t, stage s updates slice t - 2 (s - 1), its pixels
-// of that half-sweep's colour, in place in a ring of slices in shared
-// memory.  Two slices between the stages keep every read at the right
-// level: stage 2 reads slices p - 1, p, p + 1 after stage 1 (slice p + 1 was
-// done a step ago; slice p - 1 holds stage 2's own colour, which stage 2
-// does not read), and no slice a stage reads is written in the same step.
-// The tile's halo is VD pixels across x and y and VD slices along z beyond
-// the chunk; what lies beyond the loaded slices or the tile reads as zero,
-// exact at the history's border and an error that moves in one ring per
-// half-sweep inside it, so every pixel VD or more from such an edge equals
-// S in-place half-sweeps of the whole history (as k_sor32_half gives them,
-// to the bit: the same sums in the same order).  A thread owns a pair of
-// columns (one pixel of each colour per slice).  The correction and both
-// coefficients of slice t + 1 + VP are copied into the ring by cp.async
-// while step t runs (VP slices ahead), one barrier a step.
-constexpr int VX = 64;  // tile columns: 32 lanes x 2
-constexpr int VD = 2;   // half-sweeps per launch at most, and the halo
-constexpr int VP = 3;   // slices copied ahead
-constexpr int VR = 2 * VD + VP + 1;  // ring slots: slices t - 2 VD + 1 .. t + 1 + VP
-
-__device__ __forceinline__ void cp_async4(float *dst, const float *src, bool take) {
-    // 4 bytes, or (take false) a zero written without reading src
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(sh_addr(dst)), "l"(src), "r"(take ? 4 : 0)
-                 : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
-
-constexpr size_t vol_smem_of(int vy) { return (size_t)VR * 3 * vy * VX * sizeof(float); }
+// of that half-sweep's colour, in place in a ring of slices of the
+// correction in shared memory.  Two slices between the stages keep every
+// read at the right level: stage 2 reads slices p - 1, p, p + 1 after stage
+// 1 (slice p + 1 was done a step ago; slice p - 1 holds stage 2's own
+// colour, which stage 2 does not read), and no slice a stage reads is
+// written in the same step.  The tile's halo is VD pixels across x and y and
+// VD slices along z beyond the chunk; what lies beyond the loaded slices or
+// the tile reads as zero, exact at the history's border and an error that
+// moves in one ring per half-sweep inside it, so every pixel VD or more from
+// such an edge equals S in-place half-sweeps of the whole history (as
+// k_sor32_half gives them, to the bit: the same sums in the same order).
+// A thread owns a pair of columns (one pixel of each colour per slice).
+// Its loads run ahead in registers: at step t it loads slice t + 3 (the
+// correction and both coefficients), puts slice t + 2's correction into the
+// ring at the end of the step and keeps the coefficients of slices t - 2 ..
+// t + 3 for the stages that use them, so no stage waits on memory; one
+// barrier a step.
+constexpr int VX = 64;                   // tile columns: 32 lanes x 2
+constexpr int VD = 2;                    // half-sweeps per launch at most, and the halo
+constexpr int VR = 2 * VD + 2;           // ring slots: slices t - 2 VD + 1 .. t + 2
+constexpr size_t vol_smem_of(int vy) { return (size_t)VR * vy * VX * sizeof(float); }
 
 template <int VY>
 __global__ void __launch_bounds__(32 * VY) k_sor32_vol(const float *__restrict__ src, float *__restrict__ dst,
@@ -463,8 +455,8 @@ __global__ void __launch_bounds__(32 * VY) k_sor32_vol(const float *__restrict__
                                                        const int4 *__restrict__ tiles, int vz,
                                                        const float *__restrict__ omega, const int32_t *done,
                                                        int done_stride, int nhalf, int start_colour, int zero_start) {
-    constexpr int PL = VY * VX;               // floats of one slice of one array
-    extern __shared__ __align__(16) float ring[];  // [VR][3: correction, b, a][VY][VX]
+    constexpr int PL = VY * VX;
+    extern __shared__ __align__(16) float ring[];  // [VR][VY][VX]
     const int4 tl = tiles[blockIdx.x];
     const int h = tl.x;
     if (done[(int64_t)h * done_stride]) return;
@@ -485,57 +477,63 @@ __global__ void __launch_bounds__(32 * VY) k_sor32_vol(const float *__restrict__
     const bool out_y = gy >= iy0 && gy < iy1;
     const bool out0 = in0 && out_y && gx >= ix0 && gx < ix1, out1 = in1 && out_y && gx + 1 >= ix0 && gx + 1 < ix1;
     const int me_off = ty * VX + lx;
-    auto slot = [&](int z, int arr) -> float * { return ring + ((z % VR) * 3 + arr) * PL; };
-    // slice z's pair of each array into the ring (zeros outside the history;
-    // the correction zero without reading it on a launch that starts from zero);
-    // one copy group per slice, empty past the chunk's last slice
-    auto issue = [&](int z) {
-        if (z < zhi) {
+    auto slot = [&](int z) -> float * { return ring + (z % VR) * PL + me_off; };
+    const float2 z2 = make_float2(0.f, 0.f);
+    // slice z's pair of an array (zeros outside the history or the chunk's slices)
+    auto pair = [&](const float *a, int z, bool read) -> float2 {
+        float2 v = z2;
+        if (read && z >= zlo && z < zhi) {
             const int64_t i = col + (int64_t)z * plane;
-            const int64_t i0 = in0 ? i : off[h], i1 = in1 ? i + 1 : off[h];  // a valid address when not read
-            float *d = slot(z, 0) + me_off, *b = slot(z, 1) + me_off, *a = slot(z, 2) + me_off;
-            cp_async4(d, src + i0, in0 && !zero_start);
-            cp_async4(d + 1, src + i1, in1 && !zero_start);
-            cp_async4(b, rhs + i0, in0);
-            cp_async4(b + 1, rhs + i1, in1);
-            cp_async4(a, inv + i0, in0);
-            cp_async4(a + 1, inv + i1, in1);
+            if (in0) v.x = __ldg(a + i);
+            if (in1) v.y = __ldg(a + i + 1);
         }
-        cp_async_commit();
+        return v;
     };
-    for (int z = zlo; z <= zlo + VP; ++z) issue(z);
+    // the coefficients of slices t - 2 .. t + 3 (b, a pairs), the correction of
+    // slice t + 2 (loaded a step ago) and t + 3 (this step)
+    float2 b0, b1, b2, b3, b4, b5, a0, a1, a2, a3, a4, a5, dnext, dlast;
+    const int t0 = zlo;
+    b0 = pair(rhs, t0 - 2, true); a0 = pair(inv, t0 - 2, true);
+    b1 = pair(rhs, t0 - 1, true); a1 = pair(inv, t0 - 1, true);
+    b2 = pair(rhs, t0, true);     a2 = pair(inv, t0, true);
+    b3 = pair(rhs, t0 + 1, true); a3 = pair(inv, t0 + 1, true);
+    b4 = pair(rhs, t0 + 2, true); a4 = pair(inv, t0 + 2, true);
+    dnext = pair(src, t0 + 2, !zero_start);
+    *(float2 *)slot(t0) = pair(src, t0, !zero_start);
+    *(float2 *)slot(t0 + 1) = pair(src, t0 + 1, !zero_start);
+    __syncthreads();
     const int tend = zhi - 1 + 2 * (S - 1);
-    for (int t = zlo; t <= tend; ++t) {
-        // slice t + 1 landed (the VP - 1 copies after it may still be in
-        // flight), for every thread; every thread is done with step t - 1
-        cp_async_wait<VP - 1>();
-        __syncthreads();
-        issue(t + 1 + VP);  // its slot last held slice t + 1 + VP - VR, no longer read
-        for (int s = 1; s <= S; ++s) {
+    for (int t = t0; t <= tend; ++t) {
+        // slice t + 3 into registers while the stages run
+        b5 = pair(rhs, t + 3, true);
+        a5 = pair(inv, t + 3, true);
+        dlast = pair(src, t + 3, !zero_start);
+#pragma unroll
+        for (int s = 1; s <= 2; ++s) {
+            if (s > S) break;
             const int p = t - 2 * (s - 1);  // the same for the whole block
             if (p < zlo || p >= zhi) continue;
             const int c = (start_colour + s - 1) & 1;
             // the pixel of colour c in this thread's pair ((x + y + z) mod 2 == c,
             // x0 even): the same e for a warp, which holds one row
             const int e = (c + gy + p) & 1;
-            float2 *row = (float2 *)(slot(p, 0) + me_off);
+            float2 *row = (float2 *)slot(p);
             const float2 me = *row;
             // x neighbours: the left pair's second pixel, the right pair's first
             const float left = __shfl_up_sync(0xffffffffu, me.y, 1);
             const float right = __shfl_down_sync(0xffffffffu, me.x, 1);
-            const float2 z2 = make_float2(0.f, 0.f);
             const float2 ym2 = ty > 0 ? row[-VX / 2] : z2, yp2 = ty + 1 < VY ? row[VX / 2] : z2;
-            const float2 zm2 = p - 1 >= zlo ? *(const float2 *)(slot(p - 1, 0) + me_off) : z2;
-            const float2 zp2 = p + 1 < zhi ? *(const float2 *)(slot(p + 1, 0) + me_off) : z2;
-            const float2 b2 = *(const float2 *)(slot(p, 1) + me_off), a2 = *(const float2 *)(slot(p, 2) + me_off);
+            const float2 zm2 = p - 1 >= zlo ? *(const float2 *)slot(p - 1) : z2;
+            const float2 zp2 = p + 1 < zhi ? *(const float2 *)slot(p + 1) : z2;
+            const float2 bb = s == 1 ? b2 : b0, aa = s == 1 ? a2 : a0;
             if (!(e ? in1 : in0)) continue;  // outside the history: stays zero
             float xm, xp, ym, yp, zm, zp, cur, bv, av;
             if (e == 0) {
                 xm = tx > 0 ? left : 0.f; xp = me.y; ym = ym2.x; yp = yp2.x; zm = zm2.x; zp = zp2.x; cur = me.x;
-                bv = b2.x; av = a2.x;
+                bv = bb.x; av = aa.x;
             } else {
                 xm = me.x; xp = tx < 31 ? right : 0.f; ym = ym2.y; yp = yp2.y; zm = zm2.y; zp = zp2.y; cur = me.y;
-                bv = b2.y; av = a2.y;
+                bv = bb.y; av = aa.y;
             }
             // k_sor32_half's sums, in its order
             float sum = (xm + xp) + (ym + yp);
@@ -546,13 +544,19 @@ __global__ void __launch_bounds__(32 * VY) k_sor32_vol(const float *__restrict__
         // slice t - 2 (S - 1) has had every half-sweep: its interior out
         const int pf = t - 2 * (S - 1);
         if (pf >= z0 && pf < z1) {
-            const float2 q = *(const float2 *)(slot(pf, 0) + me_off);
+            const float2 q = *(const float2 *)slot(pf);
             const int64_t i = col + (int64_t)pf * plane;
             if (out0) dst[i] = q.x;
             if (out1) dst[i + 1] = q.y;
         }
+        // slice t + 2 into the ring: its slot last held slice t - 4, read by no
+        // stage since step t - 1
+        if (t + 2 < zhi) *(float2 *)slot(t + 2) = dnext;
+        dnext = dlast;
+        b0 = b1; b1 = b2; b2 = b3; b3 = b4; b4 = b5;
+        a0 = a1; a1 = a2; a2 = a3; a3 = a4; a4 = a5;
+        __syncthreads();
     }
-    cp_async_wait<0>();  // no copy in flight into shared memory at exit
 }
 
 typedef void (*TbKernel)(const float *, float *, const float *, const float *, const int4 *, const int64_t *,
