@@ -499,7 +499,7 @@ def shape_record(L, cfg, steps, warm, peak):
     # z (k_sor32_vol); a plane's, `depth` half-sweeps on chip: 16 B per site a launch
     alg = sites * SOR_BYTES_PER_SITE_PASS
     gbs = alg / (lm / 1e3) / 1e9
-    rec["sor"] = {"kernel": ("k_sor32_vol<%d> (64x%d tiles marched along z, one sweep per launch)" %
+    rec["sor"] = {"kernel": ("k_sor32_vol<2, %d> (64x%d tiles marched along z, one sweep per launch)" %
                              ((16, 16) if tuned["window"] == 1 else (32, 32))) if volume else
                   f"k_sor32_wide<{depth}> ({depth} half-sweeps per launch on chip)",
                   "launch_ms": round(lm, 4), "alg_bytes_per_launch": int(alg), "achieved_gbs": round(gbs, 1),

@@ -424,46 +424,41 @@ __global__ void k_sor32_half(float *__restrict__ dlt, const float *__restrict__ 
 
 // Temporal blocking in a volume (2.5-D: tiles across x and y marched along
 // z).  A block takes a VX x VY tile of a history's columns over a chunk of
-// its slices [z0, z1) and runs S <= 2 half-sweeps (one sweep) on it in one
-// pass along z: at step t, stage s updates slice t - 2 (s - 1), its pixels
-// of that half-sweep's colour, in place in a ring of slices of the
-// correction in shared memory.  Two slices between the stages keep every
-// read at the right level: stage 2 reads slices p - 1, p, p + 1 after stage
-// 1 (slice p + 1 was done a step ago; slice p - 1 holds stage 2's own
-// colour, which stage 2 does not read), and no slice a stage reads is
-// written in the same step.  The tile's halo is VD pixels across x and y and
-// VD slices along z beyond the chunk; what lies beyond the loaded slices or
-// the tile reads as zero, exact at the history's border and an error that
-// moves in one ring per half-sweep inside it, so every pixel VD or more from
-// such an edge equals S in-place half-sweeps of the whole history (as
-// k_sor32_half gives them, to the bit: the same sums in the same order).
-// A thread owns a pair of columns (one pixel of each colour per slice).
-// Its loads run ahead in registers: at step t it loads slice t + 3 (the
-// correction and both coefficients), puts slice t + 2's correction into the
-// ring at the end of the step and keeps the coefficients of slices t - 2 ..
-// t + 3 for the stages that use them, so no stage waits on memory; one
-// barrier a step.
-constexpr int VX = 64;                   // tile columns: 32 lanes x 2
-constexpr int VD = 2;                    // half-sweeps per launch at most, and the halo
-constexpr int VR = 2 * VD + 2;           // ring slots: slices t - 2 VD + 1 .. t + 2
-constexpr size_t vol_smem_of(int vy) { return (size_t)VR * vy * VX * sizeof(float); }
+// its slices [z0, z1) and runs S <= D half-sweeps on it in one pass along z:
+// at step t, stage s (the s-th half-sweep) updates slice t - 2 (s - 1), its
+// pixels of that half-sweep's colour, in place in a ring of slices in shared
+// memory.  Two slices between stages keep every read at the right level:
+// stage s reads slices p - 1, p, p + 1 after stage s - 1 (slice p + 1 was
+// done a step ago, slice p - 1 holds stage s's own colour, which stage s
+// does not read), and no slice a stage reads is written in the same step.
+// The tile's halo is D pixels across x and y and D slices along z beyond
+// the chunk; what lies beyond the loaded slices or the tile reads as zero,
+// exact at the history's border and an error that moves in one ring per
+// half-sweep inside it, so every pixel D or more from such an edge equals S
+// in-place half-sweeps of the whole history (as k_sor32_half gives them,
+// to the bit: the same sums in the same order).  A thread owns a pair of
+// columns (one pixel of each colour per slice); the next slice is brought
+// into registers while the stages run, then into the ring, one barrier a
+// step.  The stage's coefficients are read from global memory (L1 keeps a
+// slice's for the S steps that use it).
+constexpr int VX = 64;  // tile columns: 32 lanes x 2
 
-template <int VY>
+template <int D, int VY>
 __global__ void __launch_bounds__(32 * VY) k_sor32_vol(const float *__restrict__ src, float *__restrict__ dst,
                                                        const float *__restrict__ rhs, const float *__restrict__ inv,
                                                        const int4 *__restrict__ dims, const int64_t *__restrict__ off,
                                                        const int4 *__restrict__ tiles, int vz,
                                                        const float *__restrict__ omega, const int32_t *done,
                                                        int done_stride, int nhalf, int start_colour, int zero_start) {
-    constexpr int PL = VY * VX;
-    extern __shared__ __align__(16) float ring[];  // [VR][VY][VX]
+    constexpr int R = 2 * D + 2;  // ring slots: slices t - 2 D + 1 .. t + 2 in use at step t
+    extern __shared__ __align__(16) float ring[];  // [R][VY][VX]
     const int4 tl = tiles[blockIdx.x];
     const int h = tl.x;
     if (done[(int64_t)h * done_stride]) return;
     const int4 dm = dims[h];
     const int x0 = tl.y, y0 = tl.z, z0 = tl.w;
     const int z1 = min(z0 + vz, dm.z);
-    const int zlo = max(z0 - VD, 0), zhi = min(z1 + VD, dm.z);
+    const int zlo = max(z0 - D, 0), zhi = min(z1 + D, dm.z);
     const int S = nhalf;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     const int lx = 2 * tx, gx = x0 + lx, gy = y0 + ty;
@@ -472,89 +467,71 @@ __global__ void __launch_bounds__(32 * VY) k_sor32_vol(const float *__restrict__
     const int64_t col = off[h] + (int64_t)gy * dm.x + gx;  // this thread's first pixel in slice 0
     const float omc = 1.f - omega[h];
     // the output interior of the tile (a window edge on the history's border makes no error)
-    const int ix0 = x0 == 0 ? 0 : x0 + VD, ix1 = x0 + VX >= dm.x ? dm.x : x0 + VX - VD;
-    const int iy0 = y0 == 0 ? 0 : y0 + VD, iy1 = y0 + VY >= dm.y ? dm.y : y0 + VY - VD;
+    const int ix0 = x0 == 0 ? 0 : x0 + D, ix1 = x0 + VX >= dm.x ? dm.x : x0 + VX - D;
+    const int iy0 = y0 == 0 ? 0 : y0 + D, iy1 = y0 + VY >= dm.y ? dm.y : y0 + VY - D;
     const bool out_y = gy >= iy0 && gy < iy1;
     const bool out0 = in0 && out_y && gx >= ix0 && gx < ix1, out1 = in1 && out_y && gx + 1 >= ix0 && gx + 1 < ix1;
-    const int me_off = ty * VX + lx;
-    auto slot = [&](int z) -> float * { return ring + (z % VR) * PL + me_off; };
-    const float2 z2 = make_float2(0.f, 0.f);
-    // slice z's pair of an array (zeros outside the history or the chunk's slices)
-    auto pair = [&](const float *a, int z, bool read) -> float2 {
-        float2 v = z2;
-        if (read && z >= zlo && z < zhi) {
+    auto slot = [&](int z) -> float * { return ring + (size_t)(z % R) * (VY * VX); };
+    auto load = [&](int z, float &v0, float &v1) {
+        v0 = v1 = 0.f;
+        if (!zero_start) {
             const int64_t i = col + (int64_t)z * plane;
-            if (in0) v.x = __ldg(a + i);
-            if (in1) v.y = __ldg(a + i + 1);
+            if (in0) v0 = __ldg(src + i);
+            if (in1) v1 = __ldg(src + i + 1);
         }
-        return v;
     };
-    // the coefficients of slices t - 2 .. t + 3 (b, a pairs), the correction of
-    // slice t + 2 (loaded a step ago) and t + 3 (this step)
-    float2 b0, b1, b2, b3, b4, b5, a0, a1, a2, a3, a4, a5, dnext, dlast;
-    const int t0 = zlo;
-    b0 = pair(rhs, t0 - 2, true); a0 = pair(inv, t0 - 2, true);
-    b1 = pair(rhs, t0 - 1, true); a1 = pair(inv, t0 - 1, true);
-    b2 = pair(rhs, t0, true);     a2 = pair(inv, t0, true);
-    b3 = pair(rhs, t0 + 1, true); a3 = pair(inv, t0 + 1, true);
-    b4 = pair(rhs, t0 + 2, true); a4 = pair(inv, t0 + 2, true);
-    dnext = pair(src, t0 + 2, !zero_start);
-    *(float2 *)slot(t0) = pair(src, t0, !zero_start);
-    *(float2 *)slot(t0 + 1) = pair(src, t0 + 1, !zero_start);
+    // the first two slices
+    for (int z = zlo; z < min(zlo + 2, zhi); ++z) {
+        float v0, v1;
+        load(z, v0, v1);
+        ((float2 *)(slot(z) + ty * VX))[tx] = make_float2(v0, v1);
+    }
     __syncthreads();
     const int tend = zhi - 1 + 2 * (S - 1);
-    for (int t = t0; t <= tend; ++t) {
-        // slice t + 3 into registers while the stages run
-        b5 = pair(rhs, t + 3, true);
-        a5 = pair(inv, t + 3, true);
-        dlast = pair(src, t + 3, !zero_start);
-#pragma unroll
-        for (int s = 1; s <= 2; ++s) {
-            if (s > S) break;
+    for (int t = zlo; t <= tend; ++t) {
+        // the slice after next into registers while the stages run
+        const int zn = t + 2;
+        float n0 = 0.f, n1 = 0.f;
+        if (zn < zhi) load(zn, n0, n1);
+        for (int s = 1; s <= S; ++s) {
             const int p = t - 2 * (s - 1);  // the same for the whole block
             if (p < zlo || p >= zhi) continue;
             const int c = (start_colour + s - 1) & 1;
             // the pixel of colour c in this thread's pair ((x + y + z) mod 2 == c,
             // x0 even): the same e for a warp, which holds one row
             const int e = (c + gy + p) & 1;
-            float2 *row = (float2 *)slot(p);
+            float2 *row = (float2 *)(slot(p) + ty * VX) + tx;
             const float2 me = *row;
             // x neighbours: the left pair's second pixel, the right pair's first
             const float left = __shfl_up_sync(0xffffffffu, me.y, 1);
             const float right = __shfl_down_sync(0xffffffffu, me.x, 1);
+            const float2 z2 = make_float2(0.f, 0.f);
             const float2 ym2 = ty > 0 ? row[-VX / 2] : z2, yp2 = ty + 1 < VY ? row[VX / 2] : z2;
-            const float2 zm2 = p - 1 >= zlo ? *(const float2 *)slot(p - 1) : z2;
-            const float2 zp2 = p + 1 < zhi ? *(const float2 *)slot(p + 1) : z2;
-            const float2 bb = s == 1 ? b2 : b0, aa = s == 1 ? a2 : a0;
+            const float2 zm2 = p - 1 >= zlo ? ((const float2 *)(slot(p - 1) + ty * VX))[tx] : z2;
+            const float2 zp2 = p + 1 < zhi ? ((const float2 *)(slot(p + 1) + ty * VX))[tx] : z2;
             if (!(e ? in1 : in0)) continue;  // outside the history: stays zero
-            float xm, xp, ym, yp, zm, zp, cur, bv, av;
+            float xm, xp, ym, yp, zm, zp, cur;
             if (e == 0) {
                 xm = tx > 0 ? left : 0.f; xp = me.y; ym = ym2.x; yp = yp2.x; zm = zm2.x; zp = zp2.x; cur = me.x;
-                bv = bb.x; av = aa.x;
             } else {
                 xm = me.x; xp = tx < 31 ? right : 0.f; ym = ym2.y; yp = yp2.y; zm = zm2.y; zp = zp2.y; cur = me.y;
-                bv = bb.y; av = aa.y;
             }
             // k_sor32_half's sums, in its order
             float sum = (xm + xp) + (ym + yp);
             sum += (zm + zp);
-            const float v = fmaf(av, sum, fmaf(omc, cur, bv));
+            const int64_t i = col + (int64_t)p * plane + e;
+            const float v = fmaf(__ldg(inv + i), sum, fmaf(omc, cur, __ldg(rhs + i)));
             *row = e == 0 ? make_float2(v, me.y) : make_float2(me.x, v);
         }
         // slice t - 2 (S - 1) has had every half-sweep: its interior out
         const int pf = t - 2 * (S - 1);
         if (pf >= z0 && pf < z1) {
-            const float2 q = *(const float2 *)slot(pf);
+            const float2 q = ((const float2 *)(slot(pf) + ty * VX))[tx];
             const int64_t i = col + (int64_t)pf * plane;
             if (out0) dst[i] = q.x;
             if (out1) dst[i + 1] = q.y;
         }
-        // slice t + 2 into the ring: its slot last held slice t - 4, read by no
-        // stage since step t - 1
-        if (t + 2 < zhi) *(float2 *)slot(t + 2) = dnext;
-        dnext = dlast;
-        b0 = b1; b1 = b2; b2 = b3; b3 = b4; b4 = b5;
-        a0 = a1; a1 = a2; a2 = a3; a3 = a4; a4 = a5;
+        if (zn < zhi) ((float2 *)(slot(zn) + ty * VX))[tx] = make_float2(n0, n1);
         __syncthreads();
     }
 }
@@ -587,7 +564,12 @@ WideKernel wide_kernel_of(int depth) {
 typedef void (*VolKernel)(const float *, float *, const float *, const float *, const int4 *, const int64_t *,
                           const int4 *, int, const float *, const int32_t *, int, int, int, int);
 
-VolKernel vol_kernel(int vy) { return vy == 16 ? k_sor32_vol<16> : k_sor32_vol<32>; }
+VolKernel vol_kernel(int depth, int vy) {
+    if (vy == 16) return depth >= 4 ? k_sor32_vol<4, 16> : k_sor32_vol<2, 16>;
+    return depth >= 4 ? k_sor32_vol<4, 32> : k_sor32_vol<2, 32>;
+}
+
+size_t vol_smem(int depth, int vy) { return (size_t)(2 * depth + 2) * vy * VX * sizeof(float); }
 
 WideKernel wide_kernel(int depth, int warps) { return warps == 16 ? wide_kernel_of<16>(depth) : wide_kernel_of<8>(depth); }
 
@@ -669,10 +651,10 @@ int vol_init(Sor32 &s, cw_field_s *f, int window) {
     const Geom &g = f->g;
     for (uint32_t k = 0; k < g.nh; ++k)
         if (g.d[k] < 2) return CW_OK;
-    s.vdepth = VD;
+    s.vdepth = s.depth >= 4 ? 4 : 2;
     s.vy = window == CW_WINDOW_64 ? 16 : 32;
-    VolKernel kern = vol_kernel(s.vy);
-    const size_t smem = vol_smem_of(s.vy);
+    VolKernel kern = vol_kernel(s.vdepth, s.vy);
+    const size_t smem = vol_smem(s.vdepth, s.vy);
     CW_CUDA(cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0, dev = 0, nsm = 0;
     CW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)kern, 32 * s.vy, smem));
@@ -761,8 +743,8 @@ int Sor32::sweeps(cw_field_s *f, int n, const int32_t *done, int done_stride, fl
         // between the buffers; the first launch starts from zero
         float *a = ping, *b = pong;
         int remaining = 2 * n, done_half = 0;
-        VolKernel kern = vol_kernel(vy);
-        const size_t smem = vol_smem_of(vy);
+        VolKernel kern = vol_kernel(vdepth, vy);
+        const size_t smem = vol_smem(vdepth, vy);
         while (remaining > 0) {
             const int dd = remaining < vdepth ? remaining : vdepth;
             kern<<<nvtiles, 32 * vy, smem, stream()>>>(a, b, f->r32, f->inv32, f->g.d_dims, f->g.d_off, vtiles, vz,
