@@ -107,7 +107,7 @@ class SimConfig(C.Structure):
                 ("exposure_on", C.c_int32), ("exposure_off", C.c_int32), ("mutation_rate", C.c_double),
                 ("rewiring", C.c_double), ("field_off", C.c_int32), ("differentiated_type", C.c_int32),
                 ("apoptotic_type", C.c_int32), ("lineage", C.c_int32), ("error_tolerance", C.c_double),
-                ("suppress_before", C.c_int32)]
+                ("suppress_before", C.c_int32), ("tracing", C.c_int32), ("tracing_at", C.c_int32)]
 
 
 P = C.c_void_p
@@ -207,6 +207,7 @@ SIGNATURES = {
     "cw_network_step_clones": (C.c_int, [I32, P, I64, P, P, P, D, I32]),
     "cw_sim_create": (C.c_int, [P, P, P]),
     "cw_sim_set_lesion": (C.c_int, [P, P, C.c_uint32, D, D, D]),
+    "cw_sim_traced": (C.c_int, [P, C.c_uint32, C.c_uint32, P, P, P]),
     "cw_sim_destroy": (C.c_int, [P]),
     "cw_sim_step": (C.c_int, [P, U32]),
     "cw_sim_lattice": (C.c_int, [P, P]),

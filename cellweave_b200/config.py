@@ -19,7 +19,7 @@ at their network's node's level and leaving the layer; a lesion, whose
 cells carry a network of their own from the step it appears at; mutations
 suppressed before a step (drawn and recorded, not made).  Every other
 feature of the file (capillaries, a list of suppressed clones, angiogenesis,
-immunity, tracing) is refused by name.  ``run`` steps it for ``mcs`` steps or until the tissue touches the
+immunity) is refused by name.  ``run`` steps it for ``mcs`` steps or until the tissue touches the
 box's edge, writing measurements.csv and the snapshots as the reference
 does.
 
@@ -41,7 +41,7 @@ import numpy as np
 
 from ._lib import ConfigError
 from .engine import FP64, STOP_MAX_CHANGE, Network, Simulation, load_network_spec
-from .output import MeasurementLog, snapshot, write_snapshot
+from .output import MeasurementLog, TraceLog, snapshot, write_snapshot
 
 # SimConfig's fields without a default (config.rs:12-40) and their defaults
 REQUIRED = ("width", "height", "mcs", "temperature", "snapshot_interval", "output_dir")
@@ -118,9 +118,18 @@ def _refuse(cfg):
         if cfg["depth"] > 1:
             raise ConfigError(f"{name}: a sheet, which is a layer one cell thick, runs only in the plane; "
                               "set depth = 1")
-    for key in ("angiogenesis", "immunity", "tracing"):
+    for key in ("angiogenesis", "immunity"):
         if cfg.get(key) is not None:
             raise ConfigError(f"{name}: `{key}` is not part of the device step")
+    if cfg.get("tracing") is not None:
+        # Tracing (types.rs:208-214) and its check (simulation.rs:614-619)
+        tr = cfg["tracing"]
+        missing = [k for k in ("at", "every") if k not in tr]
+        if missing:
+            raise ConfigError(f"{name}: missing field `{missing[0]}` in the tracing")
+        if int(tr["every"]) == 0:
+            raise ConfigError(f"{name}: tracing every 0 steps: the clones are written down every so many "
+                              "steps, at least one")
     if cfg.get("lesion") is not None:
         # LesionConfig (config.rs:142-160); Lesion checks (simulation.rs:751-770)
         les = cfg["lesion"]
@@ -215,6 +224,8 @@ def simulation_kwargs(cfg, histories=1, seeds=None, subsweeps=4):
         kw.update(mutation_rate=float(cfg["mutation_rate"]), rewiring=float(cfg["rewiring"]))
     if cfg.get("suppress_before") is not None:
         kw["suppress_before"] = int(cfg["suppress_before"])
+    if cfg.get("tracing") is not None:
+        kw["tracing_at"] = int(cfg["tracing"]["at"])
     if cfg.get("waste"):
         kw["waste_production"] = float(cfg["waste"]["production"])
     if cfg.get("necrotic_factor"):
@@ -297,6 +308,8 @@ def run(path, out_dir=None, histories=1, seeds=None, subsweeps=4, steps=None, pr
     out_dir = out_dir or os.path.join(os.path.dirname(cfg["path"]), cfg["output_dir"])
     dirs = [out_dir] if histories == 1 else [os.path.join(out_dir, f"history-{k}") for k in range(histories)]
     logs = [MeasurementLog(d) for d in dirs]
+    tracing = cfg.get("tracing")
+    traces = [TraceLog(d) for d in dirs] if tracing else None
     done = [False] * histories
     n = int(cfg["mcs"] if steps is None else steps)
     taken = 0
@@ -316,6 +329,9 @@ def run(path, out_dir=None, histories=1, seeds=None, subsweeps=4, steps=None, pr
                 continue
             logs[k].record(ms[k])
             mcs = int(ms[k]["mcs"])
+            # the marked clones every `every` steps from the marking (src/main.rs:173-178)
+            if traces and mcs >= int(tracing["at"]) and (mcs - int(tracing["at"])) % int(tracing["every"]) == 0:
+                traces[k].record(mcs, sim.traced_clones(k))
             if edge[k]:
                 done[k] = True
                 write_snapshot(dirs[k], snapshot_of(sim, k, mcs))
@@ -323,7 +339,7 @@ def run(path, out_dir=None, histories=1, seeds=None, subsweeps=4, steps=None, pr
                 write_snapshot(dirs[k], snapshot_of(sim, k, mcs))
         if all(done):
             break
-    for lg in logs:
+    for lg in logs + (traces or []):
         lg.close()
     return dict(steps=taken, reached_edge=done, directories=dirs)
 

@@ -14,6 +14,7 @@
 #include <array>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <random>
 
 #include "cw_internal.cuh"
@@ -68,6 +69,10 @@ struct cw_sim_s {
     std::vector<uint8_t> clone_lesion;  // a lesion's clone, or descended from one
     std::vector<int32_t> clone_parent;
     std::vector<cw_mutation> clone_mutation;
+    // lineage tracing: every record's mark (-1: none), set at the marking
+    // step and carried by daughters
+    bool tracing = false;
+    std::vector<int32_t> h_mark;
     // a lesion (Lesion, simulation.rs:348-360): its network (the caller's), the
     // step it appears at (-1: none), its radius and centre (NaN: the box's)
     cw_network_s *lesion_net = nullptr;
@@ -643,6 +648,7 @@ int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out) {
         return fail(CW_ERR_CONFIG, "the mutation rate and the rewiring share lie in [0, 1]");
     if (c.mutation_rate > 0.0 && !c.divide)
         return fail(CW_ERR_CONFIG, "mutations come at divisions, and this simulation does not divide");
+    if (c.tracing && c.tracing_at < 0) return fail(CW_ERR_CONFIG, "lineage tracing marks the cells at a step, 0 or later");
     if (!net) return fail(CW_ERR_CONFIG, "a simulation needs a network");
     int32_t survival = network_role(net, 1);
     cw_sim_s *s = new cw_sim_s();
@@ -807,7 +813,11 @@ int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out) {
     }
     for (int32_t t : {c.necrotic_type, c.differentiated_type, c.apoptotic_type})
         if (t >= 0 && t < 32) s->leaving |= 1u << t;
-    if (c.mutation_rate > 0.0 || c.lineage) {
+    if (c.tracing) {
+        s->tracing = true;
+        s->h_mark.assign(nc, -1);
+    }
+    if (c.mutation_rate > 0.0 || c.lineage || c.tracing) {
         // every record starts in the founding clone, or (a lineage) every seeded
         // cell founds its own: its clone is its record's index in the batch
         s->track = true;
@@ -1010,7 +1020,7 @@ static int tune_depth(cw_sim_s *s) {
     int bd = 8, bw = CW_WINDOW_AUTO;
     // volumes march tiles along z at two or four half-sweeps a launch
     const bool volume = s->d[0] > 1;
-    for (int w : {CW_WINDOW_AUTO, CW_WINDOW_64})
+    for (int w : {CW_WINDOW_AUTO, CW_WINDOW_64, volume ? CW_WINDOW_64 : CW_WINDOW_TALL})
         for (int d : {volume ? 2 : 6, 4, 8}) {
             float ms = 0.f;
             int64_t launches = 0;
@@ -1079,6 +1089,7 @@ static int evolve_after_division(cw_sim_s *s) {
             if (d < 0) continue;
             const int32_t parent_clone = s->h_clone[c0 + id];
             s->h_clone[c0 + d] = parent_clone;
+            if (s->tracing) s->h_mark[c0 + d] = s->h_mark[c0 + id];  // simulation.rs:1711
             moved = true;
             if (!s->evolve) continue;
             const uint4 r0 = cw::philox((uint32_t)id, step, 6u, 0u, k0, k1);
@@ -1118,6 +1129,40 @@ static int evolve_after_division(cw_sim_s *s) {
         }
     }
     return moved ? upload_clones(s, grown) : CW_OK;
+}
+
+// Whether record g of the batch is in the layer (in_layer, simulation.rs:
+// 2400-2405): holding pixels, and cycling, quiescent or committed to
+// differentiate (not necrotic, not apoptotic).
+static bool in_layer(const cw_sim_s *s, const std::vector<int32_t> &ty, const std::vector<int32_t> &vo, int64_t g) {
+    const cw_sim_config &c = s->cfg;
+    return vo[g] > 0 && ty[g] != c.necrotic_type && !(c.apoptotic_type >= 0 && ty[g] == c.apoptotic_type);
+}
+
+// The records' types and volumes on the host.
+static int records_to_host(cw_sim_s *s, std::vector<int32_t> &ty, std::vector<int32_t> &vo) {
+    ty.resize(s->nc);
+    vo.resize(s->nc);
+    CW_CUDA(cudaMemcpyAsync(ty.data(), s->lat->type, sizeof(int32_t) * s->nc, cudaMemcpyDeviceToHost, stream()));
+    CW_CUDA(cudaMemcpyAsync(vo.data(), s->lat->volume, sizeof(int32_t) * s->nc, cudaMemcpyDeviceToHost, stream()));
+    CW_CUDA(cudaStreamSynchronize(stream()));
+    return CW_OK;
+}
+
+// mark_every_cell (simulation.rs:1908-1918): every cell in the layer takes
+// its own mark (its id less one, the reference's slot), every other record
+// none.  Draws nothing.
+static int mark_every_cell(cw_sim_s *s) {
+    std::vector<int32_t> ty, vo;
+    int rc = records_to_host(s, ty, vo);
+    if (rc != CW_OK) return rc;
+    cw_lattice_s *l = s->lat;
+    for (uint32_t h = 0; h < s->cfg.nh; ++h) {
+        const int64_t c0 = l->cell_off[h], cap = l->cell_off[h + 1] - c0;
+        for (int64_t id = 0; id < cap; ++id)
+            s->h_mark[c0 + id] = id > 0 && in_layer(s, ty, vo, c0 + id) ? (int32_t)(id - 1) : -1;
+    }
+    return CW_OK;
 }
 
 // place_lesion (simulation.rs:1920-1970), before anything else in the step
@@ -1448,6 +1493,8 @@ int cw_sim_step(cw_sim s, uint32_t nsteps) {
     int rc;
     for (uint32_t step = 0; step < nsteps; ++step, ++s->steps) {
         if (s->lesion_net && (int64_t)s->steps == s->lesion_at && (rc = place_lesion(s)) != CW_OK) return rc;
+        if (s->tracing && (int64_t)s->steps == (int64_t)c.tracing_at && (rc = mark_every_cell(s)) != CW_OK)
+            return rc;
         bool solve = c.relax_every <= 1 || (s->steps % (uint32_t)c.relax_every) == 0;
         o.block_depth = s->depth;
         o.window = s->sor_window;
@@ -1656,6 +1703,29 @@ int cw_sim_clone_records(cw_sim s, uint32_t *count, int32_t *parent, cw_mutation
         if (parent) parent[k] = s->clone_parent[k];
         if (mutation) mutation[k] = s->clone_mutation[k];
     }
+    return CW_OK;
+}
+
+int cw_sim_traced(cw_sim s, uint32_t hist, uint32_t cap, uint32_t *marks, uint64_t *cells, uint32_t *n) {
+    CW_SCOPE(s);
+    if (!s->tracing) return fail(CW_ERR_CONFIG, "this simulation traces no lineage");
+    if (hist >= s->cfg.nh) return fail(CW_ERR_NOT_FOUND, "no history " + std::to_string(hist));
+    std::vector<int32_t> ty, vo;
+    int rc = records_to_host(s, ty, vo);
+    if (rc != CW_OK) return rc;
+    const int64_t c0 = s->lat->cell_off[hist], c1 = s->lat->cell_off[hist + 1];
+    std::map<int32_t, uint64_t> count;
+    for (int64_t g = c0 + 1; g < c1; ++g)
+        if (s->h_mark[g] >= 0 && in_layer(s, ty, vo, g)) count[s->h_mark[g]] += 1;
+    uint32_t k = 0;
+    for (const auto &mc : count) {
+        if (k < cap) {
+            if (marks) marks[k] = (uint32_t)mc.first;
+            if (cells) cells[k] = mc.second;
+        }
+        ++k;
+    }
+    *n = k;
     return CW_OK;
 }
 

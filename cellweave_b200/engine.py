@@ -639,7 +639,7 @@ class Simulation:
                  cycle_median=0.0, cycle_spread=0.0, debris_loss=0.0, still_medium=0.0, exposure_intensity=0.0,
                  exposure_uptake=0.0, exposure_start=0, exposure_on=0, exposure_off=0, mutation_rate=0.0,
                  rewiring=0.0, field_off=False, differentiated_type=-1, apoptotic_type=-1, lineage=False,
-                 error_tolerance=0.0, suppress_before=0):
+                 error_tolerance=0.0, suppress_before=0, tracing_at=None):
         self.dims, w, h, z = _dims(dims)
         self._keep = [w, h, z]
         nc = np.array(ncells, np.uint32)
@@ -662,7 +662,8 @@ class Simulation:
                              float(cycle_spread), float(debris_loss), float(still_medium), float(exposure_intensity),
                              float(exposure_uptake), int(exposure_start), int(exposure_on), int(exposure_off),
                              float(mutation_rate), float(rewiring), int(bool(field_off)), int(differentiated_type),
-                             int(apoptotic_type), int(bool(lineage)), float(error_tolerance), int(suppress_before))
+                             int(apoptotic_type), int(bool(lineage)), float(error_tolerance), int(suppress_before),
+                             int(tracing_at is not None), int(tracing_at or 0))
         handle = C.c_void_p()
         call("cw_sim_create", C.byref(cfg), network.handle, C.byref(handle))
         self._h = handle
@@ -760,6 +761,16 @@ class Simulation:
         out = np.zeros(int(n), np.int32)
         call("cw_sim_clones", self._h, int(hist), int(n), ptr(out))
         return out
+
+    def traced_clones(self, hist=0):
+        """traced_clones (simulation.rs:2407-2421): (mark, cells in the layer
+        carrying it) for every mark still carried, in the order of the marks."""
+        n = C.c_uint32()
+        call("cw_sim_traced", self._h, int(hist), 0, None, None, C.byref(n))
+        k = n.value
+        marks, cells = np.zeros(max(k, 1), np.uint32), np.zeros(max(k, 1), np.uint64)
+        call("cw_sim_traced", self._h, int(hist), k, ptr(marks), ptr(cells), C.byref(n))
+        return [(int(marks[i]), int(cells[i])) for i in range(k)]
 
     def clone_records(self):
         """Every clone founded during the run so far, in order: (parent clone,

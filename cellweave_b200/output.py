@@ -61,6 +61,25 @@ class MeasurementLog:
         self.close()
 
 
+TRACE_COLUMNS = "mcs,mark,cells"
+
+
+class TraceLog(MeasurementLog):
+    """TraceLog (output.rs:115-166): traced.csv in `directory`, its header
+    first, then a row per marked clone still in the layer each time the
+    clones are written down."""
+
+    def __init__(self, directory: str):
+        os.makedirs(directory, exist_ok=True)
+        self.path = os.path.join(directory, "traced.csv")
+        self._f = open(self.path, "w", newline="\n")
+        self._f.write(TRACE_COLUMNS + "\n")
+
+    def record(self, mcs: int, clones):
+        for mark, cells in clones:
+            self._f.write(f"{int(mcs)},{int(mark)},{int(cells)}\n")
+
+
 # CellKind (crates/core/src/types.rs:61-76) by the device's type index
 KIND_NAMES = ("Medium", "Tumor", "Normal", "Necrotic", "Differentiated", "Apoptotic")
 

@@ -527,6 +527,12 @@ typedef struct {
                                     clone founded, cw_mutation.suppressed set) but not made: the daughter keeps
                                     its parent's network (Scenario::suppress_before, simulation.rs:240-244,
                                     1671-1694); <= 0: none */
+    int32_t tracing;             /* 1: lineage tracing (Tracing, types.rs:208-214; mark_every_cell,
+                                    simulation.rs:1908-1918): at the start of step tracing_at every cell in the
+                                    layer (holding pixels, neither necrotic nor apoptotic) is marked with its
+                                    record's id less one, and daughters carry their parent's mark
+                                    (cw_sim_traced); 0: none */
+    int32_t tracing_at;
 } cw_sim_config;
 int cw_sim_create(const cw_sim_config *cfg, cw_network net, cw_sim *out);
 /* A lesion (Lesion, simulation.rs:348-360; place_lesion 1920-1970): at the
@@ -555,6 +561,12 @@ int cw_sim_step(cw_sim sim, uint32_t steps);
 int cw_sim_clones(cw_sim sim, uint32_t hist, uint32_t n, int32_t *clone);
 int cw_sim_clone_count(cw_sim sim, uint32_t *nclones);
 int cw_sim_clone_records(cw_sim sim, uint32_t *count, int32_t *parent, cw_mutation *mutation);
+/* traced_clones (simulation.rs:2407-2421) of history `hist`: for every mark
+ * a cell in the layer still carries, in increasing order, the mark and the
+ * cells in the layer carrying it (cycling, quiescent or differentiating,
+ * holding pixels).  *n receives the number of marks; at most `cap` pairs are
+ * written.  Empty before the marking step; CW_ERR_CONFIG without tracing. */
+int cw_sim_traced(cw_sim sim, uint32_t hist, uint32_t cap, uint32_t *marks, uint64_t *cells, uint32_t *n);
 /* What the autotuner chose: the SOR relaxation factor of every history for
  * the oxygen and the signal field (0 until chosen: the reference's rule),
  * the FP32 blocking depth and window (CW_WINDOW_*), and whether it is still

@@ -241,6 +241,9 @@ class CpuHistory:
         self.lesion_at = int(cfg.get("lesion_at", -1))
         self.lesion_radius = float(cfg.get("lesion_radius", 0.0))
         self.lesion_centre = cfg.get("lesion_centre")
+        # lineage tracing (types.rs:208-214): every record's mark, -1 for none
+        self.tracing_at = cfg.get("tracing_at")
+        self.marks = np.full(self.ncap, -1, np.int64)
         # a lineage (a sheet, simulation.rs:780-785): every seeded cell its own
         # clone; its cells step under the one network
         self.lineage = bool(cfg.get("lineage", False))
@@ -273,8 +276,33 @@ class CpuHistory:
                                leaving=self.leaving,
                                clone=self.clone if self._tracked() else None, clone_lesion=self.clone_lesion)
 
+    def _in_layer(self):
+        """in_layer (simulation.rs:2400-2405) of every record: holding pixels,
+        neither necrotic nor apoptotic."""
+        t, vol = self.lat.type, self.lat.volume
+        nec, apop = self.cfg.get("necrotic_type", -1), self.leaving[1]
+        ok = (vol > 0) & (t != nec) if nec >= 0 else vol > 0
+        if apop >= 0:
+            ok &= t != apop
+        ok = ok.copy()
+        ok[0] = False
+        return ok
+
+    def _mark_every_cell(self):
+        """mark_every_cell (simulation.rs:1908-1918): every cell in the layer
+        marked with its slot (its id less one), every other record none."""
+        ids = np.arange(self.ncap)
+        self.marks = np.where(self._in_layer(), ids - 1, -1)
+
+    def traced_clones(self):
+        """traced_clones (simulation.rs:2407-2421): (mark, cells in the layer)."""
+        m = self.marks[self._in_layer() & (self.marks >= 0)]
+        u, c = np.unique(m, return_counts=True)
+        return [(int(a), int(b)) for a, b in zip(u, c)]
+
     def _tracked(self):
-        return self.lineage or self.mutation_rate > 0 or self.lesion_spec is not None
+        return (self.lineage or self.mutation_rate > 0 or self.lesion_spec is not None
+                or self.tracing_at is not None)
 
     def _place_lesion(self):
         """place_lesion (simulation.rs:1920-1970): every living cell whose
@@ -311,6 +339,8 @@ class CpuHistory:
         c = self.cfg
         if self.lesion_spec is not None and self.steps == self.lesion_at:
             self._place_lesion()  # before anything else in the step (simulation.rs:1135-1137)
+        if self.tracing_at is not None and self.steps == self.tracing_at:
+            self._mark_every_cell()  # simulation.rs:1138-1140
         g = self.lat.grid
         t = self.lat.type
         cells = g > 0
@@ -669,6 +699,7 @@ class CpuHistory:
             if d >= 0:
                 self.state[d] = self.state[cid]
                 self.clone[d] = self.clone[cid]
+                self.marks[d] = self.marks[cid]  # simulation.rs:1711
                 if self.mutation_rate > 0.0 and self.div_rng.random() < self.mutation_rate:
                     self._mutate(d)
                 if c.get("cycle_median", 0.0) > 0:

@@ -106,6 +106,17 @@ def test_a_lesion_and_suppressed_mutations_are_read_and_checked(tmp_path):
         C.simulation_kwargs(C.load_sim_config(write(tmp_path, vol)))
 
 
+def test_tracing_is_read_and_checked(tmp_path):
+    # Tracing (types.rs:208-214) and its check (simulation.rs:614-619)
+    sheet = BASE + "oxygen_uptake = 0.0\n[seeding]\nkind = \"sheet\"\nside = 10\n"
+    kw, _ = C.simulation_kwargs(C.load_sim_config(write(tmp_path, sheet + "[tracing]\nat = 30\nevery = 10\n")))
+    assert kw["tracing_at"] == 30
+    with pytest.raises(cw.ConfigError, match="every 0 steps"):
+        C.simulation_kwargs(C.load_sim_config(write(tmp_path, sheet + "[tracing]\nat = 30\nevery = 0\n")))
+    with pytest.raises(cw.ConfigError, match="every"):
+        C.simulation_kwargs(C.load_sim_config(write(tmp_path, sheet + "[tracing]\nat = 30\n")))
+
+
 def test_released_fields_map_onto_the_step(tmp_path):
     cfg = C.load_sim_config(write(tmp_path, BASE + "\n[waste]\nproduction = 0.01\n[necrotic_factor]\n"
                                                    "production = 0.05\nrelease_for = 12\n"))

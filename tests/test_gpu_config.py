@@ -280,6 +280,73 @@ def test_suppressed_mutations_leave_the_run_as_it_was(tmp_path):
         np.testing.assert_array_equal(a.network_state(n, k).view(np.uint64), b.network_state(n, k).view(np.uint64))
 
 
+TRACED_SHEET = ("width = 60\nheight = 60\nmcs = 400\ntemperature = 10.0\nsnapshot_interval = 100\n"
+                "output_dir = \"out\"\noxygen_uptake = 0.0\nnetwork = \"epithelium.toml\"\n"
+                "[seeding]\nkind = \"sheet\"\nside = 10\n[tracing]\nat = {at}\nevery = 10\n")
+
+
+def test_tracing_marks_every_cell_in_the_layer_and_daughters_carry_the_marks(tmp_path):
+    # mark_every_cell (simulation.rs:1908-1918) at step 150 of four sheets:
+    # every cell in the layer carries its own mark (its id less one) and each
+    # mark is one cell; 250 steps on, the marks are carried by the clones the
+    # marked cells made, in the layer, and no cell born after carries a mark
+    # of its own
+    spec = json.load(open(os.path.join(HERE, "golden", "golden.json")))["networks"]["epithelium"]
+    network_file(tmp_path, "epithelium.toml", spec)
+    p = tmp_path / "run.toml"
+    p.write_text(TRACED_SHEET.format(at=150))
+    cfg = C.load_sim_config(str(p))
+    sim, _ = C.simulation_from_config(cfg, histories=4, seeds=[61, 62, 63, 64])
+    sim.step(150)
+    assert all(sim.traced_clones(k) == [] for k in range(4))
+    lat = sim.lattice()
+    layer = []
+    for k in range(4):
+        rec = lat.cells(lat.capacity[k], k)
+        ids = np.nonzero((rec["volume"] > 0) & (rec["type"] != C.NECROTIC) & (rec["type"] != C.APOPTOTIC))[0]
+        layer.append(ids[ids > 0])
+    sim.step(1)
+    for k in range(4):
+        tr = sim.traced_clones(k)
+        # the step after the marking may have taken a cell or two out of the layer
+        marks = {m for m, _ in tr}
+        assert all(c == 1 for _, c in tr) and marks <= {int(i) - 1 for i in layer[k]}
+        assert len(marks) >= len(layer[k]) - 3
+    sim.step(250)
+    for k in range(4):
+        tr = sim.traced_clones(k)
+        assert tr and max(c for _, c in tr) >= 2 and all(m + 1 in set(layer[k].tolist()) for m, _ in tr)
+
+
+def test_traced_clones_grow_inside_the_oracle_band(tmp_path):
+    # epithelium-traced.toml's experiment on a 60 x 60 sheet: every cell marked
+    # at step 100, then the number of marked clones left in the layer and
+    # their mean size, the device's 32 histories against the oracle's
+    spec = json.load(open(os.path.join(HERE, "golden", "golden.json")))["networks"]["epithelium"]
+    network_file(tmp_path, "epithelium.toml", spec)
+    p = tmp_path / "run.toml"
+    p.write_text(TRACED_SHEET.format(at=100))
+    cfg = C.load_sim_config(str(p))
+    seeds = [8_000 + k for k in range(SEEDS)]
+    sim, _ = C.simulation_from_config(cfg, histories=SEEDS, seeds=seeds)
+    kw, _ = C.simulation_kwargs(cfg, SEEDS, seeds)
+    ocfg = dict(kw, network_spec=spec, lambda_volume=float(spec["mechanics"]["lambda_volume"]), hypoxic_level=0.1)
+    ora = [CpuHistory(ocfg, k) for k in range(SEEDS)]
+    for step in range(1, 401):
+        sim.step(1)
+        for h in ora:
+            h.step()
+        if step not in (101, 250, 400):
+            continue
+        dt = [sim.traced_clones(k) for k in range(SEEDS)]
+        ot = [h.traced_clones() for h in ora]
+        for name, f in (("clones", len), ("mean size", lambda t: np.mean([c for _, c in t]) if t else 0.0)):
+            dv = np.array([float(f(t)) for t in dt])
+            rv = np.array([float(f(t)) for t in ot])
+            assert within_band(dv, rv), (step, name, dv.mean(), rv.mean(), rv.std())
+    assert np.mean([len(t) for t in dt]) < 36
+
+
 def test_the_run_writes_the_measurements_of_every_step_and_the_snapshots(tmp_path):
     path, spec = scenario(tmp_path, "")
     out = C.run(path, str(tmp_path / "out"), steps=25)

@@ -20,6 +20,16 @@ def test_the_table_has_a_header_and_one_fixed_width_row_per_step(tmp_path):
     assert len(lines[0].split(",")) == len(lines[1].split(","))
 
 
+def test_the_trace_has_a_header_and_a_row_per_marked_clone(tmp_path):
+    # TraceLog (output.rs:115-166): mcs,mark,cells, one row per clone each time
+    with output.TraceLog(str(tmp_path)) as log:
+        log.record(1000, [(3, 1), (17, 2)])
+        log.record(1010, [])
+        log.record(1020, [(17, 5)])
+    assert (tmp_path / "traced.csv").read_text().splitlines() == [
+        "mcs,mark,cells", "1000,3,1", "1000,17,2", "1020,17,5"]
+
+
 def test_a_device_measurement_fills_the_columns_it_has():
     m = dict(mcs=3, cycling=10, quiescent=2, necrotic=4, born=20, gone=1, vessel=0, tissue_radius=5.5,
              necrotic_radius=2.0, viable_depth=3.5)
