@@ -2,7 +2,7 @@
 """Throughput of cellweave's per-step hot path on B200s.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload campaign|cord]
+                    [--workload campaign|cord|spheroid]
 
 Workload (default ``campaign``): the batched campaign of 64 independent
 histories of uneven sizes (16 each at 128^2, 256^2, 512^2, 1024^2; cells at
@@ -54,7 +54,7 @@ def parse():
     p.add_argument("--steps", type=int, default=100)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--workload", choices=["campaign", "cord"], default="campaign")
+    p.add_argument("--workload", choices=["campaign", "cord", "spheroid"], default="campaign")
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-fit", action="store_true")
@@ -69,7 +69,8 @@ def workload(name, rank=0):
     """The workload's configuration for one rank: every rank its own
     campaign, the same shapes, seeds offset by the rank (disjoint histories)."""
     from cellweave_b200 import synthetic
-    cfg = synthetic.campaign() if name == "campaign" else synthetic.tumour_cord()
+    cfg = (synthetic.campaign() if name == "campaign" else synthetic.tumour_cord() if name == "cord" else
+           synthetic.spheroid_3d())
     cfg["seeds"] = [s + 100_000 * rank for s in cfg["seeds"]]
     return cfg
 
@@ -98,8 +99,12 @@ def config_key(name, cfg):
                 "l2": "inputs larger than L2 (the lattices and fields of one step exceed 126 MB)",
                 "parallelism": "histories batched in one launch per kernel; ranks own disjoint campaigns",
                 "subsweeps": 1}
-    return {"workload": "tumour cord 2048^2, ~40k cells of target 64, 3 types, vessel column, 2 fields to "
-                        "residual 1e-8, 16-species RK4", "histories": 1,
+    if name == "cord":
+        return {"workload": "tumour cord 2048^2, ~40k cells of target 64, 3 types, vessel column, 2 fields to "
+                            "residual 1e-8, 16-species RK4", "histories": 1,
+                "l2": "inputs larger than L2", "parallelism": "one history"}
+    return {"workload": "spheroid 256^3, a ball of radius 40 of 5^3 cells (target 125), 26-neighbour contact, "
+                        "surface constraint, oxygen to residual 1e-9, 12-species RK4", "histories": 1,
             "l2": "inputs larger than L2", "parallelism": "one history"}
 
 
