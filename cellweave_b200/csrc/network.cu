@@ -2,12 +2,11 @@
 //
 // Compilation (from_spec, network.rs:283-445) runs once on the host: names
 // are resolved to indices, terms laid out per node in file order.  The RK4
-// step (rk4, network.rs:777-799) runs one cell per thread, many cells per
-// warp; every cell of a launch walks the same term list, so a warp never
-// diverges on the network's shape.  Each thread keeps its state, midpoint,
-// stage slope and accumulated slope in shared memory laid out [node][thread],
-// so dynamic node indices cost a shared-memory access and no bank conflict.
-// Built without fused multiply-add: the sums round as the reference's do.
+// step (rk4, network.rs:777-799) runs a lane per node: 8, 16 or 32 lanes hold
+// one cell (four, two or one cells a warp), each lane its node's state,
+// midpoint and accumulated slope in registers, source nodes read across the
+// cell's lanes by shuffle (k_rk4_lanes).  Built without fused multiply-add:
+// the sums round as the reference's do.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -25,92 +24,121 @@ const char *INPUTS[6] = {"oxygen", "egf", "crowding", "stress", "waste", "necrot
 
 constexpr int MAXS = 32;
 
-constexpr int RT = 64;  // threads (cells) per block
-
-// One cell's `substeps` RK4 steps (rk4, network.rs:777-799) on its column of
-// the block's shared arrays (xs: state, ms: midpoint, ks: stage slope, as:
-// accumulated slope, each [node][RT]), under the terms at sterm/spar/sptr.
-__device__ __forceinline__ void rk4_cell(const NetDev &N, const int4 *sterm, const double4 *spar, const int32_t *sptr,
-                                         double *xs, double *ms, double *ks, double *as, const double *in, double dt,
-                                         int substeps) {
-    const int S = N.S;
-    for (int sub = 0; sub < substeps; ++sub) {
-        // k1 at x
-        derivatives(N, sterm, spar, sptr, xs, in, ks, RT);
-        for (int i = 0; i < S; ++i) {
-            double k1 = ks[i * RT];
-            as[i * RT] = k1;
-            ms[i * RT] = xs[i * RT] + 0.5 * dt * k1;
-        }
-        // k2 at x + dt/2 k1, k3 at x + dt/2 k2, k4 at x + dt k3
-        for (int stage = 1; stage < 4; ++stage) {
-            derivatives(N, sterm, spar, sptr, ms, in, ks, RT);
-            double step = stage < 2 ? 0.5 * dt : dt;
-            for (int i = 0; i < S; ++i) {
-                double kv = ks[i * RT];
-                if (stage < 3) {
-                    as[i * RT] = as[i * RT] + 2.0 * kv;
-                    ms[i * RT] = xs[i * RT] + step * kv;
-                } else {
-                    as[i * RT] = as[i * RT] + kv;
-                }
-            }
-        }
-        for (int i = 0; i < S; ++i) {
-            double delta = (dt / 6.0) * as[i * RT];
-            xs[i * RT] = fmin(fmax(xs[i * RT] + delta, 0.0), 1.0);
-        }
-    }
-}
-
-// state: [S][ncells] (node-major, coalesced); inputs: [6][ncells].
-// alive (optional): cells whose entry is zero are left as they are.
-__global__ void __launch_bounds__(RT) k_rk4(NetDev N, double *state, const double *inputs, int64_t ncells,
-                                            int64_t state_stride, int64_t input_stride, double dt, int substeps,
-                                            const uint8_t *alive) {
-    extern __shared__ double sm[];
-    const int S = N.S;
-    double *x = sm, *mid = sm + S * RT, *kk = sm + 2 * S * RT, *acc = sm + 3 * S * RT;
-    int4 *sterm = (int4 *)(sm + 4 * S * RT);
-    double4 *spar = (double4 *)(sterm + N.nterms);
-    int32_t *sptr = (int32_t *)(spar + N.nterms);
-    for (int t = threadIdx.x; t < N.nterms; t += RT) { sterm[t] = N.term[t]; spar[t] = N.par[t]; }
-    for (int t = threadIdx.x; t <= S; t += RT) sptr[t] = N.node_ptr[t];
-    __syncthreads();
-    int64_t c = (int64_t)blockIdx.x * RT + threadIdx.x;
-    if (c >= ncells) return;
-    if (alive && !alive[c]) return;
-    const int tid = threadIdx.x;
-    double in[6];
-    for (int q = 0; q < 6; ++q) in[q] = inputs[q * input_stride + c];
-    double *xs = x + tid, *ms = mid + tid, *ks = kk + tid, *as = acc + tid;
-    for (int i = 0; i < S; ++i) xs[i * RT] = state[i * state_stride + c];
-    rk4_cell(N, sterm, spar, sptr, xs, ms, ks, as, in, dt, substeps);
-    for (int i = 0; i < S; ++i) state[i * state_stride + c] = xs[i * RT];
-}
-
-// The same for cells of many networks: cell c under nets[clone[c]], its
-// terms read from global memory (a network's tables are a few KB: they stay
-// in L1 across the block's cells of that network).
-// state: [S][state_stride], inputs: [6][input_stride]; alive (optional):
-// cells whose entry is zero are left as they are.
-__global__ void __launch_bounds__(RT) k_rk4_clones(const NetDev *nets, const int32_t *clone, int S, double *state,
+// RK4 with a lane per node (derivatives and term_rate, network.rs:686-734;
+// rk4, 777-799): W lanes (W >= S, a power of two) hold one cell, lane i its
+// node i's state, midpoint and accumulated slope in registers; a node's
+// terms read their source nodes from the other lanes by shuffle.  A term
+// loop runs to the most terms any node of the warp has, every lane taking
+// part in each shuffle, and a lane adds its own node's terms in file order:
+// the same operations in the same order as one cell per thread, to the bit.
+// nets null: every cell under N; else cell c under nets[clone[c]].
+template <int W>
+__global__ void __launch_bounds__(128) k_rk4_lanes(NetDev N, const NetDev *nets, const int32_t *clone, double *state,
                                                    const double *inputs, int64_t ncells, int64_t state_stride,
                                                    int64_t input_stride, double dt, int substeps,
                                                    const uint8_t *alive) {
-    extern __shared__ double sm[];
-    double *x = sm, *mid = sm + S * RT, *kk = sm + 2 * S * RT, *acc = sm + 3 * S * RT;
-    int64_t c = (int64_t)blockIdx.x * RT + threadIdx.x;
-    if (c >= ncells) return;
-    if (alive && !alive[c]) return;
-    const NetDev N = nets[clone[c]];
-    const int tid = threadIdx.x;
+    const int lane = threadIdx.x & 31, node = lane % W, base = lane - node;
+    const int64_t c = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / W;
+    const bool cell = c < ncells;
+    const NetDev M = (nets && cell) ? nets[clone[c]] : N;
+    const int S = M.S;
+    const bool live = cell && node < S && !(alive && !alive[c]);
+    int p0 = 0, cnt = 0;
+    if (cell && node < S) {
+        p0 = M.node_ptr[node];
+        cnt = M.node_ptr[node + 1] - p0;
+    }
+    int tmax = cnt;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) tmax = max(tmax, __shfl_xor_sync(0xffffffffu, tmax, o));
     double in[6];
-    for (int q = 0; q < 6; ++q) in[q] = inputs[q * input_stride + c];
-    double *xs = x + tid, *ms = mid + tid, *ks = kk + tid, *as = acc + tid;
-    for (int i = 0; i < S; ++i) xs[i * RT] = state[i * state_stride + c];
-    rk4_cell(N, N.term, N.par, N.node_ptr, xs, ms, ks, as, in, dt, substeps);
-    for (int i = 0; i < S; ++i) state[i * state_stride + c] = xs[i * RT];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) in[q] = cell ? inputs[q * input_stride + c] : 0.0;
+    double x = live ? state[node * state_stride + c] : 0.0;
+    // the rate of this lane's node at the cell's values v (one value a lane)
+    auto rate_of = [&](double own) -> double {
+        double rate = 0.0;
+        for (int t = 0; t < tmax; ++t) {
+            const bool has = t < cnt;
+            const int4 tm = has ? M.term[p0 + t] : make_int4(-1, -1, 0, 0);
+            const int from = (has && tm.y >= 0 && tm.y < S) ? base + tm.y : lane;
+            const double nodev = __shfl_sync(0xffffffffu, own, from);
+            if (!has) continue;
+            const double4 p = M.par[p0 + t];
+            // read, network.rs:670-680
+            double s = 0.0;
+            if (tm.y >= 0) s = nodev;
+            else switch (-1 - tm.y) {
+                case 0: s = fmin(fmax(in[0], 0.0), 1.0); break;
+                case 1: s = in[1]; break;
+                case 2: s = fmin(fmax(in[2], 0.0), 1.0); break;
+                case 3: s = fmax(in[3], 0.0); break;
+                case 4: s = fmax(in[4], 0.0); break;
+                default: s = fmax(in[5], 0.0); break;
+                }
+            const double k = p.x;
+            double r;
+            switch (tm.x) {
+            case CW_ACTIVATED_BY: {
+                const double drv = tm.z ? hill(s, p.y, p.z) : s;
+                r = k * drv * (1.0 - own);
+                break;
+            }
+            case CW_INHIBITED_BY: {
+                const double drv = tm.z ? hill(s, p.y, p.z) : s;
+                r = -k * drv * own;
+                break;
+            }
+            case CW_ACTIVATED_BY_ABSENCE_OF: r = k * (1.0 - s) * (1.0 - own); break;
+            case CW_PRODUCED_BY: r = k * s; break;
+            case CW_DECAYS: r = -k * own; break;
+            case CW_RELAXES_TO: r = -k * (own - p.w); break;
+            case CW_DAMAGED_BELOW: r = -k * fmax((p.w - s) / p.w, 0.0); break;
+            default: r = -k * fmax((s - p.w) / p.w, 0.0); break;
+            }
+            rate += r;
+        }
+        return rate;
+    };
+    for (int sub = 0; sub < substeps; ++sub) {
+        // k1 at x
+        double k1 = rate_of(x);
+        double acc = k1;
+        double mid = x + 0.5 * dt * k1;
+        // k2 at x + dt/2 k1, k3 at x + dt/2 k2, k4 at x + dt k3
+        for (int stage = 1; stage < 4; ++stage) {
+            const double kv = rate_of(mid);
+            const double step = stage < 2 ? 0.5 * dt : dt;
+            if (stage < 3) {
+                acc = acc + 2.0 * kv;
+                mid = x + step * kv;
+            } else {
+                acc = acc + kv;
+            }
+        }
+        const double delta = (dt / 6.0) * acc;
+        x = fmin(fmax(x + delta, 0.0), 1.0);
+    }
+    if (live) state[node * state_stride + c] = x;
+}
+
+int rk4_lanes(const NetDev &N, const NetDev *nets, const int32_t *clone, int S, double *state, const double *inputs,
+              int64_t ncells, int64_t state_stride, int64_t input_stride, double dt, int substeps,
+              const uint8_t *alive) {
+    const int W = S <= 8 ? 8 : S <= 16 ? 16 : 32;
+    const int64_t threads = ncells * W;
+    const unsigned grid = (unsigned)((threads + 127) / 128);
+    if (W == 8)
+        k_rk4_lanes<8><<<grid, 128, 0, stream()>>>(N, nets, clone, state, inputs, ncells, state_stride, input_stride,
+                                                   dt, substeps, alive);
+    else if (W == 16)
+        k_rk4_lanes<16><<<grid, 128, 0, stream()>>>(N, nets, clone, state, inputs, ncells, state_stride,
+                                                    input_stride, dt, substeps, alive);
+    else
+        k_rk4_lanes<32><<<grid, 128, 0, stream()>>>(N, nets, clone, state, inputs, ncells, state_stride,
+                                                    input_stride, dt, substeps, alive);
+    CW_LAUNCHED();
+    return CW_OK;
 }
 
 // mechanics, network.rs:811-821.
@@ -125,10 +153,6 @@ __global__ void k_mechanics(const double *state, int64_t ncells, int64_t stride,
     target[c] = isnan(t) ? 0u : (t >= 4294967295.0 ? 4294967295u : (uint32_t)t);
 }
 
-size_t rk4_smem(const cw_network_s *n) {
-    return sizeof(double) * 4 * n->S * RT + n->nterms * (sizeof(int4) + sizeof(double4)) + sizeof(int32_t) * (n->S + 1);
-}
-
 // The device copies of a network's host tables (h_ptr, h_term, h_par).
 int network_upload(cw_network_s *n) {
     n->nterms = (int32_t)n->h_term.size();
@@ -141,10 +165,6 @@ int network_upload(cw_network_s *n) {
         CW_CUDA(cudaMemcpy(n->term, n->h_term.data(), sizeof(int4) * n->nterms, cudaMemcpyHostToDevice));
         CW_CUDA(cudaMemcpy(n->par, n->h_par.data(), sizeof(double4) * n->nterms, cudaMemcpyHostToDevice));
     }
-    size_t smem = rk4_smem(n);
-    if (smem > 48 * 1024 &&
-        cudaFuncSetAttribute(k_rk4, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-        return fail(CW_ERR_CONFIG, "the network is too large for one block's shared memory");
     return CW_OK;
 }
 
@@ -197,11 +217,8 @@ NetDev net_dev(const cw_network_s *n) { return NetDev{n->node_ptr, n->term, n->p
 int network_step_device(const cw_network_s *n, double *state, const double *inputs, int64_t ncells,
                         int64_t state_stride, int64_t input_stride, double dt, int substeps, const uint8_t *alive) {
     if (ncells <= 0) return CW_OK;
-    size_t smem = rk4_smem(n);
-    k_rk4<<<(unsigned)((ncells + RT - 1) / RT), RT, smem, stream()>>>(net_dev(n), state, inputs, ncells, state_stride,
-                                                                      input_stride, dt, substeps, alive);
-    CW_LAUNCHED();
-    return CW_OK;
+    return rk4_lanes(net_dev(n), nullptr, nullptr, n->S, state, inputs, ncells, state_stride, input_stride, dt,
+                     substeps, alive);
 }
 
 // RK4 for cells of many networks on node-major state (the driver's evolving
@@ -210,14 +227,9 @@ int network_step_clones_device(const NetDev *nets, const int32_t *clone, int S, 
                                int64_t ncells, int64_t state_stride, int64_t input_stride, double dt, int substeps,
                                const uint8_t *alive) {
     if (ncells <= 0) return CW_OK;
-    const size_t smem = sizeof(double) * 4 * S * RT;
-    if (smem > 48 * 1024)
-        CW_CUDA(cudaFuncSetAttribute(k_rk4_clones, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_rk4_clones<<<(unsigned)((ncells + RT - 1) / RT), RT, smem, stream()>>>(nets, clone, S, state, inputs, ncells,
-                                                                          state_stride, input_stride, dt, substeps,
-                                                                          alive);
-    CW_LAUNCHED();
-    return CW_OK;
+    NetDev none{};
+    none.S = S;
+    return rk4_lanes(none, nets, clone, S, state, inputs, ncells, state_stride, input_stride, dt, substeps, alive);
 }
 
 int network_mechanics_device(const cw_network_s *n, const double *state, int64_t ncells, int64_t stride,
@@ -500,9 +512,6 @@ int cw_network_step_clones(int32_t nnets, const cw_network *nets, int64_t ncells
         if (clone[c] < 0 || clone[c] >= nnets)
             return fail(CW_ERR_CONFIG, "cell " + std::to_string(c) + " names network " + std::to_string(clone[c]) +
                                            " of " + std::to_string(nnets));
-    const size_t smem = sizeof(double) * 4 * S * RT;
-    if (smem > 48 * 1024)
-        CW_CUDA(cudaFuncSetAttribute(k_rk4_clones, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     NetDev *d_nets;
     int32_t *d_clone;
     double *d_state, *d_in;
@@ -519,9 +528,11 @@ int cw_network_step_clones(int32_t nnets, const cw_network *nets, int64_t ncells
     CW_CUDA(cudaMemcpy(d_in, t.data(), sizeof(double) * ncells * 6, cudaMemcpyHostToDevice));
     CW_CUDA(cudaMemcpy(d_nets, dev.data(), sizeof(NetDev) * nnets, cudaMemcpyHostToDevice));
     CW_CUDA(cudaMemcpy(d_clone, clone, sizeof(int32_t) * ncells, cudaMemcpyHostToDevice));
-    k_rk4_clones<<<(unsigned)((ncells + RT - 1) / RT), RT, smem, stream()>>>(d_nets, d_clone, S, d_state, d_in, ncells,
-                                                                          ncells, ncells, dt, substeps, nullptr);
-    CW_LAUNCHED();
+    NetDev none{};
+    none.S = S;
+    if ((rc = rk4_lanes(none, d_nets, d_clone, S, d_state, d_in, ncells, ncells, ncells, dt, substeps, nullptr)) !=
+        CW_OK)
+        return rc;
     CW_CUDA(cudaGetLastError());
     CW_CUDA(cudaMemcpyAsync(t.data(), d_state, sizeof(double) * ncells * S, cudaMemcpyDeviceToHost, stream()));
     CW_CUDA(cudaStreamSynchronize(stream()));
