@@ -83,7 +83,7 @@ __global__ void k_fit_inputs(const double *mean, int64_t nc, double egf, double 
 }
 
 // One RK4 step of the thread's cell (rk4, network.rs:777-799) on shared
-// columns x (in/out), with k and m as scratch: the same arithmetic as k_rk4.
+// columns x (in/out), with k and m as scratch: the same arithmetic as k_rk4_lanes.
 __device__ void rk4_step(const NetDev &N, const int4 *sterm, const double4 *spar, const int32_t *sptr, double *x,
                          double *m, double *k, double *acc, const double *in, double dt) {
     const int S = N.S;
