@@ -415,7 +415,8 @@ def run_ours(args, rank, world, dist):
     if not args.no_shapes and world == 1:
         from cellweave_b200 import synthetic
         shapes = {"cord2048": shape_record(L, synthetic.tumour_cord(), 10, 4, peak),
-                  "spheroid256": shape_record(L, synthetic.spheroid_3d(), 6, 3, peak)}
+                  # nine warm-up steps: the autotuner tries its seven factors on a lone history one step each
+                  "spheroid256": shape_record(L, synthetic.spheroid_3d(), 6, 9, peak)}
     fit = None
     if not args.no_fit and world == 1:
         fit = run_fit(args, L)

@@ -955,7 +955,10 @@ int cw_sim_destroy(cw_sim s) {
 // candidate; afterwards every history takes its class's best factor.
 static void tune_begin(cw_sim_s *s) {
     auto &t = s->tune;
-    t.cand = {1.80, 1.85, 1.88, 1.90, 1.92, 1.94, 1.96};
+    // volumes take larger factors (the reference's rule gives 1.94 for a span
+    // of 100 voxels, 1.976 for 256)
+    if (s->d[0] > 1) t.cand = {1.88, 1.91, 1.93, 1.95, 1.96, 1.97, 1.98};
+    else t.cand = {1.80, 1.85, 1.88, 1.90, 1.92, 1.94, 1.96};
     uint32_t nh = s->cfg.nh;
     t.cls.assign(nh, 0);
     t.rank.assign(nh, 0);
@@ -1489,7 +1492,9 @@ int cw_sim_step(cw_sim s, uint32_t nsteps) {
     o.error_tolerance = c.error_tolerance;
     o.max_sweeps = 200000;
     o.precision = c.precision;
-    o.inner_sweeps = c.inner_sweeps > 0 ? c.inner_sweeps : 32;
+    // a volume's solve takes hundreds of sweeps: 64 a correction halves its
+    // residual and correction passes
+    o.inner_sweeps = c.inner_sweeps > 0 ? c.inner_sweeps : (s->d[0] > 1 ? 64 : 32);
     int rc;
     for (uint32_t step = 0; step < nsteps; ++step, ++s->steps) {
         if (s->lesion_net && (int64_t)s->steps == s->lesion_at && (rc = place_lesion(s)) != CW_OK) return rc;
