@@ -1079,6 +1079,15 @@ static int dc_outer(cw_field_s *f, DcCache *c, RelaxState *d_st, int inner, int6
     const int stride = (int)(sizeof(RelaxState) / sizeof(int32_t));
     k_dc_check<<<(nh + 63) / 64, 64, 0, stream()>>>(d_st, nh, inner, max_sweeps, c->solver.wide ? 1 : 0);
     CW_LAUNCHED();
+    if (c->solver.vol) {
+        // volumes: the last sweep launch adds the correction to c, then the
+        // residual at the corrected field in one pass
+        int rc = c->solver.sweeps(f, inner, done_ptr, stride, start, true);
+        if (rc != CW_OK) return rc;
+        dc_residual(c, fv, nh, d_st, f->r32, nullptr, nullptr);
+        CW_LAUNCHED();
+        return CW_OK;
+    }
     if (c->solver.wide) {
         // the last sweep launch adds the correction to c, recording its
         // largest size and the largest |c| for the error estimate; then the

@@ -449,7 +449,8 @@ __global__ void __launch_bounds__(32 * VY) k_sor32_vol(const float *__restrict__
                                                        const int4 *__restrict__ dims, const int64_t *__restrict__ off,
                                                        const int4 *__restrict__ tiles, int vz,
                                                        const float *__restrict__ omega, const int32_t *done,
-                                                       int done_stride, int nhalf, int start_colour, int zero_start) {
+                                                       int done_stride, int nhalf, int start_colour, int zero_start,
+                                                       double *__restrict__ apply_c, int floor) {
     constexpr int R = 2 * D + 2;  // ring slots: slices t - 2 D + 1 .. t + 2 in use at step t
     extern __shared__ __align__(16) float ring[];  // [R][VY][VX]
     const int4 tl = tiles[blockIdx.x];
@@ -528,8 +529,22 @@ __global__ void __launch_bounds__(32 * VY) k_sor32_vol(const float *__restrict__
         if (pf >= z0 && pf < z1) {
             const float2 q = ((const float2 *)(slot(pf) + ty * VX))[tx];
             const int64_t i = col + (int64_t)pf * plane;
-            if (out0) dst[i] = q.x;
-            if (out1) dst[i + 1] = q.y;
+            if (apply_c) {
+                // the last launch of a correction: c += d on the free pixels
+                // (a held pixel has a = 0 and d = 0 throughout), floored as
+                // the reference's update is (pde.rs:395)
+                if (out0 && (q.x != 0.f || __ldg(inv + i) != 0.f)) {
+                    const double v = apply_c[i] + (double)q.x;
+                    apply_c[i] = floor ? fmax(v, 0.0) : v;
+                }
+                if (out1 && (q.y != 0.f || __ldg(inv + i + 1) != 0.f)) {
+                    const double v = apply_c[i + 1] + (double)q.y;
+                    apply_c[i + 1] = floor ? fmax(v, 0.0) : v;
+                }
+            } else {
+                if (out0) dst[i] = q.x;
+                if (out1) dst[i + 1] = q.y;
+            }
         }
         if (zn < zhi) ((float2 *)(slot(zn) + ty * VX))[tx] = make_float2(n0, n1);
         __syncthreads();
@@ -562,7 +577,7 @@ WideKernel wide_kernel_of(int depth) {
 }
 
 typedef void (*VolKernel)(const float *, float *, const float *, const float *, const int4 *, const int64_t *,
-                          const int4 *, int, const float *, const int32_t *, int, int, int, int);
+                          const int4 *, int, const float *, const int32_t *, int, int, int, int, double *, int);
 
 VolKernel vol_kernel(int depth, int vy) {
     if (vy == 16) return depth >= 4 ? k_sor32_vol<4, 16> : k_sor32_vol<2, 16>;
@@ -733,7 +748,7 @@ int Sor32::init(cw_field_s *f, int d, const std::vector<double> &om, int window)
 
 int Sor32::sweeps(cw_field_s *f, int n, const int32_t *done, int done_stride, float *start, bool apply,
                   unsigned long long *corr, int corr_stride) {
-    if (apply && !wide) return fail(CW_ERR_CONFIG, "only the wide FP32 kernel applies its correction");
+    if (apply && !wide && !vol) return fail(CW_ERR_CONFIG, "only the wide and volume FP32 kernels apply their correction");
     if (start) {  // begin from this (zeroed) buffer; the other is scratch
         ping = start;
         pong = start == f->d32a ? f->d32b : f->d32a;
@@ -747,15 +762,18 @@ int Sor32::sweeps(cw_field_s *f, int n, const int32_t *done, int done_stride, fl
         const size_t smem = vol_smem(vdepth, vy);
         while (remaining > 0) {
             const int dd = remaining < vdepth ? remaining : vdepth;
+            // with `apply` the last launch adds its correction to the field
+            const bool last = remaining == dd;
             kern<<<nvtiles, 32 * vy, smem, stream()>>>(a, b, f->r32, f->inv32, f->g.d_dims, f->g.d_off, vtiles, vz,
                                                        omega, done, done_stride, dd, done_half & 1,
-                                                       done_half == 0 ? 1 : 0);
+                                                       done_half == 0 ? 1 : 0, apply && last ? f->c : nullptr,
+                                                       f->floor ? 1 : 0);
             CW_LAUNCHED();
             remaining -= dd;
             done_half += dd;
             float *t = a; a = b; b = t;
         }
-        out = a;
+        out = apply ? nullptr : a;
         return CW_OK;
     }
     if (!blocked) {
