@@ -803,71 +803,50 @@ __global__ void __launch_bounds__(RT_THREADS, 2)
         const double den4 = 4.0 * fv.d + fv.decay;
         const int row = warp, y = v.t.y0 + row;
         double worst = 0.0;
-        // a lane takes four consecutive pixels of the row: the values, held
-        // bytes and coefficients come in 16- and 4-byte words, the outputs go
-        // out as float4 (rows start on 16 bytes: widths and offsets are
-        // multiples of 16, tiles start at multiples of 128, so four pixels
-        // are all inside the history or all outside)
-        const int col = 4 * lane, x = v.t.x0 + col;
-        if (y < v.t.ht && x < v.t.w) {
-            const int64_t i = v.t.off + (int64_t)y * v.t.w + x;
-            const int k = row * RT_X + col;
-            const double *p = sc + (row + 1) * RT_CX + (col + 2);
-            const double2 c01 = *(const double2 *)p, c23 = *(const double2 *)(p + 2);
-            const double cv[4] = {c01.x, c01.y, c23.x, c23.y};
-            // the sums of pixels with all four neighbours (pixel_sums64's order
-            // onto zero: x-1, x+1, y-1, y+1), from the rows' 16-byte words
-            double s4[4];
-            {
-                const double2 u01 = *(const double2 *)(p - RT_CX), u23 = *(const double2 *)(p - RT_CX + 2);
-                const double2 d01 = *(const double2 *)(p + RT_CX), d23 = *(const double2 *)(p + RT_CX + 2);
-                s4[0] = ((0.0 + p[-1]) + c01.y) + u01.x;
-                s4[1] = ((0.0 + c01.x) + c23.x) + u01.y;
-                s4[2] = ((0.0 + c01.y) + c23.y) + u23.x;
-                s4[3] = ((0.0 + c23.x) + p[4]) + u23.y;
-                s4[0] = s4[0] + d01.x;
-                s4[1] = s4[1] + d01.y;
-                s4[2] = s4[2] + d23.x;
-                s4[3] = s4[3] + d23.y;
-            }
-            const uchar4 hb = *(const uchar4 *)(sheld + k);
-            const uint8_t held4[4] = {hb.x, hb.y, hb.z, hb.w};
-            const bool inner_y = y > 0 && y + 1 < v.t.ht;
-            float r_out[4], inv_out[4];
+        if (y < v.t.ht) {
+            const int64_t rowbase = v.t.off + (int64_t)y * v.t.w;
 #pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                r_out[e] = inv_out[e] = 0.0f;
-                if (held4[e]) continue;
-                const int xe = x + e;
-                double sum, den;
-                if (inner_y && xe > 0 && xe + 1 < v.t.w) {
-                    // a pixel with all four neighbours real has real = 4, and
+            for (int j = 0; j < RT_X / 32; ++j) {
+                const int col = lane + 32 * j, x = v.t.x0 + col, k = row * RT_X + col;
+                if (x >= v.t.w) continue;
+                const int64_t i = rowbase + x;
+                float r_out = 0.0f, inv_out = 0.0f;
+                if (!sheld[k]) {
+                    // pixel_sums64's order onto zero: x-1, x+1, y-1, y+1; a
+                    // pixel with all four neighbours real has real = 4, and
                     // real d + decay is then one number
-                    sum = s4[e];
-                    den = den4;
-                } else {
-                    const double *q = p + e;
-                    double real = 0.0;
-                    sum = 0.0;
-                    if (xe > 0) { sum += q[-1]; real += 1.0; }
-                    if (xe + 1 < v.t.w) { sum += q[1]; real += 1.0; }
-                    if (y > 0) { sum += q[-RT_CX]; real += 1.0; }
-                    if (y + 1 < v.t.ht) { sum += q[RT_CX]; real += 1.0; }
-                    den = real * fv.d + fv.decay;
+                    const double *p = sc + (row + 1) * RT_CX + (col + 2);
+                    double sum, den;
+                    if (x > 0 && x + 1 < v.t.w && y > 0 && y + 1 < v.t.ht) {
+                        sum = 0.0 + p[-1];
+                        sum = sum + p[1];
+                        sum = sum + p[-RT_CX];
+                        sum = sum + p[RT_CX];
+                        den = den4;
+                    } else {
+                        double real = 0.0;
+                        sum = 0.0;
+                        if (x > 0) { sum += p[-1]; real += 1.0; }
+                        if (x + 1 < v.t.w) { sum += p[1]; real += 1.0; }
+                        if (y > 0) { sum += p[-RT_CX]; real += 1.0; }
+                        if (y + 1 < v.t.ht) { sum += p[RT_CX]; real += 1.0; }
+                        den = real * fv.d + fv.decay;
+                    }
+                    if (a.o_ks >= 0) den = den + sks[k];
+                    const double cv = p[0];
+                    // add_sources' order
+                    double t = fv.d * sum + fv.source;
+                    if (a.o_pr >= 0) t = t + spr[k];
+                    if (a.o_up >= 0) t = t - sup[k];
+                    double r = t - den * cv;
+                    if (fv.floor && cv <= 0.0 && r < 0.0) r = 0.0;
+                    worst = fmax(worst, fabs(r));
+                    dc_coefficients(v.omega, den, r, fv.d, r_out, inv_out);
                 }
-                if (a.o_ks >= 0) den = den + sks[k + e];
-                // add_sources' order
-                double t = fv.d * sum + fv.source;
-                if (a.o_pr >= 0) t = t + spr[k + e];
-                if (a.o_up >= 0) t = t - sup[k + e];
-                double r = t - den * cv[e];
-                if (fv.floor && cv[e] <= 0.0 && r < 0.0) r = 0.0;
-                worst = fmax(worst, fabs(r));
-                dc_coefficients(v.omega, den, r, fv.d, r_out[e], inv_out[e]);
+                if (r32) r32[i] = r_out;
+                if (inv32) inv32[i] = inv_out;
+                if (dz) dz[i] = 0.0f;
             }
-            if (r32) *(float4 *)(r32 + i) = make_float4(r_out[0], r_out[1], r_out[2], r_out[3]);
-            if (inv32) *(float4 *)(inv32 + i) = make_float4(inv_out[0], inv_out[1], inv_out[2], inv_out[3]);
-            if (dz) *(float4 *)(dz + i) = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         }
         worst = warp_max(worst);
         __syncwarp();

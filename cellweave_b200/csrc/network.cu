@@ -2,11 +2,12 @@
 //
 // Compilation (from_spec, network.rs:283-445) runs once on the host: names
 // are resolved to indices, terms laid out per node in file order.  The RK4
-// step (rk4, network.rs:777-799) runs a lane per node: 8, 16 or 32 lanes hold
-// one cell (four, two or one cells a warp), each lane its node's state,
-// midpoint and accumulated slope in registers, source nodes read across the
-// cell's lanes by shuffle (k_rk4_lanes).  Built without fused multiply-add:
-// the sums round as the reference's do.
+// step (rk4, network.rs:777-799) runs one cell per thread when there are many
+// cells (k_rk4: every cell of a launch walks the same term list, so a warp
+// never diverges; state, midpoint, stage slope and accumulated slope in
+// shared memory laid out [node][thread]), and a lane per node when there are
+// few (k_rk4_lanes: 8, 16 or 32 lanes a cell, source nodes by shuffle).
+// Built without fused multiply-add: the sums round as the reference's do.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -23,6 +24,94 @@ namespace {
 const char *INPUTS[6] = {"oxygen", "egf", "crowding", "stress", "waste", "necrotic_factor"};
 
 constexpr int MAXS = 32;
+
+constexpr int RT = 64;  // cells per block of the one-cell-per-thread kernels
+
+// One cell's `substeps` RK4 steps (rk4, network.rs:777-799) on its column of
+// the block's shared arrays (xs: state, ms: midpoint, ks: stage slope, as:
+// accumulated slope, each [node][RT]), under the terms at sterm/spar/sptr.
+__device__ __forceinline__ void rk4_cell(const NetDev &N, const int4 *sterm, const double4 *spar, const int32_t *sptr,
+                                         double *xs, double *ms, double *ks, double *as, const double *in, double dt,
+                                         int substeps) {
+    const int S = N.S;
+    for (int sub = 0; sub < substeps; ++sub) {
+        // k1 at x
+        derivatives(N, sterm, spar, sptr, xs, in, ks, RT);
+        for (int i = 0; i < S; ++i) {
+            double k1 = ks[i * RT];
+            as[i * RT] = k1;
+            ms[i * RT] = xs[i * RT] + 0.5 * dt * k1;
+        }
+        // k2 at x + dt/2 k1, k3 at x + dt/2 k2, k4 at x + dt k3
+        for (int stage = 1; stage < 4; ++stage) {
+            derivatives(N, sterm, spar, sptr, ms, in, ks, RT);
+            double step = stage < 2 ? 0.5 * dt : dt;
+            for (int i = 0; i < S; ++i) {
+                double kv = ks[i * RT];
+                if (stage < 3) {
+                    as[i * RT] = as[i * RT] + 2.0 * kv;
+                    ms[i * RT] = xs[i * RT] + step * kv;
+                } else {
+                    as[i * RT] = as[i * RT] + kv;
+                }
+            }
+        }
+        for (int i = 0; i < S; ++i) {
+            double delta = (dt / 6.0) * as[i * RT];
+            xs[i * RT] = fmin(fmax(xs[i * RT] + delta, 0.0), 1.0);
+        }
+    }
+}
+
+// state: [S][ncells] (node-major, coalesced); inputs: [6][ncells].
+// alive (optional): cells whose entry is zero are left as they are.
+__global__ void __launch_bounds__(RT) k_rk4(NetDev N, double *state, const double *inputs, int64_t ncells,
+                                            int64_t state_stride, int64_t input_stride, double dt, int substeps,
+                                            const uint8_t *alive) {
+    extern __shared__ double sm[];
+    const int S = N.S;
+    double *x = sm, *mid = sm + S * RT, *kk = sm + 2 * S * RT, *acc = sm + 3 * S * RT;
+    int4 *sterm = (int4 *)(sm + 4 * S * RT);
+    double4 *spar = (double4 *)(sterm + N.nterms);
+    int32_t *sptr = (int32_t *)(spar + N.nterms);
+    for (int t = threadIdx.x; t < N.nterms; t += RT) { sterm[t] = N.term[t]; spar[t] = N.par[t]; }
+    for (int t = threadIdx.x; t <= S; t += RT) sptr[t] = N.node_ptr[t];
+    __syncthreads();
+    int64_t c = (int64_t)blockIdx.x * RT + threadIdx.x;
+    if (c >= ncells) return;
+    if (alive && !alive[c]) return;
+    const int tid = threadIdx.x;
+    double in[6];
+    for (int q = 0; q < 6; ++q) in[q] = inputs[q * input_stride + c];
+    double *xs = x + tid, *ms = mid + tid, *ks = kk + tid, *as = acc + tid;
+    for (int i = 0; i < S; ++i) xs[i * RT] = state[i * state_stride + c];
+    rk4_cell(N, sterm, spar, sptr, xs, ms, ks, as, in, dt, substeps);
+    for (int i = 0; i < S; ++i) state[i * state_stride + c] = xs[i * RT];
+}
+
+// The same for cells of many networks: cell c under nets[clone[c]], its
+// terms read from global memory (a network's tables are a few KB: they stay
+// in L1 across the block's cells of that network).
+// state: [S][state_stride], inputs: [6][input_stride]; alive (optional):
+// cells whose entry is zero are left as they are.
+__global__ void __launch_bounds__(RT) k_rk4_clones(const NetDev *nets, const int32_t *clone, int S, double *state,
+                                                   const double *inputs, int64_t ncells, int64_t state_stride,
+                                                   int64_t input_stride, double dt, int substeps,
+                                                   const uint8_t *alive) {
+    extern __shared__ double sm[];
+    double *x = sm, *mid = sm + S * RT, *kk = sm + 2 * S * RT, *acc = sm + 3 * S * RT;
+    int64_t c = (int64_t)blockIdx.x * RT + threadIdx.x;
+    if (c >= ncells) return;
+    if (alive && !alive[c]) return;
+    const NetDev N = nets[clone[c]];
+    const int tid = threadIdx.x;
+    double in[6];
+    for (int q = 0; q < 6; ++q) in[q] = inputs[q * input_stride + c];
+    double *xs = x + tid, *ms = mid + tid, *ks = kk + tid, *as = acc + tid;
+    for (int i = 0; i < S; ++i) xs[i * RT] = state[i * state_stride + c];
+    rk4_cell(N, N.term, N.par, N.node_ptr, xs, ms, ks, as, in, dt, substeps);
+    for (int i = 0; i < S; ++i) state[i * state_stride + c] = xs[i * RT];
+}
 
 // RK4 with a lane per node (derivatives and term_rate, network.rs:686-734;
 // rk4, 777-799): W lanes (W >= S, a power of two) hold one cell, lane i its
@@ -122,9 +211,30 @@ __global__ void __launch_bounds__(128) k_rk4_lanes(NetDev N, const NetDev *nets,
     if (live) state[node * state_stride + c] = x;
 }
 
+// Cells above this many take one thread each (the warps walk one term list
+// together, no divergence); below it a lane per node puts more threads on
+// the few cells (measured: 2,144 cells of 12 nodes 384 -> 178 us; 136,384
+// cells of 8 nodes 521 -> 2,430 us with lanes, whose nodes diverge by term).
+constexpr int64_t LANES_BELOW = 16384;
+
 int rk4_lanes(const NetDev &N, const NetDev *nets, const int32_t *clone, int S, double *state, const double *inputs,
               int64_t ncells, int64_t state_stride, int64_t input_stride, double dt, int substeps,
-              const uint8_t *alive) {
+              const uint8_t *alive, size_t cell_smem) {
+    if (ncells >= LANES_BELOW) {
+        const unsigned grid = (unsigned)((ncells + RT - 1) / RT);
+        if (nets) {
+            const size_t smem = sizeof(double) * 4 * S * RT;
+            if (smem > 48 * 1024)
+                CW_CUDA(cudaFuncSetAttribute(k_rk4_clones, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            k_rk4_clones<<<grid, RT, smem, stream()>>>(nets, clone, S, state, inputs, ncells, state_stride,
+                                                       input_stride, dt, substeps, alive);
+        } else {
+            k_rk4<<<grid, RT, cell_smem, stream()>>>(N, state, inputs, ncells, state_stride, input_stride, dt, substeps,
+                                                     alive);
+        }
+        CW_LAUNCHED();
+        return CW_OK;
+    }
     const int W = S <= 8 ? 8 : S <= 16 ? 16 : 32;
     const int64_t threads = ncells * W;
     const unsigned grid = (unsigned)((threads + 127) / 128);
@@ -153,6 +263,10 @@ __global__ void k_mechanics(const double *state, int64_t ncells, int64_t stride,
     target[c] = isnan(t) ? 0u : (t >= 4294967295.0 ? 4294967295u : (uint32_t)t);
 }
 
+size_t rk4_smem(const cw_network_s *n) {
+    return sizeof(double) * 4 * n->S * RT + n->nterms * (sizeof(int4) + sizeof(double4)) + sizeof(int32_t) * (n->S + 1);
+}
+
 // The device copies of a network's host tables (h_ptr, h_term, h_par).
 int network_upload(cw_network_s *n) {
     n->nterms = (int32_t)n->h_term.size();
@@ -165,6 +279,10 @@ int network_upload(cw_network_s *n) {
         CW_CUDA(cudaMemcpy(n->term, n->h_term.data(), sizeof(int4) * n->nterms, cudaMemcpyHostToDevice));
         CW_CUDA(cudaMemcpy(n->par, n->h_par.data(), sizeof(double4) * n->nterms, cudaMemcpyHostToDevice));
     }
+    size_t smem = rk4_smem(n);
+    if (smem > 48 * 1024 &&
+        cudaFuncSetAttribute(k_rk4, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return fail(CW_ERR_CONFIG, "the network is too large for one block's shared memory");
     return CW_OK;
 }
 
@@ -218,7 +336,7 @@ int network_step_device(const cw_network_s *n, double *state, const double *inpu
                         int64_t state_stride, int64_t input_stride, double dt, int substeps, const uint8_t *alive) {
     if (ncells <= 0) return CW_OK;
     return rk4_lanes(net_dev(n), nullptr, nullptr, n->S, state, inputs, ncells, state_stride, input_stride, dt,
-                     substeps, alive);
+                     substeps, alive, rk4_smem(n));
 }
 
 // RK4 for cells of many networks on node-major state (the driver's evolving
@@ -229,7 +347,7 @@ int network_step_clones_device(const NetDev *nets, const int32_t *clone, int S, 
     if (ncells <= 0) return CW_OK;
     NetDev none{};
     none.S = S;
-    return rk4_lanes(none, nets, clone, S, state, inputs, ncells, state_stride, input_stride, dt, substeps, alive);
+    return rk4_lanes(none, nets, clone, S, state, inputs, ncells, state_stride, input_stride, dt, substeps, alive, 0);
 }
 
 int network_mechanics_device(const cw_network_s *n, const double *state, int64_t ncells, int64_t stride,
@@ -530,7 +648,7 @@ int cw_network_step_clones(int32_t nnets, const cw_network *nets, int64_t ncells
     CW_CUDA(cudaMemcpy(d_clone, clone, sizeof(int32_t) * ncells, cudaMemcpyHostToDevice));
     NetDev none{};
     none.S = S;
-    if ((rc = rk4_lanes(none, d_nets, d_clone, S, d_state, d_in, ncells, ncells, ncells, dt, substeps, nullptr)) !=
+    if ((rc = rk4_lanes(none, d_nets, d_clone, S, d_state, d_in, ncells, ncells, ncells, dt, substeps, nullptr, 0)) !=
         CW_OK)
         return rc;
     CW_CUDA(cudaGetLastError());
