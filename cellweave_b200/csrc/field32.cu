@@ -464,52 +464,65 @@ __global__ void __launch_bounds__(32 * VY) k_sor32_vol(const float *__restrict__
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     const int lx = 2 * tx, gx = x0 + lx, gy = y0 + ty;
     const bool in0 = gx < dm.x && gy < dm.y, in1 = gx + 1 < dm.x && gy < dm.y;
-    const int64_t plane = (int64_t)dm.x * dm.y;
-    const int64_t col = off[h] + (int64_t)gy * dm.x + gx;  // this thread's first pixel in slice 0
+    // offsets inside the history in 32 bits (a history holds fewer than 2^31
+    // pixels), its arrays from their first pixel
+    const int plane = dm.x * dm.y;
+    const int col = gy * dm.x + gx;  // this thread's first pixel in slice 0
+    const int64_t base = off[h];
+    const float *hsrc = src + base, *hrhs = rhs + base, *hinv = inv + base;
+    float *hdst = dst + base;
+    double *hc = apply_c ? apply_c + base : nullptr;
     const float omc = 1.f - omega[h];
     // the output interior of the tile (a window edge on the history's border makes no error)
     const int ix0 = x0 == 0 ? 0 : x0 + D, ix1 = x0 + VX >= dm.x ? dm.x : x0 + VX - D;
     const int iy0 = y0 == 0 ? 0 : y0 + D, iy1 = y0 + VY >= dm.y ? dm.y : y0 + VY - D;
     const bool out_y = gy >= iy0 && gy < iy1;
     const bool out0 = in0 && out_y && gx >= ix0 && gx < ix1, out1 = in1 && out_y && gx + 1 >= ix0 && gx + 1 < ix1;
-    auto slot = [&](int z) -> float * { return ring + (size_t)(z % R) * (VY * VX); };
-    auto load = [&](int z, float &v0, float &v1) {
+    // this thread's pair in ring slot k
+    float2 *const mine = (float2 *)(ring + ty * VX) + tx;
+    auto at = [&](int k) -> float2 * { return mine + k * (VY * VX / 2); };
+    auto wrap = [](int k) { return k < 0 ? k + R : (k >= R ? k - R : k); };
+    auto load = [&](int o, float &v0, float &v1) {  // o: the slice's offset
         v0 = v1 = 0.f;
         if (!zero_start) {
-            const int64_t i = col + (int64_t)z * plane;
-            if (in0) v0 = __ldg(src + i);
-            if (in1) v1 = __ldg(src + i + 1);
+            if (in0) v0 = __ldg(hsrc + o + col);
+            if (in1) v1 = __ldg(hsrc + o + col + 1);
         }
     };
     // the first two slices
     for (int z = zlo; z < min(zlo + 2, zhi); ++z) {
         float v0, v1;
-        load(z, v0, v1);
-        ((float2 *)(slot(z) + ty * VX))[tx] = make_float2(v0, v1);
+        load(z * plane, v0, v1);
+        *at(z % R) = make_float2(v0, v1);
     }
     __syncthreads();
     const int tend = zhi - 1 + 2 * (S - 1);
-    for (int t = zlo; t <= tend; ++t) {
+    int rt = zlo % R;     // ring slot of slice t
+    int toff = zlo * plane;  // offset of slice t
+    for (int t = zlo; t <= tend; ++t, rt = wrap(rt + 1), toff += plane) {
         // the slice after next into registers while the stages run
         const int zn = t + 2;
         float n0 = 0.f, n1 = 0.f;
-        if (zn < zhi) load(zn, n0, n1);
-        for (int s = 1; s <= S; ++s) {
+        if (zn < zhi) load(toff + 2 * plane, n0, n1);
+#pragma unroll
+        for (int s = 1; s <= D; ++s) {
+            if (s > S) break;
             const int p = t - 2 * (s - 1);  // the same for the whole block
             if (p < zlo || p >= zhi) continue;
             const int c = (start_colour + s - 1) & 1;
             // the pixel of colour c in this thread's pair ((x + y + z) mod 2 == c,
             // x0 even): the same e for a warp, which holds one row
             const int e = (c + gy + p) & 1;
-            float2 *row = (float2 *)(slot(p) + ty * VX) + tx;
+            const int k = wrap(rt - 2 * (s - 1));
+            float2 *row = at(k);
             const float2 me = *row;
             // x neighbours: the left pair's second pixel, the right pair's first
             const float left = __shfl_up_sync(0xffffffffu, me.y, 1);
             const float right = __shfl_down_sync(0xffffffffu, me.x, 1);
             const float2 z2 = make_float2(0.f, 0.f);
             const float2 ym2 = ty > 0 ? row[-VX / 2] : z2, yp2 = ty + 1 < VY ? row[VX / 2] : z2;
-            const float2 zm2 = p - 1 >= zlo ? ((const float2 *)(slot(p - 1) + ty * VX))[tx] : z2;
-            const float2 zp2 = p + 1 < zhi ? ((const float2 *)(slot(p + 1) + ty * VX))[tx] : z2;
+            const float2 zm2 = p - 1 >= zlo ? *at(wrap(k - 1)) : z2;
+            const float2 zp2 = p + 1 < zhi ? *at(wrap(k + 1)) : z2;
             if (!(e ? in1 : in0)) continue;  // outside the history: stays zero
             float xm, xp, ym, yp, zm, zp, cur;
             if (e == 0) {
@@ -520,33 +533,33 @@ __global__ void __launch_bounds__(32 * VY) k_sor32_vol(const float *__restrict__
             // k_sor32_half's sums, in its order
             float sum = (xm + xp) + (ym + yp);
             sum += (zm + zp);
-            const int64_t i = col + (int64_t)p * plane + e;
-            const float v = fmaf(__ldg(inv + i), sum, fmaf(omc, cur, __ldg(rhs + i)));
+            const int i = toff - 2 * (s - 1) * plane + col + e;
+            const float v = fmaf(__ldg(hinv + i), sum, fmaf(omc, cur, __ldg(hrhs + i)));
             *row = e == 0 ? make_float2(v, me.y) : make_float2(me.x, v);
         }
         // slice t - 2 (S - 1) has had every half-sweep: its interior out
         const int pf = t - 2 * (S - 1);
         if (pf >= z0 && pf < z1) {
-            const float2 q = ((const float2 *)(slot(pf) + ty * VX))[tx];
-            const int64_t i = col + (int64_t)pf * plane;
-            if (apply_c) {
+            const float2 q = *at(wrap(rt - 2 * (S - 1)));
+            const int i = toff - 2 * (S - 1) * plane + col;
+            if (hc) {
                 // the last launch of a correction: c += d on the free pixels
                 // (a held pixel has a = 0 and d = 0 throughout), floored as
                 // the reference's update is (pde.rs:395)
-                if (out0 && (q.x != 0.f || __ldg(inv + i) != 0.f)) {
-                    const double v = apply_c[i] + (double)q.x;
-                    apply_c[i] = floor ? fmax(v, 0.0) : v;
+                if (out0 && (q.x != 0.f || __ldg(hinv + i) != 0.f)) {
+                    const double v = hc[i] + (double)q.x;
+                    hc[i] = floor ? fmax(v, 0.0) : v;
                 }
-                if (out1 && (q.y != 0.f || __ldg(inv + i + 1) != 0.f)) {
-                    const double v = apply_c[i + 1] + (double)q.y;
-                    apply_c[i + 1] = floor ? fmax(v, 0.0) : v;
+                if (out1 && (q.y != 0.f || __ldg(hinv + i + 1) != 0.f)) {
+                    const double v = hc[i + 1] + (double)q.y;
+                    hc[i + 1] = floor ? fmax(v, 0.0) : v;
                 }
             } else {
-                if (out0) dst[i] = q.x;
-                if (out1) dst[i + 1] = q.y;
+                if (out0) hdst[i] = q.x;
+                if (out1) hdst[i + 1] = q.y;
             }
         }
-        if (zn < zhi) ((float2 *)(slot(zn) + ty * VX))[tx] = make_float2(n0, n1);
+        if (zn < zhi) *at(wrap(rt + 2)) = make_float2(n0, n1);
         __syncthreads();
     }
 }
