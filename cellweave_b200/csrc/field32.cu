@@ -696,11 +696,15 @@ int vol_init(Sor32 &s, cw_field_s *f, int window) {
         axis_starts(g.h[k], s.vy, s.vdepth, ys);
         columns[k] = (int64_t)xs.size() * ys.size();
     }
+    // chunks: the longest of 64, 32, 16 slices that still gives three tiles
+    // for every block the device holds at once (CW_WINDOW_TALL: one tile, for
+    // less of the z halo's redundant work at the cost of a fuller last wave)
+    const int64_t want = (window == CW_WINDOW_TALL ? 1LL : 3LL) * per_sm * nsm;
     s.vz = 16;
     for (int vz : {64, 32}) {
         int64_t n = 0;
         for (uint32_t k = 0; k < g.nh; ++k) n += columns[k] * ((g.d[k] + vz - 1) / vz);
-        if (n >= 3LL * per_sm * nsm) {
+        if (n >= want) {
             s.vz = vz;
             break;
         }
