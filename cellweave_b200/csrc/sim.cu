@@ -1023,7 +1023,7 @@ static int tune_depth(cw_sim_s *s) {
     int bd = 8, bw = CW_WINDOW_AUTO;
     // volumes march tiles along z at two or four half-sweeps a launch
     const bool volume = s->d[0] > 1;
-    for (int w : {CW_WINDOW_AUTO, CW_WINDOW_64, volume ? CW_WINDOW_TALL : CW_WINDOW_64})
+    for (int w : {CW_WINDOW_AUTO, CW_WINDOW_64})
         for (int d : {volume ? 2 : 6, 4, 8}) {
             float ms = 0.f;
             int64_t launches = 0;
