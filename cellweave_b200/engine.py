@@ -762,6 +762,12 @@ class Simulation:
         call("cw_sim_clones", self._h, int(hist), int(n), ptr(out))
         return out
 
+    def clone_count(self):
+        """Clones in the whole batch: the founders' and every one founded since."""
+        n = C.c_uint32()
+        call("cw_sim_clone_count", self._h, C.byref(n))
+        return n.value
+
     def traced_clones(self, hist=0):
         """traced_clones (simulation.rs:2407-2421): (mark, cells in the layer
         carrying it) for every mark still carried, in the order of the marks."""

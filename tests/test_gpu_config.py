@@ -253,6 +253,61 @@ def test_a_lesion_in_a_mutating_sheet_grows_inside_the_oracle_band(tmp_path):
         assert sim.records_match_grid(k)
 
 
+SHIPPED_LESION = ("width = 100\nheight = 100\nmcs = 6000\ntemperature = 10.0\nsnapshot_interval = 100\n"
+                  "output_dir = \"out\"\noxygen_uptake = 0.0\nmutation_rate = 0.01\nrewiring = 0.3\n"
+                  "network = \"tissue.toml\"\nhours_per_step = 0.56\n[seeding]\nkind = \"sheet\"\nside = 10\n"
+                  "[lesion]\nnetwork = \"lesion.toml\"\nat = {at}\nradius = 15.0\n")
+
+
+def test_the_shipped_lesion_turns_the_cells_at_the_centre_into_one_clone_at_its_step(tmp_path):
+    # crates/io/tests/lesion.rs:29-49: epithelium-lesion.toml on a 100 x 100 box,
+    # the lesion at step 20: nothing before it, then one clone with no parent
+    # holding 3 to 12 cells, among them the one at the centre, not the corner's
+    lesion_files(tmp_path)
+    p = tmp_path / "run.toml"
+    p.write_text(SHIPPED_LESION.format(at=20))
+    sim, _ = C.simulation_from_config(C.load_sim_config(str(p)))
+    sim.step(20)
+    assert sim.measure()[0]["lesion"] == 0 and not any(r.get("lesion") for _, r in sim.clone_records())
+    sim.step(1)
+    recs = sim.clone_records()
+    lesions = [j for j, (_, r) in enumerate(recs) if r.get("lesion")]
+    assert len(lesions) == 1 and recs[lesions[0]][0] == -1
+    base = sim.clone_count() - len(recs)
+    founded = base + lesions[0]
+
+    def in_lesion(c):
+        # descended from the lesion's clone (parents of clones founded in the run)
+        while c >= base:
+            if c == founded:
+                return True
+            c = recs[c - base][0]
+        return False
+
+    assert 3 <= sim.measure()[0]["lesion"] <= 12
+    grid = sim.grid(0).reshape(100, 100)
+    clones = sim.clones(sim.lattice().capacity[0], 0)
+    assert in_lesion(int(clones[grid[50, 50]])) and not in_lesion(int(clones[grid[2, 2]]))
+
+
+def test_a_lesion_that_never_comes_leaves_the_run_as_it_was(tmp_path):
+    # crates/io/tests/lesion.rs:51-67: a lesion set for a step never reached
+    # draws nothing: the measurements and clones are those of the run without one
+    lesion_files(tmp_path)
+    runs = []
+    for text in (SHIPPED_LESION.format(at=10_000), SHIPPED_LESION.format(at=0).split("[lesion]")[0]):
+        p = tmp_path / "run.toml"
+        p.write_text(text)
+        sim, _ = C.simulation_from_config(C.load_sim_config(str(p)))
+        measured = []
+        for _ in range(200):
+            sim.step(1)
+            measured.append(sim.measure()[0])
+        runs.append((measured, sim.clone_records(), sim.grid(0).copy()))
+    assert runs[0][0] == runs[1][0] and runs[0][1] == runs[1][1]
+    np.testing.assert_array_equal(runs[0][2], runs[1][2])
+
+
 def test_suppressed_mutations_leave_the_run_as_it_was(tmp_path):
     # Scenario::suppress_before (simulation.rs:240-244, 1671-1694): mutations
     # drawn and recorded but not made; the draws take nothing from the step's

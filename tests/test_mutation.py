@@ -76,3 +76,44 @@ def test_picks_cover_every_term_and_stay_in_range(golden, which):
     bare = {"nodes": [{"name": "a", "initial": 0.1}], "roles": spec["roles"], "mechanics": spec["mechanics"]}
     assert O.mutate_spec(bare, which, 0.5)[1] is None
     assert O.rewire_spec(bare, [0.9, which, 0.0, 0.0, 0.0])[1] is None
+
+
+def test_a_lesion_takes_the_living_cells_whose_centres_lie_within_its_radius():
+    # place_lesion (simulation.rs:1920-1962) on a hand-built 20 x 20 plane:
+    # centres of mass as x + 1/2, y + 1/2 over the pixels; a dead (necrotic)
+    # cell at the centre and a cell with no pixels are left out
+    from oracle.cpu_sim import lesion_joining
+    grid = np.zeros((20, 20), np.int32)
+    grid[8:12, 8:12] = 1      # centre (10, 10): in
+    grid[8:12, 13:17] = 2     # centre (15, 10): 5 from the middle, in at radius 5
+    grid[0:2, 0:2] = 3        # centre (1, 1): out
+    grid[12:14, 8:10] = 4     # necrotic, centre (9, 13): left out
+    types = np.array([0, 1, 1, 2, 3, 1], np.int32)
+    volume = np.array([0, 16, 16, 4, 4, 0], np.int32)  # record 5 holds no pixel
+    assert lesion_joining(grid, types, volume, (3, -1, -1), None, 5.0) == [1, 2]
+    assert lesion_joining(grid, types, volume, (3, -1, -1), None, 4.99) == [1]
+    assert lesion_joining(grid, types, volume, (3, -1, -1), (1.0, 1.0), 0.5) == [3]
+
+
+def test_tracing_marks_the_cells_in_the_layer_and_daughters_carry_them():
+    # mark_every_cell and traced_clones (simulation.rs:1908-1918, 2407-2421)
+    # on the oracle's history: marked at the step, each cell its own mark
+    import json
+    import os
+    from oracle.cpu_sim import CpuHistory
+    spec = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "golden.json")))["networks"]["epithelium"]
+    cfg = dict(dims=[(40, 40, 1)], ncells=[16], seeds=[3], temperature=10.0,
+               J=np.array([[0, 16, 16, 12, 12, 12], [16, 2, 11, 10, 11, 10], [16, 11, 6, 12, 6, 12],
+                           [12, 10, 12, 8, 12, 8], [12, 11, 6, 12, 6, 12], [12, 10, 12, 8, 12, 8]], float),
+               contact_order=1, target_volume=0, lambda_volume=50.0, seeding=4, seed_side=10, nfields=1,
+               o2_dcoef=0.2, o2_sink_by_type=(0, 0, 0, 0), o2_hold=3, tolerance=1e-8, field_off=True, dt=1.0,
+               substeps=8, sweeps=1, death_threshold=0.25, necrotic_type=3, divide=True, max_cells=2000,
+               differentiated_type=4, apoptotic_type=5, lineage=True, hypoxic_level=0.1, network_spec=spec,
+               tracing_at=2)
+    h = CpuHistory(cfg, 0)
+    h.step()
+    h.step()
+    assert h.traced_clones() == []
+    h.step()
+    tr = h.traced_clones()
+    assert [m for m, _ in tr] == list(range(16)) and all(c == 1 for _, c in tr)
