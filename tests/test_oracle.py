@@ -597,3 +597,88 @@ def test_the_fit_oracles_direct_solve_is_the_fixed_point_of_relax():
         assert a.relax(1e-13, 1_000_000, stop=1)[0] == 0
         solve_direct(b)
         np.testing.assert_allclose(b.values, a.values, rtol=0, atol=1e-10)
+
+
+# ---------------------------------------------------------------- the fuller cell
+# crates/io/tests/fuller_cell.rs: the fuller cell against the networks it fills
+# in (the same decisions at the same places), on the oracle's compile and RK4
+
+
+def _settled(golden, name, o2, stress, edit=None):
+    import copy
+    spec = copy.deepcopy(golden["networks"][name])
+    if edit:
+        edit(spec)
+    net = O.compile_network(spec, 100)
+    st = net.initial.reshape(1, -1).copy()
+    ins = np.array([[o2, 0.2, 0.0, stress, 0.0, 0.0]])
+    O.network_step(net, st, ins, 1.0, 600)  # 600 steps of one unit (fuller_cell.rs:42-48)
+    return net, st[0]
+
+
+def _level(net, st, name):
+    return st[net.names.index(name)]
+
+
+def _arrest_oxygen(golden, name):
+    lo, hi = 0.0, 1.0
+    for _ in range(30):
+        mid = 0.5 * (lo + hi)
+        net, st = _settled(golden, name, mid, 0.0)
+        if st[net.hypoxia] >= 0.45:  # QUIESCENCE_THRESHOLD
+            lo = mid
+        else:
+            hi = mid
+    return 0.5 * (lo + hi)
+
+
+def test_the_fuller_cell_asks_for_the_size_the_simpler_one_does(golden):
+    # fuller_cell.rs:69-80
+    a, sa = _settled(golden, "fuller-cell", 1.0, 0.0)
+    b, sb = _settled(golden, "ras-erk", 1.0, 0.0)
+    assert abs(_level(a, sa, "erk") - _level(b, sb, "erk")) < 0.002
+    ta = O.network_mechanics(a, sa.reshape(1, -1))[0]
+    tb = O.network_mechanics(b, sb.reshape(1, -1))[0]
+    assert abs(int(ta) - int(tb)) <= 1
+
+
+def test_the_fuller_cell_stops_dividing_at_the_oxygen_the_simpler_one_does(golden):
+    # fuller_cell.rs:82-97
+    assert abs(_arrest_oxygen(golden, "fuller-cell") - _arrest_oxygen(golden, "ras-erk")) < 0.005
+    fed, sf = _settled(golden, "fuller-cell", 1.0, 0.0)
+    assert _level(fed, sf, "rb") < 0.3 and _level(fed, sf, "p27") < 0.01
+    starved, ss = _settled(golden, "fuller-cell", 0.1, 0.0)
+    assert _level(starved, ss, "p27") > 0.5
+    assert _level(starved, ss, "cyclin_e") < _level(fed, sf, "cyclin_e") / 2.0
+
+
+def test_the_fuller_cell_dies_of_anoxia_where_the_simpler_one_does(golden):
+    # fuller_cell.rs:99-110
+    for o2 in (0.02, 0.05, 0.1, 0.2, 0.6):
+        a, sa = _settled(golden, "fuller-cell", o2, 0.0)
+        b, sb = _settled(golden, "ras-erk", o2, 0.0)
+        assert abs(sa[a.survival] - sb[b.survival]) < 0.002, o2
+
+
+def test_the_fuller_cell_answers_a_stress_as_the_stress_response_did(golden):
+    # fuller_cell.rs:112-136
+    for stress in (0.0, 0.2, 0.5, 1.0):
+        a, sa = _settled(golden, "fuller-cell", 1.0, stress)
+        b, sb = _settled(golden, "stress-response", 1.0, stress)
+        assert abs(sa[a.optional["apoptosis"]] - sb[b.optional["apoptosis"]]) < 0.015, stress
+    calm, sc = _settled(golden, "fuller-cell", 1.0, 0.0)
+    for name in ("p53", "mdm2", "p21", "bax", "caspase"):
+        assert _level(calm, sc, name) == 0.0, name
+    a, sa = _settled(golden, "fuller-cell", 1.0, 1.0)
+    b, sb = _settled(golden, "stress-response", 1.0, 1.0)
+    assert _level(a, sa, "p53") < _level(b, sb, "p53")
+
+
+def test_a_fuller_cell_starts_where_it_settles(golden):
+    # fuller_cell.rs:173-191
+    spec = golden["networks"]["fuller-cell"]
+    net, st = _settled(golden, "fuller-cell", 1.0, 0.0)
+    for node, value in zip(spec["nodes"], st):
+        if node["name"] in ("hif1", "vegf", "bcl2"):
+            continue
+        assert abs(node["initial"] - value) < 0.01, node["name"]
