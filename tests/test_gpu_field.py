@@ -348,3 +348,102 @@ def test_wide_windows_with_the_fused_correction_equal_the_64_windows(sizes, dept
             assert sa[k]["sweeps"] == sb[k]["sweeps"]
             assert sa[k]["residual"] == sb[k]["residual"] < 1e-6
             np.testing.assert_array_equal(bits(ga.values(k)), bits(gb.values(k)))
+
+
+# ---------------------------------------------------------------- the reference's field tests, on the device
+# pde.rs:951-1200, each case run on the device and on the oracle: the same
+# bits, and the reference's own assertions on the device's values
+
+
+def test_a_field_decays_and_never_goes_negative_on_the_device():
+    # pde.rs:951-977
+    for (n, d, decay, dt, steps) in [(20, 0.25, 0.1, 0.1, 200), (30, 0.5, 2.0, 0.05, 500)]:
+        o = O.Field(n, n, 1, d, decay, 1.0)
+        g = cw.ScalarField.new(n, n, d, decay, 1.0)
+        for _ in range(steps):
+            o.step(dt)
+            g.step(dt)
+        v = g.values()
+        np.testing.assert_array_equal(bits(v), bits(o.values))
+        assert v.min() >= 0.0
+        if n == 20:
+            assert v[10 * 20 + 10] < 0.5
+
+
+def test_a_held_pixel_does_not_move_and_a_cleared_uptake_refills_on_the_device():
+    # pde.rs:1047-1081
+    o, g = disc_pair(30, 6, 0.05)
+    o.relax(1e-11, 50_000)
+    g.relax(1e-11, 50_000)
+    for _ in range(200):
+        o.step(1.0)
+        g.step(1.0)
+    v = g.values()
+    np.testing.assert_array_equal(bits(v), bits(o.values))
+    assert v[0] == 1.0 and v[3 * 30 + 15] == 1.0 and v[15 * 30 + 15] < 0.5
+    o, g = disc_pair(30, 6, 0.01)
+    o.relax(1e-11, 50_000)
+    g.relax(1e-11, 50_000)
+    assert g.values()[15 * 30 + 15] < 0.9
+    o.uptake[:] = 0.0
+    g.clear_uptake()
+    rc, sweeps = o.relax(1e-7, 50_000)
+    assert g.relax(1e-7, 50_000) == sweeps
+    v = g.values()
+    np.testing.assert_array_equal(bits(v), bits(o.values))
+    assert abs(v[15 * 30 + 15] - 1.0) < 1e-5
+
+
+def test_a_held_vessel_supplies_from_the_inside_out_on_the_device():
+    # pde.rs:1083-1113
+    y, x = np.mgrid[0:60, 0:60]
+    vessel = (((x - 30) ** 2 + (y - 30) ** 2) <= 9).reshape(-1)
+    up = np.where(vessel, 0.0, 0.002)
+    o = O.Field(60, 60, 1, D, 0.0, 0.0)
+    o.uptake[:] = up
+    o.held[vessel] = 1
+    o.values[vessel] = 1.0
+    g = cw.ScalarField.new(60, 60, D, 0.0, 0.0)
+    g.set_uptake_array(up)
+    g.hold_where(1.0, vessel)
+    rc, sweeps = o.relax(1e-7, 50_000)
+    assert rc == 0 and g.relax(1e-7, 50_000) == sweeps
+    v = g.values()
+    np.testing.assert_array_equal(bits(v), bits(o.values))
+    at = lambda r: v[30 * 60 + 30 + r]
+    assert at(0) == 1.0 and at(5) > at(10) > at(15) and v[61] < 0.01
+
+
+def test_release_a_bath_and_a_vessel_and_the_box_swept_on_the_device():
+    # pde.rs:1115-1200
+    g = cw.ScalarField.new(20, 20, D, 0.0, 1.0)
+    g.hold_bath(1.0, np.ones(400, bool))
+    g.set_uptake_array(np.full(400, 0.01))
+    g.step(1.0)
+    assert g.values()[210] == 1.0
+    g.release_all()
+    g.step(1.0)
+    assert g.values()[210] < 1.0
+
+    y, x = np.mgrid[0:30, 0:30]
+    tissue = ((x >= 5) & (x < 25) & (y >= 5) & (y < 25)).reshape(-1)
+    g = cw.ScalarField.new(30, 30, D, 0.0, 0.0)
+    g.hold_bath(1.0, ~tissue)
+    g.hold_where(0.5, np.arange(900) == 15 * 30 + 15)
+    v = g.values()
+    assert v[0] == 1.0 and v[15 * 30 + 15] == 0.5 and v[10 * 30 + 10] == 0.0
+
+    y, x = np.mgrid[0:40, 0:40]
+    disc = (((x - 20) ** 2 + (y - 20) ** 2) <= 64).reshape(-1)
+    up = np.where(disc, 0.001, 0.0)
+    o = O.Field(40, 40, 1, D, 0.0, 1.0)
+    o.uptake[:] = up
+    o.hold_bath(~disc, 1.0)
+    g = cw.ScalarField.new(40, 40, D, 0.0, 1.0)
+    g.set_uptake_array(up)
+    g.hold_bath(1.0, ~disc)
+    rc, sweeps = o.relax(1e-9, 100_000)
+    assert rc == 0 and g.relax(1e-9, 100_000) == sweeps
+    v = g.values()
+    np.testing.assert_array_equal(bits(v), bits(o.values))
+    assert (v[~disc] == 1.0).all() and v[20 * 40 + 20] < 1.0

@@ -117,3 +117,58 @@ def test_tracing_marks_the_cells_in_the_layer_and_daughters_carry_them():
     h.step()
     tr = h.traced_clones()
     assert [m for m, _ in tr] == list(range(16)) and all(c == 1 for _, c in tr)
+
+
+# ---------------------------------------------------------------- closing over dead tissue and shut-in fluid
+# cpm.rs:1702-1803 on the oracle's break_down_debris / drain_shut_in helpers
+
+
+def _closing(blocks, size=30):
+    """A lattice of rectangles (kind, x, y, w, h), kinds 1 tumour and 3
+    necrotic, as the reference's add_block lays them; ids from 1 in order."""
+    from oracle import cpu_sim
+    g = np.zeros((size, size), np.int32)
+    kinds = [0]
+    for i, (kind, x, y, w, h) in enumerate(blocks, start=1):
+        g[y:y + h, x:x + w] = i
+        kinds.append(kind)
+    lat = O.Lattice(g, (size, size, 1), len(kinds), np.zeros((4, 4)), 10.0)
+    lat.type[:] = kinds
+    lat.volume[:] = np.bincount(lat.grid.clip(0), minlength=len(kinds))
+    lat.volume[0] = 0
+    hist = cpu_sim.CpuHistory.__new__(cpu_sim.CpuHistory)  # the helpers read only these
+    hist.lat, hist.cfg, hist.div_rng = lat, {"necrotic_type": 3}, np.random.default_rng(3)
+    return hist, cpu_sim.CpuHistory
+
+
+def test_a_pixel_closed_over_goes_to_living_tissue_never_to_the_dead_or_the_medium():
+    # cpm.rs:1702-1727: dead block at (10, 10), tumour at (15, 10), dead at (10, 15)
+    hist, H = _closing([(3, 10, 10, 5, 5), (1, 15, 10, 5, 5), (3, 10, 15, 5, 5)])
+    faces = H._faces(hist)
+    at = lambda x, y: y * 30 + x
+    ids, n = H._living_around(hist, np.array([at(12, 14), at(12, 12), at(14, 12), at(10, 12)]), faces)
+    # against dead tissue alone, inside its own cell, against medium alone: no taker
+    assert list(n) == [0, 0, 1, 0]
+    # against the living cell and nothing else, the living cell takes it
+    assert sorted(ids[2][ids[2] > 0]) == [2]
+    assert H._give(hist, np.array([at(14, 12)]), ids[2:3], n[2:3], hist.div_rng)[0] == 2
+
+
+def test_fluid_shut_in_is_closed_in_by_the_living_only():
+    # cpm.rs:1771-1803: four cells around a 4 x 4 hole at x, y 13..16, the right one dead
+    hist, H = _closing([(1, 10, 10, 10, 3), (1, 10, 17, 10, 3), (1, 10, 13, 3, 4), (3, 17, 13, 3, 4)])
+    hole = [y * 30 + x for y in range(13, 17) for x in range(13, 17)]
+    scratch = O.Field(30, 30, 1)
+    scratch.hold_bath(hist.lat.grid == 0, 1.0)
+    assert list(np.nonzero((hist.lat.grid == 0) & (scratch.held == 0))[0]) == hole
+    before = int(hist.lat.volume.sum())
+    H._drain_shut_in(hist)
+    g = hist.lat.grid.reshape(30, 30)
+    # every hole pixel with living tissue across a face went to a living cell;
+    # those beside only the dead cell or only more fluid stay fluid
+    closed = {(x, y) for y in range(13, 17) for x in range(13, 17) if g[y, x] != 0}
+    want = {(x, 13) for x in range(13, 17)} | {(x, 16) for x in range(13, 17)} | {(13, 14), (13, 15)}
+    assert closed == want
+    assert all(g[y, x] in (1, 2, 3) for x, y in closed)
+    assert int(hist.lat.volume.sum()) == before + len(want)
+    assert np.array_equal(np.bincount(hist.lat.grid.clip(0), minlength=5)[1:], hist.lat.volume[1:])

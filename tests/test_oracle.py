@@ -458,6 +458,87 @@ def test_explicit_step_conserves_and_refuses():
     assert O.Field(20, 20, 1, 0.1, 0.0, 1.0).step(0.0) == 1
 
 
+def test_a_field_decays_and_never_goes_negative():
+    # pde.rs:951-977
+    f = O.Field(20, 20, 1, 0.25, 0.1, 1.0)
+    for _ in range(200):
+        assert f.step(0.1) == 0
+    assert f.values[10 * 20 + 10] < 0.5
+    g = O.Field(30, 30, 1, 0.5, 2.0, 1.0)
+    for _ in range(500):
+        assert g.step(0.05) == 0
+    assert g.values.min() >= 0.0
+
+
+def test_a_held_pixel_is_a_boundary_condition_and_does_not_move():
+    # pde.rs:1047-1066
+    f = bathed_disc(30, 6, 0.05)
+    for _ in range(200):
+        assert f.step(1.0) == 0
+    v = f.values.reshape(30, 30)
+    assert v[0, 0] == 1.0 and v[3, 15] == 1.0 and v[15, 15] < 0.5
+
+
+def test_clearing_the_uptake_lets_the_field_refill():
+    # pde.rs:1069-1081
+    f = bathed_disc(30, 6, 0.01)
+    assert centre(f, 30) < 0.9
+    f.uptake[:] = 0.0
+    assert f.relax(1e-7, 50_000)[0] == 0
+    assert abs(centre(f, 30) - 1.0) < 1e-5
+
+
+def vessel_disc(size=60, r2=9):
+    y, x = np.mgrid[0:size, 0:size]
+    return (((x - size // 2) ** 2 + (y - size // 2) ** 2) <= r2).reshape(-1)
+
+
+def test_a_held_vessel_supplies_from_the_inside_out():
+    # pde.rs:1083-1113
+    f = O.Field(60, 60, 1, D, 0.0, 0.0)
+    vessel = vessel_disc()
+    f.uptake[~vessel] = 0.002
+    f.held[vessel] = 1
+    f.values[vessel] = 1.0
+    assert f.relax(1e-7, 50_000)[0] == 0
+    at = lambda r: f.values[30 * 60 + 30 + r]
+    assert at(0) == 1.0 and at(5) > at(10) > at(15)
+    assert f.values[1 * 60 + 1] < 0.01
+
+
+def test_releasing_lets_a_former_bath_pixel_move_again():
+    # pde.rs:1115-1138
+    f = O.Field(20, 20, 1, D, 0.0, 1.0)
+    f.hold_bath(np.ones(400, bool), 1.0)
+    f.uptake[:] = 0.01
+    assert f.step(1.0) == 0
+    assert f.values[10 * 20 + 10] == 1.0
+    f.held[:] = 0
+    assert f.step(1.0) == 0
+    assert f.values[10 * 20 + 10] < 1.0
+
+
+def test_a_bath_and_a_vessel_can_hold_at_once():
+    # pde.rs:1140-1156
+    f = O.Field(30, 30, 1, D, 0.0, 0.0)
+    y, x = np.mgrid[0:30, 0:30]
+    tissue = ((x >= 5) & (x < 25) & (y >= 5) & (y < 25)).reshape(-1)
+    f.hold_bath(~tissue, 1.0)
+    f.held[15 * 30 + 15] = 1
+    f.values[15 * 30 + 15] = 0.5
+    assert f.values[0] == 1.0 and f.values[15 * 30 + 15] == 0.5 and f.values[10 * 30 + 10] == 0.0
+
+
+def test_the_box_swept_leaves_what_lies_outside_it_as_it_was_held():
+    # pde.rs:1177-1200
+    f = O.Field(40, 40, 1, D, 0.0, 1.0)
+    disc = vessel_disc(40, 64)
+    f.uptake[disc] = 0.001
+    f.hold_bath(~disc, 1.0)
+    assert f.relax(1e-9, 100_000)[0] == 0
+    assert (f.values[~disc] == 1.0).all() and f.values[20 * 40 + 20] < 1.0
+
+
 def test_residual_stop_reaches_its_tolerance():
     f = O.Field(40, 40, 1, 1.0, 0.0, 0.0)
     f.lin_sink = np.full(1600, 0.01)
