@@ -353,3 +353,26 @@ def test_an_upload_past_the_capacity_is_refused_and_the_grid_kept():
     with pytest.raises(cw.ConfigError, match="pixel 5 holds id 9"):
         _lib.check(_lib.lib().cw_lattice_upload_all(lat.handle, _lib.ptr(wrong)))
     np.testing.assert_array_equal(lat.grid(0).reshape(-1), swapped[:16 * 8])
+
+
+def test_a_plane_through_a_ball_halves_it_on_the_side_it_faces():
+    # cpm.rs:1645-1673: a ball of radius 5 cut by the plane of normal +z
+    # through its centre; the centre slice stays with the parent, the
+    # daughter is the half above it; and the same cut on the oracle
+    grid = seeding.empty(30, 30, 30)
+    rec = seeding.Records()
+    seeding.add_ball(grid, rec, 1, (15, 15, 15), 5, lam=2.0)
+    size = int((grid == 1).sum())
+    g = cw.CpmLattice.from_grids([grid], [rec], 10.0, J3, 1, seeds=[1], capacity=3)
+    daughter = int(g.divide(np.array([1], np.int32), np.array([[0.0, 0.0, 1.0]]))[0])
+    assert daughter == 2
+    out = g.grid()
+    a, b = int((out == 1).sum()), int((out == 2).sum())
+    assert a + b == size and a > b and 2 * b > a
+    assert np.nonzero(out == 2)[0].min() > 15
+    o = oracle_of(grid, rec, J3, 10.0, 1)
+    lat = O.Lattice(o.grid, (30, 30, 30), 3, J3, 10.0, 1)
+    lat.type[:2], lat.volume[:2], lat.target[:2], lat.lam[:2] = o.type, o.volume, o.target, o.lam
+    assert lat.divide_across(1, (0.0, 0.0, 1.0), 2) == (2, 3)
+    np.testing.assert_array_equal(out.reshape(-1), lat.grid)
+    assert g.records_match_grid()

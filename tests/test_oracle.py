@@ -639,6 +639,20 @@ def test_division_hands_every_pixel_to_exactly_one_of_the_two():
     np.testing.assert_array_equal(vol[1:3], lat.volume[1:3])
 
 
+def test_a_plane_through_a_ball_halves_it_on_the_side_it_faces():
+    # cpm.rs:1645-1673: radius 5 at the centre of a 30^3 box, cut by the +z plane
+    grid = seeding.empty(30, 30, 30)
+    rec = seeding.Records()
+    seeding.add_ball(grid, rec, 1, (15, 15, 15), 5, lam=2.0)
+    lat = O.Lattice(grid, (30, 30, 30), 3, REF_J, 10.0)
+    t, v, tg, lam = rec.arrays()
+    lat.type[:2], lat.volume[:2], lat.target[:2], lat.lam[:2] = t, v, tg, lam
+    assert lat.divide_across(1, (0.0, 0.0, 1.0), 2) == (2, 3)
+    a, b = int(lat.volume[1]), int(lat.volume[2])
+    assert a + b == int((grid == 1).sum()) and a > b and 2 * b > a
+    assert np.nonzero(lat.grid.reshape(30, 30, 30) == 2)[0].min() > 15
+
+
 def test_what_cannot_be_divided_is_left_alone():
     # cpm.rs:1335-1379: a cell under 8 pixels, the medium, an unknown id, and a
     # cut that leaves one side empty change nothing
