@@ -207,3 +207,62 @@ def test_the_step_feeds_each_cell_its_crowding():
     O.network_step(O.compile_network(spec, ref_volume), want, ins, 0.25, 4)
     np.testing.assert_array_equal(got[live].view(np.uint64), want.view(np.uint64))
     assert (ins[:, 2] > 0.1).all()
+
+
+def _device_settled(spec, o2, stress, steps=600):
+    net = cw.Network.from_spec(spec, 100)
+    st = net.initial.reshape(1, -1).copy()
+    net.step_batch(st, np.array([[o2, 0.2, 0, stress, 0, 0]], float), 1.0, steps)
+    return st[0]
+
+
+def test_the_fuller_cell_decides_as_the_networks_it_fills_in_on_the_device(golden):
+    # crates/io/tests/fuller_cell.rs:69-136, settled by 600 RK4 steps on the
+    # device; each settled state equals the oracle's, and the decisions match
+    nets = golden["networks"]
+    ref = {k: O.compile_network(nets[k], 100) for k in ("fuller-cell", "ras-erk", "stress-response")}
+    got = {}
+    for k in ref:
+        for o2, stress in [(1.0, 0.0), (0.1, 0.0), (0.05, 0.0), (1.0, 0.5), (1.0, 1.0)]:
+            dev = _device_settled(nets[k], o2, stress)
+            want = ref[k].initial.reshape(1, -1).copy()
+            O.network_step(ref[k], want, np.array([[o2, 0.2, 0, stress, 0, 0]], float), 1.0, 600)
+            # Hill terms through pow: a few ulps a step, damped as the state settles
+            np.testing.assert_allclose(dev, want[0], rtol=1e-10, atol=1e-12)
+            got[k, o2, stress] = dev
+    f, r, s = ref["fuller-cell"], ref["ras-erk"], ref["stress-response"]
+    erk = lambda net, st: st[net.names.index("erk")]
+    assert abs(erk(f, got["fuller-cell", 1.0, 0.0]) - erk(r, got["ras-erk", 1.0, 0.0])) < 0.002
+    for o2 in (0.1, 0.05):
+        assert abs(got["fuller-cell", o2, 0.0][f.survival] - got["ras-erk", o2, 0.0][r.survival]) < 0.002
+    for stress in (0.5, 1.0):
+        a = got["fuller-cell", 1.0, stress][f.optional["apoptosis"]]
+        b = got["stress-response", 1.0, stress][s.optional["apoptosis"]]
+        assert abs(a - b) < 0.015
+
+
+def test_one_node_inputs_reach_the_device_as_the_reference_reads_them():
+    # network.rs:1268-1342, 1445-1482: waste, the necrotic factor past its
+    # threshold, a node at zero not damaged below it, crowding read by a
+    # differentiation node
+    def one(terms, initial=0.0):
+        return {"nodes": [{"name": "a", "initial": initial, "terms": terms}],
+                "roles": {"growth": "a", "survival": "a", "hypoxia_response": "a"},
+                "mechanics": {"growth_coefficient": 1.0, "lambda_volume": 1.0}}
+
+    def run(spec, inputs, dt, steps):
+        net = cw.Network.from_spec(spec, 100)
+        st = net.initial.reshape(1, -1).copy()
+        net.step_batch(st, np.array([inputs], float), dt, steps)
+        return st[0, 0]
+    slope = (run(one([{"kind": "activated_by", "source": "waste", "rate": 2.0}], 0.25),
+                 [1, 0, 0, 0, 0.5, 0], 1e-6, 1) - 0.25) / 1e-6
+    assert abs(slope - 0.75) < 1e-5
+    above = one([{"kind": "damaged_above", "source": "necrotic_factor", "threshold": 0.5, "rate": 2.0}], 0.5)
+    assert abs((run(above, [1, 0, 0, 0, 0, 0.4], 1e-6, 1) - 0.5) / 1e-6) < 1e-9
+    assert abs((run(above, [1, 0, 0, 0, 0, 1.0], 1e-6, 1) - 0.5) / 1e-6 + 2.0) < 1e-5
+    below = one([{"kind": "damaged_below", "source": "oxygen", "threshold": 0.5, "rate": 10.0}])
+    assert run(below, [0, 0, 0, 0, 0, 0], 1.0, 50) == 0.0
+    crowd = one([{"kind": "activated_by", "source": "crowding", "rate": 1.0}, {"kind": "decays", "rate": 1.0}])
+    crowd["roles"]["differentiation"] = "a"
+    assert abs(run(crowd, [1, 0, 0.6, 0, 0, 0], 1.0, 40) - 0.6 / 1.6) < 1e-6

@@ -99,6 +99,61 @@ def test_hill_inhibition_is_half_at_k():
         assert check((st[0, 0] - 0.5) / 1e-6)
 
 
+def _slope(term, initial, inputs, dt=1e-6):
+    net = O.compile_network(one_node([term], initial), 100)
+    st = net.initial.copy().reshape(1, -1)
+    O.network_step(net, st, np.array([inputs], float), dt, 1)
+    return (st[0, 0] - initial) / dt
+
+
+def test_a_node_reads_the_waste_and_the_necrotic_factor_around_its_cell():
+    # network.rs:1268-1316; inputs: oxygen, egf, crowding, stress, waste, necrotic factor
+    waste = _slope({"kind": "activated_by", "source": "waste", "rate": 2.0}, 0.25, [1, 0, 0, 0, 0.5, 0])
+    assert abs(waste - 2.0 * 0.5 * 0.75) < 1e-5
+    above = {"kind": "damaged_above", "source": "necrotic_factor", "threshold": 0.5, "rate": 2.0}
+    assert abs(_slope(above, 0.5, [1, 0, 0, 0, 0, 0.4])) < 1e-9
+    assert abs(_slope(above, 0.5, [1, 0, 0, 0, 0, 1.0]) + 2.0) < 1e-5
+
+
+def test_a_node_at_zero_cannot_be_damaged_below_zero():
+    # network.rs:1327-1342
+    net = O.compile_network(one_node([{"kind": "damaged_below", "source": "oxygen", "threshold": 0.5,
+                                       "rate": 10.0}], 0.0), 100)
+    st = net.initial.copy().reshape(1, -1)
+    O.network_step(net, st, np.zeros((1, 6)), 1.0, 50)
+    assert st[0, 0] == 0.0
+
+
+def test_decay_pulls_a_node_down_and_a_hill_term_switches_more_sharply():
+    # network.rs:1344-1377
+    net = O.compile_network(one_node([{"kind": "decays", "rate": 1.0}], 1.0), 100)
+    st = net.initial.copy().reshape(1, -1)
+    O.network_step(net, st, np.zeros((1, 6)), 0.1, 1)
+    assert 0.85 < st[0, 0] < 1.0
+
+    def run(n, egf):
+        term = {"kind": "activated_by", "source": "egf", "rate": 10.0, "hill": {"n": n, "k": 0.5}}
+        net = O.compile_network(one_node([term]), 100)
+        st = net.initial.copy().reshape(1, -1)
+        O.network_step(net, st, np.array([[0, egf, 0, 0, 0, 0]], float), 0.1, 200)
+        return st[0, 0]
+    assert run(8.0, 0.3) < run(1.0, 0.3) and run(8.0, 0.7) > run(1.0, 0.7)
+
+
+def test_a_crowded_cell_answers_with_its_differentiation_node(golden):
+    # network.rs:1445-1482: k c (1 - a) = a settles at a = c / (1 + c)
+    spec = one_node([{"kind": "activated_by", "source": "crowding", "rate": 1.0}, {"kind": "decays", "rate": 1.0}])
+    spec["roles"] = dict(spec["roles"], differentiation="a")
+    net = O.compile_network(spec, 100)
+    st = net.initial.copy().reshape(1, -1)
+    O.network_step(net, st, np.array([[1.0, 0, 0.6, 0, 0, 0]]), 1.0, 40)
+    assert abs(st[0, net.optional["differentiation"]] - 0.6 / 1.6) < 1e-6
+    spec["roles"]["differentiation"] = "nowhere"
+    with pytest.raises(O.NetworkConfigError):
+        O.compile_network(spec, 100)
+    assert O.compile_network(golden["networks"]["ras-erk"], 100).optional["differentiation"] == -1
+
+
 @pytest.mark.parametrize("spec,fragment", [
     (one_node([{"kind": "activated_by", "source": "p53", "rate": 1.0}]), "p53"),
     ({**one_node([]), "roles": {"growth": "a", "survival": "bcl2", "hypoxia_response": "a"}}, "bcl2"),
