@@ -60,6 +60,11 @@ def parse():
     p.add_argument("--no-fit", action="store_true")
     p.add_argument("--fit-iters", type=int, default=10)
     p.add_argument("--no-shapes", action="store_true")
+    p.add_argument("--tolerance", type=float, default=None,
+                   help="the field solves' residual stop (default: the workload's)")
+    p.add_argument("--error-tolerance", type=float, default=None,
+                   help="also stop a solve only once its estimated error is below this times the field's largest "
+                        "value (default: the workload's)")
     p.add_argument("--profile-step", action="store_true",
                    help="bracket one extra step with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     return p.parse_args()
@@ -92,8 +97,11 @@ def job_rate(world, histories, steps, ms):
 
 def config_key(name, cfg):
     if name == "campaign":
+        stop = f"residual {cfg['tolerance']:g}"
+        if cfg.get("error_tolerance"):
+            stop += f" and estimated error {cfg['error_tolerance']:g}"
         return {"workload": "batched campaign: 64 histories, 16 each at 128^2/256^2/512^2/1024^2, 30% fill at "
-                            "target 49, Moore contact, 2 fields to residual 1e-8 (FP32 SOR + FP64 defect "
+                            f"target 49, Moore contact, 2 fields to {stop} (FP32 SOR + FP64 defect "
                             "correction; each field within 1e-6 of its FP64 solution), 8-species RK4 x8 per MCS", "histories": len(cfg["dims"]),
                 "sites": int(sum(w * h * d for w, h, d in cfg["dims"])), "cells": int(sum(cfg["ncells"])),
                 "l2": "inputs larger than L2 (the lattices and fields of one step exceed 126 MB)",
@@ -250,6 +258,10 @@ def run_ours(args, rank, world, dist):
     local = int(os.environ.get("LOCAL_RANK", "0"))
     _lib.check(L.cw_set_device(local))
     cfg = workload(args.workload, rank)
+    if args.tolerance is not None:
+        cfg["tolerance"] = args.tolerance
+    if args.error_tolerance is not None:
+        cfg["error_tolerance"] = args.error_tolerance
     S = cfg.pop("S")
     net = network_for(S, S, cfg["target_volume"])
     nh = len(cfg["dims"])
