@@ -62,6 +62,8 @@ def parse():
     p.add_argument("--no-shapes", action="store_true")
     p.add_argument("--tolerance", type=float, default=None,
                    help="the field solves' residual stop (default: the workload's)")
+    p.add_argument("--inner-sweeps", type=int, default=None,
+                   help="FP32 sweeps per FP64 correction (default: the library's, 64)")
     p.add_argument("--error-tolerance", type=float, default=None,
                    help="also stop a solve only once its estimated error is below this times the field's largest "
                         "value (default: the workload's)")
@@ -262,6 +264,8 @@ def run_ours(args, rank, world, dist):
         cfg["tolerance"] = args.tolerance
     if args.error_tolerance is not None:
         cfg["error_tolerance"] = args.error_tolerance
+    if args.inner_sweeps is not None:
+        cfg["inner_sweeps"] = args.inner_sweeps
     S = cfg.pop("S")
     net = network_for(S, S, cfg["target_volume"])
     nh = len(cfg["dims"])

@@ -452,7 +452,7 @@ typedef struct {
     double tolerance;            /* residual tolerance of every field solve */
     int32_t precision;           /* CW_FP64 or CW_FP32_DC */
     double omega;                /* <= 0: chosen by the autotuner (CW_FP32_DC) or the reference's rule */
-    int32_t inner_sweeps;        /* CW_FP32_DC: FP32 sweeps per defect correction (0: 32 in the plane, 64 in volumes) */
+    int32_t inner_sweeps;        /* CW_FP32_DC: FP32 sweeps per defect correction (0: 64) */
     int32_t relax_every;         /* solve the fields every this many steps (1: each) */
     double dt;                   /* network time step */
     int32_t substeps;            /* RK4 steps per lattice step */
