@@ -33,6 +33,11 @@ def test_the_binding_covers_every_declared_symbol():
     assert sorted(set(declared()) - set(_lib.SIGNATURES)) == []
 
 
+def test_the_integration_guide_maps_every_declared_symbol():
+    guide = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    assert [n for n in declared() if not re.search(r"\b%s\b" % n, guide)] == []
+
+
 def test_without_a_device_calls_fail_loudly():
     import cellweave_b200 as cw
     try:
