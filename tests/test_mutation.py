@@ -172,3 +172,13 @@ def test_fluid_shut_in_is_closed_in_by_the_living_only():
     assert all(g[y, x] in (1, 2, 3) for x, y in closed)
     assert int(hist.lat.volume.sum()) == before + len(want)
     assert np.array_equal(np.bincount(hist.lat.grid.clip(0), minlength=5)[1:], hist.lat.volume[1:])
+
+
+def test_an_exposure_is_on_when_its_schedule_says():
+    # crates/io/tests/stress.rs:71-84 on the oracle's Exposure::level_at
+    from oracle import cpu_sim
+    hist = cpu_sim.CpuHistory.__new__(cpu_sim.CpuHistory)
+    hist.cfg = {"exposure_intensity": 0.8, "exposure_start": 10, "exposure_on": 3, "exposure_off": 2}
+    assert [hist._level_at(m) for m in range(8, 20)] == [0, 0, .8, .8, .8, 0, 0, .8, .8, .8, 0, 0]
+    hist.cfg = {"exposure_intensity": 1.0, "exposure_start": 5, "exposure_on": 0, "exposure_off": 0}
+    assert hist._level_at(4) == 0.0 and hist._level_at(500) == 1.0
