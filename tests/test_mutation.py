@@ -182,3 +182,14 @@ def test_an_exposure_is_on_when_its_schedule_says():
     assert [hist._level_at(m) for m in range(8, 20)] == [0, 0, .8, .8, .8, 0, 0, .8, .8, .8, 0, 0]
     hist.cfg = {"exposure_intensity": 1.0, "exposure_start": 5, "exposure_on": 0, "exposure_off": 0}
     assert hist._level_at(4) == 0.0 and hist._level_at(500) == 1.0
+
+
+def test_a_sheet_fills_the_box_with_one_cell_per_square():
+    # crates/io/tests/epithelium.rs:68-81 on the oracle's seeding: a 40 x 40
+    # box tiled by 10 x 10 cells of normal tissue, no medium, 16 cells
+    from oracle import cpu_sim
+    cfg = {"seeding": 4, "seed_side": 10, "J": np.zeros((4, 4))}
+    grid, types = cpu_sim.seed_history(cfg, 40, 40, 1, 0, 1)
+    assert (grid != 0).all() and len(types) == 17 and (types[1:] == 2).all()
+    assert sorted(np.bincount(grid.reshape(-1))[1:]) == [100] * 16
+    assert grid[0, 0, 0] == 1 and grid[0, 0, 39] == 4 and grid[0, 39, 0] == 13
