@@ -82,6 +82,19 @@ def workload(name, rank=0):
     return cfg
 
 
+def configured(args, rank=0):
+    """The workload with the solve options given on the command line, the
+    same for every arm."""
+    cfg = workload(args.workload, rank)
+    if args.tolerance is not None:
+        cfg["tolerance"] = args.tolerance
+    if args.error_tolerance is not None:
+        cfg["error_tolerance"] = args.error_tolerance
+    if args.inner_sweeps is not None:
+        cfg["inner_sweeps"] = args.inner_sweeps
+    return cfg
+
+
 def max_over_ranks(x, dist, device):
     """The largest x over the ranks (every rank calls it, in the same order)."""
     if dist is None:
@@ -259,13 +272,7 @@ def run_ours(args, rank, world, dist):
     L = _lib.lib()
     local = int(os.environ.get("LOCAL_RANK", "0"))
     _lib.check(L.cw_set_device(local))
-    cfg = workload(args.workload, rank)
-    if args.tolerance is not None:
-        cfg["tolerance"] = args.tolerance
-    if args.error_tolerance is not None:
-        cfg["error_tolerance"] = args.error_tolerance
-    if args.inner_sweeps is not None:
-        cfg["inner_sweeps"] = args.inner_sweeps
+    cfg = configured(args, rank)
     S = cfg.pop("S")
     net = network_for(S, S, cfg["target_volume"])
     nh = len(cfg["dims"])
@@ -599,7 +606,7 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return 0
-        cfg = workload(args.workload)
+        cfg = configured(args)
         cores = os.cpu_count() or 1
         v, detail, sample = cpu_sample(cfg, cores)
         line = dict(base, impl="reference", value=v, ms_per_step=1e3 * len(cfg["dims"]) / v,
@@ -622,7 +629,7 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         # the CPU leg first, before any GPU context exists in this process
-        cfg = workload(args.workload)
+        cfg = configured(args)
         cores = os.cpu_count() or 1
         v, detail, sample = cpu_sample(cfg, cores)
         cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample, "detail": detail}
