@@ -435,6 +435,9 @@ TERM_KINDS = ["activated_by", "inhibited_by", "activated_by_absence_of", "produc
               "damaged_below", "damaged_above"]
 
 
+MECHANICS_KEYS = ("growth_coefficient", "lambda_volume", "max_target")
+
+
 def load_network_spec(path: str, _seen=()) -> dict:
     """load_network_chain (crates/io/src/config.rs:416-447): a network file and
     everything it `extends`, youngest laid over oldest by merge_onto
@@ -450,6 +453,12 @@ def load_network_spec(path: str, _seen=()) -> dict:
         raise ConfigError(f"reading the network {path}: {e}") from e
     except tomllib.TOMLDecodeError as e:
         raise ConfigError(f"{path} is not a network: {e}") from e
+    # MechanicsSpec refuses a key it does not read (crates/core/src/network.rs:207-230):
+    # a contact energy is the lattice's, not a network's
+    for key in (spec.get("mechanics") or {}):
+        if key not in MECHANICS_KEYS:
+            raise ConfigError(f"{path}: unknown field `{key}` in the mechanics, expected one of "
+                              f"{', '.join(MECHANICS_KEYS)}")
     parent = spec.get("extends")
     if parent is None:
         spec.pop("extends", None)

@@ -191,3 +191,57 @@ def test_the_example_shaped_scenarios_load(tmp_path):
     kw, _ = C.simulation_kwargs(C.load_sim_config(str(tmp_path / "spheroid3d.toml")))
     assert kw["debris_loss"] == 0.024 and kw["still_medium"] == 0.606 and kw["cycle_median"] == 20.0
     assert kw["dims"] == [(320, 320, 320)] and kw["max_cells"] == 200000 and kw["sweeps"] == 4
+
+
+# crates/io/src/config.rs:702-866: a network file and the chain it extends
+EXT_BASE = ('[[nodes]]\nname = "a"\ninitial = 0.1\nterms = [ { kind = "decays", rate = 0.5 } ]\n\n'
+            '[[nodes]]\nname = "b"\ninitial = 0.2\n\n'
+            '[roles]\ngrowth = "a"\nsurvival = "b"\nhypoxia_response = "b"\n\n'
+            '[mechanics]\ngrowth_coefficient = 1.0\nlambda_volume = 2.0\n')
+
+
+def test_extending_replaces_a_node_whole_appends_new_ones_and_inherits_the_rest(tmp_path):
+    (tmp_path / "base.toml").write_text(EXT_BASE)
+    (tmp_path / "child.toml").write_text('extends = "base.toml"\n\n[[nodes]]\nname = "a"\ninitial = 0.9\nterms = []\n')
+    spec = cw.load_network_spec(str(tmp_path / "child.toml"))
+    assert [n["name"] for n in spec["nodes"]] == ["a", "b"]
+    assert spec["nodes"][0]["initial"] == 0.9 and spec["nodes"][0]["terms"] == []
+    assert spec["nodes"][1]["initial"] == 0.2
+    assert spec["roles"]["survival"] == "b" and spec["mechanics"]["lambda_volume"] == 2.0
+    assert spec.get("extends") is None
+    (tmp_path / "more.toml").write_text('extends = "base.toml"\n\n[[nodes]]\nname = "c"\ninitial = 0.3\n')
+    assert [n["name"] for n in cw.load_network_spec(str(tmp_path / "more.toml"))["nodes"]] == ["a", "b", "c"]
+
+
+def test_a_chain_of_three_is_laid_youngest_over_oldest(tmp_path):
+    (tmp_path / "base.toml").write_text(EXT_BASE)
+    (tmp_path / "middle.toml").write_text('extends = "base.toml"\n\n[[nodes]]\nname = "a"\ninitial = 0.5\n')
+    (tmp_path / "top.toml").write_text('extends = "middle.toml"\n\n[[nodes]]\nname = "b"\ninitial = 0.7\n')
+    spec = cw.load_network_spec(str(tmp_path / "top.toml"))
+    assert spec["nodes"][0]["initial"] == 0.5 and spec["nodes"][1]["initial"] == 0.7
+
+
+def test_a_loop_and_a_contact_energy_in_a_network_are_refused(tmp_path):
+    (tmp_path / "one.toml").write_text('extends = "two.toml"\n')
+    (tmp_path / "two.toml").write_text('extends = "one.toml"\n')
+    with pytest.raises(cw.ConfigError, match="loop") as e:
+        cw.load_network_spec(str(tmp_path / "one.toml"))
+    assert "one.toml" in str(e.value) and "two.toml" in str(e.value)
+    (tmp_path / "base.toml").write_text(EXT_BASE)
+    (tmp_path / "sticky.toml").write_text('extends = "base.toml"\n\n[mechanics]\ngrowth_coefficient = 1.0\n'
+                                          'lambda_volume = 2.0\nj_medium = 16.0\n')
+    with pytest.raises(cw.ConfigError, match="j_medium"):
+        cw.load_network_spec(str(tmp_path / "sticky.toml"))
+    (tmp_path / "lonely.toml").write_text('[[nodes]]\nname = "a"\n')
+    lonely = cw.load_network_spec(str(tmp_path / "lonely.toml"))
+    assert lonely.get("roles") is None and lonely.get("mechanics") is None
+    with pytest.raises(cw.ConfigError, match="no roles"):
+        cw.Network.from_spec(lonely, 100)
+
+
+def test_the_shipped_mutant_differs_from_its_base_in_one_node(golden):
+    # config.rs:866-898 on the networks the fixtures carry
+    mutant, base = golden["networks"]["ras-erk-mutant"], golden["networks"]["ras-erk"]
+    assert len(mutant["nodes"]) == len(base["nodes"])
+    assert [m["name"] for m, b in zip(mutant["nodes"], base["nodes"]) if m != b] == ["ras"]
+    assert mutant["roles"] == base["roles"] and mutant["mechanics"] == base["mechanics"]
