@@ -245,3 +245,12 @@ def test_the_shipped_mutant_differs_from_its_base_in_one_node(golden):
     assert len(mutant["nodes"]) == len(base["nodes"])
     assert [m["name"] for m, b in zip(mutant["nodes"], base["nodes"]) if m != b] == ["ras"]
     assert mutant["roles"] == base["roles"] and mutant["mechanics"] == base["mechanics"]
+
+
+def test_a_missing_network_file_is_reported_with_its_path(tmp_path):
+    # config.rs:681-692
+    with pytest.raises(cw.ConfigError, match="nowhere/at/all.toml"):
+        cw.load_network_spec(str(tmp_path / "nowhere" / "at" / "all.toml"))
+    cfg = C.load_sim_config(write(tmp_path, BASE.replace('"net.toml"', '"nowhere/at/all.toml"'), net=False))
+    with pytest.raises(cw.ConfigError, match="nowhere/at/all.toml"):
+        cw.load_network_spec(cfg["network_path"])
