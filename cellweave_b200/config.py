@@ -211,7 +211,12 @@ def simulation_kwargs(cfg, histories=1, seeds=None, subsweeps=4):
         cy = cfg["cycle"]
         if "median" not in cy or "spread" not in cy:
             raise ConfigError(f"{os.path.basename(cfg['path'])}: a cycle names its median and its spread")
-        kw.update(cycle_median=float(cy["median"]), cycle_spread=float(cy["spread"]), divide_every=1)
+        median, spread = float(cy["median"]), float(cy["spread"])
+        # simulation.rs:522-530
+        if not (math.isfinite(median) and median >= 1.0 and math.isfinite(spread) and spread >= 0.0):
+            raise ConfigError(f"{os.path.basename(cfg['path'])}: the cycle's median is {median} steps and its "
+                              f"spread {spread}; a cycle lasts a step at least, and its spread is not below zero")
+        kw.update(cycle_median=median, cycle_spread=spread, divide_every=1)
     if cfg.get("exposure"):
         kw.update(_exposure(cfg))
     if cfg.get("debris_loss") is not None:

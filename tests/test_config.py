@@ -254,3 +254,21 @@ def test_a_missing_network_file_is_reported_with_its_path(tmp_path):
     cfg = C.load_sim_config(write(tmp_path, BASE.replace('"net.toml"', '"nowhere/at/all.toml"'), net=False))
     with pytest.raises(cw.ConfigError, match="nowhere/at/all.toml"):
         cw.load_network_spec(cfg["network_path"])
+
+
+def test_a_cycle_lasts_a_step_at_least_and_spreads_by_something(tmp_path):
+    # simulation.rs:2849-2866
+    for median, spread in [("0.5", "0.2"), ("20.0", "-0.1"), ("nan", "0.2"), ("20.0", "inf")]:
+        text = BASE + f"\n[cycle]\nmedian = {median}\nspread = {spread}\n"
+        with pytest.raises(cw.ConfigError, match="a cycle lasts a step at least"):
+            C.simulation_kwargs(C.load_sim_config(write(tmp_path, text)))
+
+
+def test_the_oracles_cycle_lengths_have_the_median_and_spread_asked_for():
+    # simulation.rs:2868-2888: 4000 draws of median 40, spread 0.3
+    from oracle import cpu_sim
+    hist = cpu_sim.CpuHistory.__new__(cpu_sim.CpuHistory)
+    hist.cfg, hist.div_rng = {"cycle_median": 40.0, "cycle_spread": 0.3}, np.random.default_rng(7)
+    logs = np.sort(np.log([hist._cycle_length() for _ in range(4000)]))
+    assert abs(np.exp(logs[len(logs) // 2]) - 40.0) < 2.0
+    assert abs(logs.std() - 0.3) < 0.03
