@@ -150,6 +150,10 @@ def _refuse(cfg):
         raise ConfigError(f"{name}: `suppress` is not part of the device step (its mutations are all made)")
     if not 0.0 <= float(cfg["mutation_rate"]) <= 1.0 or not 0.0 <= float(cfg["rewiring"]) <= 1.0:
         raise ConfigError(f"{name}: mutation_rate and rewiring are chances, in [0, 1]")
+    if int(cfg["sweeps_per_step"]) < 1:
+        # simulation.rs:511-514
+        raise ConfigError(f"{name}: sweeps_per_step is {cfg['sweeps_per_step']}; a step sweeps the lattice at "
+                          "least once")
     if cfg["contact_order"] not in (1, 2, 3):
         raise ConfigError(f"{name}: contact_order is {cfg['contact_order']}; it is 1, 2 or 3")
     if cfg["network"] is None:
@@ -220,7 +224,12 @@ def simulation_kwargs(cfg, histories=1, seeds=None, subsweeps=4):
     if cfg.get("exposure"):
         kw.update(_exposure(cfg))
     if cfg.get("debris_loss") is not None:
-        kw["debris_loss"] = float(cfg["debris_loss"])
+        loss = float(cfg["debris_loss"])
+        # simulation.rs:543-550
+        if not (math.isfinite(loss) and 0.0 < loss <= 1.0):
+            raise ConfigError(f"{os.path.basename(cfg['path'])}: debris loss is {loss}; it is the share of a "
+                              "dead cell lost per step, above zero and at most one")
+        kw["debris_loss"] = loss
     if cfg.get("still_medium"):
         if "diffusion" not in cfg["still_medium"]:
             raise ConfigError(f"{os.path.basename(cfg['path'])}: a still medium names its diffusion")

@@ -272,3 +272,12 @@ def test_the_oracles_cycle_lengths_have_the_median_and_spread_asked_for():
     logs = np.sort(np.log([hist._cycle_length() for _ in range(4000)]))
     assert abs(np.exp(logs[len(logs) // 2]) - 40.0) < 2.0
     assert abs(logs.std() - 0.3) < 0.03
+
+
+def test_a_debris_loss_is_a_share_per_step_and_a_step_sweeps_at_least_once(tmp_path):
+    # simulation.rs:3085-3103
+    for loss in ("0.0", "-0.1", "1.5", "nan"):
+        with pytest.raises(cw.ConfigError, match="debris loss"):
+            C.simulation_kwargs(C.load_sim_config(write(tmp_path, f"debris_loss = {loss}\n" + BASE)))
+    with pytest.raises(cw.ConfigError, match="at least once"):
+        C.simulation_kwargs(C.load_sim_config(write(tmp_path, "sweeps_per_step = 0\n" + BASE)))
