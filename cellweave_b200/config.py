@@ -56,6 +56,7 @@ OXYGEN_TOLERANCE = 0.01      # simulation.rs:85
 NETWORK_TIME_PER_MCS = 8     # simulation.rs:115
 DEATH_THRESHOLD = 0.25       # simulation.rs:118
 DIVISION_CHECK_EVERY = 20    # simulation.rs:55
+DIVISION_RATIO = 1.4         # simulation.rs:45
 OXYGEN_WARMUP_TOLERANCE = 1e-8  # simulation.rs:95
 FIRST_CELL_RADIUS = 8        # simulation.rs:65
 FIRST_CELL_RADIUS_3D = 3     # simulation.rs:74
@@ -274,7 +275,13 @@ def _exposure(cfg):
 def simulation_from_config(cfg, histories=1, seeds=None, subsweeps=4):
     """(Simulation, Network) for a configuration read by load_sim_config."""
     kw, refvol = simulation_kwargs(cfg, histories, seeds, subsweeps)
-    net = Network.from_spec(load_network_spec(cfg["network_path"]), refvol)
+    spec = load_network_spec(cfg["network_path"])
+    cap = (spec.get("mechanics") or {}).get("max_target")
+    if cap is not None and not float(cap) >= DIVISION_RATIO:
+        # simulation.rs:621-628
+        raise ConfigError(f"{os.path.basename(cfg['path'])}: the network caps a cell's target at {cap} times its "
+                          f"reference size, and a cell divides at {DIVISION_RATIO}; no cell could ever divide")
+    net = Network.from_spec(spec, refvol)
     kw["lambda_volume"] = _network_lambda(cfg)
     sim = Simulation(net, **kw)
     if cfg.get("lesion") is not None:

@@ -281,3 +281,11 @@ def test_a_debris_loss_is_a_share_per_step_and_a_step_sweeps_at_least_once(tmp_p
             C.simulation_kwargs(C.load_sim_config(write(tmp_path, f"debris_loss = {loss}\n" + BASE)))
     with pytest.raises(cw.ConfigError, match="at least once"):
         C.simulation_kwargs(C.load_sim_config(write(tmp_path, "sweeps_per_step = 0\n" + BASE)))
+
+
+def test_a_ceiling_below_the_division_ratio_is_refused(tmp_path):
+    # simulation.rs:3416-3423 (the check, 621-628), before anything reaches the device
+    path = write(tmp_path, BASE)
+    (tmp_path / "net.toml").write_text(NET + "max_target = 1.2\n")
+    with pytest.raises(cw.ConfigError, match="no cell could ever divide"):
+        C.simulation_from_config(C.load_sim_config(path))
